@@ -1,0 +1,192 @@
+/*
+ * mf3d.h - C ABI of the B200 pressure-Poisson multigrid library.
+ *
+ * The library replaces MultiFlow3D's projection step: `newsolv_mg`
+ * (newsolv_mg.for:2-102) with the V-cycle it drives (`coeff`, `mgkcyc`,
+ * `mgrelax`, `mgrestr`, `mgcorr`, `mgbound` in mgsolver.for:2-992), the
+ * multigrid halo copies (`exchangepp`, `exchbc_mgpp` in exchangepp.for), and
+ * the FP64 projection kernels `calvel`, `calmas`, `pbound` (press.for:2-200)
+ * with the field halos `exchange(1..4)` (exchange.for, exchange_bc.for).
+ *
+ * All blocks of one solve live on one GPU.  Plain pointers and sizes only:
+ * no CUDA or torch types cross this boundary.  Every function returns an
+ * `int` status (enum mf3d_status); the library never exits the process
+ * (the reference `stop`s at newsolv_mg.for:82 and localparameters.for:205).
+ *
+ * Array layout of the field arguments (`mf3d_fields`): Fortran column-major
+ * `(ttc_i, ttc_j, ttc_k)`, i fastest, with `pl` ghost layers on each side,
+ * ttc_i = nx + 2*pl (localparameters.for:138-140).  Cell (i,j,k) of the
+ * reference (1-based) is element (i-1) + ttc_i*((j-1) + ttc_j*(k-1)).
+ * The staggered velocity u(i,j,k) sits on the east face of cell (i,j,k).
+ */
+#ifndef MF3D_H
+#define MF3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MF3D_ABI_VERSION 1
+
+/* Status codes.  Non-negative = the solve ran; negative = it did not. */
+enum mf3d_status {
+  MF3D_OK = 0,
+  MF3D_NOT_CONVERGED = 1, /* maxcy exhausted (newsolv_mg.for:59-60 prints) */
+  MF3D_DIVERGED = 2,      /* rmax > 100 (newsolv_mg.for:64-83 stops)      */
+  MF3D_E_INVALID = -1,    /* bad config (localparameters.for:84-98,201-206)*/
+  MF3D_E_CUDA = -2,       /* a CUDA runtime call failed                     */
+  MF3D_E_OOM = -3,        /* device allocation failed or over the cap       */
+  MF3D_E_TIMEOUT = -4,    /* a bounded device wait gave up                  */
+  MF3D_E_NONFINITE = -5,  /* NaN/Inf met in the residual                     */
+  MF3D_E_UNSUPPORTED = -6 /* a reference feature outside this build (LMR,
+                             L_LSM variable density, differencing=3)       */
+};
+
+/* Boundary-condition code meaning "periodic" (control.cin:17-22). Any other
+ * code on a face with no neighbour block is a homogeneous Neumann face for
+ * the pressure (mgbound, mgsolver.for:931-986; pbound, press.for:90-133). */
+#define MF3D_BC_PERIODIC 5
+
+/* Precision of the multigrid V-cycle.  The outer defect-correction loop
+ * (calvel / calmas / p += pp) is always FP64. */
+enum mf3d_precision {
+  MF3D_PREC_FP64 = 0, /* the reference's arithmetic, bit-exact              */
+  MF3D_PREC_FP32 = 1, /* FP32 smoother/transfer, FP32 correction storage    */
+  MF3D_PREC_BF16 = 2  /* FP32 arithmetic, BF16 storage of the correction    */
+};
+
+/* One block (reference `type multidom`, module_multidata.for:15-122): the
+ * fields the projection path reads.  Neighbour ids are block ids (dom_id),
+ * -1 = none, exactly as alloc_dom.for:456-1150 sets them. */
+typedef struct mf3d_block_desc {
+  int id;                  /* dom_id, 0-based, unique                       */
+  int nx, ny, nz;          /* interior cells: iep-isp+1, jep-jsp+1, kep-ksp+1 */
+  double dx, dy, dz;       /* uniform spacing (localparameters.for:245-247) */
+  double xsl, xel, ysl, yel, zsl, zel; /* block extents (infodom.cin)       */
+  int iprev, inext, jprev, jnext, kprev, knext;   /* face neighbours      */
+  int corprev[4], cornext[4];                     /* corner neighbours    */
+  int edgprev[6], edgnext[6];                     /* edge neighbours      */
+  int per_ip, per_in, per_jp, per_jn, per_kp, per_kn; /* periodic partners */
+  int bc_west, bc_east, bc_south, bc_north, bc_bottom, bc_top;
+  /* Optional non-uniform cell widths (length nx / ny / nz).  NULL = uniform
+   * spacing dx/dy/dz.  This is an extension with no reference counterpart:
+   * the reference grid is uniform per block (localparameters.for:245-247). */
+  const double *hx, *hy, *hz;
+} mf3d_block_desc;
+
+/* Solver parameters: the control.cin fields the projection path reads
+ * (initial.for:21-26). */
+typedef struct mf3d_params {
+  int ngrid;        /* multigrid levels ngrd_gl (control.cin:10)             */
+  int mg_itrsch;    /* smoother: 1 lexicographic GS, 2 line TDMA, 3 RB GS    */
+  int irestr;       /* pre-smoothing sweeps ("restriction iter")             */
+  int iproln;       /* post-smoothing sweeps ("prolongation iter")           */
+  int maxcy;        /* maximum outer iterations per solve                    */
+  double eps;       /* stopping tolerance on rmax (newsolv_mg.for:56)        */
+  int eps_relative; /* 0: rmax < eps (reference); 1: rmax < eps * rmax_0     */
+  int pl;           /* ghost layers of the field arrays (localparameters.for:17-24) */
+  int differencing; /* 1 = 2nd-order divergence in calmas (press.for:38-67)  */
+  int precision;    /* enum mf3d_precision                                   */
+  int device;       /* CUDA device ordinal                                   */
+} mf3d_params;
+
+/* Field pointers of one block, each a (ttc_i,ttc_j,ttc_k) array.
+ * ustar/vstar/wstar: in.  p: in/out.  u/v/w: in (faces on physical walls,
+ * which calvel never writes) and out (all faces calvel writes).  For the host
+ * entry point these are host pointers; for the `_device` one, device pointers.
+ * `su` may be NULL; if set it receives the final RHS div(u)/dt (calmas). */
+typedef struct mf3d_fields {
+  double *ustar, *vstar, *wstar;
+  double *u, *v, *w;
+  double *p;
+  double *su;
+} mf3d_fields;
+
+typedef struct mf3d_ctx mf3d_ctx;
+
+/* Result of one projection call. */
+typedef struct mf3d_solve_info {
+  double rmax;       /* final rmax (module vars `rmax`)                        */
+  double rmax0;      /* rmax after the initial calvel/calmas                   */
+  int iter;          /* outer iterations run (module vars `iter`)              */
+  int status;        /* same as the return value                               */
+  double ms_device;  /* device time of the solve in milliseconds               */
+} mf3d_solve_info;
+
+/* ---------------------------------------------------------------------- */
+/* Set-up.                                                                  */
+/* ---------------------------------------------------------------------- */
+
+/* Neighbour search of alloc_dom.for:456-1150 (faces 465-628, corners
+ * 632-750, edges 752-968, periodic partners 971-1150) over block extents.
+ * `extents` holds 6 doubles per block (xsl,xel,ysl,yel,zsl,zel); `bc6` the
+ * six global BC codes (W,E,S,N,B,T); dx,dy,dz the uniform spacing.  Fills
+ * ids, nx/ny/nz, spacing and all neighbour fields of `out[nblocks]`. */
+int mf3d_build_topology(int nblocks, const double *extents, const int *bc6,
+                        double dx, double dy, double dz,
+                        mf3d_block_desc *out);
+
+/* Allocate device state for a solve over `nblocks` blocks: the multigrid
+ * hierarchy (replaces `coeff`, mgsolver.for:2-222, and the `cof` storage of
+ * localparameters.for:208-237), halo maps, field mirrors and streams.
+ * Checks the divisibility rule of localparameters.for:200-206. */
+int mf3d_create(const mf3d_block_desc *blocks, int nblocks,
+                const mf3d_params *params, mf3d_ctx **ctx);
+
+int mf3d_destroy(mf3d_ctx *ctx);
+
+/* ---------------------------------------------------------------------- */
+/* The projection (newsolv_mg.for:2-102).                                  */
+/* ---------------------------------------------------------------------- */
+
+/* Host-array entry point: the drop-in for `newsolv_mg`.  `fields[nblocks]`
+ * hold host pointers in the ttc layout; they are borrowed for the call.
+ * Runs calvel/calmas, then up to maxcy x (V-cycle, p += pp, p halo, pbound,
+ * calvel, calmas) until rmax < eps and iter > 1, then writes p, u, v, w
+ * back.  The caller then runs exchange(1..3) and boundu/boundv/boundw as
+ * newsolv_mg.for:86-88 does.  `rmax_hist` (may be NULL) receives rmax after
+ * each outer iteration, at most `hist_cap` entries. */
+int mf3d_newsolv_mg(mf3d_ctx *ctx, const mf3d_fields *fields, double dt,
+                    double alfapr, mf3d_solve_info *info, double *rmax_hist,
+                    int hist_cap);
+
+/* Same, with `fields` pointing to device memory (a GPU-resident caller). */
+int mf3d_newsolv_mg_device(mf3d_ctx *ctx, const mf3d_fields *fields,
+                           double dt, double alfapr, mf3d_solve_info *info,
+                           double *rmax_hist, int hist_cap);
+
+/* One V-cycle (mgkcyc, mgsolver.for:224-369) on device arrays: reads the
+ * RHS `su` and writes the correction `pp` of each block, both in the ttc
+ * layout (pp including its first ghost layer, mgsolver.for:351-364). The
+ * V-cycle starts from pp = 0 as newsolv_mg.for:19-21 and :44 leave it. */
+int mf3d_mgkcyc_device(mf3d_ctx *ctx, double *const *su, double *const *pp);
+
+/* ---------------------------------------------------------------------- */
+/* Introspection.                                                           */
+/* ---------------------------------------------------------------------- */
+
+/* Message of the last error on this thread ("" if none). */
+const char *mf3d_last_error(void);
+const char *mf3d_status_string(int status);
+int mf3d_abi_version(void);
+
+/* Number of device kernel launches issued by the last solve on `ctx`. */
+long long mf3d_last_launch_count(const mf3d_ctx *ctx);
+
+/* Host-only view of the multigrid halo copy map of level `level` (1-based):
+ * the composition of exchangepp + mgbound + exchbc_mgpp (exchangepp.for:
+ * 43-4763, mgsolver.for:907-992) as (destination, source) cell pairs.  A
+ * cell is numbered blockpos*S + ((k*(ny+2) + j)*(nx+2) + i) with 0-based
+ * ghost-inclusive local indices, S the level's largest block volume.  With
+ * dst == NULL returns the pair count.  Needs no GPU. */
+long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid,
+                        int level, long long *dst, long long *src);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MF3D_H */

@@ -1,0 +1,161 @@
+"""ctypes mirror of include/mf3d.h and the loader of the native library.
+
+The native library ``libmf3d.so`` (CUDA sm_100a kernels + C++ host driver)
+is built in-tree by ``multiflow3d_b200.build``.  Loading fails loudly when it
+is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmf3d.so")
+
+MF3D_OK = 0
+MF3D_NOT_CONVERGED = 1
+MF3D_DIVERGED = 2
+MF3D_E_INVALID = -1
+MF3D_E_CUDA = -2
+MF3D_E_OOM = -3
+MF3D_E_TIMEOUT = -4
+MF3D_E_NONFINITE = -5
+MF3D_E_UNSUPPORTED = -6
+
+MF3D_BC_PERIODIC = 5
+MF3D_PREC_FP64 = 0
+MF3D_PREC_FP32 = 1
+MF3D_PREC_BF16 = 2
+
+_dp = C.POINTER(C.c_double)
+
+
+class BlockDesc(C.Structure):
+    """``mf3d_block_desc`` - one block (reference ``type multidom``)."""
+
+    _fields_ = [
+        ("id", C.c_int),
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("xsl", C.c_double), ("xel", C.c_double),
+        ("ysl", C.c_double), ("yel", C.c_double),
+        ("zsl", C.c_double), ("zel", C.c_double),
+        ("iprev", C.c_int), ("inext", C.c_int),
+        ("jprev", C.c_int), ("jnext", C.c_int),
+        ("kprev", C.c_int), ("knext", C.c_int),
+        ("corprev", C.c_int * 4), ("cornext", C.c_int * 4),
+        ("edgprev", C.c_int * 6), ("edgnext", C.c_int * 6),
+        ("per_ip", C.c_int), ("per_in", C.c_int),
+        ("per_jp", C.c_int), ("per_jn", C.c_int),
+        ("per_kp", C.c_int), ("per_kn", C.c_int),
+        ("bc_west", C.c_int), ("bc_east", C.c_int),
+        ("bc_south", C.c_int), ("bc_north", C.c_int),
+        ("bc_bottom", C.c_int), ("bc_top", C.c_int),
+        ("hx", _dp), ("hy", _dp), ("hz", _dp),
+    ]
+
+
+class Params(C.Structure):
+    """``mf3d_params`` - the control.cin fields the projection reads."""
+
+    _fields_ = [
+        ("ngrid", C.c_int),
+        ("mg_itrsch", C.c_int),
+        ("irestr", C.c_int),
+        ("iproln", C.c_int),
+        ("maxcy", C.c_int),
+        ("eps", C.c_double),
+        ("eps_relative", C.c_int),
+        ("pl", C.c_int),
+        ("differencing", C.c_int),
+        ("precision", C.c_int),
+        ("device", C.c_int),
+    ]
+
+
+class Fields(C.Structure):
+    """``mf3d_fields`` - per-block field pointers (ttc layout)."""
+
+    _fields_ = [
+        ("ustar", _dp), ("vstar", _dp), ("wstar", _dp),
+        ("u", _dp), ("v", _dp), ("w", _dp),
+        ("p", _dp), ("su", _dp),
+    ]
+
+
+class SolveInfo(C.Structure):
+    """``mf3d_solve_info``."""
+
+    _fields_ = [
+        ("rmax", C.c_double),
+        ("rmax0", C.c_double),
+        ("iter", C.c_int),
+        ("status", C.c_int),
+        ("ms_device", C.c_double),
+    ]
+
+
+# Every symbol include/mf3d.h declares (checked by the tests).
+EXPORTED_SYMBOLS = (
+    "mf3d_build_topology",
+    "mf3d_create",
+    "mf3d_destroy",
+    "mf3d_newsolv_mg",
+    "mf3d_newsolv_mg_device",
+    "mf3d_mgkcyc_device",
+    "mf3d_last_error",
+    "mf3d_status_string",
+    "mf3d_abi_version",
+    "mf3d_last_launch_count",
+    "mf3d_halo_map",
+)
+
+_lib = None
+
+
+def _declare(lib):
+    vp = C.c_void_p
+    lib.mf3d_build_topology.argtypes = [C.c_int, _dp, C.POINTER(C.c_int), C.c_double,
+                                        C.c_double, C.c_double, C.POINTER(BlockDesc)]
+    lib.mf3d_create.argtypes = [C.POINTER(BlockDesc), C.c_int, C.POINTER(Params), C.POINTER(vp)]
+    lib.mf3d_destroy.argtypes = [vp]
+    lib.mf3d_newsolv_mg.argtypes = [vp, C.POINTER(Fields), C.c_double, C.c_double,
+                                    C.POINTER(SolveInfo), _dp, C.c_int]
+    lib.mf3d_newsolv_mg_device.argtypes = lib.mf3d_newsolv_mg.argtypes
+    lib.mf3d_mgkcyc_device.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp)]
+    lib.mf3d_last_error.restype = C.c_char_p
+    lib.mf3d_status_string.restype = C.c_char_p
+    lib.mf3d_status_string.argtypes = [C.c_int]
+    lib.mf3d_last_launch_count.restype = C.c_longlong
+    lib.mf3d_last_launch_count.argtypes = [vp]
+    lib.mf3d_halo_map.restype = C.c_longlong
+    lib.mf3d_halo_map.argtypes = [C.POINTER(BlockDesc), C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    return lib
+
+
+def load(path: str | None = None):
+    """Load ``libmf3d.so``; raises if it has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(
+            f"native library {p} is missing: run `python -c 'import __graft_entry__ as g; g.build()'`"
+            " (there is no CPU fallback)")
+    lib = _declare(C.CDLL(p))
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def last_error(lib) -> str:
+    return lib.mf3d_last_error().decode()
+
+
+def check(lib, status: int, what: str = "") -> int:
+    """Raise on a negative status (the solve did not run)."""
+    if status < 0:
+        raise RuntimeError(f"{what}: {lib.mf3d_status_string(status).decode()} ({status}): {last_error(lib)}")
+    return status

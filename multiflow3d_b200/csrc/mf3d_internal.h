@@ -1,0 +1,56 @@
+// Internal host-side structures of libmf3d (not part of the C ABI).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/mf3d.h"
+
+namespace mf3d {
+
+void set_error(const std::string &msg);
+
+// Index geometry of one block at one multigrid level: interior n*, ghost
+// shell of one cell, 0-based ghost-inclusive indices 0..n+1.
+struct LevelGeom {
+  int nx, ny, nz;
+  long long cells() const { return (long long)(nx + 2) * (ny + 2) * (nz + 2); }
+  long long lin(int i, int j, int k) const {
+    return ((long long)k * (ny + 2) + j) * (nx + 2) + i;
+  }
+};
+
+// A halo copy: destination cell <- source cell, as level-wide cell ids
+// (block base + lin(i,j,k)).
+struct HaloPair {
+  long long dst, src;
+};
+
+// Composition of exchangepp + mgbound + exchbc_mgpp for one level
+// (exchangepp.for:43-4763, mgsolver.for:907-992, exchangepp.for:4768-5383)
+// expressed as pairs dst <- src against the state before the exchange.
+// `base[b]` is the level-wide id of cell (0,0,0) of block b.
+std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
+                                     const std::vector<LevelGeom> &geom,
+                                     const std::vector<long long> &base);
+
+// Neighbour search of alloc_dom.for:456-1150 over block extents.
+int build_topology(int nblocks, const double *ext, const int *bc6, double dx,
+                   double dy, double dz, mf3d_block_desc *out);
+
+// Level-g cell widths of one axis, ghost-inclusive (n_g + 2 entries), from
+// the block's extended fine widths (NULL = uniform h); see mf3d_block_desc.
+std::vector<double> level_widths(const double *ext, int n, double h, int ngrid, int g);
+
+// Face-ghost rule of one block face for the pressure field and the low-face
+// velocity: which block supplies the value.
+enum FaceKind { FACE_NEIGHBOUR = 0, FACE_WALL = 1 };
+struct FaceRule {
+  int kind;   // FACE_NEIGHBOUR (neighbour, periodic partner or self) / FACE_WALL
+  int src;    // position of the source block (valid for FACE_NEIGHBOUR)
+};
+// rules[6*b + f], f = W,E,S,N,B,T.  Returns MF3D_OK or an error.
+int face_rules(const std::vector<mf3d_block_desc> &blocks, std::vector<FaceRule> &rules);
+
+}  // namespace mf3d

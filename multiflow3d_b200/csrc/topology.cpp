@@ -1,0 +1,391 @@
+// Host-side set-up of libmf3d: neighbour search, multigrid halo copy maps
+// and field face rules.  Pure C++, no CUDA.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <unordered_map>
+
+#include "mf3d_internal.h"
+
+namespace mf3d {
+
+// ---------------------------------------------------------------------------
+// Neighbour search (alloc_dom.for:456-1150).  Two blocks touch when their
+// face coordinates agree within 1e-8 (the reference's tolerance); face
+// neighbours must share both tangential extents, edge neighbours the one
+// extent along the edge, corner neighbours only the corner point.  Periodic
+// partners are searched against the domain's bounding box (xst..zen).
+// ---------------------------------------------------------------------------
+int build_topology(int nb, const double *ext, const int *bc6, double dx, double dy,
+                   double dz, mf3d_block_desc *out) {
+  if (nb <= 0 || !ext || !bc6 || !out) {
+    set_error("build_topology: bad arguments");
+    return MF3D_E_INVALID;
+  }
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int b = 0; b < nb; ++b)
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], ext[6 * b + 2 * a]);
+      hi[a] = std::max(hi[a], ext[6 * b + 2 * a + 1]);
+    }
+  auto S = [&](int b, int a) { return ext[6 * b + 2 * a]; };      // start along axis a
+  auto E = [&](int b, int a) { return ext[6 * b + 2 * a + 1]; };  // end along axis a
+  auto eq = [](double x, double y) { return std::fabs(x - y) < 1e-8; };
+  auto same = [&](int b, int o, int a) { return eq(S(b, a), S(o, a)) && eq(E(b, a), E(o, a)); };
+  // Relation of block o to block b along axis a: -1 = o ends where b starts,
+  // +1 = o starts where b ends, 0 = same extent, 2 = none.
+  auto rel = [&](int b, int o, int a) -> int {
+    if (eq(S(b, a), E(o, a))) return -1;
+    if (eq(E(b, a), S(o, a))) return +1;
+    return same(b, o, a) ? 0 : 2;
+  };
+  const double h[3] = {dx, dy, dz};
+  // offsets of the reference's numbered corner / edge neighbours
+  const int corp[4][2] = {{-1, -1}, {-1, +1}, {+1, +1}, {+1, -1}};  // (x,y) at z-1
+  const int corn[4][2] = {{+1, +1}, {+1, -1}, {-1, -1}, {-1, +1}};  // (x,y) at z+1
+  // edges: (dx, dy, dz) with 0 meaning "same extent"
+  const int edp[6][3] = {{-1, 0, -1}, {0, +1, -1}, {+1, 0, -1}, {0, -1, -1}, {-1, -1, 0}, {-1, +1, 0}};
+  const int edn[6][3] = {{+1, 0, +1}, {0, -1, +1}, {-1, 0, +1}, {0, +1, +1}, {+1, +1, 0}, {+1, -1, 0}};
+  for (int b = 0; b < nb; ++b) {
+    mf3d_block_desc &d = out[b];
+    std::memset(&d, 0, sizeof d);
+    d.id = b;
+    d.dx = dx; d.dy = dy; d.dz = dz;
+    d.xsl = S(b, 0); d.xel = E(b, 0); d.ysl = S(b, 1); d.yel = E(b, 1); d.zsl = S(b, 2); d.zel = E(b, 2);
+    int n[3];
+    for (int a = 0; a < 3; ++a) {
+      double c = (E(b, a) - S(b, a)) / h[a];
+      if (std::fabs(c - std::nearbyint(c)) > 1e-8 || c < 1) {  // localparameters.for:84-98
+        set_error("block " + std::to_string(b) + ": extent is not a whole number of cells");
+        return MF3D_E_INVALID;
+      }
+      n[a] = (int)std::nearbyint(c);
+    }
+    d.nx = n[0]; d.ny = n[1]; d.nz = n[2];
+    d.bc_west = bc6[0]; d.bc_east = bc6[1]; d.bc_south = bc6[2];
+    d.bc_north = bc6[3]; d.bc_bottom = bc6[4]; d.bc_top = bc6[5];
+    int face[6];
+    for (int f = 0; f < 6; ++f) face[f] = -1;
+    for (int q = 0; q < 4; ++q) d.corprev[q] = d.cornext[q] = -1;
+    for (int q = 0; q < 6; ++q) d.edgprev[q] = d.edgnext[q] = -1;
+    int count_face[6] = {0};
+    for (int o = 0; o < nb; ++o) {
+      if (o == b) continue;
+      int r[3] = {rel(b, o, 0), rel(b, o, 1), rel(b, o, 2)};
+      for (int a = 0; a < 3; ++a) {
+        int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        if ((r[a] == -1 || r[a] == 1) && r[t1] == 0 && r[t2] == 0) {
+          int f = 2 * a + (r[a] == 1);
+          face[f] = o;
+          ++count_face[f];
+        }
+      }
+      // corners: only the corner point must coincide
+      auto corner = [&](int sx, int sy, int sz) {
+        bool x = sx < 0 ? eq(S(b, 0), E(o, 0)) : eq(E(b, 0), S(o, 0));
+        bool y = sy < 0 ? eq(S(b, 1), E(o, 1)) : eq(E(b, 1), S(o, 1));
+        bool z = sz < 0 ? eq(S(b, 2), E(o, 2)) : eq(E(b, 2), S(o, 2));
+        return x && y && z;
+      };
+      for (int q = 0; q < 4; ++q) {
+        if (corner(corp[q][0], corp[q][1], -1)) d.corprev[q] = o;
+        if (corner(corn[q][0], corn[q][1], +1)) d.cornext[q] = o;
+      }
+      auto edge = [&](const int *e) {
+        for (int a = 0; a < 3; ++a) {
+          if (e[a] == 0) { if (!same(b, o, a)) return false; }
+          else if (e[a] < 0) { if (!eq(S(b, a), E(o, a))) return false; }
+          else if (!eq(E(b, a), S(o, a))) return false;
+        }
+        return true;
+      };
+      for (int q = 0; q < 6; ++q) {
+        if (edge(edp[q])) d.edgprev[q] = o;
+        if (edge(edn[q])) d.edgnext[q] = o;
+      }
+    }
+    for (int f = 0; f < 6; ++f)
+      if (count_face[f] > 1) {  // alloc_dom.for:483-487 and alike
+        set_error("block " + std::to_string(b) + " has more than one neighbour on a face");
+        return MF3D_E_INVALID;
+      }
+    d.iprev = face[0]; d.inext = face[1]; d.jprev = face[2];
+    d.jnext = face[3]; d.kprev = face[4]; d.knext = face[5];
+    // periodic partners: the block at the far end of the box, same tangential extents
+    int *per[6] = {&d.per_ip, &d.per_in, &d.per_jp, &d.per_jn, &d.per_kp, &d.per_kn};
+    for (int f = 0; f < 6; ++f) {
+      *per[f] = -1;
+      int a = f / 2;
+      bool is_prev = (f % 2) == 0;
+      if (bc6[f] != MF3D_BC_PERIODIC || face[f] >= 0) continue;
+      for (int o = 0; o < nb; ++o) {
+        if (o == b) continue;
+        int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        if (!same(b, o, t1) || !same(b, o, t2)) continue;
+        if (is_prev ? eq(hi[a], E(o, a)) : eq(lo[a], S(o, a))) *per[f] = o;
+      }
+    }
+  }
+  return MF3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Halo copy map.  Every cell of the level carries a token (the id of the
+// cell whose pre-exchange value it holds); the reference's sequence of
+// copies is replayed on tokens, each pack/unpack phase reading from the
+// state at the start of its phase.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct TokenLevel {
+  const std::vector<mf3d_block_desc> &blk;
+  const std::vector<LevelGeom> &geom;
+  const std::vector<long long> &base;
+  std::unordered_map<int, int> pos;  // block id -> position
+  std::vector<long long> tok;
+  long long total;
+
+  TokenLevel(const std::vector<mf3d_block_desc> &b, const std::vector<LevelGeom> &g,
+             const std::vector<long long> &bs)
+      : blk(b), geom(g), base(bs) {
+    total = 0;
+    for (size_t q = 0; q < b.size(); ++q) {
+      pos[b[q].id] = (int)q;
+      total = std::max(total, bs[q] + g[q].cells());
+    }
+    tok.resize(total);
+    for (long long c = 0; c < total; ++c) tok[c] = c;
+  }
+  long long id(int p, int i, int j, int k) const { return base[p] + geom[p].lin(i, j, k); }
+  int P(int block_id) const {
+    auto it = pos.find(block_id);
+    return it == pos.end() ? -1 : it->second;
+  }
+};
+
+// A phase: ordered (dst, src) pairs read from the phase-start state; later
+// pairs override earlier ones on the same dst.
+struct Phase {
+  std::vector<HaloPair> pairs;
+  void add(long long d, long long s) { pairs.push_back({d, s}); }
+  void apply(std::vector<long long> &tok) const {
+    std::vector<long long> v(pairs.size());
+    for (size_t q = 0; q < pairs.size(); ++q) v[q] = tok[pairs[q].src];
+    for (size_t q = 0; q < pairs.size(); ++q) tok[pairs[q].dst] = v[q];
+  }
+};
+
+// Cell at index `a` along axis `ax` and (s,t) along the other two axes.
+struct AxisView {
+  int ax;
+  long long at(const TokenLevel &T, int p, int a, int s, int t) const {
+    if (ax == 0) return T.id(p, a, s, t);
+    if (ax == 1) return T.id(p, s, a, t);
+    return T.id(p, s, t, a);  // z: s = i, t = j
+  }
+};
+
+void mgbound_tokens(TokenLevel &T) {
+  for (size_t p = 0; p < T.blk.size(); ++p) {
+    const auto &d = T.blk[p];
+    const LevelGeom &g = T.geom[p];
+    int nx = g.nx, ny = g.ny, nz = g.nz;
+    auto cp = [&](long long dst, long long src) { T.tok[dst] = T.tok[src]; };
+    if (d.iprev < 0 && d.bc_west != MF3D_BC_PERIODIC)
+      for (int k = 0; k <= nz + 1; ++k) for (int j = 0; j <= ny + 1; ++j) cp(T.id(p, 0, j, k), T.id(p, 1, j, k));
+    if (d.inext < 0 && d.bc_east != MF3D_BC_PERIODIC)
+      for (int k = 0; k <= nz + 1; ++k) for (int j = 0; j <= ny + 1; ++j) cp(T.id(p, nx + 1, j, k), T.id(p, nx, j, k));
+    if (d.jprev < 0 && d.bc_south != MF3D_BC_PERIODIC)
+      for (int k = 0; k <= nz + 1; ++k) for (int i = 0; i <= nx + 1; ++i) cp(T.id(p, i, 0, k), T.id(p, i, 1, k));
+    if (d.jnext < 0 && d.bc_north != MF3D_BC_PERIODIC)
+      for (int k = 0; k <= nz + 1; ++k) for (int i = 0; i <= nx + 1; ++i) cp(T.id(p, i, ny + 1, k), T.id(p, i, ny, k));
+    if (d.kprev < 0 && d.bc_bottom != MF3D_BC_PERIODIC)
+      for (int j = 0; j <= ny + 1; ++j) for (int i = 0; i <= nx + 1; ++i) cp(T.id(p, i, j, 0), T.id(p, i, j, 1));
+    if (d.knext < 0 && d.bc_top != MF3D_BC_PERIODIC)
+      for (int j = 0; j <= ny + 1; ++j) for (int i = 0; i <= nx + 1; ++i) cp(T.id(p, i, j, nz + 1), T.id(p, i, j, nz));
+  }
+}
+
+}  // namespace
+
+std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
+                                     const std::vector<LevelGeom> &geom,
+                                     const std::vector<long long> &base) {
+  TokenLevel T(blocks, geom, base);
+  const int nb = (int)blocks.size();
+  bool periodic = false;
+  for (const auto &d : blocks)
+    if (d.bc_west == 5 || d.bc_east == 5 || d.bc_south == 5 || d.bc_north == 5 || d.bc_bottom == 5 || d.bc_top == 5)
+      periodic = true;
+
+  // exchangepp: sync_dir x, y, z
+  for (int ax = 0; ax < 3; ++ax) {
+    Phase ph;
+    AxisView V{ax};
+    for (int p = 0; p < nb; ++p) {
+      const auto &d = blocks[p];
+      const LevelGeom &g = geom[p];
+      int nA = ax == 0 ? g.nx : ax == 1 ? g.ny : g.nz;
+      int n1 = ax == 0 ? g.ny : g.nx;           // s extent (interior)
+      int n2 = ax == 2 ? g.ny : g.nz;           // t extent (interior)
+      int prev = ax == 0 ? d.iprev : ax == 1 ? d.jprev : d.kprev;
+      int next = ax == 0 ? d.inext : ax == 1 ? d.jnext : d.knext;
+      // faces: full planes including ghost rows (exchangepp.for:155-160, 4036-4043)
+      if (prev >= 0) {
+        int q = T.P(prev);
+        int nAq = ax == 0 ? geom[q].nx : ax == 1 ? geom[q].ny : geom[q].nz;
+        for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+          ph.add(V.at(T, p, 0, s, t), V.at(T, q, nAq, s, t));
+      }
+      if (next >= 0) {
+        int q = T.P(next);
+        for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+          ph.add(V.at(T, p, nA + 1, s, t), V.at(T, q, 1, s, t));
+      }
+      if (ax == 2) {
+        // corners and edges, unpacked after the faces (exchangepp.for:4433-4755)
+        int nx = g.nx, ny = g.ny, nz = g.nz;
+        auto src_last = [&](int q, int a) { return a == 0 ? geom[q].nx : a == 1 ? geom[q].ny : geom[q].nz; };
+        // previous corners #1..4: ghost (x,y,0) <- neighbour interior
+        const int cx[4] = {0, 0, 1, 1}, cy[4] = {0, 1, 1, 0};  // 0 = low side, 1 = high side
+        for (int c = 0; c < 4; ++c)
+          if (d.corprev[c] >= 0) {
+            int q = T.P(d.corprev[c]);
+            int gi = cx[c] ? nx + 1 : 0, gj = cy[c] ? ny + 1 : 0;
+            int si = cx[c] ? 1 : src_last(q, 0), sj = cy[c] ? 1 : src_last(q, 1);
+            ph.add(T.id(p, gi, gj, 0), T.id(q, si, sj, src_last(q, 2)));
+          }
+        // previous edges #1..6
+        auto edge_prev = [&](int e, int q) {
+          int lx = src_last(q, 0), ly = src_last(q, 1), lz = src_last(q, 2);
+          switch (e) {
+            case 0: for (int j = 1; j <= ny; ++j) ph.add(T.id(p, 0, j, 0), T.id(q, lx, j, lz)); break;
+            case 1: for (int i = 1; i <= nx; ++i) ph.add(T.id(p, i, ny + 1, 0), T.id(q, i, 1, lz)); break;
+            case 2: for (int j = 1; j <= ny; ++j) ph.add(T.id(p, nx + 1, j, 0), T.id(q, 1, j, lz)); break;
+            case 3: for (int i = 1; i <= nx; ++i) ph.add(T.id(p, i, 0, 0), T.id(q, i, ly, lz)); break;
+            case 4: for (int k = 1; k <= nz; ++k) ph.add(T.id(p, 0, 0, k), T.id(q, lx, ly, k)); break;
+            case 5: for (int k = 1; k <= nz; ++k) ph.add(T.id(p, 0, ny + 1, k), T.id(q, lx, 1, k)); break;
+          }
+        };
+        for (int e = 0; e < 6; ++e)
+          if (d.edgprev[e] >= 0) edge_prev(e, T.P(d.edgprev[e]));
+        // next corners #1..4: ghost (x,y,nz+1)
+        const int nxs[4] = {1, 1, 0, 0}, nys[4] = {1, 0, 0, 1};
+        for (int c = 0; c < 4; ++c)
+          if (d.cornext[c] >= 0) {
+            int q = T.P(d.cornext[c]);
+            int gi = nxs[c] ? nx + 1 : 0, gj = nys[c] ? ny + 1 : 0;
+            int si = nxs[c] ? 1 : src_last(q, 0), sj = nys[c] ? 1 : src_last(q, 1);
+            ph.add(T.id(p, gi, gj, nz + 1), T.id(q, si, sj, 1));
+          }
+        auto edge_next = [&](int e, int q) {
+          int lx = src_last(q, 0), ly = src_last(q, 1);
+          switch (e) {
+            case 0: for (int j = 1; j <= ny; ++j) ph.add(T.id(p, nx + 1, j, nz + 1), T.id(q, 1, j, 1)); break;
+            case 1: for (int i = 1; i <= nx; ++i) ph.add(T.id(p, i, 0, nz + 1), T.id(q, i, ly, 1)); break;
+            case 2: for (int j = 1; j <= ny; ++j) ph.add(T.id(p, 0, j, nz + 1), T.id(q, lx, j, 1)); break;
+            case 3: for (int i = 1; i <= nx; ++i) ph.add(T.id(p, i, ny + 1, nz + 1), T.id(q, i, 1, 1)); break;
+            case 4: for (int k = 1; k <= nz; ++k) ph.add(T.id(p, nx + 1, ny + 1, k), T.id(q, 1, 1, k)); break;
+            case 5: for (int k = 1; k <= nz; ++k) ph.add(T.id(p, nx + 1, 0, k), T.id(q, 1, ly, k)); break;
+          }
+        };
+        for (int e = 0; e < 6; ++e)
+          if (d.edgnext[e] >= 0) edge_next(e, T.P(d.edgnext[e]));
+      }
+    }
+    ph.apply(T.tok);
+  }
+  mgbound_tokens(T);
+  if (periodic) {
+    // exchbc_mgpp: x, y, z; in-block wraps are immediate, partner copies
+    // are packed from the axis-start state and unpacked afterwards.
+    for (int ax = 0; ax < 3; ++ax) {
+      AxisView V{ax};
+      Phase ph;
+      for (int p = 0; p < nb; ++p) {
+        const auto &d = blocks[p];
+        int bcp = ax == 0 ? d.bc_west : ax == 1 ? d.bc_south : d.bc_bottom;
+        int bcn = ax == 0 ? d.bc_east : ax == 1 ? d.bc_north : d.bc_top;
+        if (!(bcp == 5 || bcn == 5)) continue;
+        const LevelGeom &g = geom[p];
+        int nA = ax == 0 ? g.nx : ax == 1 ? g.ny : g.nz;
+        int n1 = ax == 0 ? g.ny : g.nx, n2 = ax == 2 ? g.ny : g.nz;
+        int prev = ax == 0 ? d.iprev : ax == 1 ? d.jprev : d.kprev;
+        int next = ax == 0 ? d.inext : ax == 1 ? d.jnext : d.knext;
+        int perp = ax == 0 ? d.per_ip : ax == 1 ? d.per_jp : d.per_kp;
+        int pern = ax == 0 ? d.per_in : ax == 1 ? d.per_jn : d.per_kn;
+        if (prev < 0 && next < 0) {
+          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+            T.tok[V.at(T, p, 0, s, t)] = T.tok[V.at(T, p, nA, s, t)];
+          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+            T.tok[V.at(T, p, nA + 1, s, t)] = T.tok[V.at(T, p, 1, s, t)];
+          continue;
+        }
+        if (prev < 0 && next >= 0 && perp >= 0) {
+          int q = T.P(perp);
+          int nAq = ax == 0 ? geom[q].nx : ax == 1 ? geom[q].ny : geom[q].nz;
+          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+            ph.add(V.at(T, p, 0, s, t), V.at(T, q, nAq, s, t));
+        }
+        if (next < 0 && prev >= 0 && pern >= 0) {
+          int q = T.P(pern);
+          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+            ph.add(V.at(T, p, nA + 1, s, t), V.at(T, q, 1, s, t));
+        }
+      }
+      ph.apply(T.tok);
+    }
+  }
+  std::vector<HaloPair> out;
+  for (long long c = 0; c < T.total; ++c)
+    if (T.tok[c] != c) out.push_back({c, T.tok[c]});
+  return out;
+}
+
+std::vector<double> level_widths(const double *ext, int n, double h, int ngrid, int g) {
+  int W = 1 << (ngrid - 1);
+  std::vector<double> e(n + 2 * W);
+  for (int q = 0; q < n + 2 * W; ++q) e[q] = ext ? ext[q] : h;
+  int Wg = W;
+  for (int l = 2; l <= g; ++l) {
+    std::vector<double> m(e.size() / 2);
+    for (size_t q = 0; q < m.size(); ++q) m[q] = e[2 * q] + e[2 * q + 1];  // pairwise: exact for uniform
+    e.swap(m);
+    Wg /= 2;
+  }
+  int nl = n >> (g - 1);
+  std::vector<double> w(nl + 2);
+  for (int c = 0; c < nl + 2; ++c) w[c] = e[Wg - 1 + c];
+  return w;
+}
+
+int face_rules(const std::vector<mf3d_block_desc> &blocks, std::vector<FaceRule> &rules) {
+  std::unordered_map<int, int> pos;
+  for (size_t q = 0; q < blocks.size(); ++q) pos[blocks[q].id] = (int)q;
+  rules.assign(6 * blocks.size(), FaceRule{FACE_WALL, -1});
+  for (size_t p = 0; p < blocks.size(); ++p) {
+    const auto &d = blocks[p];
+    const int nbr[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+    const int bc[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+    const int per[6] = {d.per_ip, d.per_in, d.per_jp, d.per_jn, d.per_kp, d.per_kn};
+    for (int f = 0; f < 6; ++f) {
+      FaceRule r{FACE_WALL, -1};
+      if (nbr[f] >= 0) {
+        r = {FACE_NEIGHBOUR, pos.count(nbr[f]) ? pos[nbr[f]] : -1};
+      } else if (bc[f] == MF3D_BC_PERIODIC) {
+        int other = nbr[f ^ 1];
+        if (other < 0) r = {FACE_NEIGHBOUR, (int)p};  // alone along the axis: wrap onto itself
+        else r = {FACE_NEIGHBOUR, (per[f] >= 0 && pos.count(per[f])) ? pos[per[f]] : -1};
+      }
+      if (r.kind == FACE_NEIGHBOUR && r.src < 0) {
+        set_error("block " + std::to_string(d.id) + ": face neighbour or periodic partner not found");
+        return MF3D_E_INVALID;
+      }
+      rules[6 * p + f] = r;
+    }
+  }
+  return MF3D_OK;
+}
+
+}  // namespace mf3d

@@ -1,0 +1,91 @@
+"""Host-side mirror of the reference's projection interface.
+
+``Projection`` owns one ``mf3d_ctx`` (device hierarchy for a fixed block
+layout) and exposes the reference's entry points by name:
+
+* ``newsolv_mg(fields, dt, alfapr)`` - newsolv_mg.for:2-102 on host arrays
+  (the drop-in; host<->device copies inside the call);
+* ``newsolv_mg_device(fields, dt, alfapr)`` - the same on device arrays
+  (``torch.Tensor`` on the context's GPU);
+* ``mgkcyc_device(su, pp)`` - one V-cycle, mgsolver.for:224-369.
+
+Return values mirror the reference's module variables: ``rmax`` and
+``iter``, plus the per-iteration rmax history the reference does not log.
+Negative library statuses raise; ``NOT_CONVERGED`` / ``DIVERGED`` are
+returned in ``info.status`` (the reference prints and continues / stops).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import abi
+
+_dp = C.POINTER(C.c_double)
+
+
+@dataclass
+class SolveResult:
+    status: int
+    rmax: float
+    rmax0: float
+    iter: int
+    ms_device: float
+    history: np.ndarray
+
+
+class Projection:
+    def __init__(self, descriptors, params: abi.Params, lib=None):
+        self.lib = lib or abi.load()
+        self.nblocks = len(descriptors)
+        self.desc = descriptors
+        self.params = params
+        ctx = C.c_void_p()
+        st = self.lib.mf3d_create(descriptors, self.nblocks, C.byref(params), C.byref(ctx))
+        abi.check(self.lib, st, "mf3d_create")
+        self.ctx = ctx
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.mf3d_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _run(self, fn, fields_arr, dt, alfapr) -> SolveResult:
+        cap = max(self.params.maxcy, 1)
+        hist = np.zeros(cap)
+        info = abi.SolveInfo()
+        st = fn(self.ctx, fields_arr, C.c_double(dt), C.c_double(alfapr), C.byref(info),
+                hist.ctypes.data_as(_dp), cap)
+        abi.check(self.lib, st, fn.__name__)
+        return SolveResult(st, info.rmax, info.rmax0, info.iter, info.ms_device, hist[:info.iter].copy())
+
+    def newsolv_mg(self, blocks, dt=1.0, alfapr=1.0) -> SolveResult:
+        """Host arrays (numpy, ttc layout) per block, updated in place."""
+        from .problems import fields_struct
+        return self._run(self.lib.mf3d_newsolv_mg, fields_struct(blocks), dt, alfapr)
+
+    def newsolv_mg_device(self, blocks, dt=1.0, alfapr=1.0) -> SolveResult:
+        """Device arrays (torch float64 CUDA tensors, ttc layout) per block."""
+        arr = (abi.Fields * len(blocks))()
+        for b, f in enumerate(blocks):
+            for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p", "su"):
+                t = f.get(k)
+                setattr(arr[b], k, C.cast(C.c_void_p(t.data_ptr()), _dp) if t is not None else None)
+        return self._run(self.lib.mf3d_newsolv_mg_device, arr, dt, alfapr)
+
+    def mgkcyc_device(self, su_list, pp_list):
+        su = (_dp * len(su_list))(*[C.cast(C.c_void_p(t.data_ptr()), _dp) for t in su_list])
+        pp = (_dp * len(pp_list))(*[C.cast(C.c_void_p(t.data_ptr()), _dp) for t in pp_list])
+        abi.check(self.lib, self.lib.mf3d_mgkcyc_device(self.ctx, su, pp), "mf3d_mgkcyc_device")
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.mf3d_last_launch_count(self.ctx))

@@ -1,0 +1,1067 @@
+/*
+ * TEST INFRASTRUCTURE ONLY - the oracle.
+ *
+ * A literal CPU restatement (C++17, -O2 -ffp-contract=off) of MultiFlow3D's
+ * pressure-Poisson path, used by the tests, by __graft_entry__.smoke() and by
+ * bench.py's CPU-baseline leg as the checker.  The shipped library never
+ * links, loads or calls this file.
+ *
+ * Parity status: the reference is Fortran 90 + MPI and this container has no
+ * Fortran compiler, so the reference cannot be run here ("parity pinned by
+ * analytic known-answer tests, not by reference outputs"): the reference
+ * ships no tests, golden vectors or fixtures.  This restatement is pinned by
+ * the known-answer tests under tests/ (discrete eigenfunctions, an FFT/DCT
+ * direct solve, nullspace and symmetry identities, decomposition invariance).
+ *
+ * Each routine follows the reference loop by loop, in the same evaluation
+ * order, with the reference's own storage:
+ *   - `cof` per block: level-g correction phi with a 1-cell ghost shell,
+ *     j fastest then i then k, followed by the 8 interior arrays
+ *     aw, ae, as, an, ab, at, ap, rhs (mgsolver.for:20-38, 112-210);
+ *   - fields p, u, v, w, ustar, ... as Fortran (ttc_i,ttc_j,ttc_k) arrays,
+ *     i fastest, pl ghost layers (initial.for:196-210).
+ * Only the same-level branches (rdiv = 1 everywhere, single MPI rank owning
+ * every block, the `dom_ad(a) .eq. dom_ad(b)` direct-buffer path) are
+ * restated; the LMR 2:1 branches and L_LSM are not on this path.
+ *
+ * Extension with no reference counterpart (marked EXT): non-uniform cell
+ * widths.  With uniform widths every EXT formula reduces bit-for-bit to the
+ * reference expression.
+ */
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "../include/mf3d.h"
+
+namespace {
+
+struct Blk {
+  mf3d_block_desc d;
+  int ngrid;
+  int isp, iep, jsp, jep, ksp, kep;
+  int isu, ieu, jsu, jeu, ksu, keu;
+  int isv, iev, jsv, jev, ksv, kev;
+  int isw, iew, jsw, jew, ksw, kew;
+  int ttc_i, ttc_j, ttc_k;
+  std::vector<long> faz;       /* faz[1..ngrd_gl] */
+  std::vector<double> cof;     /* 1-based: cof[1..nwork] */
+  double *ustar, *vstar, *wstar, *u, *v, *w, *p;
+  std::vector<double> su, pp;
+  /* same-rank receive buffers of exchangepp / exchbc_mgpp (1-based) */
+  std::vector<double> recvb_m1, recvb_p1;
+  double rcm[5], rcp[5];
+  std::vector<double> rem[7], rep[7];
+  /* receive buffers of exchange_smlvl / exchange_bc (1-based) */
+  std::vector<double> frm[4], frp[4];
+  /* EXT: cell widths per level incl. ghost cells, index 0..n+1 */
+  std::vector<std::vector<double>> hx, hy, hz;
+  bool stretched;
+};
+
+struct Ctx {
+  std::vector<Blk> b;
+  std::map<int, int> indid; /* dom_indid: block id -> position */
+  int ngrd_gl, mg_itrsch, irestr, iproln, maxcy, pl;
+  double eps;
+  int eps_relative;
+  bool periodic;
+  double dt, alfapr, rmax;
+};
+
+inline double &F(Blk &B, double *a, int i, int j, int k) {
+  return a[(size_t)(i - 1) + (size_t)B.ttc_i * ((size_t)(j - 1) + (size_t)B.ttc_j * (size_t)(k - 1))];
+}
+
+int level_n(int n, int gl) { return n / (1 << (gl - 1)) + 2; }
+
+/* EXT: widths of each level, ghost-inclusive (index 0 and n+1 are the
+ * ghost cells).  `ext` holds the fine widths of the block with
+ * W = 2^(ngrid-1) neighbour cells on each side (NULL = uniform h).  Level g
+ * merges pairs of level g-1 cells, so uniform widths stay exact powers of
+ * two times h and every EXT formula reduces to the reference's. */
+std::vector<std::vector<double>> level_widths(const double *ext, int n, double h,
+                                              int ngrid) {
+  int W = 1 << (ngrid - 1);
+  std::vector<std::vector<double>> out(ngrid + 1);
+  std::vector<double> e(n + 2 * W);
+  for (int q = 0; q < n + 2 * W; ++q) e[q] = ext ? ext[q] : h;
+  int Wg = W;
+  for (int g = 1; g <= ngrid; ++g) {
+    if (g > 1) {
+      std::vector<double> m(e.size() / 2);
+      for (size_t q = 0; q < m.size(); ++q) m[q] = e[2 * q] + e[2 * q + 1];
+      e.swap(m);
+      Wg /= 2;
+    }
+    int nl = n >> (g - 1);
+    std::vector<double> w(nl + 2);
+    for (int c = 0; c < nl + 2; ++c) w[c] = e[Wg - 1 + c];
+    out[g] = w;
+  }
+  return out;
+}
+
+/* ------------------------------------------------------------------ */
+/* coeff (mgsolver.for:2-222), uniform branch + EXT widths.           */
+/* ------------------------------------------------------------------ */
+void coeff(Ctx &C) {
+  for (auto &B : C.b) {
+    int nx = B.iep - B.isp + 1, ny = B.jep - B.jsp + 1, nz = B.kep - B.ksp + 1;
+    B.faz.assign(C.ngrd_gl + 1, 0);
+    B.faz[1] = (long)(nx + 2) * (ny + 2) * (nz + 2);
+    long pi = nx + 2, pj = ny + 2, pk = nz + 2;
+    for (int g = 2; g <= C.ngrd_gl; ++g) {
+      int gl = g > B.ngrid ? B.ngrid : g;
+      long mi = level_n(nx, gl), mj = level_n(ny, gl), mk = level_n(nz, gl);
+      B.faz[g] = B.faz[g - 1] + mi * mj * mk + 8 * (pi - 2) * (pj - 2) * (pk - 2);
+      pi = mi; pj = mj; pk = mk;
+    }
+    long nwork = 0;
+    for (int g = 1; g <= C.ngrd_gl; ++g) {
+      int gl = g > B.ngrid ? B.ngrid : g;
+      long mi = level_n(nx, gl), mj = level_n(ny, gl), mk = level_n(nz, gl);
+      nwork += mi * mj * mk + 8 * (mi - 2) * (mj - 2) * (mk - 2);
+    }
+    B.cof.assign(nwork + 1, 0.0);
+    for (int g = 1; g <= C.ngrd_gl; ++g) {
+      int gl = g > B.ngrid ? B.ngrid : g;
+      int mi = level_n(nx, gl), mj = level_n(ny, gl), mk = level_n(nz, gl);
+      double ndx = B.d.dx * (double)(1 << (gl - 1));
+      double ndy = B.d.dy * (double)(1 << (gl - 1));
+      double ndz = B.d.dz * (double)(1 << (gl - 1));
+      double dxx = ndx * ndx, dyy = ndy * ndy, dzz = ndz * ndz;
+      long cnt = B.faz[g] - (long)mi * mj * mk;
+      for (int k = 1; k <= mk; ++k)
+        for (int i = 1; i <= mi; ++i)
+          for (int j = 1; j <= mj; ++j)
+            B.cof[cnt + (long)(k - 1) * mi * mj + (long)(i - 1) * mj + j] = 0.0;
+      long incr = (long)(mi - 2) * (mj - 2) * (mk - 2);
+      for (int k = 2; k <= mk - 1; ++k)
+        for (int i = 2; i <= mi - 1; ++i)
+          for (int j = 2; j <= mj - 1; ++j) {
+            long ijk = B.faz[g] + (long)(k - 2) * (mi - 2) * (mj - 2) + (long)(i - 2) * (mj - 2) + (j - 1);
+            double aw, ae, as, an, ab, at;
+            if (!B.stretched) {
+              aw = 1.0 / dxx; ae = 1.0 / dxx;
+              as = 1.0 / dyy; an = 1.0 / dyy;
+              ab = 1.0 / dzz; at = 1.0 / dzz;
+            } else {
+              /* EXT: finite-volume coefficients 1/(h_c * d_face),
+               * d_face = 0.5*(h_c + h_nb); equals 1/dxx when uniform. */
+              const auto &wx = B.hx[gl]; const auto &wy = B.hy[gl]; const auto &wz = B.hz[gl];
+              int ic = i - 1, jc = j - 1, kc = k - 1; /* 0-based ghost-inclusive */
+              aw = 1.0 / (wx[ic] * (0.5 * (wx[ic] + wx[ic - 1])));
+              ae = 1.0 / (wx[ic] * (0.5 * (wx[ic] + wx[ic + 1])));
+              as = 1.0 / (wy[jc] * (0.5 * (wy[jc] + wy[jc - 1])));
+              an = 1.0 / (wy[jc] * (0.5 * (wy[jc] + wy[jc + 1])));
+              ab = 1.0 / (wz[kc] * (0.5 * (wz[kc] + wz[kc - 1])));
+              at = 1.0 / (wz[kc] * (0.5 * (wz[kc] + wz[kc + 1])));
+            }
+            B.cof[ijk] = aw;
+            B.cof[ijk + 1 * incr] = ae;
+            B.cof[ijk + 2 * incr] = as;
+            B.cof[ijk + 3 * incr] = an;
+            B.cof[ijk + 4 * incr] = ab;
+            B.cof[ijk + 5 * incr] = at;
+            if (B.d.iprev < 0 && B.d.bc_west != 5 && i == 2) B.cof[ijk] = 0.0;
+            if (B.d.inext < 0 && B.d.bc_east != 5 && i == mi - 1) B.cof[ijk + 1 * incr] = 0.0;
+            if (B.d.jprev < 0 && B.d.bc_south != 5 && j == 2) B.cof[ijk + 2 * incr] = 0.0;
+            if (B.d.jnext < 0 && B.d.bc_north != 5 && j == mj - 1) B.cof[ijk + 3 * incr] = 0.0;
+            if (B.d.kprev < 0 && B.d.bc_bottom != 5 && k == 2) B.cof[ijk + 4 * incr] = 0.0;
+            if (B.d.knext < 0 && B.d.bc_top != 5 && k == mk - 1) B.cof[ijk + 5 * incr] = 0.0;
+            B.cof[ijk + 6 * incr] = -1.0 * (B.cof[ijk] + B.cof[ijk + 1 * incr] + B.cof[ijk + 2 * incr] +
+                                            B.cof[ijk + 3 * incr] + B.cof[ijk + 4 * incr] + B.cof[ijk + 5 * incr]);
+            B.cof[ijk + 7 * incr] = 0.0;
+          }
+    }
+  }
+}
+
+struct Lev {
+  int ni, nj, nk, nij;
+  long nijk, base; /* base: faz(g)-ni*nj*nk, phi(i,j,k) = cof[base + (k-1)nij + (i-1)nj + j] */
+};
+Lev lev(Ctx &C, Blk &B, int g) {
+  int gl = g > B.ngrid ? B.ngrid : g;
+  Lev L;
+  L.ni = level_n(B.iep - B.isp + 1, gl);
+  L.nj = level_n(B.jep - B.jsp + 1, gl);
+  L.nk = level_n(B.kep - B.ksp + 1, gl);
+  L.nij = L.ni * L.nj;
+  L.nijk = (long)L.ni * L.nj * L.nk;
+  L.base = B.faz[g] - L.nijk;
+  (void)C;
+  return L;
+}
+inline long PH(const Lev &L, int i, int j, int k) {
+  return L.base + (long)(k - 1) * L.nij + (long)(i - 1) * L.nj + j;
+}
+
+/* ------------------------------------------------------------------ */
+/* mgbound (mgsolver.for:907-992)                                       */
+/* ------------------------------------------------------------------ */
+void mgbound(Ctx &C, int g) {
+  for (auto &B : C.b) {
+    Lev L = lev(C, B, g);
+    double *c = B.cof.data();
+    if (B.d.iprev < 0 && B.d.bc_west != 5)
+      for (int k = 1; k <= L.nk; ++k) for (int j = 1; j <= L.nj; ++j) { long q = PH(L, 1, j, k); c[q] = c[q + L.nj]; }
+    if (B.d.inext < 0 && B.d.bc_east != 5)
+      for (int k = 1; k <= L.nk; ++k) for (int j = 1; j <= L.nj; ++j) { long q = PH(L, L.ni, j, k); c[q] = c[q - L.nj]; }
+    if (B.d.jprev < 0 && B.d.bc_south != 5)
+      for (int k = 1; k <= L.nk; ++k) for (int i = 1; i <= L.ni; ++i) { long q = PH(L, i, 1, k); c[q] = c[q + 1]; }
+    if (B.d.jnext < 0 && B.d.bc_north != 5)
+      for (int k = 1; k <= L.nk; ++k) for (int i = 1; i <= L.ni; ++i) { long q = PH(L, i, L.nj, k); c[q] = c[q - 1]; }
+    if (B.d.kprev < 0 && B.d.bc_bottom != 5)
+      for (int j = 1; j <= L.nj; ++j) for (int i = 1; i <= L.ni; ++i) { long q = PH(L, i, j, 1); c[q] = c[q + L.nij]; }
+    if (B.d.knext < 0 && B.d.bc_top != 5)
+      for (int j = 1; j <= L.nj; ++j) for (int i = 1; i <= L.ni; ++i) { long q = PH(L, i, j, L.nk); c[q] = c[q - L.nij]; }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* exchbc_mgpp (exchangepp.for:4768-5383), same-rank branches.           */
+/* ------------------------------------------------------------------ */
+void exchbc_mgpp(Ctx &C, int g) {
+  for (int ax = 0; ax < 3; ++ax) {
+    /* pack (and the in-block copy of a block alone along the axis) */
+    for (auto &B : C.b) {
+      int bcp = ax == 0 ? B.d.bc_west : ax == 1 ? B.d.bc_south : B.d.bc_bottom;
+      int bcn = ax == 0 ? B.d.bc_east : ax == 1 ? B.d.bc_north : B.d.bc_top;
+      if (!(bcp == 5 || bcn == 5)) continue;
+      int prev = ax == 0 ? B.d.iprev : ax == 1 ? B.d.jprev : B.d.kprev;
+      int next = ax == 0 ? B.d.inext : ax == 1 ? B.d.jnext : B.d.knext;
+      int perp = ax == 0 ? B.d.per_ip : ax == 1 ? B.d.per_jp : B.d.per_kp;
+      int pern = ax == 0 ? B.d.per_in : ax == 1 ? B.d.per_jn : B.d.per_kn;
+      Lev L = lev(C, B, g);
+      double *c = B.cof.data();
+      int n = ax == 0 ? L.ni : ax == 1 ? L.nj : L.nk;
+      /* plane iterator over the two other axes, reference buffer order */
+      auto cell = [&](int a, int s, int t) -> long {
+        /* a: index along ax; (s,t) the other two axes in buffer order */
+        if (ax == 0) return PH(L, a, s, t);        /* ijk=(k-1)*nj+j : s=j,t=k */
+        if (ax == 1) return PH(L, s, a, t);        /* ijk=(k-1)*ni+i : s=i,t=k */
+        return PH(L, t, s, a);                     /* ijk=(i-1)*nj+j : s=j,t=i */
+      };
+      int n1 = ax == 0 ? L.nj : ax == 1 ? L.ni : L.nj;
+      int n2 = ax == 0 ? L.nk : ax == 1 ? L.nk : L.ni;
+      if (prev < 0) {
+        if (next < 0) {
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) c[cell(1, s, t)] = c[cell(n - 1, s, t)];
+        } else {
+          Blk &P = C.b[C.indid.at(perp)];
+          P.recvb_p1.assign((size_t)n1 * n2 + 1, 0.0);
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) P.recvb_p1[(size_t)(t - 1) * n1 + s] = c[cell(2, s, t)];
+        }
+      }
+      if (next < 0) {
+        if (prev < 0) {
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) c[cell(n, s, t)] = c[cell(2, s, t)];
+        } else {
+          Blk &P = C.b[C.indid.at(pern)];
+          P.recvb_m1.assign((size_t)n1 * n2 + 1, 0.0);
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) P.recvb_m1[(size_t)(t - 1) * n1 + s] = c[cell(n - 1, s, t)];
+        }
+      }
+    }
+    /* unpack */
+    for (auto &B : C.b) {
+      int bcp = ax == 0 ? B.d.bc_west : ax == 1 ? B.d.bc_south : B.d.bc_bottom;
+      int bcn = ax == 0 ? B.d.bc_east : ax == 1 ? B.d.bc_north : B.d.bc_top;
+      if (!(bcp == 5 || bcn == 5)) continue;
+      int prev = ax == 0 ? B.d.iprev : ax == 1 ? B.d.jprev : B.d.kprev;
+      int next = ax == 0 ? B.d.inext : ax == 1 ? B.d.jnext : B.d.knext;
+      Lev L = lev(C, B, g);
+      double *c = B.cof.data();
+      int n = ax == 0 ? L.ni : ax == 1 ? L.nj : L.nk;
+      auto cell = [&](int a, int s, int t) -> long {
+        if (ax == 0) return PH(L, a, s, t);
+        if (ax == 1) return PH(L, s, a, t);
+        return PH(L, t, s, a);
+      };
+      int n1 = ax == 0 ? L.nj : ax == 1 ? L.ni : L.nj;
+      int n2 = ax == 0 ? L.nk : ax == 1 ? L.nk : L.ni;
+      if (prev < 0 && next >= 0)
+        for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) c[cell(1, s, t)] = B.recvb_m1[(size_t)(t - 1) * n1 + s];
+      if (next < 0 && prev >= 0)
+        for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) c[cell(n, s, t)] = B.recvb_p1[(size_t)(t - 1) * n1 + s];
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* exchangepp (exchangepp.for:2-4766), same-level same-rank branches.   */
+/* Per sync_dir: every block packs (faces; in the z pass also corners   */
+/* and edges) into its neighbours' receive buffers, then every block    */
+/* unpacks: prev face, next face, then prev corners 1-4, prev edges    */
+/* 1-6, next corners 1-4, next edges 1-6.  Then mgbound, exchbc_mgpp.   */
+/* ------------------------------------------------------------------ */
+void exchangepp(Ctx &C, int g) {
+  for (int sd = 1; sd <= 3; ++sd) {
+    for (auto &B : C.b) {
+      Lev L = lev(C, B, g);
+      double *fi = B.cof.data();
+      int cprev = sd == 1 ? B.d.iprev : sd == 2 ? B.d.jprev : B.d.kprev;
+      int cnext = sd == 1 ? B.d.inext : sd == 2 ? B.d.jnext : B.d.knext;
+      int ns1 = sd == 1 ? L.nj : sd == 2 ? L.ni : L.nj;
+      int ns2 = sd == 1 ? L.nk : sd == 2 ? L.nk : L.ni;
+      auto face = [&](int a, int s, int t) -> long {
+        if (sd == 1) return PH(L, a, s, t);
+        if (sd == 2) return PH(L, s, a, t);
+        return PH(L, t, s, a);
+      };
+      int nd = sd == 1 ? L.ni : sd == 2 ? L.nj : L.nk;
+      if (cprev >= 0) {
+        Blk &P = C.b[C.indid.at(cprev)];
+        P.recvb_p1.assign((size_t)ns1 * ns2 + 1, 0.0);
+        for (int t = 1; t <= ns2; ++t) for (int s = 1; s <= ns1; ++s)
+          P.recvb_p1[(size_t)(t - 1) * ns1 + s] = fi[face(2, s, t)];
+      }
+      if (sd == 3) {
+        /* previous corners (exchangepp.for:439-633) */
+        const int cpi[4] = {2, 2, L.ni - 1, L.ni - 1}, cpj[4] = {2, L.nj - 1, L.nj - 1, 2};
+        for (int q = 0; q < 4; ++q)
+          if (B.d.corprev[q] >= 0) C.b[C.indid.at(B.d.corprev[q])].rcp[q + 1] = fi[PH(L, cpi[q], cpj[q], 2)];
+        /* previous edges (exchangepp.for:640-1086) */
+        if (B.d.edgprev[0] >= 0) { auto &R = C.b[C.indid.at(B.d.edgprev[0])].rep[1]; R.assign(L.nj + 1, 0.0); for (int nn = 2; nn <= L.nj - 1; ++nn) R[nn] = fi[PH(L, 2, nn, 2)]; }
+        if (B.d.edgprev[1] >= 0) { auto &R = C.b[C.indid.at(B.d.edgprev[1])].rep[2]; R.assign(L.ni + 1, 0.0); for (int nn = 2; nn <= L.ni - 1; ++nn) R[nn] = fi[PH(L, nn, L.nj - 1, 2)]; }
+        if (B.d.edgprev[2] >= 0) { auto &R = C.b[C.indid.at(B.d.edgprev[2])].rep[3]; R.assign(L.nj + 1, 0.0); for (int nn = 2; nn <= L.nj - 1; ++nn) R[nn] = fi[PH(L, L.ni - 1, nn, 2)]; }
+        if (B.d.edgprev[3] >= 0) { auto &R = C.b[C.indid.at(B.d.edgprev[3])].rep[4]; R.assign(L.ni + 1, 0.0); for (int nn = 2; nn <= L.ni - 1; ++nn) R[nn] = fi[PH(L, nn, 2, 2)]; }
+        if (B.d.edgprev[4] >= 0) { auto &R = C.b[C.indid.at(B.d.edgprev[4])].rep[5]; R.assign(L.nk + 1, 0.0); for (int nn = 2; nn <= L.nk - 1; ++nn) R[nn] = fi[PH(L, 2, 2, nn)]; }
+        if (B.d.edgprev[5] >= 0) { auto &R = C.b[C.indid.at(B.d.edgprev[5])].rep[6]; R.assign(L.nk + 1, 0.0); for (int nn = 2; nn <= L.nk - 1; ++nn) R[nn] = fi[PH(L, 2, L.nj - 1, nn)]; }
+      }
+      if (cnext >= 0) {
+        Blk &N = C.b[C.indid.at(cnext)];
+        N.recvb_m1.assign((size_t)ns1 * ns2 + 1, 0.0);
+        for (int t = 1; t <= ns2; ++t) for (int s = 1; s <= ns1; ++s)
+          N.recvb_m1[(size_t)(t - 1) * ns1 + s] = fi[face(nd - 1, s, t)];
+      }
+      if (sd == 3) {
+        /* next corners (exchangepp.for:1387-1580) */
+        const int cni[4] = {L.ni - 1, L.ni - 1, 2, 2}, cnj[4] = {L.nj - 1, 2, 2, L.nj - 1};
+        for (int q = 0; q < 4; ++q)
+          if (B.d.cornext[q] >= 0) C.b[C.indid.at(B.d.cornext[q])].rcm[q + 1] = fi[PH(L, cni[q], cnj[q], L.nk - 1)];
+        /* next edges (exchangepp.for:1587-2036) */
+        if (B.d.edgnext[0] >= 0) { auto &R = C.b[C.indid.at(B.d.edgnext[0])].rem[1]; R.assign(L.nj + 1, 0.0); for (int nn = 2; nn <= L.nj - 1; ++nn) R[nn] = fi[PH(L, L.ni - 1, nn, L.nk - 1)]; }
+        if (B.d.edgnext[1] >= 0) { auto &R = C.b[C.indid.at(B.d.edgnext[1])].rem[2]; R.assign(L.ni + 1, 0.0); for (int nn = 2; nn <= L.ni - 1; ++nn) R[nn] = fi[PH(L, nn, 2, L.nk - 1)]; }
+        if (B.d.edgnext[2] >= 0) { auto &R = C.b[C.indid.at(B.d.edgnext[2])].rem[3]; R.assign(L.nj + 1, 0.0); for (int nn = 2; nn <= L.nj - 1; ++nn) R[nn] = fi[PH(L, 2, nn, L.nk - 1)]; }
+        if (B.d.edgnext[3] >= 0) { auto &R = C.b[C.indid.at(B.d.edgnext[3])].rem[4]; R.assign(L.ni + 1, 0.0); for (int nn = 2; nn <= L.ni - 1; ++nn) R[nn] = fi[PH(L, nn, L.nj - 1, L.nk - 1)]; }
+        if (B.d.edgnext[4] >= 0) { auto &R = C.b[C.indid.at(B.d.edgnext[4])].rem[5]; R.assign(L.nk + 1, 0.0); for (int nn = 2; nn <= L.nk - 1; ++nn) R[nn] = fi[PH(L, L.ni - 1, L.nj - 1, nn)]; }
+        if (B.d.edgnext[5] >= 0) { auto &R = C.b[C.indid.at(B.d.edgnext[5])].rem[6]; R.assign(L.nk + 1, 0.0); for (int nn = 2; nn <= L.nk - 1; ++nn) R[nn] = fi[PH(L, L.ni - 1, 2, nn)]; }
+      }
+    }
+    /* unpack (exchangepp.for:3996-4755) */
+    for (auto &B : C.b) {
+      Lev L = lev(C, B, g);
+      double *fi = B.cof.data();
+      int cprev = sd == 1 ? B.d.iprev : sd == 2 ? B.d.jprev : B.d.kprev;
+      int cnext = sd == 1 ? B.d.inext : sd == 2 ? B.d.jnext : B.d.knext;
+      int ns1 = sd == 1 ? L.nj : sd == 2 ? L.ni : L.nj;
+      int ns2 = sd == 1 ? L.nk : sd == 2 ? L.nk : L.ni;
+      auto face = [&](int a, int s, int t) -> long {
+        if (sd == 1) return PH(L, a, s, t);
+        if (sd == 2) return PH(L, s, a, t);
+        return PH(L, t, s, a);
+      };
+      int nd = sd == 1 ? L.ni : sd == 2 ? L.nj : L.nk;
+      if (cprev >= 0)
+        for (int t = 1; t <= ns2; ++t) for (int s = 1; s <= ns1; ++s) fi[face(1, s, t)] = B.recvb_m1[(size_t)(t - 1) * ns1 + s];
+      if (cnext >= 0)
+        for (int t = 1; t <= ns2; ++t) for (int s = 1; s <= ns1; ++s) fi[face(nd, s, t)] = B.recvb_p1[(size_t)(t - 1) * ns1 + s];
+      if (sd == 3) {
+        const int upi[4] = {1, 1, L.ni, L.ni}, upj[4] = {1, L.nj, L.nj, 1};
+        for (int q = 0; q < 4; ++q)
+          if (B.d.corprev[q] >= 0) fi[PH(L, upi[q], upj[q], 1)] = B.rcm[q + 1];
+        if (B.d.edgprev[0] >= 0) for (int nn = 2; nn <= L.nj - 1; ++nn) fi[PH(L, 1, nn, 1)] = B.rem[1][nn];
+        if (B.d.edgprev[1] >= 0) for (int nn = 2; nn <= L.ni - 1; ++nn) fi[PH(L, nn, L.nj, 1)] = B.rem[2][nn];
+        if (B.d.edgprev[2] >= 0) for (int nn = 2; nn <= L.nj - 1; ++nn) fi[PH(L, L.ni, nn, 1)] = B.rem[3][nn];
+        if (B.d.edgprev[3] >= 0) for (int nn = 2; nn <= L.ni - 1; ++nn) fi[PH(L, nn, 1, 1)] = B.rem[4][nn];
+        if (B.d.edgprev[4] >= 0) for (int nn = 2; nn <= L.nk - 1; ++nn) fi[PH(L, 1, 1, nn)] = B.rem[5][nn];
+        if (B.d.edgprev[5] >= 0) for (int nn = 2; nn <= L.nk - 1; ++nn) fi[PH(L, 1, L.nj, nn)] = B.rem[6][nn];
+        const int uni[4] = {L.ni, L.ni, 1, 1}, unj[4] = {L.nj, 1, 1, L.nj};
+        for (int q = 0; q < 4; ++q)
+          if (B.d.cornext[q] >= 0) fi[PH(L, uni[q], unj[q], L.nk)] = B.rcp[q + 1];
+        if (B.d.edgnext[0] >= 0) for (int nn = 2; nn <= L.nj - 1; ++nn) fi[PH(L, L.ni, nn, L.nk)] = B.rep[1][nn];
+        if (B.d.edgnext[1] >= 0) for (int nn = 2; nn <= L.ni - 1; ++nn) fi[PH(L, nn, 1, L.nk)] = B.rep[2][nn];
+        if (B.d.edgnext[2] >= 0) for (int nn = 2; nn <= L.nj - 1; ++nn) fi[PH(L, 1, nn, L.nk)] = B.rep[3][nn];
+        if (B.d.edgnext[3] >= 0) for (int nn = 2; nn <= L.ni - 1; ++nn) fi[PH(L, nn, L.nj, L.nk)] = B.rep[4][nn];
+        if (B.d.edgnext[4] >= 0) for (int nn = 2; nn <= L.nk - 1; ++nn) fi[PH(L, L.ni, L.nj, nn)] = B.rep[5][nn];
+        if (B.d.edgnext[5] >= 0) for (int nn = 2; nn <= L.nk - 1; ++nn) fi[PH(L, L.ni, 1, nn)] = B.rep[6][nn];
+      }
+    }
+  }
+  mgbound(C, g);
+  if (C.periodic) exchbc_mgpp(C, g);
+}
+
+/* ------------------------------------------------------------------ */
+/* mgrelax (mgsolver.for:371-617)                                        */
+/* ------------------------------------------------------------------ */
+void mgrelax(Ctx &C, int g, int it) {
+  for (int itr = 1; itr <= it; ++itr) {
+    for (auto &B : C.b) {
+      Lev L = lev(C, B, g);
+      int ni = L.ni, nj = L.nj, nk = L.nk, nij = L.nij;
+      long nij2 = (long)(ni - 2) * (nj - 2);
+      long incr = (long)(ni - 2) * (nj - 2) * (nk - 2);
+      double *cf = B.cof.data();
+      long fz = B.faz[g];
+      auto W = [&](int i, int j, int k) -> long { return fz + (long)(k - 2) * nij2 + (long)(i - 2) * (nj - 2) + (j - 1); };
+      if (C.mg_itrsch == 1 || C.mg_itrsch == 3) {
+        for (int pass = 0; pass < (C.mg_itrsch == 3 ? 2 : 1); ++pass)
+          for (int k = 2; k <= nk - 1; ++k)
+            for (int j = 2; j <= nj - 1; ++j)
+              for (int i = 2; i <= ni - 1; ++i) {
+                if (C.mg_itrsch == 3 && ((i + j + k) % 2) != pass) continue;
+                long ph = PH(L, i, j, k);
+                long w = W(i, j, k);
+                cf[ph] = ((cf[w + 7 * incr] -
+                           (cf[w] * cf[ph - nj] + cf[w + incr] * cf[ph + nj] + cf[w + 2 * incr] * cf[ph - 1] +
+                            cf[w + 3 * incr] * cf[ph + 1] + cf[w + 4 * incr] * cf[ph - nij] +
+                            cf[w + 5 * incr] * cf[ph + nij])) /
+                          cf[w + 6 * incr]);
+              }
+      } else if (C.mg_itrsch == 2) {
+        int ngg = std::max({ni, nj, nk}) + 2;
+        std::vector<double> a(ngg + 1, 0.0), c(ngg + 1, 0.0);
+        /* j-lines */
+        for (int k = 2; k <= nk - 1; ++k)
+          for (int i = 2; i <= ni - 1; ++i) {
+            c[1] = cf[PH(L, i, 1, k)];
+            for (int j = 2; j <= nj - 1; ++j) {
+              long ph = PH(L, i, j, k), w = W(i, j, k);
+              double apr = 1.0 / (cf[w + 6 * incr] - cf[w + 2 * incr] * a[j - 1]);
+              a[j] = cf[w + 3 * incr] * apr;
+              c[j] = (cf[w + 7 * incr] - cf[w + incr] * cf[ph + nj] - cf[w] * cf[ph - nj] -
+                      cf[w + 5 * incr] * cf[ph + nij] - cf[w + 4 * incr] * cf[ph - nij] -
+                      cf[w + 2 * incr] * c[j - 1]) * apr;
+            }
+            for (int j = nj - 1; j >= 2; --j) { long ph = PH(L, i, j, k); cf[ph] = (c[j] - a[j] * cf[ph + 1]); }
+          }
+        /* i-lines */
+        for (int k = 2; k <= nk - 1; ++k)
+          for (int j = 2; j <= nj - 1; ++j) {
+            c[1] = cf[PH(L, 1, j, k)];
+            for (int i = 2; i <= ni - 1; ++i) {
+              long ph = PH(L, i, j, k), w = W(i, j, k);
+              double apr = 1.0 / (cf[w + 6 * incr] - cf[w] * a[i - 1]);
+              a[i] = cf[w + incr] * apr;
+              c[i] = (cf[w + 7 * incr] - cf[w + 3 * incr] * cf[ph + 1] - cf[w + 2 * incr] * cf[ph - 1] -
+                      cf[w + 5 * incr] * cf[ph + nij] - cf[w + 4 * incr] * cf[ph - nij] -
+                      cf[w] * c[i - 1]) * apr;
+            }
+            for (int i = ni - 1; i >= 2; --i) { long ph = PH(L, i, j, k); cf[ph] = (c[i] - a[i] * cf[ph + nj]); }
+          }
+        /* k-lines */
+        for (int i = 2; i <= ni - 1; ++i)
+          for (int j = 2; j <= nj - 1; ++j) {
+            c[1] = cf[PH(L, i, j, 1)];
+            for (int k = 2; k <= nk - 1; ++k) {
+              long ph = PH(L, i, j, k), w = W(i, j, k);
+              double apr = 1.0 / (cf[w + 6 * incr] - cf[w + 4 * incr] * a[k - 1]);
+              a[k] = cf[w + 5 * incr] * apr;
+              c[k] = (cf[w + 7 * incr] - cf[w + 3 * incr] * cf[ph + 1] - cf[w + 2 * incr] * cf[ph - 1] -
+                      cf[w + incr] * cf[ph + nj] - cf[w] * cf[ph - nj] -
+                      cf[w + 4 * incr] * c[k - 1]) * apr;
+            }
+            for (int k = nk - 1; k >= 2; --k) { long ph = PH(L, i, j, k); cf[ph] = (c[k] - a[k] * cf[ph + nij]); }
+          }
+      }
+    }
+    mgbound(C, g);
+    exchangepp(C, g);
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* mgrestr (mgsolver.for:619-761), coarsening branch + EXT weights.     */
+/* ------------------------------------------------------------------ */
+void mgrestr(Ctx &C, int g) {
+  for (auto &B : C.b) {
+    Lev Lc = lev(C, B, g), Lf = lev(C, B, g - 1);
+    int nic = Lc.ni, njc = Lc.nj, nkc = Lc.nk;
+    long nijc2 = (long)(nic - 2) * (njc - 2), incr_c = (long)(nic - 2) * (njc - 2) * (nkc - 2);
+    double *cf = B.cof.data();
+    for (int k = 1; k <= nkc; ++k) for (int i = 1; i <= nic; ++i) for (int j = 1; j <= njc; ++j) cf[PH(Lc, i, j, k)] = 0.0;
+    for (int k = 2; k <= nkc - 1; ++k) for (int i = 2; i <= nic - 1; ++i) for (int j = 2; j <= njc - 1; ++j)
+      cf[B.faz[g] + (long)(k - 2) * nijc2 + (long)(i - 2) * (njc - 2) + (j - 1) + 7 * incr_c] = 0.0;
+    int nif = Lf.ni, njf = Lf.nj, nkf = Lf.nk;
+    long nijf2 = (long)(nif - 2) * (njf - 2), incr_f = (long)(nif - 2) * (njf - 2) * (nkf - 2);
+    std::vector<double> resf((size_t)nif * njf * nkf, 0.0);
+    auto R = [&](int i, int j, int k) -> double & { return resf[(size_t)(i - 1) + (size_t)nif * ((j - 1) + (size_t)njf * (k - 1))]; };
+    for (int k = 2; k <= nkf - 1; ++k) for (int i = 2; i <= nif - 1; ++i) for (int j = 2; j <= njf - 1; ++j) {
+      long ph = PH(Lf, i, j, k);
+      long w = B.faz[g - 1] + (long)(k - 2) * nijf2 + (long)(i - 2) * (njf - 2) + (j - 1);
+      R(i, j, k) = cf[w + 7 * incr_f] -
+                   (cf[w] * cf[ph - njf] + cf[w + incr_f] * cf[ph + njf] + cf[w + 2 * incr_f] * cf[ph - 1] +
+                    cf[w + 3 * incr_f] * cf[ph + 1] + cf[w + 4 * incr_f] * cf[ph - Lf.nij] +
+                    cf[w + 5 * incr_f] * cf[ph + Lf.nij] + cf[w + 6 * incr_f] * cf[ph]);
+    }
+    int gf = g - 1, gc = g;
+    for (int k = 2; k <= nkc - 1; ++k) for (int i = 2; i <= nic - 1; ++i) for (int j = 2; j <= njc - 1; ++j) {
+      long su = B.faz[g] + (long)(k - 2) * nijc2 + (long)(i - 2) * (njc - 2) + (j - 1) + 7 * incr_c;
+      if (!B.stretched) {
+        cf[su] = 0.125 * (R(2 * i - 2, 2 * j - 2, 2 * k - 2) + R(2 * i - 1, 2 * j - 2, 2 * k - 2) +
+                          R(2 * i - 2, 2 * j - 1, 2 * k - 2) + R(2 * i - 1, 2 * j - 1, 2 * k - 2) +
+                          R(2 * i - 2, 2 * j - 2, 2 * k - 1) + R(2 * i - 1, 2 * j - 2, 2 * k - 1) +
+                          R(2 * i - 2, 2 * j - 1, 2 * k - 1) + R(2 * i - 1, 2 * j - 1, 2 * k - 1));
+      } else {
+        /* EXT: volume-weighted average, s = 8 (hx_f/Hx_c)(hy_f/Hy_c)(hz_f/Hz_c),
+         * s == 1.0 exactly on a uniform grid. */
+        double t[8];
+        int q = 0;
+        for (int dk = 0; dk < 2; ++dk) for (int dj = 0; dj < 2; ++dj) for (int di = 0; di < 2; ++di) {
+          int fi_ = 2 * i - 2 + di, fj = 2 * j - 2 + dj, fk = 2 * k - 2 + dk;
+          double s = 8.0 * (B.hx[gf][fi_ - 1] / B.hx[gc][i - 1]) * (B.hy[gf][fj - 1] / B.hy[gc][j - 1]) *
+                     (B.hz[gf][fk - 1] / B.hz[gc][k - 1]);
+          t[q++] = R(fi_, fj, fk) * s;
+        }
+        cf[su] = 0.125 * (t[0] + t[1] + t[2] + t[3] + t[4] + t[5] + t[6] + t[7]);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* mgcorr (mgsolver.for:763-905), coarsening branch.                     */
+/* ------------------------------------------------------------------ */
+void mgcorr(Ctx &C, int g) {
+  for (auto &B : C.b) {
+    Lev Lf = lev(C, B, g), Lc = lev(C, B, g + 1);
+    double *cf = B.cof.data();
+    int nijf = Lf.nij, njf = Lf.nj, nijc = Lc.nij, njc = Lc.nj;
+    for (int kc = 1; kc <= Lc.nk - 1; ++kc) {
+      int k = 2 * kc - 1;
+      for (int ic = 1; ic <= Lc.ni - 1; ++ic) {
+        int i = 2 * ic - 1;
+        for (int jc = 1; jc <= Lc.nj - 1; ++jc) {
+          int j = 2 * jc - 1;
+          long c0 = PH(Lc, ic, jc, kc), f0 = PH(Lf, i, j, k);
+          const double *q = cf;
+          double C000 = q[c0], C010 = q[c0 + 1], C001 = q[c0 + nijc], C011 = q[c0 + nijc + 1];
+          double C100 = q[c0 + njc], C110 = q[c0 + njc + 1], C101 = q[c0 + njc + nijc], C111 = q[c0 + 1 + njc + nijc];
+          cf[f0] = cf[f0] + (27.0 * C000 + 9.0 * C010 + 9.0 * C001 + 3.0 * C011 + 9.0 * C100 + 3.0 * C110 + 3.0 * C101 + 1.0 * C111) / 64.0;
+          cf[f0 + njf] = cf[f0 + njf] + (9.0 * C000 + 3.0 * C010 + 3.0 * C001 + 1.0 * C011 + 27.0 * C100 + 9.0 * C110 + 9.0 * C101 + 3.0 * C111) / 64.0;
+          cf[f0 + 1] = cf[f0 + 1] + (9.0 * C000 + 27.0 * C010 + 3.0 * C001 + 9.0 * C011 + 3.0 * C100 + 9.0 * C110 + 1.0 * C101 + 3.0 * C111) / 64.0;
+          cf[f0 + nijf] = cf[f0 + nijf] + (9.0 * C000 + 3.0 * C010 + 27.0 * C001 + 9.0 * C011 + 3.0 * C100 + 1.0 * C110 + 9.0 * C101 + 3.0 * C111) / 64.0;
+          cf[f0 + njf + 1] = cf[f0 + njf + 1] + (3.0 * C000 + 9.0 * C010 + 1.0 * C001 + 3.0 * C011 + 9.0 * C100 + 27.0 * C110 + 3.0 * C101 + 9.0 * C111) / 64.0;
+          cf[f0 + nijf + njf] = cf[f0 + nijf + njf] + (3.0 * C000 + 1.0 * C010 + 9.0 * C001 + 3.0 * C011 + 9.0 * C100 + 3.0 * C110 + 27.0 * C101 + 9.0 * C111) / 64.0;
+          cf[f0 + nijf + 1] = cf[f0 + nijf + 1] + (3.0 * C000 + 9.0 * C010 + 9.0 * C001 + 27.0 * C011 + 1.0 * C100 + 3.0 * C110 + 3.0 * C101 + 9.0 * C111) / 64.0;
+          cf[f0 + nijf + njf + 1] = cf[f0 + nijf + njf + 1] + (1.0 * C000 + 3.0 * C010 + 3.0 * C001 + 9.0 * C011 + 3.0 * C100 + 9.0 * C110 + 9.0 * C101 + 27.0 * C111) / 64.0;
+        }
+      }
+    }
+  }
+  mgbound(C, g);
+}
+
+/* ------------------------------------------------------------------ */
+/* mgkcyc (mgsolver.for:224-369): copy pp/su in, V-cycle, copy pp out.   */
+/* ------------------------------------------------------------------ */
+void mgkcyc(Ctx &C) {
+  int pl = C.pl;
+  for (auto &B : C.b) {
+    Lev L = lev(C, B, 1);
+    for (int k = 1; k <= L.nk; ++k) for (int i = 1; i <= L.ni; ++i) for (int j = 1; j <= L.nj; ++j)
+      B.cof[(long)(k - 1) * L.nij + (long)(i - 1) * L.nj + j] = F(B, B.pp.data(), i + pl - 1, j + pl - 1, k + pl - 1);
+    long incrp = 7L * (L.ni - 2) * (L.nj - 2) * (L.nk - 2);
+    for (int k = 2; k <= L.nk - 1; ++k) for (int i = 2; i <= L.ni - 1; ++i) for (int j = 2; j <= L.nj - 1; ++j)
+      B.cof[B.faz[1] + (long)(k - 2) * (L.ni - 2) * (L.nj - 2) + (long)(i - 2) * (L.nj - 2) + (j - 1) + incrp] =
+          F(B, B.su.data(), i + pl - 1, j + pl - 1, k + pl - 1);
+  }
+  int ngrd = C.ngrd_gl;
+  int glevel = 1, kcycle = 1, nrel;
+  std::vector<int> kount(ngrd + 1, 0);
+  mgrelax(C, 1, C.irestr);
+  if (ngrd != 1) {
+    mgrestr(C, glevel + 1);
+    for (int l = 1; l <= ngrd; ++l) kount[l] = 0;
+    glevel = glevel + 1;
+    nrel = C.irestr;
+    for (;;) {
+      if (glevel == 1) break;
+      kount[glevel] = kount[glevel] + 1;
+      mgrelax(C, glevel, nrel);
+      if (kount[glevel] == kcycle + 1) {
+        mgcorr(C, glevel - 1);
+        kount[glevel] = 0;
+        glevel = glevel - 1;
+        nrel = C.iproln;
+      } else if (glevel < ngrd) {
+        mgrestr(C, glevel + 1);
+        glevel = glevel + 1;
+        nrel = C.irestr;
+      } else {
+        mgrelax(C, glevel, C.iproln);
+        mgcorr(C, glevel - 1);
+        nrel = C.iproln;
+        glevel = ngrd - 1;
+      }
+    }
+  }
+  mgrelax(C, 1, C.iproln);
+  for (auto &B : C.b) {
+    Lev L = lev(C, B, 1);
+    for (int k = 1; k <= L.nk; ++k) for (int i = 1; i <= L.ni; ++i) for (int j = 1; j <= L.nj; ++j)
+      F(B, B.pp.data(), i + pl - 1, j + pl - 1, k + pl - 1) = B.cof[(long)(k - 1) * L.nij + (long)(i - 1) * L.nj + j];
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* Field halos exchange(op) for op 1..4 (exchange.for:2-23): periodic   */
+/* exchange_bc (exchange_bc.for:2-841) then the face part of            */
+/* exchange_smlvl (exchange.for:343-2498).  The corner/edge part of     */
+/* exchange_smlvl is unpacked before the faces and only its ghost       */
+/* edges and corners survive; nothing on this path reads those, so it   */
+/* is not restated.  One ghost layer (ly = 0): calvel and calmas with   */
+/* differencing = 1 read no other.                                      */
+/* ------------------------------------------------------------------ */
+double *field_of(Blk &B, int op) { return op == 1 ? B.u : op == 2 ? B.v : op == 3 ? B.w : B.p; }
+void franges(Blk &B, int op, int &is, int &ie, int &js, int &je, int &ks, int &ke) {
+  if (op == 1) { is = B.isu; ie = B.ieu; js = B.jsu; je = B.jeu; ks = B.ksu; ke = B.keu; }
+  else if (op == 2) { is = B.isv; ie = B.iev; js = B.jsv; je = B.jev; ks = B.ksv; ke = B.kev; }
+  else if (op == 3) { is = B.isw; ie = B.iew; js = B.jsw; je = B.jew; ks = B.ksw; ke = B.kew; }
+  else { is = B.isp; ie = B.iep; js = B.jsp; je = B.jep; ks = B.ksp; ke = B.kep; }
+}
+
+void exchange_bc(Ctx &C, int op) {
+  const int ly = 0;
+  for (int ax = 0; ax < 3; ++ax) {
+    for (auto &B : C.b) {
+      int bcp = ax == 0 ? B.d.bc_west : ax == 1 ? B.d.bc_south : B.d.bc_bottom;
+      int bcn = ax == 0 ? B.d.bc_east : ax == 1 ? B.d.bc_north : B.d.bc_top;
+      if (!(bcp == 5 || bcn == 5)) continue;
+      int prev = ax == 0 ? B.d.iprev : ax == 1 ? B.d.jprev : B.d.kprev;
+      int next = ax == 0 ? B.d.inext : ax == 1 ? B.d.jnext : B.d.knext;
+      int perp = ax == 0 ? B.d.per_ip : ax == 1 ? B.d.per_jp : B.d.per_kp;
+      int pern = ax == 0 ? B.d.per_in : ax == 1 ? B.d.per_jn : B.d.per_kn;
+      int is, ie, js, je, ks, ke;
+      franges(B, op, is, ie, js, je, ks, ke);
+      double *fi = field_of(B, op);
+      int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
+      int n1 = ax == 0 ? B.ttc_j : B.ttc_i, n2 = ax == 2 ? B.ttc_j : B.ttc_k;
+      auto at = [&](int a, int s, int t) -> double & {
+        if (ax == 0) return F(B, fi, a, s, t);
+        if (ax == 1) return F(B, fi, s, a, t);
+        return F(B, fi, s, t, a);
+      };
+      if (prev < 0) {
+        if (next < 0) {
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(s0 - 1 - ly, s, t) = at(e0 - ly, s, t);
+        } else {
+          Blk &P = C.b[C.indid.at(perp)];
+          P.frp[ax + 1].assign((size_t)n1 * n2 + 1, 0.0);
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) P.frp[ax + 1][(size_t)(t - 1) * n1 + s] = at(s0 + ly, s, t);
+        }
+      }
+      if (next < 0) {
+        if (prev < 0) {
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(e0 + 1 + ly, s, t) = at(s0 + ly, s, t);
+        } else {
+          Blk &N = C.b[C.indid.at(pern)];
+          N.frm[ax + 1].assign((size_t)n1 * n2 + 1, 0.0);
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) N.frm[ax + 1][(size_t)(t - 1) * n1 + s] = at(e0 - ly, s, t);
+        }
+      }
+    }
+    for (auto &B : C.b) {
+      int bcp = ax == 0 ? B.d.bc_west : ax == 1 ? B.d.bc_south : B.d.bc_bottom;
+      int bcn = ax == 0 ? B.d.bc_east : ax == 1 ? B.d.bc_north : B.d.bc_top;
+      if (!(bcp == 5 || bcn == 5)) continue;
+      int prev = ax == 0 ? B.d.iprev : ax == 1 ? B.d.jprev : B.d.kprev;
+      int next = ax == 0 ? B.d.inext : ax == 1 ? B.d.jnext : B.d.knext;
+      int is, ie, js, je, ks, ke;
+      franges(B, op, is, ie, js, je, ks, ke);
+      double *fi = field_of(B, op);
+      int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
+      int n1 = ax == 0 ? B.ttc_j : B.ttc_i, n2 = ax == 2 ? B.ttc_j : B.ttc_k;
+      auto at = [&](int a, int s, int t) -> double & {
+        if (ax == 0) return F(B, fi, a, s, t);
+        if (ax == 1) return F(B, fi, s, a, t);
+        return F(B, fi, s, t, a);
+      };
+      if (prev < 0 && next >= 0)
+        for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(s0 - 1 - ly, s, t) = B.frm[ax + 1][(size_t)(t - 1) * n1 + s];
+      if (next < 0 && prev >= 0)
+        for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(e0 + 1 + ly, s, t) = B.frp[ax + 1][(size_t)(t - 1) * n1 + s];
+    }
+  }
+}
+
+void exchange_smlvl_faces(Ctx &C, int op) {
+  const int ly = 0;
+  /* pack: all six faces of every block from one snapshot */
+  std::vector<std::vector<double>> bm(C.b.size() * 4), bp(C.b.size() * 4);
+  for (size_t ib = 0; ib < C.b.size(); ++ib) {
+    Blk &B = C.b[ib];
+    int is, ie, js, je, ks, ke;
+    franges(B, op, is, ie, js, je, ks, ke);
+    double *fi = field_of(B, op);
+    int nbr_p[3] = {B.d.iprev, B.d.jprev, B.d.kprev}, nbr_n[3] = {B.d.inext, B.d.jnext, B.d.knext};
+    for (int ax = 0; ax < 3; ++ax) {
+      int n1 = ax == 0 ? B.ttc_j : B.ttc_i, n2 = ax == 2 ? B.ttc_j : B.ttc_k;
+      auto at = [&](int a, int s, int t) -> double & {
+        if (ax == 0) return F(B, fi, a, s, t);
+        if (ax == 1) return F(B, fi, s, a, t);
+        return F(B, fi, s, t, a);
+      };
+      int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
+      if (nbr_p[ax] >= 0) { /* prev neighbour receives my first plane in its recvb_p */
+        auto &R = bp[C.indid.at(nbr_p[ax]) * 4 + ax + 1];
+        R.assign((size_t)n1 * n2 + 1, 0.0);
+        for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) R[(size_t)(t - 1) * n1 + s] = at(s0 + ly, s, t);
+      }
+      if (nbr_n[ax] >= 0) {
+        auto &R = bm[C.indid.at(nbr_n[ax]) * 4 + ax + 1];
+        R.assign((size_t)n1 * n2 + 1, 0.0);
+        for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) R[(size_t)(t - 1) * n1 + s] = at(e0 - ly, s, t);
+      }
+    }
+  }
+  /* unpack: interior tangential range pl+1 .. n-pl (exchange.for:2402-2490) */
+  for (size_t ib = 0; ib < C.b.size(); ++ib) {
+    Blk &B = C.b[ib];
+    int is, ie, js, je, ks, ke;
+    franges(B, op, is, ie, js, je, ks, ke);
+    double *fi = field_of(B, op);
+    int pl = C.pl;
+    int nbr_p[3] = {B.d.iprev, B.d.jprev, B.d.kprev}, nbr_n[3] = {B.d.inext, B.d.jnext, B.d.knext};
+    for (int ax = 0; ax < 3; ++ax) {
+      int n1 = ax == 0 ? B.ttc_j : B.ttc_i;
+      int sp1 = pl + 1, ep1 = (ax == 0 ? B.ttc_j : B.ttc_i) - pl;
+      int sp2 = pl + 1, ep2 = (ax == 2 ? B.ttc_j : B.ttc_k) - pl;
+      auto at = [&](int a, int s, int t) -> double & {
+        if (ax == 0) return F(B, fi, a, s, t);
+        if (ax == 1) return F(B, fi, s, a, t);
+        return F(B, fi, s, t, a);
+      };
+      int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
+      if (nbr_p[ax] >= 0) {
+        auto &R = bm[ib * 4 + ax + 1];
+        for (int t = sp2; t <= ep2; ++t) for (int s = sp1; s <= ep1; ++s) at(s0 - 1 - ly, s, t) = R[(size_t)(t - 1) * n1 + s];
+      }
+      if (nbr_n[ax] >= 0) {
+        auto &R = bp[ib * 4 + ax + 1];
+        for (int t = sp2; t <= ep2; ++t) for (int s = sp1; s <= ep1; ++s) at(e0 + 1 + ly, s, t) = R[(size_t)(t - 1) * n1 + s];
+      }
+    }
+  }
+}
+
+void exchange(Ctx &C, int op) {
+  if (C.periodic) exchange_bc(C, op);
+  exchange_smlvl_faces(C, op);
+}
+
+/* pbound (press.for:77-137) */
+void pbound(Ctx &C) {
+  for (auto &B : C.b) {
+    double *p = B.p;
+    int isp = B.isp, iep = B.iep, jsp = B.jsp, jep = B.jep, ksp = B.ksp, kep = B.kep;
+    if (B.d.iprev < 0 && B.d.bc_west != 5)
+      for (int k = ksp - 1; k <= kep + 1; ++k) for (int j = jsp - 1; j <= jep + 1; ++j) F(B, p, isp - 1, j, k) = F(B, p, isp, j, k);
+    if (B.d.inext < 0 && B.d.bc_east != 5)
+      for (int k = ksp - 1; k <= kep + 1; ++k) for (int j = jsp - 1; j <= jep + 1; ++j) F(B, p, iep + 1, j, k) = F(B, p, iep, j, k);
+    if (B.d.jprev < 0 && B.d.bc_south != 5)
+      for (int k = ksp - 1; k <= kep + 1; ++k) for (int i = isp - 1; i <= iep + 1; ++i) F(B, p, i, jsp - 1, k) = F(B, p, i, jsp, k);
+    if (B.d.jnext < 0 && B.d.bc_north != 5)
+      for (int k = ksp - 1; k <= kep + 1; ++k) for (int i = isp - 1; i <= iep + 1; ++i) F(B, p, i, jep + 1, k) = F(B, p, i, jep, k);
+    if (B.d.kprev < 0 && B.d.bc_bottom != 5)
+      for (int j = jsp - 1; j <= jep + 1; ++j) for (int i = isp - 1; i <= iep + 1; ++i) F(B, p, i, j, ksp - 1) = F(B, p, i, j, ksp);
+    if (B.d.knext < 0 && B.d.bc_top != 5)
+      for (int j = jsp - 1; j <= jep + 1; ++j) for (int i = isp - 1; i <= iep + 1; ++i) F(B, p, i, j, kep + 1) = F(B, p, i, j, kep);
+  }
+}
+
+/* EXT: distance between the centres of cells a and a+1 along an axis,
+ * equal to dx on a uniform grid. */
+inline double dface(const std::vector<double> &w, int a0) { return 0.5 * (w[a0] + w[a0 + 1]); }
+
+/* calvel (press.for:139-200), non-LSM branch. */
+void calvel(Ctx &C) {
+  double dt = C.dt, alfapr = C.alfapr;
+  for (auto &B : C.b) {
+    int o = B.isp - 1; /* field index i <-> level-1 ghost-inclusive index i - o */
+    for (int k = B.ksu; k <= B.keu; ++k) for (int i = B.isu; i <= B.ieu; ++i) for (int j = B.jsu; j <= B.jeu; ++j) {
+      double dxl = B.stretched ? dface(B.hx[1], i - o) : B.d.dx;
+      F(B, B.u, i, j, k) = (F(B, B.ustar, i, j, k) - dt * alfapr * (F(B, B.p, i + 1, j, k) - F(B, B.p, i, j, k)) / dxl);
+    }
+    for (int k = B.ksv; k <= B.kev; ++k) for (int i = B.isv; i <= B.iev; ++i) for (int j = B.jsv; j <= B.jev; ++j) {
+      double dyl = B.stretched ? dface(B.hy[1], j - o) : B.d.dy;
+      F(B, B.v, i, j, k) = (F(B, B.vstar, i, j, k) - dt * alfapr * (F(B, B.p, i, j + 1, k) - F(B, B.p, i, j, k)) / dyl);
+    }
+    for (int k = B.ksw; k <= B.kew; ++k) for (int i = B.isw; i <= B.iew; ++i) for (int j = B.jsw; j <= B.jew; ++j) {
+      double dzl = B.stretched ? dface(B.hz[1], k - o) : B.d.dz;
+      F(B, B.w, i, j, k) = (F(B, B.wstar, i, j, k) - dt * alfapr * (F(B, B.p, i, j, k + 1) - F(B, B.p, i, j, k)) / dzl);
+    }
+  }
+  exchange(C, 1);
+  exchange(C, 2);
+  exchange(C, 3);
+}
+
+/* calmas (press.for:2-75), differencing = 1, non-LSM branch. */
+void calmas(Ctx &C) {
+  double rmax = 0.0, resor;
+  for (auto &B : C.b) {
+    int o = B.isp - 1;
+    for (int k = B.ksp; k <= B.kep; ++k) for (int i = B.isp; i <= B.iep; ++i) for (int j = B.jsp; j <= B.jep; ++j) {
+      double hxl = B.stretched ? B.hx[1][i - o] : B.d.dx;
+      double hyl = B.stretched ? B.hy[1][j - o] : B.d.dy;
+      double hzl = B.stretched ? B.hz[1][k - o] : B.d.dz;
+      double fact = ((F(B, B.u, i, j, k) - F(B, B.u, i - 1, j, k)) / hxl +
+                     (F(B, B.v, i, j, k) - F(B, B.v, i, j - 1, k)) / hyl +
+                     (F(B, B.w, i, j, k) - F(B, B.w, i, j, k - 1)) / hzl);
+      F(B, B.su.data(), i, j, k) = fact / C.dt;
+      double fact1 = fact * hxl * hyl * hzl;
+      resor = std::max(rmax, std::fabs(fact1));
+      rmax = std::max(resor, std::fabs(fact1));
+    }
+  }
+  C.rmax = rmax; /* MPI_ALLREDUCE(MAX) over one rank */
+}
+
+/* newsolv_mg (newsolv_mg.for:2-102) */
+int newsolv_mg(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
+  calvel(C);
+  calmas(C);
+  double rmax0 = C.rmax;
+  for (auto &B : C.b) std::fill(B.pp.begin(), B.pp.end(), 0.0);
+  double eps = C.eps_relative ? C.eps * rmax0 : C.eps;
+  int iter;
+  bool conv = false;
+  for (iter = 1; iter <= C.maxcy; ++iter) {
+    mgkcyc(C);
+    double ppref = 0.0;
+    for (auto &B : C.b)
+      for (int k = B.ksp - 1; k <= B.kep + 1; ++k) for (int i = B.isp - 1; i <= B.iep + 1; ++i) for (int j = B.jsp - 1; j <= B.jep + 1; ++j) {
+        F(B, B.p, i, j, k) = (F(B, B.p, i, j, k) + (F(B, B.pp.data(), i, j, k) - ppref));
+        F(B, B.pp.data(), i, j, k) = 0.0;
+      }
+    exchange(C, 4);
+    pbound(C);
+    calvel(C);
+    calmas(C);
+    if (hist && iter - 1 < cap) hist[iter - 1] = C.rmax;
+    if (C.rmax < eps && iter > 1) { conv = true; break; }
+  }
+  int status = MF3D_OK;
+  int iters = conv ? iter : C.maxcy;
+  if (!conv) status = MF3D_NOT_CONVERGED;
+  if (C.rmax > 100.0) status = MF3D_DIVERGED;
+  if (info) {
+    info->rmax = C.rmax; info->rmax0 = rmax0; info->iter = iters; info->status = status; info->ms_device = 0.0;
+  }
+  return status;
+}
+
+std::string g_err;
+
+int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm) {
+  if (nb <= 0 || !blocks || !prm) { g_err = "bad arguments"; return MF3D_E_INVALID; }
+  if (prm->mg_itrsch < 1 || prm->mg_itrsch > 3) { g_err = "mg_itrsch"; return MF3D_E_INVALID; }
+  if (prm->differencing != 1) { g_err = "differencing"; return MF3D_E_UNSUPPORTED; }
+  C.ngrd_gl = prm->ngrid; C.mg_itrsch = prm->mg_itrsch; C.irestr = prm->irestr; C.iproln = prm->iproln;
+  C.maxcy = prm->maxcy; C.eps = prm->eps; C.eps_relative = prm->eps_relative; C.pl = prm->pl;
+  C.periodic = false;
+  C.b.resize(nb);
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    B.d = blocks[ib];
+    B.ngrid = prm->ngrid;
+    int pl = prm->pl;
+    int pow2 = 1 << (B.ngrid - 1);
+    if (B.d.nx % pow2 || B.d.ny % pow2 || B.d.nz % pow2) { g_err = "not divisible"; return MF3D_E_INVALID; }
+    C.indid[B.d.id] = ib;
+    B.isp = 1 + pl; B.iep = B.d.nx + B.isp - 1;
+    B.jsp = 1 + pl; B.jep = B.d.ny + B.jsp - 1;
+    B.ksp = 1 + pl; B.kep = B.d.nz + B.ksp - 1;
+    B.isu = B.isv = B.isw = B.isp; B.ieu = B.iev = B.iew = B.iep;
+    B.jsu = B.jsv = B.jsw = B.jsp; B.jeu = B.jev = B.jew = B.jep;
+    B.ksu = B.ksv = B.ksw = B.ksp; B.keu = B.kev = B.kew = B.kep;
+    if (B.d.inext < 0 && B.d.bc_east != 5) B.ieu = B.ieu - 1;
+    if (B.d.jnext < 0 && B.d.bc_north != 5) B.jev = B.jev - 1;
+    if (B.d.knext < 0 && B.d.bc_top != 5) B.kew = B.kew - 1;
+    B.ttc_i = B.d.nx + 2 * pl; B.ttc_j = B.d.ny + 2 * pl; B.ttc_k = B.d.nz + 2 * pl;
+    if (B.d.bc_west == 5 || B.d.bc_east == 5 || B.d.bc_south == 5 || B.d.bc_north == 5 || B.d.bc_bottom == 5 || B.d.bc_top == 5)
+      C.periodic = true;
+    B.stretched = B.d.hx || B.d.hy || B.d.hz;
+    B.hx = level_widths(B.d.hx, B.d.nx, B.d.dx, B.ngrid);
+    B.hy = level_widths(B.d.hy, B.d.ny, B.d.dy, B.ngrid);
+    B.hz = level_widths(B.d.hz, B.d.nz, B.d.dz, B.ngrid);
+    size_t ttc = (size_t)B.ttc_i * B.ttc_j * B.ttc_k;
+    B.su.assign(ttc, 0.0);
+    B.pp.assign(ttc, 0.0);
+  }
+  coeff(C);
+  return MF3D_OK;
+}
+
+} /* namespace */
+
+extern "C" {
+
+const char *orc_last_error(void) { return g_err.c_str(); }
+
+/* The whole projection on host arrays, in place. */
+int orc_newsolv_mg(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, const mf3d_fields *fields,
+                   double dt, double alfapr, mf3d_solve_info *info, double *hist, int cap) {
+  Ctx C;
+  int st = setup(C, blocks, nb, prm);
+  if (st) return st;
+  C.dt = dt; C.alfapr = alfapr;
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    B.ustar = fields[ib].ustar; B.vstar = fields[ib].vstar; B.wstar = fields[ib].wstar;
+    B.u = fields[ib].u; B.v = fields[ib].v; B.w = fields[ib].w; B.p = fields[ib].p;
+  }
+  st = newsolv_mg(C, hist, cap, info);
+  for (int ib = 0; ib < nb; ++ib)
+    if (fields[ib].su) std::memcpy(fields[ib].su, C.b[ib].su.data(), C.b[ib].su.size() * sizeof(double));
+  return st;
+}
+
+/* One V-cycle: su[b] (ttc) in, pp[b] (ttc) out, starting from pp = 0. */
+int orc_mgkcyc(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, double *const *su, double *const *pp) {
+  Ctx C;
+  int st = setup(C, blocks, nb, prm);
+  if (st) return st;
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    std::memcpy(B.su.data(), su[ib], B.su.size() * sizeof(double));
+  }
+  mgkcyc(C);
+  for (int ib = 0; ib < nb; ++ib) std::memcpy(pp[ib], C.b[ib].pp.data(), C.b[ib].pp.size() * sizeof(double));
+  return MF3D_OK;
+}
+
+/* exchangepp (+ mgbound + exchbc_mgpp) on level `level` of arrays given
+ * ghost-inclusive, i fastest: fi[b][(k*(ny+2) + j)*(nx+2) + i]. */
+int orc_exchangepp(const mf3d_block_desc *blocks, int nb, int ngrid, int level, double *const *fi) {
+  mf3d_params prm;
+  std::memset(&prm, 0, sizeof prm);
+  prm.ngrid = ngrid; prm.mg_itrsch = 3; prm.irestr = 1; prm.iproln = 1; prm.maxcy = 1; prm.pl = 1; prm.differencing = 1;
+  Ctx C;
+  int st = setup(C, blocks, nb, &prm);
+  if (st) return st;
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    Lev L = lev(C, B, level);
+    for (int k = 1; k <= L.nk; ++k) for (int j = 1; j <= L.nj; ++j) for (int i = 1; i <= L.ni; ++i)
+      B.cof[PH(L, i, j, k)] = fi[ib][((size_t)(k - 1) * L.nj + (j - 1)) * L.ni + (i - 1)];
+  }
+  exchangepp(C, level);
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    Lev L = lev(C, B, level);
+    for (int k = 1; k <= L.nk; ++k) for (int j = 1; j <= L.nj; ++j) for (int i = 1; i <= L.ni; ++i)
+      fi[ib][((size_t)(k - 1) * L.nj + (j - 1)) * L.ni + (i - 1)] = B.cof[PH(L, i, j, k)];
+  }
+  return MF3D_OK;
+}
+
+/* Apply the level-1 operator A (the residual form of mgrestr,
+ * mgsolver.for:702-709, with rhs = 0, negated) to phi given ghost-inclusive
+ * i fastest; ghosts are taken as given.  out = sum a_nb phi_nb + ap phi. */
+int orc_apply_operator(const mf3d_block_desc *blocks, int nb, int ngrid, int level, double *const *phi, double *const *out) {
+  mf3d_params prm;
+  std::memset(&prm, 0, sizeof prm);
+  prm.ngrid = ngrid; prm.mg_itrsch = 3; prm.irestr = 1; prm.iproln = 1; prm.maxcy = 1; prm.pl = 1; prm.differencing = 1;
+  Ctx C;
+  int st = setup(C, blocks, nb, &prm);
+  if (st) return st;
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    Lev L = lev(C, B, level);
+    long nij2 = (long)(L.ni - 2) * (L.nj - 2), incr = nij2 * (L.nk - 2);
+    auto G = [&](double *a, int i, int j, int k) -> double & { return a[((size_t)(k - 1) * L.nj + (j - 1)) * L.ni + (i - 1)]; };
+    for (int k = 2; k <= L.nk - 1; ++k) for (int i = 2; i <= L.ni - 1; ++i) for (int j = 2; j <= L.nj - 1; ++j) {
+      long w = B.faz[level] + (long)(k - 2) * nij2 + (long)(i - 2) * (L.nj - 2) + (j - 1);
+      const double *c = B.cof.data();
+      G(out[ib], i, j, k) = (c[w] * G(phi[ib], i - 1, j, k) + c[w + incr] * G(phi[ib], i + 1, j, k) +
+                             c[w + 2 * incr] * G(phi[ib], i, j - 1, k) + c[w + 3 * incr] * G(phi[ib], i, j + 1, k) +
+                             c[w + 4 * incr] * G(phi[ib], i, j, k - 1) + c[w + 5 * incr] * G(phi[ib], i, j, k + 1) +
+                             c[w + 6 * incr] * G(phi[ib], i, j, k));
+    }
+  }
+  return MF3D_OK;
+}
+
+/* Neighbour search restated from alloc_dom.for:456-1150 (tolerance 1e-8),
+ * over block extents; xst..zen = the bounding box (the domain extents). */
+int orc_build_topology(int nb, const double *ext, const int *bc6, double dx, double dy, double dz, mf3d_block_desc *out) {
+  double xst = 1e300, xen = -1e300, yst = 1e300, yen = -1e300, zst = 1e300, zen = -1e300;
+  for (int i = 0; i < nb; ++i) {
+    xst = std::min(xst, ext[6 * i]); xen = std::max(xen, ext[6 * i + 1]);
+    yst = std::min(yst, ext[6 * i + 2]); yen = std::max(yen, ext[6 * i + 3]);
+    zst = std::min(zst, ext[6 * i + 4]); zen = std::max(zen, ext[6 * i + 5]);
+  }
+  auto X = [&](int i, int c) { return ext[6 * i + c]; };
+  auto eq = [](double a, double b) { return std::fabs(a - b) < 1e-8; };
+  for (int b = 0; b < nb; ++b) {
+    mf3d_block_desc &d = out[b];
+    std::memset(&d, 0, sizeof d);
+    d.id = b; d.dx = dx; d.dy = dy; d.dz = dz;
+    d.xsl = X(b, 0); d.xel = X(b, 1); d.ysl = X(b, 2); d.yel = X(b, 3); d.zsl = X(b, 4); d.zel = X(b, 5);
+    d.nx = (int)std::lround((d.xel - d.xsl) / dx);
+    d.ny = (int)std::lround((d.yel - d.ysl) / dy);
+    d.nz = (int)std::lround((d.zel - d.zsl) / dz);
+    d.bc_west = bc6[0]; d.bc_east = bc6[1]; d.bc_south = bc6[2]; d.bc_north = bc6[3]; d.bc_bottom = bc6[4]; d.bc_top = bc6[5];
+    int say;
+    auto find = [&](auto pred) { int r = -1; say = 0; for (int i = 0; i < nb; ++i) if (i != b && pred(i)) { r = i; ++say; } return r; };
+    d.iprev = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.ysl, X(i, 2)) && eq(d.yel, X(i, 3)) && eq(d.zsl, X(i, 4)) && eq(d.zel, X(i, 5)); });
+    if (say > 1) { g_err = "more than one previous neighbour in x"; return MF3D_E_INVALID; }
+    d.inext = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.ysl, X(i, 2)) && eq(d.yel, X(i, 3)) && eq(d.zsl, X(i, 4)) && eq(d.zel, X(i, 5)); });
+    if (say > 1) { g_err = "more than one next neighbour in x"; return MF3D_E_INVALID; }
+    d.jprev = find([&](int i) { return eq(d.ysl, X(i, 3)) && eq(d.xsl, X(i, 0)) && eq(d.xel, X(i, 1)) && eq(d.zsl, X(i, 4)) && eq(d.zel, X(i, 5)); });
+    if (say > 1) { g_err = "more than one previous neighbour in y"; return MF3D_E_INVALID; }
+    d.jnext = find([&](int i) { return eq(d.yel, X(i, 2)) && eq(d.xsl, X(i, 0)) && eq(d.xel, X(i, 1)) && eq(d.zsl, X(i, 4)) && eq(d.zel, X(i, 5)); });
+    if (say > 1) { g_err = "more than one next neighbour in y"; return MF3D_E_INVALID; }
+    d.kprev = find([&](int i) { return eq(d.zsl, X(i, 5)) && eq(d.xsl, X(i, 0)) && eq(d.xel, X(i, 1)) && eq(d.ysl, X(i, 2)) && eq(d.yel, X(i, 3)); });
+    if (say > 1) { g_err = "more than one previous neighbour in z"; return MF3D_E_INVALID; }
+    d.knext = find([&](int i) { return eq(d.zel, X(i, 4)) && eq(d.xsl, X(i, 0)) && eq(d.xel, X(i, 1)) && eq(d.ysl, X(i, 2)) && eq(d.yel, X(i, 3)); });
+    if (say > 1) { g_err = "more than one next neighbour in z"; return MF3D_E_INVALID; }
+    /* corners (alloc_dom.for:632-750) */
+    d.corprev[0] = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.ysl, X(i, 3)) && eq(d.zsl, X(i, 5)); });
+    d.corprev[1] = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.yel, X(i, 2)) && eq(d.zsl, X(i, 5)); });
+    d.corprev[2] = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.yel, X(i, 2)) && eq(d.zsl, X(i, 5)); });
+    d.corprev[3] = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.ysl, X(i, 3)) && eq(d.zsl, X(i, 5)); });
+    d.cornext[0] = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.yel, X(i, 2)) && eq(d.zel, X(i, 4)); });
+    d.cornext[1] = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.ysl, X(i, 3)) && eq(d.zel, X(i, 4)); });
+    d.cornext[2] = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.ysl, X(i, 3)) && eq(d.zel, X(i, 4)); });
+    d.cornext[3] = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.yel, X(i, 2)) && eq(d.zel, X(i, 4)); });
+    /* edges (alloc_dom.for:752-968) */
+    auto ysame = [&](int i) { return eq(d.ysl, X(i, 2)) && eq(d.yel, X(i, 3)); };
+    auto xsame = [&](int i) { return eq(d.xsl, X(i, 0)) && eq(d.xel, X(i, 1)); };
+    auto zsame = [&](int i) { return eq(d.zsl, X(i, 4)) && eq(d.zel, X(i, 5)); };
+    d.edgprev[0] = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.zsl, X(i, 5)) && ysame(i); });
+    d.edgprev[1] = find([&](int i) { return eq(d.yel, X(i, 2)) && eq(d.zsl, X(i, 5)) && xsame(i); });
+    d.edgprev[2] = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.zsl, X(i, 5)) && ysame(i); });
+    d.edgprev[3] = find([&](int i) { return eq(d.ysl, X(i, 3)) && eq(d.zsl, X(i, 5)) && xsame(i); });
+    d.edgprev[4] = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.ysl, X(i, 3)) && zsame(i); });
+    d.edgprev[5] = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.yel, X(i, 2)) && zsame(i); });
+    d.edgnext[0] = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.zel, X(i, 4)) && ysame(i); });
+    d.edgnext[1] = find([&](int i) { return eq(d.ysl, X(i, 3)) && eq(d.zel, X(i, 4)) && xsame(i); });
+    d.edgnext[2] = find([&](int i) { return eq(d.xsl, X(i, 1)) && eq(d.zel, X(i, 4)) && ysame(i); });
+    d.edgnext[3] = find([&](int i) { return eq(d.yel, X(i, 2)) && eq(d.zel, X(i, 4)) && xsame(i); });
+    d.edgnext[4] = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.yel, X(i, 2)) && zsame(i); });
+    d.edgnext[5] = find([&](int i) { return eq(d.xel, X(i, 0)) && eq(d.ysl, X(i, 3)) && zsame(i); });
+    /* periodic partners (alloc_dom.for:971-1150) */
+    d.per_ip = d.per_in = d.per_jp = d.per_jn = d.per_kp = d.per_kn = -1;
+    if (d.bc_west == 5 && d.iprev < 0) d.per_ip = find([&](int i) { return eq(xen, X(i, 1)) && ysame(i) && zsame(i); });
+    if (d.bc_east == 5 && d.inext < 0) d.per_in = find([&](int i) { return eq(xst, X(i, 0)) && ysame(i) && zsame(i); });
+    if (d.bc_south == 5 && d.jprev < 0) d.per_jp = find([&](int i) { return eq(yen, X(i, 3)) && xsame(i) && zsame(i); });
+    if (d.bc_north == 5 && d.jnext < 0) d.per_jn = find([&](int i) { return eq(yst, X(i, 2)) && xsame(i) && zsame(i); });
+    if (d.bc_bottom == 5 && d.kprev < 0) d.per_kp = find([&](int i) { return eq(zen, X(i, 5)) && xsame(i) && ysame(i); });
+    if (d.bc_top == 5 && d.knext < 0) d.per_kn = find([&](int i) { return eq(zst, X(i, 4)) && xsame(i) && ysame(i); });
+  }
+  return MF3D_OK;
+}
+
+} /* extern "C" */

@@ -1,0 +1,139 @@
+"""GPU parity: the CUDA path against the oracle on the same seeded inputs.
+
+FP64 is expected bit-identical (the kernels keep the reference's evaluation
+order and are built with -fmad=false); the asserted bar is the stated
+tolerance: relative L2 <= 1e-10 for the pressure and the rmax history.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from multiflow3d_b200.problems import Problem, fields_struct, PERIODIC, WALL
+from multiflow3d_b200.solver import Projection
+from multiflow3d_b200.abi import SolveInfo
+import oracle_bridge as ob
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-10  # north-star parity bar for the FP64 drop-in
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    den = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (den if den > 0 else 1.0)
+
+
+def oracle_solve(oracle, pr, prm, seed, fourier=0, p_random=False):
+    blocks = pr.block_fields(seed=seed, fourier_modes=fourier, p_random=p_random)
+    desc = pr.descriptors(oracle)
+    hist = np.zeros(max(prm.maxcy, 1))
+    info = SolveInfo()
+    st = oracle.orc_newsolv_mg(desc, pr.nblocks, C.byref(prm), fields_struct(blocks), 1.0, 1.0, C.byref(info),
+                               hist.ctypes.data_as(C.POINTER(C.c_double)), len(hist))
+    assert st >= 0
+    return blocks, info, hist[:info.iter]
+
+
+def gpu_solve(lib, cuda, pr, prm, seed, fourier=0, p_random=False):
+    import torch
+    blocks = pr.block_fields(seed=seed, fourier_modes=fourier, p_random=p_random)
+    dev = [{k: torch.from_numpy(v).to(cuda) for k, v in f.items()} for f in blocks]
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    res = proj.newsolv_mg_device(dev)
+    out = [{k: v.cpu().numpy() for k, v in f.items()} for f in dev]
+    proj.close()
+    return out, res
+
+
+TOPOLOGIES = [
+    # (px,py,pz, nx,ny,nz, bc, ngrid)
+    (1, 1, 1, 16, 8, 8, (PERIODIC, PERIODIC, WALL, WALL, PERIODIC, PERIODIC), 3),
+    (1, 1, 1, 8, 8, 8, (WALL, WALL, WALL, WALL, WALL, WALL), 3),
+    (2, 1, 1, 8, 8, 8, (PERIODIC, PERIODIC, WALL, WALL, PERIODIC, PERIODIC), 3),
+    (2, 2, 1, 8, 8, 4, (WALL, WALL, PERIODIC, PERIODIC, WALL, WALL), 3),
+    (2, 2, 2, 8, 8, 8, (PERIODIC, PERIODIC, WALL, WALL, PERIODIC, PERIODIC), 4),
+    (3, 1, 2, 4, 8, 4, (PERIODIC, PERIODIC, PERIODIC, PERIODIC, PERIODIC, PERIODIC), 3),
+]
+
+
+@pytest.mark.parametrize("scheme", [3, 1, 2])
+@pytest.mark.parametrize("topo", TOPOLOGIES)
+def test_vcycle_bitwise(lib, oracle, cuda, topo, scheme):
+    """One mgkcyc on random su: pp (interior + first ghost layer) bit-identical."""
+    import torch
+    px, py, pz, nx, ny, nz, bc, ngrid = topo
+    pr = Problem(px, py, pz, nx, ny, nz, bc=bc, ngrid=ngrid, pl=2)
+    prm = pr.params(mg_itrsch=scheme, irestr=2, iproln=1)
+    rng = np.random.default_rng(42)
+    su = [rng.uniform(-1, 1, size=pr.ttc) for _ in range(pr.nblocks)]
+    pp_ref = [np.zeros(pr.ttc) for _ in range(pr.nblocks)]
+    assert oracle.orc_mgkcyc(pr.descriptors(oracle), pr.nblocks, C.byref(prm), ob.ptr_array(su),
+                             ob.ptr_array(pp_ref)) == 0
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    su_d = [torch.from_numpy(a).to(cuda) for a in su]
+    pp_d = [torch.zeros(pr.ttc, dtype=torch.float64, device=cuda) for _ in range(pr.nblocks)]
+    proj.mgkcyc_device(su_d, pp_d)
+    proj.close()
+    pl = pr.pl
+    for b in range(pr.nblocks):
+        got = pp_d[b].cpu().numpy()[pl - 1:pl + nz + 1, pl - 1:pl + ny + 1, pl - 1:pl + nx + 1]
+        ref = pp_ref[b][pl - 1:pl + nz + 1, pl - 1:pl + ny + 1, pl - 1:pl + nx + 1]
+        assert np.array_equal(got, ref), f"block {b}: max diff {np.abs(got - ref).max()}"
+
+
+@pytest.mark.parametrize("scheme", [1, 2, 3])
+def test_newsolv_config1(lib, oracle, cuda, scheme):
+    """Config 1: 64x32x32 single-block channel (periodic x,z; walls y), 4 levels,
+    stop at relative rmax 1e-8: rmax history and pressure vs the oracle."""
+    pr = Problem(1, 1, 1, 64, 32, 32, ngrid=4, pl=2)
+    prm = pr.params(mg_itrsch=scheme, maxcy=60, eps=1e-8)
+    ref, info, hist = oracle_solve(oracle, pr, prm, seed=11)
+    got, res = gpu_solve(lib, cuda, pr, prm, seed=11)
+    assert info.status == 0 and res.status == 0
+    assert res.iter == info.iter
+    assert rel_l2(res.history, hist) <= REL_TOL
+    assert abs(res.rmax0 - info.rmax0) <= REL_TOL * info.rmax0
+    p_got, p_ref = pr.gather(got, "p"), pr.gather(ref, "p")
+    assert rel_l2(p_got, p_ref) <= REL_TOL
+    for k in ("u", "v", "w"):
+        assert rel_l2(pr.gather(got, k), pr.gather(ref, k)) <= REL_TOL
+    # the drop-in is in fact bit-identical
+    assert np.array_equal(res.history, hist)
+    assert np.array_equal(p_got, p_ref)
+
+
+@pytest.mark.parametrize("bc", [
+    (PERIODIC, PERIODIC, WALL, WALL, PERIODIC, PERIODIC),
+    (WALL, WALL, WALL, WALL, WALL, WALL),
+    (PERIODIC, PERIODIC, PERIODIC, PERIODIC, PERIODIC, PERIODIC),
+])
+def test_newsolv_multiblock(lib, oracle, cuda, bc):
+    """Config 2 shape at reduced size: 2x2x2 blocks of 16^3, 4 levels, tol 1e-10,
+    velocity = uniform noise + 4 smooth Fourier modes; random initial p."""
+    pr = Problem(2, 2, 2, 16, 16, 16, bc=bc, ngrid=4, pl=2)
+    prm = pr.params(mg_itrsch=3, maxcy=120, eps=1e-10)
+    ref, info, hist = oracle_solve(oracle, pr, prm, seed=5, fourier=4, p_random=True)
+    got, res = gpu_solve(lib, cuda, pr, prm, seed=5, fourier=4, p_random=True)
+    assert res.iter == info.iter and res.status == info.status
+    assert rel_l2(res.history, hist) <= REL_TOL
+    assert rel_l2(pr.gather(got, "p"), pr.gather(ref, "p")) <= REL_TOL
+    assert np.array_equal(res.history, hist)
+
+
+def test_host_entry_point_matches_device(lib, cuda):
+    """mf3d_newsolv_mg (host arrays, copies inside) == the device entry point."""
+    pr = Problem(2, 1, 1, 16, 16, 16, ngrid=3, pl=1)
+    prm = pr.params(mg_itrsch=3, maxcy=40, eps=1e-9)
+    host = pr.block_fields(seed=3)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    r_host = proj.newsolv_mg(host)
+    proj.close()
+    dev, r_dev = gpu_solve(lib, cuda, pr, prm, seed=3)
+    assert r_host.iter == r_dev.iter
+    assert np.array_equal(r_host.history, r_dev.history)
+    for b in range(pr.nblocks):
+        for k in ("p", "u", "v", "w"):
+            assert np.array_equal(pr.interior(host[b][k]), pr.interior(dev[b][k]))

@@ -1,0 +1,109 @@
+"""CPU-only checks of the native library's host logic (no GPU needed):
+the C ABI loads and exports every symbol of include/mf3d.h, the neighbour
+search matches the oracle's restatement of alloc_dom.for, and the halo copy
+map reproduces the oracle's literal exchangepp + mgbound + exchbc_mgpp."""
+import ctypes as C
+import itertools
+import os
+import re
+
+import numpy as np
+import pytest
+
+from multiflow3d_b200 import abi
+from multiflow3d_b200.problems import Problem, PERIODIC, WALL
+import oracle_bridge as ob
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    txt = open(os.path.join(ROOT, "include", "mf3d.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|long long|const char \*)\s*\*?\s*(mf3d_\w+)\s*\(", txt, re.M)))
+
+
+def test_exports_every_header_symbol(lib):
+    syms = header_symbols()
+    assert len(syms) >= 10
+    assert set(syms) == set(abi.EXPORTED_SYMBOLS)
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert lib.mf3d_abi_version() == 1
+    assert lib.mf3d_status_string(abi.MF3D_NOT_CONVERGED) == b"not converged"
+
+
+def test_ctypes_struct_sizes_match_header(lib):
+    # a descriptor round-trips through the library's topology builder
+    pr = Problem(2, 1, 1, 8, 8, 8)
+    d = pr.descriptors(lib)
+    assert d[0].inext == 1 and d[1].iprev == 0
+    assert d[0].nx == 8 and d[1].xsl == pytest.approx(8 * pr.dx)
+
+
+FIELDS = [f for f, _ in abi.BlockDesc._fields_ if f not in ("hx", "hy", "hz")]
+LAYOUTS = [(1, 1, 1), (2, 1, 1), (1, 2, 1), (2, 2, 2), (3, 2, 1), (1, 1, 3)]
+BCS = list(itertools.product([PERIODIC, WALL], repeat=3))
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_topology_matches_oracle(lib, oracle, layout):
+    for bcs in BCS:
+        bc = (bcs[0], bcs[0], bcs[1], bcs[1], bcs[2], bcs[2])
+        pr = Problem(*layout, 8, 6, 4, bc=bc, ngrid=2)
+        d1, d2 = pr.descriptors(lib), pr.descriptors(oracle)
+        for b in range(pr.nblocks):
+            for f in FIELDS:
+                a, c = getattr(d1[b], f), getattr(d2[b], f)
+                if hasattr(a, "__len__"):
+                    a, c = list(a), list(c)
+                assert a == c, (layout, bc, b, f)
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_halo_map_matches_oracle_exchangepp(lib, oracle, layout):
+    """Applying the library's (dst, src) copy map to random level data equals
+    the oracle's sequence exchangepp -> mgbound -> exchbc_mgpp, bit for bit,
+    for every periodic/wall combination and two levels."""
+    for bcs in BCS:
+        bc = (bcs[0], bcs[0], bcs[1], bcs[1], bcs[2], bcs[2])
+        pr = Problem(*layout, 8, 6, 4, bc=bc, ngrid=2)
+        d1, d2 = pr.descriptors(lib), pr.descriptors(oracle)
+        for level in (1, 2):
+            shape = ((pr.nz >> (level - 1)) + 2, (pr.ny >> (level - 1)) + 2, (pr.nx >> (level - 1)) + 2)
+            rng = np.random.default_rng(level)
+            arrs = [rng.standard_normal(shape) for _ in range(pr.nblocks)]
+            ref = [a.copy() for a in arrs]
+            assert oracle.orc_exchangepp(d2, pr.nblocks, pr.ngrid, level, ob.ptr_array(ref)) == 0
+            n = lib.mf3d_halo_map(d1, pr.nblocks, pr.ngrid, level, None, None)
+            dst = (C.c_longlong * n)()
+            src = (C.c_longlong * n)()
+            assert lib.mf3d_halo_map(d1, pr.nblocks, pr.ngrid, level, dst, src) == n
+            flat = np.concatenate([a.ravel() for a in arrs])
+            out = flat.copy()
+            out[np.array(dst[:], dtype=np.int64)] = flat[np.array(src[:], dtype=np.int64)]
+            assert np.array_equal(out, np.concatenate([a.ravel() for a in ref])), (layout, bc, level)
+
+
+def test_create_rejects_bad_config_without_gpu(lib):
+    """Divisibility rule of localparameters.for:201-206 is checked before any
+    device work."""
+    pr = Problem(1, 1, 1, 12, 8, 8, ngrid=4)
+    ctx = C.c_void_p()
+    st = lib.mf3d_create(pr.descriptors(lib), 1, C.byref(pr.params()), C.byref(ctx))
+    assert st == abi.MF3D_E_INVALID
+    assert b"not correct for mgsolver" in lib.mf3d_last_error()
+    prm = pr.params()
+    prm.mg_itrsch = 7
+    assert lib.mf3d_create(pr.descriptors(lib), 1, C.byref(prm), C.byref(ctx)) == abi.MF3D_E_INVALID
+    prm = Problem(1, 1, 1, 8, 8, 8, ngrid=2).params()
+    prm.differencing = 2
+    assert lib.mf3d_create(Problem(1, 1, 1, 8, 8, 8, ngrid=2).descriptors(lib), 1, C.byref(prm),
+                           C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED
+
+
+def test_topology_rejects_fractional_extent(lib):
+    ext = np.array([0.0, 1.05, 0.0, 1.0, 0.0, 1.0])
+    bc6 = (C.c_int * 6)(5, 5, 4, 4, 5, 5)
+    out = (abi.BlockDesc * 1)()
+    st = lib.mf3d_build_topology(1, ext.ctypes.data_as(C.POINTER(C.c_double)), bc6, 0.1, 0.1, 0.1, out)
+    assert st == abi.MF3D_E_INVALID
