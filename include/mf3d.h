@@ -176,12 +176,31 @@ int mf3d_abi_version(void);
 /* Number of device kernel launches issued by the last solve on `ctx`. */
 long long mf3d_last_launch_count(const mf3d_ctx *ctx);
 
-/* Host-only view of the multigrid halo copy map of level `level` (1-based):
- * the composition of exchangepp + mgbound + exchbc_mgpp (exchangepp.for:
- * 43-4763, mgsolver.for:907-992) as (destination, source) cell pairs.  A
- * cell is numbered blockpos*S + ((k*(ny+2) + j)*(nx+2) + i) with 0-based
- * ghost-inclusive local indices, S the level's largest block volume.  With
- * dst == NULL returns the pair count.  Needs no GPU. */
+/* Kernel timing.  `kind` selects one kernel class whose every launch the
+ * library then brackets with CUDA events on its own stream; 0 turns timing
+ * off.  mf3d_profile_read returns, for the launches since the last
+ * mf3d_profile call: total device milliseconds, launch count and the
+ * algorithmic bytes those launches had to move (compulsory traffic). */
+enum mf3d_profile_kind {
+  MF3D_PROF_OFF = 0,
+  MF3D_PROF_SMOOTH_L1 = 1,   /* red-black half-sweeps on the finest level */
+  MF3D_PROF_CALMAS = 2,      /* fused calvel + calmas                      */
+  MF3D_PROF_RESTRICT_L1 = 3, /* residual + restriction from the finest level */
+  MF3D_PROF_PROLONG_L1 = 4   /* prolongation + correction onto the finest level */
+};
+int mf3d_profile(mf3d_ctx *ctx, int kind);
+int mf3d_profile_read(mf3d_ctx *ctx, double *total_ms, long long *launches,
+                      double *algorithmic_bytes);
+
+/* Host-only view of the multigrid halo refresh of level `level` (1-based)
+ * that follows every smoothing sweep: the composition of mgbound,
+ * exchangepp (with its trailing mgbound and exchbc_mgpp) - mgsolver.for:
+ * 610-611, exchangepp.for:43-4763 - as (destination, source) cell pairs
+ * against the state before the refresh.  Cell number = base(b) +
+ * (k*(ny+2) + j)*(nx+2) + i, with 0-based ghost-inclusive local indices of
+ * the level and base(b) the sum of the ghost-inclusive volumes of the
+ * blocks before b (in argument order).  With dst == NULL returns the pair
+ * count.  Needs no GPU. */
 long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid,
                         int level, long long *dst, long long *src);
 

@@ -506,7 +506,9 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   int st = face_rules(C->blocks, C->rules);
   if (st) return st;
   CK(cudaSetDevice(C->device));
-  CK(cudaStreamCreateWithFlags(&C->stream, cudaStreamNonBlocking));
+  // A blocking stream: it orders after work the caller queued on the legacy
+  // default stream (e.g. the copies that produced the device inputs).
+  CK(cudaStreamCreateWithFlags(&C->stream, cudaStreamDefault));
   CK(cudaEventCreate(&C->ev0));
   CK(cudaEventCreate(&C->ev1));
   CK(cudaMallocHost(&C->rmax_host, sizeof(unsigned long long) * 2));

@@ -137,7 +137,7 @@ __global__ void __launch_bounds__(kTile) k_calvel_calmas(const BlkFld *__restric
   if (q < (long long)nx * ny * F.nz) {
     const int k = (int)(q / ((long long)nx * ny)) + 1;
     const int rem = (int)(q - (long long)(k - 1) * nx * ny);
-    const int j = rem / nx + 1, i = rem - (j - 1) * nx;
+    const int j = rem / nx + 1, i = rem - (j - 1) * nx + 1;
     const double dta = dt * alfapr;
     const long long c = fidx(F, i, j, k);
     const long long sx = 1, sy = F.ti, sz = (long long)F.ti * F.tj;
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kTile) k_calvel(const BlkFld *__restrict__ fl,
   if (q >= (long long)nx * ny * F.nz) return;
   const int k = (int)(q / ((long long)nx * ny)) + 1;
   const int rem = (int)(q - (long long)(k - 1) * nx * ny);
-  const int j = rem / nx + 1, i = rem - (j - 1) * nx;
+  const int j = rem / nx + 1, i = rem - (j - 1) * nx + 1;
   const double dta = dt * alfapr;
   const long long c = fidx(F, i, j, k);
   const long long sy = F.ti, sz = (long long)F.ti * F.tj;
@@ -219,7 +219,7 @@ __global__ void k_load_rhs(const BlkFld *__restrict__ fl, const Tile *__restrict
   if (q >= (long long)nx * ny * F.nz) return;
   const int k = (int)(q / ((long long)nx * ny)) + 1;
   const int rem = (int)(q - (long long)(k - 1) * nx * ny);
-  const int j = rem / nx + 1, i = rem - (j - 1) * nx;
+  const int j = rem / nx + 1, i = rem - (j - 1) * nx + 1;
   rhs1[cell_addr(F.L1, F.L1.rhs0, i, j, k)] = (T)su[t.blk][fidx(F, i, j, k)];
 }
 

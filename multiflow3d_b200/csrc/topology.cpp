@@ -214,6 +214,8 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
                                      const std::vector<long long> &base) {
   TokenLevel T(blocks, geom, base);
   const int nb = (int)blocks.size();
+  // mgrelax calls mgbound before exchangepp (mgsolver.for:610-611)
+  mgbound_tokens(T);
   bool periodic = false;
   for (const auto &d : blocks)
     if (d.bc_west == 5 || d.bc_east == 5 || d.bc_south == 5 || d.bc_north == 5 || d.bc_bottom == 5 || d.bc_top == 5)

@@ -36,6 +36,9 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <thread>
 
 #include "../include/mf3d.h"
 
@@ -63,6 +66,25 @@ struct Blk {
   std::vector<std::vector<double>> hx, hy, hz;
   bool stretched;
 };
+
+/* The reference runs one MPI rank per block; the restatement runs the
+ * independent per-block loops of a phase on OpenMP threads (no effect on
+ * the arithmetic: blocks never read each other inside a phase). */
+int g_threads = 1;
+double *g_tstamp = nullptr; /* optional wall-clock stamps, seconds */
+int g_tcap = 0;
+inline double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+inline void stamp(int q) { if (g_tstamp && q < g_tcap) g_tstamp[q] = now_s(); }
+template <class Fn> void par_blocks(int n, Fn fn) {
+  int nt = std::min(n, g_threads);
+  if (nt <= 1) { for (int i = 0; i < n; ++i) fn(i); return; }
+  std::atomic<int> next(0);
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t) th.emplace_back([&] { for (int i; (i = next++) < n;) fn(i); });
+  for (auto &x : th) x.join();
+}
 
 struct Ctx {
   std::vector<Blk> b;
@@ -405,7 +427,7 @@ void exchangepp(Ctx &C, int g) {
 /* ------------------------------------------------------------------ */
 void mgrelax(Ctx &C, int g, int it) {
   for (int itr = 1; itr <= it; ++itr) {
-    for (auto &B : C.b) {
+    par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_];
       Lev L = lev(C, B, g);
       int ni = L.ni, nj = L.nj, nk = L.nk, nij = L.nij;
       long nij2 = (long)(ni - 2) * (nj - 2);
@@ -473,7 +495,7 @@ void mgrelax(Ctx &C, int g, int it) {
             for (int k = nk - 1; k >= 2; --k) { long ph = PH(L, i, j, k); cf[ph] = (c[k] - a[k] * cf[ph + nij]); }
           }
       }
-    }
+    });
     mgbound(C, g);
     exchangepp(C, g);
   }
@@ -483,7 +505,7 @@ void mgrelax(Ctx &C, int g, int it) {
 /* mgrestr (mgsolver.for:619-761), coarsening branch + EXT weights.     */
 /* ------------------------------------------------------------------ */
 void mgrestr(Ctx &C, int g) {
-  for (auto &B : C.b) {
+  par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_];
     Lev Lc = lev(C, B, g), Lf = lev(C, B, g - 1);
     int nic = Lc.ni, njc = Lc.nj, nkc = Lc.nk;
     long nijc2 = (long)(nic - 2) * (njc - 2), incr_c = (long)(nic - 2) * (njc - 2) * (nkc - 2);
@@ -525,14 +547,14 @@ void mgrestr(Ctx &C, int g) {
         cf[su] = 0.125 * (t[0] + t[1] + t[2] + t[3] + t[4] + t[5] + t[6] + t[7]);
       }
     }
-  }
+  });
 }
 
 /* ------------------------------------------------------------------ */
 /* mgcorr (mgsolver.for:763-905), coarsening branch.                     */
 /* ------------------------------------------------------------------ */
 void mgcorr(Ctx &C, int g) {
-  for (auto &B : C.b) {
+  par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_];
     Lev Lf = lev(C, B, g), Lc = lev(C, B, g + 1);
     double *cf = B.cof.data();
     int nijf = Lf.nij, njf = Lf.nj, nijc = Lc.nij, njc = Lc.nj;
@@ -557,7 +579,7 @@ void mgcorr(Ctx &C, int g) {
         }
       }
     }
-  }
+  });
   mgbound(C, g);
 }
 
@@ -566,7 +588,7 @@ void mgcorr(Ctx &C, int g) {
 /* ------------------------------------------------------------------ */
 void mgkcyc(Ctx &C) {
   int pl = C.pl;
-  for (auto &B : C.b) {
+  par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_];
     Lev L = lev(C, B, 1);
     for (int k = 1; k <= L.nk; ++k) for (int i = 1; i <= L.ni; ++i) for (int j = 1; j <= L.nj; ++j)
       B.cof[(long)(k - 1) * L.nij + (long)(i - 1) * L.nj + j] = F(B, B.pp.data(), i + pl - 1, j + pl - 1, k + pl - 1);
@@ -574,7 +596,7 @@ void mgkcyc(Ctx &C) {
     for (int k = 2; k <= L.nk - 1; ++k) for (int i = 2; i <= L.ni - 1; ++i) for (int j = 2; j <= L.nj - 1; ++j)
       B.cof[B.faz[1] + (long)(k - 2) * (L.ni - 2) * (L.nj - 2) + (long)(i - 2) * (L.nj - 2) + (j - 1) + incrp] =
           F(B, B.su.data(), i + pl - 1, j + pl - 1, k + pl - 1);
-  }
+  });
   int ngrd = C.ngrd_gl;
   int glevel = 1, kcycle = 1, nrel;
   std::vector<int> kount(ngrd + 1, 0);
@@ -786,7 +808,7 @@ inline double dface(const std::vector<double> &w, int a0) { return 0.5 * (w[a0] 
 /* calvel (press.for:139-200), non-LSM branch. */
 void calvel(Ctx &C) {
   double dt = C.dt, alfapr = C.alfapr;
-  for (auto &B : C.b) {
+  par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_];
     int o = B.isp - 1; /* field index i <-> level-1 ghost-inclusive index i - o */
     for (int k = B.ksu; k <= B.keu; ++k) for (int i = B.isu; i <= B.ieu; ++i) for (int j = B.jsu; j <= B.jeu; ++j) {
       double dxl = B.stretched ? dface(B.hx[1], i - o) : B.d.dx;
@@ -800,7 +822,7 @@ void calvel(Ctx &C) {
       double dzl = B.stretched ? dface(B.hz[1], k - o) : B.d.dz;
       F(B, B.w, i, j, k) = (F(B, B.wstar, i, j, k) - dt * alfapr * (F(B, B.p, i, j, k + 1) - F(B, B.p, i, j, k)) / dzl);
     }
-  }
+  });
   exchange(C, 1);
   exchange(C, 2);
   exchange(C, 3);
@@ -808,8 +830,9 @@ void calvel(Ctx &C) {
 
 /* calmas (press.for:2-75), differencing = 1, non-LSM branch. */
 void calmas(Ctx &C) {
-  double rmax = 0.0, resor;
-  for (auto &B : C.b) {
+  double rmax = 0.0;
+  std::vector<double> bmax(C.b.size(), 0.0);
+  par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_]; double rmax = 0.0, resor;
     int o = B.isp - 1;
     for (int k = B.ksp; k <= B.kep; ++k) for (int i = B.isp; i <= B.iep; ++i) for (int j = B.jsp; j <= B.jep; ++j) {
       double hxl = B.stretched ? B.hx[1][i - o] : B.d.dx;
@@ -823,14 +846,19 @@ void calmas(Ctx &C) {
       resor = std::max(rmax, std::fabs(fact1));
       rmax = std::max(resor, std::fabs(fact1));
     }
-  }
-  C.rmax = rmax; /* MPI_ALLREDUCE(MAX) over one rank */
+    bmax[ib_] = rmax;
+  });
+  /* blocks reduce like the ranks of MPI_ALLREDUCE(MAX): order-free */
+  for (double m : bmax) rmax = std::max(rmax, m);
+  C.rmax = rmax;
 }
 
 /* newsolv_mg (newsolv_mg.for:2-102) */
 int newsolv_mg(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
+  stamp(0);
   calvel(C);
   calmas(C);
+  stamp(1);
   double rmax0 = C.rmax;
   for (auto &B : C.b) std::fill(B.pp.begin(), B.pp.end(), 0.0);
   double eps = C.eps_relative ? C.eps * rmax0 : C.eps;
@@ -839,16 +867,18 @@ int newsolv_mg(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
   for (iter = 1; iter <= C.maxcy; ++iter) {
     mgkcyc(C);
     double ppref = 0.0;
-    for (auto &B : C.b)
+    par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_];
       for (int k = B.ksp - 1; k <= B.kep + 1; ++k) for (int i = B.isp - 1; i <= B.iep + 1; ++i) for (int j = B.jsp - 1; j <= B.jep + 1; ++j) {
         F(B, B.p, i, j, k) = (F(B, B.p, i, j, k) + (F(B, B.pp.data(), i, j, k) - ppref));
         F(B, B.pp.data(), i, j, k) = 0.0;
       }
+    });
     exchange(C, 4);
     pbound(C);
     calvel(C);
     calmas(C);
     if (hist && iter - 1 < cap) hist[iter - 1] = C.rmax;
+    stamp(iter + 1);
     if (C.rmax < eps && iter > 1) { conv = true; break; }
   }
   int status = MF3D_OK;
@@ -909,6 +939,13 @@ extern "C" {
 
 const char *orc_last_error(void) { return g_err.c_str(); }
 
+/* Threads for the per-block loops (1 = serial, the default). */
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+
+/* Wall-clock stamps of the next orc_newsolv_mg: t[0] at entry, t[1] after
+ * the initial calvel/calmas, t[1+q] after outer iteration q (NULL = off). */
+void orc_set_timestamps(double *t, int cap) { g_tstamp = t; g_tcap = t ? cap : 0; }
+
 /* The whole projection on host arrays, in place. */
 int orc_newsolv_mg(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, const mf3d_fields *fields,
                    double dt, double alfapr, mf3d_solve_info *info, double *hist, int cap) {
@@ -956,6 +993,7 @@ int orc_exchangepp(const mf3d_block_desc *blocks, int nb, int ngrid, int level, 
     for (int k = 1; k <= L.nk; ++k) for (int j = 1; j <= L.nj; ++j) for (int i = 1; i <= L.ni; ++i)
       B.cof[PH(L, i, j, k)] = fi[ib][((size_t)(k - 1) * L.nj + (j - 1)) * L.ni + (i - 1)];
   }
+  mgbound(C, level); /* the halo refresh mgrelax runs after a sweep (mgsolver.for:610-611) */
   exchangepp(C, level);
   for (int ib = 0; ib < nb; ++ib) {
     Blk &B = C.b[ib];
