@@ -1,0 +1,387 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 pressure-Poisson projection (MultiFlow3D newsolv_mg).
+
+One *step* = one complete projection solve (newsolv_mg.for:2-102): initial
+calvel/calmas, then V-cycles + FP64 projection until the relative rmax
+reaches the workload's tolerance.  Metric: Poisson solves per second.
+
+Default workload (the multi-block FP64 configuration): a 256^3 channel split
+into 2x2x2 blocks of 128^3, periodic in x and z, walls in y with tanh
+wall-normal stretching (factor 2.0), velocity = seeded uniform [-1,1] noise +
+4 smooth Fourier modes of amplitude 0.1, 6 multigrid levels, red-black
+smoother (2 pre-, 1 post-sweeps), tolerance 1e-10 relative to the initial
+rmax.  Synthetic data with the configuration's shapes and distributions.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints ONE JSON line (rank 0).  ``value`` = device-resident solves/s summed
+over ranks (inputs already in HBM; every step restores p, u, v, w from a
+pristine device copy first), ``e2e`` = the same through the host-array C
+entry point ``mf3d_newsolv_mg`` (pinned host buffers, all host<->device
+copies inside the timed call).  Multi-GPU: independent replicas (the solve
+has no inter-GPU exchange), ``scaling: weak``.
+
+``--impl reference`` times the reference's CPU path - the oracle, a literal
+C++ restatement of the Fortran (the Fortran itself cannot be compiled here) -
+on the host cores, one outer iteration per step, and converts to solves/s
+with the iteration count the same solve takes.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "poisson_solves_per_s_fp64"
+UNIT = "solves/s"
+
+
+def workload_config():
+    return {
+        "workload": "fp64 multi-block channel 2x2x2 blocks of 128^3 (256^3), tanh y-stretch 2.0, "
+                    "6 levels, RB-GS(2,1), rel tol 1e-10",
+        "blocks": [2, 2, 2], "block_cells": [128, 128, 128], "global_cells": [256, 256, 256],
+        "ngrid": 6, "smoother": "rbgs", "irestr": 2, "iproln": 1, "tol_rel": 1e-10,
+        "stretch_y": 2.0, "precision": "fp64", "bc": "periodic x,z; walls y",
+        "l2": "inputs larger than L2 (level-1 arrays 268 MB, fields 1.2 GB)",
+    }
+
+
+def make_problem():
+    from multiflow3d_b200.problems import Problem
+    h = 1.0 / 256
+    return Problem(2, 2, 2, 128, 128, 128, ngrid=6, pl=2, stretch_y=2.0, dx=h, dy=h, dz=h)
+
+
+SEED = 2024
+FOURIER = 4
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Bytes per launch of `kernel` from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for line in open(p):
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == kernel:
+                return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def oracle_lib():
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_bridge
+    lib = oracle_bridge.load()
+    lib.orc_set_threads.argtypes = [C.c_int]
+    lib.orc_set_timestamps.argtypes = [C.POINTER(C.c_double), C.c_int]
+    return lib
+
+
+def time_oracle_iterations(pr, n_iter: int, threads: int):
+    """Run the oracle's newsolv_mg for n_iter outer iterations on the full
+    workload; returns (seconds of the initial calvel/calmas, per-iteration
+    seconds list)."""
+    import numpy as np
+    from multiflow3d_b200.abi import SolveInfo
+    from multiflow3d_b200.problems import fields_struct
+    orc = oracle_lib()
+    orc.orc_set_threads(threads)
+    blocks = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    stamps = np.zeros(n_iter + 4)
+    orc.orc_set_timestamps(stamps.ctypes.data_as(C.POINTER(C.c_double)), len(stamps))
+    prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=n_iter, eps=1e-300)
+    info = SolveInfo()
+    hist = np.zeros(n_iter)
+    orc.orc_newsolv_mg(pr.descriptors(orc), pr.nblocks, C.byref(prm), fields_struct(blocks), 1.0, 1.0,
+                       C.byref(info), hist.ctypes.data_as(C.POINTER(C.c_double)), n_iter)
+    orc.orc_set_timestamps(None, 0)
+    t_init = float(stamps[1] - stamps[0])
+    iters = [float(x) for x in np.diff(stamps[1:info.iter + 2])]
+    return t_init, iters
+
+
+def reference_iterations():
+    """Outer iterations the default workload takes to converge (the oracle
+    and the GPU path agree bit for bit; recorded by oracle/count_iterations.py)."""
+    p = os.path.join(ROOT, "oracle", "bench_iterations.json")
+    with open(p) as f:
+        return int(json.load(f)["iterations"])
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    pr = make_problem()
+    threads = max(1, min(os.cpu_count() or 1, pr.nblocks))
+    n = args.warmup + args.steps
+    t_init, its = time_oracle_iterations(pr, n, threads)
+    timed = its[args.warmup:args.warmup + args.steps]
+    t_it = sum(timed) / len(timed)
+    I = reference_iterations()
+    per_solve = t_init + I * t_it
+    value = 1.0 / per_solve
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_it * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": workload_config(),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} timed outer iterations (after {args.warmup} warm-up) of the full "
+                                   f"256^3 solve on the oracle (C++ restatement of the Fortran; blocks on "
+                                   f"{threads} threads as the reference's one-rank-per-block MPI); solves/s = "
+                                   f"1/(t_init {t_init:.3f}s + {I} iterations x {t_it:.3f}s)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args):
+    import numpy as np
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.solver import Projection
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    lib = abi.load()
+
+    pr = make_problem()
+    host = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    keys = ("ustar", "vstar", "wstar", "u", "v", "w", "p", "su")
+    d = [{k: torch.from_numpy(f[k]).to(dev) for k in keys} for f in host]
+    pristine = [{k: f[k].clone() for k in ("u", "v", "w", "p")} for f in d]
+    for f in d:
+        f["su"] = None  # the final su is not requested
+    prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=400, eps=1e-10, eps_relative=1, device=local)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+
+    def reset():
+        for f, p0 in zip(d, pristine):
+            for k in ("u", "v", "w", "p"):
+                f[k].copy_(p0[k])
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        reset()
+        r = proj.newsolv_mg_device(d)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    iters, launches, statuses = [], 0, []
+    for _ in range(args.steps):
+        reset()
+        r = proj.newsolv_mg_device(d)
+        iters.append(r.iter)
+        statuses.append(r.status)
+        launches += proj.launches
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms)
+    value = world * args.steps / (ms_max / 1e3)
+
+    # ---- kernel timing: one more solve per kernel class, each launch of the
+    # class bracketed by CUDA events on the library's stream (a solve with
+    # timing on runs the outer loop from the host instead of as one graph) ----
+    kernels = {}
+    for name, kind in (("k_rbgs", abi.MF3D_PROF_SMOOTH_L1), ("k_calvel_calmas", abi.MF3D_PROF_CALMAS),
+                       ("k_restrict", abi.MF3D_PROF_RESTRICT_L1), ("k_prolong", abi.MF3D_PROF_PROLONG_L1)):
+        proj.profile(kind)
+        reset()
+        proj.newsolv_mg_device(d)
+        kernels[name] = proj.profile_read()
+    proj.profile(abi.MF3D_PROF_OFF)
+    k_ms, k_n, k_bytes = kernels["k_rbgs"]
+
+    # ---- end to end through the host-array C entry point (pinned buffers) ----
+    pinned = [{k: torch.from_numpy(f[k]).pin_memory() for k in keys if k != "su"} for f in host]
+    pin_p0 = [{k: f[k].clone().pin_memory() for k in ("u", "v", "w", "p")} for f in pinned]
+    hfields = [{k: t.numpy() for k, t in f.items()} for f in pinned]
+    for f in hfields:
+        f["su"] = None
+    arr = (abi.Fields * pr.nblocks)()
+    dp = C.POINTER(C.c_double)
+    for b, f in enumerate(hfields):
+        for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p"):
+            setattr(arr[b], k, f[k].ctypes.data_as(dp))
+    n_e2e = max(1, args.steps)
+    e2e_s = 0.0
+    for step in range(n_e2e + 1):
+        for f, p0 in zip(pinned, pin_p0):
+            for k in ("u", "v", "w", "p"):
+                f[k].copy_(p0[k])
+        barrier()
+        t0 = time.perf_counter()
+        r2 = proj._run(lib.mf3d_newsolv_mg, arr, 1.0, 1.0)
+        t1 = time.perf_counter()
+        if step > 0:  # first call allocates the library's device mirrors
+            e2e_s += t1 - t0
+    e2e_s = max_over_ranks(e2e_s)
+    e2e_value = world * n_e2e / e2e_s
+    ttc = int(np.prod(pr.ttc))
+    h2d = 7 * ttc * 8 * pr.nblocks
+    d2h = 4 * ttc * 8 * pr.nblocks
+    proj.close()
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        achieved = (k_bytes / (k_ms / 1e3)) / 1e9 if k_ms > 0 else None
+        per_launch_bytes = k_bytes / k_n if k_n else None
+        traffic = ncu_traffic("k_rbgs")
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(),
+            "iterations_per_solve": iters[0] if iters else None, "status": statuses[0] if statuses else None,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "k_rbgs (finest-level red/black half-sweep)",
+                         "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes,
+                         "launches": k_n, "avg_launch_ms": (k_ms / k_n) if k_n else None,
+                         "other_kernels": {n: {"avg_launch_ms": v[0] / v[1] if v[1] else None,
+                                               "GB/s": (v[2] / (v[0] / 1e3)) / 1e9 if v[0] > 0 else None,
+                                               "launches_per_solve": v[1]}
+                                           for n, v in kernels.items() if n != "k_rbgs"}},
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            threads = max(1, min(os.cpu_count() or 1, pr.nblocks))
+            t_init, its = time_oracle_iterations(pr, 2, threads)
+            t_it = sum(its) / len(its)
+            I = iters[0]
+            cpu_val = 1.0 / (t_init + I * t_it)
+            line["cpu_baseline"] = {
+                "value": cpu_val, "unit": UNIT, "cores": threads, "kind": "port",
+                "sample": f"2 outer iterations of the same 256^3 solve on the oracle (C++ restatement of the "
+                          f"reference's Fortran path, blocks on {threads} threads); solves/s = "
+                          f"1/(t_init {t_init:.3f}s + {I} iterations x {t_it:.3f}s)"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mf3d", choices=["mf3d", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -108,7 +108,15 @@ EXPORTED_SYMBOLS = (
     "mf3d_abi_version",
     "mf3d_last_launch_count",
     "mf3d_halo_map",
+    "mf3d_profile",
+    "mf3d_profile_read",
 )
+
+MF3D_PROF_OFF = 0
+MF3D_PROF_SMOOTH_L1 = 1
+MF3D_PROF_CALMAS = 2
+MF3D_PROF_RESTRICT_L1 = 3
+MF3D_PROF_PROLONG_L1 = 4
 
 _lib = None
 
@@ -131,6 +139,9 @@ def _declare(lib):
     lib.mf3d_halo_map.restype = C.c_longlong
     lib.mf3d_halo_map.argtypes = [C.POINTER(BlockDesc), C.c_int, C.c_int, C.c_int,
                                   C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.mf3d_profile.argtypes = [vp, C.c_int]
+    lib.mf3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
+                                      C.POINTER(C.c_double)]
     return lib
 
 

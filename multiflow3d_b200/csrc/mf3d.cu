@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -107,14 +108,57 @@ struct mf3d_ctx {
   std::vector<size_t> mirror_off;
   DevBuf<Tile> t_int, t_l1cells, t_faces, t_planes;
   int n_int = 0, n_l1cells = 0, n_faces = 0, n_planes = 0;
-  DevBuf<unsigned long long> rmax_slots;
+  DevBuf<unsigned long long> rmax_cur, rmax_scratch;  // atomic-max targets of calmas
+  DevBuf<SolveState> st;                     // device-resident solve control
+  DevBuf<double> hist_d;                     // rmax after each outer iteration
   unsigned long long *rmax_host = nullptr;  // pinned
+  bool use_graph = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaGraphConditionalHandle cond = 0;
+  long long launches_per_iter = 0;
   DevBuf<double *> ptrs;                     // scratch pointer table (mgkcyc_device)
+  // kernel timing (mf3d_profile)
+  int prof_kind = 0;
+  std::vector<cudaEvent_t> prof_ev;          // reusable event pool
+  std::vector<double> prof_pending_bytes;    // one entry per bracketed launch
+  double prof_ms = 0.0, prof_bytes = 0.0;
+  long long prof_n = 0;
+  long long n_l1 = 0;                        // finest-level interior cells, all blocks
 };
 
 namespace mf3d {
 
 static inline int grid_of(long long n, int tpb) { return (int)((n + tpb - 1) / tpb); }
+
+// Kernel timing: bracket one launch of the profiled class with events.
+static void prof_begin(mf3d_ctx *C, int kind, double bytes) {
+  if (C->prof_kind != kind || kind == 0) return;
+  size_t q = C->prof_pending_bytes.size();
+  while (C->prof_ev.size() < 2 * (q + 1)) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    C->prof_ev.push_back(e);
+  }
+  cudaEventRecord(C->prof_ev[2 * q], C->stream);
+  C->prof_pending_bytes.push_back(bytes);
+}
+static void prof_end(mf3d_ctx *C, int kind) {
+  if (C->prof_kind != kind || kind == 0 || C->prof_pending_bytes.empty()) return;
+  cudaEventRecord(C->prof_ev[2 * (C->prof_pending_bytes.size() - 1) + 1], C->stream);
+}
+// After a stream synchronize: fold the bracketed launches into the totals.
+static void prof_collect(mf3d_ctx *C) {
+  for (size_t q = 0; q < C->prof_pending_bytes.size(); ++q) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, C->prof_ev[2 * q], C->prof_ev[2 * q + 1]) == cudaSuccess) {
+      C->prof_ms += ms;
+      C->prof_bytes += C->prof_pending_bytes[q];
+      C->prof_n += 1;
+    }
+  }
+  C->prof_pending_bytes.clear();
+}
 
 // ---------------------------------------------------------------------------
 // Level construction (replaces coeff, mgsolver.for:2-222, and the cof sizing
@@ -265,12 +309,19 @@ static void relax(mf3d_ctx *C, Level<T> &L, int it) {
   const int sch = C->prm.mg_itrsch;
   for (int itr = 0; itr < it; ++itr) {
     if (sch == 3) {
+      const int pk = L.g == 1 ? MF3D_PROF_SMOOTH_L1 : 0;
+      const double half = 0.5 * (double)C->n_l1 * sizeof(T);  // one colour of the finest level
       if (L.zero_interior) {
+        prof_begin(C, pk, 2 * half);  // rhs in, colour out
         k_rbgs<T, true><<<L.n_sweep, kTile, 0, C->stream>>>(L.db.p, L.t_sweep.p, L.phi.p, L.rhs.p, L.coef.p, 0);
       } else {
+        prof_begin(C, pk, 3 * half);  // other colour + rhs in, colour out
         k_rbgs<T, false><<<L.n_sweep, kTile, 0, C->stream>>>(L.db.p, L.t_sweep.p, L.phi.p, L.rhs.p, L.coef.p, 0);
       }
+      prof_end(C, pk);
+      prof_begin(C, pk, 3 * half);
       k_rbgs<T, false><<<L.n_sweep, kTile, 0, C->stream>>>(L.db.p, L.t_sweep.p, L.phi.p, L.rhs.p, L.coef.p, 1);
+      prof_end(C, pk);
       C->launches += 2;
     } else if (sch == 1) {
       k_lexgs<T><<<C->nb, 1024, 0, C->stream>>>(L.db.p, L.phi.p, L.rhs.p, L.coef.p);
@@ -297,8 +348,11 @@ static void materialize_zero(mf3d_ctx *C, Level<T> &L) {
 template <typename T>
 static void restr(mf3d_ctx *C, Level<T> &F, Level<T> &Cl) {
   materialize_zero(C, F);
+  const int pk = F.g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
+  prof_begin(C, pk, (double)C->n_l1 * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse phi, rhs out
   k_restrict<T, T><<<Cl.n_cells, kTile, 0, C->stream>>>(F.db.p, Cl.db.p, Cl.t_cells.p, F.phi.p, F.rhs.p, F.coef.p,
                                                        Cl.phi.p, Cl.rhs.p, F.geo.p);
+  prof_end(C, pk);
   ++C->launches;
   Cl.zero_interior = (C->prm.mg_itrsch == 3);  // k_restrict wrote real zeros too
   if (C->prm.mg_itrsch != 3) Cl.zero_interior = false;
@@ -308,7 +362,10 @@ template <typename T>
 static void corr(mf3d_ctx *C, Level<T> &F, Level<T> &Cl) {
   materialize_zero(C, F);
   materialize_zero(C, Cl);
+  const int pk = F.g == 1 ? MF3D_PROF_PROLONG_L1 : 0;
+  prof_begin(C, pk, (double)C->n_l1 * sizeof(T) * (2.0 + 1.0 / 8.0));  // fine phi in/out, coarse phi in
   k_prolong<T, T><<<F.n_cells, kTile, 0, C->stream>>>(F.db.p, Cl.db.p, F.t_cells.p, F.phi.p, Cl.phi.p);
+  prof_end(C, pk);
   ++C->launches;
 }
 
@@ -397,60 +454,113 @@ static int bind_fields(mf3d_ctx *C, const mf3d_fields *f) {
   return MF3D_OK;
 }
 
+// One outer iteration of newsolv_mg (newsolv_mg.for:25-58): V-cycle,
+// p += pp, p halo + pbound, calvel + calmas, iteration bookkeeping.
+template <typename T>
+static void iteration_body(mf3d_ctx *C, bool in_graph) {
+  cudaStream_t s = C->stream;
+  vcycle<T>(C, levels<T>(C));
+  k_add_correction<T><<<C->n_l1cells, kTile, 0, s>>>(C->df.p, C->t_l1cells.p, level1_phi<T>(C));
+  k_p_faces<<<C->n_faces, kTile, 0, s>>>(C->df.p, C->t_faces.p);
+  prof_begin(C, MF3D_PROF_CALMAS, (double)C->n_l1 * (4 * sizeof(double) + sizeof(T)));  // p, u*, v*, w* in; su out
+  k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->st.p, level1_rhs<T>(C), C->rmax_cur.p, 0);
+  prof_end(C, MF3D_PROF_CALMAS);
+  k_iter_end<<<1, 1, 0, s>>>(C->st.p, C->rmax_cur.p, C->hist_d.p, C->cond, in_graph ? 1 : 0);
+  C->launches += 4;
+}
+
+// The whole outer loop as one graph: a conditional WHILE node whose body is
+// one iteration; k_iter_end clears the condition when the loop must stop.
+template <typename T>
+static int build_solve_graph(mf3d_ctx *C) {
+  if (C->graph_exec) return MF3D_OK;
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  C->graph = g;
+  CK(cudaGraphConditionalHandleCreate(&C->cond, g, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+  np.conditional.handle = C->cond;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(C->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  const long long before = C->launches;
+  const int saved_prof = C->prof_kind;
+  C->prof_kind = 0;  // no event records inside the graph
+  iteration_body<T>(C, true);
+  C->prof_kind = saved_prof;
+  C->launches_per_iter = C->launches - before;
+  cudaGraph_t captured;
+  CK(cudaStreamEndCapture(C->stream, &captured));
+  CK(cudaGraphInstantiate(&C->graph_exec, g, 0));
+  return MF3D_OK;
+}
+
 template <typename T>
 static int solve_device(mf3d_ctx *C, double dt, double alfapr, mf3d_solve_info *info, double *hist, int cap) {
   cudaStream_t s = C->stream;
   C->launches = 0;
-  auto &Lv = levels<T>(C);
-  T *rhs1 = level1_rhs<T>(C);
-  T *phi1 = level1_phi<T>(C);
   const int maxcy = std::max(C->prm.maxcy, 0);
-  CK(cudaMemsetAsync(C->rmax_slots.p, 0, (maxcy + 2) * sizeof(unsigned long long), s));
+  SolveState hs;
+  std::memset(&hs, 0, sizeof hs);
+  hs.dt = dt; hs.alfapr = alfapr; hs.eps = 0.0; hs.maxcy = maxcy;
+  CK(cudaMemcpyAsync(C->st.p, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(C->rmax_cur.p, 0, sizeof(unsigned long long), s));
   CK(cudaEventRecord(C->ev0, s));
   k_face_planes<<<C->n_planes, kTile, 0, s>>>(C->df.p, C->t_planes.p);
-  ++C->launches;
   // calvel; calmas (newsolv_mg.for:16-17): p's ghosts are used as given
-  k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, dt, alfapr, rhs1, C->rmax_slots.p + 0, 0);
-  ++C->launches;
-  CK(cudaMemcpyAsync(C->rmax_host, C->rmax_slots.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->st.p, level1_rhs<T>(C), C->rmax_cur.p, 0);
+  C->launches += 2;
+  CK(cudaMemcpyAsync(C->rmax_host, C->rmax_cur.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemsetAsync(C->rmax_cur.p, 0, sizeof(unsigned long long), s));
   CK(cudaStreamSynchronize(s));
   double rmax0;
   std::memcpy(&rmax0, C->rmax_host, sizeof(double));
-  double rmax = rmax0;
-  const double eps = C->prm.eps_relative ? C->prm.eps * rmax0 : C->prm.eps;
-  int iter = 0;
-  bool conv = false, nonfinite = !std::isfinite(rmax0);
-  for (iter = 1; iter <= maxcy && !nonfinite; ++iter) {
-    vcycle<T>(C, Lv);
-    k_add_correction<T><<<C->n_l1cells, kTile, 0, s>>>(C->df.p, C->t_l1cells.p, phi1);
-    k_p_faces<<<C->n_faces, kTile, 0, s>>>(C->df.p, C->t_faces.p);
-    k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, dt, alfapr, rhs1, C->rmax_slots.p + iter, 0);
-    C->launches += 3;
-    CK(cudaMemcpyAsync(C->rmax_host, C->rmax_slots.p + iter, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    std::memcpy(&rmax, C->rmax_host, sizeof(double));
-    if (hist && iter - 1 < cap) hist[iter - 1] = rmax;
-    if (!std::isfinite(rmax)) { nonfinite = true; break; }
-    if (rmax < eps && iter > 1) { conv = true; break; }
+  hs.eps = C->prm.eps_relative ? C->prm.eps * rmax0 : C->prm.eps;
+  CK(cudaMemcpyAsync(&C->st.p->eps, &hs.eps, sizeof(double), cudaMemcpyHostToDevice, s));
+  const bool nonfinite0 = !std::isfinite(rmax0);
+  if (maxcy > 0 && !nonfinite0) {
+    if (C->use_graph && C->prof_kind == 0) {
+      int st = build_solve_graph<T>(C);
+      if (st) return st;
+      CK(cudaGraphLaunch(C->graph_exec, s));
+    } else {
+      for (int it = 1; it <= maxcy; ++it) {
+        iteration_body<T>(C, false);
+        CK(cudaMemcpyAsync(&hs, C->st.p, sizeof hs, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        prof_collect(C);
+        if (hs.done) break;
+      }
+    }
   }
-  const int iters = conv || nonfinite ? iter : maxcy;
   // final su (optional) and u, v, w (calvel with the final p)
   bool want_su = false;
   for (auto &F : C->hf) want_su |= F.su != nullptr;
   if (want_su) {
-    k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, dt, alfapr, rhs1, C->rmax_slots.p + maxcy + 1, 1);
+    k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->st.p, level1_rhs<T>(C), C->rmax_scratch.p, 1);
     ++C->launches;
   }
-  k_calvel<<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, dt, alfapr);
+  k_calvel<<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->st.p);
   ++C->launches;
   CK(cudaEventRecord(C->ev1, s));
+  CK(cudaMemcpyAsync(&hs, C->st.p, sizeof hs, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
+  prof_collect(C);
+  const int iters = hs.iter;
+  if (C->use_graph && C->prof_kind == 0) C->launches += (long long)iters * C->launches_per_iter;
+  if (hist && iters > 0) {
+    CK(cudaMemcpy(hist, C->hist_d.p, std::min(iters, cap) * sizeof(double), cudaMemcpyDeviceToHost));
+  }
   float ms = 0.f;
   cudaEventElapsedTime(&ms, C->ev0, C->ev1);
+  const double rmax = iters > 0 ? hs.rmax : rmax0;
   int status = MF3D_OK;
-  if (nonfinite) status = MF3D_E_NONFINITE;
-  else if (!conv) status = MF3D_NOT_CONVERGED;
+  if (nonfinite0 || hs.done == 2) status = MF3D_E_NONFINITE;
+  else if (hs.done != 1) status = MF3D_NOT_CONVERGED;
   if (status >= 0 && rmax > 100.0) status = MF3D_DIVERGED;  // newsolv_mg.for:64
   if (info) {
     info->rmax = rmax; info->rmax0 = rmax0; info->iter = iters; info->status = status; info->ms_device = ms;
@@ -512,7 +622,14 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   CK(cudaEventCreate(&C->ev0));
   CK(cudaEventCreate(&C->ev1));
   CK(cudaMallocHost(&C->rmax_host, sizeof(unsigned long long) * 2));
-  if ((st = C->rmax_slots.alloc(std::max(prm->maxcy, 0) + 2))) return st;
+  if ((st = C->rmax_cur.alloc(1))) return st;
+  if ((st = C->rmax_scratch.alloc(1))) return st;
+  if ((st = C->st.alloc(1))) return st;
+  if ((st = C->hist_d.alloc(std::max(prm->maxcy, 0) + 1))) return st;
+  {
+    const char *e = getenv("MF3D_NO_GRAPH");
+    C->use_graph = !(e && e[0] == '1');
+  }
   if ((st = C->ptrs.alloc(2 * nb))) return st;
   const int ngrid = prm->ngrid;
   if (prm->precision == MF3D_PREC_FP64) {
@@ -574,6 +691,7 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
     F.lo[2] = pp; F.hi[2] = pp + pxy;
     F.L1 = prm->precision == MF3D_PREC_FP64 ? C->L64[1]->hb[b] : C->L32[1]->hb[b];
     it_int.push_back((long long)d.nx * d.ny * d.nz);
+    C->n_l1 += (long long)d.nx * d.ny * d.nz;
     it_l1.push_back((long long)(d.nx + 2) * (d.ny + 2) * (d.nz + 2));
     it_faces.push_back(2 * ((long long)d.ny * d.nz + (long long)d.nx * d.nz + (long long)d.nx * d.ny));
     it_planes.push_back((long long)d.ny * d.nz + (long long)d.nx * d.nz + (long long)d.nx * d.ny);
@@ -644,6 +762,9 @@ int mf3d_destroy(mf3d_ctx *ctx) {
   if (ctx->rmax_host) cudaFreeHost(ctx->rmax_host);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (auto e : ctx->prof_ev) cudaEventDestroy(e);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
   cudaStream_t s = ctx->stream;
   delete ctx;
   if (s) cudaStreamDestroy(s);
@@ -716,6 +837,22 @@ int mf3d_mgkcyc_device(mf3d_ctx *C, double *const *su, double *const *pp) {
 }
 
 long long mf3d_last_launch_count(const mf3d_ctx *C) { return C ? C->launches : 0; }
+
+int mf3d_profile(mf3d_ctx *C, int kind) {
+  if (!C || kind < 0 || kind > MF3D_PROF_PROLONG_L1) { mf3d::set_error("mf3d_profile: bad arguments"); return MF3D_E_INVALID; }
+  C->prof_kind = kind;
+  C->prof_ms = 0.0; C->prof_bytes = 0.0; C->prof_n = 0;
+  C->prof_pending_bytes.clear();
+  return MF3D_OK;
+}
+
+int mf3d_profile_read(mf3d_ctx *C, double *total_ms, long long *launches, double *bytes) {
+  if (!C) { mf3d::set_error("mf3d_profile_read: bad arguments"); return MF3D_E_INVALID; }
+  if (total_ms) *total_ms = C->prof_ms;
+  if (launches) *launches = C->prof_n;
+  if (bytes) *bytes = C->prof_bytes;
+  return MF3D_OK;
+}
 
 long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid, int level, long long *dst,
                         long long *src) {

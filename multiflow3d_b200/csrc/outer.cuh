@@ -8,6 +8,18 @@
 
 namespace mf3d {
 
+// Device-resident control state of one solve (newsolv_mg's module variables
+// dt, alfapr, eps, maxcy, iter, rmax), so the outer loop can run as a CUDA
+// graph with no host round trip per iteration.
+struct SolveState {
+  double dt, alfapr;
+  double eps;      // absolute threshold on rmax (eps * rmax0 in relative mode)
+  double rmax;     // rmax after the last outer iteration
+  int maxcy;
+  int iter;        // outer iterations done
+  int done;        // 0 running, 1 converged, 2 non-finite rmax, 3 maxcy reached
+};
+
 // Per-block view of the fields and of the level-1 multigrid arrays.
 struct BlkFld {
   double *ustar, *vstar, *wstar, *u, *v, *w, *p, *su;
@@ -127,8 +139,9 @@ __device__ inline void atomic_max_nonneg(unsigned long long *slot, double v) {
 // atomic max on the bit pattern, hence deterministic).
 template <typename T>
 __global__ void __launch_bounds__(kTile) k_calvel_calmas(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                                                         double dt, double alfapr, T *__restrict__ rhs1,
+                                                         const SolveState *__restrict__ st, T *__restrict__ rhs1,
                                                          unsigned long long *__restrict__ rmax_slot, int write_su) {
+  const double dt = st->dt, alfapr = st->alfapr;
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   const int nx = F.nx, ny = F.ny;
@@ -190,7 +203,8 @@ __global__ void __launch_bounds__(kTile) k_calvel_calmas(const BlkFld *__restric
 // Final calvel (press.for:139-198): u, v, w on the faces calvel writes
 // (isu..ieu etc., one face short at a high wall), from the final p.
 __global__ void __launch_bounds__(kTile) k_calvel(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                                                  double dt, double alfapr) {
+                                                  const SolveState *__restrict__ st) {
+  const double dt = st->dt, alfapr = st->alfapr;
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   const int nx = F.nx, ny = F.ny;
@@ -206,6 +220,25 @@ __global__ void __launch_bounds__(kTile) k_calvel(const BlkFld *__restrict__ fl,
   if (!(i == nx && F.wall[1])) F.u[c] = (F.ustar[c] - dta * (p[c + 1] - p[c]) / F.df[0][i]);
   if (!(j == ny && F.wall[3])) F.v[c] = (F.vstar[c] - dta * (p[c + sy] - p[c]) / F.df[1][j]);
   if (!(k == F.nz && F.wall[5])) F.w[c] = (F.wstar[c] - dta * (p[c + sz] - p[c]) / F.df[2][k]);
+}
+
+// End of one outer iteration (newsolv_mg.for:54-58): record rmax, count the
+// iteration, test `rmax < eps .and. iter > 1`, and - inside the solve graph -
+// set the WHILE condition that repeats the iteration body.
+__global__ void k_iter_end(SolveState *st, unsigned long long *rmax_slot, double *hist,
+                           cudaGraphConditionalHandle cond, int in_graph) {
+  const double r = __longlong_as_double((long long)*rmax_slot);
+  *rmax_slot = 0ull;
+  const int it = st->iter + 1;
+  st->iter = it;
+  st->rmax = r;
+  hist[it - 1] = r;
+  int done = 0;
+  if (!(r <= 1.7976931348623157e308)) done = 2;  // +Inf (a NaN is stored as +Inf)
+  else if (r < st->eps && it > 1) done = 1;
+  else if (it >= st->maxcy) done = 3;
+  st->done = done;
+  if (in_graph) cudaGraphSetConditional(cond, done ? 0u : 1u);
 }
 
 // Level-1 rhs := su (mgkcyc's copy-in, mgsolver.for:250-263) from a ttc array.

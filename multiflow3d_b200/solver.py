@@ -86,6 +86,17 @@ class Projection:
         pp = (_dp * len(pp_list))(*[C.cast(C.c_void_p(t.data_ptr()), _dp) for t in pp_list])
         abi.check(self.lib, self.lib.mf3d_mgkcyc_device(self.ctx, su, pp), "mf3d_mgkcyc_device")
 
+    def profile(self, kind: int):
+        """Start timing one kernel class (abi.MF3D_PROF_*; 0 = off)."""
+        abi.check(self.lib, self.lib.mf3d_profile(self.ctx, kind), "mf3d_profile")
+
+    def profile_read(self):
+        """(total device ms, launches, algorithmic bytes) since profile()."""
+        ms, n, by = C.c_double(), C.c_longlong(), C.c_double()
+        abi.check(self.lib, self.lib.mf3d_profile_read(self.ctx, C.byref(ms), C.byref(n), C.byref(by)),
+                  "mf3d_profile_read")
+        return ms.value, n.value, by.value
+
     @property
     def launches(self) -> int:
         return int(self.lib.mf3d_last_launch_count(self.ctx))
