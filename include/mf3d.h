@@ -158,6 +158,40 @@ int mf3d_newsolv_mg_device(mf3d_ctx *ctx, const mf3d_fields *fields,
                            double dt, double alfapr, mf3d_solve_info *info,
                            double *rmax_hist, int hist_cap);
 
+/* ---------------------------------------------------------------------- */
+/* Batches of independent domains (no counterpart in the reference, which   */
+/* solves one problem per call).                                            */
+/* ---------------------------------------------------------------------- */
+
+/* One independent single-block domain: its own size, spacing, boundary
+ * conditions and multigrid depth. */
+typedef struct mf3d_domain_desc {
+  int nx, ny, nz;          /* interior cells                                    */
+  double dx, dy, dz;       /* uniform spacing                                   */
+  int bc[3];               /* per axis x, y, z: MF3D_BC_PERIODIC or a wall code */
+  int ngrid;               /* levels; <= 0: the deepest mf3d_max_levels allows  */
+  const double *hx, *hy, *hz; /* optional widths as in mf3d_block_desc         */
+} mf3d_domain_desc;
+
+/* Deepest level count for an nx x ny x nz block: every edge divisible by
+ * 2^(L-1) and the coarsest edge at least 4 cells (minimum 1). */
+int mf3d_max_levels(int nx, int ny, int nz);
+
+/* A context over `ndomains` independent domains.  One launch per phase
+ * covers every domain; each domain runs exactly its own V-cycles (its own
+ * depth) and stops on its own convergence test, so its result is the same
+ * alone or in the batch. */
+int mf3d_batch_create(const mf3d_domain_desc *domains, int ndomains,
+                      const mf3d_params *params, mf3d_ctx **ctx);
+
+/* Solve every domain of a batch context: `fields[d]` (device arrays),
+ * `dt[d]`, `alfapr[d]`; `infos[d]` and rows of `rmax_hist` (ndomains x
+ * hist_cap, may be NULL) per domain.  Returns the worst status. */
+int mf3d_batch_solve_device(mf3d_ctx *ctx, const mf3d_fields *fields,
+                            const double *dt, const double *alfapr,
+                            mf3d_solve_info *infos, double *rmax_hist,
+                            int hist_cap);
+
 /* One V-cycle (mgkcyc, mgsolver.for:224-369) on device arrays: reads the
  * RHS `su` and writes the correction `pp` of each block, both in the ttc
  * layout (pp including its first ghost layer, mgsolver.for:351-364). The

@@ -55,6 +55,18 @@ class BlockDesc(C.Structure):
     ]
 
 
+class DomainDesc(C.Structure):
+    """``mf3d_domain_desc`` - one independent single-block domain of a batch."""
+
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+        ("bc", C.c_int * 3),
+        ("ngrid", C.c_int),
+        ("hx", _dp), ("hy", _dp), ("hz", _dp),
+    ]
+
+
 class Params(C.Structure):
     """``mf3d_params`` - the control.cin fields the projection reads."""
 
@@ -110,6 +122,9 @@ EXPORTED_SYMBOLS = (
     "mf3d_halo_map",
     "mf3d_profile",
     "mf3d_profile_read",
+    "mf3d_max_levels",
+    "mf3d_batch_create",
+    "mf3d_batch_solve_device",
 )
 
 MF3D_PROF_OFF = 0
@@ -139,6 +154,9 @@ def _declare(lib):
     lib.mf3d_halo_map.restype = C.c_longlong
     lib.mf3d_halo_map.argtypes = [C.POINTER(BlockDesc), C.c_int, C.c_int, C.c_int,
                                   C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.mf3d_max_levels.argtypes = [C.c_int, C.c_int, C.c_int]
+    lib.mf3d_batch_create.argtypes = [C.POINTER(DomainDesc), C.c_int, C.POINTER(Params), C.POINTER(vp)]
+    lib.mf3d_batch_solve_device.argtypes = [vp, C.POINTER(Fields), _dp, _dp, C.POINTER(SolveInfo), _dp, C.c_int]
     lib.mf3d_profile.argtypes = [vp, C.c_int]
     lib.mf3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                       C.POINTER(C.c_double)]

@@ -1,21 +1,25 @@
-// Device kernels of libmf3d (sm_100a).
+// Device kernels of libmf3d (sm_100a): the multigrid V-cycle.
 //
-// Storage of a multigrid level (the reference keeps it in `cof`,
-// mgsolver.for:20-38): every block's correction phi and right-hand side,
+// Storage of a multigrid level of one block (the reference keeps it in
+// `cof`, mgsolver.for:20-38): the correction phi and the right-hand side,
 // each with a one-cell ghost shell, split by red/black colour.  Cell (i,j,k)
 // (0-based, ghost-inclusive, 0..n+1) has colour c = (i+j+k+1)&1 - colour 0
 // is the reference's even MOD(i+j+k,2) on its 1-based indices, updated first
-// (mgsolver.for:552) - and lives at
-//     base + c*cstr + (k*(ny+2) + j)*hp + (i>>1),   hp = (nx+3)/2.
-// A red-black half-sweep then streams exactly one colour in and the other
-// out: 12 B/cell/half-sweep in FP64, contiguous and coalesced along i.
+// (mgsolver.for:552) - and lives at element
+//     c*cstr + (k*(ny+2) + j)*hp + (i>>1),   hp = (nx+3)/2
+// of the block's level array.  A red-black half-sweep streams exactly one
+// colour in and the other out: 12 B/cell/half-sweep in FP64.
+//
+// Every block owns its arrays (a resident hierarchy); a launch covers any
+// set of blocks through a table of per-block descriptors, so independent
+// domains of different sizes share one launch per phase.  Each descriptor
+// names its domain; a domain that has converged is skipped (`act`).
 //
 // The 7-point coefficients are not stored per cell (the reference streams 7
-// arrays, ~80 B/cell/sweep): per level and block, six 1-D arrays
-// (aw, ae along x; as, an along y; ab, at along z) with the Neumann faces
-// zeroed (mgsolver.for:184-203); ap = -(aw+ae+as+an+ab+at) is re-formed per
-// cell in the reference's order (mgsolver.for:205-208), so every value is
-// bit-identical to the reference's `cof` entries.
+// arrays, ~80 B/cell/sweep): per level and block, six 1-D arrays (aw, ae
+// along x; as, an along y; ab, at along z) with the Neumann faces zeroed
+// (mgsolver.for:184-203); ap = -(aw+ae+as+an+ab+at) is re-formed per cell
+// in the reference's order (mgsolver.for:205-208), bit-identical to `cof`.
 //
 // Every FP64 expression keeps the reference's evaluation order; the file is
 // built with -fmad=false so no multiply-add is contracted.
@@ -26,87 +30,155 @@
 
 namespace mf3d {
 
-constexpr int kTile = 256;  // threads (= work items) per CTA for the 1-D tiled kernels
+constexpr int kTile = 256;  // threads per CTA of the 1-D item kernels
 
 // Per-block, per-level descriptor (device side).
 struct BlkLev {
-  long long phi0;   // offset of colour 0 in the level's phi pool
-  long long rhs0;   // offset of colour 0 in the level's rhs pool
-  long long cstr;   // elements per colour array = (nz+2)*(ny+2)*hp
-  int nx, ny, nz, hp;
-  int coef;         // offset of aw in the level coefficient pool (6 arrays, see coef_*)
-  int geo;          // offset of the restriction ratio arrays (rx, ry, rz) of this level
-  int nmask;        // Neumann faces: bit f set for f = W,E,S,N,B,T
-  int pos;          // block position
+  void *phi;          // colour 0 of phi; colour 1 at +cstr elements
+  void *rhs;          // colour 0 of rhs
+  const void *coef;   // aw[nx+2] ae[nx+2] as[ny+2] an[ny+2] ab[nz+2] at[nz+2]
+  const void *geo;    // restriction ratios rx[nx+2] ry[ny+2] rz[nz+2]
+  long long cstr;     // elements per colour array (padded)
+  int nx, ny, nz, hp; // interior cells (0 = block absent at this level)
+  int nmask;          // Neumann faces: bit f set for f = W,E,S,N,B,T
+  int dom;            // domain of the block
 };
 
 __host__ __device__ inline int hp_of(int nx) { return (nx + 3) / 2; }
 __device__ inline int colour_of(int i, int j, int k) { return (i + j + k + 1) & 1; }
-__device__ inline long long cell_addr(const BlkLev &B, long long base, int i, int j, int k) {
-  int c = colour_of(i, j, k);
-  return base + c * B.cstr + ((long long)k * (B.ny + 2) + j) * B.hp + (i >> 1);
+__device__ inline long long cell_off(const BlkLev &B, int i, int j, int k) {
+  return colour_of(i, j, k) * B.cstr + ((long long)k * (B.ny + 2) + j) * B.hp + (i >> 1);
 }
-// Coefficient layout: aw[nx+2], ae[nx+2], as[ny+2], an[ny+2], ab[nz+2], at[nz+2].
-__device__ inline int coef_aw(const BlkLev &B) { return B.coef; }
-__device__ inline int coef_ae(const BlkLev &B) { return B.coef + (B.nx + 2); }
-__device__ inline int coef_as(const BlkLev &B) { return B.coef + 2 * (B.nx + 2); }
-__device__ inline int coef_an(const BlkLev &B) { return B.coef + 2 * (B.nx + 2) + (B.ny + 2); }
-__device__ inline int coef_ab(const BlkLev &B) { return B.coef + 2 * (B.nx + 2) + 2 * (B.ny + 2); }
-__device__ inline int coef_at(const BlkLev &B) { return B.coef + 2 * (B.nx + 2) + 2 * (B.ny + 2) + (B.nz + 2); }
+template <typename T>
+__device__ inline T *phi_of(const BlkLev &B) { return (T *)B.phi; }
+template <typename T>
+__device__ inline T *rhs_of(const BlkLev &B) { return (T *)B.rhs; }
+// coefficient arrays
+template <typename T>
+struct Coef {
+  const T *aw, *ae, *as, *an, *ab, *at;
+  __device__ Coef(const BlkLev &B) {
+    aw = (const T *)B.coef;
+    ae = aw + (B.nx + 2);
+    as = ae + (B.nx + 2);
+    an = as + (B.ny + 2);
+    ab = an + (B.ny + 2);
+    at = ab + (B.nz + 2);
+  }
+};
 
-// A CTA's work: block position and first item.
+// A CTA's work: block position and the origin of its tile.  2-D tiles:
+// threadIdx.x runs along i (or the compact index h), threadIdx.y along j;
+// k0 is the plane (or the first plane of a z-marching chunk).
 struct Tile {
   int blk;
-  int item0;
+  int k0;
+  int j0;
+  int i0;
 };
+
+// Tile shapes (threads per CTA = TX * RJ).
+constexpr int RB_TX = 32, RB_RJ = 8, RB_KCH = 16;   // red-black z-march
+constexpr int RW_TX = 32, RW_RJ = 8, RW_KCH = 8;    // row tiles, RW_KCH planes per CTA
+constexpr int OZ_TX = 32, OZ_RJ = 8, OZ_KCH = 16;   // outer calvel/calmas z-march
+
+// Asynchronous global->shared copy of one element (LDGSTS), and the group
+// commit / wait of the copy pipeline.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  if (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 // ---------------------------------------------------------------------------
 // Red-black Gauss-Seidel half-sweep (mgsolver.for:547-601) of one colour over
-// all blocks of a level: phi = (rhs - (aw*w + ae*e + as*s + an*n + ab*b +
-// at*t)) / ap, neighbours of the other colour.  Ghost cells are read as they
-// are: the reference refreshes them only after the whole sweep.  Items: the
-// compact (h, j, k) positions of the interior rows, hp per row.
+// a set of blocks: phi = (rhs - (aw*w + ae*e + as*s + an*n + ab*b + at*t)) /
+// ap, neighbours of the other colour.  Ghost cells are read as they are: the
+// reference refreshes them only after the whole sweep.
 // FROM_ZERO: the level was just zeroed (pp = 0 at the start of a V-cycle,
 // coarse phi = 0 after mgrestr), so the other colour is read as 0 without a
 // load; the result is bit-identical.
+// A CTA owns compact columns i0..i0+31 of rows j0..j0+7 and marches up a
+// chunk of planes.  Plane tiles of the other colour (with a one-cell halo)
+// and of the rhs are staged into shared memory by cp.async, RB_NS planes
+// deep, so several planes of loads are in flight per CTA while the current
+// plane is computed from shared memory.
 // ---------------------------------------------------------------------------
+constexpr int RB_PD = 6;              // prefetch distance in planes (covers DRAM latency)
+constexpr int RB_NS = RB_PD + 2;      // stages: planes k-1 .. k+RB_PD
+
 template <typename T, bool FROM_ZERO>
-__global__ void __launch_bounds__(kTile) k_rbgs(const BlkLev *__restrict__ bl, const Tile *__restrict__ tiles,
-                                                T *__restrict__ phi, const T *__restrict__ rhs,
-                                                const T *__restrict__ coef, int colour) {
+__global__ void __launch_bounds__(RB_TX *RB_RJ) k_rbgs(const BlkLev *__restrict__ bl, const Tile *__restrict__ tiles,
+                                                       const int *__restrict__ act, int colour) {
+  __shared__ T so[RB_NS][RB_RJ + 2][RB_TX + 2];
+  __shared__ T sr[RB_NS][RB_RJ][RB_TX];
   const Tile t = tiles[blockIdx.x];
   const BlkLev B = bl[t.blk];
-  const int hp = B.hp;
-  const long long plane = (long long)B.ny * hp;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  if (q >= plane * B.nz) return;
-  const int k = (int)(q / plane) + 1;
-  const int rem = (int)(q - (long long)(k - 1) * plane);
-  const int j = rem / hp + 1;
-  const int h = rem - (j - 1) * hp;
-  const int s = (colour + j + k + 1) & 1;
-  const int i = 2 * h + s;
-  if (i < 1 || i > B.nx) return;
-  const long long rs = (long long)(B.ny + 2) * hp;  // plane stride
-  const long long row = (long long)k * rs + (long long)j * hp;
-  const T aw = coef[coef_aw(B) + i], ae = coef[coef_ae(B) + i];
-  const T as = coef[coef_as(B) + j], an = coef[coef_an(B) + j];
-  const T ab = coef[coef_ab(B) + k], at = coef[coef_at(B) + k];
-  const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-  T w, e, so, no, bo, to;
-  if (FROM_ZERO) {
-    w = e = so = no = bo = to = (T)0;
-  } else {
-    const T *P = phi + B.phi0 + (1 - colour) * B.cstr + row;
-    w = P[h - 1 + s];
-    e = P[h + s];
-    so = P[h - hp];
-    no = P[h + hp];
-    bo = P[h - rs];
-    to = P[h + rs];
+  if (!act[B.dom]) return;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RB_TX + tx;
+  const int h = t.i0 + tx, j = t.j0 + ty;
+  const int hp = B.hp, ny = B.ny;
+  const long long rs = (long long)(ny + 2) * hp;  // plane stride
+  const T *__restrict__ O = phi_of<T>(B) + (1 - colour) * B.cstr;
+  T *__restrict__ M = phi_of<T>(B) + colour * B.cstr;
+  const T *__restrict__ R = rhs_of<T>(B) + colour * B.cstr;
+  const Coef<T> cf(B);
+  const int k0 = t.k0, k1 = min(t.k0 + RB_KCH - 1, B.nz);
+  const bool jin = j <= ny;
+  const T as = jin ? cf.as[j] : (T)0, an = jin ? cf.an[j] : (T)0;
+  // stage the tiles of plane kk (other colour with halo, rhs when kk is computed)
+  auto issue = [&](int kk) {
+    const int st = (kk - k0 + 1) % RB_NS;
+    const long long pk = (long long)kk * rs;
+    if (!FROM_ZERO) {
+      for (int e = tid; e < (RB_RJ + 2) * (RB_TX + 2); e += RB_TX * RB_RJ) {
+        const int r = e / (RB_TX + 2), c = e - r * (RB_TX + 2);
+        const int jj = t.j0 - 1 + r, hh = t.i0 - 1 + c;
+        if (jj <= ny + 1 && hh >= 0 && hh < hp) cp_async_elem(&so[st][r][c], O + pk + (long long)jj * hp + hh);
+      }
+    }
+    if (kk >= k0 && kk <= k1 && jin && h < hp) cp_async_elem(&sr[st][ty][tx], R + pk + (long long)j * hp + h);
+  };
+  // prologue: planes k0-1 .. k0+RB_PD-1, one commit group each
+  for (int kk = k0 - 1; kk < k0 + RB_PD; ++kk) {
+    if (kk <= k1 + 1 && (kk >= k0 || !FROM_ZERO)) issue(kk);
+    cp_async_commit();
   }
-  const T r = rhs[B.rhs0 + colour * B.cstr + row + h];
-  phi[B.phi0 + colour * B.cstr + row + h] = ((r - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
+  for (int k = k0; k <= k1; ++k) {
+    if (k + RB_PD <= k1 + 1) issue(k + RB_PD);
+    cp_async_commit();
+    cp_async_wait<RB_PD - 1>();  // planes up to k+1 have landed; RB_PD-1 newer groups in flight
+    __syncthreads();
+    const int s = (colour + j + k + 1) & 1;
+    const int i = 2 * h + s;
+    if (jin && h < hp && i >= 1 && i <= B.nx) {
+      const int st = (k - k0 + 1) % RB_NS;
+      T w = (T)0, e = (T)0, so_ = (T)0, no = (T)0, bo = (T)0, to = (T)0;
+      if (!FROM_ZERO) {
+        const int stb = (k - k0) % RB_NS, stt = (k - k0 + 2) % RB_NS;
+        w = so[st][ty + 1][tx + s];
+        e = so[st][ty + 1][tx + 1 + s];
+        so_ = so[st][ty][tx + 1];
+        no = so[st][ty + 2][tx + 1];
+        bo = so[stb][ty + 1][tx + 1];
+        to = so[stt][ty + 1][tx + 1];
+      }
+      const T aw = cf.aw[i], ae = cf.ae[i];
+      const T ab = cf.ab[k], at = cf.at[k];
+      const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
+      const T r = sr[st][ty][tx];
+      M[(long long)k * rs + (long long)j * hp + h] =
+          ((r - (aw * w + ae * e + as * so_ + an * no + ab * bo + at * to)) / ap);
+    }
+    __syncthreads();  // the stage of plane k-1 is refilled next iteration
+  }
+  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------
@@ -116,27 +188,25 @@ __global__ void __launch_bounds__(kTile) k_rbgs(const BlkLev *__restrict__ bl, c
 // walks the hyperplanes in order (a parity kernel for small blocks).
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_lexgs(const BlkLev *__restrict__ bl, T *__restrict__ phi, const T *__restrict__ rhs,
-                        const T *__restrict__ coef) {
-  const BlkLev B = bl[blockIdx.x];
+__global__ void k_lexgs(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, const int *__restrict__ act) {
+  const BlkLev B = bl[blocks[blockIdx.x]];
+  if (!act[B.dom]) return;
+  T *P = phi_of<T>(B);
+  const T *R = rhs_of<T>(B);
+  const Coef<T> cf(B);
   const int nx = B.nx, ny = B.ny, nz = B.nz;
-  const long long rs = (long long)(ny + 2) * B.hp;
   for (int sum = 3; sum <= nx + ny + nz; ++sum) {
-    // cells with i+j+k = sum, 1<=i<=nx, 1<=j<=ny, 1<=k<=nz; enumerate (j,k)
     for (int idx = threadIdx.x; idx < ny * nz; idx += blockDim.x) {
       const int j = idx % ny + 1, k = idx / ny + 1;
       const int i = sum - j - k;
       if (i < 1 || i > nx) continue;
-      const T aw = coef[coef_aw(B) + i], ae = coef[coef_ae(B) + i];
-      const T as = coef[coef_as(B) + j], an = coef[coef_an(B) + j];
-      const T ab = coef[coef_ab(B) + k], at = coef[coef_at(B) + k];
+      const T aw = cf.aw[i], ae = cf.ae[i], as = cf.as[j], an = cf.an[j], ab = cf.ab[k], at = cf.at[k];
       const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-      const T w = phi[cell_addr(B, B.phi0, i - 1, j, k)], e = phi[cell_addr(B, B.phi0, i + 1, j, k)];
-      const T so = phi[cell_addr(B, B.phi0, i, j - 1, k)], no = phi[cell_addr(B, B.phi0, i, j + 1, k)];
-      const T bo = phi[cell_addr(B, B.phi0, i, j, k - 1)], to = phi[cell_addr(B, B.phi0, i, j, k + 1)];
-      const T r = rhs[cell_addr(B, B.rhs0, i, j, k)];
-      phi[cell_addr(B, B.phi0, i, j, k)] = ((r - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
-      (void)rs;
+      const T w = P[cell_off(B, i - 1, j, k)], e = P[cell_off(B, i + 1, j, k)];
+      const T so = P[cell_off(B, i, j - 1, k)], no = P[cell_off(B, i, j + 1, k)];
+      const T bo = P[cell_off(B, i, j, k - 1)], to = P[cell_off(B, i, j, k + 1)];
+      const T r = R[cell_off(B, i, j, k)];
+      P[cell_off(B, i, j, k)] = ((r - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
     }
     __syncthreads();
   }
@@ -151,59 +221,52 @@ __global__ void k_lexgs(const BlkLev *__restrict__ bl, T *__restrict__ phi, cons
 // of length `ngg`.  a(1) = 0 and c(1) = the line's first ghost value.
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ void tdma_line(const BlkLev &B, T *__restrict__ phi, const T *__restrict__ rhs,
-                          const T *__restrict__ coef, int dir, int u, int v, T *a, T *c) {
+__device__ void tdma_line(const BlkLev &B, int dir, int u, int v, T *a, T *c) {
   // dir 0: j-line at (i=u, k=v); dir 1: i-line at (j=u, k=v); dir 2: k-line at (i=u, j=v)
+  T *P = phi_of<T>(B);
+  const T *R = rhs_of<T>(B);
+  const Coef<T> cf(B);
   const int n = dir == 0 ? B.ny : dir == 1 ? B.nx : B.nz;
-  auto addr = [&](int m) -> long long {
-    if (dir == 0) return cell_addr(B, B.phi0, u, m, v);
-    if (dir == 1) return cell_addr(B, B.phi0, m, u, v);
-    return cell_addr(B, B.phi0, u, v, m);
-  };
-  auto raddr = [&](int m) -> long long {
-    if (dir == 0) return cell_addr(B, B.rhs0, u, m, v);
-    if (dir == 1) return cell_addr(B, B.rhs0, m, u, v);
-    return cell_addr(B, B.rhs0, u, v, m);
+  auto off = [&](int m) -> long long {
+    if (dir == 0) return cell_off(B, u, m, v);
+    if (dir == 1) return cell_off(B, m, u, v);
+    return cell_off(B, u, v, m);
   };
   a[0] = (T)0;
-  c[0] = phi[addr(0)];
+  c[0] = P[off(0)];
   for (int m = 1; m <= n; ++m) {
     int i, j, k;
     if (dir == 0) { i = u; j = m; k = v; }
     else if (dir == 1) { i = m; j = u; k = v; }
     else { i = u; j = v; k = m; }
-    const T aw = coef[coef_aw(B) + i], ae = coef[coef_ae(B) + i];
-    const T as = coef[coef_as(B) + j], an = coef[coef_an(B) + j];
-    const T ab = coef[coef_ab(B) + k], at = coef[coef_at(B) + k];
+    const T aw = cf.aw[i], ae = cf.ae[i], as = cf.as[j], an = cf.an[j], ab = cf.ab[k], at = cf.at[k];
     const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-    const T su = rhs[raddr(m)];
+    const T su = R[off(m)];
     if (dir == 0) {
       const T apr = (T)1.0 / (ap - as * a[m - 1]);
       a[m] = an * apr;
-      c[m] = (su - ae * phi[cell_addr(B, B.phi0, i + 1, j, k)] - aw * phi[cell_addr(B, B.phi0, i - 1, j, k)] -
-              at * phi[cell_addr(B, B.phi0, i, j, k + 1)] - ab * phi[cell_addr(B, B.phi0, i, j, k - 1)] -
-              as * c[m - 1]) * apr;
+      c[m] = (su - ae * P[cell_off(B, i + 1, j, k)] - aw * P[cell_off(B, i - 1, j, k)] -
+              at * P[cell_off(B, i, j, k + 1)] - ab * P[cell_off(B, i, j, k - 1)] - as * c[m - 1]) * apr;
     } else if (dir == 1) {
       const T apr = (T)1.0 / (ap - aw * a[m - 1]);
       a[m] = ae * apr;
-      c[m] = (su - an * phi[cell_addr(B, B.phi0, i, j + 1, k)] - as * phi[cell_addr(B, B.phi0, i, j - 1, k)] -
-              at * phi[cell_addr(B, B.phi0, i, j, k + 1)] - ab * phi[cell_addr(B, B.phi0, i, j, k - 1)] -
-              aw * c[m - 1]) * apr;
+      c[m] = (su - an * P[cell_off(B, i, j + 1, k)] - as * P[cell_off(B, i, j - 1, k)] -
+              at * P[cell_off(B, i, j, k + 1)] - ab * P[cell_off(B, i, j, k - 1)] - aw * c[m - 1]) * apr;
     } else {
       const T apr = (T)1.0 / (ap - ab * a[m - 1]);
       a[m] = at * apr;
-      c[m] = (su - an * phi[cell_addr(B, B.phi0, i, j + 1, k)] - as * phi[cell_addr(B, B.phi0, i, j - 1, k)] -
-              ae * phi[cell_addr(B, B.phi0, i + 1, j, k)] - aw * phi[cell_addr(B, B.phi0, i - 1, j, k)] -
-              ab * c[m - 1]) * apr;
+      c[m] = (su - an * P[cell_off(B, i, j + 1, k)] - as * P[cell_off(B, i, j - 1, k)] -
+              ae * P[cell_off(B, i + 1, j, k)] - aw * P[cell_off(B, i - 1, j, k)] - ab * c[m - 1]) * apr;
     }
   }
-  for (int m = n; m >= 1; --m) phi[addr(m)] = (c[m] - a[m] * phi[addr(m + 1)]);
+  for (int m = n; m >= 1; --m) P[off(m)] = (c[m] - a[m] * P[off(m + 1)]);
 }
 
 template <typename T>
-__global__ void k_tdma(const BlkLev *__restrict__ bl, T *__restrict__ phi, const T *__restrict__ rhs,
-                       const T *__restrict__ coef, T *__restrict__ work, int ngg) {
-  const BlkLev B = bl[blockIdx.x];
+__global__ void k_tdma(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, const int *__restrict__ act,
+                       T *__restrict__ work, int ngg) {
+  const BlkLev B = bl[blocks[blockIdx.x]];
+  if (!act[B.dom]) return;
   T *a = work + ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2 * ngg;
   T *c = a + ngg;
   for (int dir = 0; dir < 3; ++dir) {
@@ -214,7 +277,7 @@ __global__ void k_tdma(const BlkLev *__restrict__ bl, T *__restrict__ phi, const
       for (int u = 1 + threadIdx.x; u <= nu; u += blockDim.x) {
         const int v = sum - u;
         if (v < 1 || v > nv) continue;
-        tdma_line(B, phi, rhs, coef, dir, u, v, a, c);
+        tdma_line(B, dir, u, v, a, c);
       }
       __syncthreads();
     }
@@ -230,50 +293,47 @@ __global__ void k_tdma(const BlkLev *__restrict__ bl, T *__restrict__ phi, const
 // of the non-uniform-grid extension and is exactly 1.0 on a uniform grid.
 // ---------------------------------------------------------------------------
 template <typename T>
-__device__ inline T residual_at(const BlkLev &F, const T *__restrict__ phi, const T *__restrict__ rhs,
-                                const T *__restrict__ coef, int i, int j, int k) {
-  const T aw = coef[coef_aw(F) + i], ae = coef[coef_ae(F) + i];
-  const T as = coef[coef_as(F) + j], an = coef[coef_an(F) + j];
-  const T ab = coef[coef_ab(F) + k], at = coef[coef_at(F) + k];
+__device__ inline T residual_at(const BlkLev &F, const Coef<T> &cf, int i, int j, int k) {
+  const T *P = phi_of<T>(F);
+  const T aw = cf.aw[i], ae = cf.ae[i], as = cf.as[j], an = cf.an[j], ab = cf.ab[k], at = cf.at[k];
   const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-  const T pw = phi[cell_addr(F, F.phi0, i - 1, j, k)], pe = phi[cell_addr(F, F.phi0, i + 1, j, k)];
-  const T ps = phi[cell_addr(F, F.phi0, i, j - 1, k)], pn = phi[cell_addr(F, F.phi0, i, j + 1, k)];
-  const T pb = phi[cell_addr(F, F.phi0, i, j, k - 1)], pt = phi[cell_addr(F, F.phi0, i, j, k + 1)];
-  const T pp = phi[cell_addr(F, F.phi0, i, j, k)];
-  const T r = rhs[cell_addr(F, F.rhs0, i, j, k)];
+  const T pw = P[cell_off(F, i - 1, j, k)], pe = P[cell_off(F, i + 1, j, k)];
+  const T ps = P[cell_off(F, i, j - 1, k)], pn = P[cell_off(F, i, j + 1, k)];
+  const T pb = P[cell_off(F, i, j, k - 1)], pt = P[cell_off(F, i, j, k + 1)];
+  const T pp = P[cell_off(F, i, j, k)];
+  const T r = rhs_of<T>(F)[cell_off(F, i, j, k)];
   return r - (aw * pw + ae * pe + as * ps + an * pn + ab * pb + at * pt + ap * pp);
 }
 
 template <typename TF, typename TC>
-__global__ void __launch_bounds__(kTile) k_restrict(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
-                                                    const Tile *__restrict__ tiles, const TF *__restrict__ phif,
-                                                    const TF *__restrict__ rhsf, const TF *__restrict__ coeff,
-                                                    TC *__restrict__ phic, TC *__restrict__ rhsc,
-                                                    const TF *__restrict__ geo) {
+__global__ void __launch_bounds__(RW_TX *RW_RJ) k_restrict(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
+                                                           const Tile *__restrict__ tiles, const int *__restrict__ act) {
   const Tile t = tiles[blockIdx.x];
   const BlkLev Cb = cl[t.blk];
+  if (!act[Cb.dom]) return;
   const BlkLev Fb = fl[t.blk];
-  const int W = Cb.nx + 2, H = Cb.ny + 2;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  if (q >= (long long)W * H * (Cb.nz + 2)) return;
-  const int k = (int)(q / ((long long)W * H));
-  const int rem = (int)(q - (long long)k * W * H);
-  const int j = rem / W, i = rem - j * W;
-  phic[cell_addr(Cb, Cb.phi0, i, j, k)] = (TC)0;
-  if (i < 1 || i > Cb.nx || j < 1 || j > Cb.ny || k < 1 || k > Cb.nz) return;
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i > Cb.nx + 1 || j > Cb.ny + 1) return;
+  const Coef<TF> cf(Fb);
   // restriction ratios of the fine level: rx[nxf+2], ry[nyf+2], rz[nzf+2]
-  const TF *rx = geo + Fb.geo, *ry = rx + (Fb.nx + 2), *rz = ry + (Fb.ny + 2);
-  TF acc[8];
-  int n = 0;
-  for (int dk = 0; dk < 2; ++dk)
-    for (int dj = 0; dj < 2; ++dj)
-      for (int di = 0; di < 2; ++di) {
-        const int fi = 2 * i - 1 + di, fj = 2 * j - 1 + dj, fk = 2 * k - 1 + dk;
-        const TF s = (TF)8.0 * rx[fi] * ry[fj] * rz[fk];
-        acc[n++] = residual_at(Fb, phif, rhsf, coeff, fi, fj, fk) * s;
-      }
-  const TF v = (TF)0.125 * (acc[0] + acc[1] + acc[2] + acc[3] + acc[4] + acc[5] + acc[6] + acc[7]);
-  rhsc[cell_addr(Cb, Cb.rhs0, i, j, k)] = (TC)v;
+  const TF *rx = (const TF *)Fb.geo, *ry = rx + (Fb.nx + 2), *rz = ry + (Fb.ny + 2);
+  const bool inij = i >= 1 && i <= Cb.nx && j >= 1 && j <= Cb.ny;
+  const int k1 = min(t.k0 + RW_KCH - 1, Cb.nz + 1);
+  for (int k = t.k0; k <= k1; ++k) {
+    phi_of<TC>(Cb)[cell_off(Cb, i, j, k)] = (TC)0;
+    if (!inij || k < 1 || k > Cb.nz) continue;
+    TF acc[8];
+    int n = 0;
+    for (int dk = 0; dk < 2; ++dk)
+      for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+          const int fi = 2 * i - 1 + di, fj = 2 * j - 1 + dj, fk = 2 * k - 1 + dk;
+          const TF s = (TF)8.0 * rx[fi] * ry[fj] * rz[fk];
+          acc[n++] = residual_at<TF>(Fb, cf, fi, fj, fk) * s;
+        }
+    const TF v = (TF)0.125 * (acc[0] + acc[1] + acc[2] + acc[3] + acc[4] + acc[5] + acc[6] + acc[7]);
+    rhs_of<TC>(Cb)[cell_off(Cb, i, j, k)] = (TC)v;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -285,41 +345,41 @@ __global__ void __launch_bounds__(kTile) k_restrict(const BlkLev *__restrict__ f
 // mgbound copies it to, so no cell is read after another thread wrote it.
 // ---------------------------------------------------------------------------
 template <typename TF, typename TC>
-__global__ void __launch_bounds__(kTile) k_prolong(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
-                                                   const Tile *__restrict__ tiles, TF *__restrict__ phif,
-                                                   const TC *__restrict__ phic) {
+__global__ void __launch_bounds__(RW_TX *RW_RJ) k_prolong(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
+                                                          const Tile *__restrict__ tiles, const int *__restrict__ act) {
   const Tile t = tiles[blockIdx.x];
   const BlkLev Fb = fl[t.blk];
+  if (!act[Fb.dom]) return;
   const BlkLev Cb = cl[t.blk];
-  const int W = Fb.nx + 2, H = Fb.ny + 2;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  if (q >= (long long)W * H * (Fb.nz + 2)) return;
-  const int k = (int)(q / ((long long)W * H));
-  const int rem = (int)(q - (long long)k * W * H);
-  const int j = rem / W, i = rem - j * W;
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i > Fb.nx + 1 || j > Fb.ny + 1) return;
   const int m = Fb.nmask;
   // Neumann ghost cells are written by their owners below
-  if ((i == 0 && (m & 1)) || (i == Fb.nx + 1 && (m & 2)) || (j == 0 && (m & 4)) || (j == Fb.ny + 1 && (m & 8)) ||
-      (k == 0 && (m & 16)) || (k == Fb.nz + 1 && (m & 32)))
-    return;
+  if ((i == 0 && (m & 1)) || (i == Fb.nx + 1 && (m & 2)) || (j == 0 && (m & 4)) || (j == Fb.ny + 1 && (m & 8))) return;
+  const TC *__restrict__ PC = phi_of<TC>(Cb);
+  TF *__restrict__ PF = phi_of<TF>(Fb);
+  const int k1 = min(t.k0 + RW_KCH - 1, Fb.nz + 1);
+#pragma unroll 2
+  for (int k = t.k0; k <= k1; ++k) {
+  if ((k == 0 && (m & 16)) || (k == Fb.nz + 1 && (m & 32))) continue;
   const int ic = i >> 1, jc = j >> 1, kc = k >> 1;        // lower coarse cell
   const int wi0 = (i & 1) ? 1 : 3, wj0 = (j & 1) ? 1 : 3, wk0 = (k & 1) ? 1 : 3;
   const int wi1 = 4 - wi0, wj1 = 4 - wj0, wk1 = 4 - wk0;
-  const TF c000 = (TF)phic[cell_addr(Cb, Cb.phi0, ic, jc, kc)];
-  const TF c010 = (TF)phic[cell_addr(Cb, Cb.phi0, ic, jc + 1, kc)];
-  const TF c001 = (TF)phic[cell_addr(Cb, Cb.phi0, ic, jc, kc + 1)];
-  const TF c011 = (TF)phic[cell_addr(Cb, Cb.phi0, ic, jc + 1, kc + 1)];
-  const TF c100 = (TF)phic[cell_addr(Cb, Cb.phi0, ic + 1, jc, kc)];
-  const TF c110 = (TF)phic[cell_addr(Cb, Cb.phi0, ic + 1, jc + 1, kc)];
-  const TF c101 = (TF)phic[cell_addr(Cb, Cb.phi0, ic + 1, jc, kc + 1)];
-  const TF c111 = (TF)phic[cell_addr(Cb, Cb.phi0, ic + 1, jc + 1, kc + 1)];
+  const TF c000 = (TF)PC[cell_off(Cb, ic, jc, kc)];
+  const TF c010 = (TF)PC[cell_off(Cb, ic, jc + 1, kc)];
+  const TF c001 = (TF)PC[cell_off(Cb, ic, jc, kc + 1)];
+  const TF c011 = (TF)PC[cell_off(Cb, ic, jc + 1, kc + 1)];
+  const TF c100 = (TF)PC[cell_off(Cb, ic + 1, jc, kc)];
+  const TF c110 = (TF)PC[cell_off(Cb, ic + 1, jc + 1, kc)];
+  const TF c101 = (TF)PC[cell_off(Cb, ic + 1, jc, kc + 1)];
+  const TF c111 = (TF)PC[cell_off(Cb, ic + 1, jc + 1, kc + 1)];
   const TF corr = ((TF)(wi0 * wj0 * wk0) * c000 + (TF)(wi0 * wj1 * wk0) * c010 + (TF)(wi0 * wj0 * wk1) * c001 +
                    (TF)(wi0 * wj1 * wk1) * c011 + (TF)(wi1 * wj0 * wk0) * c100 + (TF)(wi1 * wj1 * wk0) * c110 +
-                   (TF)(wi1 * wj0 * wk1) * c101 + (TF)(wi1 * wj1 * wk1) * c111) /
-                  (TF)64.0;
-  const long long a = cell_addr(Fb, Fb.phi0, i, j, k);
-  const TF v = phif[a] + corr;
-  phif[a] = v;
+                   (TF)(wi1 * wj0 * wk1) * c101 + (TF)(wi1 * wj1 * wk1) * c111) *
+                  (TF)0.015625;  // x/64 == x*2^-6 exactly in IEEE arithmetic
+  const long long a = cell_off(Fb, i, j, k);
+  const TF v = PF[a] + corr;
+  PF[a] = v;
   // mirror targets on Neumann faces (mgbound order W,E,S,N,B,T composes to a clamp)
   int xs[3] = {i, i, i}, ys[3] = {j, j, j}, zs[3] = {k, k, k};
   int nxo = 1, nyo = 1, nzo = 1;
@@ -329,49 +389,65 @@ __global__ void __launch_bounds__(kTile) k_prolong(const BlkLev *__restrict__ fl
   if (j == Fb.ny && (m & 8)) ys[nyo++] = Fb.ny + 1;
   if (k == 1 && (m & 16)) zs[nzo++] = 0;
   if (k == Fb.nz && (m & 32)) zs[nzo++] = Fb.nz + 1;
-  if (nxo == 1 && nyo == 1 && nzo == 1) return;
+  if (nxo == 1 && nyo == 1 && nzo == 1) continue;
   for (int a3 = 0; a3 < nzo; ++a3)
     for (int a2 = 0; a2 < nyo; ++a2)
       for (int a1 = 0; a1 < nxo; ++a1) {
         if (a1 == 0 && a2 == 0 && a3 == 0) continue;
-        phif[cell_addr(Fb, Fb.phi0, xs[a1], ys[a2], zs[a3])] = v;
+        PF[cell_off(Fb, xs[a1], ys[a2], zs[a3])] = v;
       }
+  }
 }
 
 // ---------------------------------------------------------------------------
-// Halo copies of one level: the composition of exchangepp + mgbound +
-// exchbc_mgpp as (dst, src) element pairs against the state before the
-// exchange.  Pairs [0, nstaged) have a source that is itself overwritten:
-// k_halo_stage reads those first, k_halo_apply writes everything.
+// Halo copies of one level: the composition of mgbound + exchangepp +
+// mgbound + exchbc_mgpp as element pairs (dst block, dst offset, src block,
+// src offset) against the state before the refresh.  Pairs [0, nstaged)
+// have a source that is itself overwritten: k_halo_stage reads those first,
+// k_halo_apply writes everything.
 // ---------------------------------------------------------------------------
+struct HaloCopy {
+  int dblk, doff, sblk, soff;
+};
 template <typename T>
-__global__ void k_halo_stage(const long long *__restrict__ src, int nstaged, const T *__restrict__ phi,
-                             T *__restrict__ buf) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < nstaged) buf[t] = phi[src[t]];
+__global__ void k_halo_stage(const BlkLev *__restrict__ bl, const HaloCopy *__restrict__ hc, int nstaged,
+                             const int *__restrict__ act, T *__restrict__ buf) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nstaged) return;
+  const HaloCopy c = hc[t];
+  const BlkLev S = bl[c.sblk];
+  if (!act[S.dom]) return;
+  buf[t] = phi_of<T>(S)[c.soff];
 }
 template <typename T>
-__global__ void k_halo_apply(const long long *__restrict__ dst, const long long *__restrict__ src, int n,
-                             int nstaged, T *__restrict__ phi, const T *__restrict__ buf) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_halo_apply(const BlkLev *__restrict__ bl, const HaloCopy *__restrict__ hc, int n, int nstaged,
+                             const int *__restrict__ act, const T *__restrict__ buf) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  T v = t < nstaged ? buf[t] : phi[src[t]];
-  phi[dst[t]] = v;
+  const HaloCopy c = hc[t];
+  const BlkLev D = bl[c.dblk];
+  if (!act[D.dom]) return;
+  const T v = t < nstaged ? buf[t] : phi_of<T>(bl[c.sblk])[c.soff];
+  phi_of<T>(D)[c.doff] = v;
 }
 
-// Zero the ghost shell of every block of a level (pp = 0 before a V-cycle).
+// Zero the ghost shell of a set of blocks (pp = 0 before a V-cycle): one
+// thread per ghost cell, enumerated face by face (edges twice - zeros).
 template <typename T>
-__global__ void k_zero_ghosts(const BlkLev *__restrict__ bl, const Tile *__restrict__ tiles, T *__restrict__ phi) {
-  const Tile t = tiles[blockIdx.x];
-  const BlkLev B = bl[t.blk];
-  const int W = B.nx + 2, H = B.ny + 2;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  if (q >= (long long)W * H * (B.nz + 2)) return;
-  const int k = (int)(q / ((long long)W * H));
-  const int rem = (int)(q - (long long)k * W * H);
-  const int j = rem / W, i = rem - j * W;
-  if (i >= 1 && i <= B.nx && j >= 1 && j <= B.ny && k >= 1 && k <= B.nz) return;
-  phi[cell_addr(B, B.phi0, i, j, k)] = (T)0;
+__global__ void k_zero_ghosts(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, int nblk) {
+  const int b = blockIdx.y;
+  if (b >= nblk) return;
+  const BlkLev B = bl[blocks[b]];
+  T *P = phi_of<T>(B);
+  const int W = B.nx + 2, H = B.ny + 2, D = B.nz + 2;
+  const int nyz = H * D, nxz = W * D, nxy = W * H;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < 2 * (nyz + nxz + nxy); q += gridDim.x * blockDim.x) {
+    int i, j, k, r = q;
+    if (r < 2 * nyz) { const int f = r / nyz; r -= f * nyz; i = f ? W - 1 : 0; j = r % H; k = r / H; }
+    else if ((r -= 2 * nyz) < 2 * nxz) { const int f = r / nxz; r -= f * nxz; j = f ? H - 1 : 0; i = r % W; k = r / W; }
+    else { r -= 2 * nxz; const int f = r / nxy; r -= f * nxy; k = f ? D - 1 : 0; i = r % W; j = r / W; }
+    P[cell_off(B, i, j, k)] = (T)0;
+  }
 }
 
 }  // namespace mf3d

@@ -1,9 +1,16 @@
 // libmf3d: B200 (sm_100a) pressure-Poisson multigrid for MultiFlow3D's
-// projection step.  Host driver (C++) + C ABI of include/mf3d.h.
+// projection step.  Host engine (C++) + C ABI of include/mf3d.h.
 //
-// One context = one device, one stream, all blocks of the solve resident.
-// The reference's per-rank MPI halo traffic becomes on-device copies; its
-// module state (vars, multidata) becomes the context.
+// Resident storage: every block owns its multigrid hierarchy (colour-split
+// phi and rhs per level, 1-D coefficient and restriction-weight arrays) and
+// its face planes.  Blocks belong to domains; a domain is one projection
+// problem (the reference's set of blocks) and converges on its own.  A view
+// is a launchable set of blocks: per level it holds the block descriptor
+// table, the tile lists and the halo-copy lists of the subsets a lock-step
+// V-cycle over domains of different depths needs, the per-domain solve
+// state and the CUDA graph of one outer iteration.  One view serves one
+// multi-block solve (one domain), a batch (many domains) or the server's
+// current mix of resident requests.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -38,6 +45,17 @@ template <typename T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf &operator=(DevBuf &&o) noexcept {
+    if (this != &o) {
+      if (p) cudaFree(p);
+      p = o.p; n = o.n; o.p = nullptr; o.n = 0;
+    }
+    return *this;
+  }
   ~DevBuf() { if (p) cudaFree(p); }
   int alloc(size_t count) {
     if (p) { cudaFree(p); p = nullptr; }
@@ -46,6 +64,7 @@ struct DevBuf {
     cudaError_t e = cudaMalloc(&p, count * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;
+      n = 0;
       set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
       return e == cudaErrorMemoryAllocation ? MF3D_E_OOM : MF3D_E_CUDA;
     }
@@ -59,29 +78,295 @@ struct DevBuf {
   }
 };
 
-// Tile list: for each block, ceil(items_b / kTile) CTAs.
+static inline int grid_of(long long n, int tpb) { return (int)((n + tpb - 1) / tpb); }
+
+// 1-D item tiles: for each block, ceil(items_b / kTile) CTAs (i0 = first item).
 static std::vector<Tile> make_tiles(const std::vector<long long> &items) {
   std::vector<Tile> t;
   for (size_t b = 0; b < items.size(); ++b)
-    for (long long s = 0; s < items[b]; s += kTile) t.push_back(Tile{(int)b, (int)s});
+    for (long long s = 0; s < items[b]; s += kTile) t.push_back(Tile{(int)b, 0, 0, (int)s});
   return t;
 }
+// A per-block index box [i0,i1] x [j0,j1] x [k0,k1] (inclusive).
+struct Box {
+  int i0, i1, j0, j1, k0, k1;
+};
+static void add_tiles_2d(std::vector<Tile> &t, int blk, const Box &x, int TX, int RJ, int kch) {
+  if (x.i1 < x.i0 || x.j1 < x.j0 || x.k1 < x.k0) return;
+  for (int k = x.k0; k <= x.k1; k += kch)
+    for (int j = x.j0; j <= x.j1; j += RJ)
+      for (int i = x.i0; i <= x.i1; i += TX) t.push_back(Tile{blk, k, j, i});
+}
 
-// One multigrid level of every block, storage type T.
-template <typename T>
-struct Level {
-  int g = 0;
-  std::vector<BlkLev> hb;
-  DevBuf<BlkLev> db;
-  DevBuf<T> phi, rhs, coef, geo;
-  DevBuf<Tile> t_sweep, t_cells;
-  int n_sweep = 0, n_cells = 0;
-  DevBuf<long long> hdst, hsrc;
-  DevBuf<T> hbuf;
-  int nhalo = 0, nstaged = 0;
-  DevBuf<T> tdma_work;
+// 1/h when h is a (normal) power of two - then x*(1/h) == x/h exactly - else 0.
+static double pow2_inverse(double h) {
+  if (!(h > 0.0) || !std::isfinite(h)) return 0.0;
+  int e;
+  const double m = std::frexp(h, &e);
+  if (m != 0.5) return 0.0;
+  const double inv = 1.0 / h;
+  return (std::isfinite(inv) && inv * h == 1.0) ? inv : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Resident storage of one block.
+// ---------------------------------------------------------------------------
+struct LevelStore {
+  DevBuf<char> phi, rhs, coef, geo;
+  BlkLev desc;  // host copy with device pointers
+};
+
+struct BlockStore {
+  mf3d_block_desc d;     // neighbour ids refer to blocks of the same domain
+  int ngrid = 1;
+  int elem = 8;          // bytes per multigrid value (8 FP64, 4 FP32)
+  std::vector<LevelStore> lv;  // [1..ngrid]
+  DevBuf<double> geo1;   // level-1 widths h[3] (n+2) and face distances df[3] (n+1)
+  DevBuf<double> planes; // face planes lo/hi of u, v, w
+  BlkFld fld;            // host template (field pointers bound per call)
+  size_t bytes = 0;      // device bytes owned
+};
+
+// Build one block's hierarchy: replaces `coeff` (mgsolver.for:2-222) and the
+// `cof` sizing of localparameters.for:208-237.
+static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int elem, int pl, cudaStream_t s) {
+  S.d = d;
+  S.ngrid = ngrid;
+  S.elem = elem;
+  S.lv.clear();
+  S.lv.resize(ngrid + 1);
+  S.bytes = 0;
+  const double *ext[3] = {d.hx, d.hy, d.hz};
+  const double hh[3] = {d.dx, d.dy, d.dz};
+  const int nfine[3] = {d.nx, d.ny, d.nz};
+  int nmask = 0;
+  const int nbr[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+  const int bc[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+  for (int f = 0; f < 6; ++f)
+    if (nbr[f] < 0 && bc[f] != MF3D_BC_PERIODIC) nmask |= 1 << f;
+  int st;
+  for (int g = 1; g <= ngrid; ++g) {
+    LevelStore &L = S.lv[g];
+    BlkLev &B = L.desc;
+    std::memset(&B, 0, sizeof B);
+    B.nx = d.nx >> (g - 1);
+    B.ny = d.ny >> (g - 1);
+    B.nz = d.nz >> (g - 1);
+    B.hp = hp_of(B.nx);
+    B.cstr = (long long)(B.nz + 2) * (B.ny + 2) * B.hp;
+    B.cstr = (B.cstr + 31) / 32 * 32;  // 256-byte aligned colour arrays
+    B.nmask = nmask;
+    const size_t nbytes = (size_t)(2 * B.cstr) * elem;
+    if ((st = L.phi.alloc(nbytes))) return st;
+    if ((st = L.rhs.alloc(nbytes))) return st;
+    CK(cudaMemsetAsync(L.phi.p, 0, nbytes, s));
+    CK(cudaMemsetAsync(L.rhs.p, 0, nbytes, s));
+    S.bytes += 2 * nbytes;
+    // coefficients aw, ae (x), as, an (y), ab, at (z); Neumann faces zeroed
+    std::vector<double> coef, geo;
+    const int nn[3] = {B.nx, B.ny, B.nz};
+    for (int a = 0; a < 3; ++a) {
+      std::vector<double> w = level_widths(ext[a], nfine[a], hh[a], ngrid, g);
+      const int n = nn[a];
+      const double hl = hh[a] * (double)(1 << (g - 1));
+      const double dd = hl * hl;
+      for (int side = 0; side < 2; ++side)
+        for (int c = 0; c < n + 2; ++c) {
+          double v = 0.0;
+          if (c >= 1 && c <= n) {
+            if (!ext[a]) v = 1.0 / dd;  // mgsolver.for:184-189
+            else v = 1.0 / (w[c] * (0.5 * (w[c] + w[side ? c + 1 : c - 1])));
+            const int f = 2 * a + side;
+            if ((nmask >> f & 1) && c == (side ? n : 1)) v = 0.0;  // mgsolver.for:192-203
+          }
+          coef.push_back(v);
+        }
+    }
+    // restriction ratios hf/Hc of this (fine) level: 0.5 exactly on uniform axes
+    for (int a = 0; a < 3; ++a) {
+      const int n = nn[a];
+      if (g < ngrid) {
+        std::vector<double> wf = level_widths(ext[a], nfine[a], hh[a], ngrid, g);
+        std::vector<double> wc = level_widths(ext[a], nfine[a], hh[a], ngrid, g + 1);
+        for (int c = 0; c < n + 2; ++c) geo.push_back((c >= 1 && c <= n) ? wf[c] / wc[(c + 1) >> 1] : 0.0);
+      } else {
+        for (int c = 0; c < n + 2; ++c) geo.push_back(0.0);
+      }
+    }
+    auto put = [&](DevBuf<char> &buf, const std::vector<double> &v) -> int {
+      int r = buf.alloc(v.size() * elem);
+      if (r) return r;
+      if (elem == 8) {
+        CK(cudaMemcpyAsync(buf.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice, s));
+      } else {
+        std::vector<float> f(v.begin(), v.end());
+        CK(cudaMemcpyAsync(buf.p, f.data(), f.size() * 4, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));  // f is a local
+      }
+      return MF3D_OK;
+    };
+    if ((st = put(L.coef, coef))) return st;
+    if ((st = put(L.geo, geo))) return st;
+    B.phi = L.phi.p;
+    B.rhs = L.rhs.p;
+    B.coef = L.coef.p;
+    B.geo = L.geo.p;
+  }
+  // level-1 field geometry: widths, face distances (bit-exact dx on a uniform axis)
+  std::vector<double> g1;
+  size_t off_h[3], off_df[3];
+  for (int a = 0; a < 3; ++a) {
+    std::vector<double> w = level_widths(ext[a], nfine[a], hh[a], ngrid, 1);
+    off_h[a] = g1.size();
+    for (int c = 0; c < nfine[a] + 2; ++c) g1.push_back(ext[a] ? w[c] : hh[a]);
+    off_df[a] = g1.size();
+    for (int c = 0; c <= nfine[a]; ++c) g1.push_back(ext[a] ? 0.5 * (w[c] + w[c + 1]) : hh[a]);
+  }
+  if ((st = S.geo1.upload(g1, s))) return st;
+  const size_t pyz = (size_t)d.ny * d.nz, pxz = (size_t)d.nx * d.nz, pxy = (size_t)d.nx * d.ny;
+  if ((st = S.planes.alloc(2 * (pyz + pxz + pxy)))) return st;
+  CK(cudaMemsetAsync(S.planes.p, 0, S.planes.n * sizeof(double), s));
+  CK(cudaStreamSynchronize(s));  // g1 is a local
+  S.bytes += (S.geo1.n + S.planes.n) * sizeof(double);
+  BlkFld &F = S.fld;
+  std::memset(&F, 0, sizeof F);
+  F.nx = d.nx; F.ny = d.ny; F.nz = d.nz; F.pl = pl;
+  F.ti = d.nx + 2 * pl; F.tj = d.ny + 2 * pl;
+  for (int a = 0; a < 3; ++a) {
+    F.h[a] = S.geo1.p + off_h[a];
+    F.df[a] = S.geo1.p + off_df[a];
+  }
+  double *pp = S.planes.p;
+  F.lo[0] = pp; F.hi[0] = pp + pyz; pp += 2 * pyz;
+  F.lo[1] = pp; F.hi[1] = pp + pxz; pp += 2 * pxz;
+  F.lo[2] = pp; F.hi[2] = pp + pxy;
+  F.L1 = S.lv[1].desc;
+  for (int a = 0; a < 3; ++a) F.pinv[a] = ext[a] ? 0.0 : pow2_inverse(hh[a]);
+  return MF3D_OK;
+}
+
+// A halo copy between blocks of one domain (domain-local block indices).
+struct HaloLocal {
+  int dblk, doff, sblk, soff;
+};
+
+// One domain: its blocks, halo copy lists per level, face rules.
+struct DomainStore {
+  int ngrid = 1;
+  std::vector<std::unique_ptr<BlockStore>> blocks;
+  std::vector<std::vector<HaloLocal>> halo;  // per level, staged pairs first
+  std::vector<int> nstaged;                  // per level
+  std::vector<FaceRule> rules;               // 6 per block, domain-local sources
+  size_t bytes = 0;
+};
+
+static long long level_off(const BlkLev &B, int i, int j, int k) {
+  const int c = (i + j + k + 1) & 1;
+  return c * B.cstr + ((long long)k * (B.ny + 2) + j) * B.hp + (i >> 1);
+}
+
+static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, int ngrid, int elem, int pl,
+                        cudaStream_t s) {
+  D.ngrid = ngrid;
+  D.blocks.clear();
+  std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
+  int st = face_rules(descs, D.rules);
+  if (st) return st;
+  D.bytes = 0;
+  for (int b = 0; b < nb; ++b) {
+    D.blocks.emplace_back(new BlockStore());
+    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, pl, s))) return st;
+    D.bytes += D.blocks.back()->bytes;
+  }
+  D.halo.assign(ngrid + 1, {});
+  D.nstaged.assign(ngrid + 1, 0);
+  for (int g = 1; g <= ngrid; ++g) {
+    std::vector<LevelGeom> geom(nb);
+    std::vector<long long> base(nb);
+    long long acc = 0;
+    for (int b = 0; b < nb; ++b) {
+      const BlkLev &B = D.blocks[b]->lv[g].desc;
+      geom[b] = LevelGeom{B.nx, B.ny, B.nz};
+      base[b] = acc;
+      acc += geom[b].cells();
+    }
+    std::vector<HaloPair> pairs = build_halo_map(descs, geom, base);
+    std::unordered_set<long long> dsts;
+    for (auto &p : pairs) dsts.insert(p.dst);
+    auto loc = [&](long long id, int &blk, int &off) {
+      int b = (int)(std::upper_bound(base.begin(), base.end(), id) - base.begin()) - 1;
+      long long lin = id - base[b];
+      const LevelGeom &G = geom[b];
+      int i = (int)(lin % (G.nx + 2));
+      long long r = lin / (G.nx + 2);
+      int j = (int)(r % (G.ny + 2));
+      int k = (int)(r / (G.ny + 2));
+      blk = b;
+      off = (int)level_off(D.blocks[b]->lv[g].desc, i, j, k);
+    };
+    for (int pass = 0; pass < 2; ++pass)
+      for (auto &p : pairs) {
+        const bool staged = dsts.count(p.src) > 0;
+        if ((pass == 0) != staged) continue;
+        HaloLocal h;
+        loc(p.dst, h.dblk, h.doff);
+        loc(p.src, h.sblk, h.soff);
+        D.halo[g].push_back(h);
+        if (staged) D.nstaged[g]++;
+      }
+  }
+  return MF3D_OK;
+}
+
+// ---------------------------------------------------------------------------
+// A view: launch tables over a set of domains.
+// ---------------------------------------------------------------------------
+enum Subset { SUB_A = 0, SUB_C = 1, SUB_D = 2 };  // all present / coarsest here / continuing down
+
+struct ViewLevel {
+  DevBuf<BlkLev> tab;                 // one entry per view block (absent: nx = 0)
+  DevBuf<Tile> sweep[3], cells[3];
+  int n_sweep[3] = {0, 0, 0}, n_cells[3] = {0, 0, 0};
+  DevBuf<int> list[3];
+  int n_list[3] = {0, 0, 0};
+  DevBuf<HaloCopy> halo[3];
+  int n_halo[3] = {0, 0, 0}, n_staged[3] = {0, 0, 0};
+  DevBuf<char> stage[3];              // staged halo values
+  long long cells_sub[3] = {0, 0, 0}; // interior cells of each subset
   int ngg = 0;
-  bool zero_interior = false;  // interior known to be all zero (right after mgrestr)
+};
+
+struct View {
+  std::vector<BlockStore *> blk;      // view position -> block
+  std::vector<int> blk_dom;           // view position -> view domain
+  std::vector<DomainStore *> dom;     // view domain -> domain
+  int Lmax = 0;
+  std::vector<ViewLevel> lv;          // [1..Lmax]
+  std::vector<BlkFld> hf;
+  DevBuf<BlkFld> df;
+  DevBuf<Tile> t_int, t_zint, t_l1cells, t_faces, t_planes;
+  int n_int = 0, n_zint = 0, n_l1cells = 0, n_faces = 0, n_planes = 0;
+  DevBuf<DomState> ds;
+  DevBuf<int> act, ones;
+  DevBuf<unsigned long long> rmax, rmax_scratch;
+  DevBuf<double> hist;
+  int hcap = 0;
+  DevBuf<char> work;                  // TDMA line scratch
+  long long n_l1 = 0;
+  // graphs: the whole outer loop (WHILE node) and a single iteration
+  cudaGraph_t g_loop = nullptr, g_once = nullptr;
+  cudaGraphExec_t x_loop = nullptr, x_once = nullptr;
+  cudaGraphConditionalHandle cond = 0;
+  long long launches_per_iter = 0;
+  void drop_graphs() {
+    if (x_loop) cudaGraphExecDestroy(x_loop);
+    if (g_loop) cudaGraphDestroy(g_loop);
+    if (x_once) cudaGraphExecDestroy(x_once);
+    if (g_once) cudaGraphDestroy(g_once);
+    x_loop = x_once = nullptr;
+    g_loop = g_once = nullptr;
+  }
+  ~View() { drop_graphs(); }
 };
 
 }  // namespace mf3d
@@ -90,46 +375,27 @@ using namespace mf3d;
 
 struct mf3d_ctx {
   mf3d_params prm;
-  std::vector<mf3d_block_desc> blocks;
-  int nb = 0;
   int device = 0;
+  int elem = 8;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long long launches = 0;
-  // hierarchy (one of the two is used, by precision)
-  std::vector<std::unique_ptr<Level<double>>> L64;
-  std::vector<std::unique_ptr<Level<float>>> L32;
-  // fields
-  std::vector<BlkFld> hf;
-  DevBuf<BlkFld> df;
-  std::vector<FaceRule> rules;
-  DevBuf<double> widths, planes;  // geometry, face planes
-  DevBuf<double> mirror;          // device mirrors of host fields (host entry point)
-  std::vector<size_t> mirror_off;
-  DevBuf<Tile> t_int, t_l1cells, t_faces, t_planes;
-  int n_int = 0, n_l1cells = 0, n_faces = 0, n_planes = 0;
-  DevBuf<unsigned long long> rmax_cur, rmax_scratch;  // atomic-max targets of calmas
-  DevBuf<SolveState> st;                     // device-resident solve control
-  DevBuf<double> hist_d;                     // rmax after each outer iteration
-  unsigned long long *rmax_host = nullptr;  // pinned
+  std::vector<std::unique_ptr<DomainStore>> doms;
+  std::unique_ptr<View> view;
   bool use_graph = true;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
-  cudaGraphConditionalHandle cond = 0;
-  long long launches_per_iter = 0;
-  DevBuf<double *> ptrs;                     // scratch pointer table (mgkcyc_device)
   // kernel timing (mf3d_profile)
   int prof_kind = 0;
-  std::vector<cudaEvent_t> prof_ev;          // reusable event pool
-  std::vector<double> prof_pending_bytes;    // one entry per bracketed launch
+  std::vector<cudaEvent_t> prof_ev;
+  std::vector<double> prof_pending_bytes;
   double prof_ms = 0.0, prof_bytes = 0.0;
   long long prof_n = 0;
-  long long n_l1 = 0;                        // finest-level interior cells, all blocks
+  // host entry point mirrors
+  DevBuf<double> mirror;
+  std::vector<size_t> mirror_off;
+  DevBuf<double *> ptrs;
 };
 
 namespace mf3d {
-
-static inline int grid_of(long long n, int tpb) { return (int)((n + tpb - 1) / tpb); }
 
 // Kernel timing: bracket one launch of the profiled class with events.
 static void prof_begin(mf3d_ctx *C, int kind, double bytes) {
@@ -147,7 +413,6 @@ static void prof_end(mf3d_ctx *C, int kind) {
   if (C->prof_kind != kind || kind == 0 || C->prof_pending_bytes.empty()) return;
   cudaEventRecord(C->prof_ev[2 * (C->prof_pending_bytes.size() - 1) + 1], C->stream);
 }
-// After a stream synchronize: fold the bracketed launches into the totals.
 static void prof_collect(mf3d_ctx *C) {
   for (size_t q = 0; q < C->prof_pending_bytes.size(); ++q) {
     float ms = 0.f;
@@ -160,289 +425,285 @@ static void prof_collect(mf3d_ctx *C) {
   C->prof_pending_bytes.clear();
 }
 
-// ---------------------------------------------------------------------------
-// Level construction (replaces coeff, mgsolver.for:2-222, and the cof sizing
-// of localparameters.for:208-237).
-// ---------------------------------------------------------------------------
-template <typename T>
-static int build_level(mf3d_ctx *C, Level<T> &L, int g) {
-  L.g = g;
-  const int nb = C->nb;
-  const int ngrid = C->prm.ngrid;
-  std::vector<T> coef, geo;
-  long long phi_off = 0;
-  std::vector<long long> it_sweep, it_cells;
-  std::vector<LevelGeom> geom(nb);
-  std::vector<long long> base(nb);
-  long long cell_base = 0;
-  L.hb.resize(nb);
-  for (int b = 0; b < nb; ++b) {
-    const mf3d_block_desc &d = C->blocks[b];
-    BlkLev &B = L.hb[b];
-    B.nx = d.nx >> (g - 1);
-    B.ny = d.ny >> (g - 1);
-    B.nz = d.nz >> (g - 1);
-    B.hp = hp_of(B.nx);
-    B.cstr = (long long)(B.nz + 2) * (B.ny + 2) * B.hp;
-    B.cstr = (B.cstr + 31) / 32 * 32;  // 256-byte aligned colour arrays (FP64)
-    B.phi0 = phi_off;
-    B.rhs0 = phi_off;
-    phi_off += 2 * B.cstr;
-    B.pos = b;
-    B.nmask = 0;
-    const int nbr[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
-    const int bc[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
-    for (int f = 0; f < 6; ++f)
-      if (nbr[f] < 0 && bc[f] != MF3D_BC_PERIODIC) B.nmask |= 1 << f;
-    // coefficients: aw, ae (x), as, an (y), ab, at (z); Neumann faces zeroed
-    B.coef = (int)coef.size();
-    const double *ext[3] = {d.hx, d.hy, d.hz};
-    const double hh[3] = {d.dx, d.dy, d.dz};
-    const int nn[3] = {B.nx, B.ny, B.nz};
-    const int nfine[3] = {d.nx, d.ny, d.nz};
-    for (int a = 0; a < 3; ++a) {
-      std::vector<double> w = level_widths(ext[a], nfine[a], hh[a], ngrid, g);
-      const int n = nn[a];
-      const double hl = hh[a] * (double)(1 << (g - 1));
-      const double dd = hl * hl;
-      for (int side = 0; side < 2; ++side) {
-        for (int c = 0; c < n + 2; ++c) {
-          double v = 0.0;
-          if (c >= 1 && c <= n) {
-            if (!ext[a]) v = 1.0 / dd;  // mgsolver.for:184-189
-            else v = 1.0 / (w[c] * (0.5 * (w[c] + w[side ? c + 1 : c - 1])));
-            const int f = 2 * a + side;
-            if ((B.nmask >> f & 1) && c == (side ? n : 1)) v = 0.0;  // mgsolver.for:192-203
-          }
-          coef.push_back((T)v);
+// Build the launch tables of a view over `doms` (all of one precision).
+static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &doms, int hcap) {
+  cudaStream_t s = C->stream;
+  V.drop_graphs();
+  V.blk.clear(); V.blk_dom.clear(); V.dom = doms; V.Lmax = 0; V.n_l1 = 0;
+  std::vector<int> dom_base;
+  for (size_t d = 0; d < doms.size(); ++d) {
+    dom_base.push_back((int)V.blk.size());
+    for (auto &b : doms[d]->blocks) {
+      V.blk.push_back(b.get());
+      V.blk_dom.push_back((int)d);
+    }
+    V.Lmax = std::max(V.Lmax, doms[d]->ngrid);
+  }
+  const int nb = (int)V.blk.size(), nd = (int)doms.size();
+  V.lv.clear();
+  V.lv.resize(V.Lmax + 1);
+  int st;
+  size_t work_elems = 0;
+  for (int g = 1; g <= V.Lmax; ++g) {
+    ViewLevel &L = V.lv[g];
+    std::vector<BlkLev> tab(nb);
+    std::vector<Tile> sw[3], ce[3];
+    std::vector<int> li[3];
+    for (int b = 0; b < nb; ++b) {
+      const BlockStore &S = *V.blk[b];
+      BlkLev B;
+      std::memset(&B, 0, sizeof B);
+      if (g <= S.ngrid) B = S.lv[g].desc;
+      B.dom = V.blk_dom[b];
+      tab[b] = B;
+      if (g > S.ngrid) continue;
+      const int sub_extra = (g == S.ngrid) ? SUB_C : SUB_D;
+      const Box bsw{0, B.hp - 1, 1, B.ny, 1, B.nz};
+      const Box bce{0, B.nx + 1, 0, B.ny + 1, 0, B.nz + 1};
+      for (int q : {(int)SUB_A, sub_extra}) {
+        add_tiles_2d(sw[q], b, bsw, RB_TX, RB_RJ, RB_KCH);
+        add_tiles_2d(ce[q], b, bce, RW_TX, RW_RJ, RW_KCH);
+        li[q].push_back(b);
+        L.cells_sub[q] += (long long)B.nx * B.ny * B.nz;
+      }
+      L.ngg = std::max(L.ngg, std::max(B.nx, std::max(B.ny, B.nz)) + 2);
+    }
+    if ((st = L.tab.upload(tab, s))) return st;
+    for (int q = 0; q < 3; ++q) {
+      L.n_sweep[q] = (int)sw[q].size();
+      L.n_cells[q] = (int)ce[q].size();
+      L.n_list[q] = (int)li[q].size();
+      if ((st = L.sweep[q].upload(sw[q], s))) return st;
+      if ((st = L.cells[q].upload(ce[q], s))) return st;
+      if ((st = L.list[q].upload(li[q], s))) return st;
+      work_elems = std::max(work_elems, (size_t)L.n_list[q] * 128 * 2 * L.ngg);
+    }
+    // halo lists: staged pairs of every domain first, then the direct ones
+    for (int q = 0; q < 3; ++q) {
+      std::vector<HaloCopy> staged, direct;
+      for (int d = 0; d < nd; ++d) {
+        const DomainStore &D = *doms[d];
+        if (g > D.ngrid) continue;
+        const bool in = q == SUB_A || (q == SUB_C ? g == D.ngrid : g < D.ngrid);
+        if (!in) continue;
+        const auto &H = D.halo[g];
+        for (size_t p = 0; p < H.size(); ++p) {
+          HaloCopy c{dom_base[d] + H[p].dblk, H[p].doff, dom_base[d] + H[p].sblk, H[p].soff};
+          ((int)p < D.nstaged[g] ? staged : direct).push_back(c);
         }
       }
+      L.n_staged[q] = (int)staged.size();
+      staged.insert(staged.end(), direct.begin(), direct.end());
+      L.n_halo[q] = (int)staged.size();
+      if ((st = L.halo[q].upload(staged, s))) return st;
+      if ((st = L.stage[q].alloc((size_t)std::max(L.n_staged[q], 1) * C->elem))) return st;
     }
-    // restriction ratios hf/Hc of this (fine) level, exactly 0.5 on uniform axes
-    B.geo = (int)geo.size();
-    for (int a = 0; a < 3; ++a) {
-      const int n = nn[a];
-      if (g < ngrid) {
-        std::vector<double> wf = level_widths(ext[a], nfine[a], hh[a], ngrid, g);
-        std::vector<double> wc = level_widths(ext[a], nfine[a], hh[a], ngrid, g + 1);
-        for (int c = 0; c < n + 2; ++c) geo.push_back((T)((c >= 1 && c <= n) ? wf[c] / wc[(c + 1) >> 1] : 0.0));
-      } else {
-        for (int c = 0; c < n + 2; ++c) geo.push_back((T)0);
-      }
-    }
-    it_sweep.push_back((long long)B.nz * B.ny * B.hp);
-    it_cells.push_back((long long)(B.nx + 2) * (B.ny + 2) * (B.nz + 2));
-    geom[b] = LevelGeom{B.nx, B.ny, B.nz};
-    base[b] = cell_base;
-    cell_base += geom[b].cells();
-    L.ngg = std::max(L.ngg, std::max(B.nx, std::max(B.ny, B.nz)) + 2);
   }
-  cudaStream_t s = C->stream;
-  int st;
-  if ((st = L.phi.alloc(phi_off))) return st;
-  if ((st = L.rhs.alloc(phi_off))) return st;
-  CK(cudaMemsetAsync(L.phi.p, 0, phi_off * sizeof(T), s));
-  CK(cudaMemsetAsync(L.rhs.p, 0, phi_off * sizeof(T), s));
-  if ((st = L.coef.upload(coef, s))) return st;
-  if ((st = L.geo.upload(geo, s))) return st;
-  if ((st = L.db.upload(L.hb, s))) return st;
-  auto ts = make_tiles(it_sweep), tc = make_tiles(it_cells);
-  L.n_sweep = (int)ts.size();
-  L.n_cells = (int)tc.size();
-  if ((st = L.t_sweep.upload(ts, s))) return st;
-  if ((st = L.t_cells.upload(tc, s))) return st;
-  // halo copy map -> element addresses in the colour-split pool
-  std::vector<HaloPair> pairs = build_halo_map(C->blocks, geom, base);
-  std::unordered_set<long long> dsts;
-  for (auto &pr : pairs) dsts.insert(pr.dst);
-  auto addr = [&](long long id) -> long long {
-    int b = (int)(std::upper_bound(base.begin(), base.end(), id) - base.begin()) - 1;
-    long long lin = id - base[b];
-    const LevelGeom &G = geom[b];
-    int i = (int)(lin % (G.nx + 2));
-    long long r = lin / (G.nx + 2);
-    int j = (int)(r % (G.ny + 2));
-    int k = (int)(r / (G.ny + 2));
-    const BlkLev &B = L.hb[b];
-    int c = (i + j + k + 1) & 1;
-    return B.phi0 + c * B.cstr + ((long long)k * (B.ny + 2) + j) * B.hp + (i >> 1);
-  };
-  std::vector<long long> hd, hs;
-  for (int pass = 0; pass < 2; ++pass)
-    for (auto &pr : pairs) {
-      bool staged = dsts.count(pr.src) > 0;
-      if ((pass == 0) != staged) continue;
-      hd.push_back(addr(pr.dst));
-      hs.push_back(addr(pr.src));
+  if (C->prm.mg_itrsch == 2 && (st = V.work.alloc(std::max<size_t>(work_elems, 1) * C->elem))) return st;
+  // level-1 field tables
+  V.hf.resize(nb);
+  std::vector<Tile> t1, t2, t5;
+  std::vector<long long> it_faces, it_planes;
+  for (int b = 0; b < nb; ++b) {
+    const BlockStore &S = *V.blk[b];
+    BlkFld F = S.fld;
+    const int d = V.blk_dom[b];
+    F.dom = d;
+    F.L1 = S.lv[1].desc;
+    F.L1.dom = d;
+    for (int f = 0; f < 6; ++f) {
+      const FaceRule &r = doms[d]->rules[6 * (b - dom_base[d]) + f];
+      F.wall[f] = r.kind == FACE_WALL;
+      F.src[f] = r.kind == FACE_WALL ? b : dom_base[d] + r.src;
     }
-  L.nstaged = 0;
-  for (auto &pr : pairs) L.nstaged += dsts.count(pr.src) > 0;
-  L.nhalo = (int)hd.size();
-  if ((st = L.hdst.upload(hd, s))) return st;
-  if ((st = L.hsrc.upload(hs, s))) return st;
-  if ((st = L.hbuf.alloc(std::max(L.nstaged, 1)))) return st;
-  if (C->prm.mg_itrsch == 2) {
-    if ((st = L.tdma_work.alloc((size_t)nb * 128 * 2 * L.ngg))) return st;
+    V.hf[b] = F;
+    const mf3d_block_desc &x = S.d;
+    add_tiles_2d(t1, b, Box{1, x.nx, 1, x.ny, 1, x.nz}, RW_TX, RW_RJ, RW_KCH);
+    add_tiles_2d(t2, b, Box{0, x.nx + 1, 0, x.ny + 1, 0, x.nz + 1}, RW_TX, RW_RJ, RW_KCH);
+    add_tiles_2d(t5, b, Box{1, x.nx, 1, x.ny, 1, x.nz}, OZ_TX, OZ_RJ, OZ_KCH);
+    it_faces.push_back(2 * ((long long)x.ny * x.nz + (long long)x.nx * x.nz + (long long)x.nx * x.ny));
+    it_planes.push_back((long long)x.ny * x.nz + (long long)x.nx * x.nz + (long long)x.nx * x.ny);
+    V.n_l1 += (long long)x.nx * x.ny * x.nz;
   }
+  auto t3 = make_tiles(it_faces), t4 = make_tiles(it_planes);
+  V.n_int = (int)t1.size(); V.n_l1cells = (int)t2.size(); V.n_faces = (int)t3.size();
+  V.n_planes = (int)t4.size(); V.n_zint = (int)t5.size();
+  if ((st = V.df.upload(V.hf, s))) return st;
+  if ((st = V.t_int.upload(t1, s))) return st;
+  if ((st = V.t_zint.upload(t5, s))) return st;
+  if ((st = V.t_l1cells.upload(t2, s))) return st;
+  if ((st = V.t_faces.upload(t3, s))) return st;
+  if ((st = V.t_planes.upload(t4, s))) return st;
+  // per-domain solve state
+  std::vector<int> ones(std::max(nd, 1), 1);
+  if ((st = V.ds.alloc(std::max(nd, 1)))) return st;
+  if ((st = V.act.upload(ones, s))) return st;
+  if ((st = V.ones.upload(ones, s))) return st;
+  if ((st = V.rmax.alloc(std::max(nd, 1)))) return st;
+  if ((st = V.rmax_scratch.alloc(std::max(nd, 1)))) return st;
+  CK(cudaMemsetAsync(V.rmax.p, 0, V.rmax.n * sizeof(unsigned long long), s));
+  V.hcap = std::max(hcap, 1);
+  if ((st = V.hist.alloc((size_t)std::max(nd, 1) * V.hcap))) return st;
+  CK(cudaStreamSynchronize(s));
   return MF3D_OK;
 }
 
 // ---------------------------------------------------------------------------
-// V-cycle building blocks.
+// V-cycle over a view.
 // ---------------------------------------------------------------------------
 template <typename T>
-static void halo(mf3d_ctx *C, Level<T> &L) {
-  if (L.nhalo == 0) return;
-  if (L.nstaged) {
-    k_halo_stage<T><<<grid_of(L.nstaged, 256), 256, 0, C->stream>>>(L.hsrc.p, L.nstaged, L.phi.p, L.hbuf.p);
+static void halo(mf3d_ctx *C, View &V, int g, int q) {
+  ViewLevel &L = V.lv[g];
+  if (!L.n_halo[q]) return;
+  T *buf = (T *)L.stage[q].p;
+  if (L.n_staged[q]) {
+    k_halo_stage<T><<<grid_of(L.n_staged[q], 256), 256, 0, C->stream>>>(L.tab.p, L.halo[q].p, L.n_staged[q],
+                                                                       V.act.p, buf);
     ++C->launches;
   }
-  k_halo_apply<T><<<grid_of(L.nhalo, 256), 256, 0, C->stream>>>(L.hdst.p, L.hsrc.p, L.nhalo, L.nstaged, L.phi.p,
-                                                                L.hbuf.p);
+  k_halo_apply<T><<<grid_of(L.n_halo[q], 256), 256, 0, C->stream>>>(L.tab.p, L.halo[q].p, L.n_halo[q],
+                                                                   L.n_staged[q], V.act.p, buf);
   ++C->launches;
 }
 
-// mgrelax(g, it) (mgsolver.for:371-617): `it` sweeps, each followed by
-// mgbound + exchangepp (+ exchbc_mgpp), here one halo-map application.
+// mgrelax(g, it) (mgsolver.for:371-617) on subset q: `it` sweeps, each
+// followed by the halo refresh (mgbound + exchangepp + exchbc_mgpp).
 template <typename T>
-static void relax(mf3d_ctx *C, Level<T> &L, int it) {
+static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
+  ViewLevel &L = V.lv[g];
+  if (!L.n_list[q]) return;
   const int sch = C->prm.mg_itrsch;
   for (int itr = 0; itr < it; ++itr) {
     if (sch == 3) {
-      const int pk = L.g == 1 ? MF3D_PROF_SMOOTH_L1 : 0;
-      const double half = 0.5 * (double)C->n_l1 * sizeof(T);  // one colour of the finest level
-      if (L.zero_interior) {
-        prof_begin(C, pk, 2 * half);  // rhs in, colour out
-        k_rbgs<T, true><<<L.n_sweep, kTile, 0, C->stream>>>(L.db.p, L.t_sweep.p, L.phi.p, L.rhs.p, L.coef.p, 0);
-      } else {
-        prof_begin(C, pk, 3 * half);  // other colour + rhs in, colour out
-        k_rbgs<T, false><<<L.n_sweep, kTile, 0, C->stream>>>(L.db.p, L.t_sweep.p, L.phi.p, L.rhs.p, L.coef.p, 0);
-      }
+      const int pk = (g == 1 && q == SUB_A) ? MF3D_PROF_SMOOTH_L1 : 0;
+      const double half = 0.5 * (double)L.cells_sub[q] * sizeof(T);
+      const bool fz = from_zero && itr == 0;
+      prof_begin(C, pk, (fz ? 2 : 3) * half);
+      if (fz)
+        k_rbgs<T, true><<<L.n_sweep[q], dim3(RB_TX, RB_RJ), 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0);
+      else
+        k_rbgs<T, false><<<L.n_sweep[q], dim3(RB_TX, RB_RJ), 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0);
       prof_end(C, pk);
       prof_begin(C, pk, 3 * half);
-      k_rbgs<T, false><<<L.n_sweep, kTile, 0, C->stream>>>(L.db.p, L.t_sweep.p, L.phi.p, L.rhs.p, L.coef.p, 1);
+      k_rbgs<T, false><<<L.n_sweep[q], dim3(RB_TX, RB_RJ), 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 1);
       prof_end(C, pk);
       C->launches += 2;
     } else if (sch == 1) {
-      k_lexgs<T><<<C->nb, 1024, 0, C->stream>>>(L.db.p, L.phi.p, L.rhs.p, L.coef.p);
+      k_lexgs<T><<<L.n_list[q], 1024, 0, C->stream>>>(L.tab.p, L.list[q].p, V.act.p);
       ++C->launches;
     } else {
-      k_tdma<T><<<C->nb, 128, 0, C->stream>>>(L.db.p, L.phi.p, L.rhs.p, L.coef.p, L.tdma_work.p, L.ngg);
+      k_tdma<T><<<L.n_list[q], 128, 0, C->stream>>>(L.tab.p, L.list[q].p, V.act.p, (T *)V.work.p, L.ngg);
       ++C->launches;
     }
-    L.zero_interior = false;
-    halo(C, L);
-  }
-}
-
-// A level whose interior must read as zero but whose first use is not a
-// red-black sweep gets real zeros.
-template <typename T>
-static void materialize_zero(mf3d_ctx *C, Level<T> &L) {
-  if (L.zero_interior) {
-    cudaMemsetAsync(L.phi.p, 0, L.phi.n * sizeof(T), C->stream);
-    L.zero_interior = false;
+    halo<T>(C, V, g, q);
   }
 }
 
 template <typename T>
-static void restr(mf3d_ctx *C, Level<T> &F, Level<T> &Cl) {
-  materialize_zero(C, F);
-  const int pk = F.g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
-  prof_begin(C, pk, (double)C->n_l1 * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse phi, rhs out
-  k_restrict<T, T><<<Cl.n_cells, kTile, 0, C->stream>>>(F.db.p, Cl.db.p, Cl.t_cells.p, F.phi.p, F.rhs.p, F.coef.p,
-                                                       Cl.phi.p, Cl.rhs.p, F.geo.p);
-  prof_end(C, pk);
-  ++C->launches;
-  Cl.zero_interior = (C->prm.mg_itrsch == 3);  // k_restrict wrote real zeros too
-  if (C->prm.mg_itrsch != 3) Cl.zero_interior = false;
-}
-
-template <typename T>
-static void corr(mf3d_ctx *C, Level<T> &F, Level<T> &Cl) {
-  materialize_zero(C, F);
-  materialize_zero(C, Cl);
-  const int pk = F.g == 1 ? MF3D_PROF_PROLONG_L1 : 0;
-  prof_begin(C, pk, (double)C->n_l1 * sizeof(T) * (2.0 + 1.0 / 8.0));  // fine phi in/out, coarse phi in
-  k_prolong<T, T><<<F.n_cells, kTile, 0, C->stream>>>(F.db.p, Cl.db.p, F.t_cells.p, F.phi.p, Cl.phi.p);
+static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks continuing down
+  ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
+  if (!Cl.n_cells[SUB_A]) return;
+  const int pk = g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
+  prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse out
+  k_restrict<T, T><<<Cl.n_cells[SUB_A], dim3(RW_TX, RW_RJ), 0, C->stream>>>(F.tab.p, Cl.tab.p, Cl.cells[SUB_A].p,
+                                                                           V.act.p);
   prof_end(C, pk);
   ++C->launches;
 }
 
-// mgkcyc (mgsolver.for:224-369) with kcycle = 1: a V-cycle, irestr
-// pre-sweeps and iproln post-sweeps, irestr + iproln sweeps on the coarsest
-// level.  The level-1 rhs must hold su; level-1 phi starts at zero.
 template <typename T>
-static void vcycle(mf3d_ctx *C, std::vector<std::unique_ptr<Level<T>>> &Lv) {
-  const int ngrd = C->prm.ngrid;
-  Level<T> &L1 = *Lv[1];
-  // pp = 0 including ghosts (newsolv_mg.for:19-21, 44)
-  if (C->prm.mg_itrsch == 3) {
-    k_zero_ghosts<T><<<L1.n_cells, kTile, 0, C->stream>>>(L1.db.p, L1.t_cells.p, L1.phi.p);
-    ++C->launches;
-    L1.zero_interior = true;
-  } else {
-    cudaMemsetAsync(L1.phi.p, 0, L1.phi.n * sizeof(T), C->stream);
-    L1.zero_interior = false;
-  }
-  int glevel = 1, nrel;
-  const int kcycle = 1;
-  std::vector<int> kount(ngrd + 1, 0);
-  relax(C, *Lv[1], C->prm.irestr);
-  if (ngrd != 1) {
-    restr(C, *Lv[1], *Lv[2]);
-    glevel = 2;
-    nrel = C->prm.irestr;
-    for (;;) {
-      if (glevel == 1) break;
-      kount[glevel] += 1;
-      relax(C, *Lv[glevel], nrel);
-      if (kount[glevel] == kcycle + 1) {
-        corr(C, *Lv[glevel - 1], *Lv[glevel]);
-        kount[glevel] = 0;
-        glevel -= 1;
-        nrel = C->prm.iproln;
-      } else if (glevel < ngrd) {
-        restr(C, *Lv[glevel], *Lv[glevel + 1]);
-        glevel += 1;
-        nrel = C->prm.irestr;
-      } else {
-        relax(C, *Lv[glevel], C->prm.iproln);
-        corr(C, *Lv[glevel - 1], *Lv[glevel]);
-        nrel = C->prm.iproln;
-        glevel = ngrd - 1;
-      }
+static void corr(mf3d_ctx *C, View &V, int g) {  // level g+1 -> g, blocks continuing down
+  ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
+  if (!F.n_cells[SUB_D]) return;
+  const int pk = g == 1 ? MF3D_PROF_PROLONG_L1 : 0;
+  prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 1.0 / 8.0));  // fine in/out, coarse in
+  k_prolong<T, T><<<F.n_cells[SUB_D], dim3(RW_TX, RW_RJ), 0, C->stream>>>(F.tab.p, Cl.tab.p, F.cells[SUB_D].p,
+                                                                         V.act.p);
+  prof_end(C, pk);
+  ++C->launches;
+}
+
+// mgkcyc (mgsolver.for:224-369, kcycle = 1) for every domain of the view,
+// each with its own depth: down the levels with irestr sweeps, irestr +
+// iproln sweeps where a domain bottoms out, back up with iproln sweeps.
+// Every domain sees exactly the operation sequence of its own V-cycle.
+// On entry the level-1 rhs holds su and the level-1 ghost shell holds zeros.
+template <typename T>
+static void vcycle(mf3d_ctx *C, View &V) {
+  const int sch = C->prm.mg_itrsch, ir = C->prm.irestr, ip = C->prm.iproln;
+  // pp = 0 (newsolv_mg.for:19-21, :44): the red-black path never reads the
+  // level-1 interior before overwriting it; the other smoothers, or no
+  // pre-smoothing, need real zeros.
+  const bool need_zero = sch != 3 || ir == 0;
+  if (need_zero)
+    for (size_t b = 0; b < V.blk.size(); ++b) {
+      const BlkLev &B = V.blk[b]->lv[1].desc;
+      cudaMemsetAsync(B.phi, 0, (size_t)2 * B.cstr * sizeof(T), C->stream);
     }
+  for (int g = 1; g <= V.Lmax; ++g) {
+    relax<T>(C, V, g, SUB_A, ir, sch == 3);  // a level starts from zero (pp = 0; mgrestr)
+    relax<T>(C, V, g, SUB_C, ip, sch == 3 && ir == 0);
+    if (g < V.Lmax) restr<T>(C, V, g);
   }
-  relax(C, *Lv[1], C->prm.iproln);
-  materialize_zero(C, L1);
+  for (int g = V.Lmax - 1; g >= 1; --g) {
+    corr<T>(C, V, g);
+    relax<T>(C, V, g, SUB_D, ip, false);
+  }
+}
+
+// One outer iteration of newsolv_mg (newsolv_mg.for:25-58) for every active
+// domain: V-cycle, p += pp, p halo + pbound, calvel + calmas, bookkeeping.
+template <typename T>
+static void iteration_body(mf3d_ctx *C, View &V, bool loop_graph) {
+  cudaStream_t s = C->stream;
+  vcycle<T>(C, V);
+  k_add_correction<T><<<V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_l1cells.p, V.act.p);
+  k_p_faces<<<V.n_faces, kTile, 0, s>>>(V.df.p, V.t_faces.p, V.act.p);
+  prof_begin(C, MF3D_PROF_CALMAS, (double)V.n_l1 * (4 * sizeof(double) + sizeof(T)));  // p, u*, v*, w* in; su out
+  k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, s>>>(V.df.p, V.t_zint.p, V.ds.p, V.act.p, V.rmax.p, 0);
+  prof_end(C, MF3D_PROF_CALMAS);
+  k_iter_end<<<1, 256, 0, s>>>(V.ds.p, (int)V.dom.size(), V.rmax.p, V.hist.p, V.hcap, V.act.p, V.cond,
+                               loop_graph ? 1 : 0);
+  C->launches += 4;
 }
 
 template <typename T>
-static T *level1_phi(mf3d_ctx *C);
-template <>
-double *level1_phi<double>(mf3d_ctx *C) { return C->L64[1]->phi.p; }
-template <>
-float *level1_phi<float>(mf3d_ctx *C) { return C->L32[1]->phi.p; }
-template <typename T>
-static T *level1_rhs(mf3d_ctx *C);
-template <>
-double *level1_rhs<double>(mf3d_ctx *C) { return C->L64[1]->rhs.p; }
-template <>
-float *level1_rhs<float>(mf3d_ctx *C) { return C->L32[1]->rhs.p; }
-template <typename T>
-static std::vector<std::unique_ptr<Level<T>>> &levels(mf3d_ctx *C);
-template <>
-std::vector<std::unique_ptr<Level<double>>> &levels<double>(mf3d_ctx *C) { return C->L64; }
-template <>
-std::vector<std::unique_ptr<Level<float>>> &levels<float>(mf3d_ctx *C) { return C->L32; }
+static int build_graphs(mf3d_ctx *C, View &V) {
+  if (V.x_loop && V.x_once) return MF3D_OK;
+  const int saved_prof = C->prof_kind;
+  const long long saved_launches = C->launches;
+  C->prof_kind = 0;  // no event records inside graphs
+  // the whole outer loop: a conditional WHILE node around one iteration
+  CK(cudaGraphCreate(&V.g_loop, 0));
+  CK(cudaGraphConditionalHandleCreate(&V.cond, V.g_loop, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+  np.conditional.handle = V.cond;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, V.g_loop, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(C->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  C->launches = 0;
+  iteration_body<T>(C, V, true);
+  V.launches_per_iter = C->launches;
+  cudaGraph_t captured;
+  CK(cudaStreamEndCapture(C->stream, &captured));
+  CK(cudaGraphInstantiate(&V.x_loop, V.g_loop, 0));
+  // one iteration (the server's per-cycle step)
+  CK(cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeRelaxed));
+  iteration_body<T>(C, V, false);
+  CK(cudaStreamEndCapture(C->stream, &V.g_once));
+  CK(cudaGraphInstantiate(&V.x_once, V.g_once, 0));
+  C->launches = saved_launches;
+  C->prof_kind = saved_prof;
+  return MF3D_OK;
+}
 
-// ---------------------------------------------------------------------------
-// Fields: bind per-block pointers and upload the BlkFld table.
-// ---------------------------------------------------------------------------
-static int bind_fields(mf3d_ctx *C, const mf3d_fields *f) {
-  for (int b = 0; b < C->nb; ++b) {
-    BlkFld &F = C->hf[b];
+// Bind the caller's field pointers (ttc layout, device) to the view blocks.
+static int bind_fields(mf3d_ctx *C, View &V, const mf3d_fields *f) {
+  for (size_t b = 0; b < V.blk.size(); ++b) {
+    BlkFld &F = V.hf[b];
     F.ustar = f[b].ustar; F.vstar = f[b].vstar; F.wstar = f[b].wstar;
     F.u = f[b].u; F.v = f[b].v; F.w = f[b].w; F.p = f[b].p; F.su = f[b].su;
     if (!F.ustar || !F.vstar || !F.wstar || !F.u || !F.v || !F.w || !F.p) {
@@ -450,154 +711,189 @@ static int bind_fields(mf3d_ctx *C, const mf3d_fields *f) {
       return MF3D_E_INVALID;
     }
   }
-  CK(cudaMemcpyAsync(C->df.p, C->hf.data(), C->hf.size() * sizeof(BlkFld), cudaMemcpyHostToDevice, C->stream));
+  CK(cudaMemcpyAsync(V.df.p, V.hf.data(), V.hf.size() * sizeof(BlkFld), cudaMemcpyHostToDevice, C->stream));
   return MF3D_OK;
 }
 
-// One outer iteration of newsolv_mg (newsolv_mg.for:25-58): V-cycle,
-// p += pp, p halo + pbound, calvel + calmas, iteration bookkeeping.
+// Start the solve of every domain of the view: state, face planes, the
+// initial calvel/calmas (newsolv_mg.for:16-17; p's ghosts used as given),
+// rmax0 and the thresholds.  Everything stays on the device.
 template <typename T>
-static void iteration_body(mf3d_ctx *C, bool in_graph) {
+static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alfapr) {
   cudaStream_t s = C->stream;
-  vcycle<T>(C, levels<T>(C));
-  k_add_correction<T><<<C->n_l1cells, kTile, 0, s>>>(C->df.p, C->t_l1cells.p, level1_phi<T>(C));
-  k_p_faces<<<C->n_faces, kTile, 0, s>>>(C->df.p, C->t_faces.p);
-  prof_begin(C, MF3D_PROF_CALMAS, (double)C->n_l1 * (4 * sizeof(double) + sizeof(T)));  // p, u*, v*, w* in; su out
-  k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->st.p, level1_rhs<T>(C), C->rmax_cur.p, 0);
-  prof_end(C, MF3D_PROF_CALMAS);
-  k_iter_end<<<1, 1, 0, s>>>(C->st.p, C->rmax_cur.p, C->hist_d.p, C->cond, in_graph ? 1 : 0);
-  C->launches += 4;
-}
-
-// The whole outer loop as one graph: a conditional WHILE node whose body is
-// one iteration; k_iter_end clears the condition when the loop must stop.
-template <typename T>
-static int build_solve_graph(mf3d_ctx *C) {
-  if (C->graph_exec) return MF3D_OK;
-  cudaGraph_t g;
-  CK(cudaGraphCreate(&g, 0));
-  C->graph = g;
-  CK(cudaGraphConditionalHandleCreate(&C->cond, g, 1u, cudaGraphCondAssignDefault));
-  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
-  np.conditional.handle = C->cond;
-  np.conditional.type = cudaGraphCondTypeWhile;
-  np.conditional.size = 1;
-  cudaGraphNode_t node;
-  CK(cudaGraphAddNode(&node, g, nullptr, 0, &np));
-  cudaGraph_t body = np.conditional.phGraph_out[0];
-  CK(cudaStreamBeginCaptureToGraph(C->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-  const long long before = C->launches;
-  const int saved_prof = C->prof_kind;
-  C->prof_kind = 0;  // no event records inside the graph
-  iteration_body<T>(C, true);
-  C->prof_kind = saved_prof;
-  C->launches_per_iter = C->launches - before;
-  cudaGraph_t captured;
-  CK(cudaStreamEndCapture(C->stream, &captured));
-  CK(cudaGraphInstantiate(&C->graph_exec, g, 0));
+  const int nd = (int)V.dom.size();
+  std::vector<DomState> hs(nd);
+  for (int d = 0; d < nd; ++d) {
+    std::memset(&hs[d], 0, sizeof(DomState));
+    hs[d].dt = dt[d];
+    hs[d].dtinv = pow2_inverse(dt[d]);
+    hs[d].alfapr = alfapr[d];
+    hs[d].tol = C->prm.eps;
+    hs[d].eps_relative = C->prm.eps_relative;
+    hs[d].maxcy = std::min(std::max(C->prm.maxcy, 0), V.hcap);
+  }
+  CK(cudaMemcpyAsync(V.ds.p, hs.data(), nd * sizeof(DomState), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));  // hs is a local
+  CK(cudaMemsetAsync(V.rmax.p, 0, nd * sizeof(unsigned long long), s));
+  k_face_planes<<<V.n_planes, kTile, 0, s>>>(V.df.p, V.t_planes.p);
+  k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, s>>>(V.df.p, V.t_zint.p, V.ds.p, V.ones.p, V.rmax.p, 0);
+  k_dom_init<<<1, 256, 0, s>>>(V.ds.p, nd, V.rmax.p, V.act.p);
+  C->launches += 3;
   return MF3D_OK;
 }
 
+// Finish: optional su, the final calvel (u, v, w from the final p).
 template <typename T>
-static int solve_device(mf3d_ctx *C, double dt, double alfapr, mf3d_solve_info *info, double *hist, int cap) {
+static int solve_end(mf3d_ctx *C, View &V) {
+  cudaStream_t s = C->stream;
+  bool want_su = false;
+  for (auto &F : V.hf) want_su |= F.su != nullptr;
+  if (want_su) {
+    k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, s>>>(V.df.p, V.t_zint.p, V.ds.p, V.ones.p,
+                                                               V.rmax_scratch.p, 1);
+    ++C->launches;
+  }
+  k_calvel<<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, V.ds.p);
+  ++C->launches;
+  return MF3D_OK;
+}
+
+// Fold the device state of every domain into the caller's infos/history.
+static int collect(mf3d_ctx *C, View &V, mf3d_solve_info *infos, double *hist, int hcap, float ms) {
+  const int nd = (int)V.dom.size();
+  std::vector<DomState> hs(nd);
+  CK(cudaMemcpy(hs.data(), V.ds.p, nd * sizeof(DomState), cudaMemcpyDeviceToHost));
+  int worst = MF3D_OK;
+  for (int d = 0; d < nd; ++d) {
+    const DomState &D = hs[d];
+    int status = MF3D_OK;
+    if (D.done == 2) status = MF3D_E_NONFINITE;
+    else if (D.done != 1) status = MF3D_NOT_CONVERGED;
+    const double rmax = D.iter > 0 ? D.rmax : D.rmax0;
+    if (status >= 0 && rmax > 100.0) status = MF3D_DIVERGED;  // newsolv_mg.for:64
+    if (infos) {
+      infos[d].rmax = rmax; infos[d].rmax0 = D.rmax0; infos[d].iter = D.iter;
+      infos[d].status = status; infos[d].ms_device = ms;
+    }
+    if (hist && hcap > 0 && D.iter > 0)
+      CK(cudaMemcpy(hist + (size_t)d * hcap, V.hist.p + (size_t)d * V.hcap, std::min(D.iter, hcap) * sizeof(double),
+                    cudaMemcpyDeviceToHost));
+    if (status < 0) worst = worst < 0 ? worst : status;
+    else if (worst >= 0) worst = std::max(worst, status);
+  }
+  if (worst == MF3D_E_NONFINITE) set_error("non-finite rmax");
+  return worst;
+}
+
+template <typename T>
+static int solve_view(mf3d_ctx *C, View &V, const double *dt, const double *alfapr, mf3d_solve_info *infos,
+                      double *hist, int hcap) {
   cudaStream_t s = C->stream;
   C->launches = 0;
-  const int maxcy = std::max(C->prm.maxcy, 0);
-  SolveState hs;
-  std::memset(&hs, 0, sizeof hs);
-  hs.dt = dt; hs.alfapr = alfapr; hs.eps = 0.0; hs.maxcy = maxcy;
-  CK(cudaMemcpyAsync(C->st.p, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(C->rmax_cur.p, 0, sizeof(unsigned long long), s));
+  const int nd = (int)V.dom.size();
   CK(cudaEventRecord(C->ev0, s));
-  k_face_planes<<<C->n_planes, kTile, 0, s>>>(C->df.p, C->t_planes.p);
-  // calvel; calmas (newsolv_mg.for:16-17): p's ghosts are used as given
-  k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->st.p, level1_rhs<T>(C), C->rmax_cur.p, 0);
-  C->launches += 2;
-  CK(cudaMemcpyAsync(C->rmax_host, C->rmax_cur.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-  CK(cudaMemsetAsync(C->rmax_cur.p, 0, sizeof(unsigned long long), s));
-  CK(cudaStreamSynchronize(s));
-  double rmax0;
-  std::memcpy(&rmax0, C->rmax_host, sizeof(double));
-  hs.eps = C->prm.eps_relative ? C->prm.eps * rmax0 : C->prm.eps;
-  CK(cudaMemcpyAsync(&C->st.p->eps, &hs.eps, sizeof(double), cudaMemcpyHostToDevice, s));
-  const bool nonfinite0 = !std::isfinite(rmax0);
-  if (maxcy > 0 && !nonfinite0) {
+  int st = solve_begin<T>(C, V, dt, alfapr);
+  if (st) return st;
+  const int maxcy = std::min(std::max(C->prm.maxcy, 0), V.hcap);
+  long long iters_run = 0;
+  if (maxcy > 0) {
     if (C->use_graph && C->prof_kind == 0) {
-      int st = build_solve_graph<T>(C);
-      if (st) return st;
-      CK(cudaGraphLaunch(C->graph_exec, s));
+      if ((st = build_graphs<T>(C, V))) return st;
+      CK(cudaGraphLaunch(V.x_loop, s));
     } else {
+      std::vector<int> act(nd);
       for (int it = 1; it <= maxcy; ++it) {
-        iteration_body<T>(C, false);
-        CK(cudaMemcpyAsync(&hs, C->st.p, sizeof hs, cudaMemcpyDeviceToHost, s));
+        iteration_body<T>(C, V, false);
+        CK(cudaMemcpyAsync(act.data(), V.act.p, nd * sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         prof_collect(C);
-        if (hs.done) break;
+        bool any = false;
+        for (int a : act) any |= a != 0;
+        if (!any) break;
       }
     }
   }
-  // final su (optional) and u, v, w (calvel with the final p)
-  bool want_su = false;
-  for (auto &F : C->hf) want_su |= F.su != nullptr;
-  if (want_su) {
-    k_calvel_calmas<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->st.p, level1_rhs<T>(C), C->rmax_scratch.p, 1);
-    ++C->launches;
-  }
-  k_calvel<<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->st.p);
-  ++C->launches;
+  if ((st = solve_end<T>(C, V))) return st;
   CK(cudaEventRecord(C->ev1, s));
-  CK(cudaMemcpyAsync(&hs, C->st.p, sizeof hs, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
   prof_collect(C);
-  const int iters = hs.iter;
-  if (C->use_graph && C->prof_kind == 0) C->launches += (long long)iters * C->launches_per_iter;
-  if (hist && iters > 0) {
-    CK(cudaMemcpy(hist, C->hist_d.p, std::min(iters, cap) * sizeof(double), cudaMemcpyDeviceToHost));
-  }
   float ms = 0.f;
   cudaEventElapsedTime(&ms, C->ev0, C->ev1);
-  const double rmax = iters > 0 ? hs.rmax : rmax0;
-  int status = MF3D_OK;
-  if (nonfinite0 || hs.done == 2) status = MF3D_E_NONFINITE;
-  else if (hs.done != 1) status = MF3D_NOT_CONVERGED;
-  if (status >= 0 && rmax > 100.0) status = MF3D_DIVERGED;  // newsolv_mg.for:64
-  if (info) {
-    info->rmax = rmax; info->rmax0 = rmax0; info->iter = iters; info->status = status; info->ms_device = ms;
+  const int res = collect(C, V, infos, hist, hcap, ms);
+  if (C->use_graph && C->prof_kind == 0 && maxcy > 0) {
+    // every domain's iterations ran inside the graph: count the body launches
+    std::vector<DomState> hs(nd);
+    if (cudaMemcpy(hs.data(), V.ds.p, nd * sizeof(DomState), cudaMemcpyDeviceToHost) == cudaSuccess)
+      for (auto &D : hs) iters_run = std::max<long long>(iters_run, D.iter);
+    C->launches += std::max(iters_run, 1LL) * V.launches_per_iter;
   }
-  if (status == MF3D_E_NONFINITE) set_error("non-finite rmax");
-  return status;
+  return res;
 }
 
 template <typename T>
-static int mgkcyc_device(mf3d_ctx *C, double *const *su, double *const *pp) {
+static int mgkcyc_view(mf3d_ctx *C, View &V, double *const *su, double *const *pp) {
   cudaStream_t s = C->stream;
+  const int nb = (int)V.blk.size();
   C->launches = 0;
-  CK(cudaMemcpyAsync(C->ptrs.p, su, C->nb * sizeof(double *), cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(C->ptrs.p + C->nb, pp, C->nb * sizeof(double *), cudaMemcpyHostToDevice, s));
-  k_load_rhs<T><<<C->n_int, kTile, 0, s>>>(C->df.p, C->t_int.p, C->ptrs.p, level1_rhs<T>(C));
-  vcycle<T>(C, levels<T>(C));
-  k_store_pp<T><<<C->n_l1cells, kTile, 0, s>>>(C->df.p, C->t_l1cells.p, C->ptrs.p + C->nb, level1_phi<T>(C));
-  C->launches += 2;
+  if (C->ptrs.n < (size_t)2 * nb && C->ptrs.alloc(2 * nb)) return MF3D_E_OOM;
+  CK(cudaMemcpyAsync(C->ptrs.p, su, nb * sizeof(double *), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(C->ptrs.p + nb, pp, nb * sizeof(double *), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(V.df.p, V.hf.data(), nb * sizeof(BlkFld), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(V.act.p, V.ones.p, V.ones.n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  k_load_rhs<T><<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, C->ptrs.p);
+  vcycle<T>(C, V);
+  k_store_pp<T><<<V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_l1cells.p, C->ptrs.p + nb);
+  // restore the invariant: the level-1 ghost shell holds zeros between calls
+  ViewLevel &L1 = V.lv[1];
+  k_zero_ghosts<T><<<dim3(64, L1.n_list[SUB_A]), kTile, 0, s>>>(L1.tab.p, L1.list[SUB_A].p, L1.n_list[SUB_A]);
+  C->launches += 3;
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
   return MF3D_OK;
 }
 
-static size_t ttc_elems(const mf3d_ctx *C, int b) {
-  const auto &d = C->blocks[b];
-  const int pl = C->prm.pl;
+static size_t ttc_elems(int pl, const mf3d_block_desc &d) {
   return (size_t)(d.nx + 2 * pl) * (d.ny + 2 * pl) * (d.nz + 2 * pl);
 }
 
-static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, mf3d_ctx **out) {
-  if (!blocks || nb <= 0 || !prm || !out) { set_error("mf3d_create: bad arguments"); return MF3D_E_INVALID; }
+static int check_params(const mf3d_params *prm) {
+  if (!prm) { set_error("params: NULL"); return MF3D_E_INVALID; }
   if (prm->ngrid < 1 || prm->ngrid > 16) { set_error("ngrid out of range"); return MF3D_E_INVALID; }
   if (prm->mg_itrsch < 1 || prm->mg_itrsch > 3) { set_error("error about mg iteration selection (mg_itrsch)"); return MF3D_E_INVALID; }
   if (prm->irestr < 0 || prm->iproln < 0 || prm->maxcy < 0) { set_error("negative sweep/cycle count"); return MF3D_E_INVALID; }
   if (prm->pl < 1) { set_error("pl must be >= 1"); return MF3D_E_INVALID; }
   if (prm->differencing != 1) { set_error("differencing != 1 (4th-order calmas) is not supported"); return MF3D_E_UNSUPPORTED; }
   if (prm->precision < 0 || prm->precision > 1) { set_error("precision mode not supported"); return MF3D_E_UNSUPPORTED; }
+  return MF3D_OK;
+}
+
+static int ctx_init(mf3d_ctx *C, const mf3d_params *prm) {
+  C->prm = *prm;
+  C->device = prm->device;
+  C->elem = prm->precision == MF3D_PREC_FP64 ? 8 : 4;
+  CK(cudaSetDevice(C->device));
+  // A blocking stream: it orders after work the caller queued on the legacy
+  // default stream (e.g. the copies that produced the device inputs).
+  CK(cudaStreamCreateWithFlags(&C->stream, cudaStreamDefault));
+  CK(cudaEventCreate(&C->ev0));
+  CK(cudaEventCreate(&C->ev1));
+  const char *e = getenv("MF3D_NO_GRAPH");
+  C->use_graph = !(e && e[0] == '1');
+  return MF3D_OK;
+}
+
+static int make_view(mf3d_ctx *C) {
+  std::vector<DomainStore *> doms;
+  for (auto &d : C->doms) doms.push_back(d.get());
+  C->view.reset(new View());
+  return build_view(C, *C->view, doms, std::max(C->prm.maxcy, 1));
+}
+
+static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, mf3d_ctx **out) {
+  if (!blocks || nb <= 0 || !out) { set_error("mf3d_create: bad arguments"); return MF3D_E_INVALID; }
+  int st = check_params(prm);
+  if (st) return st;
   const int pow2 = 1 << (prm->ngrid - 1);
   for (int b = 0; b < nb; ++b) {
     const auto &d = blocks[b];
@@ -607,112 +903,133 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
       return MF3D_E_INVALID;
     }
   }
-  auto C = std::make_unique<mf3d_ctx>();
-  C->prm = *prm;
-  C->blocks.assign(blocks, blocks + nb);
-  C->nb = nb;
-  C->device = prm->device;
-  // widths arrays are borrowed at create time only
-  int st = face_rules(C->blocks, C->rules);
-  if (st) return st;
-  CK(cudaSetDevice(C->device));
-  // A blocking stream: it orders after work the caller queued on the legacy
-  // default stream (e.g. the copies that produced the device inputs).
-  CK(cudaStreamCreateWithFlags(&C->stream, cudaStreamDefault));
-  CK(cudaEventCreate(&C->ev0));
-  CK(cudaEventCreate(&C->ev1));
-  CK(cudaMallocHost(&C->rmax_host, sizeof(unsigned long long) * 2));
-  if ((st = C->rmax_cur.alloc(1))) return st;
-  if ((st = C->rmax_scratch.alloc(1))) return st;
-  if ((st = C->st.alloc(1))) return st;
-  if ((st = C->hist_d.alloc(std::max(prm->maxcy, 0) + 1))) return st;
   {
-    const char *e = getenv("MF3D_NO_GRAPH");
-    C->use_graph = !(e && e[0] == '1');
+    std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
+    std::vector<FaceRule> rules;
+    if ((st = face_rules(descs, rules))) return st;
   }
-  if ((st = C->ptrs.alloc(2 * nb))) return st;
-  const int ngrid = prm->ngrid;
-  if (prm->precision == MF3D_PREC_FP64) {
-    C->L64.resize(ngrid + 1);
-    for (int g = 1; g <= ngrid; ++g) {
-      C->L64[g].reset(new Level<double>());
-      if ((st = build_level<double>(C.get(), *C->L64[g], g))) return st;
-    }
-  } else {
-    C->L32.resize(ngrid + 1);
-    for (int g = 1; g <= ngrid; ++g) {
-      C->L32[g].reset(new Level<float>());
-      if ((st = build_level<float>(C.get(), *C->L32[g], g))) return st;
-    }
-  }
-  // field geometry: widths, face distances, face planes
-  std::vector<double> geo;
-  std::vector<size_t> off_h(3 * nb), off_df(3 * nb);
-  size_t plane_total = 0;
-  std::vector<size_t> plane_off(nb);
-  for (int b = 0; b < nb; ++b) {
-    const auto &d = C->blocks[b];
-    const double *ext[3] = {d.hx, d.hy, d.hz};
-    const double hh[3] = {d.dx, d.dy, d.dz};
-    const int n[3] = {d.nx, d.ny, d.nz};
-    for (int a = 0; a < 3; ++a) {
-      std::vector<double> w = level_widths(ext[a], n[a], hh[a], ngrid, 1);
-      off_h[3 * b + a] = geo.size();
-      for (int c = 0; c < n[a] + 2; ++c) geo.push_back(ext[a] ? w[c] : hh[a]);
-      off_df[3 * b + a] = geo.size();
-      for (int c = 0; c <= n[a]; ++c) geo.push_back(ext[a] ? 0.5 * (w[c] + w[c + 1]) : hh[a]);
-    }
-    plane_off[b] = plane_total;
-    plane_total += 2 * ((size_t)d.ny * d.nz + (size_t)d.nx * d.nz + (size_t)d.nx * d.ny);
-  }
-  if ((st = C->widths.upload(geo, C->stream))) return st;
-  if ((st = C->planes.alloc(plane_total))) return st;
-  CK(cudaMemsetAsync(C->planes.p, 0, plane_total * sizeof(double), C->stream));
-  C->hf.resize(nb);
-  std::vector<long long> it_int, it_l1, it_faces, it_planes;
-  for (int b = 0; b < nb; ++b) {
-    const auto &d = C->blocks[b];
-    BlkFld &F = C->hf[b];
-    std::memset(&F, 0, sizeof F);
-    F.nx = d.nx; F.ny = d.ny; F.nz = d.nz; F.pl = prm->pl;
-    F.ti = d.nx + 2 * prm->pl; F.tj = d.ny + 2 * prm->pl;
-    for (int f = 0; f < 6; ++f) {
-      F.wall[f] = C->rules[6 * b + f].kind == FACE_WALL;
-      F.src[f] = C->rules[6 * b + f].src;
-    }
-    for (int a = 0; a < 3; ++a) {
-      F.h[a] = C->widths.p + off_h[3 * b + a];
-      F.df[a] = C->widths.p + off_df[3 * b + a];
-    }
-    double *pp = C->planes.p + plane_off[b];
-    const size_t pyz = (size_t)d.ny * d.nz, pxz = (size_t)d.nx * d.nz, pxy = (size_t)d.nx * d.ny;
-    F.lo[0] = pp; F.hi[0] = pp + pyz; pp += 2 * pyz;
-    F.lo[1] = pp; F.hi[1] = pp + pxz; pp += 2 * pxz;
-    F.lo[2] = pp; F.hi[2] = pp + pxy;
-    F.L1 = prm->precision == MF3D_PREC_FP64 ? C->L64[1]->hb[b] : C->L32[1]->hb[b];
-    it_int.push_back((long long)d.nx * d.ny * d.nz);
-    C->n_l1 += (long long)d.nx * d.ny * d.nz;
-    it_l1.push_back((long long)(d.nx + 2) * (d.ny + 2) * (d.nz + 2));
-    it_faces.push_back(2 * ((long long)d.ny * d.nz + (long long)d.nx * d.nz + (long long)d.nx * d.ny));
-    it_planes.push_back((long long)d.ny * d.nz + (long long)d.nx * d.nz + (long long)d.nx * d.ny);
-  }
-  if ((st = C->df.alloc(nb))) return st;
-  auto t1 = make_tiles(it_int), t2 = make_tiles(it_l1), t3 = make_tiles(it_faces), t4 = make_tiles(it_planes);
-  C->n_int = (int)t1.size(); C->n_l1cells = (int)t2.size(); C->n_faces = (int)t3.size(); C->n_planes = (int)t4.size();
-  if ((st = C->t_int.upload(t1, C->stream))) return st;
-  if ((st = C->t_l1cells.upload(t2, C->stream))) return st;
-  if ((st = C->t_faces.upload(t3, C->stream))) return st;
-  if ((st = C->t_planes.upload(t4, C->stream))) return st;
-  CK(cudaStreamSynchronize(C->stream));
-  // host-field mirrors are allocated lazily by the host entry point
-  for (auto &d : C->blocks) d.hx = d.hy = d.hz = nullptr;
+  auto C = std::make_unique<mf3d_ctx>();
+  if ((st = ctx_init(C.get(), prm))) return st;
+  C->doms.emplace_back(new DomainStore());
+  if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, prm->pl, C->stream))) return st;
+  if ((st = make_view(C.get()))) return st;
   *out = C.release();
   return MF3D_OK;
 }
 
-static int run_solve(mf3d_ctx *C, double dt, double alfapr, mf3d_solve_info *info, double *hist, int cap) {
-  if (C->prm.precision == MF3D_PREC_FP64) return solve_device<double>(C, dt, alfapr, info, hist, cap);
-  return solve_device<float>(C, dt, alfapr, info, hist, cap);
+}  // namespace mf3d
+
+// The deepest level count a domain allows: every edge divisible by 2^(L-1)
+// with the coarsest edge >= 4 (at least one level).
+int mf3d_max_levels(int nx, int ny, int nz) {
+  int L = 1;
+  while (true) {
+    const int m = 1 << L;
+    if (nx % m || ny % m || nz % m) break;
+    if (nx / m < 4 || ny / m < 4 || nz / m < 4) break;
+    ++L;
+  }
+  return L;
+}
+
+namespace mf3d {
+
+// One block alone: no neighbours, periodic axes wrap onto itself.
+static mf3d_block_desc lone_block(const mf3d_domain_desc &x) {
+  mf3d_block_desc d;
+  std::memset(&d, 0, sizeof d);
+  d.id = 0;
+  d.nx = x.nx; d.ny = x.ny; d.nz = x.nz;
+  d.dx = x.dx; d.dy = x.dy; d.dz = x.dz;
+  d.xel = x.nx * x.dx; d.yel = x.ny * x.dy; d.zel = x.nz * x.dz;
+  d.iprev = d.inext = d.jprev = d.jnext = d.kprev = d.knext = -1;
+  for (int q = 0; q < 4; ++q) d.corprev[q] = d.cornext[q] = -1;
+  for (int q = 0; q < 6; ++q) d.edgprev[q] = d.edgnext[q] = -1;
+  d.per_ip = d.per_in = d.per_jp = d.per_jn = d.per_kp = d.per_kn = -1;
+  d.bc_west = d.bc_east = x.bc[0];
+  d.bc_south = d.bc_north = x.bc[1];
+  d.bc_bottom = d.bc_top = x.bc[2];
+  d.hx = x.hx; d.hy = x.hy; d.hz = x.hz;
+  return d;
+}
+
+static int domain_ngrid(const mf3d_domain_desc &x) {
+  if (x.nx < 1 || x.ny < 1 || x.nz < 1) return -1;
+  if (x.ngrid <= 0) return mf3d_max_levels(x.nx, x.ny, x.nz);
+  const int pow2 = 1 << (x.ngrid - 1);
+  if (x.nx % pow2 || x.ny % pow2 || x.nz % pow2) return -1;
+  return x.ngrid;
+}
+
+static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params *prm, mf3d_ctx **out) {
+  if (!doms || nd <= 0 || !out) { set_error("mf3d_batch_create: bad arguments"); return MF3D_E_INVALID; }
+  int st = check_params(prm);
+  if (st) return st;
+  for (int d = 0; d < nd; ++d)
+    if (domain_ngrid(doms[d]) < 1) {
+      set_error("domain " + std::to_string(d) + ": sizes not divisible by 2^(ngrid-1)");
+      return MF3D_E_INVALID;
+    }
+  auto C = std::make_unique<mf3d_ctx>();
+  if ((st = ctx_init(C.get(), prm))) return st;
+  for (int d = 0; d < nd; ++d) {
+    mf3d_block_desc b = lone_block(doms[d]);
+    C->doms.emplace_back(new DomainStore());
+    if ((st = build_domain(*C->doms.back(), &b, 1, domain_ngrid(doms[d]), C->elem, prm->pl, C->stream))) return st;
+  }
+  if ((st = make_view(C.get()))) return st;
+  *out = C.release();
+  return MF3D_OK;
+}
+
+static int run_solve(mf3d_ctx *C, const double *dt, const double *alfapr, mf3d_solve_info *infos, double *hist,
+                     int hcap) {
+  if (C->elem == 8) return solve_view<double>(C, *C->view, dt, alfapr, infos, hist, hcap);
+  return solve_view<float>(C, *C->view, dt, alfapr, infos, hist, hcap);
+}
+
+// Host entry: mirror host arrays on the device (8 per block), solve, copy back.
+static int host_solve(mf3d_ctx *C, const mf3d_fields *fields, const double *dt, const double *alfapr,
+                      mf3d_solve_info *infos, double *hist, int hcap) {
+  View &V = *C->view;
+  cudaStream_t s = C->stream;
+  const int nb = (int)V.blk.size();
+  const int pl = C->prm.pl;
+  if (!C->mirror.p) {
+    size_t tot = 0;
+    C->mirror_off.resize(nb);
+    for (int b = 0; b < nb; ++b) { C->mirror_off[b] = tot; tot += 8 * ttc_elems(pl, V.blk[b]->d); }
+    int st = C->mirror.alloc(tot);
+    if (st) return st;
+  }
+  std::vector<mf3d_fields> dev(nb);
+  for (int b = 0; b < nb; ++b) {
+    const size_t n = ttc_elems(pl, V.blk[b]->d);
+    double *m = C->mirror.p + C->mirror_off[b];
+    double *const hsrc[7] = {fields[b].ustar, fields[b].vstar, fields[b].wstar, fields[b].u, fields[b].v, fields[b].w, fields[b].p};
+    for (int q = 0; q < 7; ++q) {
+      if (!hsrc[q]) { set_error("mf3d_fields: a required pointer is NULL"); return MF3D_E_INVALID; }
+      CK(cudaMemcpyAsync(m + q * n, hsrc[q], n * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    dev[b] = mf3d_fields{m, m + n, m + 2 * n, m + 3 * n, m + 4 * n, m + 5 * n, m + 6 * n,
+                         fields[b].su ? m + 7 * n : nullptr};
+  }
+  int st = bind_fields(C, V, dev.data());
+  if (st) return st;
+  st = run_solve(C, dt, alfapr, infos, hist, hcap);
+  if (st < 0 && st != MF3D_E_NONFINITE) return st;
+  for (int b = 0; b < nb; ++b) {
+    const size_t n = ttc_elems(pl, V.blk[b]->d);
+    double *m = C->mirror.p + C->mirror_off[b];
+    double *const hdst[5] = {fields[b].u, fields[b].v, fields[b].w, fields[b].p, fields[b].su};
+    const int q_of[5] = {3, 4, 5, 6, 7};
+    for (int q = 0; q < 5; ++q) {
+      if (!hdst[q]) continue;
+      CK(cudaMemcpyAsync(hdst[q], m + q_of[q] * n, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+  }
+  CK(cudaStreamSynchronize(s));
+  return st;
 }
 
 }  // namespace mf3d
@@ -755,16 +1072,24 @@ int mf3d_create(const mf3d_block_desc *blocks, int nblocks, const mf3d_params *p
   }
 }
 
+int mf3d_batch_create(const mf3d_domain_desc *domains, int ndomains, const mf3d_params *params, mf3d_ctx **ctx) {
+  try {
+    return mf3d::batch_create(domains, ndomains, params, ctx);
+  } catch (const std::exception &e) {
+    mf3d::set_error(std::string("mf3d_batch_create: ") + e.what());
+    return MF3D_E_OOM;
+  }
+}
+
 int mf3d_destroy(mf3d_ctx *ctx) {
   if (!ctx) return MF3D_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  if (ctx->rmax_host) cudaFreeHost(ctx->rmax_host);
+  ctx->view.reset();
+  ctx->doms.clear();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   for (auto e : ctx->prof_ev) cudaEventDestroy(e);
-  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
-  if (ctx->graph) cudaGraphDestroy(ctx->graph);
   cudaStream_t s = ctx->stream;
   delete ctx;
   if (s) cudaStreamDestroy(s);
@@ -774,66 +1099,35 @@ int mf3d_destroy(mf3d_ctx *ctx) {
 int mf3d_newsolv_mg_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr, mf3d_solve_info *info,
                            double *hist, int cap) {
   if (!C || !fields) { mf3d::set_error("mf3d_newsolv_mg_device: bad arguments"); return MF3D_E_INVALID; }
+  if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
-  int st = mf3d::bind_fields(C, fields);
+  int st = mf3d::bind_fields(C, *C->view, fields);
   if (st) return st;
-  return mf3d::run_solve(C, dt, alfapr, info, hist, cap);
+  return mf3d::run_solve(C, &dt, &alfapr, info, hist, cap);
 }
 
 int mf3d_newsolv_mg(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr, mf3d_solve_info *info,
                     double *hist, int cap) {
   if (!C || !fields) { mf3d::set_error("mf3d_newsolv_mg: bad arguments"); return MF3D_E_INVALID; }
+  if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
-  cudaStream_t s = C->stream;
-  // device mirrors: 8 arrays per block (ustar, vstar, wstar, u, v, w, p, su)
-  if (!C->mirror.p) {
-    size_t tot = 0;
-    C->mirror_off.resize(C->nb);
-    for (int b = 0; b < C->nb; ++b) { C->mirror_off[b] = tot; tot += 8 * mf3d::ttc_elems(C, b); }
-    int st = C->mirror.alloc(tot);
-    if (st) return st;
-  }
-  std::vector<mf3d_fields> dev(C->nb);
-  for (int b = 0; b < C->nb; ++b) {
-    const size_t n = mf3d::ttc_elems(C, b);
-    double *m = C->mirror.p + C->mirror_off[b];
-    double *const hsrc[7] = {fields[b].ustar, fields[b].vstar, fields[b].wstar, fields[b].u, fields[b].v, fields[b].w, fields[b].p};
-    for (int q = 0; q < 7; ++q) {
-      if (!hsrc[q]) { mf3d::set_error("mf3d_fields: a required pointer is NULL"); return MF3D_E_INVALID; }
-      if (cudaMemcpyAsync(m + q * n, hsrc[q], n * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) {
-        mf3d::set_error("host-to-device copy failed"); return MF3D_E_CUDA;
-      }
-    }
-    dev[b] = mf3d_fields{m, m + n, m + 2 * n, m + 3 * n, m + 4 * n, m + 5 * n, m + 6 * n,
-                         fields[b].su ? m + 7 * n : nullptr};
-  }
-  int st = mf3d::bind_fields(C, dev.data());
+  return mf3d::host_solve(C, fields, &dt, &alfapr, info, hist, cap);
+}
+
+int mf3d_batch_solve_device(mf3d_ctx *C, const mf3d_fields *fields, const double *dt, const double *alfapr,
+                            mf3d_solve_info *infos, double *hist, int hcap) {
+  if (!C || !fields || !dt || !alfapr) { mf3d::set_error("mf3d_batch_solve_device: bad arguments"); return MF3D_E_INVALID; }
+  if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  int st = mf3d::bind_fields(C, *C->view, fields);
   if (st) return st;
-  st = mf3d::run_solve(C, dt, alfapr, info, hist, cap);
-  if (st < 0 && st != MF3D_E_NONFINITE) return st;
-  for (int b = 0; b < C->nb; ++b) {
-    const size_t n = mf3d::ttc_elems(C, b);
-    double *m = C->mirror.p + C->mirror_off[b];
-    double *const hdst[5] = {fields[b].u, fields[b].v, fields[b].w, fields[b].p, fields[b].su};
-    const int q_of[5] = {3, 4, 5, 6, 7};
-    for (int q = 0; q < 5; ++q) {
-      if (!hdst[q]) continue;
-      if (cudaMemcpyAsync(hdst[q], m + q_of[q] * n, n * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) {
-        mf3d::set_error("device-to-host copy failed"); return MF3D_E_CUDA;
-      }
-    }
-  }
-  if (cudaStreamSynchronize(s) != cudaSuccess) { mf3d::set_error("stream sync failed"); return MF3D_E_CUDA; }
-  return st;
+  return mf3d::run_solve(C, dt, alfapr, infos, hist, hcap);
 }
 
 int mf3d_mgkcyc_device(mf3d_ctx *C, double *const *su, double *const *pp) {
   if (!C || !su || !pp) { mf3d::set_error("mf3d_mgkcyc_device: bad arguments"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
-  // the V-cycle needs the block geometry of the field table, not the fields
-  cudaMemcpyAsync(C->df.p, C->hf.data(), C->hf.size() * sizeof(mf3d::BlkFld), cudaMemcpyHostToDevice, C->stream);
-  if (C->prm.precision == MF3D_PREC_FP64) return mf3d::mgkcyc_device<double>(C, su, pp);
-  return mf3d::mgkcyc_device<float>(C, su, pp);
+  if (C->elem == 8) return mf3d::mgkcyc_view<double>(C, *C->view, su, pp);
+  return mf3d::mgkcyc_view<float>(C, *C->view, su, pp);
 }
 
 long long mf3d_last_launch_count(const mf3d_ctx *C) { return C ? C->launches : 0; }

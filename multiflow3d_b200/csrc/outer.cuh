@@ -8,14 +8,19 @@
 
 namespace mf3d {
 
-// Device-resident control state of one solve (newsolv_mg's module variables
-// dt, alfapr, eps, maxcy, iter, rmax), so the outer loop can run as a CUDA
-// graph with no host round trip per iteration.
-struct SolveState {
+// Device-resident control state of one domain's solve (newsolv_mg's module
+// variables dt, alfapr, eps, maxcy, iter, rmax), so the outer loop runs as a
+// CUDA graph with no host round trip per iteration; independent domains
+// (a batch) each carry their own.
+struct DomState {
   double dt, alfapr;
-  double eps;      // absolute threshold on rmax (eps * rmax0 in relative mode)
+  double tol;      // eps as given
+  double eps;      // absolute threshold on rmax (tol * rmax0 in relative mode)
+  double rmax0;    // rmax after the initial calvel/calmas
   double rmax;     // rmax after the last outer iteration
+  double dtinv;    // 1/dt when dt is a power of two, else 0 (see xdiv)
   int maxcy;
+  int eps_relative;
   int iter;        // outer iterations done
   int done;        // 0 running, 1 converged, 2 non-finite rmax, 3 maxcy reached
 };
@@ -30,7 +35,14 @@ struct BlkFld {
   const double *h[3];                // cell widths, n+2 entries (ghost-inclusive)
   const double *df[3];               // centre distances of faces 0..n (face a: cells a|a+1)
   BlkLev L1;                         // level-1 descriptor
+  int dom;                           // domain of the block
+  double pinv[3];                    // 1/h when the axis is uniform with h a power of two, else 0
 };
+
+// x / h.  When h is a power of two the multiplication by its reciprocal
+// (exact) rounds the same exact quotient once, so the result is the IEEE
+// quotient bit for bit; otherwise divide.
+__device__ __forceinline__ double xdiv(double x, double h, double inv) { return inv != 0.0 ? x * inv : x / h; }
 
 __device__ inline long long fidx(const BlkFld &F, int i, int j, int k) {
   // level-1 ghost-inclusive (i,j,k) -> 0-based ttc element
@@ -40,22 +52,31 @@ __device__ inline long long fidx(const BlkFld &F, int i, int j, int k) {
 // p := p + (pp - ppref) over isp-1..iep+1 (newsolv_mg.for:38-48), ppref = 0
 // (the reference-pressure code is commented out, :28-36); pp is the level-1
 // correction of the V-cycle.  One thread per ghost-inclusive level-1 cell.
+// Also zeroes the ghost shell of pp after reading it: the next V-cycle starts
+// from pp = 0 (newsolv_mg.for:44) and its first red sweep never reads the
+// interior, so the shell is all that must hold zeros.
 template <typename T>
-__global__ void __launch_bounds__(kTile) k_add_correction(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                                                          const T *__restrict__ phi1) {
+__global__ void __launch_bounds__(RW_TX *RW_RJ) k_add_correction(const BlkFld *__restrict__ fl,
+                                                                 const Tile *__restrict__ tiles,
+                                                                 const int *__restrict__ act) {
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
+  if (!act[F.dom]) return;
   const BlkLev &B = F.L1;
-  const int W = B.nx + 2, H = B.ny + 2;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  if (q >= (long long)W * H * (B.nz + 2)) return;
-  const int k = (int)(q / ((long long)W * H));
-  const int rem = (int)(q - (long long)k * W * H);
-  const int j = rem / W, i = rem - j * W;
-  const double pp = (double)phi1[cell_addr(B, B.phi0, i, j, k)];
-  const double ppref = 0.0;
-  double *p = F.p + fidx(F, i, j, k);
-  *p = (*p + (pp - ppref));
+  T *__restrict__ phi1 = phi_of<T>(B);
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i > B.nx + 1 || j > B.ny + 1) return;
+  double *__restrict__ P = F.p;
+  const int k1 = min(t.k0 + RW_KCH - 1, B.nz + 1);
+#pragma unroll 4
+  for (int k = t.k0; k <= k1; ++k) {
+    const long long a = cell_off(B, i, j, k);
+    const double pp = (double)phi1[a];
+    const double ppref = 0.0;
+    const long long f = fidx(F, i, j, k);
+    P[f] = (P[f] + (pp - ppref));
+    if (i == 0 || i == B.nx + 1 || j == 0 || j == B.ny + 1 || k == 0 || k == B.nz + 1) phi1[a] = (T)0;
+  }
 }
 
 // exchange(4) + pbound on the face ghosts of p (exchange.for:2402-2490,
@@ -63,10 +84,11 @@ __global__ void __launch_bounds__(kTile) k_add_correction(const BlkFld *__restri
 // the source block's adjacent interior value, wall faces mirror the first
 // interior cell.  Only the interior tangential range: the path reads no
 // other ghost of p.  Items per block: 2*(ny*nz + nx*nz + nx*ny).
-__global__ void k_p_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles) {
+__global__ void k_p_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, const int *__restrict__ act) {
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
-  int q = t.item0 + threadIdx.x;
+  if (!act[F.dom]) return;
+  int q = t.i0 + threadIdx.x;
   const int nx = F.nx, ny = F.ny, nz = F.nz;
   const int nyz = ny * nz, nxz = nx * nz, nxy = nx * ny;
   int f, a, b;
@@ -97,7 +119,7 @@ __global__ void k_p_faces(const BlkFld *__restrict__ fl, const Tile *__restrict_
 __global__ void k_face_planes(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles) {
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
-  int q = t.item0 + threadIdx.x;
+  int q = t.i0 + threadIdx.x;
   const int nx = F.nx, ny = F.ny, nz = F.nz;
   const int nyz = ny * nz, nxz = nx * nz, nxy = nx * ny;
   int ax, a, b;
@@ -138,138 +160,189 @@ __device__ inline void atomic_max_nonneg(unsigned long long *slot, double v) {
 // rmax = max |fact*dx*dy*dz| (MPI_MAX over one device: an order-free
 // atomic max on the bit pattern, hence deterministic).
 template <typename T>
-__global__ void __launch_bounds__(kTile) k_calvel_calmas(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                                                         const SolveState *__restrict__ st, T *__restrict__ rhs1,
-                                                         unsigned long long *__restrict__ rmax_slot, int write_su) {
-  const double dt = st->dt, alfapr = st->alfapr;
+__global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas(const BlkFld *__restrict__ fl,
+                                                               const Tile *__restrict__ tiles,
+                                                               const DomState *__restrict__ ds,
+                                                               const int *__restrict__ act,
+                                                               unsigned long long *__restrict__ rmax_slot,
+                                                               int write_su) {
+  __shared__ double red[OZ_RJ];
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
-  const int nx = F.nx, ny = F.ny;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  double fact1 = 0.0;
-  if (q < (long long)nx * ny * F.nz) {
-    const int k = (int)(q / ((long long)nx * ny)) + 1;
-    const int rem = (int)(q - (long long)(k - 1) * nx * ny);
-    const int j = rem / nx + 1, i = rem - (j - 1) * nx + 1;
-    const double dta = dt * alfapr;
-    const long long c = fidx(F, i, j, k);
-    const long long sx = 1, sy = F.ti, sz = (long long)F.ti * F.tj;
-    const double *p = F.p;
-    const double pc = p[c];
-    // x faces
-    double ue, uw;
-    if (i == nx && F.wall[1]) ue = F.hi[0][(k - 1) * ny + (j - 1)];
-    else ue = (F.ustar[c] - dta * (p[c + sx] - pc) / F.df[0][i]);
-    if (i == 1) {
-      const double lo = F.lo[0][(k - 1) * ny + (j - 1)];
-      uw = F.wall[0] ? lo : (lo - dta * (pc - p[c - sx]) / F.df[0][0]);
-    } else {
-      uw = (F.ustar[c - sx] - dta * (pc - p[c - sx]) / F.df[0][i - 1]);
-    }
-    // y faces
-    double vn, vs;
-    if (j == ny && F.wall[3]) vn = F.hi[1][(k - 1) * nx + (i - 1)];
-    else vn = (F.vstar[c] - dta * (p[c + sy] - pc) / F.df[1][j]);
-    if (j == 1) {
-      const double lo = F.lo[1][(k - 1) * nx + (i - 1)];
-      vs = F.wall[2] ? lo : (lo - dta * (pc - p[c - sy]) / F.df[1][0]);
-    } else {
-      vs = (F.vstar[c - sy] - dta * (pc - p[c - sy]) / F.df[1][j - 1]);
-    }
-    // z faces
-    double wt, wb;
-    if (k == F.nz && F.wall[5]) wt = F.hi[2][(j - 1) * nx + (i - 1)];
-    else wt = (F.wstar[c] - dta * (p[c + sz] - pc) / F.df[2][k]);
+  if (!act[F.dom]) return;
+  const double dt = ds[F.dom].dt, alfapr = ds[F.dom].alfapr, dtinv = ds[F.dom].dtinv;
+  const double dta = dt * alfapr;
+  T *__restrict__ rhs1 = rhs_of<T>(F.L1);
+  double *__restrict__ SU = write_su ? F.su : nullptr;
+  const int nx = F.nx, ny = F.ny, nz = F.nz;
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  const bool in = i <= nx && j <= ny;
+  const int ic = in ? i : 1, jc = in ? j : 1;  // clamped indices keep every load in bounds
+  const long long sy = F.ti, sz = (long long)F.ti * F.tj;
+  const double *__restrict__ p = F.p;
+  const double *__restrict__ US = F.ustar;
+  const double *__restrict__ VS = F.vstar;
+  const double *__restrict__ WS = F.wstar;
+  const double *__restrict__ DZ = F.df[2];
+  const double *__restrict__ HZ = F.h[2];
+  const double ix = F.pinv[0], iy = F.pinv[1], iz = F.pinv[2];
+  const double hx = F.h[0][ic], hy = F.h[1][jc];
+  const double dxe = F.df[0][ic], dxw = F.df[0][ic - 1];
+  const double dyn = F.df[1][jc], dys = F.df[1][jc - 1];
+  const bool ewall = F.wall[1], nwall = F.wall[3], twall = F.wall[5];
+  const bool wwall = F.wall[0], swall = F.wall[2], bwall = F.wall[4];
+  const int k1 = min(t.k0 + OZ_KCH - 1, nz);
+  double vmax = 0.0;
+  // w on the face below plane k0, carried up the march
+  double wb;
+  {
+    const int k = t.k0;
+    const long long c = fidx(F, ic, jc, k);
     if (k == 1) {
-      const double lo = F.lo[2][(j - 1) * nx + (i - 1)];
-      wb = F.wall[4] ? lo : (lo - dta * (pc - p[c - sz]) / F.df[2][0]);
+      const double lo = F.lo[2][(jc - 1) * nx + (ic - 1)];
+      wb = bwall ? lo : (lo - xdiv(dta * (p[c] - p[c - sz]), F.df[2][0], iz));
     } else {
-      wb = (F.wstar[c - sz] - dta * (pc - p[c - sz]) / F.df[2][k - 1]);
+      wb = (WS[c - sz] - xdiv(dta * (p[c] - p[c - sz]), DZ[k - 1], iz));
     }
-    const double hx = F.h[0][i], hy = F.h[1][j], hz = F.h[2][k];
-    const double fact = ((ue - uw) / hx + (vn - vs) / hy + (wt - wb) / hz);
-    const double su = fact / dt;
-    rhs1[cell_addr(F.L1, F.L1.rhs0, i, j, k)] = (T)su;
-    if (write_su && F.su) F.su[c] = su;
-    fact1 = fact * hx * hy * hz;
-    fact1 = fabs(fact1);
-    if (!(fact1 == fact1)) fact1 = __longlong_as_double(0x7ff0000000000000LL);  // NaN -> +Inf (flagged)
   }
-  // CTA max: warp shuffles, then one atomic per warp
-  for (int o = 16; o > 0; o >>= 1) fact1 = fmax(fact1, __shfl_xor_sync(0xffffffffu, fact1, o));
-  if ((threadIdx.x & 31) == 0 && fact1 > 0.0) atomic_max_nonneg(rmax_slot, fact1);
+  for (int k = t.k0; k <= k1; ++k) {
+    const long long c = fidx(F, ic, jc, k);
+    const double pc = p[c];
+    // east face of this cell; the west face is the east face of the cell to the
+    // left (the lane before), formed from the same operands
+    double ue;
+    if (ic == nx && ewall) ue = F.hi[0][(k - 1) * ny + (jc - 1)];
+    else ue = (US[c] - xdiv(dta * (p[c + 1] - pc), dxe, ix));
+    const double ul = __shfl_up_sync(0xffffffffu, ue, 1);
+    double uw;
+    if (ic == 1) {
+      const double lo = F.lo[0][(k - 1) * ny + (jc - 1)];
+      uw = wwall ? lo : (lo - xdiv(dta * (pc - p[c - 1]), dxw, ix));
+    } else if (threadIdx.x > 0) {
+      uw = ul;
+    } else {
+      uw = (US[c - 1] - xdiv(dta * (pc - p[c - 1]), dxw, ix));
+    }
+    double vn, vs, wt;
+    if (jc == ny && nwall) vn = F.hi[1][(k - 1) * nx + (ic - 1)];
+    else vn = (VS[c] - xdiv(dta * (p[c + sy] - pc), dyn, iy));
+    if (jc == 1) {
+      const double lo = F.lo[1][(k - 1) * nx + (ic - 1)];
+      vs = swall ? lo : (lo - xdiv(dta * (pc - p[c - sy]), dys, iy));
+    } else {
+      vs = (VS[c - sy] - xdiv(dta * (pc - p[c - sy]), dys, iy));
+    }
+    if (k == nz && twall) wt = F.hi[2][(jc - 1) * nx + (ic - 1)];
+    else wt = (WS[c] - xdiv(dta * (p[c + sz] - pc), DZ[k], iz));
+    const double hz = HZ[k];
+    const double fact = (xdiv(ue - uw, hx, ix) + xdiv(vn - vs, hy, iy) + xdiv(wt - wb, hz, iz));
+    wb = wt;  // the top face of plane k is the bottom face of plane k+1
+    if (!in) continue;
+    const double su = xdiv(fact, dt, dtinv);
+    rhs1[cell_off(F.L1, i, j, k)] = (T)su;
+    if (SU) SU[c] = su;
+    double f1 = fabs(fact * hx * hy * hz);
+    if (!(f1 == f1)) f1 = __longlong_as_double(0x7ff0000000000000LL);  // NaN -> +Inf (flagged)
+    vmax = vmax > f1 ? vmax : f1;
+  }
+  // CTA max: warp shuffles, shared memory, one atomic per CTA
+  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  if (threadIdx.x == 0) red[threadIdx.y] = vmax;
+  __syncthreads();
+  if (threadIdx.y == 0) {
+    double v = threadIdx.x < OZ_RJ ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0 && v > 0.0) atomic_max_nonneg(rmax_slot + F.dom, v);
+  }
 }
 
 // Final calvel (press.for:139-198): u, v, w on the faces calvel writes
 // (isu..ieu etc., one face short at a high wall), from the final p.
-__global__ void __launch_bounds__(kTile) k_calvel(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                                                  const SolveState *__restrict__ st) {
-  const double dt = st->dt, alfapr = st->alfapr;
+__global__ void __launch_bounds__(RW_TX *RW_RJ) k_calvel(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                                                         const DomState *__restrict__ ds) {
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
+  const double dt = ds[F.dom].dt, alfapr = ds[F.dom].alfapr;
   const int nx = F.nx, ny = F.ny;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  if (q >= (long long)nx * ny * F.nz) return;
-  const int k = (int)(q / ((long long)nx * ny)) + 1;
-  const int rem = (int)(q - (long long)(k - 1) * nx * ny);
-  const int j = rem / nx + 1, i = rem - (j - 1) * nx + 1;
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i > nx || j > ny) return;
   const double dta = dt * alfapr;
-  const long long c = fidx(F, i, j, k);
   const long long sy = F.ti, sz = (long long)F.ti * F.tj;
-  const double *p = F.p;
-  if (!(i == nx && F.wall[1])) F.u[c] = (F.ustar[c] - dta * (p[c + 1] - p[c]) / F.df[0][i]);
-  if (!(j == ny && F.wall[3])) F.v[c] = (F.vstar[c] - dta * (p[c + sy] - p[c]) / F.df[1][j]);
-  if (!(k == F.nz && F.wall[5])) F.w[c] = (F.wstar[c] - dta * (p[c + sz] - p[c]) / F.df[2][k]);
+  const double *__restrict__ p = F.p;
+  const int k1 = min(t.k0 + RW_KCH - 1, F.nz);
+  for (int k = t.k0; k <= k1; ++k) {
+    const long long c = fidx(F, i, j, k);
+    if (!(i == nx && F.wall[1])) F.u[c] = (F.ustar[c] - xdiv(dta * (p[c + 1] - p[c]), F.df[0][i], F.pinv[0]));
+    if (!(j == ny && F.wall[3])) F.v[c] = (F.vstar[c] - xdiv(dta * (p[c + sy] - p[c]), F.df[1][j], F.pinv[1]));
+    if (!(k == F.nz && F.wall[5])) F.w[c] = (F.wstar[c] - xdiv(dta * (p[c + sz] - p[c]), F.df[2][k], F.pinv[2]));
+  }
 }
 
-// End of one outer iteration (newsolv_mg.for:54-58): record rmax, count the
-// iteration, test `rmax < eps .and. iter > 1`, and - inside the solve graph -
-// set the WHILE condition that repeats the iteration body.
-__global__ void k_iter_end(SolveState *st, unsigned long long *rmax_slot, double *hist,
+// After the initial calvel/calmas (newsolv_mg.for:16-17): rmax0, the
+// absolute threshold, and which domains iterate at all.
+__global__ void k_dom_init(DomState *ds, int ndom, unsigned long long *rmax_slot, int *act) {
+  for (int d = threadIdx.x; d < ndom; d += blockDim.x) {
+    const double r = __longlong_as_double((long long)rmax_slot[d]);
+    rmax_slot[d] = 0ull;
+    DomState &D = ds[d];
+    D.rmax0 = r;
+    D.rmax = r;
+    D.eps = D.eps_relative ? D.tol * r : D.tol;
+    D.iter = 0;
+    D.done = !(r <= 1.7976931348623157e308) ? 2 : (D.maxcy <= 0 ? 3 : 0);
+    act[d] = D.done ? 0 : 1;
+  }
+}
+
+// End of one outer iteration (newsolv_mg.for:54-58), per active domain:
+// record rmax, count the iteration, test `rmax < eps .and. iter > 1` (or
+// maxcy); a domain that stops is switched off for every later launch.  In
+// the solve graph, also sets the WHILE condition: any domain still running.
+__global__ void k_iter_end(DomState *ds, int ndom, unsigned long long *rmax_slot, double *hist, int hcap, int *act,
                            cudaGraphConditionalHandle cond, int in_graph) {
-  const double r = __longlong_as_double((long long)*rmax_slot);
-  *rmax_slot = 0ull;
-  const int it = st->iter + 1;
-  st->iter = it;
-  st->rmax = r;
-  hist[it - 1] = r;
-  int done = 0;
-  if (!(r <= 1.7976931348623157e308)) done = 2;  // +Inf (a NaN is stored as +Inf)
-  else if (r < st->eps && it > 1) done = 1;
-  else if (it >= st->maxcy) done = 3;
-  st->done = done;
-  if (in_graph) cudaGraphSetConditional(cond, done ? 0u : 1u);
+  int any = 0;
+  for (int d = threadIdx.x; d < ndom; d += blockDim.x) {
+    if (!act[d]) continue;
+    DomState &D = ds[d];
+    const double r = __longlong_as_double((long long)rmax_slot[d]);
+    rmax_slot[d] = 0ull;
+    const int it = D.iter + 1;
+    D.iter = it;
+    D.rmax = r;
+    if (it - 1 < hcap) hist[(long long)d * hcap + it - 1] = r;
+    int done = 0;
+    if (!(r <= 1.7976931348623157e308)) done = 2;  // +Inf (a NaN is stored as +Inf)
+    else if (r < D.eps && it > 1) done = 1;
+    else if (it >= D.maxcy) done = 3;
+    D.done = done;
+    if (done) act[d] = 0;
+    else any = 1;
+  }
+  any = __syncthreads_or(any);
+  if (in_graph && threadIdx.x == 0) cudaGraphSetConditional(cond, any ? 1u : 0u);
 }
 
 // Level-1 rhs := su (mgkcyc's copy-in, mgsolver.for:250-263) from a ttc array.
 template <typename T>
-__global__ void k_load_rhs(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, double *const *__restrict__ su,
-                           T *__restrict__ rhs1) {
+__global__ void k_load_rhs(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, double *const *__restrict__ su) {
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
-  const int nx = F.nx, ny = F.ny;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  if (q >= (long long)nx * ny * F.nz) return;
-  const int k = (int)(q / ((long long)nx * ny)) + 1;
-  const int rem = (int)(q - (long long)(k - 1) * nx * ny);
-  const int j = rem / nx + 1, i = rem - (j - 1) * nx + 1;
-  rhs1[cell_addr(F.L1, F.L1.rhs0, i, j, k)] = (T)su[t.blk][fidx(F, i, j, k)];
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i < 1 || i > F.nx || j < 1 || j > F.ny) return;
+  for (int k = t.k0; k <= min(t.k0 + RW_KCH - 1, F.nz); ++k)
+    rhs_of<T>(F.L1)[cell_off(F.L1, i, j, k)] = (T)su[t.blk][fidx(F, i, j, k)];
 }
 
 // pp := level-1 phi including the first ghost layer (mgsolver.for:351-364).
 template <typename T>
-__global__ void k_store_pp(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, double *const *__restrict__ pp,
-                           const T *__restrict__ phi1) {
+__global__ void k_store_pp(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, double *const *__restrict__ pp) {
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   const BlkLev &B = F.L1;
-  const int W = B.nx + 2, H = B.ny + 2;
-  const long long q = (long long)t.item0 + threadIdx.x;
-  if (q >= (long long)W * H * (B.nz + 2)) return;
-  const int k = (int)(q / ((long long)W * H));
-  const int rem = (int)(q - (long long)k * W * H);
-  const int j = rem / W, i = rem - j * W;
-  pp[t.blk][fidx(F, i, j, k)] = (double)phi1[cell_addr(B, B.phi0, i, j, k)];
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i > B.nx + 1 || j > B.ny + 1) return;
+  for (int k = t.k0; k <= min(t.k0 + RW_KCH - 1, B.nz + 1); ++k)
+    pp[t.blk][fidx(F, i, j, k)] = (double)phi_of<T>(B)[cell_off(B, i, j, k)];
 }
 
 }  // namespace mf3d

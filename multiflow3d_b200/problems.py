@@ -245,3 +245,34 @@ def fields_struct(blocks) -> "C.Array":
             assert a.dtype == np.float64 and a.flags.c_contiguous
             setattr(arr[b], k, a.ctypes.data_as(dp))
     return arr
+
+
+def domain_problem(nx, ny, nz, bc3, ngrid, h=None, pl=1):
+    """A single-block Problem for one batch domain (bc per axis)."""
+    h = h if h is not None else 1.0 / max(nx, ny, nz)
+    bc = (bc3[0], bc3[0], bc3[1], bc3[1], bc3[2], bc3[2])
+    return Problem(1, 1, 1, nx, ny, nz, bc=bc, dx=h, dy=h, dz=h, pl=pl, ngrid=ngrid)
+
+
+def domain_desc(pr: Problem):
+    from .abi import DomainDesc
+    d = DomainDesc()
+    d.nx, d.ny, d.nz = pr.nx, pr.ny, pr.nz
+    d.dx, d.dy, d.dz = pr.dx, pr.dy, pr.dz
+    d.bc[0], d.bc[1], d.bc[2] = pr.bc[0], pr.bc[2], pr.bc[4]
+    d.ngrid = pr.ngrid
+    return d
+
+
+def random_batch(n, seed, lo=32, hi=192, multiple=8):
+    """Domain sizes as the batched configuration draws them: each edge
+    log-uniform in [lo, hi] rounded to a multiple of 8; BCs per axis drawn
+    from {periodic, wall}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        e = np.exp(rng.uniform(np.log(lo), np.log(hi), size=3))
+        nx, ny, nz = (int(max(multiple, round(x / multiple) * multiple)) for x in e)
+        bc3 = tuple(int(PERIODIC if b else WALL) for b in rng.integers(0, 2, size=3))
+        out.append((nx, ny, nz, bc3))
+    return out

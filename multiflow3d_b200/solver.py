@@ -100,3 +100,59 @@ class Projection:
     @property
     def launches(self) -> int:
         return int(self.lib.mf3d_last_launch_count(self.ctx))
+
+
+def _dev_fields(blocks):
+    arr = (abi.Fields * len(blocks))()
+    for b, f in enumerate(blocks):
+        for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p", "su"):
+            t = f.get(k)
+            setattr(arr[b], k, C.cast(C.c_void_p(t.data_ptr()), _dp) if t is not None else None)
+    return arr
+
+
+class Batch:
+    """Many independent single-block domains solved by one set of launches
+    (``mf3d_batch_create`` / ``mf3d_batch_solve_device``).  Each domain runs
+    its own V-cycles and stops on its own test; results equal solo solves."""
+
+    def __init__(self, domains, params: abi.Params, lib=None):
+        self.lib = lib or abi.load()
+        self.n = len(domains)
+        arr = (abi.DomainDesc * self.n)(*domains)
+        self._arr = arr
+        self.params = params
+        ctx = C.c_void_p()
+        abi.check(self.lib, self.lib.mf3d_batch_create(arr, self.n, C.byref(params), C.byref(ctx)),
+                  "mf3d_batch_create")
+        self.ctx = ctx
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.mf3d_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve_device(self, fields, dt=None, alfapr=None):
+        """fields: one dict of CUDA float64 tensors per domain.  Returns a
+        list of SolveResult and the batch's worst status."""
+        dt = np.asarray(dt if dt is not None else np.ones(self.n), dtype=np.float64)
+        al = np.asarray(alfapr if alfapr is not None else np.ones(self.n), dtype=np.float64)
+        cap = max(self.params.maxcy, 1)
+        hist = np.zeros((self.n, cap))
+        infos = (abi.SolveInfo * self.n)()
+        st = self.lib.mf3d_batch_solve_device(self.ctx, _dev_fields(fields), dt.ctypes.data_as(_dp),
+                                              al.ctypes.data_as(_dp), infos, hist.ctypes.data_as(_dp), cap)
+        abi.check(self.lib, st, "mf3d_batch_solve_device")
+        out = [SolveResult(infos[d].status, infos[d].rmax, infos[d].rmax0, infos[d].iter, infos[d].ms_device,
+                           hist[d, :infos[d].iter].copy()) for d in range(self.n)]
+        return out, st
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.mf3d_last_launch_count(self.ctx))
