@@ -6,8 +6,9 @@
 // (0-based, ghost-inclusive, 0..n+1) has colour c = (i+j+k+1)&1 - colour 0
 // is the reference's even MOD(i+j+k,2) on its 1-based indices, updated first
 // (mgsolver.for:552) - and lives at element
-//     c*cstr + (k*(ny+2) + j)*hp + (i>>1),   hp = (nx+3)/2
-// of the block's level array.  A red-black half-sweep streams exactly one
+//     c*cstr + (k*(ny+2) + j)*hp + (i>>1)
+// of the block's level array, hp = (nx+3)/2 rounded up to 16 bytes (the row
+// pitch of a TMA tensor map).  A red-black half-sweep streams exactly one
 // colour in and the other out: 12 B/cell/half-sweep in FP64.
 //
 // Every block owns its arrays (a resident hierarchy); a launch covers any
@@ -26,6 +27,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>  // CUtensorMap (type only: the library does not link the driver)
 #include <cuda_runtime.h>
 
 namespace mf3d {
@@ -42,9 +44,14 @@ struct BlkLev {
   int nx, ny, nz, hp; // interior cells (0 = block absent at this level)
   int nmask;          // Neumann faces: bit f set for f = W,E,S,N,B,T
   int dom;            // domain of the block
+  const CUtensorMap *tm;  // TMA maps: phi colour 0, phi colour 1 (RB_RJ+2 rows), rhs colour 0, 1 (RB_RJ rows)
 };
 
-__host__ __device__ inline int hp_of(int nx) { return (nx + 3) / 2; }
+// compact row pitch: (nx+3)/2 entries rounded up to a multiple of 16 bytes
+__host__ __device__ inline int hp_of(int nx, int elem) {
+  const int per = 16 / elem;
+  return ((nx + 3) / 2 + per - 1) / per * per;
+}
 __device__ inline int colour_of(int i, int j, int k) { return (i + j + k + 1) & 1; }
 __device__ inline long long cell_off(const BlkLev &B, int i, int j, int k) {
   return colour_of(i, j, k) * B.cstr + ((long long)k * (B.ny + 2) + j) * B.hp + (i >> 1);
@@ -78,23 +85,63 @@ struct Tile {
 };
 
 // Tile shapes (threads per CTA = TX * RJ).
-constexpr int RB_TX = 32, RB_RJ = 8, RB_KCH = 16;   // red-black z-march
+constexpr int RB_TX = 32, RB_RJ = 8;                // red-black z-march (planes per CTA chosen per level)
 constexpr int RW_TX = 32, RW_RJ = 8, RW_KCH = 8;    // row tiles, RW_KCH planes per CTA
 constexpr int OZ_TX = 32, OZ_RJ = 8, OZ_KCH = 16;   // outer calvel/calmas z-march
 
-// Asynchronous global->shared copy of one element (LDGSTS), and the group
-// commit / wait of the copy pipeline.
-template <typename T>
-__device__ __forceinline__ void cp_async_elem(T *smem, const T *gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  if (sizeof(T) == 8)
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
+// ---------------------------------------------------------------------------
+// TMA and mbarrier primitives (inline PTX, sm_90+ forms; built for sm_100a).
+// Every wait is bounded: a copy that has not landed after kMaxWaitNs records
+// an error code for the host and the CTA returns.
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kMaxWaitNs = 2000000000ull;  // 2 s
+enum : int { ERR_TMA_WAIT = 1 };
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for phase `parity` of `bar`; false (and *err set) after kMaxWaitNs.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int *err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (;;) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if (global_ns() - t0 > kMaxWaitNs) {
+      atomicExch(err, ERR_TMA_WAIT);
+      return false;
+    }
+  }
+}
+// 3-D tiled TMA load of one box into shared memory, completing on `bar`.
+// x (innermost) must be a multiple of 16 bytes / element size.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], "
+      "[%2];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
 
 // ---------------------------------------------------------------------------
 // Red-black Gauss-Seidel half-sweep (mgsolver.for:547-601) of one colour over
@@ -104,81 +151,114 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // FROM_ZERO: the level was just zeroed (pp = 0 at the start of a V-cycle,
 // coarse phi = 0 after mgrestr), so the other colour is read as 0 without a
 // load; the result is bit-identical.
-// A CTA owns compact columns i0..i0+31 of rows j0..j0+7 and marches up a
-// chunk of planes.  Plane tiles of the other colour (with a one-cell halo)
-// and of the rhs are staged into shared memory by cp.async, RB_NS planes
-// deep, so several planes of loads are in flight per CTA while the current
-// plane is computed from shared memory.
+//
+// Lanes run over q, the rank of a cell of this colour within its row: cell
+// i = 2q + 2 - s with s = i & 1 = (colour + j + k + 1) & 1, so a row of nx
+// cells keeps ceil(nx/2) lanes busy whatever its parity.  Its west and east
+// neighbours (other colour) sit at compact h = q and q+1, the others and the
+// rhs at h = q + 1 - s.  A CTA owns q0..q0+31 of rows j0..j0+RB_RJ-1 and
+// marches up `kch` planes.  Per plane one thread issues two TMA box loads -
+// the other colour over compact columns q0..q0+TB_W-1 and rows j0-1..j0+RB_RJ,
+// the rhs over the same columns and rows j0..j0+RB_RJ-1 - into a ring of
+// RB_NS stages, RB_PD planes ahead of the plane being computed.  Boxes that
+// reach past the array read zeros (never used).
 // ---------------------------------------------------------------------------
-constexpr int RB_PD = 6;              // prefetch distance in planes (covers DRAM latency)
-constexpr int RB_NS = RB_PD + 2;      // stages: planes k-1 .. k+RB_PD
+constexpr int RB_PD = 4;          // prefetch distance in planes
+constexpr int RB_NS = RB_PD + 2;  // stages: planes k-1 .. k+RB_PD
+
+template <typename T>
+struct RbShape {
+  static constexpr int W = (33 * (int)sizeof(T) + 15) / 16 * 16 / (int)sizeof(T);  // box width: 33 used
+  static constexpr int OE = (RB_RJ + 2) * W, RE = RB_RJ * W;                        // elements per box
+  static constexpr int OB = (OE * (int)sizeof(T) + 127) / 128 * 128;                // bytes per stage slot
+  static constexpr int RBY = (RE * (int)sizeof(T) + 127) / 128 * 128;
+};
 
 template <typename T, bool FROM_ZERO>
 __global__ void __launch_bounds__(RB_TX *RB_RJ) k_rbgs(const BlkLev *__restrict__ bl, const Tile *__restrict__ tiles,
-                                                       const int *__restrict__ act, int colour) {
-  __shared__ T so[RB_NS][RB_RJ + 2][RB_TX + 2];
-  __shared__ T sr[RB_NS][RB_RJ][RB_TX];
+                                                       const int *__restrict__ act, int colour, int kch,
+                                                       int *__restrict__ err) {
+  using S = RbShape<T>;
+  constexpr int W = S::W;
+  constexpr int OB = FROM_ZERO ? 0 : S::OB;
+  __shared__ __align__(128) unsigned char sbuf[RB_NS * (OB + S::RBY)];
+  __shared__ __align__(8) uint64_t bar[RB_NS];
   const Tile t = tiles[blockIdx.x];
   const BlkLev B = bl[t.blk];
   if (!act[B.dom]) return;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RB_TX + tx;
-  const int h = t.i0 + tx, j = t.j0 + ty;
-  const int hp = B.hp, ny = B.ny;
-  const long long rs = (long long)(ny + 2) * hp;  // plane stride
-  const T *__restrict__ O = phi_of<T>(B) + (1 - colour) * B.cstr;
+  const int q0 = t.i0, q = q0 + tx, j = t.j0 + ty;
+  const int nx = B.nx, ny = B.ny;
+  const long long rs = (long long)(ny + 2) * B.hp;  // plane stride
   T *__restrict__ M = phi_of<T>(B) + colour * B.cstr;
-  const T *__restrict__ R = rhs_of<T>(B) + colour * B.cstr;
+  const CUtensorMap *mo = B.tm + (1 - colour), *mr = B.tm + 2 + colour;
   const Coef<T> cf(B);
-  const int k0 = t.k0, k1 = min(t.k0 + RB_KCH - 1, B.nz);
+  const int k0 = t.k0, k1 = min(t.k0 + kch - 1, B.nz);
   const bool jin = j <= ny;
+  // coefficients of this lane's two cells (s = 0: i = 2q+2; s = 1: i = 2q+1)
+  const int ia = min(2 * q + 2, nx + 1), ib = min(2 * q + 1, nx + 1);
+  const T aw0 = cf.aw[ia], ae0 = cf.ae[ia], aw1 = cf.aw[ib], ae1 = cf.ae[ib];
   const T as = jin ? cf.as[j] : (T)0, an = jin ? cf.an[j] : (T)0;
-  // stage the tiles of plane kk (other colour with halo, rhs when kk is computed)
+  // ap = -1*(aw+ae+as+an+ab+at) summed left to right: the first four terms per lane
+  const T pa0 = ((aw0 + ae0) + as) + an, pa1 = ((aw1 + ae1) + as) + an;
+  auto slot_o = [&](int st) { return (T *)(sbuf + st * OB); };
+  auto slot_r = [&](int st) { return (T *)(sbuf + RB_NS * OB + st * S::RBY); };
+  auto loads = [&](int kk) { return FROM_ZERO ? (kk >= k0 && kk <= k1) : (kk >= k0 - 1 && kk <= k1 + 1); };
+  // the loaded planes are consecutive from slot 0, so each slot's phases
+  // complete in order (k0-1 is loaded unless FROM_ZERO)
+  constexpr int first = FROM_ZERO ? 0 : 1;
+  auto stage = [&](int kk) { return (kk - k0 + first) % RB_NS; };
+  auto parity = [&](int kk) { return (unsigned)(((kk - k0 + first) / RB_NS) & 1); };
   auto issue = [&](int kk) {
-    const int st = (kk - k0 + 1) % RB_NS;
-    const long long pk = (long long)kk * rs;
-    if (!FROM_ZERO) {
-      for (int e = tid; e < (RB_RJ + 2) * (RB_TX + 2); e += RB_TX * RB_RJ) {
-        const int r = e / (RB_TX + 2), c = e - r * (RB_TX + 2);
-        const int jj = t.j0 - 1 + r, hh = t.i0 - 1 + c;
-        if (jj <= ny + 1 && hh >= 0 && hh < hp) cp_async_elem(&so[st][r][c], O + pk + (long long)jj * hp + hh);
-      }
-    }
-    if (kk >= k0 && kk <= k1 && jin && h < hp) cp_async_elem(&sr[st][ty][tx], R + pk + (long long)j * hp + h);
+    const int st = stage(kk);
+    const bool wr = kk >= k0 && kk <= k1;
+    const unsigned bytes = (FROM_ZERO ? 0u : (unsigned)(S::OE * sizeof(T))) + (wr ? (unsigned)(S::RE * sizeof(T)) : 0u);
+    mbar_expect_tx(&bar[st], bytes);
+    if (!FROM_ZERO) tma_load_3d(slot_o(st), mo, &bar[st], q0, t.j0 - 1, kk);
+    if (wr) tma_load_3d(slot_r(st), mr, &bar[st], q0, t.j0, kk);
   };
-  // prologue: planes k0-1 .. k0+RB_PD-1, one commit group each
-  for (int kk = k0 - 1; kk < k0 + RB_PD; ++kk) {
-    if (kk <= k1 + 1 && (kk >= k0 || !FROM_ZERO)) issue(kk);
-    cp_async_commit();
+  __shared__ int abort_s;  // set when a wait gave up: every thread leaves after the next barrier
+  if (tid == 0) {
+    for (int st = 0; st < RB_NS; ++st) mbar_init(&bar[st], 1);
+    mbar_fence_init();
+    abort_s = 0;
   }
+  __syncthreads();
+  if (tid == 0)
+    for (int kk = k0 - 1; kk < k0 + RB_PD; ++kk)
+      if (loads(kk)) issue(kk);
+  bool ok = true;
+  if (loads(k0 - 1)) ok = mbar_wait(&bar[stage(k0 - 1)], parity(k0 - 1), err);
+  if (ok) ok = mbar_wait(&bar[stage(k0)], parity(k0), err);
   for (int k = k0; k <= k1; ++k) {
-    if (k + RB_PD <= k1 + 1) issue(k + RB_PD);
-    cp_async_commit();
-    cp_async_wait<RB_PD - 1>();  // planes up to k+1 have landed; RB_PD-1 newer groups in flight
-    __syncthreads();
+    if (tid == 0 && ok && loads(k + RB_PD)) issue(k + RB_PD);  // refills the slot of plane k-2
+    if (ok && !FROM_ZERO) ok = mbar_wait(&bar[stage(k + 1)], parity(k + 1), err);
+    if (ok && FROM_ZERO && k > k0) ok = mbar_wait(&bar[stage(k)], parity(k), err);
     const int s = (colour + j + k + 1) & 1;
-    const int i = 2 * h + s;
-    if (jin && h < hp && i >= 1 && i <= B.nx) {
-      const int st = (k - k0 + 1) % RB_NS;
+    const int i = 2 * q + 2 - s;
+    if (ok && jin && i <= nx) {
+      const int st = stage(k), hc = tx + 1 - s;
       T w = (T)0, e = (T)0, so_ = (T)0, no = (T)0, bo = (T)0, to = (T)0;
       if (!FROM_ZERO) {
-        const int stb = (k - k0) % RB_NS, stt = (k - k0 + 2) % RB_NS;
-        w = so[st][ty + 1][tx + s];
-        e = so[st][ty + 1][tx + 1 + s];
-        so_ = so[st][ty][tx + 1];
-        no = so[st][ty + 2][tx + 1];
-        bo = so[stb][ty + 1][tx + 1];
-        to = so[stt][ty + 1][tx + 1];
+        const T *o = slot_o(st), *ob = slot_o(stage(k - 1)), *ot = slot_o(stage(k + 1));
+        w = o[(ty + 1) * W + tx];
+        e = o[(ty + 1) * W + tx + 1];
+        so_ = o[ty * W + hc];
+        no = o[(ty + 2) * W + hc];
+        bo = ob[(ty + 1) * W + hc];
+        to = ot[(ty + 1) * W + hc];
       }
-      const T aw = cf.aw[i], ae = cf.ae[i];
       const T ab = cf.ab[k], at = cf.at[k];
-      const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-      const T r = sr[st][ty][tx];
-      M[(long long)k * rs + (long long)j * hp + h] =
+      const T aw = s ? aw1 : aw0, ae = s ? ae1 : ae0;
+      const T ap = (T)-1.0 * (((s ? pa1 : pa0) + ab) + at);
+      const T r = slot_r(st)[ty * W + hc];
+      M[(long long)k * rs + (long long)j * B.hp + q0 + hc] =
           ((r - (aw * w + ae * e + as * so_ + an * no + ab * bo + at * to)) / ap);
     }
-    __syncthreads();  // the stage of plane k-1 is refilled next iteration
+    if (!ok) abort_s = 1;
+    __syncthreads();  // plane k-1's slot is refilled next iteration
+    if (abort_s) return;
   }
-  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------

@@ -23,6 +23,8 @@
 #include <unordered_set>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "kernels.cuh"
 #include "mf3d_internal.h"
 #include "outer.cuh"
@@ -113,8 +115,38 @@ static double pow2_inverse(double h) {
 // ---------------------------------------------------------------------------
 struct LevelStore {
   DevBuf<char> phi, rhs, coef, geo;
+  DevBuf<CUtensorMap> tmaps;  // phi c0, phi c1, rhs c0, rhs c1
   BlkLev desc;  // host copy with device pointers
 };
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }();
+  return fn;
+}
+
+// A 3-D map over one colour array [nz+2][ny+2][hp] with a (W x rows x 1) box.
+static int colour_map(CUtensorMap *m, void *base, int elem, const BlkLev &B, int W, int rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc) { set_error("cuTensorMapEncodeTiled unavailable"); return MF3D_E_CUDA; }
+  const cuuint64_t dims[3] = {(cuuint64_t)B.hp, (cuuint64_t)(B.ny + 2), (cuuint64_t)(B.nz + 2)};
+  const cuuint64_t strides[2] = {(cuuint64_t)B.hp * elem, (cuuint64_t)B.hp * (B.ny + 2) * elem};
+  const cuuint32_t box[3] = {(cuuint32_t)W, (cuuint32_t)rows, 1u};
+  const cuuint32_t es[3] = {1u, 1u, 1u};
+  const CUresult r = enc(m, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
+                         dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r)); return MF3D_E_CUDA; }
+  return MF3D_OK;
+}
 
 struct BlockStore {
   mf3d_block_desc d;     // neighbour ids refer to blocks of the same domain
@@ -152,7 +184,7 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
     B.nx = d.nx >> (g - 1);
     B.ny = d.ny >> (g - 1);
     B.nz = d.nz >> (g - 1);
-    B.hp = hp_of(B.nx);
+    B.hp = hp_of(B.nx, elem);
     B.cstr = (long long)(B.nz + 2) * (B.ny + 2) * B.hp;
     B.cstr = (B.cstr + 31) / 32 * 32;  // 256-byte aligned colour arrays
     B.nmask = nmask;
@@ -211,6 +243,17 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
     B.rhs = L.rhs.p;
     B.coef = L.coef.p;
     B.geo = L.geo.p;
+    // TMA maps of the sweep (colour arrays start 256-byte aligned, rows 16-byte multiples)
+    CUtensorMap tm[4];
+    const int W = elem == 8 ? RbShape<double>::W : RbShape<float>::W;
+    for (int c = 0; c < 2; ++c) {
+      if ((st = colour_map(&tm[c], L.phi.p + (size_t)c * B.cstr * elem, elem, B, W, RB_RJ + 2))) return st;
+      if ((st = colour_map(&tm[2 + c], L.rhs.p + (size_t)c * B.cstr * elem, elem, B, W, RB_RJ))) return st;
+    }
+    if ((st = L.tmaps.alloc(4))) return st;
+    CK(cudaMemcpyAsync(L.tmaps.p, tm, sizeof tm, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // tm is a local
+    B.tm = L.tmaps.p;
   }
   // level-1 field geometry: widths, face distances (bit-exact dx on a uniform axis)
   std::vector<double> g1;
@@ -327,6 +370,7 @@ struct ViewLevel {
   DevBuf<BlkLev> tab;                 // one entry per view block (absent: nx = 0)
   DevBuf<Tile> sweep[3], cells[3];
   int n_sweep[3] = {0, 0, 0}, n_cells[3] = {0, 0, 0};
+  int kch[3] = {1, 1, 1};             // planes per sweep CTA
   DevBuf<int> list[3];
   int n_list[3] = {0, 0, 0};
   DevBuf<HaloCopy> halo[3];
@@ -348,6 +392,7 @@ struct View {
   int n_int = 0, n_zint = 0, n_l1cells = 0, n_faces = 0, n_planes = 0;
   DevBuf<DomState> ds;
   DevBuf<int> act, ones;
+  DevBuf<int> err;                    // device error code (a TMA wait that gave up)
   DevBuf<unsigned long long> rmax, rmax_scratch;
   DevBuf<double> hist;
   int hcap = 0;
@@ -377,6 +422,8 @@ struct mf3d_ctx {
   mf3d_params prm;
   int device = 0;
   int elem = 8;
+  int nsm = 148;            // SMs of the device
+  int sweep_occ = 4;        // resident sweep CTAs per SM
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long long launches = 0;
@@ -425,6 +472,33 @@ static void prof_collect(mf3d_ctx *C) {
   C->prof_pending_bytes.clear();
 }
 
+// Red-black sweep tiles of a set of blocks: 32 lanes over q (ceil(nx/2) per
+// row), RB_RJ rows, kch planes.  kch is chosen so the CTAs fill the SMs in
+// few waves: the estimated time ceil(CTAs / resident) * (kch + pipeline
+// fill) is minimised over kch in {2, 4, 8, 16, 32}.
+static int sweep_tiles(const mf3d_ctx *C, const std::vector<BlkLev> &tab, const std::vector<int> &blocks,
+                       std::vector<Tile> &out) {
+  out.clear();
+  if (blocks.empty()) return 1;
+  const long long resident = (long long)C->nsm * C->sweep_occ;
+  int best = 2;
+  double best_cost = 1e300;
+  for (int kch : {2, 4, 8, 16, 32}) {
+    long long n = 0;
+    for (int b : blocks) {
+      const BlkLev &B = tab[b];
+      n += (long long)((B.nx + 1) / 2 + RB_TX - 1) / RB_TX * ((B.ny + RB_RJ - 1) / RB_RJ) * ((B.nz + kch - 1) / kch);
+    }
+    const double cost = (double)((n + resident - 1) / resident) * (kch + RB_PD);
+    if (cost <= best_cost) { best_cost = cost; best = kch; }
+  }
+  for (int b : blocks) {
+    const BlkLev &B = tab[b];
+    add_tiles_2d(out, b, Box{0, (B.nx + 1) / 2 - 1, 1, B.ny, 1, B.nz}, RB_TX, RB_RJ, best);
+  }
+  return best;
+}
+
 // Build the launch tables of a view over `doms` (all of one precision).
 static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &doms, int hcap) {
   cudaStream_t s = C->stream;
@@ -448,7 +522,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
     ViewLevel &L = V.lv[g];
     std::vector<BlkLev> tab(nb);
     std::vector<Tile> sw[3], ce[3];
-    std::vector<int> li[3];
+    std::vector<int> li[3], sblk[3];
     for (int b = 0; b < nb; ++b) {
       const BlockStore &S = *V.blk[b];
       BlkLev B;
@@ -458,10 +532,9 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       tab[b] = B;
       if (g > S.ngrid) continue;
       const int sub_extra = (g == S.ngrid) ? SUB_C : SUB_D;
-      const Box bsw{0, B.hp - 1, 1, B.ny, 1, B.nz};
       const Box bce{0, B.nx + 1, 0, B.ny + 1, 0, B.nz + 1};
       for (int q : {(int)SUB_A, sub_extra}) {
-        add_tiles_2d(sw[q], b, bsw, RB_TX, RB_RJ, RB_KCH);
+        sblk[q].push_back(b);
         add_tiles_2d(ce[q], b, bce, RW_TX, RW_RJ, RW_KCH);
         li[q].push_back(b);
         L.cells_sub[q] += (long long)B.nx * B.ny * B.nz;
@@ -470,6 +543,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
     }
     if ((st = L.tab.upload(tab, s))) return st;
     for (int q = 0; q < 3; ++q) {
+      L.kch[q] = sweep_tiles(C, tab, sblk[q], sw[q]);
       L.n_sweep[q] = (int)sw[q].size();
       L.n_cells[q] = (int)ce[q].size();
       L.n_list[q] = (int)li[q].size();
@@ -539,6 +613,8 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
   if ((st = V.ds.alloc(std::max(nd, 1)))) return st;
   if ((st = V.act.upload(ones, s))) return st;
   if ((st = V.ones.upload(ones, s))) return st;
+  if ((st = V.err.alloc(1))) return st;
+  CK(cudaMemsetAsync(V.err.p, 0, sizeof(int), s));
   if ((st = V.rmax.alloc(std::max(nd, 1)))) return st;
   if ((st = V.rmax_scratch.alloc(std::max(nd, 1)))) return st;
   CK(cudaMemsetAsync(V.rmax.p, 0, V.rmax.n * sizeof(unsigned long long), s));
@@ -579,13 +655,14 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
       const double half = 0.5 * (double)L.cells_sub[q] * sizeof(T);
       const bool fz = from_zero && itr == 0;
       prof_begin(C, pk, (fz ? 2 : 3) * half);
+      const dim3 grid(L.n_sweep[q]), cta(RB_TX, RB_RJ);
       if (fz)
-        k_rbgs<T, true><<<L.n_sweep[q], dim3(RB_TX, RB_RJ), 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0);
+        k_rbgs<T, true><<<grid, cta, 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
       else
-        k_rbgs<T, false><<<L.n_sweep[q], dim3(RB_TX, RB_RJ), 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0);
+        k_rbgs<T, false><<<grid, cta, 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
       prof_end(C, pk);
       prof_begin(C, pk, 3 * half);
-      k_rbgs<T, false><<<L.n_sweep[q], dim3(RB_TX, RB_RJ), 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 1);
+      k_rbgs<T, false><<<grid, cta, 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 1, L.kch[q], V.err.p);
       prof_end(C, pk);
       C->launches += 2;
     } else if (sch == 1) {
@@ -758,11 +835,23 @@ static int solve_end(mf3d_ctx *C, View &V) {
   return MF3D_OK;
 }
 
+// A kernel that gave up waiting (a TMA copy that never landed) leaves its
+// code in V.err; the results of that call are not valid.
+static int check_device_error(View &V) {
+  int e = 0;
+  CK(cudaMemcpy(&e, V.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e == 0) return MF3D_OK;
+  CK(cudaMemset(V.err.p, 0, sizeof(int)));
+  set_error("a device copy did not complete within its time limit (code " + std::to_string(e) + ")");
+  return MF3D_E_TIMEOUT;
+}
+
 // Fold the device state of every domain into the caller's infos/history.
 static int collect(mf3d_ctx *C, View &V, mf3d_solve_info *infos, double *hist, int hcap, float ms) {
   const int nd = (int)V.dom.size();
   std::vector<DomState> hs(nd);
   CK(cudaMemcpy(hs.data(), V.ds.p, nd * sizeof(DomState), cudaMemcpyDeviceToHost));
+  if (int st = check_device_error(V)) return st;
   int worst = MF3D_OK;
   for (int d = 0; d < nd; ++d) {
     const DomState &D = hs[d];
@@ -850,7 +939,7 @@ static int mgkcyc_view(mf3d_ctx *C, View &V, double *const *su, double *const *p
   C->launches += 3;
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
-  return MF3D_OK;
+  return check_device_error(V);
 }
 
 static size_t ttc_elems(int pl, const mf3d_block_desc &d) {
@@ -880,6 +969,11 @@ static int ctx_init(mf3d_ctx *C, const mf3d_params *prm) {
   CK(cudaEventCreate(&C->ev1));
   const char *e = getenv("MF3D_NO_GRAPH");
   C->use_graph = !(e && e[0] == '1');
+  CK(cudaDeviceGetAttribute(&C->nsm, cudaDevAttrMultiProcessorCount, C->device));
+  int occ = 0;
+  if (C->elem == 8) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rbgs<double, false>, RB_TX * RB_RJ, 0));
+  else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rbgs<float, false>, RB_TX * RB_RJ, 0));
+  C->sweep_occ = std::max(occ, 1);
   return MF3D_OK;
 }
 
