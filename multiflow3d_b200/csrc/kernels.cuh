@@ -365,54 +365,76 @@ __global__ void k_tdma(const BlkLev *__restrict__ bl, const int *__restrict__ bl
 }
 
 // ---------------------------------------------------------------------------
-// Residual + restriction (mgrestr, mgsolver.for:619-761), one thread per
-// coarse cell including its ghost shell: coarse phi := 0 everywhere
-// (:650-657); interior coarse rhs := 0.125 * sum over the 8 children of
-// s * (rhs - (aw*w + ae*e + as*s + an*n + ab*b + at*t + ap*p)) in the
-// reference's child order (:743-747).  s = 8*rx*ry*rz is the volume weight
-// of the non-uniform-grid extension and is exactly 1.0 on a uniform grid.
+// Residual + restriction (mgrestr, mgsolver.for:619-761): coarse phi := 0
+// everywhere (:650-657); interior coarse rhs := 0.125 * sum over the 8
+// children of s * (rhs - (aw*w + ae*e + as*s + an*n + ab*b + at*t + ap*p))
+// in the reference's child order (:743-747).  s = 8*rx*ry*rz is the volume
+// weight of the non-uniform-grid extension and is exactly 1.0 on a uniform
+// grid.  One thread per coarse column (I, J) of the ghost-inclusive plane -
+// lanes run over I, so the children (fine i = 2I-1, 2I at compact I-1, I)
+// of neighbouring lanes are neighbouring elements of both colour arrays -
+// marching up `kch` coarse planes.  x and y coefficients are held per thread.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ inline T residual_at(const BlkLev &F, const Coef<T> &cf, int i, int j, int k) {
-  const T *P = phi_of<T>(F);
-  const T aw = cf.aw[i], ae = cf.ae[i], as = cf.as[j], an = cf.an[j], ab = cf.ab[k], at = cf.at[k];
-  const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-  const T pw = P[cell_off(F, i - 1, j, k)], pe = P[cell_off(F, i + 1, j, k)];
-  const T ps = P[cell_off(F, i, j - 1, k)], pn = P[cell_off(F, i, j + 1, k)];
-  const T pb = P[cell_off(F, i, j, k - 1)], pt = P[cell_off(F, i, j, k + 1)];
-  const T pp = P[cell_off(F, i, j, k)];
-  const T r = rhs_of<T>(F)[cell_off(F, i, j, k)];
-  return r - (aw * pw + ae * pe + as * ps + an * pn + ab * pb + at * pt + ap * pp);
-}
-
 template <typename TF, typename TC>
-__global__ void __launch_bounds__(RW_TX *RW_RJ) k_restrict(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
-                                                           const Tile *__restrict__ tiles, const int *__restrict__ act) {
+__global__ void __launch_bounds__(kTile, 2) k_restrict(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
+                                                      const Tile *__restrict__ tiles, const int *__restrict__ act,
+                                                      int kch) {
   const Tile t = tiles[blockIdx.x];
   const BlkLev Cb = cl[t.blk];
   if (!act[Cb.dom]) return;
+  const int GX = Cb.nx + 2, GY = Cb.ny + 2;
+  const int g = t.i0 + threadIdx.x;
+  if (g >= GX * GY) return;
+  const int J = g / GX, I = g - J * GX;
   const BlkLev Fb = fl[t.blk];
-  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
-  if (i > Cb.nx + 1 || j > Cb.ny + 1) return;
+  TC *__restrict__ PC = phi_of<TC>(Cb);
+  TC *__restrict__ RC = rhs_of<TC>(Cb);
+  const TF *__restrict__ P = phi_of<TF>(Fb);
+  const TF *__restrict__ R = rhs_of<TF>(Fb);
   const Coef<TF> cf(Fb);
-  // restriction ratios of the fine level: rx[nxf+2], ry[nyf+2], rz[nzf+2]
   const TF *rx = (const TF *)Fb.geo, *ry = rx + (Fb.nx + 2), *rz = ry + (Fb.ny + 2);
-  const bool inij = i >= 1 && i <= Cb.nx && j >= 1 && j <= Cb.ny;
-  const int k1 = min(t.k0 + RW_KCH - 1, Cb.nz + 1);
-  for (int k = t.k0; k <= k1; ++k) {
-    phi_of<TC>(Cb)[cell_off(Cb, i, j, k)] = (TC)0;
-    if (!inij || k < 1 || k > Cb.nz) continue;
-    TF acc[8];
-    int n = 0;
-    for (int dk = 0; dk < 2; ++dk)
+  const bool inij = I >= 1 && I <= Cb.nx && J >= 1 && J <= Cb.ny;
+  const int Ic = inij ? I : 1, Jc = inij ? J : 1;  // in-bounds indices for the per-thread loads
+  TF aw[2], ae[2], sx[2], as[2], an[2], sy[2];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    const int fi = 2 * Ic - 1 + d, fj = 2 * Jc - 1 + d;
+    aw[d] = cf.aw[fi]; ae[d] = cf.ae[fi]; sx[d] = rx[fi];
+    as[d] = cf.as[fj]; an[d] = cf.an[fj]; sy[d] = ry[fj];
+  }
+  const long long cs = Fb.cstr, rowf = Fb.hp, plf = (long long)(Fb.ny + 2) * Fb.hp;
+  // fine element of (i, j, k): colour (i+j+k+1)&1, compact i>>1
+  auto fo = [&](int i, int j, int k) -> long long {
+    return ((i + j + k + 1) & 1) * cs + k * plf + j * rowf + (i >> 1);
+  };
+  const int K1 = min(t.k0 + kch - 1, Cb.nz + 1);
+  for (int K = t.k0; K <= K1; ++K) {
+    PC[cell_off(Cb, I, J, K)] = (TC)0;
+    if (!inij || K < 1 || K > Cb.nz) continue;
+    TF sum = (TF)0;  // acc0 + acc1 + ... + acc7, folded left to right as it is formed
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk) {
+      const int fk = 2 * K - 1 + dk;
+      const TF ab = cf.ab[fk], at = cf.at[fk], sz = rz[fk];
+#pragma unroll
       for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
         for (int di = 0; di < 2; ++di) {
-          const int fi = 2 * i - 1 + di, fj = 2 * j - 1 + dj, fk = 2 * k - 1 + dk;
-          const TF s = (TF)8.0 * rx[fi] * ry[fj] * rz[fk];
-          acc[n++] = residual_at<TF>(Fb, cf, fi, fj, fk) * s;
+          const int fi = 2 * I - 1 + di, fj = 2 * J - 1 + dj;
+          const TF ap = (TF)-1.0 * (aw[di] + ae[di] + as[dj] + an[dj] + ab + at);
+          const TF pw = P[fo(fi - 1, fj, fk)], pe = P[fo(fi + 1, fj, fk)];
+          const TF ps = P[fo(fi, fj - 1, fk)], pn = P[fo(fi, fj + 1, fk)];
+          const TF pb = P[fo(fi, fj, fk - 1)], pt = P[fo(fi, fj, fk + 1)];
+          const TF pp = P[fo(fi, fj, fk)];
+          const TF r = R[fo(fi, fj, fk)];
+          const TF res = r - (aw[di] * pw + ae[di] * pe + as[dj] * ps + an[dj] * pn + ab * pb + at * pt + ap * pp);
+          const TF s = (TF)8.0 * sx[di] * sy[dj] * sz;
+          const TF a = res * s;
+          sum = (dk | dj | di) ? sum + a : a;
         }
-    const TF v = (TF)0.125 * (acc[0] + acc[1] + acc[2] + acc[3] + acc[4] + acc[5] + acc[6] + acc[7]);
-    rhs_of<TC>(Cb)[cell_off(Cb, i, j, k)] = (TC)v;
+    }
+    const TF v = (TF)0.125 * sum;
+    RC[cell_off(Cb, I, J, K)] = (TC)v;
   }
 }
 
@@ -420,62 +442,86 @@ __global__ void __launch_bounds__(RW_TX *RW_RJ) k_restrict(const BlkLev *__restr
 // Prolongation + correction + Neumann ghosts (mgcorr, mgsolver.for:763-905,
 // then mgbound :902).  Every fine cell, ghosts included, adds the trilinear
 // (27,9,3,1)/64 interpolant of the coarse correction, summed in the
-// reference's term order (:833-887).  A fine cell on a Neumann face of the
-// block then also writes its corrected value into the ghost cells that
-// mgbound copies it to, so no cell is read after another thread wrote it.
+// reference's term order (:833-887); a Neumann ghost then takes the value
+// of the interior cell mgbound copies into it (W,E,S,N,B,T in order
+// composes to a clamp of the index).
+// One thread per fine group (2I..2I+1) x (2J..2J+1) x (2K..2K+1): the group
+// shares its 8 coarse cells (I..I+1, J..J+1, K..K+1), its 8 fine cells sit
+// at compact index I of both colour arrays (consecutive across lanes), and
+// a Neumann ghost's mirror cell is in the same group.  Threads march up
+// `kch` coarse planes carrying the upper coarse plane.
 // ---------------------------------------------------------------------------
 template <typename TF, typename TC>
-__global__ void __launch_bounds__(RW_TX *RW_RJ) k_prolong(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
-                                                          const Tile *__restrict__ tiles, const int *__restrict__ act) {
+__global__ void __launch_bounds__(kTile) k_prolong(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
+                                                   const Tile *__restrict__ tiles, const int *__restrict__ act,
+                                                   int kch) {
   const Tile t = tiles[blockIdx.x];
   const BlkLev Fb = fl[t.blk];
   if (!act[Fb.dom]) return;
   const BlkLev Cb = cl[t.blk];
-  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
-  if (i > Fb.nx + 1 || j > Fb.ny + 1) return;
+  const int GX = Cb.nx + 1, GY = Cb.ny + 1;
+  const int g = t.i0 + threadIdx.x;
+  if (g >= GX * GY) return;
+  const int J = g / GX, I = g - J * GX;
   const int m = Fb.nmask;
-  // Neumann ghost cells are written by their owners below
-  if ((i == 0 && (m & 1)) || (i == Fb.nx + 1 && (m & 2)) || (j == 0 && (m & 4)) || (j == Fb.ny + 1 && (m & 8))) return;
+  // the member of the pair that is a Neumann ghost copies its partner
+  const bool xw = I == 0 && (m & 1), xe = I == Cb.nx && (m & 2);
+  const bool ys = J == 0 && (m & 4), yn = J == Cb.ny && (m & 8);
   const TC *__restrict__ PC = phi_of<TC>(Cb);
   TF *__restrict__ PF = phi_of<TF>(Fb);
-  const int k1 = min(t.k0 + RW_KCH - 1, Fb.nz + 1);
-#pragma unroll 2
-  for (int k = t.k0; k <= k1; ++k) {
-  if ((k == 0 && (m & 16)) || (k == Fb.nz + 1 && (m & 32))) continue;
-  const int ic = i >> 1, jc = j >> 1, kc = k >> 1;        // lower coarse cell
-  const int wi0 = (i & 1) ? 1 : 3, wj0 = (j & 1) ? 1 : 3, wk0 = (k & 1) ? 1 : 3;
-  const int wi1 = 4 - wi0, wj1 = 4 - wj0, wk1 = 4 - wk0;
-  const TF c000 = (TF)PC[cell_off(Cb, ic, jc, kc)];
-  const TF c010 = (TF)PC[cell_off(Cb, ic, jc + 1, kc)];
-  const TF c001 = (TF)PC[cell_off(Cb, ic, jc, kc + 1)];
-  const TF c011 = (TF)PC[cell_off(Cb, ic, jc + 1, kc + 1)];
-  const TF c100 = (TF)PC[cell_off(Cb, ic + 1, jc, kc)];
-  const TF c110 = (TF)PC[cell_off(Cb, ic + 1, jc + 1, kc)];
-  const TF c101 = (TF)PC[cell_off(Cb, ic + 1, jc, kc + 1)];
-  const TF c111 = (TF)PC[cell_off(Cb, ic + 1, jc + 1, kc + 1)];
-  const TF corr = ((TF)(wi0 * wj0 * wk0) * c000 + (TF)(wi0 * wj1 * wk0) * c010 + (TF)(wi0 * wj0 * wk1) * c001 +
-                   (TF)(wi0 * wj1 * wk1) * c011 + (TF)(wi1 * wj0 * wk0) * c100 + (TF)(wi1 * wj1 * wk0) * c110 +
-                   (TF)(wi1 * wj0 * wk1) * c101 + (TF)(wi1 * wj1 * wk1) * c111) *
-                  (TF)0.015625;  // x/64 == x*2^-6 exactly in IEEE arithmetic
-  const long long a = cell_off(Fb, i, j, k);
-  const TF v = PF[a] + corr;
-  PF[a] = v;
-  // mirror targets on Neumann faces (mgbound order W,E,S,N,B,T composes to a clamp)
-  int xs[3] = {i, i, i}, ys[3] = {j, j, j}, zs[3] = {k, k, k};
-  int nxo = 1, nyo = 1, nzo = 1;
-  if (i == 1 && (m & 1)) xs[nxo++] = 0;
-  if (i == Fb.nx && (m & 2)) xs[nxo++] = Fb.nx + 1;
-  if (j == 1 && (m & 4)) ys[nyo++] = 0;
-  if (j == Fb.ny && (m & 8)) ys[nyo++] = Fb.ny + 1;
-  if (k == 1 && (m & 16)) zs[nzo++] = 0;
-  if (k == Fb.nz && (m & 32)) zs[nzo++] = Fb.nz + 1;
-  if (nxo == 1 && nyo == 1 && nzo == 1) continue;
-  for (int a3 = 0; a3 < nzo; ++a3)
-    for (int a2 = 0; a2 < nyo; ++a2)
-      for (int a1 = 0; a1 < nxo; ++a1) {
-        if (a1 == 0 && a2 == 0 && a3 == 0) continue;
-        PF[cell_off(Fb, xs[a1], ys[a2], zs[a3])] = v;
-      }
+  const long long csf = Fb.cstr, rowf = Fb.hp, plf = (long long)(Fb.ny + 2) * Fb.hp;
+  auto coarse = [&](int a, int b, int c) -> TF { return (TF)PC[cell_off(Cb, I + a, J + b, c)]; };
+  const int K1 = min(t.k0 + kch - 1, Cb.nz);
+  TF lo[2][2];  // [a][b] at coarse plane K
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) lo[a][b] = coarse(a, b, t.k0);
+  for (int K = t.k0; K <= K1; ++K) {
+    TF hi[2][2];  // [a][b] at coarse plane K+1
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) hi[a][b] = coarse(a, b, K + 1);
+    const bool zb = K == 0 && (m & 16), zt = K == Cb.nz && (m & 32);
+    TF v[2][2][2];  // [dk][dj][di]
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+        for (int di = 0; di < 2; ++di) {
+          // weight of coarse (a,b,c): 3 along an axis where the child sits in that cell, else 1
+          auto w = [&](int a, int b, int c) -> TF {
+            return (TF)((a == di ? 3 : 1) * (b == dj ? 3 : 1) * (c == dk ? 3 : 1));
+          };
+          const TF corr = (w(0, 0, 0) * lo[0][0] + w(0, 1, 0) * lo[0][1] + w(0, 0, 1) * hi[0][0] +
+                           w(0, 1, 1) * hi[0][1] + w(1, 0, 0) * lo[1][0] + w(1, 1, 0) * lo[1][1] +
+                           w(1, 0, 1) * hi[1][0] + w(1, 1, 1) * hi[1][1]) *
+                          (TF)0.015625;  // x/64 == x*2^-6 exactly in IEEE arithmetic
+          const long long o = ((di + dj + dk + 1) & 1) * csf + (2 * K + dk) * plf + (2 * J + dj) * rowf + I;
+          v[dk][dj][di] = PF[o] + corr;
+        }
+#pragma unroll
+    for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+      for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+        for (int di = 0; di < 2; ++di) {
+          const int si = (di == 0 && xw) ? 1 : (di == 1 && xe) ? 0 : di;
+          const int sj = (dj == 0 && ys) ? 1 : (dj == 1 && yn) ? 0 : dj;
+          const int sk = (dk == 0 && zb) ? 1 : (dk == 1 && zt) ? 0 : dk;
+          const long long o = ((di + dj + dk + 1) & 1) * csf + (2 * K + dk) * plf + (2 * J + dj) * rowf + I;
+          // v[sk][sj][si] by selects (constant register indices)
+          const TF a0 = si ? v[0][0][1] : v[0][0][0], a1 = si ? v[0][1][1] : v[0][1][0];
+          const TF a2 = si ? v[1][0][1] : v[1][0][0], a3 = si ? v[1][1][1] : v[1][1][0];
+          const TF b0 = sj ? a1 : a0, b1 = sj ? a3 : a2;
+          PF[o] = sk ? b1 : b0;
+        }
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) lo[a][b] = hi[a][b];
   }
 }
 

@@ -371,6 +371,8 @@ struct ViewLevel {
   DevBuf<Tile> sweep[3], cells[3];
   int n_sweep[3] = {0, 0, 0}, n_cells[3] = {0, 0, 0};
   int kch[3] = {1, 1, 1};             // planes per sweep CTA
+  DevBuf<Tile> rtile, ptile;          // restriction into this level (SUB_A); prolongation from the next (SUB_D)
+  int n_rtile = 0, n_ptile = 0, rkch = 1, pkch = 1;
   DevBuf<int> list[3];
   int n_list[3] = {0, 0, 0};
   DevBuf<HaloCopy> halo[3];
@@ -499,6 +501,30 @@ static int sweep_tiles(const mf3d_ctx *C, const std::vector<BlkLev> &tab, const 
   return best;
 }
 
+// Plane tiles of kTile consecutive columns of a GX x GY plane and kch planes
+// of K0..K1, per block; kch as for the sweep (few waves of resident CTAs).
+struct PlaneExt {
+  int blk, gx, gy, k0, k1;
+};
+static int plane_tiles(const mf3d_ctx *C, const std::vector<PlaneExt> &ext, std::vector<Tile> &out) {
+  out.clear();
+  if (ext.empty()) return 1;
+  const long long resident = (long long)C->nsm * 6;
+  int best = 2;
+  double best_cost = 1e300;
+  for (int kch : {2, 4, 8, 16}) {
+    long long n = 0;
+    for (const auto &e : ext)
+      n += ((long long)e.gx * e.gy + kTile - 1) / kTile * ((e.k1 - e.k0 + 1 + kch - 1) / kch);
+    const double cost = (double)((n + resident - 1) / resident) * (kch + 2);
+    if (cost <= best_cost) { best_cost = cost; best = kch; }
+  }
+  for (const auto &e : ext)
+    for (int k = e.k0; k <= e.k1; k += best)
+      for (long long q = 0; q < (long long)e.gx * e.gy; q += kTile) out.push_back(Tile{e.blk, k, 0, (int)q});
+  return best;
+}
+
 // Build the launch tables of a view over `doms` (all of one precision).
 static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &doms, int hcap) {
   cudaStream_t s = C->stream;
@@ -542,6 +568,24 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       L.ngg = std::max(L.ngg, std::max(B.nx, std::max(B.ny, B.nz)) + 2);
     }
     if ((st = L.tab.upload(tab, s))) return st;
+    {
+      // restriction into level g (g > 1): every block present here; prolongation
+      // from level g+1 into g: every block continuing down
+      std::vector<PlaneExt> re, pe;
+      for (int b = 0; b < nb; ++b) {
+        const BlkLev &B = tab[b];
+        if (g > V.blk[b]->ngrid) continue;
+        if (g > 1) re.push_back(PlaneExt{b, B.nx + 2, B.ny + 2, 0, B.nz + 1});
+        if (g < V.blk[b]->ngrid) pe.push_back(PlaneExt{b, B.nx / 2 + 1, B.ny / 2 + 1, 0, B.nz / 2});
+      }
+      std::vector<Tile> rt, pt;
+      L.rkch = plane_tiles(C, re, rt);
+      L.pkch = plane_tiles(C, pe, pt);
+      L.n_rtile = (int)rt.size();
+      L.n_ptile = (int)pt.size();
+      if ((st = L.rtile.upload(rt, s))) return st;
+      if ((st = L.ptile.upload(pt, s))) return st;
+    }
     for (int q = 0; q < 3; ++q) {
       L.kch[q] = sweep_tiles(C, tab, sblk[q], sw[q]);
       L.n_sweep[q] = (int)sw[q].size();
@@ -679,11 +723,10 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
 template <typename T>
 static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks continuing down
   ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
-  if (!Cl.n_cells[SUB_A]) return;
+  if (!Cl.n_rtile) return;
   const int pk = g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse out
-  k_restrict<T, T><<<Cl.n_cells[SUB_A], dim3(RW_TX, RW_RJ), 0, C->stream>>>(F.tab.p, Cl.tab.p, Cl.cells[SUB_A].p,
-                                                                           V.act.p);
+  k_restrict<T, T><<<Cl.n_rtile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch);
   prof_end(C, pk);
   ++C->launches;
 }
@@ -691,11 +734,10 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
 template <typename T>
 static void corr(mf3d_ctx *C, View &V, int g) {  // level g+1 -> g, blocks continuing down
   ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
-  if (!F.n_cells[SUB_D]) return;
+  if (!F.n_ptile) return;
   const int pk = g == 1 ? MF3D_PROF_PROLONG_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 1.0 / 8.0));  // fine in/out, coarse in
-  k_prolong<T, T><<<F.n_cells[SUB_D], dim3(RW_TX, RW_RJ), 0, C->stream>>>(F.tab.p, Cl.tab.p, F.cells[SUB_D].p,
-                                                                         V.act.p);
+  k_prolong<T, T><<<F.n_ptile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, F.ptile.p, V.act.p, F.pkch);
   prof_end(C, pk);
   ++C->launches;
 }
