@@ -133,6 +133,22 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
+// A 3-D map over one FP64 field in the reference's layout [tk][tj][ti] with
+// a (CV_W x rows x 1) box.
+static int field_map(CUtensorMap *m, const double *base, int ti, int tj, int tk, int rows) {
+  auto enc = tensor_map_encoder();
+  if (!enc) { set_error("cuTensorMapEncodeTiled unavailable"); return MF3D_E_CUDA; }
+  const cuuint64_t dims[3] = {(cuuint64_t)ti, (cuuint64_t)tj, (cuuint64_t)tk};
+  const cuuint64_t strides[2] = {(cuuint64_t)ti * 8, (cuuint64_t)ti * tj * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)CV_W, (cuuint32_t)rows, 1u};
+  const cuuint32_t es[3] = {1u, 1u, 1u};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void *)base, dims, strides, box, es,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r)); return MF3D_E_CUDA; }
+  return MF3D_OK;
+}
+
 // A 3-D map over one colour array [nz+2][ny+2][hp] with a (W x rows x 1) box.
 static int colour_map(CUtensorMap *m, void *base, int elem, const BlkLev &B, int W, int rows) {
   auto enc = tensor_map_encoder();
@@ -395,6 +411,8 @@ struct View {
   DevBuf<DomState> ds;
   DevBuf<int> act, ones;
   DevBuf<int> err;                    // device error code (a TMA wait that gave up)
+  DevBuf<CUtensorMap> fmaps;          // per block: p, ustar, vstar, wstar (bound fields)
+  bool fields_tma = false;            // bound fields admit the TMA calvel/calmas
   DevBuf<unsigned long long> rmax, rmax_scratch;
   DevBuf<double> hist;
   int hcap = 0;
@@ -770,6 +788,18 @@ static void vcycle(mf3d_ctx *C, View &V) {
   }
 }
 
+// Fused calvel + calmas over the view (the TMA-staged kernel when the bound
+// fields admit it).
+template <typename T>
+static void calvel_calmas(mf3d_ctx *C, View &V, const int *act, unsigned long long *slot, int write_su) {
+  if (V.fields_tma)
+    k_calvel_calmas_tma<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, C->stream>>>(V.df.p, V.t_zint.p, V.ds.p, act, slot,
+                                                                          write_su, OZ_KCH, V.err.p);
+  else
+    k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, C->stream>>>(V.df.p, V.t_zint.p, V.ds.p, act, slot,
+                                                                      write_su);
+}
+
 // One outer iteration of newsolv_mg (newsolv_mg.for:25-58) for every active
 // domain: V-cycle, p += pp, p halo + pbound, calvel + calmas, bookkeeping.
 template <typename T>
@@ -779,7 +809,7 @@ static void iteration_body(mf3d_ctx *C, View &V, bool loop_graph) {
   k_add_correction<T><<<V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_l1cells.p, V.act.p);
   k_p_faces<<<V.n_faces, kTile, 0, s>>>(V.df.p, V.t_faces.p, V.act.p);
   prof_begin(C, MF3D_PROF_CALMAS, (double)V.n_l1 * (4 * sizeof(double) + sizeof(T)));  // p, u*, v*, w* in; su out
-  k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, s>>>(V.df.p, V.t_zint.p, V.ds.p, V.act.p, V.rmax.p, 0);
+  calvel_calmas<T>(C, V, V.act.p, V.rmax.p, 0);
   prof_end(C, MF3D_PROF_CALMAS);
   k_iter_end<<<1, 256, 0, s>>>(V.ds.p, (int)V.dom.size(), V.rmax.p, V.hist.p, V.hcap, V.act.p, V.cond,
                                loop_graph ? 1 : 0);
@@ -830,6 +860,39 @@ static int bind_fields(mf3d_ctx *C, View &V, const mf3d_fields *f) {
       return MF3D_E_INVALID;
     }
   }
+  // TMA staging of p, ustar, vstar, wstar needs 16-byte aligned bases and rows
+  // of a multiple of 16 bytes (ttc_i even); otherwise the plain-load kernel runs
+  const size_t nb = V.blk.size();
+  bool tma = tensor_map_encoder() != nullptr;
+  for (size_t b = 0; b < nb && tma; ++b) {
+    const BlkFld &F = V.hf[b];
+    const double *fp[4] = {F.p, F.ustar, F.vstar, F.wstar};
+    tma = F.ti % 2 == 0;
+    for (const double *q : fp) tma = tma && ((uintptr_t)q % 16 == 0);
+  }
+  if (tma) {
+    std::vector<CUtensorMap> maps(4 * nb);
+    const int rows[4] = {CvShape::PR, CvShape::UR, CvShape::VR, CvShape::WR};
+    int st;
+    for (size_t b = 0; b < nb; ++b) {
+      BlkFld &F = V.hf[b];
+      const double *fp[4] = {F.p, F.ustar, F.vstar, F.wstar};
+      const int tk = F.nz + 2 * F.pl;
+      for (int a = 0; a < 4; ++a)
+        if ((st = field_map(&maps[4 * b + a], fp[a], F.ti, F.tj, tk, rows[a]))) return st;
+    }
+    if (V.fmaps.n != maps.size() && (st = V.fmaps.alloc(maps.size()))) return st;
+    CK(cudaMemcpyAsync(V.fmaps.p, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice,
+                       C->stream));
+    CK(cudaStreamSynchronize(C->stream));  // maps is a local
+    for (size_t b = 0; b < nb; ++b) V.hf[b].fm = V.fmaps.p + 4 * b;
+  } else {
+    for (size_t b = 0; b < nb; ++b) V.hf[b].fm = nullptr;
+  }
+  if (tma != V.fields_tma) {
+    V.fields_tma = tma;
+    V.drop_graphs();  // the captured iteration names the calvel/calmas variant
+  }
   CK(cudaMemcpyAsync(V.df.p, V.hf.data(), V.hf.size() * sizeof(BlkFld), cudaMemcpyHostToDevice, C->stream));
   return MF3D_OK;
 }
@@ -855,7 +918,7 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
   CK(cudaStreamSynchronize(s));  // hs is a local
   CK(cudaMemsetAsync(V.rmax.p, 0, nd * sizeof(unsigned long long), s));
   k_face_planes<<<V.n_planes, kTile, 0, s>>>(V.df.p, V.t_planes.p);
-  k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, s>>>(V.df.p, V.t_zint.p, V.ds.p, V.ones.p, V.rmax.p, 0);
+  calvel_calmas<T>(C, V, V.ones.p, V.rmax.p, 0);
   k_dom_init<<<1, 256, 0, s>>>(V.ds.p, nd, V.rmax.p, V.act.p);
   C->launches += 3;
   return MF3D_OK;
@@ -868,8 +931,7 @@ static int solve_end(mf3d_ctx *C, View &V) {
   bool want_su = false;
   for (auto &F : V.hf) want_su |= F.su != nullptr;
   if (want_su) {
-    k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, s>>>(V.df.p, V.t_zint.p, V.ds.p, V.ones.p,
-                                                               V.rmax_scratch.p, 1);
+    calvel_calmas<T>(C, V, V.ones.p, V.rmax_scratch.p, 1);
     ++C->launches;
   }
   k_calvel<<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, V.ds.p);

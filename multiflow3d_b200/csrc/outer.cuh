@@ -37,6 +37,7 @@ struct BlkFld {
   BlkLev L1;                         // level-1 descriptor
   int dom;                           // domain of the block
   double pinv[3];                    // 1/h when the axis is uniform with h a power of two, else 0
+  const CUtensorMap *fm;             // TMA maps of p, ustar, vstar, wstar (CvShape boxes), or null
 };
 
 // x / h.  When h is a power of two the multiplication by its reciprocal
@@ -253,6 +254,163 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas(const BlkFld *__
     double v = threadIdx.x < OZ_RJ ? red[threadIdx.x] : 0.0;
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (threadIdx.x == 0 && v > 0.0) atomic_max_nonneg(rmax_slot + F.dom, v);
+  }
+}
+
+// The same fused calvel + calmas with its operands staged by TMA.  Per
+// plane a CTA (32 x OZ_RJ cells) needs p over its cells and a one-cell ring
+// (plane k, and plane k+1 for the top faces), ustar over its cells and the
+// column to the west, vstar over its cells and the row to the south, and
+// wstar over its cells; one thread issues the four box loads of a plane
+// CV_PD planes ahead into a ring of CV_NS slots.  Boxes start at the even
+// field column X = (first cell's column - 1) rounded down, so their x origin
+// is 16-byte aligned whatever the ghost width; CV_W = 36 columns cover the
+// tile and its ring for either parity.  Each plane's p box is loaded once
+// and serves as the upper plane of the plane below.  Arithmetic, operand
+// order and the face planes are those of k_calvel_calmas.
+constexpr int CV_PD = 3;           // planes in flight ahead of the computed one
+constexpr int CV_NS = CV_PD + 1;   // slots: planes k .. k+CV_PD
+constexpr int CV_W = 36;
+struct CvShape {
+  static constexpr int PR = OZ_RJ + 2, UR = OZ_RJ, VR = OZ_RJ + 1, WR = OZ_RJ;  // box rows
+  static constexpr int PB = (PR * CV_W * 8 + 127) / 128 * 128, UB = (UR * CV_W * 8 + 127) / 128 * 128;
+  static constexpr int VB = (VR * CV_W * 8 + 127) / 128 * 128, WB = (WR * CV_W * 8 + 127) / 128 * 128;
+  static constexpr int STAGE = PB + UB + VB + WB;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_tma(const BlkFld *__restrict__ fl,
+                                                                   const Tile *__restrict__ tiles,
+                                                                   const DomState *__restrict__ ds,
+                                                                   const int *__restrict__ act,
+                                                                   unsigned long long *__restrict__ rmax_slot,
+                                                                   int write_su, int kch, int *__restrict__ err) {
+  using S = CvShape;
+  __shared__ __align__(128) unsigned char sbuf[CV_NS * S::STAGE];
+  __shared__ __align__(8) uint64_t bar[CV_NS];
+  __shared__ double red[OZ_RJ];
+  __shared__ int abort_s;
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  if (!act[F.dom]) return;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * OZ_TX + tx;
+  const double dt = ds[F.dom].dt, alfapr = ds[F.dom].alfapr, dtinv = ds[F.dom].dtinv;
+  const double dta = dt * alfapr;
+  T *__restrict__ rhs1 = rhs_of<T>(F.L1);
+  double *__restrict__ SU = write_su ? F.su : nullptr;
+  const int nx = F.nx, ny = F.ny, nz = F.nz, pl = F.pl;
+  const int i = t.i0 + tx, j = t.j0 + ty;
+  const bool in = i <= nx && j <= ny;
+  const int ic = in ? i : 1, jc = in ? j : 1;  // clamped indices keep every global load in bounds
+  const double *__restrict__ DZ = F.df[2];
+  const double *__restrict__ HZ = F.h[2];
+  const double ix = F.pinv[0], iy = F.pinv[1], iz = F.pinv[2];
+  const double hx = F.h[0][ic], hy = F.h[1][jc];
+  const double dxe = F.df[0][ic], dxw = F.df[0][ic - 1];
+  const double dyn = F.df[1][jc], dys = F.df[1][jc - 1];
+  const bool ewall = F.wall[1], nwall = F.wall[3], twall = F.wall[5];
+  const bool wwall = F.wall[0], swall = F.wall[2], bwall = F.wall[4];
+  const int a0 = t.i0 + pl - 1;   // field column of cell i0
+  const int X = (a0 - 1) & ~1;    // box origin: even, so 16-byte aligned
+  const int cx = a0 + tx - X;     // box column of this lane's cell
+  const int yb = t.j0 + pl - 1;   // field row of row j0
+  const int k0 = t.k0, k1 = min(t.k0 + kch - 1, nz);
+  const CUtensorMap *mp = F.fm, *mu = F.fm + 1, *mv = F.fm + 2, *mw = F.fm + 3;
+  auto stage = [&](int kk) { return (kk - k0) % CV_NS; };
+  auto parity = [&](int kk) { return (unsigned)(((kk - k0) / CV_NS) & 1); };
+  auto slot = [&](int kk) { return sbuf + stage(kk) * S::STAGE; };
+  auto issue = [&](int kk) {  // planes k0..k1 all four boxes; k1+1 p only
+    const int st = stage(kk), z = kk + pl - 1;
+    unsigned char *b = sbuf + st * S::STAGE;
+    const bool all = kk <= k1;
+    const unsigned bytes = S::PR * CV_W * 8 + (all ? (S::UR + S::VR + S::WR) * CV_W * 8 : 0);
+    mbar_expect_tx(&bar[st], bytes);
+    tma_load_3d(b, mp, &bar[st], X, yb - 1, z);
+    if (all) {
+      tma_load_3d(b + S::PB, mu, &bar[st], X, yb, z);
+      tma_load_3d(b + S::PB + S::UB, mv, &bar[st], X, yb - 1, z);
+      tma_load_3d(b + S::PB + S::UB + S::VB, mw, &bar[st], X, yb, z);
+    }
+  };
+  if (tid == 0) {
+    for (int st = 0; st < CV_NS; ++st) mbar_init(&bar[st], 1);
+    mbar_fence_init();
+    abort_s = 0;
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int kk = k0; kk < k0 + CV_PD && kk <= k1 + 1; ++kk) issue(kk);
+  double vmax = 0.0;
+  // w on the face below plane k0, carried up the march (plain loads)
+  double wb;
+  {
+    const long long c = fidx(F, ic, jc, k0), sz = (long long)F.ti * F.tj;
+    if (k0 == 1) {
+      const double lo = F.lo[2][(jc - 1) * nx + (ic - 1)];
+      wb = bwall ? lo : (lo - xdiv(dta * (F.p[c] - F.p[c - sz]), F.df[2][0], iz));
+    } else {
+      wb = (F.wstar[c - sz] - xdiv(dta * (F.p[c] - F.p[c - sz]), DZ[k0 - 1], iz));
+    }
+  }
+  bool ok = mbar_wait(&bar[stage(k0)], parity(k0), err);
+  for (int k = k0; k <= k1; ++k) {
+    if (tid == 0 && ok && k + CV_PD <= k1 + 1) issue(k + CV_PD);  // into the slot of plane k-1
+    if (ok) ok = mbar_wait(&bar[stage(k + 1)], parity(k + 1), err);
+    double fact = 0.0, wt = 0.0;
+    {
+      const unsigned char *b = slot(k);
+      const double *P = (const double *)b, *U = (const double *)(b + S::PB);
+      const double *Vv = (const double *)(b + S::PB + S::UB), *Wv = (const double *)(b + S::PB + S::UB + S::VB);
+      const double *PN = (const double *)slot(k + 1);
+      const int r = (ty + 1) * CV_W + cx;  // this cell in the p box
+      const double pc = P[r];
+      double ue;
+      if (ic == nx && ewall) ue = F.hi[0][(k - 1) * ny + (jc - 1)];
+      else ue = (U[ty * CV_W + cx] - xdiv(dta * (P[r + 1] - pc), dxe, ix));
+      const double ul = __shfl_up_sync(0xffffffffu, ue, 1);
+      double uw;
+      if (ic == 1) {
+        const double lo = F.lo[0][(k - 1) * ny + (jc - 1)];
+        uw = wwall ? lo : (lo - xdiv(dta * (pc - P[r - 1]), dxw, ix));
+      } else if (tx > 0) {
+        uw = ul;
+      } else {
+        uw = (U[ty * CV_W + cx - 1] - xdiv(dta * (pc - P[r - 1]), dxw, ix));
+      }
+      double vn, vs;
+      if (jc == ny && nwall) vn = F.hi[1][(k - 1) * nx + (ic - 1)];
+      else vn = (Vv[(ty + 1) * CV_W + cx] - xdiv(dta * (P[r + CV_W] - pc), dyn, iy));
+      if (jc == 1) {
+        const double lo = F.lo[1][(k - 1) * nx + (ic - 1)];
+        vs = swall ? lo : (lo - xdiv(dta * (pc - P[r - CV_W]), dys, iy));
+      } else {
+        vs = (Vv[ty * CV_W + cx] - xdiv(dta * (pc - P[r - CV_W]), dys, iy));
+      }
+      if (k == nz && twall) wt = F.hi[2][(jc - 1) * nx + (ic - 1)];
+      else wt = (Wv[ty * CV_W + cx] - xdiv(dta * (PN[r] - pc), DZ[k], iz));
+      fact = (xdiv(ue - uw, hx, ix) + xdiv(vn - vs, hy, iy) + xdiv(wt - wb, HZ[k], iz));
+    }
+    wb = wt;  // the top face of plane k is the bottom face of plane k+1
+    if (ok && in) {
+      const double su = xdiv(fact, dt, dtinv);
+      rhs1[cell_off(F.L1, i, j, k)] = (T)su;
+      if (SU) SU[fidx(F, i, j, k)] = su;
+      double f1 = fabs(fact * hx * hy * HZ[k]);
+      if (!(f1 == f1)) f1 = __longlong_as_double(0x7ff0000000000000LL);  // NaN -> +Inf (flagged)
+      vmax = vmax > f1 ? vmax : f1;
+    }
+    if (!ok) abort_s = 1;
+    __syncthreads();  // plane k's slot is refilled next iteration
+    if (abort_s) return;
+  }
+  // CTA max: warp shuffles, shared memory, one atomic per CTA
+  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  if (tx == 0) red[ty] = vmax;
+  __syncthreads();
+  if (ty == 0) {
+    double v = tx < OZ_RJ ? red[tx] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (tx == 0 && v > 0.0) atomic_max_nonneg(rmax_slot + F.dom, v);
   }
 }
 

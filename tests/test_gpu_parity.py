@@ -153,3 +153,36 @@ def test_newsolv_stretched(lib, oracle, cuda, layout):
     assert rel_l2(res.history, hist) <= REL_TOL
     assert rel_l2(pr.gather(got, "p"), pr.gather(ref, "p")) <= REL_TOL
     assert np.array_equal(res.history, hist)
+
+
+@pytest.mark.parametrize("pl", [1, 2, 3])
+def test_calvel_staging_variants(lib, oracle, cuda, pl):
+    """calvel/calmas stages p, ustar, vstar, wstar by TMA when the fields are
+    16-byte aligned with rows of a multiple of 16 bytes, else loads them
+    directly: both give the oracle's result bit for bit, for any ghost width."""
+    import torch
+    pr = Problem(2, 1, 1, 32, 16, 16, ngrid=3, pl=pl, stretch_y=2.0, dx=1 / 64, dy=1 / 16, dz=1 / 16)
+    prm = pr.params(mg_itrsch=3, maxcy=60, eps=1e-9)
+    ref, info, hist = oracle_solve(oracle, pr, prm, seed=21, fourier=2)
+    results = []
+    for offset in (0, 1):  # 1: every field starts 8 bytes past a 16-byte boundary
+        blocks = pr.block_fields(seed=21, fourier_modes=2)
+        dev = []
+        for f in blocks:
+            d = {}
+            for k, v in f.items():
+                buf = torch.empty(v.size + 1, dtype=torch.float64, device=cuda)
+                t = buf[offset:offset + v.size].view(v.shape)
+                t.copy_(torch.from_numpy(v))
+                d[k] = t
+            dev.append(d)
+        proj = Projection(pr.descriptors(lib), prm, lib)
+        res = proj.newsolv_mg_device(dev)
+        proj.close()
+        assert res.iter == info.iter and res.status == info.status
+        assert np.array_equal(res.history, hist)
+        got = [{k: v.cpu().numpy() for k, v in f.items()} for f in dev]
+        assert np.array_equal(pr.gather(got, "p"), pr.gather(ref, "p"))
+        for k in ("u", "v", "w"):
+            assert np.array_equal(pr.gather(got, k), pr.gather(ref, k))
+        results.append(res)
