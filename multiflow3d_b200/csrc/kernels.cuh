@@ -85,7 +85,9 @@ struct Tile {
 };
 
 // Tile shapes (threads per CTA = TX * RJ).
-constexpr int RB_TX = 32, RB_RJ = 8;                // red-black z-march (planes per CTA chosen per level)
+// red-black z-march: 32 x RB_TY threads, RB_CR rows per thread (RB_RJ rows
+// per CTA); planes per CTA chosen per level
+constexpr int RB_TX = 32, RB_TY = 4, RB_CR = 4, RB_RJ = RB_TY * RB_CR;
 constexpr int RW_TX = 32, RW_RJ = 8, RW_KCH = 8;    // row tiles, RW_KCH planes per CTA
 constexpr int OZ_TX = 32, OZ_RJ = 8, OZ_KCH = 16;   // outer calvel/calmas z-march
 
@@ -156,15 +158,17 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 // i = 2q + 2 - s with s = i & 1 = (colour + j + k + 1) & 1, so a row of nx
 // cells keeps ceil(nx/2) lanes busy whatever its parity.  Its west and east
 // neighbours (other colour) sit at compact h = q and q+1, the others and the
-// rhs at h = q + 1 - s.  A CTA owns q0..q0+31 of rows j0..j0+RB_RJ-1 and
-// marches up `kch` planes.  Per plane one thread issues two TMA box loads -
-// the other colour over compact columns q0..q0+TB_W-1 and rows j0-1..j0+RB_RJ,
-// the rhs over the same columns and rows j0..j0+RB_RJ-1 - into a ring of
-// RB_NS stages, RB_PD planes ahead of the plane being computed.  Boxes that
-// reach past the array read zeros (never used).
+// rhs at h = q + 1 - s.  A CTA owns q0..q0+31 of rows j0..j0+RB_RJ-1 (each
+// thread RB_CR rows RB_TY apart, which share s) and marches up `kch` planes.
+// Per plane one thread issues two TMA box loads - the other colour over
+// compact columns q0..q0+W-1 and rows j0-1..j0+RB_RJ, the rhs over the same
+// columns and rows j0..j0+RB_RJ-1 - into a ring of RB_NS stages, RB_PD
+// planes ahead of the plane being computed.  Boxes that reach past the array
+// read zeros (never used).
 // ---------------------------------------------------------------------------
-constexpr int RB_PD = 4;          // prefetch distance in planes
-constexpr int RB_NS = RB_PD + 2;  // stages: planes k-1 .. k+RB_PD
+constexpr int RB_PD = 2;          // prefetch distance in planes
+constexpr int RB_NS = RB_PD + 2;  // stages: planes k-1 .. k+RB_PD (a power of two)
+static_assert((RB_NS & (RB_NS - 1)) == 0, "RB_NS must be a power of two");
 
 template <typename T>
 struct RbShape {
@@ -175,7 +179,7 @@ struct RbShape {
 };
 
 template <typename T, bool FROM_ZERO>
-__global__ void __launch_bounds__(RB_TX *RB_RJ) k_rbgs(const BlkLev *__restrict__ bl, const Tile *__restrict__ tiles,
+__global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict__ bl, const Tile *__restrict__ tiles,
                                                        const int *__restrict__ act, int colour, int kch,
                                                        int *__restrict__ err) {
   using S = RbShape<T>;
@@ -183,31 +187,42 @@ __global__ void __launch_bounds__(RB_TX *RB_RJ) k_rbgs(const BlkLev *__restrict_
   constexpr int OB = FROM_ZERO ? 0 : S::OB;
   __shared__ __align__(128) unsigned char sbuf[RB_NS * (OB + S::RBY)];
   __shared__ __align__(8) uint64_t bar[RB_NS];
+  __shared__ int abort_s;  // set when a wait gave up: every thread leaves after the next barrier
   const Tile t = tiles[blockIdx.x];
   const BlkLev B = bl[t.blk];
   if (!act[B.dom]) return;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RB_TX + tx;
-  const int q0 = t.i0, q = q0 + tx, j = t.j0 + ty;
-  const int nx = B.nx, ny = B.ny;
-  const long long rs = (long long)(ny + 2) * B.hp;  // plane stride
-  T *__restrict__ M = phi_of<T>(B) + colour * B.cstr;
+  const int q0 = t.i0, q = q0 + tx;
+  const int nx = B.nx, ny = B.ny, hp = B.hp;
+  const long long rs = (long long)(ny + 2) * hp;  // plane stride
+  T *__restrict__ M = phi_of<T>(B) + colour * B.cstr + q0;
   const CUtensorMap *mo = B.tm + (1 - colour), *mr = B.tm + 2 + colour;
   const Coef<T> cf(B);
   const int k0 = t.k0, k1 = min(t.k0 + kch - 1, B.nz);
-  const bool jin = j <= ny;
   // coefficients of this lane's two cells (s = 0: i = 2q+2; s = 1: i = 2q+1)
   const int ia = min(2 * q + 2, nx + 1), ib = min(2 * q + 1, nx + 1);
   const T aw0 = cf.aw[ia], ae0 = cf.ae[ia], aw1 = cf.aw[ib], ae1 = cf.ae[ib];
-  const T as = jin ? cf.as[j] : (T)0, an = jin ? cf.an[j] : (T)0;
-  // ap = -1*(aw+ae+as+an+ab+at) summed left to right: the first four terms per lane
-  const T pa0 = ((aw0 + ae0) + as) + an, pa1 = ((aw1 + ae1) + as) + an;
+  // per row: as, an and ap's first four terms (summed left to right)
+  T as[RB_CR], an[RB_CR], pa0[RB_CR], pa1[RB_CR];
+  int rowoff[RB_CR];  // j*hp of each row
+#pragma unroll
+  for (int m = 0; m < RB_CR; ++m) {
+    const int j = t.j0 + ty + RB_TY * m;
+    const bool jin = j <= ny;
+    as[m] = jin ? cf.as[j] : (T)0;
+    an[m] = jin ? cf.an[j] : (T)0;
+    pa0[m] = ((aw0 + ae0) + as[m]) + an[m];
+    pa1[m] = ((aw1 + ae1) + as[m]) + an[m];
+    rowoff[m] = j * hp;
+  }
+  const int nrow = t.j0 + ty > ny ? 0 : min(RB_CR, (ny - t.j0 - ty) / RB_TY + 1);  // rows inside the block
   auto slot_o = [&](int st) { return (T *)(sbuf + st * OB); };
   auto slot_r = [&](int st) { return (T *)(sbuf + RB_NS * OB + st * S::RBY); };
   auto loads = [&](int kk) { return FROM_ZERO ? (kk >= k0 && kk <= k1) : (kk >= k0 - 1 && kk <= k1 + 1); };
   // the loaded planes are consecutive from slot 0, so each slot's phases
   // complete in order (k0-1 is loaded unless FROM_ZERO)
   constexpr int first = FROM_ZERO ? 0 : 1;
-  auto stage = [&](int kk) { return (kk - k0 + first) % RB_NS; };
+  auto stage = [&](int kk) { return (kk - k0 + first) & (RB_NS - 1); };
   auto parity = [&](int kk) { return (unsigned)(((kk - k0 + first) / RB_NS) & 1); };
   auto issue = [&](int kk) {
     const int st = stage(kk);
@@ -217,7 +232,6 @@ __global__ void __launch_bounds__(RB_TX *RB_RJ) k_rbgs(const BlkLev *__restrict_
     if (!FROM_ZERO) tma_load_3d(slot_o(st), mo, &bar[st], q0, t.j0 - 1, kk);
     if (wr) tma_load_3d(slot_r(st), mr, &bar[st], q0, t.j0, kk);
   };
-  __shared__ int abort_s;  // set when a wait gave up: every thread leaves after the next barrier
   if (tid == 0) {
     for (int st = 0; st < RB_NS; ++st) mbar_init(&bar[st], 1);
     mbar_fence_init();
@@ -234,26 +248,32 @@ __global__ void __launch_bounds__(RB_TX *RB_RJ) k_rbgs(const BlkLev *__restrict_
     if (tid == 0 && ok && loads(k + RB_PD)) issue(k + RB_PD);  // refills the slot of plane k-2
     if (ok && !FROM_ZERO) ok = mbar_wait(&bar[stage(k + 1)], parity(k + 1), err);
     if (ok && FROM_ZERO && k > k0) ok = mbar_wait(&bar[stage(k)], parity(k), err);
-    const int s = (colour + j + k + 1) & 1;
+    const int s = (colour + t.j0 + ty + k + 1) & 1;  // the same for all rows of the thread
     const int i = 2 * q + 2 - s;
-    if (ok && jin && i <= nx) {
+    if (ok && i <= nx) {
       const int st = stage(k), hc = tx + 1 - s;
-      T w = (T)0, e = (T)0, so_ = (T)0, no = (T)0, bo = (T)0, to = (T)0;
-      if (!FROM_ZERO) {
-        const T *o = slot_o(st), *ob = slot_o(stage(k - 1)), *ot = slot_o(stage(k + 1));
-        w = o[(ty + 1) * W + tx];
-        e = o[(ty + 1) * W + tx + 1];
-        so_ = o[ty * W + hc];
-        no = o[(ty + 2) * W + hc];
-        bo = ob[(ty + 1) * W + hc];
-        to = ot[(ty + 1) * W + hc];
-      }
       const T ab = cf.ab[k], at = cf.at[k];
       const T aw = s ? aw1 : aw0, ae = s ? ae1 : ae0;
-      const T ap = (T)-1.0 * (((s ? pa1 : pa0) + ab) + at);
-      const T r = slot_r(st)[ty * W + hc];
-      M[(long long)k * rs + (long long)j * B.hp + q0 + hc] =
-          ((r - (aw * w + ae * e + as * so_ + an * no + ab * bo + at * to)) / ap);
+      const T *o = slot_o(st), *ob = slot_o(stage(k - 1)), *ot = slot_o(stage(k + 1));
+      const T *r = slot_r(st);
+      T *Mk = M + (long long)k * rs + hc;
+#pragma unroll
+      for (int m = 0; m < RB_CR; ++m) {
+        if (m < nrow) {
+          const int rr = ty + RB_TY * m;  // row within the tile
+          T w = (T)0, e = (T)0, so_ = (T)0, no = (T)0, bo = (T)0, to = (T)0;
+          if (!FROM_ZERO) {
+            w = o[(rr + 1) * W + tx];
+            e = o[(rr + 1) * W + tx + 1];
+            so_ = o[rr * W + hc];
+            no = o[(rr + 2) * W + hc];
+            bo = ob[(rr + 1) * W + hc];
+            to = ot[(rr + 1) * W + hc];
+          }
+          const T ap = (T)-1.0 * (((s ? pa1[m] : pa0[m]) + ab) + at);
+          Mk[rowoff[m]] = ((r[rr * W + hc] - (aw * w + ae * e + as[m] * so_ + an[m] * no + ab * bo + at * to)) / ap);
+        }
+      }
     }
     if (!ok) abort_s = 1;
     __syncthreads();  // plane k-1's slot is refilled next iteration

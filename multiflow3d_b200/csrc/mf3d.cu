@@ -717,7 +717,7 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
       const double half = 0.5 * (double)L.cells_sub[q] * sizeof(T);
       const bool fz = from_zero && itr == 0;
       prof_begin(C, pk, (fz ? 2 : 3) * half);
-      const dim3 grid(L.n_sweep[q]), cta(RB_TX, RB_RJ);
+      const dim3 grid(L.n_sweep[q]), cta(RB_TX, RB_TY);
       if (fz)
         k_rbgs<T, true><<<grid, cta, 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
       else
@@ -1075,8 +1075,8 @@ static int ctx_init(mf3d_ctx *C, const mf3d_params *prm) {
   C->use_graph = !(e && e[0] == '1');
   CK(cudaDeviceGetAttribute(&C->nsm, cudaDevAttrMultiProcessorCount, C->device));
   int occ = 0;
-  if (C->elem == 8) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rbgs<double, false>, RB_TX * RB_RJ, 0));
-  else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rbgs<float, false>, RB_TX * RB_RJ, 0));
+  if (C->elem == 8) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rbgs<double, false>, RB_TX * RB_TY, 0));
+  else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rbgs<float, false>, RB_TX * RB_TY, 0));
   C->sweep_occ = std::max(occ, 1);
   return MF3D_OK;
 }
