@@ -238,6 +238,14 @@ int mf3d_profile_read(mf3d_ctx *ctx, double *total_ms, long long *launches,
 long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid,
                         int level, long long *dst, long long *src);
 
+/* Self-test of the quotient the TMA calvel/calmas kernel forms on axes that
+ * are not uniform powers of two: for n pairs (x[i], b[i]) in host memory,
+ * q[i] = x[i]/b[i] from the reciprocal RN(1/b[i]) (Markstein's correction)
+ * and qref[i] = the device's IEEE division, both computed on `device`.  The
+ * two agree bit for bit.  No counterpart in the reference (a test hook of
+ * this implementation). */
+int mf3d_selftest_divide(const double *x, const double *b, long long n, double *q, double *qref, int device);
+
 #ifdef __cplusplus
 }
 #endif

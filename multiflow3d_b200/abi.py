@@ -125,6 +125,7 @@ EXPORTED_SYMBOLS = (
     "mf3d_max_levels",
     "mf3d_batch_create",
     "mf3d_batch_solve_device",
+    "mf3d_selftest_divide",
 )
 
 MF3D_PROF_OFF = 0
@@ -158,6 +159,7 @@ def _declare(lib):
     lib.mf3d_batch_create.argtypes = [C.POINTER(DomainDesc), C.c_int, C.POINTER(Params), C.POINTER(vp)]
     lib.mf3d_batch_solve_device.argtypes = [vp, C.POINTER(Fields), _dp, _dp, C.POINTER(SolveInfo), _dp, C.c_int]
     lib.mf3d_profile.argtypes = [vp, C.c_int]
+    lib.mf3d_selftest_divide.argtypes = [_dp, _dp, C.c_longlong, _dp, _dp, C.c_int]
     lib.mf3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                       C.POINTER(C.c_double)]
     return lib

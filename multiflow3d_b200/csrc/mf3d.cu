@@ -110,6 +110,12 @@ static double pow2_inverse(double h) {
   return (std::isfinite(inv) && inv * h == 1.0) ? inv : 0.0;
 }
 
+// RN(1/b) for div_rcp when 2^-100 <= b <= 2^100, else 0 (the kernel divides).
+static double div_reciprocal(double b) {
+  if (!(b >= 0x1p-100 && b <= 0x1p+100)) return 0.0;
+  return 1.0 / b;
+}
+
 // ---------------------------------------------------------------------------
 // Resident storage of one block.
 // ---------------------------------------------------------------------------
@@ -273,13 +279,17 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
   }
   // level-1 field geometry: widths, face distances (bit-exact dx on a uniform axis)
   std::vector<double> g1;
-  size_t off_h[3], off_df[3];
+  size_t off_h[3], off_df[3], off_rh[3], off_rdf[3];
   for (int a = 0; a < 3; ++a) {
     std::vector<double> w = level_widths(ext[a], nfine[a], hh[a], ngrid, 1);
     off_h[a] = g1.size();
     for (int c = 0; c < nfine[a] + 2; ++c) g1.push_back(ext[a] ? w[c] : hh[a]);
     off_df[a] = g1.size();
     for (int c = 0; c <= nfine[a]; ++c) g1.push_back(ext[a] ? 0.5 * (w[c] + w[c + 1]) : hh[a]);
+    off_rh[a] = g1.size();
+    for (int c = 0; c < nfine[a] + 2; ++c) g1.push_back(div_reciprocal(g1[off_h[a] + c]));
+    off_rdf[a] = g1.size();
+    for (int c = 0; c <= nfine[a]; ++c) g1.push_back(div_reciprocal(g1[off_df[a] + c]));
   }
   if ((st = S.geo1.upload(g1, s))) return st;
   const size_t pyz = (size_t)d.ny * d.nz, pxz = (size_t)d.nx * d.nz, pxy = (size_t)d.nx * d.ny;
@@ -294,6 +304,8 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
   for (int a = 0; a < 3; ++a) {
     F.h[a] = S.geo1.p + off_h[a];
     F.df[a] = S.geo1.p + off_df[a];
+    F.rh[a] = S.geo1.p + off_rh[a];
+    F.rdf[a] = S.geo1.p + off_rdf[a];
   }
   double *pp = S.planes.p;
   F.lo[0] = pp; F.hi[0] = pp + pyz; pp += 2 * pyz;
@@ -792,10 +804,21 @@ static void vcycle(mf3d_ctx *C, View &V) {
 // fields admit it).
 template <typename T>
 static void calvel_calmas(mf3d_ctx *C, View &V, const int *act, unsigned long long *slot, int write_su) {
-  if (V.fields_tma)
-    k_calvel_calmas_tma<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, C->stream>>>(V.df.p, V.t_zint.p, V.ds.p, act, slot,
-                                                                          write_su, OZ_KCH, V.err.p);
-  else
+  if (V.fields_tma) {
+    // axes that are uniform with a power-of-two spacing in every block
+    int mask = 7;
+    for (const auto &F : V.hf)
+      for (int a = 0; a < 3; ++a)
+        if (F.pinv[a] == 0.0) mask &= ~(1 << a);
+    const dim3 grid(V.n_zint), cta(OZ_TX, CV_TY);
+#define MF3D_CV(M)                                                                                              \
+  case M:                                                                                                        \
+    k_calvel_calmas_tma<T, M><<<grid, cta, 0, C->stream>>>(V.df.p, V.t_zint.p, V.ds.p, act, slot, write_su, OZ_KCH, \
+                                                           V.err.p);                                             \
+    break;
+    switch (mask) { MF3D_CV(0) MF3D_CV(1) MF3D_CV(2) MF3D_CV(3) MF3D_CV(4) MF3D_CV(5) MF3D_CV(6) MF3D_CV(7) }
+#undef MF3D_CV
+  } else
     k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, C->stream>>>(V.df.p, V.t_zint.p, V.ds.p, act, slot,
                                                                       write_su);
 }
@@ -909,6 +932,7 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
     std::memset(&hs[d], 0, sizeof(DomState));
     hs[d].dt = dt[d];
     hs[d].dtinv = pow2_inverse(dt[d]);
+    hs[d].rdt = div_reciprocal(dt[d]);
     hs[d].alfapr = alfapr[d];
     hs[d].tol = C->prm.eps;
     hs[d].eps_relative = C->prm.eps_relative;
@@ -1343,6 +1367,25 @@ int mf3d_profile_read(mf3d_ctx *C, double *total_ms, long long *launches, double
   if (total_ms) *total_ms = C->prof_ms;
   if (launches) *launches = C->prof_n;
   if (bytes) *bytes = C->prof_bytes;
+  return MF3D_OK;
+}
+
+int mf3d_selftest_divide(const double *x, const double *b, long long n, double *q, double *qref, int device) {
+  if (!x || !b || !q || !qref || n < 0) { mf3d::set_error("mf3d_selftest_divide: bad arguments"); return MF3D_E_INVALID; }
+  if (n == 0) return MF3D_OK;
+  CK(cudaSetDevice(device));
+  std::vector<double> rb(n);
+  for (long long i = 0; i < n; ++i) rb[i] = div_reciprocal(b[i]);
+  double *d = nullptr;
+  CK(cudaMalloc(&d, (size_t)n * 5 * sizeof(double)));
+  std::unique_ptr<double, decltype(&cudaFree)> hold(d, &cudaFree);
+  CK(cudaMemcpy(d, x, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + n, b, n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d + 2 * n, rb.data(), n * sizeof(double), cudaMemcpyHostToDevice));
+  mf3d::k_selftest_divide<<<(int)((n + 255) / 256), 256>>>(d, d + n, d + 2 * n, n, d + 3 * n, d + 4 * n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpy(q, d + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(qref, d + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost));
   return MF3D_OK;
 }
 

@@ -19,6 +19,7 @@ struct DomState {
   double rmax0;    // rmax after the initial calvel/calmas
   double rmax;     // rmax after the last outer iteration
   double dtinv;    // 1/dt when dt is a power of two, else 0 (see xdiv)
+  double rdt;      // RN(1/dt) for div_rcp (0: divide)
   int maxcy;
   int eps_relative;
   int iter;        // outer iterations done
@@ -38,12 +39,45 @@ struct BlkFld {
   int dom;                           // domain of the block
   double pinv[3];                    // 1/h when the axis is uniform with h a power of two, else 0
   const CUtensorMap *fm;             // TMA maps of p, ustar, vstar, wstar (CvShape boxes), or null
+  const double *rh[3], *rdf[3];      // RN(1/h), RN(1/df) for div_rcp (0: divide)
 };
 
 // x / h.  When h is a power of two the multiplication by its reciprocal
 // (exact) rounds the same exact quotient once, so the result is the IEEE
 // quotient bit for bit; otherwise divide.
 __device__ __forceinline__ double xdiv(double x, double h, double inv) { return inv != 0.0 ? x * inv : x / h; }
+
+// x / b, bit for bit, from rb = RN(1/b) (the IEEE-rounded reciprocal,
+// formed once per divisor) in five FP64 operations.  q0 = RN(x*rb) lies
+// within 1.5 ulp of x/b; one correction q1 = RN(q0 + RN(x - b*q0)*rb) is a
+// faithful quotient (error far below an ulp).  For faithful q1 the remainder
+// x - b*q1 is exact (one FMA), and with rb within half an ulp of 1/b,
+// RN(q1 + (x - b*q1)*rb) = RN(x/b) (Markstein's theorem: P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990).  The theorem needs no overflow
+// or underflow: rb is 0 (plain division) unless 2^-100 <= b <= 2^100, and
+// |x| outside [2^-700, 2^700] (zero, subnormal, huge, Inf, NaN) divides too.
+__device__ __forceinline__ double div_rcp(double x, double b, double rb) {
+  const double ax = fabs(x);
+  if (rb == 0.0 || !(ax >= 0x1p-700 && ax <= 0x1p+700)) return x / b;
+  const double q0 = x * rb;
+  const double q1 = fma(fma(-b, q0, x), rb, q0);
+  return fma(fma(-b, q1, x), rb, q1);
+}
+// div_rcp against the IEEE division, element by element (mf3d_selftest_divide).
+__global__ void k_selftest_divide(const double *x, const double *b, const double *rb, long long n, double *q,
+                                  double *qref) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  q[t] = div_rcp(x[t], b[t], rb[t]);
+  qref[t] = x[t] / b[t];
+}
+
+// x / b on an axis: EXACT when b is a power of two and rb its exact inverse.
+template <bool EXACT>
+__device__ __forceinline__ double qdiv(double x, double b, double rb) {
+  return EXACT ? x * rb : div_rcp(x, b, rb);
+}
 
 __device__ inline long long fidx(const BlkFld &F, int i, int j, int k) {
   // level-1 ghost-inclusive (i,j,k) -> 0-based ttc element
@@ -269,7 +303,8 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas(const BlkFld *__
 // and serves as the upper plane of the plane below.  Arithmetic, operand
 // order and the face planes are those of k_calvel_calmas.
 constexpr int CV_PD = 3;           // planes in flight ahead of the computed one
-constexpr int CV_NS = CV_PD + 1;   // slots: planes k .. k+CV_PD
+constexpr int CV_NS = CV_PD + 1;   // slots: planes k .. k+CV_PD (a power of two)
+static_assert((CV_NS & (CV_NS - 1)) == 0, "CV_NS must be a power of two");
 constexpr int CV_W = 36;
 struct CvShape {
   static constexpr int PR = OZ_RJ + 2, UR = OZ_RJ, VR = OZ_RJ + 1, WR = OZ_RJ;  // box rows
@@ -278,8 +313,12 @@ struct CvShape {
   static constexpr int STAGE = PB + UB + VB + WB;
 };
 
-template <typename T>
-__global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_tma(const BlkFld *__restrict__ fl,
+constexpr int CV_TY = 4, CV_CR = OZ_RJ / CV_TY;  // 32 x CV_TY threads, CV_CR rows each (CV_TY apart)
+
+// UMASK bit a: axis a of every block is uniform with a power-of-two spacing
+// (x/h is x*(1/h) there); other axes divide through div_rcp.
+template <typename T, int UMASK>
+__global__ void __launch_bounds__(OZ_TX *CV_TY) k_calvel_calmas_tma(const BlkFld *__restrict__ fl,
                                                                    const Tile *__restrict__ tiles,
                                                                    const DomState *__restrict__ ds,
                                                                    const int *__restrict__ act,
@@ -288,37 +327,66 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_tma(const BlkFld
   using S = CvShape;
   __shared__ __align__(128) unsigned char sbuf[CV_NS * S::STAGE];
   __shared__ __align__(8) uint64_t bar[CV_NS];
-  __shared__ double red[OZ_RJ];
+  __shared__ double red[CV_TY];
   __shared__ int abort_s;
   const Tile t = tiles[blockIdx.x];
-  const BlkFld &F = fl[t.blk];
-  if (!act[F.dom]) return;
+  if (!act[fl[t.blk].dom]) return;
+  const BlkFld F = fl[t.blk];  // by value: read once, never reloaded after the stores below
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * OZ_TX + tx;
-  const double dt = ds[F.dom].dt, alfapr = ds[F.dom].alfapr, dtinv = ds[F.dom].dtinv;
+  constexpr bool UX = UMASK & 1, UY = (UMASK >> 1) & 1, UZ = (UMASK >> 2) & 1;
+  const double dt = ds[F.dom].dt, alfapr = ds[F.dom].alfapr;
+  const double dtinv = ds[F.dom].dtinv, rdt = ds[F.dom].rdt;
   const double dta = dt * alfapr;
   T *__restrict__ rhs1 = rhs_of<T>(F.L1);
   double *__restrict__ SU = write_su ? F.su : nullptr;
   const int nx = F.nx, ny = F.ny, nz = F.nz, pl = F.pl;
-  const int i = t.i0 + tx, j = t.j0 + ty;
-  const bool in = i <= nx && j <= ny;
-  const int ic = in ? i : 1, jc = in ? j : 1;  // clamped indices keep every global load in bounds
-  const double *__restrict__ DZ = F.df[2];
-  const double *__restrict__ HZ = F.h[2];
   const double ix = F.pinv[0], iy = F.pinv[1], iz = F.pinv[2];
-  const double hx = F.h[0][ic], hy = F.h[1][jc];
-  const double dxe = F.df[0][ic], dxw = F.df[0][ic - 1];
-  const double dyn = F.df[1][jc], dys = F.df[1][jc - 1];
   const bool ewall = F.wall[1], nwall = F.wall[3], twall = F.wall[5];
   const bool wwall = F.wall[0], swall = F.wall[2], bwall = F.wall[4];
+  const int i = t.i0 + tx;
+  const bool iin = i <= nx;
+  const int ic = iin ? i : 1;  // clamped: every global load stays in bounds
+  const double hx = F.h[0][ic], dxe = F.df[0][ic], dxw = F.df[0][ic - 1];
+  // reciprocals of the x divisors (the exact inverse on a power-of-two axis)
+  const double rhx = UX ? ix : F.rh[0][ic], rdxe = UX ? ix : F.rdf[0][ic], rdxw = UX ? ix : F.rdf[0][ic - 1];
+  // rows of this thread
+  int jc[CV_CR];
+  bool in[CV_CR];
+  double hy[CV_CR], dyn[CV_CR], dys[CV_CR], wb[CV_CR], rhy[CV_CR], rdyn[CV_CR], rdys[CV_CR];
+  long long l1off[CV_CR];  // level-1 element of (i, j, 0) without the colour term
+  int c0[CV_CR];           // colour of (i, j, 0)
+  const long long ps1 = (long long)(F.L1.ny + 2) * F.L1.hp, sz = (long long)F.ti * F.tj;
+  const int k0 = t.k0, k1 = min(t.k0 + kch - 1, nz);
+#pragma unroll
+  for (int m = 0; m < CV_CR; ++m) {
+    const int j = t.j0 + ty + CV_TY * m;
+    in[m] = iin && j <= ny;
+    jc[m] = j <= ny ? j : 1;
+    hy[m] = F.h[1][jc[m]];
+    dyn[m] = F.df[1][jc[m]];
+    dys[m] = F.df[1][jc[m] - 1];
+    rhy[m] = UY ? iy : F.rh[1][jc[m]];
+    rdyn[m] = UY ? iy : F.rdf[1][jc[m]];
+    rdys[m] = UY ? iy : F.rdf[1][jc[m] - 1];
+    l1off[m] = (long long)j * F.L1.hp + (i >> 1);
+    c0[m] = (i + j + 1) & 1;
+    // w on the face below plane k0, carried up the march (plain loads)
+    const long long c = fidx(F, ic, jc[m], k0);
+    if (k0 == 1) {
+      const double lo = F.lo[2][(jc[m] - 1) * nx + (ic - 1)];
+      wb[m] = bwall ? lo : (lo - qdiv<UZ>(dta * (F.p[c] - F.p[c - sz]), F.df[2][0], UZ ? iz : F.rdf[2][0]));
+    } else {
+      wb[m] = (F.wstar[c - sz] -
+               qdiv<UZ>(dta * (F.p[c] - F.p[c - sz]), F.df[2][k0 - 1], UZ ? iz : F.rdf[2][k0 - 1]));
+    }
+  }
   const int a0 = t.i0 + pl - 1;   // field column of cell i0
   const int X = (a0 - 1) & ~1;    // box origin: even, so 16-byte aligned
   const int cx = a0 + tx - X;     // box column of this lane's cell
   const int yb = t.j0 + pl - 1;   // field row of row j0
-  const int k0 = t.k0, k1 = min(t.k0 + kch - 1, nz);
   const CUtensorMap *mp = F.fm, *mu = F.fm + 1, *mv = F.fm + 2, *mw = F.fm + 3;
-  auto stage = [&](int kk) { return (kk - k0) % CV_NS; };
+  auto stage = [&](int kk) { return (kk - k0) & (CV_NS - 1); };
   auto parity = [&](int kk) { return (unsigned)(((kk - k0) / CV_NS) & 1); };
-  auto slot = [&](int kk) { return sbuf + stage(kk) * S::STAGE; };
   auto issue = [&](int kk) {  // planes k0..k1 all four boxes; k1+1 p only
     const int st = stage(kk), z = kk + pl - 1;
     unsigned char *b = sbuf + st * S::STAGE;
@@ -341,63 +409,58 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_tma(const BlkFld
   if (tid == 0)
     for (int kk = k0; kk < k0 + CV_PD && kk <= k1 + 1; ++kk) issue(kk);
   double vmax = 0.0;
-  // w on the face below plane k0, carried up the march (plain loads)
-  double wb;
-  {
-    const long long c = fidx(F, ic, jc, k0), sz = (long long)F.ti * F.tj;
-    if (k0 == 1) {
-      const double lo = F.lo[2][(jc - 1) * nx + (ic - 1)];
-      wb = bwall ? lo : (lo - xdiv(dta * (F.p[c] - F.p[c - sz]), F.df[2][0], iz));
-    } else {
-      wb = (F.wstar[c - sz] - xdiv(dta * (F.p[c] - F.p[c - sz]), DZ[k0 - 1], iz));
-    }
-  }
   bool ok = mbar_wait(&bar[stage(k0)], parity(k0), err);
   for (int k = k0; k <= k1; ++k) {
     if (tid == 0 && ok && k + CV_PD <= k1 + 1) issue(k + CV_PD);  // into the slot of plane k-1
     if (ok) ok = mbar_wait(&bar[stage(k + 1)], parity(k + 1), err);
-    double fact = 0.0, wt = 0.0;
-    {
-      const unsigned char *b = slot(k);
-      const double *P = (const double *)b, *U = (const double *)(b + S::PB);
-      const double *Vv = (const double *)(b + S::PB + S::UB), *Wv = (const double *)(b + S::PB + S::UB + S::VB);
-      const double *PN = (const double *)slot(k + 1);
-      const int r = (ty + 1) * CV_W + cx;  // this cell in the p box
+    const unsigned char *b = sbuf + stage(k) * S::STAGE;
+    const double *P = (const double *)b, *U = (const double *)(b + S::PB);
+    const double *Vv = (const double *)(b + S::PB + S::UB), *Wv = (const double *)(b + S::PB + S::UB + S::VB);
+    const double *PN = (const double *)(sbuf + stage(k + 1) * S::STAGE);
+    const double dzk = F.df[2][k], hzk = F.h[2][k];
+    const double rdzk = UZ ? iz : F.rdf[2][k], rhzk = UZ ? iz : F.rh[2][k];
+    const bool top = k == nz && twall;
+#pragma unroll
+    for (int m = 0; m < CV_CR; ++m) {
+      const int rr = ty + CV_TY * m;   // row within the tile
+      const int r = (rr + 1) * CV_W + cx;  // this cell in the p box
       const double pc = P[r];
       double ue;
-      if (ic == nx && ewall) ue = F.hi[0][(k - 1) * ny + (jc - 1)];
-      else ue = (U[ty * CV_W + cx] - xdiv(dta * (P[r + 1] - pc), dxe, ix));
+      if (ic == nx && ewall) ue = F.hi[0][(k - 1) * ny + (jc[m] - 1)];
+      else ue = (U[rr * CV_W + cx] - qdiv<UX>(dta * (P[r + 1] - pc), dxe, rdxe));
       const double ul = __shfl_up_sync(0xffffffffu, ue, 1);
       double uw;
       if (ic == 1) {
-        const double lo = F.lo[0][(k - 1) * ny + (jc - 1)];
-        uw = wwall ? lo : (lo - xdiv(dta * (pc - P[r - 1]), dxw, ix));
+        const double lo = F.lo[0][(k - 1) * ny + (jc[m] - 1)];
+        uw = wwall ? lo : (lo - qdiv<UX>(dta * (pc - P[r - 1]), dxw, rdxw));
       } else if (tx > 0) {
         uw = ul;
       } else {
-        uw = (U[ty * CV_W + cx - 1] - xdiv(dta * (pc - P[r - 1]), dxw, ix));
+        uw = (U[rr * CV_W + cx - 1] - qdiv<UX>(dta * (pc - P[r - 1]), dxw, rdxw));
       }
       double vn, vs;
-      if (jc == ny && nwall) vn = F.hi[1][(k - 1) * nx + (ic - 1)];
-      else vn = (Vv[(ty + 1) * CV_W + cx] - xdiv(dta * (P[r + CV_W] - pc), dyn, iy));
-      if (jc == 1) {
+      if (jc[m] == ny && nwall) vn = F.hi[1][(k - 1) * nx + (ic - 1)];
+      else vn = (Vv[(rr + 1) * CV_W + cx] - qdiv<UY>(dta * (P[r + CV_W] - pc), dyn[m], rdyn[m]));
+      if (jc[m] == 1) {
         const double lo = F.lo[1][(k - 1) * nx + (ic - 1)];
-        vs = swall ? lo : (lo - xdiv(dta * (pc - P[r - CV_W]), dys, iy));
+        vs = swall ? lo : (lo - qdiv<UY>(dta * (pc - P[r - CV_W]), dys[m], rdys[m]));
       } else {
-        vs = (Vv[ty * CV_W + cx] - xdiv(dta * (pc - P[r - CV_W]), dys, iy));
+        vs = (Vv[rr * CV_W + cx] - qdiv<UY>(dta * (pc - P[r - CV_W]), dys[m], rdys[m]));
       }
-      if (k == nz && twall) wt = F.hi[2][(jc - 1) * nx + (ic - 1)];
-      else wt = (Wv[ty * CV_W + cx] - xdiv(dta * (PN[r] - pc), DZ[k], iz));
-      fact = (xdiv(ue - uw, hx, ix) + xdiv(vn - vs, hy, iy) + xdiv(wt - wb, HZ[k], iz));
-    }
-    wb = wt;  // the top face of plane k is the bottom face of plane k+1
-    if (ok && in) {
-      const double su = xdiv(fact, dt, dtinv);
-      rhs1[cell_off(F.L1, i, j, k)] = (T)su;
-      if (SU) SU[fidx(F, i, j, k)] = su;
-      double f1 = fabs(fact * hx * hy * HZ[k]);
-      if (!(f1 == f1)) f1 = __longlong_as_double(0x7ff0000000000000LL);  // NaN -> +Inf (flagged)
-      vmax = vmax > f1 ? vmax : f1;
+      double wt;
+      if (top) wt = F.hi[2][(jc[m] - 1) * nx + (ic - 1)];
+      else wt = (Wv[rr * CV_W + cx] - qdiv<UZ>(dta * (PN[r] - pc), dzk, rdzk));
+      const double fact =
+          (qdiv<UX>(ue - uw, hx, rhx) + qdiv<UY>(vn - vs, hy[m], rhy[m]) + qdiv<UZ>(wt - wb[m], hzk, rhzk));
+      wb[m] = wt;  // the top face of plane k is the bottom face of plane k+1
+      if (ok && in[m]) {
+        const double su = dtinv != 0.0 ? fact * dtinv : div_rcp(fact, dt, rdt);
+        rhs1[((c0[m] ^ (k & 1)) ? F.L1.cstr : 0) + k * ps1 + l1off[m]] = (T)su;
+        if (SU) SU[fidx(F, i, jc[m], k)] = su;
+        double f1 = fabs(fact * hx * hy[m] * hzk);
+        if (!(f1 == f1)) f1 = __longlong_as_double(0x7ff0000000000000LL);  // NaN -> +Inf (flagged)
+        vmax = vmax > f1 ? vmax : f1;
+      }
     }
     if (!ok) abort_s = 1;
     __syncthreads();  // plane k's slot is refilled next iteration
@@ -408,7 +471,7 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_tma(const BlkFld
   if (tx == 0) red[ty] = vmax;
   __syncthreads();
   if (ty == 0) {
-    double v = tx < OZ_RJ ? red[tx] : 0.0;
+    double v = tx < CV_TY ? red[tx] : 0.0;
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (tx == 0 && v > 0.0) atomic_max_nonneg(rmax_slot + F.dom, v);
   }

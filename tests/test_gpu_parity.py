@@ -186,3 +186,38 @@ def test_calvel_staging_variants(lib, oracle, cuda, pl):
         for k in ("u", "v", "w"):
             assert np.array_equal(pr.gather(got, k), pr.gather(ref, k))
         results.append(res)
+
+
+def test_division_from_reciprocal(lib, cuda):
+    """The quotient the TMA calvel/calmas kernel forms from RN(1/b) equals
+    the IEEE quotient bit for bit: random operands over a wide range, divisors
+    with all-ones significands and near powers of two, quotients close to
+    rounding midpoints, and the special values that take the plain division."""
+    rng = np.random.default_rng(7)
+    n = 1 << 20
+    x = rng.uniform(-1, 1, n) * np.exp2(rng.uniform(-40, 40, n))
+    b = np.exp2(rng.uniform(-30, 30, n)) * rng.uniform(1, 2, n)
+    k = n // 8
+    b[:k] = np.ldexp(2.0 - 2.0 ** -52, rng.integers(-20, 20, k))            # all-ones significand
+    b[k:2 * k] = 1.0 + rng.integers(0, 64, k) * 2.0 ** -52                   # just above a power of two
+    b[2 * k:3 * k] = np.ldexp(1.0, rng.integers(-20, 20, k))                 # powers of two
+    # quotients near midpoints: x = RN(b * (m + ulp/2)) for random m
+    m = rng.uniform(1, 2, k)
+    x[3 * k:4 * k] = b[3 * k:4 * k] * (m + np.spacing(m) / 2)
+    special = np.array([0.0, -0.0, 5e-324, -5e-324, 1e-310, 1e308, -1e308, np.inf, -np.inf, np.nan, 2.0 ** -701,
+                        2.0 ** 701, 1.0, -1.0])
+    x[-len(special):] = special
+    b[-len(special):] = 0.37
+    b[-20] = 1e-200  # a divisor outside the reciprocal's range: plain division
+    b[-21] = 1e200
+    q = np.empty(n)
+    qref = np.empty(n)
+    dp = C.POINTER(C.c_double)
+    st = lib.mf3d_selftest_divide(x.ctypes.data_as(dp), b.ctypes.data_as(dp), n, q.ctypes.data_as(dp),
+                                  qref.ctypes.data_as(dp), 0)
+    assert st == 0
+    bits = lambda a: a.view(np.int64)
+    assert np.array_equal(bits(q), bits(qref)), np.flatnonzero(bits(q) != bits(qref))[:10]
+    with np.errstate(all="ignore"):
+        host = x / b
+    assert np.array_equal(bits(q), bits(host))
