@@ -56,10 +56,14 @@ __device__ __forceinline__ double xdiv(double x, double h, double inv) { return 
 // "Computation of elementary functions on the IBM RISC System/6000
 // processor", IBM J. Res. Dev. 34(1), 1990).  The theorem needs no overflow
 // or underflow: rb is 0 (plain division) unless 2^-100 <= b <= 2^100, and
-// |x| outside [2^-700, 2^700] (zero, subnormal, huge, Inf, NaN) divides too.
+// |x| outside [2^-700, 2^701) (zero, subnormal, huge, Inf, NaN) divides too.
+// The range test reads the exponent field (integer pipe).
+__device__ __forceinline__ bool rcp_range(double x) {
+  const unsigned e = (unsigned)((unsigned long long)__double_as_longlong(x) >> 52) & 0x7ffu;
+  return e - (1023u - 700u) <= 1400u;  // biased exponent in [323, 1723]
+}
 __device__ __forceinline__ double div_rcp(double x, double b, double rb) {
-  const double ax = fabs(x);
-  if (rb == 0.0 || !(ax >= 0x1p-700 && ax <= 0x1p+700)) return x / b;
+  if (rb == 0.0 || !rcp_range(x)) return x / b;
   const double q0 = x * rb;
   const double q1 = fma(fma(-b, q0, x), rb, q0);
   return fma(fma(-b, q1, x), rb, q1);
@@ -313,7 +317,7 @@ struct CvShape {
   static constexpr int STAGE = PB + UB + VB + WB;
 };
 
-constexpr int CV_TY = 4, CV_CR = OZ_RJ / CV_TY;  // 32 x CV_TY threads, CV_CR rows each (CV_TY apart)
+constexpr int CV_TY = 4, CV_CR = OZ_RJ / CV_TY;  // 32 x CV_TY threads, CV_CR consecutive rows each
 
 // UMASK bit a: axis a of every block is uniform with a power-of-two spacing
 // (x/h is x*(1/h) there); other axes divide through div_rcp.
@@ -359,7 +363,7 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY) k_calvel_calmas_tma(const BlkFld
   const int k0 = t.k0, k1 = min(t.k0 + kch - 1, nz);
 #pragma unroll
   for (int m = 0; m < CV_CR; ++m) {
-    const int j = t.j0 + ty + CV_TY * m;
+    const int j = t.j0 + CV_CR * ty + m;
     in[m] = iin && j <= ny;
     jc[m] = j <= ny ? j : 1;
     hy[m] = F.h[1][jc[m]];
@@ -420,9 +424,10 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY) k_calvel_calmas_tma(const BlkFld
     const double dzk = F.df[2][k], hzk = F.h[2][k];
     const double rdzk = UZ ? iz : F.rdf[2][k], rhzk = UZ ? iz : F.rh[2][k];
     const bool top = k == nz && twall;
+    double vprev = 0.0;
 #pragma unroll
     for (int m = 0; m < CV_CR; ++m) {
-      const int rr = ty + CV_TY * m;   // row within the tile
+      const int rr = CV_CR * ty + m;   // row within the tile
       const int r = (rr + 1) * CV_W + cx;  // this cell in the p box
       const double pc = P[r];
       double ue;
@@ -441,12 +446,15 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY) k_calvel_calmas_tma(const BlkFld
       double vn, vs;
       if (jc[m] == ny && nwall) vn = F.hi[1][(k - 1) * nx + (ic - 1)];
       else vn = (Vv[(rr + 1) * CV_W + cx] - qdiv<UY>(dta * (P[r + CV_W] - pc), dyn[m], rdyn[m]));
-      if (jc[m] == 1) {
+      if (m > 0) {
+        vs = vprev;  // the south face of row j is the north face of row j-1 (same operands)
+      } else if (jc[m] == 1) {
         const double lo = F.lo[1][(k - 1) * nx + (ic - 1)];
         vs = swall ? lo : (lo - qdiv<UY>(dta * (pc - P[r - CV_W]), dys[m], rdys[m]));
       } else {
         vs = (Vv[rr * CV_W + cx] - qdiv<UY>(dta * (pc - P[r - CV_W]), dys[m], rdys[m]));
       }
+      vprev = vn;
       double wt;
       if (top) wt = F.hi[2][(jc[m] - 1) * nx + (ic - 1)];
       else wt = (Wv[rr * CV_W + cx] - qdiv<UZ>(dta * (PN[r] - pc), dzk, rdzk));
