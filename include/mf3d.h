@@ -198,6 +198,31 @@ int mf3d_batch_solve_device(mf3d_ctx *ctx, const mf3d_fields *fields,
  * V-cycle starts from pp = 0 as newsolv_mg.for:19-21 and :44 leave it. */
 int mf3d_mgkcyc_device(mf3d_ctx *ctx, double *const *su, double *const *pp);
 
+/* mf3d_mgkcyc_device that allocates nothing: no cudaMalloc, no cudaFree,
+ * no allocating library.  It runs the same V-cycle on the same context, but
+ * the per-call tables of the su and pp pointers (which mf3d_mgkcyc_device
+ * keeps in a buffer the context allocates on first use) live in a fixed
+ * device array inside the library, sized for MF3D_NOALLOC_MAX_BLOCKS blocks
+ * (2 x 512 pointers, 8 KiB).  All other device memory the call touches was
+ * allocated by mf3d_create.  No counterpart in the reference (it has no GPU).
+ *
+ * For callers that must not allocate device memory while they run: a time
+ * loop that shares the device with other streams (cudaMalloc/cudaFree may
+ * synchronise the whole device), or a process whose device memory is held
+ * by another allocator's pool.
+ *
+ * - More than MF3D_NOALLOC_MAX_BLOCKS blocks: MF3D_E_INVALID, nothing runs.
+ * - Nothing has to start at zero: both tables are written in full before
+ *   each use.  pp starts from 0 as in mf3d_mgkcyc_device.
+ * - The array is shared by every context on a device: calls on one device
+ *   must not overlap (from several threads, or on several contexts whose
+ *   streams run concurrently); overlapping calls race on the tables.
+ * - The first call on a device looks up the array's address
+ *   (cudaGetSymbolAddress) with that device current; make that first call
+ *   before any stream capture on the device. */
+#define MF3D_NOALLOC_MAX_BLOCKS 512
+int mf3d_mgkcyc_device_noalloc(mf3d_ctx *ctx, double *const *su, double *const *pp);
+
 /* ---------------------------------------------------------------------- */
 /* Introspection.                                                           */
 /* ---------------------------------------------------------------------- */

@@ -126,7 +126,10 @@ EXPORTED_SYMBOLS = (
     "mf3d_batch_create",
     "mf3d_batch_solve_device",
     "mf3d_selftest_divide",
+    "mf3d_mgkcyc_device_noalloc",
 )
+
+MF3D_NOALLOC_MAX_BLOCKS = 512
 
 MF3D_PROF_OFF = 0
 MF3D_PROF_SMOOTH_L1 = 1
@@ -147,6 +150,7 @@ def _declare(lib):
                                     C.POINTER(SolveInfo), _dp, C.c_int]
     lib.mf3d_newsolv_mg_device.argtypes = lib.mf3d_newsolv_mg.argtypes
     lib.mf3d_mgkcyc_device.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp)]
+    lib.mf3d_mgkcyc_device_noalloc.argtypes = [vp, C.POINTER(_dp), C.POINTER(_dp)]
     lib.mf3d_last_error.restype = C.c_char_p
     lib.mf3d_status_string.restype = C.c_char_p
     lib.mf3d_status_string.argtypes = [C.c_int]

@@ -1070,6 +1070,63 @@ static int mgkcyc_view(mf3d_ctx *C, View &V, double *const *su, double *const *p
   return check_device_error(V);
 }
 
+// ---------------------------------------------------------------------------
+// mf3d_mgkcyc_device_noalloc: the pointer tables in a fixed device array.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double *g_noalloc_ptrs[2 * MF3D_NOALLOC_MAX_BLOCKS];
+
+// Device address of g_noalloc_ptrs on `device` (looked up once per device,
+// with that device current).
+static int noalloc_tables(int device, double ***out) {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static void *addr[kMaxDevices] = {};
+  if (device < 0 || device >= kMaxDevices) {
+    set_error("mf3d_mgkcyc_device_noalloc: device ordinal out of range");
+    return MF3D_E_INVALID;
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[device]) {
+    void *a = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_ptrs);
+    if (e != cudaSuccess || !a) {
+      set_error(std::string("mf3d_mgkcyc_device_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      return MF3D_E_CUDA;
+    }
+    addr[device] = a;
+  }
+  *out = (double **)addr[device];
+  return MF3D_OK;
+}
+
+template <typename T>
+static int mgkcyc_view_noalloc(mf3d_ctx *C, View &V, double *const *su, double *const *pp) {
+  cudaStream_t s = C->stream;
+  const int nb = (int)V.blk.size();
+  if (nb > MF3D_NOALLOC_MAX_BLOCKS) {
+    set_error("mf3d_mgkcyc_device_noalloc: " + std::to_string(nb) + " blocks exceed MF3D_NOALLOC_MAX_BLOCKS (" +
+              std::to_string(MF3D_NOALLOC_MAX_BLOCKS) + ")");
+    return MF3D_E_INVALID;
+  }
+  double **tab = nullptr;
+  if (int st = noalloc_tables(C->device, &tab)) return st;
+  C->launches = 0;
+  CK(cudaMemcpyAsync(tab, su, nb * sizeof(double *), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(tab + nb, pp, nb * sizeof(double *), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(V.df.p, V.hf.data(), nb * sizeof(BlkFld), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(V.act.p, V.ones.p, V.ones.n * sizeof(int), cudaMemcpyDeviceToDevice, s));
+  k_load_rhs<T><<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, tab);
+  vcycle<T>(C, V);
+  k_store_pp<T><<<V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_l1cells.p, tab + nb);
+  // restore the invariant: the level-1 ghost shell holds zeros between calls
+  ViewLevel &L1 = V.lv[1];
+  k_zero_ghosts<T><<<dim3(64, L1.n_list[SUB_A]), kTile, 0, s>>>(L1.tab.p, L1.list[SUB_A].p, L1.n_list[SUB_A]);
+  C->launches += 3;
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return check_device_error(V);
+}
+
 static size_t ttc_elems(int pl, const mf3d_block_desc &d) {
   return (size_t)(d.nx + 2 * pl) * (d.ny + 2 * pl) * (d.nz + 2 * pl);
 }
@@ -1350,6 +1407,13 @@ int mf3d_mgkcyc_device(mf3d_ctx *C, double *const *su, double *const *pp) {
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   if (C->elem == 8) return mf3d::mgkcyc_view<double>(C, *C->view, su, pp);
   return mf3d::mgkcyc_view<float>(C, *C->view, su, pp);
+}
+
+int mf3d_mgkcyc_device_noalloc(mf3d_ctx *C, double *const *su, double *const *pp) {
+  if (!C || !su || !pp) { mf3d::set_error("mf3d_mgkcyc_device_noalloc: bad arguments"); return MF3D_E_INVALID; }
+  if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  if (C->elem == 8) return mf3d::mgkcyc_view_noalloc<double>(C, *C->view, su, pp);
+  return mf3d::mgkcyc_view_noalloc<float>(C, *C->view, su, pp);
 }
 
 long long mf3d_last_launch_count(const mf3d_ctx *C) { return C ? C->launches : 0; }
