@@ -370,6 +370,138 @@ def run_gpu(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Further workloads (not the default line): mixed precision on the
+# single-block 512x256x256 channel, and the batch of 64 uneven domains.
+# ---------------------------------------------------------------------------
+def _timed_solves(run_once, reset, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        reset()
+        run_once()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    out = None
+    ev0.record()
+    for _ in range(steps):
+        reset()
+        out = run_once()
+    ev1.record()
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) / 1e3, out
+
+
+def run_mixed(args):
+    """Single block 512x256x256, tanh y-stretch 2.0, 7 levels, tol 1e-8: the
+    FP32 V-cycle (FP64 coarsest level, FP64 outer loop) against the FP64 form
+    on the same inputs; error of the mixed result against the FP64 one."""
+    import numpy as np
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.problems import Problem
+    from multiflow3d_b200.solver import Projection
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    h = 1.0 / 256
+    pr = Problem(1, 1, 1, 512, 256, 256, ngrid=7, pl=2, stretch_y=2.0, dx=h, dy=h, dz=h)
+    host = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    keys = ("ustar", "vstar", "wstar", "u", "v", "w", "p")
+    d = [{k: torch.from_numpy(f[k]).to(dev) for k in keys} for f in host]
+    pristine = [{k: f[k].clone() for k in ("u", "v", "w", "p")} for f in d]
+
+    def reset():
+        for f, p0 in zip(d, pristine):
+            for k in ("u", "v", "w", "p"):
+                f[k].copy_(p0[k])
+
+    res = {}
+    for name, prec in (("mixed", abi.MF3D_PREC_FP32), ("fp64", abi.MF3D_PREC_FP64)):
+        prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=400, eps=1e-8, precision=prec)
+        proj = Projection(pr.descriptors(lib), prm, lib)
+        sec, r = _timed_solves(lambda: proj.newsolv_mg_device(d), reset, args.steps, args.warmup)
+        proj.close()
+        res[name] = (args.steps / sec, r, {k: d[0][k].cpu().numpy() for k in ("p", "u", "v", "w")})
+    pm, pf = res["mixed"][2]["p"], res["fp64"][2]["p"]
+    pm, pf = pm - pm.mean(), pf - pf.mean()
+    err_p = float(np.linalg.norm(pm - pf) / np.linalg.norm(pf))
+    err_uvw = max(float(np.abs(res["mixed"][2][k] - res["fp64"][2][k]).max() / np.abs(res["fp64"][2][k]).max())
+                  for k in ("u", "v", "w"))
+    line = {
+        "metric": "poisson_solves_per_s_mixed", "value": res["mixed"][0], "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32 V-cycle, f64 outer",
+        "data": "synthetic",
+        "config": {"workload": "mixed precision single block 512x256x256, tanh y-stretch 2.0, 7 levels, "
+                               "RB-GS(2,1), rel tol 1e-8"},
+        "iterations": res["mixed"][1].iter, "rel_rmax": res["mixed"][1].rmax / res["mixed"][1].rmax0,
+        "fp64_same_config": {"value": res["fp64"][0], "iterations": res["fp64"][1].iter},
+        "speedup_vs_fp64": res["mixed"][0] / res["fp64"][0],
+        "error_vs_fp64": {"p_rel_l2_mean_free": err_p, "uvw_max_rel": err_uvw},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batched(args):
+    """64 independent domains (edges log-uniform in [32,192], multiples of 8,
+    periodic/wall per axis), tol 1e-8: one mixed-precision batch context
+    against the same batch in FP64 and against plain FP64 solves one at a
+    time (one context per domain)."""
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.problems import domain_problem, domain_desc, random_batch
+    from multiflow3d_b200.solver import Batch
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    doms = [domain_problem(nx, ny, nz, bc, lib.mf3d_max_levels(nx, ny, nz))
+            for nx, ny, nz, bc in random_batch(64, SEED)]
+    keys = ("ustar", "vstar", "wstar", "u", "v", "w", "p")
+    fields = [{k: torch.from_numpy(v).to(dev) for k, v in pr.block_fields(seed=SEED + i)[0].items() if k in keys}
+              for i, pr in enumerate(doms)]
+    pristine = [{k: f[k].clone() for k in ("u", "v", "w", "p")} for f in fields]
+
+    def reset():
+        for f, p0 in zip(fields, pristine):
+            for k in ("u", "v", "w", "p"):
+                f[k].copy_(p0[k])
+
+    out = {}
+    for name, prec in (("mixed", abi.MF3D_PREC_FP32), ("fp64", abi.MF3D_PREC_FP64)):
+        prm = doms[0].params(mg_itrsch=3, maxcy=300, eps=1e-8, precision=prec)
+        prm.ngrid = 1
+        b = Batch([domain_desc(pr) for pr in doms], prm, lib)
+        sec, r = _timed_solves(lambda: b.solve_device(fields), reset, args.steps, args.warmup)
+        b.close()
+        rs, st = r
+        out[name] = (len(doms) * args.steps / sec, sum(x.status == 0 for x in rs), max(x.iter for x in rs))
+    # plain FP64, one domain at a time
+    prm = doms[0].params(mg_itrsch=3, maxcy=300, eps=1e-8, precision=abi.MF3D_PREC_FP64)
+    prm.ngrid = 1
+    solo = [Batch([domain_desc(pr)], prm, lib) for pr in doms]
+
+    def one_at_a_time():
+        for b, f in zip(solo, fields):
+            b.solve_device([f])
+
+    sec, _ = _timed_solves(one_at_a_time, reset, args.steps, args.warmup)
+    for b in solo:
+        b.close()
+    plain = len(doms) * args.steps / sec
+    line = {
+        "metric": "poisson_solves_per_s_batched", "value": out["mixed"][0], "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32 V-cycle, f64 outer",
+        "data": "synthetic",
+        "config": {"workload": "64 domains, edges log-uniform in [32,192] (multiples of 8), periodic/wall per "
+                               "axis, max levels per domain, RB-GS(2,1), rel tol 1e-8, one batch context"},
+        "converged": out["mixed"][1], "max_iterations": out["mixed"][2],
+        "fp64_batch": {"value": out["fp64"][0], "converged": out["fp64"][1]},
+        "plain_fp64_one_at_a_time": {"value": plain},
+        "speedup_vs_plain": out["mixed"][0] / plain,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -377,9 +509,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mf3d", choices=["mf3d", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="multiblock", choices=["multiblock", "mixed", "batched"],
+                    help="multiblock: the default FP64 line; mixed / batched: the further workloads (1 GPU)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "mixed":
+        return run_mixed(args)
+    if args.workload == "batched":
+        return run_batched(args)
     return run_gpu(args)
 
 

@@ -120,6 +120,7 @@ static double div_reciprocal(double b) {
 // Resident storage of one block.
 // ---------------------------------------------------------------------------
 struct LevelStore {
+  int elem = 8;  // bytes per value of this level
   DevBuf<char> phi, rhs, coef, geo;
   DevBuf<CUtensorMap> tmaps;  // phi c0, phi c1, rhs c0, rhs c1
   BlkLev desc;  // host copy with device pointers
@@ -183,7 +184,9 @@ struct BlockStore {
 
 // Build one block's hierarchy: replaces `coeff` (mgsolver.for:2-222) and the
 // `cof` sizing of localparameters.for:208-237.
-static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int elem, int pl, cudaStream_t s) {
+static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int elem_fine, int elem_coarsest, int pl,
+                       cudaStream_t s) {
+  const int elem = elem_fine;
   S.d = d;
   S.ngrid = ngrid;
   S.elem = elem;
@@ -203,6 +206,8 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
     LevelStore &L = S.lv[g];
     BlkLev &B = L.desc;
     std::memset(&B, 0, sizeof B);
+    const int elem = (g == ngrid && ngrid > 1) ? elem_coarsest : elem_fine;
+    L.elem = elem;
     B.nx = d.nx >> (g - 1);
     B.ny = d.ny >> (g - 1);
     B.nz = d.nz >> (g - 1);
@@ -336,8 +341,8 @@ static long long level_off(const BlkLev &B, int i, int j, int k) {
   return c * B.cstr + ((long long)k * (B.ny + 2) + j) * B.hp + (i >> 1);
 }
 
-static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, int ngrid, int elem, int pl,
-                        cudaStream_t s) {
+static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, int ngrid, int elem, int elem_coarsest,
+                        int pl, cudaStream_t s) {
   D.ngrid = ngrid;
   D.blocks.clear();
   std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
@@ -346,7 +351,7 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
   D.bytes = 0;
   for (int b = 0; b < nb; ++b) {
     D.blocks.emplace_back(new BlockStore());
-    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, pl, s))) return st;
+    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, elem_coarsest, pl, s))) return st;
     D.bytes += D.blocks.back()->bytes;
   }
   D.halo.assign(ngrid + 1, {});
@@ -454,6 +459,7 @@ struct mf3d_ctx {
   mf3d_params prm;
   int device = 0;
   int elem = 8;
+  bool coarse64 = false;    // FP32 V-cycle with the coarsest level (and its sweeps) in FP64
   int nsm = 148;            // SMs of the device
   int sweep_occ = 4;        // resident sweep CTAs per SM
   cudaStream_t stream = nullptr;
@@ -644,10 +650,10 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       staged.insert(staged.end(), direct.begin(), direct.end());
       L.n_halo[q] = (int)staged.size();
       if ((st = L.halo[q].upload(staged, s))) return st;
-      if ((st = L.stage[q].alloc((size_t)std::max(L.n_staged[q], 1) * C->elem))) return st;
+      if ((st = L.stage[q].alloc((size_t)std::max(L.n_staged[q], 1) * 8))) return st;
     }
   }
-  if (C->prm.mg_itrsch == 2 && (st = V.work.alloc(std::max<size_t>(work_elems, 1) * C->elem))) return st;
+  if (C->prm.mg_itrsch == 2 && (st = V.work.alloc(std::max<size_t>(work_elems, 1) * 8))) return st;
   // level-1 field tables
   V.hf.resize(nb);
   std::vector<Tile> t1, t2, t5;
@@ -750,24 +756,24 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
   }
 }
 
-template <typename T>
+template <typename T, typename TC>
 static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks continuing down
   ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
   if (!Cl.n_rtile) return;
   const int pk = g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse out
-  k_restrict<T, T><<<Cl.n_rtile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch);
+  k_restrict<T, TC><<<Cl.n_rtile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch);
   prof_end(C, pk);
   ++C->launches;
 }
 
-template <typename T>
+template <typename T, typename TC>
 static void corr(mf3d_ctx *C, View &V, int g) {  // level g+1 -> g, blocks continuing down
   ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
   if (!F.n_ptile) return;
   const int pk = g == 1 ? MF3D_PROF_PROLONG_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 1.0 / 8.0));  // fine in/out, coarse in
-  k_prolong<T, T><<<F.n_ptile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, F.ptile.p, V.act.p, F.pkch);
+  k_prolong<T, TC><<<F.n_ptile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, F.ptile.p, V.act.p, F.pkch);
   prof_end(C, pk);
   ++C->launches;
 }
@@ -789,14 +795,24 @@ static void vcycle(mf3d_ctx *C, View &V) {
       const BlkLev &B = V.blk[b]->lv[1].desc;
       cudaMemsetAsync(B.phi, 0, (size_t)2 * B.cstr * sizeof(T), C->stream);
     }
+  // levels >= Lc hold FP64 (the coarsest level of an FP32 V-cycle)
+  const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
+  auto relax_g = [&](int g, int q, int it, bool fz) {
+    if (g >= Lc) relax<double>(C, V, g, q, it, fz);
+    else relax<T>(C, V, g, q, it, fz);
+  };
   for (int g = 1; g <= V.Lmax; ++g) {
-    relax<T>(C, V, g, SUB_A, ir, sch == 3);  // a level starts from zero (pp = 0; mgrestr)
-    relax<T>(C, V, g, SUB_C, ip, sch == 3 && ir == 0);
-    if (g < V.Lmax) restr<T>(C, V, g);
+    relax_g(g, SUB_A, ir, sch == 3);  // a level starts from zero (pp = 0; mgrestr)
+    relax_g(g, SUB_C, ip, sch == 3 && ir == 0);
+    if (g < V.Lmax) {
+      if (g + 1 >= Lc) restr<T, double>(C, V, g);
+      else restr<T, T>(C, V, g);
+    }
   }
   for (int g = V.Lmax - 1; g >= 1; --g) {
-    corr<T>(C, V, g);
-    relax<T>(C, V, g, SUB_D, ip, false);
+    if (g + 1 >= Lc) corr<T, double>(C, V, g);
+    else corr<T, T>(C, V, g);
+    relax_g(g, SUB_D, ip, false);
   }
 }
 
@@ -1190,7 +1206,10 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   auto C = std::make_unique<mf3d_ctx>();
   if ((st = ctx_init(C.get(), prm))) return st;
   C->doms.emplace_back(new DomainStore());
-  if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, prm->pl, C->stream))) return st;
+  C->coarse64 = C->elem == 4 && prm->ngrid > 1;
+  if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, C->coarse64 ? 8 : C->elem, prm->pl,
+                         C->stream)))
+    return st;
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
   return MF3D_OK;
@@ -1251,10 +1270,17 @@ static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params 
     }
   auto C = std::make_unique<mf3d_ctx>();
   if ((st = ctx_init(C.get(), prm))) return st;
+  // FP32 V-cycles keep an FP64 coarsest level when every domain bottoms out
+  // on the same level (one launch per level needs one element type)
+  bool same_depth = true;
+  for (int d = 1; d < nd; ++d) same_depth &= domain_ngrid(doms[d]) == domain_ngrid(doms[0]);
+  C->coarse64 = C->elem == 4 && same_depth && domain_ngrid(doms[0]) > 1;
   for (int d = 0; d < nd; ++d) {
     mf3d_block_desc b = lone_block(doms[d]);
     C->doms.emplace_back(new DomainStore());
-    if ((st = build_domain(*C->doms.back(), &b, 1, domain_ngrid(doms[d]), C->elem, prm->pl, C->stream))) return st;
+    if ((st = build_domain(*C->doms.back(), &b, 1, domain_ngrid(doms[d]), C->elem, C->coarse64 ? 8 : C->elem,
+                           prm->pl, C->stream)))
+      return st;
   }
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
