@@ -36,6 +36,7 @@ enum mf3d_status {
   MF3D_OK = 0,
   MF3D_NOT_CONVERGED = 1, /* maxcy exhausted (newsolv_mg.for:59-60 prints) */
   MF3D_DIVERGED = 2,      /* rmax > 100 (newsolv_mg.for:64-83 stops)      */
+  MF3D_PENDING = 3,       /* server: the request has not finished yet       */
   MF3D_E_INVALID = -1,    /* bad config (localparameters.for:84-98,201-206)*/
   MF3D_E_CUDA = -2,       /* a CUDA runtime call failed                     */
   MF3D_E_OOM = -3,        /* device allocation failed or over the cap       */
@@ -262,6 +263,53 @@ int mf3d_profile_read(mf3d_ctx *ctx, double *total_ms, long long *launches,
  * count.  Needs no GPU. */
 long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid,
                         int level, long long *dst, long long *src);
+
+/* ---------------------------------------------------------------------- */
+/* Serving (no counterpart in the reference): a request loop on one device */
+/* that admits independent single-block solves as they arrive, keeps their  */
+/* multigrid hierarchies resident, and advances every resident request by   */
+/* one outer iteration per cycle in shared launches (continuous batching).  */
+/* A request runs exactly its own solve: its result is the same alone and   */
+/* in any mix.                                                              */
+/* ---------------------------------------------------------------------- */
+typedef struct mf3d_server mf3d_server;
+
+/* Result and timeline of one request; times in seconds on the server's
+ * steady clock (mf3d_server_clock). */
+typedef struct mf3d_request_info {
+  mf3d_solve_info info;
+  double t_submit, t_admit, t_done;
+} mf3d_request_info;
+
+/* A server for `params` (precision, smoother, sweeps, tolerance, maxcy,
+ * device; params->ngrid is ignored: each request brings its own depth).
+ * Admission: requests enter in arrival order while the resident
+ * hierarchies stay within `mem_cap_bytes` (and the device's free memory)
+ * and at most `max_resident` requests are resident.  A worker thread owns
+ * the device work; submit and poll are thread-safe.  In FP32 precision the
+ * coarsest levels stay FP32 (resident mixes have mixed depths). */
+int mf3d_server_create(const mf3d_params *params, double mem_cap_bytes, int max_resident, mf3d_server **out);
+
+/* Queue one solve: `domain` as for mf3d_batch_create, `fields` device
+ * arrays of one block (borrowed until the request completes: p, u, v, w
+ * are written), dt, alfapr.  Returns a ticket. */
+int mf3d_server_submit(mf3d_server *srv, const mf3d_domain_desc *domain, const mf3d_fields *fields, double dt,
+                       double alfapr, long long *ticket);
+
+/* MF3D_PENDING while the request runs (waiting up to wait_ms for it), else
+ * its final status with `info` filled; a finished ticket is then released. */
+int mf3d_server_poll(mf3d_server *srv, long long ticket, mf3d_request_info *info, int wait_ms);
+
+/* Counters since creation (any pointer may be NULL). */
+int mf3d_server_stats(mf3d_server *srv, long long *submitted, long long *completed, long long *resident,
+                      long long *queued, double *resident_bytes, long long *cycles);
+
+/* Seconds on the steady clock the server stamps requests with. */
+double mf3d_server_clock(void);
+
+/* Stops the worker after the cycle in flight; unfinished requests are
+ * dropped (their fields are left as they are). */
+int mf3d_server_destroy(mf3d_server *srv);
 
 /* Self-test of the quotient the TMA calvel/calmas kernel forms on axes that
  * are not uniform powers of two: for n pairs (x[i], b[i]) in host memory,

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libmf3d.so")
 MF3D_OK = 0
 MF3D_NOT_CONVERGED = 1
 MF3D_DIVERGED = 2
+MF3D_PENDING = 3
 MF3D_E_INVALID = -1
 MF3D_E_CUDA = -2
 MF3D_E_OOM = -3
@@ -107,6 +108,11 @@ class SolveInfo(C.Structure):
     ]
 
 
+class RequestInfo(C.Structure):
+    """mf3d_request_info: a served request's result and timeline (seconds)."""
+    _fields_ = [("info", SolveInfo), ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
 # Every symbol include/mf3d.h declares (checked by the tests).
 EXPORTED_SYMBOLS = (
     "mf3d_build_topology",
@@ -127,6 +133,12 @@ EXPORTED_SYMBOLS = (
     "mf3d_batch_solve_device",
     "mf3d_selftest_divide",
     "mf3d_mgkcyc_device_noalloc",
+    "mf3d_server_create",
+    "mf3d_server_submit",
+    "mf3d_server_poll",
+    "mf3d_server_stats",
+    "mf3d_server_clock",
+    "mf3d_server_destroy",
 )
 
 MF3D_NOALLOC_MAX_BLOCKS = 512
@@ -164,6 +176,15 @@ def _declare(lib):
     lib.mf3d_batch_solve_device.argtypes = [vp, C.POINTER(Fields), _dp, _dp, C.POINTER(SolveInfo), _dp, C.c_int]
     lib.mf3d_profile.argtypes = [vp, C.c_int]
     lib.mf3d_selftest_divide.argtypes = [_dp, _dp, C.c_longlong, _dp, _dp, C.c_int]
+    lib.mf3d_server_create.argtypes = [C.POINTER(Params), C.c_double, C.c_int, C.POINTER(vp)]
+    lib.mf3d_server_submit.argtypes = [vp, C.POINTER(DomainDesc), C.POINTER(Fields), C.c_double, C.c_double,
+                                       C.POINTER(C.c_longlong)]
+    lib.mf3d_server_poll.argtypes = [vp, C.c_longlong, C.POINTER(RequestInfo), C.c_int]
+    lib.mf3d_server_stats.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 4 + [C.POINTER(C.c_double),
+                                                                          C.POINTER(C.c_longlong)]
+    lib.mf3d_server_clock.restype = C.c_double
+    lib.mf3d_server_clock.argtypes = []
+    lib.mf3d_server_destroy.argtypes = [vp]
     lib.mf3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                       C.POINTER(C.c_double)]
     return lib

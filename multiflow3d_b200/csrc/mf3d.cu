@@ -974,7 +974,7 @@ static int solve_end(mf3d_ctx *C, View &V) {
     calvel_calmas<T>(C, V, V.ones.p, V.rmax_scratch.p, 1);
     ++C->launches;
   }
-  k_calvel<<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, V.ds.p);
+  k_calvel<<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, V.ds.p, nullptr);
   ++C->launches;
   return MF3D_OK;
 }
@@ -1498,3 +1498,6 @@ long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid, i
 }
 
 }  // extern "C"
+
+// Serving (request loop over this engine).
+#include "server.cuh"

@@ -487,10 +487,12 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY) k_calvel_calmas_tma(const BlkFld
 
 // Final calvel (press.for:139-198): u, v, w on the faces calvel writes
 // (isu..ieu etc., one face short at a high wall), from the final p.
+// `only` (may be null): domains to update, others are left as they are.
 __global__ void __launch_bounds__(RW_TX *RW_RJ) k_calvel(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                                                         const DomState *__restrict__ ds) {
+                                                         const DomState *__restrict__ ds, const int *__restrict__ only) {
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
+  if (only && !only[F.dom]) return;
   const double dt = ds[F.dom].dt, alfapr = ds[F.dom].alfapr;
   const int nx = F.nx, ny = F.ny;
   const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;

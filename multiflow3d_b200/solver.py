@@ -156,3 +156,60 @@ class Batch:
     @property
     def launches(self) -> int:
         return int(self.lib.mf3d_last_launch_count(self.ctx))
+
+
+class Server:
+    """The request loop (``mf3d_server_*``): submit single-block solves as
+    they arrive; a worker thread in the library admits them by memory,
+    keeps their hierarchies resident and advances all resident requests by
+    one outer iteration per cycle.  ``fields`` are device tensors (ttc
+    layout) borrowed until the request finishes."""
+
+    def __init__(self, params: abi.Params, mem_cap_bytes: float = 150e9, max_resident: int = 256, lib=None):
+        self.lib = lib or abi.load()
+        self.params = params
+        ctx = C.c_void_p()
+        abi.check(self.lib, self.lib.mf3d_server_create(C.byref(params), float(mem_cap_bytes), int(max_resident),
+                                                        C.byref(ctx)), "mf3d_server_create")
+        self.ctx = ctx
+        self._keep = {}
+
+    def submit(self, domain: abi.DomainDesc, fields: dict, dt: float = 1.0, alfapr: float = 1.0) -> int:
+        arr = _dev_fields([fields])
+        t = C.c_longlong()
+        abi.check(self.lib, self.lib.mf3d_server_submit(self.ctx, C.byref(domain), arr, dt, alfapr, C.byref(t)),
+                  "mf3d_server_submit")
+        self._keep[t.value] = (domain, arr, fields)
+        return t.value
+
+    def poll(self, ticket: int, wait_ms: int = 0):
+        """(status, RequestInfo) once finished, else (MF3D_PENDING, None)."""
+        info = abi.RequestInfo()
+        st = self.lib.mf3d_server_poll(self.ctx, ticket, C.byref(info), int(wait_ms))
+        if st == abi.MF3D_PENDING:
+            return st, None
+        self._keep.pop(ticket, None)
+        if st == abi.MF3D_E_INVALID and info.t_submit == 0.0:
+            abi.check(self.lib, st, "mf3d_server_poll")
+        return st, info
+
+    def stats(self) -> dict:
+        v = [C.c_longlong() for _ in range(4)] + [C.c_double(), C.c_longlong()]
+        abi.check(self.lib, self.lib.mf3d_server_stats(self.ctx, *[C.byref(x) for x in v]), "mf3d_server_stats")
+        keys = ("submitted", "completed", "resident", "queued", "resident_bytes", "cycles")
+        return {k: x.value for k, x in zip(keys, v)}
+
+    def clock(self) -> float:
+        return self.lib.mf3d_server_clock()
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.mf3d_server_destroy(self.ctx)
+            self.ctx = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -19,7 +19,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def header_symbols():
     txt = open(os.path.join(ROOT, "include", "mf3d.h")).read()
-    return sorted(set(re.findall(r"^\s*(?:int|long long|const char \*)\s*\*?\s*(mf3d_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|double|const char \*)\s*\*?\s*(mf3d_\w+)\s*\(", txt, re.M)))
 
 
 def test_exports_every_header_symbol(lib):
