@@ -502,6 +502,131 @@ def run_batched(args):
     return 0
 
 
+def run_served(args):
+    """Poisson arrivals at each rate of --rates: sizes as the batched
+    workload plus 10 % 384^3 requests, mixed precision at 1e-8, admission
+    capped at 150 GB of resident hierarchies.  Per rate, --requests requests;
+    latency = completion - submission on the server's clock.  Baseline:
+    plain FP64 solves one at a time, FIFO over the same arrival trace, from
+    each domain shape's measured solo solve time."""
+    import numpy as np
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.problems import domain_problem, domain_desc, random_batch, WALL, PERIODIC
+    from multiflow3d_b200.solver import Server, Batch
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(SEED)
+    small = [domain_problem(nx, ny, nz, bc, lib.mf3d_max_levels(nx, ny, nz))
+             for nx, ny, nz, bc in random_batch(64, SEED)]
+    large = [domain_problem(384, 384, 384, bc, lib.mf3d_max_levels(384, 384, 384))
+             for bc in ((PERIODIC, WALL, PERIODIC), (WALL, WALL, WALL))]
+    templates = small + large
+    ro = ("ustar", "vstar", "wstar")
+    rw = ("u", "v", "w", "p")
+    tmpl = []
+    for i, pr in enumerate(templates):
+        f = pr.block_fields(seed=SEED + 1000 + i)[0]
+        tmpl.append({k: torch.from_numpy(f[k]).to(dev) for k in ro + rw})
+
+    def fresh(i):
+        t = tmpl[i]
+        d = {k: t[k] for k in ro}
+        for k in rw:
+            d[k] = t[k].clone()
+        return d
+
+    def draw(n):
+        big = rng.random(n) < 0.10
+        return [int(len(small) + rng.integers(0, len(large))) if b else int(rng.integers(0, len(small))) for b in big]
+
+    prm = small[0].params(mg_itrsch=3, maxcy=400, eps=1e-8, precision=abi.MF3D_PREC_FP32)
+    # baseline service times: plain FP64 solo solves (warm), per template
+    p64 = small[0].params(mg_itrsch=3, maxcy=400, eps=1e-8, precision=abi.MF3D_PREC_FP64)
+    p64.ngrid = 1
+    service = []
+    for i, pr in enumerate(templates):
+        b = Batch([domain_desc(pr)], p64, lib)
+        d = fresh(i)
+        b.solve_device([d])  # warm-up (graph capture)
+        best = None
+        for _ in range(2):
+            d = fresh(i)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.solve_device([d])
+            torch.cuda.synchronize()
+            dt_ = time.perf_counter() - t0
+            best = dt_ if best is None else min(best, dt_)
+        b.close()
+        service.append(best)
+    results = []
+    rates = [float(x) for x in args.rates.split(",")]
+    for lam in rates:
+        kinds = draw(args.requests)
+        gaps = rng.exponential(1.0 / lam, size=args.requests)
+        arrivals = np.cumsum(gaps) - gaps[0]
+        srv = Server(prm, mem_cap_bytes=150e9, max_resident=512, lib=lib)
+        # warm the server's kernels with one small request
+        w0 = fresh(0)
+        torch.cuda.synchronize()
+        w = srv.submit(domain_desc(templates[0]), w0)
+        while srv.poll(w, wait_ms=50)[0] == abi.MF3D_PENDING:
+            pass
+        held, tickets = {}, []
+        t0 = time.perf_counter()
+        for a, kind in zip(arrivals, kinds):
+            now = time.perf_counter() - t0
+            if a > now:
+                time.sleep(a - now)
+            f = fresh(kind)
+            torch.cuda.current_stream().synchronize()  # the server's streams do not order after ours
+            t = srv.submit(domain_desc(templates[kind]), f)
+            held[t] = f
+            tickets.append(t)
+        done = {}
+        while len(done) < len(tickets):
+            for t in tickets:
+                if t not in done:
+                    st, info = srv.poll(t, wait_ms=2)
+                    if st != abi.MF3D_PENDING:
+                        done[t] = (st, info)
+                        held.pop(t, None)
+        stats = srv.stats()
+        prof = srv.profile()
+        srv.close()
+        lat = np.array([done[t][1].t_done - done[t][1].t_submit for t in tickets])
+        t_first = min(done[t][1].t_submit for t in tickets)
+        t_last = max(done[t][1].t_done for t in tickets)
+        ok = sum(done[t][0] == abi.MF3D_OK for t in tickets)
+        # FIFO baseline over the same trace
+        tb, lb = 0.0, []
+        for a, kind in zip(arrivals, kinds):
+            start = max(tb, a)
+            tb = start + service[kind]
+            lb.append(tb - a)
+        lb = np.array(lb)
+        results.append({
+            "rate_per_s": lam, "requests": len(tickets), "large": int(sum(k >= len(small) for k in kinds)),
+            "converged": int(ok), "throughput": len(tickets) / (t_last - t_first),
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "cycles": stats["cycles"], "worker_s": prof,
+            "plain_fp64_fifo": {"throughput": len(tickets) / tb, "p50_s": float(np.percentile(lb, 50)),
+                                "p99_s": float(np.percentile(lb, 99))},
+        })
+    line = {
+        "metric": "served_solves_per_s", "value": results[-1]["throughput"], "unit": UNIT, "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f32 V-cycle, f64 outer", "data": "synthetic",
+        "config": {"workload": "Poisson arrivals; sizes as the batched workload plus 10% 384^3; mixed precision "
+                               "tol 1e-8; admission cap 150 GB; continuous batching (one outer iteration per cycle)"},
+        "rates": results,
+        "baseline_note": "plain FP64 one-at-a-time: measured solo solve time per domain shape, FIFO over the same "
+                         "arrival trace",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -509,8 +634,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mf3d", choices=["mf3d", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="multiblock", choices=["multiblock", "mixed", "batched"],
-                    help="multiblock: the default FP64 line; mixed / batched: the further workloads (1 GPU)")
+    ap.add_argument("--workload", default="multiblock", choices=["multiblock", "mixed", "batched", "served"],
+                    help="multiblock: the default FP64 line; mixed / batched / served: the further workloads (1 GPU)")
+    ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
+    ap.add_argument("--requests", type=int, default=200, help="served: requests per rate")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -518,6 +645,8 @@ def main():
         return run_mixed(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "served":
+        return run_served(args)
     return run_gpu(args)
 
 

@@ -292,7 +292,9 @@ int mf3d_server_create(const mf3d_params *params, double mem_cap_bytes, int max_
 
 /* Queue one solve: `domain` as for mf3d_batch_create, `fields` device
  * arrays of one block (borrowed until the request completes: p, u, v, w
- * are written), dt, alfapr.  Returns a ticket. */
+ * are written), dt, alfapr.  Returns a ticket.  The server's streams do not
+ * order after the caller's: the fields' contents must be complete on the
+ * device when this is called (synchronise the stream that produced them). */
 int mf3d_server_submit(mf3d_server *srv, const mf3d_domain_desc *domain, const mf3d_fields *fields, double dt,
                        double alfapr, long long *ticket);
 
@@ -303,6 +305,12 @@ int mf3d_server_poll(mf3d_server *srv, long long ticket, mf3d_request_info *info
 /* Counters since creation (any pointer may be NULL). */
 int mf3d_server_stats(mf3d_server *srv, long long *submitted, long long *completed, long long *resident,
                       long long *queued, double *resident_bytes, long long *cycles);
+
+/* Worker seconds spent (summed over the lanes) building hierarchies,
+ * rebuilding the launch tables for a new mix, running cycles (launch to
+ * completion check) and finishing requests; counts of builds and rebuilds. */
+int mf3d_server_profile(mf3d_server *srv, double *build_s, double *rebuild_s, double *cycle_s, double *finish_s,
+                        long long *builds, long long *rebuilds);
 
 /* Seconds on the steady clock the server stamps requests with. */
 double mf3d_server_clock(void);

@@ -138,6 +138,7 @@ EXPORTED_SYMBOLS = (
     "mf3d_server_poll",
     "mf3d_server_stats",
     "mf3d_server_clock",
+    "mf3d_server_profile",
     "mf3d_server_destroy",
 )
 
@@ -182,6 +183,7 @@ def _declare(lib):
     lib.mf3d_server_poll.argtypes = [vp, C.c_longlong, C.POINTER(RequestInfo), C.c_int]
     lib.mf3d_server_stats.argtypes = [vp] + [C.POINTER(C.c_longlong)] * 4 + [C.POINTER(C.c_double),
                                                                           C.POINTER(C.c_longlong)]
+    lib.mf3d_server_profile.argtypes = [vp] + [C.POINTER(C.c_double)] * 4 + [C.POINTER(C.c_longlong)] * 2
     lib.mf3d_server_clock.restype = C.c_double
     lib.mf3d_server_clock.argtypes = []
     lib.mf3d_server_destroy.argtypes = [vp]

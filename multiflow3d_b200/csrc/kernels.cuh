@@ -548,33 +548,56 @@ __global__ void __launch_bounds__(kTile) k_prolong(const BlkLev *__restrict__ fl
 // ---------------------------------------------------------------------------
 // Halo copies of one level: the composition of mgbound + exchangepp +
 // mgbound + exchbc_mgpp as element pairs (dst block, dst offset, src block,
-// src offset) against the state before the refresh.  Pairs [0, nstaged)
-// have a source that is itself overwritten: k_halo_stage reads those first,
-// k_halo_apply writes everything.
+// src offset) against the state before the refresh.  Each domain keeps its
+// pairs resident on the device (block indices local to the domain, pairs
+// whose source is itself overwritten first); a view lists one segment per
+// domain.  k_halo_stage reads the staged sources of every segment,
+// k_halo_apply then writes every pair.  A thread finds its segment by binary
+// search over the segments' first indices.
 // ---------------------------------------------------------------------------
 struct HaloCopy {
   int dblk, doff, sblk, soff;
 };
-template <typename T>
-__global__ void k_halo_stage(const BlkLev *__restrict__ bl, const HaloCopy *__restrict__ hc, int nstaged,
-                             const int *__restrict__ act, T *__restrict__ buf) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nstaged) return;
-  const HaloCopy c = hc[t];
-  const BlkLev S = bl[c.sblk];
-  if (!act[S.dom]) return;
-  buf[t] = phi_of<T>(S)[c.soff];
+struct HaloSeg {
+  const HaloCopy *pairs;  // the domain's pairs at this level
+  long long start;        // first thread index of the segment (apply)
+  long long sstart;       // first thread index / stage slot of its staged pairs
+  int n, nstaged;         // pairs, staged pairs
+  int blk_base;           // view index of the domain's first block
+  int dom;                // view domain
+};
+// Last segment whose key(seg) <= t (segments in increasing key order).
+template <bool STAGED>
+__device__ __forceinline__ int halo_segment(const HaloSeg *__restrict__ seg, int nseg, long long t) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if ((STAGED ? seg[mid].sstart : seg[mid].start) <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
 }
 template <typename T>
-__global__ void k_halo_apply(const BlkLev *__restrict__ bl, const HaloCopy *__restrict__ hc, int n, int nstaged,
+__global__ void k_halo_stage(const BlkLev *__restrict__ bl, const HaloSeg *__restrict__ seg, int nseg,
+                             long long nstaged, const int *__restrict__ act, T *__restrict__ buf) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nstaged) return;
+  const HaloSeg &S = seg[halo_segment<true>(seg, nseg, t)];
+  if (!act[S.dom]) return;
+  const HaloCopy c = S.pairs[t - S.sstart];
+  buf[t] = phi_of<T>(bl[S.blk_base + c.sblk])[c.soff];
+}
+template <typename T>
+__global__ void k_halo_apply(const BlkLev *__restrict__ bl, const HaloSeg *__restrict__ seg, int nseg, long long n,
                              const int *__restrict__ act, const T *__restrict__ buf) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const HaloCopy c = hc[t];
-  const BlkLev D = bl[c.dblk];
-  if (!act[D.dom]) return;
-  const T v = t < nstaged ? buf[t] : phi_of<T>(bl[c.sblk])[c.soff];
-  phi_of<T>(D)[c.doff] = v;
+  const HaloSeg &S = seg[halo_segment<false>(seg, nseg, t)];
+  if (!act[S.dom]) return;
+  const long long u = t - S.start;
+  const HaloCopy c = S.pairs[u];
+  const T v = u < S.nstaged ? buf[S.sstart + u] : phi_of<T>(bl[S.blk_base + c.sblk])[c.soff];
+  phi_of<T>(bl[S.blk_base + c.dblk])[c.doff] = v;
 }
 
 // Zero the ghost shell of a set of blocks (pp = 0 before a V-cycle): one

@@ -43,33 +43,93 @@ void set_error(const std::string &msg) { g_err = msg; }
     }                                                                                              \
   } while (0)
 
+// Device memory of the library comes from a stream-ordered pool per device
+// that keeps up to kPoolKeepBytes of freed memory for reuse.  Allocations
+// and frees are ordered on the stream of the context making them (an
+// AllocScope names it), so they neither wait for other streams' kernels -
+// cudaMalloc/cudaFree may synchronise the whole device - nor go back to the
+// driver for every rebuilt table.  Outside a scope, plain cudaMalloc/cudaFree.
+constexpr unsigned long long kPoolKeepBytes = 8ull << 30;
+static thread_local cudaStream_t g_alloc_stream = nullptr;
+struct AllocScope {
+  cudaStream_t prev;
+  explicit AllocScope(cudaStream_t s) : prev(g_alloc_stream) { g_alloc_stream = s; }
+  ~AllocScope() { g_alloc_stream = prev; }
+};
+static cudaMemPool_t device_pool() {
+  constexpr int kMaxDevices = 64;
+  static std::mutex mu;
+  static cudaMemPool_t pools[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+    unsigned long long keep = kPoolKeepBytes;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = pool;
+  }
+  return pools[dev];
+}
+
+// A device array.  alloc() keeps the current allocation when it is large
+// enough (rebuilt launch tables reuse their buffers).
 template <typename T>
 struct DevBuf {
   T *p = nullptr;
   size_t n = 0;
+  size_t cap = 0;
+  cudaStream_t s_alloc = nullptr;  // stream the allocation is ordered on (null: cudaMalloc)
   DevBuf() = default;
   DevBuf(const DevBuf &) = delete;
   DevBuf &operator=(const DevBuf &) = delete;
-  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf(DevBuf &&o) noexcept : p(o.p), n(o.n), cap(o.cap), s_alloc(o.s_alloc) {
+    o.p = nullptr; o.n = 0; o.cap = 0;
+  }
   DevBuf &operator=(DevBuf &&o) noexcept {
     if (this != &o) {
-      if (p) cudaFree(p);
-      p = o.p; n = o.n; o.p = nullptr; o.n = 0;
+      release();
+      p = o.p; n = o.n; cap = o.cap; s_alloc = o.s_alloc;
+      o.p = nullptr; o.n = 0; o.cap = 0;
     }
     return *this;
   }
-  ~DevBuf() { if (p) cudaFree(p); }
+  ~DevBuf() { release(); }
+  void release() {
+    if (!p) return;
+    if (s_alloc) cudaFreeAsync(p, s_alloc);
+    else cudaFree(p);
+    p = nullptr;
+    n = cap = 0;
+  }
   int alloc(size_t count) {
-    if (p) { cudaFree(p); p = nullptr; }
-    n = count;
+    if (p && count <= cap) {
+      n = count;
+      return MF3D_OK;
+    }
+    release();
     if (count == 0) return MF3D_OK;
-    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    cudaError_t e;
+    cudaMemPool_t pool = g_alloc_stream ? device_pool() : nullptr;
+    if (pool) {
+      e = cudaMallocFromPoolAsync((void **)&p, count * sizeof(T), pool, g_alloc_stream);
+      s_alloc = g_alloc_stream;
+    } else {
+      e = cudaMalloc(&p, count * sizeof(T));
+      s_alloc = nullptr;
+    }
     if (e != cudaSuccess) {
       p = nullptr;
-      n = 0;
-      set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+      set_error(std::string("device allocation: ") + cudaGetErrorString(e));
       return e == cudaErrorMemoryAllocation ? MF3D_E_OOM : MF3D_E_CUDA;
     }
+    n = cap = count;
     return MF3D_OK;
   }
   int upload(const std::vector<T> &h, cudaStream_t s) {
@@ -121,6 +181,7 @@ static double div_reciprocal(double b) {
 // ---------------------------------------------------------------------------
 struct LevelStore {
   int elem = 8;  // bytes per value of this level
+  std::vector<std::vector<char>> host;  // host images of the uploaded small arrays
   DevBuf<char> phi, rhs, coef, geo;
   DevBuf<CUtensorMap> tmaps;  // phi c0, phi c1, rhs c0, rhs c1
   BlkLev desc;  // host copy with device pointers
@@ -252,16 +313,16 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
         for (int c = 0; c < n + 2; ++c) geo.push_back(0.0);
       }
     }
+    // host images of the small per-level arrays stay with the level until
+    // the copies have run (one synchronisation at the end of the domain build)
     auto put = [&](DevBuf<char> &buf, const std::vector<double> &v) -> int {
       int r = buf.alloc(v.size() * elem);
       if (r) return r;
-      if (elem == 8) {
-        CK(cudaMemcpyAsync(buf.p, v.data(), v.size() * 8, cudaMemcpyHostToDevice, s));
-      } else {
-        std::vector<float> f(v.begin(), v.end());
-        CK(cudaMemcpyAsync(buf.p, f.data(), f.size() * 4, cudaMemcpyHostToDevice, s));
-        CK(cudaStreamSynchronize(s));  // f is a local
-      }
+      L.host.emplace_back(v.size() * elem);
+      char *h = L.host.back().data();
+      if (elem == 8) std::memcpy(h, v.data(), v.size() * 8);
+      else for (size_t q = 0; q < v.size(); ++q) ((float *)h)[q] = (float)v[q];
+      CK(cudaMemcpyAsync(buf.p, h, v.size() * elem, cudaMemcpyHostToDevice, s));
       return MF3D_OK;
     };
     if ((st = put(L.coef, coef))) return st;
@@ -278,8 +339,9 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
       if ((st = colour_map(&tm[2 + c], L.rhs.p + (size_t)c * B.cstr * elem, elem, B, W, RB_RJ))) return st;
     }
     if ((st = L.tmaps.alloc(4))) return st;
-    CK(cudaMemcpyAsync(L.tmaps.p, tm, sizeof tm, cudaMemcpyHostToDevice, s));
-    CK(cudaStreamSynchronize(s));  // tm is a local
+    L.host.emplace_back(sizeof tm);
+    std::memcpy(L.host.back().data(), tm, sizeof tm);
+    CK(cudaMemcpyAsync(L.tmaps.p, L.host.back().data(), sizeof tm, cudaMemcpyHostToDevice, s));
     B.tm = L.tmaps.p;
   }
   // level-1 field geometry: widths, face distances (bit-exact dx on a uniform axis)
@@ -332,6 +394,7 @@ struct DomainStore {
   std::vector<std::unique_ptr<BlockStore>> blocks;
   std::vector<std::vector<HaloLocal>> halo;  // per level, staged pairs first
   std::vector<int> nstaged;                  // per level
+  std::vector<DevBuf<HaloCopy>> dhalo;       // per level, the same pairs on the device
   std::vector<FaceRule> rules;               // 6 per block, domain-local sources
   size_t bytes = 0;
 };
@@ -367,8 +430,8 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
       acc += geom[b].cells();
     }
     std::vector<HaloPair> pairs = build_halo_map(descs, geom, base);
-    std::unordered_set<long long> dsts;
-    for (auto &p : pairs) dsts.insert(p.dst);
+    std::vector<bool> is_dst(acc, false);  // cells written by the refresh
+    for (auto &p : pairs) is_dst[p.dst] = true;
     auto loc = [&](long long id, int &blk, int &off) {
       int b = (int)(std::upper_bound(base.begin(), base.end(), id) - base.begin()) - 1;
       long long lin = id - base[b];
@@ -382,7 +445,7 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
     };
     for (int pass = 0; pass < 2; ++pass)
       for (auto &p : pairs) {
-        const bool staged = dsts.count(p.src) > 0;
+        const bool staged = is_dst[p.src];
         if ((pass == 0) != staged) continue;
         HaloLocal h;
         loc(p.dst, h.dblk, h.doff);
@@ -391,6 +454,17 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
         if (staged) D.nstaged[g]++;
       }
   }
+  // resident device copies (domain-local block indices)
+  D.dhalo.clear();
+  D.dhalo.resize(ngrid + 1);
+  for (int g = 1; g <= ngrid; ++g) {
+    std::vector<HaloCopy> h(D.halo[g].size());
+    for (size_t q = 0; q < h.size(); ++q)
+      h[q] = HaloCopy{D.halo[g][q].dblk, D.halo[g][q].doff, D.halo[g][q].sblk, D.halo[g][q].soff};
+    if ((st = D.dhalo[g].upload(h, s))) return st;
+    D.bytes += h.size() * sizeof(HaloCopy);
+  }
+  CK(cudaStreamSynchronize(s));  // the host vectors are locals
   return MF3D_OK;
 }
 
@@ -408,8 +482,9 @@ struct ViewLevel {
   int n_rtile = 0, n_ptile = 0, rkch = 1, pkch = 1;
   DevBuf<int> list[3];
   int n_list[3] = {0, 0, 0};
-  DevBuf<HaloCopy> halo[3];
-  int n_halo[3] = {0, 0, 0}, n_staged[3] = {0, 0, 0};
+  DevBuf<HaloSeg> hseg[3];            // one segment per domain of the subset
+  int n_hseg[3] = {0, 0, 0};
+  long long n_halo[3] = {0, 0, 0}, n_staged[3] = {0, 0, 0};
   DevBuf<char> stage[3];              // staged halo values
   long long cells_sub[3] = {0, 0, 0}; // interior cells of each subset
   int ngg = 0;
@@ -428,6 +503,7 @@ struct View {
   DevBuf<DomState> ds;
   DevBuf<int> act, ones;
   DevBuf<int> err;                    // device error code (a TMA wait that gave up)
+  DevBuf<int> budget;                 // iterations left in the server's bounded loop
   DevBuf<CUtensorMap> fmaps;          // per block: p, ustar, vstar, wstar (bound fields)
   bool fields_tma = false;            // bound fields admit the TMA calvel/calmas
   DevBuf<unsigned long long> rmax, rmax_scratch;
@@ -632,25 +708,32 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       if ((st = L.list[q].upload(li[q], s))) return st;
       work_elems = std::max(work_elems, (size_t)L.n_list[q] * 128 * 2 * L.ngg);
     }
-    // halo lists: staged pairs of every domain first, then the direct ones
+    // halo segments: the domains' resident pair lists
     for (int q = 0; q < 3; ++q) {
-      std::vector<HaloCopy> staged, direct;
+      std::vector<HaloSeg> segs;
+      long long n = 0, ns = 0;
       for (int d = 0; d < nd; ++d) {
         const DomainStore &D = *doms[d];
         if (g > D.ngrid) continue;
         const bool in = q == SUB_A || (q == SUB_C ? g == D.ngrid : g < D.ngrid);
-        if (!in) continue;
-        const auto &H = D.halo[g];
-        for (size_t p = 0; p < H.size(); ++p) {
-          HaloCopy c{dom_base[d] + H[p].dblk, H[p].doff, dom_base[d] + H[p].sblk, H[p].soff};
-          ((int)p < D.nstaged[g] ? staged : direct).push_back(c);
-        }
+        if (!in || D.halo[g].empty()) continue;
+        HaloSeg sg;
+        sg.pairs = D.dhalo[g].p;
+        sg.start = n;
+        sg.sstart = ns;
+        sg.n = (int)D.halo[g].size();
+        sg.nstaged = D.nstaged[g];
+        sg.blk_base = dom_base[d];
+        sg.dom = d;
+        n += sg.n;
+        ns += sg.nstaged;
+        segs.push_back(sg);
       }
-      L.n_staged[q] = (int)staged.size();
-      staged.insert(staged.end(), direct.begin(), direct.end());
-      L.n_halo[q] = (int)staged.size();
-      if ((st = L.halo[q].upload(staged, s))) return st;
-      if ((st = L.stage[q].alloc((size_t)std::max(L.n_staged[q], 1) * 8))) return st;
+      L.n_hseg[q] = (int)segs.size();
+      L.n_halo[q] = n;
+      L.n_staged[q] = ns;
+      if ((st = L.hseg[q].upload(segs, s))) return st;
+      if ((st = L.stage[q].alloc((size_t)std::max<long long>(ns, 1) * 8))) return st;
     }
   }
   if (C->prm.mg_itrsch == 2 && (st = V.work.alloc(std::max<size_t>(work_elems, 1) * 8))) return st;
@@ -695,6 +778,8 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
   if ((st = V.ones.upload(ones, s))) return st;
   if ((st = V.err.alloc(1))) return st;
   CK(cudaMemsetAsync(V.err.p, 0, sizeof(int), s));
+  if ((st = V.budget.alloc(1))) return st;
+  CK(cudaMemsetAsync(V.budget.p, 0, sizeof(int), s));
   if ((st = V.rmax.alloc(std::max(nd, 1)))) return st;
   if ((st = V.rmax_scratch.alloc(std::max(nd, 1)))) return st;
   CK(cudaMemsetAsync(V.rmax.p, 0, V.rmax.n * sizeof(unsigned long long), s));
@@ -713,12 +798,12 @@ static void halo(mf3d_ctx *C, View &V, int g, int q) {
   if (!L.n_halo[q]) return;
   T *buf = (T *)L.stage[q].p;
   if (L.n_staged[q]) {
-    k_halo_stage<T><<<grid_of(L.n_staged[q], 256), 256, 0, C->stream>>>(L.tab.p, L.halo[q].p, L.n_staged[q],
-                                                                       V.act.p, buf);
+    k_halo_stage<T><<<grid_of(L.n_staged[q], 256), 256, 0, C->stream>>>(L.tab.p, L.hseg[q].p, L.n_hseg[q],
+                                                                       L.n_staged[q], V.act.p, buf);
     ++C->launches;
   }
-  k_halo_apply<T><<<grid_of(L.n_halo[q], 256), 256, 0, C->stream>>>(L.tab.p, L.halo[q].p, L.n_halo[q],
-                                                                   L.n_staged[q], V.act.p, buf);
+  k_halo_apply<T><<<grid_of(L.n_halo[q], 256), 256, 0, C->stream>>>(L.tab.p, L.hseg[q].p, L.n_hseg[q],
+                                                                   L.n_halo[q], V.act.p, buf);
   ++C->launches;
 }
 
@@ -842,7 +927,7 @@ static void calvel_calmas(mf3d_ctx *C, View &V, const int *act, unsigned long lo
 // One outer iteration of newsolv_mg (newsolv_mg.for:25-58) for every active
 // domain: V-cycle, p += pp, p halo + pbound, calvel + calmas, bookkeeping.
 template <typename T>
-static void iteration_body(mf3d_ctx *C, View &V, bool loop_graph) {
+static void iteration_body(mf3d_ctx *C, View &V, int loop_graph) {
   cudaStream_t s = C->stream;
   vcycle<T>(C, V);
   k_add_correction<T><<<V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_l1cells.p, V.act.p);
@@ -851,7 +936,7 @@ static void iteration_body(mf3d_ctx *C, View &V, bool loop_graph) {
   calvel_calmas<T>(C, V, V.act.p, V.rmax.p, 0);
   prof_end(C, MF3D_PROF_CALMAS);
   k_iter_end<<<1, 256, 0, s>>>(V.ds.p, (int)V.dom.size(), V.rmax.p, V.hist.p, V.hcap, V.act.p, V.cond,
-                               loop_graph ? 1 : 0);
+                               loop_graph, V.budget.p);
   C->launches += 4;
 }
 
@@ -873,18 +958,43 @@ static int build_graphs(mf3d_ctx *C, View &V) {
   cudaGraph_t body = np.conditional.phGraph_out[0];
   CK(cudaStreamBeginCaptureToGraph(C->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
   C->launches = 0;
-  iteration_body<T>(C, V, true);
+  iteration_body<T>(C, V, 1);
   V.launches_per_iter = C->launches;
   cudaGraph_t captured;
   CK(cudaStreamEndCapture(C->stream, &captured));
   CK(cudaGraphInstantiate(&V.x_loop, V.g_loop, 0));
   // one iteration (the server's per-cycle step)
   CK(cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeRelaxed));
-  iteration_body<T>(C, V, false);
+  iteration_body<T>(C, V, 0);
   CK(cudaStreamEndCapture(C->stream, &V.g_once));
   CK(cudaGraphInstantiate(&V.x_once, V.g_once, 0));
   C->launches = saved_launches;
   C->prof_kind = saved_prof;
+  return MF3D_OK;
+}
+
+// The server's cycle: a WHILE node around one iteration that runs until a
+// domain stops, none is left, or V.budget iterations have run.
+template <typename T>
+static int build_server_graph(mf3d_ctx *C, View &V) {
+  if (V.x_loop) return MF3D_OK;
+  CK(cudaGraphCreate(&V.g_loop, 0));
+  CK(cudaGraphConditionalHandleCreate(&V.cond, V.g_loop, 1u, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {cudaGraphNodeTypeConditional};
+  np.conditional.handle = V.cond;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, V.g_loop, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(C->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  const long long saved = C->launches;
+  iteration_body<T>(C, V, 2);
+  V.launches_per_iter = C->launches - saved;
+  C->launches = saved;
+  cudaGraph_t captured;
+  CK(cudaStreamEndCapture(C->stream, &captured));
+  CK(cudaGraphInstantiate(&V.x_loop, V.g_loop, 0));
   return MF3D_OK;
 }
 
@@ -1036,7 +1146,7 @@ static int solve_view(mf3d_ctx *C, View &V, const double *dt, const double *alfa
     } else {
       std::vector<int> act(nd);
       for (int it = 1; it <= maxcy; ++it) {
-        iteration_body<T>(C, V, false);
+        iteration_body<T>(C, V, 0);
         CK(cudaMemcpyAsync(act.data(), V.act.p, nd * sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         prof_collect(C);
@@ -1158,14 +1268,19 @@ static int check_params(const mf3d_params *prm) {
   return MF3D_OK;
 }
 
-static int ctx_init(mf3d_ctx *C, const mf3d_params *prm) {
+static int ctx_init(mf3d_ctx *C, const mf3d_params *prm, bool nonblocking = false, bool high_priority = false) {
   C->prm = *prm;
   C->device = prm->device;
   C->elem = prm->precision == MF3D_PREC_FP64 ? 8 : 4;
   CK(cudaSetDevice(C->device));
-  // A blocking stream: it orders after work the caller queued on the legacy
-  // default stream (e.g. the copies that produced the device inputs).
-  CK(cudaStreamCreateWithFlags(&C->stream, cudaStreamDefault));
+  // A blocking stream orders after work the caller queued on the legacy
+  // default stream (e.g. the copies that produced the device inputs).  The
+  // server's lanes use non-blocking streams, so that no lane waits for the
+  // caller's or the other lane's work through the legacy stream.
+  int lo = 0, hi = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+  CK(cudaStreamCreateWithPriority(&C->stream, nonblocking ? cudaStreamNonBlocking : cudaStreamDefault,
+                                  high_priority ? hi : lo));
   CK(cudaEventCreate(&C->ev0));
   CK(cudaEventCreate(&C->ev1));
   const char *e = getenv("MF3D_NO_GRAPH");
@@ -1205,6 +1320,7 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   }
   auto C = std::make_unique<mf3d_ctx>();
   if ((st = ctx_init(C.get(), prm))) return st;
+  AllocScope scope(C->stream);
   C->doms.emplace_back(new DomainStore());
   C->coarse64 = C->elem == 4 && prm->ngrid > 1;
   if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, C->coarse64 ? 8 : C->elem, prm->pl,
@@ -1270,6 +1386,7 @@ static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params 
     }
   auto C = std::make_unique<mf3d_ctx>();
   if ((st = ctx_init(C.get(), prm))) return st;
+  AllocScope scope(C->stream);
   // FP32 V-cycles keep an FP64 coarsest level when every domain bottoms out
   // on the same level (one launch per level needs one element type)
   bool same_depth = true;
@@ -1406,6 +1523,7 @@ int mf3d_newsolv_mg_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, do
   if (!C || !fields) { mf3d::set_error("mf3d_newsolv_mg_device: bad arguments"); return MF3D_E_INVALID; }
   if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  mf3d::AllocScope scope(C->stream);
   int st = mf3d::bind_fields(C, *C->view, fields);
   if (st) return st;
   return mf3d::run_solve(C, &dt, &alfapr, info, hist, cap);
@@ -1416,6 +1534,7 @@ int mf3d_newsolv_mg(mf3d_ctx *C, const mf3d_fields *fields, double dt, double al
   if (!C || !fields) { mf3d::set_error("mf3d_newsolv_mg: bad arguments"); return MF3D_E_INVALID; }
   if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  mf3d::AllocScope scope(C->stream);
   return mf3d::host_solve(C, fields, &dt, &alfapr, info, hist, cap);
 }
 
@@ -1423,6 +1542,7 @@ int mf3d_batch_solve_device(mf3d_ctx *C, const mf3d_fields *fields, const double
                             mf3d_solve_info *infos, double *hist, int hcap) {
   if (!C || !fields || !dt || !alfapr) { mf3d::set_error("mf3d_batch_solve_device: bad arguments"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  mf3d::AllocScope scope(C->stream);
   int st = mf3d::bind_fields(C, *C->view, fields);
   if (st) return st;
   return mf3d::run_solve(C, dt, alfapr, infos, hist, hcap);
@@ -1431,6 +1551,7 @@ int mf3d_batch_solve_device(mf3d_ctx *C, const mf3d_fields *fields, const double
 int mf3d_mgkcyc_device(mf3d_ctx *C, double *const *su, double *const *pp) {
   if (!C || !su || !pp) { mf3d::set_error("mf3d_mgkcyc_device: bad arguments"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  mf3d::AllocScope scope(C->stream);
   if (C->elem == 8) return mf3d::mgkcyc_view<double>(C, *C->view, su, pp);
   return mf3d::mgkcyc_view<float>(C, *C->view, su, pp);
 }

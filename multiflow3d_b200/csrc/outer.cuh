@@ -529,9 +529,12 @@ __global__ void k_dom_init(DomState *ds, int ndom, unsigned long long *rmax_slot
 // record rmax, count the iteration, test `rmax < eps .and. iter > 1` (or
 // maxcy); a domain that stops is switched off for every later launch.  In
 // the solve graph, also sets the WHILE condition: any domain still running.
+// in_graph 2 (the server's bounded loop): the WHILE condition also ends the
+// loop when a domain stops in this iteration or when `budget` iterations
+// have run, so the host can hand results back and admit new requests.
 __global__ void k_iter_end(DomState *ds, int ndom, unsigned long long *rmax_slot, double *hist, int hcap, int *act,
-                           cudaGraphConditionalHandle cond, int in_graph) {
-  int any = 0;
+                           cudaGraphConditionalHandle cond, int in_graph, int *budget) {
+  int any = 0, stopped = 0;
   for (int d = threadIdx.x; d < ndom; d += blockDim.x) {
     if (!act[d]) continue;
     DomState &D = ds[d];
@@ -546,11 +549,22 @@ __global__ void k_iter_end(DomState *ds, int ndom, unsigned long long *rmax_slot
     else if (r < D.eps && it > 1) done = 1;
     else if (it >= D.maxcy) done = 3;
     D.done = done;
-    if (done) act[d] = 0;
-    else any = 1;
+    if (done) {
+      act[d] = 0;
+      stopped = 1;
+    } else {
+      any = 1;
+    }
   }
   any = __syncthreads_or(any);
-  if (in_graph && threadIdx.x == 0) cudaGraphSetConditional(cond, any ? 1u : 0u);
+  stopped = __syncthreads_or(stopped);
+  if (threadIdx.x == 0) {
+    if (in_graph == 1) cudaGraphSetConditional(cond, any ? 1u : 0u);
+    if (in_graph == 2) {
+      const int left = --budget[0];
+      cudaGraphSetConditional(cond, (any && !stopped && left > 0) ? 1u : 0u);
+    }
+  }
 }
 
 // Level-1 rhs := su (mgkcyc's copy-in, mgsolver.for:250-263) from a ttc array.

@@ -53,34 +53,58 @@ static double domain_bytes(const mf3d_domain_desc &d, int ngrid, int elem) {
   return b;
 }
 
+// Shape key of a domain whose storage can be reused by a later request
+// (uniform spacing only: stretched widths are caller arrays); "" otherwise.
+static std::string shape_key(const mf3d_domain_desc &d, int ngrid) {
+  if (d.hx || d.hy || d.hz) return std::string();
+  char buf[256];
+  std::snprintf(buf, sizeof buf, "%d,%d,%d,%d,%d,%d,%d,%a,%a,%a", d.nx, d.ny, d.nz, d.bc[0], d.bc[1], d.bc[2], ngrid,
+                d.dx, d.dy, d.dz);
+  return buf;
+}
+
+}  // namespace mf3d
+
+// Requests run in two lanes by size, each with its own worker thread,
+// stream and view: the cycle of a lane costs about the work of its largest
+// resident domains, so small requests do not advance at the pace of large
+// ones; the lanes' kernels share the device concurrently.
+namespace mf3d {
+constexpr int kSrvLanes = 2;
+constexpr double kSrvLargeCells = 8.0e6;  // a request of at least this many cells runs in lane 1
+constexpr int kSrvIters = 8;              // outer iterations per cycle at most (fewer when a request stops)
 }  // namespace mf3d
 
 struct mf3d_server {
-  std::unique_ptr<mf3d_ctx> C;
+  std::unique_ptr<mf3d_ctx> C[mf3d::kSrvLanes];
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
-  std::deque<mf3d::SrvReq *> queue;
+  std::deque<mf3d::SrvReq *> queue[mf3d::kSrvLanes];
   std::unordered_map<long long, std::unique_ptr<mf3d::SrvReq>> reqs;
   long long next_ticket = 1;
   double cap = 0.0;
   int max_resident = 1;
-  double used = 0.0;
+  double used = 0.0;            // estimated bytes of resident requests
+  double pooled = 0.0;          // bytes of retired storage kept for reuse
   long long submitted = 0, completed = 0, resident = 0, cycles = 0;
+  double t_build = 0.0, t_rebuild = 0.0, t_cycle = 0.0, t_finish = 0.0;  // worker seconds, all lanes
+  long long builds = 0, rebuilds = 0;
   bool stop = false;
-  std::thread worker;
+  std::thread worker[mf3d::kSrvLanes];
 };
 
 namespace mf3d {
 
-// Record the end of a request (under the server lock).
-static void srv_finish(mf3d_server *S, SrvReq *r, int status) {
+// Record the end of a request (under the server lock).  `release`: its
+// device bytes are given back now (else when its storage leaves the view).
+static void srv_finish(mf3d_server *S, SrvReq *r, int status, bool release = true) {
   std::lock_guard<std::mutex> lk(S->mu);
   if (r->state == 1) S->resident--;
   r->state = 2;
   r->status = status;
   r->info.info.status = status;
   r->info.t_done = steady_now();
-  S->used -= r->est;
+  if (release) S->used -= r->est;
   S->completed++;
   S->cv_done.notify_all();
 }
@@ -149,45 +173,129 @@ static int srv_status(const DomState &D) {
   return status;
 }
 
+// A position in the current view: a running request, or the storage of one
+// that finished and has been handed back (kept until the next rebuild, since
+// the view's tables still point at it; its domain is inactive meanwhile).
+struct SrvSlot {
+  SrvReq *r = nullptr;
+  std::unique_ptr<DomainStore> dead;
+  std::string key;
+  double est = 0.0;
+};
+
 template <typename T>
-static void srv_loop(mf3d_server *S) {
-  mf3d_ctx *C = S->C.get();
+static void srv_loop(mf3d_server *S, int lane) {
+  mf3d_ctx *C = S->C[lane].get();
+  std::deque<SrvReq *> &queue = S->queue[lane];
   cudaSetDevice(C->device);
   cudaStream_t s = C->stream;
+  AllocScope scope(s);  // the lane's device memory is ordered on its own stream
   View V;
-  std::vector<SrvReq *> res;
+  std::vector<SrvSlot> slots;     // view order
+  std::vector<SrvReq *> pending;  // built, waiting for the next rebuild
   std::vector<int> act;
-  bool dirty = false;
+  // Retired hierarchies kept for later requests of the same shape (they end
+  // a solve with the invariants a fresh one starts with: zero ghost shell of
+  // the level-1 correction, coarse levels rewritten before use).  Oldest
+  // first; evicted when admission needs the memory.
+  std::vector<std::pair<std::string, std::unique_ptr<DomainStore>>> pool;
+  std::vector<double> pool_est;
+  // rebuild pacing: a rebuild (host tables, uploads) costs several cycles
+  // when many domains are resident, so joins and leaves are gathered until
+  // the cycles since the last rebuild have taken about as long as one
+  double rebuild_s = 0.0, cycle_s = 1e-3, since_rebuild_s = 0.0;
+  auto evict_oldest = [&]() {
+    if (pool.empty()) return;
+    pool.erase(pool.begin());
+    const double b = pool_est.front();
+    pool_est.erase(pool_est.begin());
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->pooled -= b;
+  };
   auto fail_all = [&](int st) {
-    for (SrvReq *r : res) {
+    for (SrvSlot &x : slots)
+      if (x.r) {
+        x.r->dom.reset();
+        srv_finish(S, x.r, st);
+      } else if (x.dead) {
+        x.dead.reset();
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->used -= x.est;
+      }
+    for (SrvReq *r : pending) {
       r->dom.reset();
       srv_finish(S, r, st);
     }
-    res.clear();
+    slots.clear();
+    pending.clear();
     V.drop_graphs();
   };
   for (;;) {
+    int live = 0, dead = 0;
+    for (const SrvSlot &x : slots) (x.r ? live : dead) += 1;
     std::vector<SrvReq *> admit;
+    std::vector<int> reuse;  // pool index per admitted request, -1: build
+    bool need_room = false;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      if (res.empty() && S->queue.empty() && !S->stop) S->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+      if (live == 0 && pending.empty() && queue.empty() && !S->stop)
+        S->cv_work.wait_for(lk, std::chrono::milliseconds(20));
       if (S->stop) break;
       // arrival order; a request waits at the head until memory frees up,
-      // unless nothing is resident (then it is admitted and may fail on OOM)
-      while (!S->queue.empty() && (int)(res.size() + admit.size()) < S->max_resident) {
-        SrvReq *r = S->queue.front();
-        if (!(res.empty() && admit.empty()) && S->used + r->est > S->cap) break;
-        S->queue.pop_front();
+      // unless nothing else is resident (then it is admitted and may fail on OOM)
+      std::vector<char> taken(pool.size(), 0);
+      while (!queue.empty() && S->resident < S->max_resident) {
+        SrvReq *r = queue.front();
+        const std::string key = shape_key(r->desc, r->ngrid);
+        int hit = -1;
+        for (size_t q = 0; q < pool.size() && !key.empty(); ++q)
+          if (!taken[q] && pool[q].first == key) { hit = (int)q; break; }
+        const double extra = hit >= 0 ? 0.0 : r->est;  // a pooled store is already counted
+        const bool alone = S->resident == 0;  // nothing resident in any lane
+        if (!alone && S->used + S->pooled + extra > S->cap) {
+          need_room = !pool.empty();
+          break;
+        }
+        queue.pop_front();
+        if (hit >= 0) {
+          taken[hit] = 1;
+          S->pooled -= pool_est[hit];
+        }
         S->used += r->est;
         r->state = 1;
         S->resident++;
         admit.push_back(r);
+        reuse.push_back(hit);
       }
     }
-    for (SrvReq *r : admit) {
-      r->dom.reset(new DomainStore());
-      mf3d_block_desc b = lone_block(r->desc);
-      const int st = build_domain(*r->dom, &b, 1, r->ngrid, C->elem, C->elem, C->prm.pl, s);
+    // take the reused stores out of the pool (highest index first)
+    std::vector<std::unique_ptr<DomainStore>> got(admit.size());
+    {
+      std::vector<std::pair<int, int>> order;
+      for (size_t a = 0; a < admit.size(); ++a)
+        if (reuse[a] >= 0) order.push_back({reuse[a], (int)a});
+      std::sort(order.rbegin(), order.rend());
+      for (auto &o : order) {
+        got[o.second] = std::move(pool[o.first].second);
+        pool.erase(pool.begin() + o.first);
+        pool_est.erase(pool_est.begin() + o.first);
+      }
+    }
+    if (need_room && admit.empty()) evict_oldest();
+    for (size_t a = 0; a < admit.size(); ++a) {
+      SrvReq *r = admit[a];
+      int st = MF3D_OK;
+      if (got[a]) {
+        r->dom = std::move(got[a]);
+      } else {
+        const double tb = steady_now();
+        r->dom.reset(new DomainStore());
+        mf3d_block_desc b = lone_block(r->desc);
+        st = build_domain(*r->dom, &b, 1, r->ngrid, C->elem, C->elem, C->prm.pl, s);
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->t_build += steady_now() - tb;
+        S->builds++;
+      }
       if (st) {
         r->dom.reset();
         srv_finish(S, r, st);
@@ -195,34 +303,81 @@ static void srv_loop(mf3d_server *S) {
       }
       r->info.t_admit = steady_now();
       r->vidx = -1;
-      res.push_back(r);
-      dirty = true;
+      pending.push_back(r);
     }
-    if (res.empty()) continue;
-    if (dirty) {
-      const int st = srv_rebuild<T>(C, V, res);
+    // rebuild the view when requests wait to join or finished ones can leave
+    const bool want = !pending.empty() || dead > 0;
+    const bool due = live == 0 || since_rebuild_s >= rebuild_s || 2 * dead >= (int)slots.size();
+    if (want && due) {
+      const double t0 = steady_now();
+      std::vector<SrvReq *> res;
+      std::vector<SrvSlot> next;
+      for (SrvSlot &x : slots) {
+        if (x.r) {
+          res.push_back(x.r);
+          continue;
+        }
+        // storage of a finished request leaves the view: reuse or free it
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->used -= x.est;
+        if (!x.key.empty()) {
+          pool.emplace_back(x.key, std::move(x.dead));
+          pool_est.push_back(x.est);
+          S->pooled += x.est;
+        }
+      }
+      for (SrvReq *r : pending) res.push_back(r);
+      pending.clear();
+      for (SrvReq *r : res) {
+        SrvSlot x;
+        x.r = r;
+        next.push_back(std::move(x));
+      }
+      const int st = res.empty() ? MF3D_OK : srv_rebuild<T>(C, V, res);
+      slots.swap(next);
+      next.clear();  // frees the storage of finished requests that was not pooled
       if (st) { fail_all(st); continue; }
-      dirty = false;
+      rebuild_s = steady_now() - t0;
+      since_rebuild_s = 0.0;
+      {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->t_rebuild += rebuild_s;
+        S->rebuilds++;
+      }
+      live = (int)slots.size();
     }
-    // one outer iteration of every resident request
-    iteration_body<T>(C, V, false);
-    const int nd = (int)res.size();
+    if (live == 0) continue;
+    // outer iterations of every running request, as one graph launch that
+    // returns when a request stops or after kSrvIters iterations
+    const double c0 = steady_now();
+    if (!V.x_loop && build_server_graph<T>(C, V)) {
+      fail_all(MF3D_E_CUDA);
+      continue;
+    }
+    const int nd = (int)slots.size();
     act.assign(nd, 0);
-    if (cudaMemcpyAsync(act.data(), V.act.p, nd * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+    if (cudaMemcpyAsync(V.budget.p, &kSrvIters, sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaGraphLaunch(V.x_loop, s) != cudaSuccess ||
+        cudaMemcpyAsync(act.data(), V.act.p, nd * sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess) {
       set_error(std::string("server cycle: ") + cudaGetErrorString(cudaGetLastError()));
       fail_all(MF3D_E_CUDA);
       continue;
     }
+    const double dc = steady_now() - c0;
+    cycle_s = 0.8 * cycle_s + 0.2 * dc;
+    since_rebuild_s += dc;
     {
       std::lock_guard<std::mutex> lk(S->mu);
       S->cycles++;
+      S->t_cycle += dc;
     }
     std::vector<int> fin(nd, 0);
     bool any = false;
-    for (int d = 0; d < nd; ++d) any |= (fin[d] = act[d] == 0);
+    for (int d = 0; d < nd; ++d) any |= (fin[d] = slots[d].r != nullptr && act[d] == 0);
     if (!any) continue;
     // final calvel of the finished requests, then hand them back
+    const double tf = steady_now();
     std::vector<DomState> hs(nd);
     DevBuf<int> fmask;
     int st = fmask.upload(fin, s);
@@ -234,20 +389,26 @@ static void srv_loop(mf3d_server *S) {
     }
     if (!st) st = check_device_error(V);
     if (st) { fail_all(st); continue; }
-    std::vector<SrvReq *> keep;
     for (int d = 0; d < nd; ++d) {
-      SrvReq *r = res[d];
-      if (!fin[d]) { keep.push_back(r); continue; }
+      if (!fin[d]) continue;
+      SrvSlot &x = slots[d];
+      SrvReq *r = x.r;
       const DomState &D = hs[d];
       r->info.info.rmax = D.iter > 0 ? D.rmax : D.rmax0;
       r->info.info.rmax0 = D.rmax0;
       r->info.info.iter = D.iter;
       r->info.info.ms_device = 0.f;
-      r->dom.reset();
-      srv_finish(S, r, srv_status(D));
+      const int status = srv_status(D);
+      x.key = status >= 0 ? shape_key(r->desc, r->ngrid) : std::string();
+      x.est = r->est;
+      x.dead = std::move(r->dom);
+      x.r = nullptr;
+      srv_finish(S, r, status, false);  // r may be released by a poll from here on
     }
-    res.swap(keep);
-    dirty = true;
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->t_finish += steady_now() - tf;
+    }
   }
   fail_all(MF3D_E_INVALID);  // stopped: drop what is resident
 }
@@ -257,6 +418,19 @@ static void srv_loop(mf3d_server *S) {
 extern "C" {
 
 double mf3d_server_clock(void) { return mf3d::steady_now(); }
+
+int mf3d_server_profile(mf3d_server *S, double *build_s, double *rebuild_s, double *cycle_s, double *finish_s,
+                        long long *builds, long long *rebuilds) {
+  if (!S) { mf3d::set_error("mf3d_server_profile: bad arguments"); return MF3D_E_INVALID; }
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (build_s) *build_s = S->t_build;
+  if (rebuild_s) *rebuild_s = S->t_rebuild;
+  if (cycle_s) *cycle_s = S->t_cycle;
+  if (finish_s) *finish_s = S->t_finish;
+  if (builds) *builds = S->builds;
+  if (rebuilds) *rebuilds = S->rebuilds;
+  return MF3D_OK;
+}
 
 int mf3d_server_create(const mf3d_params *prm, double mem_cap_bytes, int max_resident, mf3d_server **out) {
   using namespace mf3d;
@@ -269,14 +443,20 @@ int mf3d_server_create(const mf3d_params *prm, double mem_cap_bytes, int max_res
   int st = check_params(&p);
   if (st) return st;
   auto S = std::make_unique<mf3d_server>();
-  S->C = std::make_unique<mf3d_ctx>();
-  if ((st = ctx_init(S->C.get(), &p))) return st;
-  S->C->use_graph = false;
+  for (int l = 0; l < kSrvLanes; ++l) {
+    S->C[l] = std::make_unique<mf3d_ctx>();
+    // lane 0 (small requests, latency-bound cycles) gets the high-priority
+    // stream: its CTAs are scheduled ahead of lane 1's queued ones
+    if ((st = ctx_init(S->C[l].get(), &p, true, l == 0))) return st;
+    S->C[l]->use_graph = false;
+  }
   S->cap = mem_cap_bytes;
   S->max_resident = max_resident;
   mf3d_server *raw = S.get();
-  if (S->C->elem == 8) S->worker = std::thread(srv_loop<double>, raw);
-  else S->worker = std::thread(srv_loop<float>, raw);
+  for (int l = 0; l < kSrvLanes; ++l) {
+    if (S->C[l]->elem == 8) S->worker[l] = std::thread(srv_loop<double>, raw, l);
+    else S->worker[l] = std::thread(srv_loop<float>, raw, l);
+  }
   *out = S.release();
   return MF3D_OK;
 }
@@ -298,15 +478,16 @@ int mf3d_server_submit(mf3d_server *S, const mf3d_domain_desc *dom, const mf3d_f
   r->dt = dt;
   r->alfapr = alfapr;
   r->ngrid = ngrid;
-  r->est = domain_bytes(*dom, ngrid, S->C->elem);
+  r->est = domain_bytes(*dom, ngrid, S->C[0]->elem);
   r->info.t_submit = steady_now();
+  const int lane = (double)dom->nx * dom->ny * dom->nz >= kSrvLargeCells ? 1 : 0;
   std::lock_guard<std::mutex> lk(S->mu);
   r->ticket = S->next_ticket++;
   *ticket = r->ticket;
-  S->queue.push_back(r.get());
+  S->queue[lane].push_back(r.get());
   S->reqs[r->ticket] = std::move(r);
   S->submitted++;
-  S->cv_work.notify_one();
+  S->cv_work.notify_all();
   return MF3D_OK;
 }
 
@@ -333,7 +514,7 @@ int mf3d_server_stats(mf3d_server *S, long long *submitted, long long *completed
   if (submitted) *submitted = S->submitted;
   if (completed) *completed = S->completed;
   if (resident) *resident = S->resident;
-  if (queued) *queued = (long long)S->queue.size();
+  if (queued) *queued = (long long)(S->queue[0].size() + S->queue[1].size());
   if (resident_bytes) *resident_bytes = S->used;
   if (cycles) *cycles = S->cycles;
   return MF3D_OK;
@@ -346,11 +527,14 @@ int mf3d_server_destroy(mf3d_server *S) {
     S->stop = true;
     S->cv_work.notify_all();
   }
-  if (S->worker.joinable()) S->worker.join();
-  mf3d_ctx *C = S->C.release();
+  for (auto &w : S->worker)
+    if (w.joinable()) w.join();
+  mf3d_ctx *C[kSrvLanes];
+  for (int l = 0; l < kSrvLanes; ++l) C[l] = S->C[l].release();
   S->reqs.clear();
   delete S;
-  return mf3d_destroy(C);
+  for (int l = 0; l < kSrvLanes; ++l) mf3d_destroy(C[l]);
+  return MF3D_OK;
 }
 
 }  // extern "C"

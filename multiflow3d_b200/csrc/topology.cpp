@@ -143,24 +143,82 @@ struct TokenLevel {
   const std::vector<LevelGeom> &geom;
   const std::vector<long long> &base;
   std::unordered_map<int, int> pos;  // block id -> position
-  std::vector<long long> tok;
-  long long total;
+  // Only ghost cells are ever written (and interior cells keep their own
+  // token), so tokens are stored for the ghost shell of each block alone:
+  // the work and memory grow with the block surfaces, not their volumes.
+  std::vector<std::vector<long long>> shell;
+  std::vector<int> order;  // block positions by increasing base
 
   TokenLevel(const std::vector<mf3d_block_desc> &b, const std::vector<LevelGeom> &g,
              const std::vector<long long> &bs)
       : blk(b), geom(g), base(bs) {
-    total = 0;
+    shell.resize(b.size());
     for (size_t q = 0; q < b.size(); ++q) {
       pos[b[q].id] = (int)q;
-      total = std::max(total, bs[q] + g[q].cells());
+      const LevelGeom &G = g[q];
+      shell[q].resize((size_t)(G.cells() - (long long)G.nx * G.ny * G.nz));
+      order.push_back((int)q);
     }
-    tok.resize(total);
-    for (long long c = 0; c < total; ++c) tok[c] = c;
+    std::sort(order.begin(), order.end(), [&](int x, int y) { return bs[x] < bs[y]; });
+    for (size_t q = 0; q < b.size(); ++q) {
+      const LevelGeom &G = g[q];
+      for (int k = 0; k <= G.nz + 1; ++k)
+        for (int j = 0; j <= G.ny + 1; ++j)
+          for (int i = 0; i <= G.nx + 1; ++i) {
+            if (!on_shell(G, i, j, k)) {
+              i = G.nx;  // skip the interior of the row
+              continue;
+            }
+            shell[q][sidx(G, i, j, k)] = id((int)q, i, j, k);
+          }
+    }
+  }
+  static bool on_shell(const LevelGeom &G, int i, int j, int k) {
+    return i == 0 || j == 0 || k == 0 || i == G.nx + 1 || j == G.ny + 1 || k == G.nz + 1;
+  }
+  // index of a shell cell: the two z planes, then per interior plane the two
+  // y rows, then per interior row the two x ends
+  static long long sidx(const LevelGeom &G, int i, int j, int k) {
+    const long long W = G.nx + 2, H = G.ny + 2;
+    if (k == 0) return (long long)j * W + i;
+    if (k == G.nz + 1) return W * H + (long long)j * W + i;
+    const long long pl = 2 * W + 2LL * G.ny;  // shell cells of one interior plane
+    long long o = 2 * W * H + (long long)(k - 1) * pl;
+    if (j == 0) return o + i;
+    if (j == G.ny + 1) return o + W + i;
+    return o + 2 * W + 2LL * (j - 1) + (i == 0 ? 0 : 1);
   }
   long long id(int p, int i, int j, int k) const { return base[p] + geom[p].lin(i, j, k); }
   int P(int block_id) const {
     auto it = pos.find(block_id);
     return it == pos.end() ? -1 : it->second;
+  }
+  // the block and (i, j, k) of a cell id
+  void decode(long long c, int &p, int &i, int &j, int &k) const {
+    int lo = 0, hi = (int)order.size() - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (base[order[mid]] <= c) lo = mid;
+      else hi = mid - 1;
+    }
+    p = order[lo];
+    const LevelGeom &G = geom[p];
+    long long r = c - base[p];
+    i = (int)(r % (G.nx + 2));
+    r /= (G.nx + 2);
+    j = (int)(r % (G.ny + 2));
+    k = (int)(r / (G.ny + 2));
+  }
+  long long get(long long c) const {
+    int p, i, j, k;
+    decode(c, p, i, j, k);
+    const LevelGeom &G = geom[p];
+    return on_shell(G, i, j, k) ? shell[p][sidx(G, i, j, k)] : c;
+  }
+  void set(long long c, long long v) {
+    int p, i, j, k;
+    decode(c, p, i, j, k);
+    shell[p][sidx(geom[p], i, j, k)] = v;  // destinations are ghost cells
   }
 };
 
@@ -169,10 +227,10 @@ struct TokenLevel {
 struct Phase {
   std::vector<HaloPair> pairs;
   void add(long long d, long long s) { pairs.push_back({d, s}); }
-  void apply(std::vector<long long> &tok) const {
+  void apply(TokenLevel &T) const {
     std::vector<long long> v(pairs.size());
-    for (size_t q = 0; q < pairs.size(); ++q) v[q] = tok[pairs[q].src];
-    for (size_t q = 0; q < pairs.size(); ++q) tok[pairs[q].dst] = v[q];
+    for (size_t q = 0; q < pairs.size(); ++q) v[q] = T.get(pairs[q].src);
+    for (size_t q = 0; q < pairs.size(); ++q) T.set(pairs[q].dst, v[q]);
   }
 };
 
@@ -191,7 +249,7 @@ void mgbound_tokens(TokenLevel &T) {
     const auto &d = T.blk[p];
     const LevelGeom &g = T.geom[p];
     int nx = g.nx, ny = g.ny, nz = g.nz;
-    auto cp = [&](long long dst, long long src) { T.tok[dst] = T.tok[src]; };
+    auto cp = [&](long long dst, long long src) { T.set(dst, T.get(src)); };
     if (d.iprev < 0 && d.bc_west != MF3D_BC_PERIODIC)
       for (int k = 0; k <= nz + 1; ++k) for (int j = 0; j <= ny + 1; ++j) cp(T.id(p, 0, j, k), T.id(p, 1, j, k));
     if (d.inext < 0 && d.bc_east != MF3D_BC_PERIODIC)
@@ -296,7 +354,7 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
           if (d.edgnext[e] >= 0) edge_next(e, T.P(d.edgnext[e]));
       }
     }
-    ph.apply(T.tok);
+    ph.apply(T);
   }
   mgbound_tokens(T);
   if (periodic) {
@@ -319,9 +377,9 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
         int pern = ax == 0 ? d.per_in : ax == 1 ? d.per_jn : d.per_kn;
         if (prev < 0 && next < 0) {
           for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
-            T.tok[V.at(T, p, 0, s, t)] = T.tok[V.at(T, p, nA, s, t)];
+            T.set(V.at(T, p, 0, s, t), T.get(V.at(T, p, nA, s, t)));
           for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
-            T.tok[V.at(T, p, nA + 1, s, t)] = T.tok[V.at(T, p, 1, s, t)];
+            T.set(V.at(T, p, nA + 1, s, t), T.get(V.at(T, p, 1, s, t)));
           continue;
         }
         if (prev < 0 && next >= 0 && perp >= 0) {
@@ -336,12 +394,24 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
             ph.add(V.at(T, p, nA + 1, s, t), V.at(T, q, 1, s, t));
         }
       }
-      ph.apply(T.tok);
+      ph.apply(T);
     }
   }
+  // changed shell cells, in increasing cell id
   std::vector<HaloPair> out;
-  for (long long c = 0; c < T.total; ++c)
-    if (T.tok[c] != c) out.push_back({c, T.tok[c]});
+  for (int p : T.order) {
+    const LevelGeom &G = geom[p];
+    for (int k = 0; k <= G.nz + 1; ++k)
+      for (int j = 0; j <= G.ny + 1; ++j)
+        for (int i = 0; i <= G.nx + 1; ++i) {
+          if (!TokenLevel::on_shell(G, i, j, k)) {
+            i = G.nx;  // skip the interior of the row
+            continue;
+          }
+          const long long c = T.id(p, i, j, k), v = T.shell[p][TokenLevel::sidx(G, i, j, k)];
+          if (v != c) out.push_back({c, v});
+        }
+  }
   return out;
 }
 

@@ -160,10 +160,12 @@ class Batch:
 
 class Server:
     """The request loop (``mf3d_server_*``): submit single-block solves as
-    they arrive; a worker thread in the library admits them by memory,
-    keeps their hierarchies resident and advances all resident requests by
-    one outer iteration per cycle.  ``fields`` are device tensors (ttc
-    layout) borrowed until the request finishes."""
+    they arrive; worker threads in the library (one per size lane) admit
+    them by memory, keep their hierarchies resident and advance all resident
+    requests by one outer iteration per cycle.  ``fields`` are device
+    tensors (ttc layout) borrowed until the request finishes; their contents
+    must be complete on the device at submit (synchronise the producing
+    stream first)."""
 
     def __init__(self, params: abi.Params, mem_cap_bytes: float = 150e9, max_resident: int = 256, lib=None):
         self.lib = lib or abi.load()
@@ -201,6 +203,12 @@ class Server:
 
     def clock(self) -> float:
         return self.lib.mf3d_server_clock()
+
+    def profile(self) -> dict:
+        v = [C.c_double() for _ in range(4)] + [C.c_longlong() for _ in range(2)]
+        abi.check(self.lib, self.lib.mf3d_server_profile(self.ctx, *[C.byref(x) for x in v]), "mf3d_server_profile")
+        keys = ("build_s", "rebuild_s", "cycle_s", "finish_s", "builds", "rebuilds")
+        return {k: x.value for k, x in zip(keys, v)}
 
     def close(self):
         if getattr(self, "ctx", None):

@@ -24,8 +24,12 @@ def domains(n, seed):
 
 
 def dev_fields(pr, seed, cuda):
+    """Device fields, complete on the device (the server's streams do not
+    order after the caller's)."""
     import torch
-    return {k: torch.from_numpy(v).to(cuda) for k, v in pr.block_fields(seed=seed)[0].items() if k != "su"}
+    f = {k: torch.from_numpy(v).to(cuda) for k, v in pr.block_fields(seed=seed)[0].items() if k != "su"}
+    torch.cuda.synchronize()
+    return f
 
 
 def wait_all(srv, tickets, timeout=120.0):
