@@ -167,6 +167,7 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 // read zeros (never used).
 // ---------------------------------------------------------------------------
 constexpr int RB_PD = 2;          // prefetch distance in planes
+constexpr int RB_KMAX = 32;       // planes per CTA at most
 constexpr int RB_NS = RB_PD + 2;  // stages: planes k-1 .. k+RB_PD (a power of two)
 static_assert((RB_NS & (RB_NS - 1)) == 0, "RB_NS must be a power of two");
 
@@ -188,6 +189,7 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
   __shared__ __align__(128) unsigned char sbuf[RB_NS * (OB + S::RBY)];
   __shared__ __align__(8) uint64_t bar[RB_NS];
   __shared__ int abort_s;  // set when a wait gave up: every thread leaves after the next barrier
+  __shared__ T sab[RB_KMAX], sat[RB_KMAX];  // z coefficients of the CTA's planes
   const Tile t = tiles[blockIdx.x];
   const BlkLev B = bl[t.blk];
   if (!act[B.dom]) return;
@@ -237,6 +239,10 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
     mbar_fence_init();
     abort_s = 0;
   }
+  for (int q = tid; q <= k1 - k0; q += RB_TX * RB_TY) {
+    sab[q] = cf.ab[k0 + q];
+    sat[q] = cf.at[k0 + q];
+  }
   __syncthreads();
   if (tid == 0)
     for (int kk = k0 - 1; kk < k0 + RB_PD; ++kk)
@@ -252,7 +258,7 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
     const int i = 2 * q + 2 - s;
     if (ok && i <= nx) {
       const int st = stage(k), hc = tx + 1 - s;
-      const T ab = cf.ab[k], at = cf.at[k];
+      const T ab = sab[k - k0], at = sat[k - k0];
       const T aw = s ? aw1 : aw0, ae = s ? ae1 : ae0;
       const T *o = slot_o(st), *ob = slot_o(stage(k - 1)), *ot = slot_o(stage(k + 1));
       const T *r = slot_r(st);

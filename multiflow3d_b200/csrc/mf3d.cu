@@ -498,7 +498,8 @@ struct View {
   std::vector<ViewLevel> lv;          // [1..Lmax]
   std::vector<BlkFld> hf;
   DevBuf<BlkFld> df;
-  DevBuf<Tile> t_int, t_zint, t_l1cells, t_faces, t_planes;
+  DevBuf<Tile> t_int, t_zint, t_l1cells, t_faces, t_planes, t_pairs;
+  int n_pairs = 0, pairs_kch = 1;
   int n_int = 0, n_zint = 0, n_l1cells = 0, n_faces = 0, n_planes = 0;
   DevBuf<DomState> ds;
   DevBuf<int> act, ones;
@@ -597,7 +598,7 @@ static int sweep_tiles(const mf3d_ctx *C, const std::vector<BlkLev> &tab, const 
   const long long resident = (long long)C->nsm * C->sweep_occ;
   int best = 2;
   double best_cost = 1e300;
-  for (int kch : {2, 4, 8, 16, 32}) {
+  for (int kch : {2, 4, 8, 16, RB_KMAX}) {
     long long n = 0;
     for (int b : blocks) {
       const BlkLev &B = tab[b];
@@ -761,6 +762,17 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
     it_faces.push_back(2 * ((long long)x.ny * x.nz + (long long)x.nx * x.nz + (long long)x.nx * x.ny));
     it_planes.push_back((long long)x.ny * x.nz + (long long)x.nx * x.nz + (long long)x.nx * x.ny);
     V.n_l1 += (long long)x.nx * x.ny * x.nz;
+  }
+  {
+    std::vector<PlaneExt> pe;
+    for (int b = 0; b < nb; ++b) {
+      const mf3d_block_desc &x = V.blk[b]->d;
+      pe.push_back(PlaneExt{b, (x.nx + 3) / 2, x.ny + 2, 0, x.nz + 1});
+    }
+    std::vector<Tile> tp;
+    V.pairs_kch = plane_tiles(C, pe, tp);
+    V.n_pairs = (int)tp.size();
+    if ((st = V.t_pairs.upload(tp, s))) return st;
   }
   auto t3 = make_tiles(it_faces), t4 = make_tiles(it_planes);
   V.n_int = (int)t1.size(); V.n_l1cells = (int)t2.size(); V.n_faces = (int)t3.size();
@@ -930,7 +942,7 @@ template <typename T>
 static void iteration_body(mf3d_ctx *C, View &V, int loop_graph) {
   cudaStream_t s = C->stream;
   vcycle<T>(C, V);
-  k_add_correction<T><<<V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_l1cells.p, V.act.p);
+  k_add_correction<T><<<V.n_pairs, kTile, 0, s>>>(V.df.p, V.t_pairs.p, V.act.p, V.pairs_kch);
   k_p_faces<<<V.n_faces, kTile, 0, s>>>(V.df.p, V.t_faces.p, V.act.p);
   prof_begin(C, MF3D_PROF_CALMAS, (double)V.n_l1 * (4 * sizeof(double) + sizeof(T)));  // p, u*, v*, w* in; su out
   calvel_calmas<T>(C, V, V.act.p, V.rmax.p, 0);

@@ -90,31 +90,48 @@ __device__ inline long long fidx(const BlkFld &F, int i, int j, int k) {
 
 // p := p + (pp - ppref) over isp-1..iep+1 (newsolv_mg.for:38-48), ppref = 0
 // (the reference-pressure code is commented out, :28-36); pp is the level-1
-// correction of the V-cycle.  One thread per ghost-inclusive level-1 cell.
-// Also zeroes the ghost shell of pp after reading it: the next V-cycle starts
-// from pp = 0 (newsolv_mg.for:44) and its first red sweep never reads the
-// interior, so the shell is all that must hold zeros.
+// correction of the V-cycle.  Also zeroes the ghost shell of pp after
+// reading it: the next V-cycle starts from pp = 0 (newsolv_mg.for:44) and its
+// first red sweep never reads the interior, so the shell is all that must
+// hold zeros.  One thread per pair of x-neighbours (i = 2h, 2h+1: compact
+// index h in both colour arrays, so neighbouring lanes read neighbouring
+// elements of each) and row j of the ghost-inclusive plane, marching up kch
+// planes.
 template <typename T>
-__global__ void __launch_bounds__(RW_TX *RW_RJ) k_add_correction(const BlkFld *__restrict__ fl,
-                                                                 const Tile *__restrict__ tiles,
-                                                                 const int *__restrict__ act) {
+__global__ void __launch_bounds__(kTile) k_add_correction(const BlkFld *__restrict__ fl,
+                                                          const Tile *__restrict__ tiles,
+                                                          const int *__restrict__ act, int kch) {
   const Tile t = tiles[blockIdx.x];
-  const BlkFld &F = fl[t.blk];
-  if (!act[F.dom]) return;
-  const BlkLev &B = F.L1;
-  T *__restrict__ phi1 = phi_of<T>(B);
-  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
-  if (i > B.nx + 1 || j > B.ny + 1) return;
+  if (!act[fl[t.blk].dom]) return;
+  const BlkFld F = fl[t.blk];
+  const int nx = F.L1.nx, ny = F.L1.ny, nz = F.L1.nz, hp = F.L1.hp;
+  const int HX = (nx + 3) / 2;  // pairs per ghost-inclusive row
+  const int g = t.i0 + threadIdx.x;
+  if (g >= HX * (ny + 2)) return;
+  const int j = g / HX, h = g - j * HX;
+  const int i0 = 2 * h, i1 = 2 * h + 1;
+  const bool has1 = i1 <= nx + 1;
+  T *__restrict__ phi = phi_of<T>(F.L1);
   double *__restrict__ P = F.p;
-  const int k1 = min(t.k0 + RW_KCH - 1, B.nz + 1);
-#pragma unroll 4
-  for (int k = t.k0; k <= k1; ++k) {
-    const long long a = cell_off(B, i, j, k);
-    const double pp = (double)phi1[a];
+  const long long cs = F.L1.cstr, plane = (long long)(ny + 2) * hp;
+  const long long fs = (long long)F.ti * F.tj;
+  const bool jg = j == 0 || j == ny + 1;
+  const int k1 = min(t.k0 + kch - 1, nz + 1);
+  long long e = (long long)t.k0 * plane + (long long)j * hp + h;  // compact element without the colour term
+  long long f = fidx(F, i0, j, t.k0);
+  for (int k = t.k0; k <= k1; ++k, e += plane, f += fs) {
+    const int c0 = (i0 + j + k + 1) & 1;
+    const long long a0 = c0 * cs + e, a1 = (1 - c0) * cs + e;
     const double ppref = 0.0;
-    const long long f = fidx(F, i, j, k);
-    P[f] = (P[f] + (pp - ppref));
-    if (i == 0 || i == B.nx + 1 || j == 0 || j == B.ny + 1 || k == 0 || k == B.nz + 1) phi1[a] = (T)0;
+    const bool kg = k == 0 || k == nz + 1;
+    const double pp0 = (double)phi[a0];
+    P[f] = (P[f] + (pp0 - ppref));
+    if (i0 == 0 || jg || kg) phi[a0] = (T)0;
+    if (has1) {
+      const double pp1 = (double)phi[a1];
+      P[f + 1] = (P[f + 1] + (pp1 - ppref));
+      if (i1 == nx + 1 || jg || kg) phi[a1] = (T)0;
+    }
   }
 }
 
@@ -322,7 +339,7 @@ constexpr int CV_TY = 4, CV_CR = OZ_RJ / CV_TY;  // 32 x CV_TY threads, CV_CR co
 // UMASK bit a: axis a of every block is uniform with a power-of-two spacing
 // (x/h is x*(1/h) there); other axes divide through div_rcp.
 template <typename T, int UMASK>
-__global__ void __launch_bounds__(OZ_TX *CV_TY) k_calvel_calmas_tma(const BlkFld *__restrict__ fl,
+__global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const BlkFld *__restrict__ fl,
                                                                    const Tile *__restrict__ tiles,
                                                                    const DomState *__restrict__ ds,
                                                                    const int *__restrict__ act,
