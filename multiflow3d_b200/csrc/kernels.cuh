@@ -465,6 +465,129 @@ __global__ void __launch_bounds__(kTile, 2) k_restrict(const BlkLev *__restrict_
 }
 
 // ---------------------------------------------------------------------------
+// The restriction with its fine operands staged by TMA (red-black smoothing
+// only: the coarse level's first half-sweep starts from zero and reads no
+// coarse phi, so only the coarse ghost shell has to be zeroed, by a separate
+// k_zero_ghosts).  A CTA owns coarse cells I0..I0+31 x J0..J0+7 and marches
+// up kch coarse planes.  Fine plane fp is loaded once, into a ring of
+// RS_NS slots: both colours of phi over compact columns I0-1..I0-1+W and
+// fine rows 2J0-2..2J0+15 (the sweep's phi boxes), and both colours of rhs
+// over rows 2J0-1..2J0+14 (the sweep's rhs boxes) when fp holds children.
+// Coarse plane K reads fine planes 2K-2..2K+1; the next two are in flight.
+// Per coarse cell the arithmetic is k_restrict's, in its order.
+// ---------------------------------------------------------------------------
+constexpr int RS_NS = 6;  // fine-plane slots: 2K-2 .. 2K+3
+template <typename T>
+struct RsShape {
+  static constexpr int W = RbShape<T>::W;
+  static constexpr int PR = RB_RJ + 2, RR = RB_RJ;  // phi and rhs box rows (fine)
+  static constexpr int PB = (PR * W * (int)sizeof(T) + 127) / 128 * 128;
+  static constexpr int RBY = (RR * W * (int)sizeof(T) + 127) / 128 * 128;
+  static constexpr int SLOT = 2 * PB + 2 * RBY;  // phi c0, phi c1, rhs c0, rhs c1
+  static constexpr int SMEM = RS_NS * SLOT;
+};
+
+template <typename TF, typename TC>
+__global__ void __launch_bounds__(kTile) k_restrict_tma(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
+                                                        const Tile *__restrict__ tiles, const int *__restrict__ act,
+                                                        int kch, int *__restrict__ err) {
+  using S = RsShape<TF>;
+  constexpr int W = S::W;
+  extern __shared__ __align__(128) unsigned char rs_smem[];
+  __shared__ __align__(8) uint64_t bar[RS_NS];
+  __shared__ int abort_s;
+  const Tile t = tiles[blockIdx.x];
+  const BlkLev Cb = cl[t.blk];
+  if (!act[Cb.dom]) return;
+  const BlkLev Fb = fl[t.blk];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, tid = threadIdx.x;
+  const int I0 = t.i0, J0 = t.j0, K0 = t.k0, K1 = min(t.k0 + kch - 1, Cb.nz);
+  const int I = I0 + tx, J = J0 + ty;
+  const bool in = I <= Cb.nx && J <= Cb.ny;
+  const int Ic = in ? I : 1, Jc = in ? J : 1;
+  const Coef<TF> cf(Fb);
+  const TF *rx = (const TF *)Fb.geo, *ry = rx + (Fb.nx + 2), *rz = ry + (Fb.ny + 2);
+  TF aw[2], ae[2], sx[2], as[2], an[2], sy[2];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    const int fi = 2 * Ic - 1 + d, fj = 2 * Jc - 1 + d;
+    aw[d] = cf.aw[fi]; ae[d] = cf.ae[fi]; sx[d] = rx[fi];
+    as[d] = cf.as[fj]; an[d] = cf.an[fj]; sy[d] = ry[fj];
+  }
+  const int fp0 = 2 * K0 - 2, fp1 = 2 * K1 + 1;  // fine planes of the chunk
+  auto slot = [&](int fp) { return rs_smem + ((fp - fp0) % RS_NS) * S::SLOT; };
+  auto sidx = [&](int fp) { return (fp - fp0) % RS_NS; };
+  auto parity = [&](int fp) { return (unsigned)(((fp - fp0) / RS_NS) & 1); };
+  auto issue = [&](int fp) {
+    const int st = sidx(fp);
+    unsigned char *b = slot(fp);
+    const bool kids = fp > fp0 && fp < fp1;
+    const unsigned bytes = 2u * S::PR * W * sizeof(TF) + (kids ? 2u * S::RR * W * sizeof(TF) : 0u);
+    mbar_expect_tx(&bar[st], bytes);
+    tma_load_3d(b, Fb.tm + 0, &bar[st], I0 - 1, 2 * J0 - 2, fp);
+    tma_load_3d(b + S::PB, Fb.tm + 1, &bar[st], I0 - 1, 2 * J0 - 2, fp);
+    if (kids) {
+      tma_load_3d(b + 2 * S::PB, Fb.tm + 2, &bar[st], I0 - 1, 2 * J0 - 1, fp);
+      tma_load_3d(b + 2 * S::PB + S::RBY, Fb.tm + 3, &bar[st], I0 - 1, 2 * J0 - 1, fp);
+    }
+  };
+  if (tid == 0) {
+    for (int q = 0; q < RS_NS; ++q) mbar_init(&bar[q], 1);
+    mbar_fence_init();
+    abort_s = 0;
+  }
+  __syncthreads();
+  if (tid == 0)
+    for (int fp = fp0; fp < fp0 + RS_NS && fp <= fp1; ++fp) issue(fp);
+  bool ok = true;
+  for (int K = K0; K <= K1; ++K) {
+    // planes 2K-2 .. 2K+1 (the first two were waited for at K-1, except at K0)
+    for (int fp = (K == K0 ? 2 * K - 2 : 2 * K); fp <= 2 * K + 1 && ok; ++fp)
+      ok = mbar_wait(&bar[sidx(fp)], parity(fp), err);
+    if (ok && in) {
+      TF sum = (TF)0;
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk) {
+        const int fk = 2 * K - 1 + dk;
+        const TF ab = cf.ab[fk], at = cf.at[fk], sz = rz[fk];
+        const unsigned char *pc = slot(fk), *pb = slot(fk - 1), *pt = slot(fk + 1);
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+          for (int di = 0; di < 2; ++di) {
+            const int fi = 2 * I - 1 + di, fj = 2 * J - 1 + dj;
+            const int c = (fi + fj + fk + 1) & 1;        // colour of the child
+            const int col = (fi >> 1) - (I0 - 1);
+            const int row = fj - (2 * J0 - 2);            // phi box row
+            const TF *Pc = (const TF *)(pc + c * S::PB);  // same colour as the child
+            const TF *Po = (const TF *)(pc + (1 - c) * S::PB);
+            const TF *Pb = (const TF *)(pb + (1 - c) * S::PB), *Pt = (const TF *)(pt + (1 - c) * S::PB);
+            const TF *Rc = (const TF *)(pc + 2 * S::PB + c * S::RBY);
+            const TF ap = (TF)-1.0 * (aw[di] + ae[di] + as[dj] + an[dj] + ab + at);
+            const TF pw = Po[row * W + ((fi - 1) >> 1) - (I0 - 1)], pe = Po[row * W + ((fi + 1) >> 1) - (I0 - 1)];
+            const TF ps = Po[(row - 1) * W + col], pn = Po[(row + 1) * W + col];
+            const TF pbv = Pb[row * W + col], ptv = Pt[row * W + col];
+            const TF pp = Pc[row * W + col];
+            const TF r = Rc[(row - 1) * W + col];
+            const TF res = r - (aw[di] * pw + ae[di] * pe + as[dj] * ps + an[dj] * pn + ab * pbv + at * ptv + ap * pp);
+            const TF sw = (TF)8.0 * sx[di] * sy[dj] * sz;
+            const TF a = res * sw;
+            sum = (dk | dj | di) ? sum + a : a;
+          }
+      }
+      rhs_of<TC>(Cb)[cell_off(Cb, I, J, K)] = (TC)((TF)0.125 * sum);
+    }
+    if (!ok) abort_s = 1;
+    __syncthreads();  // planes 2K-2 and 2K-1 are free
+    if (abort_s) return;
+    if (tid == 0) {
+      if (2 * K + 4 <= fp1) issue(2 * K + 4);
+      if (2 * K + 5 <= fp1) issue(2 * K + 5);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Prolongation + correction + Neumann ghosts (mgcorr, mgsolver.for:763-905,
 // then mgbound :902).  Every fine cell, ghosts included, adds the trilinear
 // (27,9,3,1)/64 interpolant of the coarse correction, summed in the

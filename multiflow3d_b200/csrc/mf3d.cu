@@ -480,6 +480,8 @@ struct ViewLevel {
   int kch[3] = {1, 1, 1};             // planes per sweep CTA
   DevBuf<Tile> rtile, ptile;          // restriction into this level (SUB_A); prolongation from the next (SUB_D)
   int n_rtile = 0, n_ptile = 0, rkch = 1, pkch = 1;
+  DevBuf<Tile> rtma;                  // TMA restriction into this level: coarse interior tiles (SUB_A)
+  int n_rtma = 0, rtma_kch = 1;
   DevBuf<int> list[3];
   int n_list[3] = {0, 0, 0};
   DevBuf<HaloSeg> hseg[3];            // one segment per domain of the subset
@@ -698,6 +700,32 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       L.n_ptile = (int)pt.size();
       if ((st = L.rtile.upload(rt, s))) return st;
       if ((st = L.ptile.upload(pt, s))) return st;
+      // TMA restriction tiles: 32 x RB_RJ/2 coarse cells, kch planes chosen as
+      // for the sweep (2 resident CTAs per SM: the ring takes ~110 KB)
+      std::vector<Tile> rm;
+      if (g > 1) {
+        const long long resident = (long long)C->nsm * 2;
+        int best = 2;
+        double best_cost = 1e300;
+        for (int kch : {2, 4, 8, 16}) {
+          long long n = 0;
+          for (int b = 0; b < nb; ++b) {
+            if (g > V.blk[b]->ngrid) continue;
+            const BlkLev &B = tab[b];
+            n += (long long)((B.nx + 31) / 32) * ((B.ny + RB_RJ / 2 - 1) / (RB_RJ / 2)) * ((B.nz + kch - 1) / kch);
+          }
+          const double cost = (double)((n + resident - 1) / resident) * (kch + 3);
+          if (cost <= best_cost) { best_cost = cost; best = kch; }
+        }
+        for (int b = 0; b < nb; ++b) {
+          if (g > V.blk[b]->ngrid) continue;
+          const BlkLev &B = tab[b];
+          add_tiles_2d(rm, b, Box{1, B.nx, 1, B.ny, 1, B.nz}, 32, RB_RJ / 2, best);
+        }
+        L.rtma_kch = best;
+      }
+      L.n_rtma = (int)rm.size();
+      if ((st = L.rtma.upload(rm, s))) return st;
     }
     for (int q = 0; q < 3; ++q) {
       L.kch[q] = sweep_tiles(C, tab, sblk[q], sw[q]);
@@ -859,6 +887,27 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
   if (!Cl.n_rtile) return;
   const int pk = g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse out
+  if (C->prm.mg_itrsch == 3 && C->prm.irestr > 0 && Cl.n_rtma) {
+    // red-black from zero: the coarse interior phi is never read before it
+    // is written, so only its ghost shell is zeroed
+    static const bool attr_set = [] {
+      cudaFuncSetAttribute(k_restrict_tma<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           RsShape<double>::SMEM);
+      cudaFuncSetAttribute(k_restrict_tma<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           RsShape<float>::SMEM);
+      cudaFuncSetAttribute(k_restrict_tma<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           RsShape<float>::SMEM);
+      return true;
+    }();
+    (void)attr_set;
+    k_restrict_tma<T, TC><<<Cl.n_rtma, kTile, RsShape<T>::SMEM, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtma.p, V.act.p,
+                                                                              Cl.rtma_kch, V.err.p);
+    prof_end(C, pk);
+    k_zero_ghosts<TC><<<dim3(16, Cl.n_list[SUB_A]), kTile, 0, C->stream>>>(Cl.tab.p, Cl.list[SUB_A].p,
+                                                                          Cl.n_list[SUB_A]);
+    C->launches += 2;
+    return;
+  }
   k_restrict<T, TC><<<Cl.n_rtile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch);
   prof_end(C, pk);
   ++C->launches;
