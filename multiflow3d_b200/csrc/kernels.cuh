@@ -288,6 +288,55 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
 }
 
 // ---------------------------------------------------------------------------
+// The same half-sweep for small levels (their arrays sit in L2): one thread
+// per item (q, j, k) of a flat list over the blocks, operands loaded
+// directly - no staging pipeline whose fill would dominate a launch of a few
+// thousand cells.  Arithmetic and order as in k_rbgs.  pre[b] = first item
+// of block b (ceil(nx/2)*ny*nz items per block).
+// ---------------------------------------------------------------------------
+template <typename T, bool FROM_ZERO>
+__global__ void __launch_bounds__(kTile) k_rbgs_small(const BlkLev *__restrict__ bl, const int *__restrict__ pre,
+                                                      const int *__restrict__ blocks, int nb,
+                                                      const int *__restrict__ act, int colour) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= pre[nb]) return;
+  int lo = 0, hi = nb - 1;  // last list entry whose first item <= t
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (pre[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  const BlkLev &B = bl[blocks[lo]];
+  if (!act[B.dom]) return;
+  const int Q = (B.nx + 1) / 2;
+  int r = t - pre[lo];
+  const int q = r % Q;
+  r /= Q;
+  const int j = r % B.ny + 1, k = r / B.ny + 1;
+  const int s = (colour + j + k + 1) & 1;
+  const int i = 2 * q + 2 - s;
+  if (i > B.nx) return;
+  const Coef<T> cf(B);
+  const long long rs = (long long)(B.ny + 2) * B.hp, base = (long long)k * rs + (long long)j * B.hp;
+  const int h = q + 1 - s;
+  const T *O = phi_of<T>(B) + (1 - colour) * B.cstr;
+  T *M = phi_of<T>(B) + colour * B.cstr;
+  const T *R = rhs_of<T>(B) + colour * B.cstr;
+  T w = (T)0, e = (T)0, so = (T)0, no = (T)0, bo = (T)0, to = (T)0;
+  if (!FROM_ZERO) {
+    w = O[base + q];
+    e = O[base + q + 1];
+    so = O[base - B.hp + h];
+    no = O[base + B.hp + h];
+    bo = O[base - rs + h];
+    to = O[base + rs + h];
+  }
+  const T aw = cf.aw[i], ae = cf.ae[i], as = cf.as[j], an = cf.an[j], ab = cf.ab[k], at = cf.at[k];
+  const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
+  M[base + h] = ((R[base + h] - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
+}
+
+// ---------------------------------------------------------------------------
 // Lexicographic Gauss-Seidel (mgsolver.for:403-428), loop order k, j, i:
 // cell (i,j,k) reads new values at i-1, j-1, k-1 and old ones at i+1, j+1,
 // k+1, so every hyperplane i+j+k = const is independent.  One CTA per block
@@ -467,8 +516,8 @@ __global__ void __launch_bounds__(kTile, 2) k_restrict(const BlkLev *__restrict_
 // ---------------------------------------------------------------------------
 // The restriction with its fine operands staged by TMA (red-black smoothing
 // only: the coarse level's first half-sweep starts from zero and reads no
-// coarse phi, so only the coarse ghost shell has to be zeroed, by a separate
-// k_zero_ghosts).  A CTA owns coarse cells I0..I0+31 x J0..J0+7 and marches
+// coarse phi, so only the coarse ghost shell has to be zeroed; the threads of
+// the boundary cells zero their neighbouring ghost cells).  A CTA owns coarse cells I0..I0+31 x J0..J0+7 and marches
 // up kch coarse planes.  Fine plane fp is loaded once, into a ring of
 // RS_NS slots: both colours of phi over compact columns I0-1..I0-1+W and
 // fine rows 2J0-2..2J0+15 (the sweep's phi boxes), and both colours of rhs
@@ -576,6 +625,15 @@ __global__ void __launch_bounds__(kTile) k_restrict_tma(const BlkLev *__restrict
           }
       }
       rhs_of<TC>(Cb)[cell_off(Cb, I, J, K)] = (TC)((TF)0.125 * sum);
+      // the coarse ghost cells next to this cell (faces, edges, corners) := 0
+      const int alo = I == 1 ? -1 : 0, ahi = I == Cb.nx ? 1 : 0;
+      const int blo = J == 1 ? -1 : 0, bhi = J == Cb.ny ? 1 : 0;
+      const int clo = K == 1 ? -1 : 0, chi = K == Cb.nz ? 1 : 0;
+      if (alo | ahi | blo | bhi | clo | chi)
+        for (int c = clo; c <= chi; ++c)
+          for (int b = blo; b <= bhi; ++b)
+            for (int a = alo; a <= ahi; ++a)
+              if (a | b | c) phi_of<TC>(Cb)[cell_off(Cb, I + a, J + b, K + c)] = (TC)0;
     }
     if (!ok) abort_s = 1;
     __syncthreads();  // planes 2K-2 and 2K-1 are free

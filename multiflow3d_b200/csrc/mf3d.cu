@@ -478,6 +478,9 @@ struct ViewLevel {
   DevBuf<Tile> sweep[3], cells[3];
   int n_sweep[3] = {0, 0, 0}, n_cells[3] = {0, 0, 0};
   int kch[3] = {1, 1, 1};             // planes per sweep CTA
+  DevBuf<int> spre[3];                // small levels: first sweep item of each listed block (+ total)
+  long long small_items[3] = {0, 0, 0};
+  int small = 0;                      // 1: the level's sweeps use k_rbgs_small
   DevBuf<Tile> rtile, ptile;          // restriction into this level (SUB_A); prolongation from the next (SUB_D)
   int n_rtile = 0, n_ptile = 0, rkch = 1, pkch = 1;
   DevBuf<Tile> rtma;                  // TMA restriction into this level: coarse interior tiles (SUB_A)
@@ -588,6 +591,9 @@ static void prof_collect(mf3d_ctx *C) {
   }
   C->prof_pending_bytes.clear();
 }
+
+// Levels with at most this many interior cells sweep with k_rbgs_small.
+constexpr long long kSmallLevelCells = 1ll << 19;
 
 // Red-black sweep tiles of a set of blocks: 32 lanes over q (ceil(nx/2) per
 // row), RB_RJ rows, kch planes.  kch is chosen so the CTAs fill the SMs in
@@ -727,6 +733,19 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       L.n_rtma = (int)rm.size();
       if ((st = L.rtma.upload(rm, s))) return st;
     }
+    // level 1 always takes the pipelined sweep; MF3D_SMALL_LEVEL_CELLS overrides the limit
+    long long small_limit = kSmallLevelCells;
+    if (const char *e = std::getenv("MF3D_SMALL_LEVEL_CELLS")) small_limit = std::atoll(e);
+    L.small = g > 1 && L.cells_sub[SUB_A] <= small_limit;
+    for (int q = 0; q < 3; ++q) {
+      std::vector<int> pre(1, 0);
+      for (int b : li[q]) {
+        const BlkLev &B = tab[b];
+        pre.push_back(pre.back() + ((B.nx + 1) / 2) * B.ny * B.nz);
+      }
+      L.small_items[q] = pre.back();
+      if ((st = L.spre[q].upload(pre, s))) return st;
+    }
     for (int q = 0; q < 3; ++q) {
       L.kch[q] = sweep_tiles(C, tab, sblk[q], sw[q]);
       L.n_sweep[q] = (int)sw[q].size();
@@ -861,6 +880,21 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
       const bool fz = from_zero && itr == 0;
       prof_begin(C, pk, (fz ? 2 : 3) * half);
       const dim3 grid(L.n_sweep[q]), cta(RB_TX, RB_TY);
+      if (L.small) {
+        const int g2 = grid_of(L.small_items[q], kTile);
+        if (fz)
+          k_rbgs_small<T, true><<<g2, kTile, 0, C->stream>>>(L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 0);
+        else
+          k_rbgs_small<T, false><<<g2, kTile, 0, C->stream>>>(L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p,
+                                                             0);
+        prof_end(C, pk);
+        prof_begin(C, pk, 3 * half);
+        k_rbgs_small<T, false><<<g2, kTile, 0, C->stream>>>(L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 1);
+        prof_end(C, pk);
+        C->launches += 2;
+        halo<T>(C, V, g, q);
+        continue;
+      }
       if (fz)
         k_rbgs<T, true><<<grid, cta, 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
       else
@@ -903,9 +937,7 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
     k_restrict_tma<T, TC><<<Cl.n_rtma, kTile, RsShape<T>::SMEM, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtma.p, V.act.p,
                                                                               Cl.rtma_kch, V.err.p);
     prof_end(C, pk);
-    k_zero_ghosts<TC><<<dim3(16, Cl.n_list[SUB_A]), kTile, 0, C->stream>>>(Cl.tab.p, Cl.list[SUB_A].p,
-                                                                          Cl.n_list[SUB_A]);
-    C->launches += 2;
+    ++C->launches;
     return;
   }
   k_restrict<T, TC><<<Cl.n_rtile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch);

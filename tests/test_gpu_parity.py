@@ -221,3 +221,18 @@ def test_division_from_reciprocal(lib, cuda):
     with np.errstate(all="ignore"):
         host = x / b
     assert np.array_equal(bits(q), bits(host))
+
+
+@pytest.mark.parametrize("small_limit", ["0", "100000000"])
+def test_sweep_kernels_by_level_size(lib, oracle, cuda, small_limit, monkeypatch):
+    """Coarse levels sweep with the plain-load kernel below a size limit and
+    with the TMA-pipelined one above it: forcing either everywhere below the
+    finest level gives the oracle's solve bit for bit."""
+    monkeypatch.setenv("MF3D_SMALL_LEVEL_CELLS", small_limit)
+    pr = Problem(2, 2, 2, 32, 32, 32, ngrid=5, pl=2, stretch_y=2.0, dx=1 / 64, dy=1 / 64, dz=1 / 64)
+    prm = pr.params(mg_itrsch=3, maxcy=100, eps=1e-10)
+    ref, info, hist = oracle_solve(oracle, pr, prm, seed=13, fourier=4)
+    got, res = gpu_solve(lib, cuda, pr, prm, seed=13, fourier=4)
+    assert res.iter == info.iter and res.status == info.status
+    assert np.array_equal(res.history, hist)
+    assert np.array_equal(pr.gather(got, "p"), pr.gather(ref, "p"))
