@@ -117,20 +117,39 @@ __global__ void __launch_bounds__(kTile) k_add_correction(const BlkFld *__restri
   const long long fs = (long long)F.ti * F.tj;
   const bool jg = j == 0 || j == ny + 1;
   const int k1 = min(t.k0 + kch - 1, nz + 1);
-  long long e = (long long)t.k0 * plane + (long long)j * hp + h;  // compact element without the colour term
-  long long f = fidx(F, i0, j, t.k0);
-  for (int k = t.k0; k <= k1; ++k, e += plane, f += fs) {
-    const int c0 = (i0 + j + k + 1) & 1;
-    const long long a0 = c0 * cs + e, a1 = (1 - c0) * cs + e;
-    const double ppref = 0.0;
-    const bool kg = k == 0 || k == nz + 1;
-    const double pp0 = (double)phi[a0];
-    P[f] = (P[f] + (pp0 - ppref));
-    if (i0 == 0 || jg || kg) phi[a0] = (T)0;
-    if (has1) {
-      const double pp1 = (double)phi[a1];
-      P[f + 1] = (P[f + 1] + (pp1 - ppref));
-      if (i1 == nx + 1 || jg || kg) phi[a1] = (T)0;
+  const long long e0 = (long long)j * hp + h;  // compact element of plane 0 without the colour term
+  const long long f0 = fidx(F, i0, j, 0);
+  const double ppref = 0.0;
+  // batches of AC_U planes: every load of a batch is issued before its stores
+  constexpr int AC_U = 4;
+  for (int kb = t.k0; kb <= k1; kb += AC_U) {
+    double q0[AC_U], q1[AC_U], v0[AC_U], v1[AC_U];
+#pragma unroll
+    for (int u = 0; u < AC_U; ++u) {
+      const int k = kb + u;
+      if (k > k1) break;
+      const int c0 = (i0 + j + k + 1) & 1;
+      const long long e = e0 + k * plane, f = f0 + k * fs;
+      q0[u] = (double)phi[c0 * cs + e];
+      v0[u] = P[f];
+      if (has1) {
+        q1[u] = (double)phi[(1 - c0) * cs + e];
+        v1[u] = P[f + 1];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < AC_U; ++u) {
+      const int k = kb + u;
+      if (k > k1) break;
+      const int c0 = (i0 + j + k + 1) & 1;
+      const long long e = e0 + k * plane, f = f0 + k * fs;
+      const bool kg = k == 0 || k == nz + 1;
+      P[f] = (v0[u] + (q0[u] - ppref));
+      if (i0 == 0 || jg || kg) phi[c0 * cs + e] = (T)0;
+      if (has1) {
+        P[f + 1] = (v1[u] + (q1[u] - ppref));
+        if (i1 == nx + 1 || jg || kg) phi[(1 - c0) * cs + e] = (T)0;
+      }
     }
   }
 }
