@@ -92,11 +92,19 @@ typedef struct mf3d_params {
   int differencing; /* 1 = 2nd-order divergence in calmas (press.for:38-67)  */
   int precision;    /* enum mf3d_precision                                   */
   int device;       /* CUDA device ordinal                                   */
+  int pl_ex;        /* extra ghost planes (control.cin pl_ex; pl = LMR + pl_ex,
+                       localparameters.for:17-24): the final exchange(1..3)
+                       refreshes ghost layers 0..pl_ex of u, v, w
+                       (exchange.for:16-20).  0 <= pl_ex < pl, and every block
+                       edge must exceed pl_ex.                                */
 } mf3d_params;
 
 /* Field pointers of one block, each a (ttc_i,ttc_j,ttc_k) array.
  * ustar/vstar/wstar: in.  p: in/out.  u/v/w: in (faces on physical walls,
- * which calvel never writes) and out (all faces calvel writes).  For the host
+ * which calvel never writes) and out (all faces calvel writes, and the ghost
+ * faces exchange(1..3) refreshes: layers 0..pl_ex over the interior
+ * tangential range on every face that is not a physical wall; ghost edges and
+ * corners are left as given).  For the host
  * entry point these are host pointers; for the `_device` one, device pointers.
  * `su` may be NULL; if set it receives the final RHS div(u)/dt (calmas). */
 typedef struct mf3d_fields {

@@ -83,6 +83,7 @@ class Params(C.Structure):
         ("differencing", C.c_int),
         ("precision", C.c_int),
         ("device", C.c_int),
+        ("pl_ex", C.c_int),
     ]
 
 

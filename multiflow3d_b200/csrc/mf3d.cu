@@ -78,6 +78,16 @@ static cudaMemPool_t device_pool() {
   return pools[dev];
 }
 
+// MF3D_POISON_ALLOC=1 fills every new device allocation with 0xFF bytes
+// (a NaN in every FP64/FP32 element): a kernel that reads library memory
+// nothing wrote - which a reused pool block would otherwise hand over with
+// an earlier context's data - then ends in a non-finite residual instead of
+// a silently different result.  A testing aid; off by default.
+static bool poison_allocations() {
+  const char *e = std::getenv("MF3D_POISON_ALLOC");
+  return e && e[0] && e[0] != '0';
+}
+
 // A device array.  alloc() keeps the current allocation when it is large
 // enough (rebuilt launch tables reuse their buffers).
 template <typename T>
@@ -130,6 +140,13 @@ struct DevBuf {
       return e == cudaErrorMemoryAllocation ? MF3D_E_OOM : MF3D_E_CUDA;
     }
     n = cap = count;
+    if (poison_allocations()) {
+      e = s_alloc ? cudaMemsetAsync(p, 0xFF, count * sizeof(T), s_alloc) : cudaMemset(p, 0xFF, count * sizeof(T));
+      if (e != cudaSuccess) {
+        set_error(std::string("poisoning an allocation: ") + cudaGetErrorString(e));
+        return MF3D_E_CUDA;
+      }
+    }
     return MF3D_OK;
   }
   int upload(const std::vector<T> &h, cudaStream_t s) {
@@ -503,9 +520,9 @@ struct View {
   std::vector<ViewLevel> lv;          // [1..Lmax]
   std::vector<BlkFld> hf;
   DevBuf<BlkFld> df;
-  DevBuf<Tile> t_int, t_zint, t_l1cells, t_faces, t_planes, t_pairs;
+  DevBuf<Tile> t_int, t_zint, t_l1cells, t_faces, t_planes, t_pairs, t_vfaces;
   int n_pairs = 0, pairs_kch = 1;
-  int n_int = 0, n_zint = 0, n_l1cells = 0, n_faces = 0, n_planes = 0;
+  int n_int = 0, n_zint = 0, n_l1cells = 0, n_faces = 0, n_planes = 0, n_vfaces = 0;
   DevBuf<DomState> ds;
   DevBuf<int> act, ones;
   DevBuf<int> err;                    // device error code (a TMA wait that gave up)
@@ -788,7 +805,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
   // level-1 field tables
   V.hf.resize(nb);
   std::vector<Tile> t1, t2, t5;
-  std::vector<long long> it_faces, it_planes;
+  std::vector<long long> it_faces, it_planes, it_vfaces;
   for (int b = 0; b < nb; ++b) {
     const BlockStore &S = *V.blk[b];
     BlkFld F = S.fld;
@@ -808,6 +825,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
     add_tiles_2d(t5, b, Box{1, x.nx, 1, x.ny, 1, x.nz}, OZ_TX, OZ_RJ, OZ_KCH);
     it_faces.push_back(2 * ((long long)x.ny * x.nz + (long long)x.nx * x.nz + (long long)x.nx * x.ny));
     it_planes.push_back((long long)x.ny * x.nz + (long long)x.nx * x.nz + (long long)x.nx * x.ny);
+    it_vfaces.push_back((long long)(C->prm.pl_ex + 1) * it_faces.back());
     V.n_l1 += (long long)x.nx * x.ny * x.nz;
   }
   {
@@ -821,15 +839,16 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
     V.n_pairs = (int)tp.size();
     if ((st = V.t_pairs.upload(tp, s))) return st;
   }
-  auto t3 = make_tiles(it_faces), t4 = make_tiles(it_planes);
+  auto t3 = make_tiles(it_faces), t4 = make_tiles(it_planes), t6 = make_tiles(it_vfaces);
   V.n_int = (int)t1.size(); V.n_l1cells = (int)t2.size(); V.n_faces = (int)t3.size();
-  V.n_planes = (int)t4.size(); V.n_zint = (int)t5.size();
+  V.n_planes = (int)t4.size(); V.n_zint = (int)t5.size(); V.n_vfaces = (int)t6.size();
   if ((st = V.df.upload(V.hf, s))) return st;
   if ((st = V.t_int.upload(t1, s))) return st;
   if ((st = V.t_zint.upload(t5, s))) return st;
   if ((st = V.t_l1cells.upload(t2, s))) return st;
   if ((st = V.t_faces.upload(t3, s))) return st;
   if ((st = V.t_planes.upload(t4, s))) return st;
+  if ((st = V.t_vfaces.upload(t6, s))) return st;
   // per-domain solve state
   std::vector<int> ones(std::max(nd, 1), 1);
   if ((st = V.ds.alloc(std::max(nd, 1)))) return st;
@@ -1178,7 +1197,8 @@ static int solve_end(mf3d_ctx *C, View &V) {
     ++C->launches;
   }
   k_calvel<<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, V.ds.p, nullptr);
-  ++C->launches;
+  k_vel_faces<<<V.n_vfaces, kTile, 0, s>>>(V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
+  C->launches += 2;
   return MF3D_OK;
 }
 
@@ -1356,6 +1376,7 @@ static int check_params(const mf3d_params *prm) {
   if (prm->mg_itrsch < 1 || prm->mg_itrsch > 3) { set_error("error about mg iteration selection (mg_itrsch)"); return MF3D_E_INVALID; }
   if (prm->irestr < 0 || prm->iproln < 0 || prm->maxcy < 0) { set_error("negative sweep/cycle count"); return MF3D_E_INVALID; }
   if (prm->pl < 1) { set_error("pl must be >= 1"); return MF3D_E_INVALID; }
+  if (prm->pl_ex < 0 || prm->pl_ex >= prm->pl) { set_error("pl_ex must satisfy 0 <= pl_ex < pl"); return MF3D_E_INVALID; }
   if (prm->differencing != 1) { set_error("differencing != 1 (4th-order calmas) is not supported"); return MF3D_E_UNSUPPORTED; }
   if (prm->precision < 0 || prm->precision > 1) { set_error("precision mode not supported"); return MF3D_E_UNSUPPORTED; }
   return MF3D_OK;
@@ -1403,6 +1424,10 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
     if (d.nx < 1 || d.ny < 1 || d.nz < 1 || d.nx % pow2 || d.ny % pow2 || d.nz % pow2) {  // localparameters.for:201-206
       set_error("2:the given number not correct for mgsolver! (block " + std::to_string(d.id) +
                 " not divisible by 2^(ngrid-1))");
+      return MF3D_E_INVALID;
+    }
+    if (d.nx <= prm->pl_ex || d.ny <= prm->pl_ex || d.nz <= prm->pl_ex) {
+      set_error("block " + std::to_string(d.id) + ": an edge does not exceed pl_ex");
       return MF3D_E_INVALID;
     }
   }
@@ -1460,6 +1485,11 @@ static mf3d_block_desc lone_block(const mf3d_domain_desc &x) {
   return d;
 }
 
+// The final exchange(1..3) reads planes 1..pl_ex+1 inside each face.
+static bool edges_exceed(const mf3d_domain_desc &x, int pl_ex) {
+  return x.nx > pl_ex && x.ny > pl_ex && x.nz > pl_ex;
+}
+
 static int domain_ngrid(const mf3d_domain_desc &x) {
   if (x.nx < 1 || x.ny < 1 || x.nz < 1) return -1;
   if (x.ngrid <= 0) return mf3d_max_levels(x.nx, x.ny, x.nz);
@@ -1472,11 +1502,16 @@ static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params 
   if (!doms || nd <= 0 || !out) { set_error("mf3d_batch_create: bad arguments"); return MF3D_E_INVALID; }
   int st = check_params(prm);
   if (st) return st;
-  for (int d = 0; d < nd; ++d)
+  for (int d = 0; d < nd; ++d) {
     if (domain_ngrid(doms[d]) < 1) {
       set_error("domain " + std::to_string(d) + ": sizes not divisible by 2^(ngrid-1)");
       return MF3D_E_INVALID;
     }
+    if (!edges_exceed(doms[d], prm->pl_ex)) {
+      set_error("domain " + std::to_string(d) + ": an edge does not exceed pl_ex");
+      return MF3D_E_INVALID;
+    }
+  }
   auto C = std::make_unique<mf3d_ctx>();
   if ((st = ctx_init(C.get(), prm))) return st;
   AllocScope scope(C->stream);

@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(kTile) k_add_correction(const BlkFld *__restri
       const long long e = e0 + k * plane, f = f0 + k * fs;
       const bool kg = k == 0 || k == nz + 1;
       P[f] = (v0[u] + (q0[u] - ppref));
-      if (i0 == 0 || jg || kg) phi[c0 * cs + e] = (T)0;
+      if (i0 == 0 || i0 == nx + 1 || jg || kg) phi[c0 * cs + e] = (T)0;  // i0 = nx+1 when nx is odd
       if (has1) {
         P[f + 1] = (v1[u] + (q1[u] - ppref));
         if (i1 == nx + 1 || jg || kg) phi[(1 - c0) * cs + e] = (T)0;
@@ -183,6 +183,51 @@ __global__ void k_p_faces(const BlkFld *__restrict__ fl, const Tile *__restrict_
     default: gi = a; gj = b; gk = nz + 1; si = a; sj = b; sk = wall ? nz : 1; break;
   }
   F.p[fidx(F, gi, gj, gk)] = S.p[fidx(S, si, sj, sk)];
+}
+
+// exchange(1), (2), (3) after the final calvel (exchange.for:2-23 with
+// nly = pl_ex; exchange_bc.for:16-320; the face unpack of exchange_smlvl,
+// exchange.for:2402-2490): on every face that is not a physical wall, ghost
+// layer ly = 0..nly of u, v and w over the interior tangential range takes
+// the source block's value ly planes inside its facing boundary - low ghost
+// (0-ly) from source plane n-ly, high ghost (n+1+ly) from source plane 1+ly.
+// The velocity ranges of a face that has a source block are never cut short
+// (localparameters.for:185-190 shortens them at walls only), so the same
+// planes serve u, v and w.  Reads touch interior cells only (every edge
+// exceeds nly), writes ghost cells only: one pass, no ordering.  Ghost edges
+// and corners are not written.  Items per block: (nly+1) * 2*(ny*nz + nx*nz
+// + nx*ny); `only` (may be null) as in k_calvel.
+__global__ void k_vel_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                            const int *__restrict__ only, int nly) {
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  if (only && !only[F.dom]) return;
+  int q = t.i0 + threadIdx.x;
+  const int nx = F.nx, ny = F.ny, nz = F.nz;
+  const int nyz = ny * nz, nxz = nx * nz, nxy = nx * ny;
+  const int per_layer = 2 * (nyz + nxz + nxy);
+  const int ly = q / per_layer;
+  if (ly > nly) return;
+  q -= ly * per_layer;
+  int f, a, b;
+  if (q < 2 * nyz) { f = q / nyz; q -= f * nyz; a = q % ny + 1; b = q / ny + 1; }
+  else if ((q -= 2 * nyz) < 2 * nxz) { f = 2 + q / nxz; q -= (f - 2) * nxz; a = q % nx + 1; b = q / nx + 1; }
+  else { q -= 2 * nxz; f = 4 + q / nxy; q -= (f - 4) * nxy; a = q % nx + 1; b = q / nx + 1; }
+  if (F.wall[f]) return;
+  const BlkFld &S = fl[F.src[f]];
+  int gi, gj, gk, si, sj, sk;  // ghost cell; source cell (in the source block)
+  switch (f) {
+    case 0: gi = -ly; gj = a; gk = b; si = S.nx - ly; sj = a; sk = b; break;
+    case 1: gi = nx + 1 + ly; gj = a; gk = b; si = 1 + ly; sj = a; sk = b; break;
+    case 2: gi = a; gj = -ly; gk = b; si = a; sj = S.ny - ly; sk = b; break;
+    case 3: gi = a; gj = ny + 1 + ly; gk = b; si = a; sj = 1 + ly; sk = b; break;
+    case 4: gi = a; gj = b; gk = -ly; si = a; sj = b; sk = S.nz - ly; break;
+    default: gi = a; gj = b; gk = nz + 1 + ly; si = a; sj = b; sk = 1 + ly; break;
+  }
+  const long long g = fidx(F, gi, gj, gk), s = fidx(S, si, sj, sk);
+  F.u[g] = S.u[s];
+  F.v[g] = S.v[s];
+  F.w[g] = S.w[s];
 }
 
 // Face planes used by the fused calvel/calmas kernel, filled once per solve:

@@ -383,6 +383,7 @@ static void srv_loop(mf3d_server *S, int lane) {
     int st = fmask.upload(fin, s);
     if (!st) {
       k_calvel<<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, V.ds.p, fmask.p);
+      k_vel_faces<<<V.n_vfaces, kTile, 0, s>>>(V.df.p, V.t_vfaces.p, fmask.p, C->prm.pl_ex);
       if (cudaMemcpyAsync(hs.data(), V.ds.p, nd * sizeof(DomState), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
           cudaStreamSynchronize(s) != cudaSuccess)
         st = MF3D_E_CUDA;
@@ -471,6 +472,10 @@ int mf3d_server_submit(mf3d_server *S, const mf3d_domain_desc *dom, const mf3d_f
   }
   const int ngrid = domain_ngrid(*dom);
   if (ngrid < 1) { set_error("mf3d_server_submit: sizes not divisible by 2^(ngrid-1)"); return MF3D_E_INVALID; }
+  if (!edges_exceed(*dom, S->C[0]->prm.pl_ex)) {
+    set_error("mf3d_server_submit: an edge does not exceed pl_ex");
+    return MF3D_E_INVALID;
+  }
   auto r = std::make_unique<SrvReq>();
   r->desc = *dom;
   r->fields = *f;

@@ -126,7 +126,10 @@ class Problem:
                 C.c_double(self.dx), C.c_double(self.dy), C.c_double(self.dz), arr)
         if st != 0:
             raise RuntimeError(f"topology build failed: {st}")
-        self._keep = []
+        # the descriptors point into these arrays: keep every call's alive
+        # (descriptors for the library and for the oracle coexist)
+        if not hasattr(self, "_keep"):
+            self._keep = []
         for b in range(self.nblocks):
             hy = self.block_widths_y(b)
             if hy is not None:
@@ -135,10 +138,11 @@ class Problem:
         return arr
 
     def params(self, mg_itrsch=3, irestr=2, iproln=1, maxcy=200, eps=1e-8,
-               eps_relative=1, precision=MF3D_PREC_FP64, device=0) -> Params:
+               eps_relative=1, precision=MF3D_PREC_FP64, device=0, pl_ex=0) -> Params:
         return Params(ngrid=self.ngrid, mg_itrsch=mg_itrsch, irestr=irestr,
                       iproln=iproln, maxcy=maxcy, eps=eps, eps_relative=eps_relative,
-                      pl=self.pl, differencing=1, precision=precision, device=device)
+                      pl=self.pl, differencing=1, precision=precision, device=device,
+                      pl_ex=pl_ex)
 
     # ------------------------------------------------------------------
     # seeded inputs

@@ -89,7 +89,7 @@ template <class Fn> void par_blocks(int n, Fn fn) {
 struct Ctx {
   std::vector<Blk> b;
   std::map<int, int> indid; /* dom_indid: block id -> position */
-  int ngrd_gl, mg_itrsch, irestr, iproln, maxcy, pl;
+  int ngrd_gl, mg_itrsch, irestr, iproln, maxcy, pl, pl_ex;
   double eps;
   int eps_relative;
   bool periodic;
@@ -641,8 +641,9 @@ void mgkcyc(Ctx &C) {
 /* exchange_smlvl (exchange.for:343-2498).  The corner/edge part of     */
 /* exchange_smlvl is unpacked before the faces and only its ghost       */
 /* edges and corners survive; nothing on this path reads those, so it   */
-/* is not restated.  One ghost layer (ly = 0): calvel and calmas with   */
-/* differencing = 1 read no other.                                      */
+/* is not restated.  Layers ly = 0..nly, nly = pl_ex for u, v, w and 0  */
+/* for p (exchange.for:14-20); calvel and calmas with differencing = 1  */
+/* read layer 0 only, the others are outputs of the final calvel.       */
 /* ------------------------------------------------------------------ */
 double *field_of(Blk &B, int op) { return op == 1 ? B.u : op == 2 ? B.v : op == 3 ? B.w : B.p; }
 void franges(Blk &B, int op, int &is, int &ie, int &js, int &je, int &ks, int &ke) {
@@ -652,8 +653,8 @@ void franges(Blk &B, int op, int &is, int &ie, int &js, int &je, int &ks, int &k
   else { is = B.isp; ie = B.iep; js = B.jsp; je = B.jep; ks = B.ksp; ke = B.kep; }
 }
 
-void exchange_bc(Ctx &C, int op) {
-  const int ly = 0;
+void exchange_bc(Ctx &C, int op, int nly) {
+  for (int ly = 0; ly <= nly; ++ly)
   for (int ax = 0; ax < 3; ++ax) {
     for (auto &B : C.b) {
       int bcp = ax == 0 ? B.d.bc_west : ax == 1 ? B.d.bc_south : B.d.bc_bottom;
@@ -716,8 +717,8 @@ void exchange_bc(Ctx &C, int op) {
   }
 }
 
-void exchange_smlvl_faces(Ctx &C, int op) {
-  const int ly = 0;
+void exchange_smlvl_faces(Ctx &C, int op, int nly) {
+  for (int ly = 0; ly <= nly; ++ly) {
   /* pack: all six faces of every block from one snapshot */
   std::vector<std::vector<double>> bm(C.b.size() * 4), bp(C.b.size() * 4);
   for (size_t ib = 0; ib < C.b.size(); ++ib) {
@@ -774,11 +775,13 @@ void exchange_smlvl_faces(Ctx &C, int op) {
       }
     }
   }
+  }
 }
 
 void exchange(Ctx &C, int op) {
-  if (C.periodic) exchange_bc(C, op);
-  exchange_smlvl_faces(C, op);
+  const int nly = op == 4 ? 0 : C.pl_ex;
+  if (C.periodic) exchange_bc(C, op, nly);
+  exchange_smlvl_faces(C, op, nly);
 }
 
 /* pbound (press.for:77-137) */
@@ -899,6 +902,8 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
   if (prm->differencing != 1) { g_err = "differencing"; return MF3D_E_UNSUPPORTED; }
   C.ngrd_gl = prm->ngrid; C.mg_itrsch = prm->mg_itrsch; C.irestr = prm->irestr; C.iproln = prm->iproln;
   C.maxcy = prm->maxcy; C.eps = prm->eps; C.eps_relative = prm->eps_relative; C.pl = prm->pl;
+  C.pl_ex = prm->pl_ex;
+  if (C.pl_ex < 0 || C.pl_ex >= C.pl) { g_err = "pl_ex"; return MF3D_E_INVALID; }
   C.periodic = false;
   C.b.resize(nb);
   for (int ib = 0; ib < nb; ++ib) {
@@ -908,6 +913,7 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
     int pl = prm->pl;
     int pow2 = 1 << (B.ngrid - 1);
     if (B.d.nx % pow2 || B.d.ny % pow2 || B.d.nz % pow2) { g_err = "not divisible"; return MF3D_E_INVALID; }
+    if (B.d.nx <= C.pl_ex || B.d.ny <= C.pl_ex || B.d.nz <= C.pl_ex) { g_err = "block edge <= pl_ex"; return MF3D_E_INVALID; }
     C.indid[B.d.id] = ib;
     B.isp = 1 + pl; B.iep = B.d.nx + B.isp - 1;
     B.jsp = 1 + pl; B.jep = B.d.ny + B.jsp - 1;

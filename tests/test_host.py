@@ -101,6 +101,28 @@ def test_create_rejects_bad_config_without_gpu(lib):
                            C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED
 
 
+def test_create_rejects_bad_pl_ex_without_gpu(lib, oracle):
+    """pl_ex (extra ghost planes of u, v, w refreshed by the final
+    exchange(1..3)) must lie in 0..pl-1, and every block edge must exceed it;
+    the library and the oracle reject the same configurations."""
+    ctx = C.c_void_p()
+    pr = Problem(1, 1, 1, 8, 8, 8, ngrid=2, pl=2)
+    for pl_ex in (-1, 2):
+        prm = pr.params(pl_ex=pl_ex)
+        assert lib.mf3d_create(pr.descriptors(lib), 1, C.byref(prm), C.byref(ctx)) == abi.MF3D_E_INVALID
+        assert b"pl_ex" in lib.mf3d_last_error()
+    small = Problem(1, 1, 1, 8, 2, 8, ngrid=1, pl=3)
+    prm = small.params(pl_ex=2)
+    assert lib.mf3d_create(small.descriptors(lib), 1, C.byref(prm), C.byref(ctx)) == abi.MF3D_E_INVALID
+    assert b"pl_ex" in lib.mf3d_last_error()
+    blocks = small.block_fields(seed=1)
+    from multiflow3d_b200.abi import SolveInfo
+    from multiflow3d_b200.problems import fields_struct
+    st = oracle.orc_newsolv_mg(small.descriptors(oracle), 1, C.byref(prm), fields_struct(blocks), 1.0, 1.0,
+                               C.byref(SolveInfo()), None, 0)
+    assert st == abi.MF3D_E_INVALID
+
+
 def test_topology_rejects_fractional_extent(lib):
     ext = np.array([0.0, 1.05, 0.0, 1.0, 0.0, 1.0])
     bc6 = (C.c_int * 6)(5, 5, 4, 4, 5, 5)

@@ -210,3 +210,31 @@ def test_not_converged_and_diverged_status(oracle):
             f[k] *= 1e6
     st, info, _ = solve(oracle, pr, blocks, mg_itrsch=3, maxcy=1, eps=1e-14)
     assert st == 2  # rmax > 100 after the loop (newsolv_mg.for:64)
+
+
+@pytest.mark.parametrize("pl,pl_ex", [(1, 0), (2, 1), (3, 2)])
+def test_velocity_ghost_layers_wrap(oracle, pl, pl_ex):
+    """One block, periodic in x and y: after the projection, ghost layer ly
+    (0..pl_ex) of u, v, w holds the interior value ly planes inside the
+    opposite face (exchange_bc.for:147-178), and deeper layers are untouched."""
+    pr = Problem(1, 1, 1, 8, 8, 8, bc=(PERIODIC, PERIODIC, PERIODIC, PERIODIC, WALL, WALL), ngrid=2, pl=pl)
+    blocks = pr.block_fields(seed=5)
+    given = {k: blocks[0][k].copy() for k in ("u", "v", "w")}
+    info = SolveInfo()
+    st = oracle.orc_newsolv_mg(pr.descriptors(oracle), 1, C.byref(pr.params(maxcy=3, pl_ex=pl_ex)),
+                               fields_struct(blocks), 1.0, 1.0, C.byref(info), None, 0)
+    assert st >= 0
+    n = 8
+    K = J = I = slice(pl, pl + n)
+    for k in ("u", "v", "w"):
+        a = blocks[0][k]
+        for ly in range(pl):
+            lo, hi = pl - 1 - ly, pl + n + ly
+            if ly <= pl_ex:
+                assert np.array_equal(a[K, J, lo], a[K, J, pl + n - 1 - ly])
+                assert np.array_equal(a[K, J, hi], a[K, J, pl + ly])
+                assert np.array_equal(a[K, lo, I], a[K, pl + n - 1 - ly, I])
+                assert np.array_equal(a[K, hi, I], a[K, pl + ly, I])
+            else:
+                assert np.array_equal(a[K, J, lo], given[k][K, J, lo])
+                assert np.array_equal(a[K, lo, I], given[k][K, lo, I])
