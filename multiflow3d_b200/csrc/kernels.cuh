@@ -74,6 +74,19 @@ struct Coef {
   }
 };
 
+// Programmatic dependent launch.  The host launches the kernels of a solve
+// with programmatic stream serialisation, so a kernel's CTAs may be resident
+// before the kernel it depends on has finished: they are placed as that
+// kernel's CTAs retire, instead of after a full drain and a launch gap.
+// Every kernel therefore begins with this wait, which returns once all
+// prerequisite grids have completed and their memory operations are
+// visible; nothing is read or written before it.  Without a programmatic
+// predecessor it returns at once.  No kernel signals its dependents early
+// (griddepcontrol.launch_dependents): the next grid launches as this one's
+// CTAs exit.  Signalling right after the wait measured slower (11.0 against
+// 11.4 solves/s), the waiting CTAs taking issue slots from the last wave.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // A CTA's work: block position and the origin of its tile.  2-D tiles:
 // threadIdx.x runs along i (or the compact index h), threadIdx.y along j;
 // k0 is the plane (or the first plane of a z-marching chunk).
@@ -183,6 +196,7 @@ template <typename T, bool FROM_ZERO>
 __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict__ bl, const Tile *__restrict__ tiles,
                                                        const int *__restrict__ act, int colour, int kch,
                                                        int *__restrict__ err) {
+  pdl_wait();
   using S = RbShape<T>;
   constexpr int W = S::W;
   constexpr int OB = FROM_ZERO ? 0 : S::OB;
@@ -298,6 +312,7 @@ template <typename T, bool FROM_ZERO>
 __global__ void __launch_bounds__(kTile) k_rbgs_small(const BlkLev *__restrict__ bl, const int *__restrict__ pre,
                                                       const int *__restrict__ blocks, int nb,
                                                       const int *__restrict__ act, int colour) {
+  pdl_wait();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= pre[nb]) return;
   int lo = 0, hi = nb - 1;  // last list entry whose first item <= t
@@ -344,6 +359,7 @@ __global__ void __launch_bounds__(kTile) k_rbgs_small(const BlkLev *__restrict__
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_lexgs(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, const int *__restrict__ act) {
+  pdl_wait();
   const BlkLev B = bl[blocks[blockIdx.x]];
   if (!act[B.dom]) return;
   T *P = phi_of<T>(B);
@@ -420,6 +436,7 @@ __device__ void tdma_line(const BlkLev &B, int dir, int u, int v, T *a, T *c) {
 template <typename T>
 __global__ void k_tdma(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, const int *__restrict__ act,
                        T *__restrict__ work, int ngg) {
+  pdl_wait();
   const BlkLev B = bl[blocks[blockIdx.x]];
   if (!act[B.dom]) return;
   T *a = work + ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2 * ngg;
@@ -454,6 +471,7 @@ template <typename TF, typename TC>
 __global__ void __launch_bounds__(kTile, 2) k_restrict(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
                                                       const Tile *__restrict__ tiles, const int *__restrict__ act,
                                                       int kch) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkLev Cb = cl[t.blk];
   if (!act[Cb.dom]) return;
@@ -540,6 +558,7 @@ template <typename TF, typename TC>
 __global__ void __launch_bounds__(kTile) k_restrict_tma(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
                                                         const Tile *__restrict__ tiles, const int *__restrict__ act,
                                                         int kch, int *__restrict__ err) {
+  pdl_wait();
   using S = RsShape<TF>;
   constexpr int W = S::W;
   extern __shared__ __align__(128) unsigned char rs_smem[];
@@ -662,6 +681,7 @@ template <typename TF, typename TC>
 __global__ void __launch_bounds__(kTile) k_prolong(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
                                                    const Tile *__restrict__ tiles, const int *__restrict__ act,
                                                    int kch) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkLev Fb = fl[t.blk];
   if (!act[Fb.dom]) return;
@@ -767,6 +787,7 @@ __device__ __forceinline__ int halo_segment(const HaloSeg *__restrict__ seg, int
 template <typename T>
 __global__ void k_halo_stage(const BlkLev *__restrict__ bl, const HaloSeg *__restrict__ seg, int nseg,
                              long long nstaged, const int *__restrict__ act, T *__restrict__ buf) {
+  pdl_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nstaged) return;
   const HaloSeg &S = seg[halo_segment<true>(seg, nseg, t)];
@@ -777,6 +798,7 @@ __global__ void k_halo_stage(const BlkLev *__restrict__ bl, const HaloSeg *__res
 template <typename T>
 __global__ void k_halo_apply(const BlkLev *__restrict__ bl, const HaloSeg *__restrict__ seg, int nseg, long long n,
                              const int *__restrict__ act, const T *__restrict__ buf) {
+  pdl_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const HaloSeg &S = seg[halo_segment<false>(seg, nseg, t)];
@@ -791,6 +813,7 @@ __global__ void k_halo_apply(const BlkLev *__restrict__ bl, const HaloSeg *__res
 // thread per ghost cell, enumerated face by face (edges twice - zeros).
 template <typename T>
 __global__ void k_zero_ghosts(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, int nblk) {
+  pdl_wait();
   const int b = blockIdx.y;
   if (b >= nblk) return;
   const BlkLev B = bl[blocks[b]];

@@ -21,6 +21,7 @@
 #include <string>
 #include <unordered_map>
 #include <unordered_set>
+#include <utility>
 #include <vector>
 
 #include <cudaTypedefs.h>
@@ -158,6 +159,36 @@ struct DevBuf {
 };
 
 static inline int grid_of(long long n, int tpb) { return (int)((n + tpb - 1) / tpb); }
+
+// Every kernel of a solve is launched with programmatic stream
+// serialisation: its CTAs may be placed while the previous kernel on the
+// stream drains, and each kernel's first statement (pdl_wait) holds them
+// until that kernel has completed.  This removes the launch gap between the
+// dependent kernels of an iteration - most of the cost of the small coarse
+// levels.  The edges survive stream capture, so the solve graphs keep them.
+// MF3D_PDL=0 (read once) launches without the attribute, for comparison.
+static bool pdl_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("MF3D_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+template <typename... KArgs, typename... Args>
+static cudaError_t launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                          Args &&...args) {
+  cudaLaunchAttribute at;
+  at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at.val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = &at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // 1-D item tiles: for each block, ceil(items_b / kTile) CTAs (i0 = first item).
 static std::vector<Tile> make_tiles(const std::vector<long long> &items) {
@@ -876,11 +907,11 @@ static void halo(mf3d_ctx *C, View &V, int g, int q) {
   if (!L.n_halo[q]) return;
   T *buf = (T *)L.stage[q].p;
   if (L.n_staged[q]) {
-    k_halo_stage<T><<<grid_of(L.n_staged[q], 256), 256, 0, C->stream>>>(L.tab.p, L.hseg[q].p, L.n_hseg[q],
+    launch(k_halo_stage<T>, grid_of(L.n_staged[q], 256), 256, 0, C->stream, L.tab.p, L.hseg[q].p, L.n_hseg[q],
                                                                        L.n_staged[q], V.act.p, buf);
     ++C->launches;
   }
-  k_halo_apply<T><<<grid_of(L.n_halo[q], 256), 256, 0, C->stream>>>(L.tab.p, L.hseg[q].p, L.n_hseg[q],
+  launch(k_halo_apply<T>, grid_of(L.n_halo[q], 256), 256, 0, C->stream, L.tab.p, L.hseg[q].p, L.n_hseg[q],
                                                                    L.n_halo[q], V.act.p, buf);
   ++C->launches;
 }
@@ -902,32 +933,32 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
       if (L.small) {
         const int g2 = grid_of(L.small_items[q], kTile);
         if (fz)
-          k_rbgs_small<T, true><<<g2, kTile, 0, C->stream>>>(L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 0);
+          launch(k_rbgs_small<T, true>, g2, kTile, 0, C->stream, L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 0);
         else
-          k_rbgs_small<T, false><<<g2, kTile, 0, C->stream>>>(L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p,
+          launch(k_rbgs_small<T, false>, g2, kTile, 0, C->stream, L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p,
                                                              0);
         prof_end(C, pk);
         prof_begin(C, pk, 3 * half);
-        k_rbgs_small<T, false><<<g2, kTile, 0, C->stream>>>(L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 1);
+        launch(k_rbgs_small<T, false>, g2, kTile, 0, C->stream, L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 1);
         prof_end(C, pk);
         C->launches += 2;
         halo<T>(C, V, g, q);
         continue;
       }
       if (fz)
-        k_rbgs<T, true><<<grid, cta, 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
+        launch(k_rbgs<T, true>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
       else
-        k_rbgs<T, false><<<grid, cta, 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
+        launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
       prof_end(C, pk);
       prof_begin(C, pk, 3 * half);
-      k_rbgs<T, false><<<grid, cta, 0, C->stream>>>(L.tab.p, L.sweep[q].p, V.act.p, 1, L.kch[q], V.err.p);
+      launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 1, L.kch[q], V.err.p);
       prof_end(C, pk);
       C->launches += 2;
     } else if (sch == 1) {
-      k_lexgs<T><<<L.n_list[q], 1024, 0, C->stream>>>(L.tab.p, L.list[q].p, V.act.p);
+      launch(k_lexgs<T>, L.n_list[q], 1024, 0, C->stream, L.tab.p, L.list[q].p, V.act.p);
       ++C->launches;
     } else {
-      k_tdma<T><<<L.n_list[q], 128, 0, C->stream>>>(L.tab.p, L.list[q].p, V.act.p, (T *)V.work.p, L.ngg);
+      launch(k_tdma<T>, L.n_list[q], 128, 0, C->stream, L.tab.p, L.list[q].p, V.act.p, (T *)V.work.p, L.ngg);
       ++C->launches;
     }
     halo<T>(C, V, g, q);
@@ -953,13 +984,13 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
       return true;
     }();
     (void)attr_set;
-    k_restrict_tma<T, TC><<<Cl.n_rtma, kTile, RsShape<T>::SMEM, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtma.p, V.act.p,
+    launch(k_restrict_tma<T, TC>, Cl.n_rtma, kTile, RsShape<T>::SMEM, C->stream, F.tab.p, Cl.tab.p, Cl.rtma.p, V.act.p,
                                                                               Cl.rtma_kch, V.err.p);
     prof_end(C, pk);
     ++C->launches;
     return;
   }
-  k_restrict<T, TC><<<Cl.n_rtile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch);
+  launch(k_restrict<T, TC>, Cl.n_rtile, kTile, 0, C->stream, F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch);
   prof_end(C, pk);
   ++C->launches;
 }
@@ -970,7 +1001,7 @@ static void corr(mf3d_ctx *C, View &V, int g) {  // level g+1 -> g, blocks conti
   if (!F.n_ptile) return;
   const int pk = g == 1 ? MF3D_PROF_PROLONG_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 1.0 / 8.0));  // fine in/out, coarse in
-  k_prolong<T, TC><<<F.n_ptile, kTile, 0, C->stream>>>(F.tab.p, Cl.tab.p, F.ptile.p, V.act.p, F.pkch);
+  launch(k_prolong<T, TC>, F.n_ptile, kTile, 0, C->stream, F.tab.p, Cl.tab.p, F.ptile.p, V.act.p, F.pkch);
   prof_end(C, pk);
   ++C->launches;
 }
@@ -1026,13 +1057,13 @@ static void calvel_calmas(mf3d_ctx *C, View &V, const int *act, unsigned long lo
     const dim3 grid(V.n_zint), cta(OZ_TX, CV_TY);
 #define MF3D_CV(M)                                                                                              \
   case M:                                                                                                        \
-    k_calvel_calmas_tma<T, M><<<grid, cta, 0, C->stream>>>(V.df.p, V.t_zint.p, V.ds.p, act, slot, write_su, OZ_KCH, \
+    launch(k_calvel_calmas_tma<T, M>, grid, cta, 0, C->stream, V.df.p, V.t_zint.p, V.ds.p, act, slot, write_su, OZ_KCH, \
                                                            V.err.p);                                             \
     break;
     switch (mask) { MF3D_CV(0) MF3D_CV(1) MF3D_CV(2) MF3D_CV(3) MF3D_CV(4) MF3D_CV(5) MF3D_CV(6) MF3D_CV(7) }
 #undef MF3D_CV
   } else
-    k_calvel_calmas<T><<<V.n_zint, dim3(OZ_TX, OZ_RJ), 0, C->stream>>>(V.df.p, V.t_zint.p, V.ds.p, act, slot,
+    launch(k_calvel_calmas<T>, V.n_zint, dim3(OZ_TX, OZ_RJ), 0, C->stream, V.df.p, V.t_zint.p, V.ds.p, act, slot,
                                                                       write_su);
 }
 
@@ -1042,12 +1073,12 @@ template <typename T>
 static void iteration_body(mf3d_ctx *C, View &V, int loop_graph) {
   cudaStream_t s = C->stream;
   vcycle<T>(C, V);
-  k_add_correction<T><<<V.n_pairs, kTile, 0, s>>>(V.df.p, V.t_pairs.p, V.act.p, V.pairs_kch);
-  k_p_faces<<<V.n_faces, kTile, 0, s>>>(V.df.p, V.t_faces.p, V.act.p);
+  launch(k_add_correction<T>, V.n_pairs, kTile, 0, s, V.df.p, V.t_pairs.p, V.act.p, V.pairs_kch);
+  launch(k_p_faces, V.n_faces, kTile, 0, s, V.df.p, V.t_faces.p, V.act.p);
   prof_begin(C, MF3D_PROF_CALMAS, (double)V.n_l1 * (4 * sizeof(double) + sizeof(T)));  // p, u*, v*, w* in; su out
   calvel_calmas<T>(C, V, V.act.p, V.rmax.p, 0);
   prof_end(C, MF3D_PROF_CALMAS);
-  k_iter_end<<<1, 256, 0, s>>>(V.ds.p, (int)V.dom.size(), V.rmax.p, V.hist.p, V.hcap, V.act.p, V.cond,
+  launch(k_iter_end, 1, 256, 0, s, V.ds.p, (int)V.dom.size(), V.rmax.p, V.hist.p, V.hcap, V.act.p, V.cond,
                                loop_graph, V.budget.p);
   C->launches += 4;
 }
@@ -1179,9 +1210,9 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
   CK(cudaMemcpyAsync(V.ds.p, hs.data(), nd * sizeof(DomState), cudaMemcpyHostToDevice, s));
   CK(cudaStreamSynchronize(s));  // hs is a local
   CK(cudaMemsetAsync(V.rmax.p, 0, nd * sizeof(unsigned long long), s));
-  k_face_planes<<<V.n_planes, kTile, 0, s>>>(V.df.p, V.t_planes.p);
+  launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p);
   calvel_calmas<T>(C, V, V.ones.p, V.rmax.p, 0);
-  k_dom_init<<<1, 256, 0, s>>>(V.ds.p, nd, V.rmax.p, V.act.p);
+  launch(k_dom_init, 1, 256, 0, s, V.ds.p, nd, V.rmax.p, V.act.p);
   C->launches += 3;
   return MF3D_OK;
 }
@@ -1196,8 +1227,8 @@ static int solve_end(mf3d_ctx *C, View &V) {
     calvel_calmas<T>(C, V, V.ones.p, V.rmax_scratch.p, 1);
     ++C->launches;
   }
-  k_calvel<<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, V.ds.p, nullptr);
-  k_vel_faces<<<V.n_vfaces, kTile, 0, s>>>(V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
+  launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, nullptr);
+  launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
   C->launches += 2;
   return MF3D_OK;
 }
@@ -1297,12 +1328,12 @@ static int mgkcyc_view(mf3d_ctx *C, View &V, double *const *su, double *const *p
   CK(cudaMemcpyAsync(C->ptrs.p + nb, pp, nb * sizeof(double *), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(V.df.p, V.hf.data(), nb * sizeof(BlkFld), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(V.act.p, V.ones.p, V.ones.n * sizeof(int), cudaMemcpyDeviceToDevice, s));
-  k_load_rhs<T><<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, C->ptrs.p);
+  launch(k_load_rhs<T>, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, C->ptrs.p);
   vcycle<T>(C, V);
-  k_store_pp<T><<<V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_l1cells.p, C->ptrs.p + nb);
+  launch(k_store_pp<T>, V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_l1cells.p, C->ptrs.p + nb);
   // restore the invariant: the level-1 ghost shell holds zeros between calls
   ViewLevel &L1 = V.lv[1];
-  k_zero_ghosts<T><<<dim3(64, L1.n_list[SUB_A]), kTile, 0, s>>>(L1.tab.p, L1.list[SUB_A].p, L1.n_list[SUB_A]);
+  launch(k_zero_ghosts<T>, dim3(64, L1.n_list[SUB_A]), kTile, 0, s, L1.tab.p, L1.list[SUB_A].p, L1.n_list[SUB_A]);
   C->launches += 3;
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());
@@ -1354,12 +1385,12 @@ static int mgkcyc_view_noalloc(mf3d_ctx *C, View &V, double *const *su, double *
   CK(cudaMemcpyAsync(tab + nb, pp, nb * sizeof(double *), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(V.df.p, V.hf.data(), nb * sizeof(BlkFld), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(V.act.p, V.ones.p, V.ones.n * sizeof(int), cudaMemcpyDeviceToDevice, s));
-  k_load_rhs<T><<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, tab);
+  launch(k_load_rhs<T>, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, tab);
   vcycle<T>(C, V);
-  k_store_pp<T><<<V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_l1cells.p, tab + nb);
+  launch(k_store_pp<T>, V.n_l1cells, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_l1cells.p, tab + nb);
   // restore the invariant: the level-1 ghost shell holds zeros between calls
   ViewLevel &L1 = V.lv[1];
-  k_zero_ghosts<T><<<dim3(64, L1.n_list[SUB_A]), kTile, 0, s>>>(L1.tab.p, L1.list[SUB_A].p, L1.n_list[SUB_A]);
+  launch(k_zero_ghosts<T>, dim3(64, L1.n_list[SUB_A]), kTile, 0, s, L1.tab.p, L1.list[SUB_A].p, L1.n_list[SUB_A]);
   C->launches += 3;
   CK(cudaStreamSynchronize(s));
   CK(cudaGetLastError());

@@ -71,6 +71,7 @@ __device__ __forceinline__ double div_rcp(double x, double b, double rb) {
 // div_rcp against the IEEE division, element by element (mf3d_selftest_divide).
 __global__ void k_selftest_divide(const double *x, const double *b, const double *rb, long long n, double *q,
                                   double *qref) {
+  pdl_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   q[t] = div_rcp(x[t], b[t], rb[t]);
@@ -101,6 +102,7 @@ template <typename T>
 __global__ void __launch_bounds__(kTile) k_add_correction(const BlkFld *__restrict__ fl,
                                                           const Tile *__restrict__ tiles,
                                                           const int *__restrict__ act, int kch) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   if (!act[fl[t.blk].dom]) return;
   const BlkFld F = fl[t.blk];
@@ -160,6 +162,7 @@ __global__ void __launch_bounds__(kTile) k_add_correction(const BlkFld *__restri
 // interior cell.  Only the interior tangential range: the path reads no
 // other ghost of p.  Items per block: 2*(ny*nz + nx*nz + nx*ny).
 __global__ void k_p_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, const int *__restrict__ act) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   if (!act[F.dom]) return;
@@ -199,6 +202,7 @@ __global__ void k_p_faces(const BlkFld *__restrict__ fl, const Tile *__restrict_
 // + nx*ny); `only` (may be null) as in k_calvel.
 __global__ void k_vel_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
                             const int *__restrict__ only, int nly) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   if (only && !only[F.dom]) return;
@@ -237,6 +241,7 @@ __global__ void k_vel_faces(const BlkFld *__restrict__ fl, const Tile *__restric
 // that block's u); hi[a] = the caller's velocity on a high wall face
 // (localparameters.for:185-190 stops calvel one face short there).
 __global__ void k_face_planes(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   int q = t.i0 + threadIdx.x;
@@ -286,6 +291,7 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas(const BlkFld *__
                                                                const int *__restrict__ act,
                                                                unsigned long long *__restrict__ rmax_slot,
                                                                int write_su) {
+  pdl_wait();
   __shared__ double red[OZ_RJ];
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
@@ -409,6 +415,7 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const Blk
                                                                    const int *__restrict__ act,
                                                                    unsigned long long *__restrict__ rmax_slot,
                                                                    int write_su, int kch, int *__restrict__ err) {
+  pdl_wait();
   using S = CvShape;
   __shared__ __align__(128) unsigned char sbuf[CV_NS * S::STAGE];
   __shared__ __align__(8) uint64_t bar[CV_NS];
@@ -571,6 +578,7 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const Blk
 // `only` (may be null): domains to update, others are left as they are.
 __global__ void __launch_bounds__(RW_TX *RW_RJ) k_calvel(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
                                                          const DomState *__restrict__ ds, const int *__restrict__ only) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   if (only && !only[F.dom]) return;
@@ -593,6 +601,7 @@ __global__ void __launch_bounds__(RW_TX *RW_RJ) k_calvel(const BlkFld *__restric
 // After the initial calvel/calmas (newsolv_mg.for:16-17): rmax0, the
 // absolute threshold, and which domains iterate at all.
 __global__ void k_dom_init(DomState *ds, int ndom, unsigned long long *rmax_slot, int *act) {
+  pdl_wait();
   for (int d = threadIdx.x; d < ndom; d += blockDim.x) {
     const double r = __longlong_as_double((long long)rmax_slot[d]);
     rmax_slot[d] = 0ull;
@@ -615,6 +624,7 @@ __global__ void k_dom_init(DomState *ds, int ndom, unsigned long long *rmax_slot
 // have run, so the host can hand results back and admit new requests.
 __global__ void k_iter_end(DomState *ds, int ndom, unsigned long long *rmax_slot, double *hist, int hcap, int *act,
                            cudaGraphConditionalHandle cond, int in_graph, int *budget) {
+  pdl_wait();
   int any = 0, stopped = 0;
   for (int d = threadIdx.x; d < ndom; d += blockDim.x) {
     if (!act[d]) continue;
@@ -651,6 +661,7 @@ __global__ void k_iter_end(DomState *ds, int ndom, unsigned long long *rmax_slot
 // Level-1 rhs := su (mgkcyc's copy-in, mgsolver.for:250-263) from a ttc array.
 template <typename T>
 __global__ void k_load_rhs(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, double *const *__restrict__ su) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
@@ -662,6 +673,7 @@ __global__ void k_load_rhs(const BlkFld *__restrict__ fl, const Tile *__restrict
 // pp := level-1 phi including the first ghost layer (mgsolver.for:351-364).
 template <typename T>
 __global__ void k_store_pp(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, double *const *__restrict__ pp) {
+  pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
   const BlkLev &B = F.L1;

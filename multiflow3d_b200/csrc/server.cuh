@@ -152,9 +152,9 @@ static int srv_rebuild(mf3d_ctx *C, View &V, std::vector<SrvReq *> &res) {
   if (ncont < nd) {
     DevBuf<int> fmask;
     if ((st = fmask.upload(fresh, s))) return st;
-    k_face_planes<<<V.n_planes, kTile, 0, s>>>(V.df.p, V.t_planes.p);
+    launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p);
     calvel_calmas<T>(C, V, fmask.p, V.rmax.p, 0);
-    k_dom_init<<<1, 256, 0, s>>>(V.ds.p + ncont, nd - ncont, V.rmax.p + ncont, V.act.p + ncont);
+    launch(k_dom_init, 1, 256, 0, s, V.ds.p + ncont, nd - ncont, V.rmax.p + ncont, V.act.p + ncont);
     CK(cudaStreamSynchronize(s));  // fmask and the host vectors are locals
   } else {
     CK(cudaStreamSynchronize(s));
@@ -382,8 +382,8 @@ static void srv_loop(mf3d_server *S, int lane) {
     DevBuf<int> fmask;
     int st = fmask.upload(fin, s);
     if (!st) {
-      k_calvel<<<V.n_int, dim3(RW_TX, RW_RJ), 0, s>>>(V.df.p, V.t_int.p, V.ds.p, fmask.p);
-      k_vel_faces<<<V.n_vfaces, kTile, 0, s>>>(V.df.p, V.t_vfaces.p, fmask.p, C->prm.pl_ex);
+      launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, fmask.p);
+      launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, fmask.p, C->prm.pl_ex);
       if (cudaMemcpyAsync(hs.data(), V.ds.p, nd * sizeof(DomState), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
           cudaStreamSynchronize(s) != cudaSuccess)
         st = MF3D_E_CUDA;
