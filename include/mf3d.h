@@ -43,7 +43,7 @@ enum mf3d_status {
   MF3D_E_TIMEOUT = -4,    /* a bounded device wait gave up                  */
   MF3D_E_NONFINITE = -5,  /* NaN/Inf met in the residual                     */
   MF3D_E_UNSUPPORTED = -6 /* a reference feature outside this build (LMR,
-                             L_LSM variable density, differencing=3)       */
+                             differencing=2) or an unsupported combination */
 };
 
 /* Boundary-condition code meaning "periodic" (control.cin:17-22). Any other
@@ -97,6 +97,12 @@ typedef struct mf3d_params {
                        refreshes ghost layers 0..pl_ex of u, v, w
                        (exchange.for:16-20).  0 <= pl_ex < pl, and every block
                        edge must exceed pl_ex.                                */
+  int lsm;          /* L_LSM (control.cin): variable density.  coeff runs at
+                       every solve from mf3d_fields.dens (newsolv_mg.for:12-14,
+                       mgsolver.for:69-182), calvel divides by the face
+                       density (press.for:152-190) and the rhs is sup =
+                       div(u)*dx*dy*dz/dt (press.for:51-53).  FP64 only,
+                       uniform spacing, mf3d_create contexts only.            */
 } mf3d_params;
 
 /* Field pointers of one block, each a (ttc_i,ttc_j,ttc_k) array.
@@ -106,12 +112,15 @@ typedef struct mf3d_params {
  * tangential range on every face that is not a physical wall; ghost edges and
  * corners are left as given).  For the host
  * entry point these are host pointers; for the `_device` one, device pointers.
- * `su` may be NULL; if set it receives the final RHS div(u)/dt (calmas). */
+ * `su` may be NULL; if set it receives the final RHS div(u)/dt (calmas;
+ * sup under lsm).  `dens` (in, lsm only, else ignored): cell densities, ghost
+ * layers included - calvel reads the first ghost layer. */
 typedef struct mf3d_fields {
   double *ustar, *vstar, *wstar;
   double *u, *v, *w;
   double *p;
   double *su;
+  double *dens;
 } mf3d_fields;
 
 typedef struct mf3d_ctx mf3d_ctx;

@@ -84,6 +84,7 @@ class Params(C.Structure):
         ("precision", C.c_int),
         ("device", C.c_int),
         ("pl_ex", C.c_int),
+        ("lsm", C.c_int),
     ]
 
 
@@ -93,7 +94,7 @@ class Fields(C.Structure):
     _fields_ = [
         ("ustar", _dp), ("vstar", _dp), ("wstar", _dp),
         ("u", _dp), ("v", _dp), ("w", _dp),
-        ("p", _dp), ("su", _dp),
+        ("p", _dp), ("su", _dp), ("dens", _dp),
     ]
 
 

@@ -45,6 +45,8 @@ struct BlkLev {
   int nmask;          // Neumann faces: bit f set for f = W,E,S,N,B,T
   int dom;            // domain of the block
   const CUtensorMap *tm;  // TMA maps: phi colour 0, phi colour 1 (RB_RJ+2 rows), rhs colour 0, 1 (RB_RJ rows)
+  const void *cc;     // variable density (L_LSM): per-cell aw, ae, as, an, ab, at, six arrays of
+                      // the level's colour-split layout, array m at element m*2*cstr; else null
 };
 
 // compact row pitch: (nx+3)/2 entries rounded up to a multiple of 16 bytes
@@ -73,6 +75,20 @@ struct Coef {
     at = ab + (B.nz + 2);
   }
 };
+
+// The six coefficients of cell (i,j,k): per cell under L_LSM (the
+// reference's `cof`, mgsolver.for:120-203), else from the 1-D arrays.
+template <typename T>
+__device__ __forceinline__ void cell_coefs(const BlkLev &B, const Coef<T> &cf, int i, int j, int k, T &aw, T &ae,
+                                           T &as, T &an, T &ab, T &at) {
+  if (B.cc) {
+    const T *c = (const T *)B.cc;
+    const long long o = cell_off(B, i, j, k), m = 2 * B.cstr;
+    aw = c[o]; ae = c[o + m]; as = c[o + 2 * m]; an = c[o + 3 * m]; ab = c[o + 4 * m]; at = c[o + 5 * m];
+  } else {
+    aw = cf.aw[i]; ae = cf.ae[i]; as = cf.as[j]; an = cf.an[j]; ab = cf.ab[k]; at = cf.at[k];
+  }
+}
 
 // Programmatic dependent launch.  The host launches the kernels of a solve
 // with programmatic stream serialisation, so a kernel's CTAs may be resident
@@ -346,7 +362,8 @@ __global__ void __launch_bounds__(kTile) k_rbgs_small(const BlkLev *__restrict__
     bo = O[base - rs + h];
     to = O[base + rs + h];
   }
-  const T aw = cf.aw[i], ae = cf.ae[i], as = cf.as[j], an = cf.an[j], ab = cf.ab[k], at = cf.at[k];
+  T aw, ae, as, an, ab, at;
+  cell_coefs(B, cf, i, j, k, aw, ae, as, an, ab, at);
   const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
   M[base + h] = ((R[base + h] - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
 }
@@ -371,7 +388,8 @@ __global__ void k_lexgs(const BlkLev *__restrict__ bl, const int *__restrict__ b
       const int j = idx % ny + 1, k = idx / ny + 1;
       const int i = sum - j - k;
       if (i < 1 || i > nx) continue;
-      const T aw = cf.aw[i], ae = cf.ae[i], as = cf.as[j], an = cf.an[j], ab = cf.ab[k], at = cf.at[k];
+      T aw, ae, as, an, ab, at;
+      cell_coefs(B, cf, i, j, k, aw, ae, as, an, ab, at);
       const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
       const T w = P[cell_off(B, i - 1, j, k)], e = P[cell_off(B, i + 1, j, k)];
       const T so = P[cell_off(B, i, j - 1, k)], no = P[cell_off(B, i, j + 1, k)];
@@ -410,7 +428,8 @@ __device__ void tdma_line(const BlkLev &B, int dir, int u, int v, T *a, T *c) {
     if (dir == 0) { i = u; j = m; k = v; }
     else if (dir == 1) { i = m; j = u; k = v; }
     else { i = u; j = v; k = m; }
-    const T aw = cf.aw[i], ae = cf.ae[i], as = cf.as[j], an = cf.an[j], ab = cf.ab[k], at = cf.at[k];
+    T aw, ae, as, an, ab, at;
+    cell_coefs(B, cf, i, j, k, aw, ae, as, an, ab, at);
     const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
     const T su = R[off(m)];
     if (dir == 0) {
@@ -514,13 +533,15 @@ __global__ void __launch_bounds__(kTile, 2) k_restrict(const BlkLev *__restrict_
 #pragma unroll
         for (int di = 0; di < 2; ++di) {
           const int fi = 2 * I - 1 + di, fj = 2 * J - 1 + dj;
-          const TF ap = (TF)-1.0 * (aw[di] + ae[di] + as[dj] + an[dj] + ab + at);
+          TF cw = aw[di], ce = ae[di], cs_ = as[dj], cn = an[dj], cb = ab, ct = at;
+          if (Fb.cc) cell_coefs(Fb, cf, fi, fj, fk, cw, ce, cs_, cn, cb, ct);
+          const TF ap = (TF)-1.0 * (cw + ce + cs_ + cn + cb + ct);
           const TF pw = P[fo(fi - 1, fj, fk)], pe = P[fo(fi + 1, fj, fk)];
           const TF ps = P[fo(fi, fj - 1, fk)], pn = P[fo(fi, fj + 1, fk)];
           const TF pb = P[fo(fi, fj, fk - 1)], pt = P[fo(fi, fj, fk + 1)];
           const TF pp = P[fo(fi, fj, fk)];
           const TF r = R[fo(fi, fj, fk)];
-          const TF res = r - (aw[di] * pw + ae[di] * pe + as[dj] * ps + an[dj] * pn + ab * pb + at * pt + ap * pp);
+          const TF res = r - (cw * pw + ce * pe + cs_ * ps + cn * pn + cb * pb + ct * pt + ap * pp);
           const TF s = (TF)8.0 * sx[di] * sy[dj] * sz;
           const TF a = res * s;
           sum = (dk | dj | di) ? sum + a : a;
@@ -827,6 +848,65 @@ __global__ void k_zero_ghosts(const BlkLev *__restrict__ bl, const int *__restri
     else { r -= 2 * nxz; const int f = r / nxy; r -= f * nxy; k = f ? D - 1 : 0; i = r % W; j = r / W; }
     P[cell_off(B, i, j, k)] = (T)0;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Variable density (L_LSM): the coefficients `coeff` forms at the start of
+// every solve (newsolv_mg.for:12-14, mgsolver.for:69-203).  FP64 only.
+// ---------------------------------------------------------------------------
+// Cell densities of one level of one block: interior cell (i,j,k), 1-based,
+// at element off + i + sy*j + sz*k (the ttc field on level 1, an interior
+// array i fastest below it).
+struct DensView {
+  const double *p;
+  long long off, sy, sz;
+  __device__ double at(int i, int j, int k) const { return p[off + i + sy * j + sz * k]; }
+};
+
+// Level g > 1 densities, interior cells i fastest: 0.125 times the sum of
+// the 8 children of level g-1 in the reference's order - (j), (j+1), (i+1),
+// (i+1, j+1), then the same one plane up - summed left to right
+// (mgsolver.for:84-113).  One thread per coarse cell.
+__global__ void k_lsm_coarsen(DensView fine, double *__restrict__ coarse, int nx, int ny, int nz) {
+  pdl_wait();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * ny * nz) return;
+  const int i = (int)(t % nx) + 1, j = (int)((t / nx) % ny) + 1, k = (int)(t / ((long long)nx * ny)) + 1;
+  const int fi = 2 * i - 1, fj = 2 * j - 1, fk = 2 * k - 1;
+  const double sum = fine.at(fi, fj, fk) + fine.at(fi, fj + 1, fk) + fine.at(fi + 1, fj, fk) +
+                     fine.at(fi + 1, fj + 1, fk) + fine.at(fi, fj, fk + 1) + fine.at(fi, fj + 1, fk + 1) +
+                     fine.at(fi + 1, fj, fk + 1) + fine.at(fi + 1, fj + 1, fk + 1);
+  coarse[t] = 0.125 * sum;
+}
+
+// Per-cell coefficients of one level of one block (mgsolver.for:120-203):
+// face densities from the block's own cells (a boundary cell uses its own
+// density), aw = ((dy*dz)/dx)/densim12 and so on with the block's fine
+// spacings on every level (cx, cy, cz formed on the host in that order),
+// Neumann faces zeroed.  Written to B.cc; one thread per interior cell.
+__global__ void k_lsm_coef(BlkLev B, DensView d, double cx, double cy, double cz) {
+  pdl_wait();
+  const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)nx * ny * nz) return;
+  const int i = (int)(t % nx) + 1, j = (int)((t / nx) % ny) + 1, k = (int)(t / ((long long)nx * ny)) + 1;
+  const double dc = d.at(i, j, k);
+  const double densim12 = i == 1 ? dc : 0.5 * (dc + d.at(i - 1, j, k));
+  const double densip12 = i == nx ? dc : 0.5 * (dc + d.at(i + 1, j, k));
+  const double densjm12 = j == 1 ? dc : 0.5 * (dc + d.at(i, j - 1, k));
+  const double densjp12 = j == ny ? dc : 0.5 * (dc + d.at(i, j + 1, k));
+  const double denskm12 = k == 1 ? dc : 0.5 * (dc + d.at(i, j, k - 1));
+  const double denskp12 = k == nz ? dc : 0.5 * (dc + d.at(i, j, k + 1));
+  double c[6] = {cx / densim12, cx / densip12, cy / densjm12, cy / densjp12, cz / denskm12, cz / denskp12};
+  if ((B.nmask & 1) && i == 1) c[0] = 0.0;
+  if ((B.nmask & 2) && i == nx) c[1] = 0.0;
+  if ((B.nmask & 4) && j == 1) c[2] = 0.0;
+  if ((B.nmask & 8) && j == ny) c[3] = 0.0;
+  if ((B.nmask & 16) && k == 1) c[4] = 0.0;
+  if ((B.nmask & 32) && k == nz) c[5] = 0.0;
+  double *out = (double *)B.cc;
+  const long long o = cell_off(B, i, j, k), m = 2 * B.cstr;
+  for (int q = 0; q < 6; ++q) out[o + q * m] = c[q];
 }
 
 }  // namespace mf3d

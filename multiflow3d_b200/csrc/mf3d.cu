@@ -232,6 +232,8 @@ struct LevelStore {
   std::vector<std::vector<char>> host;  // host images of the uploaded small arrays
   DevBuf<char> phi, rhs, coef, geo;
   DevBuf<CUtensorMap> tmaps;  // phi c0, phi c1, rhs c0, rhs c1
+  DevBuf<double> cc;          // L_LSM: per-cell coefficients (six colour-split arrays)
+  DevBuf<double> dens;        // L_LSM, levels > 1: cell densities, interior, i fastest
   BlkLev desc;  // host copy with device pointers
 };
 
@@ -286,7 +288,8 @@ struct BlockStore {
   int elem = 8;          // bytes per multigrid value (8 FP64, 4 FP32)
   std::vector<LevelStore> lv;  // [1..ngrid]
   DevBuf<double> geo1;   // level-1 widths h[3] (n+2) and face distances df[3] (n+1)
-  DevBuf<double> planes; // face planes lo/hi of u, v, w
+  DevBuf<double> planes; // face planes lo/hi of u, v, w (and the L_LSM face densities)
+  bool lsm = false;      // variable-density coefficients, formed per solve
   BlkFld fld;            // host template (field pointers bound per call)
   size_t bytes = 0;      // device bytes owned
 };
@@ -294,9 +297,10 @@ struct BlockStore {
 // Build one block's hierarchy: replaces `coeff` (mgsolver.for:2-222) and the
 // `cof` sizing of localparameters.for:208-237.
 static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int elem_fine, int elem_coarsest, int pl,
-                       cudaStream_t s) {
+                       bool lsm, cudaStream_t s) {
   const int elem = elem_fine;
   S.d = d;
+  S.lsm = lsm;
   S.ngrid = ngrid;
   S.elem = elem;
   S.lv.clear();
@@ -391,6 +395,16 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
     std::memcpy(L.host.back().data(), tm, sizeof tm);
     CK(cudaMemcpyAsync(L.tmaps.p, L.host.back().data(), sizeof tm, cudaMemcpyHostToDevice, s));
     B.tm = L.tmaps.p;
+    if (lsm) {  // FP64 only: formed by k_lsm_coef at every solve
+      if ((st = L.cc.alloc((size_t)12 * B.cstr))) return st;
+      CK(cudaMemsetAsync(L.cc.p, 0, L.cc.n * sizeof(double), s));
+      B.cc = L.cc.p;
+      S.bytes += L.cc.n * sizeof(double);
+      if (g > 1) {
+        if ((st = L.dens.alloc((size_t)B.nx * B.ny * B.nz))) return st;
+        S.bytes += L.dens.n * sizeof(double);
+      }
+    }
   }
   // level-1 field geometry: widths, face distances (bit-exact dx on a uniform axis)
   std::vector<double> g1;
@@ -408,7 +422,7 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
   }
   if ((st = S.geo1.upload(g1, s))) return st;
   const size_t pyz = (size_t)d.ny * d.nz, pxz = (size_t)d.nx * d.nz, pxy = (size_t)d.nx * d.ny;
-  if ((st = S.planes.alloc(2 * (pyz + pxz + pxy)))) return st;
+  if ((st = S.planes.alloc(3 * (pyz + pxz + pxy)))) return st;
   CK(cudaMemsetAsync(S.planes.p, 0, S.planes.n * sizeof(double), s));
   CK(cudaStreamSynchronize(s));  // g1 is a local
   S.bytes += (S.geo1.n + S.planes.n) * sizeof(double);
@@ -425,7 +439,8 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
   double *pp = S.planes.p;
   F.lo[0] = pp; F.hi[0] = pp + pyz; pp += 2 * pyz;
   F.lo[1] = pp; F.hi[1] = pp + pxz; pp += 2 * pxz;
-  F.lo[2] = pp; F.hi[2] = pp + pxy;
+  F.lo[2] = pp; F.hi[2] = pp + pxy; pp += 2 * pxy;
+  F.dlo[0] = pp; F.dlo[1] = pp + pyz; F.dlo[2] = pp + pyz + pxz;
   F.L1 = S.lv[1].desc;
   for (int a = 0; a < 3; ++a) F.pinv[a] = ext[a] ? 0.0 : pow2_inverse(hh[a]);
   return MF3D_OK;
@@ -453,7 +468,7 @@ static long long level_off(const BlkLev &B, int i, int j, int k) {
 }
 
 static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, int ngrid, int elem, int elem_coarsest,
-                        int pl, cudaStream_t s) {
+                        int pl, cudaStream_t s, bool lsm = false) {
   D.ngrid = ngrid;
   D.blocks.clear();
   std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
@@ -462,7 +477,7 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
   D.bytes = 0;
   for (int b = 0; b < nb; ++b) {
     D.blocks.emplace_back(new BlockStore());
-    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, elem_coarsest, pl, s))) return st;
+    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, elem_coarsest, pl, lsm, s))) return st;
     D.bytes += D.blocks.back()->bytes;
   }
   D.halo.assign(ngrid + 1, {});
@@ -784,7 +799,8 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
     // level 1 always takes the pipelined sweep; MF3D_SMALL_LEVEL_CELLS overrides the limit
     long long small_limit = kSmallLevelCells;
     if (const char *e = std::getenv("MF3D_SMALL_LEVEL_CELLS")) small_limit = std::atoll(e);
-    L.small = g > 1 && L.cells_sub[SUB_A] <= small_limit;
+    // under L_LSM every level sweeps with the plain-load kernel (per-cell coefficients)
+    L.small = C->prm.lsm || (g > 1 && L.cells_sub[SUB_A] <= small_limit);
     for (int q = 0; q < 3; ++q) {
       std::vector<int> pre(1, 0);
       for (int b : li[q]) {
@@ -971,7 +987,7 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
   if (!Cl.n_rtile) return;
   const int pk = g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse out
-  if (C->prm.mg_itrsch == 3 && C->prm.irestr > 0 && Cl.n_rtma) {
+  if (C->prm.mg_itrsch == 3 && C->prm.irestr > 0 && Cl.n_rtma && !C->prm.lsm) {
     // red-black from zero: the coarse interior phi is never read before it
     // is written, so only its ghost shell is zeroed
     static const bool attr_set = [] {
@@ -1048,7 +1064,10 @@ static void vcycle(mf3d_ctx *C, View &V) {
 // fields admit it).
 template <typename T>
 static void calvel_calmas(mf3d_ctx *C, View &V, const int *act, unsigned long long *slot, int write_su) {
-  if (V.fields_tma) {
+  if (C->prm.lsm) {
+    launch(k_calvel_calmas_lsm, V.n_zint, dim3(OZ_TX, OZ_RJ), 0, C->stream, V.df.p, V.t_zint.p, V.ds.p, act, slot,
+           write_su);
+  } else if (V.fields_tma) {
     // axes that are uniform with a power-of-two spacing in every block
     int mask = 7;
     for (const auto &F : V.hf)
@@ -1147,7 +1166,8 @@ static int bind_fields(mf3d_ctx *C, View &V, const mf3d_fields *f) {
     BlkFld &F = V.hf[b];
     F.ustar = f[b].ustar; F.vstar = f[b].vstar; F.wstar = f[b].wstar;
     F.u = f[b].u; F.v = f[b].v; F.w = f[b].w; F.p = f[b].p; F.su = f[b].su;
-    if (!F.ustar || !F.vstar || !F.wstar || !F.u || !F.v || !F.w || !F.p) {
+    F.dens = C->prm.lsm ? f[b].dens : nullptr;
+    if (!F.ustar || !F.vstar || !F.wstar || !F.u || !F.v || !F.w || !F.p || (C->prm.lsm && !F.dens)) {
       set_error("mf3d_fields: a required pointer is NULL");
       return MF3D_E_INVALID;
     }
@@ -1189,6 +1209,32 @@ static int bind_fields(mf3d_ctx *C, View &V, const mf3d_fields *f) {
   return MF3D_OK;
 }
 
+// L_LSM: `coeff` at the start of every solve (newsolv_mg.for:12-14): the
+// level densities from the bound dens field, then every level's per-cell
+// coefficients (mgsolver.for:69-203).
+static void lsm_coefficients(mf3d_ctx *C, View &V) {
+  cudaStream_t s = C->stream;
+  for (size_t b = 0; b < V.blk.size(); ++b) {
+    const BlockStore &S = *V.blk[b];
+    const BlkFld &F = V.hf[b];
+    const double cx = S.d.dy * S.d.dz / S.d.dx, cy = S.d.dx * S.d.dz / S.d.dy, cz = S.d.dx * S.d.dy / S.d.dz;
+    const long long ps = (long long)F.ti * F.tj;
+    DensView d{F.dens, (long long)(F.pl - 1) * (1 + F.ti + ps), F.ti, ps};
+    for (int g = 1; g <= S.ngrid; ++g) {
+      const BlkLev &B = S.lv[g].desc;
+      const long long n = (long long)B.nx * B.ny * B.nz;
+      if (g > 1) {
+        launch(k_lsm_coarsen, grid_of(n, 256), 256, 0, s, d, S.lv[g].dens.p, B.nx, B.ny, B.nz);
+        const long long sy = B.nx, sz = (long long)B.nx * B.ny;
+        d = DensView{S.lv[g].dens.p, -(1 + sy + sz), sy, sz};
+        ++C->launches;
+      }
+      launch(k_lsm_coef, grid_of(n, 256), 256, 0, s, B, d, cx, cy, cz);
+      ++C->launches;
+    }
+  }
+}
+
 // Start the solve of every domain of the view: state, face planes, the
 // initial calvel/calmas (newsolv_mg.for:16-17; p's ghosts used as given),
 // rmax0 and the thresholds.  Everything stays on the device.
@@ -1210,6 +1256,7 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
   CK(cudaMemcpyAsync(V.ds.p, hs.data(), nd * sizeof(DomState), cudaMemcpyHostToDevice, s));
   CK(cudaStreamSynchronize(s));  // hs is a local
   CK(cudaMemsetAsync(V.rmax.p, 0, nd * sizeof(unsigned long long), s));
+  if (C->prm.lsm) lsm_coefficients(C, V);
   launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p);
   calvel_calmas<T>(C, V, V.ones.p, V.rmax.p, 0);
   launch(k_dom_init, 1, 256, 0, s, V.ds.p, nd, V.rmax.p, V.act.p);
@@ -1410,6 +1457,7 @@ static int check_params(const mf3d_params *prm) {
   if (prm->pl_ex < 0 || prm->pl_ex >= prm->pl) { set_error("pl_ex must satisfy 0 <= pl_ex < pl"); return MF3D_E_INVALID; }
   if (prm->differencing != 1) { set_error("differencing != 1 (4th-order calmas) is not supported"); return MF3D_E_UNSUPPORTED; }
   if (prm->precision < 0 || prm->precision > 1) { set_error("precision mode not supported"); return MF3D_E_UNSUPPORTED; }
+  if (prm->lsm && prm->precision != MF3D_PREC_FP64) { set_error("lsm runs in FP64 only"); return MF3D_E_UNSUPPORTED; }
   return MF3D_OK;
 }
 
@@ -1461,6 +1509,10 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
       set_error("block " + std::to_string(d.id) + ": an edge does not exceed pl_ex");
       return MF3D_E_INVALID;
     }
+    if (prm->lsm && (d.hx || d.hy || d.hz)) {
+      set_error("lsm: uniform spacing only (the reference's variable-density branch)");
+      return MF3D_E_UNSUPPORTED;
+    }
   }
   {
     std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
@@ -1473,7 +1525,7 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   C->doms.emplace_back(new DomainStore());
   C->coarse64 = C->elem == 4 && prm->ngrid > 1;
   if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, C->coarse64 ? 8 : C->elem, prm->pl,
-                         C->stream)))
+                         C->stream, prm->lsm != 0)))
     return st;
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
@@ -1533,6 +1585,7 @@ static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params 
   if (!doms || nd <= 0 || !out) { set_error("mf3d_batch_create: bad arguments"); return MF3D_E_INVALID; }
   int st = check_params(prm);
   if (st) return st;
+  if (prm->lsm) { set_error("lsm: single-problem contexts (mf3d_create) only"); return MF3D_E_UNSUPPORTED; }
   for (int d = 0; d < nd; ++d) {
     if (domain_ngrid(doms[d]) < 1) {
       set_error("domain " + std::to_string(d) + ": sizes not divisible by 2^(ngrid-1)");
@@ -1579,7 +1632,8 @@ static int host_solve(mf3d_ctx *C, const mf3d_fields *fields, const double *dt, 
   if (!C->mirror.p) {
     size_t tot = 0;
     C->mirror_off.resize(nb);
-    for (int b = 0; b < nb; ++b) { C->mirror_off[b] = tot; tot += 8 * ttc_elems(pl, V.blk[b]->d); }
+    const size_t arrays = C->prm.lsm ? 9 : 8;  // + dens under L_LSM
+    for (int b = 0; b < nb; ++b) { C->mirror_off[b] = tot; tot += arrays * ttc_elems(pl, V.blk[b]->d); }
     int st = C->mirror.alloc(tot);
     if (st) return st;
   }
@@ -1593,7 +1647,12 @@ static int host_solve(mf3d_ctx *C, const mf3d_fields *fields, const double *dt, 
       CK(cudaMemcpyAsync(m + q * n, hsrc[q], n * sizeof(double), cudaMemcpyHostToDevice, s));
     }
     dev[b] = mf3d_fields{m, m + n, m + 2 * n, m + 3 * n, m + 4 * n, m + 5 * n, m + 6 * n,
-                         fields[b].su ? m + 7 * n : nullptr};
+                         fields[b].su ? m + 7 * n : nullptr, nullptr};
+    if (C->prm.lsm) {
+      if (!fields[b].dens) { set_error("mf3d_fields: dens is NULL under lsm"); return MF3D_E_INVALID; }
+      CK(cudaMemcpyAsync(m + 8 * n, fields[b].dens, n * sizeof(double), cudaMemcpyHostToDevice, s));
+      dev[b].dens = m + 8 * n;
+    }
   }
   int st = bind_fields(C, V, dev.data());
   if (st) return st;
@@ -1709,6 +1768,7 @@ int mf3d_batch_solve_device(mf3d_ctx *C, const mf3d_fields *fields, const double
 
 int mf3d_mgkcyc_device(mf3d_ctx *C, double *const *su, double *const *pp) {
   if (!C || !su || !pp) { mf3d::set_error("mf3d_mgkcyc_device: bad arguments"); return MF3D_E_INVALID; }
+  if (C->prm.lsm) { mf3d::set_error("lsm: the coefficients come from a solve's dens"); return MF3D_E_UNSUPPORTED; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   mf3d::AllocScope scope(C->stream);
   if (C->elem == 8) return mf3d::mgkcyc_view<double>(C, *C->view, su, pp);
@@ -1717,6 +1777,7 @@ int mf3d_mgkcyc_device(mf3d_ctx *C, double *const *su, double *const *pp) {
 
 int mf3d_mgkcyc_device_noalloc(mf3d_ctx *C, double *const *su, double *const *pp) {
   if (!C || !su || !pp) { mf3d::set_error("mf3d_mgkcyc_device_noalloc: bad arguments"); return MF3D_E_INVALID; }
+  if (C->prm.lsm) { mf3d::set_error("lsm: the coefficients come from a solve's dens"); return MF3D_E_UNSUPPORTED; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   if (C->elem == 8) return mf3d::mgkcyc_view_noalloc<double>(C, *C->view, su, pp);
   return mf3d::mgkcyc_view_noalloc<float>(C, *C->view, su, pp);

@@ -40,6 +40,9 @@ struct BlkFld {
   double pinv[3];                    // 1/h when the axis is uniform with h a power of two, else 0
   const CUtensorMap *fm;             // TMA maps of p, ustar, vstar, wstar (CvShape boxes), or null
   const double *rh[3], *rdf[3];      // RN(1/h), RN(1/df) for div_rcp (0: divide)
+  const double *dens;                // L_LSM: cell densities (ttc layout), else null
+  double *dlo[3];                    // L_LSM: face density 0.5*(d(n)+d(n+1)) of the source block
+                                     // at a non-wall low face (k_face_planes)
 };
 
 // x / h.  When h is a power of two the multiplication by its reciprocal
@@ -265,6 +268,10 @@ __global__ void k_face_planes(const BlkFld *__restrict__ fl, const Tile *__restr
     const double *st = ax == 0 ? S.ustar : ax == 1 ? S.vstar : S.wstar;
     long long e = ax == 0 ? fidx(S, S.nx, a, b) : ax == 1 ? fidx(S, a, S.ny, b) : fidx(S, a, b, S.nz);
     F.lo[ax][o] = st[e];
+    if (F.dens) {  // the density calvel divides by on that face, in the source block (press.for:152-190)
+      const long long s1 = ax == 0 ? 1 : ax == 1 ? (long long)S.ti : (long long)S.ti * S.tj;
+      F.dlo[ax][o] = 0.5 * (S.dens[e] + S.dens[e + s1]);
+    }
   }
   // high face
   long long e = ax == 0 ? fidx(F, nx, a, b) : ax == 1 ? fidx(F, a, ny, b) : fidx(F, a, b, nz);
@@ -372,6 +379,92 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas(const BlkFld *__
     vmax = vmax > f1 ? vmax : f1;
   }
   // CTA max: warp shuffles, shared memory, one atomic per CTA
+  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  if (threadIdx.x == 0) red[threadIdx.y] = vmax;
+  __syncthreads();
+  if (threadIdx.y == 0) {
+    double v = threadIdx.x < OZ_RJ ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0 && v > 0.0) atomic_max_nonneg(rmax_slot + F.dom, v);
+  }
+}
+
+// Fused calvel + calmas under L_LSM (variable density; uniform spacing):
+// every face velocity divides by its face density last,
+//   u(i) = ustar(i) - ((dt*alfapr*(p(i+1)-p(i)))/dx)/(0.5*(dens(i)+dens(i+1)))
+// (press.for:152-190), and the level-1 rhs is sup = fact*dx*dy*dz/dt
+// (press.for:51-53, copied by mgkcyc at mgsolver.for:256-261).  A block
+// face that is not a wall takes the source block's ustar and face density
+// (k_face_planes).  One thread per (i, j) column, marching up OZ_KCH planes;
+// each face velocity is formed from the same operands by both cells that
+// share it.  rmax as in k_calvel_calmas.
+__global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_lsm(const BlkFld *__restrict__ fl,
+                                                                   const Tile *__restrict__ tiles,
+                                                                   const DomState *__restrict__ ds,
+                                                                   const int *__restrict__ act,
+                                                                   unsigned long long *__restrict__ rmax_slot,
+                                                                   int write_su) {
+  pdl_wait();
+  __shared__ double red[OZ_RJ];
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  if (!act[F.dom]) return;
+  const double dt = ds[F.dom].dt, alfapr = ds[F.dom].alfapr;
+  const double dta = dt * alfapr;
+  double *__restrict__ rhs1 = rhs_of<double>(F.L1);
+  double *__restrict__ SU = write_su ? F.su : nullptr;
+  const int nx = F.nx, ny = F.ny, nz = F.nz;
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  const bool in = i <= nx && j <= ny;
+  const int ic = in ? i : 1, jc = in ? j : 1;
+  const long long sy = F.ti, sz = (long long)F.ti * F.tj;
+  const double *__restrict__ p = F.p;
+  const double *__restrict__ D = F.dens;
+  const double ix = F.pinv[0], iy = F.pinv[1], iz = F.pinv[2];
+  const double hx = F.h[0][ic], hy = F.h[1][jc];
+  const double dx = F.df[0][ic], dy = F.df[1][jc];
+  const bool ewall = F.wall[1], nwall = F.wall[3], twall = F.wall[5];
+  const bool wwall = F.wall[0], swall = F.wall[2], bwall = F.wall[4];
+  const int k1 = min(t.k0 + OZ_KCH - 1, nz);
+  double vmax = 0.0;
+  for (int k = t.k0; k <= k1; ++k) {
+    const long long c = fidx(F, ic, jc, k);
+    const double pc = p[c], dc = D[c];
+    const double dz = F.df[2][k], hz = F.h[2][k];
+    double ue, uw, vn, vs, wt, wb;
+    if (ic == nx && ewall) ue = F.hi[0][(k - 1) * ny + (jc - 1)];
+    else ue = (F.ustar[c] - xdiv(dta * (p[c + 1] - pc), dx, ix) / (0.5 * (dc + D[c + 1])));
+    if (ic == 1) {
+      const int o = (k - 1) * ny + (jc - 1);
+      uw = wwall ? F.lo[0][o] : (F.lo[0][o] - xdiv(dta * (pc - p[c - 1]), dx, ix) / F.dlo[0][o]);
+    } else {
+      uw = (F.ustar[c - 1] - xdiv(dta * (pc - p[c - 1]), dx, ix) / (0.5 * (D[c - 1] + dc)));
+    }
+    if (jc == ny && nwall) vn = F.hi[1][(k - 1) * nx + (ic - 1)];
+    else vn = (F.vstar[c] - xdiv(dta * (p[c + sy] - pc), dy, iy) / (0.5 * (dc + D[c + sy])));
+    if (jc == 1) {
+      const int o = (k - 1) * nx + (ic - 1);
+      vs = swall ? F.lo[1][o] : (F.lo[1][o] - xdiv(dta * (pc - p[c - sy]), dy, iy) / F.dlo[1][o]);
+    } else {
+      vs = (F.vstar[c - sy] - xdiv(dta * (pc - p[c - sy]), dy, iy) / (0.5 * (D[c - sy] + dc)));
+    }
+    if (k == nz && twall) wt = F.hi[2][(jc - 1) * nx + (ic - 1)];
+    else wt = (F.wstar[c] - xdiv(dta * (p[c + sz] - pc), dz, iz) / (0.5 * (dc + D[c + sz])));
+    if (k == 1) {
+      const int o = (jc - 1) * nx + (ic - 1);
+      wb = bwall ? F.lo[2][o] : (F.lo[2][o] - xdiv(dta * (pc - p[c - sz]), dz, iz) / F.dlo[2][o]);
+    } else {
+      wb = (F.wstar[c - sz] - xdiv(dta * (pc - p[c - sz]), dz, iz) / (0.5 * (D[c - sz] + dc)));
+    }
+    const double fact = (xdiv(ue - uw, hx, ix) + xdiv(vn - vs, hy, iy) + xdiv(wt - wb, hz, iz));
+    if (!in) continue;
+    const double sup = fact * hx * hy * hz / dt;
+    rhs1[cell_off(F.L1, i, j, k)] = sup;
+    if (SU) SU[c] = sup;
+    double f1 = fabs(fact * hx * hy * hz);
+    if (!(f1 == f1)) f1 = __longlong_as_double(0x7ff0000000000000LL);  // NaN -> +Inf (flagged)
+    vmax = vmax > f1 ? vmax : f1;
+  }
   for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
   if (threadIdx.x == 0) red[threadIdx.y] = vmax;
   __syncthreads();
@@ -590,8 +683,18 @@ __global__ void __launch_bounds__(RW_TX *RW_RJ) k_calvel(const BlkFld *__restric
   const long long sy = F.ti, sz = (long long)F.ti * F.tj;
   const double *__restrict__ p = F.p;
   const int k1 = min(t.k0 + RW_KCH - 1, F.nz);
+  const double *__restrict__ D = F.dens;
   for (int k = t.k0; k <= k1; ++k) {
     const long long c = fidx(F, i, j, k);
+    if (D) {  // L_LSM (press.for:152-190): the face density divides last
+      if (!(i == nx && F.wall[1]))
+        F.u[c] = (F.ustar[c] - xdiv(dta * (p[c + 1] - p[c]), F.df[0][i], F.pinv[0]) / (0.5 * (D[c] + D[c + 1])));
+      if (!(j == ny && F.wall[3]))
+        F.v[c] = (F.vstar[c] - xdiv(dta * (p[c + sy] - p[c]), F.df[1][j], F.pinv[1]) / (0.5 * (D[c] + D[c + sy])));
+      if (!(k == F.nz && F.wall[5]))
+        F.w[c] = (F.wstar[c] - xdiv(dta * (p[c + sz] - p[c]), F.df[2][k], F.pinv[2]) / (0.5 * (D[c] + D[c + sz])));
+      continue;
+    }
     if (!(i == nx && F.wall[1])) F.u[c] = (F.ustar[c] - xdiv(dta * (p[c + 1] - p[c]), F.df[0][i], F.pinv[0]));
     if (!(j == ny && F.wall[3])) F.v[c] = (F.vstar[c] - xdiv(dta * (p[c + sy] - p[c]), F.df[1][j], F.pinv[1]));
     if (!(k == F.nz && F.wall[5])) F.w[c] = (F.wstar[c] - xdiv(dta * (p[c + sz] - p[c]), F.df[2][k], F.pinv[2]));

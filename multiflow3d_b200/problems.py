@@ -138,11 +138,30 @@ class Problem:
         return arr
 
     def params(self, mg_itrsch=3, irestr=2, iproln=1, maxcy=200, eps=1e-8,
-               eps_relative=1, precision=MF3D_PREC_FP64, device=0, pl_ex=0) -> Params:
+               eps_relative=1, precision=MF3D_PREC_FP64, device=0, pl_ex=0, lsm=0) -> Params:
         return Params(ngrid=self.ngrid, mg_itrsch=mg_itrsch, irestr=irestr,
                       iproln=iproln, maxcy=maxcy, eps=eps, eps_relative=eps_relative,
                       pl=self.pl, differencing=1, precision=precision, device=device,
-                      pl_ex=pl_ex)
+                      pl_ex=pl_ex, lsm=lsm)
+
+    def block_density(self, seed: int, lo: float = 0.5, hi: float = 2.0, const: float | None = None):
+        """Per-block cell densities (ttc layout) cut from one global field:
+        i.i.d. uniform in [lo, hi] (or ``const`` everywhere), ghost layers
+        wrapped on periodic axes, so every block sees its neighbours' cells."""
+        pl = self.pl
+        shp = (self.NZ + 2 * pl, self.NY + 2 * pl, self.NX + 2 * pl)
+        if const is not None:
+            g = np.full(shp, float(const))
+        else:
+            g = self.wrap_periodic(np.random.default_rng(seed).uniform(lo, hi, size=shp))
+        out = []
+        for b in range(self.nblocks):
+            bx, by, bz = self.block_pos(b)
+            sl = (slice(bz * self.nz, bz * self.nz + self.nz + 2 * pl),
+                  slice(by * self.ny, by * self.ny + self.ny + 2 * pl),
+                  slice(bx * self.nx, bx * self.nx + self.nx + 2 * pl))
+            out.append(np.ascontiguousarray(g[sl]))
+        return out
 
     # ------------------------------------------------------------------
     # seeded inputs
@@ -244,8 +263,10 @@ def fields_struct(blocks) -> "C.Array":
     arr = (Fields * len(blocks))()
     dp = C.POINTER(C.c_double)
     for b, f in enumerate(blocks):
-        for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p", "su"):
-            a = f[k]
+        for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p", "su", "dens"):
+            a = f.get(k)
+            if a is None and k == "dens":
+                continue
             assert a.dtype == np.float64 and a.flags.c_contiguous
             setattr(arr[b], k, a.ctypes.data_as(dp))
     return arr

@@ -76,7 +76,7 @@ class Projection:
         """Device arrays (torch float64 CUDA tensors, ttc layout) per block."""
         arr = (abi.Fields * len(blocks))()
         for b, f in enumerate(blocks):
-            for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p", "su"):
+            for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p", "su", "dens"):
                 t = f.get(k)
                 setattr(arr[b], k, C.cast(C.c_void_p(t.data_ptr()), _dp) if t is not None else None)
         return self._run(self.lib.mf3d_newsolv_mg_device, arr, dt, alfapr)

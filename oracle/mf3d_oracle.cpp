@@ -22,7 +22,8 @@
  *     i fastest, pl ghost layers (initial.for:196-210).
  * Only the same-level branches (rdiv = 1 everywhere, single MPI rank owning
  * every block, the `dom_ad(a) .eq. dom_ad(b)` direct-buffer path) are
- * restated; the LMR 2:1 branches and L_LSM are not on this path.
+ * restated, with the L_LSM variable-density branches of coeff, calvel and
+ * calmas; the LMR 2:1 branches are not.
  *
  * Extension with no reference counterpart (marked EXT): non-uniform cell
  * widths.  With uniform widths every EXT formula reduces bit-for-bit to the
@@ -55,7 +56,9 @@ struct Blk {
   std::vector<long> faz;       /* faz[1..ngrd_gl] */
   std::vector<double> cof;     /* 1-based: cof[1..nwork] */
   double *ustar, *vstar, *wstar, *u, *v, *w, *p;
-  std::vector<double> su, pp;
+  double *dens = nullptr;      /* L_LSM: cell densities (ttc layout) */
+  std::vector<std::vector<double>> dens_mg; /* L_LSM: per level, interior cells, j fastest */
+  std::vector<double> su, pp;  /* su holds sup under L_LSM (mgsolver.for:256-261) */
   /* same-rank receive buffers of exchangepp / exchbc_mgpp (1-based) */
   std::vector<double> recvb_m1, recvb_p1;
   double rcm[5], rcp[5];
@@ -90,6 +93,7 @@ struct Ctx {
   std::vector<Blk> b;
   std::map<int, int> indid; /* dom_indid: block id -> position */
   int ngrd_gl, mg_itrsch, irestr, iproln, maxcy, pl, pl_ex;
+  bool lsm; /* L_LSM: variable-density coefficients, calvel and rhs */
   double eps;
   int eps_relative;
   bool periodic;
@@ -130,10 +134,42 @@ std::vector<std::vector<double>> level_widths(const double *ext, int n, double h
 }
 
 /* ------------------------------------------------------------------ */
-/* coeff (mgsolver.for:2-222), uniform branch + EXT widths.           */
+/* coeff (mgsolver.for:2-222), uniform and L_LSM branches + EXT widths. */
 /* ------------------------------------------------------------------ */
+/* L_LSM cell densities of level g, interior cells, reference layout
+ * (j fastest, then i, then k; mgsolver.for:69-116): level 1 copies dens,
+ * level g averages the 8 children of level g-1 in the reference's order
+ * (j, j+1, i+1, i+1 j+1, then the same one plane up). */
+void lsm_density(Blk &B, int ngrd, int pl) {
+  int nx = B.iep - B.isp + 1, ny = B.jep - B.jsp + 1, nz = B.kep - B.ksp + 1;
+  B.dens_mg.assign(ngrd + 1, {});
+  for (int g = 1; g <= ngrd; ++g) {
+    int gl = g > B.ngrid ? B.ngrid : g;
+    int mi = level_n(nx, gl) - 2, mj = level_n(ny, gl) - 2, mk = level_n(nz, gl) - 2;
+    std::vector<double> &d = B.dens_mg[g];
+    d.assign((size_t)mi * mj * mk, 0.0);
+    for (int k = 2; k <= mk + 1; ++k)
+      for (int i = 2; i <= mi + 1; ++i)
+        for (int j = 2; j <= mj + 1; ++j) {
+          long q = (long)(k - 2) * mi * mj + (long)(i - 2) * mj + (j - 2);
+          if (g == 1) {
+            d[q] = F(B, B.dens, i + pl - 1, j + pl - 1, k + pl - 1);
+          } else {
+            const std::vector<double> &f = B.dens_mg[g - 1];
+            int pi = 2 * mi, pj = 2 * mj;
+            long ij1 = (long)(2 * k - 4) * pi * pj + (long)(2 * i - 4) * pj + (2 * j - 4);
+            long ij2 = ij1 + 1, ij3 = ij1 + pj, ij4 = ij1 + pj + 1;
+            long ij5 = ij1 + (long)pi * pj, ij6 = ij5 + 1, ij7 = ij5 + pj, ij8 = ij5 + pj + 1;
+            d[q] = 0.125 * (f[ij1] + f[ij2] + f[ij3] + f[ij4] + f[ij5] + f[ij6] + f[ij7] + f[ij8]);
+          }
+        }
+  }
+}
+
 void coeff(Ctx &C) {
   for (auto &B : C.b) {
+    const bool lsm = C.lsm && B.dens;
+    if (lsm) lsm_density(B, C.ngrd_gl, C.pl);
     int nx = B.iep - B.isp + 1, ny = B.jep - B.jsp + 1, nz = B.kep - B.ksp + 1;
     B.faz.assign(C.ngrd_gl + 1, 0);
     B.faz[1] = (long)(nx + 2) * (ny + 2) * (nz + 2);
@@ -169,7 +205,27 @@ void coeff(Ctx &C) {
           for (int j = 2; j <= mj - 1; ++j) {
             long ijk = B.faz[g] + (long)(k - 2) * (mi - 2) * (mj - 2) + (long)(i - 2) * (mj - 2) + (j - 1);
             double aw, ae, as, an, ab, at;
-            if (!B.stretched) {
+            if (lsm) {
+              /* mgsolver.for:120-182: face densities within the block (a
+               * boundary cell uses its own), coefficients scaled by the
+               * block's fine spacings on every level */
+              const std::vector<double> &d = B.dens_mg[g];
+              long mi2 = mi - 2, mj2 = mj - 2;
+              long q = (long)(k - 2) * mi2 * mj2 + (long)(i - 2) * mj2 + (j - 2);
+              double dc = d[q];
+              double densim12 = i == 2 ? dc : 0.5 * (dc + d[q - mj2]);
+              double densip12 = i == mi - 1 ? dc : 0.5 * (dc + d[q + mj2]);
+              double densjm12 = j == 2 ? dc : 0.5 * (dc + d[q - 1]);
+              double densjp12 = j == mj - 1 ? dc : 0.5 * (dc + d[q + 1]);
+              double denskm12 = k == 2 ? dc : 0.5 * (dc + d[q - mi2 * mj2]);
+              double denskp12 = k == mk - 1 ? dc : 0.5 * (dc + d[q + mi2 * mj2]);
+              aw = B.d.dy * B.d.dz / B.d.dx / densim12;
+              ae = B.d.dy * B.d.dz / B.d.dx / densip12;
+              as = B.d.dx * B.d.dz / B.d.dy / densjm12;
+              an = B.d.dx * B.d.dz / B.d.dy / densjp12;
+              ab = B.d.dx * B.d.dy / B.d.dz / denskm12;
+              at = B.d.dx * B.d.dy / B.d.dz / denskp12;
+            } else if (!B.stretched) {
               aw = 1.0 / dxx; ae = 1.0 / dxx;
               as = 1.0 / dyy; an = 1.0 / dyy;
               ab = 1.0 / dzz; at = 1.0 / dzz;
@@ -808,11 +864,24 @@ void pbound(Ctx &C) {
  * equal to dx on a uniform grid. */
 inline double dface(const std::vector<double> &w, int a0) { return 0.5 * (w[a0] + w[a0 + 1]); }
 
-/* calvel (press.for:139-200), non-LSM branch. */
+/* calvel (press.for:139-200), both branches. */
 void calvel(Ctx &C) {
   double dt = C.dt, alfapr = C.alfapr;
   par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_];
     int o = B.isp - 1; /* field index i <-> level-1 ghost-inclusive index i - o */
+    if (C.lsm) { /* press.for:152-190 */
+      double *d = B.dens;
+      for (int k = B.ksu; k <= B.keu; ++k) for (int i = B.isu; i <= B.ieu; ++i) for (int j = B.jsu; j <= B.jeu; ++j)
+        F(B, B.u, i, j, k) = (F(B, B.ustar, i, j, k) - dt * alfapr * (F(B, B.p, i + 1, j, k) - F(B, B.p, i, j, k)) /
+                              B.d.dx / (0.5 * (F(B, d, i, j, k) + F(B, d, i + 1, j, k))));
+      for (int k = B.ksv; k <= B.kev; ++k) for (int i = B.isv; i <= B.iev; ++i) for (int j = B.jsv; j <= B.jev; ++j)
+        F(B, B.v, i, j, k) = (F(B, B.vstar, i, j, k) - dt * alfapr * (F(B, B.p, i, j + 1, k) - F(B, B.p, i, j, k)) /
+                              B.d.dy / (0.5 * (F(B, d, i, j, k) + F(B, d, i, j + 1, k))));
+      for (int k = B.ksw; k <= B.kew; ++k) for (int i = B.isw; i <= B.iew; ++i) for (int j = B.jsw; j <= B.jew; ++j)
+        F(B, B.w, i, j, k) = (F(B, B.wstar, i, j, k) - dt * alfapr * (F(B, B.p, i, j, k + 1) - F(B, B.p, i, j, k)) /
+                              B.d.dz / (0.5 * (F(B, d, i, j, k) + F(B, d, i, j, k + 1))));
+      return;
+    }
     for (int k = B.ksu; k <= B.keu; ++k) for (int i = B.isu; i <= B.ieu; ++i) for (int j = B.jsu; j <= B.jeu; ++j) {
       double dxl = B.stretched ? dface(B.hx[1], i - o) : B.d.dx;
       F(B, B.u, i, j, k) = (F(B, B.ustar, i, j, k) - dt * alfapr * (F(B, B.p, i + 1, j, k) - F(B, B.p, i, j, k)) / dxl);
@@ -831,7 +900,7 @@ void calvel(Ctx &C) {
   exchange(C, 3);
 }
 
-/* calmas (press.for:2-75), differencing = 1, non-LSM branch. */
+/* calmas (press.for:2-75), differencing = 1, both branches. */
 void calmas(Ctx &C) {
   double rmax = 0.0;
   std::vector<double> bmax(C.b.size(), 0.0);
@@ -844,7 +913,10 @@ void calmas(Ctx &C) {
       double fact = ((F(B, B.u, i, j, k) - F(B, B.u, i - 1, j, k)) / hxl +
                      (F(B, B.v, i, j, k) - F(B, B.v, i, j - 1, k)) / hyl +
                      (F(B, B.w, i, j, k) - F(B, B.w, i, j, k - 1)) / hzl);
-      F(B, B.su.data(), i, j, k) = fact / C.dt;
+      if (C.lsm) /* press.for:51-53: sup, copied to the rhs by mgkcyc */
+        F(B, B.su.data(), i, j, k) = fact * B.d.dx * B.d.dy * B.d.dz / C.dt;
+      else
+        F(B, B.su.data(), i, j, k) = fact / C.dt;
       double fact1 = fact * hxl * hyl * hzl;
       resor = std::max(rmax, std::fabs(fact1));
       rmax = std::max(resor, std::fabs(fact1));
@@ -859,6 +931,7 @@ void calmas(Ctx &C) {
 /* newsolv_mg (newsolv_mg.for:2-102) */
 int newsolv_mg(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
   stamp(0);
+  if (C.lsm) coeff(C); /* newsolv_mg.for:12-14 */
   calvel(C);
   calmas(C);
   stamp(1);
@@ -904,6 +977,7 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
   C.maxcy = prm->maxcy; C.eps = prm->eps; C.eps_relative = prm->eps_relative; C.pl = prm->pl;
   C.pl_ex = prm->pl_ex;
   if (C.pl_ex < 0 || C.pl_ex >= C.pl) { g_err = "pl_ex"; return MF3D_E_INVALID; }
+  C.lsm = prm->lsm != 0;
   C.periodic = false;
   C.b.resize(nb);
   for (int ib = 0; ib < nb; ++ib) {
@@ -928,6 +1002,7 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
     if (B.d.bc_west == 5 || B.d.bc_east == 5 || B.d.bc_south == 5 || B.d.bc_north == 5 || B.d.bc_bottom == 5 || B.d.bc_top == 5)
       C.periodic = true;
     B.stretched = B.d.hx || B.d.hy || B.d.hz;
+    if (C.lsm && B.stretched) { g_err = "L_LSM on a stretched grid"; return MF3D_E_UNSUPPORTED; }
     B.hx = level_widths(B.d.hx, B.d.nx, B.d.dx, B.ngrid);
     B.hy = level_widths(B.d.hy, B.d.ny, B.d.dy, B.ngrid);
     B.hz = level_widths(B.d.hz, B.d.nz, B.d.dz, B.ngrid);
@@ -963,6 +1038,8 @@ int orc_newsolv_mg(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
     Blk &B = C.b[ib];
     B.ustar = fields[ib].ustar; B.vstar = fields[ib].vstar; B.wstar = fields[ib].wstar;
     B.u = fields[ib].u; B.v = fields[ib].v; B.w = fields[ib].w; B.p = fields[ib].p;
+    B.dens = fields[ib].dens;
+    if (C.lsm && !B.dens) { g_err = "L_LSM needs dens"; return MF3D_E_INVALID; }
   }
   st = newsolv_mg(C, hist, cap, info);
   for (int ib = 0; ib < nb; ++ib)

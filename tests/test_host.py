@@ -123,6 +123,24 @@ def test_create_rejects_bad_pl_ex_without_gpu(lib, oracle):
     assert st == abi.MF3D_E_INVALID
 
 
+def test_variable_density_limits_without_gpu(lib):
+    """lsm (the reference's L_LSM) runs in FP64 on uniform blocks through
+    mf3d_create only; the other combinations are refused before any device
+    work."""
+    ctx = C.c_void_p()
+    pr = Problem(1, 1, 1, 8, 8, 8, ngrid=2, pl=1)
+    prm = pr.params(lsm=1, precision=abi.MF3D_PREC_FP32)
+    assert lib.mf3d_create(pr.descriptors(lib), 1, C.byref(prm), C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED
+    st = Problem(1, 1, 1, 8, 8, 8, ngrid=2, pl=1, stretch_y=2.0)
+    assert lib.mf3d_create(st.descriptors(lib), 1, C.byref(st.params(lsm=1)), C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED
+    dom = (abi.DomainDesc * 1)()
+    dom[0].nx = dom[0].ny = dom[0].nz = 8
+    dom[0].dx = dom[0].dy = dom[0].dz = 1 / 8
+    assert lib.mf3d_batch_create(dom, 1, C.byref(pr.params(lsm=1)), C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED
+    srv = C.c_void_p()
+    assert lib.mf3d_server_create(C.byref(pr.params(lsm=1)), 1e9, 4, C.byref(srv)) == abi.MF3D_E_UNSUPPORTED
+
+
 def test_topology_rejects_fractional_extent(lib):
     ext = np.array([0.0, 1.05, 0.0, 1.0, 0.0, 1.0])
     bc6 = (C.c_int * 6)(5, 5, 4, 4, 5, 5)

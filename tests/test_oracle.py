@@ -238,3 +238,38 @@ def test_velocity_ghost_layers_wrap(oracle, pl, pl_ex):
             else:
                 assert np.array_equal(a[K, J, lo], given[k][K, J, lo])
                 assert np.array_equal(a[K, lo, I], given[k][K, lo, I])
+
+
+@pytest.mark.parametrize("rho", [1.0, 2.5])
+def test_variable_density_constant_rho_known_answer(oracle, rho):
+    """L_LSM with a constant density rho solves div(grad p / rho) = div(u*)/dt:
+    the converged pressure is rho times the uniform-density one (up to the
+    floating constant) and the projected velocities are the same.  Pins the
+    scaling of the L_LSM coefficients (mgsolver.for:120-182), of calvel
+    (press.for:152-190) and of the rhs sup (press.for:51-53)."""
+    pr = Problem(2, 1, 1, 16, 16, 16, ngrid=3, pl=1)
+    a = pr.block_fields(seed=3)
+    b = [{k: v.copy() for k, v in f.items()} for f in a]
+    for f, d in zip(b, pr.block_density(0, const=rho)):
+        f["dens"] = d
+    st_a, info_a, _ = solve(oracle, pr, a, maxcy=400, eps=1e-12)
+    st_b, info_b, _ = solve(oracle, pr, b, maxcy=400, eps=1e-12, lsm=1)
+    assert st_a == 0 and st_b == 0
+    assert info_b.rmax0 == info_a.rmax0
+    pa, pb = demean(pr.gather(a, "p")), demean(pr.gather(b, "p"))
+    assert np.abs(pb - rho * pa).max() <= 1e-9 * np.abs(rho * pa).max()
+    for k in ("u", "v", "w"):
+        assert np.abs(pr.gather(b, k) - pr.gather(a, k)).max() <= 1e-10
+
+
+def test_variable_density_projection_is_divergence_free(oracle):
+    """A random density field in [0.5, 2]: the converged projection leaves
+    u, v, w discretely divergence-free to the stopping tolerance."""
+    pr = Problem(2, 2, 1, 16, 16, 8, ngrid=3, pl=2)
+    blocks = pr.block_fields(seed=11, fourier_modes=2)
+    for f, d in zip(blocks, pr.block_density(7)):
+        f["dens"] = d
+    div0 = np.abs(divergence(pr, blocks)).max()
+    st, info, hist = solve(oracle, pr, blocks, maxcy=2000, eps=1e-11, lsm=1)
+    assert st == 0
+    assert np.abs(divergence(pr, blocks)).max() <= 1e-9 * div0
