@@ -156,19 +156,22 @@ def oracle_lib():
     return lib
 
 
-def time_oracle_iterations(pr, n_iter: int, threads: int):
+def time_oracle_iterations(pr, n_iter: int, threads: int, lsm: int = 0):
     """Run the oracle's newsolv_mg for n_iter outer iterations on the full
     workload; returns (seconds of the initial calvel/calmas, per-iteration
-    seconds list)."""
+    seconds list).  lsm: variable density (densities as run_density's)."""
     import numpy as np
     from multiflow3d_b200.abi import SolveInfo
     from multiflow3d_b200.problems import fields_struct
     orc = oracle_lib()
     orc.orc_set_threads(threads)
     blocks = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    if lsm:
+        for f, dn in zip(blocks, pr.block_density(SEED + 1)):
+            f["dens"] = dn
     stamps = np.zeros(n_iter + 4)
     orc.orc_set_timestamps(stamps.ctypes.data_as(C.POINTER(C.c_double)), len(stamps))
-    prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=n_iter, eps=1e-300)
+    prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=n_iter, eps=1e-300, lsm=lsm)
     info = SolveInfo()
     hist = np.zeros(n_iter)
     orc.orc_newsolv_mg(pr.descriptors(orc), pr.nblocks, C.byref(prm), fields_struct(blocks), 1.0, 1.0,
@@ -442,6 +445,60 @@ def run_mixed(args):
     return 0
 
 
+def run_density(args):
+    """Variable density (the reference's L_LSM branches): 2x2x2 blocks of
+    64^3 (128^3), uniform spacing, densities i.i.d. uniform in [0.5, 2],
+    5 levels, RB-GS(2,1), rel tol 1e-8, FP64.  The CPU baseline is the
+    oracle on the same inputs, 8 threads (one per block), timed over a
+    bounded number of outer iterations and scaled to the GPU's iteration
+    count (the two agree bit for bit)."""
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.problems import Problem
+    from multiflow3d_b200.solver import Projection
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    h = 1.0 / 128
+    pr = Problem(2, 2, 2, 64, 64, 64, ngrid=5, pl=2, dx=h, dy=h, dz=h)
+    host = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    dens = pr.block_density(SEED + 1)
+    keys = ("ustar", "vstar", "wstar", "u", "v", "w", "p")
+    d = [{**{k: torch.from_numpy(f[k]).to(dev) for k in keys}, "dens": torch.from_numpy(dn).to(dev)}
+         for f, dn in zip(host, dens)]
+    pristine = [{k: f[k].clone() for k in ("u", "v", "w", "p")} for f in d]
+
+    def reset():
+        for f, p0 in zip(d, pristine):
+            for k in ("u", "v", "w", "p"):
+                f[k].copy_(p0[k])
+
+    prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=5000, eps=1e-8, lsm=1)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    sec, r = _timed_solves(lambda: proj.newsolv_mg_device(d), reset, args.steps, args.warmup)
+    proj.close()
+    value = args.steps / sec
+    line = {
+        "metric": "poisson_solves_per_s_variable_density", "value": value, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "variable density (L_LSM), 2x2x2 blocks of 64^3 (128^3), uniform h, density "
+                               "U[0.5,2], 5 levels, RB-GS(2,1), rel tol 1e-8"},
+        "iterations": r.iter, "status": r.status, "rel_rmax": r.rmax / r.rmax0,
+        "ms_per_iteration": sec / args.steps * 1e3 / max(r.iter, 1),
+    }
+    if not args.no_cpu_baseline:
+        threads = max(1, min(os.cpu_count() or 1, pr.nblocks))
+        t_init, its = time_oracle_iterations(pr, 12, threads, lsm=1)
+        t_it = sum(its[2:]) / len(its[2:])
+        cpu = 1.0 / (t_init + r.iter * t_it)
+        line["cpu_baseline"] = {"value": cpu, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"10 timed outer iterations of the same solve on the oracle "
+                                          f"({threads} threads), scaled to {r.iter} iterations"}
+        line["speedup_vs_cpu"] = value / cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batched(args):
     """64 independent domains (edges log-uniform in [32,192], multiples of 8,
     periodic/wall per axis), tol 1e-8: one mixed-precision batch context
@@ -634,8 +691,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mf3d", choices=["mf3d", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="multiblock", choices=["multiblock", "mixed", "batched", "served"],
-                    help="multiblock: the default FP64 line; mixed / batched / served: the further workloads (1 GPU)")
+    ap.add_argument("--workload", default="multiblock",
+                    choices=["multiblock", "mixed", "batched", "served", "density"],
+                    help="multiblock: the default FP64 line; mixed / batched / served / density: the further "
+                         "workloads (1 GPU)")
     ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
     ap.add_argument("--requests", type=int, default=200, help="served: requests per rate")
     args = ap.parse_args()
@@ -647,6 +706,8 @@ def main():
         return run_batched(args)
     if args.workload == "served":
         return run_served(args)
+    if args.workload == "density":
+        return run_density(args)
     return run_gpu(args)
 
 
