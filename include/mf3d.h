@@ -103,6 +103,15 @@ typedef struct mf3d_params {
                        density (press.for:152-190) and the rhs is sup =
                        div(u)*dx*dy*dz/dt (press.for:51-53).  FP64 only,
                        uniform spacing, mf3d_create contexts only.            */
+  int bounds;       /* 1: after the loop, boundu/boundv/boundw (newsolv_mg.for:
+                       86-88, bounds.for:2-916) on the device: the periodic
+                       exchange_bc of u, v, w, then every face without a
+                       neighbour by its code - 3 symmetry, 4 wall, 5 periodic
+                       (others return MF3D_E_UNSUPPORTED).  Also refreshes the
+                       full periodic ghost planes of the final exchange(1..3).
+                       Skipped when the solve diverged (the reference stops).
+                       mf3d_create contexts only.  0: u, v, w face ghosts as
+                       documented at mf3d_fields.                             */
 } mf3d_params;
 
 /* Field pointers of one block, each a (ttc_i,ttc_j,ttc_k) array.

@@ -85,6 +85,7 @@ class Params(C.Structure):
         ("device", C.c_int),
         ("pl_ex", C.c_int),
         ("lsm", C.c_int),
+        ("bounds", C.c_int),
     ]
 
 

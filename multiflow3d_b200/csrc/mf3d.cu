@@ -289,6 +289,7 @@ struct BlockStore {
   std::vector<LevelStore> lv;  // [1..ngrid]
   DevBuf<double> geo1;   // level-1 widths h[3] (n+2) and face distances df[3] (n+1)
   DevBuf<double> planes; // face planes lo/hi of u, v, w (and the L_LSM face densities)
+  DevBuf<double> bcst;   // bounds mode: exchange_bc receive planes of u, v, w
   bool lsm = false;      // variable-density coefficients, formed per solve
   BlkFld fld;            // host template (field pointers bound per call)
   size_t bytes = 0;      // device bytes owned
@@ -297,7 +298,7 @@ struct BlockStore {
 // Build one block's hierarchy: replaces `coeff` (mgsolver.for:2-222) and the
 // `cof` sizing of localparameters.for:208-237.
 static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int elem_fine, int elem_coarsest, int pl,
-                       bool lsm, cudaStream_t s) {
+                       bool lsm, bool bounds, cudaStream_t s) {
   const int elem = elem_fine;
   S.d = d;
   S.lsm = lsm;
@@ -442,6 +443,19 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
   F.lo[2] = pp; F.hi[2] = pp + pxy; pp += 2 * pxy;
   F.dlo[0] = pp; F.dlo[1] = pp + pyz; F.dlo[2] = pp + pyz + pxz;
   F.L1 = S.lv[1].desc;
+  const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+  const int nbrs[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+  for (int f = 0; f < 6; ++f) {
+    F.bcode[f] = bcs[f];
+    F.pface[f] = (bcs[f] == MF3D_BC_PERIODIC && nbrs[f] < 0) ? (nbrs[f ^ 1] < 0 ? 1 : 2) : 0;
+  }
+  if (bounds) {
+    const long long ti = d.nx + 2 * pl, tj = d.ny + 2 * pl, tk = d.nz + 2 * pl;
+    F.bcplane = std::max(tj * tk, std::max(ti * tk, ti * tj));
+    if ((st = S.bcst.alloc((size_t)18 * F.bcplane))) return st;
+    F.bcst = S.bcst.p;
+    S.bytes += S.bcst.n * sizeof(double);
+  }
   for (int a = 0; a < 3; ++a) F.pinv[a] = ext[a] ? 0.0 : pow2_inverse(hh[a]);
   return MF3D_OK;
 }
@@ -468,7 +482,7 @@ static long long level_off(const BlkLev &B, int i, int j, int k) {
 }
 
 static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, int ngrid, int elem, int elem_coarsest,
-                        int pl, cudaStream_t s, bool lsm = false) {
+                        int pl, cudaStream_t s, bool lsm = false, bool bounds = false) {
   D.ngrid = ngrid;
   D.blocks.clear();
   std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
@@ -477,7 +491,7 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
   D.bytes = 0;
   for (int b = 0; b < nb; ++b) {
     D.blocks.emplace_back(new BlockStore());
-    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, elem_coarsest, pl, lsm, s))) return st;
+    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, elem_coarsest, pl, lsm, bounds, s))) return st;
     D.bytes += D.blocks.back()->bytes;
   }
   D.halo.assign(ngrid + 1, {});
@@ -567,6 +581,9 @@ struct View {
   std::vector<BlkFld> hf;
   DevBuf<BlkFld> df;
   DevBuf<Tile> t_int, t_zint, t_l1cells, t_faces, t_planes, t_pairs, t_vfaces;
+  DevBuf<Tile> t_bcax[3];             // bounds mode: 3 components x 2 faces x ttc plane per block, per axis
+  int n_bcax[3] = {0, 0, 0};
+  bool bc_periodic[3] = {false, false, false};  // some block has a periodic face along the axis
   int n_pairs = 0, pairs_kch = 1;
   int n_int = 0, n_zint = 0, n_l1cells = 0, n_faces = 0, n_planes = 0, n_vfaces = 0;
   DevBuf<DomState> ds;
@@ -852,7 +869,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
   // level-1 field tables
   V.hf.resize(nb);
   std::vector<Tile> t1, t2, t5;
-  std::vector<long long> it_faces, it_planes, it_vfaces;
+  std::vector<long long> it_faces, it_planes, it_vfaces, it_bcax[3];
   for (int b = 0; b < nb; ++b) {
     const BlockStore &S = *V.blk[b];
     BlkFld F = S.fld;
@@ -873,6 +890,13 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
     it_faces.push_back(2 * ((long long)x.ny * x.nz + (long long)x.nx * x.nz + (long long)x.nx * x.ny));
     it_planes.push_back((long long)x.ny * x.nz + (long long)x.nx * x.nz + (long long)x.nx * x.ny);
     it_vfaces.push_back((long long)(C->prm.pl_ex + 1) * it_faces.back());
+    {
+      const long long ti = x.nx + 2 * (long long)F.pl, tj = x.ny + 2 * (long long)F.pl, tk = x.nz + 2 * (long long)F.pl;
+      it_bcax[0].push_back(6 * tj * tk);
+      it_bcax[1].push_back(6 * ti * tk);
+      it_bcax[2].push_back(6 * ti * tj);
+      for (int f = 0; f < 6; ++f) V.bc_periodic[f / 2] |= F.pface[f] != 0;
+    }
     V.n_l1 += (long long)x.nx * x.ny * x.nz;
   }
   {
@@ -896,6 +920,12 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
   if ((st = V.t_faces.upload(t3, s))) return st;
   if ((st = V.t_planes.upload(t4, s))) return st;
   if ((st = V.t_vfaces.upload(t6, s))) return st;
+  if (C->prm.bounds)
+    for (int a = 0; a < 3; ++a) {
+      auto tb = make_tiles(it_bcax[a]);
+      V.n_bcax[a] = (int)tb.size();
+      if ((st = V.t_bcax[a].upload(tb, s))) return st;
+    }
   // per-domain solve state
   std::vector<int> ones(std::max(nd, 1), 1);
   if ((st = V.ds.alloc(std::max(nd, 1)))) return st;
@@ -1264,6 +1294,19 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
   return MF3D_OK;
 }
 
+// exchange_bc of u, v, w with every block on one rank (exchange_bc.for:
+// 16-838): per layer, the first walk's self-copies, the second walk's
+// self-copies and packs, the third walk's unpacks, each over x, y, z.
+static void bc_walks(mf3d_ctx *C, View &V) {
+  for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
+    for (int mode = 0; mode < 3; ++mode)
+      for (int a = 0; a < 3; ++a) {
+        if (!V.bc_periodic[a]) continue;
+        launch(k_bc_walk, V.n_bcax[a], kTile, 0, C->stream, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly, mode);
+        ++C->launches;
+      }
+}
+
 // Finish: optional su, the final calvel (u, v, w from the final p).
 template <typename T>
 static int solve_end(mf3d_ctx *C, View &V) {
@@ -1275,8 +1318,23 @@ static int solve_end(mf3d_ctx *C, View &V) {
     ++C->launches;
   }
   launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, nullptr);
+  C->launches += 1;
+  if (C->prm.bounds) {
+    // exchange(1..3) of the final calvel with full periodic planes, then
+    // boundu/boundv/boundw (newsolv_mg.for:86-88)
+    bc_walks(C, V);
+    launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
+    ++C->launches;
+    bc_walks(C, V);
+    for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
+      for (int a = 0; a < 3; ++a) {
+        launch(k_bound_faces, V.n_bcax[a], kTile, 0, s, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly);
+        ++C->launches;
+      }
+    return MF3D_OK;
+  }
   launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
-  C->launches += 2;
+  ++C->launches;
   return MF3D_OK;
 }
 
@@ -1509,6 +1567,15 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
       set_error("block " + std::to_string(d.id) + ": an edge does not exceed pl_ex");
       return MF3D_E_INVALID;
     }
+    if (prm->bounds) {
+      const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+      const int nbrs[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+      for (int f = 0; f < 6; ++f)
+        if (nbrs[f] < 0 && bcs[f] != 3 && bcs[f] != 4 && bcs[f] != MF3D_BC_PERIODIC) {
+          set_error("bounds: block " + std::to_string(d.id) + " has a face code other than 3, 4, 5");
+          return MF3D_E_UNSUPPORTED;
+        }
+    }
     if (prm->lsm && (d.hx || d.hy || d.hz)) {
       set_error("lsm: uniform spacing only (the reference's variable-density branch)");
       return MF3D_E_UNSUPPORTED;
@@ -1525,7 +1592,7 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   C->doms.emplace_back(new DomainStore());
   C->coarse64 = C->elem == 4 && prm->ngrid > 1;
   if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, C->coarse64 ? 8 : C->elem, prm->pl,
-                         C->stream, prm->lsm != 0)))
+                         C->stream, prm->lsm != 0, prm->bounds != 0)))
     return st;
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
@@ -1585,7 +1652,10 @@ static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params 
   if (!doms || nd <= 0 || !out) { set_error("mf3d_batch_create: bad arguments"); return MF3D_E_INVALID; }
   int st = check_params(prm);
   if (st) return st;
-  if (prm->lsm) { set_error("lsm: single-problem contexts (mf3d_create) only"); return MF3D_E_UNSUPPORTED; }
+  if (prm->lsm || prm->bounds) {
+    set_error("lsm and bounds: single-problem contexts (mf3d_create) only");
+    return MF3D_E_UNSUPPORTED;
+  }
   for (int d = 0; d < nd; ++d) {
     if (domain_ngrid(doms[d]) < 1) {
       set_error("domain " + std::to_string(d) + ": sizes not divisible by 2^(ngrid-1)");

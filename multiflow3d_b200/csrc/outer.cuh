@@ -43,6 +43,11 @@ struct BlkFld {
   const double *dens;                // L_LSM: cell densities (ttc layout), else null
   double *dlo[3];                    // L_LSM: face density 0.5*(d(n)+d(n+1)) of the source block
                                      // at a non-wall low face (k_face_planes)
+  int bcode[6];                      // boundary code of each face (control.cin), W,E,S,N,B,T
+  int pface[6];                      // periodic face with no neighbour: 1 block alone along the
+                                     // axis (copies onto itself), 2 partner block src[f]; else 0
+  double *bcst;                      // exchange_bc receive planes: 3 components x 6 faces x bcplane
+  long long bcplane;                 // elements per receive plane (the largest ttc plane)
 };
 
 // x / h.  When h is a power of two the multiplication by its reciprocal
@@ -276,6 +281,109 @@ __global__ void k_face_planes(const BlkFld *__restrict__ fl, const Tile *__restr
   // high face
   long long e = ax == 0 ? fidx(F, nx, a, b) : ax == 1 ? fidx(F, a, ny, b) : fidx(F, a, b, nz);
   F.hi[ax][o] = F.wall[fh] ? vel[e] : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// boundu / boundv / boundw after the loop (newsolv_mg.for:86-88), and the
+// full periodic planes of exchange(1..3) they need.  All three velocity
+// components in each launch (independent arrays).  Local indices: 1..n
+// interior, 1-pl..n+pl ghost-inclusive.
+// ---------------------------------------------------------------------------
+// The component's range along an axis (localparameters.for:185-190): the
+// normal component stops one face short at a high wall.
+__device__ inline int comp_end(const BlkFld &F, int comp, int ax) {
+  const int n = ax == 0 ? F.nx : ax == 1 ? F.ny : F.nz;
+  return n - ((comp == ax && F.wall[2 * ax + 1]) ? 1 : 0);
+}
+__device__ inline double *comp_field(const BlkFld &F, int comp) { return comp == 0 ? F.u : comp == 1 ? F.v : F.w; }
+__device__ inline long long fidx_ax(const BlkFld &F, int ax, int a, int s, int t) {
+  return ax == 0 ? fidx(F, a, s, t) : ax == 1 ? fidx(F, s, a, t) : fidx(F, s, t, a);
+}
+
+// One walk of exchange_bc (exchange_bc.for:16-838, every block on one
+// rank) over the two faces of axis `ax`, layer ly, full ghost-inclusive
+// planes.  mode 0: the first walk's self-copies of a block alone along the
+// axis, ghost(s0-1-ly) = plane(e0-ly), ghost(e0+1+ly) = plane(s0+ly) (its
+// packs are overwritten by the second walk's); mode 1: the second walk -
+// the self-copies again and the packs into the partner's receive planes;
+// mode 2: the third walk, ghost planes from the receive planes.  Launched
+// per layer as walk 1 for x, y, z, walk 2 for x, y, z, walk 3 for x, y, z:
+// a block's faces in the reference's W, E, S, N, B, T order.  Reads and
+// writes of one launch never meet (interior planes or receive planes
+// against ghost planes).  Items per block: 3 * 2 * n1 * n2 (ttc extents of
+// the other two axes).  Skipped after a diverged solve.
+__global__ void k_bc_walk(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                          const DomState *__restrict__ ds, int ax, int ly, int mode) {
+  pdl_wait();
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  if (ds[F.dom].rmax > 100.0) return;
+  const int pl = F.pl;
+  const int m1 = (ax == 0 ? F.ny : F.nx) + 2 * pl, m2 = (ax == 2 ? F.ny : F.nz) + 2 * pl;
+  int q = t.i0 + threadIdx.x;
+  const int plane = m1 * m2;
+  if (q >= 6 * plane) return;
+  const int comp = q / (2 * plane);
+  q -= comp * 2 * plane;
+  const int side = q / plane;
+  q -= side * plane;
+  const int sl = q % m1 + 1 - pl, tl = q / m1 + 1 - pl;  // local coordinates of the plane cell
+  const int f = 2 * ax + side;
+  const int pf = F.pface[f];
+  if (!pf) return;
+  double *fi = comp_field(F, comp);
+  const int s0 = 1, e0 = comp_end(F, comp, ax);
+  const long long g = fidx_ax(F, ax, side ? e0 + 1 + ly : s0 - 1 - ly, sl, tl);
+  if (mode == 2) {
+    if (pf == 2) fi[g] = F.bcst[((long long)comp * 6 + f) * F.bcplane + q];
+    return;
+  }
+  if (pf == 1) {
+    fi[g] = fi[fidx_ax(F, ax, side ? s0 + ly : e0 - ly, sl, tl)];
+  } else if (mode == 1) {
+    const BlkFld &P = fl[F.src[f]];
+    P.bcst[((long long)comp * 6 + (f ^ 1)) * P.bcplane + q] = fi[fidx_ax(F, ax, side ? e0 - ly : s0 + ly, sl, tl)];
+  }
+}
+
+// The faces of axis `ax` without a neighbour, layer ly, by their code
+// (bounds.for:2-916): over the component's ranges widened by one cell,
+//   normal component: wall -> 0; symmetry -> 0 on y and z faces;
+//   tangential: wall -> -(the cell ly inside); symmetry -> + on y and z faces;
+// x-face symmetry and periodic faces write nothing.  Launched per layer for
+// x, y, z (the reference's W, E, S, N, B, T).  Skipped after a diverged solve.
+__global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                              const DomState *__restrict__ ds, int ax, int ly) {
+  pdl_wait();
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  if (ds[F.dom].rmax > 100.0) return;
+  const int pl = F.pl;
+  const int m1 = (ax == 0 ? F.ny : F.nx) + 2 * pl, m2 = (ax == 2 ? F.ny : F.nz) + 2 * pl;
+  int q = t.i0 + threadIdx.x;
+  const int plane = m1 * m2;
+  if (q >= 6 * plane) return;
+  const int comp = q / (2 * plane);
+  q -= comp * 2 * plane;
+  const int side = q / plane;
+  q -= side * plane;
+  const int sl = q % m1 + 1 - pl, tl = q / m1 + 1 - pl;
+  const int f = 2 * ax + side;
+  if (!F.wall[f]) return;
+  const int code = F.bcode[f];
+  const bool normal = comp == ax;
+  int mode = 0;  // 1 zero, 2 -mirror, 3 +mirror
+  if (code == 4) mode = normal ? 1 : 2;
+  else if (code == 3 && ax != 0) mode = normal ? 1 : 3;
+  if (!mode) return;
+  // the widened ranges of the other two axes: 0 .. end+1
+  const int as = ax == 0 ? 1 : 0, at = ax == 2 ? 1 : 2;
+  if (sl < 0 || sl > comp_end(F, comp, as) + 1 || tl < 0 || tl > comp_end(F, comp, at) + 1) return;
+  double *fi = comp_field(F, comp);
+  const int s0 = 1, e0 = comp_end(F, comp, ax);
+  const long long g = fidx_ax(F, ax, side ? e0 + 1 + ly : s0 - 1 - ly, sl, tl);
+  const double m = fi[fidx_ax(F, ax, side ? e0 - ly : s0 + ly, sl, tl)];
+  fi[g] = mode == 1 ? 0.0 : mode == 2 ? -m : m;
 }
 
 __device__ inline void atomic_max_nonneg(unsigned long long *slot, double v) {

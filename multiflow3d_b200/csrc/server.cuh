@@ -439,7 +439,10 @@ int mf3d_server_create(const mf3d_params *prm, double mem_cap_bytes, int max_res
     set_error("mf3d_server_create: bad arguments");
     return MF3D_E_INVALID;
   }
-  if (prm->lsm) { set_error("lsm: single-problem contexts (mf3d_create) only"); return MF3D_E_UNSUPPORTED; }
+  if (prm->lsm || prm->bounds) {
+    set_error("lsm and bounds: single-problem contexts (mf3d_create) only");
+    return MF3D_E_UNSUPPORTED;
+  }
   mf3d_params p = *prm;
   p.ngrid = std::max(p.ngrid, 1);
   int st = check_params(&p);

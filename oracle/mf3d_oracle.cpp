@@ -94,6 +94,7 @@ struct Ctx {
   std::map<int, int> indid; /* dom_indid: block id -> position */
   int ngrd_gl, mg_itrsch, irestr, iproln, maxcy, pl, pl_ex;
   bool lsm; /* L_LSM: variable-density coefficients, calvel and rhs */
+  bool bounds; /* boundu/boundv/boundw after the loop (newsolv_mg.for:86-88) */
   double eps;
   int eps_relative;
   bool periodic;
@@ -709,67 +710,58 @@ void franges(Blk &B, int op, int &is, int &ie, int &js, int &je, int &ks, int &k
   else { is = B.isp; ie = B.iep; js = B.jsp; je = B.jep; ks = B.ksp; ke = B.kep; }
 }
 
+/* exchange_bc (exchange_bc.for:2-841) with every block on one MPI rank
+ * (the `dom_ad(a) .eq. dom_ad(b)` path), layers ly = 0..nly.  Per layer the
+ * reference walks the blocks three times, face by face W, E, S, N, B, T
+ * (:16-320, :322-640, :642-838).  The first two walks copy a block that is
+ * alone along a periodic axis onto itself (full ghost-inclusive planes) and
+ * pack every other periodic face straight into the partner's receive
+ * buffer - the second pack overwrites the first, from the state the first
+ * walk's self-copies left; the third walk unpacks. */
+void bc_face(Ctx &C, Blk &B, int op, int ly, int f, bool unpack) {
+  const int ax = f / 2;
+  const bool high = f & 1;
+  const int bcs[6] = {B.d.bc_west, B.d.bc_east, B.d.bc_south, B.d.bc_north, B.d.bc_bottom, B.d.bc_top};
+  const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
+  const int per[6] = {B.d.per_ip, B.d.per_in, B.d.per_jp, B.d.per_jn, B.d.per_kp, B.d.per_kn};
+  if (!(bcs[f] == 5 && nbr[f] < 0)) return;
+  const bool alone = nbr[f ^ 1] < 0;
+  int is, ie, js, je, ks, ke;
+  franges(B, op, is, ie, js, je, ks, ke);
+  double *fi = field_of(B, op);
+  int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
+  int n1 = ax == 0 ? B.ttc_j : B.ttc_i, n2 = ax == 2 ? B.ttc_j : B.ttc_k;
+  auto at = [&](int a, int s, int t) -> double & {
+    if (ax == 0) return F(B, fi, a, s, t);
+    if (ax == 1) return F(B, fi, s, a, t);
+    return F(B, fi, s, t, a);
+  };
+  const int ghost = high ? e0 + 1 + ly : s0 - 1 - ly;
+  if (unpack) {
+    if (alone) return;
+    std::vector<double> &R = high ? B.frp[ax + 1] : B.frm[ax + 1];
+    for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(ghost, s, t) = R[(size_t)(t - 1) * n1 + s];
+    return;
+  }
+  if (alone) {
+    const int src = high ? s0 + ly : e0 - ly;
+    for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(ghost, s, t) = at(src, s, t);
+    return;
+  }
+  Blk &P = C.b[C.indid.at(per[f])];
+  std::vector<double> &R = high ? P.frm[ax + 1] : P.frp[ax + 1];
+  R.assign((size_t)n1 * n2 + 1, 0.0);
+  const int src = high ? e0 - ly : s0 + ly;
+  for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) R[(size_t)(t - 1) * n1 + s] = at(src, s, t);
+}
+
 void exchange_bc(Ctx &C, int op, int nly) {
-  for (int ly = 0; ly <= nly; ++ly)
-  for (int ax = 0; ax < 3; ++ax) {
-    for (auto &B : C.b) {
-      int bcp = ax == 0 ? B.d.bc_west : ax == 1 ? B.d.bc_south : B.d.bc_bottom;
-      int bcn = ax == 0 ? B.d.bc_east : ax == 1 ? B.d.bc_north : B.d.bc_top;
-      if (!(bcp == 5 || bcn == 5)) continue;
-      int prev = ax == 0 ? B.d.iprev : ax == 1 ? B.d.jprev : B.d.kprev;
-      int next = ax == 0 ? B.d.inext : ax == 1 ? B.d.jnext : B.d.knext;
-      int perp = ax == 0 ? B.d.per_ip : ax == 1 ? B.d.per_jp : B.d.per_kp;
-      int pern = ax == 0 ? B.d.per_in : ax == 1 ? B.d.per_jn : B.d.per_kn;
-      int is, ie, js, je, ks, ke;
-      franges(B, op, is, ie, js, je, ks, ke);
-      double *fi = field_of(B, op);
-      int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
-      int n1 = ax == 0 ? B.ttc_j : B.ttc_i, n2 = ax == 2 ? B.ttc_j : B.ttc_k;
-      auto at = [&](int a, int s, int t) -> double & {
-        if (ax == 0) return F(B, fi, a, s, t);
-        if (ax == 1) return F(B, fi, s, a, t);
-        return F(B, fi, s, t, a);
-      };
-      if (prev < 0) {
-        if (next < 0) {
-          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(s0 - 1 - ly, s, t) = at(e0 - ly, s, t);
-        } else {
-          Blk &P = C.b[C.indid.at(perp)];
-          P.frp[ax + 1].assign((size_t)n1 * n2 + 1, 0.0);
-          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) P.frp[ax + 1][(size_t)(t - 1) * n1 + s] = at(s0 + ly, s, t);
-        }
-      }
-      if (next < 0) {
-        if (prev < 0) {
-          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(e0 + 1 + ly, s, t) = at(s0 + ly, s, t);
-        } else {
-          Blk &N = C.b[C.indid.at(pern)];
-          N.frm[ax + 1].assign((size_t)n1 * n2 + 1, 0.0);
-          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) N.frm[ax + 1][(size_t)(t - 1) * n1 + s] = at(e0 - ly, s, t);
-        }
-      }
-    }
-    for (auto &B : C.b) {
-      int bcp = ax == 0 ? B.d.bc_west : ax == 1 ? B.d.bc_south : B.d.bc_bottom;
-      int bcn = ax == 0 ? B.d.bc_east : ax == 1 ? B.d.bc_north : B.d.bc_top;
-      if (!(bcp == 5 || bcn == 5)) continue;
-      int prev = ax == 0 ? B.d.iprev : ax == 1 ? B.d.jprev : B.d.kprev;
-      int next = ax == 0 ? B.d.inext : ax == 1 ? B.d.jnext : B.d.knext;
-      int is, ie, js, je, ks, ke;
-      franges(B, op, is, ie, js, je, ks, ke);
-      double *fi = field_of(B, op);
-      int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
-      int n1 = ax == 0 ? B.ttc_j : B.ttc_i, n2 = ax == 2 ? B.ttc_j : B.ttc_k;
-      auto at = [&](int a, int s, int t) -> double & {
-        if (ax == 0) return F(B, fi, a, s, t);
-        if (ax == 1) return F(B, fi, s, a, t);
-        return F(B, fi, s, t, a);
-      };
-      if (prev < 0 && next >= 0)
-        for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(s0 - 1 - ly, s, t) = B.frm[ax + 1][(size_t)(t - 1) * n1 + s];
-      if (next < 0 && prev >= 0)
-        for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) at(e0 + 1 + ly, s, t) = B.frp[ax + 1][(size_t)(t - 1) * n1 + s];
-    }
+  for (int ly = 0; ly <= nly; ++ly) {
+    for (int walk = 0; walk < 2; ++walk)
+      for (auto &B : C.b)
+        for (int f = 0; f < 6; ++f) bc_face(C, B, op, ly, f, false);
+    for (auto &B : C.b)
+      for (int f = 0; f < 6; ++f) bc_face(C, B, op, ly, f, true);
   }
 }
 
@@ -858,6 +850,54 @@ void pbound(Ctx &C) {
     if (B.d.knext < 0 && B.d.bc_top != 5)
       for (int j = jsp - 1; j <= jep + 1; ++j) for (int i = isp - 1; i <= iep + 1; ++i) F(B, p, i, j, kep + 1) = F(B, p, i, j, kep);
   }
+}
+
+/* boundu, boundv, boundw (bounds.for:2-916), restated for the codes 3
+ * (symmetry), 4 (wall) and 5 (periodic); set-up rejects the others.  The
+ * periodic copy, then per layer ly = 0..pl_ex each block's faces W, E, S,
+ * N, B, T over the component's ranges widened by one cell:
+ *   normal component (u on x faces, ...): wall -> 0; symmetry -> 0 on y and
+ *     z faces, nothing on x faces;
+ *   tangential component: wall -> -(the cell ly inside); symmetry -> +(the
+ *     same) on y and z faces, nothing on x faces.
+ * (bounds.for:36-42, 136-140, 179-186, 212-219, 246-259, 301-308 for u;
+ * 369-373, 444-448, 505-533, 535-548, 588-595 for v; 657-661, 738-742,
+ * 799-806, 833-840, 866-876, 900-908 for w.) */
+void bound_face(Blk &B, int op, int ly, int f) {
+  const int ax = f / 2, comp = op - 1;
+  const bool high = f & 1;
+  const int bcs[6] = {B.d.bc_west, B.d.bc_east, B.d.bc_south, B.d.bc_north, B.d.bc_bottom, B.d.bc_top};
+  const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
+  if (nbr[f] >= 0) return;
+  const int code = bcs[f];
+  const bool normal = ax == comp;
+  int mode = 0; /* 0 nothing, 1 zero, 2 -mirror, 3 +mirror */
+  if (code == 4) mode = normal ? 1 : 2;
+  else if (code == 3 && ax != 0) mode = normal ? 1 : 3;
+  if (!mode) return;
+  int is, ie, js, je, ks, ke;
+  franges(B, op, is, ie, js, je, ks, ke);
+  double *fi = field_of(B, op);
+  int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
+  /* the other two axes, in the reference's loop order (outer t, inner s) */
+  int sa = ax == 0 ? js : is, ea = ax == 0 ? je : ie;
+  int ta = ax == 2 ? js : ks, tb = ax == 2 ? je : ke;
+  auto at = [&](int a, int s, int t) -> double & {
+    if (ax == 0) return F(B, fi, a, s, t);
+    if (ax == 1) return F(B, fi, s, a, t);
+    return F(B, fi, s, t, a);
+  };
+  const int ghost = high ? e0 + 1 + ly : s0 - 1 - ly, mirror = high ? e0 - ly : s0 + ly;
+  for (int t = ta - 1; t <= tb + 1; ++t)
+    for (int s = sa - 1; s <= ea + 1; ++s)
+      at(ghost, s, t) = mode == 1 ? 0.0 : mode == 2 ? -at(mirror, s, t) : at(mirror, s, t);
+}
+
+void bound(Ctx &C, int op) {
+  if (C.periodic) exchange_bc(C, op, C.pl_ex);
+  for (int ly = 0; ly <= C.pl_ex; ++ly)
+    for (auto &B : C.b)
+      for (int f = 0; f < 6; ++f) bound_face(B, op, ly, f);
 }
 
 /* EXT: distance between the centres of cells a and a+1 along an axis,
@@ -961,6 +1001,8 @@ int newsolv_mg(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
   int iters = conv ? iter : C.maxcy;
   if (!conv) status = MF3D_NOT_CONVERGED;
   if (C.rmax > 100.0) status = MF3D_DIVERGED;
+  /* newsolv_mg.for:84-88 (the reference stops first when rmax > 100) */
+  if (C.bounds && status != MF3D_DIVERGED) { bound(C, 1); bound(C, 2); bound(C, 3); }
   if (info) {
     info->rmax = C.rmax; info->rmax0 = rmax0; info->iter = iters; info->status = status; info->ms_device = 0.0;
   }
@@ -978,6 +1020,7 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
   C.pl_ex = prm->pl_ex;
   if (C.pl_ex < 0 || C.pl_ex >= C.pl) { g_err = "pl_ex"; return MF3D_E_INVALID; }
   C.lsm = prm->lsm != 0;
+  C.bounds = prm->bounds != 0;
   C.periodic = false;
   C.b.resize(nb);
   for (int ib = 0; ib < nb; ++ib) {
@@ -1003,6 +1046,12 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
       C.periodic = true;
     B.stretched = B.d.hx || B.d.hy || B.d.hz;
     if (C.lsm && B.stretched) { g_err = "L_LSM on a stretched grid"; return MF3D_E_UNSUPPORTED; }
+    if (C.bounds) {
+      const int bcs[6] = {B.d.bc_west, B.d.bc_east, B.d.bc_south, B.d.bc_north, B.d.bc_bottom, B.d.bc_top};
+      const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
+      for (int f = 0; f < 6; ++f)
+        if (nbr[f] < 0 && bcs[f] != 3 && bcs[f] != 4 && bcs[f] != 5) { g_err = "bounds: face code"; return MF3D_E_UNSUPPORTED; }
+    }
     B.hx = level_widths(B.d.hx, B.d.nx, B.d.dx, B.ngrid);
     B.hy = level_widths(B.d.hy, B.d.ny, B.d.dy, B.ngrid);
     B.hz = level_widths(B.d.hz, B.d.nz, B.d.dz, B.ngrid);

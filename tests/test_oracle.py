@@ -273,3 +273,41 @@ def test_variable_density_projection_is_divergence_free(oracle):
     st, info, hist = solve(oracle, pr, blocks, maxcy=2000, eps=1e-11, lsm=1)
     assert st == 0
     assert np.abs(divergence(pr, blocks)).max() <= 1e-9 * div0
+
+
+def test_bounds_known_answers(oracle):
+    """boundu/boundv/boundw after the loop (bounds: periodic x, walls in y,
+    symmetry in z, two ghost layers): a wall mirrors the tangential
+    components with a sign change and zeroes the normal one, a symmetry face
+    mirrors without it, and the periodic planes wrap."""
+    SYM = 3
+    n, pl = 8, 2
+    pr = Problem(1, 1, 1, n, n, n, bc=(PERIODIC, PERIODIC, WALL, WALL, SYM, SYM), ngrid=2, pl=pl)
+    blocks = pr.block_fields(seed=19)
+    st, info, _ = solve(oracle, pr, blocks, maxcy=6, eps=1e-12, pl_ex=1, bounds=1)
+    assert st >= 0
+    u, v, w = (blocks[0][k] for k in ("u", "v", "w"))
+    I = slice(pl - 1, pl + n + 1)          # x range widened by one (u, v, w: x periodic)
+    Ki = slice(pl, pl + n)                 # interior z
+    Ji = slice(pl, pl + n)
+    for ly in range(2):
+        lo, hi = pl - 1 - ly, pl + n + ly
+        # y walls: tangential -mirror, normal 0 (v stops one face short of the north wall)
+        for a in (u, w):
+            assert np.array_equal(a[Ki, lo, I], -a[Ki, pl + ly, I])
+            assert np.array_equal(a[Ki, hi, I], -a[Ki, pl + n - 1 - ly, I])
+        assert not v[Ki, lo, I].any() and not v[Ki, pl + n - 1 + ly, I].any()
+        # z symmetry: tangential +mirror, normal 0
+        for a in (u, v):
+            assert np.array_equal(a[lo, Ji, I], a[pl + ly, Ji, I])
+            assert np.array_equal(a[hi, Ji, I], a[pl + n - 1 - ly, Ji, I])
+        assert not w[lo, Ji, I].any() and not w[pl + n - 1 + ly, Ji, I].any()
+    for a in (u, v, w):  # periodic x: full first ghost planes wrap
+        assert np.array_equal(a[:, :, pl - 1], a[:, :, pl + n - 1])
+        assert np.array_equal(a[:, :, pl + n], a[:, :, pl])
+
+
+def test_bounds_rejects_other_codes(oracle):
+    pr = Problem(1, 1, 1, 8, 8, 8, bc=(1, 2, WALL, WALL, WALL, WALL), ngrid=2, pl=1)
+    st, _, _ = solve(oracle, pr, pr.block_fields(seed=1), maxcy=2, bounds=1)
+    assert st == -6  # MF3D_E_UNSUPPORTED: inflow / outflow codes are not restated
