@@ -499,6 +499,86 @@ def run_density(args):
     return 0
 
 
+def run_tecbin(args):
+    """Restart files (post.for:496-548 / initial.for:689-760): decode the
+    file images of the default workload's 8 blocks (ttc 132^3 each, 0.44 GB
+    per file) on the device.  value: GB of file image per second with the
+    images resident in HBM; e2e: the same from pinned host memory, copy
+    included.  CPU baseline: the numpy restatement of the reader
+    (oracle/tecbin.py) on one block."""
+    import numpy as np
+    import torch
+    from multiflow3d_b200 import abi
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import tecbin as orc_tb
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    n, nblk = 132, 8
+    rng = np.random.default_rng(SEED)
+    fields = {f: rng.standard_normal((n, n, n)) for f in orc_tb.FIELDS}
+    xyz = tuple((np.arange(n) - 2) / 256.0 for _ in range(3))
+    host_img = orc_tb.write(n, n, n, 2, 0, -1, 0, *xyz, fields)
+    nbytes = len(host_img)
+    info = abi.TecbinInfo()
+    assert lib.mf3d_tecbin_info_of(host_img, nbytes, C.byref(info)) == 0
+    pinned = torch.from_numpy(np.frombuffer(host_img, dtype=np.uint8).copy()).pin_memory()
+    imgs = [pinned.to(dev) for _ in range(nblk)]
+    outs = [torch.empty((n, n, n), dtype=torch.float64, device=dev) for _ in orc_tb.FIELDS]
+    ptrs = (C.c_void_p * 16)(*[o.data_ptr() for o in outs])
+
+    def decode(img):
+        st = lib.mf3d_tecbin_decode_device(C.c_void_p(img.data_ptr()), C.byref(info), ptrs, 0)
+        assert st == 0, abi.last_error(lib)
+
+    for _ in range(args.warmup):
+        for img in imgs:
+            decode(img)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        for img in imgs:
+            decode(img)
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3 / args.steps
+    value = nblk * nbytes / sec / 1e9
+    # end to end: pinned host image -> device -> fields
+    stage = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        for _b in range(nblk):
+            stage.copy_(pinned, non_blocking=True)
+            decode(stage)
+    e1.record()
+    torch.cuda.synchronize()
+    sec_e2e = e0.elapsed_time(e1) / 1e3 / args.steps
+    # algorithmic bytes of one decode: the image read, 16 of the 19 doubles written
+    alg = nbytes + 16 * n ** 3 * 8
+    peak, peak_src = measured_peaks()
+    line = {
+        "metric": "tecbin_decode_gb_per_s", "value": value, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "dtype": "u32 words / f64",
+        "data": "synthetic",
+        "config": {"workload": f"{nblk} restart files of ttc {n}^3 (pl 2), {nbytes / 1e9:.3f} GB each, decoded "
+                               "into the 16 fields the reader keeps"},
+        "e2e": {"value": nblk * nbytes / sec_e2e / 1e9, "unit": "GB/s", "h2d_bytes_per_step": nblk * nbytes,
+                "d2h_bytes_per_step": 0},
+        "roofline": {"bound": "hbm", "achieved": alg * nblk / sec / 1e9, "peak": peak, "peak_source": peak_src,
+                     "unit": "GB/s", "frac": alg * nblk / sec / 1e9 / peak, "traffic": None},
+    }
+    if not args.no_cpu_baseline:
+        import time
+        t = time.perf_counter()
+        orc_tb.read(host_img)
+        cpu = nbytes / (time.perf_counter() - t) / 1e9
+        line["cpu_baseline"] = {"value": cpu, "unit": "GB/s", "cores": 1, "kind": "port",
+                                "sample": "numpy restatement of the reader (oracle/tecbin.py) on one file"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batched(args):
     """64 independent domains (edges log-uniform in [32,192], multiples of 8,
     periodic/wall per axis), tol 1e-8: one mixed-precision batch context
@@ -692,7 +772,7 @@ def main():
     ap.add_argument("--impl", default="mf3d", choices=["mf3d", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="multiblock",
-                    choices=["multiblock", "mixed", "batched", "served", "density"],
+                    choices=["multiblock", "mixed", "batched", "served", "density", "tecbin"],
                     help="multiblock: the default FP64 line; mixed / batched / served / density: the further "
                          "workloads (1 GPU)")
     ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
@@ -708,6 +788,8 @@ def main():
         return run_served(args)
     if args.workload == "density":
         return run_density(args)
+    if args.workload == "tecbin":
+        return run_tecbin(args)
     return run_gpu(args)
 
 

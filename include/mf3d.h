@@ -353,6 +353,45 @@ int mf3d_server_destroy(mf3d_server *srv);
  * this implementation). */
 int mf3d_selftest_divide(const double *x, const double *b, long long n, double *q, double *qref, int device);
 
+/* ---------------------------------------------------------------------- */
+/* Restart files `tecbin<id>.bin` (the writer post.for:496-548 `tecbin`,   */
+/* the reader initial.for:689-760), decoded and encoded on the device.     */
+/* A file is gfortran unformatted sequential: each record framed by its    */
+/* byte length as a 4-byte integer before and after; records (toti, totj,  */
+/* totk), (pl), (inind, jnind, knind), then one record of 19 doubles per   */
+/* ttc cell, i fastest: x(i), y(j), z(k), p, pm, ppm, vis, u, um, uum, v,  */
+/* vm, vvm, w, wm, wwm, uvm, uwm, vwm.                                     */
+/* ---------------------------------------------------------------------- */
+typedef struct mf3d_tecbin_info {
+  int toti, totj, totk;      /* ttc extents                                */
+  int pl;                    /* ghost layers it was written with (the reader
+                                stops when they differ, initial.for:714-719) */
+  int inind, jnind, knind;   /* -1 where the block ends on a wall          */
+  long long records;         /* toti*totj*totk                             */
+  long long data_offset;     /* byte offset of the first cell record (52)  */
+} mf3d_tecbin_info;
+
+/* Checks the three header records of a file image (host memory, `nbytes`
+ * long) and that its size is exactly the cell records they announce. */
+int mf3d_tecbin_info_of(const void *image, size_t nbytes, mf3d_tecbin_info *info);
+
+/* Bytes of the file image for these extents (-1 if an extent is < 1). */
+long long mf3d_tecbin_size(int toti, int totj, int totk);
+
+/* The reader: `image` is a whole file image in device memory; out[16] are
+ * device arrays of info->records doubles receiving p, pm, ppm, vis, u, um,
+ * uum, v, vm, vvm, w, wm, wwm, uvm, uwm, vwm (initial.for:718-733), a NULL
+ * entry skipping its field.  Every cell record's framing is checked:
+ * MF3D_E_INVALID names the first bad record.  Synchronous on `device`. */
+int mf3d_tecbin_decode_device(const void *image, const mf3d_tecbin_info *info, double *const *out, int device);
+
+/* The writer: the file image of mf3d_tecbin_size bytes into device memory
+ * `image` from the node coordinates x[toti], y[totj], z[totk] and the 16
+ * fields in the reader's order (device arrays, NULL = zeros). */
+int mf3d_tecbin_encode_device(int toti, int totj, int totk, int pl, int inind, int jnind, int knind,
+                              const double *x, const double *y, const double *z, const double *const *fields,
+                              void *image, int device);
+
 #ifdef __cplusplus
 }
 #endif

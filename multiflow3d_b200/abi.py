@@ -99,6 +99,18 @@ class Fields(C.Structure):
     ]
 
 
+class TecbinInfo(C.Structure):
+    """``mf3d_tecbin_info`` - the header of a restart file."""
+
+    _fields_ = [
+        ("toti", C.c_int), ("totj", C.c_int), ("totk", C.c_int),
+        ("pl", C.c_int),
+        ("inind", C.c_int), ("jnind", C.c_int), ("knind", C.c_int),
+        ("records", C.c_longlong),
+        ("data_offset", C.c_longlong),
+    ]
+
+
 class SolveInfo(C.Structure):
     """``mf3d_solve_info``."""
 
@@ -143,6 +155,10 @@ EXPORTED_SYMBOLS = (
     "mf3d_server_clock",
     "mf3d_server_profile",
     "mf3d_server_destroy",
+    "mf3d_tecbin_info_of",
+    "mf3d_tecbin_size",
+    "mf3d_tecbin_decode_device",
+    "mf3d_tecbin_encode_device",
 )
 
 MF3D_NOALLOC_MAX_BLOCKS = 512
@@ -190,6 +206,11 @@ def _declare(lib):
     lib.mf3d_server_clock.restype = C.c_double
     lib.mf3d_server_clock.argtypes = []
     lib.mf3d_server_destroy.argtypes = [vp]
+    lib.mf3d_tecbin_info_of.argtypes = [vp, C.c_size_t, C.POINTER(TecbinInfo)]
+    lib.mf3d_tecbin_size.restype = C.c_longlong
+    lib.mf3d_tecbin_size.argtypes = [C.c_int] * 3
+    lib.mf3d_tecbin_decode_device.argtypes = [vp, C.POINTER(TecbinInfo), C.POINTER(vp), C.c_int]
+    lib.mf3d_tecbin_encode_device.argtypes = [C.c_int] * 7 + [vp] * 3 + [C.POINTER(vp), vp, C.c_int]
     lib.mf3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                       C.POINTER(C.c_double)]
     return lib

@@ -1912,3 +1912,5 @@ long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid, i
 
 // Serving (request loop over this engine).
 #include "server.cuh"
+// Restart files of the reference, decoded and encoded on the device.
+#include "tecbin.cuh"
