@@ -499,6 +499,62 @@ def run_density(args):
     return 0
 
 
+def run_sip(args):
+    """solver 1 (pressure_1sweep with Stone's SIP): 2x2x2 blocks of 32^3
+    (64^3), periodic x and z, walls in y, 4 SIP sweeps per call, rel tol
+    1e-8, FP64.  CPU baseline: the oracle on the same inputs, 8 threads,
+    the whole solve."""
+    import numpy as np
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.abi import SolveInfo
+    from multiflow3d_b200.problems import Problem, fields_struct
+    from multiflow3d_b200.solver import Projection
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    h = 1.0 / 64
+    pr = Problem(2, 2, 2, 32, 32, 32, ngrid=1, pl=1, dx=h, dy=h, dz=h)
+    host = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    keys = ("ustar", "vstar", "wstar", "u", "v", "w", "p")
+    d = [{k: torch.from_numpy(f[k]).to(dev) for k in keys} for f in host]
+    pristine = [{k: f[k].clone() for k in ("u", "v", "w", "p")} for f in d]
+
+    def reset():
+        for f, p0 in zip(d, pristine):
+            for k in ("u", "v", "w", "p"):
+                f[k].copy_(p0[k])
+
+    prm = pr.params(maxcy=2000, eps=1e-8, solver=1, nswp=4)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    sec, r = _timed_solves(lambda: proj.newsolv_mg_device(d), reset, args.steps, args.warmup)
+    proj.close()
+    value = args.steps / sec
+    line = {
+        "metric": "poisson_solves_per_s_sip", "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "solver 1 (SIP), 2x2x2 blocks of 32^3 (64^3), periodic x z, walls y, nswp 4, "
+                               "rel tol 1e-8"},
+        "sip_calls": r.iter, "status": r.status,
+    }
+    if not args.no_cpu_baseline:
+        import time
+        orc = oracle_lib()
+        threads = max(1, min(os.cpu_count() or 1, pr.nblocks))
+        orc.orc_set_threads(threads)
+        blocks = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+        info = SolveInfo()
+        t = time.perf_counter()
+        orc.orc_newsolv_mg(pr.descriptors(orc), pr.nblocks, C.byref(prm), fields_struct(blocks), 1.0, 1.0,
+                           C.byref(info), None, 0)
+        cpu = 1.0 / (time.perf_counter() - t)
+        line["cpu_baseline"] = {"value": cpu, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": "the same solve on the oracle (the SIP sweeps are serial per block)"}
+        line["speedup_vs_cpu"] = value / cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_tecbin(args):
     """Restart files (post.for:496-548 / initial.for:689-760): decode the
     file images of the default workload's 8 blocks (ttc 132^3 each, 0.44 GB
@@ -772,7 +828,7 @@ def main():
     ap.add_argument("--impl", default="mf3d", choices=["mf3d", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="multiblock",
-                    choices=["multiblock", "mixed", "batched", "served", "density", "tecbin"],
+                    choices=["multiblock", "mixed", "batched", "served", "density", "tecbin", "sip"],
                     help="multiblock: the default FP64 line; mixed / batched / served / density: the further "
                          "workloads (1 GPU)")
     ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
@@ -790,6 +846,8 @@ def main():
         return run_density(args)
     if args.workload == "tecbin":
         return run_tecbin(args)
+    if args.workload == "sip":
+        return run_sip(args)
     return run_gpu(args)
 
 

@@ -112,6 +112,11 @@ typedef struct mf3d_params {
                        Skipped when the solve diverged (the reference stops).
                        mf3d_create contexts only.  0: u, v, w face ghosts as
                        documented at mf3d_fields.                             */
+  int solver;       /* control.cin solver: 2 (or 0) multigrid newsolv_mg; 1
+                       pressure_1sweep with Stone's SIP (press.for:274-420,
+                       sipsol.for:2-206), maxcy playing niter.  FP64,
+                       mf3d_create contexts, no lsm.                          */
+  int nswp;         /* solver 1: SIP sweeps per call (control.cin nswp(4))    */
 } mf3d_params;
 
 /* Field pointers of one block, each a (ttc_i,ttc_j,ttc_k) array.

@@ -86,6 +86,8 @@ class Params(C.Structure):
         ("pl_ex", C.c_int),
         ("lsm", C.c_int),
         ("bounds", C.c_int),
+        ("solver", C.c_int),
+        ("nswp", C.c_int),
     ]
 
 

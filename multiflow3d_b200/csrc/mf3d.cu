@@ -617,6 +617,10 @@ struct View {
 
 using namespace mf3d;
 
+namespace mf3d {
+struct SipState;
+}
+
 struct mf3d_ctx {
   mf3d_params prm;
   int device = 0;
@@ -636,6 +640,9 @@ struct mf3d_ctx {
   std::vector<double> prof_pending_bytes;
   double prof_ms = 0.0, prof_bytes = 0.0;
   long long prof_n = 0;
+  // solver 1 (SIP): factors, residual, the substitution graph
+  std::unique_ptr<mf3d::SipState> sip;
+  long long sip_sweeps = 0;
   // host entry point mirrors
   DevBuf<double> mirror;
   std::vector<size_t> mirror_off;
@@ -1423,6 +1430,10 @@ static int solve_view(mf3d_ctx *C, View &V, const double *dt, const double *alfa
   return res;
 }
 
+}  // namespace mf3d
+#include "sip.cuh"
+namespace mf3d {
+
 template <typename T>
 static int mgkcyc_view(mf3d_ctx *C, View &V, double *const *su, double *const *pp) {
   cudaStream_t s = C->stream;
@@ -1516,6 +1527,14 @@ static int check_params(const mf3d_params *prm) {
   if (prm->differencing != 1) { set_error("differencing != 1 (4th-order calmas) is not supported"); return MF3D_E_UNSUPPORTED; }
   if (prm->precision < 0 || prm->precision > 1) { set_error("precision mode not supported"); return MF3D_E_UNSUPPORTED; }
   if (prm->lsm && prm->precision != MF3D_PREC_FP64) { set_error("lsm runs in FP64 only"); return MF3D_E_UNSUPPORTED; }
+  if (prm->solver != 0 && prm->solver != 1 && prm->solver != 2) { set_error("solver must be 1 or 2"); return MF3D_E_INVALID; }
+  if (prm->solver == 1) {
+    if (prm->nswp < 1) { set_error("solver 1: nswp must be >= 1"); return MF3D_E_INVALID; }
+    if (prm->precision != MF3D_PREC_FP64 || prm->lsm) {
+      set_error("solver 1 (SIP) runs in FP64 without lsm");
+      return MF3D_E_UNSUPPORTED;
+    }
+  }
   return MF3D_OK;
 }
 
@@ -1575,6 +1594,10 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
           set_error("bounds: block " + std::to_string(d.id) + " has a face code other than 3, 4, 5");
           return MF3D_E_UNSUPPORTED;
         }
+    }
+    if (prm->solver == 1 && (d.hx || d.hy || d.hz)) {
+      set_error("solver 1 (SIP): uniform spacing only (pressure_1sweep, press.for:294-320)");
+      return MF3D_E_UNSUPPORTED;
     }
     if (prm->lsm && (d.hx || d.hy || d.hz)) {
       set_error("lsm: uniform spacing only (the reference's variable-density branch)");
@@ -1652,8 +1675,8 @@ static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params 
   if (!doms || nd <= 0 || !out) { set_error("mf3d_batch_create: bad arguments"); return MF3D_E_INVALID; }
   int st = check_params(prm);
   if (st) return st;
-  if (prm->lsm || prm->bounds) {
-    set_error("lsm and bounds: single-problem contexts (mf3d_create) only");
+  if (prm->lsm || prm->bounds || prm->solver == 1) {
+    set_error("lsm, bounds and solver 1: single-problem contexts (mf3d_create) only");
     return MF3D_E_UNSUPPORTED;
   }
   for (int d = 0; d < nd; ++d) {
@@ -1688,6 +1711,7 @@ static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params 
 
 static int run_solve(mf3d_ctx *C, const double *dt, const double *alfapr, mf3d_solve_info *infos, double *hist,
                      int hcap) {
+  if (C->prm.solver == 1) return solve_view_sip(C, *C->view, dt, alfapr, infos, hist, hcap);
   if (C->elem == 8) return solve_view<double>(C, *C->view, dt, alfapr, infos, hist, hcap);
   return solve_view<float>(C, *C->view, dt, alfapr, infos, hist, hcap);
 }

@@ -439,8 +439,8 @@ int mf3d_server_create(const mf3d_params *prm, double mem_cap_bytes, int max_res
     set_error("mf3d_server_create: bad arguments");
     return MF3D_E_INVALID;
   }
-  if (prm->lsm || prm->bounds) {
-    set_error("lsm and bounds: single-problem contexts (mf3d_create) only");
+  if (prm->lsm || prm->bounds || prm->solver == 1) {
+    set_error("lsm, bounds and solver 1: single-problem contexts (mf3d_create) only");
     return MF3D_E_UNSUPPORTED;
   }
   mf3d_params p = *prm;

@@ -95,6 +95,9 @@ struct Ctx {
   int ngrd_gl, mg_itrsch, irestr, iproln, maxcy, pl, pl_ex;
   bool lsm; /* L_LSM: variable-density coefficients, calvel and rhs */
   bool bounds; /* boundu/boundv/boundw after the loop (newsolv_mg.for:86-88) */
+  int solver;   /* 2: multigrid newsolv_mg; 1: pressure_1sweep with SIP */
+  int nswp;     /* SIP inner sweeps per call (control.cin nswp(4)) */
+  long long sip_sweeps; /* nsweeps: inner sweeps run over the solve */
   double eps;
   int eps_relative;
   bool periodic;
@@ -702,7 +705,9 @@ void mgkcyc(Ctx &C) {
 /* for p (exchange.for:14-20); calvel and calmas with differencing = 1  */
 /* read layer 0 only, the others are outputs of the final calvel.       */
 /* ------------------------------------------------------------------ */
-double *field_of(Blk &B, int op) { return op == 1 ? B.u : op == 2 ? B.v : op == 3 ? B.w : B.p; }
+double *field_of(Blk &B, int op) {
+  return op == 1 ? B.u : op == 2 ? B.v : op == 3 ? B.w : op == 44 ? B.pp.data() : B.p;
+}
 void franges(Blk &B, int op, int &is, int &ie, int &js, int &je, int &ks, int &ke) {
   if (op == 1) { is = B.isu; ie = B.ieu; js = B.jsu; je = B.jeu; ks = B.ksu; ke = B.keu; }
   else if (op == 2) { is = B.isv; ie = B.iev; js = B.jsv; je = B.jev; ks = B.ksv; ke = B.kev; }
@@ -827,7 +832,7 @@ void exchange_smlvl_faces(Ctx &C, int op, int nly) {
 }
 
 void exchange(Ctx &C, int op) {
-  const int nly = op == 4 ? 0 : C.pl_ex;
+  const int nly = (op == 4 || op == 44) ? 0 : C.pl_ex;
   if (C.periodic) exchange_bc(C, op, nly);
   exchange_smlvl_faces(C, op, nly);
 }
@@ -1009,6 +1014,149 @@ int newsolv_mg(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
   return status;
 }
 
+/* ------------------------------------------------------------------ */
+/* solver = 1: pressure_1sweep (press.for:274-420) with Stone's SIP      */
+/* (sipsol.for:2-206, ifi = 44), every block on one rank.                */
+/* ------------------------------------------------------------------ */
+/* The per-cell coefficients pressure_1sweep sets (press.for:294-320):
+ * 1/(dx*dx) etc., zeroed on Neumann faces, ap = -(sum) in order. */
+struct SipCoef { double aw, ae, as, an, ab, at, ap; };
+SipCoef sip_coef(const Blk &B, int i, int j, int k) {
+  SipCoef c;
+  c.aw = 1.0 / (B.d.dx * B.d.dx); c.ae = 1.0 / (B.d.dx * B.d.dx);
+  c.an = 1.0 / (B.d.dy * B.d.dy); c.as = 1.0 / (B.d.dy * B.d.dy);
+  c.at = 1.0 / (B.d.dz * B.d.dz); c.ab = 1.0 / (B.d.dz * B.d.dz);
+  if (B.d.iprev < 0 && B.d.bc_west != 5 && i == B.isp) c.aw = 0.0;
+  if (B.d.inext < 0 && B.d.bc_east != 5 && i == B.iep) c.ae = 0.0;
+  if (B.d.jprev < 0 && B.d.bc_south != 5 && j == B.jsp) c.as = 0.0;
+  if (B.d.jnext < 0 && B.d.bc_north != 5 && j == B.jep) c.an = 0.0;
+  if (B.d.kprev < 0 && B.d.bc_bottom != 5 && k == B.ksp) c.ab = 0.0;
+  if (B.d.knext < 0 && B.d.bc_top != 5 && k == B.kep) c.at = 0.0;
+  c.ap = -1.0 * (c.aw + c.ae + c.as + c.an + c.ab + c.at);
+  return c;
+}
+
+/* sipsol(44): the ILU factors (recomputed at every call, as the reference
+ * does), then up to nswp sweeps of residual, forward and backward
+ * substitution, each followed by exchange(44); the sweep loop stops when
+ * the summed |residual| falls to 0.001 of the first sweep's or changes by
+ * at most 1e-5 of it between sweeps.  Arrays indexed as the reference:
+ * ijk = j + (i-1)*nj + (k-1)*nij over the ghost-inclusive box, j fastest,
+ * zero outside the interior. */
+void sipsol44(Ctx &C) {
+  const double alfa = 0.92, small = 1e-20;
+  size_t nmax = 0;
+  for (auto &B : C.b) nmax = std::max(nmax, (size_t)B.ttc_i * B.ttc_j * B.ttc_k);
+  size_t nb = C.b.size();
+  std::vector<double> ue(nb * (nmax + 1), 0.0), un(ue), ut(ue), lw(ue), ls(ue), lb(ue), lpr(ue), res(ue);
+  for (size_t ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    const long nj = B.ttc_j, nij = (long)B.ttc_i * B.ttc_j;
+    const size_t o = ib * (nmax + 1);
+    for (int k = B.ksp; k <= B.kep; ++k) for (int i = B.isp; i <= B.iep; ++i) for (int j = B.jsp; j <= B.jep; ++j) {
+      const long ijk = j + (long)(i - 1) * nj + (long)(k - 1) * nij;
+      const SipCoef c = sip_coef(B, i, j, k);
+      const size_t q = o + ijk;
+      lb[q] = c.ab / (1. + alfa * (un[q - nij] + ue[q - nij]));
+      lw[q] = c.aw / (1. + alfa * (un[q - nj] + ut[q - nj]));
+      ls[q] = c.as / (1. + alfa * (ue[q - 1] + ut[q - 1]));
+      const double p1 = alfa * (lb[q] * un[q - nij] + lw[q] * un[q - nj]);
+      const double p2 = alfa * (lb[q] * ue[q - nij] + ls[q] * ue[q - 1]);
+      const double p3 = alfa * (lw[q] * ut[q - nj] + ls[q] * ut[q - 1]);
+      lpr[q] = 1. / (c.ap + p1 + p2 + p3 - lb[q] * ut[q - nij] - lw[q] * ue[q - nj] - ls[q] * un[q - 1] + small);
+      un[q] = (c.an - p1) * lpr[q];
+      ue[q] = (c.ae - p2) * lpr[q];
+      ut[q] = (c.at - p3) * lpr[q];
+    }
+  }
+  double relast = 0.0, res1 = 0.0;
+  int nsweep;
+  bool stop = false;
+  for (nsweep = 1; nsweep <= C.nswp; ++nsweep) {
+    double resab = 0.0;
+    for (size_t ib = 0; ib < nb; ++ib) {
+      Blk &B = C.b[ib];
+      double *fi = B.pp.data(), *su = B.su.data();
+      const long nj = B.ttc_j, nij = (long)B.ttc_i * B.ttc_j;
+      const size_t o = ib * (nmax + 1);
+      for (int k = B.ksp; k <= B.kep; ++k) for (int i = B.isp; i <= B.iep; ++i) for (int j = B.jsp; j <= B.jep; ++j) {
+        const size_t q = o + j + (long)(i - 1) * nj + (long)(k - 1) * nij;
+        const SipCoef c = sip_coef(B, i, j, k);
+        res[q] = (F(B, su, i, j, k) - c.ap * F(B, fi, i, j, k) - c.an * F(B, fi, i, j + 1, k) -
+                  c.as * F(B, fi, i, j - 1, k) - c.ae * F(B, fi, i + 1, j, k) - c.aw * F(B, fi, i - 1, j, k) -
+                  c.ab * F(B, fi, i, j, k - 1) - c.at * F(B, fi, i, j, k + 1));
+        resab = resab + std::fabs(res[q]);
+      }
+      for (int k = B.ksp; k <= B.kep; ++k) for (int i = B.isp; i <= B.iep; ++i) for (int j = B.jsp; j <= B.jep; ++j) {
+        const size_t q = o + j + (long)(i - 1) * nj + (long)(k - 1) * nij;
+        res[q] = (res[q] - lb[q] * res[q - nij] - lw[q] * res[q - nj] - ls[q] * res[q - 1]) * lpr[q];
+      }
+      for (int k = B.kep; k >= B.ksp; --k) for (int i = B.iep; i >= B.isp; --i) for (int j = B.jep; j >= B.jsp; --j) {
+        const size_t q = o + j + (long)(i - 1) * nj + (long)(k - 1) * nij;
+        res[q] = res[q] - un[q] * res[q + 1] - ue[q] * res[q + nj] - ut[q] * res[q + nij];
+        F(B, fi, i, j, k) = F(B, fi, i, j, k) + res[q];
+      }
+    }
+    if (nsweep == 1) res1 = resab;
+    const double rsm = resab / (res1 + small);
+    exchange(C, 44);
+    const double reldif = std::fabs(rsm - relast);
+    relast = rsm;
+    if (rsm <= 0.001 || reldif <= 0.00001) { stop = true; break; }
+  }
+  if (!stop) nsweep = nsweep - 1; /* the loop variable ends at nswp+1 */
+  C.sip_sweeps += nsweep;
+}
+
+/* pressure_1sweep (press.for:274-420): calvel, then up to niter (= maxcy)
+ * rounds of calmas, the convergence test (rmax < eps and iter > 1), sipsol,
+ * p += pp, exchange(4), pbound, calvel.  hist[q] = rmax of the calmas that
+ * opens round q+2 (the last round, when the loop runs out, has none: the
+ * reported rmax and su are then those from before its sipsol, as in the
+ * reference); info.iter = SIP calls. */
+int pressure_1sweep(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
+  stamp(0);
+  for (auto &B : C.b) {
+    std::fill(B.pp.begin(), B.pp.end(), 0.0);
+    std::fill(B.su.begin(), B.su.end(), 0.0);
+  }
+  calvel(C);
+  calmas(C);
+  stamp(1);
+  const double rmax0 = C.rmax;
+  const double eps = C.eps_relative ? C.eps * rmax0 : C.eps;
+  C.sip_sweeps = 0;
+  int calls = 0;
+  bool conv = false;
+  for (int iter = 1; iter <= C.maxcy; ++iter) {
+    if (iter > 1) {
+      if (C.rmax < eps) { conv = true; break; }
+    }
+    sipsol44(C);
+    ++calls;
+    const double ppref = 0.0;
+    for (auto &B : C.b)
+      for (int k = B.ksp - 1; k <= B.kep + 1; ++k) for (int i = B.isp - 1; i <= B.iep + 1; ++i) for (int j = B.jsp - 1; j <= B.jep + 1; ++j) {
+        F(B, B.p, i, j, k) = (F(B, B.p, i, j, k) + (F(B, B.pp.data(), i, j, k) - ppref));
+        F(B, B.pp.data(), i, j, k) = 0.0;
+      }
+    exchange(C, 4);
+    pbound(C);
+    calvel(C);
+    stamp(calls + 1);
+    if (iter == C.maxcy) break; /* `if (iter.lt.niter) goto 1000` fails: no further calmas */
+    calmas(C); /* the next round starts with it (press.for:323) */
+    if (hist && calls - 1 < cap) hist[calls - 1] = C.rmax;
+  }
+  int status = conv ? MF3D_OK : MF3D_NOT_CONVERGED;
+  if (C.rmax > 100.0) status = MF3D_DIVERGED;
+  if (C.bounds && status != MF3D_DIVERGED) { bound(C, 1); bound(C, 2); bound(C, 3); }
+  if (info) {
+    info->rmax = C.rmax; info->rmax0 = rmax0; info->iter = calls; info->status = status; info->ms_device = 0.0;
+  }
+  return status;
+}
+
 std::string g_err;
 
 int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm) {
@@ -1021,6 +1169,9 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
   if (C.pl_ex < 0 || C.pl_ex >= C.pl) { g_err = "pl_ex"; return MF3D_E_INVALID; }
   C.lsm = prm->lsm != 0;
   C.bounds = prm->bounds != 0;
+  C.solver = prm->solver == 1 ? 1 : 2;
+  C.nswp = prm->nswp;
+  if (C.solver == 1 && (C.nswp < 1 || C.lsm)) { g_err = "solver 1: nswp >= 1, no lsm"; return MF3D_E_INVALID; }
   C.periodic = false;
   C.b.resize(nb);
   for (int ib = 0; ib < nb; ++ib) {
@@ -1090,7 +1241,7 @@ int orc_newsolv_mg(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
     B.dens = fields[ib].dens;
     if (C.lsm && !B.dens) { g_err = "L_LSM needs dens"; return MF3D_E_INVALID; }
   }
-  st = newsolv_mg(C, hist, cap, info);
+  st = C.solver == 1 ? pressure_1sweep(C, hist, cap, info) : newsolv_mg(C, hist, cap, info);
   for (int ib = 0; ib < nb; ++ib)
     if (fields[ib].su) std::memcpy(fields[ib].su, C.b[ib].su.data(), C.b[ib].su.size() * sizeof(double));
   return st;

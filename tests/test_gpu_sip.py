@@ -1,0 +1,54 @@
+"""solver 1: pressure_1sweep with Stone's SIP (press.for:274-420,
+sipsol.for:2-206) on the GPU against the oracle, FP64, bit for bit:
+hyperplane launches reproduce the reference's recurrences exactly.  The
+summed |residual| that steers the sweep loop is reduced in another order
+than the reference's serial sum; the stopping decisions, and with them
+every array, agree unless a ratio lies within rounding of a threshold."""
+import numpy as np
+import pytest
+
+from multiflow3d_b200.problems import Problem, PERIODIC, WALL
+from test_gpu_edges import run_both, assert_same
+
+pytestmark = pytest.mark.gpu
+P, W, S = PERIODIC, WALL, 3
+
+CASES = {
+    "1 block, periodic x z, walls y": (lambda: Problem(1, 1, 1, 16, 16, 16, ngrid=1, pl=1), 4, 300),
+    "2x2x1, periodic x y, one sweep per call": (
+        lambda: Problem(2, 2, 1, 16, 16, 8, bc=(P, P, P, P, W, W), ngrid=1, pl=2), 1, 400),
+    "2x1x2 walls, ten sweeps per call": (lambda: Problem(2, 1, 2, 8, 16, 8, bc=(W,) * 6, ngrid=1, pl=1), 10, 200),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_sip_matches_oracle(lib, oracle, cuda, case):
+    make, nswp, maxcy = CASES[case]
+    pr = make()
+    prm = pr.params(maxcy=maxcy, eps=1e-9, solver=1, nswp=nswp)
+    o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm,
+                    pr.block_fields(seed=41, fourier_modes=2))
+    assert o[0] == 0
+    assert_same(o, g, pr.pl)
+
+
+def test_sip_runs_out_of_rounds(lib, oracle, cuda):
+    """maxcy (niter) rounds without convergence: no calmas after the last
+    round, as in the reference; the arrays still agree bit for bit."""
+    pr = Problem(2, 1, 1, 16, 8, 8, ngrid=1, pl=2)
+    prm = pr.params(maxcy=5, eps=1e-12, solver=1, nswp=2)
+    o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm,
+                    pr.block_fields(seed=42, fourier_modes=2))
+    assert o[0] == 1
+    assert_same(o, g, pr.pl)
+
+
+def test_sip_with_bounds(lib, oracle, cuda):
+    pr = Problem(1, 1, 1, 16, 8, 8, bc=(P, P, W, W, S, S), ngrid=1, pl=2)
+    prm = pr.params(maxcy=200, eps=1e-9, solver=1, nswp=3, pl_ex=1, bounds=1)
+    o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm,
+                    pr.block_fields(seed=43, fourier_modes=2))
+    assert_same(o, g, pr.pl, 1)
+    ref, got = o[3], g[1]
+    for k in ("u", "v", "w"):
+        assert np.array_equal(got[0][k], ref[0][k]), k

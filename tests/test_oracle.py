@@ -311,3 +311,22 @@ def test_bounds_rejects_other_codes(oracle):
     pr = Problem(1, 1, 1, 8, 8, 8, bc=(1, 2, WALL, WALL, WALL, WALL), ngrid=2, pl=1)
     st, _, _ = solve(oracle, pr, pr.block_fields(seed=1), maxcy=2, bounds=1)
     assert st == -6  # MF3D_E_UNSUPPORTED: inflow / outflow codes are not restated
+
+
+@pytest.mark.parametrize("nswp", [1, 4])
+def test_sip_solver_reaches_the_multigrid_projection(oracle, nswp):
+    """solver 1 (pressure_1sweep with Stone's SIP, press.for:274-420 and
+    sipsol.for) and the multigrid solver converge to the same projection:
+    pressure (up to its constant) and velocities within the tolerance."""
+    pr = Problem(2, 1, 1, 16, 16, 16, ngrid=3, pl=1)
+    a = pr.block_fields(seed=3)
+    b = [{k: v.copy() for k, v in f.items()} for f in a]
+    st_a, info_a, _ = solve(oracle, pr, a, maxcy=400, eps=1e-10)
+    st_b, info_b, hist_b = solve(oracle, pr, b, maxcy=800, eps=1e-10, solver=1, nswp=nswp)
+    assert st_a == 0 and st_b == 0
+    assert info_b.rmax0 == info_a.rmax0
+    assert hist_b[-1] < 1e-10 * info_b.rmax0
+    pa, pb = demean(pr.gather(a, "p")), demean(pr.gather(b, "p"))
+    assert np.abs(pb - pa).max() <= 1e-7 * np.abs(pa).max()
+    for k in ("u", "v", "w"):
+        assert np.abs(pr.gather(b, k) - pr.gather(a, k)).max() <= 1e-8
