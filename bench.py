@@ -147,6 +147,27 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(x: float, device=None) -> float:
+    """The largest of every rank's x (one all-reduce; x itself alone).
+    Replicas only: ranks never exchange data, so the whole job takes as long
+    as its slowest rank."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(steps: int, seconds: float, device=None) -> float:
+    """Whole-job throughput of N independent replicas: N * steps over the
+    slowest rank's time."""
+    import torch.distributed as dist
+    world = dist.get_world_size() if (dist.is_available() and dist.is_initialized()) else 1
+    return world * steps / max_over_ranks(seconds, device)
+
+
 def oracle_lib():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bridge
@@ -254,13 +275,6 @@ def run_gpu(args):
         if world > 1:
             torch.distributed.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
-
     for _ in range(args.warmup):
         reset()
         r = proj.newsolv_mg_device(d)
@@ -285,7 +299,7 @@ def run_gpu(args):
     barrier()
     clocks.stop()
     ms = ev0.elapsed_time(ev1)
-    ms_max = max_over_ranks(ms)
+    ms_max = max_over_ranks(ms, dev)
     value = world * args.steps / (ms_max / 1e3)
 
     # ---- kernel timing: one more solve per kernel class, each launch of the
@@ -324,7 +338,7 @@ def run_gpu(args):
         t1 = time.perf_counter()
         if step > 0:  # first call allocates the library's device mirrors
             e2e_s += t1 - t0
-    e2e_s = max_over_ranks(e2e_s)
+    e2e_s = max_over_ranks(e2e_s, dev)
     e2e_value = world * n_e2e / e2e_s
     ttc = int(np.prod(pr.ttc))
     h2d = 7 * ttc * 8 * pr.nblocks
@@ -569,7 +583,7 @@ def run_tecbin(args):
     import tecbin as orc_tb
     lib = abi.load()
     dev = torch.device("cuda:0")
-    n, nblk = 132, 8
+    n, nblk = 132, args.files
     rng = np.random.default_rng(SEED)
     fields = {f: rng.standard_normal((n, n, n)) for f in orc_tb.FIELDS}
     xyz = tuple((np.arange(n) - 2) / 256.0 for _ in range(3))
@@ -833,6 +847,7 @@ def main():
                          "workloads (1 GPU)")
     ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
     ap.add_argument("--requests", type=int, default=200, help="served: requests per rate")
+    ap.add_argument("--files", type=int, default=8, help="tecbin: restart files decoded per step")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
