@@ -576,24 +576,26 @@ def run_tecbin(args):
     images resident in HBM; e2e: the same from pinned host memory, copy
     included.  CPU baseline: the numpy restatement of the reader
     (oracle/tecbin.py) on one block."""
-    import numpy as np
     import torch
     from multiflow3d_b200 import abi
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import tecbin as orc_tb
     lib = abi.load()
     dev = torch.device("cuda:0")
     n, nblk = 132, args.files
-    rng = np.random.default_rng(SEED)
-    fields = {f: rng.standard_normal((n, n, n)) for f in orc_tb.FIELDS}
-    xyz = tuple((np.arange(n) - 2) / 256.0 for _ in range(3))
-    host_img = orc_tb.write(n, n, n, 2, 0, -1, 0, *xyz, fields)
-    nbytes = len(host_img)
+    # the synthetic restart image, written by the library's own encoder
+    g = torch.Generator(device=dev).manual_seed(SEED)
+    fields = [torch.randn((n, n, n), dtype=torch.float64, device=dev, generator=g) for _ in range(16)]
+    xyz = [(torch.arange(n, dtype=torch.float64, device=dev) - 2) / 256.0 for _ in range(3)]
+    nbytes = int(lib.mf3d_tecbin_size(n, n, n))
+    img0 = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+    fptr = (C.c_void_p * 16)(*[t.data_ptr() for t in fields])
+    assert lib.mf3d_tecbin_encode_device(n, n, n, 2, 0, -1, 0, *[C.c_void_p(t.data_ptr()) for t in xyz], fptr,
+                                         C.c_void_p(img0.data_ptr()), 0) == 0
+    pinned = img0.cpu().pin_memory()
+    host_img = pinned.numpy().tobytes()
     info = abi.TecbinInfo()
     assert lib.mf3d_tecbin_info_of(host_img, nbytes, C.byref(info)) == 0
-    pinned = torch.from_numpy(np.frombuffer(host_img, dtype=np.uint8).copy()).pin_memory()
-    imgs = [pinned.to(dev) for _ in range(nblk)]
-    outs = [torch.empty((n, n, n), dtype=torch.float64, device=dev) for _ in orc_tb.FIELDS]
+    imgs = [img0] + [pinned.to(dev) for _ in range(nblk - 1)]
+    outs = [torch.empty((n, n, n), dtype=torch.float64, device=dev) for _ in range(16)]
     ptrs = (C.c_void_p * 16)(*[o.data_ptr() for o in outs])
 
     def decode(img):
@@ -640,6 +642,8 @@ def run_tecbin(args):
     }
     if not args.no_cpu_baseline:
         import time
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import tecbin as orc_tb
         t = time.perf_counter()
         orc_tb.read(host_img)
         cpu = nbytes / (time.perf_counter() - t) / 1e9
