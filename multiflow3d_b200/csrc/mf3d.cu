@@ -629,6 +629,12 @@ struct mf3d_ctx {
   int nsm = 148;            // SMs of the device
   int sweep_occ = 4;        // resident sweep CTAs per SM
   cudaStream_t stream = nullptr;
+  // host entry point: u, v, w travel on a side stream while the solve runs
+  // (only the final calvel needs them); their wall values go straight into
+  // the face planes first
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_side = nullptr;
+  bool walls_given = false, wait_side = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long long launches = 0;
   std::vector<std::unique_ptr<DomainStore>> doms;
@@ -1294,7 +1300,7 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
   CK(cudaStreamSynchronize(s));  // hs is a local
   CK(cudaMemsetAsync(V.rmax.p, 0, nd * sizeof(unsigned long long), s));
   if (C->prm.lsm) lsm_coefficients(C, V);
-  launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p);
+  launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p, C->walls_given ? 1 : 0);
   calvel_calmas<T>(C, V, V.ones.p, V.rmax.p, 0);
   launch(k_dom_init, 1, 256, 0, s, V.ds.p, nd, V.rmax.p, V.act.p);
   C->launches += 3;
@@ -1324,6 +1330,7 @@ static int solve_end(mf3d_ctx *C, View &V) {
     calvel_calmas<T>(C, V, V.ones.p, V.rmax_scratch.p, 1);
     ++C->launches;
   }
+  if (C->wait_side) CK(cudaStreamWaitEvent(s, C->ev_side, 0));  // the host entry's u, v, w
   launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, nullptr);
   C->launches += 1;
   if (C->prm.bounds) {
@@ -1730,27 +1737,80 @@ static int host_solve(mf3d_ctx *C, const mf3d_fields *fields, const double *dt, 
     for (int b = 0; b < nb; ++b) { C->mirror_off[b] = tot; tot += arrays * ttc_elems(pl, V.blk[b]->d); }
     int st = C->mirror.alloc(tot);
     if (st) return st;
+    CK(cudaStreamSynchronize(s));  // the side stream writes into it too
+  }
+  // ustar, vstar, wstar, p (and dens) on the solve stream.  u, v, w are
+  // read only by the final calvel (and boundu/v/w), so they travel on a
+  // side stream while the solve runs; the solve waits for them just before
+  // that calvel.  Their wall values - all the solve reads of them earlier,
+  // through the face planes - go straight from the caller's arrays into
+  // those planes on the solve stream.
+  if (!C->side) {
+    CK(cudaStreamCreateWithFlags(&C->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&C->ev_side, cudaEventDisableTiming));
+  }
+  for (int b = 0; b < nb; ++b) {  // every pointer before any copy is queued
+    const mf3d_fields &f = fields[b];
+    if (!f.ustar || !f.vstar || !f.wstar || !f.u || !f.v || !f.w || !f.p) {
+      set_error("mf3d_fields: a required pointer is NULL");
+      return MF3D_E_INVALID;
+    }
+    if (C->prm.lsm && !f.dens) { set_error("mf3d_fields: dens is NULL under lsm"); return MF3D_E_INVALID; }
   }
   std::vector<mf3d_fields> dev(nb);
   for (int b = 0; b < nb; ++b) {
     const size_t n = ttc_elems(pl, V.blk[b]->d);
     double *m = C->mirror.p + C->mirror_off[b];
     double *const hsrc[7] = {fields[b].ustar, fields[b].vstar, fields[b].wstar, fields[b].u, fields[b].v, fields[b].w, fields[b].p};
-    for (int q = 0; q < 7; ++q) {
-      if (!hsrc[q]) { set_error("mf3d_fields: a required pointer is NULL"); return MF3D_E_INVALID; }
-      CK(cudaMemcpyAsync(m + q * n, hsrc[q], n * sizeof(double), cudaMemcpyHostToDevice, s));
-    }
+    for (int q = 0; q < 7; ++q)
+      CK(cudaMemcpyAsync(m + q * n, hsrc[q], n * sizeof(double), cudaMemcpyHostToDevice,
+                         (q >= 3 && q <= 5) ? C->side : s));
     dev[b] = mf3d_fields{m, m + n, m + 2 * n, m + 3 * n, m + 4 * n, m + 5 * n, m + 6 * n,
                          fields[b].su ? m + 7 * n : nullptr, nullptr};
     if (C->prm.lsm) {
-      if (!fields[b].dens) { set_error("mf3d_fields: dens is NULL under lsm"); return MF3D_E_INVALID; }
       CK(cudaMemcpyAsync(m + 8 * n, fields[b].dens, n * sizeof(double), cudaMemcpyHostToDevice, s));
       dev[b].dens = m + 8 * n;
     }
+    // the wall planes of the normal velocity component, interior tangential
+    // range, into lo / hi as k_face_planes lays them out
+    const BlkFld &F = V.hf[b];
+    const mf3d_block_desc &d = V.blk[b]->d;
+    const size_t ti = d.nx + 2 * pl, tj = d.ny + 2 * pl;
+    for (int f = 0; f < 6; ++f) {
+      if (!F.wall[f]) continue;
+      const int ax = f / 2, side = f & 1;
+      const double *vel = ax == 0 ? fields[b].u : ax == 1 ? fields[b].v : fields[b].w;
+      const int g = side ? (ax == 0 ? d.nx : ax == 1 ? d.ny : d.nz) : 0;  // local index of the wall face
+      double *dst = side ? F.hi[ax] : F.lo[ax];
+      // host element of local (i, j, k): (i+pl-1) + ti*((j+pl-1) + tj*(k+pl-1))
+      auto at = [&](int i, int j, int k) {
+        return vel + (size_t)(i + pl - 1) + ti * ((size_t)(j + pl - 1) + tj * (size_t)(k + pl - 1));
+      };
+      if (ax == 1) {  // rows of nx along i, one per k
+        CK(cudaMemcpy2DAsync(dst, d.nx * sizeof(double), at(1, g, 1), ti * tj * sizeof(double), d.nx * sizeof(double),
+                             d.nz, cudaMemcpyHostToDevice, s));
+      } else if (ax == 2) {  // rows of nx along i, one per j
+        CK(cudaMemcpy2DAsync(dst, d.nx * sizeof(double), at(1, 1, g), ti * sizeof(double), d.nx * sizeof(double),
+                             d.ny, cudaMemcpyHostToDevice, s));
+      } else {  // single values strided by ti along j and ti*tj along k
+        cudaMemcpy3DParms p3;
+        std::memset(&p3, 0, sizeof p3);
+        p3.srcPtr = make_cudaPitchedPtr((void *)at(g, 1, 1), ti * sizeof(double), sizeof(double), tj);
+        p3.dstPtr = make_cudaPitchedPtr(dst, sizeof(double), sizeof(double), d.ny);
+        p3.extent = make_cudaExtent(sizeof(double), d.ny, d.nz);
+        p3.kind = cudaMemcpyHostToDevice;
+        CK(cudaMemcpy3DAsync(&p3, s));
+      }
+    }
   }
+  CK(cudaEventRecord(C->ev_side, C->side));
+  C->walls_given = true;
+  C->wait_side = true;
   int st = bind_fields(C, V, dev.data());
-  if (st) return st;
-  st = run_solve(C, dt, alfapr, infos, hist, hcap);
+  if (!st) st = run_solve(C, dt, alfapr, infos, hist, hcap);
+  C->walls_given = false;
+  C->wait_side = false;
+  if (st < 0) cudaStreamSynchronize(C->side);  // no copy outlives the call
   if (st < 0 && st != MF3D_E_NONFINITE) return st;
   for (int b = 0; b < nb; ++b) {
     const size_t n = ttc_elems(pl, V.blk[b]->d);
@@ -1819,6 +1879,11 @@ int mf3d_destroy(mf3d_ctx *ctx) {
   if (!ctx) return MF3D_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
+  if (ctx->ev_side) cudaEventDestroy(ctx->ev_side);
   ctx->view.reset();
   ctx->doms.clear();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);

@@ -248,7 +248,9 @@ __global__ void k_vel_faces(const BlkFld *__restrict__ fl, const Tile *__restric
 // else the source block's ustar on its last face (exchange(1..3) hands over
 // that block's u); hi[a] = the caller's velocity on a high wall face
 // (localparameters.for:185-190 stops calvel one face short there).
-__global__ void k_face_planes(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles) {
+// walls_given: the wall values are already in lo/hi (the host entry point
+// copies them there straight from the caller's arrays) and are left alone.
+__global__ void k_face_planes(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles, int walls_given) {
   pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
@@ -267,7 +269,7 @@ __global__ void k_face_planes(const BlkFld *__restrict__ fl, const Tile *__restr
   // low face
   if (F.wall[fl0]) {
     long long e = ax == 0 ? fidx(F, 0, a, b) : ax == 1 ? fidx(F, a, 0, b) : fidx(F, a, b, 0);
-    F.lo[ax][o] = vel[e];
+    if (!walls_given) F.lo[ax][o] = vel[e];
   } else {
     const BlkFld &S = fl[F.src[fl0]];
     const double *st = ax == 0 ? S.ustar : ax == 1 ? S.vstar : S.wstar;
@@ -280,7 +282,7 @@ __global__ void k_face_planes(const BlkFld *__restrict__ fl, const Tile *__restr
   }
   // high face
   long long e = ax == 0 ? fidx(F, nx, a, b) : ax == 1 ? fidx(F, a, ny, b) : fidx(F, a, b, nz);
-  F.hi[ax][o] = F.wall[fh] ? vel[e] : 0.0;
+  if (!(F.wall[fh] && walls_given)) F.hi[ax][o] = F.wall[fh] ? vel[e] : 0.0;
 }
 
 // ---------------------------------------------------------------------------

@@ -152,7 +152,7 @@ static int srv_rebuild(mf3d_ctx *C, View &V, std::vector<SrvReq *> &res) {
   if (ncont < nd) {
     DevBuf<int> fmask;
     if ((st = fmask.upload(fresh, s))) return st;
-    launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p);
+    launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p, 0);
     calvel_calmas<T>(C, V, fmask.p, V.rmax.p, 0);
     launch(k_dom_init, 1, 256, 0, s, V.ds.p + ncont, nd - ncont, V.rmax.p + ncont, V.act.p + ncont);
     CK(cudaStreamSynchronize(s));  // fmask and the host vectors are locals
