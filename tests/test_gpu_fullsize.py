@@ -75,3 +75,44 @@ def test_mixed_precision_512x256x256(lib, cuda):
         out[name] = p - p.mean()
     err = float((out["mixed"] - out["fp64"]).norm() / out["fp64"].norm())
     assert err < 1e-8, err
+
+
+def test_fp64_1024cube_single_block(lib, cuda):
+    """The largest single block this layout holds in one GPU's memory with
+    room to spare: 1024^3 cells (ttc 1028^3, 1.09 G elements per field;
+    about 80 GB for the seven fields and the multigrid hierarchy), FP64,
+    8 levels, periodic x and z, walls in y, tol 1e-8.  Inputs are made on
+    the device (uniform random face velocities, mean removed, zero normal
+    velocity on the walls).  The reported rmax is recomputed bit for bit from
+    the returned velocities, slab by slab."""
+    import torch
+    n, pl = 1024, 2
+    pr = Problem(1, 1, 1, n, n, n, ngrid=8, pl=pl, dx=1 / n, dy=1 / n, dz=1 / n)
+    t = n + 2 * pl
+    g = torch.Generator(device=cuda).manual_seed(11)
+    f = {}
+    for k in ("ustar", "vstar", "wstar"):
+        a = torch.rand((t, t, t), dtype=torch.float64, device=cuda, generator=g).mul_(2).sub_(1)
+        a.sub_(a[pl:pl + n, pl:pl + n, pl:pl + n].mean())
+        f[k] = a
+    f["vstar"][:, pl - 1, :] = 0.0
+    f["vstar"][:, pl + n - 1, :] = 0.0
+    for k in ("u", "v", "w"):
+        f[k] = f[k + "star"].clone()
+    f["p"] = torch.zeros((t, t, t), dtype=torch.float64, device=cuda)
+    proj = Projection(pr.descriptors(lib), pr.params(maxcy=400, eps=1e-8), lib)
+    res = proj.newsolv_mg_device([f])
+    proj.close()
+    assert res.status == 0 and res.rmax < 1e-8 * res.rmax0
+    del f["ustar"], f["vstar"], f["wstar"], f["p"]
+    h = 1.0 / n
+    best = 0.0
+    for k0 in range(pl, pl + n, 128):
+        K = slice(k0, k0 + 128)
+        J, I = slice(pl, pl + n), slice(pl, pl + n)
+        u, v, w = f["u"], f["v"], f["w"]
+        fact = ((u[K, J, I] - u[K, J, pl - 1:pl + n - 1]) / h + (v[K, J, I] - v[K, pl - 1:pl + n - 1, I]) / h +
+                (w[K, J, I] - w[k0 - 1:k0 + 127, J, I]) / h)
+        best = max(best, float((fact * h * h * h).abs().max().item()))
+        del fact
+    assert best == res.rmax
