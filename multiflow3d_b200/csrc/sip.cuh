@@ -152,6 +152,131 @@ __global__ void k_sip_backward(const SipBlk *__restrict__ sb, const BlkLev *__re
   fi[e] = fi[e] + r;
 }
 
+// Both substitutions of a block in one CTA: its hyperplanes one after
+// another, a CTA barrier between them (a block's recurrences never reach
+// into another block).  For small blocks, where a hyperplane holds a few
+// thousand cells at most, this replaces 2*(nx+ny+nz-2) launches per sweep
+// by one; the per-cell arithmetic is k_sip_forward's and k_sip_backward's.
+__global__ void __launch_bounds__(1024) k_sip_subst_block(const SipBlk *__restrict__ sb,
+                                                          const BlkLev *__restrict__ bl) {
+  pdl_wait();
+  const SipBlk S = sb[blockIdx.x];
+  const BlkLev &B = bl[blockIdx.x];
+  double *fi = phi_of<double>(B);
+  const int hmax = S.nx + S.ny + S.nz, pairs = S.nx * S.ny;
+  for (int h = 3; h <= hmax; ++h) {
+    for (int q = threadIdx.x; q < pairs; q += blockDim.x) {
+      const int i = q % S.nx + 1, j = q / S.nx + 1, k = h - i - j;
+      if (k < 1 || k > S.nz) continue;
+      const long long c = sip_idx(S, i, j, k);
+      S.res[c] = (S.res[c] - S.lb[c] * S.res[sip_idx(S, i, j, k - 1)] - S.lw[c] * S.res[sip_idx(S, i - 1, j, k)] -
+                  S.ls[c] * S.res[sip_idx(S, i, j - 1, k)]) *
+                 S.lpr[c];
+    }
+    __syncthreads();
+  }
+  for (int h = hmax; h >= 3; --h) {
+    for (int q = threadIdx.x; q < pairs; q += blockDim.x) {
+      const int i = q % S.nx + 1, j = q / S.nx + 1, k = h - i - j;
+      if (k < 1 || k > S.nz) continue;
+      const long long c = sip_idx(S, i, j, k);
+      const double r = S.res[c] - S.un[c] * S.res[sip_idx(S, i, j + 1, k)] -
+                       S.ue[c] * S.res[sip_idx(S, i + 1, j, k)] - S.ut[c] * S.res[sip_idx(S, i, j, k + 1)];
+      S.res[c] = r;
+      const long long e = cell_off(B, i, j, k);
+      fi[e] = fi[e] + r;
+    }
+    __syncthreads();
+  }
+}
+
+// Blocks whose (i, j) plane holds at most this many cells take the one-CTA
+// substitution kernel; larger ones the hyperplane launches.
+constexpr int kSipBlockCells = 4096;
+
+// The same two substitutions with one thread per (i, j) column, for blocks
+// of at most 1024 columns.  At hyperplane h column (i, j) holds cell
+// k = h-i-j: the cell below is its own previous value (a register), and
+// the cells west and south (forward) or east and north (backward) at the
+// same k were formed by those columns one hyperplane earlier and wait in a
+// shared-memory plane.  Each hyperplane is then two CTA barriers and no
+// dependent global load; the operands of the next cell are loaded one step
+// ahead.  The arithmetic is the reference's, operand for operand.
+__global__ void __launch_bounds__(1024) k_sip_subst_col(const SipBlk *__restrict__ sb,
+                                                        const BlkLev *__restrict__ bl) {
+  pdl_wait();
+  extern __shared__ double plane[];  // (ny+2) x (nx+2), zero border
+  const SipBlk S = sb[blockIdx.x];
+  const BlkLev &B = bl[blockIdx.x];
+  double *fi = phi_of<double>(B);
+  const int nx = S.nx, ny = S.ny, nz = S.nz, px = nx + 2;
+  const int tid = threadIdx.x;
+  for (int q = tid; q < (ny + 2) * px; q += blockDim.x) plane[q] = 0.0;
+  const bool col = tid < nx * ny;
+  const int i = tid % nx + 1, j = tid / nx + 1;
+  const int hmax = nx + ny + nz;
+  __syncthreads();
+  // forward: res = (res - lb*res(k-1) - lw*res(i-1) - ls*res(j-1)) * lpr
+  double below = 0.0;
+  int kn = 3 - i - j;  // k at the next step
+  double nres = 0.0, nlb = 0.0, nlw = 0.0, nls = 0.0, nlpr = 0.0;
+  auto fetch_f = [&](int k) {
+    if (col && k >= 1 && k <= nz) {
+      const long long c = sip_idx(S, i, j, k);
+      nres = S.res[c]; nlb = S.lb[c]; nlw = S.lw[c]; nls = S.ls[c]; nlpr = S.lpr[c];
+    }
+  };
+  fetch_f(kn);
+  for (int h = 3; h <= hmax; ++h) {
+    const int k = h - i - j;
+    const bool act = col && k >= 1 && k <= nz;
+    double v = 0.0;
+    if (act) {
+      const double w = plane[j * px + i - 1], so = plane[(j - 1) * px + i];
+      v = (nres - nlb * below - nlw * w - nls * so) * nlpr;
+    }
+    fetch_f(k + 1);
+    __syncthreads();
+    if (act) {
+      plane[j * px + i] = v;
+      S.res[sip_idx(S, i, j, k)] = v;
+      below = v;
+    }
+    __syncthreads();
+  }
+  // backward: res = res - un*res(j+1) - ue*res(i+1) - ut*res(k+1); fi += res
+  for (int q = tid; q < (ny + 2) * px; q += blockDim.x) plane[q] = 0.0;
+  __syncthreads();
+  double above = 0.0;
+  double bres = 0.0, bun = 0.0, bue = 0.0, but = 0.0;
+  auto fetch_b = [&](int k) {
+    if (col && k >= 1 && k <= nz) {
+      const long long c = sip_idx(S, i, j, k);
+      bres = S.res[c]; bun = S.un[c]; bue = S.ue[c]; but = S.ut[c];
+    }
+  };
+  fetch_b(hmax - i - j);
+  for (int h = hmax; h >= 3; --h) {
+    const int k = h - i - j;
+    const bool act = col && k >= 1 && k <= nz;
+    double r = 0.0;
+    if (act) {
+      const double no = plane[(j + 1) * px + i], ea = plane[j * px + i + 1];
+      r = bres - bun * no - bue * ea - but * above;
+    }
+    fetch_b(k - 1);
+    __syncthreads();
+    if (act) {
+      plane[j * px + i] = r;
+      S.res[sip_idx(S, i, j, k)] = r;
+      const long long e = cell_off(B, i, j, k);
+      fi[e] = fi[e] + r;
+      above = r;
+    }
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
@@ -162,6 +287,7 @@ struct SipState {
   int n_ij = 0, hmax = 0;
   DevBuf<double> part, resab;
   cudaGraphExec_t sweep = nullptr;     // forward + backward substitutions
+  int subst_launches = 0;              // kernels in that graph
   ~SipState() {
     if (sweep) cudaGraphExecDestroy(sweep);
   }
@@ -200,16 +326,28 @@ static int sip_prepare(mf3d_ctx *C, View &V) {
   const BlkLev *L1 = V.lv[1].tab.p;
   for (int h = 3; h <= S->hmax; ++h)
     launch(k_sip_factor, S->n_ij, kTile, 0, s, S->sb.p, L1, S->t_ij.p, h);
-  // one graph per context for the two substitutions of a sweep
+  // one graph per context for the two substitutions of a sweep: one CTA
+  // per block when every block is small, else a launch per hyperplane
+  int maxpairs = 0;
+  for (const auto &b : hb) maxpairs = std::max(maxpairs, b.nx * b.ny);
   cudaGraph_t g = nullptr;
   CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-  for (int h = 3; h <= S->hmax; ++h) launch(k_sip_forward, S->n_ij, kTile, 0, s, S->sb.p, S->t_ij.p, h);
-  for (int h = S->hmax; h >= 3; --h) launch(k_sip_backward, S->n_ij, kTile, 0, s, S->sb.p, L1, S->t_ij.p, h);
+  int maxplane = 0;
+  for (const auto &b : hb) maxplane = std::max(maxplane, (b.nx + 2) * (b.ny + 2));
+  if (maxpairs <= 1024 && maxplane * 8 <= 48 * 1024) {
+    launch(k_sip_subst_col, nb, 1024, (size_t)maxplane * 8, s, S->sb.p, L1);
+  } else if (maxpairs <= kSipBlockCells) {
+    launch(k_sip_subst_block, nb, 1024, 0, s, S->sb.p, L1);
+  } else {
+    for (int h = 3; h <= S->hmax; ++h) launch(k_sip_forward, S->n_ij, kTile, 0, s, S->sb.p, S->t_ij.p, h);
+    for (int h = S->hmax; h >= 3; --h) launch(k_sip_backward, S->n_ij, kTile, 0, s, S->sb.p, L1, S->t_ij.p, h);
+  }
   CK(cudaStreamEndCapture(s, &g));
   const cudaError_t e = cudaGraphInstantiate(&S->sweep, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { set_error(std::string("SIP graph: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
   CK(cudaStreamSynchronize(s));
+  S->subst_launches = maxpairs <= kSipBlockCells ? 1 : 2 * (S->hmax - 2);
   C->launches += S->hmax - 2;
   C->sip = std::move(S);
   return MF3D_OK;
@@ -234,7 +372,7 @@ static int sip_solve(mf3d_ctx *C, View &V, int *sweeps) {
     double resab = 0.0;
     CK(cudaMemcpyAsync(&resab, S.resab.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    C->launches += 2 + 2 * (S.hmax - 2);
+    C->launches += 2 + S.subst_launches;
     n = sweep;
     if (sweep == 1) res1 = resab;
     const double rsm = resab / (res1 + kSipSmall);
