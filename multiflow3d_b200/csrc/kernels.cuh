@@ -475,6 +475,21 @@ __global__ void k_tdma(const BlkLev *__restrict__ bl, const int *__restrict__ bl
   }
 }
 
+// The first half-sweep of a red-black relaxation from zero (mgrelax
+// scheme 3 right after mgrestr, mgsolver.for:547-601): every neighbour is
+// zero, so a red cell becomes rhs / ap - the from-zero sweep's expression
+// (rhs - (aw*0 + ... + at*0)) / ap, bit for bit, since subtracting +0 leaves
+// rhs unchanged.  The restriction writes it as it forms the coarse rhs,
+// which spares the coarse level its red launch.
+template <typename TC>
+__device__ __forceinline__ void red_from_zero(const BlkLev &Cb, int I, int J, int K, TC rhs) {
+  const Coef<TC> cf(Cb);
+  TC aw, ae, as, an, ab, at;
+  cell_coefs(Cb, cf, I, J, K, aw, ae, as, an, ab, at);
+  const TC ap = (TC)-1.0 * (aw + ae + as + an + ab + at);
+  phi_of<TC>(Cb)[cell_off(Cb, I, J, K)] = (rhs / ap);
+}
+
 // ---------------------------------------------------------------------------
 // Residual + restriction (mgrestr, mgsolver.for:619-761): coarse phi := 0
 // everywhere (:650-657); interior coarse rhs := 0.125 * sum over the 8
@@ -489,7 +504,7 @@ __global__ void k_tdma(const BlkLev *__restrict__ bl, const int *__restrict__ bl
 template <typename TF, typename TC>
 __global__ void __launch_bounds__(kTile, 2) k_restrict(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
                                                       const Tile *__restrict__ tiles, const int *__restrict__ act,
-                                                      int kch) {
+                                                      int kch, int red) {
   pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkLev Cb = cl[t.blk];
@@ -549,6 +564,7 @@ __global__ void __launch_bounds__(kTile, 2) k_restrict(const BlkLev *__restrict_
     }
     const TF v = (TF)0.125 * sum;
     RC[cell_off(Cb, I, J, K)] = (TC)v;
+    if (red && colour_of(I, J, K) == 0) red_from_zero(Cb, I, J, K, (TC)v);
   }
 }
 
@@ -578,7 +594,7 @@ struct RsShape {
 template <typename TF, typename TC>
 __global__ void __launch_bounds__(kTile) k_restrict_tma(const BlkLev *__restrict__ fl, const BlkLev *__restrict__ cl,
                                                         const Tile *__restrict__ tiles, const int *__restrict__ act,
-                                                        int kch, int *__restrict__ err) {
+                                                        int kch, int *__restrict__ err, int red) {
   pdl_wait();
   using S = RsShape<TF>;
   constexpr int W = S::W;
@@ -664,7 +680,9 @@ __global__ void __launch_bounds__(kTile) k_restrict_tma(const BlkLev *__restrict
             sum = (dk | dj | di) ? sum + a : a;
           }
       }
-      rhs_of<TC>(Cb)[cell_off(Cb, I, J, K)] = (TC)((TF)0.125 * sum);
+      const TC rv = (TC)((TF)0.125 * sum);
+      rhs_of<TC>(Cb)[cell_off(Cb, I, J, K)] = rv;
+      if (red && colour_of(I, J, K) == 0) red_from_zero(Cb, I, J, K, rv);
       // the coarse ghost cells next to this cell (faces, edges, corners) := 0
       const int alo = I == 1 ? -1 : 0, ahi = I == Cb.nx ? 1 : 0;
       const int blo = J == 1 ? -1 : 0, bhi = J == Cb.ny ? 1 : 0;

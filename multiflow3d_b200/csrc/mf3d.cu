@@ -978,7 +978,7 @@ static void halo(mf3d_ctx *C, View &V, int g, int q) {
 // mgrelax(g, it) (mgsolver.for:371-617) on subset q: `it` sweeps, each
 // followed by the halo refresh (mgbound + exchangepp + exchbc_mgpp).
 template <typename T>
-static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
+static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bool red_done = false) {
   ViewLevel &L = V.lv[g];
   if (!L.n_list[q]) return;
   const int sch = C->prm.mg_itrsch;
@@ -987,11 +987,14 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
       const int pk = (g == 1 && q == SUB_A) ? MF3D_PROF_SMOOTH_L1 : 0;
       const double half = 0.5 * (double)L.cells_sub[q] * sizeof(T);
       const bool fz = from_zero && itr == 0;
+      const bool skip_red = fz && red_done;  // the restriction formed the red half-sweep
       prof_begin(C, pk, (fz ? 2 : 3) * half);
       const dim3 grid(L.n_sweep[q]), cta(RB_TX, RB_TY);
       if (L.small) {
         const int g2 = grid_of(L.small_items[q], kTile);
-        if (fz)
+        if (skip_red)
+          ;
+        else if (fz)
           launch(k_rbgs_small<T, true>, g2, kTile, 0, C->stream, L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 0);
         else
           launch(k_rbgs_small<T, false>, g2, kTile, 0, C->stream, L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p,
@@ -1000,11 +1003,13 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
         prof_begin(C, pk, 3 * half);
         launch(k_rbgs_small<T, false>, g2, kTile, 0, C->stream, L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 1);
         prof_end(C, pk);
-        C->launches += 2;
+        C->launches += skip_red ? 1 : 2;
         halo<T>(C, V, g, q);
         continue;
       }
-      if (fz)
+      if (skip_red)
+        ;
+      else if (fz)
         launch(k_rbgs<T, true>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
       else
         launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
@@ -1012,7 +1017,7 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero) {
       prof_begin(C, pk, 3 * half);
       launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 1, L.kch[q], V.err.p);
       prof_end(C, pk);
-      C->launches += 2;
+      C->launches += skip_red ? 1 : 2;
     } else if (sch == 1) {
       launch(k_lexgs<T>, L.n_list[q], 1024, 0, C->stream, L.tab.p, L.list[q].p, V.act.p);
       ++C->launches;
@@ -1044,12 +1049,13 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
     }();
     (void)attr_set;
     launch(k_restrict_tma<T, TC>, Cl.n_rtma, kTile, RsShape<T>::SMEM, C->stream, F.tab.p, Cl.tab.p, Cl.rtma.p, V.act.p,
-                                                                              Cl.rtma_kch, V.err.p);
+                                                                              Cl.rtma_kch, V.err.p, 1);
     prof_end(C, pk);
     ++C->launches;
     return;
   }
-  launch(k_restrict<T, TC>, Cl.n_rtile, kTile, 0, C->stream, F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch);
+  launch(k_restrict<T, TC>, Cl.n_rtile, kTile, 0, C->stream, F.tab.p, Cl.tab.p, Cl.rtile.p, V.act.p, Cl.rkch,
+         (C->prm.mg_itrsch == 3 && C->prm.irestr > 0) ? 1 : 0);
   prof_end(C, pk);
   ++C->launches;
 }
@@ -1084,12 +1090,15 @@ static void vcycle(mf3d_ctx *C, View &V) {
     }
   // levels >= Lc hold FP64 (the coarsest level of an FP32 V-cycle)
   const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
-  auto relax_g = [&](int g, int q, int it, bool fz) {
-    if (g >= Lc) relax<double>(C, V, g, q, it, fz);
-    else relax<T>(C, V, g, q, it, fz);
+  auto relax_g = [&](int g, int q, int it, bool fz, bool red_done = false) {
+    if (g >= Lc) relax<double>(C, V, g, q, it, fz, red_done);
+    else relax<T>(C, V, g, q, it, fz, red_done);
   };
+  // with red-black pre-smoothing the restriction also forms the coarse
+  // level's first (from-zero) red half-sweep
+  const bool red_in_restr = sch == 3 && ir > 0;
   for (int g = 1; g <= V.Lmax; ++g) {
-    relax_g(g, SUB_A, ir, sch == 3);  // a level starts from zero (pp = 0; mgrestr)
+    relax_g(g, SUB_A, ir, sch == 3, g > 1 && red_in_restr);  // a level starts from zero (pp = 0; mgrestr)
     relax_g(g, SUB_C, ip, sch == 3 && ir == 0);
     if (g < V.Lmax) {
       if (g + 1 >= Lc) restr<T, double>(C, V, g);
