@@ -506,8 +506,9 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas(const BlkFld *__
 // (press.for:51-53, copied by mgkcyc at mgsolver.for:256-261).  A block
 // face that is not a wall takes the source block's ustar and face density
 // (k_face_planes).  One thread per (i, j) column, marching up OZ_KCH planes;
-// each face velocity is formed from the same operands by both cells that
-// share it.  rmax as in k_calvel_calmas.
+// the west face comes from the lane to the left and the bottom face from
+// the plane below (formed from the same operands), so a cell forms four
+// face velocities, not six.  rmax as in k_calvel_calmas.
 __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_lsm(const BlkFld *__restrict__ fl,
                                                                    const Tile *__restrict__ tiles,
                                                                    const DomState *__restrict__ ds,
@@ -537,6 +538,7 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_lsm(const BlkFld
   const bool wwall = F.wall[0], swall = F.wall[2], bwall = F.wall[4];
   const int k1 = min(t.k0 + OZ_KCH - 1, nz);
   double vmax = 0.0;
+  double wcarry = 0.0;  // the top face of the previous plane: this plane's bottom face
   for (int k = t.k0; k <= k1; ++k) {
     const long long c = fidx(F, ic, jc, k);
     const double pc = p[c], dc = D[c];
@@ -544,9 +546,13 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_lsm(const BlkFld
     double ue, uw, vn, vs, wt, wb;
     if (ic == nx && ewall) ue = F.hi[0][(k - 1) * ny + (jc - 1)];
     else ue = (F.ustar[c] - xdiv(dta * (p[c + 1] - pc), dx, ix) / (0.5 * (dc + D[c + 1])));
+    // the west face is the east face of the lane to the left (same operands)
+    const double ul = __shfl_up_sync(0xffffffffu, ue, 1);
     if (ic == 1) {
       const int o = (k - 1) * ny + (jc - 1);
       uw = wwall ? F.lo[0][o] : (F.lo[0][o] - xdiv(dta * (pc - p[c - 1]), dx, ix) / F.dlo[0][o]);
+    } else if (threadIdx.x > 0) {
+      uw = ul;
     } else {
       uw = (F.ustar[c - 1] - xdiv(dta * (pc - p[c - 1]), dx, ix) / (0.5 * (D[c - 1] + dc)));
     }
@@ -563,9 +569,12 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_lsm(const BlkFld
     if (k == 1) {
       const int o = (jc - 1) * nx + (ic - 1);
       wb = bwall ? F.lo[2][o] : (F.lo[2][o] - xdiv(dta * (pc - p[c - sz]), dz, iz) / F.dlo[2][o]);
+    } else if (k > t.k0) {
+      wb = wcarry;
     } else {
       wb = (F.wstar[c - sz] - xdiv(dta * (pc - p[c - sz]), dz, iz) / (0.5 * (D[c - sz] + dc)));
     }
+    wcarry = wt;
     const double fact = (xdiv(ue - uw, hx, ix) + xdiv(vn - vs, hy, iy) + xdiv(wt - wb, hz, iz));
     if (!in) continue;
     const double sup = fact * hx * hy * hz / dt;
