@@ -89,7 +89,10 @@ typedef struct mf3d_params {
   double eps;       /* stopping tolerance on rmax (newsolv_mg.for:56)        */
   int eps_relative; /* 0: rmax < eps (reference); 1: rmax < eps * rmax_0     */
   int pl;           /* ghost layers of the field arrays (localparameters.for:17-24) */
-  int differencing; /* 1 = 2nd-order divergence in calmas (press.for:38-67)  */
+  int differencing; /* control.cin differencing: 1 (2nd-order CDS) or 3 (WENO,
+                       which L_LSM requires, initial.for:133-135) - calmas
+                       takes its 2nd-order divergence for both
+                       (press.for:38-67); 2 (4th order) is not supported      */
   int precision;    /* enum mf3d_precision                                   */
   int device;       /* CUDA device ordinal                                   */
   int pl_ex;        /* extra ghost planes (control.cin pl_ex; pl = LMR + pl_ex,

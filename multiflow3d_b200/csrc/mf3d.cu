@@ -1540,7 +1540,10 @@ static int check_params(const mf3d_params *prm) {
   if (prm->irestr < 0 || prm->iproln < 0 || prm->maxcy < 0) { set_error("negative sweep/cycle count"); return MF3D_E_INVALID; }
   if (prm->pl < 1) { set_error("pl must be >= 1"); return MF3D_E_INVALID; }
   if (prm->pl_ex < 0 || prm->pl_ex >= prm->pl) { set_error("pl_ex must satisfy 0 <= pl_ex < pl"); return MF3D_E_INVALID; }
-  if (prm->differencing != 1) { set_error("differencing != 1 (4th-order calmas) is not supported"); return MF3D_E_UNSUPPORTED; }
+  // calmas takes its 2nd-order branch for every differencing but 2 (press.for:
+  // 13-35 is the 4th-order one); 3 (WENO convection) is the one L_LSM needs
+  if (prm->differencing == 2) { set_error("differencing = 2 (4th-order calmas) is not supported"); return MF3D_E_UNSUPPORTED; }
+  if (prm->differencing != 1 && prm->differencing != 3) { set_error("differencing must be 1, 2 or 3"); return MF3D_E_INVALID; }
   if (prm->precision < 0 || prm->precision > 1) { set_error("precision mode not supported"); return MF3D_E_UNSUPPORTED; }
   if (prm->lsm && prm->precision != MF3D_PREC_FP64) { set_error("lsm runs in FP64 only"); return MF3D_E_UNSUPPORTED; }
   if (prm->solver != 0 && prm->solver != 1 && prm->solver != 2) { set_error("solver must be 1 or 2"); return MF3D_E_INVALID; }

@@ -945,7 +945,7 @@ void calvel(Ctx &C) {
   exchange(C, 3);
 }
 
-/* calmas (press.for:2-75), differencing = 1, both branches. */
+/* calmas (press.for:2-75), the 2nd-order branch (differencing 1 or 3), both L_LSM branches. */
 void calmas(Ctx &C) {
   double rmax = 0.0;
   std::vector<double> bmax(C.b.size(), 0.0);
@@ -1162,7 +1162,8 @@ std::string g_err;
 int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm) {
   if (nb <= 0 || !blocks || !prm) { g_err = "bad arguments"; return MF3D_E_INVALID; }
   if (prm->mg_itrsch < 1 || prm->mg_itrsch > 3) { g_err = "mg_itrsch"; return MF3D_E_INVALID; }
-  if (prm->differencing != 1) { g_err = "differencing"; return MF3D_E_UNSUPPORTED; }
+  if (prm->differencing == 2) { g_err = "differencing 2"; return MF3D_E_UNSUPPORTED; }
+  if (prm->differencing != 1 && prm->differencing != 3) { g_err = "differencing"; return MF3D_E_INVALID; }
   C.ngrd_gl = prm->ngrid; C.mg_itrsch = prm->mg_itrsch; C.irestr = prm->irestr; C.iproln = prm->iproln;
   C.maxcy = prm->maxcy; C.eps = prm->eps; C.eps_relative = prm->eps_relative; C.pl = prm->pl;
   C.pl_ex = prm->pl_ex;

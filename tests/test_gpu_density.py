@@ -45,9 +45,10 @@ def test_variable_density_matches_oracle(lib, oracle, cuda, scheme, layout):
 def test_variable_density_converged_with_time_step(lib, oracle, cuda):
     """A converged solve (hundreds of outer iterations: the reference's
     variable-density coarse levels keep the fine spacings) with dt and
-    alfapr that are not powers of two."""
+    alfapr that are not powers of two, and differencing = 3 (WENO convection,
+    which the reference requires with L_LSM)."""
     pr = Problem(2, 1, 1, 16, 16, 16, ngrid=4, pl=2)
-    prm = pr.params(mg_itrsch=3, maxcy=1500, eps=1e-10, lsm=1)
+    prm = pr.params(mg_itrsch=3, maxcy=1500, eps=1e-10, lsm=1, differencing=3)
     o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm,
                     density_blocks(pr, 8), dt=0.37, alfapr=1.3)
     assert o[0] == 0

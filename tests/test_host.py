@@ -99,6 +99,9 @@ def test_create_rejects_bad_config_without_gpu(lib):
     prm.differencing = 2
     assert lib.mf3d_create(Problem(1, 1, 1, 8, 8, 8, ngrid=2).descriptors(lib), 1, C.byref(prm),
                            C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED
+    prm.differencing = 4
+    assert lib.mf3d_create(Problem(1, 1, 1, 8, 8, 8, ngrid=2).descriptors(lib), 1, C.byref(prm),
+                           C.byref(ctx)) == abi.MF3D_E_INVALID
 
 
 def test_create_rejects_bad_pl_ex_without_gpu(lib, oracle):

@@ -275,6 +275,28 @@ def test_variable_density_projection_is_divergence_free(oracle):
     assert np.abs(divergence(pr, blocks)).max() <= 1e-9 * div0
 
 
+def test_weno_differencing_takes_the_second_order_divergence(oracle):
+    """L_LSM runs with differencing = 3 (WENO convection, initial.for:133-135);
+    calmas branches only on differencing = 2 (press.for:13-35), so 3 gives
+    the same projection as 1, bit for bit, and 2 is refused."""
+    pr = Problem(2, 1, 1, 16, 8, 8, ngrid=3, pl=2)
+    runs = []
+    for d in (1, 3):
+        blocks = pr.block_fields(seed=4, fourier_modes=2)
+        for f, r in zip(blocks, pr.block_density(5)):
+            f["dens"] = r
+        st, info, hist = solve(oracle, pr, blocks, maxcy=30, eps=1e-9, lsm=1, differencing=d)
+        assert st in (0, 1)
+        runs.append((info.rmax, hist, blocks))
+    assert runs[0][0] == runs[1][0] and np.array_equal(runs[0][1], runs[1][1])
+    for a, b in zip(runs[0][2], runs[1][2]):
+        for k in ("p", "u", "v", "w", "su"):
+            assert np.array_equal(a[k], b[k])
+    blocks = pr.block_fields(seed=4)
+    assert solve(oracle, pr, blocks, maxcy=2, differencing=2)[0] == -6
+    assert solve(oracle, pr, blocks, maxcy=2, differencing=4)[0] == -1
+
+
 def test_bounds_known_answers(oracle):
     """boundu/boundv/boundw after the loop (bounds: periodic x, walls in y,
     symmetry in z, two ghost layers): a wall mirrors the tangential
