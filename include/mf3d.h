@@ -109,8 +109,15 @@ typedef struct mf3d_params {
   int bounds;       /* 1: after the loop, boundu/boundv/boundw (newsolv_mg.for:
                        86-88, bounds.for:2-916) on the device: the periodic
                        exchange_bc of u, v, w, then every face without a
-                       neighbour by its code - 3 symmetry, 4 wall, 5 periodic
-                       (others return MF3D_E_UNSUPPORTED).  Also refreshes the
+                       neighbour by its code - 1 inflow (west: u = ubulk,
+                       v = w = 0; bottom: u = v = 0, w = 1.1), 2 outflow
+                       (east, alfabc = 1: copy of the last face), 3 symmetry,
+                       4 wall, 5 periodic; a code with no branch for a face
+                       writes nothing there, as in the reference.  The codes
+                       that need data the library does not hold - 7, 8, 12,
+                       13 on the west, 21 on the east (uoo), 61 and up (wall
+                       functions), and 1 / 2 with lsm (phi) - return
+                       MF3D_E_UNSUPPORTED.  Also refreshes the
                        full periodic ghost planes of the final exchange(1..3).
                        Skipped when the solve diverged (the reference stops).
                        mf3d_create contexts only.  0: u, v, w face ghosts as
@@ -120,6 +127,10 @@ typedef struct mf3d_params {
                        sipsol.for:2-206), maxcy playing niter.  FP64,
                        mf3d_create contexts, no lsm.                          */
   int nswp;         /* solver 1: SIP sweeps per call (control.cin nswp(4))    */
+  int alfabc;       /* control.cin alfabc: 1 = bounds applies the outflow
+                       faces (code 2, bounds.for:136-170)                     */
+  double ubulk;     /* control.cin ubulk: the inflow velocity of code-1 west
+                       faces under bounds (bounds.for:42-53)                  */
 } mf3d_params;
 
 /* Field pointers of one block, each a (ttc_i,ttc_j,ttc_k) array.

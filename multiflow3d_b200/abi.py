@@ -88,6 +88,8 @@ class Params(C.Structure):
         ("bounds", C.c_int),
         ("solver", C.c_int),
         ("nswp", C.c_int),
+        ("alfabc", C.c_int),
+        ("ubulk", C.c_double),
     ]
 
 

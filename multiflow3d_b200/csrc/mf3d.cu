@@ -1319,6 +1319,20 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
 // exchange_bc of u, v, w with every block on one rank (exchange_bc.for:
 // 16-838): per layer, the first walk's self-copies, the second walk's
 // self-copies and packs, the third walk's unpacks, each over x, y, z.
+// A face code whose boundu/v/w branch needs data the library does not hold:
+// the inflow files, SEM and power-law inlets of the west face (7, 8, 12, 13;
+// bounds.for:55-124), the convective outflow of the east face (21, uoo;
+// bounds.for:143-170), wall functions (61 and up: log_law, wall_function),
+// and under L_LSM the inflow and outflow faces, which phi gates
+// (bounds.for:43-50, 146-158).
+static bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc) {
+  if (code >= 61) return true;
+  if (f == 0 && (code == 7 || code == 8 || code == 12 || code == 13)) return true;
+  if (f == 1 && code == 21 && alfabc == 1) return true;
+  if (lsm && ((f == 0 && code == 1) || (f == 1 && code == 2 && alfabc == 1))) return true;
+  return false;
+}
+
 static void bc_walks(mf3d_ctx *C, View &V) {
   for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
     for (int mode = 0; mode < 3; ++mode)
@@ -1351,7 +1365,8 @@ static int solve_end(mf3d_ctx *C, View &V) {
     bc_walks(C, V);
     for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
       for (int a = 0; a < 3; ++a) {
-        launch(k_bound_faces, V.n_bcax[a], kTile, 0, s, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly);
+        launch(k_bound_faces, V.n_bcax[a], kTile, 0, s, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly, C->prm.ubulk,
+               C->prm.alfabc);
         ++C->launches;
       }
     return MF3D_OK;
@@ -1609,8 +1624,9 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
       const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
       const int nbrs[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
       for (int f = 0; f < 6; ++f)
-        if (nbrs[f] < 0 && bcs[f] != 3 && bcs[f] != 4 && bcs[f] != MF3D_BC_PERIODIC) {
-          set_error("bounds: block " + std::to_string(d.id) + " has a face code other than 3, 4, 5");
+        if (nbrs[f] < 0 && bounds_code_unsupported(f, bcs[f], prm->lsm != 0, prm->alfabc)) {
+          set_error("bounds: block " + std::to_string(d.id) + " face " + std::to_string(f) + " has code " +
+                    std::to_string(bcs[f]) + ", whose boundu/v/w branch needs data the library does not hold");
           return MF3D_E_UNSUPPORTED;
         }
     }

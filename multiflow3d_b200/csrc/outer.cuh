@@ -352,10 +352,15 @@ __global__ void k_bc_walk(const BlkFld *__restrict__ fl, const Tile *__restrict_
 // (bounds.for:2-916): over the component's ranges widened by one cell,
 //   normal component: wall -> 0; symmetry -> 0 on y and z faces;
 //   tangential: wall -> -(the cell ly inside); symmetry -> + on y and z faces;
-// x-face symmetry and periodic faces write nothing.  Launched per layer for
-// x, y, z (the reference's W, E, S, N, B, T).  Skipped after a diverged solve.
+//   inflow (1) on the west: u = ubulk, v = w = 0; on the bottom: u = v = 0,
+//     w = 1.1 (bounds.for:42-53, 374-377, 662-665; 226-229, 536-539, 873-876);
+//   outflow (2) on the east with alfabc = 1: every layer copies the last
+//     face ie (bounds.for:136-170, 444-470);
+// x-face symmetry, periodic faces and codes without a branch write nothing.
+// Launched per layer for x, y, z (the reference's W, E, S, N, B, T).
+// Skipped after a diverged solve.
 __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                              const DomState *__restrict__ ds, int ax, int ly) {
+                              const DomState *__restrict__ ds, int ax, int ly, double ubulk, int alfabc) {
   pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
@@ -374,9 +379,14 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   if (!F.wall[f]) return;
   const int code = F.bcode[f];
   const bool normal = comp == ax;
-  int mode = 0;  // 1 zero, 2 -mirror, 3 +mirror
+  int mode = 0;  // 1 constant cv, 2 -mirror, 3 +mirror, 4 copy of the last face
+  double cv = 0.0;
   if (code == 4) mode = normal ? 1 : 2;
   else if (code == 3 && ax != 0) mode = normal ? 1 : 3;
+  else if (code == 1 && side == 0 && ax != 1) {  // inflow: west u = ubulk, bottom w = 1.1, the rest 0
+    mode = 1;
+    cv = ax == 0 ? (comp == 0 ? ubulk : 0.0) : (comp == 2 ? 1.1 : 0.0);
+  } else if (code == 2 && ax == 0 && side == 1 && alfabc == 1) mode = 4;  // outflow: u(ie+1+ly) = u(ie)
   if (!mode) return;
   // the widened ranges of the other two axes: 0 .. end+1
   const int as = ax == 0 ? 1 : 0, at = ax == 2 ? 1 : 2;
@@ -384,8 +394,9 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   double *fi = comp_field(F, comp);
   const int s0 = 1, e0 = comp_end(F, comp, ax);
   const long long g = fidx_ax(F, ax, side ? e0 + 1 + ly : s0 - 1 - ly, sl, tl);
-  const double m = fi[fidx_ax(F, ax, side ? e0 - ly : s0 + ly, sl, tl)];
-  fi[g] = mode == 1 ? 0.0 : mode == 2 ? -m : m;
+  const int src = mode == 4 ? e0 : side ? e0 - ly : s0 + ly;
+  const double m = fi[fidx_ax(F, ax, src, sl, tl)];
+  fi[g] = mode == 1 ? cv : mode == 2 ? -m : m;
 }
 
 __device__ inline void atomic_max_nonneg(unsigned long long *slot, double v) {

@@ -139,11 +139,12 @@ class Problem:
 
     def params(self, mg_itrsch=3, irestr=2, iproln=1, maxcy=200, eps=1e-8,
                eps_relative=1, precision=MF3D_PREC_FP64, device=0, pl_ex=0, lsm=0, bounds=0, solver=0,
-               nswp=0, differencing=1) -> Params:
+               nswp=0, differencing=1, alfabc=0, ubulk=0.0) -> Params:
         return Params(ngrid=self.ngrid, mg_itrsch=mg_itrsch, irestr=irestr,
                       iproln=iproln, maxcy=maxcy, eps=eps, eps_relative=eps_relative,
                       pl=self.pl, differencing=differencing, precision=precision, device=device,
-                      pl_ex=pl_ex, lsm=lsm, bounds=bounds, solver=solver, nswp=nswp)
+                      pl_ex=pl_ex, lsm=lsm, bounds=bounds, solver=solver, nswp=nswp,
+                      alfabc=alfabc, ubulk=ubulk)
 
     def block_density(self, seed: int, lo: float = 0.5, hi: float = 2.0, const: float | None = None):
         """Per-block cell densities (ttc layout) cut from one global field:

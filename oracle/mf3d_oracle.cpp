@@ -95,6 +95,8 @@ struct Ctx {
   int ngrd_gl, mg_itrsch, irestr, iproln, maxcy, pl, pl_ex;
   bool lsm; /* L_LSM: variable-density coefficients, calvel and rhs */
   bool bounds; /* boundu/boundv/boundw after the loop (newsolv_mg.for:86-88) */
+  int alfabc;   /* 1: outflow faces (code 2) copy the last face */
+  double ubulk; /* inflow velocity of code-1 west faces */
   int solver;   /* 2: multigrid newsolv_mg; 1: pressure_1sweep with SIP */
   int nswp;     /* SIP inner sweeps per call (control.cin nswp(4)) */
   long long sip_sweeps; /* nsweeps: inner sweeps run over the solve */
@@ -857,18 +859,34 @@ void pbound(Ctx &C) {
   }
 }
 
-/* boundu, boundv, boundw (bounds.for:2-916), restated for the codes 3
- * (symmetry), 4 (wall) and 5 (periodic); set-up rejects the others.  The
- * periodic copy, then per layer ly = 0..pl_ex each block's faces W, E, S,
- * N, B, T over the component's ranges widened by one cell:
+/* boundu, boundv, boundw (bounds.for:2-916), restated for the codes 1
+ * (inflow), 2 (outflow), 3 (symmetry), 4 (wall) and 5 (periodic); set-up
+ * rejects the codes whose branch reads files, phi, uoo or wall functions.
+ * The periodic copy, then per layer ly = 0..pl_ex each block's faces W, E,
+ * S, N, B, T over the component's ranges widened by one cell:
  *   normal component (u on x faces, ...): wall -> 0; symmetry -> 0 on y and
  *     z faces, nothing on x faces;
  *   tangential component: wall -> -(the cell ly inside); symmetry -> +(the
- *     same) on y and z faces, nothing on x faces.
+ *     same) on y and z faces, nothing on x faces;
+ *   inflow on the west: u = ubulk, v = w = 0 (bounds.for:42-53, 374-377,
+ *     662-665); on the bottom u = v = 0, w = 1.1 (226-229, 536-539, 873-876);
+ *   outflow on the east, alfabc = 1: ghost layer ly = the last face ie
+ *     (bounds.for:136-170, 444-470 and the same branch of boundw);
+ *   any other (face, code) pair: nothing.
  * (bounds.for:36-42, 136-140, 179-186, 212-219, 246-259, 301-308 for u;
  * 369-373, 444-448, 505-533, 535-548, 588-595 for v; 657-661, 738-742,
  * 799-806, 833-840, 866-876, 900-908 for w.) */
-void bound_face(Blk &B, int op, int ly, int f) {
+bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc) {
+  /* the branches that read data outside the projection: inflow files, SEM
+   * and power-law inlets (west 7, 8, 12, 13), the convective outflow (east
+   * 21, uoo), wall functions (61+), phi-gated inflow/outflow under L_LSM */
+  if (code >= 61) return true;
+  if (f == 0 && (code == 7 || code == 8 || code == 12 || code == 13)) return true;
+  if (f == 1 && code == 21 && alfabc == 1) return true;
+  if (lsm && ((f == 0 && code == 1) || (f == 1 && code == 2 && alfabc == 1))) return true;
+  return false;
+}
+void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
   const int ax = f / 2, comp = op - 1;
   const bool high = f & 1;
   const int bcs[6] = {B.d.bc_west, B.d.bc_east, B.d.bc_south, B.d.bc_north, B.d.bc_bottom, B.d.bc_top};
@@ -876,9 +894,13 @@ void bound_face(Blk &B, int op, int ly, int f) {
   if (nbr[f] >= 0) return;
   const int code = bcs[f];
   const bool normal = ax == comp;
-  int mode = 0; /* 0 nothing, 1 zero, 2 -mirror, 3 +mirror */
+  int mode = 0; /* 0 nothing, 1 the constant cv, 2 -mirror, 3 +mirror, 4 copy of face ie */
+  double cv = 0.0;
   if (code == 4) mode = normal ? 1 : 2;
   else if (code == 3 && ax != 0) mode = normal ? 1 : 3;
+  else if (code == 1 && f == 0) { mode = 1; cv = comp == 0 ? C.ubulk : 0.0; }
+  else if (code == 1 && f == 4) { mode = 1; cv = comp == 2 ? 1.1 : 0.0; }
+  else if (code == 2 && f == 1 && C.alfabc == 1) mode = 4;
   if (!mode) return;
   int is, ie, js, je, ks, ke;
   franges(B, op, is, ie, js, je, ks, ke);
@@ -892,17 +914,17 @@ void bound_face(Blk &B, int op, int ly, int f) {
     if (ax == 1) return F(B, fi, s, a, t);
     return F(B, fi, s, t, a);
   };
-  const int ghost = high ? e0 + 1 + ly : s0 - 1 - ly, mirror = high ? e0 - ly : s0 + ly;
+  const int ghost = high ? e0 + 1 + ly : s0 - 1 - ly, mirror = mode == 4 ? e0 : high ? e0 - ly : s0 + ly;
   for (int t = ta - 1; t <= tb + 1; ++t)
     for (int s = sa - 1; s <= ea + 1; ++s)
-      at(ghost, s, t) = mode == 1 ? 0.0 : mode == 2 ? -at(mirror, s, t) : at(mirror, s, t);
+      at(ghost, s, t) = mode == 1 ? cv : mode == 2 ? -at(mirror, s, t) : at(mirror, s, t);
 }
 
 void bound(Ctx &C, int op) {
   if (C.periodic) exchange_bc(C, op, C.pl_ex);
   for (int ly = 0; ly <= C.pl_ex; ++ly)
     for (auto &B : C.b)
-      for (int f = 0; f < 6; ++f) bound_face(B, op, ly, f);
+      for (int f = 0; f < 6; ++f) bound_face(C, B, op, ly, f);
 }
 
 /* EXT: distance between the centres of cells a and a+1 along an axis,
@@ -1170,6 +1192,8 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
   if (C.pl_ex < 0 || C.pl_ex >= C.pl) { g_err = "pl_ex"; return MF3D_E_INVALID; }
   C.lsm = prm->lsm != 0;
   C.bounds = prm->bounds != 0;
+  C.alfabc = prm->alfabc;
+  C.ubulk = prm->ubulk;
   C.solver = prm->solver == 1 ? 1 : 2;
   C.nswp = prm->nswp;
   if (C.solver == 1 && (C.nswp < 1 || C.lsm)) { g_err = "solver 1: nswp >= 1, no lsm"; return MF3D_E_INVALID; }
@@ -1202,7 +1226,7 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
       const int bcs[6] = {B.d.bc_west, B.d.bc_east, B.d.bc_south, B.d.bc_north, B.d.bc_bottom, B.d.bc_top};
       const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
       for (int f = 0; f < 6; ++f)
-        if (nbr[f] < 0 && bcs[f] != 3 && bcs[f] != 4 && bcs[f] != 5) { g_err = "bounds: face code"; return MF3D_E_UNSUPPORTED; }
+        if (nbr[f] < 0 && bounds_code_unsupported(f, bcs[f], C.lsm, C.alfabc)) { g_err = "bounds: face code"; return MF3D_E_UNSUPPORTED; }
     }
     B.hx = level_widths(B.d.hx, B.d.nx, B.d.dx, B.ngrid);
     B.hy = level_widths(B.d.hy, B.d.ny, B.d.dy, B.ngrid);

@@ -126,6 +126,18 @@ def test_create_rejects_bad_pl_ex_without_gpu(lib, oracle):
     assert st == abi.MF3D_E_INVALID
 
 
+def test_bounds_face_codes_refused_without_gpu(lib):
+    """bounds = 1 refuses, before any device work, the face codes whose
+    boundu/v/w branch needs data the library does not hold."""
+    ctx = C.c_void_p()
+    for bc, kw in (((7, 2, WALL, WALL, WALL, WALL), {}), ((1, 21, WALL, WALL, WALL, WALL), {"alfabc": 1}),
+                   ((1, 2, WALL, WALL, 63, WALL), {}), ((1, 2, WALL, WALL, WALL, WALL), {"lsm": 1})):
+        pr = Problem(1, 1, 1, 8, 8, 8, bc=bc, ngrid=2, pl=1)
+        prm = pr.params(bounds=1, **kw)
+        assert lib.mf3d_create(pr.descriptors(lib), 1, C.byref(prm), C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED, bc
+        assert b"bounds" in lib.mf3d_last_error()
+
+
 def test_variable_density_limits_without_gpu(lib):
     """lsm (the reference's L_LSM) runs in FP64 on uniform blocks through
     mf3d_create only; the other combinations are refused before any device

@@ -329,10 +329,57 @@ def test_bounds_known_answers(oracle):
         assert np.array_equal(a[:, :, pl + n], a[:, :, pl])
 
 
-def test_bounds_rejects_other_codes(oracle):
-    pr = Problem(1, 1, 1, 8, 8, 8, bc=(1, 2, WALL, WALL, WALL, WALL), ngrid=2, pl=1)
-    st, _, _ = solve(oracle, pr, pr.block_fields(seed=1), maxcy=2, bounds=1)
-    assert st == -6  # MF3D_E_UNSUPPORTED: inflow / outflow codes are not restated
+def test_bounds_inflow_outflow_known_answers(oracle):
+    """Inflow (code 1) on the west and the bottom, outflow (code 2) on the
+    east with alfabc = 1: the west ghost layers hold u = ubulk, v = w = 0
+    (bounds.for:42-53, 374-377, 662-665), the bottom ones u = v = 0 and
+    w = 1.1 (226-229, 536-539, 873-876), and every east ghost layer copies
+    the last face ie (136-170, 444-470): u's ie is one face short of the
+    boundary, v's and w's is the last cell."""
+    SYM, INF, OUT = 3, 1, 2
+    n, pl = 8, 3
+    pr = Problem(1, 1, 1, n, n, n, bc=(INF, OUT, WALL, WALL, INF, SYM), ngrid=2, pl=pl)
+    blocks = pr.block_fields(seed=23)
+    st, info, _ = solve(oracle, pr, blocks, maxcy=6, eps=1e-12, pl_ex=2, bounds=1, alfabc=1, ubulk=0.7)
+    assert st >= 0
+    u, v, w = (blocks[0][k] for k in ("u", "v", "w"))
+    Ji, Ki, Ii = slice(pl, pl + n), slice(pl, pl + n), slice(pl, pl + n)
+    for ly in range(3):
+        west = pl - 1 - ly
+        assert (u[Ki, Ji, west] == 0.7).all()
+        assert not v[Ki, Ji, west].any() and not w[Ki, Ji, west].any()
+        bottom = pl - 1 - ly
+        assert not u[bottom, Ji, Ii].any() and not v[bottom, Ji, Ii].any()
+        assert (w[bottom, Ji, Ii] == 1.1).all()
+        assert np.array_equal(u[Ki, Ji, pl + n - 1 + ly], u[Ki, Ji, pl + n - 2])
+        for a in (v, w):
+            assert np.array_equal(a[Ki, Ji, pl + n + ly], a[Ki, Ji, pl + n - 1])
+    # alfabc = 0: the outflow branch is skipped, the east ghosts keep what calvel's exchange left
+    b2 = pr.block_fields(seed=23)
+    solve(oracle, pr, b2, maxcy=6, eps=1e-12, pl_ex=2, bounds=1, alfabc=0, ubulk=0.7)
+    assert not np.array_equal(b2[0]["v"][Ki, Ji, pl + n + 1], b2[0]["v"][Ki, Ji, pl + n - 1])
+
+
+@pytest.mark.parametrize("bc,kw,ok", [
+    ((7, 2, WALL, WALL, WALL, WALL), {}, False),            # inflow slices read from files
+    ((12, 2, WALL, WALL, WALL, WALL), {}, False),           # power-law inlet
+    ((1, 21, WALL, WALL, WALL, WALL), {"alfabc": 1}, False),  # convective outflow reads uoo
+    ((1, 21, WALL, WALL, WALL, WALL), {"alfabc": 0}, True),   # ... unless alfabc skips it
+    ((1, 2, WALL, WALL, 61, WALL), {}, False),              # wall function
+    ((1, 2, WALL, WALL, WALL, WALL), {"lsm": 1}, False),    # phi-gated inflow under L_LSM
+    ((4, 4, 1, 2, 44, 6), {"alfabc": 1}, True),             # codes without a branch on those faces
+])
+def test_bounds_face_codes(oracle, bc, kw, ok):
+    """The face codes whose boundu/v/w branch reads data outside the
+    projection are refused (MF3D_E_UNSUPPORTED); every other code runs, and
+    one without a branch for its face writes nothing there."""
+    pr = Problem(1, 1, 1, 8, 8, 8, bc=bc, ngrid=2, pl=1)
+    blocks = pr.block_fields(seed=1)
+    if kw.get("lsm"):
+        for f, d in zip(blocks, pr.block_density(2)):
+            f["dens"] = d
+    st, _, _ = solve(oracle, pr, blocks, maxcy=2, bounds=1, **kw)
+    assert (st >= 0) if ok else (st == -6)
 
 
 @pytest.mark.parametrize("nswp", [1, 4])
