@@ -634,6 +634,7 @@ struct mf3d_ctx {
   // the face planes first
   cudaStream_t side = nullptr;
   cudaEvent_t ev_side = nullptr;
+  cudaEvent_t ev_in = nullptr;  // host entry: the solve's inputs are on the device
   bool walls_given = false, wait_side = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long long launches = 0;
@@ -1772,10 +1773,13 @@ static int host_solve(mf3d_ctx *C, const mf3d_fields *fields, const double *dt, 
   // side stream while the solve runs; the solve waits for them just before
   // that calvel.  Their wall values - all the solve reads of them earlier,
   // through the face planes - go straight from the caller's arrays into
-  // those planes on the solve stream.
+  // those planes on the solve stream.  The side copies start only once the
+  // inputs are in: both go host to device over one link, and the solve
+  // waits for the inputs, not for u, v, w.
   if (!C->side) {
     CK(cudaStreamCreateWithFlags(&C->side, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&C->ev_side, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&C->ev_in, cudaEventDisableTiming));
   }
   for (int b = 0; b < nb; ++b) {  // every pointer before any copy is queued
     const mf3d_fields &f = fields[b];
@@ -1789,10 +1793,10 @@ static int host_solve(mf3d_ctx *C, const mf3d_fields *fields, const double *dt, 
   for (int b = 0; b < nb; ++b) {
     const size_t n = ttc_elems(pl, V.blk[b]->d);
     double *m = C->mirror.p + C->mirror_off[b];
-    double *const hsrc[7] = {fields[b].ustar, fields[b].vstar, fields[b].wstar, fields[b].u, fields[b].v, fields[b].w, fields[b].p};
-    for (int q = 0; q < 7; ++q)
-      CK(cudaMemcpyAsync(m + q * n, hsrc[q], n * sizeof(double), cudaMemcpyHostToDevice,
-                         (q >= 3 && q <= 5) ? C->side : s));
+    double *const hsrc[4] = {fields[b].ustar, fields[b].vstar, fields[b].wstar, fields[b].p};
+    const int q_of[4] = {0, 1, 2, 6};
+    for (int q = 0; q < 4; ++q)
+      CK(cudaMemcpyAsync(m + q_of[q] * n, hsrc[q], n * sizeof(double), cudaMemcpyHostToDevice, s));
     dev[b] = mf3d_fields{m, m + n, m + 2 * n, m + 3 * n, m + 4 * n, m + 5 * n, m + 6 * n,
                          fields[b].su ? m + 7 * n : nullptr, nullptr};
     if (C->prm.lsm) {
@@ -1830,6 +1834,15 @@ static int host_solve(mf3d_ctx *C, const mf3d_fields *fields, const double *dt, 
         CK(cudaMemcpy3DAsync(&p3, s));
       }
     }
+  }
+  CK(cudaEventRecord(C->ev_in, s));
+  CK(cudaStreamWaitEvent(C->side, C->ev_in, 0));
+  for (int b = 0; b < nb; ++b) {
+    const size_t n = ttc_elems(pl, V.blk[b]->d);
+    double *m = C->mirror.p + C->mirror_off[b];
+    double *const hsrc[3] = {fields[b].u, fields[b].v, fields[b].w};
+    for (int q = 0; q < 3; ++q)
+      CK(cudaMemcpyAsync(m + (3 + q) * n, hsrc[q], n * sizeof(double), cudaMemcpyHostToDevice, C->side));
   }
   CK(cudaEventRecord(C->ev_side, C->side));
   C->walls_given = true;
@@ -1912,6 +1925,7 @@ int mf3d_destroy(mf3d_ctx *ctx) {
     cudaStreamDestroy(ctx->side);
   }
   if (ctx->ev_side) cudaEventDestroy(ctx->ev_side);
+  if (ctx->ev_in) cudaEventDestroy(ctx->ev_in);
   ctx->view.reset();
   ctx->doms.clear();
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
