@@ -47,6 +47,7 @@ struct BlkLev {
   const CUtensorMap *tm;  // TMA maps: phi colour 0, phi colour 1 (RB_RJ+2 rows), rhs colour 0, 1 (RB_RJ rows)
   const void *cc;     // variable density (L_LSM): per-cell aw, ae, as, an, ab, at, six arrays of
                       // the level's colour-split layout, array m at element m*2*cstr; else null
+  void *tdf;          // line relaxation: the TDMA factors a, apr of each direction (k_tdma_factor); else null
 };
 
 // compact row pitch: (nx+3)/2 entries rounded up to a multiple of 16 bytes
@@ -404,73 +405,222 @@ __global__ void k_lexgs(const BlkLev *__restrict__ bl, const int *__restrict__ b
 // ---------------------------------------------------------------------------
 // Line TDMA relaxation (mgsolver.for:430-545): Thomas solves along j-lines
 // (line order k, i), then i-lines (k, j), then k-lines (i, j), each pass a
-// Gauss-Seidel over lines.  Lines whose two transverse indices have the same
-// sum are independent, so one CTA per block sweeps those diagonals in order,
-// one thread per line.  `work` gives each thread two scratch vectors (a, c)
-// of length `ngg`.  a(1) = 0 and c(1) = the line's first ghost value.
+// Gauss-Seidel over lines.  A line (u, v) reads the new values of lines
+// (u-1, v) and (u, v-1) and the old ones of (u+1, v) and (u, v+1), so the
+// lines of one diagonal u + v = s are independent and the diagonals run in
+// order.  Directions: 0 j-lines at (i=u, k=v); 1 i-lines at (j=u, k=v);
+// 2 k-lines at (i=u, j=v); m runs along the line.
+//
+// The forward recurrence splits in two.  apr(m) = 1/(ap - lo*a(m-1)) and
+// a(m) = up*apr(m) (a(0) = 0; lo/up = as/an, aw/ae, ab/at) read coefficients
+// only, so k_tdma_factor forms them once per set of coefficients.  The sweep
+// then runs c(m) = (rhs'(m) - lo*c(m-1))*apr(m), c(0) = the first ghost, with
+// rhs' = su - (the four transverse terms in the reference's order), and
+// phi(m) = c(m) - a(m)*phi(m+1) from the far ghost down - the reference's
+// expressions, evaluated in its order, so the result is bit for bit.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void tdma_dims(const BlkLev &B, int dir, int &nu, int &nv, int &n) {
+  nu = dir == 1 ? B.ny : B.nx;
+  nv = dir == 2 ? B.ny : B.nz;
+  n = dir == 0 ? B.ny : dir == 1 ? B.nx : B.nz;
+}
+__device__ __forceinline__ void tdma_cell(int dir, int u, int v, int m, int &i, int &j, int &k) {
+  if (dir == 0) { i = u; j = m; k = v; }
+  else if (dir == 1) { i = m; j = u; k = v; }
+  else { i = u; j = v; k = m; }
+}
+// element of a(m) (w = 0) or apr(m) (w = 1) of line (u, v): six arrays of
+// nx*ny*nz values, each line's m contiguous
+__device__ __forceinline__ long long tdma_fidx(const BlkLev &B, int dir, int u, int v, int m, int w) {
+  int nu, nv, n;
+  tdma_dims(B, dir, nu, nv, n);
+  return (2 * dir + w) * ((long long)B.nx * B.ny * B.nz) + ((long long)(v - 1) * nu + (u - 1)) * n + (m - 1);
+}
+
+// One thread per line of direction `dir`, blockIdx.y = listed block.
 template <typename T>
-__device__ void tdma_line(const BlkLev &B, int dir, int u, int v, T *a, T *c) {
-  // dir 0: j-line at (i=u, k=v); dir 1: i-line at (j=u, k=v); dir 2: k-line at (i=u, j=v)
-  T *P = phi_of<T>(B);
-  const T *R = rhs_of<T>(B);
+__global__ void k_tdma_factor(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, int dir) {
+  pdl_wait();
+  const BlkLev B = bl[blocks[blockIdx.y]];
+  int nu, nv, n;
+  tdma_dims(B, dir, nu, nv, n);
+  const long long line = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (line >= (long long)nu * nv) return;
+  const int u = (int)(line % nu) + 1, v = (int)(line / nu) + 1;
+  T *A = (T *)B.tdf + tdma_fidx(B, dir, u, v, 1, 0);
+  T *R = (T *)B.tdf + tdma_fidx(B, dir, u, v, 1, 1);
   const Coef<T> cf(B);
-  const int n = dir == 0 ? B.ny : dir == 1 ? B.nx : B.nz;
-  auto off = [&](int m) -> long long {
-    if (dir == 0) return cell_off(B, u, m, v);
-    if (dir == 1) return cell_off(B, m, u, v);
-    return cell_off(B, u, v, m);
-  };
-  a[0] = (T)0;
-  c[0] = P[off(0)];
+  T am = (T)0;
   for (int m = 1; m <= n; ++m) {
     int i, j, k;
-    if (dir == 0) { i = u; j = m; k = v; }
-    else if (dir == 1) { i = m; j = u; k = v; }
-    else { i = u; j = v; k = m; }
+    tdma_cell(dir, u, v, m, i, j, k);
     T aw, ae, as, an, ab, at;
     cell_coefs(B, cf, i, j, k, aw, ae, as, an, ab, at);
     const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-    const T su = R[off(m)];
-    if (dir == 0) {
-      const T apr = (T)1.0 / (ap - as * a[m - 1]);
-      a[m] = an * apr;
-      c[m] = (su - ae * P[cell_off(B, i + 1, j, k)] - aw * P[cell_off(B, i - 1, j, k)] -
-              at * P[cell_off(B, i, j, k + 1)] - ab * P[cell_off(B, i, j, k - 1)] - as * c[m - 1]) * apr;
-    } else if (dir == 1) {
-      const T apr = (T)1.0 / (ap - aw * a[m - 1]);
-      a[m] = ae * apr;
-      c[m] = (su - an * P[cell_off(B, i, j + 1, k)] - as * P[cell_off(B, i, j - 1, k)] -
-              at * P[cell_off(B, i, j, k + 1)] - ab * P[cell_off(B, i, j, k - 1)] - aw * c[m - 1]) * apr;
-    } else {
-      const T apr = (T)1.0 / (ap - ab * a[m - 1]);
-      a[m] = at * apr;
-      c[m] = (su - an * P[cell_off(B, i, j + 1, k)] - as * P[cell_off(B, i, j - 1, k)] -
-              ae * P[cell_off(B, i + 1, j, k)] - aw * P[cell_off(B, i - 1, j, k)] - ab * c[m - 1]) * apr;
-    }
+    const T lo = dir == 0 ? as : dir == 1 ? aw : ab, up = dir == 0 ? an : dir == 1 ? ae : at;
+    const T apr = (T)1.0 / (ap - lo * am);
+    am = up * apr;
+    A[m - 1] = am;
+    R[m - 1] = apr;
   }
-  for (int m = n; m >= 1; --m) P[off(m)] = (c[m] - a[m] * P[off(m + 1)]);
 }
 
+// All of a cluster's CTAs (one hardware barrier; release/acquire at cluster
+// scope, so global stores before it are seen by the cluster after it).
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+constexpr int TD_THREADS = 512, TD_CH = 8;
+// Asynchronous copy of one element into shared memory (cp.async, cached at L1).
 template <typename T>
-__global__ void k_tdma(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, const int *__restrict__ act,
-                       T *__restrict__ work, int ngg) {
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(sizeof(T)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// One relaxation (the three passes) of every listed block.  Each block is a
+// cluster of `cl` CTAs (cl = 1: a plain CTA); CTA r owns the lines with u in
+// its slice of 1..nu.  Per diagonal, `gmax` of the CTA's lines at a time:
+// (1) every thread issues asynchronous copies of su, the four transverse
+// neighbours, a and apr of its cells (and the line ends' ghosts) into
+// shared memory, all in flight at once; (2) every thread forms rhs' and lo
+// of its cells there; (3) one thread per line runs the two recurrences.  A
+// cluster barrier closes the diagonal.  A line reads only lines of the
+// neighbouring diagonals, so the lines of one diagonal may run in any order.
+// Shared memory: seven arrays of gmax lines at stride nmax+1 (odd, so the
+// lanes of the recurrence hit distinct banks), then the two ghost arrays.
+template <typename T>
+__global__ void __launch_bounds__(TD_THREADS) k_tdma_lines(const BlkLev *__restrict__ bl, const int *__restrict__ blocks,
+                                                          const int *__restrict__ act, int cl, int gmax, int nmax) {
   pdl_wait();
-  const BlkLev B = bl[blocks[blockIdx.x]];
-  if (!act[B.dom]) return;
-  T *a = work + ((long long)blockIdx.x * blockDim.x + threadIdx.x) * 2 * ngg;
-  T *c = a + ngg;
+  extern __shared__ __align__(16) unsigned char td_smem[];
+  const BlkLev B = bl[blocks[blockIdx.x / cl]];
+  if (!act[B.dom]) return;  // every CTA of the cluster holds the same block
+  const int rank = blockIdx.x % cl;
+  const long long ld = nmax + 1, sl = (long long)gmax * ld;
+  T *rs = (T *)td_smem;  // su, then rhs', then c
+  T *lw = rs + sl;       // neighbour 1, then lo
+  T *rp = lw + sl;       // apr
+  T *aa = rp + sl;       // a
+  T *x2 = aa + sl;       // neighbours 2, 3, 4
+  T *x3 = x2 + sl;
+  T *x4 = x3 + sl;
+  T *g0 = x4 + sl;       // ghost before m = 1
+  T *g1 = g0 + gmax;     // ghost after m = n
+  T *P = phi_of<T>(B);
+  const T *R = rhs_of<T>(B);
+  const T *TF = (const T *)B.tdf;
+  const long long fn = (long long)B.nx * B.ny * B.nz;
+  const Coef<T> cf(B);
   for (int dir = 0; dir < 3; ++dir) {
-    // transverse extents (u, v) and the line order of the reference
-    const int nu = dir == 0 ? B.nx : dir == 1 ? B.ny : B.nx;
-    const int nv = dir == 0 ? B.nz : dir == 1 ? B.nz : B.ny;
-    for (int sum = 2; sum <= nu + nv; ++sum) {
-      for (int u = 1 + threadIdx.x; u <= nu; u += blockDim.x) {
-        const int v = sum - u;
-        if (v < 1 || v > nv) continue;
-        tdma_line(B, dir, u, v, a, c);
+    int nu, nv, n;
+    tdma_dims(B, dir, nu, nv, n);
+    const int per = (nu + cl - 1) / cl, ulo = rank * per + 1, uhi = min(nu, ulo + per - 1);
+    for (int s = 2; s <= nu + nv; ++s) {
+      const int u0 = max(ulo, s - nv), u1 = min(uhi, s - 1);
+      for (int ga = u0; ga <= u1; ga += gmax) {
+        const int gl = min(gmax, u1 - ga + 1);
+        // (1) copies in flight
+        for (int e = threadIdx.x; e < gl * n; e += TD_THREADS) {
+          const int g = e / n, m = e - g * n + 1;
+          const int u = ga + g, v = s - u;
+          int i, j, k;
+          tdma_cell(dir, u, v, m, i, j, k);
+          const long long o = g * ld + m - 1;
+          cp_async_elem(rs + o, R + cell_off(B, i, j, k));
+          if (dir == 0) {  // e, w, t, b
+            cp_async_elem(lw + o, P + cell_off(B, i + 1, j, k));
+            cp_async_elem(x2 + o, P + cell_off(B, i - 1, j, k));
+            cp_async_elem(x3 + o, P + cell_off(B, i, j, k + 1));
+            cp_async_elem(x4 + o, P + cell_off(B, i, j, k - 1));
+          } else if (dir == 1) {  // n, s, t, b
+            cp_async_elem(lw + o, P + cell_off(B, i, j + 1, k));
+            cp_async_elem(x2 + o, P + cell_off(B, i, j - 1, k));
+            cp_async_elem(x3 + o, P + cell_off(B, i, j, k + 1));
+            cp_async_elem(x4 + o, P + cell_off(B, i, j, k - 1));
+          } else {  // n, s, e, w
+            cp_async_elem(lw + o, P + cell_off(B, i, j + 1, k));
+            cp_async_elem(x2 + o, P + cell_off(B, i, j - 1, k));
+            cp_async_elem(x3 + o, P + cell_off(B, i + 1, j, k));
+            cp_async_elem(x4 + o, P + cell_off(B, i - 1, j, k));
+          }
+          const long long fo = tdma_fidx(B, dir, u, v, m, 0);
+          cp_async_elem(aa + o, TF + fo);
+          cp_async_elem(rp + o, TF + fo + fn);
+          if (m == 1) {
+            int i0, j0, k0;
+            tdma_cell(dir, u, v, 0, i0, j0, k0);
+            cp_async_elem(g0 + g, P + cell_off(B, i0, j0, k0));
+          }
+          if (m == n) {
+            tdma_cell(dir, u, v, n + 1, i, j, k);
+            cp_async_elem(g1 + g, P + cell_off(B, i, j, k));
+          }
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        // (2) rhs' = (((su - c1*n1) - c2*n2) - c3*n3) - c4*n4, and lo
+        for (int e = threadIdx.x; e < gl * n; e += TD_THREADS) {
+          const int g = e / n, m = e - g * n + 1;
+          const int u = ga + g, v = s - u;
+          int i, j, k;
+          tdma_cell(dir, u, v, m, i, j, k);
+          T aw, ae, as, an, ab, at;
+          cell_coefs(B, cf, i, j, k, aw, ae, as, an, ab, at);
+          const long long o = g * ld + m - 1;
+          T c1, c2, c3, c4, lo;
+          if (dir == 0) { c1 = ae; c2 = aw; c3 = at; c4 = ab; lo = as; }
+          else if (dir == 1) { c1 = an; c2 = as; c3 = at; c4 = ab; lo = aw; }
+          else { c1 = an; c2 = as; c3 = ae; c4 = aw; lo = ab; }
+          rs[o] = (((rs[o] - c1 * lw[o]) - c2 * x2[o]) - c3 * x3[o]) - c4 * x4[o];
+          lw[o] = lo;
+        }
+        __syncthreads();
+        // (3) the recurrences, TD_CH values at a time in registers so that
+        // the shared-memory latency stays off the chain
+        if (threadIdx.x < gl) {
+          const int g = threadIdx.x, u = ga + g, v = s - u;
+          T *cr = rs + g * ld;
+          const T *lo = lw + g * ld, *ar = rp + g * ld, *av = aa + g * ld;
+          T c = g0[g];
+          for (int m0 = 0; m0 < n; m0 += TD_CH) {
+            T x[TD_CH], y[TD_CH], z[TD_CH];
+#pragma unroll
+            for (int q = 0; q < TD_CH; ++q)
+              if (m0 + q < n) { x[q] = cr[m0 + q]; y[q] = lo[m0 + q]; z[q] = ar[m0 + q]; }
+#pragma unroll
+            for (int q = 0; q < TD_CH; ++q)
+              if (m0 + q < n) {
+                c = (x[q] - y[q] * c) * z[q];
+                x[q] = c;
+              }
+#pragma unroll
+            for (int q = 0; q < TD_CH; ++q)
+              if (m0 + q < n) cr[m0 + q] = x[q];
+          }
+          T pv = g1[g];
+          for (int m1 = n; m1 > 0; m1 -= TD_CH) {  // cells m1-1 down to m1-TD_CH
+            T x[TD_CH], y[TD_CH];
+#pragma unroll
+            for (int q = 0; q < TD_CH; ++q)
+              if (m1 - 1 - q >= 0) { x[q] = cr[m1 - 1 - q]; y[q] = av[m1 - 1 - q]; }
+#pragma unroll
+            for (int q = 0; q < TD_CH; ++q)
+              if (m1 - 1 - q >= 0) {
+                pv = (x[q] - y[q] * pv);
+                int i, j, k;
+                tdma_cell(dir, u, v, m1 - q, i, j, k);
+                P[cell_off(B, i, j, k)] = pv;
+              }
+          }
+        }
+        __syncthreads();  // the staging arrays are reused by the next group
       }
-      __syncthreads();
+      if (cl > 1) cluster_sync_all();
+      else __syncthreads();
     }
   }
 }

@@ -190,6 +190,27 @@ static cudaError_t launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
+// launch() with the grid in clusters of `cl` CTAs along x (cl = 1: none).
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_cl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, int cl,
+                             Args &&...args) {
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  at[1].id = cudaLaunchAttributeClusterDimension;
+  at[1].val.clusterDim.x = (unsigned)cl;
+  at[1].val.clusterDim.y = 1;
+  at[1].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = cl > 1 ? 2 : 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 // 1-D item tiles: for each block, ceil(items_b / kTile) CTAs (i0 = first item).
 static std::vector<Tile> make_tiles(const std::vector<long long> &items) {
   std::vector<Tile> t;
@@ -569,7 +590,12 @@ struct ViewLevel {
   long long n_halo[3] = {0, 0, 0}, n_staged[3] = {0, 0, 0};
   DevBuf<char> stage[3];              // staged halo values
   long long cells_sub[3] = {0, 0, 0}; // interior cells of each subset
-  int ngg = 0;
+  // line relaxation (mg_itrsch 2): TDMA factors of every listed block, and the
+  // k_tdma_lines shape: cluster size, lines staged at a time, longest line
+  DevBuf<char> tdf;
+  int td_cl = 1, td_gmax = 1, td_nmax = 1, td_lines[3] = {0, 0, 0};
+  size_t td_smem = 0;
+  bool td_fp64 = true;                // the level relaxes in FP64
 };
 
 struct View {
@@ -595,7 +621,6 @@ struct View {
   DevBuf<unsigned long long> rmax, rmax_scratch;
   DevBuf<double> hist;
   int hcap = 0;
-  DevBuf<char> work;                  // TDMA line scratch
   long long n_l1 = 0;
   // graphs: the whole outer loop (WHILE node) and a single iteration
   cudaGraph_t g_loop = nullptr, g_once = nullptr;
@@ -740,6 +765,66 @@ static int plane_tiles(const mf3d_ctx *C, const std::vector<PlaneExt> &ext, std:
   return best;
 }
 
+// Line relaxation (mg_itrsch 2) on level g: room for every listed block's
+// TDMA factors (six arrays of its cells, k_tdma_factor), pointed to from its
+// table entry, and the shape of k_tdma_lines.  A block whose diagonals hold
+// fewer than 64 lines is one CTA; larger ones take a cluster of up to 8 CTAs,
+// each CTA owning a slice of at least 16 line positions of every diagonal.
+static int tdma_layout(mf3d_ctx *C, View &V, int g, std::vector<BlkLev> &tab) {
+  ViewLevel &L = V.lv[g];
+  const int nb = (int)V.blk.size();
+  L.td_fp64 = C->elem == 8 || (C->coarse64 && g >= V.Lmax);
+  const size_t sz = L.td_fp64 ? 8 : 4;
+  size_t bytes = 0;
+  std::vector<size_t> off(nb, 0);
+  int numax = 1, nmax = 1;
+  L.td_lines[0] = L.td_lines[1] = L.td_lines[2] = 0;
+  for (int b = 0; b < nb; ++b) {
+    if (g > V.blk[b]->ngrid) continue;
+    const BlkLev &B = tab[b];
+    off[b] = bytes;
+    bytes += ((size_t)6 * B.nx * B.ny * B.nz * sz + 255) / 256 * 256;
+    numax = std::max(numax, std::max(B.nx, B.ny));
+    nmax = std::max(nmax, std::max(B.nx, std::max(B.ny, B.nz)));
+    L.td_lines[0] = std::max(L.td_lines[0], B.nx * B.nz);
+    L.td_lines[1] = std::max(L.td_lines[1], B.ny * B.nz);
+    L.td_lines[2] = std::max(L.td_lines[2], B.nx * B.ny);
+  }
+  int st;
+  if ((st = L.tdf.alloc(std::max<size_t>(bytes, 256)))) return st;
+  for (int b = 0; b < nb; ++b)
+    if (g <= V.blk[b]->ngrid) tab[b].tdf = L.tdf.p + off[b];
+  L.td_cl = numax >= 64 ? std::min(8, numax / 16) : 1;
+  if (const char *e = std::getenv("MF3D_TD_CLUSTER")) L.td_cl = std::max(1, std::min(8, std::atoi(e)));  // tuning
+  const int per = (numax + L.td_cl - 1) / L.td_cl;
+  const size_t cap = 200 * 1024;
+  L.td_gmax = (int)std::max<size_t>(1, std::min<size_t>(per, cap / ((7 * (size_t)nmax + 9) * sz)));
+  L.td_nmax = nmax;
+  L.td_smem = (7 * (size_t)L.td_gmax * (nmax + 1) + 2 * (size_t)L.td_gmax) * sz;
+  if (L.td_smem > cap) {
+    set_error("line relaxation: a line of " + std::to_string(nmax) + " cells does not fit in shared memory");
+    return MF3D_E_UNSUPPORTED;
+  }
+  // the limit of every level (the attribute is the kernel's, not the launch's)
+  if (L.td_fp64) CK(cudaFuncSetAttribute(k_tdma_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
+  else CK(cudaFuncSetAttribute(k_tdma_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
+  return MF3D_OK;
+}
+
+// The TDMA factors of every level of the view (after its coefficients).
+static void tdma_factors(mf3d_ctx *C, View &V) {
+  for (int g = 1; g <= V.Lmax; ++g) {
+    ViewLevel &L = V.lv[g];
+    if (!L.n_list[SUB_A]) continue;
+    for (int dir = 0; dir < 3; ++dir) {
+      const dim3 grid((unsigned)((L.td_lines[dir] + 127) / 128), (unsigned)L.n_list[SUB_A]);
+      if (L.td_fp64) launch(k_tdma_factor<double>, grid, 128, 0, C->stream, L.tab.p, L.list[SUB_A].p, dir);
+      else launch(k_tdma_factor<float>, grid, 128, 0, C->stream, L.tab.p, L.list[SUB_A].p, dir);
+      ++C->launches;
+    }
+  }
+}
+
 // Build the launch tables of a view over `doms` (all of one precision).
 static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &doms, int hcap) {
   cudaStream_t s = C->stream;
@@ -758,7 +843,6 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
   V.lv.clear();
   V.lv.resize(V.Lmax + 1);
   int st;
-  size_t work_elems = 0;
   for (int g = 1; g <= V.Lmax; ++g) {
     ViewLevel &L = V.lv[g];
     std::vector<BlkLev> tab(nb);
@@ -780,8 +864,8 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
         li[q].push_back(b);
         L.cells_sub[q] += (long long)B.nx * B.ny * B.nz;
       }
-      L.ngg = std::max(L.ngg, std::max(B.nx, std::max(B.ny, B.nz)) + 2);
     }
+    if (C->prm.mg_itrsch == 2 && (st = tdma_layout(C, V, g, tab))) return st;
     if ((st = L.tab.upload(tab, s))) return st;
     {
       // restriction into level g (g > 1): every block present here; prolongation
@@ -849,7 +933,6 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       if ((st = L.sweep[q].upload(sw[q], s))) return st;
       if ((st = L.cells[q].upload(ce[q], s))) return st;
       if ((st = L.list[q].upload(li[q], s))) return st;
-      work_elems = std::max(work_elems, (size_t)L.n_list[q] * 128 * 2 * L.ngg);
     }
     // halo segments: the domains' resident pair lists
     for (int q = 0; q < 3; ++q) {
@@ -879,7 +962,6 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       if ((st = L.stage[q].alloc((size_t)std::max<long long>(ns, 1) * 8))) return st;
     }
   }
-  if (C->prm.mg_itrsch == 2 && (st = V.work.alloc(std::max<size_t>(work_elems, 1) * 8))) return st;
   // level-1 field tables
   V.hf.resize(nb);
   std::vector<Tile> t1, t2, t5;
@@ -954,6 +1036,8 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
   CK(cudaMemsetAsync(V.rmax.p, 0, V.rmax.n * sizeof(unsigned long long), s));
   V.hcap = std::max(hcap, 1);
   if ((st = V.hist.alloc((size_t)std::max(nd, 1) * V.hcap))) return st;
+  // the line relaxation's factors; under L_LSM every solve forms them anew
+  if (C->prm.mg_itrsch == 2 && !C->prm.lsm) tdma_factors(C, V);
   CK(cudaStreamSynchronize(s));
   return MF3D_OK;
 }
@@ -1023,7 +1107,12 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bo
       launch(k_lexgs<T>, L.n_list[q], 1024, 0, C->stream, L.tab.p, L.list[q].p, V.act.p);
       ++C->launches;
     } else {
-      launch(k_tdma<T>, L.n_list[q], 128, 0, C->stream, L.tab.p, L.list[q].p, V.act.p, (T *)V.work.p, L.ngg);
+      // three passes, each reading rhs and phi and writing phi once
+      const int pk = (g == 1 && q == SUB_A) ? MF3D_PROF_SMOOTH_L1 : 0;
+      prof_begin(C, pk, 9.0 * (double)L.cells_sub[q] * sizeof(T));
+      launch_cl(k_tdma_lines<T>, L.n_list[q] * L.td_cl, TD_THREADS, L.td_smem, C->stream, L.td_cl, L.tab.p,
+                L.list[q].p, V.act.p, L.td_cl, L.td_gmax, L.td_nmax);
+      prof_end(C, pk);
       ++C->launches;
     }
     halo<T>(C, V, g, q);
@@ -1171,18 +1260,28 @@ static int build_graphs(mf3d_ctx *C, View &V) {
   cudaGraphNode_t node;
   CK(cudaGraphAddNode(&node, V.g_loop, nullptr, 0, &np));
   cudaGraph_t body = np.conditional.phGraph_out[0];
-  CK(cudaStreamBeginCaptureToGraph(C->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  // a failed capture leaves no partial graph and the counters as they were
+  auto fail = [&](cudaError_t e, const char *what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    C->launches = saved_launches;
+    C->prof_kind = saved_prof;
+    V.drop_graphs();
+    return MF3D_E_CUDA;
+  };
+  cudaError_t e = cudaStreamBeginCaptureToGraph(C->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return fail(e, "cudaStreamBeginCaptureToGraph");
   C->launches = 0;
   iteration_body<T>(C, V, 1);
   V.launches_per_iter = C->launches;
-  cudaGraph_t captured;
-  CK(cudaStreamEndCapture(C->stream, &captured));
-  CK(cudaGraphInstantiate(&V.x_loop, V.g_loop, 0));
+  cudaGraph_t captured = nullptr;
+  if ((e = cudaStreamEndCapture(C->stream, &captured)) != cudaSuccess) return fail(e, "capture of the outer loop");
+  if ((e = cudaGraphInstantiate(&V.x_loop, V.g_loop, 0)) != cudaSuccess) return fail(e, "cudaGraphInstantiate");
   // one iteration (the server's per-cycle step)
-  CK(cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeRelaxed));
+  if ((e = cudaStreamBeginCapture(C->stream, cudaStreamCaptureModeRelaxed)) != cudaSuccess)
+    return fail(e, "cudaStreamBeginCapture");
   iteration_body<T>(C, V, 0);
-  CK(cudaStreamEndCapture(C->stream, &V.g_once));
-  CK(cudaGraphInstantiate(&V.x_once, V.g_once, 0));
+  if ((e = cudaStreamEndCapture(C->stream, &V.g_once)) != cudaSuccess) return fail(e, "capture of one iteration");
+  if ((e = cudaGraphInstantiate(&V.x_once, V.g_once, 0)) != cudaSuccess) return fail(e, "cudaGraphInstantiate");
   C->launches = saved_launches;
   C->prof_kind = saved_prof;
   return MF3D_OK;
@@ -1309,7 +1408,10 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
   CK(cudaMemcpyAsync(V.ds.p, hs.data(), nd * sizeof(DomState), cudaMemcpyHostToDevice, s));
   CK(cudaStreamSynchronize(s));  // hs is a local
   CK(cudaMemsetAsync(V.rmax.p, 0, nd * sizeof(unsigned long long), s));
-  if (C->prm.lsm) lsm_coefficients(C, V);
+  if (C->prm.lsm) {
+    lsm_coefficients(C, V);
+    if (C->prm.mg_itrsch == 2) tdma_factors(C, V);
+  }
   launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p, C->walls_given ? 1 : 0);
   calvel_calmas<T>(C, V, V.ones.p, V.rmax.p, 0);
   launch(k_dom_init, 1, 256, 0, s, V.ds.p, nd, V.rmax.p, V.act.p);
