@@ -177,10 +177,11 @@ def oracle_lib():
     return lib
 
 
-def time_oracle_iterations(pr, n_iter: int, threads: int, lsm: int = 0):
+def time_oracle_iterations(pr, n_iter: int, threads: int, lsm: int = 0, scheme: int = 3):
     """Run the oracle's newsolv_mg for n_iter outer iterations on the full
     workload; returns (seconds of the initial calvel/calmas, per-iteration
-    seconds list).  lsm: variable density (densities as run_density's)."""
+    seconds list).  lsm: variable density (densities as run_density's);
+    scheme: mg_itrsch."""
     import numpy as np
     from multiflow3d_b200.abi import SolveInfo
     from multiflow3d_b200.problems import fields_struct
@@ -192,7 +193,7 @@ def time_oracle_iterations(pr, n_iter: int, threads: int, lsm: int = 0):
             f["dens"] = dn
     stamps = np.zeros(n_iter + 4)
     orc.orc_set_timestamps(stamps.ctypes.data_as(C.POINTER(C.c_double)), len(stamps))
-    prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=n_iter, eps=1e-300, lsm=lsm)
+    prm = pr.params(mg_itrsch=scheme, irestr=2, iproln=1, maxcy=n_iter, eps=1e-300, lsm=lsm)
     info = SolveInfo()
     hist = np.zeros(n_iter)
     orc.orc_newsolv_mg(pr.descriptors(orc), pr.nblocks, C.byref(prm), fields_struct(blocks), 1.0, 1.0,
@@ -507,6 +508,56 @@ def run_density(args):
         cpu = 1.0 / (t_init + r.iter * t_it)
         line["cpu_baseline"] = {"value": cpu, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"10 timed outer iterations of the same solve on the oracle "
+                                          f"({threads} threads), scaled to {r.iter} iterations"}
+        line["speedup_vs_cpu"] = value / cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_linegs(args):
+    """The reference's default smoother, line Gauss-Seidel with Thomas
+    solves (mg_itrsch 2, control.cin), on the default workload's problem:
+    2x2x2 blocks of 128^3 (256^3), tanh y-stretch 2.0, 6 levels, (2,1)
+    sweeps, rel tol 1e-10, FP64.  CPU baseline: the oracle on the same
+    inputs, 8 threads (one per block), a bounded number of outer iterations
+    scaled to the GPU's iteration count (the two agree bit for bit)."""
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.solver import Projection
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    pr = make_problem()
+    host = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    keys = ("ustar", "vstar", "wstar", "u", "v", "w", "p")
+    d = [{k: torch.from_numpy(f[k]).to(dev) for k in keys} for f in host]
+    pristine = [{k: f[k].clone() for k in ("u", "v", "w", "p")} for f in d]
+
+    def reset():
+        for f, p0 in zip(d, pristine):
+            for k in ("u", "v", "w", "p"):
+                f[k].copy_(p0[k])
+
+    prm = pr.params(mg_itrsch=2, irestr=2, iproln=1, maxcy=400, eps=1e-10, eps_relative=1)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    sec, r = _timed_solves(lambda: proj.newsolv_mg_device(d), reset, args.steps, args.warmup)
+    proj.close()
+    value = args.steps / sec
+    line = {
+        "metric": "poisson_solves_per_s_line_gs", "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3, "higher_is_better": True, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "line Gauss-Seidel (mg_itrsch 2), 2x2x2 blocks of 128^3 (256^3), tanh y-stretch "
+                               "2.0, 6 levels, (2,1) sweeps, rel tol 1e-10"},
+        "iterations": r.iter, "status": r.status, "rel_rmax": r.rmax / r.rmax0,
+        "ms_per_iteration": sec / args.steps * 1e3 / max(r.iter, 1),
+    }
+    if not args.no_cpu_baseline:
+        threads = max(1, min(os.cpu_count() or 1, pr.nblocks))
+        t_init, its = time_oracle_iterations(pr, 3, threads, scheme=2)
+        t_it = sum(its[1:]) / len(its[1:])
+        cpu = 1.0 / (t_init + r.iter * t_it)
+        line["cpu_baseline"] = {"value": cpu, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"2 timed outer iterations of the same solve on the oracle "
                                           f"({threads} threads), scaled to {r.iter} iterations"}
         line["speedup_vs_cpu"] = value / cpu
     print(json.dumps(line), flush=True)
@@ -846,7 +897,7 @@ def main():
     ap.add_argument("--impl", default="mf3d", choices=["mf3d", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="multiblock",
-                    choices=["multiblock", "mixed", "batched", "served", "density", "tecbin", "sip"],
+                    choices=["multiblock", "mixed", "batched", "served", "density", "tecbin", "sip", "linegs"],
                     help="multiblock: the default FP64 line; mixed / batched / served / density: the further "
                          "workloads (1 GPU)")
     ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
@@ -867,6 +918,8 @@ def main():
         return run_tecbin(args)
     if args.workload == "sip":
         return run_sip(args)
+    if args.workload == "linegs":
+        return run_linegs(args)
     return run_gpu(args)
 
 
