@@ -769,7 +769,7 @@ static int plane_tiles(const mf3d_ctx *C, const std::vector<PlaneExt> &ext, std:
 // TDMA factors (six arrays of its cells, k_tdma_factor), pointed to from its
 // table entry, and the shape of k_tdma_lines.  A block whose diagonals hold
 // fewer than 64 lines is one CTA; larger ones take a cluster of up to 8 CTAs,
-// each CTA owning a slice of at least 16 line positions of every diagonal.
+// each CTA owning a slice of at least 8 line positions of every diagonal.
 static int tdma_layout(mf3d_ctx *C, View &V, int g, std::vector<BlkLev> &tab) {
   ViewLevel &L = V.lv[g];
   const int nb = (int)V.blk.size();
@@ -794,20 +794,28 @@ static int tdma_layout(mf3d_ctx *C, View &V, int g, std::vector<BlkLev> &tab) {
   if ((st = L.tdf.alloc(std::max<size_t>(bytes, 256)))) return st;
   for (int b = 0; b < nb; ++b)
     if (g <= V.blk[b]->ngrid) tab[b].tdf = L.tdf.p + off[b];
-  L.td_cl = numax >= 64 ? std::min(8, numax / 16) : 1;
-  if (const char *e = std::getenv("MF3D_TD_CLUSTER")) L.td_cl = std::max(1, std::min(8, std::atoi(e)));  // tuning
-  const int per = (numax + L.td_cl - 1) / L.td_cl;
   const size_t cap = 200 * 1024;
-  L.td_gmax = (int)std::max<size_t>(1, std::min<size_t>(per, cap / ((7 * (size_t)nmax + 9) * sz)));
+  // the kernel's limits (the attributes are the kernel's, not the launch's)
+  void (*kern)(const BlkLev *, const int *, const int *, int, int, int) =
+      L.td_fp64 ? (void (*)(const BlkLev *, const int *, const int *, int, int, int))k_tdma_lines<double>
+                : (void (*)(const BlkLev *, const int *, const int *, int, int, int))k_tdma_lines<float>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
+  // shape for cl CTAs per block: lines staged at a time and shared memory
+  auto shape = [&](int cl, int &gmax, size_t &smem) {
+    const int per = (numax + cl - 1) / cl;
+    gmax = (int)std::max<size_t>(1, std::min<size_t>(per, cap / ((7 * (size_t)nmax + 9) * sz)));
+    smem = (7 * (size_t)gmax * (nmax + 1) + 2 * (size_t)gmax) * sz;
+  };
+  // 16-CTA clusters (non-portable) measured slower: 18.1 against 11.2 ms per
+  // finest-level relaxation of 2x2x2 blocks of 128^3
+  L.td_cl = numax >= 64 ? std::min(8, numax / 8) : 1;
+  if (const char *e = std::getenv("MF3D_TD_CLUSTER")) L.td_cl = std::max(1, std::min(8, std::atoi(e)));  // tuning
+  shape(L.td_cl, L.td_gmax, L.td_smem);
   L.td_nmax = nmax;
-  L.td_smem = (7 * (size_t)L.td_gmax * (nmax + 1) + 2 * (size_t)L.td_gmax) * sz;
   if (L.td_smem > cap) {
     set_error("line relaxation: a line of " + std::to_string(nmax) + " cells does not fit in shared memory");
     return MF3D_E_UNSUPPORTED;
   }
-  // the limit of every level (the attribute is the kernel's, not the launch's)
-  if (L.td_fp64) CK(cudaFuncSetAttribute(k_tdma_lines<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
-  else CK(cudaFuncSetAttribute(k_tdma_lines<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
   return MF3D_OK;
 }
 
