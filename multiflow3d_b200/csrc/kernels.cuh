@@ -369,36 +369,52 @@ __global__ void __launch_bounds__(kTile) k_rbgs_small(const BlkLev *__restrict__
   M[base + h] = ((R[base + h] - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
 }
 
+// All of a cluster's CTAs (one hardware barrier; release/acquire at cluster
+// scope, so global stores before it are seen by the cluster after it).
+// Every warp reaches it converged: a __syncthreads() comes first.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 // ---------------------------------------------------------------------------
-// Lexicographic Gauss-Seidel (mgsolver.for:403-428), loop order k, j, i:
+// Lexicographic Gauss-Seidel (mgsolver.for:403-428), loop order k, i, j:
 // cell (i,j,k) reads new values at i-1, j-1, k-1 and old ones at i+1, j+1,
-// k+1, so every hyperplane i+j+k = const is independent.  One CTA per block
-// walks the hyperplanes in order (a parity kernel for small blocks).
+// k+1, so every hyperplane i+j+k = const is independent and the planes run
+// in order.  Each block is a cluster of `cl` CTAs (cl = 1: a plain CTA),
+// CTA r owning a slice of k; per plane its threads take the slice's (j, k)
+// with i = plane - j - k inside the block, and a cluster barrier closes the
+// plane.  The neighbours are read through L2 (ld.global.cg): the k-1 layer
+// of a slice's first plane was written by the previous CTA of the cluster.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_lexgs(const BlkLev *__restrict__ bl, const int *__restrict__ blocks, const int *__restrict__ act) {
+__global__ void __launch_bounds__(1024) k_lexgs(const BlkLev *__restrict__ bl, const int *__restrict__ blocks,
+                                                const int *__restrict__ act, int cl) {
   pdl_wait();
-  const BlkLev B = bl[blocks[blockIdx.x]];
-  if (!act[B.dom]) return;
+  const BlkLev B = bl[blocks[blockIdx.x / cl]];
+  if (!act[B.dom]) return;  // every CTA of the cluster holds the same block
+  const int rank = blockIdx.x % cl;
   T *P = phi_of<T>(B);
   const T *R = rhs_of<T>(B);
   const Coef<T> cf(B);
   const int nx = B.nx, ny = B.ny, nz = B.nz;
+  const int per = (nz + cl - 1) / cl, klo = rank * per + 1, khi = min(nz, klo + per - 1);
   for (int sum = 3; sum <= nx + ny + nz; ++sum) {
-    for (int idx = threadIdx.x; idx < ny * nz; idx += blockDim.x) {
-      const int j = idx % ny + 1, k = idx / ny + 1;
+    const int kb = max(klo, sum - nx - ny), ke = min(khi, sum - 2);
+    for (int idx = threadIdx.x; idx < (ke - kb + 1) * ny; idx += blockDim.x) {
+      const int j = idx % ny + 1, k = kb + idx / ny;
       const int i = sum - j - k;
       if (i < 1 || i > nx) continue;
       T aw, ae, as, an, ab, at;
       cell_coefs(B, cf, i, j, k, aw, ae, as, an, ab, at);
       const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-      const T w = P[cell_off(B, i - 1, j, k)], e = P[cell_off(B, i + 1, j, k)];
-      const T so = P[cell_off(B, i, j - 1, k)], no = P[cell_off(B, i, j + 1, k)];
-      const T bo = P[cell_off(B, i, j, k - 1)], to = P[cell_off(B, i, j, k + 1)];
+      const T w = __ldcg(P + cell_off(B, i - 1, j, k)), e = __ldcg(P + cell_off(B, i + 1, j, k));
+      const T so = __ldcg(P + cell_off(B, i, j - 1, k)), no = __ldcg(P + cell_off(B, i, j + 1, k));
+      const T bo = __ldcg(P + cell_off(B, i, j, k - 1)), to = __ldcg(P + cell_off(B, i, j, k + 1));
       const T r = R[cell_off(B, i, j, k)];
       P[cell_off(B, i, j, k)] = ((r - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
     }
     __syncthreads();
+    if (cl > 1) cluster_sync_all();
   }
 }
 
@@ -463,12 +479,6 @@ __global__ void k_tdma_factor(const BlkLev *__restrict__ bl, const int *__restri
     A[m - 1] = am;
     R[m - 1] = apr;
   }
-}
-
-// All of a cluster's CTAs (one hardware barrier; release/acquire at cluster
-// scope, so global stores before it are seen by the cluster after it).
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 constexpr int TD_THREADS = 512, TD_CH = 8;

@@ -594,6 +594,7 @@ struct ViewLevel {
   // k_tdma_lines shape: cluster size, lines staged at a time, longest line
   DevBuf<char> tdf;
   int td_cl = 1, td_gmax = 1, td_nmax = 1, td_lines[3] = {0, 0, 0};
+  int lx_cl = 1;                      // lexicographic relaxation (mg_itrsch 1): CTAs per block
   size_t td_smem = 0;
   bool td_fp64 = true;                // the level relaxes in FP64
 };
@@ -874,6 +875,12 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       }
     }
     if (C->prm.mg_itrsch == 2 && (st = tdma_layout(C, V, g, tab))) return st;
+    if (C->prm.mg_itrsch == 1) {  // slices of k of at least 8 planes, up to 8 CTAs per block
+      int nzmax = 1;
+      for (int b = 0; b < nb; ++b)
+        if (g <= V.blk[b]->ngrid) nzmax = std::max(nzmax, tab[b].nz);
+      L.lx_cl = nzmax >= 64 ? std::min(8, nzmax / 8) : 1;
+    }
     if ((st = L.tab.upload(tab, s))) return st;
     {
       // restriction into level g (g > 1): every block present here; prolongation
@@ -1112,7 +1119,8 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bo
       prof_end(C, pk);
       C->launches += skip_red ? 1 : 2;
     } else if (sch == 1) {
-      launch(k_lexgs<T>, L.n_list[q], 1024, 0, C->stream, L.tab.p, L.list[q].p, V.act.p);
+      launch_cl(k_lexgs<T>, L.n_list[q] * L.lx_cl, 1024, 0, C->stream, L.lx_cl, L.tab.p, L.list[q].p, V.act.p,
+                L.lx_cl);
       ++C->launches;
     } else {
       // three passes, each reading rhs and phi and writing phi once

@@ -1,4 +1,6 @@
-"""Line Gauss-Seidel (mg_itrsch 2, mgsolver.for:430-545) at the block sizes
+"""Line and lexicographic Gauss-Seidel (mg_itrsch 2 and 1) at the block
+sizes where the device splits each block over a cluster of CTAs.  Line
+Gauss-Seidel (mg_itrsch 2, mgsolver.for:430-545) at the block sizes
 where the device sweeps each block's line diagonals with a cluster of CTAs
 (lines of 64 cells and more: the slices of a diagonal meet at CTA borders,
 where a line reads its neighbour line from another CTA's results) against
@@ -38,4 +40,22 @@ def test_line_gs_clustered_variable_density(lib, oracle, cuda):
     for f, d in zip(blocks, pr.block_density(43)):
         f["dens"] = d
     o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks)
+    assert_same(o, g, pr.pl)
+
+
+LEX_LAYOUTS = {
+    "2x1x1 blocks of 64^3, stretched y": lambda: Problem(2, 1, 1, 64, 64, 64, ngrid=3, pl=2, stretch_y=2.0),
+    "1 block of 96x64x128, walls": lambda: Problem(1, 1, 1, 96, 64, 128, bc=(W,) * 6, ngrid=3, pl=1),
+}
+
+
+@pytest.mark.parametrize("layout", sorted(LEX_LAYOUTS))
+def test_lex_gs_clustered_matches_oracle(lib, oracle, cuda, layout):
+    """Lexicographic Gauss-Seidel (mg_itrsch 1, mgsolver.for:403-428) where
+    each block's hyperplanes are split over a cluster of CTAs by k (64 and
+    more planes): a slice's first plane reads the previous CTA's results."""
+    pr = LEX_LAYOUTS[layout]()
+    prm = pr.params(mg_itrsch=1, maxcy=2, eps=1e-12)
+    o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm,
+                    pr.block_fields(seed=44, fourier_modes=2))
     assert_same(o, g, pr.pl)
