@@ -28,9 +28,14 @@ def dev_fields(pr, seed, cuda):
     return [{k: torch.from_numpy(v).to(cuda) for k, v in f.items()} for f in pr.block_fields(seed=seed)]
 
 
-def test_batch_matches_oracle_and_solo(lib, oracle, cuda):
-    doms = make_domains(6, seed=3, lo=8, hi=40)
-    prm = doms[0].params(mg_itrsch=3, maxcy=150, eps=1e-9, precision=MF3D_PREC_FP64)
+@pytest.mark.parametrize("scheme,seed,hi,maxcy", [(3, 3, 40, 150), (2, 3, 40, 40), (1, 3, 40, 40),
+                                                  (2, 4, 96, 6), (1, 4, 96, 6)])
+def test_batch_matches_oracle_and_solo(lib, oracle, cuda, scheme, seed, hi, maxcy):
+    """hi = 96: domains with 64 cells and more along an axis share the view
+    with small ones, so the line and lexicographic relaxations run every
+    block of a level as a CTA cluster, with empty slices for the small ones."""
+    doms = make_domains(6, seed=seed, lo=8, hi=hi)
+    prm = doms[0].params(mg_itrsch=scheme, maxcy=maxcy, eps=1e-9, precision=MF3D_PREC_FP64)
     prm.ngrid = 1  # per-domain depth comes from the domain descriptors
     batch = Batch([domain_desc(pr) for pr in doms], prm, lib)
     fields = [dev_fields(pr, 100 + d, cuda)[0] for d, pr in enumerate(doms)]
@@ -40,7 +45,7 @@ def test_batch_matches_oracle_and_solo(lib, oracle, cuda):
     for d, pr in enumerate(doms):
         # oracle, solo
         ref = pr.block_fields(seed=100 + d)
-        p = pr.params(mg_itrsch=3, maxcy=150, eps=1e-9)
+        p = pr.params(mg_itrsch=scheme, maxcy=maxcy, eps=1e-9)
         info = SolveInfo()
         hist = np.zeros(p.maxcy)
         st_ref = oracle.orc_newsolv_mg(pr.descriptors(oracle), 1, C.byref(p), fields_struct(ref), 1.0, 1.0,
