@@ -769,8 +769,9 @@ static int plane_tiles(const mf3d_ctx *C, const std::vector<PlaneExt> &ext, std:
 // Line relaxation (mg_itrsch 2) on level g: room for every listed block's
 // TDMA factors (six arrays of its cells, k_tdma_factor), pointed to from its
 // table entry, and the shape of k_tdma_lines.  A block whose diagonals hold
-// fewer than 64 lines is one CTA; larger ones take a cluster of up to 8 CTAs,
-// each CTA owning a slice of at least 8 line positions of every diagonal.
+// fewer than 64 lines is one CTA; larger ones take a cluster of 8 CTAs or
+// more (below), each CTA owning a slice of at least 8 line positions of
+// every diagonal.
 static int tdma_layout(mf3d_ctx *C, View &V, int g, std::vector<BlkLev> &tab) {
   ViewLevel &L = V.lv[g];
   const int nb = (int)V.blk.size();
@@ -807,10 +808,38 @@ static int tdma_layout(mf3d_ctx *C, View &V, int g, std::vector<BlkLev> &tab) {
     gmax = (int)std::max<size_t>(1, std::min<size_t>(per, cap / ((7 * (size_t)nmax + 9) * sz)));
     smem = (7 * (size_t)gmax * (nmax + 1) + 2 * (size_t)gmax) * sz;
   };
-  // 16-CTA clusters (non-portable) measured slower: 18.1 against 11.2 ms per
-  // finest-level relaxation of 2x2x2 blocks of 128^3
+  // Up to 8 CTAs per block (portable clusters); more (non-portable, up to
+  // 16) only where the device holds a cluster for every block of the level
+  // at once - 16 with too few resident measured slower (18.1 against 11.2 ms
+  // per finest-level relaxation of 2x2x2 blocks of 128^3; 12 CTAs, of which
+  // fewer than 8 clusters fit: 19.6 ms).  There the query picks 10: 10.5 ms.
   L.td_cl = numax >= 64 ? std::min(8, numax / 8) : 1;
-  if (const char *e = std::getenv("MF3D_TD_CLUSTER")) L.td_cl = std::max(1, std::min(8, std::atoi(e)));  // tuning
+  int nblk = 0;
+  for (int b = 0; b < nb; ++b) nblk += g <= V.blk[b]->ngrid;
+  if (numax >= 128 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+    for (int cl = std::min(16, numax / 8); cl > 8; --cl) {
+      int gm;
+      size_t sm;
+      shape(cl, gm, sm);
+      cudaLaunchAttribute at;
+      at.id = cudaLaunchAttributeClusterDimension;
+      at.val.clusterDim.x = (unsigned)cl;
+      at.val.clusterDim.y = at.val.clusterDim.z = 1;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)cl);
+      cfg.blockDim = dim3(TD_THREADS);
+      cfg.dynamicSmemBytes = sm;
+      cfg.attrs = &at;
+      cfg.numAttrs = 1;
+      int ncl = 0;
+      if (cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg) == cudaSuccess && ncl >= nblk) {
+        L.td_cl = cl;
+        break;
+      }
+    }
+    cudaGetLastError();  // a refused query leaves no error behind
+  }
+  if (const char *e = std::getenv("MF3D_TD_CLUSTER")) L.td_cl = std::max(1, std::min(16, std::atoi(e)));  // tuning
   shape(L.td_cl, L.td_gmax, L.td_smem);
   L.td_nmax = nmax;
   if (L.td_smem > cap) {
