@@ -904,11 +904,36 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       }
     }
     if (C->prm.mg_itrsch == 2 && (st = tdma_layout(C, V, g, tab))) return st;
-    if (C->prm.mg_itrsch == 1) {  // slices of k of at least 8 planes, up to 8 CTAs per block
-      int nzmax = 1;
+    if (C->prm.mg_itrsch == 1) {
+      // slices of k of at least 8 planes: up to 8 CTAs per block, up to 16
+      // (non-portable) where the device holds a cluster for every block at once
+      int nzmax = 1, nblk = 0;
       for (int b = 0; b < nb; ++b)
-        if (g <= V.blk[b]->ngrid) nzmax = std::max(nzmax, tab[b].nz);
+        if (g <= V.blk[b]->ngrid) { nzmax = std::max(nzmax, tab[b].nz); ++nblk; }
       L.lx_cl = nzmax >= 64 ? std::min(8, nzmax / 8) : 1;
+      void (*kern)(const BlkLev *, const int *, const int *, int) =
+          C->elem == 8 ? (void (*)(const BlkLev *, const int *, const int *, int))k_lexgs<double>
+                       : (void (*)(const BlkLev *, const int *, const int *, int))k_lexgs<float>;
+      if (nzmax >= 128 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+        for (int cl = std::min(16, nzmax / 8); cl > 8; --cl) {
+          cudaLaunchAttribute at;
+          at.id = cudaLaunchAttributeClusterDimension;
+          at.val.clusterDim.x = (unsigned)cl;
+          at.val.clusterDim.y = at.val.clusterDim.z = 1;
+          cudaLaunchConfig_t cfg = {};
+          cfg.gridDim = dim3((unsigned)cl);
+          cfg.blockDim = dim3(1024);
+          cfg.attrs = &at;
+          cfg.numAttrs = 1;
+          int ncl = 0;
+          if (cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg) == cudaSuccess && ncl >= nblk) {
+            L.lx_cl = cl;
+            break;
+          }
+        }
+        cudaGetLastError();  // a refused query leaves no error behind
+      }
+      if (const char *e = std::getenv("MF3D_LX_CLUSTER")) L.lx_cl = std::max(1, std::min(16, std::atoi(e)));  // tuning
     }
     if ((st = L.tab.upload(tab, s))) return st;
     {
