@@ -65,6 +65,38 @@ def test_mixed_matches_fp64_oracle(lib, oracle, cuda, case):
         assert np.abs(g - r).max() <= ERR_BAR * np.abs(r).max()
 
 
+SMOOTHER_CASES = [
+    ("line GS, 2x1x1 blocks of 64^3 (8-CTA clusters at level 1)", 2,
+     Problem(2, 1, 1, 64, 64, 64, ngrid=4, pl=2, stretch_y=2.0), 1e-8),
+    ("line GS, config 1: 64x32x32", 2, Problem(1, 1, 1, 64, 32, 32, ngrid=4, pl=2), 1e-8),
+    ("lex GS, 2x1x1 blocks of 32x32x64 (8-CTA clusters at level 1)", 1,
+     Problem(2, 1, 1, 32, 32, 64, bc=(WALL,) * 6, ngrid=3, pl=1), 1e-8),
+]
+
+
+@pytest.mark.parametrize("case", SMOOTHER_CASES, ids=[c[0] for c in SMOOTHER_CASES])
+def test_mixed_other_smoothers(lib, oracle, cuda, case):
+    """The FP32 line and lexicographic relaxations (mgsolver.for:403-545),
+    clustered and not, against the FP64 oracle with the same smoother, to
+    the bars above."""
+    import torch
+    _, sch, pr, tol = case
+    ref, info = oracle_solve(oracle, pr, pr.params(mg_itrsch=sch, maxcy=300, eps=tol), seed=6)
+    prm = pr.params(mg_itrsch=sch, maxcy=300, eps=tol, precision=abi.MF3D_PREC_FP32)
+    blocks = pr.block_fields(seed=6, fourier_modes=4)
+    dev = [{k: torch.from_numpy(v).to(cuda) for k, v in f.items()} for f in blocks]
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    res = proj.newsolv_mg_device(dev)
+    proj.close()
+    got = [{k: v.cpu().numpy() for k, v in f.items()} for f in dev]
+    assert res.status == 0 and res.rmax < tol * res.rmax0
+    assert res.iter <= info.iter + 2
+    assert rel_mean_free(pr.gather(got, "p"), pr.gather(ref, "p")) <= ERR_BAR
+    for k in ("u", "v", "w"):
+        g, r = pr.gather(got, k), pr.gather(ref, k)
+        assert np.abs(g - r).max() <= ERR_BAR * np.abs(r).max()
+
+
 @pytest.mark.parametrize("same_depth", [True, False])
 def test_mixed_batch(lib, cuda, same_depth):
     """A batch in mixed precision (FP64 coarsest level only when every domain
