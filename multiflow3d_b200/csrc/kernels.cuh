@@ -175,6 +175,37 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+// L2 eviction priorities (createpolicy): a line loaded or stored with
+// evict_last outlives evict_normal and evict_first lines in L2.
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+// tma_load_3d with an L2 eviction priority for the loaded lines
+__device__ __forceinline__ void tma_load_3d_hint(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y, int z,
+                                                 uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], "
+      "[%1, {%3, %4, %5}], [%2], %6;" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z), "l"(pol)
+      : "memory");
+}
+// a store with an L2 eviction priority
+__device__ __forceinline__ void st_hint(double *p, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(__cvta_generic_to_global(p)), "d"(v), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void st_hint(float *p, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(__cvta_generic_to_global(p)), "f"(v), "l"(pol)
+               : "memory");
+}
+
 // ---------------------------------------------------------------------------
 // Red-black Gauss-Seidel half-sweep (mgsolver.for:547-601) of one colour over
 // a set of blocks: phi = (rhs - (aw*w + ae*e + as*s + an*n + ab*b + at*t)) /
@@ -257,13 +288,16 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
   constexpr int first = FROM_ZERO ? 0 : 1;
   auto stage = [&](int kk) { return (kk - k0 + first) & (RB_NS - 1); };
   auto parity = [&](int kk) { return (unsigned)(((kk - k0 + first) / RB_NS) & 1); };
+  // L2: the rhs is read once per half-sweep (evict first); the colour
+  // written here is what the next half-sweep reads (evict last)
+  const uint64_t pol_first = l2_evict_first(), pol_last = l2_evict_last();
   auto issue = [&](int kk) {
     const int st = stage(kk);
     const bool wr = kk >= k0 && kk <= k1;
     const unsigned bytes = (FROM_ZERO ? 0u : (unsigned)(S::OE * sizeof(T))) + (wr ? (unsigned)(S::RE * sizeof(T)) : 0u);
     mbar_expect_tx(&bar[st], bytes);
     if (!FROM_ZERO) tma_load_3d(slot_o(st), mo, &bar[st], q0, t.j0 - 1, kk);
-    if (wr) tma_load_3d(slot_r(st), mr, &bar[st], q0, t.j0, kk);
+    if (wr) tma_load_3d_hint(slot_r(st), mr, &bar[st], q0, t.j0, kk, pol_first);
   };
   if (tid == 0) {
     for (int st = 0; st < RB_NS; ++st) mbar_init(&bar[st], 1);
@@ -308,7 +342,8 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
             to = ot[(rr + 1) * W + hc];
           }
           const T ap = (T)-1.0 * (((s ? pa1[m] : pa0[m]) + ab) + at);
-          Mk[rowoff[m]] = ((r[rr * W + hc] - (aw * w + ae * e + as[m] * so_ + an[m] * no + ab * bo + at * to)) / ap);
+          st_hint(Mk + rowoff[m], ((r[rr * W + hc] - (aw * w + ae * e + as[m] * so_ + an[m] * no + ab * bo + at * to)) / ap),
+                  pol_last);
         }
       }
     }
