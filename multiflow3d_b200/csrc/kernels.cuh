@@ -532,7 +532,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // (1) every thread issues asynchronous copies of su, the four transverse
 // neighbours, a and apr of its cells (and the line ends' ghosts) into
 // shared memory, all in flight at once; (2) every thread forms rhs' and lo
-// of its cells there; (3) one thread per line runs the two recurrences.  A
+// of its cells there; (3) one thread per line runs the two recurrences,
+// leaving the new values in shared memory; (4) every thread stores them.  A
 // cluster barrier closes the diagonal.  A line reads only lines of the
 // neighbouring diagonals, so the lines of one diagonal may run in any order.
 // Shared memory: seven arrays of gmax lines at stride nmax+1 (odd, so the
@@ -656,11 +657,22 @@ __global__ void __launch_bounds__(TD_THREADS) k_tdma_lines(const BlkLev *__restr
             for (int q = 0; q < TD_CH; ++q)
               if (m1 - 1 - q >= 0) {
                 pv = (x[q] - y[q] * pv);
-                int i, j, k;
-                tdma_cell(dir, u, v, m1 - q, i, j, k);
-                P[cell_off(B, i, j, k)] = pv;
+                x[q] = pv;
               }
+#pragma unroll
+            for (int q = 0; q < TD_CH; ++q)
+              if (m1 - 1 - q >= 0) cr[m1 - 1 - q] = x[q];
           }
+        }
+        __syncthreads();
+        // (4) every thread stores the group's new values: the line threads
+        // keep only the recurrences
+        for (int e = threadIdx.x; e < gl * n; e += TD_THREADS) {
+          const int g = e / n, m = e - g * n + 1;
+          const int u = ga + g, v = s - u;
+          int i, j, k;
+          tdma_cell(dir, u, v, m, i, j, k);
+          P[cell_off(B, i, j, k)] = rs[g * ld + m - 1];
         }
         __syncthreads();  // the staging arrays are reused by the next group
       }
