@@ -769,7 +769,7 @@ static int plane_tiles(const mf3d_ctx *C, const std::vector<PlaneExt> &ext, std:
 // Line relaxation (mg_itrsch 2) on level g: room for every listed block's
 // TDMA factors (six arrays of its cells, k_tdma_factor), pointed to from its
 // table entry, and the shape of k_tdma_lines.  A block whose diagonals hold
-// fewer than 64 lines is one CTA; larger ones take a cluster of 8 CTAs or
+// fewer than 32 lines is one CTA; larger ones take a cluster of 4 CTAs or
 // more (below), each CTA owning a slice of at least 8 line positions of
 // every diagonal.
 static int tdma_layout(mf3d_ctx *C, View &V, int g, std::vector<BlkLev> &tab) {
@@ -813,7 +813,7 @@ static int tdma_layout(mf3d_ctx *C, View &V, int g, std::vector<BlkLev> &tab) {
   // at once - 16 with too few resident measured slower (18.1 against 11.2 ms
   // per finest-level relaxation of 2x2x2 blocks of 128^3; 12 CTAs, of which
   // fewer than 8 clusters fit: 19.6 ms).  There the query picks 10: 10.5 ms.
-  L.td_cl = numax >= 64 ? std::min(8, numax / 8) : 1;
+  L.td_cl = numax >= 32 ? std::min(8, numax / 8) : 1;
   int nblk = 0;
   for (int b = 0; b < nb; ++b) nblk += g <= V.blk[b]->ngrid;
   if (numax >= 128 && cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
@@ -910,7 +910,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       int nzmax = 1, nblk = 0;
       for (int b = 0; b < nb; ++b)
         if (g <= V.blk[b]->ngrid) { nzmax = std::max(nzmax, tab[b].nz); ++nblk; }
-      L.lx_cl = nzmax >= 64 ? std::min(8, nzmax / 8) : 1;
+      L.lx_cl = nzmax >= 32 ? std::min(8, nzmax / 8) : 1;
       void (*kern)(const BlkLev *, const int *, const int *, int) =
           C->elem == 8 ? (void (*)(const BlkLev *, const int *, const int *, int))k_lexgs<double>
                        : (void (*)(const BlkLev *, const int *, const int *, int))k_lexgs<float>;
