@@ -18,6 +18,10 @@ P, W = PERIODIC, WALL
 LAYOUTS = {
     "2x1x1 blocks of 64^3, stretched y": (lambda: Problem(2, 1, 1, 64, 64, 64, ngrid=3, pl=2, stretch_y=2.0), 3),
     "1 block of 128x64x96, walls": (lambda: Problem(1, 1, 1, 128, 64, 96, bc=(W,) * 6, ngrid=3, pl=1), 2),
+    # 512-cell lines: a CTA's 64 lines of a diagonal no longer fit in shared
+    # memory at once and are staged in groups of 7
+    "1 block of 512x64x64, periodic x": (
+        lambda: Problem(1, 1, 1, 512, 64, 64, bc=(P, P, W, W, W, W), ngrid=3, pl=1), 2),
     "2x2x1 blocks of 128x128x32, periodic x y": (
         lambda: Problem(2, 2, 1, 128, 128, 32, bc=(P, P, P, P, W, W), ngrid=4, pl=2), 2),
 }
