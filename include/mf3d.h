@@ -205,6 +205,36 @@ int mf3d_newsolv_mg_device(mf3d_ctx *ctx, const mf3d_fields *fields,
                            double *rmax_hist, int hist_cap);
 
 /* ---------------------------------------------------------------------- */
+/* The momentum predictor before the projection (upstream of newsolv_mg).   */
+/* ---------------------------------------------------------------------- */
+
+/* Per block, what one Runge-Kutta stage reads besides u, v, w (ttc layout):
+ * the velocities at the start of the time step (flosol.for:98-104) and the
+ * cell viscosity `vis` (molecular plus eddy; the predictor reads its ghost
+ * layer 1 on the high faces). */
+typedef struct mf3d_rk_fields {
+  const double *uoo, *voo, *woo;
+  const double *vis;
+} mf3d_rk_fields;
+
+/* One Runge-Kutta stage of the velocity predictor with 2nd-order central
+ * differences and explicit diffusion (flosol.for:151-172 with
+ * differencing = 1 and diff_sch = 3): rungek_conv2nd (rungek.for:314-412) -
+ * boundu, the u predictor, boundv, the v predictor, boundw, the w predictor
+ * - then rungek_diff2nd (rungek.for:584-779), the reference's branch without
+ * L_LSM, immersed boundaries or wall functions.  In: u, v, w (their ghosts
+ * are refreshed by boundu/v/w, as in the reference), `rk`; out: ustar,
+ * vstar, wstar over the faces calvel later reads (isu..ieu etc.).
+ * `alfabc`: 1 on the first stage, 0 after (flosol.for:153-157); `alfapr`:
+ * the stage's alfark.  `pressureforce` adds dt*alfapr*forcn to ustar
+ * (rungek.for:642-656).  Device pointers; contexts from mf3d_create with
+ * `bounds = 1`, FP64, uniform spacing, no lsm (else MF3D_E_UNSUPPORTED).
+ * Between stages the reference runs calvel (flosol.for:171), after the
+ * last one the projection (mf3d_newsolv_mg_device). */
+int mf3d_rungek_2nd_device(mf3d_ctx *ctx, const mf3d_fields *fields, const mf3d_rk_fields *rk,
+                           double dt, double alfapr, int alfabc, int pressureforce, double forcn);
+
+/* ---------------------------------------------------------------------- */
 /* Batches of independent domains (no counterpart in the reference, which   */
 /* solves one problem per call).                                            */
 /* ---------------------------------------------------------------------- */

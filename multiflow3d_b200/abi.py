@@ -103,6 +103,12 @@ class Fields(C.Structure):
     ]
 
 
+class RkFields(C.Structure):
+    """``mf3d_rk_fields`` - the predictor's start-of-step velocities and viscosity."""
+
+    _fields_ = [("uoo", _dp), ("voo", _dp), ("woo", _dp), ("vis", _dp)]
+
+
 class TecbinInfo(C.Structure):
     """``mf3d_tecbin_info`` - the header of a restart file."""
 
@@ -163,6 +169,7 @@ EXPORTED_SYMBOLS = (
     "mf3d_tecbin_size",
     "mf3d_tecbin_decode_device",
     "mf3d_tecbin_encode_device",
+    "mf3d_rungek_2nd_device",
 )
 
 MF3D_NOALLOC_MAX_BLOCKS = 512
@@ -217,6 +224,8 @@ def _declare(lib):
     lib.mf3d_tecbin_encode_device.argtypes = [C.c_int] * 7 + [vp] * 3 + [C.POINTER(vp), vp, C.c_int]
     lib.mf3d_profile_read.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                       C.POINTER(C.c_double)]
+    lib.mf3d_rungek_2nd_device.argtypes = [vp, C.POINTER(Fields), C.POINTER(RkFields), C.c_double, C.c_double,
+                                           C.c_int, C.c_int, C.c_double]
     return lib
 
 

@@ -1506,14 +1506,24 @@ static bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc) {
   return false;
 }
 
-static void bc_walks(mf3d_ctx *C, View &V) {
+// exchange_bc of u, v, w (only >= 0: of that component alone)
+static void bc_walks(mf3d_ctx *C, View &V, int only = -1) {
   for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
     for (int mode = 0; mode < 3; ++mode)
       for (int a = 0; a < 3; ++a) {
         if (!V.bc_periodic[a]) continue;
-        launch(k_bc_walk, V.n_bcax[a], kTile, 0, C->stream, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly, mode);
+        launch(k_bc_walk, V.n_bcax[a], kTile, 0, C->stream, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly, mode, only);
         ++C->launches;
       }
+}
+// the faces without a neighbour by their code, layers 0..pl_ex (only as above)
+static void bound_faces(mf3d_ctx *C, View &V, int alfabc, int only = -1) {
+  for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
+    for (int a = 0; a < 3; ++a) {
+      launch(k_bound_faces, V.n_bcax[a], kTile, 0, C->stream, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly, C->prm.ubulk,
+             alfabc, only);
+      ++C->launches;
+    }
 }
 
 // Finish: optional su, the final calvel (u, v, w from the final p).
@@ -1536,12 +1546,7 @@ static int solve_end(mf3d_ctx *C, View &V) {
     launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
     ++C->launches;
     bc_walks(C, V);
-    for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
-      for (int a = 0; a < 3; ++a) {
-        launch(k_bound_faces, V.n_bcax[a], kTile, 0, s, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly, C->prm.ubulk,
-               C->prm.alfabc);
-        ++C->launches;
-      }
+    bound_faces(C, V, C->prm.alfabc);
     return MF3D_OK;
   }
   launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
@@ -2118,6 +2123,55 @@ int mf3d_newsolv_mg_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, do
   int st = mf3d::bind_fields(C, *C->view, fields);
   if (st) return st;
   return mf3d::run_solve(C, &dt, &alfapr, info, hist, cap);
+}
+
+int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk_fields *rk, double dt,
+                           double alfapr, int alfabc, int pressureforce, double forcn) {
+  using namespace mf3d;
+  if (!C || !fields || !rk) { set_error("mf3d_rungek_2nd_device: bad arguments"); return MF3D_E_INVALID; }
+  if (C->view->dom.size() != 1) { set_error("mf3d_rungek_2nd_device: mf3d_create contexts only"); return MF3D_E_INVALID; }
+  if (!C->prm.bounds || C->prm.lsm || C->elem != 8) {
+    set_error("mf3d_rungek_2nd_device: needs a context with bounds = 1, FP64 and no lsm");
+    return MF3D_E_UNSUPPORTED;
+  }
+  View &V = *C->view;
+  for (size_t b = 0; b < V.blk.size(); ++b) {
+    const mf3d_block_desc &d = V.blk[b]->d;
+    if (d.hx || d.hy || d.hz) { set_error("mf3d_rungek_2nd_device: uniform spacing only"); return MF3D_E_UNSUPPORTED; }
+    const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+    const int nbrs[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+    for (int f = 0; f < 6; ++f)
+      if (nbrs[f] < 0 && bounds_code_unsupported(f, bcs[f], false, alfabc)) {
+        set_error("mf3d_rungek_2nd_device: face code " + std::to_string(bcs[f]) + " with alfabc " +
+                  std::to_string(alfabc) + " reads data the library does not hold");
+        return MF3D_E_UNSUPPORTED;
+      }
+    if (!rk[b].uoo || !rk[b].voo || !rk[b].woo || !rk[b].vis) {
+      set_error("mf3d_rk_fields: a pointer is NULL");
+      return MF3D_E_INVALID;
+    }
+    for (int a = 0; a < 3; ++a) V.hf[b].oo[a] = a == 0 ? rk[b].uoo : a == 1 ? rk[b].voo : rk[b].woo;
+    V.hf[b].vis = rk[b].vis;
+  }
+  if (cudaSetDevice(C->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  AllocScope scope(C->stream);
+  int st = bind_fields(C, V, fields);
+  if (st) return st;
+  cudaStream_t s = C->stream;
+  C->launches = 0;
+  CK(cudaMemsetAsync(V.ds.p, 0, V.ds.n * sizeof(DomState), s));  // no domain marked diverged
+  // rungek_conv2nd: boundu, the u loop, boundv, the v loop, boundw, the w
+  // loop - each component's predictor sees the other components' ghosts as
+  // they were before their own bound; rungek_diff2nd fused per component
+  for (int comp = 0; comp < 3; ++comp) {
+    bc_walks(C, V, comp);
+    bound_faces(C, V, alfabc, comp);
+    launch(k_rk2nd, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, comp, dt, alfapr, pressureforce, forcn);
+    ++C->launches;
+  }
+  const cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) { set_error(std::string("mf3d_rungek_2nd_device: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
+  return MF3D_OK;
 }
 
 int mf3d_newsolv_mg(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr, mf3d_solve_info *info,

@@ -48,6 +48,8 @@ struct BlkFld {
                                      // axis (copies onto itself), 2 partner block src[f]; else 0
   double *bcst;                      // exchange_bc receive planes: 3 components x 6 faces x bcplane
   long long bcplane;                 // elements per receive plane (the largest ttc plane)
+  const double *oo[3];               // velocity predictor: u, v, w at the start of the time step
+  const double *vis;                 // velocity predictor: cell viscosity (ttc layout)
 };
 
 // x / h.  When h is a power of two the multiplication by its reciprocal
@@ -315,7 +317,7 @@ __device__ inline long long fidx_ax(const BlkFld &F, int ax, int a, int s, int t
 // against ghost planes).  Items per block: 3 * 2 * n1 * n2 (ttc extents of
 // the other two axes).  Skipped after a diverged solve.
 __global__ void k_bc_walk(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                          const DomState *__restrict__ ds, int ax, int ly, int mode) {
+                          const DomState *__restrict__ ds, int ax, int ly, int mode, int only) {
   pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
@@ -326,6 +328,7 @@ __global__ void k_bc_walk(const BlkFld *__restrict__ fl, const Tile *__restrict_
   const int plane = m1 * m2;
   if (q >= 6 * plane) return;
   const int comp = q / (2 * plane);
+  if (only >= 0 && comp != only) return;  // one component (boundu, boundv or boundw alone)
   q -= comp * 2 * plane;
   const int side = q / plane;
   q -= side * plane;
@@ -360,7 +363,8 @@ __global__ void k_bc_walk(const BlkFld *__restrict__ fl, const Tile *__restrict_
 // Launched per layer for x, y, z (the reference's W, E, S, N, B, T).
 // Skipped after a diverged solve.
 __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
-                              const DomState *__restrict__ ds, int ax, int ly, double ubulk, int alfabc) {
+                              const DomState *__restrict__ ds, int ax, int ly, double ubulk, int alfabc,
+                              int only) {
   pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
@@ -371,6 +375,7 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   const int plane = m1 * m2;
   if (q >= 6 * plane) return;
   const int comp = q / (2 * plane);
+  if (only >= 0 && comp != only) return;  // one component (boundu, boundv or boundw alone)
   q -= comp * 2 * plane;
   const int side = q / plane;
   q -= side * plane;
@@ -828,6 +833,69 @@ __global__ void __launch_bounds__(RW_TX *RW_RJ) k_calvel(const BlkFld *__restric
     if (!(i == nx && F.wall[1])) F.u[c] = (F.ustar[c] - xdiv(dta * (p[c + 1] - p[c]), F.df[0][i], F.pinv[0]));
     if (!(j == ny && F.wall[3])) F.v[c] = (F.vstar[c] - xdiv(dta * (p[c + sy] - p[c]), F.df[1][j], F.pinv[1]));
     if (!(k == F.nz && F.wall[5])) F.w[c] = (F.wstar[c] - xdiv(dta * (p[c + sz] - p[c]), F.df[2][k], F.pinv[2]));
+  }
+}
+
+// One Runge-Kutta stage of the velocity predictor for component `comp`
+// (rungek_conv2nd, rungek.for:314-412, then rungek_diff2nd, :584-779, the
+// branch without L_LSM, immersed boundaries or wall functions), over the
+// component's faces 1..comp_end:
+//   star = (oo - dt*alfapr*(c1 + c2 + c3)), the 2nd-order conservative
+//     convection terms as the reference writes them (x**2 is x*x);
+//   star = (star + dt*alfapr*diff), diff = -(ap*c + an*c(j+1) + as*c(j-1)
+//     + ae*c(i+1) + aw*c(i-1) + at*c(k+1) + ab*c(k-1)) with a* = -visc/d*d*
+//     from the viscosity of the cell past the face, ap = -1.0*(aw+ae+as+an+
+//     ab+at);
+//   u under pressureforce: star = star + dt*alfapr*forcn.
+// Fusing the two loops per cell keeps the reference's values: rungek_diff2nd
+// reads only the component itself, which boundv/boundw do not touch.
+__global__ void __launch_bounds__(RW_TX *RW_RJ) k_rk2nd(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                                                        int comp, double dt, double alfapr, int pforce, double forcn) {
+  pdl_wait();
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i > comp_end(F, comp, 0) || j > comp_end(F, comp, 1)) return;
+  const int k1 = min(t.k0 + RW_KCH - 1, comp_end(F, comp, 2));
+  const long long sy = F.ti, sz = (long long)F.ti * F.tj;
+  const double dx = F.h[0][1], dy = F.h[1][1], dz = F.h[2][1];
+  const double dxx = dx * dx, dyy = dy * dy, dzz = dz * dz;
+  const double *__restrict__ U = F.u;
+  const double *__restrict__ V = F.v;
+  const double *__restrict__ W = F.w;
+  const double *__restrict__ C = comp_field(F, comp);
+  const double *__restrict__ OO = F.oo[comp];
+  double *__restrict__ ST = comp == 0 ? F.ustar : comp == 1 ? F.vstar : F.wstar;
+  const long long so = comp == 0 ? 1 : comp == 1 ? sy : sz;  // the cell past the face
+  for (int k = t.k0; k <= k1; ++k) {
+    const long long c = fidx(F, i, j, k);
+    double c1, c2, c3;
+    if (comp == 0) {
+      const double up12 = 0.5 * (U[c] + U[c + 1]), um12 = 0.5 * (U[c] + U[c - 1]);
+      c1 = (up12 * up12 - um12 * um12) / dx;
+      c2 = 0.25 * ((V[c] + V[c + 1]) * (U[c] + U[c + sy]) - (V[c - sy] + V[c + 1 - sy]) * (U[c] + U[c - sy])) / dy;
+      c3 = 0.25 * ((W[c] + W[c + 1]) * (U[c] + U[c + sz]) - (W[c - sz] + W[c + 1 - sz]) * (U[c] + U[c - sz])) / dz;
+    } else if (comp == 1) {
+      const double vp12 = 0.5 * (V[c] + V[c + sy]), vm12 = 0.5 * (V[c] + V[c - sy]);
+      c2 = (vp12 * vp12 - vm12 * vm12) / dy;
+      c1 = 0.25 * ((U[c] + U[c + sy]) * (V[c] + V[c + 1]) - (U[c - 1] + U[c - 1 + sy]) * (V[c] + V[c - 1])) / dx;
+      c3 = 0.25 * ((W[c] + W[c + sy]) * (V[c] + V[c + sz]) - (W[c - sz] + W[c + sy - sz]) * (V[c] + V[c - sz])) / dz;
+    } else {
+      const double wp12 = 0.5 * (W[c] + W[c + sz]), wm12 = 0.5 * (W[c] + W[c - sz]);
+      c3 = (wp12 * wp12 - wm12 * wm12) / dz;
+      c1 = 0.25 * ((U[c] + U[c + sz]) * (W[c] + W[c + 1]) - (U[c - 1] + U[c - 1 + sz]) * (W[c] + W[c - 1])) / dx;
+      c2 = 0.25 * ((V[c] + V[c + sz]) * (W[c] + W[c + sy]) - (V[c - sy] + V[c - sy + sz]) * (W[c] + W[c - sy])) / dy;
+    }
+    double st = (OO[c] - dt * alfapr * (c1 + c2 + c3));
+    const double visc = F.vis[c + so];
+    const double aw = -visc / dxx, ae = -visc / dxx, an = -visc / dyy, as = -visc / dyy;
+    const double at = -visc / dzz, ab = -visc / dzz;
+    const double ap = -1.0 * (aw + ae + as + an + ab + at);
+    const double diff = -(ap * C[c] + an * C[c + sy] + as * C[c - sy] + ae * C[c + 1] + aw * C[c - 1] +
+                          at * C[c + sz] + ab * C[c - sz]);
+    st = (st + dt * alfapr * diff);
+    if (comp == 0 && pforce) st = st + dt * alfapr * forcn;
+    ST[c] = st;
   }
 }
 

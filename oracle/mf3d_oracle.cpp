@@ -109,6 +109,9 @@ struct Ctx {
 inline double &F(Blk &B, double *a, int i, int j, int k) {
   return a[(size_t)(i - 1) + (size_t)B.ttc_i * ((size_t)(j - 1) + (size_t)B.ttc_j * (size_t)(k - 1))];
 }
+inline double F(Blk &B, const double *a, int i, int j, int k) {
+  return a[(size_t)(i - 1) + (size_t)B.ttc_i * ((size_t)(j - 1) + (size_t)B.ttc_j * (size_t)(k - 1))];
+}
 
 int level_n(int n, int gl) { return n / (1 << (gl - 1)) + 2; }
 
@@ -927,6 +930,86 @@ void bound(Ctx &C, int op) {
       for (int f = 0; f < 6; ++f) bound_face(C, B, op, ly, f);
 }
 
+/* One Runge-Kutta stage of the velocity predictor, the reference's branch
+ * without L_LSM, immersed boundaries or wall functions:
+ * rungek_conv2nd (rungek.for:314-412) - boundu, the u loop, boundv, the v
+ * loop, boundw, the w loop, each loop
+ *   star = (oo - dt*alfapr*(conv)), conv the 2nd-order conservative terms
+ *   in the order the reference sums them -
+ * then rungek_diff2nd (rungek.for:584-779): per component over the same
+ * ranges, with visc the viscosity of the cell past the face,
+ *   aw = ae = -visc/dxx, an = as = -visc/dyy, at = ab = -visc/dzz,
+ *   ap = -1.0*(aw+ae+as+an+ab+at),
+ *   diff = -(ap*c + an*c(j+1) + as*c(j-1) + ae*c(i+1) + aw*c(i-1)
+ *            + at*c(k+1) + ab*c(k-1)),
+ *   star = (star + dt*alfapr*diff),
+ * and for u under pressureforce star = star + dt*alfapr*forcn (:650-652).
+ * The u loop reads v and w before boundv/boundw refresh their ghosts. */
+void rungek_2nd(Ctx &C, const double *const *uoo, const double *const *voo, const double *const *woo,
+                const double *const *vis, bool pforce, double forcn) {
+  const double dt = C.dt, alfapr = C.alfapr;
+  for (int op = 1; op <= 3; ++op) {
+    bound(C, op);
+    par_blocks((int)C.b.size(), [&](int ib) { Blk &B = C.b[ib];
+      const double dx = B.d.dx, dy = B.d.dy, dz = B.d.dz;
+      double *st = op == 1 ? B.ustar : op == 2 ? B.vstar : B.wstar;
+      const double *oo = op == 1 ? uoo[ib] : op == 2 ? voo[ib] : woo[ib];
+      int is, ie, js, je, ks, ke;
+      franges(B, op, is, ie, js, je, ks, ke);
+      auto u = [&](int i, int j, int k) { return F(B, B.u, i, j, k); };
+      auto v = [&](int i, int j, int k) { return F(B, B.v, i, j, k); };
+      auto w = [&](int i, int j, int k) { return F(B, B.w, i, j, k); };
+      for (int k = ks; k <= ke; ++k) for (int i = is; i <= ie; ++i) for (int j = js; j <= je; ++j) {
+        double c1, c2, c3;
+        if (op == 1) {
+          const double up12 = 0.5 * (u(i, j, k) + u(i + 1, j, k)), um12 = 0.5 * (u(i, j, k) + u(i - 1, j, k));
+          c1 = (up12 * up12 - um12 * um12) / dx;
+          c2 = 0.25 * ((v(i, j, k) + v(i + 1, j, k)) * (u(i, j, k) + u(i, j + 1, k)) -
+                       (v(i, j - 1, k) + v(i + 1, j - 1, k)) * (u(i, j, k) + u(i, j - 1, k))) / dy;
+          c3 = 0.25 * ((w(i, j, k) + w(i + 1, j, k)) * (u(i, j, k) + u(i, j, k + 1)) -
+                       (w(i, j, k - 1) + w(i + 1, j, k - 1)) * (u(i, j, k) + u(i, j, k - 1))) / dz;
+        } else if (op == 2) {
+          const double vp12 = 0.5 * (v(i, j, k) + v(i, j + 1, k)), vm12 = 0.5 * (v(i, j, k) + v(i, j - 1, k));
+          c2 = (vp12 * vp12 - vm12 * vm12) / dy;
+          c1 = 0.25 * ((u(i, j, k) + u(i, j + 1, k)) * (v(i, j, k) + v(i + 1, j, k)) -
+                       (u(i - 1, j, k) + u(i - 1, j + 1, k)) * (v(i, j, k) + v(i - 1, j, k))) / dx;
+          c3 = 0.25 * ((w(i, j, k) + w(i, j + 1, k)) * (v(i, j, k) + v(i, j, k + 1)) -
+                       (w(i, j, k - 1) + w(i, j + 1, k - 1)) * (v(i, j, k) + v(i, j, k - 1))) / dz;
+        } else {
+          const double wp12 = 0.5 * (w(i, j, k) + w(i, j, k + 1)), wm12 = 0.5 * (w(i, j, k) + w(i, j, k - 1));
+          c3 = (wp12 * wp12 - wm12 * wm12) / dz;
+          c1 = 0.25 * ((u(i, j, k) + u(i, j, k + 1)) * (w(i, j, k) + w(i + 1, j, k)) -
+                       (u(i - 1, j, k) + u(i - 1, j, k + 1)) * (w(i, j, k) + w(i - 1, j, k))) / dx;
+          c2 = 0.25 * ((v(i, j, k) + v(i, j, k + 1)) * (w(i, j, k) + w(i, j + 1, k)) -
+                       (v(i, j - 1, k) + v(i, j - 1, k + 1)) * (w(i, j, k) + w(i, j - 1, k))) / dy;
+        }
+        F(B, st, i, j, k) = (F(B, oo, i, j, k) - dt * alfapr * (c1 + c2 + c3));
+      }
+    });
+  }
+  par_blocks((int)C.b.size(), [&](int ib) { Blk &B = C.b[ib];
+    const double dxx = B.d.dx * B.d.dx, dyy = B.d.dy * B.d.dy, dzz = B.d.dz * B.d.dz;
+    for (int op = 1; op <= 3; ++op) {
+      double *st = op == 1 ? B.ustar : op == 2 ? B.vstar : B.wstar;
+      double *c = field_of(B, op);
+      int is, ie, js, je, ks, ke;
+      franges(B, op, is, ie, js, je, ks, ke);
+      for (int k = ks; k <= ke; ++k) for (int i = is; i <= ie; ++i) for (int j = js; j <= je; ++j) {
+        const double visc = op == 1 ? F(B, vis[ib], i + 1, j, k) : op == 2 ? F(B, vis[ib], i, j + 1, k)
+                                                                           : F(B, vis[ib], i, j, k + 1);
+        const double aw = -visc / dxx, ae = -visc / dxx, an = -visc / dyy, as = -visc / dyy;
+        const double at = -visc / dzz, ab = -visc / dzz;
+        const double ap = -1.0 * (aw + ae + as + an + ab + at);
+        const double diff = -(ap * F(B, c, i, j, k) + an * F(B, c, i, j + 1, k) + as * F(B, c, i, j - 1, k) +
+                              ae * F(B, c, i + 1, j, k) + aw * F(B, c, i - 1, j, k) + at * F(B, c, i, j, k + 1) +
+                              ab * F(B, c, i, j, k - 1));
+        F(B, st, i, j, k) = (F(B, st, i, j, k) + dt * alfapr * diff);
+        if (op == 1 && pforce) F(B, st, i, j, k) = F(B, st, i, j, k) + dt * alfapr * forcn;
+      }
+    }
+  });
+}
+
 /* EXT: distance between the centres of cells a and a+1 along an axis,
  * equal to dx on a uniform grid. */
 inline double dface(const std::vector<double> &w, int a0) { return 0.5 * (w[a0] + w[a0 + 1]); }
@@ -1270,6 +1353,31 @@ int orc_newsolv_mg(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
   for (int ib = 0; ib < nb; ++ib)
     if (fields[ib].su) std::memcpy(fields[ib].su, C.b[ib].su.data(), C.b[ib].su.size() * sizeof(double));
   return st;
+}
+
+/* One Runge-Kutta stage of the predictor (rungek_conv2nd + rungek_diff2nd)
+ * on host arrays: u, v, w in (ghosts refreshed by boundu/v/w), ustar, vstar,
+ * wstar out.  alfabc as the reference sets it per stage. */
+int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, const mf3d_fields *fields,
+                   const mf3d_rk_fields *rk, double dt, double alfapr, int alfabc, int pressureforce, double forcn) {
+  Ctx C;
+  mf3d_params p = *prm;
+  p.bounds = 1;
+  p.alfabc = alfabc;
+  int st = setup(C, blocks, nb, &p);
+  if (st) return st;
+  if (C.lsm) { g_err = "rungek_2nd: no L_LSM branch"; return MF3D_E_UNSUPPORTED; }
+  C.dt = dt; C.alfapr = alfapr;
+  std::vector<const double *> uoo(nb), voo(nb), woo(nb), vis(nb);
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    if (B.stretched) { g_err = "rungek_2nd: uniform spacing only"; return MF3D_E_UNSUPPORTED; }
+    B.ustar = fields[ib].ustar; B.vstar = fields[ib].vstar; B.wstar = fields[ib].wstar;
+    B.u = fields[ib].u; B.v = fields[ib].v; B.w = fields[ib].w; B.p = fields[ib].p;
+    uoo[ib] = rk[ib].uoo; voo[ib] = rk[ib].voo; woo[ib] = rk[ib].woo; vis[ib] = rk[ib].vis;
+  }
+  rungek_2nd(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
+  return MF3D_OK;
 }
 
 /* One V-cycle: su[b] (ttc) in, pp[b] (ttc) out, starting from pp = 0. */

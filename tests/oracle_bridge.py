@@ -9,7 +9,7 @@ import ctypes as C
 import os
 import subprocess
 
-from multiflow3d_b200.abi import BlockDesc, Params, Fields, SolveInfo
+from multiflow3d_b200.abi import BlockDesc, Params, Fields, SolveInfo, RkFields
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
@@ -40,6 +40,8 @@ def load():
                                            C.POINTER(_dp), C.POINTER(_dp)]
         lib.orc_build_topology.argtypes = [C.c_int, _dp, C.POINTER(C.c_int), C.c_double,
                                            C.c_double, C.c_double, C.POINTER(BlockDesc)]
+        lib.orc_rungek_2nd.argtypes = [C.POINTER(BlockDesc), C.c_int, C.POINTER(Params), C.POINTER(Fields),
+                                       C.POINTER(RkFields), C.c_double, C.c_double, C.c_int, C.c_int, C.c_double]
         lib.orc_last_error.restype = C.c_char_p
         _lib = lib
     return _lib

@@ -1,0 +1,78 @@
+"""The velocity predictor (one Runge-Kutta stage of rungek_conv2nd and
+rungek_diff2nd) on the GPU against the oracle, FP64, bit for bit: ustar,
+vstar, wstar over their faces and the u, v, w ghosts that boundu/v/w
+refresh on the way, for periodic, wall, symmetry, inflow and outflow
+faces, both stages' alfabc, and the pressure forcing."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from multiflow3d_b200 import abi
+from multiflow3d_b200.abi import RkFields
+from multiflow3d_b200.problems import Problem, PERIODIC, WALL
+from multiflow3d_b200.solver import Projection
+from test_gpu_edges import face_mask
+from test_rungek import rk_inputs, orc_rk
+
+pytestmark = pytest.mark.gpu
+P, W, S = PERIODIC, WALL, 3
+
+CASES = {
+    "2x2x1 periodic x y, walls z, first stage, forcing": (
+        lambda: Problem(2, 2, 1, 16, 16, 8, bc=(P, P, P, P, W, W), ngrid=2, pl=2), 1, 1, 1),
+    "2x1x2 inflow / outflow x, walls y, periodic z, first stage": (
+        lambda: Problem(2, 1, 2, 16, 8, 16, bc=(1, 2, W, W, P, P), ngrid=2, pl=3), 2, 1, 0),
+    "1 block, walls and symmetry, later stage": (
+        lambda: Problem(1, 1, 1, 16, 12, 8, bc=(W, W, S, S, W, W), ngrid=2, pl=2), 1, 0, 0),
+}
+
+
+def dev(t, cuda):
+    import torch
+    return torch.from_numpy(t.copy()).to(cuda)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_predictor_matches_oracle(lib, oracle, cuda, case):
+    import torch
+    make, pl_ex, alfabc, pforce = CASES[case]
+    pr = make()
+    blocks, rk = rk_inputs(pr, 21)
+    dt, alfapr, forcn, ubulk = 0.0137, 0.5, 0.31, 0.6
+    gpu = [{k: dev(v, cuda) for k, v in f.items()} for f in blocks]
+    grk = [{k: dev(v, cuda) for k, v in r.items()} for r in rk]
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfapr, alfabc=alfabc, pforce=pforce, forcn=forcn,
+                  pl_ex=pl_ex, ubulk=ubulk) == 0
+    prm = pr.params(pl_ex=pl_ex, bounds=1, alfabc=alfabc, ubulk=ubulk)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    fa = (abi.Fields * pr.nblocks)()
+    ra = (RkFields * pr.nblocks)()
+    dp = C.POINTER(C.c_double)
+    for b in range(pr.nblocks):
+        for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p"):
+            setattr(fa[b], k, C.cast(C.c_void_p(gpu[b][k].data_ptr()), dp))
+        for k in ("uoo", "voo", "woo", "vis"):
+            setattr(ra[b], k, C.cast(C.c_void_p(grk[b][k].data_ptr()), dp))
+    st = lib.mf3d_rungek_2nd_device(proj.ctx, fa, ra, dt, alfapr, alfabc, pforce, forcn)
+    proj.close()
+    assert st == 0, abi.last_error(lib)
+    torch.cuda.synchronize()
+    pl = pr.pl
+    inner = (slice(pl, pl + pr.nz), slice(pl, pl + pr.ny), slice(pl, pl + pr.nx))
+    for b in range(pr.nblocks):
+        got = {k: v.cpu().numpy() for k, v in gpu[b].items()}
+        for k in ("ustar", "vstar", "wstar"):
+            assert np.array_equal(got[k][inner], blocks[b][k][inner]), (b, k)
+        for k in ("u", "v", "w"):
+            m = face_mask(got[k].shape, pl, pl_ex)
+            assert np.array_equal(got[k][m], blocks[b][k][m]), (b, k)
+
+
+def test_predictor_refusals(lib, cuda):
+    """Without bounds = 1, or on a stretched grid, the call is refused before any device work."""
+    pr = Problem(1, 1, 1, 8, 8, 8, ngrid=1, pl=1)
+    proj = Projection(pr.descriptors(lib), pr.params(), lib)
+    st = lib.mf3d_rungek_2nd_device(proj.ctx, (abi.Fields * 1)(), (RkFields * 1)(), 0.1, 1.0, 1, 0, 0.0)
+    proj.close()
+    assert st == abi.MF3D_E_UNSUPPORTED

@@ -1,0 +1,123 @@
+"""The velocity predictor upstream of the projection: one Runge-Kutta stage
+of rungek_conv2nd (rungek.for:314-412) and rungek_diff2nd (:584-779).  The
+oracle's restatement is pinned here against an independent numpy
+evaluation of the same expressions (the same IEEE operations in the same
+order, hence bit for bit) and against the identity at dt = 0; the GPU
+parity tests are in test_gpu_rungek.py."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from multiflow3d_b200.abi import RkFields
+from multiflow3d_b200.problems import Problem, fields_struct, PERIODIC, WALL
+import oracle_bridge as ob
+
+P, W = PERIODIC, WALL
+
+
+def rk_inputs(pr, seed):
+    """u, v, w, ustar.. and p as the projection's tests build them, plus
+    start-of-step velocities and a positive viscosity field (ttc layout)."""
+    rng = np.random.default_rng(seed)
+    blocks = pr.block_fields(seed=seed, fourier_modes=2)
+    rk = []
+    for f in blocks:
+        shp = f["u"].shape
+        rk.append({"uoo": f["u"] + 0.1 * rng.standard_normal(shp), "voo": f["v"] + 0.1 * rng.standard_normal(shp),
+                   "woo": f["w"] + 0.1 * rng.standard_normal(shp), "vis": 1e-3 * (1.0 + rng.random(shp))})
+    return blocks, rk
+
+
+def rk_struct(rk):
+    arr = (RkFields * len(rk))()
+    for b, f in enumerate(rk):
+        for k in ("uoo", "voo", "woo", "vis"):
+            setattr(arr[b], k, f[k].ctypes.data_as(C.POINTER(C.c_double)))
+    return arr
+
+
+def orc_rk(oracle, pr, blocks, rk, dt, alfapr, alfabc=1, pforce=0, forcn=0.0, **kw):
+    prm = pr.params(pl_ex=kw.get("pl_ex", 0), alfabc=alfabc, ubulk=kw.get("ubulk", 0.0))
+    return oracle.orc_rungek_2nd(pr.descriptors(oracle), pr.nblocks, C.byref(prm), fields_struct(blocks),
+                                 rk_struct(rk), dt, alfapr, alfabc, pforce, forcn)
+
+
+def numpy_stage(u, v, w, uoo, voo, woo, vis, dx, dy, dz, dt, alfapr, pforce, forcn, sl):
+    """The reference's expressions, vectorised; arrays [k, j, i]; `sl` the
+    interior slices of the component's range."""
+    def at(a, di=0, dj=0, dk=0):
+        return a[sl[0].start + dk:sl[0].stop + dk, sl[1].start + dj:sl[1].stop + dj, sl[2].start + di:sl[2].stop + di]
+    out = []
+    for op in range(3):
+        c = (u, v, w)[op]
+        if op == 0:
+            up12 = 0.5 * (at(u) + at(u, 1)); um12 = 0.5 * (at(u) + at(u, -1))
+            c1 = (up12 * up12 - um12 * um12) / dx
+            c2 = 0.25 * ((at(v) + at(v, 1)) * (at(u) + at(u, 0, 1)) - (at(v, 0, -1) + at(v, 1, -1)) * (at(u) + at(u, 0, -1))) / dy
+            c3 = 0.25 * ((at(w) + at(w, 1)) * (at(u) + at(u, 0, 0, 1)) - (at(w, 0, 0, -1) + at(w, 1, 0, -1)) * (at(u) + at(u, 0, 0, -1))) / dz
+            oo, visc = at(uoo), at(vis, 1)
+        elif op == 1:
+            vp12 = 0.5 * (at(v) + at(v, 0, 1)); vm12 = 0.5 * (at(v) + at(v, 0, -1))
+            c2 = (vp12 * vp12 - vm12 * vm12) / dy
+            c1 = 0.25 * ((at(u) + at(u, 0, 1)) * (at(v) + at(v, 1)) - (at(u, -1) + at(u, -1, 1)) * (at(v) + at(v, -1))) / dx
+            c3 = 0.25 * ((at(w) + at(w, 0, 1)) * (at(v) + at(v, 0, 0, 1)) - (at(w, 0, 0, -1) + at(w, 0, 1, -1)) * (at(v) + at(v, 0, 0, -1))) / dz
+            oo, visc = at(voo), at(vis, 0, 1)
+        else:
+            wp12 = 0.5 * (at(w) + at(w, 0, 0, 1)); wm12 = 0.5 * (at(w) + at(w, 0, 0, -1))
+            c3 = (wp12 * wp12 - wm12 * wm12) / dz
+            c1 = 0.25 * ((at(u) + at(u, 0, 0, 1)) * (at(w) + at(w, 1)) - (at(u, -1) + at(u, -1, 0, 1)) * (at(w) + at(w, -1))) / dx
+            c2 = 0.25 * ((at(v) + at(v, 0, 0, 1)) * (at(w) + at(w, 0, 1)) - (at(v, 0, -1) + at(v, 0, -1, 1)) * (at(w) + at(w, 0, -1))) / dy
+            oo, visc = at(woo), at(vis, 0, 0, 1)
+        st = oo - dt * alfapr * (c1 + c2 + c3)
+        dxx, dyy, dzz = dx * dx, dy * dy, dz * dz
+        aw = -visc / dxx; ae = -visc / dxx; an = -visc / dyy; as_ = -visc / dyy; at_ = -visc / dzz; ab = -visc / dzz
+        ap = -1.0 * (aw + ae + as_ + an + ab + at_)
+        diff = -(ap * at(c) + an * at(c, 0, 1) + as_ * at(c, 0, -1) + ae * at(c, 1) + aw * at(c, -1) +
+                 at_ * at(c, 0, 0, 1) + ab * at(c, 0, 0, -1))
+        st = st + dt * alfapr * diff
+        if op == 0 and pforce:
+            st = st + dt * alfapr * forcn
+        out.append(st)
+    return out
+
+
+def test_oracle_predictor_matches_numpy(oracle):
+    """One periodic block: boundu/v/w wrap the ghosts; the u predictor reads
+    v and w as given, the v predictor w as given (their bounds come after)."""
+    pr = Problem(1, 1, 1, 12, 10, 8, bc=(P,) * 6, ngrid=1, pl=2, dx=0.1, dy=0.125, dz=0.3)
+    blocks, rk = rk_inputs(pr, 3)
+    given = {k: blocks[0][k].copy() for k in ("u", "v", "w")}
+    dt, alfapr, forcn = 0.013, 0.7, 0.25
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfapr, pforce=1, forcn=forcn) == 0
+    f = blocks[0]
+    pl, n = pr.pl, (pr.nz, pr.ny, pr.nx)
+    sl = tuple(slice(pl, pl + m) for m in n)
+    args = (rk[0]["uoo"], rk[0]["voo"], rk[0]["woo"], rk[0]["vis"], pr.dx, pr.dy, pr.dz, dt, alfapr, 1, forcn, sl)
+    us = numpy_stage(f["u"], given["v"], given["w"], *args)[0]
+    vs = numpy_stage(f["u"], f["v"], given["w"], *args)[1]
+    ws = numpy_stage(f["u"], f["v"], f["w"], *args)[2]
+    assert np.array_equal(f["ustar"][sl], us)
+    assert np.array_equal(f["vstar"][sl], vs)
+    assert np.array_equal(f["wstar"][sl], ws)
+    # the periodic wrap the bounds applied
+    assert np.array_equal(f["u"][:, :, pl - 1], f["u"][:, :, pl + pr.nx - 1])
+
+
+def test_oracle_predictor_zero_step_is_identity(oracle):
+    pr = Problem(2, 1, 1, 8, 8, 8, bc=(1, 2, W, W, P, P), ngrid=2, pl=2)
+    blocks, rk = rk_inputs(pr, 4)
+    assert orc_rk(oracle, pr, blocks, rk, 0.0, 1.0, alfabc=1, ubulk=0.5) == 0
+    pl = pr.pl
+    for f, r in zip(blocks, rk):
+        I = (slice(pl, pl + pr.nz), slice(pl, pl + pr.ny), slice(pl, pl + pr.nx - 1))
+        assert np.array_equal(f["ustar"][I], r["uoo"][I])
+
+
+def test_oracle_predictor_refuses_other_branches(oracle):
+    pr = Problem(1, 1, 1, 8, 8, 8, ngrid=1, pl=1, stretch_y=2.0)
+    blocks, rk = rk_inputs(pr, 5)
+    assert orc_rk(oracle, pr, blocks, rk, 0.1, 1.0) == -6
+    pr = Problem(1, 1, 1, 8, 8, 8, bc=(1, 21, W, W, W, W), ngrid=1, pl=1)
+    blocks, rk = rk_inputs(pr, 5)
+    assert orc_rk(oracle, pr, blocks, rk, 0.1, 1.0, alfabc=1) == -6
