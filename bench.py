@@ -564,6 +564,89 @@ def run_linegs(args):
     return 0
 
 
+def run_rungek(args):
+    """The velocity predictor upstream of the projection: one Runge-Kutta
+    stage of rungek_conv2nd + rungek_diff2nd (boundu/v/w included) on
+    2x2x2 blocks of 128^3 (256^3), uniform spacing, periodic x and z, walls
+    in y, FP64.  value: stages/s with every field resident on the device;
+    GB/s counts u, v, w, uoo, voo, woo, vis read and ustar, vstar, wstar
+    written once per interior cell (80 B).  CPU baseline: the oracle's
+    stage on the same inputs, 8 threads (one per block)."""
+    import ctypes as C
+    import time
+    import numpy as np
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.abi import RkFields
+    from multiflow3d_b200.problems import Problem, fields_struct
+    from multiflow3d_b200.solver import Projection
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    h = 1.0 / 256
+    pr = Problem(2, 2, 2, 128, 128, 128, ngrid=6, pl=2, dx=h, dy=h, dz=h)
+    host = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    rng = np.random.default_rng(SEED)
+    rk = [{"uoo": f["u"] + 0.01, "voo": f["v"] - 0.01, "woo": f["w"] + 0.02,
+           "vis": 1e-3 * (1.0 + rng.random(f["u"].shape))} for f in host]
+    keys = ("ustar", "vstar", "wstar", "u", "v", "w", "p")
+    d = [{k: torch.from_numpy(f[k]).to(dev) for k in keys} for f in host]
+    drk = [{k: torch.from_numpy(r[k]).to(dev) for k in r} for r in rk]
+    prm = pr.params(bounds=1, alfabc=1)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    fa = (abi.Fields * pr.nblocks)()
+    ra = (RkFields * pr.nblocks)()
+    dp = C.POINTER(C.c_double)
+    for b in range(pr.nblocks):
+        for k in keys:
+            setattr(fa[b], k, C.cast(C.c_void_p(d[b][k].data_ptr()), dp))
+        for k in ("uoo", "voo", "woo", "vis"):
+            setattr(ra[b], k, C.cast(C.c_void_p(drk[b][k].data_ptr()), dp))
+    dt, alfapr = 1e-3, 0.5
+
+    def stage():
+        abi.check(lib, lib.mf3d_rungek_2nd_device(proj.ctx, fa, ra, dt, alfapr, 1, 0, 0.0), "mf3d_rungek_2nd_device")
+
+    for _ in range(args.warmup):
+        stage()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        stage()
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    launches = lib.mf3d_last_launch_count(proj.ctx)
+    proj.close()
+    cells = pr.NX * pr.NY * pr.NZ
+    line = {
+        "metric": "rk_stages_per_s", "value": args.steps / sec, "unit": "stages/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "velocity predictor, one RK stage (rungek_conv2nd + rungek_diff2nd + boundu/v/w), "
+                               "2x2x2 blocks of 128^3 (256^3), periodic x z, walls y"},
+        "GB_per_s_algorithmic": 80.0 * cells / (sec / args.steps) / 1e9, "gpu_launches_per_step": launches,
+    }
+    if not args.no_cpu_baseline:
+        orc = oracle_lib()
+        threads = max(1, min(os.cpu_count() or 1, pr.nblocks))
+        orc.orc_set_threads(threads)
+        ra_h = (RkFields * pr.nblocks)()
+        for b, r in enumerate(rk):
+            for k in ("uoo", "voo", "woo", "vis"):
+                setattr(ra_h[b], k, r[k].ctypes.data_as(dp))
+        blocks = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+        t = time.perf_counter()
+        orc.orc_rungek_2nd(pr.descriptors(orc), pr.nblocks, C.byref(prm), fields_struct(blocks), ra_h, dt, alfapr,
+                           1, 0, 0.0)
+        cpu = 1.0 / (time.perf_counter() - t)
+        line["cpu_baseline"] = {"value": cpu, "unit": "stages/s", "cores": threads, "kind": "port",
+                                "sample": "one stage on the same inputs on the oracle"}
+        line["speedup_vs_cpu"] = line["value"] / cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_sip(args):
     """solver 1 (pressure_1sweep with Stone's SIP): 2x2x2 blocks of 32^3
     (64^3), periodic x and z, walls in y, 4 SIP sweeps per call, rel tol
@@ -897,7 +980,8 @@ def main():
     ap.add_argument("--impl", default="mf3d", choices=["mf3d", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="multiblock",
-                    choices=["multiblock", "mixed", "batched", "served", "density", "tecbin", "sip", "linegs"],
+                    choices=["multiblock", "mixed", "batched", "served", "density", "tecbin", "sip", "linegs",
+                             "rungek"],
                     help="multiblock: the default FP64 line; mixed / batched / served / density: the further "
                          "workloads (1 GPU)")
     ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
@@ -920,6 +1004,8 @@ def main():
         return run_sip(args)
     if args.workload == "linegs":
         return run_linegs(args)
+    if args.workload == "rungek":
+        return run_rungek(args)
     return run_gpu(args)
 
 
