@@ -229,10 +229,19 @@ typedef struct mf3d_rk_fields {
  * the stage's alfark.  `pressureforce` adds dt*alfapr*forcn to ustar
  * (rungek.for:642-656).  Device pointers; contexts from mf3d_create with
  * `bounds = 1`, FP64, uniform spacing, no lsm (else MF3D_E_UNSUPPORTED).
- * Between stages the reference runs calvel (flosol.for:171), after the
- * last one the projection (mf3d_newsolv_mg_device). */
+ * Between stages the reference runs calvel (flosol.for:171;
+ * mf3d_calvel_device), after the last one the projection
+ * (mf3d_newsolv_mg_device). */
 int mf3d_rungek_2nd_device(mf3d_ctx *ctx, const mf3d_fields *fields, const mf3d_rk_fields *rk,
                            double dt, double alfapr, int alfabc, int pressureforce, double forcn);
+
+/* calvel alone (press.for:139-198, flosol.for:171 between Runge-Kutta
+ * stages): u, v, w from ustar, vstar, wstar and p over the faces calvel
+ * writes, then the face part of its exchange(1..3) - with bounds = 1 also
+ * the full periodic planes - as mf3d_newsolv_mg_device leaves them after
+ * its final calvel, without boundu/v/w.  Device pointers; mf3d_create
+ * contexts, FP64, no lsm. */
+int mf3d_calvel_device(mf3d_ctx *ctx, const mf3d_fields *fields, double dt, double alfapr);
 
 /* ---------------------------------------------------------------------- */
 /* Batches of independent domains (no counterpart in the reference, which   */

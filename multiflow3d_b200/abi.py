@@ -170,6 +170,7 @@ EXPORTED_SYMBOLS = (
     "mf3d_tecbin_decode_device",
     "mf3d_tecbin_encode_device",
     "mf3d_rungek_2nd_device",
+    "mf3d_calvel_device",
 )
 
 MF3D_NOALLOC_MAX_BLOCKS = 512
@@ -226,6 +227,7 @@ def _declare(lib):
                                       C.POINTER(C.c_double)]
     lib.mf3d_rungek_2nd_device.argtypes = [vp, C.POINTER(Fields), C.POINTER(RkFields), C.c_double, C.c_double,
                                            C.c_int, C.c_int, C.c_double]
+    lib.mf3d_calvel_device.argtypes = [vp, C.POINTER(Fields), C.c_double, C.c_double]
     return lib
 
 

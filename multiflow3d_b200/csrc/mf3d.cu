@@ -2174,6 +2174,33 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
   return MF3D_OK;
 }
 
+int mf3d_calvel_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr) {
+  using namespace mf3d;
+  if (!C || !fields) { set_error("mf3d_calvel_device: bad arguments"); return MF3D_E_INVALID; }
+  if (C->view->dom.size() != 1) { set_error("mf3d_calvel_device: mf3d_create contexts only"); return MF3D_E_INVALID; }
+  if (C->prm.lsm || C->elem != 8) { set_error("mf3d_calvel_device: FP64 contexts without lsm"); return MF3D_E_UNSUPPORTED; }
+  if (cudaSetDevice(C->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  View &V = *C->view;
+  AllocScope scope(C->stream);
+  int st = bind_fields(C, V, fields);
+  if (st) return st;
+  cudaStream_t s = C->stream;
+  C->launches = 0;
+  DomState d0;
+  std::memset(&d0, 0, sizeof d0);
+  d0.dt = dt;
+  d0.alfapr = alfapr;
+  CK(cudaMemcpyAsync(V.ds.p, &d0, sizeof d0, cudaMemcpyHostToDevice, s));
+  launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, nullptr);
+  ++C->launches;
+  if (C->prm.bounds) bc_walks(C, V);  // the full periodic planes of exchange(1..3)
+  launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
+  ++C->launches;
+  const cudaError_t e = cudaStreamSynchronize(s);  // d0 is a local
+  if (e != cudaSuccess) { set_error(std::string("mf3d_calvel_device: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
+  return MF3D_OK;
+}
+
 int mf3d_newsolv_mg(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr, mf3d_solve_info *info,
                     double *hist, int cap) {
   if (!C || !fields) { mf3d::set_error("mf3d_newsolv_mg: bad arguments"); return MF3D_E_INVALID; }

@@ -1380,6 +1380,23 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
   return MF3D_OK;
 }
 
+/* calvel alone (press.for:139-198 with its exchange(1..3)) on host arrays. */
+int orc_calvel(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, const mf3d_fields *fields, double dt,
+               double alfapr) {
+  Ctx C;
+  int st = setup(C, blocks, nb, prm);
+  if (st) return st;
+  if (C.lsm) { g_err = "calvel: no L_LSM here"; return MF3D_E_UNSUPPORTED; }
+  C.dt = dt; C.alfapr = alfapr;
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    B.ustar = fields[ib].ustar; B.vstar = fields[ib].vstar; B.wstar = fields[ib].wstar;
+    B.u = fields[ib].u; B.v = fields[ib].v; B.w = fields[ib].w; B.p = fields[ib].p;
+  }
+  calvel(C);
+  return MF3D_OK;
+}
+
 /* One V-cycle: su[b] (ttc) in, pp[b] (ttc) out, starting from pp = 0. */
 int orc_mgkcyc(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, double *const *su, double *const *pp) {
   Ctx C;

@@ -42,6 +42,8 @@ def load():
                                            C.c_double, C.c_double, C.POINTER(BlockDesc)]
         lib.orc_rungek_2nd.argtypes = [C.POINTER(BlockDesc), C.c_int, C.POINTER(Params), C.POINTER(Fields),
                                        C.POINTER(RkFields), C.c_double, C.c_double, C.c_int, C.c_int, C.c_double]
+        lib.orc_calvel.argtypes = [C.POINTER(BlockDesc), C.c_int, C.POINTER(Params), C.POINTER(Fields),
+                                   C.c_double, C.c_double]
         lib.orc_last_error.restype = C.c_char_p
         _lib = lib
     return _lib

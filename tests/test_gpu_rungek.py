@@ -76,3 +76,48 @@ def test_predictor_refusals(lib, cuda):
     st = lib.mf3d_rungek_2nd_device(proj.ctx, (abi.Fields * 1)(), (RkFields * 1)(), 0.1, 1.0, 1, 0, 0.0)
     proj.close()
     assert st == abi.MF3D_E_UNSUPPORTED
+
+
+def test_two_stages_with_calvel_between(lib, oracle, cuda):
+    """The reference's stage loop (flosol.for:151-172) with kuttacond = 2:
+    predictor (alfabc 1), calvel, predictor (alfabc 0) - mf3d_rungek_2nd_device,
+    mf3d_calvel_device, mf3d_rungek_2nd_device on one context against the
+    oracle's rungek_2nd, calvel, rungek_2nd."""
+    import torch
+    from multiflow3d_b200.problems import fields_struct
+    pr = Problem(2, 1, 2, 16, 12, 16, bc=(1, 2, W, W, P, P), ngrid=2, pl=2)
+    pl_ex, ubulk, dt = 1, 0.4, 0.011
+    alfark = (0.5, 1.0)
+    blocks, rk = rk_inputs(pr, 23)
+    gpu = [{k: dev(v, cuda) for k, v in f.items()} for f in blocks]
+    grk = [{k: dev(v, cuda) for k, v in r.items()} for r in rk]
+    # oracle
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfark[0], alfabc=1, pl_ex=pl_ex, ubulk=ubulk) == 0
+    prm_o = pr.params(pl_ex=pl_ex, bounds=1, alfabc=1, ubulk=ubulk)
+    assert oracle.orc_calvel(pr.descriptors(oracle), pr.nblocks, C.byref(prm_o), fields_struct(blocks),
+                             dt, alfark[0]) == 0
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfark[1], alfabc=0, pl_ex=pl_ex, ubulk=ubulk) == 0
+    # device
+    proj = Projection(pr.descriptors(lib), pr.params(pl_ex=pl_ex, bounds=1, alfabc=1, ubulk=ubulk), lib)
+    fa = (abi.Fields * pr.nblocks)()
+    ra = (RkFields * pr.nblocks)()
+    dp = C.POINTER(C.c_double)
+    for b in range(pr.nblocks):
+        for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p"):
+            setattr(fa[b], k, C.cast(C.c_void_p(gpu[b][k].data_ptr()), dp))
+        for k in ("uoo", "voo", "woo", "vis"):
+            setattr(ra[b], k, C.cast(C.c_void_p(grk[b][k].data_ptr()), dp))
+    assert lib.mf3d_rungek_2nd_device(proj.ctx, fa, ra, dt, alfark[0], 1, 0, 0.0) == 0, abi.last_error(lib)
+    assert lib.mf3d_calvel_device(proj.ctx, fa, dt, alfark[0]) == 0, abi.last_error(lib)
+    assert lib.mf3d_rungek_2nd_device(proj.ctx, fa, ra, dt, alfark[1], 0, 0, 0.0) == 0, abi.last_error(lib)
+    proj.close()
+    torch.cuda.synchronize()
+    pl = pr.pl
+    inner = (slice(pl, pl + pr.nz), slice(pl, pl + pr.ny), slice(pl, pl + pr.nx))
+    for b in range(pr.nblocks):
+        got = {k: v.cpu().numpy() for k, v in gpu[b].items()}
+        for k in ("ustar", "vstar", "wstar"):
+            assert np.array_equal(got[k][inner], blocks[b][k][inner]), (b, k)
+        for k in ("u", "v", "w"):
+            m = face_mask(got[k].shape, pl, pl_ex)
+            assert np.array_equal(got[k][m], blocks[b][k][m]), (b, k)
