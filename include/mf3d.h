@@ -224,7 +224,8 @@ typedef struct mf3d_rk_fields {
  * - then rungek_diff2nd (rungek.for:584-779), the reference's branch without
  * L_LSM, immersed boundaries or wall functions.  In: u, v, w (their ghosts
  * are refreshed by boundu/v/w, as in the reference), `rk`; out: ustar,
- * vstar, wstar over the faces calvel later reads (isu..ieu etc.).
+ * vstar, wstar over the faces calvel later reads (isu..ieu etc.).  `p` must
+ * be set as for the projection (not read here; su and dens may be NULL).
  * `alfabc`: 1 on the first stage, 0 after (flosol.for:153-157); `alfapr`:
  * the stage's alfark.  `pressureforce` adds dt*alfapr*forcn to ustar
  * (rungek.for:642-656).  Device pointers; contexts from mf3d_create with
