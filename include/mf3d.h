@@ -226,8 +226,11 @@ typedef struct mf3d_rk_fields {
  * are refreshed by boundu/v/w, as in the reference), `rk`; out: ustar,
  * vstar, wstar over the faces calvel later reads (isu..ieu etc.).  `p` must
  * be set as for the projection (not read here; su and dens may be NULL).
- * `alfabc`: 1 on the first stage, 0 after (flosol.for:153-157); `alfapr`:
- * the stage's alfark.  `pressureforce` adds dt*alfapr*forcn to ustar
+ * `alfabc`: 1 on the first stage, 0 after (flosol.for:153-157) - the
+ * context's own `alfabc` stays the projection's; `alfapr`: the stage's
+ * alfark.  With the start-of-step velocities at hand, the stage's boundu/v/w
+ * also restate the convective outflow (code 21, bounds.for:143-170), which
+ * the projection's bounds mode refuses.  `pressureforce` adds dt*alfapr*forcn to ustar
  * (rungek.for:642-656).  Device pointers; contexts from mf3d_create with
  * `bounds = 1`, FP64, uniform spacing, no lsm (else MF3D_E_UNSUPPORTED).
  * Between stages the reference runs calvel (flosol.for:171;

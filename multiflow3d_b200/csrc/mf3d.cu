@@ -1498,11 +1498,11 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
 // bounds.for:143-170), wall functions (61 and up: log_law, wall_function),
 // and under L_LSM the inflow and outflow faces, which phi gates
 // (bounds.for:43-50, 146-158).
-static bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc) {
+static bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc, bool have_oo = false) {
   if (code >= 61) return true;
   if (f == 0 && (code == 7 || code == 8 || code == 12 || code == 13)) return true;
-  if (f == 1 && code == 21 && alfabc == 1) return true;
-  if (lsm && ((f == 0 && code == 1) || (f == 1 && code == 2 && alfabc == 1))) return true;
+  if (f == 1 && code == 21 && alfabc == 1 && !have_oo) return true;
+  if (lsm && ((f == 0 && code == 1) || (f == 1 && (code == 2 || code == 21) && alfabc == 1))) return true;
   return false;
 }
 
@@ -1517,11 +1517,11 @@ static void bc_walks(mf3d_ctx *C, View &V, int only = -1) {
       }
 }
 // the faces without a neighbour by their code, layers 0..pl_ex (only as above)
-static void bound_faces(mf3d_ctx *C, View &V, int alfabc, int only = -1) {
+static void bound_faces(mf3d_ctx *C, View &V, int alfabc, int only = -1, double dt = 0.0, double alfapr = 0.0) {
   for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
     for (int a = 0; a < 3; ++a) {
       launch(k_bound_faces, V.n_bcax[a], kTile, 0, C->stream, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly, C->prm.ubulk,
-             alfabc, only);
+             alfabc, only, dt, alfapr);
       ++C->launches;
     }
 }
@@ -2141,7 +2141,7 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
     const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
     const int nbrs[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
     for (int f = 0; f < 6; ++f)
-      if (nbrs[f] < 0 && bounds_code_unsupported(f, bcs[f], false, alfabc)) {
+      if (nbrs[f] < 0 && bounds_code_unsupported(f, bcs[f], false, alfabc, true)) {
         set_error("mf3d_rungek_2nd_device: face code " + std::to_string(bcs[f]) + " with alfabc " +
                   std::to_string(alfabc) + " reads data the library does not hold");
         return MF3D_E_UNSUPPORTED;
@@ -2165,11 +2165,15 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
   // they were before their own bound; rungek_diff2nd fused per component
   for (int comp = 0; comp < 3; ++comp) {
     bc_walks(C, V, comp);
-    bound_faces(C, V, alfabc, comp);
+    bound_faces(C, V, alfabc, comp, dt, alfapr);
     launch(k_rk2nd, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, comp, dt, alfapr, pressureforce, forcn);
     ++C->launches;
   }
   const cudaError_t e = cudaStreamSynchronize(s);
+  for (auto &F : V.hf) {  // the caller's buffers are bound for this call only
+    F.oo[0] = F.oo[1] = F.oo[2] = nullptr;
+    F.vis = nullptr;
+  }
   if (e != cudaSuccess) { set_error(std::string("mf3d_rungek_2nd_device: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
   return MF3D_OK;
 }

@@ -359,12 +359,15 @@ __global__ void k_bc_walk(const BlkFld *__restrict__ fl, const Tile *__restrict_
 //     w = 1.1 (bounds.for:42-53, 374-377, 662-665; 226-229, 536-539, 873-876);
 //   outflow (2) on the east with alfabc = 1: every layer copies the last
 //     face ie (bounds.for:136-170, 444-470);
+//   convective outflow (21) on the east with alfabc = 1, when the velocity
+//     predictor has bound the start-of-step velocities: oo(ie+1+ly) -
+//     dt*alfapr*(oo(ie+1+ly) - oo(ie))/dx (the same branches);
 // x-face symmetry, periodic faces and codes without a branch write nothing.
 // Launched per layer for x, y, z (the reference's W, E, S, N, B, T).
 // Skipped after a diverged solve.
 __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
                               const DomState *__restrict__ ds, int ax, int ly, double ubulk, int alfabc,
-                              int only) {
+                              int only, double dt, double alfapr) {
   pdl_wait();
   const Tile t = tiles[blockIdx.x];
   const BlkFld &F = fl[t.blk];
@@ -392,6 +395,7 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
     mode = 1;
     cv = ax == 0 ? (comp == 0 ? ubulk : 0.0) : (comp == 2 ? 1.1 : 0.0);
   } else if (code == 2 && ax == 0 && side == 1 && alfabc == 1) mode = 4;  // outflow: u(ie+1+ly) = u(ie)
+  else if (code == 21 && ax == 0 && side == 1 && alfabc == 1 && F.oo[comp]) mode = 5;  // convective outflow
   if (!mode) return;
   // the widened ranges of the other two axes: 0 .. end+1
   const int as = ax == 0 ? 1 : 0, at = ax == 2 ? 1 : 2;
@@ -399,6 +403,12 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   double *fi = comp_field(F, comp);
   const int s0 = 1, e0 = comp_end(F, comp, ax);
   const long long g = fidx_ax(F, ax, side ? e0 + 1 + ly : s0 - 1 - ly, sl, tl);
+  if (mode == 5) {  // oo(ie+1+ly) - dt*alfapr*(oo(ie+1+ly) - oo(ie))/dx, from the start-of-step velocity
+    const double *oo = F.oo[comp];
+    const double og = oo[g], oe = oo[fidx_ax(F, ax, e0, sl, tl)];
+    fi[g] = og - dt * alfapr * (og - oe) / F.h[0][1];
+    return;
+  }
   const int src = mode == 4 ? e0 : side ? e0 - ly : s0 + ly;
   const double m = fi[fidx_ax(F, ax, src, sl, tl)];
   fi[g] = mode == 1 ? cv : mode == 2 ? -m : m;

@@ -68,6 +68,8 @@ struct Blk {
   /* EXT: cell widths per level incl. ghost cells, index 0..n+1 */
   std::vector<std::vector<double>> hx, hy, hz;
   bool stretched;
+  /* the velocity predictor: uoo, voo, woo (the convective outflow, code 21) */
+  const double *oo[3] = {nullptr, nullptr, nullptr};
 };
 
 /* The reference runs one MPI rank per block; the restatement runs the
@@ -879,14 +881,15 @@ void pbound(Ctx &C) {
  * (bounds.for:36-42, 136-140, 179-186, 212-219, 246-259, 301-308 for u;
  * 369-373, 444-448, 505-533, 535-548, 588-595 for v; 657-661, 738-742,
  * 799-806, 833-840, 866-876, 900-908 for w.) */
-bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc) {
+bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc, bool have_oo = false) {
   /* the branches that read data outside the projection: inflow files, SEM
    * and power-law inlets (west 7, 8, 12, 13), the convective outflow (east
-   * 21, uoo), wall functions (61+), phi-gated inflow/outflow under L_LSM */
+   * 21) unless uoo, voo, woo are at hand (the velocity predictor), wall
+   * functions (61+), phi-gated inflow/outflow under L_LSM */
   if (code >= 61) return true;
   if (f == 0 && (code == 7 || code == 8 || code == 12 || code == 13)) return true;
-  if (f == 1 && code == 21 && alfabc == 1) return true;
-  if (lsm && ((f == 0 && code == 1) || (f == 1 && code == 2 && alfabc == 1))) return true;
+  if (f == 1 && code == 21 && alfabc == 1 && !have_oo) return true;
+  if (lsm && ((f == 0 && code == 1) || (f == 1 && (code == 2 || code == 21) && alfabc == 1))) return true;
   return false;
 }
 void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
@@ -904,6 +907,7 @@ void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
   else if (code == 1 && f == 0) { mode = 1; cv = comp == 0 ? C.ubulk : 0.0; }
   else if (code == 1 && f == 4) { mode = 1; cv = comp == 2 ? 1.1 : 0.0; }
   else if (code == 2 && f == 1 && C.alfabc == 1) mode = 4;
+  else if (code == 21 && f == 1 && C.alfabc == 1 && B.oo[op - 1]) mode = 5;
   if (!mode) return;
   int is, ie, js, je, ks, ke;
   franges(B, op, is, ie, js, je, ks, ke);
@@ -917,7 +921,17 @@ void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
     if (ax == 1) return F(B, fi, s, a, t);
     return F(B, fi, s, t, a);
   };
-  const int ghost = high ? e0 + 1 + ly : s0 - 1 - ly, mirror = mode == 4 ? e0 : high ? e0 - ly : s0 + ly;
+  const int ghost = high ? e0 + 1 + ly : s0 - 1 - ly, mirror = mode >= 4 ? e0 : high ? e0 - ly : s0 + ly;
+  if (mode == 5) {  /* convective outflow (bounds.for:143-170 and boundv/w's branch) */
+    const double *oo = B.oo[op - 1];
+    const double dt = C.dt, alfapr = C.alfapr, dx = B.d.dx;
+    for (int t = ta - 1; t <= tb + 1; ++t)
+      for (int s = sa - 1; s <= ea + 1; ++s) {
+        const double og = F(B, oo, ghost, s, t), oe = F(B, oo, e0, s, t);
+        at(ghost, s, t) = og - dt * alfapr * (og - oe) / dx;
+      }
+    return;
+  }
   for (int t = ta - 1; t <= tb + 1; ++t)
     for (int s = sa - 1; s <= ea + 1; ++s)
       at(ghost, s, t) = mode == 1 ? cv : mode == 2 ? -at(mirror, s, t) : at(mirror, s, t);
@@ -1362,11 +1376,18 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
                    const mf3d_rk_fields *rk, double dt, double alfapr, int alfabc, int pressureforce, double forcn) {
   Ctx C;
   mf3d_params p = *prm;
-  p.bounds = 1;
+  p.bounds = 0;  /* the face codes are checked below, with uoo at hand */
   p.alfabc = alfabc;
   int st = setup(C, blocks, nb, &p);
   if (st) return st;
   if (C.lsm) { g_err = "rungek_2nd: no L_LSM branch"; return MF3D_E_UNSUPPORTED; }
+  C.bounds = true;
+  for (auto &B : C.b) {
+    const int bcs[6] = {B.d.bc_west, B.d.bc_east, B.d.bc_south, B.d.bc_north, B.d.bc_bottom, B.d.bc_top};
+    const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
+    for (int f = 0; f < 6; ++f)
+      if (nbr[f] < 0 && bounds_code_unsupported(f, bcs[f], false, alfabc, true)) { g_err = "bounds: face code"; return MF3D_E_UNSUPPORTED; }
+  }
   C.dt = dt; C.alfapr = alfapr;
   std::vector<const double *> uoo(nb), voo(nb), woo(nb), vis(nb);
   for (int ib = 0; ib < nb; ++ib) {
@@ -1375,6 +1396,7 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
     B.ustar = fields[ib].ustar; B.vstar = fields[ib].vstar; B.wstar = fields[ib].wstar;
     B.u = fields[ib].u; B.v = fields[ib].v; B.w = fields[ib].w; B.p = fields[ib].p;
     uoo[ib] = rk[ib].uoo; voo[ib] = rk[ib].voo; woo[ib] = rk[ib].woo; vis[ib] = rk[ib].vis;
+    B.oo[0] = rk[ib].uoo; B.oo[1] = rk[ib].voo; B.oo[2] = rk[ib].woo;
   }
   rungek_2nd(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
   return MF3D_OK;

@@ -23,6 +23,8 @@ CASES = {
         lambda: Problem(2, 2, 1, 16, 16, 8, bc=(P, P, P, P, W, W), ngrid=2, pl=2), 1, 1, 1),
     "2x1x2 inflow / outflow x, walls y, periodic z, first stage": (
         lambda: Problem(2, 1, 2, 16, 8, 16, bc=(1, 2, W, W, P, P), ngrid=2, pl=3), 2, 1, 0),
+    "2x1x1 inflow / convective outflow x, walls y, periodic z, first stage": (
+        lambda: Problem(2, 1, 1, 16, 8, 8, bc=(1, 21, W, W, P, P), ngrid=2, pl=2), 1, 1, 0),
     "1 block, walls and symmetry, later stage": (
         lambda: Problem(1, 1, 1, 16, 12, 8, bc=(W, W, S, S, W, W), ngrid=2, pl=2), 1, 0, 0),
 }
@@ -44,7 +46,9 @@ def test_predictor_matches_oracle(lib, oracle, cuda, case):
     grk = [{k: dev(v, cuda) for k, v in r.items()} for r in rk]
     assert orc_rk(oracle, pr, blocks, rk, dt, alfapr, alfabc=alfabc, pforce=pforce, forcn=forcn,
                   pl_ex=pl_ex, ubulk=ubulk) == 0
-    prm = pr.params(pl_ex=pl_ex, bounds=1, alfabc=alfabc, ubulk=ubulk)
+    # the context's alfabc is the projection's own (its final boundu/v/w);
+    # the stage's comes with each predictor call
+    prm = pr.params(pl_ex=pl_ex, bounds=1, alfabc=0, ubulk=ubulk)
     proj = Projection(pr.descriptors(lib), prm, lib)
     fa = (abi.Fields * pr.nblocks)()
     ra = (RkFields * pr.nblocks)()

@@ -114,10 +114,31 @@ def test_oracle_predictor_zero_step_is_identity(oracle):
         assert np.array_equal(f["ustar"][I], r["uoo"][I])
 
 
+def test_oracle_predictor_convective_outflow(oracle):
+    """Code 21 on the east face, first stage: every ghost layer of u, v, w
+    holds oo(g) - dt*alfapr*(oo(g) - oo(ie))/dx from the start-of-step
+    velocity (bounds.for:143-170 and boundv/boundw's branch); ie is one face
+    short of the boundary for u.  v's row on the north wall face is checked
+    out: the north face comes after the east one and zeroes it there."""
+    pr = Problem(1, 1, 1, 12, 8, 8, bc=(1, 21, W, W, P, P), ngrid=1, pl=2, dx=0.1, dy=0.1, dz=0.1)
+    blocks, rk = rk_inputs(pr, 6)
+    dt, alfapr = 0.02, 0.5
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfapr, alfabc=1, pl_ex=1, ubulk=0.3) == 0
+    pl, n = pr.pl, pr.nx
+    J, K = slice(pl, pl + pr.ny), slice(pl, pl + pr.nz)
+    for k, ie in (("u", pl + n - 2), ("v", pl + n - 1), ("w", pl + n - 1)):
+        oo = rk[0][k[0] + "oo"]
+        Jc = slice(pl, pl + pr.ny - 1) if k == "v" else J
+        for ly in range(2):
+            g = ie + 1 + ly
+            want = oo[K, Jc, g] - dt * alfapr * (oo[K, Jc, g] - oo[K, Jc, ie]) / pr.dx
+            assert np.array_equal(blocks[0][k][K, Jc, g], want), (k, ly)
+
+
 def test_oracle_predictor_refuses_other_branches(oracle):
     pr = Problem(1, 1, 1, 8, 8, 8, ngrid=1, pl=1, stretch_y=2.0)
     blocks, rk = rk_inputs(pr, 5)
     assert orc_rk(oracle, pr, blocks, rk, 0.1, 1.0) == -6
-    pr = Problem(1, 1, 1, 8, 8, 8, bc=(1, 21, W, W, W, W), ngrid=1, pl=1)
+    pr = Problem(1, 1, 1, 8, 8, 8, bc=(7, 2, W, W, W, W), ngrid=1, pl=1)
     blocks, rk = rk_inputs(pr, 5)
     assert orc_rk(oracle, pr, blocks, rk, 0.1, 1.0, alfabc=1) == -6
