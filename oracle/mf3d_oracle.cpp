@@ -1264,7 +1264,7 @@ int pressure_1sweep(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
     calvel(C);
     stamp(calls + 1);
     if (iter == C.maxcy) break; /* `if (iter.lt.niter) goto 1000` fails: no further calmas */
-    calmas(C); /* the next round starts with it (press.for:323) */
+    calmas(C); /* the next sipsol call starts from it (press.for:323) */
     if (hist && calls - 1 < cap) hist[calls - 1] = C.rmax;
   }
   int status = conv ? MF3D_OK : MF3D_NOT_CONVERGED;
