@@ -42,8 +42,8 @@ enum mf3d_status {
   MF3D_E_OOM = -3,        /* device allocation failed or over the cap       */
   MF3D_E_TIMEOUT = -4,    /* a bounded device wait gave up                  */
   MF3D_E_NONFINITE = -5,  /* NaN/Inf met in the residual                     */
-  MF3D_E_UNSUPPORTED = -6 /* a reference feature outside this build (LMR,
-                             differencing=2) or an unsupported combination */
+  MF3D_E_UNSUPPORTED = -6 /* a reference feature outside this build (LMR)
+                             or an unsupported combination              */
 };
 
 /* Boundary-condition code meaning "periodic" (control.cin:17-22). Any other
@@ -92,7 +92,9 @@ typedef struct mf3d_params {
   int differencing; /* control.cin differencing: 1 (2nd-order CDS) or 3 (WENO,
                        which L_LSM requires, initial.for:133-135) - calmas
                        takes its 2nd-order divergence for both
-                       (press.for:38-67); 2 (4th order) is not supported      */
+                       (press.for:38-67); 2 (4th-order CDS): calmas' 4th-order
+                       divergence (press.for:13-35), which reads u(i-2) and
+                       u(i+1): needs pl >= 2, uniform spacing, no lsm          */
   int precision;    /* enum mf3d_precision                                   */
   int device;       /* CUDA device ordinal                                   */
   int pl_ex;        /* extra ghost planes (control.cin pl_ex; pl = LMR + pl_ex,
@@ -134,11 +136,14 @@ typedef struct mf3d_params {
 } mf3d_params;
 
 /* Field pointers of one block, each a (ttc_i,ttc_j,ttc_k) array.
- * ustar/vstar/wstar: in.  p: in/out.  u/v/w: in (faces on physical walls,
- * which calvel never writes) and out (all faces calvel writes, and the ghost
- * faces exchange(1..3) refreshes: layers 0..pl_ex over the interior
- * tangential range on every face that is not a physical wall; ghost edges and
- * corners are left as given).  For the host
+ * ustar/vstar/wstar: in.  p: in/out (interior and every ghost that
+ * p = p + pp, exchange(4) and pbound write).  u/v/w: in (faces on physical
+ * walls, which calvel never writes) and out (all faces calvel writes, and
+ * every ghost exchange(1..3) writes: in mf3d_create contexts its periodic
+ * planes, face layers 0..pl_ex and the ghost edges and corners of its
+ * corner and edge neighbours, exchange.for:343-2498; in batch and server
+ * contexts the face layers 0..pl_ex over the interior tangential range
+ * alone, other ghosts left as given).  For the host
  * entry point these are host pointers; for the `_device` one, device pointers.
  * `su` may be NULL; if set it receives the final RHS div(u)/dt (calmas;
  * sup under lsm).  `dens` (in, lsm only, else ignored): cell densities, ghost
@@ -306,9 +311,11 @@ int mf3d_mgkcyc_device(mf3d_ctx *ctx, double *const *su, double *const *pp);
  * - The array is shared by every context on a device: calls on one device
  *   must not overlap (from several threads, or on several contexts whose
  *   streams run concurrently); overlapping calls race on the tables.
- * - The first call on a device looks up the array's address
- *   (cudaGetSymbolAddress) with that device current; make that first call
- *   before any stream capture on the device. */
+ * - The set-up happens when the context is created: mf3d_create looks up
+ *   the array's device address (cudaGetSymbolAddress) with the context's
+ *   device current, keeps it in the context, and loads every kernel the
+ *   V-cycle can launch, so that no call makes the driver load code on first
+ *   use.  A context created after a device reset looks the address up anew. */
 #define MF3D_NOALLOC_MAX_BLOCKS 512
 int mf3d_mgkcyc_device_noalloc(mf3d_ctx *ctx, double *const *su, double *const *pp);
 
@@ -339,6 +346,29 @@ enum mf3d_profile_kind {
 int mf3d_profile(mf3d_ctx *ctx, int kind);
 int mf3d_profile_read(mf3d_ctx *ctx, double *total_ms, long long *launches,
                       double *algorithmic_bytes);
+
+/* Host-only view of a field exchange: exchange(op) of exchange.for:2-23
+ * (exchange_bc on the periodic faces, then exchange_smlvl with its corners,
+ * edges and faces), followed by pbound for op 4 (press.for:77-137), as
+ * (destination, source) cell pairs against the state before the exchange.
+ * op 1, 2, 3: u, v, w with layers 0..pl_ex; op 4: p with one layer.  Cell
+ * number = base(b) + (i-1) + ttc_i*((j-1) + ttc_j*(k-1)), 1-based field
+ * indices, base(b) the sum of the ttc volumes of the blocks before b.  With
+ * dst == NULL returns the pair count; -1 on bad arguments.  Needs no GPU. */
+long long mf3d_field_exchange_map(const mf3d_block_desc *blocks, int nblocks, int pl, int pl_ex, int op,
+                                  long long *dst, long long *src);
+
+/* Testing aids for the failure paths (no counterpart in the reference, which
+ * prints and stops).  Neither faults the device.
+ * mf3d_test_fail_alloc: the device allocation `after` allocations from now
+ * (0 = the next one) fails as if the device were out of memory, so the call
+ * making it returns MF3D_E_OOM; -1 turns the injection off.  Process-wide.
+ * mf3d_test_stall_copy: on `device`, the next red-black half-sweep declares
+ * `bytes` (1..65536) more on one CTA's first copy barrier than its copies
+ * deliver; that CTA's bounded wait gives up after 2 s and the call returns
+ * MF3D_E_TIMEOUT.  The copies themselves complete; 0 clears it. */
+int mf3d_test_fail_alloc(long long after);
+int mf3d_test_stall_copy(int device, int bytes);
 
 /* Host-only view of the multigrid halo refresh of level `level` (1-based)
  * that follows every smoothing sweep: the composition of mgbound,

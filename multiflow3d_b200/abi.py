@@ -171,6 +171,9 @@ EXPORTED_SYMBOLS = (
     "mf3d_tecbin_encode_device",
     "mf3d_rungek_2nd_device",
     "mf3d_calvel_device",
+    "mf3d_field_exchange_map",
+    "mf3d_test_fail_alloc",
+    "mf3d_test_stall_copy",
 )
 
 MF3D_NOALLOC_MAX_BLOCKS = 512
@@ -228,6 +231,11 @@ def _declare(lib):
     lib.mf3d_rungek_2nd_device.argtypes = [vp, C.POINTER(Fields), C.POINTER(RkFields), C.c_double, C.c_double,
                                            C.c_int, C.c_int, C.c_double]
     lib.mf3d_calvel_device.argtypes = [vp, C.POINTER(Fields), C.c_double, C.c_double]
+    lib.mf3d_field_exchange_map.restype = C.c_longlong
+    lib.mf3d_field_exchange_map.argtypes = [C.POINTER(BlockDesc), C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.mf3d_test_fail_alloc.argtypes = [C.c_longlong]
+    lib.mf3d_test_stall_copy.argtypes = [C.c_int, C.c_int]
     return lib
 
 

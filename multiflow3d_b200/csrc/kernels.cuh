@@ -129,6 +129,14 @@ constexpr int OZ_TX = 32, OZ_RJ = 8, OZ_KCH = 16;   // outer calvel/calmas z-mar
 constexpr unsigned long long kMaxWaitNs = 2000000000ull;  // 2 s
 enum : int { ERR_TMA_WAIT = 1 };
 
+// Testing aid (mf3d_test_stall_copy): when nonzero, the first red-black
+// half-sweep CTA that sees it takes it (atomically, so exactly one CTA) and
+// declares that many more bytes on its first plane's barrier than its
+// copies deliver.  That barrier's phase then never completes: the bounded
+// wait gives up after kMaxWaitNs, records ERR_TMA_WAIT and the CTA leaves,
+// its copies long since landed.  Zero (no effect) unless a test sets it.
+__device__ int g_test_extra_tx = 0;
+
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
@@ -141,6 +149,10 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
 __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Raise the current phase's expected transaction bytes without arriving.
+__device__ __forceinline__ void mbar_add_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
   unsigned ok;
@@ -219,18 +231,30 @@ __device__ __forceinline__ void st_hint(float *p, float v, uint64_t pol) {
 // i = 2q + 2 - s with s = i & 1 = (colour + j + k + 1) & 1, so a row of nx
 // cells keeps ceil(nx/2) lanes busy whatever its parity.  Its west and east
 // neighbours (other colour) sit at compact h = q and q+1, the others and the
-// rhs at h = q + 1 - s.  A CTA owns q0..q0+31 of rows j0..j0+RB_RJ-1 (each
-// thread RB_CR rows RB_TY apart, which share s) and marches up `kch` planes.
+// rhs at h = q + 1 - s.  A column is q0..q0+31 of rows j0..j0+RB_RJ-1 of one
+// block (each thread RB_CR rows RB_TY apart, which share s); a segment is a
+// run of planes k0..k1 of one column.  The planes of all columns of the
+// launch are laid end to end and split evenly over the CTAs the device holds
+// at once, so every CTA marches the same number of planes - a CTA whose
+// share crosses a column boundary runs two segments, each with its own ring
+// fill - and the launch is one wave with no tail.
 // Per plane one thread issues two TMA box loads - the other colour over
 // compact columns q0..q0+W-1 and rows j0-1..j0+RB_RJ, the rhs over the same
 // columns and rows j0..j0+RB_RJ-1 - into a ring of RB_NS stages, RB_PD
-// planes ahead of the plane being computed.  Boxes that reach past the array
-// read zeros (never used).
+// planes ahead of the plane being computed.  Loads are numbered across the
+// CTA's segments, which fixes each one's stage and mbarrier phase.  Boxes
+// that reach past the array read zeros (never used).
 // ---------------------------------------------------------------------------
 constexpr int RB_PD = 2;          // prefetch distance in planes
-constexpr int RB_KMAX = 32;       // planes per CTA at most
+constexpr int RB_KMAX = 64;       // planes per segment at most
 constexpr int RB_NS = RB_PD + 2;  // stages: planes k-1 .. k+RB_PD (a power of two)
 static_assert((RB_NS & (RB_NS - 1)) == 0, "RB_NS must be a power of two");
+
+// A run of planes k0..k1 of one sweep column (block blk, compact columns
+// q0.., rows j0..).
+struct RbSeg {
+  int blk, k0, k1, j0, q0, pad0, pad1, pad2;
+};
 
 template <typename T>
 struct RbShape {
@@ -240,10 +264,11 @@ struct RbShape {
   static constexpr int RBY = (RE * (int)sizeof(T) + 127) / 128 * 128;
 };
 
+// CTA c runs segments first[c] .. first[c+1]-1 of `segs`.
 template <typename T, bool FROM_ZERO>
-__global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict__ bl, const Tile *__restrict__ tiles,
-                                                       const int *__restrict__ act, int colour, int kch,
-                                                       int *__restrict__ err) {
+__global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict__ bl, const RbSeg *__restrict__ segs,
+                                                       const int *__restrict__ first, const int *__restrict__ act,
+                                                       int colour, int *__restrict__ err) {
   pdl_wait();
   using S = RbShape<T>;
   constexpr int W = S::W;
@@ -251,105 +276,120 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
   __shared__ __align__(128) unsigned char sbuf[RB_NS * (OB + S::RBY)];
   __shared__ __align__(8) uint64_t bar[RB_NS];
   __shared__ int abort_s;  // set when a wait gave up: every thread leaves after the next barrier
-  __shared__ T sab[RB_KMAX], sat[RB_KMAX];  // z coefficients of the CTA's planes
-  const Tile t = tiles[blockIdx.x];
-  const BlkLev B = bl[t.blk];
-  if (!act[B.dom]) return;
+  __shared__ T sab[RB_KMAX], sat[RB_KMAX];  // z coefficients of the segment's planes
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * RB_TX + tx;
-  const int q0 = t.i0, q = q0 + tx;
-  const int nx = B.nx, ny = B.ny, hp = B.hp;
-  const long long rs = (long long)(ny + 2) * hp;  // plane stride
-  T *__restrict__ M = phi_of<T>(B) + colour * B.cstr + q0;
-  const CUtensorMap *mo = B.tm + (1 - colour), *mr = B.tm + 2 + colour;
-  const Coef<T> cf(B);
-  const int k0 = t.k0, k1 = min(t.k0 + kch - 1, B.nz);
-  // coefficients of this lane's two cells (s = 0: i = 2q+2; s = 1: i = 2q+1)
-  const int ia = min(2 * q + 2, nx + 1), ib = min(2 * q + 1, nx + 1);
-  const T aw0 = cf.aw[ia], ae0 = cf.ae[ia], aw1 = cf.aw[ib], ae1 = cf.ae[ib];
-  // per row: as, an and ap's first four terms (summed left to right)
-  T as[RB_CR], an[RB_CR], pa0[RB_CR], pa1[RB_CR];
-  int rowoff[RB_CR];  // j*hp of each row
-#pragma unroll
-  for (int m = 0; m < RB_CR; ++m) {
-    const int j = t.j0 + ty + RB_TY * m;
-    const bool jin = j <= ny;
-    as[m] = jin ? cf.as[j] : (T)0;
-    an[m] = jin ? cf.an[j] : (T)0;
-    pa0[m] = ((aw0 + ae0) + as[m]) + an[m];
-    pa1[m] = ((aw1 + ae1) + as[m]) + an[m];
-    rowoff[m] = j * hp;
-  }
-  const int nrow = t.j0 + ty > ny ? 0 : min(RB_CR, (ny - t.j0 - ty) / RB_TY + 1);  // rows inside the block
   auto slot_o = [&](int st) { return (T *)(sbuf + st * OB); };
   auto slot_r = [&](int st) { return (T *)(sbuf + RB_NS * OB + st * S::RBY); };
-  auto loads = [&](int kk) { return FROM_ZERO ? (kk >= k0 && kk <= k1) : (kk >= k0 - 1 && kk <= k1 + 1); };
-  // the loaded planes are consecutive from slot 0, so each slot's phases
-  // complete in order (k0-1 is loaded unless FROM_ZERO)
-  constexpr int first = FROM_ZERO ? 0 : 1;
-  auto stage = [&](int kk) { return (kk - k0 + first) & (RB_NS - 1); };
-  auto parity = [&](int kk) { return (unsigned)(((kk - k0 + first) / RB_NS) & 1); };
   // L2: the rhs is read once per half-sweep (evict first); the colour
   // written here is what the next half-sweep reads (evict last)
   const uint64_t pol_first = l2_evict_first(), pol_last = l2_evict_last();
-  auto issue = [&](int kk) {
-    const int st = stage(kk);
-    const bool wr = kk >= k0 && kk <= k1;
-    const unsigned bytes = (FROM_ZERO ? 0u : (unsigned)(S::OE * sizeof(T))) + (wr ? (unsigned)(S::RE * sizeof(T)) : 0u);
-    mbar_expect_tx(&bar[st], bytes);
-    if (!FROM_ZERO) tma_load_3d(slot_o(st), mo, &bar[st], q0, t.j0 - 1, kk);
-    if (wr) tma_load_3d_hint(slot_r(st), mr, &bar[st], q0, t.j0, kk, pol_first);
-  };
   if (tid == 0) {
     for (int st = 0; st < RB_NS; ++st) mbar_init(&bar[st], 1);
     mbar_fence_init();
     abort_s = 0;
   }
-  for (int q = tid; q <= k1 - k0; q += RB_TX * RB_TY) {
-    sab[q] = cf.ab[k0 + q];
-    sat[q] = cf.at[k0 + q];
-  }
-  __syncthreads();
-  if (tid == 0)
-    for (int kk = k0 - 1; kk < k0 + RB_PD; ++kk)
-      if (loads(kk)) issue(kk);
-  bool ok = true;
-  if (loads(k0 - 1)) ok = mbar_wait(&bar[stage(k0 - 1)], parity(k0 - 1), err);
-  if (ok) ok = mbar_wait(&bar[stage(k0)], parity(k0), err);
-  for (int k = k0; k <= k1; ++k) {
-    if (tid == 0 && ok && loads(k + RB_PD)) issue(k + RB_PD);  // refills the slot of plane k-2
-    if (ok && !FROM_ZERO) ok = mbar_wait(&bar[stage(k + 1)], parity(k + 1), err);
-    if (ok && FROM_ZERO && k > k0) ok = mbar_wait(&bar[stage(k)], parity(k), err);
-    const int s = (colour + t.j0 + ty + k + 1) & 1;  // the same for all rows of the thread
-    const int i = 2 * q + 2 - s;
-    if (ok && i <= nx) {
-      const int st = stage(k), hc = tx + 1 - s;
-      const T ab = sab[k - k0], at = sat[k - k0];
-      const T aw = s ? aw1 : aw0, ae = s ? ae1 : ae0;
-      const T *o = slot_o(st), *ob = slot_o(stage(k - 1)), *ot = slot_o(stage(k + 1));
-      const T *r = slot_r(st);
-      T *Mk = M + (long long)k * rs + hc;
+  // loads the CTA issued in earlier segments: load n goes to stage n % RB_NS
+  // and completes phase (n / RB_NS) & 1 of that stage's mbarrier
+  int base = 0;
+  bool hook = tid == 0;  // testing aid, looked at once per CTA
+  const int s_end = first[blockIdx.x + 1];
+  for (int si = first[blockIdx.x]; si < s_end; ++si) {
+    const RbSeg t = segs[si];
+    const BlkLev B = bl[t.blk];
+    if (!act[B.dom]) continue;
+    const int q0 = t.q0, q = q0 + tx;
+    const int nx = B.nx, ny = B.ny, hp = B.hp;
+    const long long rs = (long long)(ny + 2) * hp;  // plane stride
+    T *__restrict__ M = phi_of<T>(B) + colour * B.cstr + q0;
+    const CUtensorMap *mo = B.tm + (1 - colour), *mr = B.tm + 2 + colour;
+    const Coef<T> cf(B);
+    const int k0 = t.k0, k1 = t.k1;
+    // coefficients of this lane's two cells (s = 0: i = 2q+2; s = 1: i = 2q+1)
+    const int ia = min(2 * q + 2, nx + 1), ib = min(2 * q + 1, nx + 1);
+    const T aw0 = cf.aw[ia], ae0 = cf.ae[ia], aw1 = cf.aw[ib], ae1 = cf.ae[ib];
+    // per row: as, an and ap's first four terms (summed left to right)
+    T as[RB_CR], an[RB_CR], pa0[RB_CR], pa1[RB_CR];
+    int rowoff[RB_CR];  // j*hp of each row
 #pragma unroll
-      for (int m = 0; m < RB_CR; ++m) {
-        if (m < nrow) {
-          const int rr = ty + RB_TY * m;  // row within the tile
-          T w = (T)0, e = (T)0, so_ = (T)0, no = (T)0, bo = (T)0, to = (T)0;
-          if (!FROM_ZERO) {
-            w = o[(rr + 1) * W + tx];
-            e = o[(rr + 1) * W + tx + 1];
-            so_ = o[rr * W + hc];
-            no = o[(rr + 2) * W + hc];
-            bo = ob[(rr + 1) * W + hc];
-            to = ot[(rr + 1) * W + hc];
+    for (int m = 0; m < RB_CR; ++m) {
+      const int j = t.j0 + ty + RB_TY * m;
+      const bool jin = j <= ny;
+      as[m] = jin ? cf.as[j] : (T)0;
+      an[m] = jin ? cf.an[j] : (T)0;
+      pa0[m] = ((aw0 + ae0) + as[m]) + an[m];
+      pa1[m] = ((aw1 + ae1) + as[m]) + an[m];
+      rowoff[m] = j * hp;
+    }
+    const int nrow = t.j0 + ty > ny ? 0 : min(RB_CR, (ny - t.j0 - ty) / RB_TY + 1);  // rows inside the block
+    auto loads = [&](int kk) { return FROM_ZERO ? (kk >= k0 && kk <= k1) : (kk >= k0 - 1 && kk <= k1 + 1); };
+    // the loaded planes are consecutive (k0-1 is loaded unless FROM_ZERO)
+    constexpr int lead = FROM_ZERO ? 0 : 1;
+    auto stage = [&](int kk) { return (base + kk - k0 + lead) & (RB_NS - 1); };
+    auto parity = [&](int kk) { return (unsigned)(((base + kk - k0 + lead) / RB_NS) & 1); };
+    auto issue = [&](int kk) {
+      const int st = stage(kk);
+      const bool wr = kk >= k0 && kk <= k1;
+      const unsigned bytes =
+          (FROM_ZERO ? 0u : (unsigned)(S::OE * sizeof(T))) + (wr ? (unsigned)(S::RE * sizeof(T)) : 0u);
+      mbar_expect_tx(&bar[st], bytes);
+      if (!FROM_ZERO) tma_load_3d(slot_o(st), mo, &bar[st], q0, t.j0 - 1, kk);
+      if (wr) tma_load_3d_hint(slot_r(st), mr, &bar[st], q0, t.j0, kk, pol_first);
+    };
+    for (int z = tid; z <= k1 - k0; z += RB_TX * RB_TY) {
+      sab[z] = cf.ab[k0 + z];
+      sat[z] = cf.at[k0 + z];
+    }
+    __syncthreads();  // the barriers' init; the previous segment's readers of sab/sat and of the ring are done
+    if (tid == 0) {
+      if (hook && *(volatile int *)&g_test_extra_tx) {
+        const unsigned extra = (unsigned)atomicExch(&g_test_extra_tx, 0);
+        if (extra) mbar_add_tx(&bar[stage(FROM_ZERO ? k0 : k0 - 1)], extra);
+      }
+      hook = false;
+      for (int kk = k0 - 1; kk < k0 + RB_PD; ++kk)
+        if (loads(kk)) issue(kk);
+    }
+    bool ok = true;
+    if (loads(k0 - 1)) ok = mbar_wait(&bar[stage(k0 - 1)], parity(k0 - 1), err);
+    if (ok) ok = mbar_wait(&bar[stage(k0)], parity(k0), err);
+    for (int k = k0; k <= k1; ++k) {
+      if (tid == 0 && ok && loads(k + RB_PD)) issue(k + RB_PD);  // refills the slot of plane k-2
+      if (ok && !FROM_ZERO) ok = mbar_wait(&bar[stage(k + 1)], parity(k + 1), err);
+      if (ok && FROM_ZERO && k > k0) ok = mbar_wait(&bar[stage(k)], parity(k), err);
+      const int s = (colour + t.j0 + ty + k + 1) & 1;  // the same for all rows of the thread
+      const int i = 2 * q + 2 - s;
+      if (ok && i <= nx) {
+        const int st = stage(k), hc = tx + 1 - s;
+        const T ab = sab[k - k0], at = sat[k - k0];
+        const T aw = s ? aw1 : aw0, ae = s ? ae1 : ae0;
+        const T *o = slot_o(st), *ob = slot_o(stage(k - 1)), *ot = slot_o(stage(k + 1));
+        const T *r = slot_r(st);
+        T *Mk = M + (long long)k * rs + hc;
+#pragma unroll
+        for (int m = 0; m < RB_CR; ++m) {
+          if (m < nrow) {
+            const int rr = ty + RB_TY * m;  // row within the tile
+            T w = (T)0, e = (T)0, so_ = (T)0, no = (T)0, bo = (T)0, to = (T)0;
+            if (!FROM_ZERO) {
+              w = o[(rr + 1) * W + tx];
+              e = o[(rr + 1) * W + tx + 1];
+              so_ = o[rr * W + hc];
+              no = o[(rr + 2) * W + hc];
+              bo = ob[(rr + 1) * W + hc];
+              to = ot[(rr + 1) * W + hc];
+            }
+            const T ap = (T)-1.0 * (((s ? pa1[m] : pa0[m]) + ab) + at);
+            st_hint(Mk + rowoff[m],
+                    ((r[rr * W + hc] - (aw * w + ae * e + as[m] * so_ + an[m] * no + ab * bo + at * to)) / ap),
+                    pol_last);
           }
-          const T ap = (T)-1.0 * (((s ? pa1[m] : pa0[m]) + ab) + at);
-          st_hint(Mk + rowoff[m], ((r[rr * W + hc] - (aw * w + ae * e + as[m] * so_ + an[m] * no + ab * bo + at * to)) / ap),
-                  pol_last);
         }
       }
+      if (!ok) abort_s = 1;
+      __syncthreads();  // plane k-1's slot is refilled next iteration
+      if (abort_s) return;
     }
-    if (!ok) abort_s = 1;
-    __syncthreads();  // plane k-1's slot is refilled next iteration
-    if (abort_s) return;
+    base += (k1 - k0 + 1) + (FROM_ZERO ? 0 : 2);
   }
 }
 

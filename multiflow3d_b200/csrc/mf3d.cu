@@ -16,7 +16,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -89,6 +91,16 @@ static bool poison_allocations() {
   return e && e[0] && e[0] != '0';
 }
 
+// Testing aid (mf3d_test_fail_alloc): the allocation that brings this
+// countdown from 0 to -1 fails as if the device were out of memory; -1 = off.
+static std::atomic<long long> g_fail_alloc_countdown{-1};
+static bool injected_alloc_failure() {
+  long long c = g_fail_alloc_countdown.load();
+  while (c >= 0 && !g_fail_alloc_countdown.compare_exchange_weak(c, c - 1)) {
+  }
+  return c == 0;
+}
+
 // A device array.  alloc() keeps the current allocation when it is large
 // enough (rebuilt launch tables reuse their buffers).
 template <typename T>
@@ -126,6 +138,10 @@ struct DevBuf {
     }
     release();
     if (count == 0) return MF3D_OK;
+    if (injected_alloc_failure()) {
+      set_error("device allocation: out of memory (injected by mf3d_test_fail_alloc)");
+      return MF3D_E_OOM;
+    }
     cudaError_t e;
     cudaMemPool_t pool = g_alloc_stream ? device_pool() : nullptr;
     if (pool) {
@@ -494,8 +510,64 @@ struct DomainStore {
   std::vector<int> nstaged;                  // per level
   std::vector<DevBuf<HaloCopy>> dhalo;       // per level, the same pairs on the device
   std::vector<FaceRule> rules;               // 6 per block, domain-local sources
+  // exchange(1..3) and exchange(4) + pbound of the fields as copy maps
+  // (mf3d_create contexts): u, v, w pairs and p pairs, staged pairs first
+  DevBuf<FxCopy> fx_uvw, fx_p;
+  long long nfx_uvw = 0, nsfx_uvw = 0, nfx_p = 0, nsfx_p = 0;
   size_t bytes = 0;
 };
+
+// The field exchange maps of a domain: exchange(1), (2), (3) with pl_ex
+// layers (u, v, w) and exchange(4) + pbound (p), as FxCopy lists with the
+// pairs whose source is itself written first (they are staged).
+static int build_field_maps(DomainStore &D, const std::vector<mf3d_block_desc> &descs, int pl, int pl_ex,
+                            cudaStream_t s) {
+  const int nb = (int)descs.size();
+  std::vector<long long> base(nb);
+  long long acc = 0;
+  for (int b = 0; b < nb; ++b) {
+    base[b] = acc;
+    acc += (long long)(descs[b].nx + 2 * pl) * (descs[b].ny + 2 * pl) * (descs[b].nz + 2 * pl);
+  }
+  if (nb > 65535) { set_error("field exchange map: more than 65535 blocks"); return MF3D_E_UNSUPPORTED; }
+  auto loc = [&](long long id, unsigned short &blk, unsigned &off) {
+    const int b = (int)(std::upper_bound(base.begin(), base.end(), id) - base.begin()) - 1;
+    blk = (unsigned short)b;
+    off = (unsigned)(id - base[b]);
+  };
+  auto lists = [&](const std::vector<int> &ops, std::vector<FxCopy> &out, long long &nstaged) {
+    std::vector<FxCopy> staged, plain;
+    for (int op : ops) {
+      std::vector<HaloPair> pr = build_field_map(descs, base, pl, op, op == 4 ? 0 : pl_ex, op == 4);
+      // pr is sorted by dst: a source that is some pair's dst must be staged
+      auto written = [&](long long id) {
+        auto it = std::lower_bound(pr.begin(), pr.end(), id, [](const HaloPair &a, long long v) { return a.dst < v; });
+        return it != pr.end() && it->dst == id;
+      };
+      for (const auto &x : pr) {
+        FxCopy c;
+        loc(x.dst, c.dblk, c.doff);
+        loc(x.src, c.sblk, c.soff);
+        c.comp = op - 1;
+        (written(x.src) ? staged : plain).push_back(c);
+      }
+    }
+    nstaged = (long long)staged.size();
+    out = std::move(staged);
+    out.insert(out.end(), plain.begin(), plain.end());
+  };
+  std::vector<FxCopy> uvw, pp;
+  lists({1, 2, 3}, uvw, D.nsfx_uvw);
+  lists({4}, pp, D.nsfx_p);
+  D.nfx_uvw = (long long)uvw.size();
+  D.nfx_p = (long long)pp.size();
+  int st;
+  if ((st = D.fx_uvw.upload(uvw, s))) return st;
+  if ((st = D.fx_p.upload(pp, s))) return st;
+  D.bytes += (uvw.size() + pp.size()) * sizeof(FxCopy);
+  CK(cudaStreamSynchronize(s));  // the host vectors are locals
+  return MF3D_OK;
+}
 
 static long long level_off(const BlkLev &B, int i, int j, int k) {
   const int c = (i + j + k + 1) & 1;
@@ -503,7 +575,7 @@ static long long level_off(const BlkLev &B, int i, int j, int k) {
 }
 
 static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, int ngrid, int elem, int elem_coarsest,
-                        int pl, cudaStream_t s, bool lsm = false, bool bounds = false) {
+                        int pl, cudaStream_t s, bool lsm = false, bool bounds = false, int field_maps_pl_ex = -1) {
   D.ngrid = ngrid;
   D.blocks.clear();
   std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
@@ -563,6 +635,7 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
     D.bytes += h.size() * sizeof(HaloCopy);
   }
   CK(cudaStreamSynchronize(s));  // the host vectors are locals
+  if (field_maps_pl_ex >= 0 && (st = build_field_maps(D, descs, pl, field_maps_pl_ex, s))) return st;
   return MF3D_OK;
 }
 
@@ -573,9 +646,13 @@ enum Subset { SUB_A = 0, SUB_C = 1, SUB_D = 2 };  // all present / coarsest here
 
 struct ViewLevel {
   DevBuf<BlkLev> tab;                 // one entry per view block (absent: nx = 0)
-  DevBuf<Tile> sweep[3], cells[3];
-  int n_sweep[3] = {0, 0, 0}, n_cells[3] = {0, 0, 0};
-  int kch[3] = {1, 1, 1};             // planes per sweep CTA
+  std::vector<BlkLev> htab;           // host copy of tab (the autotuner rebuilds tables from it)
+  std::vector<int> hblk[3];           // view blocks of each subset
+  int sched = 0;                      // red-black sweep schedule (sweep_segments)
+  DevBuf<RbSeg> sweep[3];             // red-black sweep segments (k_rbgs), per subset
+  DevBuf<int> sfirst[3];              // first segment of each sweep CTA (+ total)
+  DevBuf<Tile> cells[3];
+  int n_sweep[3] = {0, 0, 0}, n_cells[3] = {0, 0, 0};  // sweep CTAs; cell tiles
   DevBuf<int> spre[3];                // small levels: first sweep item of each listed block (+ total)
   long long small_items[3] = {0, 0, 0};
   int small = 0;                      // 1: the level's sweeps use k_rbgs_small
@@ -593,7 +670,7 @@ struct ViewLevel {
   // line relaxation (mg_itrsch 2): TDMA factors of every listed block, and the
   // k_tdma_lines shape: cluster size, lines staged at a time, longest line
   DevBuf<char> tdf;
-  int td_cl = 1, td_gmax = 1, td_nmax = 1, td_lines[3] = {0, 0, 0};
+  int td_cl = 1, td_gmax = 1, td_nmax = 1, td_numax = 1, td_lines[3] = {0, 0, 0};
   int lx_cl = 1;                      // lexicographic relaxation (mg_itrsch 1): CTAs per block
   size_t td_smem = 0;
   bool td_fp64 = true;                // the level relaxes in FP64
@@ -613,6 +690,11 @@ struct View {
   bool bc_periodic[3] = {false, false, false};  // some block has a periodic face along the axis
   int n_pairs = 0, pairs_kch = 1;
   int n_int = 0, n_zint = 0, n_l1cells = 0, n_faces = 0, n_planes = 0, n_vfaces = 0;
+  // field exchanges as copy maps (a view over one domain that has them):
+  // exchange(1..3) of u, v, w and exchange(4) + pbound of p
+  const FxCopy *fx_uvw = nullptr, *fx_p = nullptr;
+  long long nfx_uvw = 0, nsfx_uvw = 0, nfx_p = 0, nsfx_p = 0;
+  DevBuf<double> fx_stage;
   DevBuf<DomState> ds;
   DevBuf<int> act, ones;
   DevBuf<int> err;                    // device error code (a TMA wait that gave up)
@@ -680,6 +762,8 @@ struct mf3d_ctx {
   DevBuf<double> mirror;
   std::vector<size_t> mirror_off;
   DevBuf<double *> ptrs;
+  // mf3d_mgkcyc_device_noalloc: device address of its fixed pointer tables
+  void *noalloc_tab = nullptr;
 };
 
 namespace mf3d {
@@ -715,31 +799,97 @@ static void prof_collect(mf3d_ctx *C) {
 // Levels with at most this many interior cells sweep with k_rbgs_small.
 constexpr long long kSmallLevelCells = 1ll << 19;
 
-// Red-black sweep tiles of a set of blocks: 32 lanes over q (ceil(nx/2) per
-// row), RB_RJ rows, kch planes.  kch is chosen so the CTAs fill the SMs in
-// few waves: the estimated time ceil(CTAs / resident) * (kch + pipeline
-// fill) is minimised over kch in {2, 4, 8, 16, 32}.
-static int sweep_tiles(const mf3d_ctx *C, const std::vector<BlkLev> &tab, const std::vector<int> &blocks,
-                       std::vector<Tile> &out) {
-  out.clear();
-  if (blocks.empty()) return 1;
+// Red-black sweep segments of a set of blocks (k_rbgs).  A column is 32
+// lanes over q (ceil(nx/2) per row) by RB_RJ rows of one block.  Schedules:
+//   0  the planes of all columns laid end to end and cut into equal runs, one
+//      per CTA: as many CTAs as the device holds at once (whole multiples of
+//      that when a run would exceed RB_KMAX planes), so the launch has no
+//      partial wave; a run that crosses a column boundary becomes two
+//      segments;
+//   1  the same over twice as many CTAs (two waves);
+//   2  each column cut into c equal runs, c = resident CTAs / columns (at
+//      least 1): no run crosses a column, at most one wave;
+//   3  the same with c + 1 runs per column.
+// Runs are at least kMinRun planes (shorter ones would be mostly ring fill)
+// and at most RB_KMAX.  Returns the CTA count; first[c] .. first[c+1]-1 are
+// CTA c's segments.
+constexpr long long kMinRun = 4;
+constexpr int kSweepSchedules = 4;
+static int sweep_segments(const mf3d_ctx *C, const std::vector<BlkLev> &tab, const std::vector<int> &blocks,
+                          std::vector<RbSeg> &segs, std::vector<int> &first, int sched = 0) {
+  segs.clear();
+  first.assign(1, 0);
+  long long planes = 0, columns = 0;
+  for (int b : blocks) {
+    const BlkLev &B = tab[b];
+    const long long cols = (long long)((B.nx + 1) / 2 + RB_TX - 1) / RB_TX * ((B.ny + RB_RJ - 1) / RB_RJ);
+    columns += cols;
+    planes += cols * B.nz;
+  }
+  if (planes == 0) return 0;
   const long long resident = (long long)C->nsm * C->sweep_occ;
-  int best = 2;
-  double best_cost = 1e300;
-  for (int kch : {2, 4, 8, 16, RB_KMAX}) {
-    long long n = 0;
+  if (sched >= 2) {
+    const long long c = std::max(1LL, resident / columns) + (sched == 3 ? 1 : 0);
     for (int b : blocks) {
       const BlkLev &B = tab[b];
-      n += (long long)((B.nx + 1) / 2 + RB_TX - 1) / RB_TX * ((B.ny + RB_RJ - 1) / RB_RJ) * ((B.nz + kch - 1) / kch);
+      const long long run = std::min<long long>(RB_KMAX, std::max(kMinRun, (B.nz + c - 1) / c));
+      for (int j0 = 1; j0 <= B.ny; j0 += RB_RJ)
+        for (int q0 = 0; q0 < (B.nx + 1) / 2; q0 += RB_TX)
+          for (int k = 1; k <= B.nz; k += (int)run) {
+            segs.push_back(RbSeg{b, k, (int)std::min<long long>(k + run - 1, B.nz), j0, q0, 0, 0, 0});
+            first.push_back((int)segs.size());
+          }
     }
-    const double cost = (double)((n + resident - 1) / resident) * (kch + RB_PD);
-    if (cost <= best_cost) { best_cost = cost; best = kch; }
+    return (int)first.size() - 1;
+  }
+  const long long target = resident * (sched == 1 ? 2 : 1);
+  const long long waves = (planes + target * RB_KMAX - 1) / (target * RB_KMAX);
+  const long long run = std::max(kMinRun, (planes + target * waves - 1) / (target * waves));
+  long long left = run;
+  for (int b : blocks) {
+    const BlkLev &B = tab[b];
+    for (int j0 = 1; j0 <= B.ny; j0 += RB_RJ)
+      for (int q0 = 0; q0 < (B.nx + 1) / 2; q0 += RB_TX)
+        for (int k = 1; k <= B.nz;) {
+          const int take = (int)std::min<long long>(left, B.nz - k + 1);
+          segs.push_back(RbSeg{b, k, k + take - 1, j0, q0, 0, 0, 0});
+          k += take;
+          left -= take;
+          if (left == 0) {
+            first.push_back((int)segs.size());
+            left = run;
+          }
+        }
+  }
+  if (first.back() != (int)segs.size()) first.push_back((int)segs.size());
+  return (int)first.size() - 1;
+}
+
+// TMA restriction tiles into a coarse level: 32 x RB_RJ/2 coarse cells, kch
+// planes; kch = 0 picks it as for the sweep's estimate (2 resident CTAs per
+// SM: the ring takes ~110 KB).  Returns kch.
+static int rtma_tiles(const mf3d_ctx *C, const std::vector<BlkLev> &tab, const std::vector<int> &blocks, int kch,
+                      std::vector<Tile> &out) {
+  out.clear();
+  if (kch <= 0) {
+    const long long resident = (long long)C->nsm * 2;
+    kch = 2;
+    double best_cost = 1e300;
+    for (int kc : {2, 4, 8, 16}) {
+      long long n = 0;
+      for (int b : blocks) {
+        const BlkLev &B = tab[b];
+        n += (long long)((B.nx + 31) / 32) * ((B.ny + RB_RJ / 2 - 1) / (RB_RJ / 2)) * ((B.nz + kc - 1) / kc);
+      }
+      const double cost = (double)((n + resident - 1) / resident) * (kc + 3);
+      if (cost <= best_cost) { best_cost = cost; kch = kc; }
+    }
   }
   for (int b : blocks) {
     const BlkLev &B = tab[b];
-    add_tiles_2d(out, b, Box{0, (B.nx + 1) / 2 - 1, 1, B.ny, 1, B.nz}, RB_TX, RB_RJ, best);
+    add_tiles_2d(out, b, Box{1, B.nx, 1, B.ny, 1, B.nz}, 32, RB_RJ / 2, kch);
   }
-  return best;
+  return kch;
 }
 
 // Plane tiles of kTile consecutive columns of a GX x GY plane and kch planes
@@ -842,6 +992,7 @@ static int tdma_layout(mf3d_ctx *C, View &V, int g, std::vector<BlkLev> &tab) {
   if (const char *e = std::getenv("MF3D_TD_CLUSTER")) L.td_cl = std::max(1, std::min(16, std::atoi(e)));  // tuning
   shape(L.td_cl, L.td_gmax, L.td_smem);
   L.td_nmax = nmax;
+  L.td_numax = numax;
   if (L.td_smem > cap) {
     set_error("line relaxation: a line of " + std::to_string(nmax) + " cells does not fit in shared memory");
     return MF3D_E_UNSUPPORTED;
@@ -884,7 +1035,8 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
   for (int g = 1; g <= V.Lmax; ++g) {
     ViewLevel &L = V.lv[g];
     std::vector<BlkLev> tab(nb);
-    std::vector<Tile> sw[3], ce[3];
+    std::vector<RbSeg> sw[3];
+    std::vector<Tile> ce[3];
     std::vector<int> li[3], sblk[3];
     for (int b = 0; b < nb; ++b) {
       const BlockStore &S = *V.blk[b];
@@ -953,30 +1105,8 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       L.n_ptile = (int)pt.size();
       if ((st = L.rtile.upload(rt, s))) return st;
       if ((st = L.ptile.upload(pt, s))) return st;
-      // TMA restriction tiles: 32 x RB_RJ/2 coarse cells, kch planes chosen as
-      // for the sweep (2 resident CTAs per SM: the ring takes ~110 KB)
       std::vector<Tile> rm;
-      if (g > 1) {
-        const long long resident = (long long)C->nsm * 2;
-        int best = 2;
-        double best_cost = 1e300;
-        for (int kch : {2, 4, 8, 16}) {
-          long long n = 0;
-          for (int b = 0; b < nb; ++b) {
-            if (g > V.blk[b]->ngrid) continue;
-            const BlkLev &B = tab[b];
-            n += (long long)((B.nx + 31) / 32) * ((B.ny + RB_RJ / 2 - 1) / (RB_RJ / 2)) * ((B.nz + kch - 1) / kch);
-          }
-          const double cost = (double)((n + resident - 1) / resident) * (kch + 3);
-          if (cost <= best_cost) { best_cost = cost; best = kch; }
-        }
-        for (int b = 0; b < nb; ++b) {
-          if (g > V.blk[b]->ngrid) continue;
-          const BlkLev &B = tab[b];
-          add_tiles_2d(rm, b, Box{1, B.nx, 1, B.ny, 1, B.nz}, 32, RB_RJ / 2, best);
-        }
-        L.rtma_kch = best;
-      }
+      if (g > 1) L.rtma_kch = rtma_tiles(C, tab, sblk[SUB_A], 0, rm);
       L.n_rtma = (int)rm.size();
       if ((st = L.rtma.upload(rm, s))) return st;
     }
@@ -994,9 +1124,12 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       L.small_items[q] = pre.back();
       if ((st = L.spre[q].upload(pre, s))) return st;
     }
+    L.htab = tab;
     for (int q = 0; q < 3; ++q) {
-      L.kch[q] = sweep_tiles(C, tab, sblk[q], sw[q]);
-      L.n_sweep[q] = (int)sw[q].size();
+      L.hblk[q] = sblk[q];
+      std::vector<int> sf;
+      L.n_sweep[q] = sweep_segments(C, tab, sblk[q], sw[q], sf, L.sched);
+      if ((st = L.sfirst[q].upload(sf, s))) return st;
       L.n_cells[q] = (int)ce[q].size();
       L.n_list[q] = (int)li[q].size();
       if ((st = L.sweep[q].upload(sw[q], s))) return st;
@@ -1091,6 +1224,14 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       V.n_bcax[a] = (int)tb.size();
       if ((st = V.t_bcax[a].upload(tb, s))) return st;
     }
+  V.fx_uvw = V.fx_p = nullptr;
+  V.nfx_uvw = V.nsfx_uvw = V.nfx_p = V.nsfx_p = 0;
+  if (nd == 1 && doms[0]->nfx_uvw + doms[0]->nfx_p > 0) {
+    const DomainStore &D = *doms[0];
+    V.fx_uvw = D.fx_uvw.p; V.nfx_uvw = D.nfx_uvw; V.nsfx_uvw = D.nsfx_uvw;
+    V.fx_p = D.fx_p.p; V.nfx_p = D.nfx_p; V.nsfx_p = D.nsfx_p;
+    if ((st = V.fx_stage.alloc((size_t)std::max<long long>(std::max(V.nsfx_uvw, V.nsfx_p), 1)))) return st;
+  }
   // per-domain solve state
   std::vector<int> ones(std::max(nd, 1), 1);
   if ((st = V.ds.alloc(std::max(nd, 1)))) return st;
@@ -1164,12 +1305,12 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bo
       if (skip_red)
         ;
       else if (fz)
-        launch(k_rbgs<T, true>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
+        launch(k_rbgs<T, true>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, L.sfirst[q].p, V.act.p, 0, V.err.p);
       else
-        launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 0, L.kch[q], V.err.p);
+        launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, L.sfirst[q].p, V.act.p, 0, V.err.p);
       prof_end(C, pk);
       prof_begin(C, pk, 3 * half);
-      launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, V.act.p, 1, L.kch[q], V.err.p);
+      launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, L.sfirst[q].p, V.act.p, 1, V.err.p);
       prof_end(C, pk);
       C->launches += skip_red ? 1 : 2;
     } else if (sch == 1) {
@@ -1197,17 +1338,8 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse out
   if (C->prm.mg_itrsch == 3 && C->prm.irestr > 0 && Cl.n_rtma && !C->prm.lsm) {
     // red-black from zero: the coarse interior phi is never read before it
-    // is written, so only its ghost shell is zeroed
-    static const bool attr_set = [] {
-      cudaFuncSetAttribute(k_restrict_tma<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           RsShape<double>::SMEM);
-      cudaFuncSetAttribute(k_restrict_tma<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           RsShape<float>::SMEM);
-      cudaFuncSetAttribute(k_restrict_tma<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           RsShape<float>::SMEM);
-      return true;
-    }();
-    (void)attr_set;
+    // is written, so only its ghost shell is zeroed (the kernel's shared
+    // memory limit is raised on the context's device in ctx_init)
     launch(k_restrict_tma<T, TC>, Cl.n_rtma, kTile, RsShape<T>::SMEM, C->stream, F.tab.p, Cl.tab.p, Cl.rtma.p, V.act.p,
                                                                               Cl.rtma_kch, V.err.p, 1);
     prof_end(C, pk);
@@ -1272,10 +1404,236 @@ static void vcycle(mf3d_ctx *C, View &V) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Autotuner.  Per level it picks, by timing the candidates on the view's own
+// arrays, (a) the schedule of the red-black half-sweep (sweep_segments: one
+// wave of equal plane runs across columns, two waves, or c / c+1 runs per
+// column), (b) for levels between 64 K and 4 M cells, the sweep kernel
+// (TMA-staged k_rbgs or the plain-load k_rbgs_small), (c) the planes per CTA
+// of the TMA restriction into the level, and (d) the CTAs per block of the
+// line and lexicographic relaxations.  Every candidate computes the same
+// values bit for bit - a half-sweep updates each cell from the other colour
+// alone, a restriction each coarse cell from its own children, a line or
+// lexicographic sweep keeps its recurrence order whatever the CTA split -
+// so the choice changes only the time.  Choices are cached for the process
+// by device, precision, smoother and the level's block shapes; a context
+// whose levels are all cached times nothing.  The server's lanes look the
+// cache up and keep the defaults on a miss.  MF3D_AUTOTUNE=0 turns it off.
+// ---------------------------------------------------------------------------
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tune;
+
+static bool autotune_enabled() {
+  const char *e = std::getenv("MF3D_AUTOTUNE");
+  return !(e && e[0] == '0');
+}
+static std::string tune_key(const mf3d_ctx *C, const ViewLevel &L, const char *what, int elem) {
+  std::string k = std::string(what) + "|dev" + std::to_string(C->device) + "|e" + std::to_string(elem) + "|s" +
+                  std::to_string(C->prm.mg_itrsch) + "|occ" + std::to_string(C->sweep_occ);
+  for (int b : L.hblk[SUB_A]) {
+    const BlkLev &B = L.htab[b];
+    k += "|" + std::to_string(B.nx) + "x" + std::to_string(B.ny) + "x" + std::to_string(B.nz);
+  }
+  return k;
+}
+static bool tune_get(const std::string &k, int &v) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(k);
+  if (it == g_tune.end()) return false;
+  v = it->second;
+  return true;
+}
+static void tune_put(const std::string &k, int v) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[k] = v;
+}
+// Mean device milliseconds of f() over 3 runs after one warm-up run; a
+// failed launch counts as infinitely slow.
+template <class Fn>
+static double tune_time(mf3d_ctx *C, Fn &&f) {
+  f();
+  if (cudaEventRecord(C->ev0, C->stream) != cudaSuccess) return 1e30;
+  for (int r = 0; r < 3; ++r) f();
+  if (cudaEventRecord(C->ev1, C->stream) != cudaSuccess || cudaEventSynchronize(C->ev1) != cudaSuccess) {
+    cudaGetLastError();
+    return 1e30;
+  }
+  if (cudaGetLastError() != cudaSuccess) return 1e30;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, C->ev0, C->ev1);
+  return ms / 3.0;
+}
+static int upload_sweeps(mf3d_ctx *C, ViewLevel &L, int sched, int only_q = -1) {
+  for (int q = 0; q < 3; ++q) {
+    if (only_q >= 0 && q != only_q) continue;
+    std::vector<RbSeg> sw;
+    std::vector<int> sf;
+    L.n_sweep[q] = sweep_segments(C, L.htab, L.hblk[q], sw, sf, sched);
+    int st;
+    if ((st = L.sweep[q].upload(sw, C->stream))) return st;
+    if ((st = L.sfirst[q].upload(sf, C->stream))) return st;
+  }
+  L.sched = sched;
+  return MF3D_OK;
+}
+// line relaxation shape for cl CTAs per block (as tdma_layout's)
+static void td_shape(ViewLevel &L, int cl) {
+  const size_t sz = L.td_fp64 ? 8 : 4, cap = 200 * 1024;
+  const int per = (L.td_numax + cl - 1) / cl;
+  L.td_gmax = (int)std::max<size_t>(1, std::min<size_t>(per, cap / ((7 * (size_t)L.td_nmax + 9) * sz)));
+  L.td_smem = (7 * (size_t)L.td_gmax * (L.td_nmax + 1) + 2 * (size_t)L.td_gmax) * sz;
+  L.td_cl = cl;
+}
+
+template <typename T>
+static int autotune_level(mf3d_ctx *C, View &V, int g, bool time_new) {
+  ViewLevel &L = V.lv[g];
+  if (!L.n_list[SUB_A]) return MF3D_OK;
+  cudaStream_t s = C->stream;
+  const int sch = C->prm.mg_itrsch;
+  int st;
+  const dim3 cta(RB_TX, RB_TY);
+  if (sch == 3 && !C->prm.lsm) {
+    // (a) sweep schedule, (b) sweep kernel
+    const std::string ks = tune_key(C, L, "sweep", sizeof(T));
+    int v;
+    if (tune_get(ks, v)) {
+      if ((st = upload_sweeps(C, L, v & 7))) return st;
+      if (g > 1) L.small = (v >> 3) & 1;
+    } else if (time_new) {
+      double best = 1e30;
+      int bs = 0;
+      for (int sc = 0; sc < kSweepSchedules; ++sc) {
+        if ((st = upload_sweeps(C, L, sc, SUB_A))) return st;
+        const double t = tune_time(C, [&] {
+          launch(k_rbgs<T, false>, dim3(L.n_sweep[SUB_A]), cta, 0, s, L.tab.p, L.sweep[SUB_A].p, L.sfirst[SUB_A].p,
+                 V.act.p, 0, V.err.p);
+        });
+        if (t < best) { best = t; bs = sc; }
+      }
+      if ((st = upload_sweeps(C, L, bs))) return st;
+      const long long cells = L.cells_sub[SUB_A];
+      if (g > 1 && cells >= (1LL << 16) && cells <= (1LL << 22)) {
+        const int g2 = grid_of(L.small_items[SUB_A], kTile);
+        const double ts = tune_time(C, [&] {
+          launch(k_rbgs_small<T, false>, g2, kTile, 0, s, L.tab.p, L.spre[SUB_A].p, L.list[SUB_A].p, L.n_list[SUB_A],
+                 V.act.p, 0);
+        });
+        L.small = ts < best ? 1 : 0;
+      }
+      tune_put(ks, bs | (L.small << 3));
+    }
+  }
+  if ((sch == 2 || sch == 1) && !C->prm.lsm) {
+    // (d) CTAs per block of the line / lexicographic relaxation: the
+    // default and the portable sizes below it
+    const std::string kl = tune_key(C, L, sch == 2 ? "tdma" : "lex", sizeof(T));
+    const int def = sch == 2 ? L.td_cl : L.lx_cl;
+    int v;
+    auto set_cl = [&](int cl) {
+      if (sch == 2) td_shape(L, cl);
+      else L.lx_cl = cl;
+    };
+    if (tune_get(kl, v)) {
+      if (v <= def) set_cl(v);
+    } else if (time_new && def > 1) {
+      double best = 1e30;
+      int bc = def;
+      for (int cl : {def, 8, 4}) {
+        if (cl > def || (cl != def && cl == 8 && def == 8)) continue;
+        set_cl(cl);
+        const double t = tune_time(C, [&] {
+          if (sch == 2)
+            launch_cl(k_tdma_lines<T>, L.n_list[SUB_A] * L.td_cl, TD_THREADS, L.td_smem, s, L.td_cl, L.tab.p,
+                      L.list[SUB_A].p, V.act.p, L.td_cl, L.td_gmax, L.td_nmax);
+          else
+            launch_cl(k_lexgs<T>, L.n_list[SUB_A] * L.lx_cl, 1024, 0, s, L.lx_cl, L.tab.p, L.list[SUB_A].p, V.act.p,
+                      L.lx_cl);
+        });
+        if (t < best) { best = t; bc = cl; }
+      }
+      set_cl(bc);
+      tune_put(kl, bc);
+    }
+  }
+  return MF3D_OK;
+}
+
+// (c) planes per CTA of the TMA restriction into level g (from g-1).
+static int autotune_restrict(mf3d_ctx *C, View &V, int g, bool time_new) {
+  ViewLevel &L = V.lv[g];
+  if (!(C->prm.mg_itrsch == 3 && C->prm.irestr > 0 && g > 1 && L.n_rtma && !C->prm.lsm)) return MF3D_OK;
+  const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
+  const bool f64 = C->elem == 8 || g - 1 >= Lc, c64 = C->elem == 8 || g >= Lc;
+  const std::string kr = tune_key(C, L, "restrict", (f64 ? 80 : 40) + (c64 ? 8 : 4));
+  auto set_kch = [&](int kch) {
+    std::vector<Tile> rm;
+    L.rtma_kch = rtma_tiles(C, L.htab, L.hblk[SUB_A], kch, rm);
+    L.n_rtma = (int)rm.size();
+    return L.rtma.upload(rm, C->stream);
+  };
+  int v, st;
+  if (tune_get(kr, v)) return set_kch(v);
+  if (!time_new) return MF3D_OK;
+  double best = 1e30;
+  int bk = L.rtma_kch;
+  for (int kch : {2, 4, 8, 16}) {
+    if ((st = set_kch(kch))) return st;
+    const double t = tune_time(C, [&] {
+      if (f64) restr<double, double>(C, V, g - 1);
+      else if (c64) restr<float, double>(C, V, g - 1);
+      else restr<float, float>(C, V, g - 1);
+    });
+    if (t < best) { best = t; bk = kch; }
+  }
+  if ((st = set_kch(bk))) return st;
+  tune_put(kr, bk);
+  return MF3D_OK;
+}
+
+// Tunes (or looks up) every level of the view; time_new = false only looks
+// the cache up.  The arrays are scratch at this point (the solve writes every
+// value it reads), and the level-1 ghost shell, which must hold zeros, is
+// never written by a sweep or a restriction into level 2.
+static int autotune_view(mf3d_ctx *C, View &V, bool time_new) {
+  if (!autotune_enabled()) return MF3D_OK;
+  if (C->prm.mg_itrsch == 2 && C->prm.lsm) return MF3D_OK;
+  const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
+  int st;
+  for (int g = 1; g <= V.Lmax; ++g) {
+    const bool fp64 = C->elem == 8 || g >= Lc;
+    if ((st = fp64 ? autotune_level<double>(C, V, g, time_new) : autotune_level<float>(C, V, g, time_new))) return st;
+    if ((st = autotune_restrict(C, V, g, time_new))) return st;
+  }
+  CK(cudaStreamSynchronize(C->stream));
+  CK(cudaMemsetAsync(V.err.p, 0, sizeof(int), C->stream));
+  CK(cudaStreamSynchronize(C->stream));
+  return MF3D_OK;
+}
+
+// A field exchange copy map (k_fx_stage + k_fx_apply); returns the launches.
+static int field_exchange(mf3d_ctx *C, View &V, const FxCopy *pairs, long long n, long long nstaged,
+                          const int *only) {
+  if (!n) return 0;
+  if (nstaged)
+    launch(k_fx_stage, grid_of(nstaged, kTile), kTile, 0, C->stream, V.df.p, pairs, nstaged, only, V.fx_stage.p);
+  launch(k_fx_apply, grid_of(n, kTile), kTile, 0, C->stream, V.df.p, pairs, n, nstaged, only, V.fx_stage.p);
+  return nstaged ? 2 : 1;
+}
+
 // Fused calvel + calmas over the view (the TMA-staged kernel when the bound
 // fields admit it).
 template <typename T>
 static void calvel_calmas(mf3d_ctx *C, View &V, const int *act, unsigned long long *slot, int write_su) {
+  if (C->prm.differencing == 2) {
+    // the 4th-order divergence reads two face layers past the cell: calvel,
+    // its exchange(1..3) and calmas in the reference's order
+    launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, C->stream, V.df.p, V.t_int.p, V.ds.p, act);
+    launch(k_vel_faces, V.n_vfaces, kTile, 0, C->stream, V.df.p, V.t_vfaces.p, act, C->prm.pl_ex);
+    launch(k_calmas4<T>, V.n_int, dim3(RW_TX, RW_RJ), 0, C->stream, V.df.p, V.t_int.p, V.ds.p, act, slot, write_su);
+    C->launches += 2;
+    return;
+  }
   if (C->prm.lsm) {
     launch(k_calvel_calmas_lsm, V.n_zint, dim3(OZ_TX, OZ_RJ), 0, C->stream, V.df.p, V.t_zint.p, V.ds.p, act, slot,
            write_su);
@@ -1305,7 +1663,10 @@ static void iteration_body(mf3d_ctx *C, View &V, int loop_graph) {
   cudaStream_t s = C->stream;
   vcycle<T>(C, V);
   launch(k_add_correction<T>, V.n_pairs, kTile, 0, s, V.df.p, V.t_pairs.p, V.act.p, V.pairs_kch);
-  launch(k_p_faces, V.n_faces, kTile, 0, s, V.df.p, V.t_faces.p, V.act.p);
+  // exchange(4) + pbound: the whole copy map where the view has one (every
+  // ghost the reference writes), else the face ghosts that calvel reads
+  if (V.nfx_p) C->launches += field_exchange(C, V, V.fx_p, V.nfx_p, V.nsfx_p, V.act.p) - 1;
+  else launch(k_p_faces, V.n_faces, kTile, 0, s, V.df.p, V.t_faces.p, V.act.p);
   prof_begin(C, MF3D_PROF_CALMAS, (double)V.n_l1 * (4 * sizeof(double) + sizeof(T)));  // p, u*, v*, w* in; su out
   calvel_calmas<T>(C, V, V.act.p, V.rmax.p, 0);
   prof_end(C, MF3D_PROF_CALMAS);
@@ -1483,6 +1844,8 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
     if (C->prm.mg_itrsch == 2) tdma_factors(C, V);
   }
   launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p, C->walls_given ? 1 : 0);
+  // the 4th-order calmas reads ghost faces of u, v, w from the first pass on
+  if (C->wait_side && C->prm.differencing == 2) CK(cudaStreamWaitEvent(s, C->ev_side, 0));
   calvel_calmas<T>(C, V, V.ones.p, V.rmax.p, 0);
   launch(k_dom_init, 1, 256, 0, s, V.ds.p, nd, V.rmax.p, V.act.p);
   C->launches += 3;
@@ -1539,18 +1902,21 @@ static int solve_end(mf3d_ctx *C, View &V) {
   if (C->wait_side) CK(cudaStreamWaitEvent(s, C->ev_side, 0));  // the host entry's u, v, w
   launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, nullptr);
   C->launches += 1;
-  if (C->prm.bounds) {
-    // exchange(1..3) of the final calvel with full periodic planes, then
-    // boundu/boundv/boundw (newsolv_mg.for:86-88)
-    bc_walks(C, V);
+  // exchange(1..3) of the final calvel (press.for:196-198): the copy map of
+  // every ghost it writes where the view has one; else the full periodic
+  // planes (bounds mode) and the face ghosts
+  if (V.nfx_uvw) {
+    C->launches += field_exchange(C, V, V.fx_uvw, V.nfx_uvw, V.nsfx_uvw, nullptr);
+  } else {
+    if (C->prm.bounds) bc_walks(C, V);
     launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
     ++C->launches;
+  }
+  if (C->prm.bounds) {
+    // boundu/boundv/boundw (newsolv_mg.for:86-88)
     bc_walks(C, V);
     bound_faces(C, V, C->prm.alfabc);
-    return MF3D_OK;
   }
-  launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
-  ++C->launches;
   return MF3D_OK;
 }
 
@@ -1670,27 +2036,39 @@ static int mgkcyc_view(mf3d_ctx *C, View &V, double *const *su, double *const *p
 // ---------------------------------------------------------------------------
 static __device__ __align__(256) double *g_noalloc_ptrs[2 * MF3D_NOALLOC_MAX_BLOCKS];
 
-// Device address of g_noalloc_ptrs on `device` (looked up once per device,
-// with that device current).
-static int noalloc_tables(int device, double ***out) {
-  constexpr int kMaxDevices = 64;
-  static std::mutex mu;
-  static void *addr[kMaxDevices] = {};
-  if (device < 0 || device >= kMaxDevices) {
-    set_error("mf3d_mgkcyc_device_noalloc: device ordinal out of range");
-    return MF3D_E_INVALID;
+// Device address of g_noalloc_ptrs in the current device's context, looked
+// up when a context is created (ctx_init), with its device current.  The
+// address is kept in the context, so a context created after a device reset
+// (which reloads the module, possibly elsewhere) holds the new address.
+static int noalloc_tables(void **out) {
+  void *a = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_ptrs);
+  if (e != cudaSuccess || !a) {
+    set_error(std::string("mf3d_mgkcyc_device_noalloc set-up: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return MF3D_E_CUDA;
   }
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[device]) {
-    void *a = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_ptrs);
-    if (e != cudaSuccess || !a) {
-      set_error(std::string("mf3d_mgkcyc_device_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      return MF3D_E_CUDA;
-    }
-    addr[device] = a;
-  }
-  *out = (double **)addr[device];
+  *out = a;
+  return MF3D_OK;
+}
+
+// Loads every kernel a V-cycle call can launch (cudaFuncGetAttributes forces
+// a lazily loaded module function in), so that no later call - in particular
+// mf3d_mgkcyc_device_noalloc - makes the driver load code on first use.
+template <typename T>
+static int preload_vcycle_kernels() {
+  cudaFuncAttributes fa;
+  const void *k[] = {
+      (const void *)k_rbgs<T, true>, (const void *)k_rbgs<T, false>, (const void *)k_rbgs_small<T, true>,
+      (const void *)k_rbgs_small<T, false>, (const void *)k_rbgs_small<double, true>,
+      (const void *)k_rbgs_small<double, false>, (const void *)k_rbgs<double, true>,
+      (const void *)k_rbgs<double, false>, (const void *)k_lexgs<T>, (const void *)k_lexgs<double>,
+      (const void *)k_tdma_factor<T>, (const void *)k_tdma_factor<double>, (const void *)k_tdma_lines<T>,
+      (const void *)k_tdma_lines<double>, (const void *)k_restrict<T, T>, (const void *)k_restrict<T, double>,
+      (const void *)k_restrict_tma<T, T>, (const void *)k_restrict_tma<T, double>, (const void *)k_prolong<T, T>,
+      (const void *)k_prolong<T, double>, (const void *)k_halo_stage<T>, (const void *)k_halo_apply<T>,
+      (const void *)k_halo_stage<double>, (const void *)k_halo_apply<double>, (const void *)k_zero_ghosts<T>,
+      (const void *)k_load_rhs<T>, (const void *)k_store_pp<T>};
+  for (const void *f : k) CK(cudaFuncGetAttributes(&fa, f));
   return MF3D_OK;
 }
 
@@ -1703,8 +2081,7 @@ static int mgkcyc_view_noalloc(mf3d_ctx *C, View &V, double *const *su, double *
               std::to_string(MF3D_NOALLOC_MAX_BLOCKS) + ")");
     return MF3D_E_INVALID;
   }
-  double **tab = nullptr;
-  if (int st = noalloc_tables(C->device, &tab)) return st;
+  double **tab = (double **)C->noalloc_tab;
   C->launches = 0;
   CK(cudaMemcpyAsync(tab, su, nb * sizeof(double *), cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(tab + nb, pp, nb * sizeof(double *), cudaMemcpyHostToDevice, s));
@@ -1733,10 +2110,14 @@ static int check_params(const mf3d_params *prm) {
   if (prm->irestr < 0 || prm->iproln < 0 || prm->maxcy < 0) { set_error("negative sweep/cycle count"); return MF3D_E_INVALID; }
   if (prm->pl < 1) { set_error("pl must be >= 1"); return MF3D_E_INVALID; }
   if (prm->pl_ex < 0 || prm->pl_ex >= prm->pl) { set_error("pl_ex must satisfy 0 <= pl_ex < pl"); return MF3D_E_INVALID; }
-  // calmas takes its 2nd-order branch for every differencing but 2 (press.for:
-  // 13-35 is the 4th-order one); 3 (WENO convection) is the one L_LSM needs
-  if (prm->differencing == 2) { set_error("differencing = 2 (4th-order calmas) is not supported"); return MF3D_E_UNSUPPORTED; }
-  if (prm->differencing != 1 && prm->differencing != 3) { set_error("differencing must be 1, 2 or 3"); return MF3D_E_INVALID; }
+  // calmas takes its 4th-order branch for differencing 2 (press.for:13-35)
+  // and the 2nd-order one otherwise; 3 (WENO convection) is the one L_LSM needs
+  if (prm->differencing < 1 || prm->differencing > 3) { set_error("differencing must be 1, 2 or 3"); return MF3D_E_INVALID; }
+  if (prm->differencing == 2 && prm->pl < 2) {
+    set_error("differencing = 2: the 4th-order divergence reads u(i-2), which needs pl >= 2");
+    return MF3D_E_INVALID;
+  }
+  if (prm->differencing == 2 && prm->lsm) { set_error("differencing = 2 with lsm (L_LSM needs WENO, 3)"); return MF3D_E_INVALID; }
   if (prm->precision < 0 || prm->precision > 1) { set_error("precision mode not supported"); return MF3D_E_UNSUPPORTED; }
   if (prm->lsm && prm->precision != MF3D_PREC_FP64) { set_error("lsm runs in FP64 only"); return MF3D_E_UNSUPPORTED; }
   if (prm->solver != 0 && prm->solver != 1 && prm->solver != 2) { set_error("solver must be 1 or 2"); return MF3D_E_INVALID; }
@@ -1772,14 +2153,25 @@ static int ctx_init(mf3d_ctx *C, const mf3d_params *prm, bool nonblocking = fals
   if (C->elem == 8) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rbgs<double, false>, RB_TX * RB_TY, 0));
   else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_rbgs<float, false>, RB_TX * RB_TY, 0));
   C->sweep_occ = std::max(occ, 1);
-  return MF3D_OK;
+  // Per-device kernel attributes: every context sets them on its own device
+  // (an attribute set on one device does not carry to another).
+  CK(cudaFuncSetAttribute(k_restrict_tma<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          RsShape<double>::SMEM));
+  CK(cudaFuncSetAttribute(k_restrict_tma<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          RsShape<float>::SMEM));
+  CK(cudaFuncSetAttribute(k_restrict_tma<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          RsShape<float>::SMEM));
+  if (int st = C->elem == 8 ? preload_vcycle_kernels<double>() : preload_vcycle_kernels<float>()) return st;
+  return noalloc_tables(&C->noalloc_tab);
 }
 
 static int make_view(mf3d_ctx *C) {
   std::vector<DomainStore *> doms;
   for (auto &d : C->doms) doms.push_back(d.get());
   C->view.reset(new View());
-  return build_view(C, *C->view, doms, std::max(C->prm.maxcy, 1));
+  int st = build_view(C, *C->view, doms, std::max(C->prm.maxcy, 1));
+  if (st) return st;
+  return autotune_view(C, *C->view, true);
 }
 
 static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, mf3d_ctx **out) {
@@ -1816,6 +2208,10 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
       set_error("lsm: uniform spacing only (the reference's variable-density branch)");
       return MF3D_E_UNSUPPORTED;
     }
+    if (prm->differencing == 2 && (d.hx || d.hy || d.hz)) {
+      set_error("differencing = 2: uniform spacing only (the reference's 4th-order divergence)");
+      return MF3D_E_UNSUPPORTED;
+    }
   }
   {
     std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
@@ -1828,7 +2224,7 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   C->doms.emplace_back(new DomainStore());
   C->coarse64 = C->elem == 4 && prm->ngrid > 1;
   if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, C->coarse64 ? 8 : C->elem, prm->pl,
-                         C->stream, prm->lsm != 0, prm->bounds != 0)))
+                         C->stream, prm->lsm != 0, prm->bounds != 0, prm->pl_ex)))
     return st;
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
@@ -1900,6 +2296,10 @@ static int batch_create(const mf3d_domain_desc *doms, int nd, const mf3d_params 
     if (!edges_exceed(doms[d], prm->pl_ex)) {
       set_error("domain " + std::to_string(d) + ": an edge does not exceed pl_ex");
       return MF3D_E_INVALID;
+    }
+    if (prm->differencing == 2 && (doms[d].hx || doms[d].hy || doms[d].hz)) {
+      set_error("differencing = 2: uniform spacing only (the reference's 4th-order divergence)");
+      return MF3D_E_UNSUPPORTED;
     }
   }
   auto C = std::make_unique<mf3d_ctx>();
@@ -2150,6 +2550,20 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
       set_error("mf3d_rk_fields: a pointer is NULL");
       return MF3D_E_INVALID;
     }
+  }
+  // Every entry is valid: bind the caller's buffers for this call only; the
+  // guard unbinds them on every way out, so no later upload of the field
+  // table carries a pointer the caller may have freed.
+  struct Unbind {
+    View &V;
+    ~Unbind() {
+      for (auto &F : V.hf) {
+        F.oo[0] = F.oo[1] = F.oo[2] = nullptr;
+        F.vis = nullptr;
+      }
+    }
+  } unbind{V};
+  for (size_t b = 0; b < V.blk.size(); ++b) {
     for (int a = 0; a < 3; ++a) V.hf[b].oo[a] = a == 0 ? rk[b].uoo : a == 1 ? rk[b].voo : rk[b].woo;
     V.hf[b].vis = rk[b].vis;
   }
@@ -2170,10 +2584,6 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
     ++C->launches;
   }
   const cudaError_t e = cudaStreamSynchronize(s);
-  for (auto &F : V.hf) {  // the caller's buffers are bound for this call only
-    F.oo[0] = F.oo[1] = F.oo[2] = nullptr;
-    F.vis = nullptr;
-  }
   if (e != cudaSuccess) { set_error(std::string("mf3d_rungek_2nd_device: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
   return MF3D_OK;
 }
@@ -2197,9 +2607,15 @@ int mf3d_calvel_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double
   CK(cudaMemcpyAsync(V.ds.p, &d0, sizeof d0, cudaMemcpyHostToDevice, s));
   launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, nullptr);
   ++C->launches;
-  if (C->prm.bounds) bc_walks(C, V);  // the full periodic planes of exchange(1..3)
-  launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
-  ++C->launches;
+  // exchange(1..3) (press.for:196-198): every ghost it writes, edges and
+  // corners included, which the next predictor stage reads
+  if (V.nfx_uvw) {
+    C->launches += field_exchange(C, V, V.fx_uvw, V.nfx_uvw, V.nsfx_uvw, nullptr);
+  } else {
+    if (C->prm.bounds) bc_walks(C, V);  // the full periodic planes of exchange(1..3)
+    launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
+    ++C->launches;
+  }
   const cudaError_t e = cudaStreamSynchronize(s);  // d0 is a local
   if (e != cudaSuccess) { set_error(std::string("mf3d_calvel_device: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
   return MF3D_OK;
@@ -2242,6 +2658,19 @@ int mf3d_mgkcyc_device_noalloc(mf3d_ctx *C, double *const *su, double *const *pp
 }
 
 long long mf3d_last_launch_count(const mf3d_ctx *C) { return C ? C->launches : 0; }
+
+int mf3d_test_fail_alloc(long long after) {
+  mf3d::g_fail_alloc_countdown.store(after < 0 ? -1 : after);
+  return MF3D_OK;
+}
+
+int mf3d_test_stall_copy(int device, int bytes) {
+  if (bytes < 0 || bytes > 65536) { mf3d::set_error("mf3d_test_stall_copy: bytes out of range"); return MF3D_E_INVALID; }
+  if (cudaSetDevice(device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  const cudaError_t e = cudaMemcpyToSymbol(mf3d::g_test_extra_tx, &bytes, sizeof(int));
+  if (e != cudaSuccess) { mf3d::set_error(std::string("mf3d_test_stall_copy: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
+  return MF3D_OK;
+}
 
 int mf3d_profile(mf3d_ctx *C, int kind) {
   if (!C || kind < 0 || kind > MF3D_PROF_PROLONG_L1) { mf3d::set_error("mf3d_profile: bad arguments"); return MF3D_E_INVALID; }
@@ -2291,6 +2720,23 @@ long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid, i
     acc += geom[q].cells();
   }
   auto pairs = mf3d::build_halo_map(b, geom, base);
+  if (dst && src)
+    for (size_t q = 0; q < pairs.size(); ++q) { dst[q] = pairs[q].dst; src[q] = pairs[q].src; }
+  return (long long)pairs.size();
+}
+
+long long mf3d_field_exchange_map(const mf3d_block_desc *blocks, int nblocks, int pl, int pl_ex, int op,
+                                  long long *dst, long long *src) {
+  if (!blocks || nblocks <= 0 || pl < 1 || pl_ex < 0 || pl_ex >= pl || op < 1 || op > 4) return -1;
+  std::vector<mf3d_block_desc> b(blocks, blocks + nblocks);
+  std::vector<long long> base(nblocks);
+  long long acc = 0;
+  for (int q = 0; q < nblocks; ++q) {
+    if (b[q].nx <= pl_ex || b[q].ny <= pl_ex || b[q].nz <= pl_ex) return -1;
+    base[q] = acc;
+    acc += (long long)(b[q].nx + 2 * pl) * (b[q].ny + 2 * pl) * (b[q].nz + 2 * pl);
+  }
+  auto pairs = mf3d::build_field_map(b, base, pl, op, op == 4 ? 0 : pl_ex, op == 4);
   if (dst && src)
     for (size_t q = 0; q < pairs.size(); ++q) { dst[q] = pairs[q].dst; src[q] = pairs[q].src; }
   return (long long)pairs.size();

@@ -35,6 +35,15 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
                                      const std::vector<LevelGeom> &geom,
                                      const std::vector<long long> &base);
 
+// exchange(op) on field arrays (exchange.for:2-23: exchange_bc on the
+// periodic faces, then exchange_smlvl with its corners, edges and faces),
+// and pbound after it when `with_pbound` (press.for:77-137), as pairs
+// dst <- src against the state before the exchange.  op 1, 2, 3: u, v, w
+// (their index ranges), 4: p; nly: the layers exchanged (pl_ex, 0 for p).
+// Cell id = base[b] + (i-1) + ti*((j-1) + tj*(k-1)), 1-based field indices.
+std::vector<HaloPair> build_field_map(const std::vector<mf3d_block_desc> &blocks, const std::vector<long long> &base,
+                                      int pl, int op, int nly, bool with_pbound);
+
 // Neighbour search of alloc_dom.for:456-1150 over block extents.
 int build_topology(int nblocks, const double *ext, const int *bc6, double dx,
                    double dy, double dz, mf3d_block_desc *out);

@@ -244,6 +244,42 @@ __global__ void k_vel_faces(const BlkFld *__restrict__ fl, const Tile *__restric
   F.w[g] = S.w[s];
 }
 
+// exchange(op) on the fields as a copy map (the host replays exchange_bc,
+// exchange_smlvl's corners, edges and faces, and pbound for the pressure, on
+// cell tokens: exchange.for:2-23, 343-2498; exchange_bc.for:2-841; press.for:
+// 77-137).  Each pair sets a ghost cell of component comp (0 u, 1 v, 2 w, 3 p)
+// of block dblk from the pre-exchange value of cell soff of block sblk.
+// Pairs whose source is itself written come first; k_fx_stage reads their
+// sources, then k_fx_apply writes every pair.  `only` (may be null) as in
+// k_calvel.
+struct FxCopy {
+  unsigned doff, soff;
+  unsigned short dblk, sblk;
+  int comp;
+};
+__device__ __forceinline__ double *fx_field(const BlkFld &F, int comp) {
+  return comp == 0 ? F.u : comp == 1 ? F.v : comp == 2 ? F.w : F.p;
+}
+__global__ void k_fx_stage(const BlkFld *__restrict__ fl, const FxCopy *__restrict__ c, long long nstaged,
+                           const int *__restrict__ only, double *__restrict__ buf) {
+  pdl_wait();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nstaged) return;
+  const FxCopy x = c[t];
+  if (only && !only[fl[x.dblk].dom]) return;
+  buf[t] = fx_field(fl[x.sblk], x.comp)[x.soff];
+}
+__global__ void k_fx_apply(const BlkFld *__restrict__ fl, const FxCopy *__restrict__ c, long long n,
+                           long long nstaged, const int *__restrict__ only, const double *__restrict__ buf) {
+  pdl_wait();
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const FxCopy x = c[t];
+  if (only && !only[fl[x.dblk].dom]) return;
+  const double v = t < nstaged ? buf[t] : fx_field(fl[x.sblk], x.comp)[x.soff];
+  fx_field(fl[x.dblk], x.comp)[x.doff] = v;
+}
+
 // Face planes used by the fused calvel/calmas kernel, filled once per solve:
 // lo[a] = the velocity component normal to the block's low face on that face
 // when it is a wall (the caller's boundary value, never rewritten by calvel),
@@ -843,6 +879,63 @@ __global__ void __launch_bounds__(RW_TX *RW_RJ) k_calvel(const BlkFld *__restric
     if (!(i == nx && F.wall[1])) F.u[c] = (F.ustar[c] - xdiv(dta * (p[c + 1] - p[c]), F.df[0][i], F.pinv[0]));
     if (!(j == ny && F.wall[3])) F.v[c] = (F.vstar[c] - xdiv(dta * (p[c + sy] - p[c]), F.df[1][j], F.pinv[1]));
     if (!(k == F.nz && F.wall[5])) F.w[c] = (F.wstar[c] - xdiv(dta * (p[c + sz] - p[c]), F.df[2][k], F.pinv[2]));
+  }
+}
+
+// calmas, 4th-order branch (press.for:13-35, differencing = 2), on the
+// velocities that calvel and exchange(1..3) left in u, v, w (k_calvel +
+// k_vel_faces, the reference's order):
+//   fact = (-u(i+1)+27.0*u(i)-27.0*u(i-1)+u(i-2))/(24.0*dx) + (the same in
+//          v along j)/(24.0*dy) + (the same in w along k)/(24.0*dz),
+// each numerator summed left to right; su = fact/dt into the level-1 rhs
+// (and F.su when asked), rmax = max |((fact*dx)*dy)*dz| as in k_calvel_calmas.
+// u(i+1) at i = nx and u(i-2) at i = 1 are ghost faces: the neighbour's
+// values for the exchanged layers, else whatever the caller's arrays hold,
+// as in the reference.  Uniform spacing (h[a][1] is the block's dx, dy, dz).
+template <typename T>
+__global__ void __launch_bounds__(RW_TX *RW_RJ) k_calmas4(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                                                          const DomState *__restrict__ ds, const int *__restrict__ act,
+                                                          unsigned long long *__restrict__ rmax_slot, int write_su) {
+  pdl_wait();
+  __shared__ double red[RW_RJ];
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  if (!act[F.dom]) return;
+  const double dt = ds[F.dom].dt, dtinv = ds[F.dom].dtinv;
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  const bool in = i <= F.nx && j <= F.ny;
+  const double dx = F.h[0][1], dy = F.h[1][1], dz = F.h[2][1];
+  const double d24x = 24.0 * dx, d24y = 24.0 * dy, d24z = 24.0 * dz;
+  const long long sy = F.ti, sz = (long long)F.ti * F.tj;
+  const double *__restrict__ U = F.u;
+  const double *__restrict__ Vv = F.v;
+  const double *__restrict__ Wv = F.w;
+  T *__restrict__ rhs1 = rhs_of<T>(F.L1);
+  double *__restrict__ SU = write_su ? F.su : nullptr;
+  double vmax = 0.0;
+  if (in) {
+    const int k1 = min(t.k0 + RW_KCH - 1, F.nz);
+    for (int k = t.k0; k <= k1; ++k) {
+      const long long c = fidx(F, i, j, k);
+      const double fx = ((((-U[c + 1]) + 27.0 * U[c]) - 27.0 * U[c - 1]) + U[c - 2]) / d24x;
+      const double fy = ((((-Vv[c + sy]) + 27.0 * Vv[c]) - 27.0 * Vv[c - sy]) + Vv[c - 2 * sy]) / d24y;
+      const double fz = ((((-Wv[c + sz]) + 27.0 * Wv[c]) - 27.0 * Wv[c - sz]) + Wv[c - 2 * sz]) / d24z;
+      const double fact = (fx + fy) + fz;
+      const double su = xdiv(fact, dt, dtinv);
+      rhs1[cell_off(F.L1, i, j, k)] = (T)su;
+      if (SU) SU[c] = su;
+      double f1 = fabs(fact * dx * dy * dz);
+      if (!(f1 == f1)) f1 = __longlong_as_double(0x7ff0000000000000LL);  // NaN -> +Inf (flagged)
+      vmax = vmax > f1 ? vmax : f1;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+  if (threadIdx.x == 0) red[threadIdx.y] = vmax;
+  __syncthreads();
+  if (threadIdx.y == 0) {
+    double v = threadIdx.x < RW_RJ ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0 && v > 0.0) atomic_max_nonneg(rmax_slot + F.dom, v);
   }
 }
 

@@ -128,6 +128,9 @@ static int srv_rebuild(mf3d_ctx *C, View &V, std::vector<SrvReq *> &res) {
   }
   int st;
   if ((st = build_view(C, V, doms, 1))) return st;
+  // tuned schedules of levels seen before; a miss keeps the defaults (no
+  // timing inside a serving cycle)
+  if ((st = autotune_view(C, V, false))) return st;
   std::vector<DomState> hs(nd);
   std::vector<int> fresh(nd, 0);
   for (int d = 0; d < nd; ++d) {
@@ -479,6 +482,10 @@ int mf3d_server_submit(mf3d_server *S, const mf3d_domain_desc *dom, const mf3d_f
   if (!edges_exceed(*dom, S->C[0]->prm.pl_ex)) {
     set_error("mf3d_server_submit: an edge does not exceed pl_ex");
     return MF3D_E_INVALID;
+  }
+  if (S->C[0]->prm.differencing == 2 && (dom->hx || dom->hy || dom->hz)) {
+    set_error("mf3d_server_submit: differencing = 2 needs uniform spacing");
+    return MF3D_E_UNSUPPORTED;
   }
   auto r = std::make_unique<SrvReq>();
   r->desc = *dom;

@@ -415,6 +415,292 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
   return out;
 }
 
+// ---------------------------------------------------------------------------
+// Field exchange copy map.  exchange(op) (exchange.for:2-23) is exchange_bc
+// on the periodic faces (exchange_bc.for:2-841) followed by exchange_smlvl
+// (exchange.for:343-2498); for the pressure pbound follows (press.for:
+// 77-137).  The sequence is replayed on tokens over the blocks' ttc arrays:
+// a written cell remembers the id of the cell whose pre-exchange value it
+// now holds.  Cells are numbered base[b] + (i-1) + ti*((j-1) + tj*(k-1))
+// with 1-based field indices i = 1..ti.  Only written cells are stored.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct FieldTokens {
+  const std::vector<mf3d_block_desc> &blk;
+  const std::vector<long long> &base;
+  int pl;
+  std::vector<int> ti, tj, tk;
+  std::unordered_map<int, int> pos;
+  // Only ghost cells are written, so tokens are kept for the ghost region
+  // of each block alone (pl-thick shell): z slabs, then per interior plane
+  // the y rows, then per interior row the x ends.
+  std::vector<std::vector<long long>> shell;
+  FieldTokens(const std::vector<mf3d_block_desc> &b, const std::vector<long long> &bs, int pl_)
+      : blk(b), base(bs), pl(pl_) {
+    shell.resize(b.size());
+    for (size_t q = 0; q < b.size(); ++q) {
+      pos[b[q].id] = (int)q;
+      ti.push_back(b[q].nx + 2 * pl);
+      tj.push_back(b[q].ny + 2 * pl);
+      tk.push_back(b[q].nz + 2 * pl);
+      const long long W = ti[q], H = tj[q];
+      shell[q].assign((size_t)(2 * pl * W * H + (long long)b[q].nz * (2 * pl * W + (long long)b[q].ny * 2 * pl)), -1);
+    }
+  }
+  long long id(int p, int i, int j, int k) const {
+    return base[p] + (i - 1) + (long long)ti[p] * ((j - 1) + (long long)tj[p] * (k - 1));
+  }
+  // index of a ghost cell in the shell, -1 for an interior cell
+  long long sidx(int p, int i, int j, int k) const {
+    const long long W = ti[p], H = tj[p];
+    const int nx = ti[p] - 2 * pl, ny = tj[p] - 2 * pl, nz = tk[p] - 2 * pl;
+    if (k <= pl) return ((long long)(k - 1) * H + (j - 1)) * W + (i - 1);
+    if (k > nz + pl) return (pl * H + (long long)(k - nz - pl - 1) * H + (j - 1)) * W + (i - 1);
+    long long o = 2 * pl * W * H + (long long)(k - pl - 1) * (2 * pl * W + (long long)ny * 2 * pl);
+    if (j <= pl) return o + (long long)(j - 1) * W + (i - 1);
+    if (j > ny + pl) return o + (long long)(pl + j - ny - pl - 1) * W + (i - 1);
+    o += 2 * pl * W + (long long)(j - pl - 1) * 2 * pl;
+    if (i <= pl) return o + (i - 1);
+    if (i > nx + pl) return o + pl + (i - nx - pl - 1);
+    return -1;
+  }
+  long long get(int p, int i, int j, int k) const {
+    const long long s = sidx(p, i, j, k);
+    if (s < 0) return id(p, i, j, k);
+    const long long v = shell[p][(size_t)s];
+    return v < 0 ? id(p, i, j, k) : v;
+  }
+  void set(int p, int i, int j, int k, long long v) {
+    const long long s = sidx(p, i, j, k);
+    if (s >= 0) shell[p][(size_t)s] = v;  // destinations are ghost cells
+  }
+  int P(int block_id) const {
+    auto it = pos.find(block_id);
+    return it == pos.end() ? -1 : it->second;
+  }
+};
+
+// A field cell (block position, 1-based i, j, k).
+struct FCell {
+  int p, i, j, k;
+};
+// cell of block p at index a along axis ax and (s, t) along the others
+FCell axis_cell(int p, int ax, int a, int s, int t) {
+  if (ax == 0) return {p, a, s, t};
+  if (ax == 1) return {p, s, a, t};
+  return {p, s, t, a};
+}
+
+// Index ranges of the field: the pressure range spr..epr of every axis, and
+// the field's own range lo..hi (velocities stop one face short of a high
+// wall, localparameters.for:185-190).
+struct FieldRange {
+  int spr[3], epr[3], lo[3], hi[3], n[3];
+};
+FieldRange field_range(const mf3d_block_desc &d, int pl, int op) {
+  FieldRange r;
+  const int nn[3] = {d.nx, d.ny, d.nz};
+  const int nbrn[3] = {d.inext, d.jnext, d.knext}, bcn[3] = {d.bc_east, d.bc_north, d.bc_top};
+  for (int a = 0; a < 3; ++a) {
+    r.n[a] = nn[a] + 2 * pl;
+    r.spr[a] = pl + 1;
+    r.epr[a] = nn[a] + pl;
+    r.lo[a] = r.spr[a];
+    r.hi[a] = r.epr[a];
+    if (op == a + 1 && nbrn[a] < 0 && bcn[a] != MF3D_BC_PERIODIC) r.hi[a] -= 1;
+  }
+  return r;
+}
+
+// Directions of the corner and edge neighbours (x, y, z; 0 = the axis an
+// edge runs along), in mf3d_block_desc's corprev/cornext/edgprev/edgnext order.
+constexpr int kCP[4][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1}};
+constexpr int kCN[4][3] = {{1, 1, 1}, {1, -1, 1}, {-1, -1, 1}, {-1, 1, 1}};
+constexpr int kEP[6][3] = {{-1, 0, -1}, {0, 1, -1}, {1, 0, -1}, {0, -1, -1}, {-1, -1, 0}, {-1, 1, 0}};
+constexpr int kEN[6][3] = {{1, 0, 1}, {0, -1, 1}, {-1, 0, 1}, {0, 1, 1}, {1, 1, 0}, {1, -1, 0}};
+
+}  // namespace
+
+std::vector<HaloPair> build_field_map(const std::vector<mf3d_block_desc> &blocks, const std::vector<long long> &base,
+                                      int pl, int op, int nly, bool with_pbound) {
+  FieldTokens T(blocks, base, pl);
+  const int nb = (int)blocks.size();
+  auto get = [&](const FCell &c) { return T.get(c.p, c.i, c.j, c.k); };
+  auto set = [&](const FCell &c, long long v) { T.set(c.p, c.i, c.j, c.k, v); };
+  std::vector<FieldRange> R(nb);
+  bool periodic = false;
+  for (int p = 0; p < nb; ++p) {
+    R[p] = field_range(blocks[p], pl, op);
+    const auto &d = blocks[p];
+    periodic |= d.bc_west == 5 || d.bc_east == 5 || d.bc_south == 5 || d.bc_north == 5 || d.bc_bottom == 5 ||
+                d.bc_top == 5;
+  }
+  // exchange_bc, all blocks on one rank: per layer two walks over the blocks
+  // (a block alone along a periodic axis copies its own full ghost-inclusive
+  // planes at once; other periodic faces pack into the partner's receive
+  // plane, the second walk's pack replacing the first), then a walk that
+  // unpacks the receive planes.
+  if (periodic) {
+    for (int ly = 0; ly <= nly; ++ly) {
+      std::vector<std::vector<long long>> recv((size_t)nb * 6);
+      auto bc_face = [&](int p, int f, bool unpack) {
+        const auto &d = blocks[p];
+        const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+        const int nbr[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+        const int per[6] = {d.per_ip, d.per_in, d.per_jp, d.per_jn, d.per_kp, d.per_kn};
+        if (!(bcs[f] == MF3D_BC_PERIODIC && nbr[f] < 0)) return;
+        const int ax = f / 2;
+        const bool high = f & 1, alone = nbr[f ^ 1] < 0;
+        const FieldRange &r = R[p];
+        const int n1 = ax == 0 ? r.n[1] : r.n[0], n2 = ax == 2 ? r.n[1] : r.n[2];
+        const int ghost = high ? r.hi[ax] + 1 + ly : r.lo[ax] - 1 - ly;
+        if (unpack) {
+          if (alone) return;
+          const auto &B = recv[(size_t)p * 6 + f];
+          if (B.empty()) return;
+          for (int t = 1; t <= n2; ++t)
+            for (int s = 1; s <= n1; ++s) set(axis_cell(p, ax, ghost, s, t), B[(size_t)(t - 1) * n1 + (s - 1)]);
+          return;
+        }
+        if (alone) {
+          const int src = high ? r.lo[ax] + ly : r.hi[ax] - ly;
+          for (int t = 1; t <= n2; ++t)
+            for (int s = 1; s <= n1; ++s) set(axis_cell(p, ax, ghost, s, t), get(axis_cell(p, ax, src, s, t)));
+          return;
+        }
+        const int q = T.P(per[f]);
+        if (q < 0) return;
+        // the partner's opposite face receives this face's plane
+        auto &B = recv[(size_t)q * 6 + (f ^ 1)];
+        B.assign((size_t)n1 * n2, 0);
+        const int src = high ? r.hi[ax] - ly : r.lo[ax] + ly;
+        for (int t = 1; t <= n2; ++t)
+          for (int s = 1; s <= n1; ++s) B[(size_t)(t - 1) * n1 + (s - 1)] = get(axis_cell(p, ax, src, s, t));
+      };
+      for (int walk = 0; walk < 2; ++walk)
+        for (int p = 0; p < nb; ++p)
+          for (int f = 0; f < 6; ++f) bc_face(p, f, false);
+      for (int p = 0; p < nb; ++p)
+        for (int f = 0; f < 6; ++f) bc_face(p, f, true);
+    }
+  }
+  // exchange_smlvl: per layer every block packs from the layer-start state
+  // (faces: plane lo+ly / hi-ly of the field's range, whole ttc planes; for
+  // ly = 0 also the (pl+1)^3 corner cubes and (pl+1)^2 x n edge bars, from
+  // spr-1 or epr+1 inward); then each block unpacks its corners and edges
+  // (cells outside the field's range in some axis) and last its faces (ghost
+  // plane lo-1-ly / hi+1+ly, interior tangential range).  A phase reads the
+  // state at its start, so every pair names its source token then.
+  struct CP {
+    FCell dst, src;
+  };
+  for (int ly = 0; ly <= nly; ++ly) {
+    std::vector<CP> ph, faces;  // in unpack order; later pairs win
+    for (int p = 0; p < nb; ++p) {
+      const auto &d = blocks[p];
+      const FieldRange &r = R[p];
+      if (ly == 0) {
+        auto ridx = [&](int ax, int dd, int m) { return dd < 0 ? r.spr[ax] - m : r.epr[ax] + m; };
+        auto out = [&](int ax, int dd, int v) { return dd < 0 ? v < r.lo[ax] : v > r.hi[ax]; };
+        for (int c = 0; c < 8; ++c) {
+          const int *dir = c < 4 ? kCP[c] : kCN[c - 4];
+          const int nbr = c < 4 ? d.corprev[c] : d.cornext[c - 4];
+          if (nbr < 0) continue;
+          const int q = T.P(nbr);
+          if (q < 0) continue;
+          const FieldRange &rq = R[q];
+          // the sender sees this block on the opposite side: receiver spr-m <-> sender epr+1-m
+          auto sidx = [&](int ax, int dd, int m) { return dd < 0 ? rq.epr[ax] + 1 - m : rq.spr[ax] - 1 + m; };
+          for (int m1 = 0; m1 <= pl; ++m1)
+            for (int m2 = 0; m2 <= pl; ++m2)
+              for (int m3 = 0; m3 <= pl; ++m3) {
+                const int i = ridx(0, dir[0], m1), j = ridx(1, dir[1], m2), k = ridx(2, dir[2], m3);
+                if (out(0, dir[0], i) || out(1, dir[1], j) || out(2, dir[2], k))
+                  ph.push_back({{p, i, j, k}, {q, sidx(0, dir[0], m1), sidx(1, dir[1], m2), sidx(2, dir[2], m3)}});
+              }
+        }
+        for (int e = 0; e < 12; ++e) {
+          const int *dir = e < 6 ? kEP[e] : kEN[e - 6];
+          const int nbr = e < 6 ? d.edgprev[e] : d.edgnext[e - 6];
+          if (nbr < 0) continue;
+          const int q = T.P(nbr);
+          if (q < 0) continue;
+          const FieldRange &rq = R[q];
+          auto sidx = [&](int ax, int dd, int m) { return dd < 0 ? rq.epr[ax] + 1 - m : rq.spr[ax] - 1 + m; };
+          const int along = dir[0] == 0 ? 0 : dir[1] == 0 ? 1 : 2;
+          const int ta = along == 0 ? 1 : 0, tb = along == 2 ? 1 : 2;
+          for (int m1 = 0; m1 <= pl; ++m1)
+            for (int m2 = 0; m2 <= pl; ++m2)
+              for (int nn = r.spr[along]; nn <= r.epr[along]; ++nn) {
+                int dst[3], src[3];
+                dst[along] = src[along] = nn;
+                dst[ta] = ridx(ta, dir[ta], m1);
+                dst[tb] = ridx(tb, dir[tb], m2);
+                if (!(out(ta, dir[ta], dst[ta]) || out(tb, dir[tb], dst[tb]))) continue;
+                src[ta] = sidx(ta, dir[ta], m1);
+                src[tb] = sidx(tb, dir[tb], m2);
+                ph.push_back({{p, dst[0], dst[1], dst[2]}, {q, src[0], src[1], src[2]}});
+              }
+        }
+      }
+      const int nbr_p[3] = {d.iprev, d.jprev, d.kprev}, nbr_n[3] = {d.inext, d.jnext, d.knext};
+      for (int ax = 0; ax < 3; ++ax) {
+        const int ta = ax == 0 ? 1 : 0, tb = ax == 2 ? 1 : 2;
+        for (int side = 0; side < 2; ++side) {
+          const int nbr = side ? nbr_n[ax] : nbr_p[ax];
+          if (nbr < 0) continue;
+          const int q = T.P(nbr);
+          if (q < 0) continue;
+          const FieldRange &rq = R[q];
+          const int g = side ? r.hi[ax] + 1 + ly : r.lo[ax] - 1 - ly;
+          const int sa = side ? rq.lo[ax] + ly : rq.hi[ax] - ly;
+          for (int t = r.spr[tb]; t <= r.epr[tb]; ++t)
+            for (int s = r.spr[ta]; s <= r.epr[ta]; ++s)
+              faces.push_back({axis_cell(p, ax, g, s, t), axis_cell(q, ax, sa, s, t)});
+        }
+      }
+    }
+    ph.insert(ph.end(), faces.begin(), faces.end());
+    std::vector<long long> v(ph.size());
+    for (size_t q = 0; q < ph.size(); ++q) v[q] = get(ph[q].src);
+    for (size_t q = 0; q < ph.size(); ++q) set(ph[q].dst, v[q]);
+  }
+  // pbound: W, E, S, N, B, T on physical non-periodic faces, whole planes of
+  // the ghost-inclusive range spr-1..epr+1, in order
+  if (with_pbound) {
+    for (int p = 0; p < nb; ++p) {
+      const auto &d = blocks[p];
+      const FieldRange &r = R[p];
+      const int nbr[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+      const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+      for (int f = 0; f < 6; ++f) {
+        if (!(nbr[f] < 0 && bcs[f] != MF3D_BC_PERIODIC)) continue;
+        const int ax = f / 2, ta = ax == 0 ? 1 : 0, tb = ax == 2 ? 1 : 2;
+        const int g = (f & 1) ? r.epr[ax] + 1 : r.spr[ax] - 1, src = (f & 1) ? r.epr[ax] : r.spr[ax];
+        for (int t = r.spr[tb] - 1; t <= r.epr[tb] + 1; ++t)
+          for (int s = r.spr[ta] - 1; s <= r.epr[ta] + 1; ++s)
+            set(axis_cell(p, ax, g, s, t), get(axis_cell(p, ax, src, s, t)));
+      }
+    }
+  }
+  // every ghost cell whose token changed, in increasing cell id
+  std::vector<HaloPair> outp;
+  for (int p = 0; p < nb; ++p)
+    for (int k = 1; k <= T.tk[p]; ++k)
+      for (int j = 1; j <= T.tj[p]; ++j)
+        for (int i = 1; i <= T.ti[p]; ++i) {
+          const long long si = T.sidx(p, i, j, k);
+          if (si < 0) {  // skip the interior of the row
+            i = T.ti[p] - pl;
+            continue;
+          }
+          const long long v = T.shell[p][(size_t)si];
+          if (v >= 0 && v != T.id(p, i, j, k)) outp.push_back({T.id(p, i, j, k), v});
+        }
+  return outp;
+}
+
 std::vector<double> level_widths(const double *ext, int n, double h, int ngrid, int g) {
   int W = 1 << (ngrid - 1);
   std::vector<double> e(n + 2 * W);

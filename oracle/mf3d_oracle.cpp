@@ -104,6 +104,7 @@ struct Ctx {
   long long sip_sweeps; /* nsweeps: inner sweeps run over the solve */
   double eps;
   int eps_relative;
+  int differencing; /* 2: calmas' 4th-order divergence (press.for:13-35) */
   bool periodic;
   double dt, alfapr, rmax;
 };
@@ -704,13 +705,9 @@ void mgkcyc(Ctx &C) {
 
 /* ------------------------------------------------------------------ */
 /* Field halos exchange(op) for op 1..4 (exchange.for:2-23): periodic   */
-/* exchange_bc (exchange_bc.for:2-841) then the face part of            */
-/* exchange_smlvl (exchange.for:343-2498).  The corner/edge part of     */
-/* exchange_smlvl is unpacked before the faces and only its ghost       */
-/* edges and corners survive; nothing on this path reads those, so it   */
-/* is not restated.  Layers ly = 0..nly, nly = pl_ex for u, v, w and 0  */
-/* for p (exchange.for:14-20); calvel and calmas with differencing = 1  */
-/* read layer 0 only, the others are outputs of the final calvel.       */
+/* exchange_bc (exchange_bc.for:2-841) then exchange_smlvl              */
+/* (exchange.for:343-2498).  Layers ly = 0..nly, nly = pl_ex for u, v, w */
+/* and 0 for p (exchange.for:14-20).                                    */
 /* ------------------------------------------------------------------ */
 double *field_of(Blk &B, int op) {
   return op == 1 ? B.u : op == 2 ? B.v : op == 3 ? B.w : op == 44 ? B.pp.data() : B.p;
@@ -777,15 +774,42 @@ void exchange_bc(Ctx &C, int op, int nly) {
   }
 }
 
-void exchange_smlvl_faces(Ctx &C, int op, int nly) {
+/* Corner and edge neighbours of exchange_smlvl, as the direction of the
+ * neighbour along x, y, z (-1 low side, +1 high side, 0 the axis an edge
+ * runs along).  corprev[c] / cornext[c] and edgprev[e] / edgnext[e] of
+ * mf3d_block_desc (alloc_dom.for), in the order exchange.for packs and
+ * unpacks them (:671-1201, :2120-2397). */
+const int kCorPrev[4][3] = {{-1, -1, -1}, {-1, 1, -1}, {1, 1, -1}, {1, -1, -1}};
+const int kCorNext[4][3] = {{1, 1, 1}, {1, -1, 1}, {-1, -1, 1}, {-1, 1, 1}};
+const int kEdgPrev[6][3] = {{-1, 0, -1}, {0, 1, -1}, {1, 0, -1}, {0, -1, -1}, {-1, -1, 0}, {-1, 1, 0}};
+const int kEdgNext[6][3] = {{1, 0, 1}, {0, -1, 1}, {-1, 0, 1}, {0, 1, 1}, {1, 1, 0}, {1, -1, 0}};
+
+/* exchange_smlvl (exchange.for:343-2498) with every block on one rank (the
+ * `dom_ad(a) .eq. dom_ad(b)` path: a sender packs straight into the
+ * receiver's buffer).  Per layer ly every block packs from the state at the
+ * start of the layer - faces (plane is+ly / ie-ly of the field's range,
+ * full ghost-inclusive ttc planes) and, for ly = 0 only, the (pl+1)^3 corner
+ * cubes and the (pl+1)^2 x n edge bars at the block's corners and edges,
+ * from index spr-1 (low side) or epr+1 (high side) of the pressure range
+ * inward (:671-1201).  Then every block unpacks: the corners, at spr-pl..spr
+ * or epr..epr+pl, only cells outside the field's range is..ie in some axis
+ * (:2120-2229); the edges alike over the interior of the edge's axis
+ * (:2231-2397); last the faces, ghost plane is-1-ly / ie+1+ly over the
+ * interior tangential range (:2405-2490). */
+void exchange_smlvl(Ctx &C, int op, int nly) {
+  const int pl = C.pl, pll = (pl + 1) * (pl + 1);
+  const size_t nb = C.b.size();
   for (int ly = 0; ly <= nly; ++ly) {
-  /* pack: all six faces of every block from one snapshot */
-  std::vector<std::vector<double>> bm(C.b.size() * 4), bp(C.b.size() * 4);
-  for (size_t ib = 0; ib < C.b.size(); ++ib) {
+  /* receive buffers of every block: faces bm/bp per axis, corners rcm/rcp, edges rem/rep */
+  std::vector<std::vector<double>> bm(nb * 4), bp(nb * 4);
+  std::vector<std::vector<double>> rcm(nb * 4), rcp(nb * 4), rem(nb * 6), rep(nb * 6);
+  for (size_t ib = 0; ib < nb; ++ib) {
     Blk &B = C.b[ib];
     int is, ie, js, je, ks, ke;
     franges(B, op, is, ie, js, je, ks, ke);
     double *fi = field_of(B, op);
+    const int ni = B.ttc_i, nj = B.ttc_j, nk = B.ttc_k;
+    const int spr[3] = {pl + 1, pl + 1, pl + 1}, epr[3] = {ni - pl, nj - pl, nk - pl}, nn3[3] = {ni, nj, nk};
     int nbr_p[3] = {B.d.iprev, B.d.jprev, B.d.kprev}, nbr_n[3] = {B.d.inext, B.d.jnext, B.d.knext};
     for (int ax = 0; ax < 3; ++ax) {
       int n1 = ax == 0 ? B.ttc_j : B.ttc_i, n2 = ax == 2 ? B.ttc_j : B.ttc_k;
@@ -806,14 +830,83 @@ void exchange_smlvl_faces(Ctx &C, int op, int nly) {
         for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) R[(size_t)(t - 1) * n1 + s] = at(e0 - ly, s, t);
       }
     }
+    if (ly != 0) continue;
+    /* sender index along an axis toward side d of the neighbour, layer q = 0..pl */
+    auto sidx = [&](int ax, int d, int q) { return d < 0 ? spr[ax] - 1 + q : epr[ax] + 1 - q; };
+    for (int c = 0; c < 8; ++c) {
+      const bool prev = c < 4;
+      const int *dir = prev ? kCorPrev[c] : kCorNext[c - 4];
+      const int nbr = prev ? B.d.corprev[c] : B.d.cornext[c - 4];
+      if (nbr < 0) continue;
+      /* corprev c fills the receiver's rc(c)p, cornext c its rc(c)m */
+      auto &R = (prev ? rcp : rcm)[C.indid.at(nbr) * 4 + (c & 3)];
+      R.assign((size_t)(pl + 1) * pll + 1, 0.0);
+      for (int p1 = 0; p1 <= pl; ++p1) for (int p2 = 0; p2 <= pl; ++p2) for (int p3 = 0; p3 <= pl; ++p3)
+        R[(size_t)p1 * pll + p2 * (pl + 1) + p3 + 1] = F(B, fi, sidx(0, dir[0], p1), sidx(1, dir[1], p2), sidx(2, dir[2], p3));
+    }
+    for (int e = 0; e < 12; ++e) {
+      const bool prev = e < 6;
+      const int *dir = prev ? kEdgPrev[e] : kEdgNext[e - 6];
+      const int nbr = prev ? B.d.edgprev[e] : B.d.edgnext[e - 6];
+      if (nbr < 0) continue;
+      const int along = dir[0] == 0 ? 0 : dir[1] == 0 ? 1 : 2;
+      const int ta = along == 0 ? 1 : 0, tb = along == 2 ? 1 : 2;  /* transverse axes, in x, y, z order */
+      auto &R = (prev ? rep : rem)[C.indid.at(nbr) * 6 + (e % 6)];
+      R.assign((size_t)nn3[along] * pll + 1, 0.0);
+      for (int p1 = 0; p1 <= pl; ++p1) for (int p2 = 0; p2 <= pl; ++p2) for (int nn = 1; nn <= nn3[along]; ++nn) {
+        int idx[3];
+        idx[along] = nn;
+        idx[ta] = sidx(ta, dir[ta], p1);
+        idx[tb] = sidx(tb, dir[tb], p2);
+        R[(size_t)(nn - 1) * pll + p1 * (pl + 1) + p2 + 1] = F(B, fi, idx[0], idx[1], idx[2]);
+      }
+    }
   }
-  /* unpack: interior tangential range pl+1 .. n-pl (exchange.for:2402-2490) */
-  for (size_t ib = 0; ib < C.b.size(); ++ib) {
+  /* unpack: corners and edges (ly = 0), then the faces over the interior
+   * tangential range pl+1 .. n-pl (exchange.for:2402-2490) */
+  for (size_t ib = 0; ib < nb; ++ib) {
     Blk &B = C.b[ib];
     int is, ie, js, je, ks, ke;
     franges(B, op, is, ie, js, je, ks, ke);
     double *fi = field_of(B, op);
-    int pl = C.pl;
+    const int ni = B.ttc_i, nj = B.ttc_j, nk = B.ttc_k;
+    const int spr[3] = {pl + 1, pl + 1, pl + 1}, epr[3] = {ni - pl, nj - pl, nk - pl};
+    const int lo[3] = {is, js, ks}, hi[3] = {ie, je, ke};
+    /* receiver index toward side d, layer q = 0..pl; `out` when beyond the field's range */
+    auto ridx = [&](int ax, int d, int q) { return d < 0 ? spr[ax] - q : epr[ax] + q; };
+    auto out = [&](int ax, int d, int v) { return d < 0 ? v < lo[ax] : v > hi[ax]; };
+    if (ly == 0) {
+      for (int c = 0; c < 8; ++c) {
+        const bool prev = c < 4;
+        const int *dir = prev ? kCorPrev[c] : kCorNext[c - 4];
+        const int nbr = prev ? B.d.corprev[c] : B.d.cornext[c - 4];
+        if (nbr < 0) continue;
+        const auto &R = (prev ? rcm : rcp)[ib * 4 + (c & 3)];
+        for (int p1 = 0; p1 <= pl; ++p1) for (int p2 = 0; p2 <= pl; ++p2) for (int p3 = 0; p3 <= pl; ++p3) {
+          const int i = ridx(0, dir[0], p1), j = ridx(1, dir[1], p2), k = ridx(2, dir[2], p3);
+          if (out(0, dir[0], i) || out(1, dir[1], j) || out(2, dir[2], k))
+            F(B, fi, i, j, k) = R[(size_t)p1 * pll + p2 * (pl + 1) + p3 + 1];
+        }
+      }
+      for (int e = 0; e < 12; ++e) {
+        const bool prev = e < 6;
+        const int *dir = prev ? kEdgPrev[e] : kEdgNext[e - 6];
+        const int nbr = prev ? B.d.edgprev[e] : B.d.edgnext[e - 6];
+        if (nbr < 0) continue;
+        const int along = dir[0] == 0 ? 0 : dir[1] == 0 ? 1 : 2;
+        const int ta = along == 0 ? 1 : 0, tb = along == 2 ? 1 : 2;
+        const auto &R = (prev ? rem : rep)[ib * 6 + (e % 6)];
+        for (int p1 = 0; p1 <= pl; ++p1) for (int p2 = 0; p2 <= pl; ++p2)
+          for (int nn = spr[along]; nn <= epr[along]; ++nn) {
+            int idx[3];
+            idx[along] = nn;
+            idx[ta] = ridx(ta, dir[ta], p1);
+            idx[tb] = ridx(tb, dir[tb], p2);
+            if (out(ta, dir[ta], idx[ta]) || out(tb, dir[tb], idx[tb]))
+              F(B, fi, idx[0], idx[1], idx[2]) = R[(size_t)(nn - 1) * pll + p1 * (pl + 1) + p2 + 1];
+          }
+      }
+    }
     int nbr_p[3] = {B.d.iprev, B.d.jprev, B.d.kprev}, nbr_n[3] = {B.d.inext, B.d.jnext, B.d.knext};
     for (int ax = 0; ax < 3; ++ax) {
       int n1 = ax == 0 ? B.ttc_j : B.ttc_i;
@@ -841,7 +934,7 @@ void exchange_smlvl_faces(Ctx &C, int op, int nly) {
 void exchange(Ctx &C, int op) {
   const int nly = (op == 4 || op == 44) ? 0 : C.pl_ex;
   if (C.periodic) exchange_bc(C, op, nly);
-  exchange_smlvl_faces(C, op, nly);
+  exchange_smlvl(C, op, nly);
 }
 
 /* pbound (press.for:77-137) */
@@ -1064,10 +1157,34 @@ void calvel(Ctx &C) {
   exchange(C, 3);
 }
 
-/* calmas (press.for:2-75), the 2nd-order branch (differencing 1 or 3), both L_LSM branches. */
+/* calmas (press.for:2-75): the 4th-order branch (differencing 2, :13-35;
+ * uniform spacing only, 27.0 and 24.0 are double under -fdefault-real-8)
+ * and the 2nd-order one (differencing 1 or 3, :38-67) with both L_LSM
+ * branches. */
 void calmas(Ctx &C) {
   double rmax = 0.0;
   std::vector<double> bmax(C.b.size(), 0.0);
+  if (C.differencing == 2) {
+    par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_]; double rmax = 0.0, resor;
+      const double dx = B.d.dx, dy = B.d.dy, dz = B.d.dz;
+      for (int k = B.ksp; k <= B.kep; ++k) for (int i = B.isp; i <= B.iep; ++i) for (int j = B.jsp; j <= B.jep; ++j) {
+        double fact = ((-F(B, B.u, i + 1, j, k) + 27.0 * F(B, B.u, i, j, k) - 27.0 * F(B, B.u, i - 1, j, k) +
+                        F(B, B.u, i - 2, j, k)) / (24.0 * dx) +
+                       (-F(B, B.v, i, j + 1, k) + 27.0 * F(B, B.v, i, j, k) - 27.0 * F(B, B.v, i, j - 1, k) +
+                        F(B, B.v, i, j - 2, k)) / (24.0 * dy) +
+                       (-F(B, B.w, i, j, k + 1) + 27.0 * F(B, B.w, i, j, k) - 27.0 * F(B, B.w, i, j, k - 1) +
+                        F(B, B.w, i, j, k - 2)) / (24.0 * dz));
+        F(B, B.su.data(), i, j, k) = fact / C.dt;
+        double fact1 = fact * dx * dy * dz;
+        resor = std::max(rmax, std::fabs(fact1));
+        rmax = std::max(resor, std::fabs(fact1));
+      }
+      bmax[ib_] = rmax;
+    });
+    for (double m : bmax) rmax = std::max(rmax, m);
+    C.rmax = rmax;
+    return;
+  }
   par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_]; double rmax = 0.0, resor;
     int o = B.isp - 1;
     for (int k = B.ksp; k <= B.kep; ++k) for (int i = B.isp; i <= B.iep; ++i) for (int j = B.jsp; j <= B.jep; ++j) {
@@ -1281,8 +1398,11 @@ std::string g_err;
 int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm) {
   if (nb <= 0 || !blocks || !prm) { g_err = "bad arguments"; return MF3D_E_INVALID; }
   if (prm->mg_itrsch < 1 || prm->mg_itrsch > 3) { g_err = "mg_itrsch"; return MF3D_E_INVALID; }
-  if (prm->differencing == 2) { g_err = "differencing 2"; return MF3D_E_UNSUPPORTED; }
-  if (prm->differencing != 1 && prm->differencing != 3) { g_err = "differencing"; return MF3D_E_INVALID; }
+  if (prm->differencing < 1 || prm->differencing > 3) { g_err = "differencing"; return MF3D_E_INVALID; }
+  /* the 4th-order divergence reads u(i-2): two ghost layers */
+  if (prm->differencing == 2 && prm->pl < 2) { g_err = "differencing 2 needs pl >= 2"; return MF3D_E_INVALID; }
+  if (prm->differencing == 2 && prm->lsm) { g_err = "differencing 2 with L_LSM"; return MF3D_E_INVALID; }
+  C.differencing = prm->differencing;
   C.ngrd_gl = prm->ngrid; C.mg_itrsch = prm->mg_itrsch; C.irestr = prm->irestr; C.iproln = prm->iproln;
   C.maxcy = prm->maxcy; C.eps = prm->eps; C.eps_relative = prm->eps_relative; C.pl = prm->pl;
   C.pl_ex = prm->pl_ex;
@@ -1319,6 +1439,7 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
       C.periodic = true;
     B.stretched = B.d.hx || B.d.hy || B.d.hz;
     if (C.lsm && B.stretched) { g_err = "L_LSM on a stretched grid"; return MF3D_E_UNSUPPORTED; }
+    if (C.differencing == 2 && B.stretched) { g_err = "differencing 2 on a stretched grid"; return MF3D_E_UNSUPPORTED; }
     if (C.bounds) {
       const int bcs[6] = {B.d.bc_west, B.d.bc_east, B.d.bc_south, B.d.bc_north, B.d.bc_bottom, B.d.bc_top};
       const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
@@ -1399,6 +1520,22 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
     B.oo[0] = rk[ib].uoo; B.oo[1] = rk[ib].voo; B.oo[2] = rk[ib].woo;
   }
   rungek_2nd(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
+  return MF3D_OK;
+}
+
+/* exchange(op) alone on host arrays (exchange.for:2-23), op 1..3 = u, v, w
+ * with pl_ex layers, 4 = p with one layer followed by pbound. */
+int orc_exchange(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, const mf3d_fields *fields, int op) {
+  if (op < 1 || op > 4) { g_err = "op"; return MF3D_E_INVALID; }
+  Ctx C;
+  int st = setup(C, blocks, nb, prm);
+  if (st) return st;
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    B.u = fields[ib].u; B.v = fields[ib].v; B.w = fields[ib].w; B.p = fields[ib].p;
+  }
+  exchange(C, op);
+  if (op == 4) pbound(C);
   return MF3D_OK;
 }
 

@@ -44,6 +44,7 @@ def load():
                                        C.POINTER(RkFields), C.c_double, C.c_double, C.c_int, C.c_int, C.c_double]
         lib.orc_calvel.argtypes = [C.POINTER(BlockDesc), C.c_int, C.POINTER(Params), C.POINTER(Fields),
                                    C.c_double, C.c_double]
+        lib.orc_exchange.argtypes = [C.POINTER(BlockDesc), C.c_int, C.POINTER(Params), C.POINTER(Fields), C.c_int]
         lib.orc_last_error.restype = C.c_char_p
         _lib = lib
     return _lib

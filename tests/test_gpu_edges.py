@@ -50,10 +50,13 @@ def face_mask(shape, pl, nly):
     return m
 
 
-def assert_same(o, g, pl, pl_ex=0):
-    """Status, iterations, history and rmax0 equal; p on the interior and
-    its first ghost layer (exchange(4) + pbound), u, v, w on the interior
-    and ghost layers 0..pl_ex (exchange(1..3)), all bit for bit."""
+def assert_same(o, g, pl, pl_ex=0, every_cell=True):
+    """Status, iterations, history and rmax0 equal; p, u, v, w bit for bit
+    on every cell - interior and every ghost that p = p + pp, exchange(1..4)
+    (periodic planes, faces, the corner and edge neighbours' ghosts) and
+    pbound write, and the ghosts they leave as given (an mf3d_create
+    context).  every_cell=False: p on the interior and its first ghost
+    layer, u, v, w on the interior and face ghost layers 0..pl_ex."""
     st, info, hist, ref = o
     res, got = g
     assert res.status == st and res.iter == info.iter
@@ -61,8 +64,12 @@ def assert_same(o, g, pl, pl_ex=0):
     assert res.rmax0 == info.rmax0
     for b in range(len(ref)):
         for k in ("p", "u", "v", "w"):
-            m = face_mask(ref[b][k].shape, pl, 0 if k == "p" else pl_ex)
-            assert np.array_equal(got[b][k][m], ref[b][k][m]), (b, k)
+            if every_cell:
+                diff = np.argwhere(got[b][k] != ref[b][k])
+                assert diff.size == 0, (b, k, len(diff), diff[:4].tolist())
+            else:
+                m = face_mask(ref[b][k].shape, pl, 0 if k == "p" else pl_ex)
+                assert np.array_equal(got[b][k][m], ref[b][k][m]), (b, k)
 
 
 @pytest.mark.parametrize("maxcy", [0, 1, 2])
@@ -191,3 +198,63 @@ def test_poisoned_allocations(lib, oracle, cuda, monkeypatch):
         for k in ("p", "u", "v", "w"):
             m = face_mask(blocks[b][k].shape, pr.pl, 0)
             assert np.array_equal(poisoned[1][b][k][m], clean[1][b][k][m]), (b, k)
+
+
+@pytest.mark.parametrize("pl,pl_ex,layout", [(2, 0, "2x2x1 periodic x y"), (2, 1, "2x2x1 periodic x y"),
+                                             (3, 2, "2x1x2 walls"), (2, 1, "1 block, walls")])
+def test_fourth_order_calmas(lib, oracle, cuda, pl, pl_ex, layout):
+    """differencing = 2: calmas' 4th-order divergence (press.for:13-35) on
+    the velocities of calvel and its exchange(1..3), every outer iteration;
+    u(i-2) and u(i+1) at the block faces are the exchanged layers where
+    pl_ex reaches them, else the caller's ghost values.  The whole solve -
+    rmax history, p, u, v, w - bit-identical to the oracle."""
+    if layout.startswith("2x2x1"):
+        pr = Problem(2, 2, 1, 16, 16, 8, bc=(PERIODIC, PERIODIC, PERIODIC, PERIODIC, WALL, WALL), ngrid=3, pl=pl)
+    elif layout.startswith("2x1x2"):
+        pr = Problem(2, 1, 2, 16, 8, 16, bc=(WALL,) * 6, ngrid=3, pl=pl)
+    else:
+        pr = Problem(1, 1, 1, 32, 16, 16, bc=(WALL,) * 6, ngrid=3, pl=pl)
+    prm = pr.params(mg_itrsch=3, maxcy=60, eps=1e-9, pl_ex=pl_ex, differencing=2)
+    o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm,
+                    pr.block_fields(seed=23, fourier_modes=2))
+    assert o[0] == 0, o[0]
+    assert_same(o, g, pl, pl_ex)
+
+
+def test_fourth_order_calmas_host_entry(lib, oracle, cuda):
+    """The host-array entry point with differencing = 2: u, v, w reach the
+    device before the first calmas (which reads their ghost faces)."""
+    pr = Problem(2, 1, 1, 16, 16, 16, bc=(PERIODIC, PERIODIC, WALL, WALL, WALL, WALL), ngrid=3, pl=2)
+    prm = pr.params(mg_itrsch=3, maxcy=60, eps=1e-9, pl_ex=1, differencing=2)
+    blocks = pr.block_fields(seed=29, fourier_modes=2)
+    o, _ = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks)
+    host = [{k: v.copy() for k, v in f.items()} for f in blocks]
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    res = proj.newsolv_mg(host)
+    proj.close()
+    assert_same(o, (res, host), 2, 1)
+
+
+@pytest.mark.parametrize("layout", ["2x2x2 walls", "3x2x1 periodic x", "2x2x2 periodic"])
+def test_corner_and_edge_ghosts(lib, oracle, cuda, layout):
+    """Every ghost cell of p, u, v, w after the projection, corner and edge
+    ghosts included: exchange_smlvl unpacks (pl+1)^3 corner cubes and
+    (pl+1)^2 edge bars from the corner and edge neighbours
+    (exchange.for:671-1201, 2120-2397) before the faces, and pbound writes
+    whole ghost-inclusive planes; the library replays that sequence as a copy
+    map, the oracle literally."""
+    if layout == "2x2x2 walls":
+        pr = Problem(2, 2, 2, 16, 8, 8, bc=(WALL,) * 6, ngrid=3, pl=2)
+    elif layout == "3x2x1 periodic x":
+        pr = Problem(3, 2, 1, 8, 8, 16, bc=(PERIODIC, PERIODIC, WALL, WALL, WALL, WALL), ngrid=3, pl=3)
+    else:
+        pr = Problem(2, 2, 2, 8, 8, 8, bc=(PERIODIC,) * 6, ngrid=3, pl=2)
+    pl_ex = 1
+    prm = pr.params(mg_itrsch=3, maxcy=40, eps=1e-9, pl_ex=pl_ex)
+    blocks = pr.block_fields(seed=31, fourier_modes=2, p_random=True)
+    rng = np.random.default_rng(5)
+    for f in blocks:  # every ghost starts distinct, so a missed or extra copy shows
+        for k in ("u", "v", "w"):
+            f[k] += 1e-3 * rng.standard_normal(f[k].shape)
+    o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks)
+    assert_same(o, g, pr.pl, pl_ex)

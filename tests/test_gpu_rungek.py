@@ -125,3 +125,46 @@ def test_two_stages_with_calvel_between(lib, oracle, cuda):
         for k in ("u", "v", "w"):
             m = face_mask(got[k].shape, pl, pl_ex)
             assert np.array_equal(got[k][m], blocks[b][k][m]), (b, k)
+
+
+def test_stage_loop_reads_block_edge_ghosts(lib, oracle, cuda):
+    """2x2x1 blocks with walls outside: the interior block edges along z join
+    four blocks.  The u predictor reads v(i+1,j-1,k) and w(i+1,j,k-1)
+    (rungek.for:336-343), which at a block's outer i-edge are the (x,y) and
+    (x,z) edge ghosts that calvel's exchange(2), (3) fill from the edge
+    neighbour (exchange.for:2231-2397).  Stage (alfabc 1) -> calvel ->
+    stage (alfabc 0) on the device against the oracle: ustar, vstar, wstar,
+    u, v, w bit for bit on every cell."""
+    import torch
+    from multiflow3d_b200.problems import fields_struct
+    pr = Problem(2, 2, 1, 16, 16, 8, bc=(W,) * 6, ngrid=2, pl=2)
+    pl_ex, dt = 1, 0.013
+    alfark = (0.5, 1.0)
+    blocks, rk = rk_inputs(pr, 37)
+    gpu = [{k: dev(v, cuda) for k, v in f.items()} for f in blocks]
+    grk = [{k: dev(v, cuda) for k, v in r.items()} for r in rk]
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfark[0], alfabc=1, pl_ex=pl_ex) == 0
+    prm_o = pr.params(pl_ex=pl_ex, bounds=1, alfabc=1)
+    assert oracle.orc_calvel(pr.descriptors(oracle), pr.nblocks, C.byref(prm_o), fields_struct(blocks),
+                             dt, alfark[0]) == 0
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfark[1], alfabc=0, pl_ex=pl_ex) == 0
+    proj = Projection(pr.descriptors(lib), pr.params(pl_ex=pl_ex, bounds=1, alfabc=1), lib)
+    fa = (abi.Fields * pr.nblocks)()
+    ra = (RkFields * pr.nblocks)()
+    dp = C.POINTER(C.c_double)
+    for b in range(pr.nblocks):
+        for k in ("ustar", "vstar", "wstar", "u", "v", "w", "p"):
+            setattr(fa[b], k, C.cast(C.c_void_p(gpu[b][k].data_ptr()), dp))
+        for k in ("uoo", "voo", "woo", "vis"):
+            setattr(ra[b], k, C.cast(C.c_void_p(grk[b][k].data_ptr()), dp))
+    assert lib.mf3d_rungek_2nd_device(proj.ctx, fa, ra, dt, alfark[0], 1, 0, 0.0) == 0, abi.last_error(lib)
+    assert lib.mf3d_calvel_device(proj.ctx, fa, dt, alfark[0]) == 0, abi.last_error(lib)
+    assert lib.mf3d_rungek_2nd_device(proj.ctx, fa, ra, dt, alfark[1], 0, 0, 0.0) == 0, abi.last_error(lib)
+    proj.close()
+    torch.cuda.synchronize()
+    pl = pr.pl
+    for b in range(pr.nblocks):
+        got = {k: v.cpu().numpy() for k, v in gpu[b].items()}
+        for k in ("ustar", "vstar", "wstar", "u", "v", "w"):
+            diff = np.argwhere(got[k] != blocks[b][k])
+            assert diff.size == 0, (b, k, len(diff), diff[:4].tolist())

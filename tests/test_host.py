@@ -84,6 +84,40 @@ def test_halo_map_matches_oracle_exchangepp(lib, oracle, layout):
             assert np.array_equal(out, np.concatenate([a.ravel() for a in ref])), (layout, bc, level)
 
 
+FX_CASES = [((2, 2, 2), (WALL,) * 6, 2, 0), ((2, 2, 2), (WALL,) * 6, 3, 2), ((2, 2, 1), (PERIODIC,) * 4 + (WALL,) * 2, 2, 1),
+            ((3, 2, 2), (PERIODIC, PERIODIC, WALL, WALL, PERIODIC, PERIODIC), 2, 1),
+            ((1, 1, 1), (PERIODIC,) * 6, 2, 1), ((2, 1, 1), (WALL,) * 6, 1, 0),
+            ((2, 2, 2), (PERIODIC,) * 6, 1, 0)]
+
+
+@pytest.mark.parametrize("layout,bc,pl,pl_ex", FX_CASES)
+def test_field_exchange_map_matches_oracle(lib, oracle, layout, bc, pl, pl_ex):
+    """The library's copy map of exchange(op) - exchange_bc on periodic faces,
+    exchange_smlvl with its corner cubes, edge bars and faces
+    (exchange.for:343-2498), and pbound after exchange(4) - applied to
+    random fields equals the oracle's literal sequence on every cell of u, v,
+    w and p, bit for bit."""
+    from multiflow3d_b200.problems import fields_struct
+    pr = Problem(*layout, 8, 6, 4, bc=bc, ngrid=2, pl=pl)
+    d1, d2 = pr.descriptors(lib), pr.descriptors(oracle)
+    prm = pr.params(pl_ex=pl_ex)
+    rng = np.random.default_rng(pl * 10 + pl_ex)
+    for op, key in ((1, "u"), (2, "v"), (3, "w"), (4, "p")):
+        blocks = pr.block_fields(seed=3)
+        for f in blocks:
+            f[key][...] = rng.standard_normal(f[key].shape)
+        flat = np.concatenate([f[key].ravel() for f in blocks])
+        assert oracle.orc_exchange(d2, pr.nblocks, C.byref(prm), fields_struct(blocks), op) == 0
+        n = lib.mf3d_field_exchange_map(d1, pr.nblocks, pl, pl_ex, op, None, None)
+        assert n > 0
+        dst = (C.c_longlong * n)()
+        src = (C.c_longlong * n)()
+        assert lib.mf3d_field_exchange_map(d1, pr.nblocks, pl, pl_ex, op, dst, src) == n
+        out = flat.copy()
+        out[np.array(dst[:], dtype=np.int64)] = flat[np.array(src[:], dtype=np.int64)]
+        assert np.array_equal(out, np.concatenate([f[key].ravel() for f in blocks])), (op, key)
+
+
 def test_create_rejects_bad_config_without_gpu(lib):
     """Divisibility rule of localparameters.for:201-206 is checked before any
     device work."""
@@ -96,9 +130,13 @@ def test_create_rejects_bad_config_without_gpu(lib):
     prm.mg_itrsch = 7
     assert lib.mf3d_create(pr.descriptors(lib), 1, C.byref(prm), C.byref(ctx)) == abi.MF3D_E_INVALID
     prm = Problem(1, 1, 1, 8, 8, 8, ngrid=2).params()
-    prm.differencing = 2
+    prm.differencing = 2  # the 4th-order divergence reads u(i-2): pl = 1 has no such ghost
     assert lib.mf3d_create(Problem(1, 1, 1, 8, 8, 8, ngrid=2).descriptors(lib), 1, C.byref(prm),
-                           C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED
+                           C.byref(ctx)) == abi.MF3D_E_INVALID
+    assert b"pl >= 2" in lib.mf3d_last_error()
+    pst = Problem(1, 1, 1, 8, 8, 8, ngrid=2, pl=2, stretch_y=2.0)
+    prm = pst.params(differencing=2)  # 4th order on a stretched grid: no reference definition
+    assert lib.mf3d_create(pst.descriptors(lib), 1, C.byref(prm), C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED
     prm.differencing = 4
     assert lib.mf3d_create(Problem(1, 1, 1, 8, 8, 8, ngrid=2).descriptors(lib), 1, C.byref(prm),
                            C.byref(ctx)) == abi.MF3D_E_INVALID

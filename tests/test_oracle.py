@@ -293,8 +293,71 @@ def test_weno_differencing_takes_the_second_order_divergence(oracle):
         for k in ("p", "u", "v", "w", "su"):
             assert np.array_equal(a[k], b[k])
     blocks = pr.block_fields(seed=4)
-    assert solve(oracle, pr, blocks, maxcy=2, differencing=2)[0] == -6
+    for f, r in zip(blocks, pr.block_density(5)):
+        f["dens"] = r
+    assert solve(oracle, pr, blocks, maxcy=2, differencing=2, lsm=1)[0] == -1  # L_LSM needs WENO
     assert solve(oracle, pr, blocks, maxcy=2, differencing=4)[0] == -1
+
+
+@pytest.mark.parametrize("layout", ["1 block, walls", "2x2x1 blocks, walls"])
+def test_fourth_order_divergence_known_answer(oracle, layout):
+    """calmas' 4th-order branch (press.for:13-35) is exact for cubic face
+    velocities: with u = f(x), v = g(y), w = q(z) cubic on every face
+    (ghosts included) and p = 0, the initial calvel leaves u = ustar and the
+    exchange hands over the same polynomial, so su = f'(x) + g'(y) + q'(z)
+    at the cell centres and rmax0 = max |su * dx*dy*dz|.  The 2nd-order
+    branch misses the cubic term (its error h^2/24 times the third
+    derivative is visible).  A pl = 1 layout, with no second ghost face, is
+    refused."""
+    h = 1.0 / 16
+    if layout.startswith("1"):
+        pr = Problem(1, 1, 1, 16, 8, 8, bc=(WALL,) * 6, ngrid=2, pl=2, dx=h, dy=h, dz=h)
+    else:
+        pr = Problem(2, 2, 1, 8, 8, 8, bc=(WALL,) * 6, ngrid=2, pl=2, dx=h, dy=h, dz=h)
+    f = lambda x: 0.3 + 1.7 * x - 2.1 * x ** 2 + 3.3 * x ** 3
+    g = lambda y: -0.4 + 0.9 * y + 1.1 * y ** 2 - 0.7 * y ** 3
+    q = lambda z: 0.2 - 1.3 * z + 0.5 * z ** 2 + 2.9 * z ** 3
+    df = lambda x: 1.7 - 4.2 * x + 9.9 * x ** 2
+    dg = lambda y: 0.9 + 2.2 * y - 2.1 * y ** 2
+    dq = lambda z: -1.3 + 1.0 * z + 8.7 * z ** 2
+
+    def fields():
+        out = []
+        for b in range(pr.nblocks):
+            bx, by, bz = pr.block_pos(b)
+            # u(i) sits on the face between cells i and i+1: x = (global cell index + 1) * h
+            xi = (bx * pr.nx + np.arange(-pr.pl, pr.nx + pr.pl) + 1) * h
+            yj = (by * pr.ny + np.arange(-pr.pl, pr.ny + pr.pl) + 1) * h
+            zk = (bz * pr.nz + np.arange(-pr.pl, pr.nz + pr.pl) + 1) * h
+            shp = pr.ttc
+            us = np.broadcast_to(f(xi)[None, None, :], shp).copy()
+            vs = np.broadcast_to(g(yj)[None, :, None], shp).copy()
+            ws = np.broadcast_to(q(zk)[:, None, None], shp).copy()
+            out.append({"ustar": us, "vstar": vs, "wstar": ws, "u": us.copy(), "v": vs.copy(), "w": ws.copy(),
+                        "p": np.zeros(shp), "su": np.zeros(shp)})
+        return out
+
+    blocks = fields()
+    st, info, _ = solve(oracle, pr, blocks, maxcy=0, differencing=2)
+    assert st in (0, 1), st
+    worst = 0.0
+    for b, fb in enumerate(blocks):
+        bx, by, bz = pr.block_pos(b)
+        xc = (bx * pr.nx + np.arange(pr.nx) + 0.5) * h
+        yc = (by * pr.ny + np.arange(pr.ny) + 0.5) * h
+        zc = (bz * pr.nz + np.arange(pr.nz) + 0.5) * h
+        exact = dq(zc)[:, None, None] + dg(yc)[None, :, None] + df(xc)[None, None, :]
+        got = pr.interior(fb["su"])
+        assert np.abs(got - exact).max() <= 1e-10 * np.abs(exact).max()
+        worst = max(worst, float(np.abs(got * h ** 3).max()))
+    assert abs(info.rmax0 - worst) <= 1e-14 * worst
+    # the 2nd-order branch on the same faces misses the cubic term
+    blocks2 = fields()
+    solve(oracle, pr, blocks2, maxcy=0, differencing=1)
+    assert np.abs(pr.interior(blocks2[0]["su"]) - pr.interior(blocks[0]["su"])).max() > 1e-4
+    # pl = 1 has no u(isp-2)
+    pr1 = Problem(1, 1, 1, 16, 8, 8, bc=(WALL,) * 6, ngrid=2, pl=1)
+    assert solve(oracle, pr1, pr1.block_fields(seed=1), maxcy=1, differencing=2)[0] == -1
 
 
 def test_bounds_known_answers(oracle):

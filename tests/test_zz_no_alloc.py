@@ -58,6 +58,39 @@ def test_noalloc_matches_mgkcyc_device(lib, cuda, precision):
         assert np.array_equal(again[b], ref[0][b])
 
 
+@pytest.mark.parametrize("precision", [abi.MF3D_PREC_FP64, abi.MF3D_PREC_FP32])
+def test_noalloc_first_on_fresh_context_allocates_nothing(lib, cuda, precision):
+    """The no-allocation entry point as the first call on a new context: the
+    device's free memory is the same before and after two calls (no lazily
+    loaded kernel, no pool growth), and the results equal those of
+    mf3d_mgkcyc_device on a second context."""
+    import torch
+    pr = Problem(2, 1, 2, 16, 16, 8, bc=(WALL, WALL, WALL, WALL, PERIODIC, PERIODIC), ngrid=3, pl=1)
+    prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, precision=precision)
+    rng = np.random.default_rng(9)
+    rhs = [[torch.from_numpy(rng.uniform(-1, 1, size=pr.ttc)).to(cuda) for _ in range(pr.nblocks)]
+           for _ in range(2)]
+    pps = [[torch.zeros(pr.ttc, dtype=torch.float64, device=cuda) for _ in range(pr.nblocks)] for _ in range(2)]
+    fresh = Projection(pr.descriptors(lib), prm, lib)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(cuda)[0]
+    for su, pp in zip(rhs, pps):
+        assert lib.mf3d_mgkcyc_device_noalloc(fresh.ctx, _ptrs(su), _ptrs(pp)) == abi.MF3D_OK, lib.mf3d_last_error()
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info(cuda)[0]
+    fresh.close()
+    assert free1 == free0, (free0, free1)
+    other = Projection(pr.descriptors(lib), prm, lib)
+    for su, pp in zip(rhs, pps):
+        ref = [torch.zeros(pr.ttc, dtype=torch.float64, device=cuda) for _ in range(pr.nblocks)]
+        assert lib.mf3d_mgkcyc_device(other.ctx, _ptrs(su), _ptrs(ref)) == abi.MF3D_OK
+        for b in range(pr.nblocks):
+            g, r = pp[b].cpu().numpy(), ref[b].cpu().numpy()
+            assert _rel(g, r) <= TOL
+            assert np.array_equal(g, r)
+    other.close()
+
+
 def test_noalloc_rejects_too_many_blocks(lib, cuda):
     import torch
     n = abi.MF3D_NOALLOC_MAX_BLOCKS + 1
