@@ -266,6 +266,7 @@ def run_gpu(args):
         f["su"] = None  # the final su is not requested
     prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=400, eps=1e-10, eps_relative=1, device=local)
     proj = Projection(pr.descriptors(lib), prm, lib)
+    tuning = {g: proj.tuning(g) for g in range(1, pr.ngrid + 1)}
 
     def reset():
         for f, p0 in zip(d, pristine):
@@ -369,6 +370,7 @@ def run_gpu(args):
                                                "launches_per_solve": v[1]}
                                            for n, v in kernels.items() if n != "k_rbgs"}},
             "clocks": clocks.summary(),
+            "tuning": tuning,
         }
         if world == 1 and not args.no_cpu_baseline:
             threads = max(1, min(os.cpu_count() or 1, pr.nblocks))

@@ -347,6 +347,17 @@ int mf3d_profile(mf3d_ctx *ctx, int kind);
 int mf3d_profile_read(mf3d_ctx *ctx, double *total_ms, long long *launches,
                       double *algorithmic_bytes);
 
+/* Launch shapes the library chose for level `level` (1-based) of `ctx` -
+ * by its autotuner (timed at mf3d_create / mf3d_batch_create, cached per
+ * process by device, precision, smoother and block shapes; MF3D_AUTOTUNE=0
+ * turns it off) or by default: the red-black sweep schedule (0..3), 1 when
+ * the level sweeps with the plain-load kernel, the planes per CTA of the
+ * restriction into the level, and the CTAs per block of the line or
+ * lexicographic relaxation.  Any of the outputs may be NULL.  No
+ * counterpart in the reference. */
+int mf3d_tuning(const mf3d_ctx *ctx, int level, int *sweep_schedule, int *small_sweep, int *restrict_planes,
+                int *cluster_ctas);
+
 /* Host-only view of a field exchange: exchange(op) of exchange.for:2-23
  * (exchange_bc on the periodic faces, then exchange_smlvl with its corners,
  * edges and faces), followed by pbound for op 4 (press.for:77-137), as

@@ -172,6 +172,7 @@ EXPORTED_SYMBOLS = (
     "mf3d_rungek_2nd_device",
     "mf3d_calvel_device",
     "mf3d_field_exchange_map",
+    "mf3d_tuning",
     "mf3d_test_fail_alloc",
     "mf3d_test_stall_copy",
 )
@@ -234,6 +235,7 @@ def _declare(lib):
     lib.mf3d_field_exchange_map.restype = C.c_longlong
     lib.mf3d_field_exchange_map.argtypes = [C.POINTER(BlockDesc), C.c_int, C.c_int, C.c_int, C.c_int,
                                             C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.mf3d_tuning.argtypes = [vp, C.c_int] + [C.POINTER(C.c_int)] * 4
     lib.mf3d_test_fail_alloc.argtypes = [C.c_longlong]
     lib.mf3d_test_stall_copy.argtypes = [C.c_int, C.c_int]
     return lib

@@ -511,17 +511,29 @@ struct DomainStore {
   std::vector<DevBuf<HaloCopy>> dhalo;       // per level, the same pairs on the device
   std::vector<FaceRule> rules;               // 6 per block, domain-local sources
   // exchange(1..3) and exchange(4) + pbound of the fields as copy maps
-  // (mf3d_create contexts): u, v, w pairs and p pairs, staged pairs first
-  DevBuf<FxCopy> fx_uvw, fx_p;
+  // (mf3d_create contexts, build_field_maps): u, v, w pairs and p pairs,
+  // staged pairs first; the evolution lists of the chained u, v, w ghosts
+  DevBuf<FxCopy> fx_uvw, fx_p, fxe_sub, fxe_chain;
+  DevBuf<FxCell> fxe_cells;
   long long nfx_uvw = 0, nsfx_uvw = 0, nfx_p = 0, nsfx_p = 0;
+  long long nfxe_sub = 0, nsfxe_sub = 0, nfxe_chain = 0, nfxe_cells = 0;
+  bool fx_per_iteration = false;
   size_t bytes = 0;
 };
 
-// The field exchange maps of a domain: exchange(1), (2), (3) with pl_ex
-// layers (u, v, w) and exchange(4) + pbound (p), as FxCopy lists with the
-// pairs whose source is itself written first (they are staged).
+// The field exchange maps of a domain (FxCopy lists, pairs whose source is
+// itself written first: they are staged).
+//   p:  exchange(4) + pbound, applied whole after every p += pp.
+//   u, v, w, `per_iteration` (the 4th-order calmas path, which writes u, v, w
+//       in every outer iteration): exchange(1..3) whole, applied at every
+//       calvel point.
+//   u, v, w otherwise (the fused path writes u, v, w once, after the loop):
+//       the final exchange, whose chained sources - ghost cells of the state
+//       before it that an earlier exchange wrote - read the `prev` slots
+//       that k_fx_evolve fills; and the evolution lists of those chains (see
+//       k_fx_evolve).
 static int build_field_maps(DomainStore &D, const std::vector<mf3d_block_desc> &descs, int pl, int pl_ex,
-                            cudaStream_t s) {
+                            bool per_iteration, cudaStream_t s) {
   const int nb = (int)descs.size();
   std::vector<long long> base(nb);
   long long acc = 0;
@@ -530,41 +542,146 @@ static int build_field_maps(DomainStore &D, const std::vector<mf3d_block_desc> &
     acc += (long long)(descs[b].nx + 2 * pl) * (descs[b].ny + 2 * pl) * (descs[b].nz + 2 * pl);
   }
   if (nb > 65535) { set_error("field exchange map: more than 65535 blocks"); return MF3D_E_UNSUPPORTED; }
+  auto blk_of = [&](long long id) { return (int)(std::upper_bound(base.begin(), base.end(), id) - base.begin()) - 1; };
   auto loc = [&](long long id, unsigned short &blk, unsigned &off) {
-    const int b = (int)(std::upper_bound(base.begin(), base.end(), id) - base.begin()) - 1;
+    const int b = blk_of(id);
     blk = (unsigned short)b;
     off = (unsigned)(id - base[b]);
   };
-  auto lists = [&](const std::vector<int> &ops, std::vector<FxCopy> &out, long long &nstaged) {
+  // 1-based field indices of a cell and whether it is a ghost cell
+  auto ijk = [&](long long id, int &b, int &i, int &j, int &k) {
+    b = blk_of(id);
+    long long r = id - base[b];
+    const long long ti = descs[b].nx + 2 * pl, tj = descs[b].ny + 2 * pl;
+    i = (int)(r % ti) + 1;
+    r /= ti;
+    j = (int)(r % tj) + 1;
+    k = (int)(r / tj) + 1;
+  };
+  auto ghost = [&](long long id) {
+    int b, i, j, k;
+    ijk(id, b, i, j, k);
+    return i <= pl || j <= pl || k <= pl || i > descs[b].nx + pl || j > descs[b].ny + pl || k > descs[b].nz + pl;
+  };
+  int st;
+  // p: whole
+  {
+    std::vector<HaloPair> pr = build_field_map(descs, base, pl, 4, 0, true);
     std::vector<FxCopy> staged, plain;
-    for (int op : ops) {
-      std::vector<HaloPair> pr = build_field_map(descs, base, pl, op, op == 4 ? 0 : pl_ex, op == 4);
-      // pr is sorted by dst: a source that is some pair's dst must be staged
-      auto written = [&](long long id) {
-        auto it = std::lower_bound(pr.begin(), pr.end(), id, [](const HaloPair &a, long long v) { return a.dst < v; });
-        return it != pr.end() && it->dst == id;
-      };
+    auto written = [&](long long id) {
+      auto it = std::lower_bound(pr.begin(), pr.end(), id, [](const HaloPair &x, long long v) { return x.dst < v; });
+      return it != pr.end() && it->dst == id;
+    };
+    for (const auto &x : pr) {
+      FxCopy c;
+      loc(x.dst, c.dblk, c.doff);
+      loc(x.src, c.sblk, c.soff);
+      c.comp = 3;
+      (written(x.src) ? staged : plain).push_back(c);
+    }
+    D.nsfx_p = (long long)staged.size();
+    staged.insert(staged.end(), plain.begin(), plain.end());
+    D.nfx_p = (long long)staged.size();
+    if ((st = D.fx_p.upload(staged, s))) return st;
+    D.bytes += staged.size() * sizeof(FxCopy);
+  }
+  // u, v, w
+  std::vector<FxCopy> fin_staged, fin_plain, sub_staged, sub_plain, chain;
+  std::vector<FxCell> cells;
+  for (int op = 1; op <= 3; ++op) {
+    std::vector<HaloPair> pr = build_field_map(descs, base, pl, op, pl_ex, false);
+    auto find = [&](long long id) {
+      auto it = std::lower_bound(pr.begin(), pr.end(), id, [](const HaloPair &x, long long v) { return x.dst < v; });
+      return (it != pr.end() && it->dst == id) ? (long long)(it - pr.begin()) : -1LL;
+    };
+    if (per_iteration) {
       for (const auto &x : pr) {
         FxCopy c;
         loc(x.dst, c.dblk, c.doff);
         loc(x.src, c.sblk, c.soff);
         c.comp = op - 1;
-        (written(x.src) ? staged : plain).push_back(c);
+        (find(x.src) >= 0 ? fin_staged : fin_plain).push_back(c);
+      }
+      continue;
+    }
+    // C: the ghost cells whose values chains carry across exchanges - chained
+    // sources that some exchange writes, closed over the ghost sources of
+    // the pairs writing them
+    std::vector<char> inC(pr.size(), 0);  // by pair index (the pair writing the cell)
+    std::vector<long long> work;
+    for (const auto &x : pr)
+      if (ghost(x.src)) {
+        const long long q = find(x.src);
+        if (q >= 0 && !inC[q]) { inC[q] = 1; work.push_back(q); }
+      }
+    while (!work.empty()) {
+      const long long q = work.back();
+      work.pop_back();
+      if (!ghost(pr[q].src)) continue;
+      const long long r = find(pr[q].src);
+      if (r >= 0 && !inC[r]) { inC[r] = 1; work.push_back(r); }
+    }
+    // prev slots: one per chained source in C
+    std::unordered_map<long long, unsigned> slot;
+    for (const auto &x : pr)
+      if (ghost(x.src) && find(x.src) >= 0 && !slot.count(x.src)) {
+        const unsigned sl = (unsigned)chain.size();
+        slot[x.src] = sl;
+        FxCopy c;
+        loc(x.src, c.sblk, c.doff);
+        c.dblk = c.sblk;
+        c.soff = sl;
+        c.comp = op - 1;
+        chain.push_back(c);
+      }
+    std::unordered_set<long long> seen_cell;
+    for (size_t q = 0; q < pr.size(); ++q) {
+      const auto &x = pr[q];
+      // the final exchange
+      FxCopy f;
+      loc(x.dst, f.dblk, f.doff);
+      loc(x.src, f.sblk, f.soff);
+      f.comp = op - 1;
+      auto it = slot.find(x.src);
+      if (it != slot.end()) {
+        f.comp |= 8;
+        f.soff = it->second;
+        fin_plain.push_back(f);  // prev is not written by the apply: no staging
+      } else {
+        (find(x.src) >= 0 ? fin_staged : fin_plain).push_back(f);
+      }
+      if (!inC[q]) continue;
+      // the evolution sub-map: pairs writing C, staged when their source is
+      // written by the sub-map; interior sources formed by calvel first
+      FxCopy c;
+      loc(x.dst, c.dblk, c.doff);
+      loc(x.src, c.sblk, c.soff);
+      c.comp = op - 1;
+      const long long r = find(x.src);
+      (r >= 0 && inC[r] ? sub_staged : sub_plain).push_back(c);
+      if (!ghost(x.src) && seen_cell.insert(x.src).second) {
+        FxCell e;
+        int b, i, j, k;
+        ijk(x.src, b, i, j, k);
+        e.blk = b; e.comp = op - 1; e.i = i - pl; e.j = j - pl; e.k = k - pl;  // level-1 indices
+        cells.push_back(e);
       }
     }
-    nstaged = (long long)staged.size();
-    out = std::move(staged);
-    out.insert(out.end(), plain.begin(), plain.end());
-  };
-  std::vector<FxCopy> uvw, pp;
-  lists({1, 2, 3}, uvw, D.nsfx_uvw);
-  lists({4}, pp, D.nsfx_p);
-  D.nfx_uvw = (long long)uvw.size();
-  D.nfx_p = (long long)pp.size();
-  int st;
-  if ((st = D.fx_uvw.upload(uvw, s))) return st;
-  if ((st = D.fx_p.upload(pp, s))) return st;
-  D.bytes += (uvw.size() + pp.size()) * sizeof(FxCopy);
+  }
+  D.nsfx_uvw = (long long)fin_staged.size();
+  fin_staged.insert(fin_staged.end(), fin_plain.begin(), fin_plain.end());
+  D.nfx_uvw = (long long)fin_staged.size();
+  D.nsfxe_sub = (long long)sub_staged.size();
+  sub_staged.insert(sub_staged.end(), sub_plain.begin(), sub_plain.end());
+  D.nfxe_sub = (long long)sub_staged.size();
+  D.nfxe_chain = (long long)chain.size();
+  D.nfxe_cells = (long long)cells.size();
+  D.fx_per_iteration = per_iteration;
+  if ((st = D.fx_uvw.upload(fin_staged, s))) return st;
+  if ((st = D.fxe_sub.upload(sub_staged, s))) return st;
+  if ((st = D.fxe_chain.upload(chain, s))) return st;
+  if ((st = D.fxe_cells.upload(cells, s))) return st;
+  D.bytes += (fin_staged.size() + sub_staged.size() + chain.size()) * sizeof(FxCopy) + cells.size() * sizeof(FxCell);
   CK(cudaStreamSynchronize(s));  // the host vectors are locals
   return MF3D_OK;
 }
@@ -575,7 +692,8 @@ static long long level_off(const BlkLev &B, int i, int j, int k) {
 }
 
 static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, int ngrid, int elem, int elem_coarsest,
-                        int pl, cudaStream_t s, bool lsm = false, bool bounds = false, int field_maps_pl_ex = -1) {
+                        int pl, cudaStream_t s, bool lsm = false, bool bounds = false, int field_maps_pl_ex = -1,
+                        bool fx_per_iteration = false) {
   D.ngrid = ngrid;
   D.blocks.clear();
   std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
@@ -635,7 +753,7 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
     D.bytes += h.size() * sizeof(HaloCopy);
   }
   CK(cudaStreamSynchronize(s));  // the host vectors are locals
-  if (field_maps_pl_ex >= 0 && (st = build_field_maps(D, descs, pl, field_maps_pl_ex, s))) return st;
+  if (field_maps_pl_ex >= 0 && (st = build_field_maps(D, descs, pl, field_maps_pl_ex, fx_per_iteration, s))) return st;
   return MF3D_OK;
 }
 
@@ -692,9 +810,12 @@ struct View {
   int n_int = 0, n_zint = 0, n_l1cells = 0, n_faces = 0, n_planes = 0, n_vfaces = 0;
   // field exchanges as copy maps (a view over one domain that has them):
   // exchange(1..3) of u, v, w and exchange(4) + pbound of p
-  const FxCopy *fx_uvw = nullptr, *fx_p = nullptr;
+  const FxCopy *fx_uvw = nullptr, *fx_p = nullptr, *fxe_sub = nullptr, *fxe_chain = nullptr;
+  const FxCell *fxe_cells = nullptr;
   long long nfx_uvw = 0, nsfx_uvw = 0, nfx_p = 0, nsfx_p = 0;
-  DevBuf<double> fx_stage;
+  long long nfxe_sub = 0, nsfxe_sub = 0, nfxe_chain = 0, nfxe_cells = 0;
+  bool fx_per_iteration = false;      // u, v, w exchanged whole at every calvel point (4th-order calmas)
+  DevBuf<double> fx_stage, fx_prev;   // staged sources; chained sources before the last exchange
   DevBuf<DomState> ds;
   DevBuf<int> act, ones;
   DevBuf<int> err;                    // device error code (a TMA wait that gave up)
@@ -1224,13 +1345,22 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       V.n_bcax[a] = (int)tb.size();
       if ((st = V.t_bcax[a].upload(tb, s))) return st;
     }
-  V.fx_uvw = V.fx_p = nullptr;
+  V.fx_uvw = V.fx_p = V.fxe_sub = V.fxe_chain = nullptr;
+  V.fxe_cells = nullptr;
   V.nfx_uvw = V.nsfx_uvw = V.nfx_p = V.nsfx_p = 0;
+  V.nfxe_sub = V.nsfxe_sub = V.nfxe_chain = V.nfxe_cells = 0;
+  V.fx_per_iteration = false;
   if (nd == 1 && doms[0]->nfx_uvw + doms[0]->nfx_p > 0) {
     const DomainStore &D = *doms[0];
     V.fx_uvw = D.fx_uvw.p; V.nfx_uvw = D.nfx_uvw; V.nsfx_uvw = D.nsfx_uvw;
     V.fx_p = D.fx_p.p; V.nfx_p = D.nfx_p; V.nsfx_p = D.nsfx_p;
-    if ((st = V.fx_stage.alloc((size_t)std::max<long long>(std::max(V.nsfx_uvw, V.nsfx_p), 1)))) return st;
+    V.fxe_sub = D.fxe_sub.p; V.nfxe_sub = D.nfxe_sub; V.nsfxe_sub = D.nsfxe_sub;
+    V.fxe_chain = D.fxe_chain.p; V.nfxe_chain = D.nfxe_chain;
+    V.fxe_cells = D.fxe_cells.p; V.nfxe_cells = D.nfxe_cells;
+    V.fx_per_iteration = D.fx_per_iteration;
+    const long long ns = std::max(std::max(V.nsfx_uvw, V.nsfx_p), V.nsfxe_sub);
+    if ((st = V.fx_stage.alloc((size_t)std::max<long long>(ns, 1)))) return st;
+    if ((st = V.fx_prev.alloc((size_t)std::max<long long>(V.nfxe_chain, 1)))) return st;
   }
   // per-domain solve state
   std::vector<int> ones(std::max(nd, 1), 1);
@@ -1497,7 +1627,10 @@ static int autotune_level(mf3d_ctx *C, View &V, int g, bool time_new) {
     // (a) sweep schedule, (b) sweep kernel
     const std::string ks = tune_key(C, L, "sweep", sizeof(T));
     int v;
-    if (tune_get(ks, v)) {
+    const char *forced = std::getenv("MF3D_SWEEP_SCHED");  // a fixed schedule 0..3 (tuning comparisons)
+    if (forced) {
+      if ((st = upload_sweeps(C, L, std::max(0, std::min(kSweepSchedules - 1, std::atoi(forced)))))) return st;
+    } else if (tune_get(ks, v)) {
       if ((st = upload_sweeps(C, L, v & 7))) return st;
       if (g > 1) L.small = (v >> 3) & 1;
     } else if (time_new) {
@@ -1505,9 +1638,12 @@ static int autotune_level(mf3d_ctx *C, View &V, int g, bool time_new) {
       int bs = 0;
       for (int sc = 0; sc < kSweepSchedules; ++sc) {
         if ((st = upload_sweeps(C, L, sc, SUB_A))) return st;
+        // a red and a black half-sweep, as a sweep runs them (each reads what
+        // the other wrote, with the L2 traffic of a real sweep)
         const double t = tune_time(C, [&] {
-          launch(k_rbgs<T, false>, dim3(L.n_sweep[SUB_A]), cta, 0, s, L.tab.p, L.sweep[SUB_A].p, L.sfirst[SUB_A].p,
-                 V.act.p, 0, V.err.p);
+          for (int colour = 0; colour < 2; ++colour)
+            launch(k_rbgs<T, false>, dim3(L.n_sweep[SUB_A]), cta, 0, s, L.tab.p, L.sweep[SUB_A].p,
+                   L.sfirst[SUB_A].p, V.act.p, colour, V.err.p);
         });
         if (t < best) { best = t; bs = sc; }
       }
@@ -1516,8 +1652,9 @@ static int autotune_level(mf3d_ctx *C, View &V, int g, bool time_new) {
       if (g > 1 && cells >= (1LL << 16) && cells <= (1LL << 22)) {
         const int g2 = grid_of(L.small_items[SUB_A], kTile);
         const double ts = tune_time(C, [&] {
-          launch(k_rbgs_small<T, false>, g2, kTile, 0, s, L.tab.p, L.spre[SUB_A].p, L.list[SUB_A].p, L.n_list[SUB_A],
-                 V.act.p, 0);
+          for (int colour = 0; colour < 2; ++colour)
+            launch(k_rbgs_small<T, false>, g2, kTile, 0, s, L.tab.p, L.spre[SUB_A].p, L.list[SUB_A].p,
+                   L.n_list[SUB_A], V.act.p, colour);
         });
         L.small = ts < best ? 1 : 0;
       }
@@ -1613,25 +1750,63 @@ static int autotune_view(mf3d_ctx *C, View &V, bool time_new) {
 
 // A field exchange copy map (k_fx_stage + k_fx_apply); returns the launches.
 static int field_exchange(mf3d_ctx *C, View &V, const FxCopy *pairs, long long n, long long nstaged,
-                          const int *only) {
+                          const int *only, const double *prev = nullptr) {
   if (!n) return 0;
   if (nstaged)
-    launch(k_fx_stage, grid_of(nstaged, kTile), kTile, 0, C->stream, V.df.p, pairs, nstaged, only, V.fx_stage.p);
-  launch(k_fx_apply, grid_of(n, kTile), kTile, 0, C->stream, V.df.p, pairs, n, nstaged, only, V.fx_stage.p);
+    launch(k_fx_stage, grid_of(nstaged, kTile), kTile, 0, C->stream, V.df.p, pairs, nstaged, only, V.fx_stage.p,
+           prev);
+  launch(k_fx_apply, grid_of(n, kTile), kTile, 0, C->stream, V.df.p, pairs, n, nstaged, only, V.fx_stage.p, prev);
   return nstaged ? 2 : 1;
+}
+
+// exchange(4) + pbound after p += pp: the whole copy map where the view has
+// one (every ghost the reference writes), else the face ghosts calvel reads.
+static void p_exchange(mf3d_ctx *C, View &V, const int *act) {
+  if (V.nfx_p) {
+    C->launches += field_exchange(C, V, V.fx_p, V.nfx_p, V.nsfx_p, act);
+  } else {
+    launch(k_p_faces, V.n_faces, kTile, 0, C->stream, V.df.p, V.t_faces.p, act);
+    ++C->launches;
+  }
+}
+
+// At a calvel point of the fused path (the initial calvel, each outer
+// iteration), the chained ghosts of exchange(1..3): k_fx_evolve + the
+// sub-map (see k_fx_evolve).  Nothing when the layout has no such chains.
+static void field_evolve(mf3d_ctx *C, View &V, const int *act) {
+  if (V.fx_per_iteration) return;
+  const long long n1 = V.nfxe_cells + V.nfxe_chain + V.nsfxe_sub;
+  if (n1) {
+    launch(k_fx_evolve, grid_of(n1, kTile), kTile, 0, C->stream, V.df.p, V.ds.p, act, V.fxe_cells, V.nfxe_cells,
+           V.fxe_chain, V.nfxe_chain, V.fx_prev.p, V.fxe_sub, V.nsfxe_sub, V.fx_stage.p);
+    ++C->launches;
+  }
+  if (V.nfxe_sub) {
+    launch(k_fx_apply, grid_of(V.nfxe_sub, kTile), kTile, 0, C->stream, V.df.p, V.fxe_sub, V.nfxe_sub, V.nsfxe_sub,
+           act, V.fx_stage.p, (const double *)nullptr);
+    ++C->launches;
+  }
 }
 
 // Fused calvel + calmas over the view (the TMA-staged kernel when the bound
 // fields admit it).
 template <typename T>
-static void calvel_calmas(mf3d_ctx *C, View &V, const int *act, unsigned long long *slot, int write_su) {
+static void calvel_calmas(mf3d_ctx *C, View &V, const int *act, unsigned long long *slot, int write_su,
+                          bool exchange = true) {
   if (C->prm.differencing == 2) {
     // the 4th-order divergence reads two face layers past the cell: calvel,
-    // its exchange(1..3) and calmas in the reference's order
+    // its exchange(1..3) and calmas in the reference's order (the whole
+    // exchange where the view has its copy map; `exchange` false when the
+    // velocities are already this calvel point's, exchanged)
     launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, C->stream, V.df.p, V.t_int.p, V.ds.p, act);
-    launch(k_vel_faces, V.n_vfaces, kTile, 0, C->stream, V.df.p, V.t_vfaces.p, act, C->prm.pl_ex);
+    ++C->launches;
+    if (exchange && V.nfx_uvw) {
+      C->launches += field_exchange(C, V, V.fx_uvw, V.nfx_uvw, V.nsfx_uvw, act);
+    } else if (exchange) {
+      launch(k_vel_faces, V.n_vfaces, kTile, 0, C->stream, V.df.p, V.t_vfaces.p, act, C->prm.pl_ex);
+      ++C->launches;
+    }
     launch(k_calmas4<T>, V.n_int, dim3(RW_TX, RW_RJ), 0, C->stream, V.df.p, V.t_int.p, V.ds.p, act, slot, write_su);
-    C->launches += 2;
     return;
   }
   if (C->prm.lsm) {
@@ -1663,16 +1838,14 @@ static void iteration_body(mf3d_ctx *C, View &V, int loop_graph) {
   cudaStream_t s = C->stream;
   vcycle<T>(C, V);
   launch(k_add_correction<T>, V.n_pairs, kTile, 0, s, V.df.p, V.t_pairs.p, V.act.p, V.pairs_kch);
-  // exchange(4) + pbound: the whole copy map where the view has one (every
-  // ghost the reference writes), else the face ghosts that calvel reads
-  if (V.nfx_p) C->launches += field_exchange(C, V, V.fx_p, V.nfx_p, V.nsfx_p, V.act.p) - 1;
-  else launch(k_p_faces, V.n_faces, kTile, 0, s, V.df.p, V.t_faces.p, V.act.p);
+  p_exchange(C, V, V.act.p);
   prof_begin(C, MF3D_PROF_CALMAS, (double)V.n_l1 * (4 * sizeof(double) + sizeof(T)));  // p, u*, v*, w* in; su out
   calvel_calmas<T>(C, V, V.act.p, V.rmax.p, 0);
   prof_end(C, MF3D_PROF_CALMAS);
+  field_evolve(C, V, V.act.p);
   launch(k_iter_end, 1, 256, 0, s, V.ds.p, (int)V.dom.size(), V.rmax.p, V.hist.p, V.hcap, V.act.p, V.cond,
                                loop_graph, V.budget.p);
-  C->launches += 4;
+  C->launches += 3;
 }
 
 template <typename T>
@@ -1844,9 +2017,12 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
     if (C->prm.mg_itrsch == 2) tdma_factors(C, V);
   }
   launch(k_face_planes, V.n_planes, kTile, 0, s, V.df.p, V.t_planes.p, C->walls_given ? 1 : 0);
-  // the 4th-order calmas reads ghost faces of u, v, w from the first pass on
-  if (C->wait_side && C->prm.differencing == 2) CK(cudaStreamWaitEvent(s, C->ev_side, 0));
+  // the 4th-order calmas, and the chained ghosts of the exchange, read the
+  // caller's u, v, w from the first calvel point on
+  if (C->wait_side && (C->prm.differencing == 2 || V.nfxe_chain + V.nfxe_sub))
+    CK(cudaStreamWaitEvent(s, C->ev_side, 0));
   calvel_calmas<T>(C, V, V.ones.p, V.rmax.p, 0);
+  field_evolve(C, V, V.ones.p);
   launch(k_dom_init, 1, 256, 0, s, V.ds.p, nd, V.rmax.p, V.act.p);
   C->launches += 3;
   return MF3D_OK;
@@ -1896,17 +2072,19 @@ static int solve_end(mf3d_ctx *C, View &V) {
   bool want_su = false;
   for (auto &F : V.hf) want_su |= F.su != nullptr;
   if (want_su) {
-    calvel_calmas<T>(C, V, V.ones.p, V.rmax_scratch.p, 1);
+    calvel_calmas<T>(C, V, V.ones.p, V.rmax_scratch.p, 1, false);
     ++C->launches;
   }
   if (C->wait_side) CK(cudaStreamWaitEvent(s, C->ev_side, 0));  // the host entry's u, v, w
   launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, nullptr);
   C->launches += 1;
-  // exchange(1..3) of the final calvel (press.for:196-198): the copy map of
-  // every ghost it writes where the view has one; else the full periodic
-  // planes (bounds mode) and the face ghosts
+  // exchange(1..3) of the last calvel (press.for:196-198): the copy map of
+  // every ghost it writes where the view has one, chained sources from
+  // their state before that exchange (the 4th-order path has exchanged
+  // already); else the full periodic planes (bounds mode) and the face ghosts
   if (V.nfx_uvw) {
-    C->launches += field_exchange(C, V, V.fx_uvw, V.nfx_uvw, V.nsfx_uvw, nullptr);
+    if (!V.fx_per_iteration)
+      C->launches += field_exchange(C, V, V.fx_uvw, V.nfx_uvw, V.nsfx_uvw, nullptr, V.fx_prev.p);
   } else {
     if (C->prm.bounds) bc_walks(C, V);
     launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
@@ -2224,7 +2402,7 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   C->doms.emplace_back(new DomainStore());
   C->coarse64 = C->elem == 4 && prm->ngrid > 1;
   if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, C->coarse64 ? 8 : C->elem, prm->pl,
-                         C->stream, prm->lsm != 0, prm->bounds != 0, prm->pl_ex)))
+                         C->stream, prm->lsm != 0, prm->bounds != 0, prm->pl_ex, prm->differencing == 2)))
     return st;
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
@@ -2608,9 +2786,16 @@ int mf3d_calvel_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double
   launch(k_calvel, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, V.ds.p, nullptr);
   ++C->launches;
   // exchange(1..3) (press.for:196-198): every ghost it writes, edges and
-  // corners included, which the next predictor stage reads
+  // corners included, which the next predictor stage reads; its chained
+  // sources are the caller's ghosts as they stand (saved first)
   if (V.nfx_uvw) {
-    C->launches += field_exchange(C, V, V.fx_uvw, V.nfx_uvw, V.nsfx_uvw, nullptr);
+    if (V.nfxe_chain && !V.fx_per_iteration) {
+      launch(k_fx_evolve, grid_of(V.nfxe_chain, kTile), kTile, 0, s, V.df.p, V.ds.p, (const int *)nullptr,
+             V.fxe_cells, 0LL, V.fxe_chain, V.nfxe_chain, V.fx_prev.p, V.fxe_sub, 0LL, V.fx_stage.p);
+      ++C->launches;
+    }
+    C->launches += field_exchange(C, V, V.fx_uvw, V.nfx_uvw, V.nsfx_uvw, nullptr,
+                                  V.fx_per_iteration ? nullptr : V.fx_prev.p);
   } else {
     if (C->prm.bounds) bc_walks(C, V);  // the full periodic planes of exchange(1..3)
     launch(k_vel_faces, V.n_vfaces, kTile, 0, s, V.df.p, V.t_vfaces.p, nullptr, C->prm.pl_ex);
@@ -2658,6 +2843,17 @@ int mf3d_mgkcyc_device_noalloc(mf3d_ctx *C, double *const *su, double *const *pp
 }
 
 long long mf3d_last_launch_count(const mf3d_ctx *C) { return C ? C->launches : 0; }
+
+int mf3d_tuning(const mf3d_ctx *C, int level, int *sweep_schedule, int *small_sweep, int *restrict_planes,
+                int *cluster_ctas) {
+  if (!C || !C->view || level < 1 || level > C->view->Lmax) { mf3d::set_error("mf3d_tuning: bad arguments"); return MF3D_E_INVALID; }
+  const mf3d::ViewLevel &L = C->view->lv[level];
+  if (sweep_schedule) *sweep_schedule = L.sched;
+  if (small_sweep) *small_sweep = L.small;
+  if (restrict_planes) *restrict_planes = level > 1 ? L.rtma_kch : 0;
+  if (cluster_ctas) *cluster_ctas = C->prm.mg_itrsch == 2 ? L.td_cl : C->prm.mg_itrsch == 1 ? L.lx_cl : 1;
+  return MF3D_OK;
+}
 
 int mf3d_test_fail_alloc(long long after) {
   mf3d::g_fail_alloc_countdown.store(after < 0 ? -1 : after);

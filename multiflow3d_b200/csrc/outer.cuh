@@ -260,24 +260,30 @@ struct FxCopy {
 __device__ __forceinline__ double *fx_field(const BlkFld &F, int comp) {
   return comp == 0 ? F.u : comp == 1 ? F.v : comp == 2 ? F.w : F.p;
 }
+// the pre-exchange value a pair copies: from `prev` (slot soff) when comp
+// carries bit 8 (a chained source, saved by k_fx_evolve), else the field
+__device__ __forceinline__ double fx_source(const BlkFld *fl, const FxCopy &x, const double *prev) {
+  return (x.comp & 8) ? prev[x.soff] : fx_field(fl[x.sblk], x.comp & 7)[x.soff];
+}
 __global__ void k_fx_stage(const BlkFld *__restrict__ fl, const FxCopy *__restrict__ c, long long nstaged,
-                           const int *__restrict__ only, double *__restrict__ buf) {
+                           const int *__restrict__ only, double *__restrict__ buf, const double *__restrict__ prev) {
   pdl_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nstaged) return;
   const FxCopy x = c[t];
   if (only && !only[fl[x.dblk].dom]) return;
-  buf[t] = fx_field(fl[x.sblk], x.comp)[x.soff];
+  buf[t] = fx_source(fl, x, prev);
 }
 __global__ void k_fx_apply(const BlkFld *__restrict__ fl, const FxCopy *__restrict__ c, long long n,
-                           long long nstaged, const int *__restrict__ only, const double *__restrict__ buf) {
+                           long long nstaged, const int *__restrict__ only, const double *__restrict__ buf,
+                           const double *__restrict__ prev) {
   pdl_wait();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   const FxCopy x = c[t];
   if (only && !only[fl[x.dblk].dom]) return;
-  const double v = t < nstaged ? buf[t] : fx_field(fl[x.sblk], x.comp)[x.soff];
-  fx_field(fl[x.dblk], x.comp)[x.doff] = v;
+  const double v = t < nstaged ? buf[t] : fx_source(fl, x, prev);
+  fx_field(fl[x.dblk], x.comp & 7)[x.doff] = v;
 }
 
 // Face planes used by the fused calvel/calmas kernel, filled once per solve:
@@ -847,6 +853,23 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const Blk
   }
 }
 
+// calvel (press.for:139-198) of one face: component comp (0 u, 1 v, 2 w) at
+// level-1 cell (i, j, k), when calvel writes it (isu..ieu etc.: one face short
+// at a high wall).  Under L_LSM the face density divides last (:152-190).
+__device__ __forceinline__ void calvel_face(const BlkFld &F, int comp, int i, int j, int k, double dta) {
+  const long long c = fidx(F, i, j, k);
+  const long long st = comp == 0 ? 1 : comp == 1 ? (long long)F.ti : (long long)F.ti * F.tj;
+  const int a = comp == 0 ? i : comp == 1 ? j : k;
+  const int n = comp == 0 ? F.nx : comp == 1 ? F.ny : F.nz;
+  if (a == n && F.wall[2 * comp + 1]) return;
+  const double *__restrict__ p = F.p;
+  const double *S = comp == 0 ? F.ustar : comp == 1 ? F.vstar : F.wstar;
+  double *O = comp == 0 ? F.u : comp == 1 ? F.v : F.w;
+  const double *__restrict__ D = F.dens;
+  if (D) O[c] = (S[c] - xdiv(dta * (p[c + st] - p[c]), F.df[comp][a], F.pinv[comp]) / (0.5 * (D[c] + D[c + st])));
+  else O[c] = (S[c] - xdiv(dta * (p[c + st] - p[c]), F.df[comp][a], F.pinv[comp]));
+}
+
 // Final calvel (press.for:139-198): u, v, w on the faces calvel writes
 // (isu..ieu etc., one face short at a high wall), from the final p.
 // `only` (may be null): domains to update, others are left as they are.
@@ -857,28 +880,60 @@ __global__ void __launch_bounds__(RW_TX *RW_RJ) k_calvel(const BlkFld *__restric
   const BlkFld &F = fl[t.blk];
   if (only && !only[F.dom]) return;
   const double dt = ds[F.dom].dt, alfapr = ds[F.dom].alfapr;
-  const int nx = F.nx, ny = F.ny;
   const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
-  if (i > nx || j > ny) return;
+  if (i > F.nx || j > F.ny) return;
   const double dta = dt * alfapr;
-  const long long sy = F.ti, sz = (long long)F.ti * F.tj;
-  const double *__restrict__ p = F.p;
   const int k1 = min(t.k0 + RW_KCH - 1, F.nz);
-  const double *__restrict__ D = F.dens;
   for (int k = t.k0; k <= k1; ++k) {
-    const long long c = fidx(F, i, j, k);
-    if (D) {  // L_LSM (press.for:152-190): the face density divides last
-      if (!(i == nx && F.wall[1]))
-        F.u[c] = (F.ustar[c] - xdiv(dta * (p[c + 1] - p[c]), F.df[0][i], F.pinv[0]) / (0.5 * (D[c] + D[c + 1])));
-      if (!(j == ny && F.wall[3]))
-        F.v[c] = (F.vstar[c] - xdiv(dta * (p[c + sy] - p[c]), F.df[1][j], F.pinv[1]) / (0.5 * (D[c] + D[c + sy])));
-      if (!(k == F.nz && F.wall[5]))
-        F.w[c] = (F.wstar[c] - xdiv(dta * (p[c + sz] - p[c]), F.df[2][k], F.pinv[2]) / (0.5 * (D[c] + D[c + sz])));
-      continue;
-    }
-    if (!(i == nx && F.wall[1])) F.u[c] = (F.ustar[c] - xdiv(dta * (p[c + 1] - p[c]), F.df[0][i], F.pinv[0]));
-    if (!(j == ny && F.wall[3])) F.v[c] = (F.vstar[c] - xdiv(dta * (p[c + sy] - p[c]), F.df[1][j], F.pinv[1]));
-    if (!(k == F.nz && F.wall[5])) F.w[c] = (F.wstar[c] - xdiv(dta * (p[c + sz] - p[c]), F.df[2][k], F.pinv[2]));
+    calvel_face(F, 0, i, j, k, dta);
+    calvel_face(F, 1, i, j, k, dta);
+    calvel_face(F, 2, i, j, k, dta);
+  }
+}
+
+// exchange(1..3) across outer iterations.  The reference runs calvel and
+// its exchange in every outer iteration; some ghost cells of an exchange
+// take a ghost cell of the state before it (exchange_bc copies whole ghost-
+// inclusive planes, corner cubes reach a neighbour's ghost layer), so their
+// final values come from earlier iterations' exchanges.  The library
+// evolves exactly those cells: the closure C of ghost cells such chains
+// reach is re-exchanged at every calvel point (the initial calvel and each
+// outer iteration).  k_fx_evolve (i) forms calvel at the interior faces the
+// sub-map of C reads (`cells`: block, component, i, j, k; u, v, w written
+// there as calvel writes them - the final calvel rewrites them with the same
+// values), (ii) saves the pre-exchange value of every chained source into
+// `prev`, and (iii) stages the sources of the sub-map's staged pairs; then
+// k_fx_apply writes the sub-map.  The final exchange reads chained sources
+// from `prev` (FxCopy comp bit 8).  Reads in k_fx_evolve touch ghost cells
+// only, writes interior cells only, so the three parts do not race.
+struct FxCell {
+  int blk, comp, i, j, k;
+};
+__global__ void k_fx_evolve(const BlkFld *__restrict__ fl, const DomState *__restrict__ ds,
+                            const int *__restrict__ only, const FxCell *__restrict__ cells, long long ncell,
+                            const FxCopy *__restrict__ chain, long long nchain, double *__restrict__ prev,
+                            const FxCopy *__restrict__ sub, long long nstaged, double *__restrict__ buf) {
+  pdl_wait();
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < ncell) {
+    const FxCell c = cells[t];
+    const BlkFld &F = fl[c.blk];
+    if (only && !only[F.dom]) return;
+    calvel_face(F, c.comp, c.i, c.j, c.k, ds[F.dom].dt * ds[F.dom].alfapr);
+    return;
+  }
+  t -= ncell;
+  if (t < nchain) {  // chain[t]: src = the chained source cell, soff its prev slot
+    const FxCopy x = chain[t];
+    if (only && !only[fl[x.sblk].dom]) return;
+    prev[t] = fx_field(fl[x.sblk], x.comp & 7)[x.doff];
+    return;
+  }
+  t -= nchain;
+  if (t < nstaged) {
+    const FxCopy x = sub[t];
+    if (only && !only[fl[x.dblk].dom]) return;
+    buf[t] = fx_field(fl[x.sblk], x.comp & 7)[x.soff];
   }
 }
 

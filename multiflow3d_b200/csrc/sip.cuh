@@ -408,10 +408,11 @@ static int solve_view_sip(mf3d_ctx *C, View &V, const double *dt, const double *
     sweeps += n;
     ++calls;
     launch(k_add_correction<double>, V.n_pairs, kTile, 0, s, V.df.p, V.t_pairs.p, V.act.p, V.pairs_kch);
-    launch(k_p_faces, V.n_faces, kTile, 0, s, V.df.p, V.t_faces.p, V.act.p);
+    p_exchange(C, V, V.act.p);
     CK(cudaMemsetAsync(V.rmax.p, 0, sizeof(unsigned long long), s));
     calvel_calmas<double>(C, V, V.act.p, V.rmax.p, 0);
-    C->launches += 3;
+    field_evolve(C, V, V.act.p);
+    C->launches += 2;
     if (iter == maxcy) break;  // the reference runs no calmas after its last round
     unsigned long long bits = 0;
     CK(cudaMemcpyAsync(&bits, V.rmax.p, sizeof bits, cudaMemcpyDeviceToHost, s));

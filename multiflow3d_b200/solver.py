@@ -101,6 +101,12 @@ class Projection:
     def launches(self) -> int:
         return int(self.lib.mf3d_last_launch_count(self.ctx))
 
+    def tuning(self, level: int) -> dict:
+        """Launch shapes chosen for one level (mf3d_tuning)."""
+        v = [C.c_int() for _ in range(4)]
+        abi.check(self.lib, self.lib.mf3d_tuning(self.ctx, level, *[C.byref(x) for x in v]), "mf3d_tuning")
+        return dict(zip(("sweep_schedule", "small_sweep", "restrict_planes", "cluster_ctas"), (x.value for x in v)))
+
 
 def _dev_fields(blocks):
     arr = (abi.Fields * len(blocks))()
