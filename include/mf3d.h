@@ -222,12 +222,15 @@ typedef struct mf3d_rk_fields {
   const double *vis;
 } mf3d_rk_fields;
 
-/* One Runge-Kutta stage of the velocity predictor with 2nd-order central
- * differences and explicit diffusion (flosol.for:151-172 with
- * differencing = 1 and diff_sch = 3): rungek_conv2nd (rungek.for:314-412) -
- * boundu, the u predictor, boundv, the v predictor, boundw, the w predictor
- * - then rungek_diff2nd (rungek.for:584-779), the reference's branch without
- * L_LSM, immersed boundaries or wall functions.  In: u, v, w (their ghosts
+/* One Runge-Kutta stage of the velocity predictor with central differences
+ * and explicit diffusion (flosol.for:151-172 with diff_sch = 3), by the
+ * context's `differencing`: 1 - rungek_conv2nd (rungek.for:314-412) then
+ * rungek_diff2nd (rungek.for:584-779); 2 - rungek_conv4th (rungek.for:2-212)
+ * then rungek_diff4th (rungek.for:214-312), which read three ghost layers
+ * (pl >= 3, else MF3D_E_INVALID).  Each convection is boundu, the u
+ * predictor, boundv, the v predictor, boundw, the w predictor; the
+ * reference's branch without L_LSM, immersed boundaries or wall functions.
+ * differencing = 3 (WENO convection) returns MF3D_E_UNSUPPORTED.  In: u, v, w (their ghosts
  * are refreshed by boundu/v/w, as in the reference), `rk`; out: ustar,
  * vstar, wstar over the faces calvel later reads (isu..ieu etc.).  `p` must
  * be set as for the projection (not read here; su and dens may be NULL).
@@ -246,10 +249,10 @@ int mf3d_rungek_2nd_device(mf3d_ctx *ctx, const mf3d_fields *fields, const mf3d_
 
 /* calvel alone (press.for:139-198, flosol.for:171 between Runge-Kutta
  * stages): u, v, w from ustar, vstar, wstar and p over the faces calvel
- * writes, then the face part of its exchange(1..3) - with bounds = 1 also
- * the full periodic planes - as mf3d_newsolv_mg_device leaves them after
- * its final calvel, without boundu/v/w.  Device pointers; mf3d_create
- * contexts, FP64, no lsm. */
+ * writes, then its exchange(1..3) (exchange.for:2-23: the periodic planes,
+ * the face layers and the corner and edge ghosts of exchange_smlvl), from
+ * the ghosts as they stand, without boundu/v/w.  Device pointers;
+ * mf3d_create contexts, FP64, no lsm. */
 int mf3d_calvel_device(mf3d_ctx *ctx, const mf3d_fields *fields, double dt, double alfapr);
 
 /* ---------------------------------------------------------------------- */

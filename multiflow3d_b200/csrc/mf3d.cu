@@ -29,6 +29,7 @@
 #include <cudaTypedefs.h>
 
 #include "kernels.cuh"
+#include "coarse.cuh"
 #include "mf3d_internal.h"
 #include "outer.cuh"
 
@@ -816,6 +817,13 @@ struct View {
   long long nfxe_sub = 0, nsfxe_sub = 0, nfxe_chain = 0, nfxe_cells = 0;
   bool fx_per_iteration = false;      // u, v, w exchanged whole at every calvel point (4th-order calmas)
   DevBuf<double> fx_stage, fx_prev;   // staged sources; chained sources before the last exchange
+  // the coarse end of the red-black V-cycle in one cluster launch (k_coarse_cycle):
+  // levels cc_g0..Lmax, 0 = off
+  int cc_g0 = 0;
+  size_t cc_smem = 0;
+  CcArgs cc_args;
+  DevBuf<CcHalo> cc_halo;
+  DevBuf<HaloCopy> cc_pairs;
   DevBuf<DomState> ds;
   DevBuf<int> act, ones;
   DevBuf<int> err;                    // device error code (a TMA wait that gave up)
@@ -930,12 +938,15 @@ constexpr long long kSmallLevelCells = 1ll << 19;
 //   1  the same over twice as many CTAs (two waves);
 //   2  each column cut into c equal runs, c = resident CTAs / columns (at
 //      least 1): no run crosses a column, at most one wave;
-//   3  the same with c + 1 runs per column.
+//   3  the same with c + 1 runs per column;
+//   4  runs of kch planes in several waves, kch in {2, 4, 8, 16, 32} the
+//      one whose estimated time ceil(CTAs / resident) * (kch + ring fill) is
+//      least (concurrent CTAs cover neighbouring columns of the same planes).
 // Runs are at least kMinRun planes (shorter ones would be mostly ring fill)
 // and at most RB_KMAX.  Returns the CTA count; first[c] .. first[c+1]-1 are
-// CTA c's segments.
+// CTA c's segments; the CTAs run columns in order of their first plane.
 constexpr long long kMinRun = 4;
-constexpr int kSweepSchedules = 4;
+constexpr int kSweepSchedules = 5;
 static int sweep_segments(const mf3d_ctx *C, const std::vector<BlkLev> &tab, const std::vector<int> &blocks,
                           std::vector<RbSeg> &segs, std::vector<int> &first, int sched = 0) {
   segs.clear();
@@ -950,13 +961,32 @@ static int sweep_segments(const mf3d_ctx *C, const std::vector<BlkLev> &tab, con
   if (planes == 0) return 0;
   const long long resident = (long long)C->nsm * C->sweep_occ;
   if (sched >= 2) {
-    const long long c = std::max(1LL, resident / columns) + (sched == 3 ? 1 : 0);
+    // per block, runs of `run` planes; CTAs ordered plane run first, so the
+    // CTAs resident together share planes (their halo rows meet in L2)
+    auto run_of = [&](const BlkLev &B) -> long long {
+      if (sched == 4) return 0;
+      const long long c = std::max(1LL, resident / columns) + (sched == 3 ? 1 : 0);
+      return std::min<long long>(RB_KMAX, std::max(kMinRun, (B.nz + c - 1) / c));
+    };
+    long long kch4 = 2;
+    if (sched == 4) {
+      double best = 1e300;
+      for (long long kc : {2LL, 4LL, 8LL, 16LL, (long long)std::min(32, RB_KMAX)}) {
+        long long n = 0;
+        for (int b : blocks) {
+          const BlkLev &B = tab[b];
+          n += (long long)((B.nx + 1) / 2 + RB_TX - 1) / RB_TX * ((B.ny + RB_RJ - 1) / RB_RJ) * ((B.nz + kc - 1) / kc);
+        }
+        const double cost = (double)((n + resident - 1) / resident) * (kc + RB_PD);
+        if (cost <= best) { best = cost; kch4 = kc; }
+      }
+    }
     for (int b : blocks) {
       const BlkLev &B = tab[b];
-      const long long run = std::min<long long>(RB_KMAX, std::max(kMinRun, (B.nz + c - 1) / c));
-      for (int j0 = 1; j0 <= B.ny; j0 += RB_RJ)
-        for (int q0 = 0; q0 < (B.nx + 1) / 2; q0 += RB_TX)
-          for (int k = 1; k <= B.nz; k += (int)run) {
+      const long long run = sched == 4 ? kch4 : run_of(B);
+      for (int k = 1; k <= B.nz; k += (int)run)
+        for (int j0 = 1; j0 <= B.ny; j0 += RB_RJ)
+          for (int q0 = 0; q0 < (B.nx + 1) / 2; q0 += RB_TX) {
             segs.push_back(RbSeg{b, k, (int)std::min<long long>(k + run - 1, B.nz), j0, q0, 0, 0, 0});
             first.push_back((int)segs.size());
           }
@@ -1133,6 +1163,97 @@ static void tdma_factors(mf3d_ctx *C, View &V) {
       ++C->launches;
     }
   }
+}
+
+// The coarse levels of a red-black V-cycle as one cluster launch
+// (k_coarse_cycle): a view over one domain of at most CC_MAX_BLOCKS blocks,
+// with ir >= 1; g0 = the finest level from which every block's levels (phi
+// and rhs) and halo staging fit one CTA's shared memory.  The domain's halo
+// pairs of those levels are regrouped by destination block.
+// MF3D_COARSE_CLUSTER=0 turns it off.
+constexpr size_t kCcSmemCap = 200 * 1024;
+static int coarse_cycle_plan(mf3d_ctx *C, View &V) {
+  V.cc_g0 = 0;
+  const char *e = std::getenv("MF3D_COARSE_CLUSTER");
+  if (e && e[0] == '0') return MF3D_OK;
+  const int nb = (int)V.blk.size();
+  if (V.dom.size() != 1 || C->prm.mg_itrsch != 3 || C->prm.lsm || C->prm.irestr < 1 || nb > CC_MAX_BLOCKS ||
+      V.Lmax < 3)
+    return MF3D_OK;
+  const DomainStore &D = *V.dom[0];
+  const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
+  auto elem_of = [&](int g) { return (C->elem == 8 || g >= Lc) ? 8 : 4; };
+  int g0 = 0;
+  size_t smem = 0;
+  int bufn = 0;
+  for (int g = 2; g < V.Lmax && !g0; ++g) {
+    if (V.Lmax - g + 1 > CC_MAX_LEVELS) continue;
+    int bn = 0;
+    for (int l = g; l <= V.Lmax; ++l) {
+      std::vector<int> cnt(nb, 0);
+      for (const auto &h : D.halo[l]) cnt[h.dblk]++;
+      for (int c : cnt) bn = std::max(bn, c);
+    }
+    size_t worst = 0;
+    for (int b = 0; b < nb; ++b) {
+      long long bytes = 0;
+      for (int l = g; l <= V.Lmax; ++l) bytes += 2 * cc_level_bytes(V.lv[l].htab[b], elem_of(l));
+      worst = std::max(worst, (size_t)((bytes + 15) / 16 * 16 + (long long)bn * 8));
+    }
+    if (worst <= kCcSmemCap) { g0 = g; smem = worst; bufn = bn; }
+  }
+  if (!g0) return MF3D_OK;
+  void (*kern)(const CcArgs, const int *) = C->elem == 8 ? k_coarse_cycle<double> : k_coarse_cycle<float>;
+  // the device holds such a cluster at all (else the launch path stays)
+  {
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = (unsigned)nb;
+    at.val.clusterDim.y = at.val.clusterDim.z = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)nb);
+    cfg.blockDim = dim3(CC_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg) != cudaSuccess || ncl < 1) {
+      cudaGetLastError();
+      return MF3D_OK;
+    }
+  }
+  // halo pairs of the held levels grouped by destination block
+  std::vector<HaloCopy> pairs;
+  std::vector<CcHalo> hs((size_t)(V.Lmax - g0 + 1) * nb);
+  std::vector<long long> start(hs.size());
+  for (int l = g0; l <= V.Lmax; ++l)
+    for (int b = 0; b < nb; ++b) {
+      start[(size_t)(l - g0) * nb + b] = (long long)pairs.size();
+      for (const auto &h : D.halo[l])
+        if (h.dblk == b) pairs.push_back(HaloCopy{h.dblk, h.doff, h.sblk, h.soff});
+      hs[(size_t)(l - g0) * nb + b].n = (int)(pairs.size() - start[(size_t)(l - g0) * nb + b]);
+    }
+  int st;
+  if ((st = V.cc_pairs.upload(pairs, C->stream))) return st;
+  for (size_t q = 0; q < hs.size(); ++q) hs[q].pairs = V.cc_pairs.p + start[q];
+  if ((st = V.cc_halo.upload(hs, C->stream))) return st;
+  CcArgs &a = V.cc_args;
+  std::memset(&a, 0, sizeof a);
+  for (int l = g0; l <= V.Lmax; ++l) a.tab[l - g0] = V.lv[l].tab.p;
+  a.halo = V.cc_halo.p;
+  a.blk0 = 0;
+  a.nb = nb;
+  a.nlev = V.Lmax - g0 + 1;
+  a.g0 = g0;
+  a.lc = Lc;
+  a.ir = C->prm.irestr;
+  a.ip = C->prm.iproln;
+  a.dom = 0;
+  a.bufn = bufn;
+  V.cc_g0 = g0;
+  V.cc_smem = smem;
+  CK(cudaStreamSynchronize(C->stream));  // the host vectors are locals
+  return MF3D_OK;
 }
 
 // Build the launch tables of a view over `doms` (all of one precision).
@@ -1345,6 +1466,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       V.n_bcax[a] = (int)tb.size();
       if ((st = V.t_bcax[a].upload(tb, s))) return st;
     }
+  if ((st = coarse_cycle_plan(C, V))) return st;
   V.fx_uvw = V.fx_p = V.fxe_sub = V.fxe_chain = nullptr;
   V.fxe_cells = nullptr;
   V.nfx_uvw = V.nsfx_uvw = V.nfx_p = V.nsfx_p = 0;
@@ -1519,7 +1641,9 @@ static void vcycle(mf3d_ctx *C, View &V) {
   // with red-black pre-smoothing the restriction also forms the coarse
   // level's first (from-zero) red half-sweep
   const bool red_in_restr = sch == 3 && ir > 0;
-  for (int g = 1; g <= V.Lmax; ++g) {
+  // levels cc_g0.. run as one cluster launch (k_coarse_cycle) where planned
+  const int gtop = V.cc_g0 ? V.cc_g0 - 1 : V.Lmax;
+  for (int g = 1; g <= gtop; ++g) {
     relax_g(g, SUB_A, ir, sch == 3, g > 1 && red_in_restr);  // a level starts from zero (pp = 0; mgrestr)
     relax_g(g, SUB_C, ip, sch == 3 && ir == 0);
     if (g < V.Lmax) {
@@ -1527,7 +1651,12 @@ static void vcycle(mf3d_ctx *C, View &V) {
       else restr<T, T>(C, V, g);
     }
   }
-  for (int g = V.Lmax - 1; g >= 1; --g) {
+  if (V.cc_g0) {
+    launch_cl(k_coarse_cycle<T>, (int)V.blk.size(), CC_THREADS, V.cc_smem, C->stream, (int)V.blk.size(), V.cc_args,
+              (const int *)V.act.p);
+    ++C->launches;
+  }
+  for (int g = gtop - (V.cc_g0 ? 0 : 1); g >= 1; --g) {
     if (g + 1 >= Lc) corr<T, double>(C, V, g);
     else corr<T, T>(C, V, g);
     relax_g(g, SUB_D, ip, false);
@@ -2339,6 +2468,8 @@ static int ctx_init(mf3d_ctx *C, const mf3d_params *prm, bool nonblocking = fals
                           RsShape<float>::SMEM));
   CK(cudaFuncSetAttribute(k_restrict_tma<float, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                           RsShape<float>::SMEM));
+  CK(cudaFuncSetAttribute(k_coarse_cycle<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCcSmemCap));
+  CK(cudaFuncSetAttribute(k_coarse_cycle<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kCcSmemCap));
   if (int st = C->elem == 8 ? preload_vcycle_kernels<double>() : preload_vcycle_kernels<float>()) return st;
   return noalloc_tables(&C->noalloc_tab);
 }
@@ -2712,6 +2843,14 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
     set_error("mf3d_rungek_2nd_device: needs a context with bounds = 1, FP64 and no lsm");
     return MF3D_E_UNSUPPORTED;
   }
+  if (C->prm.differencing == 3) {
+    set_error("mf3d_rungek_2nd_device: WENO convection (differencing = 3) is not restated");
+    return MF3D_E_UNSUPPORTED;
+  }
+  if (C->prm.differencing == 2 && C->prm.pl < 3) {
+    set_error("mf3d_rungek_2nd_device: the 4th-order stage reads three ghost layers (pl >= 3)");
+    return MF3D_E_INVALID;
+  }
   View &V = *C->view;
   for (size_t b = 0; b < V.blk.size(); ++b) {
     const mf3d_block_desc &d = V.blk[b]->d;
@@ -2758,7 +2897,10 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
   for (int comp = 0; comp < 3; ++comp) {
     bc_walks(C, V, comp);
     bound_faces(C, V, alfabc, comp, dt, alfapr);
-    launch(k_rk2nd, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, comp, dt, alfapr, pressureforce, forcn);
+    if (C->prm.differencing == 2)
+      launch(k_rk4th, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, comp, dt, alfapr, pressureforce, forcn);
+    else
+      launch(k_rk2nd, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, comp, dt, alfapr, pressureforce, forcn);
     ++C->launches;
   }
   const cudaError_t e = cudaStreamSynchronize(s);

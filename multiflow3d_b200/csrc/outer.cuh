@@ -1057,6 +1057,83 @@ __global__ void __launch_bounds__(RW_TX *RW_RJ) k_rk2nd(const BlkFld *__restrict
   }
 }
 
+// The same stage with differencing = 2: rungek_conv4th (rungek.for:2-212)
+// and rungek_diff4th (rungek.for:214-312) for component `comp` (axis a):
+//   star = (oo - dt*alfapr*(t_x + t_y + t_z)), t_a = (-s(+2) + 27 s(+1) -
+//     27 s(0) + s(-1))/(24 h_a) with s(m) the square of the component
+//     interpolated to the cell centre m - 1/2 along a, and for b != a
+//     t_b = (-P(+1) + 27 P(0) - 27 P(-1) + P(-2))/(24 h_b), P(m) = the
+//     component interpolated along b times the b-velocity interpolated along
+//     a, at b-offset m - each interpolant (-f(+1) + 9 f(0) + 9 f(-1) -
+//     f(-2))/16 as the reference writes them;
+//   star = (star + dt*alfapr*diff), diff = visc*(L_x + L_y + L_z),
+//     L_b = (-c(+2) + 16 c(+1) - 30 c + 16 c(-1) - c(-2))/(12 h_b^2), visc
+//     the viscosity of the face's own cell for u and of the cell past the
+//     face for v and w (rungek.for:230, 262, 290);
+//   u under pressureforce: star = star + dt*alfapr*forcn.
+// The stencils reach three cells each way (pl >= 3).
+__global__ void __launch_bounds__(RW_TX *RW_RJ) k_rk4th(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                                                        int comp, double dt, double alfapr, int pforce, double forcn) {
+  pdl_wait();
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i > comp_end(F, comp, 0) || j > comp_end(F, comp, 1)) return;
+  const int k1 = min(t.k0 + RW_KCH - 1, comp_end(F, comp, 2));
+  const long long st3[3] = {1, (long long)F.ti, (long long)F.ti * F.tj};
+  const double h[3] = {F.h[0][1], F.h[1][1], F.h[2][1]};
+  const double *vel[3] = {F.u, F.v, F.w};
+  const double *__restrict__ Cf = vel[comp];
+  const double *__restrict__ OO = F.oo[comp];
+  double *__restrict__ ST = comp == 0 ? F.ustar : comp == 1 ? F.vstar : F.wstar;
+  const long long sa = st3[comp];
+  // (-f(+1) + 9 f(0) + 9 f(-1) - f(-2)) / 16 along stride s, around element e
+  auto q4 = [](const double *f, long long e, long long s) {
+    return (-f[e + s] + 9.0 * f[e] + 9.0 * f[e - s] - f[e - 2 * s]) / 16.0;
+  };
+  auto d4 = [](double p1, double p0, double m1, double m2, double hh) {
+    return (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * hh);
+  };
+  for (int k = t.k0; k <= k1; ++k) {
+    const long long c = fidx(F, i, j, k);
+    double term[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      if (b == comp) {
+        double s4[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const double q = q4(Cf, c + (2 - m) * sa, sa);
+          s4[m] = q * q;
+        }
+        term[b] = d4(s4[0], s4[1], s4[2], s4[3], h[b]);
+      } else {
+        const long long sb = st3[b];
+        double p4[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const long long e = c + (1 - m) * sb;  // b-offset 1, 0, -1, -2
+          p4[m] = q4(Cf, e + sb, sb) * q4(vel[b], e + sa, sa);
+        }
+        term[b] = d4(p4[0], p4[1], p4[2], p4[3], h[b]);
+      }
+    }
+    double st = (OO[c] - dt * alfapr * (term[0] + term[1] + term[2]));
+    const double visc = F.vis[comp == 0 ? c : c + sa];
+    double lap[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      const long long sb = st3[b];
+      lap[b] = (-Cf[c + 2 * sb] + 16.0 * Cf[c + sb] - 30.0 * Cf[c] + 16.0 * Cf[c - sb] - Cf[c - 2 * sb]) /
+               (12.0 * (h[b] * h[b]));
+    }
+    const double diff = visc * (lap[0] + lap[1] + lap[2]);
+    st = (st + dt * alfapr * diff);
+    if (comp == 0 && pforce) st = st + dt * alfapr * forcn;
+    ST[c] = st;
+  }
+}
+
 // After the initial calvel/calmas (newsolv_mg.for:16-17): rmax0, the
 // absolute threshold, and which domains iterate at all.
 __global__ void k_dom_init(DomState *ds, int ndom, unsigned long long *rmax_slot, int *act) {

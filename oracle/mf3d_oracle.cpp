@@ -1117,6 +1117,103 @@ void rungek_2nd(Ctx &C, const double *const *uoo, const double *const *voo, cons
   });
 }
 
+/* One Runge-Kutta stage of rungek_conv4th (rungek.for:2-212) and
+ * rungek_diff4th (rungek.for:214-312) in the reference's order: boundu, the
+ * u loop, boundv, the v loop, boundw, the w loop; then the diffusion of u,
+ * v, w.  9.0, 16.0, 27.0, 24.0, 30.0, 12.0 are double (-fdefault-real-8);
+ * x**2 is x*x. */
+void rungek_4th(Ctx &C, const double *const *uoo, const double *const *voo, const double *const *woo,
+                const double *const *vis, bool pforce, double forcn) {
+  const double dt = C.dt, alfapr = C.alfapr;
+  for (int op = 1; op <= 3; ++op) {
+    bound(C, op);
+    par_blocks((int)C.b.size(), [&](int ib) { Blk &B = C.b[ib];
+      const double dx = B.d.dx, dy = B.d.dy, dz = B.d.dz;
+      double *st = op == 1 ? B.ustar : op == 2 ? B.vstar : B.wstar;
+      const double *oo = op == 1 ? uoo[ib] : op == 2 ? voo[ib] : woo[ib];
+      int is, ie, js, je, ks, ke;
+      franges(B, op, is, ie, js, je, ks, ke);
+      auto u = [&](int i, int j, int k) { return F(B, B.u, i, j, k); };
+      auto v = [&](int i, int j, int k) { return F(B, B.v, i, j, k); };
+      auto w = [&](int i, int j, int k) { return F(B, B.w, i, j, k); };
+      /* (-f(+1) + 9 f(0) + 9 f(-1) - f(-2)) / 16 */
+      auto q4 = [](double p1, double p0, double m1, double m2) { return (-p1 + 9.0 * p0 + 9.0 * m1 - m2) / 16.0; };
+      /* (-s(+1) + 27 s(0) - 27 s(-1) + s(-2)) / (24 h) */
+      auto d4 = [](double p1, double p0, double m1, double m2, double h) {
+        return (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * h);
+      };
+      for (int k = ks; k <= ke; ++k) for (int i = is; i <= ie; ++i) for (int j = js; j <= je; ++j) {
+        double t1, t2, t3;
+        if (op == 1) {
+          auto sx = [&](int ii) { double a = q4(u(ii + 1, j, k), u(ii, j, k), u(ii - 1, j, k), u(ii - 2, j, k)); return a * a; };
+          t1 = d4(sx(i + 2), sx(i + 1), sx(i), sx(i - 1), dx);  /* du2dx */
+          auto py = [&](int jj) {
+            return q4(u(i, jj + 2, k), u(i, jj + 1, k), u(i, jj, k), u(i, jj - 1, k)) *
+                   q4(v(i + 2, jj, k), v(i + 1, jj, k), v(i, jj, k), v(i - 1, jj, k));
+          };
+          t2 = d4(py(j + 1), py(j), py(j - 1), py(j - 2), dy);  /* duvdy */
+          auto pz = [&](int kk) {
+            return q4(u(i, j, kk + 2), u(i, j, kk + 1), u(i, j, kk), u(i, j, kk - 1)) *
+                   q4(w(i + 2, j, kk), w(i + 1, j, kk), w(i, j, kk), w(i - 1, j, kk));
+          };
+          t3 = d4(pz(k + 1), pz(k), pz(k - 1), pz(k - 2), dz);  /* duwdz */
+        } else if (op == 2) {
+          auto sy = [&](int jj) { double a = q4(v(i, jj + 1, k), v(i, jj, k), v(i, jj - 1, k), v(i, jj - 2, k)); return a * a; };
+          t2 = d4(sy(j + 2), sy(j + 1), sy(j), sy(j - 1), dy);  /* dv2dy */
+          auto px = [&](int ii) {
+            return q4(v(ii + 2, j, k), v(ii + 1, j, k), v(ii, j, k), v(ii - 1, j, k)) *
+                   q4(u(ii, j + 2, k), u(ii, j + 1, k), u(ii, j, k), u(ii, j - 1, k));
+          };
+          t1 = d4(px(i + 1), px(i), px(i - 1), px(i - 2), dx);  /* duvdx */
+          auto pz = [&](int kk) {
+            return q4(v(i, j, kk + 2), v(i, j, kk + 1), v(i, j, kk), v(i, j, kk - 1)) *
+                   q4(w(i, j + 2, kk), w(i, j + 1, kk), w(i, j, kk), w(i, j - 1, kk));
+          };
+          t3 = d4(pz(k + 1), pz(k), pz(k - 1), pz(k - 2), dz);  /* dvwdz */
+        } else {
+          auto sz = [&](int kk) { double a = q4(w(i, j, kk + 1), w(i, j, kk), w(i, j, kk - 1), w(i, j, kk - 2)); return a * a; };
+          t3 = d4(sz(k + 2), sz(k + 1), sz(k), sz(k - 1), dz);  /* dw2dz */
+          auto px = [&](int ii) {
+            return q4(w(ii + 2, j, k), w(ii + 1, j, k), w(ii, j, k), w(ii - 1, j, k)) *
+                   q4(u(ii, j, k + 2), u(ii, j, k + 1), u(ii, j, k), u(ii, j, k - 1));
+          };
+          t1 = d4(px(i + 1), px(i), px(i - 1), px(i - 2), dx);  /* duwdx */
+          auto py = [&](int jj) {
+            return q4(w(i, jj + 2, k), w(i, jj + 1, k), w(i, jj, k), w(i, jj - 1, k)) *
+                   q4(v(i, jj, k + 2), v(i, jj, k + 1), v(i, jj, k), v(i, jj, k - 1));
+          };
+          t2 = d4(py(j + 1), py(j), py(j - 1), py(j - 2), dy);  /* dvwdy */
+        }
+        F(B, st, i, j, k) = (F(B, oo, i, j, k) - dt * alfapr * (t1 + t2 + t3));
+      }
+    });
+  }
+  par_blocks((int)C.b.size(), [&](int ib) { Blk &B = C.b[ib];
+    const double dxx = B.d.dx * B.d.dx, dyy = B.d.dy * B.d.dy, dzz = B.d.dz * B.d.dz;
+    for (int op = 1; op <= 3; ++op) {
+      double *st = op == 1 ? B.ustar : op == 2 ? B.vstar : B.wstar;
+      double *c = field_of(B, op);
+      int is, ie, js, je, ks, ke;
+      franges(B, op, is, ie, js, je, ks, ke);
+      auto f = [&](int i, int j, int k) { return F(B, c, i, j, k); };
+      for (int k = ks; k <= ke; ++k) for (int i = is; i <= ie; ++i) for (int j = js; j <= je; ++j) {
+        /* u takes the viscosity of its own cell, v and w the one past the face (rungek.for:230, 262, 290) */
+        const double visc = op == 1 ? F(B, vis[ib], i, j, k) : op == 2 ? F(B, vis[ib], i, j + 1, k)
+                                                                       : F(B, vis[ib], i, j, k + 1);
+        const double diff = visc * (
+            ((-f(i + 2, j, k) + 16.0 * f(i + 1, j, k) - 30.0 * f(i, j, k) + 16.0 * f(i - 1, j, k) - f(i - 2, j, k)) /
+             (12.0 * dxx)) +
+            ((-f(i, j + 2, k) + 16.0 * f(i, j + 1, k) - 30.0 * f(i, j, k) + 16.0 * f(i, j - 1, k) - f(i, j - 2, k)) /
+             (12.0 * dyy)) +
+            ((-f(i, j, k + 2) + 16.0 * f(i, j, k + 1) - 30.0 * f(i, j, k) + 16.0 * f(i, j, k - 1) - f(i, j, k - 2)) /
+             (12.0 * dzz)));
+        F(B, st, i, j, k) = (F(B, st, i, j, k) + dt * alfapr * diff);
+        if (op == 1 && pforce) F(B, st, i, j, k) = F(B, st, i, j, k) + dt * alfapr * forcn;
+      }
+    }
+  });
+}
+
 /* EXT: distance between the centres of cells a and a+1 along an axis,
  * equal to dx on a uniform grid. */
 inline double dface(const std::vector<double> &w, int a0) { return 0.5 * (w[a0] + w[a0 + 1]); }
@@ -1519,7 +1616,13 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
     uoo[ib] = rk[ib].uoo; voo[ib] = rk[ib].voo; woo[ib] = rk[ib].woo; vis[ib] = rk[ib].vis;
     B.oo[0] = rk[ib].uoo; B.oo[1] = rk[ib].voo; B.oo[2] = rk[ib].woo;
   }
-  rungek_2nd(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
+  if (C.differencing == 2) {
+    /* rungek_conv4th reads u(i-3) .. u(i+3) */
+    if (C.pl < 3) { g_err = "rungek 4th order: needs pl >= 3"; return MF3D_E_INVALID; }
+    rungek_4th(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
+  } else {
+    rungek_2nd(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
+  }
   return MF3D_OK;
 }
 

@@ -1,5 +1,6 @@
 """The velocity predictor (one Runge-Kutta stage of rungek_conv2nd and
-rungek_diff2nd) on the GPU against the oracle, FP64, bit for bit: ustar,
+rungek_diff2nd, or with differencing = 2 rungek_conv4th and rungek_diff4th)
+on the GPU against the oracle, FP64, bit for bit: ustar,
 vstar, wstar over their faces and the u, v, w ghosts that boundu/v/w
 refresh on the way, for periodic, wall, symmetry, inflow and outflow
 faces, both stages' alfabc, and the pressure forcing."""
@@ -35,20 +36,31 @@ def dev(t, cuda):
     return torch.from_numpy(t.copy()).to(cuda)
 
 
-@pytest.mark.parametrize("case", sorted(CASES))
+CASES4 = {
+    "4th order, 2x2x1 periodic x y, walls z, first stage, forcing": (
+        lambda: Problem(2, 2, 1, 16, 16, 8, bc=(P, P, P, P, W, W), ngrid=2, pl=3), 1, 1, 1),
+    "4th order, 2x1x2 inflow / outflow x, walls y, periodic z, first stage": (
+        lambda: Problem(2, 1, 2, 16, 8, 16, bc=(1, 2, W, W, P, P), ngrid=2, pl=3), 2, 1, 0),
+    "4th order, 1 block, walls and symmetry, later stage": (
+        lambda: Problem(1, 1, 1, 16, 12, 8, bc=(W, W, S, S, W, W), ngrid=2, pl=4), 1, 0, 0),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES) + sorted(CASES4))
 def test_predictor_matches_oracle(lib, oracle, cuda, case):
     import torch
-    make, pl_ex, alfabc, pforce = CASES[case]
+    differencing = 2 if case in CASES4 else 1
+    make, pl_ex, alfabc, pforce = CASES4[case] if differencing == 2 else CASES[case]
     pr = make()
     blocks, rk = rk_inputs(pr, 21)
     dt, alfapr, forcn, ubulk = 0.0137, 0.5, 0.31, 0.6
     gpu = [{k: dev(v, cuda) for k, v in f.items()} for f in blocks]
     grk = [{k: dev(v, cuda) for k, v in r.items()} for r in rk]
     assert orc_rk(oracle, pr, blocks, rk, dt, alfapr, alfabc=alfabc, pforce=pforce, forcn=forcn,
-                  pl_ex=pl_ex, ubulk=ubulk) == 0
+                  pl_ex=pl_ex, ubulk=ubulk, differencing=differencing) == 0
     # the context's alfabc is the projection's own (its final boundu/v/w);
     # the stage's comes with each predictor call
-    prm = pr.params(pl_ex=pl_ex, bounds=1, alfabc=0, ubulk=ubulk)
+    prm = pr.params(pl_ex=pl_ex, bounds=1, alfabc=0, ubulk=ubulk, differencing=differencing)
     proj = Projection(pr.descriptors(lib), prm, lib)
     fa = (abi.Fields * pr.nblocks)()
     ra = (RkFields * pr.nblocks)()

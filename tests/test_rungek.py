@@ -38,7 +38,8 @@ def rk_struct(rk):
 
 
 def orc_rk(oracle, pr, blocks, rk, dt, alfapr, alfabc=1, pforce=0, forcn=0.0, **kw):
-    prm = pr.params(pl_ex=kw.get("pl_ex", 0), alfabc=alfabc, ubulk=kw.get("ubulk", 0.0))
+    prm = pr.params(pl_ex=kw.get("pl_ex", 0), alfabc=alfabc, ubulk=kw.get("ubulk", 0.0),
+                    differencing=kw.get("differencing", 1))
     return oracle.orc_rungek_2nd(pr.descriptors(oracle), pr.nblocks, C.byref(prm), fields_struct(blocks),
                                  rk_struct(rk), dt, alfapr, alfabc, pforce, forcn)
 
@@ -80,6 +81,77 @@ def numpy_stage(u, v, w, uoo, voo, woo, vis, dx, dy, dz, dt, alfapr, pforce, for
             st = st + dt * alfapr * forcn
         out.append(st)
     return out
+
+
+def numpy_stage4(u, v, w, uoo, voo, woo, vis, dx, dy, dz, dt, alfapr, pforce, forcn, sl):
+    """rungek_conv4th + rungek_diff4th (rungek.for:2-312), vectorised the
+    way the reference writes each term; arrays [k, j, i]."""
+    def at(a, di=0, dj=0, dk=0):
+        return a[sl[0].start + dk:sl[0].stop + dk, sl[1].start + dj:sl[1].stop + dj, sl[2].start + di:sl[2].stop + di]
+
+    def sh(ax, m):  # offset m along axis ax (0 x, 1 y, 2 z) as (di, dj, dk)
+        return tuple(m if a == ax else 0 for a in range(3))
+
+    def add(o1, o2):
+        return tuple(x + y for x, y in zip(o1, o2))
+
+    def q4(f, ax, base):  # (-f(+1) + 9 f(0) + 9 f(-1) - f(-2)) / 16 along ax, around offset `base`
+        return (-at(f, *add(base, sh(ax, 1))) + 9.0 * at(f, *base) + 9.0 * at(f, *add(base, sh(ax, -1)))
+                - at(f, *add(base, sh(ax, -2)))) / 16.0
+
+    def d4(p1, p0, m1, m2, h):
+        return (-p1 + 27.0 * p0 - 27.0 * m1 + m2) / (24.0 * h)
+    vel = (u, v, w)
+    oos = (uoo, voo, woo)
+    hs = (dx, dy, dz)
+    out = []
+    for a in range(3):
+        c = vel[a]
+        terms = []
+        for b in range(3):
+            if b == a:  # self term: the squared interpolant at faces +2 .. -1
+                s = [q4(c, a, sh(a, m)) for m in (2, 1, 0, -1)]
+                terms.append(d4(*[x * x for x in s], hs[a]))
+            else:  # cross term: c interpolated along b times the b-velocity interpolated along a
+                prod = [q4(c, b, sh(b, m + 1)) * q4(vel[b], a, add(sh(b, m), sh(a, 1))) for m in (1, 0, -1, -2)]
+                terms.append(d4(*prod, hs[b]))
+        st = at(oos[a]) - dt * alfapr * (terms[0] + terms[1] + terms[2])
+        visc = at(vis) if a == 0 else at(vis, *sh(a, 1))
+        lap = []
+        for b in range(3):
+            lap.append((-at(c, *sh(b, 2)) + 16.0 * at(c, *sh(b, 1)) - 30.0 * at(c) + 16.0 * at(c, *sh(b, -1))
+                        - at(c, *sh(b, -2))) / (12.0 * (hs[b] * hs[b])))
+        diff = visc * (lap[0] + lap[1] + lap[2])
+        st = st + dt * alfapr * diff
+        if a == 0 and pforce:
+            st = st + dt * alfapr * forcn
+        out.append(st)
+    return out
+
+
+def test_oracle_predictor_4th_order_matches_numpy(oracle):
+    """differencing = 2: rungek_conv4th and rungek_diff4th (rungek.for:2-312),
+    the oracle against a vectorised evaluation of the same expressions, on a
+    periodic block with three ghost layers (the stencils reach i-3 .. i+3);
+    pl = 2 is refused."""
+    pr = Problem(1, 1, 1, 12, 10, 8, bc=(P,) * 6, ngrid=1, pl=3, dx=0.1, dy=0.125, dz=0.3)
+    blocks, rk = rk_inputs(pr, 8)
+    given = {k: blocks[0][k].copy() for k in ("u", "v", "w")}
+    dt, alfapr, forcn = 0.017, 0.6, 0.2
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfapr, pforce=1, forcn=forcn, differencing=2) == 0
+    f = blocks[0]
+    pl, n = pr.pl, (pr.nz, pr.ny, pr.nx)
+    sl = tuple(slice(pl, pl + m) for m in n)
+    args = (rk[0]["uoo"], rk[0]["voo"], rk[0]["woo"], rk[0]["vis"], pr.dx, pr.dy, pr.dz, dt, alfapr, 1, forcn, sl)
+    us = numpy_stage4(f["u"], given["v"], given["w"], *args)[0]
+    vs = numpy_stage4(f["u"], f["v"], given["w"], *args)[1]
+    ws = numpy_stage4(f["u"], f["v"], f["w"], *args)[2]
+    assert np.array_equal(f["ustar"][sl], us)
+    assert np.array_equal(f["vstar"][sl], vs)
+    assert np.array_equal(f["wstar"][sl], ws)
+    pr2 = Problem(1, 1, 1, 12, 10, 8, bc=(P,) * 6, ngrid=1, pl=2)
+    b2, r2 = rk_inputs(pr2, 8)
+    assert orc_rk(oracle, pr2, b2, r2, dt, alfapr, differencing=2) == -1
 
 
 def test_oracle_predictor_matches_numpy(oracle):
