@@ -222,15 +222,17 @@ typedef struct mf3d_rk_fields {
   const double *vis;
 } mf3d_rk_fields;
 
-/* One Runge-Kutta stage of the velocity predictor with central differences
- * and explicit diffusion (flosol.for:151-172 with diff_sch = 3), by the
- * context's `differencing`: 1 - rungek_conv2nd (rungek.for:314-412) then
- * rungek_diff2nd (rungek.for:584-779); 2 - rungek_conv4th (rungek.for:2-212)
- * then rungek_diff4th (rungek.for:214-312), which read three ghost layers
- * (pl >= 3, else MF3D_E_INVALID).  Each convection is boundu, the u
- * predictor, boundv, the v predictor, boundw, the w predictor; the
+/* One Runge-Kutta stage of the velocity predictor with explicit diffusion
+ * (flosol.for:151-172 with diff_sch = 3), by the context's `differencing`:
+ * 1 - rungek_conv2nd (rungek.for:314-412) then rungek_diff2nd
+ * (rungek.for:584-779); 2 - rungek_conv4th (rungek.for:2-212) then
+ * rungek_diff4th (rungek.for:214-312); 3 - rungek_convWENO (rungek.for:
+ * 414-582, the HJ_WENO derivatives of weno.for) then rungek_diff2nd.  2 and 3
+ * read three ghost layers (pl >= 3, else MF3D_E_INVALID; the reference sets
+ * pl_ex = 2 for WENO, initial.for:114-117).  Each convection is boundu, the
+ * u predictor, boundv, the v predictor, boundw, the w predictor; the
  * reference's branch without L_LSM, immersed boundaries or wall functions.
- * differencing = 3 (WENO convection) returns MF3D_E_UNSUPPORTED.  In: u, v, w (their ghosts
+ * In: u, v, w (their ghosts
  * are refreshed by boundu/v/w, as in the reference), `rk`; out: ustar,
  * vstar, wstar over the faces calvel later reads (isu..ieu etc.).  `p` must
  * be set as for the projection (not read here; su and dens may be NULL).

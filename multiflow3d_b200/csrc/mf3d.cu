@@ -767,7 +767,7 @@ struct ViewLevel {
   DevBuf<BlkLev> tab;                 // one entry per view block (absent: nx = 0)
   std::vector<BlkLev> htab;           // host copy of tab (the autotuner rebuilds tables from it)
   std::vector<int> hblk[3];           // view blocks of each subset
-  int sched = 0;                      // red-black sweep schedule (sweep_segments)
+  int sched = 2;                      // red-black sweep schedule (sweep_segments; 2 by default)
   DevBuf<RbSeg> sweep[3];             // red-black sweep segments (k_rbgs), per subset
   DevBuf<int> sfirst[3];              // first segment of each sweep CTA (+ total)
   DevBuf<Tile> cells[3];
@@ -1767,13 +1767,10 @@ static int autotune_level(mf3d_ctx *C, View &V, int g, bool time_new) {
       int bs = 0;
       for (int sc = 0; sc < kSweepSchedules; ++sc) {
         if ((st = upload_sweeps(C, L, sc, SUB_A))) return st;
-        // a red and a black half-sweep, as a sweep runs them (each reads what
-        // the other wrote, with the L2 traffic of a real sweep)
-        const double t = tune_time(C, [&] {
-          for (int colour = 0; colour < 2; ++colour)
-            launch(k_rbgs<T, false>, dim3(L.n_sweep[SUB_A]), cta, 0, s, L.tab.p, L.sweep[SUB_A].p,
-                   L.sfirst[SUB_A].p, V.act.p, colour, V.err.p);
-        });
+        // the level's pre-smoothing as a V-cycle runs it: from-zero red,
+        // black, halo, red, black, halo (the kernels around a half-sweep set
+        // the L2 contents and launch overlap it meets in a solve)
+        const double t = tune_time(C, [&] { relax<T>(C, V, g, SUB_A, std::max(C->prm.irestr, 1), true, false); });
         if (t < best) { best = t; bs = sc; }
       }
       if ((st = upload_sweeps(C, L, bs))) return st;
@@ -2843,12 +2840,8 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
     set_error("mf3d_rungek_2nd_device: needs a context with bounds = 1, FP64 and no lsm");
     return MF3D_E_UNSUPPORTED;
   }
-  if (C->prm.differencing == 3) {
-    set_error("mf3d_rungek_2nd_device: WENO convection (differencing = 3) is not restated");
-    return MF3D_E_UNSUPPORTED;
-  }
-  if (C->prm.differencing == 2 && C->prm.pl < 3) {
-    set_error("mf3d_rungek_2nd_device: the 4th-order stage reads three ghost layers (pl >= 3)");
+  if ((C->prm.differencing == 2 || C->prm.differencing == 3) && C->prm.pl < 3) {
+    set_error("mf3d_rungek_2nd_device: the 4th-order and WENO stages read three ghost layers (pl >= 3)");
     return MF3D_E_INVALID;
   }
   View &V = *C->view;
@@ -2899,6 +2892,9 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
     bound_faces(C, V, alfabc, comp, dt, alfapr);
     if (C->prm.differencing == 2)
       launch(k_rk4th, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, comp, dt, alfapr, pressureforce, forcn);
+    else if (C->prm.differencing == 3)
+      launch(k_rkweno, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, comp, C->prm.pl_ex, dt, alfapr,
+             pressureforce, forcn);
     else
       launch(k_rk2nd, V.n_int, dim3(RW_TX, RW_RJ), 0, s, V.df.p, V.t_int.p, comp, dt, alfapr, pressureforce, forcn);
     ++C->launches;

@@ -1134,6 +1134,106 @@ __global__ void __launch_bounds__(RW_TX *RW_RJ) k_rk4th(const BlkFld *__restrict
   }
 }
 
+// HJ_WENO's fifth-order one-sided derivative from five divided differences
+// (weno.for:56-78; REAL is double, x**2 is x*x, MAX of the five squares).
+__device__ __forceinline__ double weno5(double v1, double v2, double v3, double v4, double v5) {
+  const double v11 = v1 * v1, v22 = v2 * v2, v33 = v3 * v3, v44 = v4 * v4, v55 = v5 * v5;
+  const double e = (1.0E-6) * fmax(fmax(fmax(fmax(v11, v22), v33), v44), v55) + 1.0E-99;
+  const double t11 = v1 - 2.0 * v2 + v3, t12 = v1 - 4.0 * v2 + 3.0 * v3;
+  const double t21 = v2 - 2.0 * v3 + v4, t22 = v2 - v4;
+  const double t31 = v3 - 2.0 * v4 + v5, t32 = 3.0 * v3 - 4.0 * v4 + v5;
+  const double S1 = (13.0 / 12.0) * (t11 * t11) + 0.25 * (t12 * t12);
+  const double S2 = (13.0 / 12.0) * (t21 * t21) + 0.25 * (t22 * t22);
+  const double S3 = (13.0 / 12.0) * (t31 * t31) + 0.25 * (t32 * t32);
+  const double d1 = e + S1, d2 = e + S2, d3 = e + S3;
+  const double a1 = 0.1 / (d1 * d1), a2 = 0.6 / (d2 * d2), a3 = 0.3 / (d3 * d3);
+  const double w1 = a1 / (a1 + a2 + a3), w2 = a2 / (a1 + a2 + a3), w3 = a3 / (a1 + a2 + a3);
+  return w1 * (v1 * (1.0 / 3.0) - v2 * (7.0 / 6.0) + v3 * (11.0 / 6.0)) +
+         w2 * (-(v2 * (1.0 / 6.0)) + v3 * (5.0 / 6.0) + v4 * (1.0 / 3.0)) +
+         w3 * (v3 * (1.0 / 3.0) + v4 * (5.0 / 6.0) - v5 * (1.0 / 6.0));
+}
+
+// The same stage with differencing = 3: rungek_convWENO (rungek.for:
+// 414-582) then rungek_diff2nd, for component `comp`.  Each derivative is
+// HJ_WENO's (weno.for:2-354) at this cell - the divided differences
+// D1(m) = (f(m+1) - f(m))/h formed on the fly - upwinded by the sign of the
+// advecting velocity (its own value along its axis, the 4-face average
+// 0.25*(...) along the others), 0 where that is 0; HJ_WENO leaves 0 outside
+// cells 4 .. end + pl_ex + 1 - 3 of each axis (1-based field indices; end
+// the component's range end), and so does this.  Then rungek_diff2nd's
+// terms as k_rk2nd forms them.
+__global__ void __launch_bounds__(RW_TX *RW_RJ) k_rkweno(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                                                         int comp, int pl_ex, double dt, double alfapr, int pforce,
+                                                         double forcn) {
+  pdl_wait();
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  const int i = t.i0 + threadIdx.x, j = t.j0 + threadIdx.y;
+  if (i > comp_end(F, comp, 0) || j > comp_end(F, comp, 1)) return;
+  const int k1 = min(t.k0 + RW_KCH - 1, comp_end(F, comp, 2));
+  const long long st3[3] = {1, (long long)F.ti, (long long)F.ti * F.tj};
+  const double h[3] = {F.h[0][1], F.h[1][1], F.h[2][1]};
+  const double *__restrict__ U = F.u;
+  const double *__restrict__ V = F.v;
+  const double *__restrict__ W = F.w;
+  const double *__restrict__ Cf = comp_field(F, comp);
+  const double *__restrict__ OO = F.oo[comp];
+  double *__restrict__ ST = comp == 0 ? F.ustar : comp == 1 ? F.vstar : F.wstar;
+  // HJ_WENO's range ends, 1-based field indices: the component's ends + pl_ex + 1
+  int lim[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) lim[a] = comp_end(F, comp, a) + F.pl + pl_ex + 1;
+  const long long sy = st3[1], sz = st3[2];
+  for (int k = t.k0; k <= k1; ++k) {
+    const long long c = fidx(F, i, j, k);
+    const int fx[3] = {i + F.pl, j + F.pl, k + F.pl};  // 1-based field indices
+    // the advecting velocity of each axis at this face
+    double adv[3];
+    if (comp == 0) {
+      adv[0] = U[c];
+      adv[1] = 0.25 * (V[c] + V[c + 1] + V[c - sy] + V[c + 1 - sy]);
+      adv[2] = 0.25 * (W[c] + W[c + 1] + W[c - sz] + W[c + 1 - sz]);
+    } else if (comp == 1) {
+      adv[0] = 0.25 * (U[c] + U[c + sy] + U[c - 1] + U[c - 1 + sy]);
+      adv[1] = V[c];
+      adv[2] = 0.25 * (W[c] + W[c + sy] + W[c - sz] + W[c + sy - sz]);
+    } else {
+      adv[0] = 0.25 * (U[c] + U[c + sz] + U[c - 1] + U[c - 1 + sz]);
+      adv[1] = 0.25 * (V[c] + V[c + sz] + V[c - sy] + V[c - sy + sz]);
+      adv[2] = W[c];
+    }
+    double term[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double sgn = adv[a];
+      double d = 0.0;
+      // HJ_WENO writes cells 4 .. lim-3 along a, 1 .. lim of the others
+      bool inside = fx[a] >= 4 && fx[a] <= lim[a] - 3;
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        if (b != a) inside = inside && fx[b] >= 1 && fx[b] <= lim[b];
+      if (inside && sgn != 0.0) {
+        const long long s = st3[a];
+        auto D1 = [&](int m) { return (Cf[c + (m + 1) * s] - Cf[c + m * s]) / h[a]; };
+        // plus (L = I = cell - 3): D1(+2) .. D1(-2); minus (L = I - 1): D1(-3) .. D1(+1)
+        d = sgn > 0.0 ? weno5(D1(-3), D1(-2), D1(-1), D1(0), D1(1)) : weno5(D1(2), D1(1), D1(0), D1(-1), D1(-2));
+      }
+      term[a] = sgn * d;
+    }
+    double st = (OO[c] - dt * alfapr * (term[0] + term[1] + term[2]));
+    const double dxx = h[0] * h[0], dyy = h[1] * h[1], dzz = h[2] * h[2];
+    const double visc = F.vis[c + st3[comp]];
+    const double aw = -visc / dxx, ae = -visc / dxx, an = -visc / dyy, as = -visc / dyy;
+    const double at = -visc / dzz, ab = -visc / dzz;
+    const double ap = -1.0 * (aw + ae + as + an + ab + at);
+    const double diff = -(ap * Cf[c] + an * Cf[c + sy] + as * Cf[c - sy] + ae * Cf[c + 1] + aw * Cf[c - 1] +
+                          at * Cf[c + sz] + ab * Cf[c - sz]);
+    st = (st + dt * alfapr * diff);
+    if (comp == 0 && pforce) st = st + dt * alfapr * forcn;
+    ST[c] = st;
+  }
+}
+
 // After the initial calvel/calmas (newsolv_mg.for:16-17): rmax0, the
 // absolute threshold, and which domains iterate at all.
 __global__ void k_dom_init(DomState *ds, int ndom, unsigned long long *rmax_slot, int *act) {

@@ -1052,6 +1052,7 @@ void bound(Ctx &C, int op) {
  *   star = (star + dt*alfapr*diff),
  * and for u under pressureforce star = star + dt*alfapr*forcn (:650-652).
  * The u loop reads v and w before boundv/boundw refresh their ghosts. */
+void diff2nd(Ctx &C, const double *const *vis, bool pforce, double forcn);
 void rungek_2nd(Ctx &C, const double *const *uoo, const double *const *voo, const double *const *woo,
                 const double *const *vis, bool pforce, double forcn) {
   const double dt = C.dt, alfapr = C.alfapr;
@@ -1094,6 +1095,12 @@ void rungek_2nd(Ctx &C, const double *const *uoo, const double *const *voo, cons
       }
     });
   }
+  diff2nd(C, vis, pforce, forcn);
+}
+
+/* rungek_diff2nd (rungek.for:584-779), the branch without L_LSM. */
+void diff2nd(Ctx &C, const double *const *vis, bool pforce, double forcn) {
+  const double dt = C.dt, alfapr = C.alfapr;
   par_blocks((int)C.b.size(), [&](int ib) { Blk &B = C.b[ib];
     const double dxx = B.d.dx * B.d.dx, dyy = B.d.dy * B.d.dy, dzz = B.d.dz * B.d.dz;
     for (int op = 1; op <= 3; ++op) {
@@ -1212,6 +1219,118 @@ void rungek_4th(Ctx &C, const double *const *uoo, const double *const *voo, cons
       }
     }
   });
+}
+
+/* HJ_WENO_dx/dy/dz (weno.for:2-354) of field fi of component op along
+ * axis ax: the divided differences D1 over 1..n-1 of the axis, then the
+ * fifth-order one-sided derivatives at 4..n-3 (plus: D1(L+5)..D1(L+1) with
+ * L = I; minus: D1(L+1)..D1(L+5) with L = I-1), zero elsewhere; n, nq, nr
+ * are the component's range ends plus pl_ex + 1.  REAL is double
+ * (-fdefault-real-8): 1.0E-6, 1.0E-99, 13.0/12.0, 1.0/3.0, ... are double;
+ * x**2 is x*x; MAX of the five squares. */
+double weno5(double v1, double v2, double v3, double v4, double v5) {
+  const double v11 = v1 * v1, v22 = v2 * v2, v33 = v3 * v3, v44 = v4 * v4, v55 = v5 * v5;
+  const double e = (1.0E-6) * std::max(std::max(std::max(std::max(v11, v22), v33), v44), v55) + 1.0E-99;
+  const double t11 = v1 - 2.0 * v2 + v3, t12 = v1 - 4.0 * v2 + 3.0 * v3;
+  const double t21 = v2 - 2.0 * v3 + v4, t22 = v2 - v4;
+  const double t31 = v3 - 2.0 * v4 + v5, t32 = 3.0 * v3 - 4.0 * v4 + v5;
+  const double S1 = (13.0 / 12.0) * (t11 * t11) + 0.25 * (t12 * t12);
+  const double S2 = (13.0 / 12.0) * (t21 * t21) + 0.25 * (t22 * t22);
+  const double S3 = (13.0 / 12.0) * (t31 * t31) + 0.25 * (t32 * t32);
+  const double d1 = e + S1, d2 = e + S2, d3 = e + S3;
+  const double a1 = 0.1 / (d1 * d1), a2 = 0.6 / (d2 * d2), a3 = 0.3 / (d3 * d3);
+  const double w1 = a1 / (a1 + a2 + a3), w2 = a2 / (a1 + a2 + a3), w3 = a3 / (a1 + a2 + a3);
+  return w1 * (v1 * (1.0 / 3.0) - v2 * (7.0 / 6.0) + v3 * (11.0 / 6.0)) +
+         w2 * (-(v2 * (1.0 / 6.0)) + v3 * (5.0 / 6.0) + v4 * (1.0 / 3.0)) +
+         w3 * (v3 * (1.0 / 3.0) + v4 * (5.0 / 6.0) - v5 * (1.0 / 6.0));
+}
+void hj_weno(Blk &B, const double *fi, int ax, int npp, int nq, int nr, double h, std::vector<double> &plus,
+             std::vector<double> &minus) {
+  const size_t n = (size_t)B.ttc_i * B.ttc_j * B.ttc_k;
+  std::vector<double> D1(n, 0.0);
+  plus.assign(n, 0.0);
+  minus.assign(n, 0.0);
+  const int lim[3] = {npp, nq, nr};
+  auto id = [&](int i, int j, int k) {
+    return (size_t)(i - 1) + (size_t)B.ttc_i * ((size_t)(j - 1) + (size_t)B.ttc_j * (size_t)(k - 1));
+  };
+  auto shift = [&](int i, int j, int k, int d, int &a, int &b, int &c) {
+    a = i + (ax == 0 ? d : 0); b = j + (ax == 1 ? d : 0); c = k + (ax == 2 ? d : 0);
+  };
+  /* divided differences over 1..lim-1 along ax, 1..lim of the others */
+  for (int k = 1; k <= lim[2] - (ax == 2); ++k) for (int i = 1; i <= lim[0] - (ax == 0); ++i)
+    for (int j = 1; j <= lim[1] - (ax == 1); ++j) {
+      int a, b, c;
+      shift(i, j, k, 1, a, b, c);
+      D1[id(i, j, k)] = (fi[id(a, b, c)] - fi[id(i, j, k)]) / h;
+    }
+  for (int k = 1; k <= lim[2] - (ax == 2 ? 6 : 0); ++k) for (int i = 1; i <= lim[0] - (ax == 0 ? 6 : 0); ++i)
+    for (int j = 1; j <= lim[1] - (ax == 1 ? 6 : 0); ++j) {
+      auto d1 = [&](int m) { int a, b, c; shift(i, j, k, m, a, b, c); return D1[id(a, b, c)]; };
+      int a, b, c;
+      shift(i, j, k, 3, a, b, c);
+      plus[id(a, b, c)] = weno5(d1(5), d1(4), d1(3), d1(2), d1(1));    /* L = I */
+      minus[id(a, b, c)] = weno5(d1(0), d1(1), d1(2), d1(3), d1(4));   /* L = I - 1 */
+    }
+}
+
+/* One Runge-Kutta stage of rungek_convWENO (rungek.for:414-582) then
+ * rungek_diff2nd, as flosol.for:157-170 runs them for differencing = 3:
+ * boundu, HJ_WENO along x, y, z of u, the u loop (each derivative upwinded
+ * by the sign of the advecting velocity at the face, 0 where it is 0), and
+ * so on for v and w. */
+void rungek_weno(Ctx &C, const double *const *uoo, const double *const *voo, const double *const *woo,
+                 const double *const *vis, bool pforce, double forcn) {
+  const double dt = C.dt, alfapr = C.alfapr;
+  const int pll = C.pl_ex + 1;
+  for (int op = 1; op <= 3; ++op) {
+    bound(C, op);
+    par_blocks((int)C.b.size(), [&](int ib) { Blk &B = C.b[ib];
+      int is, ie, js, je, ks, ke;
+      franges(B, op, is, ie, js, je, ks, ke);
+      const double *fi = field_of(B, op);
+      std::vector<double> px, mx, py, my, pz, mz;
+      hj_weno(B, fi, 0, ie + pll, je + pll, ke + pll, B.d.dx, px, mx);
+      hj_weno(B, fi, 1, ie + pll, je + pll, ke + pll, B.d.dy, py, my);
+      hj_weno(B, fi, 2, ie + pll, je + pll, ke + pll, B.d.dz, pz, mz);
+      double *st = op == 1 ? B.ustar : op == 2 ? B.vstar : B.wstar;
+      const double *oo = op == 1 ? uoo[ib] : op == 2 ? voo[ib] : woo[ib];
+      auto u = [&](int i, int j, int k) { return F(B, B.u, i, j, k); };
+      auto v = [&](int i, int j, int k) { return F(B, B.v, i, j, k); };
+      auto w = [&](int i, int j, int k) { return F(B, B.w, i, j, k); };
+      auto up = [&](double a, const std::vector<double> &mn, const std::vector<double> &pls, int i, int j, int k) {
+        const double m = F(B, mn.data(), i, j, k), pv = F(B, pls.data(), i, j, k);
+        return a > 0.0 ? m : a < 0.0 ? pv : 0.0;
+      };
+      for (int k = ks; k <= ke; ++k) for (int i = is; i <= ie; ++i) for (int j = js; j <= je; ++j) {
+        double t1, t2, t3;
+        if (op == 1) {
+          const double uc = u(i, j, k);
+          const double vijk = 0.25 * (v(i, j, k) + v(i + 1, j, k) + v(i, j - 1, k) + v(i + 1, j - 1, k));
+          const double wijk = 0.25 * (w(i, j, k) + w(i + 1, j, k) + w(i, j, k - 1) + w(i + 1, j, k - 1));
+          t1 = uc * up(uc, mx, px, i, j, k);
+          t2 = vijk * up(vijk, my, py, i, j, k);
+          t3 = wijk * up(wijk, mz, pz, i, j, k);
+        } else if (op == 2) {
+          const double vc = v(i, j, k);
+          const double uijk = 0.25 * (u(i, j, k) + u(i, j + 1, k) + u(i - 1, j, k) + u(i - 1, j + 1, k));
+          const double wijk = 0.25 * (w(i, j, k) + w(i, j + 1, k) + w(i, j, k - 1) + w(i, j + 1, k - 1));
+          t1 = uijk * up(uijk, mx, px, i, j, k);
+          t2 = vc * up(vc, my, py, i, j, k);
+          t3 = wijk * up(wijk, mz, pz, i, j, k);
+        } else {
+          const double wc = w(i, j, k);
+          const double uijk = 0.25 * (u(i, j, k) + u(i, j, k + 1) + u(i - 1, j, k) + u(i - 1, j, k + 1));
+          const double vijk = 0.25 * (v(i, j, k) + v(i, j, k + 1) + v(i, j - 1, k) + v(i, j - 1, k + 1));
+          t1 = uijk * up(uijk, mx, px, i, j, k);
+          t2 = vijk * up(vijk, my, py, i, j, k);
+          t3 = wc * up(wc, mz, pz, i, j, k);
+        }
+        F(B, st, i, j, k) = (F(B, oo, i, j, k) - dt * alfapr * (t1 + t2 + t3));
+      }
+    });
+  }
+  diff2nd(C, vis, pforce, forcn);
 }
 
 /* EXT: distance between the centres of cells a and a+1 along an axis,
@@ -1620,6 +1739,11 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
     /* rungek_conv4th reads u(i-3) .. u(i+3) */
     if (C.pl < 3) { g_err = "rungek 4th order: needs pl >= 3"; return MF3D_E_INVALID; }
     rungek_4th(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
+  } else if (C.differencing == 3) {
+    /* HJ_WENO's stencils reach 3 cells and its ranges pl_ex + 1 past the
+     * component's end; initial.for:114-117 sets pl_ex = 2 for WENO */
+    if (C.pl < 3 || C.pl_ex + 1 > C.pl) { g_err = "rungek WENO: needs pl >= 3"; return MF3D_E_INVALID; }
+    rungek_weno(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
   } else {
     rungek_2nd(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
   }

@@ -1,6 +1,7 @@
 """The velocity predictor (one Runge-Kutta stage of rungek_conv2nd and
-rungek_diff2nd, or with differencing = 2 rungek_conv4th and rungek_diff4th)
-on the GPU against the oracle, FP64, bit for bit: ustar,
+rungek_diff2nd; with differencing = 2 rungek_conv4th and rungek_diff4th;
+with 3 rungek_convWENO and rungek_diff2nd) on the GPU against the oracle,
+FP64, bit for bit: ustar,
 vstar, wstar over their faces and the u, v, w ghosts that boundu/v/w
 refresh on the way, for periodic, wall, symmetry, inflow and outflow
 faces, both stages' alfabc, and the pressure forcing."""
@@ -46,11 +47,19 @@ CASES4 = {
 }
 
 
-@pytest.mark.parametrize("case", sorted(CASES) + sorted(CASES4))
+CASESW = {
+    "WENO, 2x2x1 periodic x y, walls z, first stage, forcing": (
+        lambda: Problem(2, 2, 1, 16, 16, 8, bc=(P, P, P, P, W, W), ngrid=2, pl=4), 2, 1, 1),
+    "WENO, 2x1x2 inflow / outflow x, walls y, periodic z, later stage": (
+        lambda: Problem(2, 1, 2, 16, 8, 16, bc=(1, 2, W, W, P, P), ngrid=2, pl=4), 2, 0, 0),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES) + sorted(CASES4) + sorted(CASESW))
 def test_predictor_matches_oracle(lib, oracle, cuda, case):
     import torch
-    differencing = 2 if case in CASES4 else 1
-    make, pl_ex, alfabc, pforce = CASES4[case] if differencing == 2 else CASES[case]
+    differencing = 2 if case in CASES4 else 3 if case in CASESW else 1
+    make, pl_ex, alfabc, pforce = (CASES4 if differencing == 2 else CASESW if differencing == 3 else CASES)[case]
     pr = make()
     blocks, rk = rk_inputs(pr, 21)
     dt, alfapr, forcn, ubulk = 0.0137, 0.5, 0.31, 0.6

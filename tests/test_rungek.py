@@ -154,6 +154,104 @@ def test_oracle_predictor_4th_order_matches_numpy(oracle):
     assert orc_rk(oracle, pr2, b2, r2, dt, alfapr, differencing=2) == -1
 
 
+def numpy_weno5(v1, v2, v3, v4, v5):
+    """HJ_WENO's fifth-order derivative from five divided differences (weno.for:56-78)."""
+    e = 1.0e-6 * np.maximum(np.maximum(np.maximum(np.maximum(v1 * v1, v2 * v2), v3 * v3), v4 * v4), v5 * v5) + 1.0e-99
+    t11, t12 = v1 - 2.0 * v2 + v3, v1 - 4.0 * v2 + 3.0 * v3
+    t21, t22 = v2 - 2.0 * v3 + v4, v2 - v4
+    t31, t32 = v3 - 2.0 * v4 + v5, 3.0 * v3 - 4.0 * v4 + v5
+    s1 = (13.0 / 12.0) * (t11 * t11) + 0.25 * (t12 * t12)
+    s2 = (13.0 / 12.0) * (t21 * t21) + 0.25 * (t22 * t22)
+    s3 = (13.0 / 12.0) * (t31 * t31) + 0.25 * (t32 * t32)
+    a1, a2, a3 = 0.1 / ((e + s1) * (e + s1)), 0.6 / ((e + s2) * (e + s2)), 0.3 / ((e + s3) * (e + s3))
+    w1, w2, w3 = a1 / (a1 + a2 + a3), a2 / (a1 + a2 + a3), a3 / (a1 + a2 + a3)
+    return (w1 * (v1 * (1.0 / 3.0) - v2 * (7.0 / 6.0) + v3 * (11.0 / 6.0)) +
+            w2 * (-(v2 * (1.0 / 6.0)) + v3 * (5.0 / 6.0) + v4 * (1.0 / 3.0)) +
+            w3 * (v3 * (1.0 / 3.0) + v4 * (5.0 / 6.0) - v5 * (1.0 / 6.0)))
+
+
+def numpy_weno_derivs(f, ax, ends, h):
+    """HJ_WENO along numpy axis ax (2 = x, 1 = y, 0 = z) of field f [k, j, i]:
+    (plus, minus), zero outside the computed range; ends = 1-based range
+    ends (x, y, z) = component ends + pl_ex + 1."""
+    lim = (ends[2], ends[1], ends[0])  # numpy axis order (z, y, x)
+    d1 = np.zeros_like(f)
+    sl = [slice(0, lim[0]), slice(0, lim[1]), slice(0, lim[2])]
+    sl[ax] = slice(0, lim[ax] - 1)
+    hi = list(sl)
+    hi[ax] = slice(1, lim[ax])
+    d1[tuple(sl)] = (f[tuple(hi)] - f[tuple(sl)]) / h
+    plus, minus = np.zeros_like(f), np.zeros_like(f)
+    n = lim[ax] - 6
+
+    def take(m):
+        s2 = [slice(0, lim[0]), slice(0, lim[1]), slice(0, lim[2])]
+        s2[ax] = slice(m, m + n)
+        return d1[tuple(s2)]
+    dst = [slice(0, lim[0]), slice(0, lim[1]), slice(0, lim[2])]
+    dst[ax] = slice(3, 3 + n)
+    plus[tuple(dst)] = numpy_weno5(take(5), take(4), take(3), take(2), take(1))
+    minus[tuple(dst)] = numpy_weno5(take(0), take(1), take(2), take(3), take(4))
+    return plus, minus
+
+
+def test_oracle_predictor_weno_matches_numpy(oracle):
+    """differencing = 3: rungek_convWENO (rungek.for:414-582, HJ_WENO of
+    weno.for) and rungek_diff2nd, the oracle against a vectorised
+    evaluation on a periodic block with pl = 4, pl_ex = 2 (as initial.for
+    sets them for WENO)."""
+    pr = Problem(1, 1, 1, 12, 10, 8, bc=(P,) * 6, ngrid=1, pl=4, dx=0.1, dy=0.125, dz=0.3)
+    blocks, rk = rk_inputs(pr, 9)
+    for k in ("u", "v", "w"):  # some exact zeros: the upwinding's third branch
+        blocks[0][k][5, 5, 5:9] = 0.0
+    given = {k: blocks[0][k].copy() for k in ("u", "v", "w")}
+    dt, alfapr, forcn, pl_ex = 0.011, 0.6, 0.15, 2
+    assert orc_rk(oracle, pr, blocks, rk, dt, alfapr, pforce=1, forcn=forcn, differencing=3, pl_ex=pl_ex) == 0
+    f = blocks[0]
+    pl = pr.pl
+    sl = tuple(slice(pl, pl + m) for m in (pr.nz, pr.ny, pr.nx))
+    ends = (pr.nx + pl + pl_ex + 1, pr.ny + pl + pl_ex + 1, pr.nz + pl + pl_ex + 1)
+    hs = {2: pr.dx, 1: pr.dy, 0: pr.dz}
+
+    def at(a, di=0, dj=0, dk=0):
+        return a[sl[0].start + dk:sl[0].stop + dk, sl[1].start + dj:sl[1].stop + dj, sl[2].start + di:sl[2].stop + di]
+
+    def upwind(a, ax, fld):
+        plus, minus = numpy_weno_derivs(fld, ax, ends, hs[ax])
+        return np.where(a > 0.0, at(minus), np.where(a < 0.0, at(plus), 0.0))
+    # the u loop sees v, w as given; the v loop w as given (their bounds come later)
+    u, v, w = f["u"], given["v"], given["w"]
+    uc = at(u)
+    vijk = 0.25 * (at(v) + at(v, 1) + at(v, 0, -1) + at(v, 1, -1))
+    wijk = 0.25 * (at(w) + at(w, 1) + at(w, 0, 0, -1) + at(w, 1, 0, -1))
+    conv_u = uc * upwind(uc, 2, u) + vijk * upwind(vijk, 1, u) + wijk * upwind(wijk, 0, u)
+    v = f["v"]
+    vc = at(v)
+    uijk = 0.25 * (at(u) + at(u, 0, 1) + at(u, -1) + at(u, -1, 1))
+    wijk = 0.25 * (at(w) + at(w, 0, 1) + at(w, 0, 0, -1) + at(w, 0, 1, -1))
+    conv_v = uijk * upwind(uijk, 2, v) + vc * upwind(vc, 1, v) + wijk * upwind(wijk, 0, v)
+    w = f["w"]
+    wc = at(w)
+    uijk = 0.25 * (at(u) + at(u, 0, 0, 1) + at(u, -1) + at(u, -1, 0, 1))
+    vijk = 0.25 * (at(v) + at(v, 0, 0, 1) + at(v, 0, -1) + at(v, 0, -1, 1))
+    conv_w = uijk * upwind(uijk, 2, w) + vijk * upwind(vijk, 1, w) + wc * upwind(wc, 0, w)
+    # rungek_diff2nd after the three loops, on the final u, v, w
+    dxx, dyy, dzz = pr.dx * pr.dx, pr.dy * pr.dy, pr.dz * pr.dz
+    for a, (key, oo, conv, vshift) in enumerate((("ustar", "uoo", conv_u, (1, 0, 0)), ("vstar", "voo", conv_v, (0, 1, 0)),
+                                                 ("wstar", "woo", conv_w, (0, 0, 1)))):
+        c = f["uvw"[a]]
+        st = at(rk[0][oo]) - dt * alfapr * conv
+        visc = at(rk[0]["vis"], *vshift)
+        aw = -visc / dxx; ae = -visc / dxx; an = -visc / dyy; as_ = -visc / dyy; at_ = -visc / dzz; ab = -visc / dzz
+        ap = -1.0 * (aw + ae + as_ + an + ab + at_)
+        diff = -(ap * at(c) + an * at(c, 0, 1) + as_ * at(c, 0, -1) + ae * at(c, 1) + aw * at(c, -1) +
+                 at_ * at(c, 0, 0, 1) + ab * at(c, 0, 0, -1))
+        st = st + dt * alfapr * diff
+        if a == 0:
+            st = st + dt * alfapr * forcn
+        assert np.array_equal(f[key][sl], st), key
+
+
 def test_oracle_predictor_matches_numpy(oracle):
     """One periodic block: boundu/v/w wrap the ghosts; the u predictor reads
     v and w as given, the v predictor w as given (their bounds come after)."""
