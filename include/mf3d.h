@@ -114,11 +114,14 @@ typedef struct mf3d_params {
                        neighbour by its code - 1 inflow (west: u = ubulk,
                        v = w = 0; bottom: u = v = 0, w = 1.1), 2 outflow
                        (east, alfabc = 1: copy of the last face), 3 symmetry,
-                       4 wall, 5 periodic; a code with no branch for a face
-                       writes nothing there, as in the reference.  The codes
-                       that need data the library does not hold - 7, 8, 12,
-                       13 on the west, 21 on the east (uoo), 61 and up (wall
-                       functions), and 1 / 2 with lsm (phi) - return
+                       4 wall, 5 periodic, and the west inlets 7, 8 (file
+                       values, mf3d_set_inlet), 12, 13 (1/7 power law); a
+                       code with no branch for a face writes nothing there,
+                       as in the reference; 21 on the east (convective
+                       outflow, alfabc = 1) from the old velocities of
+                       mf3d_bind_old_velocity.  The codes that need data the
+                       library does not hold - 61 and up (wall functions),
+                       and 1 / 2 with lsm (phi) - return
                        MF3D_E_UNSUPPORTED.  Also refreshes the
                        full periodic ghost planes of the final exchange(1..3).
                        Skipped when the solve diverged (the reference stops).
@@ -256,6 +259,39 @@ int mf3d_rungek_2nd_device(mf3d_ctx *ctx, const mf3d_fields *fields, const mf3d_
  * the ghosts as they stand, without boundu/v/w.  Device pointers;
  * mf3d_create contexts, FP64, no lsm. */
 int mf3d_calvel_device(mf3d_ctx *ctx, const mf3d_fields *fields, double dt, double alfapr);
+
+/* The inlet file of a west face of code 7 or 8 (boundu, bounds.for:55-103),
+ * for the boundu/v/w of the solve (bounds = 1) and of the velocity
+ * predictor.  The reference opens the file itself at every boundu; here the
+ * caller reads it and hands the values over, once per file (the library
+ * keeps the plane until the next call).
+ *   code 7: the values of Inlet/Inlet_<dom>_<n>.dat, one u per line, k
+ *           outer, j inner over j = js-1..je+1, k = ks-1..ke+1:
+ *           n = (ny+2)*(nz+2);
+ *   code 8: the first column ("up") of inflow/Inlet_<dom>_<n>.dat after its
+ *           two header lines, over j = js-1..je, k = ks-1..ke (the rows the
+ *           reference reads, k outer): n = (ny+1)*(nz+1); u = up + ubulk, or
+ *           up + the 1/7 power-law profile when uprof_sem = 12 (UPROF_SEM,
+ *           initial.for:37).
+ * Every ghost layer 0..pl_ex of u takes the plane; v and w are left as the
+ * reference leaves them.  The power-law inlets (codes 12, 13,
+ * bounds.for:105-135) need no call: the library forms them at create from
+ * ubulk, the cell centres and the extents of all blocks.  Host values;
+ * mf3d_create contexts with bounds = 1; a solve or predictor stage with a
+ * code-7/8 face whose values were never set returns MF3D_E_INVALID. */
+int mf3d_set_inlet(mf3d_ctx *ctx, int block_id, int code, int uprof_sem, const double *values, long long n);
+
+/* The velocities at the start of the time step (uoo, voo, woo of `rk`, one
+ * entry per block; vis is not read) for the convective outflow of the
+ * solve's boundu/v/w: an east face of code 21 with alfabc = 1 sets
+ *   u(ie+1+ly) = uoo(ie+1+ly) - dt*alfapr*(uoo(ie+1+ly) - uoo(ie))/dx
+ * and the same for v and w (bounds.for:141-170, 449-474, 743-768), with the
+ * solve's dt and alfapr.  The reference reaches that branch when the last
+ * Runge-Kutta stage left alfabc = 1 (one stage, flosol.for:151-157).
+ * Device pointers, borrowed until the next call; NULL unbinds.  A solve of
+ * a bounds context with such a face and nothing bound returns
+ * MF3D_E_INVALID.  mf3d_create contexts. */
+int mf3d_bind_old_velocity(mf3d_ctx *ctx, const mf3d_rk_fields *rk);
 
 /* ---------------------------------------------------------------------- */
 /* Batches of independent domains (no counterpart in the reference, which   */

@@ -173,6 +173,8 @@ EXPORTED_SYMBOLS = (
     "mf3d_calvel_device",
     "mf3d_field_exchange_map",
     "mf3d_tuning",
+    "mf3d_set_inlet",
+    "mf3d_bind_old_velocity",
     "mf3d_test_fail_alloc",
     "mf3d_test_stall_copy",
 )
@@ -236,6 +238,8 @@ def _declare(lib):
     lib.mf3d_field_exchange_map.argtypes = [C.POINTER(BlockDesc), C.c_int, C.c_int, C.c_int, C.c_int,
                                             C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     lib.mf3d_tuning.argtypes = [vp, C.c_int] + [C.POINTER(C.c_int)] * 4
+    lib.mf3d_set_inlet.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_longlong]
+    lib.mf3d_bind_old_velocity.argtypes = [vp, vp]
     lib.mf3d_test_fail_alloc.argtypes = [C.c_longlong]
     lib.mf3d_test_stall_copy.argtypes = [C.c_int, C.c_int]
     return lib

@@ -12,6 +12,7 @@
 // multi-block solve (one domain), a batch (many domains) or the server's
 // current mix of resident requests.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -330,6 +331,7 @@ struct BlockStore {
   DevBuf<double> bcst;   // bounds mode: exchange_bc receive planes of u, v, w
   bool lsm = false;      // variable-density coefficients, formed per solve
   BlkFld fld;            // host template (field pointers bound per call)
+  DevBuf<double> inlet;  // west inlet plane of the codes 7, 8, 12, 13 (BlkFld::inl)
   size_t bytes = 0;      // device bytes owned
 };
 
@@ -763,11 +765,15 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
 // ---------------------------------------------------------------------------
 enum Subset { SUB_A = 0, SUB_C = 1, SUB_D = 2 };  // all present / coarsest here / continuing down
 
+// the red-black sweep schedule a level starts with (sweep_segments): the
+// fastest on whole solves of 128^3 blocks
+constexpr int kDefaultSweepSchedule = 2;
+
 struct ViewLevel {
   DevBuf<BlkLev> tab;                 // one entry per view block (absent: nx = 0)
   std::vector<BlkLev> htab;           // host copy of tab (the autotuner rebuilds tables from it)
   std::vector<int> hblk[3];           // view blocks of each subset
-  int sched = 2;                      // red-black sweep schedule (sweep_segments; 2 by default)
+  int sched = kDefaultSweepSchedule;  // red-black sweep schedule (sweep_segments)
   DevBuf<RbSeg> sweep[3];             // red-black sweep segments (k_rbgs), per subset
   DevBuf<int> sfirst[3];              // first segment of each sweep CTA (+ total)
   DevBuf<Tile> cells[3];
@@ -893,6 +899,9 @@ struct mf3d_ctx {
   DevBuf<double *> ptrs;
   // mf3d_mgkcyc_device_noalloc: device address of its fixed pointer tables
   void *noalloc_tab = nullptr;
+  // mf3d_bind_old_velocity: uoo, voo, woo per block (view order) for the
+  // convective outflow of the solve's boundu/v/w; empty = none bound
+  std::vector<std::array<const double *, 3>> oo_bound;
 };
 
 namespace mf3d {
@@ -1706,13 +1715,23 @@ static void tune_put(const std::string &k, int v) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[k] = v;
 }
-// Mean device milliseconds of f() over 3 runs after one warm-up run; a
-// failed launch counts as infinitely slow.
+// MF3D_TUNE_LOG=1 prints each choice the tuner makes to stderr.
+static void tune_log(const mf3d_ctx *C, int g, const char *what, int v) {
+  static const bool on = [] {
+    const char *e = std::getenv("MF3D_TUNE_LOG");
+    return e && e[0] == '1';
+  }();
+  if (on) std::fprintf(stderr, "mf3d tune: device %d level %d %s = %d\n", C->device, g, what, v);
+}
+// Mean device milliseconds of f() over kTuneReps runs after one warm-up
+// run; a failed launch counts as infinitely slow.
+constexpr int kTuneReps = 3, kTuneTrials = 3;
+constexpr double kTuneMargin = 0.03;  // a candidate must beat the default by 3 %
 template <class Fn>
 static double tune_time(mf3d_ctx *C, Fn &&f) {
   f();
   if (cudaEventRecord(C->ev0, C->stream) != cudaSuccess) return 1e30;
-  for (int r = 0; r < 3; ++r) f();
+  for (int r = 0; r < kTuneReps; ++r) f();
   if (cudaEventRecord(C->ev1, C->stream) != cudaSuccess || cudaEventSynchronize(C->ev1) != cudaSuccess) {
     cudaGetLastError();
     return 1e30;
@@ -1720,7 +1739,29 @@ static double tune_time(mf3d_ctx *C, Fn &&f) {
   if (cudaGetLastError() != cudaSuccess) return 1e30;
   float ms = 0.f;
   cudaEventElapsedTime(&ms, C->ev0, C->ev1);
-  return ms / 3.0;
+  return ms / kTuneReps;
+}
+// Picks one of n candidates: set(c) installs candidate c, run() is the work
+// it is timed on.  The candidates are timed in kTuneTrials interleaved
+// rounds and each keeps its fastest round, so a slow moment of the GPU
+// (another context, a clock change) hits every candidate alike and no single
+// run decides.  The default def stays unless the fastest candidate beats it
+// by kTuneMargin: a close call keeps the shape that was chosen by measuring
+// whole solves.  Installs the pick; returns a status.
+template <class Set, class Run>
+static int tune_pick(mf3d_ctx *C, int n, int def, Set &&set, Run &&run, int &pick) {
+  std::vector<double> t(n, 1e30);
+  int st;
+  for (int tr = 0; tr < kTuneTrials; ++tr)
+    for (int c = 0; c < n; ++c) {
+      if ((st = set(c))) return st;
+      t[c] = std::min(t[c], tune_time(C, run));
+    }
+  int best = def;
+  for (int c = 0; c < n; ++c)
+    if (t[c] < t[best]) best = c;
+  pick = t[best] < (1.0 - kTuneMargin) * t[def] ? best : def;
+  return set(pick);
 }
 static int upload_sweeps(mf3d_ctx *C, ViewLevel &L, int sched, int only_q = -1) {
   for (int q = 0; q < 3; ++q) {
@@ -1756,35 +1797,45 @@ static int autotune_level(mf3d_ctx *C, View &V, int g, bool time_new) {
     // (a) sweep schedule, (b) sweep kernel
     const std::string ks = tune_key(C, L, "sweep", sizeof(T));
     int v;
-    const char *forced = std::getenv("MF3D_SWEEP_SCHED");  // a fixed schedule 0..3 (tuning comparisons)
+    const char *forced = std::getenv("MF3D_SWEEP_SCHED");  // a fixed schedule (tuning comparisons)
     if (forced) {
       if ((st = upload_sweeps(C, L, std::max(0, std::min(kSweepSchedules - 1, std::atoi(forced)))))) return st;
+    } else if (g == 1) {
+      // level 1 keeps the default: timed on its own (no outer kernels
+      // around it, no fields bound yet) it ranks the schedules differently
+      // from whole solves, where schedule 0 measured 52.1 us a half-sweep
+      // against 46.6 us for the default on 2x2x2 blocks of 128^3
     } else if (tune_get(ks, v)) {
       if ((st = upload_sweeps(C, L, v & 7))) return st;
-      if (g > 1) L.small = (v >> 3) & 1;
+      L.small = (v >> 3) & 1;
     } else if (time_new) {
-      double best = 1e30;
-      int bs = 0;
-      for (int sc = 0; sc < kSweepSchedules; ++sc) {
-        if ((st = upload_sweeps(C, L, sc, SUB_A))) return st;
-        // the level's pre-smoothing as a V-cycle runs it: from-zero red,
-        // black, halo, red, black, halo (the kernels around a half-sweep set
-        // the L2 contents and launch overlap it meets in a solve)
-        const double t = tune_time(C, [&] { relax<T>(C, V, g, SUB_A, std::max(C->prm.irestr, 1), true, false); });
-        if (t < best) { best = t; bs = sc; }
-      }
-      if ((st = upload_sweeps(C, L, bs))) return st;
+      // candidates 0 .. kSweepSchedules-1: k_rbgs with that schedule;
+      // kSweepSchedules: k_rbgs_small (levels of 64 K to 4 M cells)
       const long long cells = L.cells_sub[SUB_A];
-      if (g > 1 && cells >= (1LL << 16) && cells <= (1LL << 22)) {
-        const int g2 = grid_of(L.small_items[SUB_A], kTile);
-        const double ts = tune_time(C, [&] {
-          for (int colour = 0; colour < 2; ++colour)
-            launch(k_rbgs_small<T, false>, g2, kTile, 0, s, L.tab.p, L.spre[SUB_A].p, L.list[SUB_A].p,
-                   L.n_list[SUB_A], V.act.p, colour);
-        });
-        L.small = ts < best ? 1 : 0;
-      }
-      tune_put(ks, bs | (L.small << 3));
+      const bool small_ok = g > 1 && cells >= (1LL << 16) && cells <= (1LL << 22);
+      const int n = kSweepSchedules + (small_ok ? 1 : 0);
+      const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
+      const int ir = std::max(C->prm.irestr, 1), ip = C->prm.iproln;
+      // the level's share of a V-cycle: pre-smoothing from zero, the
+      // restriction below it and the correction from below, post-smoothing
+      // (the kernels around the half-sweeps set the L2 contents and the
+      // launch overlap that the sweeps meet in a solve)
+      auto pass = [&] {
+        relax<T>(C, V, g, SUB_A, ir, true, false);
+        if (g < V.Lmax) {
+          if (g + 1 >= Lc) { restr<T, double>(C, V, g); corr<T, double>(C, V, g); }
+          else { restr<T, T>(C, V, g); corr<T, T>(C, V, g); }
+        }
+        relax<T>(C, V, g, SUB_D, ip, false);
+      };
+      auto set = [&](int c) {
+        L.small = c == kSweepSchedules ? 1 : 0;
+        return upload_sweeps(C, L, L.small ? kDefaultSweepSchedule : c);
+      };
+      int pick;
+      if ((st = tune_pick(C, n, kDefaultSweepSchedule, set, pass, pick))) return st;
+      tune_log(C, g, L.small ? "sweep kernel: plain loads" : "sweep schedule", L.sched);
+      tune_put(ks, L.sched | (L.small << 3));
     }
   }
   if ((sch == 2 || sch == 1) && !C->prm.lsm) {
@@ -1800,23 +1851,25 @@ static int autotune_level(mf3d_ctx *C, View &V, int g, bool time_new) {
     if (tune_get(kl, v)) {
       if (v <= def) set_cl(v);
     } else if (time_new && def > 1) {
-      double best = 1e30;
-      int bc = def;
-      for (int cl : {def, 8, 4}) {
-        if (cl > def || (cl != def && cl == 8 && def == 8)) continue;
-        set_cl(cl);
-        const double t = tune_time(C, [&] {
-          if (sch == 2)
-            launch_cl(k_tdma_lines<T>, L.n_list[SUB_A] * L.td_cl, TD_THREADS, L.td_smem, s, L.td_cl, L.tab.p,
-                      L.list[SUB_A].p, V.act.p, L.td_cl, L.td_gmax, L.td_nmax);
-          else
-            launch_cl(k_lexgs<T>, L.n_list[SUB_A] * L.lx_cl, 1024, 0, s, L.lx_cl, L.tab.p, L.list[SUB_A].p, V.act.p,
-                      L.lx_cl);
-        });
-        if (t < best) { best = t; bc = cl; }
-      }
-      set_cl(bc);
-      tune_put(kl, bc);
+      // the default and the portable cluster sizes below it
+      std::vector<int> cls{def};
+      for (int cl : {8, 4})
+        if (cl < def) cls.push_back(cl);
+      int pick;
+      if ((st = tune_pick(
+               C, (int)cls.size(), 0, [&](int c) { set_cl(cls[c]); return (int)MF3D_OK; },
+               [&] {
+                 if (sch == 2)
+                   launch_cl(k_tdma_lines<T>, L.n_list[SUB_A] * L.td_cl, TD_THREADS, L.td_smem, s, L.td_cl, L.tab.p,
+                             L.list[SUB_A].p, V.act.p, L.td_cl, L.td_gmax, L.td_nmax);
+                 else
+                   launch_cl(k_lexgs<T>, L.n_list[SUB_A] * L.lx_cl, 1024, 0, s, L.lx_cl, L.tab.p, L.list[SUB_A].p,
+                             V.act.p, L.lx_cl);
+               },
+               pick)))
+        return st;
+      tune_log(C, g, sch == 2 ? "line CTAs per block" : "lex CTAs per block", cls[pick]);
+      tune_put(kl, cls[pick]);
     }
   }
   return MF3D_OK;
@@ -1838,37 +1891,51 @@ static int autotune_restrict(mf3d_ctx *C, View &V, int g, bool time_new) {
   int v, st;
   if (tune_get(kr, v)) return set_kch(v);
   if (!time_new) return MF3D_OK;
-  double best = 1e30;
-  int bk = L.rtma_kch;
-  for (int kch : {2, 4, 8, 16}) {
-    if ((st = set_kch(kch))) return st;
-    const double t = tune_time(C, [&] {
-      if (f64) restr<double, double>(C, V, g - 1);
-      else if (c64) restr<float, double>(C, V, g - 1);
-      else restr<float, float>(C, V, g - 1);
-    });
-    if (t < best) { best = t; bk = kch; }
-  }
-  if ((st = set_kch(bk))) return st;
-  tune_put(kr, bk);
+  static const int kch_of[4] = {2, 4, 8, 16};
+  int def = 0;
+  for (int c = 0; c < 4; ++c)
+    if (kch_of[c] == L.rtma_kch) def = c;  // the wave model's choice (rtma_tiles)
+  int pick;
+  if ((st = tune_pick(
+           C, 4, def, [&](int c) { return set_kch(kch_of[c]); },
+           [&] {
+             if (f64) restr<double, double>(C, V, g - 1);
+             else if (c64) restr<float, double>(C, V, g - 1);
+             else restr<float, float>(C, V, g - 1);
+           },
+           pick)))
+    return st;
+  tune_log(C, g, "restrict planes", kch_of[pick]);
+  tune_put(kr, kch_of[pick]);
   return MF3D_OK;
 }
 
 // Tunes (or looks up) every level of the view; time_new = false only looks
 // the cache up.  The arrays are scratch at this point (the solve writes every
-// value it reads), and the level-1 ghost shell, which must hold zeros, is
-// never written by a sweep or a restriction into level 2.
+// value it reads) except the level-1 ghost shell, which must hold zeros: the
+// timed corrections write it, so level 1's phi is cleared at the end.  The
+// restrictions are tuned first, since a level's sweep is timed together with
+// the restriction below it.  Levels inside the coarse cluster launch
+// (k_coarse_cycle) run no sweep or restriction of their own.
 static int autotune_view(mf3d_ctx *C, View &V, bool time_new) {
   if (!autotune_enabled()) return MF3D_OK;
   if (C->prm.mg_itrsch == 2 && C->prm.lsm) return MF3D_OK;
   const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
+  const int gl = V.cc_g0 ? V.cc_g0 - 1 : V.Lmax;  // last level with its own sweeps
   int st;
-  for (int g = 1; g <= V.Lmax; ++g) {
+  for (int g = 2; g <= std::min(gl + 1, V.Lmax); ++g)
+    if ((st = autotune_restrict(C, V, g, time_new))) return st;
+  for (int g = 1; g <= gl; ++g) {
     const bool fp64 = C->elem == 8 || g >= Lc;
     if ((st = fp64 ? autotune_level<double>(C, V, g, time_new) : autotune_level<float>(C, V, g, time_new))) return st;
-    if ((st = autotune_restrict(C, V, g, time_new))) return st;
   }
+  if (!time_new) return MF3D_OK;
   CK(cudaStreamSynchronize(C->stream));
+  const size_t e1 = (C->elem == 8 || 1 >= Lc) ? 8 : 4;
+  for (size_t b = 0; b < V.blk.size(); ++b) {
+    const BlkLev &B = V.blk[b]->lv[1].desc;
+    CK(cudaMemsetAsync(B.phi, 0, (size_t)2 * B.cstr * e1, C->stream));
+  }
   CK(cudaMemsetAsync(V.err.p, 0, sizeof(int), C->stream));
   CK(cudaStreamSynchronize(C->stream));
   return MF3D_OK;
@@ -2046,6 +2113,10 @@ static int build_server_graph(mf3d_ctx *C, View &V) {
 static int bind_fields(mf3d_ctx *C, View &V, const mf3d_fields *f) {
   for (size_t b = 0; b < V.blk.size(); ++b) {
     BlkFld &F = V.hf[b];
+    // the old velocities of mf3d_bind_old_velocity, unless this call (the
+    // velocity predictor) bound its own
+    if (!C->oo_bound.empty() && !F.oo[0])
+      for (int a = 0; a < 3; ++a) F.oo[a] = C->oo_bound[b][a];
     F.ustar = f[b].ustar; F.vstar = f[b].vstar; F.wstar = f[b].wstar;
     F.u = f[b].u; F.v = f[b].v; F.w = f[b].w; F.p = f[b].p; F.su = f[b].su;
     F.dens = C->prm.lsm ? f[b].dens : nullptr;
@@ -2158,14 +2229,13 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
 // 16-838): per layer, the first walk's self-copies, the second walk's
 // self-copies and packs, the third walk's unpacks, each over x, y, z.
 // A face code whose boundu/v/w branch needs data the library does not hold:
-// the inflow files, SEM and power-law inlets of the west face (7, 8, 12, 13;
-// bounds.for:55-124), the convective outflow of the east face (21, uoo;
-// bounds.for:143-170), wall functions (61 and up: log_law, wall_function),
-// and under L_LSM the inflow and outflow faces, which phi gates
-// (bounds.for:43-50, 146-158).
+// the convective outflow of the east face (21, uoo; bounds.for:143-170)
+// outside the velocity predictor, wall functions (61 and up: log_law,
+// wall_function), and under L_LSM the inflow and outflow faces, which phi
+// gates (bounds.for:43-50, 146-158).  The inlet files of the west codes 7
+// and 8 come through mf3d_set_inlet.
 static bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc, bool have_oo = false) {
   if (code >= 61) return true;
-  if (f == 0 && (code == 7 || code == 8 || code == 12 || code == 13)) return true;
   if (f == 1 && code == 21 && alfabc == 1 && !have_oo) return true;
   if (lsm && ((f == 0 && code == 1) || (f == 1 && (code == 2 || code == 21) && alfabc == 1))) return true;
   return false;
@@ -2217,9 +2287,10 @@ static int solve_end(mf3d_ctx *C, View &V) {
     ++C->launches;
   }
   if (C->prm.bounds) {
-    // boundu/boundv/boundw (newsolv_mg.for:86-88)
+    // boundu/boundv/boundw (newsolv_mg.for:86-88); a convective outflow
+    // takes the solve's dt and alfapr (dt < 0) and the bound old velocities
     bc_walks(C, V);
-    bound_faces(C, V, C->prm.alfabc);
+    bound_faces(C, V, C->prm.alfabc, -1, -1.0, 0.0);
   }
   return MF3D_OK;
 }
@@ -2480,6 +2551,105 @@ static int make_view(mf3d_ctx *C) {
   return autotune_view(C, *C->view, true);
 }
 
+// The west inlets of boundu (bounds.for:55-135) on a block without a west
+// neighbour.  Codes 12 and 13 are the 1/7 power law of the wall distance in
+// y (13), times the same law in z (12):
+//   u = ubulk*(1+1/7)*|2*yc/H|^(1/7)          yc < H/2
+//   u = ubulk*(1+1/7)*|2*(H-yc)/H|^(1/7)      otherwise, H = yen - yst
+//   u = u*(1+1/7)*|zc/(zen-zst)|^(1/7)        code 12
+// formed once on the host in that order, from the cell centres the
+// reference forms (a running sum, initial.for:341-365) and the extents of the
+// whole domain (alloc_dom.for:427-439).  Code 7 takes u from the caller's
+// inlet file, code 8 the SEM fluctuations up added to ubulk or to the code-12
+// profile (UPROF_SEM = 12), both through mf3d_set_inlet.  The plane covers
+// rows 0..ny+1 and planes 0..nz+1 of u at the ghost layers 0..pl_ex; code 8
+// writes rows 0..ny and planes 0..nz only (bounds.for:84-86).
+struct Extents {
+  double yst, yen, zst, zen;
+};
+static Extents domain_extents(const mf3d_block_desc *blocks, int nb) {
+  Extents e{blocks[0].ysl, blocks[0].yel, blocks[0].zsl, blocks[0].zel};
+  for (int b = 1; b < nb; ++b) {
+    e.yst = std::min(e.yst, blocks[b].ysl); e.yen = std::max(e.yen, blocks[b].yel);
+    e.zst = std::min(e.zst, blocks[b].zsl); e.zen = std::max(e.zen, blocks[b].zel);
+  }
+  return e;
+}
+static double cell_centre(double lo, double h, int pl, int c) {  // field index c, 1-based
+  double x = lo + (double)(-pl + 1) * h;
+  for (int i = 2; i <= c; ++i) x = x + h;
+  return x - 0.5 * h;
+}
+static double power_law_y(double ubulk, const Extents &e, double yc) {
+  const double H = e.yen - e.yst;
+  if (yc < H / 2) return ubulk * (1.0 + 1.0 / 7.0) * std::pow(std::fabs(2 * yc / H), 1. / 7.);
+  return ubulk * (1.0 + 1.0 / 7.0) * std::pow(std::fabs(2 * (H - yc) / H), 1.0 / 7.0);
+}
+static double power_law_z(double u, const Extents &e, double zc) {
+  return u * (1.0 + 1. / 7.) * std::pow(std::fabs(zc / (e.zen - e.zst)), 1. / 7.);
+}
+// Forms (codes 12, 13) or installs (7, 8: vals) the inlet plane of block S.
+static int install_inlet(mf3d_ctx *C, BlockStore &S, const Extents &e, int code, int uprof, const double *vals) {
+  const mf3d_block_desc &d = S.d;
+  const int pl = C->prm.pl, rows = d.ny + 2;
+  std::vector<double> pln((size_t)rows * (d.nz + 2), 0.0);
+  int s1 = d.ny + 1, t1 = d.nz + 1;
+  if (code == 7) {
+    std::copy(vals, vals + pln.size(), pln.begin());
+  } else if (code == 8) {
+    s1 = d.ny; t1 = d.nz;
+    for (int t = 0; t <= d.nz; ++t)
+      for (int r = 0; r <= d.ny; ++r) {
+        const double up = vals[(size_t)t * (d.ny + 1) + r];
+        double u;
+        if (uprof == 12) {
+          u = power_law_y(C->prm.ubulk, e, cell_centre(d.ysl, d.dy, pl, r + pl));
+          u = power_law_z(u, e, cell_centre(d.zsl, d.dz, pl, t + pl)) + up;
+        } else {
+          u = C->prm.ubulk + up;
+        }
+        pln[(size_t)t * rows + r] = u;
+      }
+  } else {
+    for (int t = 0; t <= d.nz + 1; ++t)
+      for (int r = 0; r <= d.ny + 1; ++r) {
+        double u = power_law_y(C->prm.ubulk, e, cell_centre(d.ysl, d.dy, pl, r + pl));
+        if (code == 12) u = power_law_z(u, e, cell_centre(d.zsl, d.dz, pl, t + pl));
+        pln[(size_t)t * rows + r] = u;
+      }
+  }
+  int st;
+  if ((st = S.inlet.upload(pln, C->stream))) return st;
+  CK(cudaStreamSynchronize(C->stream));  // pln is a local
+  S.fld.inl = S.inlet.p;
+  S.fld.inl_s1 = s1;
+  S.fld.inl_t1 = t1;
+  return MF3D_OK;
+}
+static bool inlet_code(const mf3d_block_desc &d) {
+  return d.iprev < 0 && (d.bc_west == 7 || d.bc_west == 8 || d.bc_west == 12 || d.bc_west == 13);
+}
+// Every code-7 and code-8 inlet of a bounds context has its plane; with
+// `outflow` (the solve's boundu/v/w), every convective outflow face (code 21,
+// alfabc = 1) has the old velocities (mf3d_bind_old_velocity).
+static int inlets_ready(const mf3d_ctx *C, bool outflow = false) {
+  if (!C->prm.bounds) return MF3D_OK;
+  for (const auto &D : C->doms)
+    for (const auto &S : D->blocks) {
+      if (inlet_code(S->d) && !S->fld.inl) {
+        set_error("bounds: block " + std::to_string(S->d.id) + " has west code " + std::to_string(S->d.bc_west) +
+                  " and no inlet values (mf3d_set_inlet)");
+        return MF3D_E_INVALID;
+      }
+      if (outflow && S->d.inext < 0 && S->d.bc_east == 21 && C->prm.alfabc == 1 && C->oo_bound.empty()) {
+        set_error("bounds: block " + std::to_string(S->d.id) +
+                  " has a convective outflow (code 21, alfabc 1) and no old velocities (mf3d_bind_old_velocity)");
+        return MF3D_E_INVALID;
+      }
+    }
+  return MF3D_OK;
+}
+
 static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, mf3d_ctx **out) {
   if (!blocks || nb <= 0 || !out) { set_error("mf3d_create: bad arguments"); return MF3D_E_INVALID; }
   int st = check_params(prm);
@@ -2500,11 +2670,16 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
       const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
       const int nbrs[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
       for (int f = 0; f < 6; ++f)
-        if (nbrs[f] < 0 && bounds_code_unsupported(f, bcs[f], prm->lsm != 0, prm->alfabc)) {
+        if (nbrs[f] < 0 && bounds_code_unsupported(f, bcs[f], prm->lsm != 0, prm->alfabc, true)) {
           set_error("bounds: block " + std::to_string(d.id) + " face " + std::to_string(f) + " has code " +
                     std::to_string(bcs[f]) + ", whose boundu/v/w branch needs data the library does not hold");
           return MF3D_E_UNSUPPORTED;
         }
+    }
+    if (prm->bounds && inlet_code(d) && d.bc_west != 7 && (d.hy || d.hz)) {
+      set_error("bounds: the power-law inlet of block " + std::to_string(d.id) +
+                " reads uniform cell centres (initial.for:341-365)");
+      return MF3D_E_UNSUPPORTED;
     }
     if (prm->solver == 1 && (d.hx || d.hy || d.hz)) {
       set_error("solver 1 (SIP): uniform spacing only (pressure_1sweep, press.for:294-320)");
@@ -2532,6 +2707,13 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, C->coarse64 ? 8 : C->elem, prm->pl,
                          C->stream, prm->lsm != 0, prm->bounds != 0, prm->pl_ex, prm->differencing == 2)))
     return st;
+  if (prm->bounds) {
+    const Extents e = domain_extents(blocks, nb);
+    for (auto &S : C->doms[0]->blocks)
+      if (inlet_code(S->d) && (S->d.bc_west == 12 || S->d.bc_west == 13) &&
+          (st = install_inlet(C.get(), *S, e, S->d.bc_west, 0, nullptr)))
+        return st;
+  }
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
   return MF3D_OK;
@@ -2826,8 +3008,9 @@ int mf3d_newsolv_mg_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, do
   if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   mf3d::AllocScope scope(C->stream);
-  int st = mf3d::bind_fields(C, *C->view, fields);
+  int st = mf3d::inlets_ready(C, true);
   if (st) return st;
+  if ((st = mf3d::bind_fields(C, *C->view, fields))) return st;
   return mf3d::run_solve(C, &dt, &alfapr, info, hist, cap);
 }
 
@@ -2844,6 +3027,7 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
     set_error("mf3d_rungek_2nd_device: the 4th-order and WENO stages read three ghost layers (pl >= 3)");
     return MF3D_E_INVALID;
   }
+  if (int st = inlets_ready(C)) return st;
   View &V = *C->view;
   for (size_t b = 0; b < V.blk.size(); ++b) {
     const mf3d_block_desc &d = V.blk[b]->d;
@@ -2950,6 +3134,7 @@ int mf3d_newsolv_mg(mf3d_ctx *C, const mf3d_fields *fields, double dt, double al
   if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   mf3d::AllocScope scope(C->stream);
+  if (int st = mf3d::inlets_ready(C, true)) return st;
   return mf3d::host_solve(C, fields, &dt, &alfapr, info, hist, cap);
 }
 
@@ -2981,6 +3166,70 @@ int mf3d_mgkcyc_device_noalloc(mf3d_ctx *C, double *const *su, double *const *pp
 }
 
 long long mf3d_last_launch_count(const mf3d_ctx *C) { return C ? C->launches : 0; }
+
+int mf3d_bind_old_velocity(mf3d_ctx *C, const mf3d_rk_fields *rk) {
+  if (!C || !C->view || C->doms.size() != 1) { mf3d::set_error("mf3d_bind_old_velocity: bad arguments"); return MF3D_E_INVALID; }
+  mf3d::View &V = *C->view;
+  if (!rk) {
+    C->oo_bound.clear();
+    for (auto &F : V.hf) F.oo[0] = F.oo[1] = F.oo[2] = nullptr;
+    return MF3D_OK;
+  }
+  std::vector<std::array<const double *, 3>> oo(V.blk.size());
+  for (size_t b = 0; b < V.blk.size(); ++b) {
+    if (!rk[b].uoo || !rk[b].voo || !rk[b].woo) {
+      mf3d::set_error("mf3d_bind_old_velocity: a pointer is NULL");
+      return MF3D_E_INVALID;
+    }
+    oo[b] = {rk[b].uoo, rk[b].voo, rk[b].woo};
+  }
+  C->oo_bound = oo;
+  for (size_t b = 0; b < V.blk.size(); ++b)
+    for (int a = 0; a < 3; ++a) V.hf[b].oo[a] = oo[b][a];
+  return MF3D_OK;
+}
+
+int mf3d_set_inlet(mf3d_ctx *C, int block_id, int code, int uprof_sem, const double *values, long long n) {
+  if (!C || !values || C->doms.size() != 1 || !C->view) {
+    mf3d::set_error("mf3d_set_inlet: bad arguments");
+    return MF3D_E_INVALID;
+  }
+  if (!C->prm.bounds) { mf3d::set_error("mf3d_set_inlet: a context with bounds = 1"); return MF3D_E_INVALID; }
+  mf3d::DomainStore &D = *C->doms[0];
+  for (size_t b = 0; b < D.blocks.size(); ++b) {
+    mf3d::BlockStore &S = *D.blocks[b];
+    if (S.d.id != block_id) continue;
+    if (S.d.iprev >= 0 || S.d.bc_west != code || (code != 7 && code != 8)) {
+      mf3d::set_error("mf3d_set_inlet: block " + std::to_string(block_id) + " has no west face of code " +
+                      std::to_string(code) + " (7 or 8)");
+      return MF3D_E_INVALID;
+    }
+    const long long want = code == 7 ? (long long)(S.d.ny + 2) * (S.d.nz + 2) : (long long)(S.d.ny + 1) * (S.d.nz + 1);
+    if (n != want) {
+      mf3d::set_error("mf3d_set_inlet: " + std::to_string(want) + " values expected, got " + std::to_string(n));
+      return MF3D_E_INVALID;
+    }
+    if (code == 8 && uprof_sem == 12 && (S.d.hy || S.d.hz)) {
+      mf3d::set_error("mf3d_set_inlet: the power-law profile reads uniform cell centres");
+      return MF3D_E_UNSUPPORTED;
+    }
+    if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+    std::vector<mf3d_block_desc> descs;
+    for (auto &T : D.blocks) descs.push_back(T->d);
+    int st = mf3d::install_inlet(C, S, mf3d::domain_extents(descs.data(), (int)descs.size()), code, uprof_sem, values);
+    if (st) return st;
+    // the view's copy of the block (the solve uploads it with the fields)
+    for (size_t v = 0; v < C->view->blk.size(); ++v)
+      if (C->view->blk[v] == &S) {
+        C->view->hf[v].inl = S.fld.inl;
+        C->view->hf[v].inl_s1 = S.fld.inl_s1;
+        C->view->hf[v].inl_t1 = S.fld.inl_t1;
+      }
+    return MF3D_OK;
+  }
+  mf3d::set_error("mf3d_set_inlet: no block " + std::to_string(block_id));
+  return MF3D_E_INVALID;
+}
 
 int mf3d_tuning(const mf3d_ctx *C, int level, int *sweep_schedule, int *small_sweep, int *restrict_planes,
                 int *cluster_ctas) {

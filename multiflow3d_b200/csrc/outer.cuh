@@ -50,6 +50,9 @@ struct BlkFld {
   long long bcplane;                 // elements per receive plane (the largest ttc plane)
   const double *oo[3];               // velocity predictor: u, v, w at the start of the time step
   const double *vis;                 // velocity predictor: cell viscosity (ttc layout)
+  const double *inl;                 // west inlet (codes 7, 8, 12, 13): u over level-1 rows 0..ny+1,
+                                     // planes 0..nz+1, row fastest; null = not set
+  int inl_s1, inl_t1;                // last row / plane the inlet writes (code 8: ny, nz)
 };
 
 // x / h.  When h is a power of two the multiplication by its reciprocal
@@ -429,7 +432,9 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   if (!F.wall[f]) return;
   const int code = F.bcode[f];
   const bool normal = comp == ax;
-  int mode = 0;  // 1 constant cv, 2 -mirror, 3 +mirror, 4 copy of the last face
+  // 1 constant cv, 2 -mirror, 3 +mirror, 4 copy of the last face,
+  // 5 convective outflow, 6 the inlet plane
+  int mode = 0;
   double cv = 0.0;
   if (code == 4) mode = normal ? 1 : 2;
   else if (code == 3 && ax != 0) mode = normal ? 1 : 3;
@@ -438,6 +443,12 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
     cv = ax == 0 ? (comp == 0 ? ubulk : 0.0) : (comp == 2 ? 1.1 : 0.0);
   } else if (code == 2 && ax == 0 && side == 1 && alfabc == 1) mode = 4;  // outflow: u(ie+1+ly) = u(ie)
   else if (code == 21 && ax == 0 && side == 1 && alfabc == 1 && F.oo[comp]) mode = 5;  // convective outflow
+  else if (f == 0 && (code == 7 || code == 8 || code == 12 || code == 13)) {
+    // the inlets (bounds.for:55-135): u from the inlet plane; code 12 also
+    // sets v = w = 0 (:374-377, 662-665); 7, 8, 13 leave v and w
+    if (comp == 0 && F.inl) mode = 6;
+    else if (comp != 0 && code == 12) mode = 1;
+  }
   if (!mode) return;
   // the widened ranges of the other two axes: 0 .. end+1
   const int as = ax == 0 ? 1 : 0, at = ax == 2 ? 1 : 2;
@@ -445,7 +456,15 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   double *fi = comp_field(F, comp);
   const int s0 = 1, e0 = comp_end(F, comp, ax);
   const long long g = fidx_ax(F, ax, side ? e0 + 1 + ly : s0 - 1 - ly, sl, tl);
+  if (mode == 6) {
+    if (sl <= F.inl_s1 && tl <= F.inl_t1) fi[g] = F.inl[(long long)tl * (F.ny + 2) + sl];
+    return;
+  }
   if (mode == 5) {  // oo(ie+1+ly) - dt*alfapr*(oo(ie+1+ly) - oo(ie))/dx, from the start-of-step velocity
+    if (dt < 0.0) {  // the solve's own dt and alfapr
+      dt = ds[F.dom].dt;
+      alfapr = ds[F.dom].alfapr;
+    }
     const double *oo = F.oo[comp];
     const double og = oo[g], oe = oo[fidx_ax(F, ax, e0, sl, tl)];
     fi[g] = og - dt * alfapr * (og - oe) / F.h[0][1];

@@ -101,11 +101,50 @@ class Projection:
     def launches(self) -> int:
         return int(self.lib.mf3d_last_launch_count(self.ctx))
 
+    def set_inlet(self, block_id: int, code: int, values, uprof_sem: int = 0):
+        """The inlet values of a west face of code 7 or 8 (mf3d_set_inlet):
+        ``values`` as ``read_inlet_file`` returns them."""
+        v = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        abi.check(self.lib, self.lib.mf3d_set_inlet(self.ctx, int(block_id), int(code), int(uprof_sem),
+                                                    v.ctypes.data_as(_dp), v.size), "mf3d_set_inlet")
+
+    def bind_old_velocity(self, blocks=None):
+        """uoo, voo, woo (device tensors, one dict per block) for the
+        convective outflow of the solve's bounds (mf3d_bind_old_velocity);
+        None unbinds.  The tensors stay borrowed until the next call."""
+        if blocks is None:
+            self._oo = None
+            abi.check(self.lib, self.lib.mf3d_bind_old_velocity(self.ctx, None), "mf3d_bind_old_velocity")
+            return
+        arr = (abi.RkFields * len(blocks))()
+        for b, f in enumerate(blocks):
+            for k in ("uoo", "voo", "woo"):
+                setattr(arr[b], k, C.cast(C.c_void_p(f[k].data_ptr()), _dp))
+        self._oo = (arr, blocks)
+        abi.check(self.lib, self.lib.mf3d_bind_old_velocity(self.ctx, arr), "mf3d_bind_old_velocity")
+
     def tuning(self, level: int) -> dict:
         """Launch shapes chosen for one level (mf3d_tuning)."""
         v = [C.c_int() for _ in range(4)]
         abi.check(self.lib, self.lib.mf3d_tuning(self.ctx, level, *[C.byref(x) for x in v]), "mf3d_tuning")
         return dict(zip(("sweep_schedule", "small_sweep", "restrict_planes", "cluster_ctas"), (x.value for x in v)))
+
+
+def read_inlet_file(path: str, code: int) -> np.ndarray:
+    """The values boundu reads from an inlet file (bounds.for:55-103): code 7
+    (Inlet/Inlet_<dom>_<n>.dat) one u per line; code 8
+    (inflow/Inlet_<dom>_<n>.dat) two header lines, then "up dummy dummy" per
+    line, of which the first column.  In file order (k outer, j inner), as
+    ``Projection.set_inlet`` takes them."""
+    with open(path) as f:
+        lines = f.read().splitlines()
+    if code == 7:
+        rows = [ln for ln in lines if ln.strip()]
+        return np.array([float(ln.split()[0].replace("D", "E").replace("d", "e")) for ln in rows])
+    if code == 8:
+        rows = [ln for ln in lines[2:] if ln.strip()]
+        return np.array([float(ln.split()[0].replace("D", "E").replace("d", "e")) for ln in rows])
+    raise ValueError("inlet files exist for the west codes 7 and 8")
 
 
 def _dev_fields(blocks):

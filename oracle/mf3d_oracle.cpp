@@ -37,6 +37,7 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <chrono>
 #include <thread>
@@ -70,6 +71,9 @@ struct Blk {
   bool stretched;
   /* the velocity predictor: uoo, voo, woo (the convective outflow, code 21) */
   const double *oo[3] = {nullptr, nullptr, nullptr};
+  /* west inlet of the codes 7, 8 (the file's values) and 12, 13 (the
+   * power-law profile): u over j = js-1..je+1, k = ks-1..ke+1, j fastest */
+  std::vector<double> inlet;
 };
 
 /* The reference runs one MPI rank per block; the restatement runs the
@@ -107,7 +111,21 @@ struct Ctx {
   int differencing; /* 2: calmas' 4th-order divergence (press.for:13-35) */
   bool periodic;
   double dt, alfapr, rmax;
+  double yst, yen, zst, zen; /* extents of the whole domain (alloc_dom.for:427-439) */
 };
+
+/* The inlet files of the west codes 7 (Inlet/Inlet_<dom>_<n>.dat: u per
+ * line) and 8 (inflow/Inlet_<dom>_<n>.dat: two header lines, then
+ * "up dummy dummy" per line) stand here as value arrays registered per block
+ * id, together with UPROF_SEM for code 8 (initial.for:37). */
+struct InletFile {
+  int code, uprof;
+  std::vector<double> v;
+};
+std::map<int, InletFile> g_inlets;
+/* uoo, voo, woo per block position for the convective outflow (code 21) of
+ * the solve's boundu/v/w; empty = none */
+std::vector<std::array<const double *, 3>> g_old;
 
 inline double &F(Blk &B, double *a, int i, int j, int k) {
   return a[(size_t)(i - 1) + (size_t)B.ttc_i * ((size_t)(j - 1) + (size_t)B.ttc_j * (size_t)(k - 1))];
@@ -975,16 +993,69 @@ void pbound(Ctx &C) {
  * 369-373, 444-448, 505-533, 535-548, 588-595 for v; 657-661, 738-742,
  * 799-806, 833-840, 866-876, 900-908 for w.) */
 bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc, bool have_oo = false) {
-  /* the branches that read data outside the projection: inflow files, SEM
-   * and power-law inlets (west 7, 8, 12, 13), the convective outflow (east
-   * 21) unless uoo, voo, woo are at hand (the velocity predictor), wall
-   * functions (61+), phi-gated inflow/outflow under L_LSM */
+  /* the branches that read data outside the projection: the convective
+   * outflow (east 21) unless uoo, voo, woo are at hand (the velocity
+   * predictor), wall functions (61+), phi-gated inflow/outflow under L_LSM.
+   * The inlet files of the west codes 7 and 8 come from g_inlets. */
   if (code >= 61) return true;
-  if (f == 0 && (code == 7 || code == 8 || code == 12 || code == 13)) return true;
   if (f == 1 && code == 21 && alfabc == 1 && !have_oo) return true;
   if (lsm && ((f == 0 && code == 1) || (f == 1 && (code == 2 || code == 21) && alfabc == 1))) return true;
   return false;
 }
+/* Cell-centre coordinate of field index c (1-based) along an axis of a
+ * block: x(1) = xsl + (1-pl)*dx, x(c) = x(c-1) + dx, xc(c) = x(c) - 0.5*dx
+ * (initial.for:341-365), the running sum in the reference's order. */
+double centre(double lo, double h, int pl, int c) {
+  double x = lo + (double)(-pl + 1) * h;
+  for (int i = 2; i <= c; ++i) x = x + h;
+  return x - 0.5 * h;
+}
+/* The 1/7 power-law inlet in y (bounds.for:105-112, 127-133, 86-93) */
+double power_law_y(const Ctx &C, double yc) {
+  const double H = C.yen - C.yst;
+  if (yc < H / 2) return C.ubulk * (1.0 + 1.0 / 7.0) * std::pow(std::fabs(2 * yc / H), 1. / 7.);
+  return C.ubulk * (1.0 + 1.0 / 7.0) * std::pow(std::fabs(2 * (H - yc) / H), 1.0 / 7.0);
+}
+/* ... times the same law in z (bounds.for:113-114, 94-95) */
+double power_law_z(const Ctx &C, double u, double zc) {
+  return u * (1.0 + 1. / 7.) * std::pow(std::fabs(zc / (C.zen - C.zst)), 1. / 7.);
+}
+
+/* boundu's west branches of the codes 7, 8, 12 and 13 on ghost layer ly
+ * (bounds.for:55-135). */
+void bound_inlet(const Ctx &C, Blk &B, int ly) {
+  const int code = B.d.bc_west;
+  const int is = B.isu, js = B.jsu, je = B.jeu, ks = B.ksu, ke = B.keu, pl = C.pl;
+  if (code == 7) {  /* one value per line, k outer (bounds.for:55-73) */
+    const std::vector<double> &v = g_inlets.at(B.d.id).v;
+    size_t r = 0;
+    for (int k = ks - 1; k <= ke + 1; ++k)
+      for (int j = js - 1; j <= je + 1; ++j) F(B, B.u, is - 1 - ly, j, k) = v[r++];
+  } else if (code == 8) {  /* SEM fluctuations on the interior rows and the low ghost row (:75-103) */
+    const InletFile &in = g_inlets.at(B.d.id);
+    size_t r = 0;
+    for (int kk = 1; kk <= ke - ks + 2; ++kk)
+      for (int jj = 1; jj <= je - js + 2; ++jj) {
+        const int k = kk + pl - 1, j = jj + pl - 1;
+        const double up = in.v[r++];
+        double &u = F(B, B.u, is - 1 - ly, j, k);
+        if (in.uprof == 12) {
+          u = power_law_y(C, centre(B.d.ysl, B.d.dy, pl, j));
+          u = power_law_z(C, u, centre(B.d.zsl, B.d.dz, pl, k)) + up;
+        } else {
+          u = C.ubulk + up;
+        }
+      }
+  } else if (code == 12 || code == 13) {  /* :105-135 */
+    for (int k = ks - 1; k <= ke + 1; ++k)
+      for (int j = js - 1; j <= je + 1; ++j) {
+        double &u = F(B, B.u, is - 1 - ly, j, k);
+        u = power_law_y(C, centre(B.d.ysl, B.d.dy, pl, j));
+        if (code == 12) u = power_law_z(C, u, centre(B.d.zsl, B.d.dz, pl, k));
+      }
+  }
+}
+
 void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
   const int ax = f / 2, comp = op - 1;
   const bool high = f & 1;
@@ -992,12 +1063,17 @@ void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
   const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
   if (nbr[f] >= 0) return;
   const int code = bcs[f];
+  if (f == 0 && op == 1 && (code == 7 || code == 8 || code == 12 || code == 13)) {
+    bound_inlet(C, B, ly);
+    return;
+  }
   const bool normal = ax == comp;
   int mode = 0; /* 0 nothing, 1 the constant cv, 2 -mirror, 3 +mirror, 4 copy of face ie */
   double cv = 0.0;
   if (code == 4) mode = normal ? 1 : 2;
   else if (code == 3 && ax != 0) mode = normal ? 1 : 3;
   else if (code == 1 && f == 0) { mode = 1; cv = comp == 0 ? C.ubulk : 0.0; }
+  else if (code == 12 && f == 0) { mode = 1; cv = 0.0; } /* v, w (bounds.for:374-377, 662-665) */
   else if (code == 1 && f == 4) { mode = 1; cv = comp == 2 ? 1.1 : 0.0; }
   else if (code == 2 && f == 1 && C.alfabc == 1) mode = 4;
   else if (code == 21 && f == 1 && C.alfabc == 1 && B.oo[op - 1]) mode = 5;
@@ -1611,6 +1687,21 @@ int pressure_1sweep(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
 
 std::string g_err;
 
+/* An inlet code on a west face without a neighbour: its file is there, and
+ * the profile codes read uniform cell centres (initial.for:341-365). */
+int inlet_check(const Blk &B) {
+  const int code = B.d.bc_west;
+  if (B.d.iprev >= 0 || !(code == 7 || code == 8 || code == 12 || code == 13)) return MF3D_OK;
+  if (code == 7 || code == 8) {
+    auto it = g_inlets.find(B.d.id);
+    if (it == g_inlets.end() || it->second.code != code) { g_err = "inlet values not set"; return MF3D_E_INVALID; }
+    const size_t n = code == 7 ? (size_t)(B.d.ny + 2) * (B.d.nz + 2) : (size_t)(B.d.ny + 1) * (B.d.nz + 1);
+    if (it->second.v.size() != n) { g_err = "inlet values: wrong count"; return MF3D_E_INVALID; }
+  }
+  if (code != 7 && (B.d.hy || B.d.hz)) { g_err = "power-law inlet on a stretched grid"; return MF3D_E_UNSUPPORTED; }
+  return MF3D_OK;
+}
+
 int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm) {
   if (nb <= 0 || !blocks || !prm) { g_err = "bad arguments"; return MF3D_E_INVALID; }
   if (prm->mg_itrsch < 1 || prm->mg_itrsch > 3) { g_err = "mg_itrsch"; return MF3D_E_INVALID; }
@@ -1632,6 +1723,11 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
   if (C.solver == 1 && (C.nswp < 1 || C.lsm)) { g_err = "solver 1: nswp >= 1, no lsm"; return MF3D_E_INVALID; }
   C.periodic = false;
   C.b.resize(nb);
+  C.yst = blocks[0].ysl; C.yen = blocks[0].yel; C.zst = blocks[0].zsl; C.zen = blocks[0].zel;
+  for (int ib = 1; ib < nb; ++ib) {
+    C.yst = std::min(C.yst, blocks[ib].ysl); C.yen = std::max(C.yen, blocks[ib].yel);
+    C.zst = std::min(C.zst, blocks[ib].zsl); C.zen = std::max(C.zen, blocks[ib].zel);
+  }
   for (int ib = 0; ib < nb; ++ib) {
     Blk &B = C.b[ib];
     B.d = blocks[ib];
@@ -1660,7 +1756,11 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
       const int bcs[6] = {B.d.bc_west, B.d.bc_east, B.d.bc_south, B.d.bc_north, B.d.bc_bottom, B.d.bc_top};
       const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
       for (int f = 0; f < 6; ++f)
-        if (nbr[f] < 0 && bounds_code_unsupported(f, bcs[f], C.lsm, C.alfabc)) { g_err = "bounds: face code"; return MF3D_E_UNSUPPORTED; }
+        if (nbr[f] < 0 && bounds_code_unsupported(f, bcs[f], C.lsm, C.alfabc, (size_t)ib < g_old.size()))
+          { g_err = "bounds: face code"; return MF3D_E_UNSUPPORTED; }
+      if (int st = inlet_check(B)) return st;
+      if ((size_t)ib < g_old.size())
+        for (int a = 0; a < 3; ++a) B.oo[a] = g_old[ib][a];
     }
     B.hx = level_widths(B.d.hx, B.d.nx, B.d.dx, B.ngrid);
     B.hy = level_widths(B.d.hy, B.d.ny, B.d.dy, B.ngrid);
@@ -1678,6 +1778,23 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
 extern "C" {
 
 const char *orc_last_error(void) { return g_err.c_str(); }
+
+/* The content of block `id`'s inlet file (west code 7: u per line; code 8:
+ * the first column "up" of the SEM file, UPROF_SEM = uprof); n values. */
+int orc_set_inlet(int id, int code, int uprof, const double *v, long long n) {
+  if ((code != 7 && code != 8) || n < 0 || (n && !v)) { g_err = "orc_set_inlet: bad arguments"; return MF3D_E_INVALID; }
+  g_inlets[id] = InletFile{code, uprof, std::vector<double>(v, v + n)};
+  return MF3D_OK;
+}
+void orc_clear_inlets(void) { g_inlets.clear(); }
+
+/* uoo, voo, woo of every block (position order) for the solve's convective
+ * outflow faces; nb = 0 unbinds. */
+int orc_bind_old_velocity(int nb, const double *const *uoo, const double *const *voo, const double *const *woo) {
+  g_old.clear();
+  for (int b = 0; b < nb; ++b) g_old.push_back({uoo[b], voo[b], woo[b]});
+  return MF3D_OK;
+}
 
 /* Threads for the per-block loops (1 = serial, the default). */
 void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
@@ -1724,6 +1841,7 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
     const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
     for (int f = 0; f < 6; ++f)
       if (nbr[f] < 0 && bounds_code_unsupported(f, bcs[f], false, alfabc, true)) { g_err = "bounds: face code"; return MF3D_E_UNSUPPORTED; }
+    if (int e = inlet_check(B)) return e;
   }
   C.dt = dt; C.alfapr = alfapr;
   std::vector<const double *> uoo(nb), voo(nb), woo(nb), vis(nb);

@@ -83,3 +83,109 @@ def test_bounds_inflow_outflow_every_cell(lib, oracle, cuda, layout):
     o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm,
                     pr.block_fields(seed=35, fourier_modes=2))
     assert_all_cells(o, g, pr.pl, pl_ex)
+
+
+INLETS = {
+    "code 12: 1/7 power law in y and z": (12, 0),
+    "code 13: 1/7 power law in y": (13, 0),
+    "code 7: inlet file values": (7, 0),
+    "code 8: SEM fluctuations on ubulk": (8, 0),
+    "code 8: SEM fluctuations on the power law (UPROF_SEM 12)": (8, 12),
+}
+
+
+def inlet_values(pr, desc, code, seed):
+    """Random inlet-file contents for every block with a west inlet face."""
+    rng = np.random.default_rng(seed)
+    vals = {}
+    for b in range(pr.nblocks):
+        if desc[b].iprev < 0:
+            n = (pr.ny + 2) * (pr.nz + 2) if code == 7 else (pr.ny + 1) * (pr.nz + 1)
+            vals[desc[b].id] = rng.uniform(-1.0, 1.0, n)
+    return vals
+
+
+@pytest.mark.parametrize("case", sorted(INLETS))
+def test_bounds_inlets_every_cell(lib, oracle, cuda, case):
+    """The west inlets of boundu (bounds.for:55-135): file values (7), SEM
+    fluctuations (8), the power-law profiles (12, 13), each on every ghost
+    layer 0..pl_ex, with v = w = 0 for code 12 (:374-377, 662-665); every
+    cell of u, v, w against the oracle."""
+    import ctypes as C
+    code, uprof = INLETS[case]
+    pr = Problem(2, 2, 1, 16, 16, 8, bc=(code, 2, W, W, S, S), ngrid=3, pl=2)
+    prm = pr.params(mg_itrsch=3, maxcy=40, eps=1e-9, pl_ex=1, bounds=1, alfabc=1, ubulk=0.7)
+    desc_l, desc_o = pr.descriptors(lib), pr.descriptors(oracle)
+    vals = inlet_values(pr, desc_l, code, 36) if code in (7, 8) else {}
+    for i, v in vals.items():
+        assert oracle.orc_set_inlet(i, code, uprof, v.ctypes.data_as(C.POINTER(C.c_double)), v.size) == 0
+    try:
+        o, g = run_both(lib, oracle, cuda, desc_l, desc_o, pr.nblocks, prm, pr.block_fields(seed=37, fourier_modes=2),
+                        prepare=lambda proj: [proj.set_inlet(i, code, v, uprof) for i, v in vals.items()])
+    finally:
+        oracle.orc_clear_inlets()
+    assert_all_cells(o, g, pr.pl, 1)
+    # the inlet is in place: u on the west ghost layers differs from the input
+    west = [b for b in range(pr.nblocks) if desc_l[b].iprev < 0]
+    assert west and all(np.any(g[1][b]["u"][:, :, pr.pl - 1] != 0.0) for b in west)
+
+
+def test_bounds_inlet_needs_values(lib, cuda):
+    """A code-7 inlet with no values: the solve refuses (the reference would
+    fail to open its file)."""
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.solver import Projection
+    pr = Problem(1, 1, 1, 16, 8, 8, bc=(7, 2, W, W, S, S), ngrid=3, pl=2)
+    prm = pr.params(mg_itrsch=3, maxcy=5, eps=1e-9, pl_ex=1, bounds=1, alfabc=1, ubulk=0.7)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    dev = [{k: torch.from_numpy(v).to(cuda) for k, v in f.items()} for f in pr.block_fields(seed=38)]
+    with pytest.raises(RuntimeError):
+        proj.newsolv_mg_device(dev)
+    with pytest.raises(RuntimeError):  # the wrong count
+        proj.set_inlet(0, 7, np.zeros(3))
+    proj.set_inlet(0, 7, np.zeros((pr.ny + 2) * (pr.nz + 2)))
+    assert proj.newsolv_mg_device(dev).status in (abi.MF3D_OK, abi.MF3D_NOT_CONVERGED)
+    proj.close()
+
+
+def test_bounds_convective_outflow_every_cell(lib, oracle, cuda):
+    """East code 21 with alfabc = 1 after the solve: the bound old
+    velocities (mf3d_bind_old_velocity) give every east ghost layer of u, v,
+    w (bounds.for:141-170, 449-474, 743-768) with the solve's dt and alfapr;
+    every cell against the oracle."""
+    import ctypes as C
+    import torch
+    from oracle_bridge import _dp
+    pr = Problem(2, 1, 2, 16, 8, 8, bc=(1, 21, W, W, S, S), ngrid=3, pl=2)
+    prm = pr.params(mg_itrsch=3, maxcy=40, eps=1e-9, pl_ex=1, bounds=1, alfabc=1, ubulk=0.7)
+    blocks = pr.block_fields(seed=39, fourier_modes=2)
+    rng = np.random.default_rng(40)
+    oo = [{k: rng.uniform(-1, 1, f["u"].shape) for k in ("uoo", "voo", "woo")} for f in blocks]
+    ptrs = [(_dp * pr.nblocks)(*[o[k].ctypes.data_as(_dp) for o in oo]) for k in ("uoo", "voo", "woo")]
+    dev_oo = [{k: torch.from_numpy(v).to(cuda) for k, v in o.items()} for o in oo]
+    oracle.orc_bind_old_velocity(pr.nblocks, *ptrs)
+    try:
+        o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks,
+                        dt=0.37, alfapr=1.3, prepare=lambda proj: proj.bind_old_velocity(dev_oo))
+    finally:
+        oracle.orc_bind_old_velocity(0, None, None, None)
+    assert_all_cells(o, g, pr.pl, 1)
+
+
+def test_bounds_convective_outflow_needs_old_velocities(lib, cuda):
+    import torch
+    from multiflow3d_b200.solver import Projection
+    pr = Problem(1, 1, 1, 16, 8, 8, bc=(1, 21, W, W, S, S), ngrid=3, pl=2)
+    prm = pr.params(mg_itrsch=3, maxcy=5, eps=1e-9, pl_ex=1, bounds=1, alfabc=1, ubulk=0.7)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    dev = [{k: torch.from_numpy(v).to(cuda) for k, v in f.items()} for f in pr.block_fields(seed=41)]
+    with pytest.raises(RuntimeError):
+        proj.newsolv_mg_device(dev)
+    oo = [{k: torch.zeros_like(f["u"]) for k in ("uoo", "voo", "woo")} for f in dev]
+    proj.bind_old_velocity(oo)
+    proj.newsolv_mg_device(dev)
+    proj.bind_old_velocity(None)
+    with pytest.raises(RuntimeError):
+        proj.newsolv_mg_device(dev)
+    proj.close()

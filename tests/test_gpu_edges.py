@@ -16,9 +16,10 @@ from multiflow3d_b200.solver import Projection
 pytestmark = pytest.mark.gpu
 
 
-def run_both(lib, oracle, cuda, desc_lib, desc_orc, nb, prm, blocks, dt=1.0, alfapr=1.0):
+def run_both(lib, oracle, cuda, desc_lib, desc_orc, nb, prm, blocks, dt=1.0, alfapr=1.0, prepare=None):
     """The same solve on the oracle (host arrays) and on the GPU (device
-    arrays); returns (oracle status, info, history, blocks), (GPU result, blocks)."""
+    arrays); returns (oracle status, info, history, blocks), (GPU result, blocks).
+    `prepare(proj)` runs on the GPU context before its solve."""
     import torch
     ref = [{k: v.copy() for k, v in f.items()} for f in blocks]
     info = SolveInfo()
@@ -29,6 +30,8 @@ def run_both(lib, oracle, cuda, desc_lib, desc_orc, nb, prm, blocks, dt=1.0, alf
     assert st >= 0, st
     dev = [{k: torch.from_numpy(v.copy()).to(cuda) for k, v in f.items()} for f in blocks]
     proj = Projection(desc_lib, prm, lib)
+    if prepare is not None:
+        prepare(proj)
     res = proj.newsolv_mg_device(dev, dt=dt, alfapr=alfapr)
     proj.close()
     got = [{k: v.cpu().numpy() for k, v in f.items()} for f in dev]

@@ -423,26 +423,106 @@ def test_bounds_inflow_outflow_known_answers(oracle):
     assert not np.array_equal(b2[0]["v"][Ki, Ji, pl + n + 1], b2[0]["v"][Ki, Ji, pl + n - 1])
 
 
-@pytest.mark.parametrize("bc,kw,ok", [
-    ((7, 2, WALL, WALL, WALL, WALL), {}, False),            # inflow slices read from files
-    ((12, 2, WALL, WALL, WALL, WALL), {}, False),           # power-law inlet
-    ((1, 21, WALL, WALL, WALL, WALL), {"alfabc": 1}, False),  # convective outflow reads uoo
-    ((1, 21, WALL, WALL, WALL, WALL), {"alfabc": 0}, True),   # ... unless alfabc skips it
-    ((1, 2, WALL, WALL, 61, WALL), {}, False),              # wall function
-    ((1, 2, WALL, WALL, WALL, WALL), {"lsm": 1}, False),    # phi-gated inflow under L_LSM
-    ((4, 4, 1, 2, 44, 6), {"alfabc": 1}, True),             # codes without a branch on those faces
+@pytest.mark.parametrize("bc,kw,expect", [
+    ((7, 2, WALL, WALL, WALL, WALL), {}, -1),               # inflow slices: no file values given
+    ((12, 2, WALL, WALL, WALL, WALL), {}, 0),               # power-law inlet
+    ((13, 2, WALL, WALL, WALL, WALL), {}, 0),
+    ((1, 21, WALL, WALL, WALL, WALL), {"alfabc": 1}, -6),   # convective outflow reads uoo
+    ((1, 21, WALL, WALL, WALL, WALL), {"alfabc": 0}, 0),    # ... unless alfabc skips it
+    ((1, 2, WALL, WALL, 61, WALL), {}, -6),                 # wall function
+    ((1, 2, WALL, WALL, WALL, WALL), {"lsm": 1}, -6),       # phi-gated inflow under L_LSM
+    ((4, 4, 1, 2, 44, 6), {"alfabc": 1}, 0),                # codes without a branch on those faces
 ])
-def test_bounds_face_codes(oracle, bc, kw, ok):
+def test_bounds_face_codes(oracle, bc, kw, expect):
     """The face codes whose boundu/v/w branch reads data outside the
-    projection are refused (MF3D_E_UNSUPPORTED); every other code runs, and
-    one without a branch for its face writes nothing there."""
+    projection are refused (MF3D_E_UNSUPPORTED), an inlet file that was never
+    given is invalid; every other code runs, and one without a branch for its
+    face writes nothing there."""
     pr = Problem(1, 1, 1, 8, 8, 8, bc=bc, ngrid=2, pl=1)
     blocks = pr.block_fields(seed=1)
     if kw.get("lsm"):
         for f, d in zip(blocks, pr.block_density(2)):
             f["dens"] = d
     st, _, _ = solve(oracle, pr, blocks, maxcy=2, bounds=1, **kw)
-    assert (st >= 0) if ok else (st == -6)
+    assert (st >= 0) if expect == 0 else (st == expect)
+
+
+def power_law(ubulk, yc, zc, H, Z, code):
+    """bounds.for:105-135 in numpy: the 1/7 law of the distance to the
+    nearer y wall, times the same law in z for code 12."""
+    a = np.where(yc < H / 2, ubulk * (1.0 + 1.0 / 7.0) * np.abs(2 * yc / H) ** (1.0 / 7.0),
+                 ubulk * (1.0 + 1.0 / 7.0) * np.abs(2 * (H - yc) / H) ** (1.0 / 7.0))
+    if code == 12:
+        a = a[None, :] * (1.0 + 1.0 / 7.0) * (np.abs(zc / Z) ** (1.0 / 7.0))[:, None]
+    else:
+        a = np.broadcast_to(a[None, :], (len(zc), len(yc)))
+    return a
+
+
+@pytest.mark.parametrize("code", [12, 13])
+def test_bounds_power_law_inlet_known_answer(oracle, code):
+    """Codes 12 and 13 put the 1/7 power-law profile on every west ghost
+    layer of u (bounds.for:105-135; cell centres xc = x - dx/2 from the
+    running sum x(i) = x(i-1) + dx, initial.for:341-365) and, for 12,
+    v = w = 0 there; 13 leaves v and w."""
+    n, pl, ubulk = 8, 2, 0.7
+    pr = Problem(1, 1, 1, 2 * n, n, n, bc=(code, 2, WALL, WALL, WALL, WALL), ngrid=2, pl=pl,
+                 dx=0.05, dy=0.1, dz=0.125)
+    blocks = pr.block_fields(seed=24)
+    before = {k: blocks[0][k].copy() for k in ("v", "w")}
+    st, _, _ = solve(oracle, pr, blocks, maxcy=4, eps=1e-12, pl_ex=1, bounds=1, alfabc=1, ubulk=ubulk)
+    assert st >= 0
+    d = pr.descriptors(oracle)[0]
+    y = np.cumsum(np.concatenate([[d.ysl + (1 - pl) * d.dy], np.full(n + 2 * pl - 1, d.dy)]))
+    z = np.cumsum(np.concatenate([[d.zsl + (1 - pl) * d.dz], np.full(n + 2 * pl - 1, d.dz)]))
+    yc, zc = y - 0.5 * d.dy, z - 0.5 * d.dz
+    # js..je, ks..ke: the wall faces after the west one (S, N, B, T) mirror
+    # into the ghost rows js-1, je+1, ks-1, ke+1 of the same layer
+    rows = slice(pl, pl + n)
+    want = power_law(ubulk, yc[rows], zc[rows], d.yel - d.ysl, d.zel - d.zsl, code)
+    u = blocks[0]["u"]
+    for ly in range(2):
+        np.testing.assert_allclose(u[rows, rows, pl - 1 - ly], want, rtol=1e-15, atol=0)  # numpy and libm pow
+        if code == 12:
+            assert not blocks[0]["v"][rows, rows, pl - 1 - ly].any()
+    if code == 13:  # the v and w west ghosts are left as calvel's exchange left them
+        assert not np.array_equal(blocks[0]["v"][:, :, pl - 1], 0 * before["v"][:, :, pl - 1])
+
+
+def test_bounds_inlet_files(oracle, tmp_path):
+    """Codes 7 and 8 take the inlet file's values (bounds.for:55-103): 7 one
+    u per line over rows js-1..je+1 and planes ks-1..ke+1; 8 ubulk plus the
+    first column of the SEM file (after two header lines) over rows js-1..je
+    and planes ks-1..ke only.  The files are written in the reference's
+    formats and read back with read_inlet_file."""
+    from multiflow3d_b200.solver import read_inlet_file
+    n, pl, ubulk = 8, 2, 0.7
+    rng = np.random.default_rng(3)
+    f7 = tmp_path / "Inlet_000_00001.dat"
+    v7 = rng.uniform(-1, 1, (n + 2) * (n + 2))
+    f7.write_text("".join(f"  {x:.17E}\n" for x in v7))
+    f8 = tmp_path / "Inlet_0000_000001.dat"
+    v8 = rng.uniform(-1, 1, (n + 1) * (n + 1))
+    f8.write_text("header one\nheader two\n" + "".join(f" {x:.17E}  1  2\n" for x in v8))
+    for code, path, vals in ((7, f7, v7), (8, f8, v8)):
+        got = read_inlet_file(str(path), code)
+        assert np.array_equal(got, vals)
+        pr = Problem(1, 1, 1, 2 * n, n, n, bc=(code, 2, WALL, WALL, WALL, WALL), ngrid=2, pl=pl)
+        blocks = pr.block_fields(seed=25)
+        assert oracle.orc_set_inlet(0, code, 0, got.ctypes.data_as(C.POINTER(C.c_double)), got.size) == 0
+        try:
+            st, _, _ = solve(oracle, pr, blocks, maxcy=3, eps=1e-12, pl_ex=1, bounds=1, alfabc=1, ubulk=ubulk)
+        finally:
+            oracle.orc_clear_inlets()
+        assert st >= 0
+        u = blocks[0]["u"]
+        # rows js..je, planes ks..ke (the wall faces mirror into the ghost rows)
+        I = slice(pl, pl + n)
+        for ly in range(2):
+            if code == 7:
+                assert np.array_equal(u[I, I, pl - 1 - ly], vals.reshape(n + 2, n + 2)[1:n + 1, 1:n + 1])
+            else:
+                assert np.array_equal(u[I, I, pl - 1 - ly], ubulk + vals.reshape(n + 1, n + 1)[1:, 1:])
 
 
 @pytest.mark.parametrize("nswp", [1, 4])
@@ -462,3 +542,38 @@ def test_sip_solver_reaches_the_multigrid_projection(oracle, nswp):
     assert np.abs(pb - pa).max() <= 1e-7 * np.abs(pa).max()
     for k in ("u", "v", "w"):
         assert np.abs(pr.gather(b, k) - pr.gather(a, k)).max() <= 1e-8
+
+
+def test_bounds_convective_outflow_in_the_solve(oracle):
+    """East code 21 with alfabc = 1 at the end of the solve (bounds.for:
+    141-170, 449-474, 743-768): every east ghost layer of u, v, w is
+    oo(ie+1+ly) - dt*alfapr*(oo(ie+1+ly) - oo(ie))/dx from the bound old
+    velocities, with the solve's dt and alfapr; with nothing bound the face
+    is refused."""
+    n, pl, dt, alfapr = 8, 2, 0.37, 1.3
+    pr = Problem(1, 1, 1, 2 * n, n, n, bc=(1, 21, WALL, WALL, WALL, WALL), ngrid=2, pl=pl)
+    blocks = pr.block_fields(seed=26)
+    rng = np.random.default_rng(27)
+    oo = {k: rng.uniform(-1, 1, blocks[0]["u"].shape) for k in ("uoo", "voo", "woo")}
+    ptrs = [(ob._dp * 1)(oo[k].ctypes.data_as(ob._dp)) for k in ("uoo", "voo", "woo")]
+    oracle.orc_bind_old_velocity(1, *ptrs)
+    try:
+        prm = pr.params(maxcy=4, eps=1e-12, pl_ex=1, bounds=1, alfabc=1, ubulk=0.7)
+        hist = np.zeros(4)
+        info = SolveInfo()
+        st = oracle.orc_newsolv_mg(pr.descriptors(oracle), 1, C.byref(prm), fields_struct(blocks), dt, alfapr,
+                                   C.byref(info), hist.ctypes.data_as(C.POINTER(C.c_double)), 4)
+    finally:
+        oracle.orc_bind_old_velocity(0, None, None, None)
+    assert st >= 0
+    J, K = slice(pl, pl + n), slice(pl, pl + n)
+    for k, ie in (("u", pl + 2 * n - 2), ("v", pl + 2 * n - 1), ("w", pl + 2 * n - 1)):
+        o = oo[k + "oo"]
+        Jc = slice(pl, pl + n - 1) if k == "v" else J  # v's last face is a wall face
+        Kc = slice(pl, pl + n - 1) if k == "w" else K
+        for ly in range(2):
+            g = ie + 1 + ly
+            want = o[Kc, Jc, g] - dt * alfapr * (o[Kc, Jc, g] - o[Kc, Jc, ie]) / pr.dx
+            assert np.array_equal(blocks[0][k][Kc, Jc, g], want), (k, ly)
+    st, _, _ = solve(oracle, pr, pr.block_fields(seed=26), maxcy=2, bounds=1, alfabc=1)
+    assert st == -6

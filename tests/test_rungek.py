@@ -311,4 +311,4 @@ def test_oracle_predictor_refuses_other_branches(oracle):
     assert orc_rk(oracle, pr, blocks, rk, 0.1, 1.0) == -6
     pr = Problem(1, 1, 1, 8, 8, 8, bc=(7, 2, W, W, W, W), ngrid=1, pl=1)
     blocks, rk = rk_inputs(pr, 5)
-    assert orc_rk(oracle, pr, blocks, rk, 0.1, 1.0, alfabc=1) == -6
+    assert orc_rk(oracle, pr, blocks, rk, 0.1, 1.0, alfabc=1) == -1  # code 7 with no inlet values
