@@ -119,10 +119,12 @@ typedef struct mf3d_params {
                        code with no branch for a face writes nothing there,
                        as in the reference; 21 on the east (convective
                        outflow, alfabc = 1) from the old velocities of
-                       mf3d_bind_old_velocity.  The codes that need data the
-                       library does not hold - 61 and up (wall functions),
-                       and 1 / 2 with lsm (phi) - return
-                       MF3D_E_UNSUPPORTED.  Also refreshes the
+                       mf3d_bind_old_velocity; the wall functions 61 to 65
+                       with the Re and fric of mf3d_set_wall_model.  The
+                       codes that need data the library does not hold -
+                       above 65 (no branch), 61 to 65 and 1 / 2 with lsm
+                       (mu, dens, phi) - return MF3D_E_UNSUPPORTED.  Also
+                       refreshes the
                        full periodic ghost planes of the final exchange(1..3).
                        Skipped when the solve diverged (the reference stops).
                        mf3d_create contexts only.  0: u, v, w face ghosts as
@@ -292,6 +294,32 @@ int mf3d_set_inlet(mf3d_ctx *ctx, int block_id, int code, int uprof_sem, const d
  * a bounds context with such a face and nothing bound returns
  * MF3D_E_INVALID.  mf3d_create contexts. */
 int mf3d_bind_old_velocity(mf3d_ctx *ctx, const mf3d_rk_fields *rk);
+
+/* Re and fric (control.cin) for the wall functions of boundu/v/w: codes 61
+ * (smooth wall, log law), 62 (rough wall, log law with the roughness fric),
+ * 63, 64, 65 (the Werner-Wengle 1/6, 1/7, 1/8 power laws) on faces without a
+ * neighbour (bounds.for:187-206 and the matching branches; log_law.for,
+ * wall_function.for).  At layer 0 a face's law gives the wall stress tau2
+ * per face cell from the first cell layer's tangential speed; the
+ * tangential component's first cell c takes c += sign(tau2*c/h, -c)*alfapr*dt
+ * and its ghost -c; deeper layers mirror; the normal component is 0.  The
+ * stresses stay in the context across calls (log_law keeps tau2 where y+ is
+ * below 11.067) and this call clears them.  The laws take CUDA's sqrt, log
+ * and pow, so the velocities they touch agree with the reference's libm to
+ * rounding, not bit for bit.  A smooth-wall law that does not converge in
+ * 10 steps (the reference stops) fails the call with MF3D_E_INVALID.  The
+ * reference sets the power laws' constants with DATA statements inside the
+ * CASE arms (wall_function.for:34-49); the library takes each arm's own
+ * pair.  Needs uniform spacing and two or more cells along the face
+ * normal; no lsm (the laws would read mu/dens). */
+int mf3d_set_wall_model(mf3d_ctx *ctx, double re, double fric);
+
+/* boundu, boundv, boundw alone (bounds.for:2-916) on device arrays u, v, w
+ * of `fields` (the other pointers must be set as for a solve), with the
+ * caller's dt, alfapr and alfabc: each component's periodic copy, then its
+ * faces W, E, S, N, B, T per ghost layer 0..pl_ex, every code the bounds
+ * mode of the solve handles.  mf3d_create contexts with bounds = 1, FP64. */
+int mf3d_bounds_device(mf3d_ctx *ctx, const mf3d_fields *fields, double dt, double alfapr, int alfabc);
 
 /* ---------------------------------------------------------------------- */
 /* Batches of independent domains (no counterpart in the reference, which   */

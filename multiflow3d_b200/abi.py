@@ -175,6 +175,8 @@ EXPORTED_SYMBOLS = (
     "mf3d_tuning",
     "mf3d_set_inlet",
     "mf3d_bind_old_velocity",
+    "mf3d_set_wall_model",
+    "mf3d_bounds_device",
     "mf3d_test_fail_alloc",
     "mf3d_test_stall_copy",
 )
@@ -240,6 +242,8 @@ def _declare(lib):
     lib.mf3d_tuning.argtypes = [vp, C.c_int] + [C.POINTER(C.c_int)] * 4
     lib.mf3d_set_inlet.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double), C.c_longlong]
     lib.mf3d_bind_old_velocity.argtypes = [vp, vp]
+    lib.mf3d_set_wall_model.argtypes = [vp, C.c_double, C.c_double]
+    lib.mf3d_bounds_device.argtypes = [vp, C.POINTER(Fields), C.c_double, C.c_double, C.c_int]
     lib.mf3d_test_fail_alloc.argtypes = [C.c_longlong]
     lib.mf3d_test_stall_copy.argtypes = [C.c_int, C.c_int]
     return lib

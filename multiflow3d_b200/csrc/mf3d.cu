@@ -332,6 +332,7 @@ struct BlockStore {
   bool lsm = false;      // variable-density coefficients, formed per solve
   BlkFld fld;            // host template (field pointers bound per call)
   DevBuf<double> inlet;  // west inlet plane of the codes 7, 8, 12, 13 (BlkFld::inl)
+  DevBuf<double> wall;   // wall functions: tau, tau2 planes of the six faces (BlkFld::wtau)
   size_t bytes = 0;      // device bytes owned
 };
 
@@ -836,6 +837,7 @@ struct View {
   DevBuf<int> budget;                 // iterations left in the server's bounded loop
   DevBuf<CUtensorMap> fmaps;          // per block: p, ustar, vstar, wstar (bound fields)
   bool fields_tma = false;            // bound fields admit the TMA calvel/calmas
+  bool wall_law = false;              // some block has wall-function faces (BlkFld::wtau)
   DevBuf<unsigned long long> rmax, rmax_scratch;
   DevBuf<double> hist;
   int hcap = 0;
@@ -902,6 +904,8 @@ struct mf3d_ctx {
   // mf3d_bind_old_velocity: uoo, voo, woo per block (view order) for the
   // convective outflow of the solve's boundu/v/w; empty = none bound
   std::vector<std::array<const double *, 3>> oo_bound;
+  // mf3d_set_wall_model: Re and fric (control.cin) of the wall functions
+  double wall_re = 0.0, wall_fric = 0.0;
 };
 
 namespace mf3d {
@@ -1432,6 +1436,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       F.src[f] = r.kind == FACE_WALL ? b : dom_base[d] + r.src;
     }
     V.hf[b] = F;
+    V.wall_law |= F.wtau != nullptr;
     const mf3d_block_desc &x = S.d;
     add_tiles_2d(t1, b, Box{1, x.nx, 1, x.ny, 1, x.nz}, RW_TX, RW_RJ, RW_KCH);
     add_tiles_2d(t2, b, Box{0, x.nx + 1, 0, x.ny + 1, 0, x.nz + 1}, RW_TX, RW_RJ, RW_KCH);
@@ -2230,12 +2235,13 @@ static int solve_begin(mf3d_ctx *C, View &V, const double *dt, const double *alf
 // self-copies and packs, the third walk's unpacks, each over x, y, z.
 // A face code whose boundu/v/w branch needs data the library does not hold:
 // the convective outflow of the east face (21, uoo; bounds.for:143-170)
-// outside the velocity predictor, wall functions (61 and up: log_law,
-// wall_function), and under L_LSM the inflow and outflow faces, which phi
-// gates (bounds.for:43-50, 146-158).  The inlet files of the west codes 7
-// and 8 come through mf3d_set_inlet.
+// without the old velocities, wall functions above 65 (no branch) or under
+// L_LSM (mu/dens, log_law.for:22), and under L_LSM the inflow and outflow
+// faces, which phi gates (bounds.for:43-50, 146-158).  The inlet files of
+// the west codes 7 and 8 come through mf3d_set_inlet, Re and fric of the
+// wall functions through mf3d_set_wall_model.
 static bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc, bool have_oo = false) {
-  if (code >= 61) return true;
+  if (code >= 61 && (code > 65 || lsm)) return true;
   if (f == 1 && code == 21 && alfabc == 1 && !have_oo) return true;
   if (lsm && ((f == 0 && code == 1) || (f == 1 && (code == 2 || code == 21) && alfabc == 1))) return true;
   return false;
@@ -2251,10 +2257,17 @@ static void bc_walks(mf3d_ctx *C, View &V, int only = -1) {
         ++C->launches;
       }
 }
-// the faces without a neighbour by their code, layers 0..pl_ex (only as above)
+// the faces without a neighbour by their code, layers 0..pl_ex (only as above);
+// dt < 0: the solve's dt and alfapr.  The wall functions of a tangential
+// component (one component at a time) run their face law first, on layer 0.
 static void bound_faces(mf3d_ctx *C, View &V, int alfabc, int only = -1, double dt = 0.0, double alfapr = 0.0) {
   for (int ly = 0; ly <= C->prm.pl_ex; ++ly)
     for (int a = 0; a < 3; ++a) {
+      if (V.wall_law && ly == 0 && only >= 0 && only != a) {
+        launch(k_wall_law, V.n_bcax[a], kTile, 0, C->stream, V.df.p, V.t_bcax[a].p, V.ds.p, a, C->wall_re,
+               C->wall_fric, V.err.p);
+        ++C->launches;
+      }
       launch(k_bound_faces, V.n_bcax[a], kTile, 0, C->stream, V.df.p, V.t_bcax[a].p, V.ds.p, a, ly, C->prm.ubulk,
              alfabc, only, dt, alfapr);
       ++C->launches;
@@ -2288,9 +2301,19 @@ static int solve_end(mf3d_ctx *C, View &V) {
   }
   if (C->prm.bounds) {
     // boundu/boundv/boundw (newsolv_mg.for:86-88); a convective outflow
-    // takes the solve's dt and alfapr (dt < 0) and the bound old velocities
-    bc_walks(C, V);
-    bound_faces(C, V, C->prm.alfabc, -1, -1.0, 0.0);
+    // takes the solve's dt and alfapr (dt < 0) and the bound old velocities.
+    // The components are independent but for the wall functions, whose laws
+    // read all three: then boundu, boundv, boundw one after the other, each
+    // with its own periodic copy first, as the reference runs them
+    if (V.wall_law) {
+      for (int comp = 0; comp < 3; ++comp) {
+        bc_walks(C, V, comp);
+        bound_faces(C, V, C->prm.alfabc, comp, -1.0, 0.0);
+      }
+    } else {
+      bc_walks(C, V);
+      bound_faces(C, V, C->prm.alfabc, -1, -1.0, 0.0);
+    }
   }
   return MF3D_OK;
 }
@@ -2302,6 +2325,10 @@ static int check_device_error(View &V) {
   CK(cudaMemcpy(&e, V.err.p, sizeof(int), cudaMemcpyDeviceToHost));
   if (e == 0) return MF3D_OK;
   CK(cudaMemset(V.err.p, 0, sizeof(int)));
+  if (e == ERR_WALL_LAW) {
+    set_error("log_law: USTAR DOESNT CONVERGE (a smooth-wall law took 10 steps, log_law.for:47-62)");
+    return MF3D_E_INVALID;
+  }
   set_error("a device copy did not complete within its time limit (code " + std::to_string(e) + ")");
   return MF3D_E_TIMEOUT;
 }
@@ -2629,9 +2656,23 @@ static int install_inlet(mf3d_ctx *C, BlockStore &S, const Extents &e, int code,
 static bool inlet_code(const mf3d_block_desc &d) {
   return d.iprev < 0 && (d.bc_west == 7 || d.bc_west == 8 || d.bc_west == 12 || d.bc_west == 13);
 }
-// Every code-7 and code-8 inlet of a bounds context has its plane; with
-// `outflow` (the solve's boundu/v/w), every convective outflow face (code 21,
-// alfabc = 1) has the old velocities (mf3d_bind_old_velocity).
+// The wall-function codes (61 to 65) of a block's faces without a neighbour:
+// bit f set for face f; `rough` when one of them is 62.
+static int wall_law_faces(const mf3d_block_desc &d, bool *rough = nullptr) {
+  const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+  const int nbrs[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+  int m = 0;
+  for (int f = 0; f < 6; ++f)
+    if (nbrs[f] < 0 && bcs[f] >= 61 && bcs[f] <= 65) {
+      m |= 1 << f;
+      if (rough && bcs[f] == 62) *rough = true;
+    }
+  return m;
+}
+// Every code-7 and code-8 inlet of a bounds context has its plane, every
+// wall-function face its Re (and fric); with `outflow` (bounds run with
+// alfabc = 1), every convective outflow face (code 21) has the old
+// velocities (mf3d_bind_old_velocity).
 static int inlets_ready(const mf3d_ctx *C, bool outflow = false) {
   if (!C->prm.bounds) return MF3D_OK;
   for (const auto &D : C->doms)
@@ -2641,9 +2682,15 @@ static int inlets_ready(const mf3d_ctx *C, bool outflow = false) {
                   " and no inlet values (mf3d_set_inlet)");
         return MF3D_E_INVALID;
       }
-      if (outflow && S->d.inext < 0 && S->d.bc_east == 21 && C->prm.alfabc == 1 && C->oo_bound.empty()) {
+      if (outflow && S->d.inext < 0 && S->d.bc_east == 21 && C->oo_bound.empty()) {
         set_error("bounds: block " + std::to_string(S->d.id) +
                   " has a convective outflow (code 21, alfabc 1) and no old velocities (mf3d_bind_old_velocity)");
+        return MF3D_E_INVALID;
+      }
+      bool rough = false;
+      if (wall_law_faces(S->d, &rough) && (C->wall_re <= 0.0 || (rough && C->wall_fric <= 0.0))) {
+        set_error("bounds: block " + std::to_string(S->d.id) +
+                  " has wall-function faces and no Re (or no fric for code 62): mf3d_set_wall_model");
         return MF3D_E_INVALID;
       }
     }
@@ -2675,6 +2722,20 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
                     std::to_string(bcs[f]) + ", whose boundu/v/w branch needs data the library does not hold");
           return MF3D_E_UNSUPPORTED;
         }
+    }
+    if (prm->bounds && wall_law_faces(d)) {
+      const int m = wall_law_faces(d);
+      const int n[3] = {d.nx, d.ny, d.nz};
+      for (int f = 0; f < 6; ++f)
+        if (((m >> f) & 1) && n[f / 2] < 2) {
+          set_error("bounds: a wall-function face of block " + std::to_string(d.id) +
+                    " with one cell along its normal (the two faces' laws would read each other's updates)");
+          return MF3D_E_UNSUPPORTED;
+        }
+      if (d.hx || d.hy || d.hz) {
+        set_error("bounds: the wall functions of block " + std::to_string(d.id) + " read uniform spacings");
+        return MF3D_E_UNSUPPORTED;
+      }
     }
     if (prm->bounds && inlet_code(d) && d.bc_west != 7 && (d.hy || d.hz)) {
       set_error("bounds: the power-law inlet of block " + std::to_string(d.id) +
@@ -2709,10 +2770,21 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
     return st;
   if (prm->bounds) {
     const Extents e = domain_extents(blocks, nb);
-    for (auto &S : C->doms[0]->blocks)
+    for (auto &S : C->doms[0]->blocks) {
       if (inlet_code(S->d) && (S->d.bc_west == 12 || S->d.bc_west == 13) &&
           (st = install_inlet(C.get(), *S, e, S->d.bc_west, 0, nullptr)))
         return st;
+      if (wall_law_faces(S->d)) {
+        // the wall stresses of the six faces, zero at the start
+        // (initial.for:878-883) and kept across calls
+        const long long ti = S->d.nx + 2 * prm->pl, tj = S->d.ny + 2 * prm->pl, tk = S->d.nz + 2 * prm->pl;
+        S->fld.wplane = std::max(tj * tk, std::max(ti * tk, ti * tj));
+        if ((st = S->wall.alloc((size_t)12 * S->fld.wplane))) return st;
+        CK(cudaMemsetAsync(S->wall.p, 0, S->wall.n * sizeof(double), C->stream));
+        S->fld.wtau = S->wall.p;
+      }
+    }
+    CK(cudaStreamSynchronize(C->stream));
   }
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
@@ -3008,7 +3080,7 @@ int mf3d_newsolv_mg_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, do
   if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   mf3d::AllocScope scope(C->stream);
-  int st = mf3d::inlets_ready(C, true);
+  int st = mf3d::inlets_ready(C, C->prm.alfabc == 1);
   if (st) return st;
   if ((st = mf3d::bind_fields(C, *C->view, fields))) return st;
   return mf3d::run_solve(C, &dt, &alfapr, info, hist, cap);
@@ -3085,7 +3157,43 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
   }
   const cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) { set_error(std::string("mf3d_rungek_2nd_device: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
-  return MF3D_OK;
+  return check_device_error(V);
+}
+
+int mf3d_bounds_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr, int alfabc) {
+  using namespace mf3d;
+  if (!C || !fields) { set_error("mf3d_bounds_device: bad arguments"); return MF3D_E_INVALID; }
+  if (C->view->dom.size() != 1) { set_error("mf3d_bounds_device: mf3d_create contexts only"); return MF3D_E_INVALID; }
+  if (!C->prm.bounds || C->elem != 8) {
+    set_error("mf3d_bounds_device: needs a context with bounds = 1, FP64");
+    return MF3D_E_UNSUPPORTED;
+  }
+  View &V = *C->view;
+  for (size_t b = 0; b < V.blk.size(); ++b) {
+    const mf3d_block_desc &d = V.blk[b]->d;
+    const int bcs[6] = {d.bc_west, d.bc_east, d.bc_south, d.bc_north, d.bc_bottom, d.bc_top};
+    const int nbrs[6] = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+    for (int f = 0; f < 6; ++f)
+      if (nbrs[f] < 0 && bounds_code_unsupported(f, bcs[f], C->prm.lsm != 0, alfabc, true)) {
+        set_error("mf3d_bounds_device: face code " + std::to_string(bcs[f]) + " reads data the library does not hold");
+        return MF3D_E_UNSUPPORTED;
+      }
+  }
+  if (int st = inlets_ready(C, alfabc == 1)) return st;
+  if (cudaSetDevice(C->device) != cudaSuccess) { set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  AllocScope scope(C->stream);
+  int st = bind_fields(C, V, fields);
+  if (st) return st;
+  C->launches = 0;
+  CK(cudaMemsetAsync(V.ds.p, 0, V.ds.n * sizeof(DomState), C->stream));  // no domain marked diverged
+  // boundu, boundv, boundw, each with its periodic copy first
+  for (int comp = 0; comp < 3; ++comp) {
+    bc_walks(C, V, comp);
+    bound_faces(C, V, alfabc, comp, dt, alfapr);
+  }
+  const cudaError_t e = cudaStreamSynchronize(C->stream);
+  if (e != cudaSuccess) { set_error(std::string("mf3d_bounds_device: ") + cudaGetErrorString(e)); return MF3D_E_CUDA; }
+  return check_device_error(V);
 }
 
 int mf3d_calvel_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr) {
@@ -3134,7 +3242,7 @@ int mf3d_newsolv_mg(mf3d_ctx *C, const mf3d_fields *fields, double dt, double al
   if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   mf3d::AllocScope scope(C->stream);
-  if (int st = mf3d::inlets_ready(C, true)) return st;
+  if (int st = mf3d::inlets_ready(C, C->prm.alfabc == 1)) return st;
   return mf3d::host_solve(C, fields, &dt, &alfapr, info, hist, cap);
 }
 
@@ -3166,6 +3274,23 @@ int mf3d_mgkcyc_device_noalloc(mf3d_ctx *C, double *const *su, double *const *pp
 }
 
 long long mf3d_last_launch_count(const mf3d_ctx *C) { return C ? C->launches : 0; }
+
+int mf3d_set_wall_model(mf3d_ctx *C, double re, double fric) {
+  if (!C || !C->view || C->doms.size() != 1 || !(re >= 0.0) || !(fric >= 0.0)) {
+    mf3d::set_error("mf3d_set_wall_model: bad arguments");
+    return MF3D_E_INVALID;
+  }
+  if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
+  C->wall_re = re;
+  C->wall_fric = fric;
+  for (auto &S : C->doms[0]->blocks)
+    if (S->wall.p && cudaMemsetAsync(S->wall.p, 0, S->wall.n * sizeof(double), C->stream) != cudaSuccess) {
+      mf3d::set_error("mf3d_set_wall_model: clearing the wall stresses failed");
+      return MF3D_E_CUDA;
+    }
+  if (cudaStreamSynchronize(C->stream) != cudaSuccess) { mf3d::set_error("mf3d_set_wall_model: sync"); return MF3D_E_CUDA; }
+  return MF3D_OK;
+}
 
 int mf3d_bind_old_velocity(mf3d_ctx *C, const mf3d_rk_fields *rk) {
   if (!C || !C->view || C->doms.size() != 1) { mf3d::set_error("mf3d_bind_old_velocity: bad arguments"); return MF3D_E_INVALID; }

@@ -53,6 +53,8 @@ struct BlkFld {
   const double *inl;                 // west inlet (codes 7, 8, 12, 13): u over level-1 rows 0..ny+1,
                                      // planes 0..nz+1, row fastest; null = not set
   int inl_s1, inl_t1;                // last row / plane the inlet writes (code 8: ny, nz)
+  double *wtau;                      // wall functions (codes 61-65): tau, tau2 of face f at
+  long long wplane;                  // wtau + (2f or 2f+1)*wplane, ttc face planes; else null
 };
 
 // x / h.  When h is a power of two the multiplication by its reciprocal
@@ -410,6 +412,96 @@ __global__ void k_bc_walk(const BlkFld *__restrict__ fl, const Tile *__restrict_
 // x-face symmetry, periodic faces and codes without a branch write nothing.
 // Launched per layer for x, y, z (the reference's W, E, S, N, B, T).
 // Skipped after a diverged solve.
+// log_law (log_law.for:2-310, codes 61 smooth and 62 rough) and
+// wall_function (wall_function.for:2-250, the power laws of 63, 64, 65) of
+// the two faces of axis `ax` with a wall-function code: per cell of the
+// face's plane (the cell ranges widened by one) the tangential speed of the
+// first cell layer,
+//   vtan = sqrt(|uc*uc + vc*vc + wc*wc - vnor*vnor + 1e-30|),
+// cell-centred uc, vc, wc and vnor along the inward normal, and the wall
+// stress tau, tau2 = tau/vtan into the face's planes.  log_law keeps the old
+// tau2 where y+ is below 11.067 (11.63 on the top face).  The smooth-wall
+// iteration records ERR_WALL_LAW where it does not converge in 10 steps
+// (the reference prints and stops).  Transcendentals (sqrt, log, pow) are
+// CUDA's.  Launched over the bounds tiles of the axis (before the faces'
+// k_bound_faces of the same layer and component).
+__global__ void k_wall_law(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
+                           const DomState *__restrict__ ds, int ax, double re, double fric, int *err) {
+  pdl_wait();
+  const Tile t = tiles[blockIdx.x];
+  const BlkFld &F = fl[t.blk];
+  if (ds[F.dom].rmax > 100.0 || !F.wtau) return;
+  const int pl = F.pl;
+  const int m1 = (ax == 0 ? F.ny : F.nx) + 2 * pl, m2 = (ax == 2 ? F.ny : F.nz) + 2 * pl;
+  int q = t.i0 + threadIdx.x;
+  const int plane = m1 * m2;
+  if (q >= 2 * plane) return;
+  const int side = q / plane;
+  q -= side * plane;
+  const int sl = q % m1 + 1 - pl, tl = q / m1 + 1 - pl;
+  const int f = 2 * ax + side;
+  const int code = F.bcode[f];
+  if (!F.wall[f] || code < 61) return;
+  const int n1 = ax == 0 ? F.ny : F.nx, n2 = ax == 2 ? F.ny : F.nz;
+  if (sl < 0 || sl > n1 + 1 || tl < 0 || tl > n2 + 1) return;
+  const int fix = side ? (ax == 0 ? F.nx : ax == 1 ? F.ny : F.nz) : 1;
+  const int i = ax == 0 ? fix : sl, j = ax == 0 ? sl : ax == 1 ? fix : tl, k = ax == 2 ? fix : tl;
+  const double rrey = 1.0 / re, small = 1.e-30, kappa = 0.41, Ecte = 9.0;
+  const double delta = F.h[ax][1];
+  const double nx = ax == 0 ? (side ? -1.0 : 1.0) : 0.0, ny = ax == 1 ? (side ? -1.0 : 1.0) : 0.0,
+               nz = ax == 2 ? (side ? -1.0 : 1.0) : 0.0;
+  const long long c = fidx(F, i, j, k);
+  const long long sy = F.ti, sz = (long long)F.ti * F.tj;
+  const double uc = 0.5 * (F.u[c] + F.u[c - 1]);
+  const double vc = 0.5 * (F.v[c] + F.v[c - sy]);
+  const double wc = 0.5 * (F.w[c] + F.w[c - sz]);
+  const double vnor = nx * uc + ny * vc + nz * wc;
+  const double vtan = sqrt(fabs(uc * uc + vc * vc + wc * wc - vnor * vnor + small));
+  const long long e = (long long)(tl + pl - 1) * m1 + (sl + pl - 1);
+  double *tau = F.wtau + 2 * f * F.wplane, *tau2 = tau + F.wplane;
+  if (code >= 63) {
+    // the 1/6, 1/7 and 1/8 power laws (wall_function.for:34-49)
+    const double aaa = 8.3, bbb = code == 63 ? 0.1666666666 : code == 64 ? 0.1428571429 : 0.125;
+    const double const1 = 0.5 * (1. - bbb) * pow(aaa, (1. + bbb) / (1. - bbb));
+    const double const2 = (1. + bbb) / aaa;
+    const double const3 = pow(aaa, 2. / (1. - bbb));
+    const double const4 = 2. / (1. + bbb);
+    const double dycell = 2. * delta, rycell = 1. / dycell;
+    const double vtankr = 0.5 * rrey * rycell * const3;
+    const double dvtan = vtankr - vtan;
+    const double sub = fmax(copysign(1., dvtan), 0.);
+    const double tausub = rrey * vtan / delta;
+    const double taupow = pow(const1 * pow(rrey * rycell, 1. + bbb) + (const2 * pow(rrey * rycell, bbb)) * vtan, const4);
+    tau[e] = (sub * tausub + (1. - sub) * taupow);
+    tau2[e] = tau[e] / vtan;
+    return;
+  }
+  double ustar = 0.0, yplus = 0.0;
+  if (code == 62) {
+    ustar = kappa * vtan / log(30.0 * delta / fric);
+    yplus = delta * ustar / rrey;
+  } else if (code == 61) {
+    double conv = 1., ustarold;
+    int icont = 0;
+    const int tkmax = 10;
+    ustar = 1.;
+    while (conv > 1.e-3 && icont < tkmax) {
+      ++icont;
+      ustarold = ustar;
+      yplus = fmax(1.0000001, delta * ustar / rrey);
+      ustar = vtan * kappa / log(Ecte * yplus);
+      conv = fabs((ustar - ustarold) / ustar);
+    }
+    if (icont == tkmax) atomicExch(err, ERR_WALL_LAW);
+  }
+  if (yplus < (f == 5 ? 11.63 : 11.067)) {
+    tau[e] = rrey * vtan / delta;
+  } else {
+    tau[e] = ustar * ustar;  // ustar**2.0
+    tau2[e] = tau[e] / vtan;
+  }
+}
+
 __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restrict__ tiles,
                               const DomState *__restrict__ ds, int ax, int ly, double ubulk, int alfabc,
                               int only, double dt, double alfapr) {
@@ -433,10 +525,12 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   const int code = F.bcode[f];
   const bool normal = comp == ax;
   // 1 constant cv, 2 -mirror, 3 +mirror, 4 copy of the last face,
-  // 5 convective outflow, 6 the inlet plane
+  // 5 convective outflow, 6 the inlet plane, 7 wall-function update of the
+  // first cell (layer 0), 8 wall-function mirror (deeper layers)
   int mode = 0;
   double cv = 0.0;
-  if (code == 4) mode = normal ? 1 : 2;
+  if (code >= 61 && F.wtau) mode = normal ? 1 : ly == 0 ? 7 : 8;
+  else if (code == 4) mode = normal ? 1 : 2;
   else if (code == 3 && ax != 0) mode = normal ? 1 : 3;
   else if (code == 1 && side == 0 && ax != 1) {  // inflow: west u = ubulk, bottom w = 1.1, the rest 0
     mode = 1;
@@ -460,11 +554,29 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
     if (sl <= F.inl_s1 && tl <= F.inl_t1) fi[g] = F.inl[(long long)tl * (F.ny + 2) + sl];
     return;
   }
+  if (dt < 0.0) {  // the solve's own dt and alfapr
+    dt = ds[F.dom].dt;
+    alfapr = ds[F.dom].alfapr;
+  }
+  if (mode == 7) {
+    // F = sign(tau2*c(first)/h, -c(first)), h along the component's own
+    // axis; c(first) += F*alfapr*dt; c(ghost 0) = -c(first)
+    const long long first = fidx_ax(F, ax, side ? e0 : s0, sl, tl);
+    const double t2 = F.wtau[(2 * f + 1) * F.wplane + (long long)(tl + pl - 1) * m1 + (sl + pl - 1)];
+    double c = fi[first];
+    double fw = t2 * c / F.h[comp][1];
+    fw = copysign(fabs(fw), -c);
+    c = c + fw * alfapr * dt;
+    fi[first] = c;
+    fi[g] = -c;
+    return;
+  }
+  if (mode == 8) {  // deeper layers: minus the first cell (u on the S, N, B faces: the cell ly inside)
+    const int src = (comp == 0 && f != 5) ? (side ? e0 - ly : s0 + ly) : (side ? e0 : s0);
+    fi[g] = -fi[fidx_ax(F, ax, src, sl, tl)];
+    return;
+  }
   if (mode == 5) {  // oo(ie+1+ly) - dt*alfapr*(oo(ie+1+ly) - oo(ie))/dx, from the start-of-step velocity
-    if (dt < 0.0) {  // the solve's own dt and alfapr
-      dt = ds[F.dom].dt;
-      alfapr = ds[F.dom].alfapr;
-    }
     const double *oo = F.oo[comp];
     const double og = oo[g], oe = oo[fidx_ax(F, ax, e0, sl, tl)];
     fi[g] = og - dt * alfapr * (og - oe) / F.h[0][1];

@@ -123,6 +123,15 @@ class Projection:
         self._oo = (arr, blocks)
         abi.check(self.lib, self.lib.mf3d_bind_old_velocity(self.ctx, arr), "mf3d_bind_old_velocity")
 
+    def set_wall_model(self, re: float, fric: float = 0.0):
+        """Re and fric of the wall functions (mf3d_set_wall_model)."""
+        abi.check(self.lib, self.lib.mf3d_set_wall_model(self.ctx, float(re), float(fric)), "mf3d_set_wall_model")
+
+    def bounds_device(self, blocks, dt=1.0, alfapr=1.0, alfabc=1):
+        """boundu/v/w alone on device arrays (mf3d_bounds_device)."""
+        abi.check(self.lib, self.lib.mf3d_bounds_device(self.ctx, _dev_fields(blocks), float(dt), float(alfapr),
+                                                        int(alfabc)), "mf3d_bounds_device")
+
     def tuning(self, level: int) -> dict:
         """Launch shapes chosen for one level (mf3d_tuning)."""
         v = [C.c_int() for _ in range(4)]

@@ -126,6 +126,10 @@ std::map<int, InletFile> g_inlets;
 /* uoo, voo, woo per block position for the convective outflow (code 21) of
  * the solve's boundu/v/w; empty = none */
 std::vector<std::array<const double *, 3>> g_old;
+/* Re and fric (control.cin) for the wall functions; Re = 0: not given */
+double g_re = 0.0, g_fric = 0.0;
+bool g_wall_fail = false; /* a smooth-wall law did not converge */
+std::string g_err;        /* the last error (orc_last_error) */
 
 inline double &F(Blk &B, double *a, int i, int j, int k) {
   return a[(size_t)(i - 1) + (size_t)B.ttc_i * ((size_t)(j - 1) + (size_t)B.ttc_j * (size_t)(k - 1))];
@@ -994,10 +998,11 @@ void pbound(Ctx &C) {
  * 799-806, 833-840, 866-876, 900-908 for w.) */
 bool bounds_code_unsupported(int f, int code, bool lsm, int alfabc, bool have_oo = false) {
   /* the branches that read data outside the projection: the convective
-   * outflow (east 21) unless uoo, voo, woo are at hand (the velocity
-   * predictor), wall functions (61+), phi-gated inflow/outflow under L_LSM.
-   * The inlet files of the west codes 7 and 8 come from g_inlets. */
-  if (code >= 61) return true;
+   * outflow (east 21) unless uoo, voo, woo are at hand, wall functions
+   * (61 to 65) without Re (and fric for 62) or under L_LSM (mu/dens), codes
+   * above 65, phi-gated inflow/outflow under L_LSM.  The inlet files of the
+   * west codes 7 and 8 come from g_inlets. */
+  if (code >= 61 && (code > 65 || lsm || g_re == 0.0 || (code == 62 && g_fric == 0.0))) return true;
   if (f == 1 && code == 21 && alfabc == 1 && !have_oo) return true;
   if (lsm && ((f == 0 && code == 1) || (f == 1 && (code == 2 || code == 21) && alfabc == 1))) return true;
   return false;
@@ -1056,6 +1061,142 @@ void bound_inlet(const Ctx &C, Blk &B, int ly) {
   }
 }
 
+/* The wall stresses of the six faces of each block (tauww, tauwe, tauws,
+ * tauwn, tauwb, tauwt and their "2" arrays, initial.for:288-299): zero at
+ * the start (initial.for:878-883) and kept across calls, as the reference
+ * keeps them across time steps.  Element of face f (W, E, S, N, B, T) at
+ * the two tangential field indices (j,k), (j,k), (i,k), (i,k), (i,j), (i,j);
+ * which = 0: tau, 1: tau2. */
+std::map<int, std::array<std::vector<double>, 12>> g_tau; /* per block id: tau[6], tau2[6] */
+double &tau_at(Blk &B, int which, int f, int a, int b) {
+  std::vector<double> &v = g_tau[B.d.id][6 * which + f];
+  const int n1 = f < 2 ? B.ttc_j : B.ttc_i, n2 = f < 4 ? B.ttc_k : B.ttc_j;
+  if (v.empty()) v.assign((size_t)n1 * n2, 0.0);
+  return v[(size_t)(a - 1) + (size_t)n1 * (b - 1)];
+}
+
+/* log_law(bound, ib) (log_law.for:2-310, codes 61 smooth and 62 rough) and
+ * wall_function(bound, ib) (wall_function.for:2-250, the power laws of
+ * codes 63, 64, 65) for face f of block B: per cell of the face's plane
+ * (the cell ranges widened by one) the tangential speed of the first cell
+ * layer and the wall stress tau, tau2 = tau/vtan.  log_law keeps the old
+ * tau2 where y+ is below 11.067 (11.63 on the top face).  Returns false
+ * where the smooth-wall iteration does not converge (the reference prints
+ * "USTAR DOESNT CONVERGE" and stops). */
+bool wall_law(const Ctx &C, Blk &B, int f) {
+  const int code = f == 0 ? B.d.bc_west : f == 1 ? B.d.bc_east : f == 2 ? B.d.bc_south : f == 3 ? B.d.bc_north
+                   : f == 4 ? B.d.bc_bottom : B.d.bc_top;
+  const double rrey = 1.0 / g_re, small = 1.e-30, kappa = 0.41, Ecte = 9.0;
+  const int ax = f / 2;
+  const double delta = ax == 0 ? B.d.dx : ax == 1 ? B.d.dy : B.d.dz;
+  const double nx = ax == 0 ? (f == 0 ? 1.0 : -1.0) : 0.0, ny = ax == 1 ? (f == 2 ? 1.0 : -1.0) : 0.0,
+               nz = ax == 2 ? (f == 4 ? 1.0 : -1.0) : 0.0;
+  /* wall_function's constants; the reference sets aaa, bbb by DATA
+   * statements inside the CASE arms (wall_function.for:34-49); taken here by
+   * the arms' intent: 1/6, 1/7 and 1/8 power laws */
+  double aaa = 8.3, bbb = code == 63 ? 0.1666666666 : code == 64 ? 0.1428571429 : 0.125;
+  const double const1 = 0.5 * (1. - bbb) * std::pow(aaa, (1. + bbb) / (1. - bbb));
+  const double const2 = (1. + bbb) / aaa;
+  const double const3 = std::pow(aaa, 2. / (1. - bbb));
+  const double const4 = 2. / (1. + bbb);
+  bool ok = true;
+  /* loops: W/E k outer, j inner at i = isp/iep; S/N k outer, i inner at
+   * j = jsp/jep; B/T j outer, i inner at k = ksp/kep */
+  const int fix = f == 0 ? B.isp : f == 1 ? B.iep : f == 2 ? B.jsp : f == 3 ? B.jep : f == 4 ? B.ksp : B.kep;
+  const int o0 = ax == 2 ? B.jsp : B.ksp, o1 = ax == 2 ? B.jep : B.kep;
+  const int i0 = ax == 0 ? B.jsp : B.isp, i1 = ax == 0 ? B.jep : B.iep;
+  for (int o = o0 - 1; o <= o1 + 1; ++o)
+    for (int q = i0 - 1; q <= i1 + 1; ++q) {
+      const int i = ax == 0 ? fix : q, j = ax == 0 ? q : ax == 1 ? fix : o, k = ax == 2 ? fix : o;
+      const double uc = 0.5 * (F(B, B.u, i, j, k) + F(B, B.u, i - 1, j, k));
+      const double vc = 0.5 * (F(B, B.v, i, j, k) + F(B, B.v, i, j - 1, k));
+      const double wc = 0.5 * (F(B, B.w, i, j, k) + F(B, B.w, i, j, k - 1));
+      const double vnor = nx * uc + ny * vc + nz * wc;
+      const double vtan = std::sqrt(std::fabs(uc * uc + vc * vc + wc * wc - vnor * vnor + small));
+      double &tau = tau_at(B, 0, f, q, o), &tau2 = tau_at(B, 1, f, q, o);
+      if (code >= 63) {
+        const double dycell = 2. * delta, rycell = 1. / dycell;
+        const double vtankr = 0.5 * rrey * rycell * const3;
+        const double dvtan = vtankr - vtan;
+        const double sub = std::max(std::copysign(1., dvtan), 0.);
+        const double tausub = rrey * vtan / delta;
+        const double taupow = std::pow(const1 * std::pow(rrey * rycell, 1. + bbb) +
+                                       (const2 * std::pow(rrey * rycell, bbb)) * vtan, const4);
+        tau = (sub * tausub + (1. - sub) * taupow);
+        tau2 = tau / vtan;
+        continue;
+      }
+      double ustar = 0.0, yplus = 0.0;
+      if (code == 62) {
+        ustar = kappa * vtan / std::log(30.0 * delta / g_fric);
+        yplus = delta * ustar / rrey;
+      } else if (code == 61) {
+        double conv = 1., ustarold;
+        int icont = 0;
+        const int tkmax = 10;
+        ustar = 1.;
+        while (conv > 1.e-3 && icont < tkmax) {
+          ++icont;
+          ustarold = ustar;
+          yplus = std::max(1.0000001, delta * ustar / rrey);
+          ustar = vtan * kappa / std::log(Ecte * yplus);
+          conv = std::fabs((ustar - ustarold) / ustar);
+        }
+        if (icont == tkmax) ok = false;
+      }
+      if (yplus < (f == 5 ? 11.63 : 11.067)) {
+        tau = rrey * vtan / delta;
+      } else {
+        tau = ustar * ustar;  /* ustar**2.0 */
+        tau2 = tau / vtan;
+      }
+    }
+  return ok;
+}
+
+/* boundu/v/w's wall-function branch (codes 61 and up) for the tangential
+ * component op on face f at layer ly (bounds.for:187-206, 221-239, 260-283,
+ * 309-329 for u; 378-397, 480-499, 549-568, 596-615 for v; 666-685,
+ * 773-792, 808-827, 841-860 for w).  Layer 0: the face's wall law, then per
+ * face cell F = sign(tau2*c(first)/h_c, -c(first)), c(first) += F*alfapr*dt
+ * and c(ghost 0) = -c(first), h_c the spacing along the component's own
+ * axis; deeper layers mirror the first cell (u on the S, N and B faces:
+ * the cell ly inside). */
+bool bound_wall_law(const Ctx &C, Blk &B, int op, int ly, int f) {
+  const int ax = f / 2, comp = op - 1;
+  const bool high = f & 1;
+  int is, ie, js, je, ks, ke;
+  franges(B, op, is, ie, js, je, ks, ke);
+  double *fi = field_of(B, op);
+  const int s0 = ax == 0 ? is : ax == 1 ? js : ks, e0 = ax == 0 ? ie : ax == 1 ? je : ke;
+  const int sa = ax == 0 ? js : is, ea = ax == 0 ? je : ie;
+  const int ta = ax == 2 ? js : ks, tb = ax == 2 ? je : ke;
+  auto at = [&](int a, int s, int t) -> double & {
+    if (ax == 0) return F(B, fi, a, s, t);
+    if (ax == 1) return F(B, fi, s, a, t);
+    return F(B, fi, s, t, a);
+  };
+  const int first = high ? e0 : s0;
+  if (ly == 0) {
+    const bool ok = wall_law(C, B, f);
+    const double h = comp == 0 ? B.d.dx : comp == 1 ? B.d.dy : B.d.dz;
+    for (int t = ta - 1; t <= tb + 1; ++t)
+      for (int s = sa - 1; s <= ea + 1; ++s) {
+        double &c = at(first, s, t);
+        double fw = tau_at(B, 1, f, s, t) * c / h;
+        fw = std::copysign(std::fabs(fw), -c);  /* SIGN(Fwall, -c) */
+        c = c + fw * C.alfapr * C.dt;
+        at(high ? e0 + 1 : s0 - 1, s, t) = -c;
+      }
+    return ok;
+  }
+  const bool deep = comp == 0 && f != 5;
+  for (int t = ta - 1; t <= tb + 1; ++t)
+    for (int s = sa - 1; s <= ea + 1; ++s)
+      at(high ? e0 + 1 + ly : s0 - 1 - ly, s, t) = -at(deep ? (high ? e0 - ly : s0 + ly) : first, s, t);
+  return true;
+}
+
 void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
   const int ax = f / 2, comp = op - 1;
   const bool high = f & 1;
@@ -1068,9 +1209,14 @@ void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
     return;
   }
   const bool normal = ax == comp;
+  if (code >= 61 && !normal) {  /* the wall functions of the tangential components */
+    if (!bound_wall_law(C, B, op, ly, f)) g_wall_fail = true;
+    return;
+  }
   int mode = 0; /* 0 nothing, 1 the constant cv, 2 -mirror, 3 +mirror, 4 copy of face ie */
   double cv = 0.0;
   if (code == 4) mode = normal ? 1 : 2;
+  else if (code >= 61) mode = 1;  /* the normal component at a wall-function face: 0 */
   else if (code == 3 && ax != 0) mode = normal ? 1 : 3;
   else if (code == 1 && f == 0) { mode = 1; cv = comp == 0 ? C.ubulk : 0.0; }
   else if (code == 12 && f == 0) { mode = 1; cv = 0.0; } /* v, w (bounds.for:374-377, 662-665) */
@@ -1535,7 +1681,11 @@ int newsolv_mg(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
   if (!conv) status = MF3D_NOT_CONVERGED;
   if (C.rmax > 100.0) status = MF3D_DIVERGED;
   /* newsolv_mg.for:84-88 (the reference stops first when rmax > 100) */
-  if (C.bounds && status != MF3D_DIVERGED) { bound(C, 1); bound(C, 2); bound(C, 3); }
+  if (C.bounds && status != MF3D_DIVERGED) {
+    g_wall_fail = false;
+    bound(C, 1); bound(C, 2); bound(C, 3);
+    if (g_wall_fail) { g_err = "log_law: USTAR DOESNT CONVERGE"; return MF3D_E_INVALID; }
+  }
   if (info) {
     info->rmax = C.rmax; info->rmax0 = rmax0; info->iter = iters; info->status = status; info->ms_device = 0.0;
   }
@@ -1678,14 +1828,17 @@ int pressure_1sweep(Ctx &C, double *hist, int cap, mf3d_solve_info *info) {
   }
   int status = conv ? MF3D_OK : MF3D_NOT_CONVERGED;
   if (C.rmax > 100.0) status = MF3D_DIVERGED;
-  if (C.bounds && status != MF3D_DIVERGED) { bound(C, 1); bound(C, 2); bound(C, 3); }
+  if (C.bounds && status != MF3D_DIVERGED) {
+    g_wall_fail = false;
+    bound(C, 1); bound(C, 2); bound(C, 3);
+    if (g_wall_fail) { g_err = "log_law: USTAR DOESNT CONVERGE"; return MF3D_E_INVALID; }
+  }
   if (info) {
     info->rmax = C.rmax; info->rmax0 = rmax0; info->iter = calls; info->status = status; info->ms_device = 0.0;
   }
   return status;
 }
 
-std::string g_err;
 
 /* An inlet code on a west face without a neighbour: its file is there, and
  * the profile codes read uniform cell centres (initial.for:341-365). */
@@ -1788,6 +1941,15 @@ int orc_set_inlet(int id, int code, int uprof, const double *v, long long n) {
 }
 void orc_clear_inlets(void) { g_inlets.clear(); }
 
+/* Re and fric (control.cin) of the wall functions; re = 0 withdraws them.
+ * Clears the kept wall stresses. */
+int orc_set_wall_model(double re, double fric) {
+  g_re = re;
+  g_fric = fric;
+  g_tau.clear();
+  return MF3D_OK;
+}
+
 /* uoo, voo, woo of every block (position order) for the solve's convective
  * outflow faces; nb = 0 unbinds. */
 int orc_bind_old_velocity(int nb, const double *const *uoo, const double *const *voo, const double *const *woo) {
@@ -1865,6 +2027,27 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
   } else {
     rungek_2nd(C, uoo.data(), voo.data(), woo.data(), vis.data(), pressureforce != 0, forcn);
   }
+  return MF3D_OK;
+}
+
+/* boundu, boundv, boundw alone on host arrays (bounds.for:2-916): u, v, w
+ * in/out, with dt, alfapr and alfabc as the caller's time step has them. */
+int orc_bounds(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, const mf3d_fields *fields, double dt,
+               double alfapr, int alfabc) {
+  Ctx C;
+  mf3d_params p = *prm;
+  p.bounds = 1;
+  p.alfabc = alfabc;
+  int st = setup(C, blocks, nb, &p);
+  if (st) return st;
+  C.dt = dt; C.alfapr = alfapr;
+  for (int ib = 0; ib < nb; ++ib) {
+    Blk &B = C.b[ib];
+    B.u = fields[ib].u; B.v = fields[ib].v; B.w = fields[ib].w;
+  }
+  g_wall_fail = false;
+  bound(C, 1); bound(C, 2); bound(C, 3);
+  if (g_wall_fail) { g_err = "log_law: USTAR DOESNT CONVERGE"; return MF3D_E_INVALID; }
   return MF3D_OK;
 }
 

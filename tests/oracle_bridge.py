@@ -47,6 +47,9 @@ def load():
         lib.orc_exchange.argtypes = [C.POINTER(BlockDesc), C.c_int, C.POINTER(Params), C.POINTER(Fields), C.c_int]
         lib.orc_set_inlet.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_longlong]
         lib.orc_bind_old_velocity.argtypes = [C.c_int, C.POINTER(_dp), C.POINTER(_dp), C.POINTER(_dp)]
+        lib.orc_set_wall_model.argtypes = [C.c_double, C.c_double]
+        lib.orc_bounds.argtypes = [C.POINTER(BlockDesc), C.c_int, C.POINTER(Params), C.POINTER(Fields), C.c_double,
+                                   C.c_double, C.c_int]
         lib.orc_last_error.restype = C.c_char_p
         _lib = lib
     return _lib

@@ -189,3 +189,85 @@ def test_bounds_convective_outflow_needs_old_velocities(lib, cuda):
     with pytest.raises(RuntimeError):
         proj.newsolv_mg_device(dev)
     proj.close()
+
+
+WALL_LAWS = {
+    "61 smooth log law on the bottom, 62 rough on the top": ((4, 4, W, W, 61, 62), 1.0e-3),
+    "63 and 64 power laws on south and north, 65 on the west": ((65, 4, 63, 64, S, S), 0.0),
+}
+
+
+def _wall_fields(pr, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for f in pr.block_fields(seed=seed, fourier_modes=2):
+        for k in ("u", "v", "w"):
+            f[k] = f[k] + rng.uniform(0.5, 1.5, f[k].shape)  # a mean flow along every axis
+        out.append(f)
+    return out
+
+
+def assert_close_velocities(o, g, rtol=1e-12):
+    """p bit for bit; u, v, w to rounding (the wall laws take CUDA's sqrt,
+    log and pow against libm's)."""
+    st, info, hist, ref = o
+    res, got = g
+    assert res.status == st and res.iter == info.iter and np.array_equal(res.history, hist)
+    for b in range(len(ref)):
+        assert np.array_equal(got[b]["p"], ref[b]["p"]), b
+        for k in ("u", "v", "w"):
+            np.testing.assert_allclose(got[b][k], ref[b][k], rtol=rtol, atol=1e-15, err_msg=f"{b} {k}")
+
+
+@pytest.mark.parametrize("case", sorted(WALL_LAWS))
+def test_bounds_wall_functions(lib, oracle, cuda, case):
+    """The wall functions of boundu/v/w after the solve (codes 61-65:
+    log_law.for, wall_function.for, bounds.for:187-206 and the matching
+    branches): against the oracle, two consecutive solves on one context so
+    the kept wall stresses carry over."""
+    bc, fric = WALL_LAWS[case]
+    pr = Problem(2, 1, 1, 16, 8, 8, bc=bc, ngrid=3, pl=2, dx=0.01, dy=0.01, dz=0.01)
+    prm = pr.params(mg_itrsch=3, maxcy=30, eps=1e-9, pl_ex=1, bounds=1, alfabc=1, ubulk=0.7)
+    re = 5.0e4
+    oracle.orc_set_wall_model(re, fric)
+    try:
+        blocks = _wall_fields(pr, 42)
+        o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks,
+                        dt=0.02, prepare=lambda proj: proj.set_wall_model(re, fric))
+    finally:
+        oracle.orc_set_wall_model(0.0, 0.0)
+    assert_close_velocities(o, g)
+    # the laws changed the first cells: the bounds without them differ
+    plain = Problem(2, 1, 1, 16, 8, 8, bc=tuple(4 if c >= 61 else c for c in bc), ngrid=3, pl=2,
+                    dx=0.01, dy=0.01, dz=0.01)
+    o2, g2 = run_both(lib, oracle, cuda, plain.descriptors(lib), plain.descriptors(oracle), plain.nblocks, prm,
+                      _wall_fields(pr, 42), dt=0.02)
+    assert any(not np.array_equal(g[1][b]["u"], g2[1][b]["u"]) for b in range(pr.nblocks))
+
+
+def test_bounds_device_with_wall_functions(lib, oracle, cuda):
+    """mf3d_bounds_device against orc_bounds, twice in a row (the second
+    reads the wall stresses the first kept), codes 61 and 64 with inflow and
+    outflow faces."""
+    import ctypes as C
+    import torch
+    from multiflow3d_b200.problems import fields_struct
+    from multiflow3d_b200.solver import Projection
+    pr = Problem(1, 2, 1, 16, 8, 16, bc=(1, 2, 61, 64, S, S), ngrid=2, pl=2, dx=0.01, dy=0.01, dz=0.01)
+    prm = pr.params(pl_ex=1, bounds=1, alfabc=1, ubulk=0.7)
+    host = _wall_fields(pr, 43)
+    dev = [{k: torch.from_numpy(v.copy()).to(cuda) for k, v in f.items()} for f in host]
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    proj.set_wall_model(3.0e4, 0.0)
+    oracle.orc_set_wall_model(3.0e4, 0.0)
+    try:
+        for _ in range(2):
+            assert oracle.orc_bounds(pr.descriptors(oracle), pr.nblocks, C.byref(prm), fields_struct(host), 0.02,
+                                     1.0, 1) == 0
+            proj.bounds_device(dev, dt=0.02, alfapr=1.0, alfabc=1)
+    finally:
+        oracle.orc_set_wall_model(0.0, 0.0)
+        proj.close()
+    for b in range(pr.nblocks):
+        for k in ("u", "v", "w"):
+            np.testing.assert_allclose(dev[b][k].cpu().numpy(), host[b][k], rtol=1e-12, atol=1e-15, err_msg=f"{b} {k}")

@@ -172,7 +172,7 @@ def test_bounds_face_codes_refused_without_gpu(lib):
     solve, once their inputs can have been handed over."""
     ctx = C.c_void_p()
     for bc, kw, stretch in (((12, 2, WALL, WALL, WALL, WALL), {}, 2.0),
-                            ((1, 2, WALL, WALL, 63, WALL), {}, 0.0), ((1, 2, WALL, WALL, WALL, WALL), {"lsm": 1}, 0.0)):
+                            ((1, 2, WALL, WALL, 66, WALL), {}, 0.0), ((1, 2, WALL, WALL, WALL, WALL), {"lsm": 1}, 0.0)):
         pr = Problem(1, 1, 1, 8, 8, 8, bc=bc, ngrid=2, pl=1, stretch_y=stretch)
         prm = pr.params(bounds=1, **kw)
         assert lib.mf3d_create(pr.descriptors(lib), 1, C.byref(prm), C.byref(ctx)) == abi.MF3D_E_UNSUPPORTED, bc

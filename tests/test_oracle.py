@@ -577,3 +577,64 @@ def test_bounds_convective_outflow_in_the_solve(oracle):
             assert np.array_equal(blocks[0][k][Kc, Jc, g], want), (k, ly)
     st, _, _ = solve(oracle, pr, pr.block_fields(seed=26), maxcy=2, bounds=1, alfabc=1)
     assert st == -6
+
+
+def smooth_wall_tau2(vtan, delta, re):
+    """log_law.for:47-75 in numpy (smooth wall, code 61): tau2 of the log law
+    where y+ >= 11.067, else the kept value (0 at the start)."""
+    rrey, kappa, E = 1.0 / re, 0.41, 9.0
+    out = np.zeros_like(vtan)
+    for idx, vt in np.ndenumerate(vtan):
+        ustar, conv, it = 1.0, 1.0, 0
+        while conv > 1e-3 and it < 10:
+            it += 1
+            old = ustar
+            yplus = max(1.0000001, delta * ustar / rrey)
+            ustar = vt * kappa / np.log(E * yplus)
+            conv = abs((ustar - old) / ustar)
+        assert it < 10
+        if yplus >= 11.067:
+            out[idx] = ustar * ustar / vt
+    return out
+
+
+def test_bounds_wall_function_known_answer(oracle):
+    """Code 61 on the bottom face (boundu, bounds.for:260-283, with
+    log_law(5), log_law.for:206-254): on the interior face cells u(i,j,ks)
+    += sign(tau2*u/dx, -u)*alfapr*dt and u(i,j,ks-1) = -u(i,j,ks), tau2 from
+    the smooth-wall log law of the first cell layer; the normal component w
+    is 0 on every ghost layer; without Re the code is refused."""
+    from multiflow3d_b200.problems import fields_struct
+    n, pl, dt, alfapr, re = 8, 2, 0.05, 1.0, 2.0e4
+    pr = Problem(1, 1, 1, n, n, n, bc=(WALL, WALL, WALL, WALL, 61, WALL), ngrid=2, pl=pl, dx=0.1, dy=0.1, dz=0.1)
+    rng = np.random.default_rng(28)
+    shape = (n + 2 * pl,) * 3
+    f = {k: rng.uniform(0.5, 1.5, shape) for k in ("u", "v", "w")}
+    f.update({k: np.zeros(shape) for k in ("ustar", "vstar", "wstar", "p", "su")})
+    before = {k: f[k].copy() for k in ("u", "v", "w")}
+    prm = pr.params(pl_ex=1, bounds=1)
+    assert oracle.orc_bounds(pr.descriptors(oracle), 1, C.byref(prm), fields_struct([f]), dt, alfapr, 1) == -6
+    oracle.orc_set_wall_model(re, 0.0)
+    try:
+        assert oracle.orc_bounds(pr.descriptors(oracle), 1, C.byref(prm), fields_struct([f]), dt, alfapr, 1) == 0
+    finally:
+        oracle.orc_set_wall_model(0.0, 0.0)
+    u0, v0, w0 = before["u"], before["v"], before["w"]
+    ks = pl  # 0-based first interior plane
+    # i = isp+1 .. iep-1 (the law reads u(i-1) inside; u(iep) is the east
+    # wall face, zeroed by boundu's east branch first), j = jsp+1 .. jep
+    I, Im = slice(pl + 1, pl + n - 1), slice(pl, pl + n - 2)
+    J, Jm = slice(pl + 1, pl + n), slice(pl, pl + n - 1)
+    uc = 0.5 * (u0[ks, J, I] + u0[ks, J, Im])
+    vc = 0.5 * (v0[ks, J, I] + v0[ks, Jm, I])
+    wc = 0.5 * (w0[ks, J, I] + w0[ks - 1, J, I])
+    vtan = np.sqrt(np.abs(uc * uc + vc * vc + wc * wc - wc * wc + 1e-30))
+    tau2 = smooth_wall_tau2(vtan, 0.1, re)
+    assert (tau2 > 0).any()
+    uu = u0[ks, J, I]
+    fw = np.copysign(np.abs(tau2 * uu / 0.1), -uu)
+    want = uu + fw * alfapr * dt
+    np.testing.assert_allclose(f["u"][ks, J, I], want, rtol=1e-14, atol=0)
+    assert np.array_equal(f["u"][ks - 1, J, I], -f["u"][ks, J, I])
+    for ly in range(2):
+        assert not f["w"][ks - 1 - ly, pl:pl + n, pl:pl + n].any()
