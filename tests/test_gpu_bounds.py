@@ -201,7 +201,7 @@ def _wall_fields(pr, seed):
     rng = np.random.default_rng(seed)
     out = []
     for f in pr.block_fields(seed=seed, fourier_modes=2):
-        for k in ("u", "v", "w"):
+        for k in ("u", "v", "w", "ustar", "vstar", "wstar"):
             f[k] = f[k] + rng.uniform(0.5, 1.5, f[k].shape)  # a mean flow along every axis
         out.append(f)
     return out
