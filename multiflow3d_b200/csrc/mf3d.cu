@@ -2586,11 +2586,12 @@ static int make_view(mf3d_ctx *C) {
 //   u = u*(1+1/7)*|zc/(zen-zst)|^(1/7)        code 12
 // formed once on the host in that order, from the cell centres the
 // reference forms (a running sum, initial.for:341-365) and the extents of the
-// whole domain (alloc_dom.for:427-439).  Code 7 takes u from the caller's
-// inlet file, code 8 the SEM fluctuations up added to ubulk or to the code-12
-// profile (UPROF_SEM = 12), both through mf3d_set_inlet.  The plane covers
-// rows 0..ny+1 and planes 0..nz+1 of u at the ghost layers 0..pl_ex; code 8
-// writes rows 0..ny and planes 0..nz only (bounds.for:84-86).
+// whole domain (alloc_dom.for:427-439).  Code 7 takes u, v and w from the
+// caller's inlet file, code 8 v and w from the SEM file and u as its
+// fluctuation up added to ubulk or to the code-12 profile (UPROF_SEM = 12),
+// both through mf3d_set_inlet.  A component's plane covers its rows
+// js-1..je+1 and planes ks-1..ke+1 (code 8: js-1..je, ks-1..ke,
+// bounds.for:84-86) at the ghost layers 0..pl_ex.
 struct Extents {
   double yst, yen, zst, zen;
 };
@@ -2615,42 +2616,73 @@ static double power_law_y(double ubulk, const Extents &e, double yc) {
 static double power_law_z(double u, const Extents &e, double zc) {
   return u * (1.0 + 1. / 7.) * std::pow(std::fabs(zc / (e.zen - e.zst)), 1. / 7.);
 }
-// Forms (codes 12, 13) or installs (7, 8: vals) the inlet plane of block S.
+// The last local row and plane of component c (0 u, 1 v, 2 w) on a west
+// face: v stops one row short of a north wall, w one plane short of a top
+// wall (jsv..jev, ksw..kew; localparameters.for:185-190).
+static void west_ranges(const mf3d_block_desc &d, int c, int &je, int &ke) {
+  je = d.ny - ((c == 1 && d.jnext < 0 && d.bc_north != MF3D_BC_PERIODIC) ? 1 : 0);
+  ke = d.nz - ((c == 2 && d.knext < 0 && d.bc_top != MF3D_BC_PERIODIC) ? 1 : 0);
+}
+// Values a west inlet of code 7 or 8 reads, u, v, w one after the other:
+// code 7 each component over rows js-1..je+1 and planes ks-1..ke+1 of its
+// own ranges, code 8 over js-1..je and ks-1..ke (bounds.for:84-86).
+static long long inlet_count(const mf3d_block_desc &d, int code) {
+  long long n = 0;
+  for (int c = 0; c < 3; ++c) {
+    int je, ke;
+    west_ranges(d, c, je, ke);
+    n += code == 7 ? (long long)(je + 2) * (ke + 2) : (long long)(je + 1) * (ke + 1);
+  }
+  return n;
+}
+// Forms (codes 12, 13) or installs (7, 8: vals, inlet_count of them) the
+// inlet planes of block S.
 static int install_inlet(mf3d_ctx *C, BlockStore &S, const Extents &e, int code, int uprof, const double *vals) {
   const mf3d_block_desc &d = S.d;
   const int pl = C->prm.pl, rows = d.ny + 2;
-  std::vector<double> pln((size_t)rows * (d.nz + 2), 0.0);
-  int s1 = d.ny + 1, t1 = d.nz + 1;
-  if (code == 7) {
-    std::copy(vals, vals + pln.size(), pln.begin());
-  } else if (code == 8) {
-    s1 = d.ny; t1 = d.nz;
-    for (int t = 0; t <= d.nz; ++t)
-      for (int r = 0; r <= d.ny; ++r) {
-        const double up = vals[(size_t)t * (d.ny + 1) + r];
-        double u;
-        if (uprof == 12) {
-          u = power_law_y(C->prm.ubulk, e, cell_centre(d.ysl, d.dy, pl, r + pl));
-          u = power_law_z(u, e, cell_centre(d.zsl, d.dz, pl, t + pl)) + up;
-        } else {
-          u = C->prm.ubulk + up;
+  const size_t pn = (size_t)rows * (d.nz + 2);
+  std::vector<double> pln(3 * pn, 0.0);
+  int s1[3] = {-1, -1, -1}, t1[3] = {-1, -1, -1};
+  if (code == 7 || code == 8) {
+    size_t r = 0;
+    for (int c = 0; c < 3; ++c) {
+      int je, ke;
+      west_ranges(d, c, je, ke);
+      s1[c] = code == 7 ? je + 1 : je;
+      t1[c] = code == 7 ? ke + 1 : ke;
+      for (int t = 0; t <= t1[c]; ++t)
+        for (int q = 0; q <= s1[c]; ++q) {
+          double u = vals[r++];
+          if (code == 8 && c == 0) {  // u = up + ubulk, or up + the code-12 profile
+            const double up = u;
+            if (uprof == 12) {
+              u = power_law_y(C->prm.ubulk, e, cell_centre(d.ysl, d.dy, pl, q + pl));
+              u = power_law_z(u, e, cell_centre(d.zsl, d.dz, pl, t + pl)) + up;
+            } else {
+              u = C->prm.ubulk + up;
+            }
+          }
+          pln[c * pn + (size_t)t * rows + q] = u;
         }
-        pln[(size_t)t * rows + r] = u;
-      }
+    }
   } else {
+    s1[0] = d.ny + 1;
+    t1[0] = d.nz + 1;
     for (int t = 0; t <= d.nz + 1; ++t)
-      for (int r = 0; r <= d.ny + 1; ++r) {
-        double u = power_law_y(C->prm.ubulk, e, cell_centre(d.ysl, d.dy, pl, r + pl));
+      for (int q = 0; q <= d.ny + 1; ++q) {
+        double u = power_law_y(C->prm.ubulk, e, cell_centre(d.ysl, d.dy, pl, q + pl));
         if (code == 12) u = power_law_z(u, e, cell_centre(d.zsl, d.dz, pl, t + pl));
-        pln[(size_t)t * rows + r] = u;
+        pln[(size_t)t * rows + q] = u;
       }
   }
   int st;
   if ((st = S.inlet.upload(pln, C->stream))) return st;
   CK(cudaStreamSynchronize(C->stream));  // pln is a local
   S.fld.inl = S.inlet.p;
-  S.fld.inl_s1 = s1;
-  S.fld.inl_t1 = t1;
+  for (int c = 0; c < 3; ++c) {
+    S.fld.inl_s1[c] = s1[c];
+    S.fld.inl_t1[c] = t1[c];
+  }
   return MF3D_OK;
 }
 static bool inlet_code(const mf3d_block_desc &d) {
@@ -3329,7 +3361,7 @@ int mf3d_set_inlet(mf3d_ctx *C, int block_id, int code, int uprof_sem, const dou
                       std::to_string(code) + " (7 or 8)");
       return MF3D_E_INVALID;
     }
-    const long long want = code == 7 ? (long long)(S.d.ny + 2) * (S.d.nz + 2) : (long long)(S.d.ny + 1) * (S.d.nz + 1);
+    const long long want = mf3d::inlet_count(S.d, code);
     if (n != want) {
       mf3d::set_error("mf3d_set_inlet: " + std::to_string(want) + " values expected, got " + std::to_string(n));
       return MF3D_E_INVALID;
@@ -3347,8 +3379,10 @@ int mf3d_set_inlet(mf3d_ctx *C, int block_id, int code, int uprof_sem, const dou
     for (size_t v = 0; v < C->view->blk.size(); ++v)
       if (C->view->blk[v] == &S) {
         C->view->hf[v].inl = S.fld.inl;
-        C->view->hf[v].inl_s1 = S.fld.inl_s1;
-        C->view->hf[v].inl_t1 = S.fld.inl_t1;
+        for (int c = 0; c < 3; ++c) {
+          C->view->hf[v].inl_s1[c] = S.fld.inl_s1[c];
+          C->view->hf[v].inl_t1[c] = S.fld.inl_t1[c];
+        }
       }
     return MF3D_OK;
   }

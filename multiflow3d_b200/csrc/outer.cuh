@@ -50,9 +50,9 @@ struct BlkFld {
   long long bcplane;                 // elements per receive plane (the largest ttc plane)
   const double *oo[3];               // velocity predictor: u, v, w at the start of the time step
   const double *vis;                 // velocity predictor: cell viscosity (ttc layout)
-  const double *inl;                 // west inlet (codes 7, 8, 12, 13): u over level-1 rows 0..ny+1,
-                                     // planes 0..nz+1, row fastest; null = not set
-  int inl_s1, inl_t1;                // last row / plane the inlet writes (code 8: ny, nz)
+  const double *inl;                 // west inlet (codes 7, 8, 12, 13): u, v, w planes of level-1
+                                     // rows 0..ny+1 x planes 0..nz+1, row fastest; null = not set
+  int inl_s1[3], inl_t1[3];          // per component the last row / plane the inlet writes (-1: none)
   double *wtau;                      // wall functions (codes 61-65): tau, tau2 of face f at
   long long wplane;                  // wtau + (2f or 2f+1)*wplane, ttc face planes; else null
 };
@@ -538,9 +538,10 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   } else if (code == 2 && ax == 0 && side == 1 && alfabc == 1) mode = 4;  // outflow: u(ie+1+ly) = u(ie)
   else if (code == 21 && ax == 0 && side == 1 && alfabc == 1 && F.oo[comp]) mode = 5;  // convective outflow
   else if (f == 0 && (code == 7 || code == 8 || code == 12 || code == 13)) {
-    // the inlets (bounds.for:55-135): u from the inlet plane; code 12 also
-    // sets v = w = 0 (:374-377, 662-665); 7, 8, 13 leave v and w
-    if (comp == 0 && F.inl) mode = 6;
+    // the inlets (bounds.for:55-135, 397-438, 686-730): each component from
+    // its inlet plane where it has one; code 12 sets v = w = 0 (:374-377,
+    // 662-665), 13 leaves them
+    if (F.inl && F.inl_s1[comp] >= 0) mode = 6;
     else if (comp != 0 && code == 12) mode = 1;
   }
   if (!mode) return;
@@ -551,7 +552,8 @@ __global__ void k_bound_faces(const BlkFld *__restrict__ fl, const Tile *__restr
   const int s0 = 1, e0 = comp_end(F, comp, ax);
   const long long g = fidx_ax(F, ax, side ? e0 + 1 + ly : s0 - 1 - ly, sl, tl);
   if (mode == 6) {
-    if (sl <= F.inl_s1 && tl <= F.inl_t1) fi[g] = F.inl[(long long)tl * (F.ny + 2) + sl];
+    const long long pn = (long long)(F.ny + 2) * (F.nz + 2);
+    if (sl <= F.inl_s1[comp] && tl <= F.inl_t1[comp]) fi[g] = F.inl[comp * pn + (long long)tl * (F.ny + 2) + sl];
     return;
   }
   if (dt < 0.0) {  // the solve's own dt and alfapr

@@ -140,20 +140,45 @@ class Projection:
 
 
 def read_inlet_file(path: str, code: int) -> np.ndarray:
-    """The values boundu reads from an inlet file (bounds.for:55-103): code 7
-    (Inlet/Inlet_<dom>_<n>.dat) one u per line; code 8
-    (inflow/Inlet_<dom>_<n>.dat) two header lines, then "up dummy dummy" per
-    line, of which the first column.  In file order (k outer, j inner), as
-    ``Projection.set_inlet`` takes them."""
+    """The numbers boundu/v/w read from an inlet file (bounds.for:55-103,
+    397-438, 686-730): code 7 (Inlet/Inlet_<dom>_<n>.dat) one value per line,
+    u's lines then v's then w's, returned in file order; code 8
+    (inflow/Inlet_<dom>_<n>.dat) two header lines, then "up v w" per line,
+    returned as an (lines, 3) array.  ``inlet_values`` turns them into what
+    ``Projection.set_inlet`` takes."""
     with open(path) as f:
         lines = f.read().splitlines()
+    conv = lambda x: float(x.replace("D", "E").replace("d", "e"))
     if code == 7:
-        rows = [ln for ln in lines if ln.strip()]
-        return np.array([float(ln.split()[0].replace("D", "E").replace("d", "e")) for ln in rows])
+        return np.array([conv(ln.split()[0]) for ln in lines if ln.strip()])
     if code == 8:
-        rows = [ln for ln in lines[2:] if ln.strip()]
-        return np.array([float(ln.split()[0].replace("D", "E").replace("d", "e")) for ln in rows])
+        return np.array([[conv(x) for x in ln.split()[:3]] for ln in lines[2:] if ln.strip()])
     raise ValueError("inlet files exist for the west codes 7 and 8")
+
+
+def inlet_counts(desc, code: int):
+    """Values of u, v, w a west inlet of code 7 or 8 reads for block ``desc``:
+    each component over its own rows and planes (v one row short of a north
+    wall, w one plane short of a top wall), code 7 with both ghost rows,
+    code 8 with the low one only (bounds.for:84-86)."""
+    out = []
+    for c in range(3):
+        je = desc.ny - (1 if c == 1 and desc.jnext < 0 and desc.bc_north != 5 else 0)
+        ke = desc.nz - (1 if c == 2 and desc.knext < 0 and desc.bc_top != 5 else 0)
+        out.append((je + 2) * (ke + 2) if code == 7 else (je + 1) * (ke + 1))
+    return out
+
+
+def inlet_values(desc, code: int, data, data_vw=None) -> np.ndarray:
+    """The values of ``Projection.set_inlet`` from ``read_inlet_file``'s
+    output: code 7 the file's numbers as they stand; code 8 the first column
+    for u and the second and third for v and w (``data_vw``: the file boundv
+    and boundw open, when it is another one)."""
+    nu, nv, nw = inlet_counts(desc, code)
+    if code == 7:
+        return np.asarray(data, dtype=np.float64)[:nu + nv + nw]
+    vw = data if data_vw is None else data_vw
+    return np.concatenate([data[:nu, 0], vw[:nv, 1], vw[:nw, 2]])
 
 
 def _dev_fields(blocks):

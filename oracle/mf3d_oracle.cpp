@@ -1026,32 +1026,47 @@ double power_law_z(const Ctx &C, double u, double zc) {
   return u * (1.0 + 1. / 7.) * std::pow(std::fabs(zc / (C.zen - C.zst)), 1. / 7.);
 }
 
-/* boundu's west branches of the codes 7, 8, 12 and 13 on ghost layer ly
- * (bounds.for:55-135). */
-void bound_inlet(const Ctx &C, Blk &B, int ly) {
-  const int code = B.d.bc_west;
-  const int is = B.isu, js = B.jsu, je = B.jeu, ks = B.ksu, ke = B.keu, pl = C.pl;
-  if (code == 7) {  /* one value per line, k outer (bounds.for:55-73) */
-    const std::vector<double> &v = g_inlets.at(B.d.id).v;
-    size_t r = 0;
-    for (int k = ks - 1; k <= ke + 1; ++k)
-      for (int j = js - 1; j <= je + 1; ++j) F(B, B.u, is - 1 - ly, j, k) = v[r++];
-  } else if (code == 8) {  /* SEM fluctuations on the interior rows and the low ghost row (:75-103) */
+/* boundu's, boundv's and boundw's west branches of the codes 7, 8, 12 and
+ * 13 on ghost layer ly for component op (bounds.for:55-135, 397-438,
+ * 686-730).  The inlet file's values are u's, then v's, then w's, each over
+ * the component's own ranges: code 7 reads rows js-1..je+1 and planes
+ * ks-1..ke+1 per component (boundv skips u's lines, boundw u's and v's);
+ * code 8 reads rows js-1..je and planes ks-1..ke, u as the fluctuation up
+ * (the first column) on ubulk or on the code-12 profile (UPROF_SEM = 12),
+ * v and w as the second and third columns. */
+void bound_inlet(const Ctx &C, Blk &B, int op, int ly) {
+  const int code = B.d.bc_west, pl = C.pl;
+  int is, ie, js, je, ks, ke;
+  franges(B, op, is, ie, js, je, ks, ke);
+  double *fi = field_of(B, op);
+  if (code == 7 || code == 8) {
     const InletFile &in = g_inlets.at(B.d.id);
     size_t r = 0;
-    for (int kk = 1; kk <= ke - ks + 2; ++kk)
-      for (int jj = 1; jj <= je - js + 2; ++jj) {
-        const int k = kk + pl - 1, j = jj + pl - 1;
-        const double up = in.v[r++];
-        double &u = F(B, B.u, is - 1 - ly, j, k);
-        if (in.uprof == 12) {
-          u = power_law_y(C, centre(B.d.ysl, B.d.dy, pl, j));
-          u = power_law_z(C, u, centre(B.d.zsl, B.d.dz, pl, k)) + up;
-        } else {
-          u = C.ubulk + up;
+    for (int c = 1; c < op; ++c) {  /* the lines of the components before this one */
+      int cis, cie, cjs, cje, cks, cke;
+      franges(B, c, cis, cie, cjs, cje, cks, cke);
+      r += code == 7 ? (size_t)(cje - cjs + 3) * (cke - cks + 3) : (size_t)(cje - cjs + 2) * (cke - cks + 2);
+    }
+    if (code == 7) {
+      for (int k = ks - 1; k <= ke + 1; ++k)
+        for (int j = js - 1; j <= je + 1; ++j) F(B, fi, is - 1 - ly, j, k) = in.v[r++];
+    } else {
+      for (int kk = 1; kk <= ke - ks + 2; ++kk)
+        for (int jj = 1; jj <= je - js + 2; ++jj) {
+          const int k = kk + pl - 1, j = jj + pl - 1;
+          const double x = in.v[r++];
+          double &u = F(B, fi, is - 1 - ly, j, k);
+          if (op != 1) {
+            u = x;
+          } else if (in.uprof == 12) {
+            u = power_law_y(C, centre(B.d.ysl, B.d.dy, pl, j));
+            u = power_law_z(C, u, centre(B.d.zsl, B.d.dz, pl, k)) + x;
+          } else {
+            u = C.ubulk + x;
+          }
         }
-      }
-  } else if (code == 12 || code == 13) {  /* :105-135 */
+    }
+  } else if ((code == 12 || code == 13) && op == 1) {  /* :105-135 */
     for (int k = ks - 1; k <= ke + 1; ++k)
       for (int j = js - 1; j <= je + 1; ++j) {
         double &u = F(B, B.u, is - 1 - ly, j, k);
@@ -1204,8 +1219,8 @@ void bound_face(const Ctx &C, Blk &B, int op, int ly, int f) {
   const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
   if (nbr[f] >= 0) return;
   const int code = bcs[f];
-  if (f == 0 && op == 1 && (code == 7 || code == 8 || code == 12 || code == 13)) {
-    bound_inlet(C, B, ly);
+  if (f == 0 && ((code == 7 || code == 8) || (op == 1 && (code == 12 || code == 13)))) {
+    bound_inlet(C, B, op, ly);
     return;
   }
   const bool normal = ax == comp;
@@ -1848,7 +1863,12 @@ int inlet_check(const Blk &B) {
   if (code == 7 || code == 8) {
     auto it = g_inlets.find(B.d.id);
     if (it == g_inlets.end() || it->second.code != code) { g_err = "inlet values not set"; return MF3D_E_INVALID; }
-    const size_t n = code == 7 ? (size_t)(B.d.ny + 2) * (B.d.nz + 2) : (size_t)(B.d.ny + 1) * (B.d.nz + 1);
+    /* u's, v's and w's lines over their own ranges */
+    const int js[3] = {B.jsu, B.jsv, B.jsw}, je[3] = {B.jeu, B.jev, B.jew};
+    const int ks[3] = {B.ksu, B.ksv, B.ksw}, ke[3] = {B.keu, B.kev, B.kew};
+    size_t n = 0;
+    for (int c = 0; c < 3; ++c)
+      n += code == 7 ? (size_t)(je[c] - js[c] + 3) * (ke[c] - ks[c] + 3) : (size_t)(je[c] - js[c] + 2) * (ke[c] - ks[c] + 2);
     if (it->second.v.size() != n) { g_err = "inlet values: wrong count"; return MF3D_E_INVALID; }
   }
   if (code != 7 && (B.d.hy || B.d.hz)) { g_err = "power-law inlet on a stretched grid"; return MF3D_E_UNSUPPORTED; }

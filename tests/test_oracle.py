@@ -490,24 +490,29 @@ def test_bounds_power_law_inlet_known_answer(oracle, code):
 
 
 def test_bounds_inlet_files(oracle, tmp_path):
-    """Codes 7 and 8 take the inlet file's values (bounds.for:55-103): 7 one
-    u per line over rows js-1..je+1 and planes ks-1..ke+1; 8 ubulk plus the
-    first column of the SEM file (after two header lines) over rows js-1..je
-    and planes ks-1..ke only.  The files are written in the reference's
-    formats and read back with read_inlet_file."""
-    from multiflow3d_b200.solver import read_inlet_file
+    """Codes 7 and 8 take the inlet file's values (bounds.for:55-103,
+    397-438, 686-730): 7 one value per line, u's over its rows js-1..je+1 and
+    planes ks-1..ke+1, then v's and w's over theirs (v one row short at the
+    north wall, w one plane short at the top wall); 8 u = ubulk plus the first
+    column of the SEM file (after two header lines), v and w the second and
+    third, over rows js-1..je and planes ks-1..ke only.  The files are
+    written in the reference's formats and read back with read_inlet_file."""
+    from multiflow3d_b200.solver import read_inlet_file, inlet_values, inlet_counts
     n, pl, ubulk = 8, 2, 0.7
     rng = np.random.default_rng(3)
-    f7 = tmp_path / "Inlet_000_00001.dat"
-    v7 = rng.uniform(-1, 1, (n + 2) * (n + 2))
-    f7.write_text("".join(f"  {x:.17E}\n" for x in v7))
-    f8 = tmp_path / "Inlet_0000_000001.dat"
-    v8 = rng.uniform(-1, 1, (n + 1) * (n + 1))
-    f8.write_text("header one\nheader two\n" + "".join(f" {x:.17E}  1  2\n" for x in v8))
-    for code, path, vals in ((7, f7, v7), (8, f8, v8)):
-        got = read_inlet_file(str(path), code)
-        assert np.array_equal(got, vals)
+    for code in (7, 8):
         pr = Problem(1, 1, 1, 2 * n, n, n, bc=(code, 2, WALL, WALL, WALL, WALL), ngrid=2, pl=pl)
+        d = pr.descriptors(oracle)[0]
+        nu, nv, nw = inlet_counts(d, code)
+        if code == 7:
+            vals = rng.uniform(-1, 1, nu + nv + nw)
+            path = tmp_path / "Inlet_000_00001.dat"
+            path.write_text("".join(f"  {x:.17E}\n" for x in vals))
+        else:
+            cols = rng.uniform(-1, 1, (max(nu, nv, nw), 3))
+            path = tmp_path / "Inlet_0000_000001.dat"
+            path.write_text("header one\nheader two\n" + "".join(f" {a:.17E} {b:.17E} {c:.17E}\n" for a, b, c in cols))
+        got = inlet_values(d, code, read_inlet_file(str(path), code))
         blocks = pr.block_fields(seed=25)
         assert oracle.orc_set_inlet(0, code, 0, got.ctypes.data_as(C.POINTER(C.c_double)), got.size) == 0
         try:
@@ -515,33 +520,22 @@ def test_bounds_inlet_files(oracle, tmp_path):
         finally:
             oracle.orc_clear_inlets()
         assert st >= 0
-        u = blocks[0]["u"]
         # rows js..je, planes ks..ke (the wall faces mirror into the ghost rows)
         I = slice(pl, pl + n)
+        Iv, Iw = slice(pl, pl + n - 1), slice(pl, pl + n - 1)
         for ly in range(2):
+            x = pl - 1 - ly
             if code == 7:
-                assert np.array_equal(u[I, I, pl - 1 - ly], vals.reshape(n + 2, n + 2)[1:n + 1, 1:n + 1])
+                u_plane = got[:nu].reshape(n + 2, n + 2)
+                v_plane = got[nu:nu + nv].reshape(n + 2, n + 1)
+                w_plane = got[nu + nv:].reshape(n + 1, n + 2)
+                assert np.array_equal(blocks[0]["u"][I, I, x], u_plane[1:n + 1, 1:n + 1])
+                assert np.array_equal(blocks[0]["v"][I, Iv, x], v_plane[1:n + 1, 1:n])
+                assert np.array_equal(blocks[0]["w"][Iw, I, x], w_plane[1:n, 1:n + 1])
             else:
-                assert np.array_equal(u[I, I, pl - 1 - ly], ubulk + vals.reshape(n + 1, n + 1)[1:, 1:])
-
-
-@pytest.mark.parametrize("nswp", [1, 4])
-def test_sip_solver_reaches_the_multigrid_projection(oracle, nswp):
-    """solver 1 (pressure_1sweep with Stone's SIP, press.for:274-420 and
-    sipsol.for) and the multigrid solver converge to the same projection:
-    pressure (up to its constant) and velocities within the tolerance."""
-    pr = Problem(2, 1, 1, 16, 16, 16, ngrid=3, pl=1)
-    a = pr.block_fields(seed=3)
-    b = [{k: v.copy() for k, v in f.items()} for f in a]
-    st_a, info_a, _ = solve(oracle, pr, a, maxcy=400, eps=1e-10)
-    st_b, info_b, hist_b = solve(oracle, pr, b, maxcy=800, eps=1e-10, solver=1, nswp=nswp)
-    assert st_a == 0 and st_b == 0
-    assert info_b.rmax0 == info_a.rmax0
-    assert hist_b[-1] < 1e-10 * info_b.rmax0
-    pa, pb = demean(pr.gather(a, "p")), demean(pr.gather(b, "p"))
-    assert np.abs(pb - pa).max() <= 1e-7 * np.abs(pa).max()
-    for k in ("u", "v", "w"):
-        assert np.abs(pr.gather(b, k) - pr.gather(a, k)).max() <= 1e-8
+                assert np.array_equal(blocks[0]["u"][I, I, x], ubulk + got[:nu].reshape(n + 1, n + 1)[1:, 1:])
+                assert np.array_equal(blocks[0]["v"][I, Iv, x], got[nu:nu + nv].reshape(n + 1, n)[1:, 1:])
+                assert np.array_equal(blocks[0]["w"][Iw, I, x], got[nu + nv:].reshape(n, n + 1)[1:, 1:])
 
 
 def test_bounds_convective_outflow_in_the_solve(oracle):
