@@ -42,6 +42,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "poisson_solves_per_s_fp64"
+NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e, NVIDIA's DGX figure (the measured copy peak is the roofline's denominator)
 UNIT = "solves/s"
 
 
@@ -360,13 +361,19 @@ def run_gpu(args):
             "iterations_per_solve": iters[0] if iters else None, "status": statuses[0] if statuses else None,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": "k_rbgs (finest-level red/black half-sweep)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "k_rbgs<double, false> (finest-level red/black half-sweep: reads the other "
+                                   "colour and rhs, writes its own colour, 12 B per cell)",
                          "achieved": achieved, "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
+                         "frac_nominal": (achieved / NOMINAL_HBM_GBS) if achieved else None,
                          "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes,
                          "launches": k_n, "avg_launch_ms": (k_ms / k_n) if k_n else None,
                          "other_kernels": {n: {"avg_launch_ms": v[0] / v[1] if v[1] else None,
                                                "GB/s": (v[2] / (v[0] / 1e3)) / 1e9 if v[0] > 0 else None,
+                                               "frac": (v[2] / (v[0] / 1e3)) / 1e9 / peak if v[0] > 0 else None,
+                                               "frac_nominal": ((v[2] / (v[0] / 1e3)) / 1e9 / NOMINAL_HBM_GBS
+                                                                if v[0] > 0 else None),
                                                "launches_per_solve": v[1]}
                                            for n, v in kernels.items() if n != "k_rbgs"}},
             "clocks": clocks.summary(),

@@ -1545,11 +1545,14 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bo
   const int sch = C->prm.mg_itrsch;
   for (int itr = 0; itr < it; ++itr) {
     if (sch == 3) {
-      const int pk = (g == 1 && q == SUB_A) ? MF3D_PROF_SMOOTH_L1 : 0;
+      // timed (mf3d_profile): level 1's half-sweeps that read the other
+      // colour, rhs and write their own (12 B per cell in FP64), pre- and
+      // post-smoothing; not the from-zero red half-sweep (8 B per cell)
+      const int pk = (g == 1 && q != SUB_C) ? MF3D_PROF_SMOOTH_L1 : 0;
       const double half = 0.5 * (double)L.cells_sub[q] * sizeof(T);
       const bool fz = from_zero && itr == 0;
       const bool skip_red = fz && red_done;  // the restriction formed the red half-sweep
-      prof_begin(C, pk, (fz ? 2 : 3) * half);
+      prof_begin(C, fz ? 0 : pk, 3 * half);
       const dim3 grid(L.n_sweep[q]), cta(RB_TX, RB_TY);
       if (L.small) {
         const int g2 = grid_of(L.small_items[q], kTile);
@@ -1560,7 +1563,7 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bo
         else
           launch(k_rbgs_small<T, false>, g2, kTile, 0, C->stream, L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p,
                                                              0);
-        prof_end(C, pk);
+        prof_end(C, fz ? 0 : pk);
         prof_begin(C, pk, 3 * half);
         launch(k_rbgs_small<T, false>, g2, kTile, 0, C->stream, L.tab.p, L.spre[q].p, L.list[q].p, L.n_list[q], V.act.p, 1);
         prof_end(C, pk);
@@ -1574,7 +1577,7 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bo
         launch(k_rbgs<T, true>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, L.sfirst[q].p, V.act.p, 0, V.err.p);
       else
         launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, L.sfirst[q].p, V.act.p, 0, V.err.p);
-      prof_end(C, pk);
+      prof_end(C, fz ? 0 : pk);
       prof_begin(C, pk, 3 * half);
       launch(k_rbgs<T, false>, grid, cta, 0, C->stream, L.tab.p, L.sweep[q].p, L.sfirst[q].p, V.act.p, 1, V.err.p);
       prof_end(C, pk);

@@ -819,6 +819,79 @@ struct CvShape {
 
 constexpr int CV_TY = 4, CV_CR = OZ_RJ / CV_TY;  // 32 x CV_TY threads, CV_CR consecutive rows each
 
+// x / b for k_calvel_calmas_tma's march: on an EXACT axis the product with
+// the exact inverse; otherwise Markstein's correction of div_rcp without its
+// branch - `bad` records an x outside the range where the correction is the
+// IEEE quotient (zero, subnormal, huge, non-finite), and the tile then
+// divides again (cv_cells_divide).
+template <bool EXACT>
+__device__ __forceinline__ double qdv(double x, double b, double rb, bool &bad) {
+  if (EXACT) return x * rb;
+  bad |= !rcp_range(x);
+  const double q0 = x * rb;
+  const double q1 = fma(fma(-b, q0, x), rb, q0);
+  return fma(fma(-b, q1, x), rb, q1);
+}
+
+// The cells of one thread of k_calvel_calmas_tma (column i, rows j0 ..
+// j0+CV_CR-1, planes k0..k1) from global memory with IEEE division
+// throughout - calvel's six face velocities, calmas' divergence in the
+// reference's order (press.for:38-67, 139-198) - writing su and returning
+// the rmax contribution.  The tile's fallback where the march met an operand
+// outside Markstein's range, or a divisor without its reciprocal.
+template <typename T>
+__device__ double cv_cells_divide(const BlkFld &F, int i, int j0, int k0, int k1, double dt, double dta, T *rhs1,
+                                  double *SU) {
+  const int nx = F.nx, ny = F.ny, nz = F.nz;
+  const long long sy = F.ti, sz = (long long)F.ti * F.tj;
+  const long long ps1 = (long long)(F.L1.ny + 2) * F.L1.hp;
+  const double *p = F.p;
+  double vmax = 0.0;
+  if (i > nx) return vmax;
+  for (int m = 0; m < CV_CR; ++m) {
+    const int j = j0 + m;
+    if (j > ny) break;
+    for (int k = k0; k <= k1; ++k) {
+      const long long c = fidx(F, i, j, k);
+      const double pc = p[c];
+      double ue, uw, vn, vs, wt, wb;
+      if (i == nx && F.wall[1]) ue = F.hi[0][(k - 1) * ny + (j - 1)];
+      else ue = (F.ustar[c] - dta * (p[c + 1] - pc) / F.df[0][i]);
+      if (i == 1) {
+        const double lo = F.lo[0][(k - 1) * ny + (j - 1)];
+        uw = F.wall[0] ? lo : (lo - dta * (pc - p[c - 1]) / F.df[0][0]);
+      } else {
+        uw = (F.ustar[c - 1] - dta * (pc - p[c - 1]) / F.df[0][i - 1]);
+      }
+      if (j == ny && F.wall[3]) vn = F.hi[1][(k - 1) * nx + (i - 1)];
+      else vn = (F.vstar[c] - dta * (p[c + sy] - pc) / F.df[1][j]);
+      if (j == 1) {
+        const double lo = F.lo[1][(k - 1) * nx + (i - 1)];
+        vs = F.wall[2] ? lo : (lo - dta * (pc - p[c - sy]) / F.df[1][0]);
+      } else {
+        vs = (F.vstar[c - sy] - dta * (pc - p[c - sy]) / F.df[1][j - 1]);
+      }
+      if (k == nz && F.wall[5]) wt = F.hi[2][(j - 1) * nx + (i - 1)];
+      else wt = (F.wstar[c] - dta * (p[c + sz] - pc) / F.df[2][k]);
+      if (k == 1) {
+        const double lo = F.lo[2][(j - 1) * nx + (i - 1)];
+        wb = F.wall[4] ? lo : (lo - dta * (pc - p[c - sz]) / F.df[2][0]);
+      } else {
+        wb = (F.wstar[c - sz] - dta * (pc - p[c - sz]) / F.df[2][k - 1]);
+      }
+      const double hx = F.h[0][i], hy = F.h[1][j], hz = F.h[2][k];
+      const double fact = ((ue - uw) / hx + (vn - vs) / hy + (wt - wb) / hz);
+      const double su = fact / dt;
+      rhs1[(((i + j + k + 1) & 1) ? F.L1.cstr : 0) + k * ps1 + (long long)j * F.L1.hp + (i >> 1)] = (T)su;
+      if (SU) SU[c] = su;
+      double f1 = fabs(fact * hx * hy * hz);
+      if (!(f1 == f1)) f1 = __longlong_as_double(0x7ff0000000000000LL);  // NaN -> +Inf (flagged)
+      vmax = vmax > f1 ? vmax : f1;
+    }
+  }
+  return vmax;
+}
+
 // UMASK bit a: axis a of every block is uniform with a power-of-two spacing
 // (x/h is x*(1/h) there); other axes divide through div_rcp.
 template <typename T, int UMASK>
@@ -833,7 +906,6 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const Blk
   __shared__ __align__(128) unsigned char sbuf[CV_NS * S::STAGE];
   __shared__ __align__(8) uint64_t bar[CV_NS];
   __shared__ double red[CV_TY];
-  __shared__ int abort_s;
   const Tile t = tiles[blockIdx.x];
   if (!act[fl[t.blk].dom]) return;
   const BlkFld F = fl[t.blk];  // by value: read once, never reloaded after the stores below
@@ -905,15 +977,25 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const Blk
       tma_load_3d(b + S::PB + S::UB + S::VB, mw, &bar[st], X, yb, z);
     }
   };
+  // every divisor of the march has its reciprocal (Markstein's correction
+  // needs RN(1/b)); else the tile divides throughout
+  bool fast = dtinv != 0.0 || rdt != 0.0;
+  if (!UX) fast = fast && rhx != 0.0 && rdxe != 0.0 && rdxw != 0.0;
+  if (!UY)
+#pragma unroll
+    for (int m = 0; m < CV_CR; ++m) fast = fast && rhy[m] != 0.0 && rdyn[m] != 0.0 && rdys[m] != 0.0;
+  if (!UZ)
+    for (int kk = k0; kk <= k1; ++kk) fast = fast && F.rdf[2][kk] != 0.0 && F.rh[2][kk] != 0.0;
+  double vmax = 0.0;
+  bool bad = !__syncthreads_and(fast);
+  if (!bad) {
   if (tid == 0) {
     for (int st = 0; st < CV_NS; ++st) mbar_init(&bar[st], 1);
     mbar_fence_init();
-    abort_s = 0;
   }
   __syncthreads();
   if (tid == 0)
     for (int kk = k0; kk < k0 + CV_PD && kk <= k1 + 1; ++kk) issue(kk);
-  double vmax = 0.0;
   bool ok = mbar_wait(&bar[stage(k0)], parity(k0), err);
   for (int k = k0; k <= k1; ++k) {
     if (tid == 0 && ok && k + CV_PD <= k1 + 1) issue(k + CV_PD);  // into the slot of plane k-1
@@ -929,41 +1011,43 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const Blk
 #pragma unroll
     for (int m = 0; m < CV_CR; ++m) {
       const int rr = CV_CR * ty + m;   // row within the tile
+      bool cb = false;                 // an operand out of Markstein's range
       const int r = (rr + 1) * CV_W + cx;  // this cell in the p box
       const double pc = P[r];
       double ue;
       if (ic == nx && ewall) ue = F.hi[0][(k - 1) * ny + (jc[m] - 1)];
-      else ue = (U[rr * CV_W + cx] - qdiv<UX>(dta * (P[r + 1] - pc), dxe, rdxe));
+      else ue = (U[rr * CV_W + cx] - qdv<UX>(dta * (P[r + 1] - pc), dxe, rdxe, cb));
       const double ul = __shfl_up_sync(0xffffffffu, ue, 1);
       double uw;
       if (ic == 1) {
         const double lo = F.lo[0][(k - 1) * ny + (jc[m] - 1)];
-        uw = wwall ? lo : (lo - qdiv<UX>(dta * (pc - P[r - 1]), dxw, rdxw));
+        uw = wwall ? lo : (lo - qdv<UX>(dta * (pc - P[r - 1]), dxw, rdxw, cb));
       } else if (tx > 0) {
         uw = ul;
       } else {
-        uw = (U[rr * CV_W + cx - 1] - qdiv<UX>(dta * (pc - P[r - 1]), dxw, rdxw));
+        uw = (U[rr * CV_W + cx - 1] - qdv<UX>(dta * (pc - P[r - 1]), dxw, rdxw, cb));
       }
       double vn, vs;
       if (jc[m] == ny && nwall) vn = F.hi[1][(k - 1) * nx + (ic - 1)];
-      else vn = (Vv[(rr + 1) * CV_W + cx] - qdiv<UY>(dta * (P[r + CV_W] - pc), dyn[m], rdyn[m]));
+      else vn = (Vv[(rr + 1) * CV_W + cx] - qdv<UY>(dta * (P[r + CV_W] - pc), dyn[m], rdyn[m], cb));
       if (m > 0) {
         vs = vprev;  // the south face of row j is the north face of row j-1 (same operands)
       } else if (jc[m] == 1) {
         const double lo = F.lo[1][(k - 1) * nx + (ic - 1)];
-        vs = swall ? lo : (lo - qdiv<UY>(dta * (pc - P[r - CV_W]), dys[m], rdys[m]));
+        vs = swall ? lo : (lo - qdv<UY>(dta * (pc - P[r - CV_W]), dys[m], rdys[m], cb));
       } else {
-        vs = (Vv[rr * CV_W + cx] - qdiv<UY>(dta * (pc - P[r - CV_W]), dys[m], rdys[m]));
+        vs = (Vv[rr * CV_W + cx] - qdv<UY>(dta * (pc - P[r - CV_W]), dys[m], rdys[m], cb));
       }
       vprev = vn;
       double wt;
       if (top) wt = F.hi[2][(jc[m] - 1) * nx + (ic - 1)];
-      else wt = (Wv[rr * CV_W + cx] - qdiv<UZ>(dta * (PN[r] - pc), dzk, rdzk));
+      else wt = (Wv[rr * CV_W + cx] - qdv<UZ>(dta * (PN[r] - pc), dzk, rdzk, cb));
       const double fact =
-          (qdiv<UX>(ue - uw, hx, rhx) + qdiv<UY>(vn - vs, hy[m], rhy[m]) + qdiv<UZ>(wt - wb[m], hzk, rhzk));
+          (qdv<UX>(ue - uw, hx, rhx, cb) + qdv<UY>(vn - vs, hy[m], rhy[m], cb) + qdv<UZ>(wt - wb[m], hzk, rhzk, cb));
       wb[m] = wt;  // the top face of plane k is the bottom face of plane k+1
+      const double su = dtinv != 0.0 ? fact * dtinv : qdv<false>(fact, dt, rdt, cb);
+      bad |= cb && in[m];
       if (ok && in[m]) {
-        const double su = dtinv != 0.0 ? fact * dtinv : div_rcp(fact, dt, rdt);
         rhs1[((c0[m] ^ (k & 1)) ? F.L1.cstr : 0) + k * ps1 + l1off[m]] = (T)su;
         if (SU) SU[fidx(F, i, jc[m], k)] = su;
         double f1 = fabs(fact * hx * hy[m] * hzk);
@@ -971,10 +1055,11 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const Blk
         vmax = vmax > f1 ? vmax : f1;
       }
     }
-    if (!ok) abort_s = 1;
-    __syncthreads();  // plane k's slot is refilled next iteration
-    if (abort_s) return;
+    if (__syncthreads_or(!ok)) return;  // plane k's slot is refilled next iteration
   }
+  }
+  // an operand out of range somewhere in the tile: divide it again
+  if (__syncthreads_or(bad)) vmax = cv_cells_divide<T>(F, i, t.j0 + CV_CR * ty, k0, k1, dt, dta, rhs1, SU);
   // CTA max: warp shuffles, shared memory, one atomic per CTA
   for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
   if (tx == 0) red[ty] = vmax;
