@@ -34,6 +34,15 @@ struct CcHalo {
   int n;
 };
 
+// t / d for t * d < 2^32 without a division: ceil(2^32 / d) by a high
+// multiply (exact in that range: the rounding of the reciprocal adds less
+// than 1/d to t/d).
+struct FastDiv {
+  unsigned d, m;
+  __device__ explicit FastDiv(unsigned d_) : d(d_), m(d_ > 1 ? 0xffffffffu / d_ + 1u : 0u) {}
+  __device__ __forceinline__ unsigned div(unsigned t) const { return d > 1 ? __umulhi(t, m) : t; }
+};
+
 // Kernel arguments.
 struct CcArgs {
   const BlkLev *tab[CC_MAX_LEVELS];   // per held level (g0 + l): the view's level table (global arrays)
@@ -43,7 +52,15 @@ struct CcArgs {
   int ir, ip;                         // pre-/post-smoothing sweeps
   int dom;                            // the domain (act)
   int bufn;                           // halo staging slots per CTA
+  long long coef_off;                 // shared-memory byte offset of the levels' coefficient and
+                                      // restriction-ratio arrays (cc_coef_bytes each, level order)
 };
+
+// shared-memory bytes of one level's 1-D coefficients (six arrays) and
+// restriction ratios (three) in element size elem, 16-byte aligned
+__host__ __device__ inline long long cc_coef_bytes(const BlkLev &B, int elem) {
+  return ((long long)(3 * (B.nx + B.ny + B.nz + 6)) * elem + 15) / 16 * 16;
+}
 
 // shared-memory layout of one block's held levels: phi (2*cstr) then rhs
 // (2*cstr) per level, each 16-byte aligned; returns the bytes
@@ -60,11 +77,12 @@ __device__ __forceinline__ void cc_sweep(const BlkLev &B, T *phi, const T *rhs, 
   const T *O = phi + (1 - colour) * B.cstr;
   T *M = phi + colour * B.cstr;
   const T *R = rhs + colour * B.cstr;
+  const FastDiv fq((unsigned)Q), fy((unsigned)B.ny);
   for (int t = threadIdx.x; t < items; t += blockDim.x) {
-    int r = t;
-    const int q = r % Q;
-    r /= Q;
-    const int j = r % B.ny + 1, k = r / B.ny + 1;
+    const int r = (int)fq.div((unsigned)t);
+    const int q = t - r * Q;
+    const int kk = (int)fy.div((unsigned)r);
+    const int j = r - kk * B.ny + 1, k = kk + 1;
     const int s = (colour + j + k + 1) & 1;
     const int i = 2 * q + 2 - s;
     if (i > B.nx) continue;
@@ -94,8 +112,10 @@ __device__ __forceinline__ void cc_restrict(const BlkLev &Fb, const TF *P, const
     return ((i + j + k + 1) & 1) * cs + k * plf + j * rowf + (i >> 1);
   };
   const Coef<TC> cc(Cb);
+  const FastDiv fx((unsigned)GX), fy((unsigned)GY);
   for (int t = threadIdx.x; t < GX * GY * GZ; t += blockDim.x) {
-    const int I = t % GX, J = (t / GX) % GY, K = t / (GX * GY);
+    const int r = (int)fx.div((unsigned)t), K = (int)fy.div((unsigned)r);
+    const int I = t - r * GX, J = r - K * GY;
     const long long co = cell_off(Cb, I, J, K);
     PC[co] = (TC)0;
     if (I < 1 || I > Cb.nx || J < 1 || J > Cb.ny || K < 1 || K > Cb.nz) continue;
@@ -141,8 +161,10 @@ __device__ __forceinline__ void cc_prolong(const BlkLev &Fb, TF *PF, const BlkLe
   const int GX = Cb.nx + 1, GY = Cb.ny + 1, GZ = Cb.nz + 1;
   const int m = Fb.nmask;
   const long long csf = Fb.cstr, rowf = Fb.hp, plf = (long long)(Fb.ny + 2) * Fb.hp;
+  const FastDiv fx((unsigned)GX), fy((unsigned)GY);
   for (int t = threadIdx.x; t < GX * GY * GZ; t += blockDim.x) {
-    const int I = t % GX, J = (t / GX) % GY, K = t / (GX * GY);
+    const int r = (int)fx.div((unsigned)t), K = (int)fy.div((unsigned)r);
+    const int I = t - r * GX, J = r - K * GY;
     const bool xw = I == 0 && (m & 1), xe = I == Cb.nx && (m & 2);
     const bool ys = J == 0 && (m & 4), yn = J == Cb.ny && (m & 8);
     const bool zb = K == 0 && (m & 16), zt = K == Cb.nz && (m & 32);
@@ -197,8 +219,10 @@ __global__ void __launch_bounds__(CC_THREADS, 1) k_coarse_cycle(const CcArgs a, 
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char cc_smem[];
   __shared__ long long off[CC_MAX_BLOCKS][CC_MAX_LEVELS];  // byte offset of each rank's level arrays
+  __shared__ BlkLev sdesc[CC_MAX_LEVELS];  // this block's levels, coefficients in shared memory
   if (!act[a.dom]) return;  // the whole cluster is one domain: uniform
   const int b = (int)cluster.block_rank();
+  if (threadIdx.x < a.nlev) sdesc[threadIdx.x] = a.tab[threadIdx.x][a.blk0 + b];
   if (threadIdx.x < a.nb) {
     long long o = 0;
     for (int l = 0; l < a.nlev; ++l) {
@@ -215,7 +239,30 @@ __global__ void __launch_bounds__(CC_THREADS, 1) k_coarse_cycle(const CcArgs a, 
     total += 2 * cc_level_bytes(a.tab[l][a.blk0 + b], elem);
   }
   double *buf = (double *)(cc_smem + (total + 15) / 16 * 16);  // halo staging: values as double
-  auto desc = [&](int l) -> BlkLev { return a.tab[l][a.blk0 + b]; };
+  // the 1-D coefficients and restriction ratios of every held level, read
+  // at each cell of every sweep, restriction and residual: into shared memory
+  {
+    unsigned char *cp = cc_smem + a.coef_off;
+    for (int l = 0; l < a.nlev; ++l) {
+      const BlkLev B = sdesc[l];
+      const int elem = a.g0 + l >= a.lc ? 8 : (int)sizeof(TF);
+      const int nco = 2 * (B.nx + B.ny + B.nz + 6), ngeo = B.nx + B.ny + B.nz + 6;
+      for (int e = threadIdx.x; e < nco + ngeo; e += blockDim.x) {
+        const unsigned char *src = e < nco ? (const unsigned char *)B.coef + (long long)e * elem
+                                           : (const unsigned char *)B.geo + (long long)(e - nco) * elem;
+        if (elem == 8) ((double *)cp)[e] = *(const double *)src;
+        else ((float *)cp)[e] = *(const float *)src;
+      }
+      __syncthreads();  // every thread has read sdesc[l] before it changes
+      if (threadIdx.x == 0) {
+        sdesc[l].coef = cp;
+        sdesc[l].geo = cp + (long long)nco * elem;
+      }
+      cp += cc_coef_bytes(B, elem);
+    }
+    __syncthreads();
+  }
+  auto desc = [&](int l) -> BlkLev { return sdesc[l]; };
   auto phi_at = [&](int r, int l) -> unsigned char * { return cc_smem + off[r][l]; };
   auto rhs_at = [&](int l) -> unsigned char * {
     const int elem = a.g0 + l >= a.lc ? 8 : (int)sizeof(TF);

@@ -1209,13 +1209,36 @@ static int coarse_cycle_plan(mf3d_ctx *C, View &V) {
     }
     size_t worst = 0;
     for (int b = 0; b < nb; ++b) {
-      long long bytes = 0;
-      for (int l = g; l <= V.Lmax; ++l) bytes += 2 * cc_level_bytes(V.lv[l].htab[b], elem_of(l));
-      worst = std::max(worst, (size_t)((bytes + 15) / 16 * 16 + (long long)bn * 8));
+      long long bytes = 0, coef = 0;
+      for (int l = g; l <= V.Lmax; ++l) {
+        bytes += 2 * cc_level_bytes(V.lv[l].htab[b], elem_of(l));
+        coef += cc_coef_bytes(V.lv[l].htab[b], elem_of(l));
+      }
+      worst = std::max(worst, (size_t)((bytes + 15) / 16 * 16 + ((long long)bn * 8 + 15) / 16 * 16 + coef));
     }
     if (worst <= kCcSmemCap) { g0 = g; smem = worst; bufn = bn; }
   }
   if (!g0) return MF3D_OK;
+  long long coef_off = 0;
+  // the coefficient region follows the largest block's levels and halo
+  // buffer (every CTA gets the same dynamic size)
+  {
+    long long worst = 0;
+    for (int b = 0; b < nb; ++b) {
+      long long bytes = 0;
+      for (int l = g0; l <= V.Lmax; ++l) bytes += 2 * cc_level_bytes(V.lv[l].htab[b], elem_of(l));
+      worst = std::max(worst, (bytes + 15) / 16 * 16 + ((long long)bufn * 8 + 15) / 16 * 16);
+    }
+    coef_off = worst;
+    long long coef = 0;
+    for (int b = 0; b < nb; ++b) {
+      long long c = 0;
+      for (int l = g0; l <= V.Lmax; ++l) c += cc_coef_bytes(V.lv[l].htab[b], elem_of(l));
+      coef = std::max(coef, c);
+    }
+    smem = (size_t)(worst + coef);
+    if (smem > kCcSmemCap) return MF3D_OK;  // the launch path stays
+  }
   void (*kern)(const CcArgs, const int *) = C->elem == 8 ? k_coarse_cycle<double> : k_coarse_cycle<float>;
   // the device holds such a cluster at all (else the launch path stays)
   {
@@ -1263,6 +1286,7 @@ static int coarse_cycle_plan(mf3d_ctx *C, View &V) {
   a.ip = C->prm.iproln;
   a.dom = 0;
   a.bufn = bufn;
+  a.coef_off = coef_off;
   V.cc_g0 = g0;
   V.cc_smem = smem;
   CK(cudaStreamSynchronize(C->stream));  // the host vectors are locals
