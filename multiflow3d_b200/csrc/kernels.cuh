@@ -44,8 +44,7 @@ struct BlkLev {
   int nx, ny, nz, hp; // interior cells (0 = block absent at this level)
   int nmask;          // Neumann faces: bit f set for f = W,E,S,N,B,T
   int dom;            // domain of the block
-  const CUtensorMap *tm;  // TMA maps: phi colour 0, phi colour 1 (RB_RJ+2 rows), rhs colour 0, 1 (RB_RJ rows);
-                          // then the sweep's: phi c0, c1 (SW_RJ+2 rows), rhs c0, c1 (SW_RJ rows)
+  const CUtensorMap *tm;  // TMA maps: phi colour 0, phi colour 1 (RB_RJ+2 rows), rhs colour 0, 1 (RB_RJ rows)
   const void *cc;     // variable density (L_LSM): per-cell aw, ae, as, an, ab, at, six arrays of
                       // the level's colour-split layout, array m at element m*2*cstr; else null
   void *tdf;          // line relaxation: the TDMA factors a, apr of each direction (k_tdma_factor); else null
@@ -118,11 +117,7 @@ struct Tile {
 // Tile shapes (threads per CTA = TX * RJ).
 // red-black z-march: 32 x RB_TY threads, RB_CR rows per thread (RB_RJ rows
 // per CTA); planes per CTA chosen per level
-constexpr int RB_TX = 32, RB_TY = 4, RB_CR = 4, RB_RJ = RB_TY * RB_CR;  // restriction boxes (k_restrict_tma)
-// the red-black sweep's tile: RB_TX compact columns x SW_RJ rows, SW_CR rows
-// per thread; thinner than the restriction's so that its plane ring keeps
-// more planes in flight in the same shared memory
-constexpr int SW_CR = 2, SW_RJ = RB_TY * SW_CR;
+constexpr int RB_TX = 32, RB_TY = 4, RB_CR = 4, RB_RJ = RB_TY * RB_CR;
 constexpr int RW_TX = 32, RW_RJ = 8, RW_KCH = 8;    // row tiles, RW_KCH planes per CTA
 constexpr int OZ_TX = 32, OZ_RJ = 8, OZ_KCH = 16;   // outer calvel/calmas z-march
 
@@ -236,21 +231,21 @@ __device__ __forceinline__ void st_hint(float *p, float v, uint64_t pol) {
 // i = 2q + 2 - s with s = i & 1 = (colour + j + k + 1) & 1, so a row of nx
 // cells keeps ceil(nx/2) lanes busy whatever its parity.  Its west and east
 // neighbours (other colour) sit at compact h = q and q+1, the others and the
-// rhs at h = q + 1 - s.  A column is q0..q0+31 of rows j0..j0+SW_RJ-1 of one
-// block (each thread SW_CR rows RB_TY apart, which share s); a segment is a
+// rhs at h = q + 1 - s.  A column is q0..q0+31 of rows j0..j0+RB_RJ-1 of one
+// block (each thread RB_CR rows RB_TY apart, which share s); a segment is a
 // run of planes k0..k1 of one column.  The planes of all columns of the
 // launch are laid end to end and split evenly over the CTAs the device holds
 // at once, so every CTA marches the same number of planes - a CTA whose
 // share crosses a column boundary runs two segments, each with its own ring
 // fill - and the launch is one wave with no tail.
 // Per plane one thread issues two TMA box loads - the other colour over
-// compact columns q0..q0+W-1 and rows j0-1..j0+SW_RJ, the rhs over the same
-// columns and rows j0..j0+SW_RJ-1 - into a ring of RB_NS stages, RB_PD
+// compact columns q0..q0+W-1 and rows j0-1..j0+RB_RJ, the rhs over the same
+// columns and rows j0..j0+RB_RJ-1 - into a ring of RB_NS stages, RB_PD
 // planes ahead of the plane being computed.  Loads are numbered across the
 // CTA's segments, which fixes each one's stage and mbarrier phase.  Boxes
 // that reach past the array read zeros (never used).
 // ---------------------------------------------------------------------------
-constexpr int RB_PD = 6;          // prefetch distance in planes
+constexpr int RB_PD = 2;          // prefetch distance in planes
 constexpr int RB_KMAX = 64;       // planes per segment at most
 constexpr int RB_NS = RB_PD + 2;  // stages: planes k-1 .. k+RB_PD (a power of two)
 static_assert((RB_NS & (RB_NS - 1)) == 0, "RB_NS must be a power of two");
@@ -264,7 +259,7 @@ struct RbSeg {
 template <typename T>
 struct RbShape {
   static constexpr int W = (33 * (int)sizeof(T) + 15) / 16 * 16 / (int)sizeof(T);  // box width: 33 used
-  static constexpr int OE = (SW_RJ + 2) * W, RE = SW_RJ * W;                        // elements per box
+  static constexpr int OE = (RB_RJ + 2) * W, RE = RB_RJ * W;                        // elements per box
   static constexpr int OB = (OE * (int)sizeof(T) + 127) / 128 * 128;                // bytes per stage slot
   static constexpr int RBY = (RE * (int)sizeof(T) + 127) / 128 * 128;
 };
@@ -306,17 +301,17 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
     const int nx = B.nx, ny = B.ny, hp = B.hp;
     const long long rs = (long long)(ny + 2) * hp;  // plane stride
     T *__restrict__ M = phi_of<T>(B) + colour * B.cstr + q0;
-    const CUtensorMap *mo = B.tm + 4 + (1 - colour), *mr = B.tm + 6 + colour;  // the sweep's maps
+    const CUtensorMap *mo = B.tm + (1 - colour), *mr = B.tm + 2 + colour;
     const Coef<T> cf(B);
     const int k0 = t.k0, k1 = t.k1;
     // coefficients of this lane's two cells (s = 0: i = 2q+2; s = 1: i = 2q+1)
     const int ia = min(2 * q + 2, nx + 1), ib = min(2 * q + 1, nx + 1);
     const T aw0 = cf.aw[ia], ae0 = cf.ae[ia], aw1 = cf.aw[ib], ae1 = cf.ae[ib];
     // per row: as, an and ap's first four terms (summed left to right)
-    T as[SW_CR], an[SW_CR], pa0[SW_CR], pa1[SW_CR];
-    int rowoff[SW_CR];  // j*hp of each row
+    T as[RB_CR], an[RB_CR], pa0[RB_CR], pa1[RB_CR];
+    int rowoff[RB_CR];  // j*hp of each row
 #pragma unroll
-    for (int m = 0; m < SW_CR; ++m) {
+    for (int m = 0; m < RB_CR; ++m) {
       const int j = t.j0 + ty + RB_TY * m;
       const bool jin = j <= ny;
       as[m] = jin ? cf.as[j] : (T)0;
@@ -325,7 +320,7 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
       pa1[m] = ((aw1 + ae1) + as[m]) + an[m];
       rowoff[m] = j * hp;
     }
-    const int nrow = t.j0 + ty > ny ? 0 : min(SW_CR, (ny - t.j0 - ty) / RB_TY + 1);  // rows inside the block
+    const int nrow = t.j0 + ty > ny ? 0 : min(RB_CR, (ny - t.j0 - ty) / RB_TY + 1);  // rows inside the block
     auto loads = [&](int kk) { return FROM_ZERO ? (kk >= k0 && kk <= k1) : (kk >= k0 - 1 && kk <= k1 + 1); };
     // the loaded planes are consecutive (k0-1 is loaded unless FROM_ZERO)
     constexpr int lead = FROM_ZERO ? 0 : 1;
@@ -371,7 +366,7 @@ __global__ void __launch_bounds__(RB_TX *RB_TY) k_rbgs(const BlkLev *__restrict_
         const T *r = slot_r(st);
         T *Mk = M + (long long)k * rs + hc;
 #pragma unroll
-        for (int m = 0; m < SW_CR; ++m) {
+        for (int m = 0; m < RB_CR; ++m) {
           if (m < nrow) {
             const int rr = ty + RB_TY * m;  // row within the tile
             T w = (T)0, e = (T)0, so_ = (T)0, no = (T)0, bo = (T)0, to = (T)0;

@@ -270,7 +270,7 @@ struct LevelStore {
   int elem = 8;  // bytes per value of this level
   std::vector<std::vector<char>> host;  // host images of the uploaded small arrays
   DevBuf<char> phi, rhs, coef, geo;
-  DevBuf<CUtensorMap> tmaps;  // restriction: phi c0, c1, rhs c0, c1; sweep: the same
+  DevBuf<CUtensorMap> tmaps;  // phi c0, phi c1, rhs c0, rhs c1
   DevBuf<double> cc;          // L_LSM: per-cell coefficients (six colour-split arrays)
   DevBuf<double> dens;        // L_LSM, levels > 1: cell densities, interior, i fastest
   BlkLev desc;  // host copy with device pointers
@@ -425,17 +425,14 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
     B.rhs = L.rhs.p;
     B.coef = L.coef.p;
     B.geo = L.geo.p;
-    // TMA maps of the restriction and of the sweep (colour arrays start
-    // 256-byte aligned, rows 16-byte multiples)
-    CUtensorMap tm[8];
+    // TMA maps of the sweep (colour arrays start 256-byte aligned, rows 16-byte multiples)
+    CUtensorMap tm[4];
     const int W = elem == 8 ? RbShape<double>::W : RbShape<float>::W;
     for (int c = 0; c < 2; ++c) {
       if ((st = colour_map(&tm[c], L.phi.p + (size_t)c * B.cstr * elem, elem, B, W, RB_RJ + 2))) return st;
       if ((st = colour_map(&tm[2 + c], L.rhs.p + (size_t)c * B.cstr * elem, elem, B, W, RB_RJ))) return st;
-      if ((st = colour_map(&tm[4 + c], L.phi.p + (size_t)c * B.cstr * elem, elem, B, W, SW_RJ + 2))) return st;
-      if ((st = colour_map(&tm[6 + c], L.rhs.p + (size_t)c * B.cstr * elem, elem, B, W, SW_RJ))) return st;
     }
-    if ((st = L.tmaps.alloc(8))) return st;
+    if ((st = L.tmaps.alloc(4))) return st;
     L.host.emplace_back(sizeof tm);
     std::memcpy(L.host.back().data(), tm, sizeof tm);
     CK(cudaMemcpyAsync(L.tmaps.p, L.host.back().data(), sizeof tm, cudaMemcpyHostToDevice, s));
@@ -945,7 +942,7 @@ static void prof_collect(mf3d_ctx *C) {
 constexpr long long kSmallLevelCells = 1ll << 19;
 
 // Red-black sweep segments of a set of blocks (k_rbgs).  A column is 32
-// lanes over q (ceil(nx/2) per row) by SW_RJ rows of one block.  Schedules:
+// lanes over q (ceil(nx/2) per row) by RB_RJ rows of one block.  Schedules:
 //   0  the planes of all columns laid end to end and cut into equal runs, one
 //      per CTA: as many CTAs as the device holds at once (whole multiples of
 //      that when a run would exceed RB_KMAX planes), so the launch has no
@@ -970,7 +967,7 @@ static int sweep_segments(const mf3d_ctx *C, const std::vector<BlkLev> &tab, con
   long long planes = 0, columns = 0;
   for (int b : blocks) {
     const BlkLev &B = tab[b];
-    const long long cols = (long long)((B.nx + 1) / 2 + RB_TX - 1) / RB_TX * ((B.ny + SW_RJ - 1) / SW_RJ);
+    const long long cols = (long long)((B.nx + 1) / 2 + RB_TX - 1) / RB_TX * ((B.ny + RB_RJ - 1) / RB_RJ);
     columns += cols;
     planes += cols * B.nz;
   }
@@ -991,7 +988,7 @@ static int sweep_segments(const mf3d_ctx *C, const std::vector<BlkLev> &tab, con
         long long n = 0;
         for (int b : blocks) {
           const BlkLev &B = tab[b];
-          n += (long long)((B.nx + 1) / 2 + RB_TX - 1) / RB_TX * ((B.ny + SW_RJ - 1) / SW_RJ) * ((B.nz + kc - 1) / kc);
+          n += (long long)((B.nx + 1) / 2 + RB_TX - 1) / RB_TX * ((B.ny + RB_RJ - 1) / RB_RJ) * ((B.nz + kc - 1) / kc);
         }
         const double cost = (double)((n + resident - 1) / resident) * (kc + RB_PD);
         if (cost <= best) { best = cost; kch4 = kc; }
@@ -1001,7 +998,7 @@ static int sweep_segments(const mf3d_ctx *C, const std::vector<BlkLev> &tab, con
       const BlkLev &B = tab[b];
       const long long run = sched == 4 ? kch4 : run_of(B);
       for (int k = 1; k <= B.nz; k += (int)run)
-        for (int j0 = 1; j0 <= B.ny; j0 += SW_RJ)
+        for (int j0 = 1; j0 <= B.ny; j0 += RB_RJ)
           for (int q0 = 0; q0 < (B.nx + 1) / 2; q0 += RB_TX) {
             segs.push_back(RbSeg{b, k, (int)std::min<long long>(k + run - 1, B.nz), j0, q0, 0, 0, 0});
             first.push_back((int)segs.size());
@@ -1015,7 +1012,7 @@ static int sweep_segments(const mf3d_ctx *C, const std::vector<BlkLev> &tab, con
   long long left = run;
   for (int b : blocks) {
     const BlkLev &B = tab[b];
-    for (int j0 = 1; j0 <= B.ny; j0 += SW_RJ)
+    for (int j0 = 1; j0 <= B.ny; j0 += RB_RJ)
       for (int q0 = 0; q0 < (B.nx + 1) / 2; q0 += RB_TX)
         for (int k = 1; k <= B.nz;) {
           const int take = (int)std::min<long long>(left, B.nz - k + 1);
