@@ -68,34 +68,97 @@ __host__ __device__ inline long long cc_level_bytes(const BlkLev &B, int elem) {
   return ((long long)2 * B.cstr * elem + 15) / 16 * 16;
 }
 
+// One item of a red-black half-sweep: the cell of colour `colour` in
+// compact column q of row j, plane k (none where i = 2q+2-s passes nx);
+// FROM_ZERO: every neighbour reads as 0 (the first red half-sweep after
+// mgrestr zeroed the level).  The arithmetic of k_rbgs / k_rbgs_small.
+template <typename T, bool FROM_ZERO>
+__device__ __forceinline__ void sweep_cell(const BlkLev &B, const Coef<T> &cf, T *phi, const T *rhs, int colour, int q,
+                                           int j, int k) {
+  const int s = (colour + j + k + 1) & 1;
+  const int i = 2 * q + 2 - s;
+  if (i > B.nx) return;
+  const long long rs = (long long)(B.ny + 2) * B.hp;
+  const T *O = phi + (1 - colour) * B.cstr;
+  T *M = phi + colour * B.cstr;
+  const T *R = rhs + colour * B.cstr;
+  const long long base = (long long)k * rs + (long long)j * B.hp;
+  const int h = q + 1 - s;
+  T w = (T)0, e = (T)0, so = (T)0, no = (T)0, bo = (T)0, to = (T)0;
+  if (!FROM_ZERO) {
+    w = O[base + q]; e = O[base + q + 1]; so = O[base - B.hp + h]; no = O[base + B.hp + h];
+    bo = O[base - rs + h]; to = O[base + rs + h];
+  }
+  T aw, ae, as, an, ab, at;
+  cell_coefs(B, cf, i, j, k, aw, ae, as, an, ab, at);
+  const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
+  M[base + h] = ((R[base + h] - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
+}
+
 template <typename T>
 __device__ __forceinline__ void cc_sweep(const BlkLev &B, T *phi, const T *rhs, int colour) {
   const int Q = (B.nx + 1) / 2;
   const int items = Q * B.ny * B.nz;
   const Coef<T> cf(B);
-  const long long rs = (long long)(B.ny + 2) * B.hp;
-  const T *O = phi + (1 - colour) * B.cstr;
-  T *M = phi + colour * B.cstr;
-  const T *R = rhs + colour * B.cstr;
   const FastDiv fq((unsigned)Q), fy((unsigned)B.ny);
   for (int t = threadIdx.x; t < items; t += blockDim.x) {
     const int r = (int)fq.div((unsigned)t);
     const int q = t - r * Q;
     const int kk = (int)fy.div((unsigned)r);
-    const int j = r - kk * B.ny + 1, k = kk + 1;
-    const int s = (colour + j + k + 1) & 1;
-    const int i = 2 * q + 2 - s;
-    if (i > B.nx) continue;
-    const long long base = (long long)k * rs + (long long)j * B.hp;
-    const int h = q + 1 - s;
-    const T w = O[base + q], e = O[base + q + 1], so = O[base - B.hp + h], no = O[base + B.hp + h];
-    const T bo = O[base - rs + h], to = O[base + rs + h];
-    T aw, ae, as, an, ab, at;
-    cell_coefs(B, cf, i, j, k, aw, ae, as, an, ab, at);
-    const T ap = (T)-1.0 * (aw + ae + as + an + ab + at);
-    M[base + h] = ((R[base + h] - (aw * w + ae * e + as * so + an * no + ab * bo + at * to)) / ap);
+    sweep_cell<T, false>(B, cf, phi, rhs, colour, q, r - kk * B.ny + 1, kk + 1);
   }
   __syncthreads();
+}
+
+// mgrestr from the fine level (Fb, P, R) into the coarse one (Cb, PC, RC):
+// coarse phi := 0 on every cell, the interior coarse rhs from the 8
+// children's residuals, and the coarse from-zero red half-sweep - k_restrict.
+// One coarse cell (I, J, K) of mgrestr, ghost-inclusive indices: phi := 0;
+// an interior cell also takes the rhs from its 8 children's residuals and,
+// red, the level's from-zero red half-sweep - k_restrict_tma's arithmetic.
+template <typename TF, typename TC>
+__device__ __forceinline__ void restrict_cell(const BlkLev &Fb, const Coef<TF> &cf, const TF *P, const TF *R,
+                                              const BlkLev &Cb, const Coef<TC> &cc, TC *PC, TC *RC, int I, int J,
+                                              int K) {
+  const TF *rx = (const TF *)Fb.geo, *ry = rx + (Fb.nx + 2), *rz = ry + (Fb.ny + 2);
+  const long long cs = Fb.cstr, rowf = Fb.hp, plf = (long long)(Fb.ny + 2) * Fb.hp;
+  auto fo = [&](int i, int j, int k) -> long long {
+    return ((i + j + k + 1) & 1) * cs + k * plf + j * rowf + (i >> 1);
+  };
+  const long long co = cell_off(Cb, I, J, K);
+  PC[co] = (TC)0;
+  if (I < 1 || I > Cb.nx || J < 1 || J > Cb.ny || K < 1 || K > Cb.nz) return;
+  TF sum = (TF)0;
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk) {
+    const int fk = 2 * K - 1 + dk;
+    const TF ab = cf.ab[fk], at = cf.at[fk], sz = rz[fk];
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int di = 0; di < 2; ++di) {
+        const int fi = 2 * I - 1 + di, fj = 2 * J - 1 + dj;
+        const TF cw = cf.aw[fi], ce = cf.ae[fi], cs_ = cf.as[fj], cn = cf.an[fj];
+        const TF ap = (TF)-1.0 * (cw + ce + cs_ + cn + ab + at);
+        const TF pw = P[fo(fi - 1, fj, fk)], pe = P[fo(fi + 1, fj, fk)];
+        const TF ps = P[fo(fi, fj - 1, fk)], pn = P[fo(fi, fj + 1, fk)];
+        const TF pb = P[fo(fi, fj, fk - 1)], pt = P[fo(fi, fj, fk + 1)];
+        const TF pp = P[fo(fi, fj, fk)];
+        const TF r = R[fo(fi, fj, fk)];
+        const TF res = r - (cw * pw + ce * pe + cs_ * ps + cn * pn + ab * pb + at * pt + ap * pp);
+        const TF s = (TF)8.0 * rx[fi] * ry[fj] * sz;
+        const TF a = res * s;
+        sum = (dk | dj | di) ? sum + a : a;
+      }
+  }
+  const TF v = (TF)0.125 * sum;
+  RC[co] = (TC)v;
+  if (colour_of(I, J, K) == 0) {
+    TC aw, ae, as, an, ab, at;
+    cell_coefs(Cb, cc, I, J, K, aw, ae, as, an, ab, at);
+    const TC ap = (TC)-1.0 * (aw + ae + as + an + ab + at);
+    PC[co] = ((TC)v / ap);
+  }
 }
 
 // mgrestr from the fine level (Fb, P, R) into the coarse one (Cb, PC, RC):
@@ -106,52 +169,67 @@ __device__ __forceinline__ void cc_restrict(const BlkLev &Fb, const TF *P, const
                                             TC *RC) {
   const int GX = Cb.nx + 2, GY = Cb.ny + 2, GZ = Cb.nz + 2;
   const Coef<TF> cf(Fb);
-  const TF *rx = (const TF *)Fb.geo, *ry = rx + (Fb.nx + 2), *rz = ry + (Fb.ny + 2);
-  const long long cs = Fb.cstr, rowf = Fb.hp, plf = (long long)(Fb.ny + 2) * Fb.hp;
-  auto fo = [&](int i, int j, int k) -> long long {
-    return ((i + j + k + 1) & 1) * cs + k * plf + j * rowf + (i >> 1);
-  };
   const Coef<TC> cc(Cb);
   const FastDiv fx((unsigned)GX), fy((unsigned)GY);
   for (int t = threadIdx.x; t < GX * GY * GZ; t += blockDim.x) {
     const int r = (int)fx.div((unsigned)t), K = (int)fy.div((unsigned)r);
-    const int I = t - r * GX, J = r - K * GY;
-    const long long co = cell_off(Cb, I, J, K);
-    PC[co] = (TC)0;
-    if (I < 1 || I > Cb.nx || J < 1 || J > Cb.ny || K < 1 || K > Cb.nz) continue;
-    TF sum = (TF)0;
-#pragma unroll
-    for (int dk = 0; dk < 2; ++dk) {
-      const int fk = 2 * K - 1 + dk;
-      const TF ab = cf.ab[fk], at = cf.at[fk], sz = rz[fk];
-#pragma unroll
-      for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-        for (int di = 0; di < 2; ++di) {
-          const int fi = 2 * I - 1 + di, fj = 2 * J - 1 + dj;
-          const TF cw = cf.aw[fi], ce = cf.ae[fi], cs_ = cf.as[fj], cn = cf.an[fj];
-          const TF ap = (TF)-1.0 * (cw + ce + cs_ + cn + ab + at);
-          const TF pw = P[fo(fi - 1, fj, fk)], pe = P[fo(fi + 1, fj, fk)];
-          const TF ps = P[fo(fi, fj - 1, fk)], pn = P[fo(fi, fj + 1, fk)];
-          const TF pb = P[fo(fi, fj, fk - 1)], pt = P[fo(fi, fj, fk + 1)];
-          const TF pp = P[fo(fi, fj, fk)];
-          const TF r = R[fo(fi, fj, fk)];
-          const TF res = r - (cw * pw + ce * pe + cs_ * ps + cn * pn + ab * pb + at * pt + ap * pp);
-          const TF s = (TF)8.0 * rx[fi] * ry[fj] * sz;
-          const TF a = res * s;
-          sum = (dk | dj | di) ? sum + a : a;
-        }
-    }
-    const TF v = (TF)0.125 * sum;
-    RC[co] = (TC)v;
-    if (colour_of(I, J, K) == 0) {
-      TC aw, ae, as, an, ab, at;
-      cell_coefs(Cb, cc, I, J, K, aw, ae, as, an, ab, at);
-      const TC ap = (TC)-1.0 * (aw + ae + as + an + ab + at);
-      PC[co] = ((TC)v / ap);
-    }
+    restrict_cell<TF, TC>(Fb, cf, P, R, Cb, cc, PC, RC, t - r * GX, r - K * GY, K);
   }
   __syncthreads();
+}
+
+// mgcorr + mgbound from the coarse level (Cb, PC) onto the fine one (Fb, PF):
+// one 2x2x2 fine group per thread - k_prolong.
+// One fine group (2I..2I+1) x (2J..2J+1) x (2K..2K+1) of mgcorr + mgbound,
+// from the coarse cells (I..I+1, J..J+1, K..K+1) - k_prolong's arithmetic.
+template <typename TF, typename TC>
+__device__ __forceinline__ void prolong_group(const BlkLev &Fb, TF *PF, const BlkLev &Cb, const TC *PC, int I, int J,
+                                              int K) {
+  const int m = Fb.nmask;
+  const long long csf = Fb.cstr, rowf = Fb.hp, plf = (long long)(Fb.ny + 2) * Fb.hp;
+  const bool xw = I == 0 && (m & 1), xe = I == Cb.nx && (m & 2);
+  const bool ys = J == 0 && (m & 4), yn = J == Cb.ny && (m & 8);
+  const bool zb = K == 0 && (m & 16), zt = K == Cb.nz && (m & 32);
+  TF lo[2][2], hi[2][2];
+#pragma unroll
+  for (int a = 0; a < 2; ++a)
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      lo[a][b] = (TF)PC[cell_off(Cb, I + a, J + b, K)];
+      hi[a][b] = (TF)PC[cell_off(Cb, I + a, J + b, K + 1)];
+    }
+  TF v[2][2][2];
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int di = 0; di < 2; ++di) {
+        auto w = [&](int a, int b, int c) -> TF {
+          return (TF)((a == di ? 3 : 1) * (b == dj ? 3 : 1) * (c == dk ? 3 : 1));
+        };
+        const TF corr = (w(0, 0, 0) * lo[0][0] + w(0, 1, 0) * lo[0][1] + w(0, 0, 1) * hi[0][0] +
+                         w(0, 1, 1) * hi[0][1] + w(1, 0, 0) * lo[1][0] + w(1, 1, 0) * lo[1][1] +
+                         w(1, 0, 1) * hi[1][0] + w(1, 1, 1) * hi[1][1]) *
+                        (TF)0.015625;
+        const long long o = ((di + dj + dk + 1) & 1) * csf + (2 * K + dk) * plf + (2 * J + dj) * rowf + I;
+        v[dk][dj][di] = PF[o] + corr;
+      }
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int di = 0; di < 2; ++di) {
+        const int si = (di == 0 && xw) ? 1 : (di == 1 && xe) ? 0 : di;
+        const int sj = (dj == 0 && ys) ? 1 : (dj == 1 && yn) ? 0 : dj;
+        const int sk = (dk == 0 && zb) ? 1 : (dk == 1 && zt) ? 0 : dk;
+        const long long o = ((di + dj + dk + 1) & 1) * csf + (2 * K + dk) * plf + (2 * J + dj) * rowf + I;
+        const TF a0 = si ? v[0][0][1] : v[0][0][0], a1 = si ? v[0][1][1] : v[0][1][0];
+        const TF a2 = si ? v[1][0][1] : v[1][0][0], a3 = si ? v[1][1][1] : v[1][1][0];
+        const TF b0 = sj ? a1 : a0, b1 = sj ? a3 : a2;
+        PF[o] = sk ? b1 : b0;
+      }
 }
 
 // mgcorr + mgbound from the coarse level (Cb, PC) onto the fine one (Fb, PF):
@@ -159,55 +237,10 @@ __device__ __forceinline__ void cc_restrict(const BlkLev &Fb, const TF *P, const
 template <typename TF, typename TC>
 __device__ __forceinline__ void cc_prolong(const BlkLev &Fb, TF *PF, const BlkLev &Cb, const TC *PC) {
   const int GX = Cb.nx + 1, GY = Cb.ny + 1, GZ = Cb.nz + 1;
-  const int m = Fb.nmask;
-  const long long csf = Fb.cstr, rowf = Fb.hp, plf = (long long)(Fb.ny + 2) * Fb.hp;
   const FastDiv fx((unsigned)GX), fy((unsigned)GY);
   for (int t = threadIdx.x; t < GX * GY * GZ; t += blockDim.x) {
     const int r = (int)fx.div((unsigned)t), K = (int)fy.div((unsigned)r);
-    const int I = t - r * GX, J = r - K * GY;
-    const bool xw = I == 0 && (m & 1), xe = I == Cb.nx && (m & 2);
-    const bool ys = J == 0 && (m & 4), yn = J == Cb.ny && (m & 8);
-    const bool zb = K == 0 && (m & 16), zt = K == Cb.nz && (m & 32);
-    TF lo[2][2], hi[2][2];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        lo[a][b] = (TF)PC[cell_off(Cb, I + a, J + b, K)];
-        hi[a][b] = (TF)PC[cell_off(Cb, I + a, J + b, K + 1)];
-      }
-    TF v[2][2][2];
-#pragma unroll
-    for (int dk = 0; dk < 2; ++dk)
-#pragma unroll
-      for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-        for (int di = 0; di < 2; ++di) {
-          auto w = [&](int a, int b, int c) -> TF {
-            return (TF)((a == di ? 3 : 1) * (b == dj ? 3 : 1) * (c == dk ? 3 : 1));
-          };
-          const TF corr = (w(0, 0, 0) * lo[0][0] + w(0, 1, 0) * lo[0][1] + w(0, 0, 1) * hi[0][0] +
-                           w(0, 1, 1) * hi[0][1] + w(1, 0, 0) * lo[1][0] + w(1, 1, 0) * lo[1][1] +
-                           w(1, 0, 1) * hi[1][0] + w(1, 1, 1) * hi[1][1]) *
-                          (TF)0.015625;
-          const long long o = ((di + dj + dk + 1) & 1) * csf + (2 * K + dk) * plf + (2 * J + dj) * rowf + I;
-          v[dk][dj][di] = PF[o] + corr;
-        }
-#pragma unroll
-    for (int dk = 0; dk < 2; ++dk)
-#pragma unroll
-      for (int dj = 0; dj < 2; ++dj)
-#pragma unroll
-        for (int di = 0; di < 2; ++di) {
-          const int si = (di == 0 && xw) ? 1 : (di == 1 && xe) ? 0 : di;
-          const int sj = (dj == 0 && ys) ? 1 : (dj == 1 && yn) ? 0 : dj;
-          const int sk = (dk == 0 && zb) ? 1 : (dk == 1 && zt) ? 0 : dk;
-          const long long o = ((di + dj + dk + 1) & 1) * csf + (2 * K + dk) * plf + (2 * J + dj) * rowf + I;
-          const TF a0 = si ? v[0][0][1] : v[0][0][0], a1 = si ? v[0][1][1] : v[0][1][0];
-          const TF a2 = si ? v[1][0][1] : v[1][0][0], a3 = si ? v[1][1][1] : v[1][1][0];
-          const TF b0 = sj ? a1 : a0, b1 = sj ? a3 : a2;
-          PF[o] = sk ? b1 : b0;
-        }
+    prolong_group<TF, TC>(Fb, PF, Cb, PC, t - r * GX, r - K * GY, K);
   }
   __syncthreads();
 }

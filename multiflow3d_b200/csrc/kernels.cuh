@@ -127,7 +127,9 @@ constexpr int OZ_TX = 32, OZ_RJ = 8, OZ_KCH = 16;   // outer calvel/calmas z-mar
 // an error code for the host and the CTA returns.
 // ---------------------------------------------------------------------------
 constexpr unsigned long long kMaxWaitNs = 2000000000ull;  // 2 s
-enum : int { ERR_TMA_WAIT = 1, ERR_WALL_LAW = 2 };  // ERR_WALL_LAW: a smooth-wall law did not converge
+// ERR_WALL_LAW: a smooth-wall law did not converge; ERR_MID_BARRIER: a grid
+// barrier of the middle-level launch gave up waiting
+enum : int { ERR_TMA_WAIT = 1, ERR_WALL_LAW = 2, ERR_MID_BARRIER = 3 };
 
 // Testing aid (mf3d_test_stall_copy): when nonzero, the first red-black
 // half-sweep CTA that sees it takes it (atomically, so exactly one CTA) and

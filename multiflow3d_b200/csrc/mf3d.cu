@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <atomic>
@@ -31,6 +32,7 @@
 
 #include "kernels.cuh"
 #include "coarse.cuh"
+#include "midcycle.cuh"
 #include "mf3d_internal.h"
 #include "outer.cuh"
 
@@ -226,6 +228,25 @@ static cudaError_t launch_cl(void (*kernel)(KArgs...), dim3 grid, dim3 block, si
   cfg.stream = s;
   cfg.attrs = at;
   cfg.numAttrs = cl > 1 ? 2 : 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// A cooperative launch (every CTA resident at once, for a kernel with grid
+// barriers), in plain stream order: no programmatic overlap with the kernels
+// around it, so no other grid holds the SMs its CTAs need.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_coop(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                               Args &&...args) {
+  cudaLaunchAttribute at;
+  at.id = cudaLaunchAttributeCooperative;
+  at.val.cooperative = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = &at;
+  cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
@@ -829,6 +850,14 @@ struct View {
   int cc_g0 = 0;
   size_t cc_smem = 0;
   CcArgs cc_args;
+  // the middle levels in one cooperative launch per direction (k_mid_cycle):
+  // phases down (levels 2 .. first cluster level - 1, or the coarsest) and up
+  bool mid_on = false;
+  DevBuf<MidPhase> mid_down, mid_up;
+  int n_mid_down = 0, n_mid_up = 0, mid_grid = 0;
+  std::vector<DevBuf<int>> mid_lists;
+  std::vector<DevBuf<long long>> mid_pres;
+  DevBuf<MidBar> mid_bar;
   DevBuf<CcHalo> cc_halo;
   DevBuf<HaloCopy> cc_pairs;
   DevBuf<DomState> ds;
@@ -1293,6 +1322,137 @@ static int coarse_cycle_plan(mf3d_ctx *C, View &V) {
   return MF3D_OK;
 }
 
+// The phases of the middle levels (k_mid_cycle), in vcycle's order: down,
+// for levels 2 .. gtop, the pre-smoothing of every present block (the first
+// red half-sweep came with the restriction into the level), the extra
+// sweeps of blocks bottoming out there, the restriction into the next
+// level; up, from the level above the cluster (or the one above the
+// coarsest) to 2, the prolongation from below and the post-smoothing.  Red-
+// black smoothing without L_LSM, levels of one element type, the levels'
+// items below 2^31; otherwise the launch path stays.
+static int mid_cycle_plan(mf3d_ctx *C, View &V) {
+  V.mid_on = false;
+  const char *e = std::getenv("MF3D_MID_CYCLE");
+  if (e && e[0] == '0') return MF3D_OK;
+  const int sch = C->prm.mg_itrsch, ir = C->prm.irestr, ip = C->prm.iproln;
+  if (sch != 3 || C->prm.lsm || V.Lmax < 2 || ir < 1) return MF3D_OK;
+  const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
+  const int gtop = V.cc_g0 ? V.cc_g0 - 1 : V.Lmax;
+  if (gtop < 2) return MF3D_OK;
+  const int glast = V.cc_g0 ? V.cc_g0 : V.Lmax;  // deepest level a mid phase touches
+  const bool f64 = C->elem == 8;
+  if (!f64)
+    for (int g = 2; g <= glast; ++g)
+      if (g >= Lc) return MF3D_OK;  // an FP64 coarsest level among FP32 ones: the launch path
+  int occ = 0;
+  void (*kern)(const MidPhase *, int, const int *, MidBar *, int *) = f64 ? k_mid_cycle<double> : k_mid_cycle<float>;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, MID_THREADS, 0) != cudaSuccess || occ < 1) {
+    cudaGetLastError();
+    return MF3D_OK;
+  }
+  std::vector<MidPhase> down, up;
+  int st;
+  // a device list of blocks and its item prefix
+  auto make_list = [&](const std::vector<int> &blocks, const std::function<long long(int)> &items,
+                       const int *&lp, const long long *&pp, int &n, long long &total) -> int {
+    std::vector<long long> pre(1, 0);
+    for (int b : blocks) pre.push_back(pre.back() + items(b));
+    n = (int)blocks.size();
+    total = pre.back();
+    V.mid_lists.emplace_back();
+    V.mid_pres.emplace_back();
+    int r;
+    if ((r = V.mid_lists.back().upload(blocks, C->stream))) return r;
+    if ((r = V.mid_pres.back().upload(pre, C->stream))) return r;
+    lp = V.mid_lists.back().p;
+    pp = V.mid_pres.back().p;
+    return MF3D_OK;
+  };
+  auto add_sweeps = [&](std::vector<MidPhase> &out, int g, int q, int it, bool fz, bool red_done) -> int {
+    ViewLevel &L = V.lv[g];
+    if (!L.n_list[q] || it <= 0) return MF3D_OK;
+    MidPhase sw = {};
+    sw.kind = MID_SWEEP;
+    sw.tab = L.tab.p;
+    int r;
+    if ((r = make_list(L.hblk[q], [&](int b) { const BlkLev &B = L.htab[b]; return (long long)((B.nx + 1) / 2) * B.ny * B.nz; },
+                       sw.list, sw.pre, sw.nlist, sw.items)))
+      return r;
+    for (int itr = 0; itr < it; ++itr) {
+      const bool f = fz && itr == 0;
+      if (!(f && red_done)) {
+        MidPhase red = sw;
+        red.colour = 0;
+        red.fz = f ? 1 : 0;
+        out.push_back(red);
+      }
+      MidPhase black = sw;
+      black.colour = 1;
+      black.fz = 0;
+      out.push_back(black);
+      if (L.n_halo[q]) {
+        MidPhase h = {};
+        h.tab = L.tab.p;
+        h.seg = L.hseg[q].p;
+        h.nseg = L.n_hseg[q];
+        h.nstaged = L.n_staged[q];
+        h.items = L.n_halo[q];
+        h.buf = L.stage[q].p;
+        if (L.n_staged[q]) {
+          h.kind = MID_HALO_STAGE;
+          out.push_back(h);
+        }
+        h.kind = MID_HALO_APPLY;
+        out.push_back(h);
+      }
+    }
+    return MF3D_OK;
+  };
+  for (int g = 2; g <= gtop; ++g) {
+    if ((st = add_sweeps(down, g, SUB_A, ir, true, true))) return st;
+    if ((st = add_sweeps(down, g, SUB_C, ip, ir == 0, false))) return st;
+    if (g < V.Lmax && V.lv[g + 1].n_list[SUB_A]) {
+      ViewLevel &Cl = V.lv[g + 1];
+      MidPhase rs = {};
+      rs.kind = MID_RESTRICT;
+      rs.tab = V.lv[g].tab.p;
+      rs.tab2 = Cl.tab.p;
+      if ((st = make_list(Cl.hblk[SUB_A], [&](int b) { const BlkLev &B = Cl.htab[b]; return (long long)(B.nx + 2) * (B.ny + 2) * (B.nz + 2); },
+                          rs.list, rs.pre, rs.nlist, rs.items)))
+        return st;
+      down.push_back(rs);
+    }
+  }
+  for (int g = V.cc_g0 ? gtop : V.Lmax - 1; g >= 2; --g) {
+    ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
+    if (F.n_list[SUB_D]) {
+      MidPhase pr = {};
+      pr.kind = MID_PROLONG;
+      pr.tab = F.tab.p;
+      pr.tab2 = Cl.tab.p;
+      if ((st = make_list(F.hblk[SUB_D], [&](int b) { const BlkLev &B = Cl.htab[b]; return (long long)(B.nx + 1) * (B.ny + 1) * (B.nz + 1); },
+                          pr.list, pr.pre, pr.nlist, pr.items)))
+        return st;
+      up.push_back(pr);
+    }
+    if ((st = add_sweeps(up, g, SUB_D, ip, false, false))) return st;
+  }
+  for (const auto &ph : down)
+    if (ph.items >= (1LL << 31)) return MF3D_OK;
+  for (const auto &ph : up)
+    if (ph.items >= (1LL << 31)) return MF3D_OK;
+  if ((st = V.mid_down.upload(down, C->stream))) return st;
+  if ((st = V.mid_up.upload(up, C->stream))) return st;
+  if ((st = V.mid_bar.alloc(1))) return st;
+  CK(cudaMemsetAsync(V.mid_bar.p, 0, sizeof(MidBar), C->stream));
+  CK(cudaStreamSynchronize(C->stream));  // the host vectors are locals
+  V.n_mid_down = (int)down.size();
+  V.n_mid_up = (int)up.size();
+  V.mid_grid = C->nsm;
+  V.mid_on = V.n_mid_down > 0;
+  return MF3D_OK;
+}
+
 // Build the launch tables of a view over `doms` (all of one precision).
 static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &doms, int hcap) {
   cudaStream_t s = C->stream;
@@ -1505,6 +1665,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       if ((st = V.t_bcax[a].upload(tb, s))) return st;
     }
   if ((st = coarse_cycle_plan(C, V))) return st;
+  if ((st = mid_cycle_plan(C, V))) return st;
   V.fx_uvw = V.fx_p = V.fxe_sub = V.fxe_chain = nullptr;
   V.fxe_cells = nullptr;
   V.nfx_uvw = V.nsfx_uvw = V.nfx_p = V.nsfx_p = 0;
@@ -1682,9 +1843,11 @@ static void vcycle(mf3d_ctx *C, View &V) {
   // with red-black pre-smoothing the restriction also forms the coarse
   // level's first (from-zero) red half-sweep
   const bool red_in_restr = sch == 3 && ir > 0;
-  // levels cc_g0.. run as one cluster launch (k_coarse_cycle) where planned
+  // levels cc_g0.. run as one cluster launch (k_coarse_cycle) where planned,
+  // levels 2 .. cc_g0-1 (or the coarsest) as one cooperative launch per
+  // direction (k_mid_cycle) where planned
   const int gtop = V.cc_g0 ? V.cc_g0 - 1 : V.Lmax;
-  for (int g = 1; g <= gtop; ++g) {
+  for (int g = 1; g <= (V.mid_on ? 1 : gtop); ++g) {
     relax_g(g, SUB_A, ir, sch == 3, g > 1 && red_in_restr);  // a level starts from zero (pp = 0; mgrestr)
     relax_g(g, SUB_C, ip, sch == 3 && ir == 0);
     if (g < V.Lmax) {
@@ -1692,12 +1855,25 @@ static void vcycle(mf3d_ctx *C, View &V) {
       else restr<T, T>(C, V, g);
     }
   }
+  if (V.mid_on) {
+    // the barrier's count starts at 0 even after a launch that gave up waiting
+    cudaMemsetAsync(V.mid_bar.p, 0, sizeof(MidBar), C->stream);
+    launch_coop(k_mid_cycle<T>, V.mid_grid, MID_THREADS, 0, C->stream, (const MidPhase *)V.mid_down.p, V.n_mid_down,
+                (const int *)V.act.p, V.mid_bar.p, V.err.p);
+    ++C->launches;
+  }
   if (V.cc_g0) {
     launch_cl(k_coarse_cycle<T>, (int)V.blk.size(), CC_THREADS, V.cc_smem, C->stream, (int)V.blk.size(), V.cc_args,
               (const int *)V.act.p);
     ++C->launches;
   }
-  for (int g = gtop - (V.cc_g0 ? 0 : 1); g >= 1; --g) {
+  if (V.mid_on && V.n_mid_up) {
+    cudaMemsetAsync(V.mid_bar.p, 0, sizeof(MidBar), C->stream);
+    launch_coop(k_mid_cycle<T>, V.mid_grid, MID_THREADS, 0, C->stream, (const MidPhase *)V.mid_up.p, V.n_mid_up,
+                (const int *)V.act.p, V.mid_bar.p, V.err.p);
+    ++C->launches;
+  }
+  for (int g = V.mid_on ? 1 : gtop - (V.cc_g0 ? 0 : 1); g >= 1; --g) {
     if (g + 1 >= Lc) corr<T, double>(C, V, g);
     else corr<T, T>(C, V, g);
     relax_g(g, SUB_D, ip, false);
@@ -1953,7 +2129,9 @@ static int autotune_view(mf3d_ctx *C, View &V, bool time_new) {
   if (!autotune_enabled()) return MF3D_OK;
   if (C->prm.mg_itrsch == 2 && C->prm.lsm) return MF3D_OK;
   const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
-  const int gl = V.cc_g0 ? V.cc_g0 - 1 : V.Lmax;  // last level with its own sweeps
+  // last level with its own sweep launches (the middle-level launch and the
+  // coarse cluster compute per cell, untuned)
+  const int gl = V.mid_on ? 1 : V.cc_g0 ? V.cc_g0 - 1 : V.Lmax;
   int st;
   for (int g = 2; g <= std::min(gl + 1, V.Lmax); ++g)
     if ((st = autotune_restrict(C, V, g, time_new))) return st;
@@ -2355,6 +2533,10 @@ static int check_device_error(View &V) {
   if (e == ERR_WALL_LAW) {
     set_error("log_law: USTAR DOESNT CONVERGE (a smooth-wall law took 10 steps, log_law.for:47-62)");
     return MF3D_E_INVALID;
+  }
+  if (e == ERR_MID_BARRIER) {
+    set_error("a grid barrier of the middle-level V-cycle launch did not complete within its time limit");
+    return MF3D_E_TIMEOUT;
   }
   set_error("a device copy did not complete within its time limit (code " + std::to_string(e) + ")");
   return MF3D_E_TIMEOUT;

@@ -263,3 +263,26 @@ def test_corner_and_edge_ghosts(lib, oracle, cuda, layout):
             f[k] += 1e-3 * rng.standard_normal(f[k].shape)
     o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks)
     assert_same(o, g, pr.pl, pl_ex)
+
+
+@pytest.mark.parametrize("layout", ["2x2x2 blocks of 32^3, 4 levels", "2x1x1 blocks of 64x32x32, 5 levels, no cluster"])
+def test_middle_level_launch_matches_launch_path(lib, oracle, cuda, layout, monkeypatch):
+    """The middle levels as one cooperative launch per direction
+    (k_mid_cycle) against the launch-per-phase path (MF3D_MID_CYCLE=0) and
+    the oracle: bit for bit.  Without the coarse cluster launch
+    (MF3D_COARSE_CLUSTER=0) the middle launch runs down to the coarsest
+    level."""
+    if layout.startswith("2x2x2"):
+        pr = Problem(2, 2, 2, 32, 32, 32, ngrid=4, pl=2, stretch_y=1.5, dx=1 / 64, dy=1 / 64, dz=1 / 64)
+    else:
+        monkeypatch.setenv("MF3D_COARSE_CLUSTER", "0")
+        pr = Problem(2, 1, 1, 64, 32, 32, ngrid=5, pl=2)
+    prm = pr.params(mg_itrsch=3, maxcy=60, eps=1e-10)
+    blocks = pr.block_fields(seed=44, fourier_modes=2)
+    o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks)
+    assert_same(o, g, pr.pl)
+    monkeypatch.setenv("MF3D_MID_CYCLE", "0")
+    o2, g2 = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks)
+    for b in range(pr.nblocks):
+        for k in ("p", "u", "v", "w"):
+            assert np.array_equal(g[1][b][k], g2[1][b][k]), (b, k)
