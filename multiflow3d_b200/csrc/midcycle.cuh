@@ -93,6 +93,7 @@ __global__ void __launch_bounds__(MID_THREADS, 1) k_mid_cycle(const MidPhase *__
                                                                const int *__restrict__ act, MidBar *bar,
                                                                int *__restrict__ err) {
   pdl_wait();
+  if (*(volatile const int *)err) return;  // an earlier wait gave up: the call is failing already
   const long long stride = (long long)gridDim.x * blockDim.x;
   const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   for (int p = 0; p < nph; ++p) {
