@@ -2583,7 +2583,14 @@ static int solve_view(mf3d_ctx *C, View &V, const double *dt, const double *alfa
   long long iters_run = 0;
   if (maxcy > 0) {
     if (C->use_graph && C->prof_kind == 0) {
-      if ((st = build_graphs<T>(C, V))) return st;
+      if ((st = build_graphs<T>(C, V)) && V.mid_on) {
+        // a driver that does not capture the cooperative middle-level launch
+        // into the loop graph: the launch path instead
+        V.mid_on = false;
+        cudaGetLastError();
+        st = build_graphs<T>(C, V);
+      }
+      if (st) return st;
       CK(cudaGraphLaunch(V.x_loop, s));
     } else {
       std::vector<int> act(nd);
