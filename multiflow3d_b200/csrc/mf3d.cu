@@ -1437,10 +1437,15 @@ static int mid_cycle_plan(mf3d_ctx *C, View &V) {
     }
     if ((st = add_sweeps(up, g, SUB_D, ip, false, false))) return st;
   }
+  // the kernel splits item indices with 32-bit high multiplies: exact while
+  // a block's items times the divisor (a row or plane extent) stay below 2^32
   for (const auto &ph : down)
     if (ph.items >= (1LL << 31)) return MF3D_OK;
   for (const auto &ph : up)
     if (ph.items >= (1LL << 31)) return MF3D_OK;
+  for (int g = 2; g <= glast; ++g)
+    for (const BlkLev &B : V.lv[g].htab)
+      if ((long long)(B.nx + 2) * (B.ny + 2) * (B.nz + 2) * (std::max(B.nx, B.ny) + 2) >= (1LL << 32)) return MF3D_OK;
   if ((st = V.mid_down.upload(down, C->stream))) return st;
   if ((st = V.mid_up.upload(up, C->stream))) return st;
   if ((st = V.mid_bar.alloc(1))) return st;

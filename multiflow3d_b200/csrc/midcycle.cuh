@@ -88,33 +88,57 @@ __device__ __forceinline__ int mid_block(const long long *pre, int n, long long 
   return lo;
 }
 
+constexpr int MID_MAX_LIST = 64;  // listed blocks a phase keeps in shared memory (more: read from the table)
+
 template <typename T>
 __global__ void __launch_bounds__(MID_THREADS, 1) k_mid_cycle(const MidPhase *__restrict__ phases, int nph,
                                                                const int *__restrict__ act, MidBar *bar,
                                                                int *__restrict__ err) {
   pdl_wait();
   if (*(volatile const int *)err) return;  // an earlier wait gave up: the call is failing already
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // the phase's listed blocks: fine (and coarse) descriptors, item prefix
+  __shared__ BlkLev sf[MID_MAX_LIST], sc[MID_MAX_LIST];
+  __shared__ long long spre[MID_MAX_LIST + 1];
+  const unsigned stride = gridDim.x * blockDim.x;
+  const unsigned t0 = blockIdx.x * blockDim.x + threadIdx.x;
   for (int p = 0; p < nph; ++p) {
     const MidPhase P = phases[p];
+    const bool listed = P.kind == MID_SWEEP || P.kind == MID_RESTRICT || P.kind == MID_PROLONG;
+    const bool cached = listed && P.nlist <= MID_MAX_LIST;
+    if (cached) {
+      for (int i = threadIdx.x; i < P.nlist; i += blockDim.x) {
+        sf[i] = P.tab[P.list[i]];
+        if (P.kind != MID_SWEEP) sc[i] = P.tab2[P.list[i]];
+      }
+      for (int i = threadIdx.x; i <= P.nlist; i += blockDim.x) spre[i] = P.pre[i];
+      __syncthreads();
+    }
+    auto find = [&](unsigned t) -> int {
+      const long long *pre = cached ? spre : P.pre;
+      int lo = 0, hi = P.nlist - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= (long long)t) lo = mid;
+        else hi = mid - 1;
+      }
+      return lo;
+    };
     if (P.kind == MID_SWEEP) {
-      for (long long t = t0; t < P.items; t += stride) {
-        const int li = mid_block(P.pre, P.nlist, t);
-        const BlkLev B = P.tab[P.list[li]];
+      for (unsigned t = t0; t < (unsigned long long)P.items; t += stride) {
+        const int li = find(t);
+        const BlkLev B = cached ? sf[li] : P.tab[P.list[li]];
         if (!act[B.dom]) continue;
-        const int Q = (B.nx + 1) / 2;
-        long long r = t - P.pre[li];
-        const int q = (int)(r % Q);
-        r /= Q;
-        const int j = (int)(r % B.ny) + 1, k = (int)(r / B.ny) + 1;
+        const unsigned Q = (unsigned)((B.nx + 1) / 2);
+        const unsigned r0 = t - (unsigned)(cached ? spre[li] : P.pre[li]);
+        const unsigned r = FastDiv(Q).div(r0), kk = FastDiv((unsigned)B.ny).div(r);
+        const int q = (int)(r0 - r * Q), j = (int)(r - kk * (unsigned)B.ny) + 1, k = (int)kk + 1;
         const Coef<T> cf(B);
         if (P.fz) sweep_cell<T, true>(B, cf, phi_of<T>(B), rhs_of<T>(B), P.colour, q, j, k);
         else sweep_cell<T, false>(B, cf, phi_of<T>(B), rhs_of<T>(B), P.colour, q, j, k);
       }
     } else if (P.kind == MID_HALO_STAGE) {
       T *buf = (T *)P.buf;
-      for (long long t = t0; t < P.nstaged; t += stride) {
+      for (unsigned t = t0; t < (unsigned long long)P.nstaged; t += stride) {
         const HaloSeg &S = P.seg[halo_segment<true>(P.seg, P.nseg, t)];
         if (!act[S.dom]) continue;
         const HaloCopy c = S.pairs[t - S.sstart];
@@ -122,7 +146,7 @@ __global__ void __launch_bounds__(MID_THREADS, 1) k_mid_cycle(const MidPhase *__
       }
     } else if (P.kind == MID_HALO_APPLY) {
       const T *buf = (const T *)P.buf;
-      for (long long t = t0; t < P.items; t += stride) {
+      for (unsigned t = t0; t < (unsigned long long)P.items; t += stride) {
         const HaloSeg &S = P.seg[halo_segment<false>(P.seg, P.nseg, t)];
         if (!act[S.dom]) continue;
         const long long u = t - S.start;
@@ -130,31 +154,25 @@ __global__ void __launch_bounds__(MID_THREADS, 1) k_mid_cycle(const MidPhase *__
         const T v = u < S.nstaged ? buf[S.sstart + u] : phi_of<T>(P.tab[S.blk_base + c.sblk])[c.soff];
         phi_of<T>(P.tab[S.blk_base + c.dblk])[c.doff] = v;
       }
-    } else if (P.kind == MID_RESTRICT) {
-      for (long long t = t0; t < P.items; t += stride) {
-        const int li = mid_block(P.pre, P.nlist, t);
-        const int b = P.list[li];
-        const BlkLev Fb = P.tab[b], Cb = P.tab2[b];
+    } else {  // MID_RESTRICT, MID_PROLONG
+      const int add = P.kind == MID_RESTRICT ? 2 : 1;  // coarse ghost-inclusive cells / fine groups
+      for (unsigned t = t0; t < (unsigned long long)P.items; t += stride) {
+        const int li = find(t);
+        const BlkLev Fb = cached ? sf[li] : P.tab[P.list[li]];
+        const BlkLev Cb = cached ? sc[li] : P.tab2[P.list[li]];
         if (!act[Cb.dom]) continue;
-        const int GX = Cb.nx + 2, GY = Cb.ny + 2;
-        const long long r = t - P.pre[li];
-        const int I = (int)(r % GX), J = (int)((r / GX) % GY), K = (int)(r / ((long long)GX * GY));
-        restrict_cell<T, T>(Fb, Coef<T>(Fb), phi_of<T>(Fb), rhs_of<T>(Fb), Cb, Coef<T>(Cb), phi_of<T>(Cb),
-                            rhs_of<T>(Cb), I, J, K);
-      }
-    } else {  // MID_PROLONG
-      for (long long t = t0; t < P.items; t += stride) {
-        const int li = mid_block(P.pre, P.nlist, t);
-        const int b = P.list[li];
-        const BlkLev Fb = P.tab[b], Cb = P.tab2[b];
-        if (!act[Fb.dom]) continue;
-        const int GX = Cb.nx + 1, GY = Cb.ny + 1;
-        const long long r = t - P.pre[li];
-        const int I = (int)(r % GX), J = (int)((r / GX) % GY), K = (int)(r / ((long long)GX * GY));
-        prolong_group<T, T>(Fb, phi_of<T>(Fb), Cb, phi_of<T>(Cb), I, J, K);
+        const unsigned GX = (unsigned)(Cb.nx + add), GY = (unsigned)(Cb.ny + add);
+        const unsigned r0 = t - (unsigned)(cached ? spre[li] : P.pre[li]);
+        const unsigned r = FastDiv(GX).div(r0), K = FastDiv(GY).div(r);
+        const int I = (int)(r0 - r * GX), J = (int)(r - K * GY);
+        if (P.kind == MID_RESTRICT)
+          restrict_cell<T, T>(Fb, Coef<T>(Fb), phi_of<T>(Fb), rhs_of<T>(Fb), Cb, Coef<T>(Cb), phi_of<T>(Cb),
+                              rhs_of<T>(Cb), I, J, (int)K);
+        else
+          prolong_group<T, T>(Fb, phi_of<T>(Fb), Cb, phi_of<T>(Cb), I, J, (int)K);
       }
     }
-    if (p + 1 < nph && !mid_barrier(bar, err)) return;
+    if (p + 1 < nph && !mid_barrier(bar, err)) return;  // (its __syncthreads also frees sf, sc, spre)
   }
 }
 
