@@ -39,6 +39,7 @@ struct CcHalo {
 // than 1/d to t/d).
 struct FastDiv {
   unsigned d, m;
+  FastDiv() = default;
   __device__ explicit FastDiv(unsigned d_) : d(d_), m(d_ > 1 ? 0xffffffffu / d_ + 1u : 0u) {}
   __device__ __forceinline__ unsigned div(unsigned t) const { return d > 1 ? __umulhi(t, m) : t; }
 };

@@ -1440,9 +1440,9 @@ static int mid_cycle_plan(mf3d_ctx *C, View &V) {
   // the kernel splits item indices with 32-bit high multiplies: exact while
   // a block's items times the divisor (a row or plane extent) stay below 2^32
   for (const auto &ph : down)
-    if (ph.items >= (1LL << 31)) return MF3D_OK;
+    if (ph.items >= (1LL << 31) || ph.nlist > MID_MAX_LIST) return MF3D_OK;
   for (const auto &ph : up)
-    if (ph.items >= (1LL << 31)) return MF3D_OK;
+    if (ph.items >= (1LL << 31) || ph.nlist > MID_MAX_LIST) return MF3D_OK;
   for (int g = 2; g <= glast; ++g)
     for (const BlkLev &B : V.lv[g].htab)
       if ((long long)(B.nx + 2) * (B.ny + 2) * (B.nz + 2) * (std::max(B.nx, B.ny) + 2) >= (1LL << 32)) return MF3D_OK;
@@ -1453,7 +1453,7 @@ static int mid_cycle_plan(mf3d_ctx *C, View &V) {
   CK(cudaStreamSynchronize(C->stream));  // the host vectors are locals
   V.n_mid_down = (int)down.size();
   V.n_mid_up = (int)up.size();
-  V.mid_grid = C->nsm;
+  V.mid_grid = C->nsm * std::min(occ, MID_CTAS_PER_SM);
   V.mid_on = V.n_mid_down > 0;
   return MF3D_OK;
 }

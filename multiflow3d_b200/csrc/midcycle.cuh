@@ -43,8 +43,8 @@ struct MidBar {
   unsigned count, gen;
 };
 
-constexpr int MID_THREADS = 512;
-constexpr long long kMidSpinLimit = 1LL << 26;  // polls before a barrier gives up (a few seconds)
+constexpr int MID_THREADS = 384;
+constexpr long long kMidSpinLimit = 1LL << 25;  // polls before a barrier gives up (a few seconds)
 
 // All CTAs of the (co-resident) grid.  A CTA that waits past the poll limit
 // records ERR_MID_BARRIER and leaves with the others' work unsynchronised:
@@ -62,13 +62,12 @@ __device__ __forceinline__ bool mid_barrier(MidBar *bar, int *err) {
       atomicAdd(&bar->gen, 1u);
     } else {
       long long spins = 0;
-      while (*(volatile unsigned *)&bar->gen == gen) {
+      while (*(volatile unsigned *)&bar->gen == gen) {  // an L2 round trip per poll
         if (++spins > kMidSpinLimit) {
           atomicExch(err, ERR_MID_BARRIER);
           ok_s = 0;
           break;
         }
-        __nanosleep(64);
       }
     }
     __threadfence();
@@ -88,83 +87,92 @@ __device__ __forceinline__ int mid_block(const long long *pre, int n, long long 
   return lo;
 }
 
-constexpr int MID_MAX_LIST = 64;  // listed blocks a phase keeps in shared memory (more: read from the table)
+constexpr int MID_MAX_LIST = 64;   // listed blocks of a phase (the plan keeps to it)
+constexpr int MID_CTAS_PER_SM = 2;
 
 template <typename T>
-__global__ void __launch_bounds__(MID_THREADS, 1) k_mid_cycle(const MidPhase *__restrict__ phases, int nph,
-                                                               const int *__restrict__ act, MidBar *bar,
-                                                               int *__restrict__ err) {
+__global__ void __launch_bounds__(MID_THREADS, MID_CTAS_PER_SM) k_mid_cycle(const MidPhase *__restrict__ phases,
+                                                                             int nph, const int *__restrict__ act,
+                                                                             MidBar *bar, int *__restrict__ err) {
   pdl_wait();
   if (*(volatile const int *)err) return;  // an earlier wait gave up: the call is failing already
-  // the phase's listed blocks: fine (and coarse) descriptors, item prefix
+  // the phase's listed blocks: fine (and coarse) descriptors, item prefix,
+  // the divisors that split a block's item index
   __shared__ BlkLev sf[MID_MAX_LIST], sc[MID_MAX_LIST];
-  __shared__ long long spre[MID_MAX_LIST + 1];
-  const unsigned stride = gridDim.x * blockDim.x;
-  const unsigned t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ unsigned spre[MID_MAX_LIST + 1];
+  __shared__ FastDiv sd1[MID_MAX_LIST], sd2[MID_MAX_LIST];
+  __shared__ unsigned sn1[MID_MAX_LIST], sn2[MID_MAX_LIST];
   for (int p = 0; p < nph; ++p) {
     const MidPhase P = phases[p];
     const bool listed = P.kind == MID_SWEEP || P.kind == MID_RESTRICT || P.kind == MID_PROLONG;
-    const bool cached = listed && P.nlist <= MID_MAX_LIST;
-    if (cached) {
+    const unsigned items = (unsigned)(P.kind == MID_HALO_STAGE ? P.nstaged : P.items);
+    if (listed) {
       for (int i = threadIdx.x; i < P.nlist; i += blockDim.x) {
-        sf[i] = P.tab[P.list[i]];
-        if (P.kind != MID_SWEEP) sc[i] = P.tab2[P.list[i]];
+        const BlkLev F = P.tab[P.list[i]];
+        sf[i] = F;
+        unsigned d1, d2;
+        if (P.kind == MID_SWEEP) {
+          d1 = (unsigned)((F.nx + 1) / 2);
+          d2 = (unsigned)F.ny;
+        } else {
+          const BlkLev Cb = P.tab2[P.list[i]];
+          sc[i] = Cb;
+          const int add = P.kind == MID_RESTRICT ? 2 : 1;  // coarse ghost-inclusive cells / fine groups
+          d1 = (unsigned)(Cb.nx + add);
+          d2 = (unsigned)(Cb.ny + add);
+        }
+        sd1[i] = FastDiv(d1);
+        sd2[i] = FastDiv(d2);
+        sn1[i] = d1;
+        sn2[i] = d2;
       }
-      for (int i = threadIdx.x; i <= P.nlist; i += blockDim.x) spre[i] = P.pre[i];
+      for (int i = threadIdx.x; i <= P.nlist; i += blockDim.x) spre[i] = (unsigned)P.pre[i];
       __syncthreads();
     }
-    auto find = [&](unsigned t) -> int {
-      const long long *pre = cached ? spre : P.pre;
-      int lo = 0, hi = P.nlist - 1;
+    // each CTA a contiguous chunk of the phase's items, its threads striding
+    // through it: a thread's block changes at most a few times per phase
+    const unsigned chunk = (items + gridDim.x - 1) / gridDim.x;
+    const unsigned c0 = blockIdx.x * chunk, c1 = min(items, c0 + chunk);
+    int li = 0;
+    if (listed && c0 < c1) {
+      int lo = 0, hi = P.nlist - 1;  // last listed block whose first item <= c0
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (pre[mid] <= (long long)t) lo = mid;
+        if (spre[mid] <= c0) lo = mid;
         else hi = mid - 1;
       }
-      return lo;
-    };
-    if (P.kind == MID_SWEEP) {
-      for (unsigned t = t0; t < (unsigned long long)P.items; t += stride) {
-        const int li = find(t);
-        const BlkLev B = cached ? sf[li] : P.tab[P.list[li]];
+      li = lo;
+    }
+    for (unsigned t = c0 + threadIdx.x; t < c1; t += blockDim.x) {
+      if (listed)
+        while (t >= spre[li + 1]) ++li;
+      if (P.kind == MID_SWEEP) {
+        const BlkLev &B = sf[li];
         if (!act[B.dom]) continue;
-        const unsigned Q = (unsigned)((B.nx + 1) / 2);
-        const unsigned r0 = t - (unsigned)(cached ? spre[li] : P.pre[li]);
-        const unsigned r = FastDiv(Q).div(r0), kk = FastDiv((unsigned)B.ny).div(r);
-        const int q = (int)(r0 - r * Q), j = (int)(r - kk * (unsigned)B.ny) + 1, k = (int)kk + 1;
+        const unsigned r0 = t - spre[li];
+        const unsigned r = sd1[li].div(r0), kk = sd2[li].div(r);
+        const int q = (int)(r0 - r * sn1[li]), j = (int)(r - kk * sn2[li]) + 1, k = (int)kk + 1;
         const Coef<T> cf(B);
         if (P.fz) sweep_cell<T, true>(B, cf, phi_of<T>(B), rhs_of<T>(B), P.colour, q, j, k);
         else sweep_cell<T, false>(B, cf, phi_of<T>(B), rhs_of<T>(B), P.colour, q, j, k);
-      }
-    } else if (P.kind == MID_HALO_STAGE) {
-      T *buf = (T *)P.buf;
-      for (unsigned t = t0; t < (unsigned long long)P.nstaged; t += stride) {
+      } else if (P.kind == MID_HALO_STAGE) {
         const HaloSeg &S = P.seg[halo_segment<true>(P.seg, P.nseg, t)];
         if (!act[S.dom]) continue;
         const HaloCopy c = S.pairs[t - S.sstart];
-        buf[t] = phi_of<T>(P.tab[S.blk_base + c.sblk])[c.soff];
-      }
-    } else if (P.kind == MID_HALO_APPLY) {
-      const T *buf = (const T *)P.buf;
-      for (unsigned t = t0; t < (unsigned long long)P.items; t += stride) {
+        ((T *)P.buf)[t] = phi_of<T>(P.tab[S.blk_base + c.sblk])[c.soff];
+      } else if (P.kind == MID_HALO_APPLY) {
         const HaloSeg &S = P.seg[halo_segment<false>(P.seg, P.nseg, t)];
         if (!act[S.dom]) continue;
         const long long u = t - S.start;
         const HaloCopy c = S.pairs[u];
-        const T v = u < S.nstaged ? buf[S.sstart + u] : phi_of<T>(P.tab[S.blk_base + c.sblk])[c.soff];
+        const T v = u < S.nstaged ? ((const T *)P.buf)[S.sstart + u] : phi_of<T>(P.tab[S.blk_base + c.sblk])[c.soff];
         phi_of<T>(P.tab[S.blk_base + c.dblk])[c.doff] = v;
-      }
-    } else {  // MID_RESTRICT, MID_PROLONG
-      const int add = P.kind == MID_RESTRICT ? 2 : 1;  // coarse ghost-inclusive cells / fine groups
-      for (unsigned t = t0; t < (unsigned long long)P.items; t += stride) {
-        const int li = find(t);
-        const BlkLev Fb = cached ? sf[li] : P.tab[P.list[li]];
-        const BlkLev Cb = cached ? sc[li] : P.tab2[P.list[li]];
+      } else {  // MID_RESTRICT, MID_PROLONG
+        const BlkLev &Fb = sf[li], &Cb = sc[li];
         if (!act[Cb.dom]) continue;
-        const unsigned GX = (unsigned)(Cb.nx + add), GY = (unsigned)(Cb.ny + add);
-        const unsigned r0 = t - (unsigned)(cached ? spre[li] : P.pre[li]);
-        const unsigned r = FastDiv(GX).div(r0), K = FastDiv(GY).div(r);
-        const int I = (int)(r0 - r * GX), J = (int)(r - K * GY);
+        const unsigned r0 = t - spre[li];
+        const unsigned r = sd1[li].div(r0), K = sd2[li].div(r);
+        const int I = (int)(r0 - r * sn1[li]), J = (int)(r - K * sn2[li]);
         if (P.kind == MID_RESTRICT)
           restrict_cell<T, T>(Fb, Coef<T>(Fb), phi_of<T>(Fb), rhs_of<T>(Fb), Cb, Coef<T>(Cb), phi_of<T>(Cb),
                               rhs_of<T>(Cb), I, J, (int)K);
@@ -172,7 +180,7 @@ __global__ void __launch_bounds__(MID_THREADS, 1) k_mid_cycle(const MidPhase *__
           prolong_group<T, T>(Fb, phi_of<T>(Fb), Cb, phi_of<T>(Cb), I, J, (int)K);
       }
     }
-    if (p + 1 < nph && !mid_barrier(bar, err)) return;  // (its __syncthreads also frees sf, sc, spre)
+    if (p + 1 < nph && !mid_barrier(bar, err)) return;  // (its __syncthreads also frees the shared tables)
   }
 }
 
