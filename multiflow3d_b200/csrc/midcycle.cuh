@@ -43,7 +43,7 @@ struct MidBar {
   unsigned count, gen;
 };
 
-constexpr int MID_THREADS = 384;
+constexpr int MID_THREADS = 512;
 constexpr long long kMidSpinLimit = 1LL << 25;  // polls before a barrier gives up (a few seconds)
 
 // All CTAs of the (co-resident) grid.  A CTA that waits past the poll limit
@@ -88,7 +88,7 @@ __device__ __forceinline__ int mid_block(const long long *pre, int n, long long 
 }
 
 constexpr int MID_MAX_LIST = 64;   // listed blocks of a phase (the plan keeps to it)
-constexpr int MID_CTAS_PER_SM = 2;
+constexpr int MID_CTAS_PER_SM = 1;
 
 template <typename T>
 __global__ void __launch_bounds__(MID_THREADS, MID_CTAS_PER_SM) k_mid_cycle(const MidPhase *__restrict__ phases,

@@ -268,7 +268,7 @@ def test_corner_and_edge_ghosts(lib, oracle, cuda, layout):
 @pytest.mark.parametrize("layout", ["2x2x2 blocks of 32^3, 4 levels", "2x1x1 blocks of 64x32x32, 5 levels, no cluster"])
 def test_middle_level_launch_matches_launch_path(lib, oracle, cuda, layout, monkeypatch):
     """The middle levels as one cooperative launch per direction
-    (k_mid_cycle) against the launch-per-phase path (MF3D_MID_CYCLE=0) and
+    (k_mid_cycle, MF3D_MID_CYCLE=1) against the launch-per-phase path and
     the oracle: bit for bit.  Without the coarse cluster launch
     (MF3D_COARSE_CLUSTER=0) the middle launch runs down to the coarsest
     level."""
@@ -279,6 +279,7 @@ def test_middle_level_launch_matches_launch_path(lib, oracle, cuda, layout, monk
         pr = Problem(2, 1, 1, 64, 32, 32, ngrid=5, pl=2)
     prm = pr.params(mg_itrsch=3, maxcy=60, eps=1e-10)
     blocks = pr.block_fields(seed=44, fourier_modes=2)
+    monkeypatch.setenv("MF3D_MID_CYCLE", "1")
     o, g = run_both(lib, oracle, cuda, pr.descriptors(lib), pr.descriptors(oracle), pr.nblocks, prm, blocks)
     assert_same(o, g, pr.pl)
     monkeypatch.setenv("MF3D_MID_CYCLE", "0")
