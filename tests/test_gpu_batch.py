@@ -83,3 +83,41 @@ def test_batch_config4_shapes_converge(lib, cuda):
     assert len(conv) >= 0.9 * len(res), [(r.status, r.iter) for r in res]
     for r in conv:
         assert r.rmax < 1e-8 * r.rmax0
+
+
+def test_autotuned_batch_equals_untuned(lib, cuda, monkeypatch):
+    """A config-4 style batch (16 uneven domains, edges 32-96, FP64 red-black)
+    with the autotuner's launch shapes and with the defaults
+    (MF3D_AUTOTUNE=0): the same values bit for bit (every candidate computes
+    the same arithmetic), and the tuned batch no slower than the untuned one
+    beyond timing noise."""
+    import time
+    import torch
+    doms = make_domains(16, seed=9, lo=32, hi=96)
+    prm = doms[0].params(mg_itrsch=3, maxcy=60, eps=1e-10, precision=MF3D_PREC_FP64)
+    prm.ngrid = 1
+
+    def run():
+        batch = Batch([domain_desc(pr) for pr in doms], prm, lib)
+        fields = [dev_fields(pr, 70 + i, cuda)[0] for i, pr in enumerate(doms)]
+        batch.solve_device([{k: v.clone() for k, v in f.items()} for f in fields])  # warm: graph capture
+        best = None
+        for _ in range(3):
+            f2 = [{k: v.clone() for k, v in f.items()} for f in fields]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res, st = batch.solve_device(f2)
+            torch.cuda.synchronize()
+            best = min(best or 1e30, time.perf_counter() - t0)
+        batch.close()
+        return res, f2, best
+
+    res_t, f_t, t_tuned = run()
+    monkeypatch.setenv("MF3D_AUTOTUNE", "0")
+    res_u, f_u, t_untuned = run()
+    for a, b in zip(res_t, res_u):
+        assert a.status == b.status and a.iter == b.iter and np.array_equal(a.history, b.history)
+    for a, b in zip(f_t, f_u):
+        for k in ("p", "u", "v", "w"):
+            assert torch.equal(a[k], b[k]), k
+    assert t_tuned <= 1.25 * t_untuned, (t_tuned, t_untuned)
