@@ -20,10 +20,20 @@
  *     aw, ae, as, an, ab, at, ap, rhs (mgsolver.for:20-38, 112-210);
  *   - fields p, u, v, w, ustar, ... as Fortran (ttc_i,ttc_j,ttc_k) arrays,
  *     i fastest, pl ghost layers (initial.for:196-210).
- * Only the same-level branches (rdiv = 1 everywhere, single MPI rank owning
- * every block, the `dom_ad(a) .eq. dom_ad(b)` direct-buffer path) are
- * restated, with the L_LSM variable-density branches of coeff, calvel and
- * calmas; the LMR 2:1 branches are not.
+ * The single-rank branches (one MPI rank owning every block, the
+ * `dom_ad(a) .eq. dom_ad(b)` direct-buffer path) are restated, with the
+ * L_LSM variable-density branches of coeff, calvel and calmas.  The LMR 2:1
+ * branches are restated for the multigrid V-cycle (mgkcyc): the per-block
+ * level clamping of localparameters.for:26-75 and mgsolver.for, and the
+ * fine/coarse cases of exchangepp.  The outer loop's field exchanges at
+ * refinement interfaces (exchangep.for, exchangeu/v/w.for) are not, so
+ * orc_newsolv_mg refuses an LMR layout.  The LMR unpack of a fine block's
+ * face reads entries of its receive buffer that the coarse sender never
+ * writes (the ring s = 1, ns1 or t = 1, ns2; exchangepp.for:4036-4060):
+ * the reference leaves there whatever an earlier exchange of any field put
+ * in the shared buffer.  Here every pack starts from a buffer holding one
+ * value, g_lmr_ring (0 by default, orc_set_lmr_ring), so that the cells
+ * that depend on those entries can be found by changing it.
  *
  * Extension with no reference counterpart (marked EXT): non-uniform cell
  * widths.  With uniform widths every EXT formula reduces bit-for-bit to the
@@ -49,6 +59,8 @@ namespace {
 struct Blk {
   mf3d_block_desc d;
   int ngrid;
+  int rdiv = 1;                /* LMR refinement (localparameters.for:100-102) */
+  std::vector<int> rdv;        /* rdv(dom, g), g = 1..ngrd_gl (localparameters.for:39-57) */
   int isp, iep, jsp, jep, ksp, kep;
   int isu, ieu, jsu, jeu, ksu, keu;
   int isv, iev, jsv, jev, ksv, kev;
@@ -112,6 +124,7 @@ struct Ctx {
   bool periodic;
   double dt, alfapr, rmax;
   double yst, yen, zst, zen; /* extents of the whole domain (alloc_dom.for:427-439) */
+  bool lmr = false;          /* blocks of different refinement */
 };
 
 /* The inlet files of the west codes 7 (Inlet/Inlet_<dom>_<n>.dat: u per
@@ -130,6 +143,7 @@ std::vector<std::array<const double *, 3>> g_old;
 double g_re = 0.0, g_fric = 0.0;
 bool g_wall_fail = false; /* a smooth-wall law did not converge */
 std::string g_err;        /* the last error (orc_last_error) */
+double g_lmr_ring = 0.0;  /* LMR: the receive-buffer entries no sender writes */
 
 inline double &F(Blk &B, double *a, int i, int j, int k) {
   return a[(size_t)(i - 1) + (size_t)B.ttc_i * ((size_t)(j - 1) + (size_t)B.ttc_j * (size_t)(k - 1))];
@@ -414,7 +428,209 @@ void exchbc_mgpp(Ctx &C, int g) {
 /* unpacks: prev face, next face, then prev corners 1-4, prev edges    */
 /* 1-6, next corners 1-4, next edges 1-6.  Then mgbound, exchbc_mgpp.   */
 /* ------------------------------------------------------------------ */
+/* ------------------------------------------------------------------ */
+/* exchangepp with LMR (exchangepp.for:43-4763), single-rank branches:  */
+/* per sync_dir every block packs into its neighbours' receive buffers  */
+/* by the three cases of rdv(me, g) against rdv(neighbour, g), then     */
+/* every block unpacks.  Equal: the copies above.  Sender finer: the    */
+/* 8-cell average of the two layers next to the receiver (faces         */
+/* 0.125*(...) with the tangential axes in buffer order before the      */
+/* normal, exchangepp.for:163-172; corners and edges (...)/8.0 in j, i, */
+/* k order, :448-452, :652-656).  Sender coarser: a face cell goes to   */
+/* the four fine buffer entries as 2*phi (:174-187), a corner or edge   */
+/* cell as the trilinear (27, 9, 9, 3, 9, 3, 3, 1)/64 blend toward the  */
+/* receiver (:454-460, :658-669).  Unpack: a finer receiver takes       */
+/* (recv + 3 phi(1 in) - phi(2 in))/4 on its whole face plane           */
+/* (:4046-4056), a coarser one copies the interior of the plane         */
+/* (:4057-4063), corners and edges are copies (:4433-4755).             */
+/* ------------------------------------------------------------------ */
+/* cell of the face plane of sync_dir sd: a along the normal, (s, t) the
+ * buffer's axes (ijk = (t-1)*ns1 + s): sd 1 (j, k), sd 2 (i, k), sd 3 (j, i) */
+inline long face_cell(const Lev &L, int sd, int a, int s, int t) {
+  if (sd == 1) return PH(L, a, s, t);
+  if (sd == 2) return PH(L, s, a, t);
+  return PH(L, t, s, a);
+}
+/* the interior index along an axis next to a neighbour in direction e
+ * (-1: the low side, 2; +1: the high side, n-1) and the first of the two
+ * layers next to it (2 or n-2) */
+inline int near_cell(int e, int n) { return e < 0 ? 2 : n - 1; }
+inline int near_pair(int e, int n) { return e < 0 ? 2 : n - 2; }
+
+void exchangepp_lmr(Ctx &C, int g) {
+  for (int sd = 1; sd <= 3; ++sd) {
+    /* pack */
+    for (auto &B : C.b) {
+      Lev L = lev(C, B, g);
+      double *fi = B.cof.data();
+      const int ni = L.ni, nj = L.nj, nk = L.nk, nij = L.nij;
+      const int nn3[3] = {ni, nj, nk};
+      const int cprev = sd == 1 ? B.d.iprev : sd == 2 ? B.d.jprev : B.d.kprev;
+      const int cnext = sd == 1 ? B.d.inext : sd == 2 ? B.d.jnext : B.d.knext;
+      const int ns1 = sd == 2 ? ni : nj, ns2 = sd == 1 ? nk : sd == 2 ? nk : ni;
+      const int nd = sd == 1 ? ni : sd == 2 ? nj : nk;
+      const int me = B.rdv[g];
+      /* coarsened counts of a finer sender (exchangepp.for:63-72) */
+      auto coarse_n = [&](int n) { return B.rdiv == 1 ? n : (n - 2) / 2 + 2; };
+      const int nsc1 = coarse_n(ns1), nsc2 = coarse_n(ns2);
+      const int nsr1 = 2 * (ns1 - 2) + 2, nsr2 = 2 * (ns2 - 2) + 2;
+      auto pack_face = [&](Blk &N, std::vector<double> &R, bool prev) {
+        const int nb_ = N.rdv[g];
+        if (me == nb_) {
+          R.assign((size_t)ns1 * ns2 + 1, g_lmr_ring);
+          const int a = prev ? 2 : nd - 1;
+          for (int t = 1; t <= ns2; ++t) for (int s = 1; s <= ns1; ++s)
+            R[(size_t)(t - 1) * ns1 + s] = fi[face_cell(L, sd, a, s, t)];
+        } else if (me > nb_) {
+          R.assign((size_t)nsc1 * nsc2 + 1, g_lmr_ring);
+          const int a = prev ? 2 : nd - 2;
+          for (int t = 2; t <= nsc2 - 1; ++t) for (int s = 2; s <= nsc1 - 1; ++s) {
+            const int s0 = 2 * s - 2, t0 = 2 * t - 2;
+            R[(size_t)(t - 1) * nsc1 + s] =
+                0.125 * (fi[face_cell(L, sd, a, s0, t0)] + fi[face_cell(L, sd, a, s0 + 1, t0)] +
+                         fi[face_cell(L, sd, a, s0, t0 + 1)] + fi[face_cell(L, sd, a, s0 + 1, t0 + 1)] +
+                         fi[face_cell(L, sd, a + 1, s0, t0)] + fi[face_cell(L, sd, a + 1, s0 + 1, t0)] +
+                         fi[face_cell(L, sd, a + 1, s0, t0 + 1)] + fi[face_cell(L, sd, a + 1, s0 + 1, t0 + 1)]);
+          }
+        } else {
+          R.assign((size_t)nsr1 * nsr2 + 1, g_lmr_ring);
+          const int a = prev ? 2 : nd - 1;
+          for (int tc = 2; tc <= ns2 - 1; ++tc) for (int sc = 2; sc <= ns1 - 1; ++sc) {
+            const double v = 2.0 * fi[face_cell(L, sd, a, sc, tc)];
+            for (int dt = 0; dt < 2; ++dt) for (int ds = 0; ds < 2; ++ds)
+              R[(size_t)(2 * tc - 2 + dt - 1) * nsr1 + (2 * sc - 2 + ds)] = v;
+          }
+        }
+      };
+      if (cprev >= 0) { Blk &N = C.b[C.indid.at(cprev)]; pack_face(N, N.recvb_p1, true); }
+      if (cnext >= 0) { Blk &N = C.b[C.indid.at(cnext)]; pack_face(N, N.recvb_m1, false); }
+      if (sd != 3) continue;
+      /* the value sent toward a corner or edge neighbour N in direction e
+       * (e[a] = 0 along an edge's axis, where q is the index along it) */
+      auto avg8 = [&](int i0, int j0, int k0) {
+        const long l = PH(L, i0, j0, k0);
+        return (fi[l] + fi[l + 1] + fi[l + nj] + fi[l + 1 + nj] + fi[l + nij] + fi[l + 1 + nij] + fi[l + nj + nij] +
+                fi[l + 1 + nj + nij]) / 8.0;
+      };
+      auto tri = [&](int i, int j, int k, int ei, int ej, int ek) {
+        const long l = PH(L, i, j, k);
+        const long dj = ej, di = (long)ei * nj, dk = (long)ek * nij;
+        return (27.0 * fi[l] + 9.0 * fi[l + dj] + 9.0 * fi[l + di] + 3.0 * fi[l + di + dj] + 9.0 * fi[l + dk] +
+                3.0 * fi[l + dj + dk] + 3.0 * fi[l + di + dk] + 1.0 * fi[l + di + dj + dk]) / 64.0;
+      };
+      /* corners (exchangepp.for:439-633, 1387-1580): prev #1..4 at z-1,
+       * next #1..4 at z+1 */
+      const int cpx[4] = {-1, -1, +1, +1}, cpy[4] = {-1, +1, +1, -1};
+      const int cnx[4] = {+1, +1, -1, -1}, cny[4] = {+1, -1, -1, +1};
+      for (int side = 0; side < 2; ++side)
+        for (int q = 0; q < 4; ++q) {
+          const int id = side ? B.d.cornext[q] : B.d.corprev[q];
+          if (id < 0) continue;
+          Blk &N = C.b[C.indid.at(id)];
+          const int e[3] = {side ? cnx[q] : cpx[q], side ? cny[q] : cpy[q], side ? +1 : -1};
+          double v;
+          if (me == N.rdv[g]) v = fi[PH(L, near_cell(e[0], ni), near_cell(e[1], nj), near_cell(e[2], nk))];
+          else if (me > N.rdv[g]) v = avg8(near_pair(e[0], ni), near_pair(e[1], nj), near_pair(e[2], nk));
+          else v = tri(near_cell(e[0], ni), near_cell(e[1], nj), near_cell(e[2], nk), e[0], e[1], e[2]);
+          (side ? N.rcm : N.rcp)[q + 1] = v;
+        }
+      /* edges (exchangepp.for:640-1086, 1587-2036): prev #1..6, next #1..6 */
+      const int epd[6][3] = {{-1, 0, -1}, {0, +1, -1}, {+1, 0, -1}, {0, -1, -1}, {-1, -1, 0}, {-1, +1, 0}};
+      const int end_[6][3] = {{+1, 0, +1}, {0, -1, +1}, {-1, 0, +1}, {0, +1, +1}, {+1, +1, 0}, {+1, -1, 0}};
+      for (int side = 0; side < 2; ++side)
+        for (int q = 0; q < 6; ++q) {
+          const int id = side ? B.d.edgnext[q] : B.d.edgprev[q];
+          if (id < 0) continue;
+          Blk &N = C.b[C.indid.at(id)];
+          const int *e = side ? end_[q] : epd[q];
+          const int ax = e[0] == 0 ? 0 : e[1] == 0 ? 1 : 2;  /* the edge's axis */
+          const int n = nn3[ax];
+          std::vector<double> &R = side ? N.rem[q + 1] : N.rep[q + 1];
+          if (me == N.rdv[g]) {
+            R.assign(n + 1, g_lmr_ring);
+            for (int nn = 2; nn <= n - 1; ++nn) {
+              int c[3] = {near_cell(e[0], ni), near_cell(e[1], nj), near_cell(e[2], nk)};
+              c[ax] = nn;
+              R[nn] = fi[PH(L, c[0], c[1], c[2])];
+            }
+          } else if (me > N.rdv[g]) {
+            const int nc = coarse_n(n);
+            R.assign(nc + 1, g_lmr_ring);
+            for (int nn = 2; nn <= nc - 1; ++nn) {
+              int c[3] = {near_pair(e[0], ni), near_pair(e[1], nj), near_pair(e[2], nk)};
+              c[ax] = 2 * nn - 2;
+              R[nn] = avg8(c[0], c[1], c[2]);
+            }
+          } else {
+            const int nf = 2 * (n - 2) + 2;
+            R.assign(nf + 1, g_lmr_ring);
+            for (int nn = 2; nn <= n - 1; ++nn) {
+              int c[3] = {near_cell(e[0], ni), near_cell(e[1], nj), near_cell(e[2], nk)};
+              c[ax] = nn;
+              for (int h = 0; h < 2; ++h) {
+                int ee[3] = {e[0], e[1], e[2]};
+                ee[ax] = h ? +1 : -1;
+                R[2 * nn - 2 + h] = tri(c[0], c[1], c[2], ee[0], ee[1], ee[2]);
+              }
+            }
+          }
+        }
+    }
+    /* unpack */
+    for (auto &B : C.b) {
+      Lev L = lev(C, B, g);
+      double *fi = B.cof.data();
+      const int ni = L.ni, nj = L.nj, nk = L.nk;
+      const int cprev = sd == 1 ? B.d.iprev : sd == 2 ? B.d.jprev : B.d.kprev;
+      const int cnext = sd == 1 ? B.d.inext : sd == 2 ? B.d.jnext : B.d.knext;
+      const int ns1 = sd == 2 ? ni : nj, ns2 = sd == 1 ? nk : sd == 2 ? nk : ni;
+      const int nd = sd == 1 ? ni : sd == 2 ? nj : nk;
+      const int me = B.rdv[g];
+      auto unpack_face = [&](int nbr, const std::vector<double> &R, bool prev) {
+        const int nb_ = C.b[C.indid.at(nbr)].rdv[g];
+        const int a = prev ? 1 : nd, a1 = prev ? 2 : nd - 1, a2 = prev ? 3 : nd - 2;
+        if (me == nb_) {
+          for (int t = 1; t <= ns2; ++t) for (int s = 1; s <= ns1; ++s)
+            fi[face_cell(L, sd, a, s, t)] = R[(size_t)(t - 1) * ns1 + s];
+        } else if (me > nb_) {
+          for (int t = 1; t <= ns2; ++t) for (int s = 1; s <= ns1; ++s)
+            fi[face_cell(L, sd, a, s, t)] =
+                (R[(size_t)(t - 1) * ns1 + s] + 3.0 * fi[face_cell(L, sd, a1, s, t)] - fi[face_cell(L, sd, a2, s, t)]) /
+                4.0;
+        } else {
+          for (int t = 2; t <= ns2 - 1; ++t) for (int s = 2; s <= ns1 - 1; ++s)
+            fi[face_cell(L, sd, a, s, t)] = R[(size_t)(t - 1) * ns1 + s];
+        }
+      };
+      if (cprev >= 0) unpack_face(cprev, B.recvb_m1, true);
+      if (cnext >= 0) unpack_face(cnext, B.recvb_p1, false);
+      if (sd != 3) continue;
+      const int upi[4] = {1, 1, ni, ni}, upj[4] = {1, nj, nj, 1};
+      for (int q = 0; q < 4; ++q)
+        if (B.d.corprev[q] >= 0) fi[PH(L, upi[q], upj[q], 1)] = B.rcm[q + 1];
+      if (B.d.edgprev[0] >= 0) for (int nn = 2; nn <= nj - 1; ++nn) fi[PH(L, 1, nn, 1)] = B.rem[1][nn];
+      if (B.d.edgprev[1] >= 0) for (int nn = 2; nn <= ni - 1; ++nn) fi[PH(L, nn, nj, 1)] = B.rem[2][nn];
+      if (B.d.edgprev[2] >= 0) for (int nn = 2; nn <= nj - 1; ++nn) fi[PH(L, ni, nn, 1)] = B.rem[3][nn];
+      if (B.d.edgprev[3] >= 0) for (int nn = 2; nn <= ni - 1; ++nn) fi[PH(L, nn, 1, 1)] = B.rem[4][nn];
+      if (B.d.edgprev[4] >= 0) for (int nn = 2; nn <= nk - 1; ++nn) fi[PH(L, 1, 1, nn)] = B.rem[5][nn];
+      if (B.d.edgprev[5] >= 0) for (int nn = 2; nn <= nk - 1; ++nn) fi[PH(L, 1, nj, nn)] = B.rem[6][nn];
+      const int uni[4] = {ni, ni, 1, 1}, unj[4] = {nj, 1, 1, nj};
+      for (int q = 0; q < 4; ++q)
+        if (B.d.cornext[q] >= 0) fi[PH(L, uni[q], unj[q], nk)] = B.rcp[q + 1];
+      if (B.d.edgnext[0] >= 0) for (int nn = 2; nn <= nj - 1; ++nn) fi[PH(L, ni, nn, nk)] = B.rep[1][nn];
+      if (B.d.edgnext[1] >= 0) for (int nn = 2; nn <= ni - 1; ++nn) fi[PH(L, nn, 1, nk)] = B.rep[2][nn];
+      if (B.d.edgnext[2] >= 0) for (int nn = 2; nn <= nj - 1; ++nn) fi[PH(L, 1, nn, nk)] = B.rep[3][nn];
+      if (B.d.edgnext[3] >= 0) for (int nn = 2; nn <= ni - 1; ++nn) fi[PH(L, nn, nj, nk)] = B.rep[4][nn];
+      if (B.d.edgnext[4] >= 0) for (int nn = 2; nn <= nk - 1; ++nn) fi[PH(L, ni, nj, nn)] = B.rep[5][nn];
+      if (B.d.edgnext[5] >= 0) for (int nn = 2; nn <= nk - 1; ++nn) fi[PH(L, ni, 1, nn)] = B.rep[6][nn];
+    }
+  }
+  mgbound(C, g);
+  if (C.periodic) exchbc_mgpp(C, g);
+}
+
 void exchangepp(Ctx &C, int g) {
+  if (C.lmr) { exchangepp_lmr(C, g); return; }
   for (int sd = 1; sd <= 3; ++sd) {
     for (auto &B : C.b) {
       Lev L = lev(C, B, g);
@@ -618,7 +834,11 @@ void mgrestr(Ctx &C, int g) {
     int gf = g - 1, gc = g;
     for (int k = 2; k <= nkc - 1; ++k) for (int i = 2; i <= nic - 1; ++i) for (int j = 2; j <= njc - 1; ++j) {
       long su = B.faz[g] + (long)(k - 2) * nijc2 + (long)(i - 2) * (njc - 2) + (j - 1) + 7 * incr_c;
-      if (!B.stretched) {
+      if (g > B.ngrid) {
+        /* LMR: a block past its own last level keeps its size; the rhs is
+         * the residual itself (mgsolver.for:714-727) */
+        cf[su] = R(i, j, k);
+      } else if (!B.stretched) {
         cf[su] = 0.125 * (R(2 * i - 2, 2 * j - 2, 2 * k - 2) + R(2 * i - 1, 2 * j - 2, 2 * k - 2) +
                           R(2 * i - 2, 2 * j - 1, 2 * k - 2) + R(2 * i - 1, 2 * j - 1, 2 * k - 2) +
                           R(2 * i - 2, 2 * j - 2, 2 * k - 1) + R(2 * i - 1, 2 * j - 2, 2 * k - 1) +
@@ -647,6 +867,13 @@ void mgcorr(Ctx &C, int g) {
   par_blocks((int)C.b.size(), [&](int ib_) { Blk &B = C.b[ib_];
     Lev Lf = lev(C, B, g), Lc = lev(C, B, g + 1);
     double *cf = B.cof.data();
+    if (g >= B.ngrid) {
+      /* LMR: both levels have the block's last size; the correction is
+       * added on every cell, ghosts included (mgsolver.for:806-818) */
+      for (int kc = 1; kc <= Lc.nk; ++kc) for (int ic = 1; ic <= Lc.ni; ++ic) for (int jc = 1; jc <= Lc.nj; ++jc)
+        cf[PH(Lf, ic, jc, kc)] = cf[PH(Lf, ic, jc, kc)] + cf[PH(Lc, ic, jc, kc)];
+      return;
+    }
     int nijf = Lf.nij, njf = Lf.nj, nijc = Lc.nij, njc = Lc.nj;
     for (int kc = 1; kc <= Lc.nk - 1; ++kc) {
       int k = 2 * kc - 1;
@@ -1901,10 +2128,47 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
     C.yst = std::min(C.yst, blocks[ib].ysl); C.yen = std::max(C.yen, blocks[ib].yel);
     C.zst = std::min(C.zst, blocks[ib].zsl); C.zen = std::max(C.zen, blocks[ib].zel);
   }
+  /* LMR (localparameters.for:26-102): a block's refinement rdiv is its
+   * spacing against the coarsest block's, a power of two; ngrd_gl =
+   * ngrid_input + log2(max rdiv) is the level count passed in, and a block
+   * of refinement r keeps ngrid_input + log2(r) levels of its own. */
+  std::vector<int> rdiv(nb, 1);
+  int lg_max = 0;
+  {
+    double hmax = 0.0;
+    for (int ib = 0; ib < nb; ++ib) hmax = std::max(hmax, blocks[ib].dx);
+    for (int ib = 0; ib < nb; ++ib) {
+      const mf3d_block_desc &d = blocks[ib];
+      const double r = hmax / d.dx;
+      const long q = std::lround(r);
+      if (q < 1 || (q & (q - 1)) || std::fabs(r - (double)q) > 1e-8 * r ||
+          std::fabs(blocks[0].dx / blocks[0].dy * d.dy - d.dx) > 1e-8 * d.dx ||
+          std::fabs(blocks[0].dx / blocks[0].dz * d.dz - d.dx) > 1e-8 * d.dx) {
+        g_err = "LMR: block spacings are not powers of two of one another"; return MF3D_E_INVALID;
+      }
+      rdiv[ib] = (int)q;
+      if (q > 1) C.lmr = true;
+      int lg = 0;
+      while ((1L << lg) < q) ++lg;
+      lg_max = std::max(lg_max, lg);
+    }
+    if (C.lmr) {
+      if (prm->ngrid - lg_max < 1) { g_err = "LMR: ngrid below log2(max rdiv) + 1"; return MF3D_E_INVALID; }
+      if (C.lsm) { g_err = "LMR with L_LSM"; return MF3D_E_UNSUPPORTED; }
+      if (C.solver == 1) { g_err = "LMR with solver 1"; return MF3D_E_UNSUPPORTED; }
+      for (int ib = 0; ib < nb; ++ib)
+        if (blocks[ib].hx || blocks[ib].hy || blocks[ib].hz) { g_err = "LMR on a stretched grid"; return MF3D_E_UNSUPPORTED; }
+    }
+  }
   for (int ib = 0; ib < nb; ++ib) {
     Blk &B = C.b[ib];
     B.d = blocks[ib];
-    B.ngrid = prm->ngrid;
+    B.rdiv = rdiv[ib];
+    {
+      int lg = 0;
+      while ((1 << lg) < B.rdiv) ++lg;
+      B.ngrid = prm->ngrid - lg_max + lg; /* localparameters.for:42-45 */
+    }
     int pl = prm->pl;
     int pow2 = 1 << (B.ngrid - 1);
     if (B.d.nx % pow2 || B.d.ny % pow2 || B.d.nz % pow2) { g_err = "not divisible"; return MF3D_E_INVALID; }
@@ -1941,6 +2205,40 @@ int setup(Ctx &C, const mf3d_block_desc *blocks, int nb, const mf3d_params *prm)
     size_t ttc = (size_t)B.ttc_i * B.ttc_j * B.ttc_k;
     B.su.assign(ttc, 0.0);
     B.pp.assign(ttc, 0.0);
+  }
+  /* rdv(dom, g) (localparameters.for:47-57): the block's refinement on the
+   * levels the coarsest blocks have, halving on its extra levels, 1 below
+   * its own last level */
+  const int act_ngrid = prm->ngrid - lg_max;
+  for (auto &B : C.b) {
+    B.rdv.assign(C.ngrd_gl + 1, 1);
+    for (int g = 1; g <= C.ngrd_gl; ++g) {
+      if (g > B.ngrid) B.rdv[g] = 1;
+      else if (g <= act_ngrid) B.rdv[g] = B.rdiv;
+      else B.rdv[g] = B.rdv[g - 1] / 2;
+    }
+  }
+  if (C.lmr) {
+    /* alloc_dom.for:12-230: neighbours differ by a factor of 2 at most, and
+     * periodic partners not at all */
+    for (auto &B : C.b) {
+      const int nbr[6] = {B.d.iprev, B.d.inext, B.d.jprev, B.d.jnext, B.d.kprev, B.d.knext};
+      std::vector<int> all(nbr, nbr + 6);
+      for (int q = 0; q < 4; ++q) { all.push_back(B.d.corprev[q]); all.push_back(B.d.cornext[q]); }
+      for (int q = 0; q < 6; ++q) { all.push_back(B.d.edgprev[q]); all.push_back(B.d.edgnext[q]); }
+      for (int id : all) {
+        if (id < 0) continue;
+        auto it = C.indid.find(id);
+        if (it == C.indid.end()) { g_err = "neighbour id not in the layout"; return MF3D_E_INVALID; }
+        const int r = C.b[it->second].rdiv;
+        if (r != B.rdiv && r != 2 * B.rdiv && 2 * r != B.rdiv) { g_err = "wrong rdiv"; return MF3D_E_INVALID; }
+      }
+      const int per[6] = {B.d.per_ip, B.d.per_in, B.d.per_jp, B.d.per_jn, B.d.per_kp, B.d.per_kn};
+      for (int id : per)
+        if (id >= 0 && C.indid.count(id) && C.b[C.indid.at(id)].rdiv != B.rdiv) {
+          g_err = "wrong rdiv for a periodic partner"; return MF3D_E_INVALID;
+        }
+    }
   }
   coeff(C);
   return MF3D_OK;
@@ -1981,6 +2279,10 @@ int orc_bind_old_velocity(int nb, const double *const *uoo, const double *const 
 /* Threads for the per-block loops (1 = serial, the default). */
 void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
 
+/* LMR: the value of the receive-buffer entries that no sender writes (the
+ * ring of a fine block's face buffer next to a coarser neighbour). */
+void orc_set_lmr_ring(double v) { g_lmr_ring = v; }
+
 /* Wall-clock stamps of the next orc_newsolv_mg: t[0] at entry, t[1] after
  * the initial calvel/calmas, t[1+q] after outer iteration q (NULL = off). */
 void orc_set_timestamps(double *t, int cap) { g_tstamp = t; g_tcap = t ? cap : 0; }
@@ -1991,6 +2293,7 @@ int orc_newsolv_mg(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
   Ctx C;
   int st = setup(C, blocks, nb, prm);
   if (st) return st;
+  if (C.lmr) { g_err = "LMR: the field exchanges at refinement interfaces (exchangep.for, exchangeu/v/w.for) are not restated"; return MF3D_E_UNSUPPORTED; }
   C.dt = dt; C.alfapr = alfapr;
   for (int ib = 0; ib < nb; ++ib) {
     Blk &B = C.b[ib];
@@ -2016,6 +2319,7 @@ int orc_rungek_2nd(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm
   p.alfabc = alfabc;
   int st = setup(C, blocks, nb, &p);
   if (st) return st;
+  if (C.lmr) { g_err = "LMR: the field exchanges at refinement interfaces (exchangep.for, exchangeu/v/w.for) are not restated"; return MF3D_E_UNSUPPORTED; }
   if (C.lsm) { g_err = "rungek_2nd: no L_LSM branch"; return MF3D_E_UNSUPPORTED; }
   C.bounds = true;
   for (auto &B : C.b) {
@@ -2060,6 +2364,7 @@ int orc_bounds(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, co
   p.alfabc = alfabc;
   int st = setup(C, blocks, nb, &p);
   if (st) return st;
+  if (C.lmr) { g_err = "LMR: the field exchanges at refinement interfaces (exchangep.for, exchangeu/v/w.for) are not restated"; return MF3D_E_UNSUPPORTED; }
   C.dt = dt; C.alfapr = alfapr;
   for (int ib = 0; ib < nb; ++ib) {
     Blk &B = C.b[ib];
@@ -2078,6 +2383,7 @@ int orc_exchange(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, 
   Ctx C;
   int st = setup(C, blocks, nb, prm);
   if (st) return st;
+  if (C.lmr) { g_err = "LMR: the field exchanges at refinement interfaces (exchangep.for, exchangeu/v/w.for) are not restated"; return MF3D_E_UNSUPPORTED; }
   for (int ib = 0; ib < nb; ++ib) {
     Blk &B = C.b[ib];
     B.u = fields[ib].u; B.v = fields[ib].v; B.w = fields[ib].w; B.p = fields[ib].p;
@@ -2093,6 +2399,7 @@ int orc_calvel(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, co
   Ctx C;
   int st = setup(C, blocks, nb, prm);
   if (st) return st;
+  if (C.lmr) { g_err = "LMR: the field exchanges at refinement interfaces (exchangep.for, exchangeu/v/w.for) are not restated"; return MF3D_E_UNSUPPORTED; }
   if (C.lsm) { g_err = "calvel: no L_LSM here"; return MF3D_E_UNSUPPORTED; }
   C.dt = dt; C.alfapr = alfapr;
   for (int ib = 0; ib < nb; ++ib) {
