@@ -462,6 +462,18 @@ int mf3d_test_stall_copy(int device, int bytes);
 long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid,
                         int level, long long *dst, long long *src);
 
+/* Host-only: the same refresh applied to host arrays, for any layout - LMR
+ * included, where a level on which refinements meet (rdv differing,
+ * localparameters.for:47-57) takes the weighted sums of exchangepp's
+ * fine/coarse branches instead of copies (exchangepp.for:43-4763).  fi[b]
+ * holds block b's level-`level` array, ghost-inclusive, i fastest, of the
+ * block's level size (an LMR block past its own last level keeps that
+ * size).  Same arithmetic, in the same order, as the device's refresh; the
+ * entries of a refined block's face buffer that no coarse sender writes
+ * are taken as 0.  Needs no GPU.  Returns MF3D_OK or an error status. */
+int mf3d_halo_refresh_host(const mf3d_block_desc *blocks, int nblocks, int ngrid,
+                           int level, double *const *fi);
+
 /* ---------------------------------------------------------------------- */
 /* Serving (no counterpart in the reference): a request loop on one device */
 /* that admits independent single-block solves as they arrive, keeps their  */

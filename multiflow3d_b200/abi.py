@@ -151,6 +151,7 @@ EXPORTED_SYMBOLS = (
     "mf3d_abi_version",
     "mf3d_last_launch_count",
     "mf3d_halo_map",
+    "mf3d_halo_refresh_host",
     "mf3d_profile",
     "mf3d_profile_read",
     "mf3d_max_levels",
@@ -211,6 +212,7 @@ def _declare(lib):
     lib.mf3d_halo_map.restype = C.c_longlong
     lib.mf3d_halo_map.argtypes = [C.POINTER(BlockDesc), C.c_int, C.c_int, C.c_int,
                                   C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.mf3d_halo_refresh_host.argtypes = [C.POINTER(BlockDesc), C.c_int, C.c_int, C.c_int, C.POINTER(_dp)]
     lib.mf3d_max_levels.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.mf3d_batch_create.argtypes = [C.POINTER(DomainDesc), C.c_int, C.POINTER(Params), C.POINTER(vp)]
     lib.mf3d_batch_solve_device.argtypes = [vp, C.POINTER(Fields), _dp, _dp, C.POINTER(SolveInfo), _dp, C.c_int]

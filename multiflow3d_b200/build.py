@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmf3d.so")
 SOURCES = ["mf3d.cu", "topology.cpp"]
-HEADERS = ["kernels.cuh", "coarse.cuh", "midcycle.cuh", "outer.cuh", "server.cuh", "tecbin.cuh", "sip.cuh", "mf3d_internal.h", "../../include/mf3d.h"]
+HEADERS = ["kernels.cuh", "coarse.cuh", "midcycle.cuh", "lmr.cuh", "outer.cuh", "server.cuh", "tecbin.cuh", "sip.cuh", "mf3d_internal.h", "../../include/mf3d.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

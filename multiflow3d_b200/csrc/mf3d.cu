@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <type_traits>
 #include <map>
 #include <memory>
 #include <atomic>
@@ -33,6 +34,7 @@
 #include "kernels.cuh"
 #include "coarse.cuh"
 #include "midcycle.cuh"
+#include "lmr.cuh"
 #include "mf3d_internal.h"
 #include "outer.cuh"
 
@@ -345,6 +347,7 @@ static int colour_map(CUtensorMap *m, void *base, int elem, const BlkLev &B, int
 struct BlockStore {
   mf3d_block_desc d;     // neighbour ids refer to blocks of the same domain
   int ngrid = 1;
+  int own = 1;           // levels of the block's own size (LMR: below them it keeps the last size)
   int elem = 8;          // bytes per multigrid value (8 FP64, 4 FP32)
   std::vector<LevelStore> lv;  // [1..ngrid]
   DevBuf<double> geo1;   // level-1 widths h[3] (n+2) and face distances df[3] (n+1)
@@ -360,11 +363,12 @@ struct BlockStore {
 // Build one block's hierarchy: replaces `coeff` (mgsolver.for:2-222) and the
 // `cof` sizing of localparameters.for:208-237.
 static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int elem_fine, int elem_coarsest, int pl,
-                       bool lsm, bool bounds, cudaStream_t s) {
+                       bool lsm, bool bounds, cudaStream_t s, int own = 0) {
   const int elem = elem_fine;
   S.d = d;
   S.lsm = lsm;
   S.ngrid = ngrid;
+  S.own = own > 0 ? std::min(own, ngrid) : ngrid;
   S.elem = elem;
   S.lv.clear();
   S.lv.resize(ngrid + 1);
@@ -384,9 +388,10 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
     std::memset(&B, 0, sizeof B);
     const int elem = (g == ngrid && ngrid > 1) ? elem_coarsest : elem_fine;
     L.elem = elem;
-    B.nx = d.nx >> (g - 1);
-    B.ny = d.ny >> (g - 1);
-    B.nz = d.nz >> (g - 1);
+    const int gl = std::min(g, S.own);  // LMR: past its own levels a block keeps its last size
+    B.nx = d.nx >> (gl - 1);
+    B.ny = d.ny >> (gl - 1);
+    B.nz = d.nz >> (gl - 1);
     B.hp = hp_of(B.nx, elem);
     B.cstr = (long long)(B.nz + 2) * (B.ny + 2) * B.hp;
     B.cstr = (B.cstr + 31) / 32 * 32;  // 256-byte aligned colour arrays
@@ -401,9 +406,9 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
     std::vector<double> coef, geo;
     const int nn[3] = {B.nx, B.ny, B.nz};
     for (int a = 0; a < 3; ++a) {
-      std::vector<double> w = level_widths(ext[a], nfine[a], hh[a], ngrid, g);
+      std::vector<double> w = level_widths(ext[a], nfine[a], hh[a], ngrid, gl);
       const int n = nn[a];
-      const double hl = hh[a] * (double)(1 << (g - 1));
+      const double hl = hh[a] * (double)(1 << (gl - 1));
       const double dd = hl * hl;
       for (int side = 0; side < 2; ++side)
         for (int c = 0; c < n + 2; ++c) {
@@ -420,7 +425,7 @@ static int build_block(BlockStore &S, const mf3d_block_desc &d, int ngrid, int e
     // restriction ratios hf/Hc of this (fine) level: 0.5 exactly on uniform axes
     for (int a = 0; a < 3; ++a) {
       const int n = nn[a];
-      if (g < ngrid) {
+      if (g < S.own) {
         std::vector<double> wf = level_widths(ext[a], nfine[a], hh[a], ngrid, g);
         std::vector<double> wc = level_widths(ext[a], nfine[a], hh[a], ngrid, g + 1);
         for (int c = 0; c < n + 2; ++c) geo.push_back((c >= 1 && c <= n) ? wf[c] / wc[(c + 1) >> 1] : 0.0);
@@ -543,6 +548,16 @@ struct DomainStore {
   long long nfx_uvw = 0, nsfx_uvw = 0, nfx_p = 0, nsfx_p = 0;
   long long nfxe_sub = 0, nsfxe_sub = 0, nfxe_chain = 0, nfxe_cells = 0;
   bool fx_per_iteration = false;
+  // LMR: per level, the halo refresh as a program (build_halo_lmr) where
+  // refinements meet on the level; empty elsewhere
+  struct LmrLevel {
+    DevBuf<LmrTerm> terms;
+    DevBuf<LmrNode> nodes;
+    DevBuf<LmrWrite> writes;
+    std::vector<int> depth_start;
+    int n_writes = 0;
+  };
+  std::vector<LmrLevel> lmr;
   size_t bytes = 0;
 };
 
@@ -716,9 +731,12 @@ static long long level_off(const BlkLev &B, int i, int j, int k) {
   return c * B.cstr + ((long long)k * (B.ny + 2) + j) * B.hp + (i >> 1);
 }
 
+// `own` (LMR, else null): each block's levels of its own size; `rdv`:
+// rdv(block, g) per block, indexed [b][g].
 static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, int ngrid, int elem, int elem_coarsest,
                         int pl, cudaStream_t s, bool lsm = false, bool bounds = false, int field_maps_pl_ex = -1,
-                        bool fx_per_iteration = false) {
+                        bool fx_per_iteration = false, const std::vector<int> *own = nullptr,
+                        const std::vector<std::vector<int>> *rdv = nullptr) {
   D.ngrid = ngrid;
   D.blocks.clear();
   std::vector<mf3d_block_desc> descs(blocks, blocks + nb);
@@ -727,12 +745,69 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
   D.bytes = 0;
   for (int b = 0; b < nb; ++b) {
     D.blocks.emplace_back(new BlockStore());
-    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, elem_coarsest, pl, lsm, bounds, s))) return st;
+    if ((st = build_block(*D.blocks.back(), descs[b], ngrid, elem, elem_coarsest, pl, lsm, bounds, s,
+                          own ? (*own)[b] : 0)))
+      return st;
     D.bytes += D.blocks.back()->bytes;
   }
   D.halo.assign(ngrid + 1, {});
   D.nstaged.assign(ngrid + 1, 0);
+  D.lmr.clear();
+  D.lmr.resize(ngrid + 1);
   for (int g = 1; g <= ngrid; ++g) {
+    if (rdv) {
+      bool mixed = false;
+      for (int b = 1; b < nb; ++b) mixed |= (*rdv)[b][g] != (*rdv)[0][g];
+      if (mixed) {
+        std::vector<LevelGeom> geom(nb);
+        std::vector<long long> base(nb);
+        std::vector<int> rg(nb);
+        long long acc = 0;
+        for (int b = 0; b < nb; ++b) {
+          const BlkLev &B = D.blocks[b]->lv[g].desc;
+          geom[b] = LevelGeom{B.nx, B.ny, B.nz};
+          base[b] = acc;
+          acc += geom[b].cells();
+          rg[b] = (*rdv)[b][g];
+        }
+        const LmrProgram P = build_halo_lmr(descs, geom, base, rg);
+        auto loc = [&](long long id, int &blk, int &off) {
+          const int b = (int)(std::upper_bound(base.begin(), base.end(), id) - base.begin()) - 1;
+          long long lin = id - base[b];
+          const LevelGeom &G = geom[b];
+          const int i = (int)(lin % (G.nx + 2));
+          lin /= (G.nx + 2);
+          const int j = (int)(lin % (G.ny + 2));
+          const int k = (int)(lin / (G.ny + 2));
+          blk = b;
+          off = (int)level_off(D.blocks[b]->lv[g].desc, i, j, k);
+        };
+        std::vector<LmrTerm> terms(P.terms.size());
+        for (size_t q = 0; q < terms.size(); ++q) {
+          const auto &t = P.terms[q];
+          terms[q].w = t.w;
+          if (t.ref >= 0) loc(t.ref, terms[q].blk, terms[q].off);
+          else if (t.ref == kLmrZero) { terms[q].blk = -2; terms[q].off = 0; }
+          else { terms[q].blk = -1; terms[q].off = (int)(-2 - t.ref); }
+        }
+        std::vector<LmrNode> nodes(P.nodes.size());
+        for (size_t q = 0; q < nodes.size(); ++q) nodes[q] = LmrNode{P.nodes[q].t0, P.nodes[q].nt, P.nodes[q].scale};
+        std::vector<LmrWrite> writes(P.writes.size());
+        for (size_t q = 0; q < writes.size(); ++q) {
+          loc(P.writes[q].first, writes[q].blk, writes[q].off);
+          writes[q].node = P.writes[q].second;
+        }
+        DomainStore::LmrLevel &M = D.lmr[g];
+        if ((st = M.terms.upload(terms, s))) return st;
+        if ((st = M.nodes.upload(nodes, s))) return st;
+        if ((st = M.writes.upload(writes, s))) return st;
+        CK(cudaStreamSynchronize(s));  // the host vectors are locals
+        M.depth_start = P.depth_start;
+        M.n_writes = (int)writes.size();
+        D.bytes += terms.size() * sizeof(LmrTerm) + nodes.size() * sizeof(LmrNode) + writes.size() * sizeof(LmrWrite);
+        continue;  // no copy map on this level
+      }
+    }
     std::vector<LevelGeom> geom(nb);
     std::vector<long long> base(nb);
     long long acc = 0;
@@ -821,6 +896,20 @@ struct ViewLevel {
   int lx_cl = 1;                      // lexicographic relaxation (mg_itrsch 1): CTAs per block
   size_t td_smem = 0;
   bool td_fp64 = true;                // the level relaxes in FP64
+  // LMR (single-domain views): the level's halo program where refinements
+  // meet on it (DomainStore::LmrLevel), and the blocks past their own last
+  // level - restricted into this level by injection, corrected from the next
+  // one by addition - as item lists over their ghost-inclusive cells
+  const LmrTerm *lmr_terms = nullptr;
+  const LmrNode *lmr_nodes = nullptr;
+  const LmrWrite *lmr_writes = nullptr;
+  std::vector<int> lmr_depth;
+  int lmr_nwrites = 0;
+  DevBuf<double> lmr_val;
+  DevBuf<int> inj_list, add_list;
+  DevBuf<long long> inj_pre, add_pre;
+  int n_inj = 0, n_add = 0;
+  long long inj_items = 0, add_items = 0;
 };
 
 struct View {
@@ -900,6 +989,7 @@ struct mf3d_ctx {
   int device = 0;
   int elem = 8;
   bool coarse64 = false;    // FP32 V-cycle with the coarsest level (and its sweeps) in FP64
+  bool lmr = false;         // blocks of different refinement (LMR): the V-cycle only
   int nsm = 148;            // SMs of the device
   int sweep_occ = 4;        // resident sweep CTAs per SM
   cudaStream_t stream = nullptr;
@@ -1216,6 +1306,7 @@ static void tdma_factors(mf3d_ctx *C, View &V) {
 constexpr size_t kCcSmemCap = 200 * 1024;
 static int coarse_cycle_plan(mf3d_ctx *C, View &V) {
   V.cc_g0 = 0;
+  if (C->lmr) return MF3D_OK;  // the cluster kernel holds no LMR halo programs
   const char *e = std::getenv("MF3D_COARSE_CLUSTER");
   if (e && e[0] == '0') return MF3D_OK;
   const int nb = (int)V.blk.size();
@@ -1332,6 +1423,7 @@ static int coarse_cycle_plan(mf3d_ctx *C, View &V) {
 // items below 2^31; otherwise the launch path stays.
 static int mid_cycle_plan(mf3d_ctx *C, View &V) {
   V.mid_on = false;
+  if (C->lmr) return MF3D_OK;
   // off unless MF3D_MID_CYCLE=1: on 2x2x2 blocks of 128^3 the launch path
   // measured 85.7 ms a solve against 92.9 for this one (its grid barriers
   // cost more than the launches they replace)
@@ -1539,12 +1631,36 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       // restriction into level g (g > 1): every block present here; prolongation
       // from level g+1 into g: every block continuing down
       std::vector<PlaneExt> re, pe;
+      std::vector<int> inj, add, rblk;
+      std::vector<long long> inj_pre(1, 0), add_pre(1, 0);
       for (int b = 0; b < nb; ++b) {
         const BlkLev &B = tab[b];
-        if (g > V.blk[b]->ngrid) continue;
-        if (g > 1) re.push_back(PlaneExt{b, B.nx + 2, B.ny + 2, 0, B.nz + 1});
-        if (g < V.blk[b]->ngrid) pe.push_back(PlaneExt{b, B.nx / 2 + 1, B.ny / 2 + 1, 0, B.nz / 2});
+        const BlockStore &S = *V.blk[b];
+        if (g > S.ngrid) continue;
+        const long long cells = (long long)(B.nx + 2) * (B.ny + 2) * (B.nz + 2);
+        if (g > 1 && g > S.own) {  // LMR: into a level of the same size
+          inj.push_back(b);
+          inj_pre.push_back(inj_pre.back() + cells);
+        } else if (g > 1) {
+          re.push_back(PlaneExt{b, B.nx + 2, B.ny + 2, 0, B.nz + 1});
+        }
+        if (g < S.ngrid && g >= S.own) {  // LMR: from a level of the same size
+          add.push_back(b);
+          add_pre.push_back(add_pre.back() + cells);
+        } else if (g < S.ngrid) {
+          pe.push_back(PlaneExt{b, B.nx / 2 + 1, B.ny / 2 + 1, 0, B.nz / 2});
+        }
       }
+      for (int b : sblk[SUB_A])
+        if (!(g > 1 && g > V.blk[b]->own)) rblk.push_back(b);
+      L.n_inj = (int)inj.size();
+      L.n_add = (int)add.size();
+      L.inj_items = inj_pre.back();
+      L.add_items = add_pre.back();
+      if ((st = L.inj_list.upload(inj, s))) return st;
+      if ((st = L.inj_pre.upload(inj_pre, s))) return st;
+      if ((st = L.add_list.upload(add, s))) return st;
+      if ((st = L.add_pre.upload(add_pre, s))) return st;
       std::vector<Tile> rt, pt;
       L.rkch = plane_tiles(C, re, rt);
       L.pkch = plane_tiles(C, pe, pt);
@@ -1553,7 +1669,7 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       if ((st = L.rtile.upload(rt, s))) return st;
       if ((st = L.ptile.upload(pt, s))) return st;
       std::vector<Tile> rm;
-      if (g > 1) L.rtma_kch = rtma_tiles(C, tab, sblk[SUB_A], 0, rm);
+      if (g > 1 && !rblk.empty()) L.rtma_kch = rtma_tiles(C, tab, rblk, 0, rm);
       L.n_rtma = (int)rm.size();
       if ((st = L.rtma.upload(rm, s))) return st;
     }
@@ -1582,6 +1698,18 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
       if ((st = L.sweep[q].upload(sw[q], s))) return st;
       if ((st = L.cells[q].upload(ce[q], s))) return st;
       if ((st = L.list[q].upload(li[q], s))) return st;
+    }
+    // LMR: the level's halo program (single-domain views)
+    L.lmr_depth.clear();
+    L.lmr_nwrites = 0;
+    if (nd == 1 && (int)doms[0]->lmr.size() > g && !doms[0]->lmr[g].depth_start.empty()) {
+      const DomainStore::LmrLevel &M = doms[0]->lmr[g];
+      L.lmr_terms = M.terms.p;
+      L.lmr_nodes = M.nodes.p;
+      L.lmr_writes = M.writes.p;
+      L.lmr_depth = M.depth_start;
+      L.lmr_nwrites = M.n_writes;
+      if ((st = L.lmr_val.alloc((size_t)std::max(M.depth_start.back(), 1)))) return st;
     }
     // halo segments: the domains' resident pair lists
     for (int q = 0; q < 3; ++q) {
@@ -1717,6 +1845,22 @@ static int build_view(mf3d_ctx *C, View &V, const std::vector<DomainStore *> &do
 template <typename T>
 static void halo(mf3d_ctx *C, View &V, int g, int q) {
   ViewLevel &L = V.lv[g];
+  if (!L.lmr_depth.empty()) {
+    // LMR: the nodes depth by depth from the pre-exchange state, then the writes
+    for (size_t d = 1; d < L.lmr_depth.size(); ++d) {
+      const int n0 = L.lmr_depth[d - 1], n1 = L.lmr_depth[d];
+      if (n1 <= n0) continue;
+      launch(k_lmr_nodes<T>, grid_of(n1 - n0, 256), 256, 0, C->stream, L.tab.p, L.lmr_terms, L.lmr_nodes, n0, n1,
+             L.lmr_val.p);
+      ++C->launches;
+    }
+    if (L.lmr_nwrites) {
+      launch(k_lmr_write<T>, grid_of(L.lmr_nwrites, 256), 256, 0, C->stream, L.tab.p, L.lmr_writes, L.lmr_nwrites,
+             (const double *)L.lmr_val.p);
+      ++C->launches;
+    }
+    return;
+  }
   if (!L.n_halo[q]) return;
   T *buf = (T *)L.stage[q].p;
   if (L.n_staged[q]) {
@@ -1795,6 +1939,12 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bo
 template <typename T, typename TC>
 static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks continuing down
   ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
+  if constexpr (std::is_same<T, TC>::value)
+    if (Cl.n_inj) {  // LMR: blocks past their own last level
+      launch(k_lmr_inject<T>, grid_of(Cl.inj_items, 256), 256, 0, C->stream, F.tab.p, Cl.tab.p, Cl.inj_list.p,
+             Cl.inj_pre.p, Cl.n_inj, V.act.p, (C->prm.mg_itrsch == 3 && C->prm.irestr > 0) ? 1 : 0);
+      ++C->launches;
+    }
   if (!Cl.n_rtile) return;
   const int pk = g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse out
@@ -1817,6 +1967,13 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
 template <typename T, typename TC>
 static void corr(mf3d_ctx *C, View &V, int g) {  // level g+1 -> g, blocks continuing down
   ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
+  if constexpr (std::is_same<T, TC>::value)
+    if (F.n_add) {  // LMR: blocks past their own last level
+      for (int mode = 0; mode < 2; ++mode)
+        launch(k_lmr_add<T>, grid_of(F.add_items, 256), 256, 0, C->stream, F.tab.p, Cl.tab.p, F.add_list.p,
+               F.add_pre.p, F.n_add, V.act.p, mode);
+      C->launches += 2;
+    }
   if (!F.n_ptile) return;
   const int pk = g == 1 ? MF3D_PROF_PROLONG_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 1.0 / 8.0));  // fine in/out, coarse in
@@ -2134,7 +2291,7 @@ static int autotune_restrict(mf3d_ctx *C, View &V, int g, bool time_new) {
 // the restriction below it.  Levels inside the coarse cluster launch
 // (k_coarse_cycle) run no sweep or restriction of their own.
 static int autotune_view(mf3d_ctx *C, View &V, bool time_new) {
-  if (!autotune_enabled()) return MF3D_OK;
+  if (!autotune_enabled() || C->lmr) return MF3D_OK;
   if (C->prm.mg_itrsch == 2 && C->prm.lsm) return MF3D_OK;
   const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
   // last level with its own sweep launches (the middle-level launch and the
@@ -2953,13 +3110,95 @@ static int inlets_ready(const mf3d_ctx *C, bool outflow = false) {
   return MF3D_OK;
 }
 
+// LMR (localparameters.for:26-102): a block's refinement rdiv is the
+// coarsest block's spacing over its own, a power of two; params.ngrid is
+// ngrd_gl = ngrid_input + log2(max rdiv), and a block of refinement r keeps
+// ngrid_input + log2(r) levels of its own size (`own`).  rdv[b][g]
+// (localparameters.for:47-57): r on the levels every block has, halving on
+// the block's extra levels, 1 below its own.  Returns whether the layout
+// mixes refinements; the rules of alloc_dom.for:12-230 (neighbours at most
+// 2:1 apart, periodic partners equal) and the scope of the restatement (the
+// V-cycle in FP64 on uniform blocks) are checked here.
+static int lmr_plan(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, bool &lmr, std::vector<int> &own,
+                    std::vector<std::vector<int>> &rdv) {
+  lmr = false;
+  own.assign(nb, prm->ngrid);
+  rdv.assign(nb, std::vector<int>(prm->ngrid + 1, 1));
+  double hmax = 0.0;
+  for (int b = 0; b < nb; ++b) hmax = std::max(hmax, blocks[b].dx);
+  std::vector<int> r(nb, 1), lg(nb, 0);
+  int lg_max = 0;
+  for (int b = 0; b < nb; ++b) {
+    const mf3d_block_desc &d = blocks[b];
+    const double x = hmax / d.dx;
+    const long q = std::lround(x);
+    if (!(d.dx > 0.0) || q < 1 || (q & (q - 1)) || std::fabs(x - (double)q) > 1e-8 * x ||
+        std::fabs(blocks[0].dx / blocks[0].dy * d.dy - d.dx) > 1e-8 * d.dx ||
+        std::fabs(blocks[0].dx / blocks[0].dz * d.dz - d.dx) > 1e-8 * d.dx) {
+      set_error("block " + std::to_string(d.id) + ": spacings are not the coarsest block's over a power of two");
+      return MF3D_E_INVALID;
+    }
+    r[b] = (int)q;
+    while ((1 << lg[b]) < r[b]) ++lg[b];
+    lg_max = std::max(lg_max, lg[b]);
+    lmr |= q > 1;
+  }
+  if (!lmr) return MF3D_OK;
+  if (prm->ngrid - lg_max < 1) {
+    set_error("LMR: ngrid (ngrd_gl) must exceed log2 of the largest refinement");
+    return MF3D_E_INVALID;
+  }
+  if (prm->precision != MF3D_PREC_FP64 || prm->lsm || prm->solver == 1 || prm->bounds) {
+    set_error("LMR: the V-cycle runs in FP64, without lsm, bounds or solver 1");
+    return MF3D_E_UNSUPPORTED;
+  }
+  std::map<int, int> pos;
+  for (int b = 0; b < nb; ++b) pos[blocks[b].id] = b;
+  const int act = prm->ngrid - lg_max;
+  for (int b = 0; b < nb; ++b) {
+    const mf3d_block_desc &d = blocks[b];
+    if (d.hx || d.hy || d.hz) {
+      set_error("LMR: uniform spacing only (block " + std::to_string(d.id) + ")");
+      return MF3D_E_UNSUPPORTED;
+    }
+    std::vector<int> nbr = {d.iprev, d.inext, d.jprev, d.jnext, d.kprev, d.knext};
+    for (int q = 0; q < 4; ++q) { nbr.push_back(d.corprev[q]); nbr.push_back(d.cornext[q]); }
+    for (int q = 0; q < 6; ++q) { nbr.push_back(d.edgprev[q]); nbr.push_back(d.edgnext[q]); }
+    for (int id : nbr) {
+      if (id < 0) continue;
+      auto it = pos.find(id);
+      if (it == pos.end()) { set_error("neighbour id " + std::to_string(id) + " not in the layout"); return MF3D_E_INVALID; }
+      const int o = r[it->second];
+      if (o != r[b] && o != 2 * r[b] && 2 * o != r[b]) {
+        set_error("====ERROR===>  wrong rdiv " + std::to_string(d.id) + " (neighbours more than 2:1 apart)");
+        return MF3D_E_INVALID;
+      }
+    }
+    for (int id : {d.per_ip, d.per_in, d.per_jp, d.per_jn, d.per_kp, d.per_kn}) {
+      auto it = pos.find(id);
+      if (id >= 0 && it != pos.end() && r[it->second] != r[b]) {
+        set_error("==ERROR==>wrong rdiv for a periodic partner of block " + std::to_string(d.id));
+        return MF3D_E_INVALID;
+      }
+    }
+    own[b] = act + lg[b];
+    for (int g = 1; g <= prm->ngrid; ++g)
+      rdv[b][g] = g > own[b] ? 1 : g <= act ? r[b] : rdv[b][g - 1] / 2;
+  }
+  return MF3D_OK;
+}
+
 static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm, mf3d_ctx **out) {
   if (!blocks || nb <= 0 || !out) { set_error("mf3d_create: bad arguments"); return MF3D_E_INVALID; }
   int st = check_params(prm);
   if (st) return st;
-  const int pow2 = 1 << (prm->ngrid - 1);
+  bool lmr = false;
+  std::vector<int> own;
+  std::vector<std::vector<int>> rdv;
+  if ((st = lmr_plan(blocks, nb, prm, lmr, own, rdv))) return st;
   for (int b = 0; b < nb; ++b) {
     const auto &d = blocks[b];
+    const int pow2 = 1 << (own[b] - 1);
     if (d.nx < 1 || d.ny < 1 || d.nz < 1 || d.nx % pow2 || d.ny % pow2 || d.nz % pow2) {  // localparameters.for:201-206
       set_error("2:the given number not correct for mgsolver! (block " + std::to_string(d.id) +
                 " not divisible by 2^(ngrid-1))");
@@ -3021,8 +3260,10 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   AllocScope scope(C->stream);
   C->doms.emplace_back(new DomainStore());
   C->coarse64 = C->elem == 4 && prm->ngrid > 1;
+  C->lmr = lmr;
   if ((st = build_domain(*C->doms[0], blocks, nb, prm->ngrid, C->elem, C->coarse64 ? 8 : C->elem, prm->pl,
-                         C->stream, prm->lsm != 0, prm->bounds != 0, prm->pl_ex, prm->differencing == 2)))
+                         C->stream, prm->lsm != 0, prm->bounds != 0, lmr ? -1 : prm->pl_ex, prm->differencing == 2,
+                         lmr ? &own : nullptr, lmr ? &rdv : nullptr)))
     return st;
   if (prm->bounds) {
     const Extents e = domain_extents(blocks, nb);
@@ -3045,6 +3286,16 @@ static int create(const mf3d_block_desc *blocks, int nb, const mf3d_params *prm,
   if ((st = make_view(C.get()))) return st;
   *out = C.release();
   return MF3D_OK;
+}
+
+// LMR contexts run the V-cycle only: the outer loop's field exchanges at
+// refinement interfaces (exchangep.for, exchangeu/v/w.for) are not restated.
+static int lmr_refused(const mf3d_ctx *C, const char *what) {
+  if (!C || !C->lmr) return MF3D_OK;
+  set_error(std::string(what) +
+            ": an LMR layout (blocks of different refinement) runs mf3d_mgkcyc_device only; the field exchanges "
+            "at refinement interfaces (exchangep.for, exchangeu/v/w.for) are not restated");
+  return MF3D_E_UNSUPPORTED;
 }
 
 }  // namespace mf3d
@@ -3333,6 +3584,7 @@ int mf3d_destroy(mf3d_ctx *ctx) {
 int mf3d_newsolv_mg_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr, mf3d_solve_info *info,
                            double *hist, int cap) {
   if (!C || !fields) { mf3d::set_error("mf3d_newsolv_mg_device: bad arguments"); return MF3D_E_INVALID; }
+  if (int st_lmr = mf3d::lmr_refused(C, "mf3d_newsolv_mg_device")) return st_lmr;
   if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   mf3d::AllocScope scope(C->stream);
@@ -3345,6 +3597,7 @@ int mf3d_newsolv_mg_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, do
 int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk_fields *rk, double dt,
                            double alfapr, int alfabc, int pressureforce, double forcn) {
   using namespace mf3d;
+  if (int st_lmr = mf3d::lmr_refused(C, "mf3d_rungek_2nd_device")) return st_lmr;
   if (!C || !fields || !rk) { set_error("mf3d_rungek_2nd_device: bad arguments"); return MF3D_E_INVALID; }
   if (C->view->dom.size() != 1) { set_error("mf3d_rungek_2nd_device: mf3d_create contexts only"); return MF3D_E_INVALID; }
   if (!C->prm.bounds || C->prm.lsm || C->elem != 8) {
@@ -3418,6 +3671,7 @@ int mf3d_rungek_2nd_device(mf3d_ctx *C, const mf3d_fields *fields, const mf3d_rk
 
 int mf3d_bounds_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr, int alfabc) {
   using namespace mf3d;
+  if (int st_lmr = mf3d::lmr_refused(C, "mf3d_bounds_device")) return st_lmr;
   if (!C || !fields) { set_error("mf3d_bounds_device: bad arguments"); return MF3D_E_INVALID; }
   if (C->view->dom.size() != 1) { set_error("mf3d_bounds_device: mf3d_create contexts only"); return MF3D_E_INVALID; }
   if (!C->prm.bounds || C->elem != 8) {
@@ -3454,6 +3708,7 @@ int mf3d_bounds_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double
 
 int mf3d_calvel_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr) {
   using namespace mf3d;
+  if (int st_lmr = mf3d::lmr_refused(C, "mf3d_calvel_device")) return st_lmr;
   if (!C || !fields) { set_error("mf3d_calvel_device: bad arguments"); return MF3D_E_INVALID; }
   if (C->view->dom.size() != 1) { set_error("mf3d_calvel_device: mf3d_create contexts only"); return MF3D_E_INVALID; }
   if (C->prm.lsm || C->elem != 8) { set_error("mf3d_calvel_device: FP64 contexts without lsm"); return MF3D_E_UNSUPPORTED; }
@@ -3495,6 +3750,7 @@ int mf3d_calvel_device(mf3d_ctx *C, const mf3d_fields *fields, double dt, double
 int mf3d_newsolv_mg(mf3d_ctx *C, const mf3d_fields *fields, double dt, double alfapr, mf3d_solve_info *info,
                     double *hist, int cap) {
   if (!C || !fields) { mf3d::set_error("mf3d_newsolv_mg: bad arguments"); return MF3D_E_INVALID; }
+  if (int st_lmr = mf3d::lmr_refused(C, "mf3d_newsolv_mg")) return st_lmr;
   if (C->view->dom.size() != 1) { mf3d::set_error("a batch context: use mf3d_batch_solve_device"); return MF3D_E_INVALID; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   mf3d::AllocScope scope(C->stream);
@@ -3523,6 +3779,7 @@ int mf3d_mgkcyc_device(mf3d_ctx *C, double *const *su, double *const *pp) {
 
 int mf3d_mgkcyc_device_noalloc(mf3d_ctx *C, double *const *su, double *const *pp) {
   if (!C || !su || !pp) { mf3d::set_error("mf3d_mgkcyc_device_noalloc: bad arguments"); return MF3D_E_INVALID; }
+  if (int st_lmr = mf3d::lmr_refused(C, "mf3d_mgkcyc_device_noalloc")) return st_lmr;
   if (C->prm.lsm) { mf3d::set_error("lsm: the coefficients come from a solve's dens"); return MF3D_E_UNSUPPORTED; }
   if (cudaSetDevice(C->device) != cudaSuccess) { mf3d::set_error("cudaSetDevice failed"); return MF3D_E_CUDA; }
   if (C->elem == 8) return mf3d::mgkcyc_view_noalloc<double>(C, *C->view, su, pp);
@@ -3689,6 +3946,68 @@ long long mf3d_halo_map(const mf3d_block_desc *blocks, int nblocks, int ngrid, i
   if (dst && src)
     for (size_t q = 0; q < pairs.size(); ++q) { dst[q] = pairs[q].dst; src[q] = pairs[q].src; }
   return (long long)pairs.size();
+}
+
+int mf3d_halo_refresh_host(const mf3d_block_desc *blocks, int nblocks, int ngrid, int level, double *const *fi) {
+  if (!blocks || nblocks <= 0 || !fi || ngrid < 1 || level < 1 || level > ngrid) {
+    mf3d::set_error("mf3d_halo_refresh_host: bad arguments");
+    return MF3D_E_INVALID;
+  }
+  try {
+    mf3d_params prm;
+    std::memset(&prm, 0, sizeof prm);
+    prm.ngrid = ngrid;
+    prm.mg_itrsch = 3;
+    prm.pl = 1;
+    prm.differencing = 1;
+    bool lmr = false;
+    std::vector<int> own;
+    std::vector<std::vector<int>> rdv;
+    if (int st = mf3d::lmr_plan(blocks, nblocks, &prm, lmr, own, rdv)) return st;
+    std::vector<mf3d_block_desc> b(blocks, blocks + nblocks);
+    std::vector<mf3d::LevelGeom> geom(nblocks);
+    std::vector<long long> base(nblocks);
+    std::vector<int> rg(nblocks);
+    long long acc = 0;
+    bool mixed = false;
+    for (int q = 0; q < nblocks; ++q) {
+      const int gl = std::min(level, own[q]);
+      geom[q] = mf3d::LevelGeom{b[q].nx >> (gl - 1), b[q].ny >> (gl - 1), b[q].nz >> (gl - 1)};
+      base[q] = acc;
+      acc += geom[q].cells();
+      rg[q] = rdv[q][level];
+      mixed |= rg[q] != rg[0];
+    }
+    auto cell = [&](long long id) -> double & {
+      const int q = (int)(std::upper_bound(base.begin(), base.end(), id) - base.begin()) - 1;
+      return fi[q][id - base[q]];
+    };
+    if (mixed) {
+      // k_lmr_nodes / k_lmr_write on the host
+      const mf3d::LmrProgram P = mf3d::build_halo_lmr(b, geom, base, rg);
+      std::vector<double> val(P.nodes.size());
+      for (size_t n = 0; n < P.nodes.size(); ++n) {
+        const auto &N = P.nodes[n];
+        double t = 0.0;
+        for (int q = 0; q < N.nt; ++q) {
+          const auto &a = P.terms[N.t0 + q];
+          const double x = a.ref >= 0 ? cell(a.ref) : a.ref == mf3d::kLmrZero ? 0.0 : val[(size_t)(-2 - a.ref)];
+          t = q == 0 ? a.w * x : t + a.w * x;
+        }
+        val[n] = t * N.scale;
+      }
+      for (auto &w : P.writes) cell(w.first) = val[w.second];
+    } else {
+      const auto pairs = mf3d::build_halo_map(b, geom, base);
+      std::vector<double> v(pairs.size());
+      for (size_t q = 0; q < pairs.size(); ++q) v[q] = cell(pairs[q].src);
+      for (size_t q = 0; q < pairs.size(); ++q) cell(pairs[q].dst) = v[q];
+    }
+  } catch (const std::exception &e) {
+    mf3d::set_error(std::string("mf3d_halo_refresh_host: ") + e.what());
+    return MF3D_E_OOM;
+  }
+  return MF3D_OK;
 }
 
 long long mf3d_field_exchange_map(const mf3d_block_desc *blocks, int nblocks, int pl, int pl_ex, int op,

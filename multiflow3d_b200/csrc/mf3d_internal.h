@@ -35,6 +35,35 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
                                      const std::vector<LevelGeom> &geom,
                                      const std::vector<long long> &base);
 
+// The same refresh on a level where blocks of different refinement meet
+// (LMR, rdv differing across an interface; exchangepp.for:43-4763).  The
+// values are no longer copies: a refined block's ghosts next to a coarser
+// neighbour are (2 phi_coarse + 3 phi_1 - phi_2) / 4, a coarser block's the
+// 8-cell averages of the refined neighbour, corner and edge ghosts of a
+// refined block trilinear blends of the coarser one's cells.  The map is
+// a program over the state before the exchange: nodes, each a sum
+// w_0 x_0 + w_1 x_1 + ... (in that order, the reference's order) times
+// `scale`, whose terms are cells or earlier nodes, evaluated in order of
+// depth; then every changed ghost cell takes its node's value.  `rdv` is
+// rdv(block, g) of each block at this level (localparameters.for:47-57).
+struct LmrProgram {
+  struct Term {
+    long long ref;  // >= 0: cell id; kLmrZero: the constant 0; <= -2: node (-2 - ref)
+    double w;
+  };
+  struct Node {
+    int t0, nt;     // terms [t0, t0 + nt)
+    double scale;
+  };
+  std::vector<Term> terms;
+  std::vector<Node> nodes;                        // in order of depth
+  std::vector<int> depth_start;                   // nodes of depth d: [depth_start[d-1], depth_start[d])
+  std::vector<std::pair<long long, int>> writes;  // ghost cell id <- node
+};
+constexpr long long kLmrZero = -1;
+LmrProgram build_halo_lmr(const std::vector<mf3d_block_desc> &blocks, const std::vector<LevelGeom> &geom,
+                          const std::vector<long long> &base, const std::vector<int> &rdv);
+
 // exchange(op) on field arrays (exchange.for:2-23: exchange_bc on the
 // periodic faces, then exchange_smlvl with its corners, edges and faces),
 // and pbound after it when `with_pbound` (press.for:77-137), as pairs

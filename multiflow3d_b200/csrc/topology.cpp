@@ -265,6 +265,53 @@ void mgbound_tokens(TokenLevel &T) {
   }
 }
 
+// exchbc_mgpp (exchangepp.for:4768-5383) on tokens: x, y, z; in-block wraps
+// are immediate, partner copies are packed from the axis-start state and
+// unpacked afterwards.
+void exchbc_tokens(TokenLevel &T) {
+  const std::vector<mf3d_block_desc> &blocks = T.blk;
+  const std::vector<LevelGeom> &geom = T.geom;
+  const int nb = (int)blocks.size();
+  // exchbc_mgpp: x, y, z; in-block wraps are immediate, partner copies
+  // are packed from the axis-start state and unpacked afterwards.
+  for (int ax = 0; ax < 3; ++ax) {
+    AxisView V{ax};
+    Phase ph;
+    for (int p = 0; p < nb; ++p) {
+      const auto &d = blocks[p];
+      int bcp = ax == 0 ? d.bc_west : ax == 1 ? d.bc_south : d.bc_bottom;
+      int bcn = ax == 0 ? d.bc_east : ax == 1 ? d.bc_north : d.bc_top;
+      if (!(bcp == 5 || bcn == 5)) continue;
+      const LevelGeom &g = geom[p];
+      int nA = ax == 0 ? g.nx : ax == 1 ? g.ny : g.nz;
+      int n1 = ax == 0 ? g.ny : g.nx, n2 = ax == 2 ? g.ny : g.nz;
+      int prev = ax == 0 ? d.iprev : ax == 1 ? d.jprev : d.kprev;
+      int next = ax == 0 ? d.inext : ax == 1 ? d.jnext : d.knext;
+      int perp = ax == 0 ? d.per_ip : ax == 1 ? d.per_jp : d.per_kp;
+      int pern = ax == 0 ? d.per_in : ax == 1 ? d.per_jn : d.per_kn;
+      if (prev < 0 && next < 0) {
+        for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+          T.set(V.at(T, p, 0, s, t), T.get(V.at(T, p, nA, s, t)));
+        for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+          T.set(V.at(T, p, nA + 1, s, t), T.get(V.at(T, p, 1, s, t)));
+        continue;
+      }
+      if (prev < 0 && next >= 0 && perp >= 0) {
+        int q = T.P(perp);
+        int nAq = ax == 0 ? geom[q].nx : ax == 1 ? geom[q].ny : geom[q].nz;
+        for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+          ph.add(V.at(T, p, 0, s, t), V.at(T, q, nAq, s, t));
+      }
+      if (next < 0 && prev >= 0 && pern >= 0) {
+        int q = T.P(pern);
+        for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+          ph.add(V.at(T, p, nA + 1, s, t), V.at(T, q, 1, s, t));
+      }
+    }
+    ph.apply(T);
+  }
+}
+
 }  // namespace
 
 std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
@@ -357,46 +404,7 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
     ph.apply(T);
   }
   mgbound_tokens(T);
-  if (periodic) {
-    // exchbc_mgpp: x, y, z; in-block wraps are immediate, partner copies
-    // are packed from the axis-start state and unpacked afterwards.
-    for (int ax = 0; ax < 3; ++ax) {
-      AxisView V{ax};
-      Phase ph;
-      for (int p = 0; p < nb; ++p) {
-        const auto &d = blocks[p];
-        int bcp = ax == 0 ? d.bc_west : ax == 1 ? d.bc_south : d.bc_bottom;
-        int bcn = ax == 0 ? d.bc_east : ax == 1 ? d.bc_north : d.bc_top;
-        if (!(bcp == 5 || bcn == 5)) continue;
-        const LevelGeom &g = geom[p];
-        int nA = ax == 0 ? g.nx : ax == 1 ? g.ny : g.nz;
-        int n1 = ax == 0 ? g.ny : g.nx, n2 = ax == 2 ? g.ny : g.nz;
-        int prev = ax == 0 ? d.iprev : ax == 1 ? d.jprev : d.kprev;
-        int next = ax == 0 ? d.inext : ax == 1 ? d.jnext : d.knext;
-        int perp = ax == 0 ? d.per_ip : ax == 1 ? d.per_jp : d.per_kp;
-        int pern = ax == 0 ? d.per_in : ax == 1 ? d.per_jn : d.per_kn;
-        if (prev < 0 && next < 0) {
-          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
-            T.set(V.at(T, p, 0, s, t), T.get(V.at(T, p, nA, s, t)));
-          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
-            T.set(V.at(T, p, nA + 1, s, t), T.get(V.at(T, p, 1, s, t)));
-          continue;
-        }
-        if (prev < 0 && next >= 0 && perp >= 0) {
-          int q = T.P(perp);
-          int nAq = ax == 0 ? geom[q].nx : ax == 1 ? geom[q].ny : geom[q].nz;
-          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
-            ph.add(V.at(T, p, 0, s, t), V.at(T, q, nAq, s, t));
-        }
-        if (next < 0 && prev >= 0 && pern >= 0) {
-          int q = T.P(pern);
-          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
-            ph.add(V.at(T, p, nA + 1, s, t), V.at(T, q, 1, s, t));
-        }
-      }
-      ph.apply(T);
-    }
-  }
+  if (periodic) exchbc_tokens(T);
   // changed shell cells, in increasing cell id
   std::vector<HaloPair> out;
   for (int p : T.order) {
@@ -411,6 +419,243 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
           const long long c = T.id(p, i, j, k), v = T.shell[p][TokenLevel::sidx(G, i, j, k)];
           if (v != c) out.push_back({c, v});
         }
+  }
+  return out;
+}
+
+// ---------------------------------------------------------------------------
+// The refresh of a level with refinement interfaces (LMR).  Tokens are cell
+// ids (the value the cell held before the exchange) or nodes: weighted sums
+// of tokens built when a phase starts.  Each sync_dir is one phase: the
+// reference packs every block's buffers from the state at the start of the
+// phase and unpacks them afterwards, and an unpack formula reads only cells
+// that no unpack of the same phase writes (a refined block's interior layers
+// next to the face; its ghost rows of the other axes).  So every value of
+// the phase is a function of the phase-start state, and later entries win.
+// The cases, from the receiving block p and its neighbour q (exchangepp.for
+// lines of the sender's pack and the receiver's unpack):
+//   rdv equal:            copy of q's cell (as build_halo_map);
+//   p finer than q, face: (2 phi_q + 3 phi_p(1 in) - phi_p(2 in)) / 4 on the
+//                         whole ghost plane (:174-187, :4046-4056); the
+//                         plane's ring rows receive no coarse value - the
+//                         buffer entries the coarse sender never writes,
+//                         taken as 0 here;
+//   p coarser, face:      0.125 * (8 cells of q), q's two layers next to p,
+//                         tangential pairs, the buffer's fast axis first and
+//                         the normal last (:163-172), on the plane's interior
+//                         (:4057-4063);
+//   p coarser, corner/edge: (8 cells of q) / 8 in j, i, k order (:448-452,
+//                         :652-656);
+//   p finer, corner/edge: (27 c + 9 c_j + 9 c_i + 3 c_ij + 9 c_k + 3 c_jk +
+//                         3 c_ik + 1 c_ijk) / 64 from q's cell c toward p
+//                         (:454-460, :658-669), along an edge toward the fine
+//                         cell's half of c.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct LmrNodeR {
+  std::vector<std::pair<long long, double>> t;  // (token, weight)
+  double scale;
+};
+
+struct LmrReplay {
+  TokenLevel &T;
+  const std::vector<int> &rdv;
+  std::vector<LmrNodeR> nodes;
+  static long long node_token(size_t n) { return -2 - (long long)n; }
+  long long make(std::vector<std::pair<long long, double>> t, double scale) {
+    nodes.push_back(LmrNodeR{std::move(t), scale});
+    return node_token(nodes.size() - 1);
+  }
+  // cell of the face plane of axis ax: a along the axis, (s, t) the
+  // reference buffer's axes (ijk = (t-1)*ns1 + s): x (j, k), y (i, k), z (j, i)
+  long long fcell(int p, int ax, int a, int s, int t) const {
+    if (ax == 0) return T.id(p, a, s, t);
+    if (ax == 1) return T.id(p, s, a, t);
+    return T.id(p, t, s, a);
+  }
+  int nax(int p, int a) const { return a == 0 ? T.geom[p].nx : a == 1 ? T.geom[p].ny : T.geom[p].nz; }
+};
+
+}  // namespace
+
+LmrProgram build_halo_lmr(const std::vector<mf3d_block_desc> &blocks, const std::vector<LevelGeom> &geom,
+                          const std::vector<long long> &base, const std::vector<int> &rdv) {
+  TokenLevel T(blocks, geom, base);
+  LmrReplay R{T, rdv, {}};
+  const int nb = (int)blocks.size();
+  mgbound_tokens(T);  // mgrelax's mgbound before exchangepp (mgsolver.for:610-611)
+  bool periodic = false;
+  for (const auto &d : blocks)
+    if (d.bc_west == 5 || d.bc_east == 5 || d.bc_south == 5 || d.bc_north == 5 || d.bc_bottom == 5 || d.bc_top == 5)
+      periodic = true;
+  using Terms = std::vector<std::pair<long long, double>>;
+  for (int ax = 0; ax < 3; ++ax) {
+    std::vector<std::pair<long long, long long>> ph;  // (dst, token), in unpack order
+    for (int p = 0; p < nb; ++p) {
+      const auto &d = blocks[p];
+      const int nA = R.nax(p, ax);
+      const int n1 = ax == 1 ? geom[p].nx : geom[p].ny;  // s extent
+      const int n2 = ax == 2 ? geom[p].nx : geom[p].nz;  // t extent
+      const int nbr[2] = {ax == 0 ? d.iprev : ax == 1 ? d.jprev : d.kprev, ax == 0 ? d.inext : ax == 1 ? d.jnext : d.knext};
+      for (int side = 0; side < 2; ++side) {
+        if (nbr[side] < 0) continue;
+        const int q = T.P(nbr[side]);
+        const int nAq = R.nax(q, ax);
+        const int ga = side ? nA + 1 : 0;         // p's ghost plane
+        const int a1 = side ? nA : 1, a2 = side ? nA - 1 : 2;  // p's first two layers inward
+        const int qa = side ? 1 : nAq;            // q's layer next to p
+        const int qa0 = side ? 1 : nAq - 1;       // the first of q's two layers next to p
+        if (rdv[p] == rdv[q]) {
+          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s)
+            ph.push_back({R.fcell(p, ax, ga, s, t), T.get(R.fcell(q, ax, qa, s, t))});
+        } else if (rdv[p] > rdv[q]) {
+          for (int t = 0; t <= n2 + 1; ++t) for (int s = 0; s <= n1 + 1; ++s) {
+            const bool in = s >= 1 && s <= n1 && t >= 1 && t <= n2;
+            const long long recv =
+                in ? R.make(Terms{{T.get(R.fcell(q, ax, qa, (s + 1) / 2, (t + 1) / 2)), 2.0}}, 1.0) : kLmrZero;
+            ph.push_back({R.fcell(p, ax, ga, s, t),
+                          R.make(Terms{{recv, 1.0}, {T.get(R.fcell(p, ax, a1, s, t)), 3.0},
+                                       {T.get(R.fcell(p, ax, a2, s, t)), -1.0}},
+                                 0.25)});
+          }
+        } else {
+          for (int t = 1; t <= n2; ++t) for (int s = 1; s <= n1; ++s) {
+            Terms tt;
+            for (int da = 0; da < 2; ++da) for (int dt = 0; dt < 2; ++dt) for (int ds = 0; ds < 2; ++ds)
+              tt.push_back({T.get(R.fcell(q, ax, qa0 + da, 2 * s - 1 + ds, 2 * t - 1 + dt)), 1.0});
+            ph.push_back({R.fcell(p, ax, ga, s, t), R.make(std::move(tt), 0.125)});
+          }
+        }
+      }
+      if (ax != 2) continue;
+      // corners and edges, after the faces: prev corners #1..4, prev edges
+      // #1..6, next corners, next edges (exchangepp.for:4433-4755)
+      const int n3[3] = {geom[p].nx, geom[p].ny, geom[p].nz};
+      auto ghost = [&](int e, int a, int m) { return e < 0 ? 0 : e > 0 ? n3[a] + 1 : m; };
+      // the value p receives from q in direction D (p toward q); m: index
+      // along an edge (0 for a corner); E = -D points from q toward p
+      auto from = [&](int q, const int D[3], int m) -> long long {
+        const int E[3] = {-D[0], -D[1], -D[2]};
+        const int nq[3] = {R.nax(q, 0), R.nax(q, 1), R.nax(q, 2)};
+        int c[3];
+        if (rdv[p] == rdv[q]) {
+          for (int a = 0; a < 3; ++a) c[a] = E[a] > 0 ? nq[a] : E[a] < 0 ? 1 : m;
+          return T.get(T.id(q, c[0], c[1], c[2]));
+        }
+        if (rdv[q] > rdv[p]) {  // q finer: its 2x2x2 cells next to p
+          int lo[3];
+          for (int a = 0; a < 3; ++a) lo[a] = E[a] > 0 ? nq[a] - 1 : E[a] < 0 ? 1 : 2 * m - 1;
+          Terms tt;
+          for (int dk = 0; dk < 2; ++dk) for (int di = 0; di < 2; ++di) for (int dj = 0; dj < 2; ++dj)
+            tt.push_back({T.get(T.id(q, lo[0] + di, lo[1] + dj, lo[2] + dk)), 1.0});
+          return R.make(std::move(tt), 0.125);
+        }
+        // q coarser: from its cell next to p toward p; along an edge toward
+        // the half of the coarse cell that holds p's cell m
+        int o[3];
+        for (int a = 0; a < 3; ++a) {
+          c[a] = E[a] > 0 ? nq[a] : E[a] < 0 ? 1 : (m + 1) / 2;
+          o[a] = E[a] != 0 ? E[a] : ((m & 1) ? -1 : +1);
+        }
+        Terms tt;
+        for (int b = 0; b < 8; ++b) {
+          const int oj = (b & 1) ? o[1] : 0, oi = (b & 2) ? o[0] : 0, ok = (b & 4) ? o[2] : 0;
+          const int pc = ((b & 1) != 0) + ((b & 2) != 0) + ((b & 4) != 0);
+          tt.push_back({T.get(T.id(q, c[0] + oi, c[1] + oj, c[2] + ok)), pc == 0 ? 27.0 : pc == 1 ? 9.0 : pc == 2 ? 3.0 : 1.0});
+        }
+        return R.make(std::move(tt), 1.0 / 64.0);
+      };
+      const int cp[4][2] = {{-1, -1}, {-1, +1}, {+1, +1}, {+1, -1}};
+      const int cn[4][2] = {{+1, +1}, {+1, -1}, {-1, -1}, {-1, +1}};
+      const int edp[6][3] = {{-1, 0, -1}, {0, +1, -1}, {+1, 0, -1}, {0, -1, -1}, {-1, -1, 0}, {-1, +1, 0}};
+      const int edn[6][3] = {{+1, 0, +1}, {0, -1, +1}, {-1, 0, +1}, {0, +1, +1}, {+1, +1, 0}, {+1, -1, 0}};
+      for (int side = 0; side < 2; ++side) {
+        for (int c = 0; c < 4; ++c) {
+          const int id = side ? d.cornext[c] : d.corprev[c];
+          if (id < 0) continue;
+          const int D[3] = {side ? cn[c][0] : cp[c][0], side ? cn[c][1] : cp[c][1], side ? +1 : -1};
+          ph.push_back({T.id(p, ghost(D[0], 0, 0), ghost(D[1], 1, 0), ghost(D[2], 2, 0)), from(T.P(id), D, 0)});
+        }
+        for (int e = 0; e < 6; ++e) {
+          const int id = side ? d.edgnext[e] : d.edgprev[e];
+          if (id < 0) continue;
+          const int *D = side ? edn[e] : edp[e];
+          const int ax_e = D[0] == 0 ? 0 : D[1] == 0 ? 1 : 2;
+          for (int m = 1; m <= n3[ax_e]; ++m)
+            ph.push_back({T.id(p, ghost(D[0], 0, m), ghost(D[1], 1, m), ghost(D[2], 2, m)), from(T.P(id), D, m)});
+        }
+      }
+    }
+    for (auto &w : ph) T.set(w.first, w.second);
+  }
+  mgbound_tokens(T);
+  if (periodic) exchbc_tokens(T);
+  // the changed shell cells and the nodes they reach, ordered by depth
+  std::vector<std::pair<long long, long long>> fin;  // (cell, token)
+  for (int p : T.order) {
+    const LevelGeom &G = geom[p];
+    for (int k = 0; k <= G.nz + 1; ++k)
+      for (int j = 0; j <= G.ny + 1; ++j)
+        for (int i = 0; i <= G.nx + 1; ++i) {
+          if (!TokenLevel::on_shell(G, i, j, k)) {
+            i = G.nx;
+            continue;
+          }
+          const long long c = T.id(p, i, j, k), v = T.shell[p][TokenLevel::sidx(G, i, j, k)];
+          if (v != c) fin.push_back({c, v});
+        }
+  }
+  const size_t nn = R.nodes.size();
+  std::vector<int> depth(nn, 0);  // 0 = not reached
+  // nodes only refer to earlier nodes, so one backward pass marks the reached
+  // ones and a forward pass gives each its depth
+  std::vector<char> reached(nn, 0);
+  for (auto &f : fin)
+    if (f.second <= -2) reached[(size_t)(-2 - f.second)] = 1;
+  for (size_t n = nn; n-- > 0;)
+    if (reached[n])
+      for (auto &t : R.nodes[n].t)
+        if (t.first <= -2) reached[(size_t)(-2 - t.first)] = 1;
+  int dmax = 1;
+  for (size_t n = 0; n < nn; ++n) {
+    if (!reached[n]) continue;
+    int dd = 1;
+    for (auto &t : R.nodes[n].t)
+      if (t.first <= -2) dd = std::max(dd, depth[(size_t)(-2 - t.first)] + 1);
+    depth[n] = dd;
+    dmax = std::max(dmax, dd);
+  }
+  LmrProgram out;
+  // copies of pre-exchange cells become one-term nodes of depth 1
+  std::vector<long long> copy_of;
+  for (auto &f : fin)
+    if (f.second >= 0) copy_of.push_back(f.second);
+  std::sort(copy_of.begin(), copy_of.end());
+  copy_of.erase(std::unique(copy_of.begin(), copy_of.end()), copy_of.end());
+  std::vector<int> newid(nn, -1);
+  out.depth_start.push_back(0);
+  for (int dd = 1; dd <= dmax; ++dd) {
+    if (dd == 1)
+      for (long long c : copy_of) {
+        out.nodes.push_back(LmrProgram::Node{(int)out.terms.size(), 1, 1.0});
+        out.terms.push_back(LmrProgram::Term{c, 1.0});
+      }
+    for (size_t n = 0; n < nn; ++n) {
+      if (!reached[n] || depth[n] != dd) continue;
+      newid[n] = (int)out.nodes.size();
+      out.nodes.push_back(LmrProgram::Node{(int)out.terms.size(), (int)R.nodes[n].t.size(), R.nodes[n].scale});
+      for (auto &t : R.nodes[n].t)
+        out.terms.push_back(LmrProgram::Term{t.first <= -2 ? -2 - (long long)newid[(size_t)(-2 - t.first)] : t.first,
+                                             t.second});
+    }
+    out.depth_start.push_back((int)out.nodes.size());
+  }
+  for (auto &f : fin) {
+    int node;
+    if (f.second >= 0) node = (int)(std::lower_bound(copy_of.begin(), copy_of.end(), f.second) - copy_of.begin());
+    else node = newid[(size_t)(-2 - f.second)];
+    out.writes.push_back({f.first, node});
   }
   return out;
 }

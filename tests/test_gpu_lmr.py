@@ -1,0 +1,108 @@
+"""GPU parity of the V-cycle across LMR 2:1 refinement interfaces.
+
+mf3d_mgkcyc_device on layouts whose blocks differ in refinement (rdiv 1
+and 2) against the oracle's mgkcyc: the levels past a block's own last
+(injection and whole-array correction, mgsolver.for:714-727, 806-818) and
+the fine/coarse exchangepp branches.  FP64, bit for bit on pp's interior
+and first ghost layer.  The ring entries of a fine block's face buffer are
+0 on both sides; the L-shaped layout, where the V-cycle reads them, also
+shows the cells that do not depend on them (the oracle run with another
+ring value).
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle_bridge as ob
+from lmr_layouts import LmrLayout
+from multiflow3d_b200.problems import PERIODIC, WALL
+from multiflow3d_b200.solver import Projection
+
+pytestmark = pytest.mark.gpu
+
+ALL_WALLS = (WALL,) * 6
+
+LAYOUTS = [
+    dict(px=2, py=1, pz=1, n=8, refine=[1], bc=ALL_WALLS),
+    dict(px=2, py=2, pz=2, n=8, refine=[0], bc=ALL_WALLS),
+    dict(px=2, py=2, pz=2, n=8, refine=[3, 4], bc=ALL_WALLS),
+    dict(px=3, py=2, pz=1, n=8, refine=[1, 4], bc=(WALL, WALL, PERIODIC, PERIODIC, WALL, WALL)),
+    dict(px=2, py=2, pz=1, n=8, refine=[0], bc=ALL_WALLS, drop=((1, 1, 0),)),
+    dict(px=2, py=1, pz=1, n=32, refine=[0], bc=ALL_WALLS),
+]
+
+
+def run_pair(lib, oracle, cuda, L, scheme, seed=42, ring=0.0):
+    import torch
+    prm = L.params(mg_itrsch=scheme)
+    rng = np.random.default_rng(seed)
+    su = [rng.uniform(-1, 1, size=L.ttc(b)) for b in range(L.nblocks)]
+    pp_ref = [np.zeros(L.ttc(b)) for b in range(L.nblocks)]
+    oracle.orc_set_lmr_ring.argtypes = [C.c_double]
+    oracle.orc_set_lmr_ring(ring)
+    try:
+        assert oracle.orc_mgkcyc(L.descriptors(oracle), L.nblocks, C.byref(prm), ob.ptr_array(su),
+                                 ob.ptr_array(pp_ref)) == 0
+    finally:
+        oracle.orc_set_lmr_ring(0.0)
+    proj = Projection(L.descriptors(lib), prm, lib)
+    su_d = [torch.from_numpy(a).to(cuda) for a in su]
+    pp_d = [torch.zeros(L.ttc(b), dtype=torch.float64, device=cuda) for b in range(L.nblocks)]
+    proj.mgkcyc_device(su_d, pp_d)
+    launches = proj.launches
+    proj.close()
+    pl = L.pl
+    got, ref = [], []
+    for b in range(L.nblocks):
+        nx, ny, nz = L.cells(b)
+        s = (slice(pl - 1, pl + nz + 1), slice(pl - 1, pl + ny + 1), slice(pl - 1, pl + nx + 1))
+        got.append(pp_d[b].cpu().numpy()[s])
+        ref.append(pp_ref[b][s])
+    return got, ref, launches
+
+
+@pytest.mark.parametrize("scheme", [3, 1, 2])
+@pytest.mark.parametrize("lay", LAYOUTS, ids=lambda d: f"{d['px']}x{d['py']}x{d['pz']}-n{d['n']}-ref{d['refine']}"
+                         + ("-L" if d.get("drop") else ""))
+def test_lmr_vcycle_bitwise(lib, oracle, cuda, lay, scheme):
+    L = LmrLayout(lay["px"], lay["py"], lay["pz"], lay["n"], lay["refine"], lay["bc"], 3, drop=lay.get("drop", ()))
+    got, ref, launches = run_pair(lib, oracle, cuda, L, scheme)
+    assert launches > 0
+    for b in range(L.nblocks):
+        assert np.array_equal(got[b], ref[b]), f"block {b}: max diff {np.abs(got[b] - ref[b]).max()}"
+
+
+def test_lmr_ring_independent_cells(lib, oracle, cuda):
+    """On the L-shaped layout with the refined block at the re-entrant edge,
+    the V-cycle reads the ring entries: the device equals the oracle with
+    ring 0 on every cell, and the cells where the oracle with ring 1e3
+    agrees (those that do not depend on the ring) are most of the domain."""
+    L = LmrLayout(2, 2, 1, 8, [0], ALL_WALLS, 3, drop=((1, 1, 0),))
+    got, ref, _ = run_pair(lib, oracle, cuda, L, 3)
+    _, ref2, _ = run_pair(lib, oracle, cuda, L, 3, ring=1.0e3)
+    dep = tot = 0
+    for b in range(L.nblocks):
+        assert np.array_equal(got[b], ref[b])
+        same = ref[b] == ref2[b]
+        assert np.array_equal(got[b][same], ref2[b][same])
+        dep += int((~same).sum())
+        tot += same.size
+    assert 0 < dep < tot // 2
+
+
+def test_lmr_refusals(lib, cuda):
+    """The outer loop refuses an LMR context (its field exchanges at
+    refinement interfaces are not restated); FP32 and neighbours more than
+    2:1 apart are refused at create."""
+    import torch
+    from multiflow3d_b200 import abi
+    L = LmrLayout(2, 1, 1, 8, [1], ALL_WALLS, 3)
+    proj = Projection(L.descriptors(lib), L.params(), lib)
+    fields = [{k: torch.zeros(L.ttc(b), dtype=torch.float64, device=cuda)
+               for k in ("u", "v", "w", "p", "pp", "su", "ustar", "vstar", "wstar")} for b in range(L.nblocks)]
+    with pytest.raises(RuntimeError, match="LMR"):
+        proj.newsolv_mg_device(fields)
+    proj.close()
+    with pytest.raises(RuntimeError):
+        Projection(L.descriptors(lib), L.params(precision=abi.MF3D_PREC_FP32), lib)

@@ -261,3 +261,35 @@ def test_lmr_refusals(orc):
     su = [np.zeros((8 + 4,) * 3), np.zeros((32 + 4,) * 3)]
     pp = [np.zeros_like(a) for a in su]
     assert orc.orc_mgkcyc(d4, 2, C.byref(prm4), ob.ptr_array(su), ob.ptr_array(pp)) != 0
+
+
+HOST_LAYOUTS = [
+    dict(px=2, py=1, pz=1, refine=[1], bc=ALL_WALLS),
+    dict(px=2, py=2, pz=2, refine=[0], bc=ALL_WALLS),
+    dict(px=2, py=2, pz=2, refine=[3, 4], bc=ALL_WALLS),
+    dict(px=2, py=2, pz=1, refine=[0], bc=ALL_WALLS, drop=((1, 1, 0),)),
+    dict(px=3, py=2, pz=1, refine=[1, 4], bc=(WALL, WALL, PERIODIC, PERIODIC, WALL, WALL)),
+]
+
+
+@pytest.mark.parametrize("lay", HOST_LAYOUTS)
+def test_library_lmr_refresh_matches_oracle(lib, orc, lay):
+    """The library's halo refresh (its LMR program evaluated on the host with
+    the device kernels' arithmetic, mf3d_halo_refresh_host) against the
+    oracle's mgbound + exchangepp, bit for bit, on every level of LMR
+    layouts - walls, an L-shaped domain (the ring entries read as 0 on both
+    sides), periodic partners of equal refinement."""
+    L = LmrLayout(lay["px"], lay["py"], lay["pz"], 8, lay["refine"], lay["bc"], 3, drop=lay.get("drop", ()))
+    dl, do = L.descriptors(lib), L.descriptors(orc)
+    rng = np.random.default_rng(11)
+    for g in range(1, L.ngrid + 1):
+        a = []
+        for b in range(L.nblocks):
+            (nx, ny, nz), _ = level_dims(L, b, g)
+            a.append(rng.uniform(-1, 1, size=(nz + 2, ny + 2, nx + 2)))
+        mine = [np.ascontiguousarray(x.copy()) for x in a]
+        ref = [np.ascontiguousarray(x.copy()) for x in a]
+        assert lib.mf3d_halo_refresh_host(dl, L.nblocks, L.ngrid, g, ob.ptr_array(mine)) == 0
+        assert orc.orc_exchangepp(do, L.nblocks, L.ngrid, g, ob.ptr_array(ref)) == 0
+        for b in range(L.nblocks):
+            assert np.array_equal(mine[b], ref[b]), f"level {g} block {b}: {np.argwhere(mine[b] != ref[b])[:5]}"
