@@ -188,7 +188,19 @@ int mf3d_build_topology(int nblocks, const double *extents, const int *bc6,
 /* Allocate device state for a solve over `nblocks` blocks: the multigrid
  * hierarchy (replaces `coeff`, mgsolver.for:2-222, and the `cof` storage of
  * localparameters.for:208-237), halo maps, field mirrors and streams.
- * Checks the divisibility rule of localparameters.for:200-206. */
+ * Checks the divisibility rule of localparameters.for:200-206.
+ *
+ * LMR (2:1 refinement, localparameters.for:26-102): blocks whose spacings
+ * differ by powers of two.  A block's rdiv is the coarsest block's dx over
+ * its own; a refined block is given with rdiv times the cells over the
+ * same extents.  params.ngrid is then ngrd_gl = ngrid_input + log2(max
+ * rdiv); a block keeps ngrid_input + log2(rdiv) levels of its own size and
+ * must be divisible by 2^(that - 1).  Neighbours may differ by 2:1 at most
+ * and periodic partners not at all (alloc_dom.for:12-230).  FP64, uniform
+ * spacing, no lsm, bounds or solver 1 (MF3D_E_UNSUPPORTED otherwise).  Such
+ * a context runs mf3d_mgkcyc_device only: the outer loop's field exchanges
+ * at refinement interfaces are not restated, and the other entry points
+ * return MF3D_E_UNSUPPORTED. */
 int mf3d_create(const mf3d_block_desc *blocks, int nblocks,
                 const mf3d_params *params, mf3d_ctx **ctx);
 
@@ -358,7 +370,12 @@ int mf3d_batch_solve_device(mf3d_ctx *ctx, const mf3d_fields *fields,
 /* One V-cycle (mgkcyc, mgsolver.for:224-369) on device arrays: reads the
  * RHS `su` and writes the correction `pp` of each block, both in the ttc
  * layout (pp including its first ghost layer, mgsolver.for:351-364). The
- * V-cycle starts from pp = 0 as newsolv_mg.for:19-21 and :44 leave it. */
+ * V-cycle starts from pp = 0 as newsolv_mg.for:19-21 and :44 leave it.
+ * On an LMR context it runs the reference's LMR branches: levels past a
+ * block's own keep its size (injection in mgrestr, whole-array addition in
+ * mgcorr), and exchangepp's fine/coarse cases across refinement interfaces;
+ * the entries of a refined block's face buffer that no coarse sender
+ * writes (the reference leaves them to earlier exchanges) read as 0. */
 int mf3d_mgkcyc_device(mf3d_ctx *ctx, double *const *su, double *const *pp);
 
 /* mf3d_mgkcyc_device that allocates nothing: no cudaMalloc, no cudaFree,
