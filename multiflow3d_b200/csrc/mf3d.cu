@@ -1158,7 +1158,7 @@ static int rtma_tiles(const mf3d_ctx *C, const std::vector<BlkLev> &tab, const s
     const long long resident = (long long)C->nsm * 2;
     kch = 2;
     double best_cost = 1e300;
-    for (int kc : {2, 4, 8, 16}) {
+    for (int kc : {2, 4, 8, 16, 32}) {
       long long n = 0;
       for (int b : blocks) {
         const BlkLev &B = tab[b];
@@ -2264,13 +2264,13 @@ static int autotune_restrict(mf3d_ctx *C, View &V, int g, bool time_new) {
   int v, st;
   if (tune_get(kr, v)) return set_kch(v);
   if (!time_new) return MF3D_OK;
-  static const int kch_of[4] = {2, 4, 8, 16};
+  static const int kch_of[5] = {2, 4, 8, 16, 32};
   int def = 0;
-  for (int c = 0; c < 4; ++c)
+  for (int c = 0; c < 5; ++c)
     if (kch_of[c] == L.rtma_kch) def = c;  // the wave model's choice (rtma_tiles)
   int pick;
   if ((st = tune_pick(
-           C, 4, def, [&](int c) { return set_kch(kch_of[c]); },
+           C, 5, def, [&](int c) { return set_kch(kch_of[c]); },
            [&] {
              if (f64) restr<double, double>(C, V, g - 1);
              else if (c64) restr<float, double>(C, V, g - 1);

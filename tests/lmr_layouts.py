@@ -13,9 +13,12 @@ from multiflow3d_b200.abi import BlockDesc, Params
 
 
 class LmrLayout:
+    """`refine`: block positions of rdiv 2, or a dict position -> rdiv."""
+
     def __init__(self, px, py, pz, n, refine, bc, ngrid_in, pl=2, drop=()):
         self.px, self.py, self.pz, self.n = px, py, pz, n
-        self.refine = sorted(refine)
+        self.rdiv = dict(refine) if isinstance(refine, dict) else {b: 2 for b in refine}
+        self.refine = sorted(self.rdiv)
         self.bc = tuple(bc)
         # grid positions (i, j, k) of the blocks, x fastest; `drop` leaves
         # some out (an L-shaped domain has a re-entrant edge)
@@ -23,7 +26,8 @@ class LmrLayout:
         self.nblocks = len(self.pos)
         self.pl = pl
         # ngrd_gl = ngrid_input + log2(max rdiv) (localparameters.for:33-34)
-        self.ngrid = ngrid_in + (1 if self.refine else 0)
+        self.ngrid_in = ngrid_in
+        self.ngrid = ngrid_in + max([0] + [r.bit_length() - 1 for r in self.rdiv.values()])
         self.h = 1.0 / n
 
     def extents(self):
@@ -37,15 +41,18 @@ class LmrLayout:
                 C.c_double(self.h), C.c_double(self.h), C.c_double(self.h), arr)
         if st != 0:
             raise RuntimeError(f"topology build failed: {st}")
-        for b in self.refine:
+        for b, r in self.rdiv.items():
             d = arr[b]
-            d.nx, d.ny, d.nz = 2 * d.nx, 2 * d.ny, 2 * d.nz
-            d.dx, d.dy, d.dz = d.dx / 2, d.dy / 2, d.dz / 2
+            d.nx, d.ny, d.nz = r * d.nx, r * d.ny, r * d.nz
+            d.dx, d.dy, d.dz = d.dx / r, d.dy / r, d.dz / r
         return arr
 
     def cells(self, b):
-        r = 2 if b in self.refine else 1
-        return (self.n * r,) * 3
+        return (self.n * self.rdiv.get(b, 1),) * 3
+
+    def own_levels(self, b):
+        """Levels of the block's own size: ngrid_input + log2(rdiv)."""
+        return self.ngrid_in + self.rdiv.get(b, 1).bit_length() - 1
 
     def ttc(self, b):
         nx, ny, nz = self.cells(b)

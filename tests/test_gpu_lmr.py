@@ -3,7 +3,8 @@
 mf3d_mgkcyc_device on layouts whose blocks differ in refinement (rdiv 1
 and 2) against the oracle's mgkcyc: the levels past a block's own last
 (injection and whole-array correction, mgsolver.for:714-727, 806-818) and
-the fine/coarse exchangepp branches.  FP64, bit for bit on pp's interior
+the fine/coarse exchangepp branches; also a chain of rdiv 1, 2 and 4, whose
+finest block halves its refinement on its extra levels.  FP64, bit for bit on pp's interior
 and first ghost layer.  The ring entries of a fine block's face buffer are
 0 on both sides; the L-shaped layout, where the V-cycle reads them, also
 shows the cells that do not depend on them (the oracle run with another
@@ -30,6 +31,7 @@ LAYOUTS = [
     dict(px=3, py=2, pz=1, n=8, refine=[1, 4], bc=(WALL, WALL, PERIODIC, PERIODIC, WALL, WALL)),
     dict(px=2, py=2, pz=1, n=8, refine=[0], bc=ALL_WALLS, drop=((1, 1, 0),)),
     dict(px=2, py=1, pz=1, n=32, refine=[0], bc=ALL_WALLS),
+    dict(px=3, py=1, pz=1, n=8, refine={1: 2, 2: 4}, bc=ALL_WALLS),  # rdiv 1 | 2 | 4
 ]
 
 
@@ -63,8 +65,8 @@ def run_pair(lib, oracle, cuda, L, scheme, seed=42, ring=0.0):
 
 
 @pytest.mark.parametrize("scheme", [3, 1, 2])
-@pytest.mark.parametrize("lay", LAYOUTS, ids=lambda d: f"{d['px']}x{d['py']}x{d['pz']}-n{d['n']}-ref{d['refine']}"
-                         + ("-L" if d.get("drop") else ""))
+@pytest.mark.parametrize("lay", LAYOUTS, ids=lambda d: f"{d['px']}x{d['py']}x{d['pz']}-n{d['n']}-ref"
+                         + "-".join(map(str, d['refine'])) + ("-L" if d.get("drop") else ""))
 def test_lmr_vcycle_bitwise(lib, oracle, cuda, lay, scheme):
     L = LmrLayout(lay["px"], lay["py"], lay["pz"], lay["n"], lay["refine"], lay["bc"], 3, drop=lay.get("drop", ()))
     got, ref, launches = run_pair(lib, oracle, cuda, L, scheme)

@@ -40,9 +40,8 @@ def orc():
 
 def level_dims(L, b, g):
     """Interior cells of block b on level g: clamped to the block's own
-    last level (ngrid_input levels for rdiv 1, one more for rdiv 2)."""
-    own = L.ngrid - 1 + (1 if b in L.refine else 0)
-    gl = min(g, own)
+    last level (ngrid_input + log2(rdiv) levels)."""
+    gl = min(g, L.own_levels(b))
     return tuple(n >> (gl - 1) for n in L.cells(b)), gl
 
 
@@ -50,7 +49,7 @@ def centres(L, b, g):
     """Cell-centre coordinates (x, y, z) of block b's ghost-inclusive level-g
     array, shaped (nz+2, ny+2, nx+2)."""
     (nx, ny, nz), gl = level_dims(L, b, g)
-    h = L.h / (2 if b in L.refine else 1) * 2 ** (gl - 1)
+    h = L.h / L.rdiv.get(b, 1) * 2 ** (gl - 1)
     o = L.origin(b)
     ax = [o[a] + (np.arange(n + 2) - 0.5) * h for a, n in enumerate((nx, ny, nz))]
     z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
@@ -58,11 +57,15 @@ def centres(L, b, g):
 
 
 def rdv(L, b, g):
-    """rdv(dom, g) (localparameters.for:47-57) for rdiv 1 / 2 blocks."""
-    own = L.ngrid - 1 + (1 if b in L.refine else 0)
-    if b not in L.refine or g > own:
-        return 1
-    return 2 if g <= L.ngrid - 1 else 1
+    """rdv(dom, g) (localparameters.for:47-57): rdiv on the levels every
+    block has, halving on the block's extra levels, 1 below its own."""
+    r = L.rdiv.get(b, 1)
+    for lev in range(1, g + 1):
+        if lev > L.own_levels(b):
+            return 1
+        if lev > L.ngrid_in:
+            r //= 2
+    return r
 
 
 def interface_cells(L, desc, b, g, fine_normal_axis=None):
@@ -114,6 +117,7 @@ LAYOUTS = [
     dict(px=2, py=2, pz=2, refine=[0]),
     dict(px=2, py=2, pz=2, refine=[7]),
     dict(px=2, py=2, pz=1, refine=[1, 2]),
+    dict(px=3, py=1, pz=1, refine={1: 2, 2: 4}),
 ]
 
 
@@ -269,6 +273,7 @@ HOST_LAYOUTS = [
     dict(px=2, py=2, pz=2, refine=[3, 4], bc=ALL_WALLS),
     dict(px=2, py=2, pz=1, refine=[0], bc=ALL_WALLS, drop=((1, 1, 0),)),
     dict(px=3, py=2, pz=1, refine=[1, 4], bc=(WALL, WALL, PERIODIC, PERIODIC, WALL, WALL)),
+    dict(px=3, py=1, pz=1, refine={1: 2, 2: 4}, bc=ALL_WALLS),  # rdiv 1 | 2 | 4
 ]
 
 
