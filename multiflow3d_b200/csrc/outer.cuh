@@ -806,9 +806,9 @@ __global__ void __launch_bounds__(OZ_TX *OZ_RJ) k_calvel_calmas_lsm(const BlkFld
 // tile and its ring for either parity.  Each plane's p box is loaded once
 // and serves as the upper plane of the plane below.  Arithmetic, operand
 // order and the face planes are those of k_calvel_calmas.
-constexpr int CV_PD = 3;           // planes in flight ahead of the computed one
-constexpr int CV_NS = CV_PD + 1;   // slots: planes k .. k+CV_PD (a power of two)
-static_assert((CV_NS & (CV_NS - 1)) == 0, "CV_NS must be a power of two");
+constexpr int CV_PD = 2;           // planes in flight ahead of the computed one
+constexpr int CV_NS = CV_PD + 1;   // slots: planes k .. k+CV_PD
+constexpr int CV_MINB = 6;         // resident CTAs per SM the kernel is built for
 constexpr int CV_W = 36;
 struct CvShape {
   static constexpr int PR = OZ_RJ + 2, UR = OZ_RJ, VR = OZ_RJ + 1, WR = OZ_RJ;  // box rows
@@ -895,7 +895,7 @@ __device__ double cv_cells_divide(const BlkFld &F, int i, int j0, int k0, int k1
 // UMASK bit a: axis a of every block is uniform with a power-of-two spacing
 // (x/h is x*(1/h) there); other axes divide through div_rcp.
 template <typename T, int UMASK>
-__global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const BlkFld *__restrict__ fl,
+__global__ void __launch_bounds__(OZ_TX *CV_TY, CV_MINB) k_calvel_calmas_tma(const BlkFld *__restrict__ fl,
                                                                    const Tile *__restrict__ tiles,
                                                                    const DomState *__restrict__ ds,
                                                                    const int *__restrict__ act,
@@ -962,7 +962,7 @@ __global__ void __launch_bounds__(OZ_TX *CV_TY, 5) k_calvel_calmas_tma(const Blk
   const int cx = a0 + tx - X;     // box column of this lane's cell
   const int yb = t.j0 + pl - 1;   // field row of row j0
   const CUtensorMap *mp = F.fm, *mu = F.fm + 1, *mv = F.fm + 2, *mw = F.fm + 3;
-  auto stage = [&](int kk) { return (kk - k0) & (CV_NS - 1); };
+  auto stage = [&](int kk) { return (kk - k0) % CV_NS; };
   auto parity = [&](int kk) { return (unsigned)(((kk - k0) / CV_NS) & 1); };
   auto issue = [&](int kk) {  // planes k0..k1 all four boxes; k1+1 p only
     const int st = stage(kk), z = kk + pl - 1;
