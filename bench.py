@@ -419,6 +419,33 @@ def _timed_solves(run_once, reset, steps, warmup):
     return ev0.elapsed_time(ev1) / 1e3, out
 
 
+def run_probe(args):
+    """A short solve of the bench's layout at a chosen block edge, for
+    profiler captures of one kernel (not a benchmark line): 2x2x2 blocks of
+    n^3 with the bench's y-stretch and fields, `--probe-iters` outer
+    iterations, the default launch path (MF3D_NO_GRAPH=1 launches every
+    kernel on the stream, which a profiler can see)."""
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.problems import Problem
+    from multiflow3d_b200.solver import Projection
+    n = args.probe_cells
+    h = 1.0 / 256
+    pr = Problem(2, 2, 2, n, n, n, ngrid=6 if n % 32 == 0 else 5, pl=2, stretch_y=2.0, dx=h, dy=h, dz=h)
+    lib = abi.load()
+    host = pr.block_fields(seed=SEED, fourier_modes=FOURIER)
+    keys = ("ustar", "vstar", "wstar", "u", "v", "w", "p")
+    dev = [{k: torch.from_numpy(f[k]).cuda() for k in keys} for f in host]
+    prm = pr.params(mg_itrsch=3, irestr=2, iproln=1, maxcy=args.probe_iters, eps=1e-10, eps_relative=1, device=0)
+    proj = Projection(pr.descriptors(lib), prm, lib)
+    res = proj.newsolv_mg_device(dev)
+    torch.cuda.synchronize()
+    proj.close()
+    print(json.dumps({"workload": "probe", "block_cells": n, "iterations": res.iter, "status": res.status,
+                      "ms_device": res.ms_device}))
+    return 0
+
+
 def run_mixed(args):
     """Single block 512x256x256, tanh y-stretch 2.0, 7 levels, tol 1e-8: the
     FP32 V-cycle (FP64 coarsest level, FP64 outer loop) against the FP64 form
@@ -1019,15 +1046,19 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="multiblock",
                     choices=["multiblock", "mixed", "batched", "served", "density", "tecbin", "sip", "linegs",
-                             "rungek"],
+                             "rungek", "probe"],
                     help="multiblock: the default FP64 line; mixed / batched / served / density: the further "
                          "workloads (1 GPU)")
     ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
     ap.add_argument("--requests", type=int, default=1000, help="served: requests per rate")
     ap.add_argument("--files", type=int, default=8, help="tecbin: restart files decoded per step")
+    ap.add_argument("--probe-cells", type=int, default=96, help="probe: block edge of the 2x2x2 layout")
+    ap.add_argument("--probe-iters", type=int, default=3, help="probe: outer iterations")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "probe":
+        return run_probe(args)
     if args.workload == "mixed":
         return run_mixed(args)
     if args.workload == "batched":

@@ -987,17 +987,25 @@ __global__ void __launch_bounds__(kTile) k_prolong(const BlkLev *__restrict__ fl
   const long long csf = Fb.cstr, rowf = Fb.hp, plf = (long long)(Fb.ny + 2) * Fb.hp;
   auto coarse = [&](int a, int b, int c) -> TF { return (TF)PC[cell_off(Cb, I + a, J + b, c)]; };
   const int K1 = min(t.k0 + kch - 1, Cb.nz);
-  TF lo[2][2];  // [a][b] at coarse plane K
+  // the group's 8 fine cells of coarse plane K (colour-split offsets)
+  auto fine = [&](int K, int di, int dj, int dk) -> long long {
+    return ((di + dj + dk + 1) & 1) * csf + (2 * K + dk) * plf + (2 * J + dj) * rowf + I;
+  };
+  TF lo[2][2], hi[2][2], f[2][2][2];  // coarse planes K, K+1; the fine cells of plane K
 #pragma unroll
   for (int a = 0; a < 2; ++a)
 #pragma unroll
-    for (int b = 0; b < 2; ++b) lo[a][b] = coarse(a, b, t.k0);
+    for (int b = 0; b < 2; ++b) {
+      lo[a][b] = coarse(a, b, t.k0);
+      hi[a][b] = coarse(a, b, t.k0 + 1);
+    }
+#pragma unroll
+  for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+    for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+      for (int di = 0; di < 2; ++di) f[dk][dj][di] = PF[fine(t.k0, di, dj, dk)];
   for (int K = t.k0; K <= K1; ++K) {
-    TF hi[2][2];  // [a][b] at coarse plane K+1
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int b = 0; b < 2; ++b) hi[a][b] = coarse(a, b, K + 1);
     const bool zb = K == 0 && (m & 16), zt = K == Cb.nz && (m & 32);
     TF v[2][2][2];  // [dk][dj][di]
 #pragma unroll
@@ -1014,9 +1022,23 @@ __global__ void __launch_bounds__(kTile) k_prolong(const BlkLev *__restrict__ fl
                            w(0, 1, 1) * hi[0][1] + w(1, 0, 0) * lo[1][0] + w(1, 1, 0) * lo[1][1] +
                            w(1, 0, 1) * hi[1][0] + w(1, 1, 1) * hi[1][1]) *
                           (TF)0.015625;  // x/64 == x*2^-6 exactly in IEEE arithmetic
-          const long long o = ((di + dj + dk + 1) & 1) * csf + (2 * K + dk) * plf + (2 * J + dj) * rowf + I;
-          v[dk][dj][di] = PF[o] + corr;
+          v[dk][dj][di] = f[dk][dj][di] + corr;
         }
+    // the next plane's operands load before this plane's stores (other
+    // cells: plane K+1's fine cells are 2K+2, 2K+3)
+    TF hn[2][2] = {{hi[0][0], hi[0][1]}, {hi[1][0], hi[1][1]}};
+    if (K < K1) {
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) hn[a][b] = coarse(a, b, K + 2);
+#pragma unroll
+      for (int dk = 0; dk < 2; ++dk)
+#pragma unroll
+        for (int dj = 0; dj < 2; ++dj)
+#pragma unroll
+          for (int di = 0; di < 2; ++di) f[dk][dj][di] = PF[fine(K + 1, di, dj, dk)];
+    }
 #pragma unroll
     for (int dk = 0; dk < 2; ++dk)
 #pragma unroll
@@ -1036,7 +1058,10 @@ __global__ void __launch_bounds__(kTile) k_prolong(const BlkLev *__restrict__ fl
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int b = 0; b < 2; ++b) lo[a][b] = hi[a][b];
+      for (int b = 0; b < 2; ++b) {
+        lo[a][b] = hi[a][b];
+        hi[a][b] = hn[a][b];
+      }
   }
 }
 
