@@ -5,7 +5,7 @@ A *problem* is a Cartesian box split into ``px x py x pz`` equal blocks of
 (5 = periodic, anything else = wall, i.e. homogeneous Neumann for p).  Block
 ids are numbered x fastest, like infodom.cin.
 
-Inputs follow the parity recipe of the north-star configurations:
+Inputs follow one parity recipe for every configuration:
 ``ustar, vstar, wstar`` i.i.d. uniform [-1, 1] (optionally plus smooth
 Fourier modes), each component made mean-free over the interior faces, wall
 faces zeroed as ``boundu/boundv/boundw`` leave them (bounds.for:2-916).  The

@@ -16,7 +16,7 @@ import oracle_bridge as ob
 
 pytestmark = pytest.mark.gpu
 
-REL_TOL = 1e-10  # north-star parity bar for the FP64 drop-in
+REL_TOL = 1e-10  # parity bar of the FP64 drop-in
 
 
 def rel_l2(a, b):
