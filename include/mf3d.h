@@ -438,7 +438,8 @@ int mf3d_profile_read(mf3d_ctx *ctx, double *total_ms, long long *launches,
  * process by device, precision, smoother and block shapes; MF3D_AUTOTUNE=0
  * turns it off) or by default: the red-black sweep schedule (0..3), 1 when
  * the level sweeps with the plain-load kernel, the planes per CTA of the
- * restriction into the level, and the CTAs per block of the line or
+ * TMA restriction into the level (-1: the plain-load restriction), and the
+ * CTAs per block of the line or
  * lexicographic relaxation.  Any of the outputs may be NULL.  No
  * counterpart in the reference. */
 int mf3d_tuning(const mf3d_ctx *ctx, int level, int *sweep_schedule, int *small_sweep, int *restrict_planes,

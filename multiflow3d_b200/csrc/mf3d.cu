@@ -2255,22 +2255,24 @@ static int autotune_restrict(mf3d_ctx *C, View &V, int g, bool time_new) {
   const int Lc = C->coarse64 ? V.Lmax : V.Lmax + 1;
   const bool f64 = C->elem == 8 || g - 1 >= Lc, c64 = C->elem == 8 || g >= Lc;
   const std::string kr = tune_key(C, L, "restrict", (f64 ? 80 : 40) + (c64 ? 8 : 4));
+  // kch < 0: the plain-load restriction (k_restrict over the level's plane
+  // tiles), which small levels can prefer to the TMA ring's fill latency
   auto set_kch = [&](int kch) {
     std::vector<Tile> rm;
-    L.rtma_kch = rtma_tiles(C, L.htab, L.hblk[SUB_A], kch, rm);
+    if (kch >= 0) L.rtma_kch = rtma_tiles(C, L.htab, L.hblk[SUB_A], kch, rm);
     L.n_rtma = (int)rm.size();
     return L.rtma.upload(rm, C->stream);
   };
   int v, st;
   if (tune_get(kr, v)) return set_kch(v);
   if (!time_new) return MF3D_OK;
-  static const int kch_of[5] = {2, 4, 8, 16, 32};
+  static const int kch_of[6] = {2, 4, 8, 16, 32, -1};
   int def = 0;
   for (int c = 0; c < 5; ++c)
     if (kch_of[c] == L.rtma_kch) def = c;  // the wave model's choice (rtma_tiles)
   int pick;
   if ((st = tune_pick(
-           C, 5, def, [&](int c) { return set_kch(kch_of[c]); },
+           C, 6, def, [&](int c) { return set_kch(kch_of[c]); },
            [&] {
              if (f64) restr<double, double>(C, V, g - 1);
              else if (c64) restr<float, double>(C, V, g - 1);
@@ -3877,7 +3879,7 @@ int mf3d_tuning(const mf3d_ctx *C, int level, int *sweep_schedule, int *small_sw
   const mf3d::ViewLevel &L = C->view->lv[level];
   if (sweep_schedule) *sweep_schedule = L.sched;
   if (small_sweep) *small_sweep = L.small;
-  if (restrict_planes) *restrict_planes = level > 1 ? L.rtma_kch : 0;
+  if (restrict_planes) *restrict_planes = level > 1 ? (L.n_rtma ? L.rtma_kch : -1) : 0;
   if (cluster_ctas) *cluster_ctas = C->prm.mg_itrsch == 2 ? L.td_cl : C->prm.mg_itrsch == 1 ? L.lx_cl : 1;
   return MF3D_OK;
 }
