@@ -32,6 +32,7 @@ struct SrvReq {
   int state = 0;               // 0 queued, 1 resident, 2 finished
   int status = MF3D_PENDING;
   int vidx = -1;               // index in the current view (-1: not yet in one)
+  int lane = 0;
   mf3d_request_info info{};
   std::unique_ptr<DomainStore> dom;
 };
@@ -72,6 +73,10 @@ static std::string shape_key(const mf3d_domain_desc &d, int ngrid) {
 namespace mf3d {
 constexpr int kSrvLanes = 2;
 constexpr double kSrvLargeCells = 8.0e6;  // a request of at least this many cells runs in lane 1
+// Lane 1 holds one request at a time: a request that size fills the device
+// alone, so two resident together each advance at half the pace and both
+// finish late; one at a time they finish in arrival order at full pace.
+constexpr int kSrvLargeResident = 1;
 constexpr int kSrvIters = 8;              // outer iterations per cycle at most (fewer when a request stops)
 }  // namespace mf3d
 
@@ -87,6 +92,7 @@ struct mf3d_server {
   double used = 0.0;            // estimated bytes of resident requests
   double pooled = 0.0;          // bytes of retired storage kept for reuse
   long long submitted = 0, completed = 0, resident = 0, cycles = 0;
+  int lane_resident[mf3d::kSrvLanes] = {};  // resident requests per lane
   double t_build = 0.0, t_rebuild = 0.0, t_cycle = 0.0, t_finish = 0.0;  // worker seconds, all lanes
   long long builds = 0, rebuilds = 0;
   bool stop = false;
@@ -99,7 +105,10 @@ namespace mf3d {
 // device bytes are given back now (else when its storage leaves the view).
 static void srv_finish(mf3d_server *S, SrvReq *r, int status, bool release = true) {
   std::lock_guard<std::mutex> lk(S->mu);
-  if (r->state == 1) S->resident--;
+  if (r->state == 1) {
+    S->resident--;
+    S->lane_resident[r->lane]--;
+  }
   r->state = 2;
   r->status = status;
   r->info.info.status = status;
@@ -247,7 +256,8 @@ static void srv_loop(mf3d_server *S, int lane) {
       // arrival order; a request waits at the head until memory frees up,
       // unless nothing else is resident (then it is admitted and may fail on OOM)
       std::vector<char> taken(pool.size(), 0);
-      while (!queue.empty() && S->resident < S->max_resident) {
+      while (!queue.empty() && S->resident < S->max_resident &&
+             (lane == 0 || S->lane_resident[lane] < kSrvLargeResident)) {
         SrvReq *r = queue.front();
         const std::string key = shape_key(r->desc, r->ngrid);
         int hit = -1;
@@ -267,6 +277,7 @@ static void srv_loop(mf3d_server *S, int lane) {
         S->used += r->est;
         r->state = 1;
         S->resident++;
+        S->lane_resident[lane]++;
         admit.push_back(r);
         reuse.push_back(hit);
       }
@@ -497,6 +508,7 @@ int mf3d_server_submit(mf3d_server *S, const mf3d_domain_desc *dom, const mf3d_f
   r->est = domain_bytes(*dom, ngrid, S->C[0]->elem);
   r->info.t_submit = steady_now();
   const int lane = (double)dom->nx * dom->ny * dom->nz >= kSrvLargeCells ? 1 : 0;
+  r->lane = lane;
   std::lock_guard<std::mutex> lk(S->mu);
   r->ticket = S->next_ticket++;
   *ticket = r->ticket;
