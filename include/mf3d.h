@@ -42,8 +42,9 @@ enum mf3d_status {
   MF3D_E_OOM = -3,        /* device allocation failed or over the cap       */
   MF3D_E_TIMEOUT = -4,    /* a bounded device wait gave up                  */
   MF3D_E_NONFINITE = -5,  /* NaN/Inf met in the residual                     */
-  MF3D_E_UNSUPPORTED = -6 /* a reference feature outside this build (LMR)
-                             or an unsupported combination              */
+  MF3D_E_UNSUPPORTED = -6 /* a reference feature outside this build (LMR
+                             in the outer loop) or an unsupported
+                             combination                                   */
 };
 
 /* Boundary-condition code meaning "periodic" (control.cin:17-22). Any other

@@ -298,3 +298,27 @@ def test_library_lmr_refresh_matches_oracle(lib, orc, lay):
         assert orc.orc_exchangepp(do, L.nblocks, L.ngrid, g, ob.ptr_array(ref)) == 0
         for b in range(L.nblocks):
             assert np.array_equal(mine[b], ref[b]), f"level {g} block {b}: {np.argwhere(mine[b] != ref[b])[:5]}"
+
+
+def test_library_lmr_plan_refusals(lib):
+    """mf3d_create checks an LMR layout before it touches the device
+    (alloc_dom.for:12-230 and the restated scope): FP32, periodic partners
+    of different refinement, neighbours more than 2:1 apart, and spacings
+    that are not powers of two of one another are refused with no GPU."""
+    from multiflow3d_b200 import abi
+    ctx = C.c_void_p()
+    L = LmrLayout(2, 1, 1, 8, [1], ALL_WALLS, 3)
+    d = L.descriptors(lib)
+    p = L.params(precision=abi.MF3D_PREC_FP32)
+    assert lib.mf3d_create(d, L.nblocks, C.byref(p), C.byref(ctx)) == -6  # MF3D_E_UNSUPPORTED
+    assert b"LMR" in lib.mf3d_last_error()
+    Lp = LmrLayout(2, 1, 1, 8, [1], (PERIODIC, PERIODIC, WALL, WALL, WALL, WALL), 3)
+    assert lib.mf3d_create(Lp.descriptors(lib), Lp.nblocks, C.byref(Lp.params()), C.byref(ctx)) == -1  # INVALID
+    assert b"periodic" in lib.mf3d_last_error()
+    L4 = LmrLayout(2, 1, 1, 8, {1: 4}, ALL_WALLS, 3)
+    assert lib.mf3d_create(L4.descriptors(lib), L4.nblocks, C.byref(L4.params()), C.byref(ctx)) == -1
+    assert b"rdiv" in lib.mf3d_last_error()
+    d3 = L.descriptors(lib)
+    d3[1].dx = d3[1].dy = d3[1].dz = 1.0 / 24  # a ratio of 3
+    d3[1].nx = d3[1].ny = d3[1].nz = 24
+    assert lib.mf3d_create(d3, 2, C.byref(L.params()), C.byref(ctx)) == -1
