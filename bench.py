@@ -446,6 +446,102 @@ def run_probe(args):
     return 0
 
 
+def lmr_layout(lib, n=96):
+    """2x2x2 unit-cube blocks, walls around, block 0 at refinement 2 (twice
+    the cells and half the spacing over the same extents, rdiv = 2); the
+    others n^3.  Returns the descriptors; ngrd_gl = 6 (ngrid_input 5)."""
+    import numpy as np
+    from multiflow3d_b200.abi import BlockDesc
+    ext = np.array([[i, i + 1, j, j + 1, k, k + 1] for k in range(2) for j in range(2) for i in range(2)],
+                   dtype=np.float64).ravel()
+    arr = (BlockDesc * 8)()
+    fn = getattr(lib, "mf3d_build_topology", None) or getattr(lib, "orc_build_topology")
+    h = 1.0 / n
+    if fn(8, ext.ctypes.data_as(C.POINTER(C.c_double)), (C.c_int * 6)(*([4] * 6)), C.c_double(h), C.c_double(h),
+          C.c_double(h), arr) != 0:
+        raise RuntimeError("topology")
+    d = arr[0]
+    d.nx, d.ny, d.nz = 2 * n, 2 * n, 2 * n
+    d.dx, d.dy, d.dz = h / 2, h / 2, h / 2
+    return arr
+
+
+def run_lmr(args):
+    """The V-cycle across a 2:1 refinement interface (LMR): 2x2x2 blocks,
+    one at twice the resolution (192^3 beside seven 96^3, 13.3 M cells),
+    walls, 6 levels, RB-GS(2,1), FP64, mf3d_mgkcyc_device on device arrays.
+    A step is one V-cycle on a seeded right-hand side.  CPU baseline: the
+    oracle's mgkcyc on the same inputs, one thread per block."""
+    import numpy as np
+    import torch
+    from multiflow3d_b200 import abi
+    from multiflow3d_b200.abi import Params
+    from multiflow3d_b200.solver import Projection
+    lib = abi.load()
+    dev = torch.device("cuda:0")
+    n, pl = 96, 2
+    desc = lmr_layout(lib, n)
+    prm = Params(ngrid=6, mg_itrsch=3, irestr=2, iproln=1, maxcy=1, eps=1e-8, eps_relative=1, pl=pl,
+                 differencing=1, precision=0)
+    shapes = [(desc[b].nz + 2 * pl, desc[b].ny + 2 * pl, desc[b].nx + 2 * pl) for b in range(8)]
+    rng = np.random.default_rng(SEED)
+    su_h = [rng.uniform(-1, 1, size=sh) for sh in shapes]
+    su = [torch.from_numpy(a).to(dev) for a in su_h]
+    pp = [torch.zeros(sh, dtype=torch.float64, device=dev) for sh in shapes]
+    proj = Projection(desc, prm, lib)
+
+    def once():
+        for t in pp:
+            t.zero_()
+        proj.mgkcyc_device(su, pp)
+
+    for _ in range(args.warmup):
+        once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        once()
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    launches = proj.launches
+    proj.close()
+    cells = sum(desc[b].nx * desc[b].ny * desc[b].nz for b in range(8))
+    value = args.steps / sec
+    line = {
+        "metric": "lmr_vcycles_per_s_fp64", "value": value, "unit": "V-cycles/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec / args.steps * 1e3,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"LMR 2:1: 2x2x2 unit blocks, one at {2 * n}^3 beside seven {n}^3 ({cells / 1e6:.1f} M "
+                               f"cells), walls, 6 levels, RB-GS(2,1), one V-cycle (mgkcyc) per step"},
+        "gpu_launches_per_step": launches,
+    }
+    if not args.no_cpu_baseline:
+        orc = oracle_lib()
+        threads = max(1, min(os.cpu_count() or 1, 8))
+        orc.orc_set_threads(threads)
+        odesc = lmr_layout(orc, n)
+        pp_h = [np.zeros(sh) for sh in shapes]
+        import oracle_bridge
+        t0 = time.perf_counter()
+        st = orc.orc_mgkcyc(odesc, 8, C.byref(prm), oracle_bridge.ptr_array(su_h), oracle_bridge.ptr_array(pp_h))
+        t1 = time.perf_counter()
+        line["cpu_baseline"] = {"value": 1.0 / (t1 - t0), "unit": "V-cycles/s", "cores": threads, "kind": "port",
+                                "sample": f"one V-cycle of the same inputs on the oracle ({threads} threads)",
+                                "status": st}
+        line["speedup_vs_cpu"] = value * (t1 - t0)
+        # the first device V-cycle equals the oracle's bit for bit
+        for t in pp:
+            t.zero_()
+        proj2 = Projection(desc, prm, lib)
+        proj2.mgkcyc_device(su, pp)
+        proj2.close()
+        line["bitwise_vs_oracle"] = all(np.array_equal(pp[b].cpu().numpy(), pp_h[b]) for b in range(8))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_mixed(args):
     """Single block 512x256x256, tanh y-stretch 2.0, 7 levels, tol 1e-8: the
     FP32 V-cycle (FP64 coarsest level, FP64 outer loop) against the FP64 form
@@ -1046,7 +1142,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="multiblock",
                     choices=["multiblock", "mixed", "batched", "served", "density", "tecbin", "sip", "linegs",
-                             "rungek", "probe"],
+                             "rungek", "probe", "lmr"],
                     help="multiblock: the default FP64 line; mixed / batched / served / density: the further "
                          "workloads (1 GPU)")
     ap.add_argument("--rates", default="50,200,800", help="served: arrival rates per second")
@@ -1059,6 +1155,8 @@ def main():
         return run_reference(args)
     if args.workload == "probe":
         return run_probe(args)
+    if args.workload == "lmr":
+        return run_lmr(args)
     if args.workload == "mixed":
         return run_mixed(args)
     if args.workload == "batched":
