@@ -23,36 +23,65 @@ struct LmrNode {
   double scale;
 };
 struct LmrWrite {
-  int blk, off, node;
+  int blk, off, node;  // node < 0: a copy of (sblk, soff), a cell no write touches
+  int sblk, soff;
 };
 
-// Nodes [n0, n1): val[n] = (w_0 x_0 + w_1 x_1 + ...) * scale, summed left to
-// right as the reference writes each formula.
+constexpr int LMR_MAX_TERMS = 8;   // the longest formula: an 8-cell average or blend
+constexpr int LMR_SMEM_BLOCKS = 64; // view blocks whose phi pointers a CTA keeps in shared memory
+
+// The phi pointer of view block b: from shared memory for the first
+// LMR_SMEM_BLOCKS blocks (one dependent load fewer per term), else the table.
 template <typename T>
-__global__ void __launch_bounds__(256) k_lmr_nodes(const BlkLev *__restrict__ tab, const LmrTerm *__restrict__ terms,
-                                                   const LmrNode *__restrict__ nodes, int n0, int n1,
-                                                   double *__restrict__ val) {
+__device__ __forceinline__ T *lmr_phi(const BlkLev *__restrict__ tab, T *const *sphi, int b) {
+  return b < LMR_SMEM_BLOCKS ? sphi[b] : phi_of<T>(tab[b]);
+}
+template <typename T>
+__device__ __forceinline__ void lmr_stage_phi(const BlkLev *__restrict__ tab, int nblk, T **sphi) {
+  for (int b = threadIdx.x; b < nblk && b < LMR_SMEM_BLOCKS; b += blockDim.x) sphi[b] = phi_of<T>(tab[b]);
+  __syncthreads();
+}
+
+// Nodes [n0, n1): val[n] = (w_0 x_0 + w_1 x_1 + ...) * scale, summed left to
+// right as the reference writes each formula.  The terms' operands load
+// first, all in flight at once; the sum then runs in order.
+template <typename T>
+__global__ void __launch_bounds__(256) k_lmr_nodes(const BlkLev *__restrict__ tab, int nblk,
+                                                   const LmrTerm *__restrict__ terms, const LmrNode *__restrict__ nodes,
+                                                   int n0, int n1, double *__restrict__ val) {
   pdl_wait();
+  __shared__ T *sphi[LMR_SMEM_BLOCKS];
+  lmr_stage_phi<T>(tab, nblk, sphi);
   const int n = n0 + (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (n >= n1) return;
   const LmrNode N = nodes[n];
-  double t = 0.0;
-  for (int q = 0; q < N.nt; ++q) {
-    const LmrTerm a = terms[N.t0 + q];
-    const double x = a.blk >= 0 ? (double)phi_of<T>(tab[a.blk])[a.off] : a.blk == -1 ? val[a.off] : 0.0;
-    t = q == 0 ? a.w * x : t + a.w * x;
+  double x[LMR_MAX_TERMS], w[LMR_MAX_TERMS];
+#pragma unroll
+  for (int q = 0; q < LMR_MAX_TERMS; ++q) {
+    if (q < N.nt) {
+      const LmrTerm a = terms[N.t0 + q];
+      w[q] = a.w;
+      x[q] = a.blk >= 0 ? (double)lmr_phi<T>(tab, sphi, a.blk)[a.off] : a.blk == -1 ? val[a.off] : 0.0;
+    }
   }
+  double t = w[0] * x[0];
+#pragma unroll
+  for (int q = 1; q < LMR_MAX_TERMS; ++q)
+    if (q < N.nt) t = t + w[q] * x[q];
   val[n] = t * N.scale;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_lmr_write(const BlkLev *__restrict__ tab, const LmrWrite *__restrict__ w,
-                                                   int n, const double *__restrict__ val) {
+__global__ void __launch_bounds__(256) k_lmr_write(const BlkLev *__restrict__ tab, int nblk,
+                                                   const LmrWrite *__restrict__ w, int n,
+                                                   const double *__restrict__ val) {
   pdl_wait();
+  __shared__ T *sphi[LMR_SMEM_BLOCKS];
+  lmr_stage_phi<T>(tab, nblk, sphi);
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= n) return;
   const LmrWrite W = w[i];
-  phi_of<T>(tab[W.blk])[W.off] = (T)val[W.node];
+  lmr_phi<T>(tab, sphi, W.blk)[W.off] = W.node >= 0 ? (T)val[W.node] : lmr_phi<T>(tab, sphi, W.sblk)[W.soff];
 }
 
 // The listed blocks' ghost-inclusive cells, item t: block list[b] with

@@ -791,11 +791,24 @@ static int build_domain(DomainStore &D, const mf3d_block_desc *blocks, int nb, i
           else { terms[q].blk = -1; terms[q].off = (int)(-2 - t.ref); }
         }
         std::vector<LmrNode> nodes(P.nodes.size());
-        for (size_t q = 0; q < nodes.size(); ++q) nodes[q] = LmrNode{P.nodes[q].t0, P.nodes[q].nt, P.nodes[q].scale};
-        std::vector<LmrWrite> writes(P.writes.size());
-        for (size_t q = 0; q < writes.size(); ++q) {
+        for (size_t q = 0; q < nodes.size(); ++q) {
+          nodes[q] = LmrNode{P.nodes[q].t0, P.nodes[q].nt, P.nodes[q].scale};
+          if (nodes[q].nt < 1 || nodes[q].nt > LMR_MAX_TERMS) {
+            set_error("LMR halo program: a node of " + std::to_string(nodes[q].nt) + " terms");
+            return MF3D_E_INVALID;
+          }
+        }
+        std::vector<LmrWrite> writes(P.writes.size() + P.copies.size());
+        for (size_t q = 0; q < P.writes.size(); ++q) {
           loc(P.writes[q].first, writes[q].blk, writes[q].off);
           writes[q].node = P.writes[q].second;
+          writes[q].sblk = writes[q].soff = 0;
+        }
+        for (size_t q = 0; q < P.copies.size(); ++q) {
+          LmrWrite &W = writes[P.writes.size() + q];
+          loc(P.copies[q].first, W.blk, W.off);
+          loc(P.copies[q].second, W.sblk, W.soff);
+          W.node = -1;
         }
         DomainStore::LmrLevel &M = D.lmr[g];
         if ((st = M.terms.upload(terms, s))) return st;
@@ -1850,13 +1863,13 @@ static void halo(mf3d_ctx *C, View &V, int g, int q) {
     for (size_t d = 1; d < L.lmr_depth.size(); ++d) {
       const int n0 = L.lmr_depth[d - 1], n1 = L.lmr_depth[d];
       if (n1 <= n0) continue;
-      launch(k_lmr_nodes<T>, grid_of(n1 - n0, 256), 256, 0, C->stream, L.tab.p, L.lmr_terms, L.lmr_nodes, n0, n1,
-             L.lmr_val.p);
+      launch(k_lmr_nodes<T>, grid_of(n1 - n0, 256), 256, 0, C->stream, L.tab.p, (int)V.blk.size(), L.lmr_terms,
+             L.lmr_nodes, n0, n1, L.lmr_val.p);
       ++C->launches;
     }
     if (L.lmr_nwrites) {
-      launch(k_lmr_write<T>, grid_of(L.lmr_nwrites, 256), 256, 0, C->stream, L.tab.p, L.lmr_writes, L.lmr_nwrites,
-             (const double *)L.lmr_val.p);
+      launch(k_lmr_write<T>, grid_of(L.lmr_nwrites, 256), 256, 0, C->stream, L.tab.p, (int)V.blk.size(),
+             L.lmr_writes, L.lmr_nwrites, (const double *)L.lmr_val.p);
       ++C->launches;
     }
     return;
@@ -3999,6 +4012,7 @@ int mf3d_halo_refresh_host(const mf3d_block_desc *blocks, int nblocks, int ngrid
         val[n] = t * N.scale;
       }
       for (auto &w : P.writes) cell(w.first) = val[w.second];
+      for (auto &c : P.copies) cell(c.first) = cell(c.second);  // sources no write touches
     } else {
       const auto pairs = mf3d::build_halo_map(b, geom, base);
       std::vector<double> v(pairs.size());

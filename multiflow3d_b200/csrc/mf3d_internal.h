@@ -44,7 +44,8 @@ std::vector<HaloPair> build_halo_map(const std::vector<mf3d_block_desc> &blocks,
 // a program over the state before the exchange: nodes, each a sum
 // w_0 x_0 + w_1 x_1 + ... (in that order, the reference's order) times
 // `scale`, whose terms are cells or earlier nodes, evaluated in order of
-// depth; then every changed ghost cell takes its node's value.  `rdv` is
+// depth; then every changed ghost cell takes its node's value, or the value
+// of the cell it copies where no write touches that cell.  `rdv` is
 // rdv(block, g) of each block at this level (localparameters.for:47-57).
 struct LmrProgram {
   struct Term {
@@ -59,6 +60,7 @@ struct LmrProgram {
   std::vector<Node> nodes;                        // in order of depth
   std::vector<int> depth_start;                   // nodes of depth d: [depth_start[d-1], depth_start[d])
   std::vector<std::pair<long long, int>> writes;  // ghost cell id <- node
+  std::vector<std::pair<long long, long long>> copies;  // ghost cell id <- a cell no write touches
 };
 constexpr long long kLmrZero = -1;
 LmrProgram build_halo_lmr(const std::vector<mf3d_block_desc> &blocks, const std::vector<LevelGeom> &geom,

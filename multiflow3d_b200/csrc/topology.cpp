@@ -627,10 +627,16 @@ LmrProgram build_halo_lmr(const std::vector<mf3d_block_desc> &blocks, const std:
     dmax = std::max(dmax, dd);
   }
   LmrProgram out;
-  // copies of pre-exchange cells become one-term nodes of depth 1
+  // a copy of a cell the refresh does not write is applied directly with
+  // the writes; a copy of one it writes becomes a one-term node of depth 1
+  // (read before any write)
+  std::vector<long long> dsts;
+  for (auto &f : fin) dsts.push_back(f.first);
+  std::sort(dsts.begin(), dsts.end());
+  auto written = [&](long long c) { return std::binary_search(dsts.begin(), dsts.end(), c); };
   std::vector<long long> copy_of;
   for (auto &f : fin)
-    if (f.second >= 0) copy_of.push_back(f.second);
+    if (f.second >= 0 && written(f.second)) copy_of.push_back(f.second);
   std::sort(copy_of.begin(), copy_of.end());
   copy_of.erase(std::unique(copy_of.begin(), copy_of.end()), copy_of.end());
   std::vector<int> newid(nn, -1);
@@ -652,6 +658,10 @@ LmrProgram build_halo_lmr(const std::vector<mf3d_block_desc> &blocks, const std:
     out.depth_start.push_back((int)out.nodes.size());
   }
   for (auto &f : fin) {
+    if (f.second >= 0 && !written(f.second)) {
+      out.copies.push_back({f.first, f.second});
+      continue;
+    }
     int node;
     if (f.second >= 0) node = (int)(std::lower_bound(copy_of.begin(), copy_of.end(), f.second) - copy_of.begin());
     else node = newid[(size_t)(-2 - f.second)];
