@@ -64,3 +64,42 @@ class LmrLayout:
 
     def origin(self, b):
         return tuple(float(c) for c in self.pos[b])
+
+
+def random_layouts(seed, count, n=8, ngrid_in=3):
+    """Seeded LMR layouts: grids of up to 3x3x2 blocks, some positions left
+    out, a random set of refined blocks, walls or a periodic axis.  Along a
+    periodic axis the refinement depends only on the other coordinates, so
+    periodic partners share it (alloc_dom.for:210-221)."""
+    import numpy as np
+    from multiflow3d_b200.problems import PERIODIC, WALL
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < count:
+        px, py, pz = int(rng.integers(1, 4)), int(rng.integers(1, 4)), int(rng.integers(1, 3))
+        if px * py * pz < 2:
+            continue
+        per = int(rng.integers(0, 4))  # 0: walls; 1..3: that axis periodic
+        if per and (px, py, pz)[per - 1] < 2:
+            per = 0
+        bc = [WALL] * 6
+        if per:
+            bc[2 * (per - 1)] = bc[2 * (per - 1) + 1] = PERIODIC
+        cells = [(i, j, k) for k in range(pz) for j in range(py) for i in range(px)]
+        drop = ()
+        if not per and len(cells) > 3 and rng.random() < 0.4:
+            drop = (cells[int(rng.integers(0, len(cells)))],)
+        kept = [c for c in cells if c not in drop]
+        # refinement keyed on the coordinates other than the periodic axis
+        key = {}
+        refine = []
+        for b, c in enumerate(kept):
+            kk = tuple(v for a, v in enumerate(c) if a != per - 1) if per else c
+            if kk not in key:
+                key[kk] = bool(rng.random() < 0.4)
+            if key[kk]:
+                refine.append(b)
+        if not refine or len(refine) == len(kept):
+            continue
+        out.append(LmrLayout(px, py, pz, n, refine, tuple(bc), ngrid_in, drop=drop))
+    return out

@@ -108,3 +108,14 @@ def test_lmr_refusals(lib, cuda):
     proj.close()
     with pytest.raises(RuntimeError):
         Projection(L.descriptors(lib), L.params(precision=abi.MF3D_PREC_FP32), lib)
+
+
+def test_lmr_vcycle_random_layouts(lib, oracle, cuda):
+    """The V-cycle on 12 seeded random LMR layouts (grids with a block left
+    out, periodic axes, random refined sets), the three smoothers in turn:
+    pp bit-identical to the oracle."""
+    from lmr_layouts import random_layouts
+    for q, L in enumerate(random_layouts(4242, 12)):
+        got, ref, _ = run_pair(lib, oracle, cuda, L, (3, 1, 2)[q % 3], seed=q)
+        for b in range(L.nblocks):
+            assert np.array_equal(got[b], ref[b]), (L.pos, L.refine, L.bc, b)

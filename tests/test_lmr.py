@@ -322,3 +322,24 @@ def test_library_lmr_plan_refusals(lib):
     d3[1].dx = d3[1].dy = d3[1].dz = 1.0 / 24  # a ratio of 3
     d3[1].nx = d3[1].ny = d3[1].nz = 24
     assert lib.mf3d_create(d3, 2, C.byref(L.params()), C.byref(ctx)) == -1
+
+
+def test_library_lmr_refresh_random_layouts(lib, orc):
+    """The library's LMR refresh against the oracle's on every level of 16
+    seeded random layouts (grids with a block left out, periodic axes,
+    random refined sets), bit for bit."""
+    from lmr_layouts import random_layouts
+    rng = np.random.default_rng(7)
+    for L in random_layouts(2024, 16):
+        dl, do = L.descriptors(lib), L.descriptors(orc)
+        for g in range(1, L.ngrid + 1):
+            a = []
+            for b in range(L.nblocks):
+                (nx, ny, nz), _ = level_dims(L, b, g)
+                a.append(rng.uniform(-1, 1, size=(nz + 2, ny + 2, nx + 2)))
+            mine = [np.ascontiguousarray(x.copy()) for x in a]
+            ref = [np.ascontiguousarray(x.copy()) for x in a]
+            assert lib.mf3d_halo_refresh_host(dl, L.nblocks, L.ngrid, g, ob.ptr_array(mine)) == 0
+            assert orc.orc_exchangepp(do, L.nblocks, L.ngrid, g, ob.ptr_array(ref)) == 0
+            for b in range(L.nblocks):
+                assert np.array_equal(mine[b], ref[b]), (L.pos, L.refine, L.bc, g, b)
