@@ -119,3 +119,13 @@ def test_lmr_vcycle_random_layouts(lib, oracle, cuda):
         got, ref, _ = run_pair(lib, oracle, cuda, L, (3, 1, 2)[q % 3], seed=q)
         for b in range(L.nblocks):
             assert np.array_equal(got[b], ref[b]), (L.pos, L.refine, L.bc, b)
+
+
+@pytest.mark.parametrize("pl", [1, 3])
+def test_lmr_vcycle_ghost_widths(lib, oracle, cuda, pl):
+    """su and pp with 1 and 3 ghost layers (the ttc layout the V-cycle reads
+    and writes): pp bit-identical to the oracle."""
+    L = LmrLayout(2, 2, 1, 8, [0, 3], ALL_WALLS, 3, pl=pl)
+    got, ref, _ = run_pair(lib, oracle, cuda, L, 3, seed=pl)
+    for b in range(L.nblocks):
+        assert np.array_equal(got[b], ref[b])
