@@ -197,8 +197,9 @@ int mf3d_build_topology(int nblocks, const double *extents, const int *bc6,
  * same extents.  params.ngrid is then ngrd_gl = ngrid_input + log2(max
  * rdiv); a block keeps ngrid_input + log2(rdiv) levels of its own size and
  * must be divisible by 2^(that - 1).  Neighbours may differ by 2:1 at most
- * and periodic partners not at all (alloc_dom.for:12-230).  FP64, uniform
- * spacing, no lsm, bounds or solver 1 (MF3D_E_UNSUPPORTED otherwise).  Such
+ * and periodic partners not at all (alloc_dom.for:12-230).  FP64 or FP32
+ * (the FP32 V-cycle keeps its coarsest level in FP64), uniform spacing, no
+ * lsm, bounds or solver 1 (MF3D_E_UNSUPPORTED otherwise).  Such
  * a context runs mf3d_mgkcyc_device only: the outer loop's field exchanges
  * at refinement interfaces are not restated, and the other entry points
  * return MF3D_E_UNSUPPORTED. */

@@ -1,4 +1,4 @@
-// LMR: the V-cycle across 2:1 refinement interfaces (FP64).
+// LMR: the V-cycle across 2:1 refinement interfaces.
 //
 // A block of refinement rdiv keeps ngrid_input + log2(rdiv) levels of its
 // own (localparameters.for:42-45); below its last level it stays at that
@@ -107,8 +107,11 @@ __device__ __forceinline__ bool lmr_item(const BlkLev *tab, const int *list, con
 
 // mgrestr into a level past the block's own last (same size): phi := 0 on
 // every cell, the interior rhs := the fine level's residual at the same
-// cell, and with `red` the level's from-zero red half-sweep.
-template <typename T>
+// cell, and with `red` the level's from-zero red half-sweep.  TF / TC: the
+// fine and coarse levels' types (an FP32 V-cycle keeps its coarsest level
+// in FP64); the residual is formed in TF as the regular restriction forms
+// it, the red half-sweep in TC.
+template <typename TF, typename TC>
 __global__ void __launch_bounds__(256) k_lmr_inject(const BlkLev *__restrict__ ftab, const BlkLev *__restrict__ ctab,
                                                     const int *__restrict__ list, const long long *__restrict__ pre,
                                                     int nlist, const int *__restrict__ act, int red) {
@@ -117,24 +120,24 @@ __global__ void __launch_bounds__(256) k_lmr_inject(const BlkLev *__restrict__ f
   if (!lmr_item(ctab, list, pre, nlist, (long long)blockIdx.x * blockDim.x + threadIdx.x, b, i, j, k)) return;
   const BlkLev Cb = ctab[b], Fb = ftab[b];
   if (!act[Cb.dom]) return;
-  T *PC = phi_of<T>(Cb), *RC = rhs_of<T>(Cb);
-  const T *P = phi_of<T>(Fb), *R = rhs_of<T>(Fb);
+  TC *PC = phi_of<TC>(Cb), *RC = rhs_of<TC>(Cb);
+  const TF *P = phi_of<TF>(Fb), *R = rhs_of<TF>(Fb);
   const long long co = cell_off(Cb, i, j, k);
-  PC[co] = (T)0;
+  PC[co] = (TC)0;
   if (i < 1 || i > Cb.nx || j < 1 || j > Cb.ny || k < 1 || k > Cb.nz) return;
-  T cw, ce, cs, cn, cb, ct;
-  cell_coefs(Fb, Coef<T>(Fb), i, j, k, cw, ce, cs, cn, cb, ct);
-  const T ap = (T)-1.0 * (cw + ce + cs + cn + cb + ct);
-  const T res = R[cell_off(Fb, i, j, k)] -
-                (cw * P[cell_off(Fb, i - 1, j, k)] + ce * P[cell_off(Fb, i + 1, j, k)] +
-                 cs * P[cell_off(Fb, i, j - 1, k)] + cn * P[cell_off(Fb, i, j + 1, k)] +
-                 cb * P[cell_off(Fb, i, j, k - 1)] + ct * P[cell_off(Fb, i, j, k + 1)] + ap * P[cell_off(Fb, i, j, k)]);
-  RC[co] = res;
+  TF cw, ce, cs, cn, cb, ct;
+  cell_coefs(Fb, Coef<TF>(Fb), i, j, k, cw, ce, cs, cn, cb, ct);
+  const TF ap = (TF)-1.0 * (cw + ce + cs + cn + cb + ct);
+  const TF res = R[cell_off(Fb, i, j, k)] -
+                 (cw * P[cell_off(Fb, i - 1, j, k)] + ce * P[cell_off(Fb, i + 1, j, k)] +
+                  cs * P[cell_off(Fb, i, j - 1, k)] + cn * P[cell_off(Fb, i, j + 1, k)] +
+                  cb * P[cell_off(Fb, i, j, k - 1)] + ct * P[cell_off(Fb, i, j, k + 1)] + ap * P[cell_off(Fb, i, j, k)]);
+  RC[co] = (TC)res;
   if (red && colour_of(i, j, k) == 0) {
-    T aw, ae, as, an, ab, at;
-    cell_coefs(Cb, Coef<T>(Cb), i, j, k, aw, ae, as, an, ab, at);
-    const T apc = (T)-1.0 * (aw + ae + as + an + ab + at);
-    PC[co] = res / apc;
+    TC aw, ae, as, an, ab, at;
+    cell_coefs(Cb, Coef<TC>(Cb), i, j, k, aw, ae, as, an, ab, at);
+    const TC apc = (TC)-1.0 * (aw + ae + as + an + ab + at);
+    PC[co] = (TC)res / apc;
   }
 }
 
@@ -143,7 +146,7 @@ __global__ void __launch_bounds__(256) k_lmr_inject(const BlkLev *__restrict__ f
 // each wall-face ghost taking the cell it mirrors - west, east, south,
 // north, bottom, top in turn, so a ghost on two or three walls ends with the
 // interior cell diagonal to it.
-template <typename T>
+template <typename TF, typename TC>
 __global__ void __launch_bounds__(256) k_lmr_add(const BlkLev *__restrict__ ftab, const BlkLev *__restrict__ ctab,
                                                  const int *__restrict__ list, const long long *__restrict__ pre,
                                                  int nlist, const int *__restrict__ act, int mode) {
@@ -152,10 +155,10 @@ __global__ void __launch_bounds__(256) k_lmr_add(const BlkLev *__restrict__ ftab
   if (!lmr_item(ftab, list, pre, nlist, (long long)blockIdx.x * blockDim.x + threadIdx.x, b, i, j, k)) return;
   const BlkLev Fb = ftab[b], Cb = ctab[b];
   if (!act[Fb.dom]) return;
-  T *PF = phi_of<T>(Fb);
+  TF *PF = phi_of<TF>(Fb);
   if (mode == 0) {
     const long long o = cell_off(Fb, i, j, k);
-    PF[o] = PF[o] + phi_of<T>(Cb)[cell_off(Cb, i, j, k)];
+    PF[o] = PF[o] + (TF)phi_of<TC>(Cb)[cell_off(Cb, i, j, k)];
     return;
   }
   const int m = Fb.nmask;

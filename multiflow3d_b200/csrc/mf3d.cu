@@ -1952,12 +1952,11 @@ static void relax(mf3d_ctx *C, View &V, int g, int q, int it, bool from_zero, bo
 template <typename T, typename TC>
 static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks continuing down
   ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
-  if constexpr (std::is_same<T, TC>::value)
-    if (Cl.n_inj) {  // LMR: blocks past their own last level
-      launch(k_lmr_inject<T>, grid_of(Cl.inj_items, 256), 256, 0, C->stream, F.tab.p, Cl.tab.p, Cl.inj_list.p,
-             Cl.inj_pre.p, Cl.n_inj, V.act.p, (C->prm.mg_itrsch == 3 && C->prm.irestr > 0) ? 1 : 0);
-      ++C->launches;
-    }
+  if (Cl.n_inj) {  // LMR: blocks past their own last level
+    launch(k_lmr_inject<T, TC>, grid_of(Cl.inj_items, 256), 256, 0, C->stream, F.tab.p, Cl.tab.p, Cl.inj_list.p,
+           Cl.inj_pre.p, Cl.n_inj, V.act.p, (C->prm.mg_itrsch == 3 && C->prm.irestr > 0) ? 1 : 0);
+    ++C->launches;
+  }
   if (!Cl.n_rtile) return;
   const int pk = g == 1 ? MF3D_PROF_RESTRICT_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 2.0 / 8.0));  // fine phi, rhs in; coarse out
@@ -1980,13 +1979,12 @@ static void restr(mf3d_ctx *C, View &V, int g) {  // level g -> g+1, blocks cont
 template <typename T, typename TC>
 static void corr(mf3d_ctx *C, View &V, int g) {  // level g+1 -> g, blocks continuing down
   ViewLevel &F = V.lv[g], &Cl = V.lv[g + 1];
-  if constexpr (std::is_same<T, TC>::value)
-    if (F.n_add) {  // LMR: blocks past their own last level
-      for (int mode = 0; mode < 2; ++mode)
-        launch(k_lmr_add<T>, grid_of(F.add_items, 256), 256, 0, C->stream, F.tab.p, Cl.tab.p, F.add_list.p,
-               F.add_pre.p, F.n_add, V.act.p, mode);
-      C->launches += 2;
-    }
+  if (F.n_add) {  // LMR: blocks past their own last level
+    for (int mode = 0; mode < 2; ++mode)
+      launch(k_lmr_add<T, TC>, grid_of(F.add_items, 256), 256, 0, C->stream, F.tab.p, Cl.tab.p, F.add_list.p,
+             F.add_pre.p, F.n_add, V.act.p, mode);
+    C->launches += 2;
+  }
   if (!F.n_ptile) return;
   const int pk = g == 1 ? MF3D_PROF_PROLONG_L1 : 0;
   prof_begin(C, pk, (double)F.cells_sub[SUB_D] * sizeof(T) * (2.0 + 1.0 / 8.0));  // fine in/out, coarse in
@@ -3163,8 +3161,8 @@ static int lmr_plan(const mf3d_block_desc *blocks, int nb, const mf3d_params *pr
     set_error("LMR: ngrid (ngrd_gl) must exceed log2 of the largest refinement");
     return MF3D_E_INVALID;
   }
-  if (prm->precision != MF3D_PREC_FP64 || prm->lsm || prm->solver == 1 || prm->bounds) {
-    set_error("LMR: the V-cycle runs in FP64, without lsm, bounds or solver 1");
+  if (prm->lsm || prm->solver == 1 || prm->bounds) {
+    set_error("LMR: the V-cycle runs without lsm, bounds or solver 1");
     return MF3D_E_UNSUPPORTED;
   }
   std::map<int, int> pos;

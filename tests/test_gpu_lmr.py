@@ -4,8 +4,8 @@ mf3d_mgkcyc_device on layouts whose blocks differ in refinement (rdiv 1
 and 2) against the oracle's mgkcyc: the levels past a block's own last
 (injection and whole-array correction, mgsolver.for:714-727, 806-818) and
 the fine/coarse exchangepp branches; also a chain of rdiv 1, 2 and 4, whose
-finest block halves its refinement on its extra levels.  FP64, bit for bit on pp's interior
-and first ghost layer.  The ring entries of a fine block's face buffer are
+finest block halves its refinement on its extra levels.  FP64 bit for bit on pp's interior
+and first ghost layer; FP32 (coarsest level in FP64) within a stated bar.  The ring entries of a fine block's face buffer are
 0 on both sides; the L-shaped layout, where the V-cycle reads them, also
 shows the cells that do not depend on them (the oracle run with another
 ring value).
@@ -35,7 +35,7 @@ LAYOUTS = [
 ]
 
 
-def run_pair(lib, oracle, cuda, L, scheme, seed=42, ring=0.0):
+def run_pair(lib, oracle, cuda, L, scheme, seed=42, ring=0.0, precision=0):
     import torch
     prm = L.params(mg_itrsch=scheme)
     rng = np.random.default_rng(seed)
@@ -48,7 +48,7 @@ def run_pair(lib, oracle, cuda, L, scheme, seed=42, ring=0.0):
                                  ob.ptr_array(pp_ref)) == 0
     finally:
         oracle.orc_set_lmr_ring(0.0)
-    proj = Projection(L.descriptors(lib), prm, lib)
+    proj = Projection(L.descriptors(lib), L.params(mg_itrsch=scheme, precision=precision), lib)
     su_d = [torch.from_numpy(a).to(cuda) for a in su]
     pp_d = [torch.zeros(L.ttc(b), dtype=torch.float64, device=cuda) for b in range(L.nblocks)]
     proj.mgkcyc_device(su_d, pp_d)
@@ -95,10 +95,8 @@ def test_lmr_ring_independent_cells(lib, oracle, cuda):
 
 def test_lmr_refusals(lib, cuda):
     """The outer loop refuses an LMR context (its field exchanges at
-    refinement interfaces are not restated); FP32 and neighbours more than
-    2:1 apart are refused at create."""
+    refinement interfaces are not restated)."""
     import torch
-    from multiflow3d_b200 import abi
     L = LmrLayout(2, 1, 1, 8, [1], ALL_WALLS, 3)
     proj = Projection(L.descriptors(lib), L.params(), lib)
     fields = [{k: torch.zeros(L.ttc(b), dtype=torch.float64, device=cuda)
@@ -106,8 +104,29 @@ def test_lmr_refusals(lib, cuda):
     with pytest.raises(RuntimeError, match="LMR"):
         proj.newsolv_mg_device(fields)
     proj.close()
-    with pytest.raises(RuntimeError):
-        Projection(L.descriptors(lib), L.params(precision=abi.MF3D_PREC_FP32), lib)
+
+
+FP32_BAR = 2e-5
+
+
+@pytest.mark.parametrize("scheme", [3, 1, 2])
+@pytest.mark.parametrize("lay", LAYOUTS, ids=lambda d: f"{d['px']}x{d['py']}x{d['pz']}-n{d['n']}-ref"
+                         + "-".join(map(str, d['refine'])) + ("-L" if d.get("drop") else ""))
+def test_lmr_vcycle_fp32(lib, oracle, cuda, lay, scheme):
+    """The FP32 V-cycle (coarsest level in FP64) on the LMR layouts against
+    the FP64 oracle: pp within FP32_BAR of the largest |pp| on every block,
+    cells of levels past a block's own and across refinement interfaces
+    included."""
+    from multiflow3d_b200 import abi
+    L = LmrLayout(lay["px"], lay["py"], lay["pz"], lay["n"], lay["refine"], lay["bc"], 3, drop=lay.get("drop", ()))
+    got, ref, launches = run_pair(lib, oracle, cuda, L, scheme, precision=abi.MF3D_PREC_FP32)
+    assert launches > 0
+    scale = max(np.abs(r).max() for r in ref)
+    assert scale > 0
+    for b in range(L.nblocks):
+        err = np.abs(got[b] - ref[b]).max()
+        assert err <= FP32_BAR * scale, f"block {b}: {err / scale:.3e} of max |pp|"
+    assert any(not np.array_equal(g, r) for g, r in zip(got, ref))  # the FP32 path ran: its rounding shows
 
 
 def test_lmr_vcycle_random_layouts(lib, oracle, cuda):

@@ -302,14 +302,14 @@ def test_library_lmr_refresh_matches_oracle(lib, orc, lay):
 
 def test_library_lmr_plan_refusals(lib):
     """mf3d_create checks an LMR layout before it touches the device
-    (alloc_dom.for:12-230 and the restated scope): FP32, periodic partners
+    (alloc_dom.for:12-230 and the restated scope): lsm, periodic partners
     of different refinement, neighbours more than 2:1 apart, and spacings
     that are not powers of two of one another are refused with no GPU."""
-    from multiflow3d_b200 import abi
     ctx = C.c_void_p()
     L = LmrLayout(2, 1, 1, 8, [1], ALL_WALLS, 3)
     d = L.descriptors(lib)
-    p = L.params(precision=abi.MF3D_PREC_FP32)
+    p = L.params()
+    p.lsm = 1
     assert lib.mf3d_create(d, L.nblocks, C.byref(p), C.byref(ctx)) == -6  # MF3D_E_UNSUPPORTED
     assert b"LMR" in lib.mf3d_last_error()
     Lp = LmrLayout(2, 1, 1, 8, [1], (PERIODIC, PERIODIC, WALL, WALL, WALL, WALL), 3)
