@@ -488,25 +488,34 @@ def run_lmr(args):
     su_h = [rng.uniform(-1, 1, size=sh) for sh in shapes]
     su = [torch.from_numpy(a).to(dev) for a in su_h]
     pp = [torch.zeros(sh, dtype=torch.float64, device=dev) for sh in shapes]
-    proj = Projection(desc, prm, lib)
 
-    def once():
-        for t in pp:
-            t.zero_()
-        proj.mgkcyc_device(su, pp)
+    def timed(precision):
+        prm.precision = precision
+        proj = Projection(desc, prm, lib)
 
-    for _ in range(args.warmup):
-        once()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.steps):
-        once()
-    e1.record()
-    torch.cuda.synchronize()
-    sec = e0.elapsed_time(e1) / 1e3
-    launches = proj.launches
-    proj.close()
+        def once():
+            for t in pp:
+                t.zero_()
+            proj.mgkcyc_device(su, pp)
+
+        for _ in range(args.warmup):
+            once()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            once()
+        e1.record()
+        torch.cuda.synchronize()
+        launches = proj.launches
+        proj.close()
+        prm.precision = abi.MF3D_PREC_FP64
+        return e0.elapsed_time(e1) / 1e3, launches
+
+    # the FP32 V-cycle (coarsest level in FP64) first: pp then holds its result
+    sec32, _ = timed(abi.MF3D_PREC_FP32)
+    pp32 = [t.cpu().numpy() for t in pp]
+    sec, launches = timed(abi.MF3D_PREC_FP64)
     cells = sum(desc[b].nx * desc[b].ny * desc[b].nz for b in range(8))
     value = args.steps / sec
     line = {
@@ -516,6 +525,8 @@ def run_lmr(args):
         "config": {"workload": f"LMR 2:1: 2x2x2 unit blocks, one at {2 * n}^3 beside seven {n}^3 ({cells / 1e6:.1f} M "
                                f"cells), walls, 6 levels, RB-GS(2,1), one V-cycle (mgkcyc) per step"},
         "gpu_launches_per_step": launches,
+        "fp32_vcycle": {"value": args.steps / sec32, "unit": "V-cycles/s",
+                        "note": "the same V-cycle in FP32, coarsest level in FP64"},
     }
     if not args.no_cpu_baseline:
         orc = oracle_lib()
@@ -538,6 +549,9 @@ def run_lmr(args):
         proj2.mgkcyc_device(su, pp)
         proj2.close()
         line["bitwise_vs_oracle"] = all(np.array_equal(pp[b].cpu().numpy(), pp_h[b]) for b in range(8))
+        # the FP32 V-cycle's largest deviation from the FP64 oracle, over max |pp|
+        scale = max(np.abs(a).max() for a in pp_h)
+        line["fp32_vcycle"]["max_err_rel_to_max_pp"] = max(np.abs(pp32[b] - pp_h[b]).max() for b in range(8)) / scale
     print(json.dumps(line), flush=True)
     return 0
 
