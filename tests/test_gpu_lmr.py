@@ -148,3 +148,15 @@ def test_lmr_vcycle_ghost_widths(lib, oracle, cuda, pl):
     got, ref, _ = run_pair(lib, oracle, cuda, L, 3, seed=pl)
     for b in range(L.nblocks):
         assert np.array_equal(got[b], ref[b])
+
+
+def test_lmr_vcycle_fp32_random_layouts(lib, oracle, cuda):
+    """The FP32 V-cycle on the 12 seeded random LMR layouts, the three
+    smoothers in turn: pp within FP32_BAR of max |pp| of the FP64 oracle."""
+    from lmr_layouts import random_layouts
+    from multiflow3d_b200 import abi
+    for q, L in enumerate(random_layouts(4242, 12)):
+        got, ref, _ = run_pair(lib, oracle, cuda, L, (3, 1, 2)[q % 3], seed=q, precision=abi.MF3D_PREC_FP32)
+        scale = max(np.abs(r).max() for r in ref)
+        for b in range(L.nblocks):
+            assert np.abs(got[b] - ref[b]).max() <= FP32_BAR * scale, (L.pos, L.refine, L.bc, b)
